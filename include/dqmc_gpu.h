@@ -1,0 +1,161 @@
+/*
+ * dqmc_gpu.h -- C ABI of the B200 (sm_100a) DQMC sweep library
+ * (sunhubbardmy_b200/_lib/libdqmc_gpu.so).
+ *
+ * Drop-in boundary for the finite-temperature sweep of sun-hubbard
+ * (YuanyueChen/sunhubbardmy).  In the reference the path is reached through
+ * Fortran module procedures (no FFI exists); each entry point below names the
+ * reference routine whose effect it reproduces, so a Fortran iso_c_binding
+ * shim can replace them one by one.
+ *
+ * Conventions
+ *  - Matrices are complex128, column-major (Fortran layout), passed as
+ *    interleaved double (re, im) arrays of 2*N*N doubles.
+ *  - The HS field conf is int32 [ltrot][nsites] with the site index fastest
+ *    and values 1..lcomp, i.e. the memory of uconf%conf(nsites, ltrot)
+ *    (src/dqmc_config_u.f90:11).
+ *  - Every function returns 0 on success and a negative DQMC_E* code on
+ *    failure; dqmc_gpu_last_error() describes the last failure.  Calls on one
+ *    handle are synchronous and not thread-safe; use one handle per host
+ *    thread.  The caller owns every host buffer; the library owns all device
+ *    state.
+ *  - A handle holds n_chains independent Markov chains (the reference's MPI
+ *    ranks) that are advanced together, one CTA per chain.
+ */
+#ifndef DQMC_GPU_H
+#define DQMC_GPU_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* error codes */
+#define DQMC_OK 0
+#define DQMC_EINVAL (-1)     /* invalid argument / unsupported parameter set */
+#define DQMC_ECUDA (-2)      /* CUDA runtime error */
+#define DQMC_ENOMEM (-3)     /* device allocation failed */
+#define DQMC_ESTATE (-4)     /* call out of order (e.g. sweep before sweep_start) */
+
+/* enums (compile-time RUNMODE flags of src/make.sys.* turned into values) */
+#define DQMC_LATT_SQUARE 1     /* -DSQUARE */
+#define DQMC_LATT_HONEYCOMB 2  /* -DHONEYCOMB */
+#define DQMC_UPD_FAST 0        /* default (no flag) */
+#define DQMC_UPD_DELAY 1       /* -DDELAY */
+#define DQMC_UPD_SUBMATRIX 2   /* -DSUBMATRIX */
+#define DQMC_KIN_CHECKERBOARD 0 /* -DBREAKUP_T */
+#define DQMC_KIN_FFT 1          /* -DFFT (square lattice, l1 == l2) */
+#define DQMC_HS_EXACT 0        /* -DEXACTHS */
+#define DQMC_HS_GENERAL4 1     /* no -DEXACTHS */
+
+/* &model_para and &ctrl_para of dqmc.in (src/model_para.f90:155-218) plus the
+ * compile-time choices.  dqmc_params_derive fills the derived fields. */
+typedef struct dqmc_params {
+    int32_t lattice, l1, l2;
+    double beta, dtau, rt, t2, t3, nu, mu, rhub, rv, alpha, theta;
+    double xmag, flux_x, flux_y, dimer, rndness;
+    int32_t nflr, lproju, lstabilize;
+    int32_t nwrap, nsweep, nbin, nublock;
+    int32_t update, kinetic, hs;
+    /* derived (src/model_para.f90:334-453) */
+    int32_t ndim, lq, ltrot, nst, ne, lcomp;
+} dqmc_params;
+
+/* per-chain diagnostics (src/dqmc_util.f90:15-57, 287-299) */
+typedef struct dqmc_diag {
+    double phase_re, phase_im;          /* phase of the determinant weight */
+    double logweight_re, logweight_im;  /* logweightf */
+    double max_wrap_error;              /* max |G_scratch - G_wrapped| */
+    double max_phasediff;
+    double avglog10error_sum;           /* sum of log10(wrap error) */
+    double logcount;                    /* number of wrap checks */
+    double avgexpphasediff_sum;
+    double accepted, proposed;          /* main_obs(3) */
+    double nobs;                        /* measurements in the current bin */
+} dqmc_diag;
+
+typedef struct dqmc_handle dqmc_handle;
+
+/* Derive ndim, lq, ltrot, nst, ne, lcomp and the default nublock exactly as
+ * make_tables does (src/model_para.f90:334-453). */
+int dqmc_params_derive(dqmc_params* p);
+
+/* Create n_chains chains on the current CUDA device.  params points to
+ * n_params parameter sets; chain c uses params[c % n_params] (all sets must
+ * share beta, dtau and nwrap).  seeds[c] seeds chain c's SFMT generator
+ * (spring_sfmt_init, lib/m_spring.f90:187); if draw_conf is nonzero the HS
+ * field is drawn from it as dqmc_input_conf does for a fresh start
+ * (src/dqmc_config_u/dqmc_input_conf.f90:55-63).  Replaces dqmc_start's
+ * set_h0conf / set_conf / input_conf / allocate_core (src/dqmc_ft_ctrl.f90:9-45). */
+int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_chains, const int32_t* seeds,
+                    int draw_conf, dqmc_handle** out);
+int dqmc_gpu_destroy(dqmc_handle* h);
+const char* dqmc_gpu_last_error(void);
+
+/* HS field of one chain (uconf%conf; input_conf / output_conf). */
+int dqmc_gpu_set_conf(dqmc_handle* h, int chain, const int32_t* conf);
+int dqmc_gpu_get_conf(dqmc_handle* h, int chain, int32_t* conf);
+/* all chains at once: conf arrays concatenated chain after chain */
+int dqmc_gpu_set_conf_all(dqmc_handle* h, const int32_t* conf);
+int dqmc_gpu_get_conf_all(dqmc_handle* h, int32_t* conf);
+
+/* Equal-time Green's function G = <c c^+> of one chain (gf%blk1). */
+int dqmc_gpu_get_green(dqmc_handle* h, int chain, double* g);
+int dqmc_gpu_set_green(dqmc_handle* h, int chain, const double* g);
+
+/* dqmc_ft_sweep_start_0b (src/dqmc_ft_core/dqmc_ft_sweep_start_0b.f90): UDV
+ * stack 0 -> beta and G(beta, beta). */
+int dqmc_gpu_sweep_start(dqmc_handle* h);
+/* dqmc_ft_sweep_b0 / dqmc_ft_sweep_0b (src/dqmc_ft_core/dqmc_ft_sweep_*.f90)
+ * with lupdate / lmeasure_equaltime (lmeasure_dyn = .false.). */
+int dqmc_gpu_sweep_b0(dqmc_handle* h, int lupdate, int lmeasure);
+int dqmc_gpu_sweep_0b(dqmc_handle* h, int lupdate, int lmeasure);
+/* n x (sweep_b0 + sweep_0b) with updates, the body of dqmc_sweep
+ * (src/dqmc_ft_ctrl.f90:80-126) without the bin output. */
+int dqmc_gpu_sweeps(dqmc_handle* h, int n, int lmeasure);
+
+/* obser_init (src/dqmc_measure_2d.f90:105-130) and the per-chain bin sums of
+ * equaltime_measure before the MPI reduction of equaltime_output.  Layout of
+ * out (complex, 2 doubles each): energy_bin[10], zcpcm, zspsm, znn,
+ * pair_onsite [lq*4 each, index d + lq*(no_i + 2*no_j), d = imj - 1],
+ * zjj, zbb, pair_nn, pair_sn [lq each], zn[2], zj, zb; nbins() complex. */
+int dqmc_gpu_obser_init(dqmc_handle* h);
+int dqmc_gpu_nbins(dqmc_handle* h, int chain);
+int dqmc_gpu_get_bins(dqmc_handle* h, int chain, double* out);
+int dqmc_gpu_get_diag(dqmc_handle* h, int chain, dqmc_diag* out);
+int dqmc_gpu_reset_diag(dqmc_handle* h);
+
+/* Operator-level entry points of the reference's type-bound procedures
+ * (h0conf / uconf, src/dqmc_config_h0.f90:6-31, src/dqmc_config_u.f90:5-29),
+ * acting on each chain's current G.  op: 0 left_forward, 1 left_backward,
+ * 2 right_forward, 3 right_backward, 4 left_forward_hc; nf: bond family
+ * (checkerboard, 1-based; ignored for FFT); nt: time slice (1-based). */
+int dqmc_gpu_h0_prop(dqmc_handle* h, int op, int nf);
+int dqmc_gpu_u_prop(dqmc_handle* h, int op, int nt);
+/* uconf%update(gf, nt): local updates of slice nt on each chain's G
+ * (dqmc_update*.f90).  Consumes 2*nsites draws per chain. */
+int dqmc_gpu_update(dqmc_handle* h, int nt);
+/* equaltime_measure(nt, gf, gfc) on each chain's current G. */
+int dqmc_gpu_measure(dqmc_handle* h);
+/* set the determinant phase of a chain (global `phase` of model_para) */
+int dqmc_gpu_set_phase(dqmc_handle* h, int chain, double re, double im);
+/* raw SFMT draws (spring_sfmt_source) of a chain, advancing its generator */
+int dqmc_gpu_draw_u32(dqmc_handle* h, int chain, int count, uint32_t* out);
+
+/* Diagnostics: batched complex GEMM C = op(A) op(B) + beta C on per-chain
+ * N x N work matrices, and a QR factorisation (R, Q, log det Q) of one; used
+ * by the parity tests of the tensor-core kernels.  Matrices are uploaded and
+ * downloaded through the work-matrix accessors. */
+int dqmc_gpu_set_work(dqmc_handle* h, int chain, int which, const double* m);
+int dqmc_gpu_get_work(dqmc_handle* h, int chain, int which, double* m);
+int dqmc_gpu_test_zgemm(dqmc_handle* h, int m, int n, int k, int opa, int opb, int a, int b, int c, double beta);
+int dqmc_gpu_test_qr(dqmc_handle* h, int a, int q, double* logdetq /* 2 per chain */);
+
+/* Stream-ordered timing helper: average device time (ms) of the last
+ * dqmc_gpu_sweeps call, measured with CUDA events on the library's stream. */
+double dqmc_gpu_last_sweeps_ms(dqmc_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

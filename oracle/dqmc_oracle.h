@@ -1,0 +1,145 @@
+/*
+ * CPU oracle for the DQMC sweep of sun-hubbard (YuanyueChen/sunhubbardmy).
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker that the CUDA path
+ * is compared against, and the timed CPU baseline.  Only tests/, the smoke
+ * check and the cpu_baseline / reference arm of bench.py may load it.  The
+ * product library (sunhubbardmy_b200) never links, loads or calls it.
+ *
+ * It restates, in plain C99, the Fortran reference's finite-temperature hot
+ * path: SFMT RNG (lib/m_spring.f90), square/honeycomb lattice tables
+ * (src/lattice.f90), HS constants (src/dqmc_config_u/dqmc_set_conf.f90),
+ * kinetic propagators (src/dqmc_config_h0/ directory), local updates
+ * (src/dqmc_config_u/dqmc_update*.f90), the UDV stack
+ * (src/dqmc_ft_core/dqmc_ft_stablize_*.f90, lib/s_matrix.f90), the Green's
+ * functions (src/dqmc_ft_core/green_equaltime*.f90) and the equal-time
+ * measurement (src/dqmc_measure/equaltime_measure.f90).
+ *
+ * Parity status: UNPINNED against reference output.  The reference is Fortran
+ * + MPI + MKL; none of the three exist on either machine, and the reference
+ * ships no golden vectors or stored outputs.  The oracle is pinned instead by
+ * known answers (free-fermion Green's function, atomic limit, an independent
+ * SFMT restatement, scipy LAPACK for the linear-algebra kernels).
+ *
+ * Matrices are column-major complex128 (Fortran layout), indices 0-based
+ * internally; HS-field values are 1..lcomp exactly as in the reference.
+ */
+#ifndef DQMC_ORACLE_H
+#define DQMC_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------- SFMT-19937 (lib/m_spring.f90:187-379) ---------- */
+typedef struct { uint32_t st[624]; int idx; } orc_sfmt;
+void     orc_sfmt_init(orc_sfmt *s, int32_t seed);
+uint32_t orc_sfmt_u32(orc_sfmt *s);
+double   orc_sfmt_stream(orc_sfmt *s);
+int32_t  orc_test_seed(int32_t irank);   /* src/dqmc_util.f90:72 under -DTEST */
+
+/* ---------- parameters (src/model_para.f90 &model_para/&ctrl_para) ---------- */
+enum { ORC_SQUARE = 1, ORC_HONEYCOMB = 2 };
+enum { ORC_FAST = 0, ORC_DELAY = 1, ORC_SUBMATRIX = 2 };
+enum { ORC_CHECKERBOARD = 0, ORC_FFT = 1 };
+enum { ORC_HS_EXACT = 0, ORC_HS_GENERAL4 = 1 };
+
+typedef struct {
+    int32_t lattice, l1, l2;
+    double beta, dtau, rt, t2, t3, nu, mu, rhub, rv, alpha, theta;
+    double xmag, flux_x, flux_y, dimer, rndness;
+    int32_t nflr, lproju, lstabilize;
+    int32_t nwrap, nsweep, nbin, nublock;
+    int32_t update, kinetic, hs;
+} orc_params;
+
+typedef struct orc_model orc_model;
+typedef struct orc_chain orc_chain;
+
+/* Function-pointer hooks for BLAS/LAPACK (Fortran calling convention, no
+ * hidden string lengths, e.g. scipy.linalg.cython_* capsules).  Any NULL
+ * entry falls back to the oracle's own unblocked restatement. */
+typedef void (*orc_zgemm_fn)(const char*, const char*, const int*, const int*, const int*,
+                             const void*, const void*, const int*, const void*, const int*,
+                             const void*, void*, const int*);
+typedef void (*orc_zgeqrf_fn)(const int*, const int*, void*, const int*, void*, void*, const int*, int*);
+typedef void (*orc_zgeqp3_fn)(const int*, const int*, void*, const int*, int*, void*, void*, const int*, double*, int*);
+typedef void (*orc_zungqr_fn)(const int*, const int*, const int*, void*, const int*, const void*, void*, const int*, int*);
+typedef void (*orc_zgetrf_fn)(const int*, const int*, void*, const int*, int*, int*);
+typedef void (*orc_ztrtri_fn)(const char*, const char*, const int*, void*, const int*, int*);
+void orc_set_lapack(orc_zgemm_fn, orc_zgeqrf_fn, orc_zgeqp3_fn, orc_zungqr_fn, orc_zgetrf_fn, orc_ztrtri_fn);
+
+/* ---------- model / chain ---------- */
+orc_model *orc_model_new(const orc_params *p);
+void       orc_model_free(orc_model *m);
+/* derived: ndim, lq, ltrot, nst, nublock, lcomp, nn_nf, nn_lf, nsub, z_plq */
+void orc_model_dims(const orc_model *m, int32_t out[10]);
+/* lattice tables, 1-based values as in src/lattice.f90 (sizes from dims) */
+void orc_model_tables(const orc_model *m, int32_t *nnlist, int32_t *nnlf_list, int32_t *list,
+                      int32_t *imj, int32_t *plq_cord, int32_t *snlist);
+/* HS constants: bmat[lcomp], bmat_inv[lcomp], delta[(lcomp-1)*lcomp], phase[lcomp],
+ * phase_ratio[(lcomp-1)*lcomp], gaml[lcomp], etal[lcomp], alpha */
+void orc_model_hs(const orc_model *m, double *bmat, double *bmat_inv, double *delta,
+                  double *phase, double *phase_ratio, double *gaml, double *etal, double *alpha);
+/* kinetic: urt/urtm1 [nn_nf*nn_lf][2][2] complex (bond-major, Fortran (ist,i,j)) or exph0k */
+void orc_model_kinetic(const orc_model *m, double *urt, double *urtm1, double *exph0k, double *exph0kinv);
+/* dense hopping matrix h0mat (seth0) */
+void orc_model_h0mat(const orc_model *m, double *h0);
+
+orc_chain *orc_chain_new(const orc_model *m, int32_t seed, int draw_conf);
+void       orc_chain_free(orc_chain *c);
+void orc_chain_set_conf(orc_chain *c, const int32_t *conf);
+void orc_chain_get_conf(const orc_chain *c, int32_t *conf);
+void orc_chain_set_green(orc_chain *c, const double *g);
+void orc_chain_get_green(const orc_chain *c, double *g);
+void orc_chain_set_phase(orc_chain *c, double re, double im);
+/* diag: [0]=phase.re [1]=phase.im [2]=logw.re [3]=logw.im [4]=max_wrap_error
+ * [5]=max_phasediff [6]=avglog10error [7]=logcount [8]=accepted [9]=proposed */
+void orc_chain_get_diag(const orc_chain *c, double *out);
+double orc_chain_uniform(orc_chain *c);
+
+/* drivers (src/dqmc_ft_core/ directory) */
+int  orc_sweep_start_0b(orc_chain *c);
+int  orc_sweep_b0(orc_chain *c, int lupdate, int lmeasure);
+int  orc_sweep_0b(orc_chain *c, int lupdate, int lmeasure);
+void orc_obser_init(orc_chain *c);
+
+/* operator-level entry points acting on an explicit N x N matrix */
+enum { ORC_LEFT_FORWARD = 0, ORC_LEFT_BACKWARD = 1, ORC_RIGHT_FORWARD = 2,
+       ORC_RIGHT_BACKWARD = 3, ORC_LEFT_FORWARD_HC = 4 };
+void orc_h0_prop(const orc_model *m, int op, int nf, double *g, int n2);
+void orc_u_prop(const orc_model *m, const int32_t *conf, int op, int nt, double *g, int n2);
+void orc_bmat_left_forward(const orc_chain *c, int nt1, int nt2, double *g);
+void orc_bmat_left_forward_hc(const orc_chain *c, int nt1, int nt2, double *g);
+/* one local update of slice nt (1-based) on the chain's G with its RNG;
+ * writes the accept flags of each site to acc (may be NULL) */
+void orc_update(orc_chain *c, int nt, int32_t *acc);
+/* one equal-time measurement of the chain's current G */
+void orc_measure(orc_chain *c, int nt);
+/* stack access: which=0 U, 1 V; D and logdetQ */
+void orc_stack_get(const orc_chain *c, int n, double *u, double *d, double *v, double *logdetq);
+void orc_stack_set(orc_chain *c, int n, const double *u, const double *d, const double *v, const double *logdetq);
+void orc_stablize_0b(orc_chain *c, int n);
+void orc_stablize_b0(orc_chain *c, int n);
+/* green_equaltime with explicit operands */
+int  orc_green_equaltime(int n, const double *ur, const double *dr, const double *vr,
+                         const double *vl, const double *dl, const double *ul,
+                         double *g, const double *logdetqr, const double *logdetql, double *logw);
+
+/* bins: energy[20] (10 complex), nobs, then the per-array bins */
+int  orc_bins_size(const orc_model *m);
+void orc_get_bins(const orc_chain *c, double *out);
+
+/* linear-algebra restatements exposed for pinning against LAPACK */
+void   orc_zgeqr2(int m, int n, double *a, int lda, double *tau);
+void   orc_zgeqp2(int m, int n, double *a, int lda, int32_t *jpvt, double *tau);
+void   orc_zung2r(int m, int n, int k, double *a, int lda, const double *tau);
+int    orc_zgetf2(int m, int n, double *a, int lda, int32_t *ipiv);
+void   orc_zmcpt(int rdim, int cdim, double *a, int32_t *jpvt);
+void   orc_inv_logdet_lu(int n, double *a, double *logdet);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,82 @@
+/* Internal declarations shared by the oracle's C files.  Test infrastructure
+ * only (see dqmc_oracle.h). */
+#ifndef ORC_INTERNAL_H
+#define ORC_INTERNAL_H
+#include <complex.h>
+#include <stdint.h>
+#include "dqmc_oracle.h"
+
+typedef double _Complex zc;
+#define ZIDX(i, j, ld) ((size_t)(i) + (size_t)(j) * (size_t)(ld))
+
+typedef struct {
+    int kind, l1, l2, ncell, nsub, nsites, z_plq, nn_nf, nn_lf, nsn;
+    double a1[2], a2[2], b1[2], b2[2];
+    int *ulist;      /* [ncell][2] 1-based cell coordinates, ulist[c*2+d]        */
+    int *list;       /* [nsites][2] (cell, orb), 1-based values                  */
+    int *cord;       /* [nsites][2] cell coordinates                              */
+    double *rcord;   /* [nsites][2]                                               */
+    int *nnlist;     /* [nsites][nn_nf] 1-based neighbour (nnlist[i*nn_nf+nf])    */
+    int *snlist;     /* [nsites][nsn]                                             */
+    int *nnlf_list;  /* [nn_lf] 1-based A sites                                   */
+    int *nnveci;     /* [nsites][nn_nf][2]                                        */
+    double *nnvecr;  /* [nsites][nn_nf][2]                                        */
+    int *imj;        /* [ncell][ncell] imj[i*ncell+j] = imj(i,j), 1-based         */
+    int *plq_cord;   /* [ncell][z_plq] plq_cord[id*z_plq+k] = plq_cord(k,id)      */
+    int *listk;      /* [ncell][2]                                                */
+    zc *zexpiqr;     /* [ncell(site)][ncell(k)] zexpiqr(nk,i) at [i*ncell+nk]    */
+} orc_latt;
+
+int  orc_latt_build(orc_latt *L, int kind, int l1, int l2);
+void orc_latt_free(orc_latt *L);
+zc   orc_expar(const orc_latt *L, int i, int nf, double xmag, double fx, double fy, double dimer);
+
+struct orc_model {
+    orc_params p;
+    orc_latt L;
+    int ndim, lq, ltrot, nst, nublock, ne;
+    int lwrapT, lwrapu;
+    int *iwrap_nt;   /* [ltrot+1] */
+    int *wrap_step;  /* [nst][2] 1-based slice range */
+    /* HS constants */
+    int lcomp;
+    double hs_alpha;
+    double etal[4], gaml[4];
+    zc bmat[4], bmat_inv[4], phase[4];
+    zc delta[3 * 4], phase_ratio[3 * 4];   /* [(is-1)*(lcomp-1) + (iflip-1)] */
+    /* kinetic */
+    zc *urt, *urtm1;          /* [ist][2][2] with urt[ist*4 + (i-1)*2 + (j-1)] */
+    zc *exph0k, *exph0kinv;   /* [lq] */
+    zc *h0mat;                /* [N*N] */
+    zc *expar_nn;             /* [nsites][nn_nf] */
+};
+
+struct orc_chain {
+    const orc_model *m;
+    orc_sfmt rng;
+    int32_t *conf;            /* [ltrot][nsites], site fastest */
+    zc *gf, *gfc;             /* N*N */
+    zc **Ust, **Vst;          /* (nst+1) of N*N */
+    double **Dst;
+    zc *logdetQst;
+    zc phase, logweightf;
+    double max_wrap_error, max_phasediff, avglog10error, avgexpphasediff, logcount;
+    double acc_u, prop_u;
+    /* bins */
+    int nobs;
+    zc energy_bin[10];
+    zc *zcpcm_bin, *zspsm_bin, *znn_bin, *pair_onsite_bin;  /* [lq][2][2] */
+    zc *zjj_bin, *zbb_bin, *pair_nn_bin, *pair_sn_bin;       /* [lq] */
+    zc zn_bin[2], zj_bin, zb_bin;
+};
+
+/* linear algebra helpers (orc_linalg.c) */
+void orc_zgemm(char ta, char tb, int m, int n, int k, zc alpha, const zc *a, int lda,
+               const zc *b, int ldb, zc beta, zc *c, int ldc);
+void orc_qr_logdet(int n, zc *a, zc *q, zc *r, zc *logdet);                 /* s_zgeQR_logdetQ */
+void orc_qrpt_logdet(int n, zc *a, zc *q, zc *r, int32_t *jpvt, zc *logdet); /* s_zgeQRPT_logdetQ */
+void orc_zinv_logdet(int n, zc *a, zc *logdet);                              /* s_inv_logdet_lu_z */
+void orc_zinv(int n, zc *a);                                                 /* s_invlu_z */
+double orc_dznrm2(int n, const zc *x, int incx);
+
+#endif

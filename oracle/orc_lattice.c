@@ -1,0 +1,262 @@
+/* Square and honeycomb lattice tables, restated from src/lattice.f90
+ * (setup_latt2d_sub 386-491, setup_honeycomb_sub 611-776,
+ * setup_square_sub 792-961) and the hopping phase expar
+ * (src/dqmc_config_h0/expar.f90).  Test infrastructure only.
+ * Stored values are 1-based as in the reference. */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include "orc_internal.h"
+
+static int npbc(int nr, int l) {   /* lattice.f90:493-500 */
+    if (nr > l) return nr - l;
+    if (nr < 1) return nr + l;
+    return nr;
+}
+
+void orc_latt_free(orc_latt *L) {
+    free(L->ulist); free(L->list); free(L->cord); free(L->rcord); free(L->nnlist);
+    free(L->snlist); free(L->nnlf_list); free(L->nnveci); free(L->nnvecr); free(L->imj);
+    free(L->plq_cord); free(L->listk); free(L->zexpiqr);
+    memset(L, 0, sizeof(*L));
+}
+
+static void setup_2d(orc_latt *L, int l1, int l2, const double a1[2], const double a2[2]) {
+    L->l1 = l1; L->l2 = l2; L->ncell = l1 * l2;
+    L->a1[0] = a1[0]; L->a1[1] = a1[1]; L->a2[0] = a2[0]; L->a2[1] = a2[1];
+    int nc = L->ncell;
+    L->ulist = malloc(sizeof(int) * 2 * nc);
+    for (int i1 = 1; i1 <= l1; ++i1)
+        for (int i2 = 1; i2 <= l2; ++i2) {
+            int c = i2 + (i1 - 1) * l2 - 1;
+            L->ulist[c * 2 + 0] = i1;
+            L->ulist[c * 2 + 1] = i2;
+        }
+    /* lattice reciprocal vectors b = 2 pi [l1 a1, l2 a2]^{-1} */
+    double m11 = l1 * a1[0], m12 = l1 * a1[1], m21 = l2 * a2[0], m22 = l2 * a2[1];
+    double x = m11 * m22 - m21 * m12;
+    double i11 = m22 / x, i22 = m11 / x, i12 = -m12 / x, i21 = -m21 / x;
+    L->b1[0] = 2 * M_PI * i11; L->b1[1] = 2 * M_PI * i21;
+    L->b2[0] = 2 * M_PI * i12; L->b2[1] = 2 * M_PI * i22;
+    L->listk = malloc(sizeof(int) * 2 * nc);
+    int k = 0;
+    for (int m = -(l1 + 1) / 2 + 1; m <= l1 / 2; ++m)
+        for (int n = -(l2 + 1) / 2 + 1; n <= l2 / 2; ++n) {
+            L->listk[k * 2 + 0] = m; L->listk[k * 2 + 1] = n; ++k;
+        }
+    L->imj = malloc(sizeof(int) * nc * nc);
+    for (int j = 0; j < nc; ++j)
+        for (int i = 0; i < nc; ++i) {
+            int nx = npbc(L->ulist[i * 2] - L->ulist[j * 2], l1);
+            int ny = npbc(L->ulist[i * 2 + 1] - L->ulist[j * 2 + 1], l2);
+            L->imj[i * nc + j] = ny + (nx - 1) * l2;
+        }
+    L->zexpiqr = malloc(sizeof(zc) * nc * nc);
+    for (int i = 0; i < nc; ++i) {
+        double ax = L->ulist[i * 2] * a1[0] + L->ulist[i * 2 + 1] * a2[0];
+        double ay = L->ulist[i * 2] * a1[1] + L->ulist[i * 2 + 1] * a2[1];
+        for (int nk = 0; nk < nc; ++nk) {
+            double kx = L->listk[nk * 2] * L->b1[0] + L->listk[nk * 2 + 1] * L->b2[0];
+            double ky = L->listk[nk * 2] * L->b1[1] + L->listk[nk * 2 + 1] * L->b2[1];
+            L->zexpiqr[i * nc + nk] = cexp(I * (kx * ax + ky * ay));
+        }
+    }
+}
+
+static void setup_square(orc_latt *L, int l1, int l2) {
+    const double a1[2] = {1.0, 0.0}, a2[2] = {0.0, 1.0};
+    setup_2d(L, l1, l2, a1, a2);
+    L->kind = ORC_SQUARE; L->nsub = 1; L->nsites = l1 * l2; L->z_plq = 4;
+    L->nn_nf = 4; L->nn_lf = l1 * l2 / 2; L->nsn = 4;
+    int ns = L->nsites;
+    L->cord = malloc(sizeof(int) * 2 * ns);
+    L->rcord = malloc(sizeof(double) * 2 * ns);
+    L->nnlf_list = malloc(sizeof(int) * L->nn_lf);
+    L->list = malloc(sizeof(int) * 2 * ns);
+    int ind = 0;
+    for (int i1 = 1; i1 <= l1; ++i1)
+        for (int i2 = 1; i2 <= l2; ++i2) {
+            int s = i2 + (i1 - 1) * l2 - 1;
+            L->list[s * 2] = s + 1; L->list[s * 2 + 1] = 1;
+            L->rcord[s * 2] = i1; L->rcord[s * 2 + 1] = i2;
+            if ((i1 + i2) % 2 == 0) L->nnlf_list[ind++] = s + 1;
+        }
+    memcpy(L->cord, L->ulist, sizeof(int) * 2 * ns);
+    L->nnvecr = malloc(sizeof(double) * ns * 4 * 2);
+    L->nnveci = malloc(sizeof(int) * ns * 4 * 2);
+    static const int v[4][2] = {{1, 0}, {0, 1}, {-1, 0}, {0, -1}};
+    for (int i = 0; i < ns; ++i)
+        for (int nf = 0; nf < 4; ++nf) {
+            L->nnvecr[(i * 4 + nf) * 2] = v[nf][0]; L->nnvecr[(i * 4 + nf) * 2 + 1] = v[nf][1];
+            L->nnveci[(i * 4 + nf) * 2] = v[nf][0]; L->nnveci[(i * 4 + nf) * 2 + 1] = v[nf][1];
+        }
+    L->nnlist = malloc(sizeof(int) * ns * 4);
+    L->snlist = malloc(sizeof(int) * ns * 4);
+    for (int i = 0; i < L->ncell; ++i) {
+        int u1 = L->ulist[i * 2], u2 = L->ulist[i * 2 + 1];
+#define SQ(d1, d2) ((npbc(u1 + (d1), l1) - 1) * l2 + npbc(u2 + (d2), l2))
+        L->nnlist[i * 4 + 0] = SQ(1, 0);
+        L->nnlist[i * 4 + 1] = SQ(0, 1);
+        L->nnlist[i * 4 + 2] = SQ(-1, 0);
+        L->nnlist[i * 4 + 3] = SQ(0, -1);
+        L->snlist[i * 4 + 0] = SQ(1, 1);
+        L->snlist[i * 4 + 1] = SQ(-1, 1);
+        L->snlist[i * 4 + 2] = SQ(-1, -1);
+        L->snlist[i * 4 + 3] = SQ(1, -1);
+#undef SQ
+    }
+    /* plaquettes: A (odd,odd), B (even,odd), C (even,even), D (odd,even) */
+    L->plq_cord = malloc(sizeof(int) * 4 * L->ncell);
+    int nd[4] = {0, 0, 0, 0};
+    for (int i1 = 1; i1 <= l1; ++i1)
+        for (int i2 = 1; i2 <= l2; ++i2) {
+            int t = (i1 % 2 == 1 && i2 % 2 == 1) ? 0 : (i1 % 2 == 0 && i2 % 2 == 1) ? 1
+                  : (i1 % 2 == 0 && i2 % 2 == 0) ? 2 : 3;
+            nd[t]++;
+        }
+    int id[4] = {0, 0, 0, 0};
+    for (int i1 = 1; i1 <= l1; ++i1)
+        for (int i2 = 1; i2 <= l2; ++i2) {
+            int t = (i1 % 2 == 1 && i2 % 2 == 1) ? 0 : (i1 % 2 == 0 && i2 % 2 == 1) ? 1
+                  : (i1 % 2 == 0 && i2 % 2 == 0) ? 2 : 3;
+            int off = 0;
+            for (int q = 0; q < t; ++q) off += nd[q];
+            int pid = ++id[t] + off - 1;
+#define INV(a, b) ((b) + ((a) - 1) * l2)
+            L->plq_cord[pid * 4 + 0] = INV(i1, i2);
+            L->plq_cord[pid * 4 + 1] = INV(npbc(i1 + 1, l1), i2);
+            L->plq_cord[pid * 4 + 2] = INV(npbc(i1 + 1, l1), npbc(i2 + 1, l2));
+            L->plq_cord[pid * 4 + 3] = INV(i1, npbc(i2 + 1, l2));
+#undef INV
+        }
+}
+
+static void setup_honeycomb(orc_latt *L, int l1, int l2) {
+    const double a1[2] = {0.5, -0.5 * sqrt(3.0)}, a2[2] = {0.5, 0.5 * sqrt(3.0)};
+    setup_2d(L, l1, l2, a1, a2);
+    L->kind = ORC_HONEYCOMB; L->nsub = 2; L->nsites = l1 * l2 * 2; L->z_plq = 6;
+    L->nn_nf = 3; L->nn_lf = l1 * l2; L->nsn = 6;
+    int ns = L->nsites;
+    L->cord = malloc(sizeof(int) * 2 * ns);
+    L->rcord = malloc(sizeof(double) * 2 * ns);
+    L->nnlf_list = malloc(sizeof(int) * L->nn_lf);
+    L->list = malloc(sizeof(int) * 2 * ns);
+    for (int i = 0; i < L->nn_lf; ++i) L->nnlf_list[i] = 2 * (i + 1) - 1;
+    int ind = 0;
+    for (int i1 = 1; i1 <= l1; ++i1)
+        for (int i2 = 1; i2 <= l2; ++i2)
+            for (int o = 1; o <= 2; ++o) {
+                int s = ind++;
+                L->list[s * 2] = i2 + (i1 - 1) * l2; L->list[s * 2 + 1] = o;
+                L->cord[s * 2] = i1; L->cord[s * 2 + 1] = i2;
+                if (o == 1) { L->rcord[s * 2] = i1; L->rcord[s * 2 + 1] = i2; }
+                else { L->rcord[s * 2] = i1 - 1.0 / 3.0; L->rcord[s * 2 + 1] = i2 + 1.0 / 3.0; }
+            }
+    L->nnvecr = malloc(sizeof(double) * ns * 3 * 2);
+    L->nnveci = malloc(sizeof(int) * ns * 3 * 2);
+    static const double vrA[3][2] = {{-1.0 / 3, 1.0 / 3}, {2.0 / 3, 1.0 / 3}, {-1.0 / 3, -2.0 / 3}};
+    static const int viA[3][2] = {{0, 0}, {1, 0}, {0, -1}};
+    static const double vrB[3][2] = {{1.0 / 3, -1.0 / 3}, {-2.0 / 3, -1.0 / 3}, {1.0 / 3, 2.0 / 3}};
+    static const int viB[3][2] = {{0, 0}, {-1, 0}, {0, 1}};
+    for (int i = 0; i < ns; ++i)
+        for (int nf = 0; nf < 3; ++nf) {
+            int isA = (i % 2 == 0);
+            L->nnvecr[(i * 3 + nf) * 2] = isA ? vrA[nf][0] : vrB[nf][0];
+            L->nnvecr[(i * 3 + nf) * 2 + 1] = isA ? vrA[nf][1] : vrB[nf][1];
+            L->nnveci[(i * 3 + nf) * 2] = isA ? viA[nf][0] : viB[nf][0];
+            L->nnveci[(i * 3 + nf) * 2 + 1] = isA ? viA[nf][1] : viB[nf][1];
+        }
+    L->nnlist = malloc(sizeof(int) * ns * 3);
+    L->snlist = malloc(sizeof(int) * ns * 6);
+    for (int i = 0; i < ns; ++i) {
+        int c1 = L->cord[i * 2], c2 = L->cord[i * 2 + 1], i1 = i + 1;
+#define HC(d1, d2) (((npbc(c1 + (d1), l1) - 1) * l2 + npbc(c2 + (d2), l2)) * 2)
+        if (i1 % 2 == 1) {
+            L->nnlist[i * 3 + 0] = i1 + 1;
+            L->nnlist[i * 3 + 1] = HC(1, 0);
+            L->nnlist[i * 3 + 2] = HC(0, -1);
+            L->snlist[i * 6 + 0] = HC(1, 1) - 1;
+            L->snlist[i * 6 + 1] = HC(1, 0) - 1;
+            L->snlist[i * 6 + 2] = HC(0, -1) - 1;
+            L->snlist[i * 6 + 3] = HC(-1, -1) - 1;
+            L->snlist[i * 6 + 4] = HC(-1, 0) - 1;
+            L->snlist[i * 6 + 5] = HC(0, 1) - 1;
+        } else {
+            L->nnlist[i * 3 + 0] = i1 - 1;
+            L->nnlist[i * 3 + 1] = HC(-1, 0) - 1;
+            L->nnlist[i * 3 + 2] = HC(0, 1) - 1;
+            L->snlist[i * 6 + 0] = HC(1, 1);
+            L->snlist[i * 6 + 1] = HC(1, 0);
+            L->snlist[i * 6 + 2] = HC(0, -1);
+            L->snlist[i * 6 + 3] = HC(-1, -1);
+            L->snlist[i * 6 + 4] = HC(-1, 0);
+            L->snlist[i * 6 + 5] = HC(0, 1);
+        }
+#undef HC
+    }
+    /* plaquettes: A (i1+i2 mod 3 == 2), B (else), C (== 0) */
+    L->plq_cord = malloc(sizeof(int) * 6 * L->ncell);
+    int nd[3] = {0, 0, 0};
+    for (int i1 = 1; i1 <= l1; ++i1)
+        for (int i2 = 1; i2 <= l2; ++i2) {
+            int r = (i1 + i2) % 3;
+            nd[r == 2 ? 0 : (r == 0 ? 2 : 1)]++;
+        }
+    int id[3] = {0, 0, 0};
+    for (int i1 = 1; i1 <= l1; ++i1)
+        for (int i2 = 1; i2 <= l2; ++i2) {
+            int r = (i1 + i2) % 3;
+            int t = r == 2 ? 0 : (r == 0 ? 2 : 1);
+            int off = 0;
+            for (int q = 0; q < t; ++q) off += nd[q];
+            int pid = ++id[t] + off - 1;
+#define INV(a, b, o) ((((b) + ((a) - 1) * l2) - 1) * 2 + (o))
+            L->plq_cord[pid * 6 + 0] = INV(i1, i2, 2);
+            L->plq_cord[pid * 6 + 1] = INV(i1, i2, 1);
+            L->plq_cord[pid * 6 + 2] = INV(i1, npbc(i2 - 1, l2), 2);
+            L->plq_cord[pid * 6 + 3] = INV(npbc(i1 - 1, l1), npbc(i2 - 1, l2), 1);
+            L->plq_cord[pid * 6 + 4] = INV(npbc(i1 - 1, l1), npbc(i2 - 1, l2), 2);
+            L->plq_cord[pid * 6 + 5] = INV(npbc(i1 - 1, l1), i2, 1);
+#undef INV
+        }
+}
+
+int orc_latt_build(orc_latt *L, int kind, int l1, int l2) {
+    memset(L, 0, sizeof(*L));
+    if (kind == ORC_SQUARE) setup_square(L, l1, l2);
+    else if (kind == ORC_HONEYCOMB) setup_honeycomb(L, l1, l2);
+    else return -1;
+    return 0;
+}
+
+/* expar.f90: Landau-gauge Peierls phase for bond (i, nf), twist flux and
+ * dimerisation.  i is 0-based, nf is 1-based as in the reference. */
+zc orc_expar(const orc_latt *L, int i, int nf, double xmag, double fx, double fy, double dimer) {
+    int k = (i * L->nn_nf + (nf - 1)) * 2;
+    int nax = L->nnveci[k], nay = L->nnveci[k + 1];
+    double vr1 = L->nnvecr[k], vr2 = L->nnvecr[k + 1];
+    double rc1 = L->rcord[i * 2], rc2 = L->rcord[i * 2 + 1];
+    int c1 = L->cord[i * 2], c2 = L->cord[i * 2 + 1];
+    double xmag1 = xmag / L->ncell * (L->a1[0] * L->a2[1] - L->a1[1] * L->a2[0]);
+    double x = -xmag1 * vr1 * (2.0 * rc2 + vr2) * M_PI;
+    double x1 = 0.0;
+    int edge2 = ((c2 == L->l2 && nay > 0) || (c2 == 1 && nay < 0));
+    int edge1 = ((c1 == L->l1 && nax > 0) || (c1 == 1 && nax < 0));
+    double proj = (rc2 + vr2) * L->a2[0] + (rc1 + vr1) * L->a1[0];
+    int sx = nax > 0 ? 1 : -1, sy = nay > 0 ? 1 : -1;
+    if (edge2 && nax == 0) {
+        x1 = 2.0 * M_PI * xmag1 * (double)(sy * L->l2) * L->a2[1] * proj;
+    } else if (edge1 && nay == 0) {
+        x1 = 2.0 * M_PI * xmag1 * (double)(sx * L->l1) * L->a1[1] * proj;
+    } else if (edge1 && edge2) {
+        x1 = 2.0 * M_PI * xmag1 * ((double)(sx * L->l1) * L->a1[1] + (double)(sy * L->l2) * L->a2[1]) * proj;
+    }
+    zc e = cexp(I * (x + x1));
+    double av0 = fx * L->a1[0] / L->l1 + fy * L->a2[0] / L->l2;
+    double av1 = fx * L->a1[1] / L->l1 + fy * L->a2[1] / L->l2;
+    double rv0 = nax * L->a1[0] + nay * L->a2[0];
+    double rv1 = nax * L->a1[1] + nay * L->a2[1];
+    e *= cexp(I * 2.0 * M_PI * (av0 * rv0 + av1 * rv1));
+    if (nf == 1) e *= (1.0 + dimer);
+    return e;
+}

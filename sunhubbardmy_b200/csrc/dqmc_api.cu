@@ -1,0 +1,1044 @@
+// Host side of the C ABI in include/dqmc_gpu.h: parameter derivation, model
+// tables (lattice, HS constants, kinetic propagators), device allocation and
+// the slice-by-slice orchestration of the finite-temperature sweep.
+//
+// The sweep follows the reference's control flow exactly
+// (src/dqmc_ft_core/dqmc_ft_sweep_b0.f90, dqmc_ft_sweep_0b.f90,
+// dqmc_ft_sweep_start_0b.f90); every chain of a handle is advanced by the same
+// kernel launches (one CTA, or a few, per chain), and a full sweep is captured
+// once into a CUDA graph and replayed.
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/dqmc_gpu.h"
+#include "dqmc_types.h"
+#include "kernels.h"
+
+typedef std::complex<double> zc;
+
+static thread_local std::string g_err = "";
+static int fail(int code, const std::string& msg) { g_err = msg; return code; }
+#define CK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) return fail(DQMC_ECUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); } while (0)
+
+extern "C" const char* dqmc_gpu_last_error(void) { return g_err.c_str(); }
+
+// ---------------------------------------------------------------------------
+// parameters (src/model_para.f90:334-453)
+// ---------------------------------------------------------------------------
+extern "C" int dqmc_params_derive(dqmc_params* p) {
+    if (!p) return fail(DQMC_EINVAL, "null params");
+    if (p->lattice != DQMC_LATT_SQUARE && p->lattice != DQMC_LATT_HONEYCOMB)
+        return fail(DQMC_EINVAL, "lattice must be square or honeycomb");
+    if (p->l1 < 2 || p->l2 < 2) return fail(DQMC_EINVAL, "l1, l2 must be >= 2");
+    if (p->dtau <= 0 || p->beta <= 0) return fail(DQMC_EINVAL, "beta, dtau must be > 0");
+    p->lq = p->l1 * p->l2;
+    p->ndim = (p->lattice == DQMC_LATT_SQUARE) ? p->lq : 2 * p->lq;
+    p->ne = p->ndim / 2 + (int)(p->nu * p->ndim / 8.0);
+    p->ltrot = (int)std::lround(p->beta / p->dtau);
+    if (p->nublock == 0) {
+        if (p->update == DQMC_UPD_DELAY) {
+            int q = p->ndim / 5;
+            p->nublock = q < 16 ? 4 : q < 32 ? 8 : q < 64 ? 16 : q < 256 ? 32 : 64;
+        } else if (p->update == DQMC_UPD_SUBMATRIX) {
+            int q = p->ndim / 20;
+            p->nublock = q < 32 ? 32 : q < 64 ? 64 : q < 128 ? 16 : q < 256 ? 256 : q < 512 ? 512 : 1024;
+        }
+    }
+    if (p->ltrot < p->nwrap) p->nwrap = p->ltrot;
+    if (p->ltrot < p->nwrap || !p->lstabilize) p->nst = 0;
+    else p->nst = (p->ltrot % p->nwrap == 0) ? p->ltrot / p->nwrap : p->ltrot / p->nwrap + 1;
+    if (p->lproju) p->lcomp = p->nflr / 2 + 1 + (int)(0.5 * std::fabs(p->nu));
+    else if (p->hs == DQMC_HS_EXACT && p->nflr == 2) p->lcomp = 2;
+    else p->lcomp = 4;
+    return DQMC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// host model: lattice tables (src/lattice.f90) and model constants
+// ---------------------------------------------------------------------------
+static int npbc(int nr, int l) { return nr > l ? nr - l : (nr < 1 ? nr + l : nr); }
+
+struct HostModel {
+    dqmc_params p;
+    int N, lq, nsub, nn_nf, nn_lf, z_plq, nsn, lcomp, nublock_dev;
+    double a1[2], a2[2];
+    std::vector<int> cell1, cell2;        // unit-cell coordinates of site (1-based)
+    std::vector<double> rc1, rc2;         // real-space coordinates of site
+    std::vector<int> nnlist, snlist;      // [site][nf] 0-based
+    std::vector<int> nnveci;              // [site][nf][2]
+    std::vector<double> nnvecr;           // [site][nf][2]
+    std::vector<int> nnlf;                // A sites, 0-based
+    std::vector<int> imj;                 // [i][j] 0-based distance index
+    std::vector<int> plq;                 // [lq][z_plq] 0-based
+    std::vector<zc> expar;                // [site][nf]
+    std::vector<zc> urt, urtm1;           // [bond][4]
+    std::vector<zc> exph0k, exph0kinv;    // divided by lq
+    std::vector<int> bond_i1, bond_i2;
+    std::vector<int> cell_plus;           // [d][j]
+    ModelDev dev;                         // host copy with device pointers
+    ModelDev* d_dev = nullptr;
+    std::vector<void*> allocs;
+    int iwrap_first_nonzero;
+    std::vector<int> iwrap_nt;            // [0..ltrot]
+    std::vector<int> wrap_step;           // [n][2] 1-based
+};
+
+static void build_lattice(HostModel& m) {
+    const dqmc_params& p = m.p;
+    int l1 = p.l1, l2 = p.l2;
+    m.lq = l1 * l2;
+    bool sq = (p.lattice == DQMC_LATT_SQUARE);
+    if (sq) { m.a1[0] = 1; m.a1[1] = 0; m.a2[0] = 0; m.a2[1] = 1; }
+    else { m.a1[0] = 0.5; m.a1[1] = -0.5 * std::sqrt(3.0); m.a2[0] = 0.5; m.a2[1] = 0.5 * std::sqrt(3.0); }
+    m.nsub = sq ? 1 : 2;
+    m.N = m.lq * m.nsub;
+    m.nn_nf = sq ? 4 : 3;
+    m.nn_lf = sq ? m.lq / 2 : m.lq;
+    m.z_plq = sq ? 4 : 6;
+    m.nsn = sq ? 4 : 6;
+    int N = m.N;
+    m.cell1.resize(N); m.cell2.resize(N); m.rc1.resize(N); m.rc2.resize(N);
+    // unit cell index c = i2 + (i1-1) l2 (1-based); site = c (square) or 2(c-1)+orb
+    for (int i1 = 1; i1 <= l1; ++i1)
+        for (int i2 = 1; i2 <= l2; ++i2)
+            for (int o = 1; o <= m.nsub; ++o) {
+                int cidx = i2 + (i1 - 1) * l2;
+                int s = (cidx - 1) * m.nsub + (o - 1);
+                m.cell1[s] = i1; m.cell2[s] = i2;
+                if (sq || o == 1) { m.rc1[s] = i1; m.rc2[s] = i2; }
+                else { m.rc1[s] = i1 - 1.0 / 3.0; m.rc2[s] = i2 + 1.0 / 3.0; }
+            }
+    auto cellsite = [&](int i1, int i2, int o) { return ((npbc(i1, l1) - 1) * l2 + npbc(i2, l2) - 1) * m.nsub + o; };
+    m.nnlist.assign(N * m.nn_nf, 0);
+    m.snlist.assign(N * m.nsn, 0);
+    m.nnveci.assign(N * m.nn_nf * 2, 0);
+    m.nnvecr.assign(N * m.nn_nf * 2, 0.0);
+    if (sq) {
+        const int v[4][2] = {{1, 0}, {0, 1}, {-1, 0}, {0, -1}};
+        const int s[4][2] = {{1, 1}, {-1, 1}, {-1, -1}, {1, -1}};
+        for (int i = 0; i < N; ++i) {
+            for (int f = 0; f < 4; ++f) {
+                m.nnlist[i * 4 + f] = cellsite(m.cell1[i] + v[f][0], m.cell2[i] + v[f][1], 0);
+                m.snlist[i * 4 + f] = cellsite(m.cell1[i] + s[f][0], m.cell2[i] + s[f][1], 0);
+                m.nnveci[(i * 4 + f) * 2] = v[f][0]; m.nnveci[(i * 4 + f) * 2 + 1] = v[f][1];
+                m.nnvecr[(i * 4 + f) * 2] = v[f][0]; m.nnvecr[(i * 4 + f) * 2 + 1] = v[f][1];
+            }
+        }
+        for (int i1 = 1; i1 <= l1; ++i1)
+            for (int i2 = 1; i2 <= l2; ++i2)
+                if ((i1 + i2) % 2 == 0) m.nnlf.push_back(i2 + (i1 - 1) * l2 - 1);
+    } else {
+        // A (orb 0) -> B neighbours: same cell, cell + a1, cell - a2 (lattice.f90:713-742)
+        const int vA[3][2] = {{0, 0}, {1, 0}, {0, -1}}, vB[3][2] = {{0, 0}, {-1, 0}, {0, 1}};
+        const double rA[3][2] = {{-1.0 / 3, 1.0 / 3}, {2.0 / 3, 1.0 / 3}, {-1.0 / 3, -2.0 / 3}};
+        const double rB[3][2] = {{1.0 / 3, -1.0 / 3}, {-2.0 / 3, -1.0 / 3}, {1.0 / 3, 2.0 / 3}};
+        const int sn[6][2] = {{1, 1}, {1, 0}, {0, -1}, {-1, -1}, {-1, 0}, {0, 1}};
+        for (int i = 0; i < N; ++i) {
+            bool A = (i % 2 == 0);
+            int c1 = m.cell1[i], c2 = m.cell2[i];
+            for (int f = 0; f < 3; ++f) {
+                const int* v = A ? vA[f] : vB[f];
+                m.nnlist[i * 3 + f] = cellsite(c1 + v[0], c2 + v[1], A ? 1 : 0);
+                m.nnveci[(i * 3 + f) * 2] = v[0]; m.nnveci[(i * 3 + f) * 2 + 1] = v[1];
+                m.nnvecr[(i * 3 + f) * 2] = A ? rA[f][0] : rB[f][0];
+                m.nnvecr[(i * 3 + f) * 2 + 1] = A ? rA[f][1] : rB[f][1];
+            }
+            for (int f = 0; f < 6; ++f) m.snlist[i * 6 + f] = cellsite(c1 + sn[f][0], c2 + sn[f][1], A ? 0 : 1);
+        }
+        for (int c = 0; c < m.lq; ++c) m.nnlf.push_back(2 * c);
+    }
+    // imj (setup_latt2d_sub) and the cell table cell_plus[d][j]
+    m.imj.assign(m.lq * m.lq, 0);
+    m.cell_plus.assign(m.lq * m.lq, 0);
+    for (int j = 0; j < m.lq; ++j)
+        for (int i = 0; i < m.lq; ++i) {
+            int ui1 = i / l2 + 1, ui2 = i % l2 + 1, uj1 = j / l2 + 1, uj2 = j % l2 + 1;
+            int nx = npbc(ui1 - uj1, l1), ny = npbc(ui2 - uj2, l2);
+            int d = ny + (nx - 1) * l2 - 1;
+            m.imj[i * m.lq + j] = d;
+            m.cell_plus[d * m.lq + j] = i;
+        }
+    // plaquettes
+    m.plq.assign(m.lq * m.z_plq, 0);
+    if (sq) {
+        int nd[4] = {0, 0, 0, 0}, id[4] = {0, 0, 0, 0};
+        auto typ = [](int i1, int i2) {
+            return (i1 % 2 == 1 && i2 % 2 == 1) ? 0 : (i1 % 2 == 0 && i2 % 2 == 1) ? 1 : (i1 % 2 == 0 && i2 % 2 == 0) ? 2 : 3;
+        };
+        for (int i1 = 1; i1 <= l1; ++i1) for (int i2 = 1; i2 <= l2; ++i2) nd[typ(i1, i2)]++;
+        for (int i1 = 1; i1 <= l1; ++i1)
+            for (int i2 = 1; i2 <= l2; ++i2) {
+                int t = typ(i1, i2), off = 0;
+                for (int q = 0; q < t; ++q) off += nd[q];
+                int pid = id[t]++ + off;
+                m.plq[pid * 4 + 0] = cellsite(i1, i2, 0);
+                m.plq[pid * 4 + 1] = cellsite(i1 + 1, i2, 0);
+                m.plq[pid * 4 + 2] = cellsite(i1 + 1, i2 + 1, 0);
+                m.plq[pid * 4 + 3] = cellsite(i1, i2 + 1, 0);
+            }
+    } else {
+        int nd[3] = {0, 0, 0}, id[3] = {0, 0, 0};
+        auto typ = [](int i1, int i2) { int r = (i1 + i2) % 3; return r == 2 ? 0 : (r == 0 ? 2 : 1); };
+        for (int i1 = 1; i1 <= l1; ++i1) for (int i2 = 1; i2 <= l2; ++i2) nd[typ(i1, i2)]++;
+        for (int i1 = 1; i1 <= l1; ++i1)
+            for (int i2 = 1; i2 <= l2; ++i2) {
+                int t = typ(i1, i2), off = 0;
+                for (int q = 0; q < t; ++q) off += nd[q];
+                int pid = id[t]++ + off;
+                m.plq[pid * 6 + 0] = cellsite(i1, i2, 1);
+                m.plq[pid * 6 + 1] = cellsite(i1, i2, 0);
+                m.plq[pid * 6 + 2] = cellsite(i1, i2 - 1, 1);
+                m.plq[pid * 6 + 3] = cellsite(i1 - 1, i2 - 1, 0);
+                m.plq[pid * 6 + 4] = cellsite(i1 - 1, i2 - 1, 1);
+                m.plq[pid * 6 + 5] = cellsite(i1 - 1, i2, 0);
+            }
+    }
+}
+
+// Peierls / twist / dimerisation phase of bond (site i, family nf 1-based): expar.f90
+static zc expar(const HostModel& m, int i, int nf) {
+    const dqmc_params& p = m.p;
+    int k = (i * m.nn_nf + nf - 1) * 2;
+    int nax = m.nnveci[k], nay = m.nnveci[k + 1];
+    double vr1 = m.nnvecr[k], vr2 = m.nnvecr[k + 1];
+    double rc1 = m.rc1[i], rc2 = m.rc2[i];
+    int c1 = m.cell1[i], c2 = m.cell2[i];
+    double xmag1 = p.xmag / m.lq * (m.a1[0] * m.a2[1] - m.a1[1] * m.a2[0]);
+    double x = -xmag1 * vr1 * (2.0 * rc2 + vr2) * M_PI, x1 = 0.0;
+    bool e2 = (c2 == p.l2 && nay > 0) || (c2 == 1 && nay < 0);
+    bool e1 = (c1 == p.l1 && nax > 0) || (c1 == 1 && nax < 0);
+    double proj = (rc2 + vr2) * m.a2[0] + (rc1 + vr1) * m.a1[0];
+    int sx = nax > 0 ? 1 : -1, sy = nay > 0 ? 1 : -1;
+    if (e2 && nax == 0) x1 = 2.0 * M_PI * xmag1 * (double)(sy * p.l2) * m.a2[1] * proj;
+    else if (e1 && nay == 0) x1 = 2.0 * M_PI * xmag1 * (double)(sx * p.l1) * m.a1[1] * proj;
+    else if (e1 && e2) x1 = 2.0 * M_PI * xmag1 * ((double)(sx * p.l1) * m.a1[1] + (double)(sy * p.l2) * m.a2[1]) * proj;
+    zc e = std::exp(zc(0.0, x + x1));
+    double av0 = p.flux_x * m.a1[0] / p.l1 + p.flux_y * m.a2[0] / p.l2;
+    double av1 = p.flux_x * m.a1[1] / p.l1 + p.flux_y * m.a2[1] / p.l2;
+    double rv0 = nax * m.a1[0] + nay * m.a2[0], rv1 = nax * m.a1[1] + nay * m.a2[1];
+    e *= std::exp(zc(0.0, 2.0 * M_PI * (av0 * rv0 + av1 * rv1)));
+    if (nf == 1) e *= (1.0 + p.dimer);
+    return e;
+}
+
+// exp(-s h) of h = [[d, z],[conj z, d]] in closed form
+static void exp2x2(double d, zc z, double s, zc* out) {
+    double az = std::abs(z), e = std::exp(-s * d);
+    double ch = std::cosh(s * az), sh = az > 0 ? std::sinh(s * az) / az : 0.0;
+    out[0] = e * ch; out[1] = -e * sh * z; out[2] = -e * sh * std::conj(z); out[3] = e * ch;
+}
+
+static int build_model(HostModel& m) {
+    dqmc_params& p = m.p;
+    if (p.t3 != 0.0) return fail(DQMC_EINVAL, "t3 != 0 is not supported");
+    if (p.rv != 0.0) return fail(DQMC_EINVAL, "nearest-neighbour V (t-V) is not supported by the finite-T GPU sweep");
+    if (p.kinetic == DQMC_KIN_FFT && (p.lattice != DQMC_LATT_SQUARE || p.l1 != p.l2))
+        return fail(DQMC_EINVAL, "FFT kinetic term needs a square lattice with l1 == l2");
+    if (p.lattice == DQMC_LATT_SQUARE && ((p.l1 * p.l2) % 2 != 0 || p.l1 % 2 || p.l2 % 2) && p.kinetic == DQMC_KIN_CHECKERBOARD)
+        return fail(DQMC_EINVAL, "checkerboard square lattice needs even l1, l2");
+    build_lattice(m);
+    if (m.N > 512) return fail(DQMC_EINVAL, "ndim > 512 is not supported");
+    if (p.nst < 1) return fail(DQMC_EINVAL, "the sweep needs stabilisation (nst >= 1)");
+    int N = m.N;
+    m.lcomp = p.lcomp;
+    m.nublock_dev = (p.update == DQMC_UPD_FAST) ? 32 : p.nublock;
+    if (m.nublock_dev > 64) m.nublock_dev = 64;
+    if (m.nublock_dev < 1) m.nublock_dev = 1;
+    m.expar.resize(N * m.nn_nf);
+    for (int i = 0; i < N; ++i)
+        for (int f = 1; f <= m.nn_nf; ++f) m.expar[i * m.nn_nf + f - 1] = expar(m, i, f);
+    // bonds (dqmc_set_h0conf.f90:76-123)
+    int nb = m.nn_nf * m.nn_lf;
+    m.bond_i1.resize(nb); m.bond_i2.resize(nb); m.urt.resize(nb * 4); m.urtm1.resize(nb * 4);
+    for (int f = 1; f <= m.nn_nf; ++f)
+        for (int b = 0; b < m.nn_lf; ++b) {
+            int ist = b + (f - 1) * m.nn_lf;
+            int i0 = m.nnlf[b], i1 = m.nnlist[i0 * m.nn_nf + f - 1];
+            m.bond_i1[ist] = i0; m.bond_i2[ist] = i1;
+            zc z = -p.rt * m.expar[i0 * m.nn_nf + f - 1];
+            double d = -p.mu / m.nn_nf;
+            exp2x2(d, z, 0.5 * p.dtau, &m.urt[ist * 4]);
+            exp2x2(d, z, -0.5 * p.dtau, &m.urtm1[ist * 4]);
+        }
+    if (p.kinetic == DQMC_KIN_FFT) {
+        // eigenvalues h0k = diag(F H F^-1), F the unitary forward DFT over (l1, l2)
+        // with column index j1 + l1 j2 (dqmc_set_h0conf.f90:225-291); H from seth0.f90
+        int l1 = p.l1, l2 = p.l2, lq = m.lq;
+        std::vector<std::pair<std::pair<int, int>, zc>> H;
+        for (int b = 0; b < nb; ++b) {
+            int f = b / m.nn_lf + 1;
+            zc z = -p.rt * m.expar[m.bond_i1[b] * m.nn_nf + f - 1];
+            H.push_back({{m.bond_i1[b], m.bond_i2[b]}, z});
+            H.push_back({{m.bond_i2[b], m.bond_i1[b]}, std::conj(z)});
+        }
+        for (int i = 0; i < N; ++i) H.push_back({{i, i}, zc(-p.mu, 0.0)});
+        m.exph0k.resize(lq); m.exph0kinv.resize(lq);
+        for (int k = 0; k < lq; ++k) {
+            int k1 = k % l1, k2 = k / l1;
+            zc h = 0;
+            for (auto& e : H) {
+                int j = e.first.first, jp = e.first.second;
+                double ph = -2 * M_PI * ((double)(j % l1) * k1 / l1 + (double)(j / l1) * k2 / l2)
+                            + 2 * M_PI * ((double)(jp % l1) * k1 / l1 + (double)(jp / l1) * k2 / l2);
+                h += e.second * std::exp(zc(0.0, ph));
+            }
+            h /= (double)lq;
+            m.exph0k[k] = std::exp(-0.5 * p.dtau * h) / (double)lq;
+            m.exph0kinv[k] = std::exp(0.5 * p.dtau * h) / (double)lq;
+        }
+    }
+    // stabilisation schedule
+    m.iwrap_nt.assign(p.ltrot + 1, 0);
+    m.wrap_step.assign(2 * p.nst, 0);
+    for (int i = 1; i <= p.nst; ++i) {
+        int hi = (i == p.nst) ? p.ltrot : i * p.nwrap;
+        m.iwrap_nt[hi] = i;
+        m.wrap_step[(i - 1) * 2] = (i - 1) * p.nwrap + 1;
+        m.wrap_step[(i - 1) * 2 + 1] = hi;
+    }
+    return DQMC_OK;
+}
+
+// HS constants (src/dqmc_config_u/dqmc_set_conf.f90:1-176)
+static void set_hs(const HostModel& m, ModelDev& d) {
+    const dqmc_params& p = m.p;
+    int nflr = p.nflr, lc = m.lcomp;
+    double u = p.rhub, dtau = p.dtau, nu = p.nu, al;
+    double eta[4], gam[4];
+    bool exact = (p.hs == DQMC_HS_EXACT);
+    bool general = !exact || (nflr != 2 && nflr != 4 && nflr != 6);
+    if (!general && nflr == 2) {
+        eta[0] = -1; eta[1] = 1;
+        al = (u >= 0) ? std::acos(std::exp(-dtau * std::fabs(u) * 0.5)) : std::acosh(std::exp(dtau * std::fabs(u) * 0.5));
+        gam[0] = gam[1] = 1.0;
+    } else if (!general) {
+        double a = std::exp(-0.5 * dtau * u);
+        double dd = std::sqrt(8.0 + a * a * (3.0 + a * a) * (3.0 + a * a));
+        double xp = (a + 2 * a * a * a + std::pow(a, 5) + (a * a - 1.0) * dd) / 4.0;
+        double xm = (a + 2 * a * a * a + std::pow(a, 5) - (a * a - 1.0) * dd) / 4.0;
+        if (u >= 0) { eta[0] = -std::acos(xm); eta[1] = -std::acos(xp); eta[2] = std::acos(xp); eta[3] = std::acos(xm); }
+        else { eta[0] = -std::acosh(xm); eta[1] = -std::acosh(xp); eta[2] = std::acosh(xp); eta[3] = std::acosh(xm); }
+        al = 1.0;
+        double t = a * (3.0 + a * a);
+        gam[0] = (t + dd) / dd; gam[1] = (-t + dd) / dd; gam[2] = (-t + dd) / dd; gam[3] = (t + dd) / dd;
+    } else {
+        double s6 = std::sqrt(6.0);
+        eta[0] = -std::sqrt(2.0 * (3.0 + s6)); eta[1] = -std::sqrt(2.0 * (3.0 - s6));
+        eta[2] = std::sqrt(2.0 * (3.0 - s6)); eta[3] = std::sqrt(2.0 * (3.0 + s6));
+        al = std::sqrt(dtau * std::fabs(u) * 0.5);
+        gam[0] = 1.0 - s6 / 3.0; gam[1] = 1.0 + s6 / 3.0; gam[2] = 1.0 + s6 / 3.0; gam[3] = 1.0 - s6 / 3.0;
+    }
+    auto put = [](double2& o, zc z) { o.x = z.real(); o.y = z.imag(); };
+    for (int is = 1; is <= lc; ++is) {
+        zc ph, b, bi;
+        double ang;
+        if (p.lproju) {
+            ang = M_PI * (-2.0 * is) * 0.5 * (nflr + nu) / lc;
+            ph = std::exp(zc(0, ang));
+            b = std::exp(zc(0, M_PI * 2.0 * is / lc));
+            bi = std::exp(zc(0, -M_PI * 2.0 * is / lc));
+        } else if (u >= 0) {
+            ang = al * (-eta[is - 1]) * 0.5 * (nflr + nu);
+            ph = std::exp(zc(0, ang));
+            b = std::exp(zc(0, al * eta[is - 1]));
+            bi = std::exp(zc(0, -al * eta[is - 1]));
+        } else {
+            ang = 0.0;
+            ph = std::exp(al * (-eta[is - 1]) * 0.5 * (nflr + nu));
+            b = std::exp(al * eta[is - 1]);
+            bi = std::exp(-al * eta[is - 1]);
+        }
+        put(d.phase[is - 1], ph); put(d.bmat[is - 1], b); put(d.bmat_inv[is - 1], bi);
+        d.phase_angle[is - 1] = ang;
+    }
+    for (int is = 1; is <= lc; ++is)
+        for (int iflip = 1; iflip <= lc - 1; ++iflip) {
+            int isp = (is + iflip - 1) % lc + 1, k = (is - 1) * (lc - 1) + iflip - 1;
+            zc pr, dl;
+            if (p.lproju) {
+                pr = std::exp(zc(0, M_PI * (2.0 * is - 2.0 * isp) * 0.5 * (nflr + nu) / lc));
+                dl = std::exp(zc(0, M_PI * (2.0 * isp - 2.0 * is) / lc)) - 1.0;
+            } else if (u >= 0) {
+                pr = std::exp(zc(0, al * (eta[is - 1] - eta[isp - 1]) * 0.5 * (nflr + nu)));
+                dl = std::exp(zc(0, al * (eta[isp - 1] - eta[is - 1]))) - 1.0;
+            } else {
+                pr = std::exp(al * (eta[is - 1] - eta[isp - 1]) * 0.5 * (nflr + nu));
+                dl = std::exp(al * (eta[isp - 1] - eta[is - 1])) - 1.0;
+            }
+            put(d.phase_ratio[k], pr); put(d.delta[k], dl);
+            d.gam_ratio[k] = p.lproju ? 1.0 : gam[isp - 1] / gam[is - 1];
+        }
+}
+
+template <class T>
+static int upload(HostModel& m, const std::vector<T>& v, const T** out) {
+    void* p = nullptr;
+    size_t bytes = v.size() * sizeof(T);
+    if (bytes == 0) { *out = nullptr; return DQMC_OK; }
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return fail(DQMC_ENOMEM, "cudaMalloc model table");
+    if (cudaMemcpy(p, v.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess) return fail(DQMC_ECUDA, "model upload");
+    m.allocs.push_back(p);
+    *out = (const T*)p;
+    return DQMC_OK;
+}
+
+static std::vector<double2> to_d2(const std::vector<zc>& v) {
+    std::vector<double2> o(v.size());
+    for (size_t i = 0; i < v.size(); ++i) { o[i].x = v[i].real(); o[i].y = v[i].imag(); }
+    return o;
+}
+
+static int upload_model(HostModel& m) {
+    ModelDev& d = m.dev;
+    memset(&d, 0, sizeof(d));
+    const dqmc_params& p = m.p;
+    d.N = m.N; d.lq = m.lq; d.nsub = m.nsub; d.l1 = p.l1; d.l2 = p.l2; d.nn_nf = m.nn_nf; d.nn_lf = m.nn_lf;
+    d.z_plq = m.z_plq; d.nsn = m.nsn; d.lcomp = m.lcomp; d.nflr = p.nflr; d.lproju = p.lproju;
+    d.kinetic = p.kinetic; d.update = p.update; d.nublock = m.nublock_dev; d.ltrot = p.ltrot; d.nst = p.nst;
+    d.nwrap = p.nwrap; d.lwrapT = (p.rt != 0.0); d.lwrapu = (p.rhub != 0.0);
+    d.phase_on = (p.rhub > 0.0) ? 1 : 0;
+    d.rt = p.rt; d.rv = p.rv; d.t2 = p.t2; d.theta = p.theta * M_PI;
+    set_hs(m, d);
+    int rc;
+    if ((rc = upload(m, m.bond_i1, &d.bond_i1))) return rc;
+    if ((rc = upload(m, m.bond_i2, &d.bond_i2))) return rc;
+    std::vector<double2> t;
+    t = to_d2(m.urt); if ((rc = upload(m, t, &d.urt))) return rc;
+    t = to_d2(m.urtm1); if ((rc = upload(m, t, &d.urtm1))) return rc;
+    if (p.kinetic == DQMC_KIN_FFT) {
+        t = to_d2(m.exph0k); if ((rc = upload(m, t, &d.exph0k))) return rc;
+        t = to_d2(m.exph0kinv); if ((rc = upload(m, t, &d.exph0kinv))) return rc;
+        std::vector<zc> w1(p.l1), w2(p.l2);
+        for (int k = 0; k < p.l1; ++k) w1[k] = std::exp(zc(0, -2 * M_PI * k / p.l1));
+        for (int k = 0; k < p.l2; ++k) w2[k] = std::exp(zc(0, -2 * M_PI * k / p.l2));
+        t = to_d2(w1); if ((rc = upload(m, t, &d.tw1))) return rc;
+        t = to_d2(w2); if ((rc = upload(m, t, &d.tw2))) return rc;
+    }
+    if ((rc = upload(m, m.cell_plus, &d.cell_plus))) return rc;
+    if ((rc = upload(m, m.nnlist, &d.nnlist))) return rc;
+    if ((rc = upload(m, m.snlist, &d.snlist))) return rc;
+    if ((rc = upload(m, m.plq, &d.plq_cord))) return rc;
+    t = to_d2(m.expar); if ((rc = upload(m, t, &d.expar_nn))) return rc;
+    void* pd = nullptr;
+    if (cudaMalloc(&pd, sizeof(ModelDev)) != cudaSuccess) return fail(DQMC_ENOMEM, "cudaMalloc model");
+    m.allocs.push_back(pd);
+    m.d_dev = (ModelDev*)pd;
+    if (cudaMemcpy(pd, &d, sizeof(ModelDev), cudaMemcpyHostToDevice) != cudaSuccess) return fail(DQMC_ECUDA, "model upload");
+    return DQMC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// SFMT seeding (lib/m_spring.f90:187-243), on the host
+// ---------------------------------------------------------------------------
+static void sfmt_seed(uint32_t* st, int32_t seed) {
+    static const uint32_t parity[4] = {1u, 0u, 0u, 0x13c9e684u};
+    st[0] = (uint32_t)seed;
+    for (int i = 1; i < 624; ++i) st[i] = 1812433253u * (st[i - 1] ^ (st[i - 1] >> 30)) + (uint32_t)i;
+    uint32_t inner = 0;
+    for (int i = 0; i < 4; ++i) inner ^= st[i] & parity[i];
+    for (int i = 16; i > 0; i >>= 1) inner ^= inner >> i;
+    if ((inner & 1) != 1) {
+        bool done = false;
+        for (int i = 0; i < 4 && !done; ++i) {
+            uint32_t work = 1;
+            for (int j = 0; j < 32; ++j) {
+                if (work & parity[i]) { st[i] ^= work; done = true; break; }
+                work <<= 1;
+            }
+        }
+    }
+    st[624] = 624;   // read index: the first draw regenerates the block
+}
+
+// host restatement of spring_sfmt_source for the fresh-start conf draw
+struct HostSfmt {
+    uint32_t st[625];
+    void gen() {
+        static const uint32_t msk[4] = {0xdfffffefU, 0xddfecb7fU, 0xbffaffffU, 0xbffffff6U};
+        auto rec = [&](uint32_t* r, const uint32_t* a, const uint32_t* b, const uint32_t* c, const uint32_t* d) {
+            uint64_t ah = ((uint64_t)a[3] << 32) | a[2], al = ((uint64_t)a[1] << 32) | a[0];
+            uint64_t ch = ((uint64_t)c[3] << 32) | c[2], cl = ((uint64_t)c[1] << 32) | c[0];
+            uint64_t xh = (ah << 8) | (al >> 56), xl = al << 8, yh = ch >> 8, yl = (cl >> 8) | (ch << 56);
+            uint32_t x[4] = {(uint32_t)xl, (uint32_t)(xl >> 32), (uint32_t)xh, (uint32_t)(xh >> 32)};
+            uint32_t y[4] = {(uint32_t)yl, (uint32_t)(yl >> 32), (uint32_t)yh, (uint32_t)(yh >> 32)};
+            uint32_t o[4];
+            for (int k = 0; k < 4; ++k) o[k] = a[k] ^ x[k] ^ ((b[k] >> 11) & msk[k]) ^ y[k] ^ (d[k] << 18);
+            for (int k = 0; k < 4; ++k) r[k] = o[k];
+        };
+        uint32_t *r1 = st + 4 * 154, *r2 = st + 4 * 155;
+        for (int i = 0; i < 156; ++i) {
+            int bi = i < 34 ? i + 122 : i + 122 - 156;
+            rec(st + 4 * i, st + 4 * i, st + 4 * bi, r1, r2);
+            r1 = r2; r2 = st + 4 * i;
+        }
+    }
+    uint32_t next() { if (st[624] >= 624) { gen(); st[624] = 0; } return st[st[624]++]; }
+    double stream() { return ((double)next() + 0.5) * (1.0 / 4294967296.0); }
+};
+
+// ---------------------------------------------------------------------------
+// handle
+// ---------------------------------------------------------------------------
+struct ChainHost {
+    int model;
+    ChainDev dev;
+};
+
+struct dqmc_handle {
+    std::vector<HostModel*> models;
+    std::vector<ChainHost> chains;
+    ChainDev* d_chains = nullptr;
+    int* d_slotmap = nullptr;
+    std::vector<void*> allocs;
+    cudaStream_t st = nullptr;
+    int nch = 0, maxN = 0, ltrot = 0, nst = 0, nwrap = 0, nnf_max = 0;
+    int started = 0;
+    cudaGraphExec_t sweep_graph = nullptr;
+    int graph_meas = -1;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0.0;
+    int ctas_per_chain = 1;
+};
+
+static void* dalloc(dqmc_handle* h, size_t bytes) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess) return nullptr;
+    cudaMemset(p, 0, bytes ? bytes : 16);
+    h->allocs.push_back(p);
+    return p;
+}
+
+extern "C" int dqmc_gpu_destroy(dqmc_handle* h) {
+    if (!h) return DQMC_OK;
+    if (h->st) cudaStreamSynchronize(h->st);
+    if (h->sweep_graph) cudaGraphExecDestroy(h->sweep_graph);
+    for (void* p : h->allocs) cudaFree(p);
+    for (HostModel* m : h->models) { for (void* p : m->allocs) cudaFree(p); delete m; }
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->st) cudaStreamDestroy(h->st);
+    delete h;
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_chains, const int32_t* seeds,
+                               int draw_conf, dqmc_handle** out) {
+    if (!params || n_params < 1 || n_chains < 1 || !out) return fail(DQMC_EINVAL, "invalid arguments");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(DQMC_ECUDA, "no CUDA device");
+    dqmc_handle* h = new dqmc_handle();
+    *out = nullptr;
+    int rc;
+    for (int k = 0; k < n_params; ++k) {
+        HostModel* m = new HostModel();
+        m->p = params[k];
+        if ((rc = dqmc_params_derive(&m->p))) { delete m; dqmc_gpu_destroy(h); return rc; }
+        if ((rc = build_model(*m))) { delete m; dqmc_gpu_destroy(h); return rc; }
+        h->models.push_back(m);
+        if (k == 0) { h->ltrot = m->p.ltrot; h->nst = m->p.nst; h->nwrap = m->p.nwrap; }
+        else if (m->p.ltrot != h->ltrot || m->p.nst != h->nst || m->p.nwrap != h->nwrap) {
+            dqmc_gpu_destroy(h);
+            return fail(DQMC_EINVAL, "all parameter sets of a handle must share ltrot and nwrap");
+        }
+        if ((rc = upload_model(*m))) { dqmc_gpu_destroy(h); return rc; }
+        h->maxN = std::max(h->maxN, m->N);
+        h->nnf_max = std::max(h->nnf_max, m->nn_nf);
+    }
+    if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) { dqmc_gpu_destroy(h); return fail(DQMC_ECUDA, "stream"); }
+    cudaEventCreate(&h->ev0);
+    cudaEventCreate(&h->ev1);
+    h->nch = n_chains;
+    int nst = h->nst, lt = h->ltrot;
+    h->d_slotmap = (int*)dalloc(h, sizeof(int) * (nst + 2));
+    {
+        std::vector<int> sm(nst + 2);
+        for (int i = 0; i < nst + 2; ++i) sm[i] = i;
+        cudaMemcpy(h->d_slotmap, sm.data(), sizeof(int) * (nst + 2), cudaMemcpyHostToDevice);
+    }
+    h->chains.resize(n_chains);
+    for (int c = 0; c < n_chains; ++c) {
+        HostModel* m = h->models[c % n_params];
+        ChainHost& ch = h->chains[c];
+        ch.model = c % n_params;
+        ChainDev& d = ch.dev;
+        memset(&d, 0, sizeof(d));
+        int N = m->N;
+        size_t NN = (size_t)N * N, z = sizeof(double2);
+        d.md = m->d_dev;
+        d.N = N;
+        d.G = (double2*)dalloc(h, NN * z);
+        d.Gnew = (double2*)dalloc(h, NN * z);
+        for (int k = 0; k < 6; ++k) d.W[k] = (double2*)dalloc(h, NN * z);
+        d.U = (double2*)dalloc(h, (size_t)(nst + 2) * NN * z);
+        d.V = (double2*)dalloc(h, (size_t)(nst + 2) * NN * z);
+        d.D = (double*)dalloc(h, (size_t)(nst + 2) * N * sizeof(double));
+        d.logdetQ = (double2*)dalloc(h, (size_t)(nst + 2) * z);
+        d.A = (double2*)dalloc(h, (size_t)N * m->nublock_dev * z);
+        d.B = (double2*)dalloc(h, (size_t)N * m->nublock_dev * z);
+        d.tau = (double2*)dalloc(h, (size_t)N * z);
+        d.T = (double2*)dalloc(h, (size_t)(N / 16 + 1) * 256 * z);
+        d.smallw = (double2*)dalloc(h, (size_t)32 * N * z);
+        d.vecs = (double*)dalloc(h, (size_t)8 * N * sizeof(double));
+        d.perm = (int*)dalloc(h, (size_t)N * sizeof(int));
+        d.conf = (int32_t*)dalloc(h, (size_t)lt * N * sizeof(int32_t));
+        d.sfmt = (uint32_t*)dalloc(h, 625 * sizeof(uint32_t));
+        d.rnd = (uint32_t*)dalloc(h, (size_t)lt * 2 * N * sizeof(uint32_t));
+        d.bins = (double2*)dalloc(h, (size_t)(10 + 20 * m->lq + 4) * z);
+        d.stats = (double*)dalloc(h, ST_COUNT * sizeof(double));
+        d.slotmap = h->d_slotmap;
+        if (!d.G || !d.Gnew || !d.W[5] || !d.U || !d.V || !d.D || !d.rnd || !d.stats || !d.bins) {
+            dqmc_gpu_destroy(h);
+            return fail(DQMC_ENOMEM, "device allocation failed");
+        }
+        // generator state and fresh-start field
+        HostSfmt rng;
+        sfmt_seed(rng.st, seeds ? seeds[c] : 0);
+        std::vector<int32_t> conf((size_t)lt * N, 1);
+        if (draw_conf)
+            for (size_t e = 0; e < conf.size(); ++e) conf[e] = (int32_t)std::ceil(rng.stream() * m->lcomp);
+        cudaMemcpy(d.sfmt, rng.st, 625 * sizeof(uint32_t), cudaMemcpyHostToDevice);
+        cudaMemcpy(d.conf, conf.data(), conf.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+        double stats[ST_COUNT] = {0};
+        stats[ST_PHASE_RE] = 1.0;
+        cudaMemcpy(d.stats, stats, sizeof(stats), cudaMemcpyHostToDevice);
+    }
+    h->d_chains = (ChainDev*)dalloc(h, sizeof(ChainDev) * n_chains);
+    {
+        std::vector<ChainDev> v(n_chains);
+        for (int c = 0; c < n_chains; ++c) v[c] = h->chains[c].dev;
+        cudaMemcpy(h->d_chains, v.data(), sizeof(ChainDev) * n_chains, cudaMemcpyHostToDevice);
+    }
+    set_stab_maxN(h->maxN);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    h->ctas_per_chain = std::max(1, std::min(h->maxN / 16, (2 * sms + n_chains - 1) / n_chains));
+    CK(cudaDeviceSynchronize());
+    CK(cudaGetLastError());
+    *out = h;
+    return DQMC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// propagation programs
+// ---------------------------------------------------------------------------
+static void prog_add(PropProg& p, int kind, int which, int nf, int nt) {
+    if (p.n < DQ_MAX_PROG) p.op[p.n++] = kind | (which << 4) | (nf << 8) | (nt << 16);
+}
+
+// kinetic half step, families 1..nnf (reversed = nnf..1); `which` urt/urtm1
+static void prog_k(const HostModel& m, PropProg& p, int which, int reversed) {
+    if (m.p.rt == 0.0) return;
+    if (m.p.kinetic == DQMC_KIN_FFT) { prog_add(p, PK_FFT, which, 0, 0); return; }
+    for (int k = 1; k <= m.nn_nf; ++k) prog_add(p, PK_CB, which == PW_CONJ ? PW_FWD : which, reversed ? m.nn_nf + 1 - k : k, 0);
+}
+static void prog_v(const HostModel& m, PropProg& p, int which, int nt) {
+    if (m.p.rhub == 0.0) return;
+    prog_add(p, PK_DIAG, which, 0, nt);
+}
+
+// all chains share structure; programs are built from model 0 (same nn_nf
+// per handle for a given lattice kind)
+static int launch_prog(dqmc_handle* h, int mat_id, const PropProg& prog, int right) {
+    if (prog.n == 0) return DQMC_OK;
+    launch_prop(h->d_chains, h->nch, h->maxN, mat_id, prog, right, h->ctas_per_chain, h->st);
+    return DQMC_OK;
+}
+
+// B(nt1, nt2) from the left (Bmat_left_forward, src/dqmc_ft_core.f90:70-121)
+static PropProg prog_bmat(const HostModel& m, int nt1, int nt2) {
+    PropProg p; p.n = 0;
+    for (int nt = nt2; nt <= nt1; ++nt) {
+        prog_k(m, p, PW_FWD, 0);
+        prog_v(m, p, PW_FWD, nt);
+        prog_k(m, p, PW_FWD, 1);
+    }
+    return p;
+}
+// B(nt1, nt2)^H from the left (Bmat_left_forward_hc, src/dqmc_ft_core.f90:123-175)
+static PropProg prog_bmat_hc(const HostModel& m, int nt1, int nt2) {
+    PropProg p; p.n = 0;
+    for (int nt = nt1; nt >= nt2; --nt) {
+        prog_k(m, p, PW_CONJ, 0);
+        prog_v(m, p, PW_CONJ, nt);
+        prog_k(m, p, PW_CONJ, 1);
+    }
+    return p;
+}
+
+enum { MAT_G = 0, MAT_U = 100, MAT_V = 400 };
+
+// one stabilisation of the 0b sweep at stack index n: new factor into the spare
+// slot, Green's function from (new R, old L), wrap check, then swap slots.
+static void stab_0b(dqmc_handle* h, int n, int record) {
+    const HostModel& m = *h->models[0];
+    int spare = h->nst + 1;
+    launch_copy_mat(h->d_chains, h->nch, 2 /*W0*/, MAT_U + (n - 1), 0, h->st);
+    PropProg p = prog_bmat(m, m.wrap_step[(n - 1) * 2 + 1], m.wrap_step[(n - 1) * 2]);
+    launch_prog(h, 2, p, 0);
+    launch_stab_slots(h->d_chains, h->nch, n - 1, spare, h->st);
+    launch_green(h->d_chains, h->nch, spare, n, 0, 0, 0, 0, 0, h->st);
+    launch_wrap_check(h->d_chains, h->nch, record, h->st);
+    launch_swap_slots(h->d_slotmap, n, spare, h->st);
+}
+
+// one stabilisation of the b0 sweep at stack index n (stablize_b0(n+1))
+static void stab_b0(dqmc_handle* h, int n) {
+    const HostModel& m = *h->models[0];
+    int spare = h->nst + 1;
+    launch_copy_mat(h->d_chains, h->nch, 2, MAT_U + (n + 1), 0, h->st);
+    PropProg p = prog_bmat_hc(m, m.wrap_step[n * 2 + 1], m.wrap_step[n * 2]);
+    launch_prog(h, 2, p, 0);
+    launch_stab_slots(h->d_chains, h->nch, n + 1, spare, h->st);
+    launch_green(h->d_chains, h->nch, n, spare, 0, 0, 0, 0, 0, h->st);
+    launch_wrap_check(h->d_chains, h->nch, 1, h->st);
+    launch_swap_slots(h->d_slotmap, n, spare, h->st);
+}
+
+extern "C" int dqmc_gpu_sweep_start(dqmc_handle* h) {
+    if (!h) return fail(DQMC_EINVAL, "null handle");
+    const HostModel& m = *h->models[0];
+    {
+        std::vector<int> sm(h->nst + 2);
+        for (int i = 0; i < h->nst + 2; ++i) sm[i] = i;
+        CK(cudaMemcpyAsync(h->d_slotmap, sm.data(), sizeof(int) * sm.size(), cudaMemcpyHostToDevice, h->st));
+    }
+    launch_stack_identity(h->d_chains, h->nch, 0, h->st);
+    for (int n = 1; n <= h->nst; ++n) {
+        launch_copy_mat(h->d_chains, h->nch, 2, MAT_U + (n - 1), 0, h->st);
+        PropProg p = prog_bmat(m, m.wrap_step[(n - 1) * 2 + 1], m.wrap_step[(n - 1) * 2]);
+        launch_prog(h, 2, p, 0);
+        launch_stab_slots(h->d_chains, h->nch, n - 1, n, h->st);
+    }
+    launch_green(h->d_chains, h->nch, h->nst, 0, 0, 0, 0, 0, 1, h->st);
+    launch_wrap_check(h->d_chains, h->nch, 0, h->st);
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaGetLastError());
+    h->started = 1;
+    return DQMC_OK;
+}
+
+static void enqueue_b0(dqmc_handle* h, int lupdate, int lmeasure) {
+    const HostModel& m = *h->models[0];
+    int lt = h->ltrot;
+    launch_stack_identity(h->d_chains, h->nch, h->nst, h->st);
+    if (lupdate && m.p.rhub != 0.0) launch_sfmt(h->d_chains, h->nch, lt, h->st);
+    for (int nt = lt; nt >= 1; --nt) {
+        int visit = lt - nt;
+        if (lmeasure) launch_measure(h->d_chains, h->nch, h->st);
+        PropProg pl; pl.n = 0; PropProg pr; pr.n = 0;
+        prog_k(m, pl, PW_INV, 0);          // left_backward, nf = 1..nnf
+        prog_k(m, pr, PW_FWD, 0);          // right_forward, nf = 1..nnf
+        launch_prog(h, MAT_G, pl, 0);
+        launch_prog(h, MAT_G, pr, 1);
+        if (lupdate && m.p.rhub != 0.0) launch_update(h->d_chains, h->nch, nt, visit, h->st);
+        pl.n = 0; pr.n = 0;
+        prog_v(m, pl, PW_INV, nt);         // u left_backward
+        prog_k(m, pl, PW_INV, 1);          // h0 left_backward, nf = nnf..1
+        prog_v(m, pr, PW_FWD, nt);         // u right_forward
+        prog_k(m, pr, PW_FWD, 1);
+        launch_prog(h, MAT_G, pl, 0);
+        launch_prog(h, MAT_G, pr, 1);
+        if ((m.iwrap_nt[nt - 1] > 0 || m.p.nwrap == 1) || nt == 1) stab_b0(h, m.iwrap_nt[nt - 1]);
+    }
+}
+
+static void enqueue_0b(dqmc_handle* h, int lupdate, int lmeasure) {
+    const HostModel& m = *h->models[0];
+    int lt = h->ltrot;
+    launch_stack_identity(h->d_chains, h->nch, 0, h->st);
+    if (lupdate && m.p.rhub != 0.0) launch_sfmt(h->d_chains, h->nch, lt, h->st);
+    for (int nt = 1; nt <= lt; ++nt) {
+        int visit = nt - 1;
+        PropProg pl; pl.n = 0; PropProg pr; pr.n = 0;
+        prog_k(m, pl, PW_FWD, 0);          // left_forward, nf = 1..nnf
+        prog_v(m, pl, PW_FWD, nt);         // u left_forward
+        prog_k(m, pr, PW_INV, 0);          // right_backward
+        prog_v(m, pr, PW_INV, nt);         // u right_backward
+        launch_prog(h, MAT_G, pl, 0);
+        launch_prog(h, MAT_G, pr, 1);
+        if (lupdate && m.p.rhub != 0.0) launch_update(h->d_chains, h->nch, nt, visit, h->st);
+        pl.n = 0; pr.n = 0;
+        prog_k(m, pl, PW_FWD, 1);
+        prog_k(m, pr, PW_INV, 1);
+        launch_prog(h, MAT_G, pl, 0);
+        launch_prog(h, MAT_G, pr, 1);
+        if (lmeasure) launch_measure(h->d_chains, h->nch, h->st);
+        if (m.iwrap_nt[nt] > 0) stab_0b(h, m.iwrap_nt[nt], 1);
+    }
+}
+
+extern "C" int dqmc_gpu_sweep_b0(dqmc_handle* h, int lupdate, int lmeasure) {
+    if (!h) return fail(DQMC_EINVAL, "null handle");
+    if (!h->started) return fail(DQMC_ESTATE, "sweep before sweep_start");
+    enqueue_b0(h, lupdate, lmeasure);
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaGetLastError());
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_sweep_0b(dqmc_handle* h, int lupdate, int lmeasure) {
+    if (!h) return fail(DQMC_EINVAL, "null handle");
+    if (!h->started) return fail(DQMC_ESTATE, "sweep before sweep_start");
+    enqueue_0b(h, lupdate, lmeasure);
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaGetLastError());
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_sweeps(dqmc_handle* h, int n, int lmeasure) {
+    if (!h) return fail(DQMC_EINVAL, "null handle");
+    if (!h->started) return fail(DQMC_ESTATE, "sweep before sweep_start");
+    if (n <= 0) return DQMC_OK;
+    if (!h->sweep_graph || h->graph_meas != lmeasure) {
+        if (h->sweep_graph) { cudaGraphExecDestroy(h->sweep_graph); h->sweep_graph = nullptr; }
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+        enqueue_b0(h, 1, lmeasure);
+        enqueue_0b(h, 1, lmeasure);
+        CK(cudaStreamEndCapture(h->st, &g));
+        CK(cudaGraphInstantiate(&h->sweep_graph, g, 0));
+        cudaGraphDestroy(g);
+        h->graph_meas = lmeasure;
+    }
+    CK(cudaEventRecord(h->ev0, h->st));
+    for (int i = 0; i < n; ++i) CK(cudaGraphLaunch(h->sweep_graph, h->st));
+    CK(cudaEventRecord(h->ev1, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaGetLastError());
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    h->last_ms = ms / n;
+    return DQMC_OK;
+}
+
+extern "C" double dqmc_gpu_last_sweeps_ms(dqmc_handle* h) { return h ? h->last_ms : 0.0; }
+
+// ---------------------------------------------------------------------------
+// data access
+// ---------------------------------------------------------------------------
+static int chk_chain(dqmc_handle* h, int c) {
+    if (!h) return fail(DQMC_EINVAL, "null handle");
+    if (c < 0 || c >= h->nch) return fail(DQMC_EINVAL, "chain index out of range");
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_set_conf(dqmc_handle* h, int chain, const int32_t* conf) {
+    int rc = chk_chain(h, chain); if (rc) return rc;
+    const ChainDev& d = h->chains[chain].dev;
+    int lcomp = h->models[h->chains[chain].model]->lcomp;
+    size_t n = (size_t)h->ltrot * d.N;
+    for (size_t e = 0; e < n; ++e)
+        if (conf[e] < 1 || conf[e] > lcomp) return fail(DQMC_EINVAL, "HS field value out of range 1..lcomp");
+    CK(cudaMemcpy(d.conf, conf, n * sizeof(int32_t), cudaMemcpyHostToDevice));
+    h->started = 0;
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_get_conf(dqmc_handle* h, int chain, int32_t* conf) {
+    int rc = chk_chain(h, chain); if (rc) return rc;
+    const ChainDev& d = h->chains[chain].dev;
+    CK(cudaMemcpy(conf, d.conf, (size_t)h->ltrot * d.N * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_set_conf_all(dqmc_handle* h, const int32_t* conf) {
+    if (!h) return fail(DQMC_EINVAL, "null handle");
+    size_t off = 0;
+    for (int c = 0; c < h->nch; ++c) {
+        const ChainDev& d = h->chains[c].dev;
+        size_t n = (size_t)h->ltrot * d.N;
+        int lcomp = h->models[h->chains[c].model]->lcomp;
+        for (size_t e = 0; e < n; ++e)
+            if (conf[off + e] < 1 || conf[off + e] > lcomp) return fail(DQMC_EINVAL, "HS field value out of range 1..lcomp");
+        CK(cudaMemcpyAsync(d.conf, conf + off, n * sizeof(int32_t), cudaMemcpyHostToDevice, h->st));
+        off += n;
+    }
+    CK(cudaStreamSynchronize(h->st));
+    h->started = 0;
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_get_conf_all(dqmc_handle* h, int32_t* conf) {
+    if (!h) return fail(DQMC_EINVAL, "null handle");
+    size_t off = 0;
+    for (int c = 0; c < h->nch; ++c) {
+        const ChainDev& d = h->chains[c].dev;
+        size_t n = (size_t)h->ltrot * d.N;
+        CK(cudaMemcpyAsync(conf + off, d.conf, n * sizeof(int32_t), cudaMemcpyDeviceToHost, h->st));
+        off += n;
+    }
+    CK(cudaStreamSynchronize(h->st));
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_get_green(dqmc_handle* h, int chain, double* g) {
+    int rc = chk_chain(h, chain); if (rc) return rc;
+    const ChainDev& d = h->chains[chain].dev;
+    CK(cudaMemcpy(g, d.G, (size_t)d.N * d.N * sizeof(double2), cudaMemcpyDeviceToHost));
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_set_green(dqmc_handle* h, int chain, const double* g) {
+    int rc = chk_chain(h, chain); if (rc) return rc;
+    const ChainDev& d = h->chains[chain].dev;
+    CK(cudaMemcpy(d.G, g, (size_t)d.N * d.N * sizeof(double2), cudaMemcpyHostToDevice));
+    h->started = 1;
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_set_work(dqmc_handle* h, int chain, int which, const double* mtx) {
+    int rc = chk_chain(h, chain); if (rc) return rc;
+    if (which < 0 || which > 5) return fail(DQMC_EINVAL, "work index 0..5");
+    const ChainDev& d = h->chains[chain].dev;
+    CK(cudaMemcpy(d.W[which], mtx, (size_t)d.N * d.N * sizeof(double2), cudaMemcpyHostToDevice));
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_get_work(dqmc_handle* h, int chain, int which, double* mtx) {
+    int rc = chk_chain(h, chain); if (rc) return rc;
+    if (which < 0 || which > 5) return fail(DQMC_EINVAL, "work index 0..5");
+    const ChainDev& d = h->chains[chain].dev;
+    CK(cudaMemcpy(mtx, d.W[which], (size_t)d.N * d.N * sizeof(double2), cudaMemcpyDeviceToHost));
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_test_zgemm(dqmc_handle* h, int m, int n, int k, int opa, int opb, int a, int b, int c, double beta) {
+    if (!h) return fail(DQMC_EINVAL, "null handle");
+    if (m < 0 || n < 0 || k < 0 || m > h->maxN || n > h->maxN || k > h->maxN) return fail(DQMC_EINVAL, "gemm size");
+    if (a < 0 || a > 5 || b < 0 || b > 5 || c < 0 || c > 5) return fail(DQMC_EINVAL, "work index 0..5");
+    launch_zgemm_test(h->d_chains, h->nch, m, n, k, opa, opb, 2 + a, 2 + b, 2 + c, beta, h->st);
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaGetLastError());
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_test_qr(dqmc_handle* h, int a, int q, double* logdetq) {
+    if (!h) return fail(DQMC_EINVAL, "null handle");
+    if (a < 0 || a > 4 || q < 0 || q > 4 || a == q) return fail(DQMC_EINVAL, "work index 0..4, a != q");
+    launch_qr_test(h->d_chains, h->nch, 2 + a, 2 + q, h->st);
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaGetLastError());
+    for (int c = 0; c < h->nch; ++c) {
+        double st[ST_COUNT];
+        CK(cudaMemcpy(st, h->chains[c].dev.stats, sizeof(st), cudaMemcpyDeviceToHost));
+        logdetq[2 * c] = st[ST_LOGDETM_RE];
+        logdetq[2 * c + 1] = st[ST_LOGDETM_IM];
+    }
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_obser_init(dqmc_handle* h) {
+    if (!h) return fail(DQMC_EINVAL, "null handle");
+    int maxb = 0;
+    for (auto* m : h->models) maxb = std::max(maxb, 10 + 20 * m->lq + 4);
+    launch_bins_clear(h->d_chains, h->nch, maxb, h->st);
+    CK(cudaStreamSynchronize(h->st));
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_nbins(dqmc_handle* h, int chain) {
+    int rc = chk_chain(h, chain); if (rc) return rc;
+    return 10 + 20 * h->models[h->chains[chain].model]->lq + 4;
+}
+
+extern "C" int dqmc_gpu_get_bins(dqmc_handle* h, int chain, double* out) {
+    int rc = chk_chain(h, chain); if (rc) return rc;
+    int nb = dqmc_gpu_nbins(h, chain);
+    CK(cudaMemcpy(out, h->chains[chain].dev.bins, (size_t)nb * sizeof(double2), cudaMemcpyDeviceToHost));
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_get_diag(dqmc_handle* h, int chain, dqmc_diag* out) {
+    int rc = chk_chain(h, chain); if (rc) return rc;
+    double st[ST_COUNT];
+    CK(cudaMemcpy(st, h->chains[chain].dev.stats, sizeof(st), cudaMemcpyDeviceToHost));
+    out->phase_re = st[ST_PHASE_RE]; out->phase_im = st[ST_PHASE_IM];
+    out->logweight_re = st[ST_LOGW_RE]; out->logweight_im = st[ST_LOGW_IM];
+    out->max_wrap_error = st[ST_MAX_WRAP]; out->max_phasediff = st[ST_MAX_PHASEDIFF];
+    out->avglog10error_sum = st[ST_AVGLOG10]; out->logcount = st[ST_LOGCOUNT];
+    out->avgexpphasediff_sum = st[ST_AVGEXPPD];
+    out->accepted = st[ST_ACC]; out->proposed = st[ST_PROP]; out->nobs = st[ST_NOBS];
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_reset_diag(dqmc_handle* h) {
+    if (!h) return fail(DQMC_EINVAL, "null handle");
+    for (int c = 0; c < h->nch; ++c) {
+        double st[ST_COUNT];
+        CK(cudaMemcpy(st, h->chains[c].dev.stats, sizeof(st), cudaMemcpyDeviceToHost));
+        st[ST_MAX_WRAP] = st[ST_MAX_PHASEDIFF] = st[ST_AVGLOG10] = st[ST_LOGCOUNT] = st[ST_AVGEXPPD] = 0.0;
+        st[ST_ACC] = st[ST_PROP] = 0.0;
+        CK(cudaMemcpy(h->chains[c].dev.stats, st, sizeof(st), cudaMemcpyHostToDevice));
+    }
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_set_phase(dqmc_handle* h, int chain, double re, double im) {
+    int rc = chk_chain(h, chain); if (rc) return rc;
+    double v[2] = {re, im};
+    CK(cudaMemcpy(h->chains[chain].dev.stats + ST_PHASE_RE, v, sizeof(v), cudaMemcpyHostToDevice));
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_draw_u32(dqmc_handle* h, int chain, int count, uint32_t* out) {
+    int rc = chk_chain(h, chain); if (rc) return rc;
+    const ChainDev& d = h->chains[chain].dev;
+    if (count < 0 || count > h->ltrot * 2 * d.N) return fail(DQMC_EINVAL, "count out of range");
+    launch_sfmt_raw(h->d_chains, chain, count, h->st);
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaMemcpy(out, d.rnd, (size_t)count * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    return DQMC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// operator-level entry points
+// ---------------------------------------------------------------------------
+extern "C" int dqmc_gpu_h0_prop(dqmc_handle* h, int op, int nf) {
+    if (!h) return fail(DQMC_EINVAL, "null handle");
+    const HostModel& m = *h->models[0];
+    if (op < 0 || op > 4) return fail(DQMC_EINVAL, "op 0..4");
+    if (m.p.kinetic == DQMC_KIN_CHECKERBOARD && (nf < 1 || nf > m.nn_nf)) return fail(DQMC_EINVAL, "nf out of range");
+    PropProg p; p.n = 0;
+    int which = (op == 1 || op == 3) ? PW_INV : (op == 4 ? PW_CONJ : PW_FWD);
+    if (m.p.kinetic == DQMC_KIN_FFT) prog_add(p, PK_FFT, which, 0, 0);
+    else prog_add(p, PK_CB, which == PW_CONJ ? PW_FWD : which, nf, 0);
+    launch_prog(h, MAT_G, p, (op == 2 || op == 3) ? 1 : 0);
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaGetLastError());
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_u_prop(dqmc_handle* h, int op, int nt) {
+    if (!h) return fail(DQMC_EINVAL, "null handle");
+    if (op < 0 || op > 4) return fail(DQMC_EINVAL, "op 0..4");
+    if (nt < 1 || nt > h->ltrot) return fail(DQMC_EINVAL, "nt out of range");
+    PropProg p; p.n = 0;
+    int which = (op == 1 || op == 3) ? PW_INV : (op == 4 ? PW_CONJ : PW_FWD);
+    prog_add(p, PK_DIAG, which, 0, nt);
+    launch_prog(h, MAT_G, p, (op == 2 || op == 3) ? 1 : 0);
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaGetLastError());
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_update(dqmc_handle* h, int nt) {
+    if (!h) return fail(DQMC_EINVAL, "null handle");
+    if (nt < 1 || nt > h->ltrot) return fail(DQMC_EINVAL, "nt out of range");
+    launch_sfmt(h->d_chains, h->nch, 1, h->st);
+    launch_update(h->d_chains, h->nch, nt, 0, h->st);
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaGetLastError());
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_measure(dqmc_handle* h) {
+    if (!h) return fail(DQMC_EINVAL, "null handle");
+    launch_measure(h->d_chains, h->nch, h->st);
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaGetLastError());
+    return DQMC_OK;
+}

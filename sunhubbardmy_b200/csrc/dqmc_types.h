@@ -1,0 +1,78 @@
+// Device-side descriptors shared by the host code and the kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define DQ_MAX_LCOMP 4
+#define DQ_MAX_PROG 160   // propagation ops per pass (nwrap slices x (2 nn_nf + 1))
+
+// Model tables for one lattice/parameter set (read-only during a sweep).
+struct ModelDev {
+    int N, lq, nsub, l1, l2, nn_nf, nn_lf, z_plq, nsn;
+    int lcomp, nflr, lproju, kinetic, update, nublock, ltrot, nst, nwrap;
+    int lwrapT, lwrapu, phase_on;        // phase_on: rhub > 0 (set_phase multiplies conf phases)
+    double rt, rv, t2, theta;
+    // HS constants (src/dqmc_config_u/dqmc_set_conf.f90)
+    double2 bmat[DQ_MAX_LCOMP], bmat_inv[DQ_MAX_LCOMP], phase[DQ_MAX_LCOMP];
+    double2 delta[DQ_MAX_LCOMP * (DQ_MAX_LCOMP - 1)];        // [(is-1)*(lc-1) + iflip-1]
+    double2 phase_ratio[DQ_MAX_LCOMP * (DQ_MAX_LCOMP - 1)];
+    double gam_ratio[DQ_MAX_LCOMP * (DQ_MAX_LCOMP - 1)];     // gaml(isp)/gaml(is) or 1 (lproju)
+    double phase_angle[DQ_MAX_LCOMP];                        // arg(phase(is)) for set_phase
+    // kinetic
+    const int* bond_i1;        // [nn_nf * nn_lf] 0-based (A site)
+    const int* bond_i2;        // [nn_nf * nn_lf] 0-based (B site)
+    const double2* urt;        // [nn_nf*nn_lf][4]
+    const double2* urtm1;
+    const double2* exph0k;     // [lq], already divided by lq (FFT normalisation)
+    const double2* exph0kinv;
+    const double2* tw1;        // [l1] exp(-2 pi i k / l1)
+    const double2* tw2;        // [l2]
+    // measurement tables (0-based)
+    const int* cell_plus;      // [lq][lq]: cell i with imj(i, j) = d, at [d*lq + j]
+    const int* nnlist;         // [N][nn_nf]
+    const int* snlist;         // [N][nsn]
+    const int* plq_cord;       // [lq][z_plq]
+    const double2* expar_nn;   // [N][nn_nf]
+};
+
+// Per-chain state.  All pointers are device memory.
+struct ChainDev {
+    const ModelDev* md;        // device pointer to this chain's model
+    int N;
+    double2* G;                // current equal-time Green's function
+    double2* Gnew;             // scratch Green's function
+    double2* W[6];             // N x N work matrices
+    double2* U;                // stack (nst+1) x N x N
+    double2* V;
+    double* D;                 // (nst+1) x N
+    double2* logdetQ;          // nst+1
+    double2* A;                // delay / submatrix factors N x nublock
+    double2* B;
+    double2* tau;              // N (Householder scalars)
+    double2* T;                // (N/16+1) x 16 x 16 block-reflector factors
+    double2* smallw;           // 32 x N scratch
+    double* vecs;              // 8 x N real scratch (norms, dmax/dmin)
+    int* perm;                 // N
+    int32_t* conf;             // ltrot x N (site fastest), values 1..lcomp
+    uint32_t* sfmt;            // 624 words + index
+    uint32_t* rnd;             // random words for the current half sweep
+    double2* bins;             // measurement bins (layout: see kern_measure.cu)
+    const int* slotmap;        // logical stack slot -> physical slot (shared by all chains)
+    double* stats;             // per-chain scalars, see ST_* below
+};
+
+// indices into ChainDev::stats
+enum {
+    ST_PHASE_RE = 0, ST_PHASE_IM, ST_LOGW_RE, ST_LOGW_IM,
+    ST_MAX_WRAP, ST_MAX_PHASEDIFF, ST_AVGLOG10, ST_LOGCOUNT, ST_AVGEXPPD,
+    ST_ACC, ST_PROP, ST_NOBS, ST_INFO, ST_LOGDETM_RE, ST_LOGDETM_IM, ST_LAST_WRAP,
+    ST_COUNT = 24
+};
+
+// propagation op encoding: kind | which << 4 | nf << 8 | nt << 16
+enum { PK_CB = 1, PK_FFT = 2, PK_DIAG = 3 };
+enum { PW_FWD = 0, PW_INV = 1, PW_CONJ = 2 };   // urt/bmat/exph0k, urtm1/bmat_inv/exph0kinv, conj(...)
+struct PropProg {
+    int n;
+    int op[DQ_MAX_PROG];
+};

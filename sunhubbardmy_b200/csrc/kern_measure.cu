@@ -1,0 +1,204 @@
+// Equal-time measurement of one time slice, one CTA per chain.
+//
+// Reference: src/dqmc_measure/equaltime_measure.f90 (equaltime_measure 1-69,
+// zkint, zint_u, zint_v, zqsq, ztsq, ztq, measure_cpcm/spsm/nn/jj/bondcorr/
+// paircorr).  Observables use Gc(i,j) = delta_ij - G(j,i) and are weighted
+// with zphi = sgn/Re(phase) * phase.  The distance-binned correlations are
+// accumulated without atomics: one thread owns one bin (distance d, orbitals
+// a, b) and walks the unit cells j, pairing each with cell i = j + d from a
+// precomputed table (imj(i, j) = d).
+//
+// Bin layout per chain (complex): energy[10], cpcm, spsm, nn, pair_onsite
+// [lq*4 each, index (d) + lq*(no_i + 2 no_j)], jj, bb, pair_nn, pair_sn [lq
+// each], zn[2], zj, zb.
+#include "chain_access.cuh"
+#include "kernels.h"
+
+DQ_DEV double2 gcf(const double2* G, int N, int i, int j) {   // Gc(i,j)
+    double2 g = G[MIDX(j, i, N)];
+    return cmk((i == j ? 1.0 : 0.0) - g.x, -g.y);
+}
+DQ_DEV double2 gf(const double2* G, int N, int i, int j) { return G[MIDX(i, j, N)]; }
+
+__global__ void __launch_bounds__(256) k_measure(const ChainDev* __restrict__ chains) {
+    __shared__ double red[64];
+    const ChainDev c = chains[blockIdx.x];
+    const ModelDev& md = *c.md;
+    const int N = c.N, lq = md.lq, tid = threadIdx.x, nth = blockDim.x;
+    const int nnf = md.nn_nf, zp = md.z_plq, nflr = md.nflr;
+    const double2* G = c.G;
+    double2* bins = c.bins;
+    const double2 phase = cmk(c.stats[ST_PHASE_RE], c.stats[ST_PHASE_IM]);
+    const double sgn = phase.x < 0.0 ? -1.0 : 1.0;
+    const double2 zphi = cscale(phase, sgn / phase.x);
+    const double fsp = 1.0 - 1.0 / (double)(nflr * nflr), fn = 1.0 / (double)nflr;
+    const bool hc = (md.nsub == 2);
+
+    // ---- energy terms ----
+    double2 zne = cmk(0, 0), zu = cmk(0, 0), zk = cmk(0, 0), zv = cmk(0, 0);
+    for (int i = tid; i < N; i += nth) {
+        double2 d = gcf(G, N, i, i);
+        zne = cadd(zne, d);
+        zu = cadd(zu, cmul(d, d));
+        if (md.t2 != 0.0) {
+            int ns = hc ? 6 : 4;
+            for (int f = 0; f < ns; ++f) zk.x += -md.t2 * gcf(G, N, i, md.snlist[i * md.nsn + f]).x;
+        }
+    }
+    for (int b = tid; b < md.nn_lf * nnf; b += nth) {
+        int i1 = md.bond_i1[b], i2 = md.bond_i2[b], nf = b / md.nn_lf;
+        double2 g = gcf(G, N, i1, i2);
+        zk.x += -2.0 * cmul(g, md.expar_nn[i1 * nnf + nf]).x;
+        zv.x += g.x;
+    }
+    // plaquette terms
+    double2 zq = cmk(0, 0), zt = cmk(0, 0), ztq = cmk(0, 0);
+    const double2 em = cexpi(-md.theta), ep = cexpi(md.theta);
+    for (int q = tid; q < lq; q += nth) {
+        const int* pc = md.plq_cord + q * zp;
+        double2 tmp = cmk(0, 0);
+        for (int a = 0; a < zp; ++a) tmp = cadd(tmp, gcf(G, N, pc[a], pc[a]));
+        zq = cadd(zq, cscale(cmul(tmp, tmp), (double)nflr));
+        for (int a = 0; a < zp; ++a)
+            for (int b = 0; b < zp; ++b) zq = cfma(gcf(G, N, pc[a], pc[b]), gf(G, N, pc[a], pc[b]), zq);
+        double tt = 0.0, t1 = 0.0;
+        double2 t2 = cmk(0, 0);
+        for (int a = 1; a <= zp; ++a) {
+            int i1 = pc[a - 1], i1a = pc[(a % zp)];
+            double2 z1 = (a % 2 == 0) ? cmk(-ep.x, -ep.y) : em;
+            double v = 2.0 * cmul(z1, gcf(G, N, i1, i1a)).x;
+            tt += v; t1 += v;
+            t2 = cadd(t2, cscale(gcf(G, N, i1, i1), 1.0 / 3.0));
+        }
+        zt.x += tt * tt * nflr;
+        ztq = cadd(ztq, cscale(t2, t1 * nflr));
+        for (int a = 1; a <= zp; ++a) {
+            int i1 = pc[a - 1], i1a = pc[(a % zp)];
+            double2 z1 = (a % 2 == 0) ? cmk(-ep.x, -ep.y) : em, z2 = cconj(z1);
+            double2 y1 = cscale(z1, 1.0 / 3.0), y2 = cconj(y1);
+            for (int b = 1; b <= zp; ++b) {
+                int i2 = pc[b - 1], i2a = pc[(b % zp)];
+                double2 z3 = (b % 2 == 0) ? cmk(-ep.x, -ep.y) : em, z4 = cconj(z3);
+                zt = cadd(zt, cmul(cmul(z1, z3), cmul(gcf(G, N, i1, i2a), gf(G, N, i1a, i2))));
+                zt = cadd(zt, cmul(cmul(z1, z4), cmul(gcf(G, N, i1, i2), gf(G, N, i1a, i2a))));
+                zt = cadd(zt, cmul(cmul(z2, z3), cmul(gcf(G, N, i1a, i2a), gf(G, N, i1, i2))));
+                zt = cadd(zt, cmul(cmul(z2, z4), cmul(gcf(G, N, i1a, i2), gf(G, N, i1, i2a))));
+                ztq = cadd(ztq, cmul(y1, cmul(gcf(G, N, i1, i2), gf(G, N, i1a, i2))));
+                ztq = cadd(ztq, cmul(y2, cmul(gcf(G, N, i1a, i2), gf(G, N, i1, i2))));
+            }
+        }
+    }
+    zne = block_csum(zne, red);
+    zu = block_csum(zu, red);
+    zk = block_csum(zk, red);
+    zv = block_csum(zv, red);
+    zq = block_csum(zq, red);
+    zt = block_csum(zt, red);
+    ztq = block_csum(ztq, red);
+    // background terms zn, zj, zb
+    double2 zn0 = cmk(0, 0), zn1 = cmk(0, 0), zj = cmk(0, 0), zb = cmk(0, 0);
+    for (int j = tid; j < N; j += nth) {
+        double2 d = gcf(G, N, j, j);
+        if (hc && (j & 1)) zn1 = cadd(zn1, d); else zn0 = cadd(zn0, d);
+    }
+    for (int cj = tid; cj < lq; cj += nth) {
+        int j0 = hc ? 2 * cj : cj;
+        int jnj = hc ? md.snlist[j0 * md.nsn] : md.nnlist[j0 * nnf];
+        int jnb = md.nnlist[j0 * nnf];
+        double2 e = md.expar_nn[j0 * nnf];
+        double2 dj = csub(gcf(G, N, j0, jnj), gcf(G, N, jnj, j0));
+        zj = cadd(zj, cmk(-dj.y, dj.x));
+        zb = cadd(zb, cadd(cmul(e, gcf(G, N, j0, jnb)), cmul(cconj(e), gcf(G, N, jnb, j0))));
+    }
+    zn0 = block_csum(zn0, red);
+    zn1 = block_csum(zn1, red);
+    zj = block_csum(zj, red);
+    zb = block_csum(zb, red);
+    if (tid == 0) {
+        bins[0] = cadd(bins[0], cmk(sgn, 0));
+        bins[1] = cadd(bins[1], cscale(cmul(zne, zphi), 1.0 / lq));
+        bins[2] = cadd(bins[2], cmul(zk, zphi));
+        bins[3] = cadd(bins[3], cmul(zu, zphi));
+        bins[4] = cadd(bins[4], cscale(cmul(zq, zphi), 1.0 / 9.0));
+        bins[5] = cadd(bins[5], cmul(zt, zphi));
+        bins[6] = cadd(bins[6], cmul(ztq, zphi));
+        bins[7] = cadd(bins[7], cscale(cmul(zv, zphi), md.rv));
+        size_t tail = 10 + 20 * (size_t)lq;
+        bins[tail + 0] = cadd(bins[tail + 0], cmul(zn0, zphi));
+        bins[tail + 1] = cadd(bins[tail + 1], cmul(zn1, zphi));
+        bins[tail + 2] = cadd(bins[tail + 2], cmul(zj, zphi));
+        bins[tail + 3] = cadd(bins[tail + 3], cmul(zb, zphi));
+        c.stats[ST_NOBS] += 1.0;
+    }
+    // ---- distance-binned correlations ----
+    double2* cpcm = bins + 10;
+    double2* spsm = cpcm + 4 * lq;
+    double2* znn = spsm + 4 * lq;
+    double2* pons = znn + 4 * lq;
+    double2* zjj = pons + 4 * lq;
+    double2* zbb = zjj + lq;
+    double2* pnn = zbb + lq;
+    double2* psn = pnn + lq;
+    const int nsub = md.nsub;
+    for (int bin = tid; bin < lq * nsub * nsub; bin += nth) {
+        int d = bin % lq, ab = bin / lq, a = ab % nsub, b = ab / nsub;
+        double2 s1 = cmk(0, 0), s2 = cmk(0, 0), s3 = cmk(0, 0), s4 = cmk(0, 0);
+        for (int cj = 0; cj < lq; ++cj) {
+            int ci = md.cell_plus[d * lq + cj];
+            int i = ci * nsub + a, j = cj * nsub + b;
+            double2 gc = gcf(G, N, i, j), g = gf(G, N, i, j);
+            s1 = cadd(s1, gc);
+            s2 = cfma(gc, g, s2);
+            s3 = cadd(s3, cadd(cmul(gcf(G, N, i, i), gcf(G, N, j, j)), cscale(cmul(gc, g), fn)));
+            s4 = cfma(g, g, s4);
+        }
+        int k = d + lq * (a + 2 * b);
+        cpcm[k] = cfma(s1, zphi, cpcm[k]);
+        spsm[k] = cfma(cscale(s2, fsp), zphi, spsm[k]);
+        znn[k] = cfma(s3, zphi, znn[k]);
+        pons[k] = cfma(s4, zphi, pons[k]);
+    }
+    for (int d = tid; d < lq; d += nth) {
+        double2 sj = cmk(0, 0), sb = cmk(0, 0), sn = cmk(0, 0), ss = cmk(0, 0);
+        for (int cj = 0; cj < lq; ++cj) {
+            int ci = md.cell_plus[d * lq + cj];
+            int j0 = hc ? 2 * cj : cj, i0 = hc ? 2 * ci : ci;
+            int jnj = hc ? md.snlist[j0 * md.nsn] : md.nnlist[j0 * nnf];
+            int inj = hc ? md.snlist[i0 * md.nsn] : md.nnlist[i0 * nnf];
+            int jnb = md.nnlist[j0 * nnf], inb = md.nnlist[i0 * nnf];
+            int jns = md.snlist[j0 * md.nsn], ins = md.snlist[i0 * md.nsn];
+            double2 z1 = cmul(csub(gcf(G, N, i0, inj), gcf(G, N, inj, i0)), csub(gcf(G, N, j0, jnj), gcf(G, N, jnj, j0)));
+            double2 z3 = cadd(cmul(gcf(G, N, i0, jnj), gf(G, N, inj, j0)), cmul(gcf(G, N, inj, j0), gf(G, N, i0, jnj)));
+            z3 = csub(z3, cadd(cmul(gcf(G, N, i0, j0), gf(G, N, inj, jnj)), cmul(gcf(G, N, inj, jnj), gf(G, N, i0, j0))));
+            sj = csub(sj, cadd(z1, cscale(z3, fn)));
+            double2 ej = md.expar_nn[j0 * nnf], ei = md.expar_nn[i0 * nnf];
+            double2 bj = cadd(cmul(ej, gcf(G, N, j0, jnb)), cmul(cconj(ej), gcf(G, N, jnb, j0)));
+            double2 bi = cadd(cmul(ei, gcf(G, N, i0, inb)), cmul(cconj(ei), gcf(G, N, inb, i0)));
+            double2 x = cmul(cmul(ei, ej), cmul(gcf(G, N, i0, jnb), gf(G, N, inb, j0)));
+            x = cadd(x, cmul(cmul(cconj(ei), cconj(ej)), cmul(gcf(G, N, inb, j0), gf(G, N, i0, jnb))));
+            x = cadd(x, cmul(cmul(ei, cconj(ej)), cmul(gcf(G, N, i0, j0), gf(G, N, inb, jnb))));
+            x = cadd(x, cmul(cmul(cconj(ei), ej), cmul(gcf(G, N, inb, jnb), gf(G, N, i0, j0))));
+            sb = cadd(sb, cadd(cmul(bj, bi), cscale(x, fn)));
+            sn = cfma(gf(G, N, i0, j0), gf(G, N, inb, jnb), sn);
+            ss = cfma(gf(G, N, i0, j0), gf(G, N, ins, jns), ss);
+        }
+        zjj[d] = cfma(sj, zphi, zjj[d]);
+        zbb[d] = cfma(sb, zphi, zbb[d]);
+        pnn[d] = cfma(sn, zphi, pnn[d]);
+        psn[d] = cfma(ss, zphi, psn[d]);
+    }
+}
+
+__global__ void k_bins_clear(const ChainDev* __restrict__ chains, int nbins) {
+    const ChainDev c = chains[blockIdx.x];
+    for (int e = threadIdx.x; e < nbins; e += blockDim.x) c.bins[e] = cmk(0, 0);
+    if (threadIdx.x == 0) c.stats[ST_NOBS] = 0.0;
+}
+
+void launch_measure(const ChainDev* chains, int nchains, cudaStream_t st) {
+    k_measure<<<nchains, 256, 0, st>>>(chains);
+}
+
+void launch_bins_clear(const ChainDev* chains, int nchains, int nbins, cudaStream_t st) {
+    k_bins_clear<<<nchains, 256, 0, st>>>(chains, nbins);
+}

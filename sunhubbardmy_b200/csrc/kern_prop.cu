@@ -1,0 +1,140 @@
+// Time-slice propagation: the kinetic factor exp(-dtau K/2) (checkerboard
+// bond families or FFT) and the diagonal HS factor exp(+-V), applied from the
+// left (column pass) or from the right (row pass) to a per-chain N x N matrix.
+//
+// Reference operators: src/dqmc_config_h0/dqmc_{left,right}_{forward,backward}_prop.f90
+// and _hc (checkerboard 18-44, FFT 95-134), src/dqmc_config_u/dqmc_*_prop.f90 (27-32).
+// A pass streams each column (row) of the matrix through shared memory once and
+// applies a whole program of such operators to it, so a full slice wrap (or
+// an nwrap-slice B product for the stabilisation) costs one read and one write
+// of the matrix per side: the pass is HBM/L2-bandwidth bound.
+#include "chain_access.cuh"
+#include "kernels.h"
+
+// One operator applied to `nv` vectors held in shared memory (vector v at
+// S + v*vs, element stride 1).  right = 0: vectors are columns and the operator
+// multiplies from the left; right = 1: vectors are rows (x -> x * Op).
+__device__ void apply_op(const ModelDev& md, const int32_t* conf, int code, int right,
+                         double2* S, int nv, int vs) {
+    const int kind = code & 15, which = (code >> 4) & 15, nf = (code >> 8) & 255, nt = code >> 16;
+    const int N = md.N, tid = threadIdx.x, nth = blockDim.x;
+    if (kind == PK_CB) {
+        const int lf = md.nn_lf;
+        const double2* U = (which == PW_INV) ? md.urtm1 : md.urt;
+        for (int w = tid; w < nv * lf; w += nth) {
+            int v = w / lf, b = w % lf;
+            int ist = (nf - 1) * lf + b;
+            int i1 = md.bond_i1[ist], i2 = md.bond_i2[ist];
+            const double2* u = U + 4 * ist;   // u[0]=(1,1) u[1]=(1,2) u[2]=(2,1) u[3]=(2,2)
+            double2* x = S + (size_t)v * vs;
+            double2 a = x[i1], c = x[i2];
+            if (!right) {
+                x[i1] = cadd(cmul(u[0], a), cmul(u[1], c));
+                x[i2] = cadd(cmul(u[2], a), cmul(u[3], c));
+            } else {
+                x[i1] = cadd(cmul(a, u[0]), cmul(c, u[2]));
+                x[i2] = cadd(cmul(a, u[1]), cmul(c, u[3]));
+            }
+        }
+    } else if (kind == PK_DIAG) {
+        const int32_t* cf = conf + (size_t)(nt - 1) * N;
+        for (int w = tid; w < nv * N; w += nth) {
+            int v = w / N, i = w % N;
+            int is = cf[i] - 1;
+            double2 b = (which == PW_INV) ? md.bmat_inv[is] : md.bmat[is];
+            if (which == PW_CONJ) b.y = -b.y;
+            double2* x = S + (size_t)v * vs;
+            x[i] = cmul(x[i], b);
+        }
+    } else if (kind == PK_FFT) {
+        // left:  x <- F^-1 D F x ; right (row r): r <- F D F^-1 r  (F symmetric)
+        const int l1 = md.l1, l2 = md.l2, lq = md.lq;
+        const double2* d = (which == PW_INV) ? md.exph0kinv : md.exph0k;
+        const int s1 = right ? +1 : -1;
+        // dim 1 (stride 1, l2 lines), then dim 2 (stride l1, l1 lines)
+        for (int w = tid; w < nv * l2; w += nth) {
+            int v = w / l2, j2 = w % l2;
+            line_dft(S + (size_t)v * vs + j2 * l1, l1, 1, md.tw1, s1);
+        }
+        __syncthreads();
+        for (int w = tid; w < nv * l1; w += nth) {
+            int v = w / l1, j1 = w % l1;
+            line_dft(S + (size_t)v * vs + j1, l2, l1, md.tw2, s1);
+        }
+        __syncthreads();
+        for (int w = tid; w < nv * lq; w += nth) {
+            int v = w / lq, k = w % lq;
+            double2 dk = d[k];
+            if (which == PW_CONJ) dk.y = -dk.y;
+            double2* x = S + (size_t)v * vs;
+            x[k] = cmul(x[k], dk);
+        }
+        __syncthreads();
+        for (int w = tid; w < nv * l2; w += nth) {
+            int v = w / l2, j2 = w % l2;
+            line_dft(S + (size_t)v * vs + j2 * l1, l1, 1, md.tw1, -s1);
+        }
+        __syncthreads();
+        for (int w = tid; w < nv * l1; w += nth) {
+            int v = w / l1, j1 = w % l1;
+            line_dft(S + (size_t)v * vs + j1, l2, l1, md.tw2, -s1);
+        }
+    }
+    __syncthreads();
+}
+
+// Column pass: X <- Op_k ... Op_1 X for the program prog.
+__global__ void k_prop_cols(const ChainDev* __restrict__ chains, int mat_id, PropProg prog, int cb) {
+    extern __shared__ double2 sm[];
+    const ChainDev c = chains[blockIdx.y];
+    const ModelDev& md = *c.md;
+    const int N = c.N;
+    double2* X = chain_mat(c, mat_id);
+    for (int c0 = blockIdx.x * cb; c0 < N; c0 += gridDim.x * cb) {
+        int nv = min(cb, N - c0);
+        for (int e = threadIdx.x; e < nv * N; e += blockDim.x) sm[e] = X[(size_t)c0 * N + e];
+        __syncthreads();
+        for (int k = 0; k < prog.n; ++k) apply_op(md, c.conf, prog.op[k], 0, sm, nv, N);
+        for (int e = threadIdx.x; e < nv * N; e += blockDim.x) X[(size_t)c0 * N + e] = sm[e];
+        __syncthreads();
+    }
+}
+
+// Row pass: X <- X Op_1 ... Op_k.  Rows are staged with a padded stride.
+__global__ void k_prop_rows(const ChainDev* __restrict__ chains, int mat_id, PropProg prog, int rb) {
+    extern __shared__ double2 sm[];
+    const ChainDev c = chains[blockIdx.y];
+    const ModelDev& md = *c.md;
+    const int N = c.N, vs = N + 1;
+    double2* X = chain_mat(c, mat_id);
+    for (int r0 = blockIdx.x * rb; r0 < N; r0 += gridDim.x * rb) {
+        int nv = min(rb, N - r0);
+        for (int e = threadIdx.x; e < nv * N; e += blockDim.x) {
+            int r = e % nv, j = e / nv;
+            sm[r * vs + j] = X[MIDX(r0 + r, j, N)];
+        }
+        __syncthreads();
+        for (int k = 0; k < prog.n; ++k) apply_op(md, c.conf, prog.op[k], 1, sm, nv, vs);
+        for (int e = threadIdx.x; e < nv * N; e += blockDim.x) {
+            int r = e % nv, j = e / nv;
+            X[MIDX(r0 + r, j, N)] = sm[r * vs + j];
+        }
+        __syncthreads();
+    }
+}
+
+static int g_prop_smem_ok = 0;
+
+void launch_prop(const ChainDev* chains, int nchains, int maxN, int mat_id, const PropProg& prog,
+                 int right, int ctas_per_chain, cudaStream_t st) {
+    const int nb = 16;
+    size_t smem = (size_t)nb * (maxN + 1) * sizeof(double2);
+    if (!g_prop_smem_ok) {
+        cudaFuncSetAttribute(k_prop_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(k_prop_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        g_prop_smem_ok = 1;
+    }
+    dim3 grid(ctas_per_chain, nchains);
+    if (right) k_prop_rows<<<grid, 256, smem, st>>>(chains, mat_id, prog, nb);
+    else k_prop_cols<<<grid, 256, smem, st>>>(chains, mat_id, prog, nb);
+}

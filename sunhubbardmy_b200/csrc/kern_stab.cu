@@ -1,0 +1,375 @@
+// UDV stabilisation and the equal-time Green's function, one CTA per chain.
+//
+// Reference: src/dqmc_ft_core/dqmc_ft_stablize_0b_qr.f90 / _b0_qr.f90 (1-61),
+// green_equaltime.f90 (1-107), green_equaltimebb.f90 (1-84), set_phase.f90,
+// and the s_matrix helpers they call (s_z_x_diag_d, s_zmcpt, s_zgeQR_logdetQ,
+// s_invdiag_d_x_zr, s_zpm, s_dvec_min_max, s_compare_max_z).
+//
+// Differences in method, not in result:
+//  * the columns are always pre-sorted by norm (s_zmcpt) and factored without
+//    pivoting; the reference uses zgeqp3 for its first/last step, where the
+//    previous D is 1 and V is the identity, so the same code path applies;
+//  * the inverse of the scaled middle matrix M is taken through its QR
+//    factors (G = U_L dlmax^-1 R^-1 Q^H drmax^-1 U_R^H, log det M = log det Q +
+//    sum log R_ii) instead of an LU factorisation and explicit inverse.
+#include "chain_access.cuh"
+#include "kernels.h"
+#include "linalg.cuh"
+
+struct StabSmem {
+    LinalgSmem L;
+    double red[64];
+};
+
+DQ_DEV LinalgScratch make_scratch(const ChainDev& c) {
+    LinalgScratch s;
+    s.Vs = c.W[5];
+    s.Ws = c.smallw;
+    s.Ws2 = c.smallw + (size_t)QR_NB * c.N;
+    s.T = c.T;
+    s.tau = c.tau;
+    return s;
+}
+
+static size_t stab_smem_bytes(int maxN) {
+    size_t a = (size_t)maxN * QR_NB;
+    size_t b = GemmBig::SMEM_ELEMS;
+    if ((size_t)GemmWide::SMEM_ELEMS > b) b = GemmWide::SMEM_ELEMS;
+    return (a > b ? a : b) * sizeof(double2) + sizeof(StabSmem) + 64;
+}
+
+// one UDV step: W0 holds B(slices) * U[src]; writes U/D/V/logdetQ of slot dst.
+__global__ void __launch_bounds__(256) k_stab(const ChainDev* __restrict__ chains, int src, int dst) {
+    extern __shared__ double2 ssm[];
+    const ChainDev c = chains[blockIdx.x];
+    const int N = c.N, tid = threadIdx.x, nth = blockDim.x;
+    const size_t NN = (size_t)N * N;
+    double2* buf = ssm;
+    StabSmem* S = (StabSmem*)(ssm + (((size_t)N * QR_NB > (size_t)GemmBig::SMEM_ELEMS) ? (size_t)N * QR_NB : (size_t)GemmBig::SMEM_ELEMS));
+    LinalgScratch sc = make_scratch(c);
+    double2* W0 = c.W[0];
+    double2* W2 = c.W[1];
+    double2* W3 = c.W[2];
+    double2* W4 = c.W[3];
+    src = c.slotmap[src];
+    dst = c.slotmap[dst];
+    const double* Dsrc = c.D + (size_t)src * N;
+    double* Ddst = c.D + (size_t)dst * N;
+    double* nrm = c.vecs;
+    int* perm = c.perm;
+
+    // column norms of B U D (s_z_x_diag_d + s_zmcpt)
+    const int lane = tid & 31, warp = tid >> 5, nw = nth >> 5;
+    for (int j = warp; j < N; j += nw) {
+        double s = 0.0;
+        for (int r = lane; r < N; r += 32) s += cabs2(W0[MIDX(r, j, N)]);
+        s = warp_sum(s);
+        if (lane == 0) nrm[j] = sqrt(s) * fabs(Dsrc[j]);
+    }
+    __syncthreads();
+    // descending stable rank sort
+    for (int j = tid; j < N; j += nth) {
+        double v = nrm[j];
+        int rank = 0;
+        for (int k = 0; k < N; ++k) {
+            double w = nrm[k];
+            rank += (w > v) || (w == v && k < j);
+        }
+        perm[rank] = j;
+    }
+    __syncthreads();
+    for (size_t e = tid; e < NN; e += nth) {
+        int r = (int)(e % N), k = (int)(e / N);
+        int j = perm[k];
+        W2[e] = cscale(W0[MIDX(r, j, N)], Dsrc[j]);
+    }
+    __syncthreads();
+    cta_qr(W2, N, sc, buf, buf, &S->L);
+    for (int i = tid; i < N; i += nth) Ddst[i] = W2[MIDX(i, i, N)].x;
+    double2 ldq = cta_logdet_q(sc.tau, N, S->red);
+    if (tid == 0) c.logdetQ[dst] = ldq;
+    __syncthreads();
+    // Vt = D^-1 R
+    for (size_t e = tid; e < NN; e += nth) {
+        int r = (int)(e % N), k = (int)(e / N);
+        W3[e] = (r <= k) ? cscale(W2[e], 1.0 / Ddst[r]) : cmk(0, 0);
+    }
+    // P^T V_src: row k <- row perm[k]
+    const double2* Vsrc = c.V + (size_t)src * NN;
+    for (size_t e = tid; e < NN; e += nth) {
+        int r = (int)(e % N), k = (int)(e / N);
+        W4[e] = Vsrc[MIDX(perm[r], k, N)];
+    }
+    __syncthreads();
+    cta_form_q(W2, N, c.U + (size_t)dst * NN, sc, buf);
+    ZGemmArgs g;
+    g.M = N; g.N = N; g.K = N; g.alpha = cmk(1, 0); g.beta = cmk(0, 0);
+    g.A = W3; g.lda = N; g.opA = OP_N; g.B = W4; g.ldb = N; g.opB = OP_N;
+    g.C = c.V + (size_t)dst * NN; g.ldc = N;
+    zgemm_cta<GemmBig>(g, 0, 1, buf);
+}
+
+// s_dvec_min_max
+DQ_DEV void dminmax(double d, double& dmax, double& dmin) {
+    if (fabs(d) > 1.0) { dmax = fabs(d); dmin = copysign(1.0, d); }
+    else { dmax = 1.0; dmin = d; }
+}
+
+// Green's function into Gnew.  mode 0: green_equaltime(R = slot nr, L = slot nl);
+// mode 1: green_equaltimebb (R = slot nr).  New log weight -> stats[ST_LOGDETM_*].
+__global__ void __launch_bounds__(256) k_green(const ChainDev* __restrict__ chains, int nr, int nl, int mode) {
+    extern __shared__ double2 ssm[];
+    const ChainDev c = chains[blockIdx.x];
+    const int N = c.N, tid = threadIdx.x, nth = blockDim.x;
+    const size_t NN = (size_t)N * N;
+    double2* buf = ssm;
+    StabSmem* S = (StabSmem*)(ssm + (((size_t)N * QR_NB > (size_t)GemmBig::SMEM_ELEMS) ? (size_t)N * QR_NB : (size_t)GemmBig::SMEM_ELEMS));
+    LinalgScratch sc = make_scratch(c);
+    nr = c.slotmap[nr];
+    if (mode == 0) nl = c.slotmap[nl];
+    const double2* UR = c.U + (size_t)nr * NN;
+    const double2* VR = c.V + (size_t)nr * NN;
+    const double* DR = c.D + (size_t)nr * N;
+    double* drmax = c.vecs + 0 * N;
+    double* drmin = c.vecs + 1 * N;
+    double* dlmax = c.vecs + 2 * N;
+    double* dlmin = c.vecs + 3 * N;
+    double2* M = c.W[0];
+    double2* Z = c.W[1];
+    double slog = 0.0;
+    for (int i = tid; i < N; i += nth) {
+        double a, b;
+        dminmax(DR[i], a, b);
+        drmax[i] = a; drmin[i] = b;
+        slog += log(a);
+    }
+    if (mode == 0) {
+        const double2* UL = c.U + (size_t)nl * NN;
+        const double2* VL = c.V + (size_t)nl * NN;
+        const double* DL = c.D + (size_t)nl * N;
+        for (int i = tid; i < N; i += nth) {
+            double a, b;
+            dminmax(DL[i], a, b);
+            dlmax[i] = a; dlmin[i] = b;
+            slog += log(a);
+        }
+        ZGemmArgs g;
+        g.M = N; g.N = N; g.K = N; g.alpha = cmk(1, 0); g.beta = cmk(0, 0);
+        g.A = UR; g.lda = N; g.opA = OP_C; g.B = UL; g.ldb = N; g.opB = OP_N; g.C = M; g.ldc = N;
+        zgemm_cta<GemmBig>(g, 0, 1, buf);
+        g.A = VR; g.opA = OP_N; g.B = VL; g.opB = OP_C; g.C = Z;
+        zgemm_cta<GemmBig>(g, 0, 1, buf);
+        for (size_t e = tid; e < NN; e += nth) {
+            int i = (int)(e % N), j = (int)(e / N);
+            double2 u = cscale(M[e], 1.0 / (drmax[i] * dlmax[j]));
+            M[e] = cadd(u, cscale(Z[e], drmin[i] * dlmin[j]));
+        }
+    } else {
+        for (size_t e = tid; e < NN; e += nth) {
+            int i = (int)(e % N), j = (int)(e / N);
+            M[e] = cadd(cscale(cconj(UR[MIDX(j, i, N)]), 1.0 / drmax[i]), cscale(VR[e], drmin[i]));
+        }
+    }
+    slog = block_sum(slog, S->red);
+    __syncthreads();
+    cta_qr(M, N, sc, buf, buf, &S->L);
+    double2 ldm = cta_logdet_q(sc.tau, N, S->red);
+    double2 lr = cmk(0, 0);
+    for (int i = tid; i < N; i += nth) {
+        double r = M[MIDX(i, i, N)].x;
+        lr = cadd(lr, cmk(log(fabs(r)), r < 0.0 ? M_PI : 0.0));
+    }
+    lr = block_csum(lr, S->red);
+    ldm = cadd(ldm, lr);
+    double2* X = (mode == 0) ? Z : c.Gnew;
+    for (size_t e = tid; e < NN; e += nth) {
+        int i = (int)(e % N), j = (int)(e / N);
+        X[e] = cscale(cconj(UR[MIDX(j, i, N)]), 1.0 / drmax[i]);
+    }
+    __syncthreads();
+    cta_apply_qh(M, N, X, sc, buf);
+    cta_trsm_upper(M, N, X, buf, &S->L);
+    if (mode == 0) {
+        const double2* UL = c.U + (size_t)nl * NN;
+        double2* UL2 = c.W[2];
+        for (size_t e = tid; e < NN; e += nth) {
+            int j = (int)(e / N);
+            UL2[e] = cscale(UL[e], 1.0 / dlmax[j]);
+        }
+        __syncthreads();
+        ZGemmArgs g;
+        g.M = N; g.N = N; g.K = N; g.alpha = cmk(1, 0); g.beta = cmk(0, 0);
+        g.A = UL2; g.lda = N; g.opA = OP_N; g.B = Z; g.ldb = N; g.opB = OP_N; g.C = c.Gnew; g.ldc = N;
+        zgemm_cta<GemmBig>(g, 0, 1, buf);
+    }
+    if (tid == 0) {
+        double2 lw = cadd(ldm, cmk(slog, 0.0));
+        lw = cadd(lw, c.logdetQ[nr]);
+        if (mode == 0) lw = csub(lw, c.logdetQ[nl]);
+        c.stats[ST_LOGDETM_RE] = lw.x;
+        c.stats[ST_LOGDETM_IM] = lw.y;
+    }
+}
+
+// s_compare_max_z + set_phase + replacement of G (dqmc_ft_sweep_b0.f90:145-194)
+__global__ void __launch_bounds__(256) k_wrap_check(const ChainDev* __restrict__ chains, int record) {
+    __shared__ double red[64];
+    const ChainDev c = chains[blockIdx.x];
+    const ModelDev& md = *c.md;
+    const int N = c.N, tid = threadIdx.x, nth = blockDim.x;
+    const size_t NN = (size_t)N * N;
+    double mx = 0.0;
+    for (size_t e = tid; e < NN; e += nth) {
+        double2 d = csub(c.Gnew[e], c.G[e]);
+        mx = fmax(mx, cabsd(d));
+        c.G[e] = c.Gnew[e];
+    }
+    mx = block_max(mx, red);
+    double ang = 0.0;
+    if (md.phase_on) {
+        const size_t nconf = (size_t)md.ltrot * N;
+        for (size_t e = tid; e < nconf; e += nth) ang += md.phase_angle[c.conf[e] - 1];
+    }
+    ang = block_sum(ang, red);
+    if (tid == 0) {
+        double2 lw = cmk(c.stats[ST_LOGDETM_RE], c.stats[ST_LOGDETM_IM]);
+        double2 ph = cexpi(md.nflr * lw.y + ang);
+        if (record) {
+            double2 old = cmk(c.stats[ST_PHASE_RE], c.stats[ST_PHASE_IM]);
+            double pd = cabsd(csub(old, ph));
+            c.stats[ST_MAX_WRAP] = fmax(c.stats[ST_MAX_WRAP], mx);
+            c.stats[ST_MAX_PHASEDIFF] = fmax(c.stats[ST_MAX_PHASEDIFF], pd);
+            c.stats[ST_LOGCOUNT] += 1.0;
+            c.stats[ST_AVGLOG10] += log10(mx);
+            c.stats[ST_AVGEXPPD] += exp(pd);
+            c.stats[ST_LAST_WRAP] = mx;
+        }
+        c.stats[ST_PHASE_RE] = ph.x;
+        c.stats[ST_PHASE_IM] = ph.y;
+        c.stats[ST_LOGW_RE] = lw.x;
+        c.stats[ST_LOGW_IM] = lw.y;
+    }
+}
+
+__global__ void k_copy_mat(const ChainDev* __restrict__ chains, int dst_id, int src_id, int identity) {
+    const ChainDev c = chains[blockIdx.y];
+    const size_t NN = (size_t)c.N * c.N;
+    double2* d = chain_mat(c, dst_id);
+    const double2* s = identity ? nullptr : chain_mat(c, src_id);
+    for (size_t e = blockIdx.x * blockDim.x + threadIdx.x; e < NN; e += (size_t)gridDim.x * blockDim.x) {
+        if (identity) d[e] = cmk((e % c.N) == (e / c.N) ? 1.0 : 0.0, 0.0);
+        else d[e] = s[e];
+    }
+}
+
+// identity stack entry: U = V = I, D = 1, logdetQ = 0
+__global__ void k_stack_identity(const ChainDev* __restrict__ chains, int slot) {
+    const ChainDev c = chains[blockIdx.y];
+    slot = c.slotmap[slot];
+    const int N = c.N;
+    const size_t NN = (size_t)N * N;
+    double2* U = c.U + (size_t)slot * NN;
+    double2* V = c.V + (size_t)slot * NN;
+    for (size_t e = blockIdx.x * blockDim.x + threadIdx.x; e < NN; e += (size_t)gridDim.x * blockDim.x) {
+        double2 v = cmk((e % N) == (e / N) ? 1.0 : 0.0, 0.0);
+        U[e] = v; V[e] = v;
+        if (e < (size_t)N) c.D[(size_t)slot * N + e] = 1.0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) c.logdetQ[slot] = cmk(0, 0);
+}
+
+__global__ void __launch_bounds__(256) k_zgemm_test(const ChainDev* __restrict__ chains, int m, int n, int k, int opa, int opb,
+                                                    int a_id, int b_id, int c_id, double beta_re) {
+    extern __shared__ double2 ssm[];
+    const ChainDev c = chains[blockIdx.y];
+    ZGemmArgs g;
+    g.M = m; g.N = n; g.K = k; g.alpha = cmk(1, 0); g.beta = cmk(beta_re, 0);
+    g.A = chain_mat(c, a_id); g.lda = c.N; g.opA = opa;
+    g.B = chain_mat(c, b_id); g.ldb = c.N; g.opB = opb;
+    g.C = chain_mat(c, c_id); g.ldc = c.N;
+    zgemm_cta<GemmBig>(g, blockIdx.x, gridDim.x, ssm);
+}
+
+// QR of matrix a_id in place; Q into q_id; logdetQ into stats[ST_LOGDETM]
+__global__ void __launch_bounds__(256) k_qr_test(const ChainDev* __restrict__ chains, int a_id, int q_id) {
+    extern __shared__ double2 ssm[];
+    const ChainDev c = chains[blockIdx.x];
+    const int N = c.N;
+    StabSmem* S = (StabSmem*)(ssm + (((size_t)N * QR_NB > (size_t)GemmBig::SMEM_ELEMS) ? (size_t)N * QR_NB : (size_t)GemmBig::SMEM_ELEMS));
+    LinalgScratch sc = make_scratch(c);
+    double2* A = chain_mat(c, a_id);
+    cta_qr(A, N, sc, ssm, ssm, &S->L);
+    double2 ld = cta_logdet_q(sc.tau, N, S->red);
+    if (threadIdx.x == 0) { c.stats[ST_LOGDETM_RE] = ld.x; c.stats[ST_LOGDETM_IM] = ld.y; }
+    __syncthreads();
+    cta_form_q(A, N, chain_mat(c, q_id), sc, ssm);
+}
+
+// swap logical slot n with the spare slot (logical id `spare`)
+__global__ void k_swap_slots(int* slotmap, int n, int spare) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        int t = slotmap[n]; slotmap[n] = slotmap[spare]; slotmap[spare] = t;
+    }
+}
+
+static int g_stab_attr = 0;
+static void stab_attrs() {
+    if (g_stab_attr) return;
+    cudaFuncSetAttribute(k_stab, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_green, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_qr_test, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_zgemm_test, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    g_stab_attr = 1;
+}
+
+static int g_maxN = 512;
+void set_stab_maxN(int n) { g_maxN = n; }
+
+void launch_stab(const ChainDev* chains, int nchains, int n, int dir, int pivoted, cudaStream_t st) {
+    (void)pivoted;
+    stab_attrs();
+    int src = dir == 0 ? n - 1 : n, dst = dir == 0 ? n : n - 1;
+    k_stab<<<nchains, 256, stab_smem_bytes(g_maxN), st>>>(chains, src, dst);
+}
+
+void launch_stab_slots(const ChainDev* chains, int nchains, int src, int dst, cudaStream_t st) {
+    stab_attrs();
+    k_stab<<<nchains, 256, stab_smem_bytes(g_maxN), st>>>(chains, src, dst);
+}
+
+void launch_green(const ChainDev* chains, int nchains, int nr, int nl, int rmat_u, int rmat_v,
+                  int lmat_u, int lmat_v, int mode, cudaStream_t st) {
+    (void)rmat_u; (void)rmat_v; (void)lmat_u; (void)lmat_v;
+    stab_attrs();
+    k_green<<<nchains, 256, stab_smem_bytes(g_maxN), st>>>(chains, nr, nl, mode);
+}
+
+void launch_wrap_check(const ChainDev* chains, int nchains, int record, cudaStream_t st) {
+    k_wrap_check<<<nchains, 256, 0, st>>>(chains, record);
+}
+
+void launch_copy_mat(const ChainDev* chains, int nchains, int dst_id, int src_id, int identity, cudaStream_t st) {
+    dim3 grid(8, nchains);
+    k_copy_mat<<<grid, 256, 0, st>>>(chains, dst_id, src_id, identity);
+}
+
+void launch_swap_slots(int* slotmap, int n, int spare, cudaStream_t st) {
+    k_swap_slots<<<1, 32, 0, st>>>(slotmap, n, spare);
+}
+
+void launch_stack_identity(const ChainDev* chains, int nchains, int slot, cudaStream_t st) {
+    dim3 grid(8, nchains);
+    k_stack_identity<<<grid, 256, 0, st>>>(chains, slot);
+}
+
+void launch_zgemm_test(const ChainDev* chains, int nchains, int m, int n, int k, int opa, int opb,
+                       int a_id, int b_id, int c_id, double beta_re, cudaStream_t st) {
+    stab_attrs();
+    dim3 grid(4, nchains);
+    k_zgemm_test<<<grid, 256, GemmBig::SMEM_ELEMS * sizeof(double2), st>>>(chains, m, n, k, opa, opb, a_id, b_id, c_id, beta_re);
+}
+
+void launch_qr_test(const ChainDev* chains, int nchains, int a_id, int q_id, cudaStream_t st) {
+    stab_attrs();
+    k_qr_test<<<nchains, 256, stab_smem_bytes(g_maxN), st>>>(chains, a_id, q_id);
+}

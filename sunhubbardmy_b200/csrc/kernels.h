@@ -1,0 +1,31 @@
+// Host-side launch wrappers of the CUDA kernels (one CTA or a few CTAs per
+// Markov chain; blockIdx.y / blockIdx.x selects the chain).
+#pragma once
+#include <cuda_runtime.h>
+#include "dqmc_types.h"
+
+void launch_prop(const ChainDev* chains, int nchains, int maxN, int mat_id, const PropProg& prog,
+                 int right, int ctas_per_chain, cudaStream_t st);
+void launch_sfmt(const ChainDev* chains, int nchains, int slices, cudaStream_t st);
+void launch_sfmt_raw(const ChainDev* chains, int chain, int count, cudaStream_t st);
+void launch_update(const ChainDev* chains, int nchains, int nt, int visit, cudaStream_t st);
+void launch_measure(const ChainDev* chains, int nchains, cudaStream_t st);
+void launch_bins_clear(const ChainDev* chains, int nchains, int nbins, cudaStream_t st);
+void launch_stab_slots(const ChainDev* chains, int nchains, int src, int dst, cudaStream_t st);
+void launch_swap_slots(int* slotmap, int n, int spare, cudaStream_t st);
+void launch_stack_identity(const ChainDev* chains, int nchains, int slot, cudaStream_t st);
+void set_stab_maxN(int n);
+void launch_copy_mat(const ChainDev* chains, int nchains, int dst_id, int src_id, int identity, cudaStream_t st);
+// stabilisation step: dir 0 = 0b (writes stack n from n-1), 1 = b0 (writes n-1 from n);
+// pivoted selects the QR with column pivoting of the first/last step.
+void launch_stab(const ChainDev* chains, int nchains, int n, int dir, int pivoted, cudaStream_t st);
+// Green's function from the stack entries (r side, l side) into Gnew; mode 0 =
+// green_equaltime, 1 = green_equaltimebb (l side = identity)
+void launch_green(const ChainDev* chains, int nchains, int nr, int nl, int rmat_u, int rmat_v,
+                  int lmat_u, int lmat_v, int mode, cudaStream_t st);
+// wrap check: compare Gnew with G, recompute the phase, replace G (record = 0: just replace)
+void launch_wrap_check(const ChainDev* chains, int nchains, int record, cudaStream_t st);
+// generic batched complex GEMM on per-chain matrices (diagnostics)
+void launch_zgemm_test(const ChainDev* chains, int nchains, int m, int n, int k, int opa, int opb,
+                       int a_id, int b_id, int c_id, double beta_re, cudaStream_t st);
+void launch_qr_test(const ChainDev* chains, int nchains, int a_id, int q_id, cudaStream_t st);

@@ -1,0 +1,280 @@
+// CTA-level dense complex linear algebra for the UDV stabilisation:
+// blocked Householder QR (LAPACK zgeqrf/zlarft conventions: beta real,
+// H = I - tau v v^H, v(1) = 1), explicit Q (zungqr), Q^H applied to a matrix,
+// and an upper-triangular solve.  The trailing updates and the triangular
+// solve's off-diagonal blocks run through the DMMA GEMM of zgemm.cuh; the
+// panel factorisation runs in shared memory.  One CTA of 256 threads owns
+// one chain's matrices (leading dimension N, N <= 512).
+#pragma once
+#include "zgemm.cuh"
+
+#define QR_NB 16
+
+struct LinalgScratch {
+    double2* Vs;      // N x 16 explicit reflector block (ld N)
+    double2* Ws;      // 16 x N (ld 16)
+    double2* Ws2;     // 16 x N (ld 16)
+    double2* T;       // (N/16 + 1) x 16 x 16 block-reflector triangles
+    double2* tau;     // N
+};
+
+struct LinalgSmem {
+    double red[64];
+    double2 tau_j, scal;
+    double2 Tl[QR_NB * QR_NB];
+    double2 S[QR_NB * QR_NB];
+    double2 w[QR_NB];
+    int flag;
+};
+
+// ---- panel factorisation (zgeqr2 on an m x jb panel in shared memory) ----
+__device__ void panel_qr(double2* P, int m, int jb, double2* taus, LinalgSmem* L) {
+    const int tid = threadIdx.x, nth = blockDim.x;
+    for (int j = 0; j < jb; ++j) {
+        double2* col = P + (size_t)j * m;
+        double ss = 0.0;
+        for (int r = j + 1 + tid; r < m; r += nth) ss += cabs2(col[r]);
+        ss = block_sum(ss, L->red);
+        double xnorm = sqrt(ss);
+        // rescale when the plain sum of squares under/overflows (block-uniform branch)
+        if (!(ss < 1e300) || (ss > 0.0 && ss < 1e-280)) {
+            double mx = 0.0;
+            for (int r = j + 1 + tid; r < m; r += nth) mx = fmax(mx, fmax(fabs(col[r].x), fabs(col[r].y)));
+            mx = block_max(mx, L->red);
+            double s2 = 0.0;
+            if (mx > 0.0)
+                for (int r = j + 1 + tid; r < m; r += nth) s2 += cabs2(cscale(col[r], 1.0 / mx));
+            s2 = block_sum(s2, L->red);
+            xnorm = mx * sqrt(s2);
+        }
+        if (tid == 0) {
+            double2 alpha = col[j];
+            if (xnorm == 0.0 && alpha.y == 0.0) {
+                L->tau_j = cmk(0, 0);
+                L->scal = cmk(1, 0);
+            } else {
+                double ax = fabs(alpha.x), ay = fabs(alpha.y);
+                double w = fmax(ax, fmax(ay, xnorm));
+                double nrm = w * sqrt((ax / w) * (ax / w) + (ay / w) * (ay / w) + (xnorm / w) * (xnorm / w));
+                double beta = -copysign(nrm, alpha.x);
+                L->tau_j = cmk((beta - alpha.x) / beta, -alpha.y / beta);
+                L->scal = cdiv(cmk(1, 0), csub(alpha, cmk(beta, 0)));
+                col[j] = cmk(beta, 0.0);
+            }
+            taus[j] = L->tau_j;
+        }
+        __syncthreads();
+        const double2 tau = L->tau_j, scal = L->scal;
+        if (tau.x == 0.0 && tau.y == 0.0) { __syncthreads(); continue; }
+        for (int r = j + 1 + tid; r < m; r += nth) col[r] = cmul(col[r], scal);
+        __syncthreads();
+        // w_c = v^H P[:, c], c > j ; 16 groups of 16 threads
+        const int grp = tid >> 4, gl = tid & 15;
+        for (int base = j + 1; base < jb; base += nth / 16) {     // uniform trip count
+            const int cc = base + grp;
+            const bool ok = cc < jb;
+            double2 acc = cmk(0, 0);
+            if (ok) {
+                const double2* pc = P + (size_t)cc * m;
+                if (gl == 0) acc = pc[j];
+                for (int r = j + 1 + gl; r < m; r += 16) acc = cfma(cconj(col[r]), pc[r], acc);
+            }
+#pragma unroll
+            for (int o = 8; o > 0; o >>= 1) {
+                acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o, 16);
+                acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o, 16);
+            }
+            if (ok && gl == 0) L->w[cc] = acc;
+        }
+        __syncthreads();
+        // P[r, c] -= conj(tau) v_r w_c
+        const double2 ctau = cconj(tau);
+        const int nc = jb - j - 1, nr = m - j;
+        for (int e = tid; e < nc * nr; e += nth) {
+            int cc = j + 1 + e / nr, r = j + e % nr;
+            double2 v = (r == j) ? cmk(1, 0) : col[r];
+            double2 f = cmul(ctau, L->w[cc]);
+            P[(size_t)cc * m + r] = csub(P[(size_t)cc * m + r], cmul(v, f));
+        }
+        __syncthreads();
+    }
+}
+
+// T (jb x jb upper) of the block reflector H_1..H_jb = I - V T V^H (zlarft 'F','C').
+// V is the unit-lower panel in shared memory (m x jb).
+__device__ void panel_larft(const double2* P, int m, int jb, const double2* taus, double2* Tout, LinalgSmem* L) {
+    const int tid = threadIdx.x;
+    // Gram S(a,b) = V(:,a)^H V(:,b) for a < b
+    for (int e = tid; e < jb * jb; e += blockDim.x) {
+        int a = e % jb, b = e / jb;
+        if (a < b) {
+            double2 s = P[(size_t)a * m + b];          // V(b,a)^* * V(b,b)=1, rows r >= b
+            s = cconj(s);
+            for (int r = b + 1; r < m; ++r) s = cfma(cconj(P[(size_t)a * m + r]), P[(size_t)b * m + r], s);
+            L->S[a + b * QR_NB] = s;
+        }
+    }
+    __syncthreads();
+    if (tid < 32) {
+        for (int i = 0; i < jb; ++i) {
+            double2 ti = taus[i];
+            // t_a = -tau_i S(a, i), a < i ;  T(0:i, i) = T(0:i,0:i) t
+            if (tid < i) {
+                double2 acc = cmk(0, 0);
+                for (int b = tid; b < i; ++b) {
+                    double2 tb = cmul(cmk(-ti.x, -ti.y), L->S[b + i * QR_NB]);
+                    acc = cfma(L->Tl[tid + b * QR_NB], tb, acc);
+                }
+                L->Tl[tid + i * QR_NB] = acc;
+            }
+            if (tid == 0) L->Tl[i + i * QR_NB] = ti;
+            for (int a = i + 1 + tid; a < QR_NB; a += 32) L->Tl[a + i * QR_NB] = cmk(0, 0);
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    for (int e = tid; e < QR_NB * QR_NB; e += blockDim.x) {
+        int a = e % QR_NB, b = e / QR_NB;
+        Tout[e] = (a < jb && b < jb && a <= b) ? L->Tl[e] : cmk(0, 0);
+    }
+    __syncthreads();
+}
+
+// Explicit reflector block of panel p into Vs (rows p..N-1 stored at Vs[r - p], ld N)
+__device__ void build_vblock(const double2* A, int N, int p, int jb, double2* Vs) {
+    int m = N - p;
+    for (int e = threadIdx.x; e < m * jb; e += blockDim.x) {
+        int r = e % m, cc = e / m;
+        double2 v = (r < cc) ? cmk(0, 0) : (r == cc) ? cmk(1, 0) : A[MIDX(p + r, p + cc, N)];
+        Vs[MIDX(r, cc, N)] = v;
+    }
+    __syncthreads();
+}
+
+// X[p:N, c0:c0+nc] <- (I - V T V^H)^op X,  op = H (apply Q^H) or none (apply Q)
+__device__ void apply_block(const double2* Vs, const double2* Tp, int N, int p, int jb,
+                            double2* X, int c0, int nc, int use_th, LinalgScratch& sc, cplx* gsm) {
+    if (nc <= 0) return;
+    int m = N - p;
+    ZGemmArgs g;
+    // W = V^H X
+    g.M = jb; g.N = nc; g.K = m; g.alpha = cmk(1, 0); g.beta = cmk(0, 0);
+    g.A = Vs; g.lda = N; g.opA = OP_C;
+    g.B = X + MIDX(p, c0, N); g.ldb = N; g.opB = OP_N;
+    g.C = sc.Ws; g.ldc = QR_NB;
+    zgemm_cta<GemmWide>(g, 0, 1, gsm);
+    // W2 = T^H W  or  T W
+    for (int e = threadIdx.x; e < jb * nc; e += blockDim.x) {
+        int a = e % jb, cc = e / jb;
+        double2 acc = cmk(0, 0);
+        if (use_th) {
+            for (int b = 0; b <= a; ++b) acc = cfma(cconj(Tp[b + a * QR_NB]), sc.Ws[b + cc * QR_NB], acc);
+        } else {
+            for (int b = a; b < jb; ++b) acc = cfma(Tp[a + b * QR_NB], sc.Ws[b + cc * QR_NB], acc);
+        }
+        sc.Ws2[a + cc * QR_NB] = acc;
+    }
+    __syncthreads();
+    // X -= V W2
+    g.M = m; g.N = nc; g.K = jb; g.alpha = cmk(-1, 0); g.beta = cmk(1, 0);
+    g.A = Vs; g.lda = N; g.opA = OP_N;
+    g.B = sc.Ws2; g.ldb = QR_NB; g.opB = OP_N;
+    g.C = X + MIDX(p, c0, N); g.ldc = N;
+    zgemm_cta<GemmBig>(g, 0, 1, gsm);
+}
+
+// In-place QR of A (N x N): R in the upper triangle, reflectors below,
+// tau and the per-panel T factors in the scratch.  smem_panel holds >= N*16 double2.
+__device__ void cta_qr(double2* A, int N, LinalgScratch& sc, double2* smem_panel, cplx* gsm, LinalgSmem* L) {
+    for (int p = 0; p < N; p += QR_NB) {
+        const int jb = min(QR_NB, N - p), m = N - p;
+        double2* P = smem_panel;
+        for (int e = threadIdx.x; e < m * jb; e += blockDim.x) {
+            int r = e % m, cc = e / m;
+            P[(size_t)cc * m + r] = A[MIDX(p + r, p + cc, N)];
+        }
+        __syncthreads();
+        panel_qr(P, m, jb, sc.tau + p, L);
+        double2* Tp = sc.T + (size_t)(p / QR_NB) * QR_NB * QR_NB;
+        panel_larft(P, m, jb, sc.tau + p, Tp, L);
+        for (int e = threadIdx.x; e < m * jb; e += blockDim.x) {
+            int r = e % m, cc = e / m;
+            A[MIDX(p + r, p + cc, N)] = P[(size_t)cc * m + r];
+            sc.Vs[MIDX(r, cc, N)] = (r < cc) ? cmk(0, 0) : (r == cc) ? cmk(1, 0) : P[(size_t)cc * m + r];
+        }
+        __syncthreads();
+        if (p + jb < N) apply_block(sc.Vs, Tp, N, p, jb, A, p + jb, N - p - jb, 1, sc, gsm);
+    }
+}
+
+// log det Q = sum_i log(1 - tau_i 2 Re(tau_i) / |tau_i|^2)  (s_matrix.f90:1290-1298)
+__device__ double2 cta_logdet_q(const double2* tau, int N, double* red) {
+    double2 acc = cmk(0, 0);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        double2 t = tau[i];
+        double a2 = cabs2(t);
+        if (a2 != 0.0) {
+            double2 z = csub(cmk(1, 0), cscale(t, 2.0 * t.x / a2));
+            acc = cadd(acc, clog_(z));
+        }
+    }
+    return block_csum(acc, red);
+}
+
+// Q (N x N) from the factored A into Qout (zungqr, blocked backward).
+__device__ void cta_form_q(const double2* A, int N, double2* Qout, LinalgScratch& sc, cplx* gsm) {
+    for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
+        int r = e % N, cc = e / N;
+        Qout[e] = cmk(r == cc ? 1.0 : 0.0, 0.0);
+    }
+    __syncthreads();
+    int last = ((N - 1) / QR_NB) * QR_NB;
+    for (int p = last; p >= 0; p -= QR_NB) {
+        const int jb = min(QR_NB, N - p);
+        build_vblock(A, N, p, jb, sc.Vs);
+        const double2* Tp = sc.T + (size_t)(p / QR_NB) * QR_NB * QR_NB;
+        apply_block(sc.Vs, Tp, N, p, jb, Qout, p, N - p, 0, sc, gsm);
+    }
+}
+
+// X <- Q^H X for all N columns of X (Q from the factored A).
+__device__ void cta_apply_qh(const double2* A, int N, double2* X, LinalgScratch& sc, cplx* gsm) {
+    for (int p = 0; p < N; p += QR_NB) {
+        const int jb = min(QR_NB, N - p);
+        build_vblock(A, N, p, jb, sc.Vs);
+        const double2* Tp = sc.T + (size_t)(p / QR_NB) * QR_NB * QR_NB;
+        apply_block(sc.Vs, Tp, N, p, jb, X, 0, N, 1, sc, gsm);
+    }
+}
+
+// X <- R^{-1} X with R the upper triangle of A (blocked back substitution).
+__device__ void cta_trsm_upper(const double2* A, int N, double2* X, cplx* gsm, LinalgSmem* L) {
+    int last = ((N - 1) / QR_NB) * QR_NB;
+    for (int p = last; p >= 0; p -= QR_NB) {
+        const int jb = min(QR_NB, N - p);
+        if (p + jb < N) {
+            ZGemmArgs g;
+            g.M = jb; g.N = N; g.K = N - p - jb; g.alpha = cmk(-1, 0); g.beta = cmk(1, 0);
+            g.A = A + MIDX(p, p + jb, N); g.lda = N; g.opA = OP_N;
+            g.B = X + (p + jb); g.ldb = N; g.opB = OP_N;
+            g.C = X + p; g.ldc = N;
+            zgemm_cta<GemmWide>(g, 0, 1, gsm);
+        }
+        for (int e = threadIdx.x; e < jb * jb; e += blockDim.x) {
+            int a = e % jb, b = e / jb;
+            L->S[a + b * QR_NB] = A[MIDX(p + a, p + b, N)];
+        }
+        __syncthreads();
+        for (int cc = threadIdx.x; cc < N; cc += blockDim.x) {
+            double2 x[QR_NB];
+            for (int a = 0; a < jb; ++a) x[a] = X[MIDX(p + a, cc, N)];
+            for (int a = jb - 1; a >= 0; --a) {
+                double2 s = x[a];
+                for (int b = a + 1; b < jb; ++b) s = csub(s, cmul(L->S[a + b * QR_NB], x[b]));
+                x[a] = cdiv(s, L->S[a + a * QR_NB]);
+            }
+            for (int a = 0; a < jb; ++a) X[MIDX(p + a, cc, N)] = x[a];
+        }
+        __syncthreads();
+    }
+}

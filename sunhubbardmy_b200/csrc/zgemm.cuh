@@ -1,0 +1,195 @@
+// CTA-level complex FP64 GEMM on the FP64 tensor pipe (DMMA, mma.sync m8n8k4).
+//
+//   C[M x N] = alpha * op(A)[M x K] * op(B)[K x N] + beta * C
+//
+// Operand tiles are staged global -> shared with 16-byte cp.async (one complex
+// element per copy, zero-filled outside the matrix) in a two-stage pipeline.
+// A complex product is four real DMMAs on split real/imaginary fragments:
+//   Cr += Ar Br - Ai Bi,  Ci += Ar Bi + Ai Br.
+// The CTA walks output tiles tile0, tile0+tstep, ..., so a single CTA can do a
+// whole matrix (one CTA per Markov chain) or several CTAs can share one.
+#pragma once
+#include "common.cuh"
+
+enum { OP_N = 0, OP_T = 1, OP_C = 2 };
+
+struct ZGemmArgs {
+    int M, N, K;
+    cplx alpha, beta;
+    const cplx* A; int lda; int opA;
+    const cplx* B; int ldb; int opB;
+    cplx* C; int ldc;
+};
+
+DQ_DEV void dmma(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
+}
+
+DQ_DEV void cp_async16(void* smem, const void* gmem, bool valid) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    int n = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" :: "r"(s), "l"(gmem), "r"(n));
+}
+DQ_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+DQ_DEV void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" :: "n"(N)); }
+
+template <int BM_, int BN_, int BK_, int WM_, int WN_>
+struct ZGemmCfg {
+    static constexpr int BM = BM_, BN = BN_, BK = BK_, WM = WM_, WN = WN_;
+    static constexpr int NT = WM * WN * 32;
+    static constexpr int WTM = BM / WM, WTN = BN / WN;
+    static constexpr int FM = WTM / 8, FN = WTN / 8;
+    static constexpr int LDA = BM + 2, LDB = BN + 2;       // = 2 (mod 8): conflict-free fragments
+    static constexpr int SA = BK * LDA, SB = BK * LDB;
+    static constexpr int SMEM_ELEMS = 2 * (SA + SB);       // double2 elements
+    static constexpr int LDC = BM + 1;
+    static_assert(BN * LDC <= SMEM_ELEMS, "epilogue tile must fit in the staging buffers");
+    static_assert(BK % 4 == 0 && WTM % 8 == 0 && WTN % 8 == 0, "tile shape");
+};
+
+template <class Cfg>
+DQ_DEV void zgemm_load_stage(const ZGemmArgs& g, int m0, int n0, int k0, cplx* As, cplx* Bs, int tid, int nthr) {
+    constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK;
+    // A tile -> As[k][m]
+    if (g.opA == OP_N) {
+        for (int e = tid; e < BM * BK; e += nthr) {
+            int m = e % BM, k = e / BM;
+            int gm = m0 + m, gk = k0 + k;
+            bool v = gm < g.M && gk < g.K;
+            const cplx* src = v ? g.A + MIDX(gm, gk, g.lda) : g.A;
+            cp_async16(&As[k * Cfg::LDA + m], src, v);
+        }
+    } else {
+        for (int e = tid; e < BM * BK; e += nthr) {
+            int k = e % BK, m = e / BK;
+            int gm = m0 + m, gk = k0 + k;
+            bool v = gm < g.M && gk < g.K;
+            const cplx* src = v ? g.A + MIDX(gk, gm, g.lda) : g.A;
+            cp_async16(&As[k * Cfg::LDA + m], src, v);
+        }
+    }
+    // B tile -> Bs[k][n]
+    if (g.opB == OP_N) {
+        for (int e = tid; e < BN * BK; e += nthr) {
+            int k = e % BK, n = e / BK;
+            int gn = n0 + n, gk = k0 + k;
+            bool v = gn < g.N && gk < g.K;
+            const cplx* src = v ? g.B + MIDX(gk, gn, g.ldb) : g.B;
+            cp_async16(&Bs[k * Cfg::LDB + n], src, v);
+        }
+    } else {
+        for (int e = tid; e < BN * BK; e += nthr) {
+            int n = e % BN, k = e / BN;
+            int gn = n0 + n, gk = k0 + k;
+            bool v = gn < g.N && gk < g.K;
+            const cplx* src = v ? g.B + MIDX(gn, gk, g.ldb) : g.B;
+            cp_async16(&Bs[k * Cfg::LDB + n], src, v);
+        }
+    }
+}
+
+// Compute all tiles assigned to this CTA.  Must be called by all threads of
+// the CTA (threadIdx.x < Cfg::NT do the math; extra threads only help load).
+// smem must hold Cfg::SMEM_ELEMS double2.
+template <class Cfg>
+__device__ void zgemm_cta(const ZGemmArgs& g, int tile0, int tstep, cplx* smem) {
+    constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, FM = Cfg::FM, FN = Cfg::FN;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const bool mathw = warp < Cfg::WM * Cfg::WN;
+    const int wm0 = (warp % Cfg::WM) * Cfg::WTM, wn0 = (warp / Cfg::WM) * Cfg::WTN;
+    const int tm = (g.M + BM - 1) / BM, tn = (g.N + BN - 1) / BN;
+    const int ntiles = tm * tn;
+    const bool conjA = (g.opA == OP_C), conjB = (g.opB == OP_C);
+    const bool beta0 = (g.beta.x == 0.0 && g.beta.y == 0.0);
+    cplx* As0 = smem;
+    cplx* Bs0 = smem + Cfg::SA;
+    cplx* As1 = smem + Cfg::SA + Cfg::SB;
+    cplx* Bs1 = smem + 2 * Cfg::SA + Cfg::SB;
+
+    for (int t = tile0; t < ntiles; t += tstep) {
+        const int m0 = (t % tm) * BM, n0 = (t / tm) * BN;
+        double accr[FM][FN][2], acci[FM][FN][2];
+#pragma unroll
+        for (int a = 0; a < FM; ++a)
+#pragma unroll
+            for (int b = 0; b < FN; ++b) { accr[a][b][0] = accr[a][b][1] = acci[a][b][0] = acci[a][b][1] = 0.0; }
+
+        const int nk = (g.K + BK - 1) / BK;
+        if (nk > 0) {
+            zgemm_load_stage<Cfg>(g, m0, n0, 0, As0, Bs0, tid, nthr);
+            cp_async_commit();
+        }
+        for (int kt = 0; kt < nk; ++kt) {
+            cplx* As = (kt & 1) ? As1 : As0;
+            cplx* Bs = (kt & 1) ? Bs1 : Bs0;
+            if (kt + 1 < nk) {
+                zgemm_load_stage<Cfg>(g, m0, n0, (kt + 1) * BK, (kt & 1) ? As0 : As1, (kt & 1) ? Bs0 : Bs1, tid, nthr);
+                cp_async_commit();
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncthreads();
+            if (mathw) {
+#pragma unroll
+                for (int kk = 0; kk < BK; kk += 4) {
+                    const int kr = kk + (lane & 3);
+                    double ar[FM], ai[FM], ain[FM], br[FN], bi[FN];
+#pragma unroll
+                    for (int a = 0; a < FM; ++a) {
+                        cplx v = As[kr * Cfg::LDA + wm0 + a * 8 + (lane >> 2)];
+                        ar[a] = v.x; ai[a] = conjA ? -v.y : v.y; ain[a] = -ai[a];
+                    }
+#pragma unroll
+                    for (int b = 0; b < FN; ++b) {
+                        cplx v = Bs[kr * Cfg::LDB + wn0 + b * 8 + (lane >> 2)];
+                        br[b] = v.x; bi[b] = conjB ? -v.y : v.y;
+                    }
+#pragma unroll
+                    for (int a = 0; a < FM; ++a)
+#pragma unroll
+                        for (int b = 0; b < FN; ++b) {
+                            dmma(accr[a][b][0], accr[a][b][1], ar[a], br[b]);
+                            dmma(accr[a][b][0], accr[a][b][1], ain[a], bi[b]);
+                            dmma(acci[a][b][0], acci[a][b][1], ar[a], bi[b]);
+                            dmma(acci[a][b][0], acci[a][b][1], ai[a], br[b]);
+                        }
+                }
+            }
+            __syncthreads();
+        }
+        // epilogue through shared memory: Cs[n][m], ld = BM + 1
+        cplx* Cs = smem;
+        if (mathw) {
+#pragma unroll
+            for (int a = 0; a < FM; ++a)
+#pragma unroll
+                for (int b = 0; b < FN; ++b) {
+                    int m = wm0 + a * 8 + (lane >> 2);
+                    int n = wn0 + b * 8 + (lane & 3) * 2;
+                    Cs[n * Cfg::LDC + m] = cmk(accr[a][b][0], acci[a][b][0]);
+                    Cs[(n + 1) * Cfg::LDC + m] = cmk(accr[a][b][1], acci[a][b][1]);
+                }
+        }
+        __syncthreads();
+        for (int e = tid; e < BM * BN; e += nthr) {
+            int m = e % BM, n = e / BM;
+            int gm = m0 + m, gn = n0 + n;
+            if (gm < g.M && gn < g.N) {
+                cplx r = cmul(g.alpha, Cs[n * Cfg::LDC + m]);
+                cplx* cp = g.C + MIDX(gm, gn, g.ldc);
+                if (!beta0) r = cfma(g.beta, *cp, r);
+                *cp = r;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Default tile configurations (256 threads).
+typedef ZGemmCfg<64, 64, 16, 2, 4> GemmBig;     // square-ish products
+typedef ZGemmCfg<32, 64, 16, 2, 4> GemmMid;     // panels with M <= 32
+typedef ZGemmCfg<16, 128, 16, 1, 8> GemmWide;   // M = 16 rows (reflector blocks)

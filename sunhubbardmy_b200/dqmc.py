@@ -1,0 +1,353 @@
+"""ctypes host mirror of the reference's sweep driver over libdqmc_gpu.so.
+
+Names follow the reference: ``dqmc.in`` namelists (src/model_para.f90),
+``sweep_start`` (dqmc_ft_sweep_start_0b), ``sweep_b0`` / ``sweep_0b``
+(dqmc_ft_sweep_b0/0b), ``obser_init``, ``update``, ``h0_prop`` / ``u_prop``
+(the h0conf / uconf type-bound procedures).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+SQUARE, HONEYCOMB = 1, 2
+FAST, DELAY, SUBMATRIX = 0, 1, 2
+CHECKERBOARD, FFT = 0, 1
+EXACT, GENERAL4 = 0, 1
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def lib_path() -> str:
+    return os.path.join(_HERE, "_lib", "libdqmc_gpu.so")
+
+
+class DqmcError(RuntimeError):
+    pass
+
+
+class DqmcParams(C.Structure):
+    """Mirror of ``dqmc_params`` in include/dqmc_gpu.h."""
+    _fields_ = [
+        ("lattice", C.c_int32), ("l1", C.c_int32), ("l2", C.c_int32),
+        ("beta", C.c_double), ("dtau", C.c_double), ("rt", C.c_double), ("t2", C.c_double),
+        ("t3", C.c_double), ("nu", C.c_double), ("mu", C.c_double), ("rhub", C.c_double),
+        ("rv", C.c_double), ("alpha", C.c_double), ("theta", C.c_double),
+        ("xmag", C.c_double), ("flux_x", C.c_double), ("flux_y", C.c_double),
+        ("dimer", C.c_double), ("rndness", C.c_double),
+        ("nflr", C.c_int32), ("lproju", C.c_int32), ("lstabilize", C.c_int32),
+        ("nwrap", C.c_int32), ("nsweep", C.c_int32), ("nbin", C.c_int32), ("nublock", C.c_int32),
+        ("update", C.c_int32), ("kinetic", C.c_int32), ("hs", C.c_int32),
+        ("ndim", C.c_int32), ("lq", C.c_int32), ("ltrot", C.c_int32), ("nst", C.c_int32),
+        ("ne", C.c_int32), ("lcomp", C.c_int32),
+    ]
+
+    @classmethod
+    def make(cls, **kw) -> "DqmcParams":
+        """Defaults of src/model_para.f90:166-206, overridden by keywords."""
+        d = dict(lattice=SQUARE, l1=2, l2=2, beta=20.0, dtau=0.05, rt=1.0, t2=0.0, t3=0.0, nu=0.0,
+                 mu=0.0, rhub=0.0, rv=0.0, alpha=0.2, theta=0.0, xmag=0.0, flux_x=0.0, flux_y=0.0,
+                 dimer=0.0, rndness=0.0, nflr=2, lproju=0, lstabilize=1, nwrap=10, nsweep=20,
+                 nbin=10, nublock=0, update=DELAY, kinetic=CHECKERBOARD, hs=GENERAL4)
+        d.update(kw)
+        p = cls(**d)
+        rc = load_library().dqmc_params_derive(C.byref(p))
+        if rc != 0:
+            raise DqmcError(f"dqmc_params_derive: {_last_error()}")
+        return p
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class DqmcDiag(C.Structure):
+    _fields_ = [(n, C.c_double) for n in (
+        "phase_re", "phase_im", "logweight_re", "logweight_im", "max_wrap_error", "max_phasediff",
+        "avglog10error_sum", "logcount", "avgexpphasediff_sum", "accepted", "proposed", "nobs")]
+
+
+_lib = None
+
+# Every entry point declared in include/dqmc_gpu.h with (restype, argtypes).
+_vp, _i, _d = C.c_void_p, C.c_int, C.c_double
+SIGNATURES = {
+    "dqmc_params_derive": (_i, [_vp]),
+    "dqmc_gpu_create": (_i, [_vp, _i, _i, _vp, _i, C.POINTER(_vp)]),
+    "dqmc_gpu_destroy": (_i, [_vp]),
+    "dqmc_gpu_last_error": (C.c_char_p, []),
+    "dqmc_gpu_set_conf": (_i, [_vp, _i, _vp]),
+    "dqmc_gpu_get_conf": (_i, [_vp, _i, _vp]),
+    "dqmc_gpu_set_conf_all": (_i, [_vp, _vp]),
+    "dqmc_gpu_get_conf_all": (_i, [_vp, _vp]),
+    "dqmc_gpu_get_green": (_i, [_vp, _i, _vp]),
+    "dqmc_gpu_set_green": (_i, [_vp, _i, _vp]),
+    "dqmc_gpu_sweep_start": (_i, [_vp]),
+    "dqmc_gpu_sweep_b0": (_i, [_vp, _i, _i]),
+    "dqmc_gpu_sweep_0b": (_i, [_vp, _i, _i]),
+    "dqmc_gpu_sweeps": (_i, [_vp, _i, _i]),
+    "dqmc_gpu_obser_init": (_i, [_vp]),
+    "dqmc_gpu_nbins": (_i, [_vp, _i]),
+    "dqmc_gpu_get_bins": (_i, [_vp, _i, _vp]),
+    "dqmc_gpu_get_diag": (_i, [_vp, _i, _vp]),
+    "dqmc_gpu_reset_diag": (_i, [_vp]),
+    "dqmc_gpu_h0_prop": (_i, [_vp, _i, _i]),
+    "dqmc_gpu_u_prop": (_i, [_vp, _i, _i]),
+    "dqmc_gpu_update": (_i, [_vp, _i]),
+    "dqmc_gpu_measure": (_i, [_vp]),
+    "dqmc_gpu_set_phase": (_i, [_vp, _i, _d, _d]),
+    "dqmc_gpu_draw_u32": (_i, [_vp, _i, _i, _vp]),
+    "dqmc_gpu_set_work": (_i, [_vp, _i, _i, _vp]),
+    "dqmc_gpu_get_work": (_i, [_vp, _i, _i, _vp]),
+    "dqmc_gpu_test_zgemm": (_i, [_vp, _i, _i, _i, _i, _i, _i, _i, _i, _d]),
+    "dqmc_gpu_test_qr": (_i, [_vp, _i, _i, _vp]),
+    "dqmc_gpu_last_sweeps_ms": (_d, [_vp]),
+}
+
+
+def load_library() -> C.CDLL:
+    """Load the CUDA library; raises if it has not been built (no fallback)."""
+    global _lib
+    if _lib is None:
+        path = lib_path()
+        if not os.path.exists(path):
+            raise DqmcError(f"{path} is missing: build it with __graft_entry__.build() "
+                            "(make -C sunhubbardmy_b200/csrc); there is no CPU fallback")
+        L = C.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _last_error() -> str:
+    s = load_library().dqmc_gpu_last_error()
+    return s.decode() if s else ""
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != 0:
+        raise DqmcError(f"{what} failed ({rc}): {_last_error()}")
+
+
+def _ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+def test_seed(irank: int) -> int:
+    """abs((irank*1981+2008)*951049) in 32-bit integers (src/dqmc_util.f90:72)."""
+    v = ((irank * 1981 + 2008) * 951049) & 0xFFFFFFFF
+    if v >= 1 << 31:
+        v -= 1 << 32
+    return abs(v)
+
+
+# ----------------------------------------------------------------------------
+# dqmc.in namelist reader (src/model_para.f90:155-218)
+# ----------------------------------------------------------------------------
+_NL_RE = re.compile(r"&(\w+)(.*?)/", re.S)
+
+
+def _parse_value(v: str):
+    v = v.strip().rstrip(",").strip()
+    lv = v.lower()
+    if lv in (".true.", "t", ".t.", "true"):
+        return True
+    if lv in (".false.", "f", ".f.", "false"):
+        return False
+    lv = lv.replace("d", "e")
+    try:
+        if re.fullmatch(r"[+-]?\d+", lv):
+            return int(lv)
+        return float(lv)
+    except ValueError:
+        return v.strip("'\"")
+
+
+def read_dqmc_in(path_or_text: str) -> dict:
+    """Parse the &model_para and &ctrl_para namelists of a dqmc.in file."""
+    text = path_or_text
+    if os.path.exists(path_or_text):
+        with open(path_or_text) as f:
+            text = f.read()
+    text = re.sub(r"!.*", "", text)
+    out = {}
+    for grp, body in _NL_RE.findall(text):
+        for key, val in re.findall(r"(\w+)\s*=\s*([^=]+?)(?=,?\s*\w+\s*=|$)", body.strip(), re.S):
+            out[key.lower()] = _parse_value(val)
+    if "la" in out:
+        out["l1"] = out.pop("la")
+    if "lb" in out:
+        out["l2"] = out.pop("lb")
+    for k in ("lprojv", "lproju", "lprojplqu", "lstabilize", "ltau"):
+        if k in out:
+            out[k] = int(bool(out[k]))
+    keep = {f for f, _ in DqmcParams._fields_}
+    return {k: v for k, v in out.items() if k in keep}
+
+
+# ----------------------------------------------------------------------------
+# driver
+# ----------------------------------------------------------------------------
+class Dqmc:
+    """n_chains independent DQMC chains advanced together on the GPU."""
+
+    def __init__(self, params, n_chains: int = 1, seeds=None, draw_conf: bool = True):
+        if isinstance(params, DqmcParams):
+            params = [params]
+        self.params = list(params)
+        arr = (DqmcParams * len(self.params))(*self.params)
+        if seeds is None:
+            seeds = [test_seed(c) for c in range(n_chains)]
+        self.seeds = np.ascontiguousarray(seeds, np.int32)
+        assert len(self.seeds) == n_chains
+        self.n_chains = n_chains
+        h = C.c_void_p()
+        L = load_library()
+        _check(L.dqmc_gpu_create(C.cast(arr, C.c_void_p), len(self.params), n_chains, _ptr(self.seeds),
+                                 int(draw_conf), C.byref(h)), "dqmc_gpu_create")
+        self.h = h
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            load_library().dqmc_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def chain_params(self, c: int) -> DqmcParams:
+        return self.params[c % len(self.params)]
+
+    def ndim(self, c: int = 0) -> int:
+        return self.chain_params(c).ndim
+
+    @property
+    def ltrot(self) -> int:
+        return self.params[0].ltrot
+
+    # state
+    def conf(self, c: int = 0) -> np.ndarray:
+        out = np.zeros((self.ltrot, self.ndim(c)), np.int32)
+        _check(load_library().dqmc_gpu_get_conf(self.h, c, _ptr(out)), "get_conf")
+        return out
+
+    def set_conf(self, conf: np.ndarray, c: int = 0) -> None:
+        a = np.ascontiguousarray(conf, np.int32)
+        _check(load_library().dqmc_gpu_set_conf(self.h, c, _ptr(a)), "set_conf")
+
+    def conf_all(self, out: np.ndarray | None = None) -> np.ndarray:
+        n = sum(self.ltrot * self.ndim(c) for c in range(self.n_chains))
+        if out is None:
+            out = np.zeros(n, np.int32)
+        _check(load_library().dqmc_gpu_get_conf_all(self.h, _ptr(out)), "get_conf_all")
+        return out
+
+    def set_conf_all(self, conf: np.ndarray) -> None:
+        _check(load_library().dqmc_gpu_set_conf_all(self.h, _ptr(conf)), "set_conf_all")
+
+    def green(self, c: int = 0) -> np.ndarray:
+        N = self.ndim(c)
+        g = np.zeros((N, N), complex, order="F")
+        _check(load_library().dqmc_gpu_get_green(self.h, c, _ptr(g)), "get_green")
+        return g
+
+    def set_green(self, g: np.ndarray, c: int = 0) -> None:
+        a = np.asfortranarray(g, complex)
+        _check(load_library().dqmc_gpu_set_green(self.h, c, _ptr(a)), "set_green")
+
+    def set_phase(self, z: complex, c: int = 0) -> None:
+        _check(load_library().dqmc_gpu_set_phase(self.h, c, z.real, z.imag), "set_phase")
+
+    def diag(self, c: int = 0) -> dict:
+        d = DqmcDiag()
+        _check(load_library().dqmc_gpu_get_diag(self.h, c, C.byref(d)), "get_diag")
+        return dict(phase=complex(d.phase_re, d.phase_im), logweight=complex(d.logweight_re, d.logweight_im),
+                    max_wrap_error=d.max_wrap_error, max_phasediff=d.max_phasediff,
+                    avglog10error=d.avglog10error_sum, logcount=d.logcount,
+                    avgexpphasediff=d.avgexpphasediff_sum, accepted=d.accepted, proposed=d.proposed,
+                    nobs=d.nobs)
+
+    def reset_diag(self) -> None:
+        _check(load_library().dqmc_gpu_reset_diag(self.h), "reset_diag")
+
+    # sweep
+    def sweep_start(self) -> None:
+        _check(load_library().dqmc_gpu_sweep_start(self.h), "sweep_start")
+
+    def sweep_b0(self, lupdate: bool = True, lmeasure: bool = True) -> None:
+        _check(load_library().dqmc_gpu_sweep_b0(self.h, int(lupdate), int(lmeasure)), "sweep_b0")
+
+    def sweep_0b(self, lupdate: bool = True, lmeasure: bool = True) -> None:
+        _check(load_library().dqmc_gpu_sweep_0b(self.h, int(lupdate), int(lmeasure)), "sweep_0b")
+
+    def sweeps(self, n: int, lmeasure: bool = True) -> float:
+        """n x (b0 + 0b) through a captured CUDA graph; returns device ms per sweep."""
+        L = load_library()
+        _check(L.dqmc_gpu_sweeps(self.h, int(n), int(lmeasure)), "sweeps")
+        return L.dqmc_gpu_last_sweeps_ms(self.h)
+
+    def obser_init(self) -> None:
+        _check(load_library().dqmc_gpu_obser_init(self.h), "obser_init")
+
+    def bins_raw(self, c: int = 0) -> np.ndarray:
+        L = load_library()
+        n = L.dqmc_gpu_nbins(self.h, c)
+        out = np.zeros(n, complex)
+        _check(L.dqmc_gpu_get_bins(self.h, c, _ptr(out)), "get_bins")
+        return out
+
+    def bins(self, c: int = 0) -> dict:
+        from .io import unpack_bins
+        d = self.diag(c)
+        return unpack_bins(self.bins_raw(c), self.chain_params(c).lq, int(round(d["nobs"])))
+
+    # operator-level procedures
+    def h0_prop(self, op: int, nf: int = 1) -> None:
+        _check(load_library().dqmc_gpu_h0_prop(self.h, op, nf), "h0_prop")
+
+    def u_prop(self, op: int, nt: int) -> None:
+        _check(load_library().dqmc_gpu_u_prop(self.h, op, nt), "u_prop")
+
+    def update(self, nt: int) -> None:
+        _check(load_library().dqmc_gpu_update(self.h, nt), "update")
+
+    def measure(self) -> None:
+        _check(load_library().dqmc_gpu_measure(self.h), "measure")
+
+    def draw_u32(self, count: int, c: int = 0) -> np.ndarray:
+        out = np.zeros(count, np.uint32)
+        _check(load_library().dqmc_gpu_draw_u32(self.h, c, count, _ptr(out)), "draw_u32")
+        return out
+
+    # diagnostics on the tensor-core kernels
+    def set_work(self, which: int, m: np.ndarray, c: int = 0) -> None:
+        a = np.asfortranarray(m, complex)
+        _check(load_library().dqmc_gpu_set_work(self.h, c, which, _ptr(a)), "set_work")
+
+    def work(self, which: int, c: int = 0) -> np.ndarray:
+        N = self.ndim(c)
+        g = np.zeros((N, N), complex, order="F")
+        _check(load_library().dqmc_gpu_get_work(self.h, c, which, _ptr(g)), "get_work")
+        return g
+
+    def test_zgemm(self, m, n, k, opa, opb, a, b, c, beta=0.0) -> None:
+        _check(load_library().dqmc_gpu_test_zgemm(self.h, m, n, k, opa, opb, a, b, c, float(beta)), "test_zgemm")
+
+    def test_qr(self, a: int, q: int) -> np.ndarray:
+        ld = np.zeros(2 * self.n_chains)
+        _check(load_library().dqmc_gpu_test_qr(self.h, a, q, _ptr(ld)), "test_qr")
+        return ld.view(complex)

@@ -1,0 +1,100 @@
+"""On-disk formats of the reference, written from the GPU sweep's results.
+
+* ``conf_u.in`` / ``conf_u.out`` (src/dqmc_config_u/dqmc_input_conf.f90:36-102,
+  dqmc_output_conf.f90:27-42): a first line with a nonzero integer, then
+  ``ltrot*nsites`` integers, one per line, site fastest, chain (rank) after
+  chain.
+* ``energy.bin`` and the ``*.bin`` files of equaltime_output
+  (src/dqmc_measure/equaltime_output.f90:67-180): per bin, the bin sums
+  reduced over chains and divided by ``n_chains * nobs``.
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+
+
+def unpack_bins(z: np.ndarray, lq: int, nobs: int = 0) -> dict:
+    """Split the flat bin array of dqmc_gpu_get_bins (see include/dqmc_gpu.h)."""
+    k = 0
+    out = {"energy": z[k:k + 10].copy()}
+    k += 10
+    for name in ("cpcm", "spsm", "nn", "pair_onsite"):
+        out[name] = z[k:k + 4 * lq].reshape(2, 2, lq).copy()   # [no_j][no_i][d]
+        k += 4 * lq
+    for name in ("jj", "bb", "pair_nn", "pair_sn"):
+        out[name] = z[k:k + lq].copy()
+        k += lq
+    out["zn"] = z[k:k + 2].copy()
+    out["zj"] = z[k + 2]
+    out["zb"] = z[k + 3]
+    out["nobs"] = nobs
+    return out
+
+
+def write_conf(path: str, confs) -> None:
+    """conf_u.out: '1' then every chain's field, site fastest ((i4) per line)."""
+    with open(path, "w") as f:
+        f.write("           1\n")
+        for conf in confs:
+            for v in np.asarray(conf, np.int32).ravel():
+                f.write(f"{int(v):4d}\n")
+
+
+def read_conf(path: str, ltrot: int, nsites: int, n_chains: int = 1):
+    """conf_u.in reader; returns None for a fresh start (first integer 0).
+    Missing chains copy chain 0, as dqmc_input_conf does (lines 86-100)."""
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        vals = [int(x) for x in f.read().split()]
+    if not vals or vals[0] == 0:
+        return None
+    body = np.asarray(vals[1:], np.int32)
+    per = ltrot * nsites
+    out = []
+    for c in range(n_chains):
+        if (c + 1) * per <= body.size:
+            out.append(body[c * per:(c + 1) * per].reshape(ltrot, nsites).copy())
+        else:
+            out.append(out[0].copy())
+    return out
+
+
+def _fourier(gr: np.ndarray, zexpiqr: np.ndarray) -> np.ndarray:
+    """k-space transform of a distance-binned array (fourier_trans_eqt)."""
+    return zexpiqr @ gr
+
+
+def equaltime_output(bins_per_chain, outdir: str = ".", zexpiqr: np.ndarray | None = None) -> dict:
+    """Reduce chain bins, normalise by n_chains*nobs and append to the
+    reference's files (energy.bin '(16e16.8)', n.bin, j.bin, b.bin, *_r.bin)."""
+    n = len(bins_per_chain)
+    nobs = bins_per_chain[0]["nobs"]
+    rnorm = float(n * nobs)
+    red = {}
+    for key in bins_per_chain[0]:
+        if key == "nobs":
+            continue
+        red[key] = sum(b[key] for b in bins_per_chain) / rnorm
+    os.makedirs(outdir, exist_ok=True)
+    with open(os.path.join(outdir, "energy.bin"), "a") as f:
+        e = red["energy"][:8]
+        f.write("".join(f"{v:16.8e}" for z in e for v in (z.real, z.imag)) + "\n")
+    with open(os.path.join(outdir, "n.bin"), "a") as f:
+        f.write("".join(f"{v:16.8e}" for z in red["zn"] for v in (z.real, z.imag)) + "\n")
+    for name, key in (("j.bin", "zj"), ("b.bin", "zb")):
+        with open(os.path.join(outdir, name), "a") as f:
+            z = red[key]
+            f.write(f"{z.real:16.8e}{z.imag:16.8e}\n")
+    for key in ("cpcm", "spsm", "nn", "pair_onsite", "jj", "bb", "pair_nn", "pair_sn"):
+        with open(os.path.join(outdir, f"{key}_r.bin"), "a") as f:
+            arr = np.asarray(red[key]).reshape(-1)
+            f.write("".join(f"{v:16.8e}" for z in arr for v in (z.real, z.imag)) + "\n")
+        if zexpiqr is not None:
+            with open(os.path.join(outdir, f"{key}_k.bin"), "a") as f:
+                arr = np.asarray(red[key])
+                kk = _fourier(arr.reshape(-1, arr.shape[-1]).T, zexpiqr).T.reshape(-1)
+                f.write("".join(f"{v:16.8e}" for z in kk for v in (z.real, z.imag)) + "\n")
+    return red

@@ -1,0 +1,34 @@
+"""Shared parameter sets and helpers for the parity tests.
+
+The cases are small versions of the benchmark configurations (square Hubbard
+with checkerboard or FFT kinetic term, exact or general HS field; honeycomb
+SU(4)) sized so the oracle finishes each in well under a second.
+"""
+import numpy as np
+
+# keyword sets accepted by both sunhubbardmy_b200.DqmcParams.make and
+# oracle.pyoracle.Model (same names as dqmc.in)
+CASES = {
+    "sq4_cb_exact_fast": dict(lattice=1, l1=4, l2=4, beta=2.0, dtau=0.1, rhub=4.0, nflr=2,
+                              kinetic=0, update=0, hs=0, nwrap=10),
+    "sq4_fft_gen4_delay": dict(lattice=1, l1=4, l2=4, beta=2.0, dtau=0.05, rhub=4.0, nflr=2,
+                               kinetic=1, update=1, hs=1, nwrap=10, nublock=4),
+    "hc3_cb_su4_sub": dict(lattice=2, l1=3, l2=3, beta=2.0, dtau=0.1, rhub=6.0, nflr=4,
+                           kinetic=0, update=2, hs=0, nwrap=10, nublock=8),
+    "sq6_cb_gen4_delay_mu": dict(lattice=1, l1=6, l2=6, beta=1.5, dtau=0.1, rhub=3.0, nflr=2, mu=0.3,
+                                 kinetic=0, update=1, hs=1, nwrap=5, nublock=8),
+}
+
+TEST_SEED0 = 1909706392   # abs((0*1981+2008)*951049)
+
+
+def rand_green(n: int, seed: int = 0) -> np.ndarray:
+    """A well-conditioned complex matrix shaped like an equal-time G."""
+    rng = np.random.default_rng(seed)
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    return np.asfortranarray(0.5 * np.eye(n) + 0.05 * a)
+
+
+def rel_err(a, b) -> float:
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.max(np.abs(a - b)) / max(1e-300, np.max(np.abs(b))))
