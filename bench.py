@@ -1,0 +1,317 @@
+"""Benchmark: HS site-slice updates/s of the finite-temperature DQMC sweep.
+
+Workload (the single-chain GPU drop-in configuration): SU(2) Hubbard on the
+16 x 16 square lattice (N = 256 sites), U/t = 4, mu = 0, beta = 10,
+dtau = 0.05 (ltrot = 200), FFT kinetic propagator, delayed update with
+nublock = 32, general 4-component HS field, nwrap = 10 (nst = 20).  A step is
+one full sweep (b0 + 0b: 2 * ltrot * N = 102,400 proposals per chain) with
+equal-time measurement of every slice, stabilisation and wrap checks.  Each GPU
+advances --chains independent chains (the reference's one-chain-per-MPI-rank
+parallelism, batched: one CTA per chain); the HS fields are drawn from the
+reference's -DTEST seeds, one per chain.  The working set (about 52 MiB per
+chain) is far larger than L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--chains C] [--impl reference]
+
+--impl reference times the reference algorithm on the host CPU cores (the C
+restatement in oracle/, with BLAS/LAPACK from scipy's OpenBLAS, one chain per
+core) on the same configuration; each step is a bounded sample of 20 slices of
+a b0 sweep per core.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIG = dict(lattice=1, l1=16, l2=16, beta=10.0, dtau=0.05, rhub=4.0, nflr=2, mu=0.0,
+              kinetic=1, update=1, hs=1, nwrap=10, nublock=32)
+WORKLOAD = "square L=16 (N=256) SU(2) Hubbard U=4 beta=10 dtau=0.05 (ltrot=200) FFT kinetic, delay nublock=32, general 4-comp HS, nwrap=10"
+METRIC = "HS site-slice updates/s"
+
+
+def test_seed(irank: int) -> int:
+    v = ((irank * 1981 + 2008) * 951049) & 0xFFFFFFFF
+    if v >= 1 << 31:
+        v -= 1 << 32
+    return abs(v)
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[3 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------------ CPU arm
+def cpu_sample(nslices: int, threads: int, steps: int = 1, warmup: int = 0):
+    """Time the oracle (reference restatement, OpenBLAS) on `threads` cores:
+    each core runs its own chain of the benchmark configuration for `nslices`
+    slices of a b0 sweep (updates, measurement, stabilisation) per step."""
+    from threadpoolctl import threadpool_limits
+
+    from oracle import pyoracle
+    pyoracle.build()
+    pyoracle.use_scipy_lapack(True)
+    model = pyoracle.Model(**CONFIG)
+    chains = [pyoracle.Chain(model, test_seed(c)) for c in range(threads)]
+
+    def run(fn):
+        ts = [threading.Thread(target=fn, args=(c,)) for c in chains]
+        t0 = time.perf_counter()
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        return time.perf_counter() - t0
+
+    with threadpool_limits(1):
+        run(lambda c: c.sweep_start())
+        for _ in range(warmup):
+            run(lambda c: c.sweep_b0_slices(nslices))
+        times = [run(lambda c: c.sweep_b0_slices(nslices)) for _ in range(steps)]
+    per_step = threads * nslices * model.ndim
+    return per_step, times, model
+
+
+def reference_arm(args, rank: int) -> None:
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    nsl = 20
+    per_step, times, model = cpu_sample(nsl, threads, steps=args.steps, warmup=args.warmup)
+    tot = sum(times)
+    value = per_step * len(times) / tot
+    sample = f"{nsl} slices of a b0 sweep per chain per step, {threads} chains on {threads} cores (one per core)"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic (HS field drawn from the reference's -DTEST seeds)",
+        "config": {"workload": WORKLOAD, "chains": threads, "threads": threads,
+                   "implementation": "C restatement of the Fortran reference (oracle/), OpenBLAS single-threaded per chain"},
+        "cpu_baseline": {"value": value, "unit": "updates/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU arm
+def fp64_peak_tflops() -> float:
+    """Measured FP64 tensor throughput: cuBLAS DGEMM 8192^3 via torch (best of 5)."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(); torch.matmul(a, b); e1.record(); e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
+    import numpy as np
+    import torch
+    import sunhubbardmy_b200 as sb
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    C = args.chains
+    p = sb.DqmcParams.make(**CONFIG)
+    N, lt = p.ndim, p.ltrot
+    g = sb.Dqmc(p, n_chains=C, seeds=[test_seed(rank * C + c) for c in range(C)])
+    g.sweep_start()
+    g.obser_init()
+    g.sweeps(max(args.warmup, 1), True)
+    g.reset_diag()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    barrier()
+    with ClockSampler(local_rank) as clk:
+        ms = g.sweeps(args.steps, True)          # CUDA events on the library stream
+    barrier()
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    per_step = world * C * 2 * lt * N
+    value = per_step / (ms * 1e-3)
+    kernels_per_sweep = g.sweep_kernels()
+    d0 = g.diag(0)
+    wrap = max(g.diag(c)["max_wrap_error"] for c in range(C))
+    acc = d0["accepted"] / max(1.0, d0["proposed"])
+
+    # end to end through the public API with host buffers: h2d of every chain's
+    # HS field, sweep_start + one sweep, d2h of every chain's bins and field
+    nconf = C * lt * N
+    conf_host = torch.empty(nconf, dtype=torch.int32, pin_memory=True).numpy()
+    g.conf_all(conf_host)
+    nbins = len(g.bins_raw(0))
+    e2e_steps = max(1, min(args.steps, 2))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        g.set_conf_all(conf_host)
+        g.sweep_start()
+        g.sweeps(1, True)
+        bins = [g.bins_raw(c) for c in range(C)]
+        g.conf_all(conf_host)
+    barrier()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_s = float(t.item())
+    del bins
+
+    result = None
+    if rank == 0:
+        # roofline of the dominant kernel: per-kernel device times (CUDA events)
+        names = {0: "k_update_delay", 1: "k_stab", 2: "k_green", 3: "k_prop_cols", 4: "k_measure", 5: "k_prop_rows"}
+        ops = {k: g.time_op(k, 3) for k in (1, 2, 3, 5, 4, 0)}
+        nst = p.nst
+        per_sweep = {1: 2 * nst, 2: 2 * nst, 3: 4 * lt + 2 * nst, 5: 4 * lt, 4: 2 * lt, 0: 2 * lt}
+        share = {k: ops[k] * per_sweep[k] for k in ops}
+        total = sum(share.values())
+        dom = max(share, key=share.get)
+        N3 = float(N) ** 3
+        flops = {1: 18.0 + 2.0 / 3.0, 2: 41.0 + 1.0 / 3.0}   # real flops / N^3 per chain
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+        fp64 = fp64_peak_tflops()
+        if dom in flops:
+            ach = C * flops[dom] * N3 / (ops[dom] * 1e-3) / 1e12
+            roof = {"kernel": names[dom], "bound": "tensor", "achieved": ach, "peak": fp64, "unit": "TFLOP/s",
+                    "frac": ach / fp64, "traffic": None,
+                    "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (FP64 tensor)"}
+        elif dom in (3, 5):
+            ach = C * 32.0 * N * N / (ops[dom] * 1e-3) / 1e9
+            pk = peaks.get("hbm_gbs", 6650.0)
+            roof = {"kernel": names[dom], "bound": "hbm", "achieved": ach, "peak": pk, "unit": "GB/s",
+                    "frac": ach / pk, "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
+        else:
+            acc_n = acc * N
+            ach = C * 8.0 * N * N * acc_n / (ops[dom] * 1e-3) / 1e12
+            roof = {"kernel": names[dom], "bound": "tensor", "achieved": ach, "peak": fp64, "unit": "TFLOP/s",
+                    "frac": ach / fp64, "traffic": None,
+                    "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (FP64 tensor)"}
+        roof["kernel_ms_per_launch"] = {names[k]: ops[k] for k in ops}
+        roof["sweep_share"] = {names[k]: share[k] / total for k in ops}
+        trf = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(trf):
+            tr = json.load(open(trf)).get(roof["kernel"])
+            if tr:
+                roof["traffic"] = tr["bytes_per_chain"] * C
+                roof["traffic_note"] = tr.get("note", "")
+        result = {
+            "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic (HS field drawn from the reference's -DTEST seeds, one per chain)",
+            "config": {"workload": WORKLOAD, "chains_per_gpu": C, "parallelism": f"replicas x{world}",
+                       "l2": "working set ~52 MiB/chain >> L2 (no flush needed)",
+                       "acceptance": acc, "max_wrap_error": wrap},
+            "e2e": {"value": per_step / e2e_s, "unit": "updates/s",
+                    "h2d_bytes_per_step": nconf * 4,
+                    "d2h_bytes_per_step": C * nbins * 16 + nconf * 4,
+                    "note": "per step: set_conf_all (pinned host) + sweep_start + 1 sweep + get_bins + get_conf_all"},
+            "gpu_launches": kernels_per_sweep * args.steps,
+            "roofline": roof,
+            "clocks": clk.summary(),
+        }
+        if world == 1 and not args.no_cpu:
+            per, times, _ = cpu_sample(20, os.cpu_count() or 1, steps=1)
+            cv = per / times[0]
+            result["cpu_baseline"] = {"value": cv, "unit": "updates/s", "cores": os.cpu_count() or 1, "kind": "port",
+                                      "sample": f"20 slices of a b0 sweep per chain, one chain per core ({os.cpu_count()} cores), OpenBLAS"}
+    g.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if result is not None:
+        print(json.dumps(result), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--chains", type=int, default=148)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+    gpu_arm(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -154,6 +154,14 @@ int dqmc_gpu_test_qr(dqmc_handle* h, int a, int q, double* logdetq /* 2 per chai
 /* Stream-ordered timing helper: average device time (ms) of the last
  * dqmc_gpu_sweeps call, measured with CUDA events on the library's stream. */
 double dqmc_gpu_last_sweeps_ms(dqmc_handle* h);
+/* Number of kernel launches in one captured sweep (b0 + 0b) of dqmc_gpu_sweeps. */
+int dqmc_gpu_sweep_kernels(dqmc_handle* h);
+/* Average device time (ms) of `reps` back-to-back launches of one sweep kernel
+ * over all chains, timed with CUDA events on the library's stream.  op: 0
+ * update of slice 1, 1 UDV stabilisation step, 2 equal-time Green's function,
+ * 3 kinetic + HS column pass, 4 equal-time measurement, 5 row pass.  Modifies
+ * chain state; intended for benchmarks after the timed sweeps. */
+int dqmc_gpu_time_op(dqmc_handle* h, int op, int reps, double* ms_out);
 
 #ifdef __cplusplus
 }

@@ -102,6 +102,7 @@ double orc_chain_uniform(orc_chain *c);
 /* drivers (src/dqmc_ft_core/ directory) */
 int  orc_sweep_start_0b(orc_chain *c);
 int  orc_sweep_b0(orc_chain *c, int lupdate, int lmeasure);
+int  orc_sweep_b0_slices(orc_chain *c, int lupdate, int lmeasure, int nslices);
 int  orc_sweep_0b(orc_chain *c, int lupdate, int lmeasure);
 void orc_obser_init(orc_chain *c);
 

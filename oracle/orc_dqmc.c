@@ -94,24 +94,48 @@ static void exp2x2(double d, zc z, double s, zc out[4]) {
     out[3] = e * ch;          /* (2,2) */
 }
 
-/* forward 2D DFT (scale 1/sqrt(lq)) of a length-lq vector, index j1 + l1*j2 */
+/* In-place 1D DFT of n points with stride st: radix-2 for powers of two,
+ * direct sum otherwise; tw[k] = exp(-2 pi i k / n), sign -1 forward. */
+static void dft1(zc *x, int n, int st, const zc *tw, int sign, zc *tmp) {
+    if ((n & (n - 1)) == 0) {
+        for (int i = 1, j = 0; i < n; ++i) {
+            int bit = n >> 1;
+            for (; j & bit; bit >>= 1) j ^= bit;
+            j ^= bit;
+            if (i < j) { zc t = x[i * st]; x[i * st] = x[j * st]; x[j * st] = t; }
+        }
+        for (int len = 2; len <= n; len <<= 1) {
+            int half = len >> 1, step = n / len;
+            for (int s0 = 0; s0 < n; s0 += len)
+                for (int k = 0; k < half; ++k) {
+                    zc w = tw[k * step];
+                    if (sign > 0) w = conj(w);
+                    zc u = x[(s0 + k) * st], v = w * x[(s0 + k + half) * st];
+                    x[(s0 + k) * st] = u + v;
+                    x[(s0 + k + half) * st] = u - v;
+                }
+        }
+    } else {
+        for (int k = 0; k < n; ++k) {
+            zc acc = 0;
+            for (int j = 0; j < n; ++j) {
+                zc w = tw[(j * k) % n];
+                acc += (sign > 0 ? conj(w) : w) * x[j * st];
+            }
+            tmp[k] = acc;
+        }
+        for (int k = 0; k < n; ++k) x[k * st] = tmp[k];
+    }
+}
+
+/* 2D DFT over (l1, l2) of a length-lq vector, index j1 + l1*j2, scale 1/sqrt(lq) */
 static void dft2(const orc_model *m, zc *x, int sign) {
     int l1 = m->p.l1, l2 = m->p.l2, lq = l1 * l2;
-    zc *t = zalloc(lq);
-    for (int k2 = 0; k2 < l2; ++k2)
-        for (int j1 = 0; j1 < l1; ++j1) {
-            zc s = 0;
-            for (int j2 = 0; j2 < l2; ++j2) s += x[j1 + l1 * j2] * cexp(sign * I * 2.0 * M_PI * j2 * k2 / l2);
-            t[j1 + l1 * k2] = s;
-        }
+    zc tmp[512];
+    for (int j2 = 0; j2 < l2; ++j2) dft1(x + l1 * j2, l1, 1, m->tw1, sign, tmp);
+    for (int j1 = 0; j1 < l1; ++j1) dft1(x + j1, l2, l1, m->tw2, sign, tmp);
     double sc = 1.0 / sqrt((double)lq);
-    for (int k2 = 0; k2 < l2; ++k2)
-        for (int k1 = 0; k1 < l1; ++k1) {
-            zc s = 0;
-            for (int j1 = 0; j1 < l1; ++j1) s += t[j1 + l1 * k2] * cexp(sign * I * 2.0 * M_PI * j1 * k1 / l1);
-            x[k1 + l1 * k2] = s * sc;
-        }
-    free(t);
+    for (int k = 0; k < lq; ++k) x[k] *= sc;
 }
 
 /* dqmc_set_h0conf.f90 + seth0.f90 */
@@ -150,6 +174,10 @@ static void set_h0(orc_model *m) {
     } else {
         /* h0k = diag(F H F^-1) with F the scaled forward DFT over (l1, l2) */
         int lq = m->lq;
+        m->tw1 = zalloc(p->l1);
+        m->tw2 = zalloc(p->l2);
+        for (int k = 0; k < p->l1; ++k) m->tw1[k] = cexp(-I * 2.0 * M_PI * k / p->l1);
+        for (int k = 0; k < p->l2; ++k) m->tw2[k] = cexp(-I * 2.0 * M_PI * k / p->l2);
         m->exph0k = zalloc(lq);
         m->exph0kinv = zalloc(lq);
         zc *tmp = zalloc((size_t)lq * lq);
@@ -228,7 +256,7 @@ void orc_model_free(orc_model *m) {
     if (!m) return;
     orc_latt_free(&m->L);
     free(m->iwrap_nt); free(m->wrap_step); free(m->urt); free(m->urtm1);
-    free(m->exph0k); free(m->exph0kinv); free(m->h0mat); free(m->expar_nn);
+    free(m->exph0k); free(m->exph0kinv); free(m->tw1); free(m->tw2); free(m->h0mat); free(m->expar_nn);
     free(m);
 }
 
@@ -1113,8 +1141,11 @@ static void record_wrap(orc_chain *c, const zc *gtmp, zc logw) {
     c->phase = ph;
 }
 
-/* dqmc_ft_sweep_b0 (src/dqmc_ft_core/dqmc_ft_sweep_b0.f90:1-216) */
-int orc_sweep_b0(orc_chain *c, int lupdate, int lmeasure) {
+/* dqmc_ft_sweep_b0 (src/dqmc_ft_core/dqmc_ft_sweep_b0.f90:1-216); nslices
+ * limits the sweep to its first nslices time slices (bounded CPU samples). */
+int orc_sweep_b0_slices(orc_chain *c, int lupdate, int lmeasure, int nslices);
+int orc_sweep_b0(orc_chain *c, int lupdate, int lmeasure) { return orc_sweep_b0_slices(c, lupdate, lmeasure, c->m->ltrot); }
+int orc_sweep_b0_slices(orc_chain *c, int lupdate, int lmeasure, int nslices) {
     const orc_model *m = c->m;
     int N = m->ndim, nst = m->nst;
     zc *gtmp = zalloc((size_t)N * N), *ur = zalloc((size_t)N * N), *vr = zalloc((size_t)N * N);
@@ -1125,7 +1156,7 @@ int orc_sweep_b0(orc_chain *c, int lupdate, int lmeasure) {
         for (int i = 0; i < N; ++i) { c->Ust[nst][ZIDX(i, i, N)] = 1; c->Vst[nst][ZIDX(i, i, N)] = 1; c->Dst[nst][i] = 1; }
         c->logdetQst[nst] = 0;
     }
-    for (int nt = m->ltrot; nt >= 1; --nt) {
+    for (int nt = m->ltrot; nt >= 1 && nt > m->ltrot - nslices; --nt) {
         if (lmeasure) orc_measure(c, nt);
         h0_half(c, ORC_LEFT_BACKWARD, ORC_RIGHT_FORWARD, 0);
         if (m->lwrapu) {

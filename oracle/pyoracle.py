@@ -74,6 +74,7 @@ def lib() -> C.CDLL:
             getattr(L, name).argtypes = [vp]
         L.orc_sweep_b0.argtypes = [vp, C.c_int, C.c_int]
         L.orc_sweep_0b.argtypes = [vp, C.c_int, C.c_int]
+        L.orc_sweep_b0_slices.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         L.orc_bins_size.argtypes = [vp]
         L.orc_bins_size.restype = C.c_int
         L.orc_update.argtypes = [vp, C.c_int, vp]
@@ -256,6 +257,9 @@ class Chain:
 
     def sweep_b0(self, lupdate=True, lmeasure=True) -> None:
         lib().orc_sweep_b0(self._p, int(lupdate), int(lmeasure))
+
+    def sweep_b0_slices(self, nslices: int, lupdate=True, lmeasure=True) -> None:
+        lib().orc_sweep_b0_slices(self._p, int(lupdate), int(lmeasure), int(nslices))
 
     def sweep_0b(self, lupdate=True, lmeasure=True) -> None:
         lib().orc_sweep_0b(self._p, int(lupdate), int(lmeasure))

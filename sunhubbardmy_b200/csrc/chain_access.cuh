@@ -15,11 +15,47 @@ DQ_DEV double2* chain_mat(const ChainDev& c, int id) {
     return c.W[id - MAT_W0];
 }
 
+// Radix-2 DFT of a length-n line held in registers (n a power of two, fully
+// unrolled).  tw[k] = exp(-2 pi i k / n); sign -1 forward, +1 backward.
+template <int n>
+DQ_DEV void line_fft_reg(double2* x, int st, const double2* __restrict__ tw, int sign) {
+    double2 r[n];
+#pragma unroll
+    for (int i = 0; i < n; ++i) {
+        int j = 0;
+#pragma unroll
+        for (int b = 1, t = i; b < n; b <<= 1, t >>= 1) j = (j << 1) | (t & 1);
+        r[j] = x[i * st];
+    }
+#pragma unroll
+    for (int len = 2; len <= n; len <<= 1) {
+        const int half = len >> 1, step = n / len;
+#pragma unroll
+        for (int s0 = 0; s0 < n; s0 += len)
+#pragma unroll
+            for (int k = 0; k < half; ++k) {
+                double2 w = __ldg(&tw[k * step]);
+                if (sign > 0) w.y = -w.y;
+                double2 u = r[s0 + k], v = cmul(w, r[s0 + k + half]);
+                r[s0 + k] = cadd(u, v);
+                r[s0 + k + half] = csub(u, v);
+            }
+    }
+#pragma unroll
+    for (int i = 0; i < n; ++i) x[i * st] = r[i];
+}
+
 // In-place DFT of a length-n line (element stride `st`) in shared memory.
 // sign = -1: forward exp(-2 pi i j k / n); sign = +1: backward.  tw[k] =
 // exp(-2 pi i k / n).  Unnormalised.  Power-of-two lengths use an iterative
 // radix-2 transform; other lengths a direct O(n^2) sum (n <= 64).
 DQ_DEV void line_dft(double2* x, int n, int st, const double2* tw, int sign) {
+    switch (n) {
+    case 4: line_fft_reg<4>(x, st, tw, sign); return;
+    case 8: line_fft_reg<8>(x, st, tw, sign); return;
+    case 16: line_fft_reg<16>(x, st, tw, sign); return;
+    default: break;
+    }
     if ((n & (n - 1)) == 0) {
         // bit reversal
         for (int i = 1, j = 0; i < n; ++i) {

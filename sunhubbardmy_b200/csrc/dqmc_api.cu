@@ -502,6 +502,7 @@ struct dqmc_handle {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0.0;
     int ctas_per_chain = 1;
+    size_t graph_nodes = 0;
 };
 
 static void* dalloc(dqmc_handle* h, size_t bytes) {
@@ -728,7 +729,7 @@ static void enqueue_b0(dqmc_handle* h, int lupdate, int lmeasure) {
     if (lupdate && m.p.rhub != 0.0) launch_sfmt(h->d_chains, h->nch, lt, h->st);
     for (int nt = lt; nt >= 1; --nt) {
         int visit = lt - nt;
-        if (lmeasure) launch_measure(h->d_chains, h->nch, h->st);
+        if (lmeasure) launch_measure(h->d_chains, h->nch, h->ctas_per_chain, h->st);
         PropProg pl; pl.n = 0; PropProg pr; pr.n = 0;
         prog_k(m, pl, PW_INV, 0);          // left_backward, nf = 1..nnf
         prog_k(m, pr, PW_FWD, 0);          // right_forward, nf = 1..nnf
@@ -766,7 +767,7 @@ static void enqueue_0b(dqmc_handle* h, int lupdate, int lmeasure) {
         prog_k(m, pr, PW_INV, 1);
         launch_prog(h, MAT_G, pl, 0);
         launch_prog(h, MAT_G, pr, 1);
-        if (lmeasure) launch_measure(h->d_chains, h->nch, h->st);
+        if (lmeasure) launch_measure(h->d_chains, h->nch, h->ctas_per_chain, h->st);
         if (m.iwrap_nt[nt] > 0) stab_0b(h, m.iwrap_nt[nt], 1);
     }
 }
@@ -801,6 +802,9 @@ extern "C" int dqmc_gpu_sweeps(dqmc_handle* h, int n, int lmeasure) {
         enqueue_0b(h, 1, lmeasure);
         CK(cudaStreamEndCapture(h->st, &g));
         CK(cudaGraphInstantiate(&h->sweep_graph, g, 0));
+        size_t nn = 0;
+        cudaGraphGetNodes(g, nullptr, &nn);
+        h->graph_nodes = nn;
         cudaGraphDestroy(g);
         h->graph_meas = lmeasure;
     }
@@ -816,6 +820,8 @@ extern "C" int dqmc_gpu_sweeps(dqmc_handle* h, int n, int lmeasure) {
 }
 
 extern "C" double dqmc_gpu_last_sweeps_ms(dqmc_handle* h) { return h ? h->last_ms : 0.0; }
+
+extern "C" int dqmc_gpu_sweep_kernels(dqmc_handle* h) { return h ? (int)h->graph_nodes : 0; }
 
 // ---------------------------------------------------------------------------
 // data access
@@ -1037,8 +1043,48 @@ extern "C" int dqmc_gpu_update(dqmc_handle* h, int nt) {
 
 extern "C" int dqmc_gpu_measure(dqmc_handle* h) {
     if (!h) return fail(DQMC_EINVAL, "null handle");
-    launch_measure(h->d_chains, h->nch, h->st);
+    launch_measure(h->d_chains, h->nch, h->ctas_per_chain, h->st);
     CK(cudaStreamSynchronize(h->st));
     CK(cudaGetLastError());
+    return DQMC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// per-kernel timing on the library stream (CUDA events), used by bench.py for
+// the roofline of the dominant kernel.  op: 0 update (slice 1), 1 UDV step
+// (stabilisation kernel, into the spare stack slot), 2 Green's function
+// (equal-time, stack slots 1 and 0, into Gnew), 3 kinetic+HS column pass on
+// G, 4 measurement, 5 kinetic+HS row pass on G.  The chains' state is
+// modified (update, measurement): call it after the timed region.
+// ---------------------------------------------------------------------------
+extern "C" int dqmc_gpu_time_op(dqmc_handle* h, int op, int reps, double* ms_out) {
+    if (!h || reps < 1 || !ms_out) return fail(DQMC_EINVAL, "invalid arguments");
+    const HostModel& m = *h->models[0];
+    int spare = h->nst + 1;
+    auto enqueue = [&]() {
+        switch (op) {
+        case 0: launch_update(h->d_chains, h->nch, 1, 0, h->st); break;
+        case 1: launch_stab_slots(h->d_chains, h->nch, 0, spare, h->st); break;
+        case 2: launch_green(h->d_chains, h->nch, 1, 0, 0, 0, 0, 0, 0, h->st); break;
+        case 3: { PropProg p; p.n = 0; prog_k(m, p, PW_INV, 0); prog_v(m, p, PW_INV, 1); prog_k(m, p, PW_INV, 1);
+                  launch_prog(h, MAT_G, p, 0); break; }
+        case 4: launch_measure(h->d_chains, h->nch, h->ctas_per_chain, h->st); break;
+        case 5: { PropProg p; p.n = 0; prog_k(m, p, PW_FWD, 0); prog_v(m, p, PW_FWD, 1); prog_k(m, p, PW_FWD, 1);
+                  launch_prog(h, MAT_G, p, 1); break; }
+        default: break;
+        }
+    };
+    if (op < 0 || op > 5) return fail(DQMC_EINVAL, "op 0..5");
+    if (op == 0) launch_sfmt(h->d_chains, h->nch, 1, h->st);
+    enqueue();   // warm-up
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaEventRecord(h->ev0, h->st));
+    for (int r = 0; r < reps; ++r) enqueue();
+    CK(cudaEventRecord(h->ev1, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaGetLastError());
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    *ms_out = ms / reps;
     return DQMC_OK;
 }

@@ -1,12 +1,13 @@
-// Equal-time measurement of one time slice, one CTA per chain.
+// Equal-time measurement of one time slice; a few CTAs per chain.
 //
 // Reference: src/dqmc_measure/equaltime_measure.f90 (equaltime_measure 1-69,
 // zkint, zint_u, zint_v, zqsq, ztsq, ztq, measure_cpcm/spsm/nn/jj/bondcorr/
 // paircorr).  Observables use Gc(i,j) = delta_ij - G(j,i) and are weighted
 // with zphi = sgn/Re(phase) * phase.  The distance-binned correlations are
-// accumulated without atomics: one thread owns one bin (distance d, orbitals
-// a, b) and walks the unit cells j, pairing each with cell i = j + d from a
-// precomputed table (imj(i, j) = d).
+// accumulated without atomics: one warp owns one bin (distance d, orbitals
+// a, b), its lanes walk the unit cells j, pairing each with cell i = j + d from
+// a precomputed table (imj(i, j) = d), and a warp reduction closes the bin.
+// The single-number energy terms run on the chain's first CTA.
 //
 // Bin layout per chain (complex): energy[10], cpcm, spsm, nn, pair_onsite
 // [lq*4 each, index (d) + lq*(no_i + 2 no_j)], jj, bb, pair_nn, pair_sn [lq
@@ -22,7 +23,7 @@ DQ_DEV double2 gf(const double2* G, int N, int i, int j) { return G[MIDX(i, j, N
 
 __global__ void __launch_bounds__(256) k_measure(const ChainDev* __restrict__ chains) {
     __shared__ double red[64];
-    const ChainDev c = chains[blockIdx.x];
+    const ChainDev c = chains[blockIdx.y];
     const ModelDev& md = *c.md;
     const int N = c.N, lq = md.lq, tid = threadIdx.x, nth = blockDim.x;
     const int nnf = md.nn_nf, zp = md.z_plq, nflr = md.nflr;
@@ -34,6 +35,77 @@ __global__ void __launch_bounds__(256) k_measure(const ChainDev* __restrict__ ch
     const double fsp = 1.0 - 1.0 / (double)(nflr * nflr), fn = 1.0 / (double)nflr;
     const bool hc = (md.nsub == 2);
 
+    // ---- distance-binned correlations: one warp per bin, lanes over cells ----
+    double2* cpcm = bins + 10;
+    double2* spsm = cpcm + 4 * lq;
+    double2* znn = spsm + 4 * lq;
+    double2* pons = znn + 4 * lq;
+    double2* zjj = pons + 4 * lq;
+    double2* zbb = zjj + lq;
+    double2* pnn = zbb + lq;
+    double2* psn = pnn + lq;
+    const int nsub = md.nsub;
+    const int lane = tid & 31;
+    const int nbin_a = lq * nsub * nsub, nbin = nbin_a + lq;
+    const int gw0 = blockIdx.x * (nth >> 5) + (tid >> 5), gws = gridDim.x * (nth >> 5);
+    for (int bin = gw0; bin < nbin; bin += gws) {
+        if (bin < nbin_a) {
+            int d = bin % lq, ab = bin / lq, a = ab % nsub, b = ab / nsub;
+            double2 s1 = cmk(0, 0), s2 = cmk(0, 0), s3 = cmk(0, 0), s4 = cmk(0, 0);
+            for (int cj = lane; cj < lq; cj += 32) {
+                int ci = md.cell_plus[d * lq + cj];
+                int i = ci * nsub + a, j = cj * nsub + b;
+                double2 gc = gcf(G, N, i, j), g = gf(G, N, i, j);
+                s1 = cadd(s1, gc);
+                s2 = cfma(gc, g, s2);
+                s3 = cadd(s3, cadd(cmul(gcf(G, N, i, i), gcf(G, N, j, j)), cscale(cmul(gc, g), fn)));
+                s4 = cfma(g, g, s4);
+            }
+            s1.x = warp_sum(s1.x); s1.y = warp_sum(s1.y); s2.x = warp_sum(s2.x); s2.y = warp_sum(s2.y);
+            s3.x = warp_sum(s3.x); s3.y = warp_sum(s3.y); s4.x = warp_sum(s4.x); s4.y = warp_sum(s4.y);
+            if (lane == 0) {
+                int k = d + lq * (a + 2 * b);
+                cpcm[k] = cfma(s1, zphi, cpcm[k]);
+                spsm[k] = cfma(cscale(s2, fsp), zphi, spsm[k]);
+                znn[k] = cfma(s3, zphi, znn[k]);
+                pons[k] = cfma(s4, zphi, pons[k]);
+            }
+        } else {
+            int d = bin - nbin_a;
+            double2 sj = cmk(0, 0), sb = cmk(0, 0), sn = cmk(0, 0), ss = cmk(0, 0);
+            for (int cj = lane; cj < lq; cj += 32) {
+                int ci = md.cell_plus[d * lq + cj];
+                int j0 = hc ? 2 * cj : cj, i0 = hc ? 2 * ci : ci;
+                int jnj = hc ? md.snlist[j0 * md.nsn] : md.nnlist[j0 * nnf];
+                int inj = hc ? md.snlist[i0 * md.nsn] : md.nnlist[i0 * nnf];
+                int jnb = md.nnlist[j0 * nnf], inb = md.nnlist[i0 * nnf];
+                int jns = md.snlist[j0 * md.nsn], ins = md.snlist[i0 * md.nsn];
+                double2 z1 = cmul(csub(gcf(G, N, i0, inj), gcf(G, N, inj, i0)), csub(gcf(G, N, j0, jnj), gcf(G, N, jnj, j0)));
+                double2 z3 = cadd(cmul(gcf(G, N, i0, jnj), gf(G, N, inj, j0)), cmul(gcf(G, N, inj, j0), gf(G, N, i0, jnj)));
+                z3 = csub(z3, cadd(cmul(gcf(G, N, i0, j0), gf(G, N, inj, jnj)), cmul(gcf(G, N, inj, jnj), gf(G, N, i0, j0))));
+                sj = csub(sj, cadd(z1, cscale(z3, fn)));
+                double2 ej = md.expar_nn[j0 * nnf], ei = md.expar_nn[i0 * nnf];
+                double2 bj = cadd(cmul(ej, gcf(G, N, j0, jnb)), cmul(cconj(ej), gcf(G, N, jnb, j0)));
+                double2 bi = cadd(cmul(ei, gcf(G, N, i0, inb)), cmul(cconj(ei), gcf(G, N, inb, i0)));
+                double2 x = cmul(cmul(ei, ej), cmul(gcf(G, N, i0, jnb), gf(G, N, inb, j0)));
+                x = cadd(x, cmul(cmul(cconj(ei), cconj(ej)), cmul(gcf(G, N, inb, j0), gf(G, N, i0, jnb))));
+                x = cadd(x, cmul(cmul(ei, cconj(ej)), cmul(gcf(G, N, i0, j0), gf(G, N, inb, jnb))));
+                x = cadd(x, cmul(cmul(cconj(ei), ej), cmul(gcf(G, N, inb, jnb), gf(G, N, i0, j0))));
+                sb = cadd(sb, cadd(cmul(bj, bi), cscale(x, fn)));
+                sn = cfma(gf(G, N, i0, j0), gf(G, N, inb, jnb), sn);
+                ss = cfma(gf(G, N, i0, j0), gf(G, N, ins, jns), ss);
+            }
+            sj.x = warp_sum(sj.x); sj.y = warp_sum(sj.y); sb.x = warp_sum(sb.x); sb.y = warp_sum(sb.y);
+            sn.x = warp_sum(sn.x); sn.y = warp_sum(sn.y); ss.x = warp_sum(ss.x); ss.y = warp_sum(ss.y);
+            if (lane == 0) {
+                zjj[d] = cfma(sj, zphi, zjj[d]);
+                zbb[d] = cfma(sb, zphi, zbb[d]);
+                pnn[d] = cfma(sn, zphi, pnn[d]);
+                psn[d] = cfma(ss, zphi, psn[d]);
+            }
+        }
+    }
+    if (blockIdx.x != 0) return;
     // ---- energy terms ----
     double2 zne = cmk(0, 0), zu = cmk(0, 0), zk = cmk(0, 0), zv = cmk(0, 0);
     for (int i = tid; i < N; i += nth) {
@@ -130,63 +202,6 @@ __global__ void __launch_bounds__(256) k_measure(const ChainDev* __restrict__ ch
         bins[tail + 3] = cadd(bins[tail + 3], cmul(zb, zphi));
         c.stats[ST_NOBS] += 1.0;
     }
-    // ---- distance-binned correlations ----
-    double2* cpcm = bins + 10;
-    double2* spsm = cpcm + 4 * lq;
-    double2* znn = spsm + 4 * lq;
-    double2* pons = znn + 4 * lq;
-    double2* zjj = pons + 4 * lq;
-    double2* zbb = zjj + lq;
-    double2* pnn = zbb + lq;
-    double2* psn = pnn + lq;
-    const int nsub = md.nsub;
-    for (int bin = tid; bin < lq * nsub * nsub; bin += nth) {
-        int d = bin % lq, ab = bin / lq, a = ab % nsub, b = ab / nsub;
-        double2 s1 = cmk(0, 0), s2 = cmk(0, 0), s3 = cmk(0, 0), s4 = cmk(0, 0);
-        for (int cj = 0; cj < lq; ++cj) {
-            int ci = md.cell_plus[d * lq + cj];
-            int i = ci * nsub + a, j = cj * nsub + b;
-            double2 gc = gcf(G, N, i, j), g = gf(G, N, i, j);
-            s1 = cadd(s1, gc);
-            s2 = cfma(gc, g, s2);
-            s3 = cadd(s3, cadd(cmul(gcf(G, N, i, i), gcf(G, N, j, j)), cscale(cmul(gc, g), fn)));
-            s4 = cfma(g, g, s4);
-        }
-        int k = d + lq * (a + 2 * b);
-        cpcm[k] = cfma(s1, zphi, cpcm[k]);
-        spsm[k] = cfma(cscale(s2, fsp), zphi, spsm[k]);
-        znn[k] = cfma(s3, zphi, znn[k]);
-        pons[k] = cfma(s4, zphi, pons[k]);
-    }
-    for (int d = tid; d < lq; d += nth) {
-        double2 sj = cmk(0, 0), sb = cmk(0, 0), sn = cmk(0, 0), ss = cmk(0, 0);
-        for (int cj = 0; cj < lq; ++cj) {
-            int ci = md.cell_plus[d * lq + cj];
-            int j0 = hc ? 2 * cj : cj, i0 = hc ? 2 * ci : ci;
-            int jnj = hc ? md.snlist[j0 * md.nsn] : md.nnlist[j0 * nnf];
-            int inj = hc ? md.snlist[i0 * md.nsn] : md.nnlist[i0 * nnf];
-            int jnb = md.nnlist[j0 * nnf], inb = md.nnlist[i0 * nnf];
-            int jns = md.snlist[j0 * md.nsn], ins = md.snlist[i0 * md.nsn];
-            double2 z1 = cmul(csub(gcf(G, N, i0, inj), gcf(G, N, inj, i0)), csub(gcf(G, N, j0, jnj), gcf(G, N, jnj, j0)));
-            double2 z3 = cadd(cmul(gcf(G, N, i0, jnj), gf(G, N, inj, j0)), cmul(gcf(G, N, inj, j0), gf(G, N, i0, jnj)));
-            z3 = csub(z3, cadd(cmul(gcf(G, N, i0, j0), gf(G, N, inj, jnj)), cmul(gcf(G, N, inj, jnj), gf(G, N, i0, j0))));
-            sj = csub(sj, cadd(z1, cscale(z3, fn)));
-            double2 ej = md.expar_nn[j0 * nnf], ei = md.expar_nn[i0 * nnf];
-            double2 bj = cadd(cmul(ej, gcf(G, N, j0, jnb)), cmul(cconj(ej), gcf(G, N, jnb, j0)));
-            double2 bi = cadd(cmul(ei, gcf(G, N, i0, inb)), cmul(cconj(ei), gcf(G, N, inb, i0)));
-            double2 x = cmul(cmul(ei, ej), cmul(gcf(G, N, i0, jnb), gf(G, N, inb, j0)));
-            x = cadd(x, cmul(cmul(cconj(ei), cconj(ej)), cmul(gcf(G, N, inb, j0), gf(G, N, i0, jnb))));
-            x = cadd(x, cmul(cmul(ei, cconj(ej)), cmul(gcf(G, N, i0, j0), gf(G, N, inb, jnb))));
-            x = cadd(x, cmul(cmul(cconj(ei), ej), cmul(gcf(G, N, inb, jnb), gf(G, N, i0, j0))));
-            sb = cadd(sb, cadd(cmul(bj, bi), cscale(x, fn)));
-            sn = cfma(gf(G, N, i0, j0), gf(G, N, inb, jnb), sn);
-            ss = cfma(gf(G, N, i0, j0), gf(G, N, ins, jns), ss);
-        }
-        zjj[d] = cfma(sj, zphi, zjj[d]);
-        zbb[d] = cfma(sb, zphi, zbb[d]);
-        pnn[d] = cfma(sn, zphi, pnn[d]);
-        psn[d] = cfma(ss, zphi, psn[d]);
-    }
 }
 
 __global__ void k_bins_clear(const ChainDev* __restrict__ chains, int nbins) {
@@ -195,8 +210,9 @@ __global__ void k_bins_clear(const ChainDev* __restrict__ chains, int nbins) {
     if (threadIdx.x == 0) c.stats[ST_NOBS] = 0.0;
 }
 
-void launch_measure(const ChainDev* chains, int nchains, cudaStream_t st) {
-    k_measure<<<nchains, 256, 0, st>>>(chains);
+void launch_measure(const ChainDev* chains, int nchains, int ctas_per_chain, cudaStream_t st) {
+    dim3 grid(ctas_per_chain, nchains);
+    k_measure<<<grid, 256, 0, st>>>(chains);
 }
 
 void launch_bins_clear(const ChainDev* chains, int nchains, int nbins, cudaStream_t st) {

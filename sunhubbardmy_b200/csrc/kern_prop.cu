@@ -51,14 +51,16 @@ __device__ void apply_op(const ModelDev& md, const int32_t* conf, int code, int 
         const int l1 = md.l1, l2 = md.l2, lq = md.lq;
         const double2* d = (which == PW_INV) ? md.exph0kinv : md.exph0k;
         const int s1 = right ? +1 : -1;
-        // dim 1 (stride 1, l2 lines), then dim 2 (stride l1, l1 lines)
+        // dim 1: nv*l2 contiguous lines; consecutive threads take different
+        // vectors (vector stride vs is odd, so their lines sit in different banks)
         for (int w = tid; w < nv * l2; w += nth) {
-            int v = w / l2, j2 = w % l2;
+            int v = w % nv, j2 = w / nv;
             line_dft(S + (size_t)v * vs + j2 * l1, l1, 1, md.tw1, s1);
         }
         __syncthreads();
+        // dim 2: nv*l1 lines of stride l1; consecutive threads take consecutive j1
         for (int w = tid; w < nv * l1; w += nth) {
-            int v = w / l1, j1 = w % l1;
+            int j1 = w % l1, v = w / l1;
             line_dft(S + (size_t)v * vs + j1, l2, l1, md.tw2, s1);
         }
         __syncthreads();
@@ -71,12 +73,12 @@ __device__ void apply_op(const ModelDev& md, const int32_t* conf, int code, int 
         }
         __syncthreads();
         for (int w = tid; w < nv * l2; w += nth) {
-            int v = w / l2, j2 = w % l2;
+            int v = w % nv, j2 = w / nv;
             line_dft(S + (size_t)v * vs + j2 * l1, l1, 1, md.tw1, -s1);
         }
         __syncthreads();
         for (int w = tid; w < nv * l1; w += nth) {
-            int v = w / l1, j1 = w % l1;
+            int j1 = w % l1, v = w / l1;
             line_dft(S + (size_t)v * vs + j1, l2, l1, md.tw2, -s1);
         }
     }
@@ -84,24 +86,25 @@ __device__ void apply_op(const ModelDev& md, const int32_t* conf, int code, int 
 }
 
 // Column pass: X <- Op_k ... Op_1 X for the program prog.
-__global__ void k_prop_cols(const ChainDev* __restrict__ chains, int mat_id, PropProg prog, int cb) {
+__global__ void __launch_bounds__(256, 2) k_prop_cols(const ChainDev* __restrict__ chains, int mat_id, PropProg prog, int cb) {
     extern __shared__ double2 sm[];
     const ChainDev c = chains[blockIdx.y];
     const ModelDev& md = *c.md;
     const int N = c.N;
     double2* X = chain_mat(c, mat_id);
+    const int vs = N + 1;   // odd vector stride: conflict-free strided lines
     for (int c0 = blockIdx.x * cb; c0 < N; c0 += gridDim.x * cb) {
         int nv = min(cb, N - c0);
-        for (int e = threadIdx.x; e < nv * N; e += blockDim.x) sm[e] = X[(size_t)c0 * N + e];
+        for (int e = threadIdx.x; e < nv * N; e += blockDim.x) sm[(e / N) * vs + e % N] = X[(size_t)c0 * N + e];
         __syncthreads();
-        for (int k = 0; k < prog.n; ++k) apply_op(md, c.conf, prog.op[k], 0, sm, nv, N);
-        for (int e = threadIdx.x; e < nv * N; e += blockDim.x) X[(size_t)c0 * N + e] = sm[e];
+        for (int k = 0; k < prog.n; ++k) apply_op(md, c.conf, prog.op[k], 0, sm, nv, vs);
+        for (int e = threadIdx.x; e < nv * N; e += blockDim.x) X[(size_t)c0 * N + e] = sm[(e / N) * vs + e % N];
         __syncthreads();
     }
 }
 
 // Row pass: X <- X Op_1 ... Op_k.  Rows are staged with a padded stride.
-__global__ void k_prop_rows(const ChainDev* __restrict__ chains, int mat_id, PropProg prog, int rb) {
+__global__ void __launch_bounds__(256, 2) k_prop_rows(const ChainDev* __restrict__ chains, int mat_id, PropProg prog, int rb) {
     extern __shared__ double2 sm[];
     const ChainDev c = chains[blockIdx.y];
     const ModelDev& md = *c.md;

@@ -21,9 +21,10 @@ struct ZGemmArgs {
     cplx* C; int ldc;
 };
 
+// no `volatile`: the compiler may interleave independent DMMAs
 DQ_DEV void dmma(double& d0, double& d1, double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-                 : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+        : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
 }
 
 DQ_DEV void cp_async16(void* smem, const void* gmem, bool valid) {
@@ -148,15 +149,24 @@ __device__ void zgemm_cta(const ZGemmArgs& g, int tile0, int tstep, cplx* smem) 
                         cplx v = Bs[kr * Cfg::LDB + wn0 + b * 8 + (lane >> 2)];
                         br[b] = v.x; bi[b] = conjB ? -v.y : v.y;
                     }
+                    // four independent sweeps over the fragments, so that two
+                    // DMMAs into one accumulator are 2*FM*FN instructions apart
 #pragma unroll
                     for (int a = 0; a < FM; ++a)
 #pragma unroll
-                        for (int b = 0; b < FN; ++b) {
-                            dmma(accr[a][b][0], accr[a][b][1], ar[a], br[b]);
-                            dmma(accr[a][b][0], accr[a][b][1], ain[a], bi[b]);
-                            dmma(acci[a][b][0], acci[a][b][1], ar[a], bi[b]);
-                            dmma(acci[a][b][0], acci[a][b][1], ai[a], br[b]);
-                        }
+                        for (int b = 0; b < FN; ++b) dmma(accr[a][b][0], accr[a][b][1], ar[a], br[b]);
+#pragma unroll
+                    for (int a = 0; a < FM; ++a)
+#pragma unroll
+                        for (int b = 0; b < FN; ++b) dmma(acci[a][b][0], acci[a][b][1], ar[a], bi[b]);
+#pragma unroll
+                    for (int a = 0; a < FM; ++a)
+#pragma unroll
+                        for (int b = 0; b < FN; ++b) dmma(accr[a][b][0], accr[a][b][1], ain[a], bi[b]);
+#pragma unroll
+                    for (int a = 0; a < FM; ++a)
+#pragma unroll
+                        for (int b = 0; b < FN; ++b) dmma(acci[a][b][0], acci[a][b][1], ai[a], br[b]);
                 }
             }
             __syncthreads();

@@ -104,6 +104,8 @@ SIGNATURES = {
     "dqmc_gpu_test_zgemm": (_i, [_vp, _i, _i, _i, _i, _i, _i, _i, _i, _d]),
     "dqmc_gpu_test_qr": (_i, [_vp, _i, _i, _vp]),
     "dqmc_gpu_last_sweeps_ms": (_d, [_vp]),
+    "dqmc_gpu_time_op": (_i, [_vp, _i, _i, _vp]),
+    "dqmc_gpu_sweep_kernels": (_i, [_vp]),
 }
 
 
@@ -332,6 +334,16 @@ class Dqmc:
         out = np.zeros(count, np.uint32)
         _check(load_library().dqmc_gpu_draw_u32(self.h, c, count, _ptr(out)), "draw_u32")
         return out
+
+    def sweep_kernels(self) -> int:
+        """Kernel launches in one captured sweep (b0 + 0b)."""
+        return load_library().dqmc_gpu_sweep_kernels(self.h)
+
+    def time_op(self, op: int, reps: int = 3) -> float:
+        """Device ms of one launch of sweep kernel `op` over all chains."""
+        ms = C.c_double()
+        _check(load_library().dqmc_gpu_time_op(self.h, op, reps, C.byref(ms)), "time_op")
+        return ms.value
 
     # diagnostics on the tensor-core kernels
     def set_work(self, which: int, m: np.ndarray, c: int = 0) -> None:
