@@ -153,6 +153,7 @@ __global__ void __launch_bounds__(256) k_green(const ChainDev* __restrict__ chai
             dlmax[i] = a; dlmin[i] = b;
             slog += log(a);
         }
+        __syncthreads();   // dmax/dmin are read by other threads below
         ZGemmArgs g;
         g.M = N; g.N = N; g.K = N; g.alpha = cmk(1, 0); g.beta = cmk(0, 0);
         g.A = UR; g.lda = N; g.opA = OP_C; g.B = UL; g.ldb = N; g.opB = OP_N; g.C = M; g.ldc = N;
@@ -165,6 +166,7 @@ __global__ void __launch_bounds__(256) k_green(const ChainDev* __restrict__ chai
             M[e] = cadd(u, cscale(Z[e], drmin[i] * dlmin[j]));
         }
     } else {
+        __syncthreads();   // drmax/drmin are read by other threads below
         for (size_t e = tid; e < NN; e += nth) {
             int i = (int)(e % N), j = (int)(e / N);
             M[e] = cadd(cscale(cconj(UR[MIDX(j, i, N)]), 1.0 / drmax[i]), cscale(VR[e], drmin[i]));
