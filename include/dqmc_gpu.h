@@ -163,6 +163,28 @@ int dqmc_gpu_sweep_kernels(dqmc_handle* h);
  * chain state; intended for benchmarks after the timed sweeps. */
 int dqmc_gpu_time_op(dqmc_handle* h, int op, int reps, double* ms_out);
 
+/* Allocation-free QR factorisation with log det Q.  No counterpart in the
+ * reference: it is an extra entry point for host codes that cannot allocate
+ * device memory themselves (their device memory comes from a pool they do not
+ * control, or they must not allocate once a run has started).  It allocates
+ * nothing: the caller passes device pointers to its own buffers and the
+ * library uses a fixed scratch area compiled into it (about 0.55 MB, held on
+ * every GPU that loads the library until the process exits).
+ *   a        device, n x n complex (2*n*n doubles), column-major.  In: the
+ *            matrix.  Out: R in the upper triangle (real diagonal) and the
+ *            Householder vectors below it (zgeqrf layout, tau not returned).
+ *   q        device, n x n complex out: the explicit unitary factor Q.
+ *   logdetq  device, one complex (2 doubles) out: log det Q.
+ *   stream   cudaStream_t to launch on (NULL = legacy default stream).
+ * n must be 1..512; larger n returns DQMC_EINVAL.  The call is asynchronous on
+ * `stream`.  The first call on each device looks up the scratch address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the scratch, so calls whose kernels overlap on the GPU
+ * (other streams, other host threads) race; serialise them.  Errors are
+ * described by dqmc_gpu_noalloc_error(). */
+int dqmc_gpu_qr_logdet_noalloc(int n, double* a, double* q, double* logdetq, void* stream);
+const char* dqmc_gpu_noalloc_error(void);
+
 #ifdef __cplusplus
 }
 #endif

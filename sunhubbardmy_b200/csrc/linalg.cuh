@@ -28,7 +28,7 @@ struct LinalgSmem {
 };
 
 // ---- panel factorisation (zgeqr2 on an m x jb panel in shared memory) ----
-__device__ void panel_qr(double2* P, int m, int jb, double2* taus, LinalgSmem* L) {
+static __device__ void panel_qr(double2* P, int m, int jb, double2* taus, LinalgSmem* L) {
     const int tid = threadIdx.x, nth = blockDim.x;
     for (int j = 0; j < jb; ++j) {
         double2* col = P + (size_t)j * m;
@@ -102,7 +102,7 @@ __device__ void panel_qr(double2* P, int m, int jb, double2* taus, LinalgSmem* L
 
 // T (jb x jb upper) of the block reflector H_1..H_jb = I - V T V^H (zlarft 'F','C').
 // V is the unit-lower panel in shared memory (m x jb).
-__device__ void panel_larft(const double2* P, int m, int jb, const double2* taus, double2* Tout, LinalgSmem* L) {
+static __device__ void panel_larft(const double2* P, int m, int jb, const double2* taus, double2* Tout, LinalgSmem* L) {
     const int tid = threadIdx.x;
     // Gram S(a,b) = V(:,a)^H V(:,b) for a < b
     for (int e = tid; e < jb * jb; e += blockDim.x) {
@@ -141,7 +141,7 @@ __device__ void panel_larft(const double2* P, int m, int jb, const double2* taus
 }
 
 // Explicit reflector block of panel p into Vs (rows p..N-1 stored at Vs[r - p], ld N)
-__device__ void build_vblock(const double2* A, int N, int p, int jb, double2* Vs) {
+static __device__ void build_vblock(const double2* A, int N, int p, int jb, double2* Vs) {
     int m = N - p;
     for (int e = threadIdx.x; e < m * jb; e += blockDim.x) {
         int r = e % m, cc = e / m;
@@ -152,7 +152,7 @@ __device__ void build_vblock(const double2* A, int N, int p, int jb, double2* Vs
 }
 
 // X[p:N, c0:c0+nc] <- (I - V T V^H)^op X,  op = H (apply Q^H) or none (apply Q)
-__device__ void apply_block(const double2* Vs, const double2* Tp, int N, int p, int jb,
+static __device__ void apply_block(const double2* Vs, const double2* Tp, int N, int p, int jb,
                             double2* X, int c0, int nc, int use_th, LinalgScratch& sc, cplx* gsm) {
     if (nc <= 0) return;
     int m = N - p;
@@ -185,7 +185,7 @@ __device__ void apply_block(const double2* Vs, const double2* Tp, int N, int p, 
 
 // In-place QR of A (N x N): R in the upper triangle, reflectors below,
 // tau and the per-panel T factors in the scratch.  smem_panel holds >= N*16 double2.
-__device__ void cta_qr(double2* A, int N, LinalgScratch& sc, double2* smem_panel, cplx* gsm, LinalgSmem* L) {
+static __device__ void cta_qr(double2* A, int N, LinalgScratch& sc, double2* smem_panel, cplx* gsm, LinalgSmem* L) {
     for (int p = 0; p < N; p += QR_NB) {
         const int jb = min(QR_NB, N - p), m = N - p;
         double2* P = smem_panel;
@@ -208,7 +208,7 @@ __device__ void cta_qr(double2* A, int N, LinalgScratch& sc, double2* smem_panel
 }
 
 // log det Q = sum_i log(1 - tau_i 2 Re(tau_i) / |tau_i|^2)  (s_matrix.f90:1290-1298)
-__device__ double2 cta_logdet_q(const double2* tau, int N, double* red) {
+static __device__ double2 cta_logdet_q(const double2* tau, int N, double* red) {
     double2 acc = cmk(0, 0);
     for (int i = threadIdx.x; i < N; i += blockDim.x) {
         double2 t = tau[i];
@@ -222,7 +222,7 @@ __device__ double2 cta_logdet_q(const double2* tau, int N, double* red) {
 }
 
 // Q (N x N) from the factored A into Qout (zungqr, blocked backward).
-__device__ void cta_form_q(const double2* A, int N, double2* Qout, LinalgScratch& sc, cplx* gsm) {
+static __device__ void cta_form_q(const double2* A, int N, double2* Qout, LinalgScratch& sc, cplx* gsm) {
     for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
         int r = e % N, cc = e / N;
         Qout[e] = cmk(r == cc ? 1.0 : 0.0, 0.0);
@@ -238,7 +238,7 @@ __device__ void cta_form_q(const double2* A, int N, double2* Qout, LinalgScratch
 }
 
 // X <- Q^H X for all N columns of X (Q from the factored A).
-__device__ void cta_apply_qh(const double2* A, int N, double2* X, LinalgScratch& sc, cplx* gsm) {
+static __device__ void cta_apply_qh(const double2* A, int N, double2* X, LinalgScratch& sc, cplx* gsm) {
     for (int p = 0; p < N; p += QR_NB) {
         const int jb = min(QR_NB, N - p);
         build_vblock(A, N, p, jb, sc.Vs);
@@ -248,7 +248,7 @@ __device__ void cta_apply_qh(const double2* A, int N, double2* X, LinalgScratch&
 }
 
 // X <- R^{-1} X with R the upper triangle of A (blocked back substitution).
-__device__ void cta_trsm_upper(const double2* A, int N, double2* X, cplx* gsm, LinalgSmem* L) {
+static __device__ void cta_trsm_upper(const double2* A, int N, double2* X, cplx* gsm, LinalgSmem* L) {
     int last = ((N - 1) / QR_NB) * QR_NB;
     for (int p = last; p >= 0; p -= QR_NB) {
         const int jb = min(QR_NB, N - p);

@@ -106,6 +106,8 @@ SIGNATURES = {
     "dqmc_gpu_last_sweeps_ms": (_d, [_vp]),
     "dqmc_gpu_time_op": (_i, [_vp, _i, _i, _vp]),
     "dqmc_gpu_sweep_kernels": (_i, [_vp]),
+    "dqmc_gpu_qr_logdet_noalloc": (_i, [_i, _vp, _vp, _vp, _vp]),
+    "dqmc_gpu_noalloc_error": (C.c_char_p, []),
 }
 
 
@@ -146,6 +148,17 @@ def test_seed(irank: int) -> int:
     if v >= 1 << 31:
         v -= 1 << 32
     return abs(v)
+
+
+def qr_logdet_noalloc(n: int, a_dev: int, q_dev: int, logdetq_dev: int, stream: int = 0) -> None:
+    """Allocation-free QR of a caller-owned device matrix (see
+    dqmc_gpu_qr_logdet_noalloc in include/dqmc_gpu.h): for callers that cannot
+    allocate device memory; all arguments are raw device addresses."""
+    L = load_library()
+    rc = L.dqmc_gpu_qr_logdet_noalloc(int(n), C.c_void_p(a_dev), C.c_void_p(q_dev),
+                                      C.c_void_p(logdetq_dev), C.c_void_p(stream))
+    if rc != 0:
+        raise DqmcError(f"qr_logdet_noalloc failed ({rc}): {L.dqmc_gpu_noalloc_error().decode()}")
 
 
 # ----------------------------------------------------------------------------
