@@ -1,0 +1,150 @@
+"""CPU tests of the host side: the C ABI library loads and exports every
+declared symbol, parameter derivation matches make_tables, the library fails
+cleanly without a GPU, dqmc.in / conf files round-trip, and the replica bin
+reduction works across two gloo ranks."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+from tests._cases import CASES
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_symbols():
+    text = open(os.path.join(ROOT, "include", "dqmc_gpu.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(dqmc_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    import ctypes
+    import sunhubbardmy_b200 as sb
+    lib = sb.load_library()
+    names = _declared_symbols()
+    assert len(names) > 30
+    for n in names:
+        assert hasattr(lib, n), n
+        assert isinstance(getattr(lib, n), ctypes._CFuncPtr)
+    # and the Python binding declares a signature for each of them
+    assert set(names) <= set(sb.dqmc.SIGNATURES)
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_params_derive_matches_oracle(oracle, case):
+    import sunhubbardmy_b200 as sb
+    p = sb.DqmcParams.make(**CASES[case])
+    m = oracle.Model(**CASES[case])
+    assert (p.ndim, p.lq, p.ltrot, p.nst, p.lcomp) == (m.ndim, m.lq, m.ltrot, m.nst, m.lcomp)
+    if CASES[case]["update"] != 0:
+        assert p.nublock == m.nublock
+
+
+def test_params_defaults_like_make_tables():
+    import sunhubbardmy_b200 as sb
+    # nublock defaults (src/model_para.f90:384-415)
+    assert sb.DqmcParams.make(l1=16, l2=16, update=sb.DELAY, nublock=0).nublock == 32
+    assert sb.DqmcParams.make(l1=4, l2=4, update=sb.DELAY, nublock=0).nublock == 4
+    assert sb.DqmcParams.make(l1=20, l2=20, update=sb.DELAY, nublock=0).nublock == 32   # 400/5 < 256
+    assert sb.DqmcParams.make(l1=12, l2=12, lattice=sb.HONEYCOMB, update=sb.SUBMATRIX, nublock=0).nublock == 32
+    p = sb.DqmcParams.make(beta=8.0, dtau=0.1, nwrap=10)
+    assert (p.ltrot, p.nst) == (80, 8)
+    p = sb.DqmcParams.make(beta=8.5, dtau=0.1, nwrap=10)
+    assert (p.ltrot, p.nst) == (85, 9)
+    with pytest.raises(sb.DqmcError):
+        sb.DqmcParams.make(lattice=7)
+
+
+def test_create_without_gpu_fails_cleanly():
+    import torch
+    import sunhubbardmy_b200 as sb
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    p = sb.DqmcParams.make(**CASES["sq4_cb_exact_fast"])
+    with pytest.raises(sb.DqmcError, match="CUDA"):
+        sb.Dqmc(p, 1)
+
+
+def test_read_dqmc_in():
+    import sunhubbardmy_b200 as sb
+    text = """&model_para
+  la = 6, lb = 6,
+  beta = 8.d0, dtau = 0.1d0,
+  rt = 1.0d0, rhub = 6.d0,
+  nflr = 4, lproju = .false.,
+/
+&ctrl_para
+  nwrap = 10, nsweep = 20, nbin = 5,
+  nublock = 32, ltau = .false.
+/
+"""
+    kw = sb.read_dqmc_in(text)
+    assert kw["l1"] == 6 and kw["l2"] == 6 and kw["nflr"] == 4
+    assert kw["beta"] == 8.0 and kw["dtau"] == 0.1 and kw["rhub"] == 6.0
+    assert kw["nwrap"] == 10 and kw["nublock"] == 32 and kw["lproju"] == 0
+    p = sb.DqmcParams.make(lattice=sb.HONEYCOMB, **kw)
+    assert (p.ndim, p.ltrot) == (72, 80)
+
+
+def test_conf_file_roundtrip(tmp_path):
+    import sunhubbardmy_b200 as sb
+    rng = np.random.default_rng(0)
+    confs = [rng.integers(1, 5, size=(8, 16), dtype=np.int32) for _ in range(3)]
+    path = tmp_path / "conf_u.out"
+    sb.write_conf(str(path), confs)
+    back = sb.read_conf(str(path), 8, 16, n_chains=4)
+    for a, b in zip(confs, back):
+        assert np.array_equal(a, b)
+    assert np.array_equal(back[3], confs[0])        # missing chains copy chain 0
+    (tmp_path / "fresh").write_text("0\n")
+    assert sb.read_conf(str(tmp_path / "fresh"), 8, 16) is None
+
+
+def test_equaltime_output_normalisation(tmp_path):
+    import sunhubbardmy_b200 as sb
+    lq = 4
+    rng = np.random.default_rng(1)
+    flat = [rng.standard_normal(10 + 20 * lq + 4) + 1j * rng.standard_normal(10 + 20 * lq + 4) for _ in range(2)]
+    bins = [sb.unpack_bins(f, lq, nobs=5) for f in flat]
+    red = sb.equaltime_output(bins, str(tmp_path))
+    assert np.allclose(red["energy"], (flat[0][:10] + flat[1][:10]) / 10.0)
+    line = (tmp_path / "energy.bin").read_text().strip()
+    assert len(line.split()) == 16
+
+
+def _gloo_worker(rank, world, port, q):
+    import torch.distributed as dist
+    import sunhubbardmy_b200 as sb
+    from sunhubbardmy_b200.replicas import reduce_bins, replica_seeds
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    lq = 4
+    flat = [np.full(10 + 20 * lq + 4, rank + 1.0 + c, complex) for c in range(2)]
+    bins = [sb.unpack_bins(f, lq, nobs=3) for f in flat]
+    red = reduce_bins(bins)
+    q.put((rank, replica_seeds(rank, 2), red["energy"][0], red["chains"]))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_replica_bin_reduction_two_gloo_ranks():
+    import socket
+    import torch.multiprocessing as mp
+    s = socket.socket(); s.bind(("127.0.0.1", 0)); port = s.getsockname()[1]; s.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_gloo_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    # chain values 1,2 (rank 0) and 2,3 (rank 1): sum 8 over 4 chains, nobs 3
+    for rank, seeds, e0, nch in res:
+        assert nch == 4
+        assert abs(e0 - 8.0 / (4 * 3)) < 1e-12
+    assert res[0][1] == [1909706392, 501232835]
+    assert set(res[0][1]).isdisjoint(res[1][1])

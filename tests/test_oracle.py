@@ -1,0 +1,238 @@
+"""CPU checks of the oracle (the parity checker) against independent references.
+
+The oracle restates the Fortran reference; the reference itself cannot run
+here (no Fortran compiler, MPI or MKL), so these tests pin the restatement by
+  * an independent numpy restatement of the reference's SFMT, written in the
+    reference's own 64-bit formulation (lib/m_spring.f90:256-379);
+  * scipy's LAPACK for the restated zgeqr2 / zlaqp2 / zung2r / zgetf2;
+  * known answers: the free-fermion Green's function and the Hubbard atom;
+  * internal consistency of the three local-update flavours.
+"""
+import numpy as np
+import pytest
+import scipy.linalg as sl
+from scipy.linalg import lapack
+
+from tests._cases import CASES
+
+
+# ---------------------------------------------------------------- SFMT
+def sfmt_numpy(seed: int, count: int) -> np.ndarray:
+    """spring_sfmt_init + spring_sfmt_source in the reference's 64-bit form."""
+    M64 = (1 << 64) - 1
+    pt32 = [0] * 624
+    pt32[0] = seed & 0xFFFFFFFF
+    for i in range(1, 624):
+        pt32[i] = (1812433253 * (pt32[i - 1] ^ (pt32[i - 1] >> 30)) + i) & 0xFFFFFFFF
+    parity = (1, 0, 0, 331998852)
+    inner = 0
+    for i in range(4):
+        work = pt32[i] & parity[i]
+        for _ in range(32):
+            inner ^= work & 1
+            work >>= 1
+    if inner != 1:
+        done = False
+        for i in range(4):
+            work = 1
+            for _ in range(32):
+                if work & parity[i]:
+                    pt32[i] ^= work
+                    done = True
+                    break
+                work <<= 1
+            if done:
+                break
+    pt64 = [(pt32[2 * i + 1] << 32) | pt32[2 * i] for i in range(312)]
+
+    def core(a_t, a_b, b_t, b_b, c_t, c_b, d_t, d_b):
+        x_t = ((a_t << 8) | (a_b >> 56)) & M64
+        x_b = (a_b << 8) & M64
+        y_t = c_t >> 8
+        y_b = ((c_t << 56) & M64) | (c_b >> 8)
+        r_b = a_b ^ x_b ^ ((b_b >> 11) & 8667995624701935) ^ y_b ^ (((d_b & 70364449226751) << 18) & M64)
+        r_t = a_t ^ x_t ^ ((b_t >> 11) & 9007156306837503) ^ y_t ^ (((d_t & 70364449226751) << 18) & M64)
+        return r_t, r_b
+
+    def kernel():
+        r1_b, r1_t, r2_b, r2_t = pt64[308], pt64[309], pt64[310], pt64[311]
+        for i in range(156):
+            j = i + 122 if i < 34 else i + 122 - 156
+            t, b = core(pt64[2 * i + 1], pt64[2 * i], pt64[2 * j + 1], pt64[2 * j], r1_t, r1_b, r2_t, r2_b)
+            pt64[2 * i + 1], pt64[2 * i] = t, b
+            r1_b, r1_t = r2_b, r2_t
+            r2_b, r2_t = pt64[2 * i], pt64[2 * i + 1]
+
+    out = []
+    idx = 624
+    for _ in range(count):
+        if idx >= 624:
+            kernel()
+            idx = 0
+        w = pt64[idx // 2]
+        out.append((w >> 32) & 0xFFFFFFFF if idx & 1 else w & 0xFFFFFFFF)
+        idx += 1
+    return np.array(out, dtype=np.uint32)
+
+
+def test_sfmt_matches_independent_restatement(oracle):
+    seed = oracle.lib().orc_test_seed(0)
+    assert seed == 1909706392
+    ref = sfmt_numpy(seed, 2000)
+    m = oracle.Model(**CASES["sq4_cb_exact_fast"])
+    c = oracle.Chain(m, seed, draw_conf=False)
+    got = np.array([int(round(c.uniform() * 4294967296.0 - 0.5)) for _ in range(2000)], np.uint32)
+    assert np.array_equal(got, ref)
+
+
+def test_test_seed_wraps_like_int32(oracle):
+    import sunhubbardmy_b200 as sb
+    for r in range(8):
+        assert oracle.lib().orc_test_seed(r) == sb.test_seed(r)
+    assert sb.test_seed(1) == 501232835      # |(3989 * 951049) mod 2^32 as int32|
+
+
+# ---------------------------------------------------------------- LAPACK restatements
+def _cmat(m, n, seed):
+    rng = np.random.default_rng(seed)
+    return np.asfortranarray(rng.standard_normal((m, n)) + 1j * rng.standard_normal((m, n)))
+
+
+def test_zgeqr2_matches_lapack(oracle):
+    a = _cmat(40, 40, 1)
+    ours, tau = a.copy(order="F"), np.zeros(40, complex)
+    oracle.lib().orc_zgeqr2(40, 40, oracle._ptr(ours), 40, oracle._ptr(tau))
+    qr, tau_ref, _, info = lapack.zgeqrf(a)
+    assert info == 0
+    assert np.max(np.abs(np.triu(ours) - np.triu(qr))) < 1e-12
+    assert np.max(np.abs(tau - tau_ref)) < 1e-12
+    q = ours.copy(order="F")
+    oracle.lib().orc_zung2r(40, 40, 40, oracle._ptr(q), 40, oracle._ptr(tau))
+    q_ref, _, info = lapack.zungqr(qr, tau_ref)
+    assert np.max(np.abs(q - q_ref)) < 1e-12
+
+
+def test_zgeqp2_matches_zgeqp3(oracle):
+    a = _cmat(30, 30, 2) * np.logspace(3, -3, 30)[None, :][:, np.random.default_rng(5).permutation(30)]
+    ours, tau = np.asfortranarray(a), np.zeros(30, complex)
+    ours = ours.copy(order="F")
+    jp = np.zeros(30, np.int32)
+    oracle.lib().orc_zgeqp2(30, 30, oracle._ptr(ours), 30, oracle._ptr(jp), oracle._ptr(tau))
+    qr, jpvt, tau_ref, _, info = lapack.zgeqp3(np.asfortranarray(a))
+    assert np.array_equal(jp, jpvt)          # scipy returns 1-based pivots too
+    assert np.max(np.abs(np.triu(ours) - np.triu(qr))) < 1e-10 * np.max(np.abs(qr))
+
+
+def test_zgetf2_matches_zgetrf(oracle):
+    a = _cmat(25, 25, 3)
+    ours, ipiv = a.copy(order="F"), np.zeros(25, np.int32)
+    oracle.lib().orc_zgetf2(25, 25, oracle._ptr(ours), 25, oracle._ptr(ipiv))
+    lu, piv, info = lapack.zgetrf(a)
+    assert np.array_equal(ipiv - 1, piv)
+    assert np.max(np.abs(ours - lu)) < 1e-12
+
+
+def test_inv_logdet(oracle):
+    a = _cmat(20, 20, 4) + 3 * np.eye(20)
+    inv = a.copy(order="F")
+    ld = np.zeros(2)
+    oracle.lib().orc_inv_logdet_lu(20, oracle._ptr(inv), oracle._ptr(ld))
+    sign, logabs = np.linalg.slogdet(a)
+    assert np.max(np.abs(inv - np.linalg.inv(a))) < 1e-12
+    assert abs(ld[0] - logabs) < 1e-12
+    assert abs(np.exp(1j * ld[1]) - sign) < 1e-12
+
+
+# ---------------------------------------------------------------- known answers
+def test_free_fermion_green_fft(oracle):
+    m = oracle.Model(lattice=1, l1=4, l2=4, beta=4.0, dtau=0.1, rhub=0.0, kinetic=1, nwrap=10)
+    c = oracle.Chain(m, 1)
+    c.sweep_start()
+    H = m.h0mat()
+    w, v = np.linalg.eigh(H)
+    g_ex = (v * (1.0 / (1.0 + np.exp(-m.params.beta * w)))[None, :]) @ v.conj().T
+    assert np.max(np.abs(c.green() - g_ex)) < 1e-12
+
+
+def test_free_fermion_green_checkerboard(oracle):
+    kw = dict(lattice=2, l1=3, l2=3, beta=3.0, dtau=0.1, rhub=0.0, kinetic=0, nwrap=10, mu=0.2)
+    m = oracle.Model(**kw)
+    c = oracle.Chain(m, 1)
+    c.sweep_start()
+    # B(beta, 0) from the 2x2 bond exponentials, applied in the reference's order
+    N = m.ndim
+    B = np.eye(N, dtype=complex, order="F")
+    for _ in range(m.ltrot):
+        for nf in list(range(1, m.nn_nf + 1)) + list(range(m.nn_nf, 0, -1)):
+            m.h0_prop(oracle.LEFT_FORWARD, nf, B)
+    g_ex = np.linalg.inv(np.eye(N) + B)
+    assert np.max(np.abs(c.green() - g_ex)) < 1e-11
+    # and the bond exponential really is exp(-dtau/2 h_bond)
+    kin = m.kinetic()
+    t = m.tables()
+    i0 = t["nnlf_list"][0] - 1
+    i1 = t["nnlist"][i0, 0] - 1
+    H = m.h0mat()
+    h = np.array([[-kw["mu"] / m.nn_nf, H[i0, i1]], [H[i1, i0], -kw["mu"] / m.nn_nf]])
+    assert np.max(np.abs(kin["urt"][0] - sl.expm(-0.5 * kw["dtau"] * h))) < 1e-14
+
+
+def test_hubbard_atom_double_occupancy(oracle):
+    """rt = 0: independent sites, H = U/2 (n - 1)^2 per site at half filling;
+    D = e^{-beta U / 2} / (2 (1 + e^{-beta U/2})).  EXACTHS is exact here, so the
+    Monte Carlo mean must agree within its statistical error."""
+    U, beta = 2.0, 1.0
+    kw = dict(lattice=1, l1=2, l2=2, beta=beta, dtau=0.1, rt=0.0, rhub=U, nflr=2, kinetic=0,
+              update=1, hs=0, nwrap=10, nublock=4)
+    m = oracle.Model(**kw)
+    c = oracle.Chain(m, 7)
+    c.sweep_start()
+    for _ in range(20):
+        c.sweep_b0(True, False); c.sweep_0b(True, False)
+    series = []
+    for _ in range(300):
+        c.obser_init()
+        c.sweep_b0(True, True); c.sweep_0b(True, True)
+        b = c.bins()
+        series.append((b["energy"][3] / b["energy"][0]).real / m.ndim)
+    s = np.asarray(series)
+    d_exact = np.exp(-beta * U / 2) / (2 * (1 + np.exp(-beta * U / 2)))
+    err = s.std(ddof=1) / np.sqrt(len(s)) * 3.0      # generous: autocorrelation
+    assert abs(s.mean() - d_exact) < max(err, 2e-3), (s.mean(), d_exact)
+
+
+# ---------------------------------------------------------------- consistency
+@pytest.mark.parametrize("case", ["sq4_cb_exact_fast", "hc3_cb_su4_sub"])
+def test_update_flavours_agree(oracle, case):
+    kw = dict(CASES[case])
+    out = []
+    for upd in (0, 1, 2):
+        kw["update"] = upd
+        kw["nublock"] = 8 if upd else 0
+        m = oracle.Model(**kw)
+        c = oracle.Chain(m, 1909706392)
+        c.sweep_start()
+        c.sweep_b0(); c.sweep_0b()
+        out.append((c.conf(), c.green(), c.diag()))
+    for conf, g, d in out[1:]:
+        assert np.array_equal(conf, out[0][0])
+        assert np.max(np.abs(g - out[0][1])) < 1e-10
+        assert d["accepted"] == out[0][2]["accepted"]
+        assert d["max_wrap_error"] < 1e-10
+
+
+def test_lattice_tables(oracle):
+    for kw in (dict(lattice=1, l1=4, l2=6), dict(lattice=2, l1=3, l2=4)):
+        m = oracle.Model(beta=1.0, dtau=0.1, **kw)
+        t = m.tables()
+        N, lq = m.ndim, m.lq
+        # every family pairs each A site with a distinct B site
+        for f in range(m.nn_nf):
+            b = t["nnlist"][t["nnlf_list"] - 1, f]
+            assert len(set(b.tolist())) == m.nn_lf
+            assert not set(b.tolist()) & set(t["nnlf_list"].tolist())
+        # imj: zero distance is the last bin, and each row is a permutation
+        assert np.all(np.diag(t["imj"]) == lq)
+        for i in range(lq):
+            assert sorted(t["imj"][i].tolist()) == list(range(1, lq + 1))
+        assert t["list"][:, 0].max() == lq and t["list"][:, 1].max() == m.nsub
