@@ -45,7 +45,7 @@ def test_params_derive_matches_oracle(oracle, case):
 def test_params_defaults_like_make_tables():
     import sunhubbardmy_b200 as sb
     # nublock defaults (src/model_para.f90:384-415)
-    assert sb.DqmcParams.make(l1=16, l2=16, update=sb.DELAY, nublock=0).nublock == 32
+    assert sb.DqmcParams.make(l1=16, l2=16, update=sb.DELAY, nublock=0).nublock == 16   # 256/5 < 64
     assert sb.DqmcParams.make(l1=4, l2=4, update=sb.DELAY, nublock=0).nublock == 4
     assert sb.DqmcParams.make(l1=20, l2=20, update=sb.DELAY, nublock=0).nublock == 32   # 400/5 < 256
     assert sb.DqmcParams.make(l1=12, l2=12, lattice=sb.HONEYCOMB, update=sb.SUBMATRIX, nublock=0).nublock == 32
