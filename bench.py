@@ -7,7 +7,7 @@ nublock = 32, general 4-component HS field, nwrap = 10 (nst = 20).  A step is
 one full sweep (b0 + 0b: 2 * ltrot * N = 102,400 proposals per chain) with
 equal-time measurement of every slice, stabilisation and wrap checks.  Each GPU
 advances --chains independent chains (the reference's one-chain-per-MPI-rank
-parallelism, batched: one CTA per chain); the HS fields are drawn from the
+parallelism, batched: one CTA per chain, 296 = two per SM by default); the HS fields are drawn from the
 reference's -DTEST seeds, one per chain.  The working set (about 52 MiB per
 chain) is far larger than L2, so no flush is needed between steps.
 
@@ -300,7 +300,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--chains", type=int, default=148)
+    ap.add_argument("--chains", type=int, default=296)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     args = ap.parse_args()

@@ -35,6 +35,22 @@ __global__ void __launch_bounds__(256) k_measure(const ChainDev* __restrict__ ch
     const double fsp = 1.0 - 1.0 / (double)(nflr * nflr), fn = 1.0 / (double)nflr;
     const bool hc = (md.nsub == 2);
 
+    // ---- per-site and per-cell quantities shared by all bins (shared memory) ----
+    __shared__ double2 gcd[512];     // Gc(i,i)
+    __shared__ double2 jcell[512];   // Gc(i0,in) - Gc(in,i0), current partner
+    __shared__ double2 bcell[512];   // e Gc(i0,ib) + conj(e) Gc(ib,i0), bond partner
+    __shared__ int pj[512], pb[512], ps[512];
+    for (int i = tid; i < N; i += nth) gcd[i] = gcf(G, N, i, i);
+    for (int cc = tid; cc < lq; cc += nth) {
+        int i0 = hc ? 2 * cc : cc;
+        int inj = hc ? md.snlist[i0 * md.nsn] : md.nnlist[i0 * nnf];
+        int inb = md.nnlist[i0 * nnf];
+        double2 e = md.expar_nn[i0 * nnf];
+        pj[cc] = inj; pb[cc] = inb; ps[cc] = md.snlist[i0 * md.nsn];
+        jcell[cc] = csub(gcf(G, N, i0, inj), gcf(G, N, inj, i0));
+        bcell[cc] = cadd(cmul(e, gcf(G, N, i0, inb)), cmul(cconj(e), gcf(G, N, inb, i0)));
+    }
+    __syncthreads();
     // ---- distance-binned correlations: one warp per bin, lanes over cells ----
     double2* cpcm = bins + 10;
     double2* spsm = cpcm + 4 * lq;
@@ -58,7 +74,7 @@ __global__ void __launch_bounds__(256) k_measure(const ChainDev* __restrict__ ch
                 double2 gc = gcf(G, N, i, j), g = gf(G, N, i, j);
                 s1 = cadd(s1, gc);
                 s2 = cfma(gc, g, s2);
-                s3 = cadd(s3, cadd(cmul(gcf(G, N, i, i), gcf(G, N, j, j)), cscale(cmul(gc, g), fn)));
+                s3 = cadd(s3, cadd(cmul(gcd[i], gcd[j]), cscale(cmul(gc, g), fn)));
                 s4 = cfma(g, g, s4);
             }
             s1.x = warp_sum(s1.x); s1.y = warp_sum(s1.y); s2.x = warp_sum(s2.x); s2.y = warp_sum(s2.y);
@@ -76,24 +92,25 @@ __global__ void __launch_bounds__(256) k_measure(const ChainDev* __restrict__ ch
             for (int cj = lane; cj < lq; cj += 32) {
                 int ci = md.cell_plus[d * lq + cj];
                 int j0 = hc ? 2 * cj : cj, i0 = hc ? 2 * ci : ci;
-                int jnj = hc ? md.snlist[j0 * md.nsn] : md.nnlist[j0 * nnf];
-                int inj = hc ? md.snlist[i0 * md.nsn] : md.nnlist[i0 * nnf];
-                int jnb = md.nnlist[j0 * nnf], inb = md.nnlist[i0 * nnf];
-                int jns = md.snlist[j0 * md.nsn], ins = md.snlist[i0 * md.nsn];
-                double2 z1 = cmul(csub(gcf(G, N, i0, inj), gcf(G, N, inj, i0)), csub(gcf(G, N, j0, jnj), gcf(G, N, jnj, j0)));
+                int jnj = pj[cj], inj = pj[ci], jnb = pb[cj], inb = pb[ci];
+                double2 g00 = gf(G, N, i0, j0), gc00 = gcf(G, N, i0, j0);
+                // current-current, connected part (measure_jj)
                 double2 z3 = cadd(cmul(gcf(G, N, i0, jnj), gf(G, N, inj, j0)), cmul(gcf(G, N, inj, j0), gf(G, N, i0, jnj)));
-                z3 = csub(z3, cadd(cmul(gcf(G, N, i0, j0), gf(G, N, inj, jnj)), cmul(gcf(G, N, inj, jnj), gf(G, N, i0, j0))));
-                sj = csub(sj, cadd(z1, cscale(z3, fn)));
+                double2 gnn_j = gf(G, N, inj, jnj), gcnn_j = gcf(G, N, inj, jnj);
+                z3 = csub(z3, cadd(cmul(gc00, gnn_j), cmul(gcnn_j, g00)));
+                sj = csub(sj, cadd(cmul(jcell[ci], jcell[cj]), cscale(z3, fn)));
+                // bond-bond (measure_bondcorr)
                 double2 ej = md.expar_nn[j0 * nnf], ei = md.expar_nn[i0 * nnf];
-                double2 bj = cadd(cmul(ej, gcf(G, N, j0, jnb)), cmul(cconj(ej), gcf(G, N, jnb, j0)));
-                double2 bi = cadd(cmul(ei, gcf(G, N, i0, inb)), cmul(cconj(ei), gcf(G, N, inb, i0)));
+                double2 gnn_b = (jnb == jnj && inb == inj) ? gnn_j : gf(G, N, inb, jnb);
+                double2 gcnn_b = (jnb == jnj && inb == inj) ? gcnn_j : gcf(G, N, inb, jnb);
                 double2 x = cmul(cmul(ei, ej), cmul(gcf(G, N, i0, jnb), gf(G, N, inb, j0)));
                 x = cadd(x, cmul(cmul(cconj(ei), cconj(ej)), cmul(gcf(G, N, inb, j0), gf(G, N, i0, jnb))));
-                x = cadd(x, cmul(cmul(ei, cconj(ej)), cmul(gcf(G, N, i0, j0), gf(G, N, inb, jnb))));
-                x = cadd(x, cmul(cmul(cconj(ei), ej), cmul(gcf(G, N, inb, jnb), gf(G, N, i0, j0))));
-                sb = cadd(sb, cadd(cmul(bj, bi), cscale(x, fn)));
-                sn = cfma(gf(G, N, i0, j0), gf(G, N, inb, jnb), sn);
-                ss = cfma(gf(G, N, i0, j0), gf(G, N, ins, jns), ss);
+                x = cadd(x, cmul(cmul(ei, cconj(ej)), cmul(gc00, gnn_b)));
+                x = cadd(x, cmul(cmul(cconj(ei), ej), cmul(gcnn_b, g00)));
+                sb = cadd(sb, cadd(cmul(bcell[cj], bcell[ci]), cscale(x, fn)));
+                // pair correlations (measure_paircorr)
+                sn = cfma(g00, gnn_b, sn);
+                ss = cfma(g00, gf(G, N, ps[ci], ps[cj]), ss);
             }
             sj.x = warp_sum(sj.x); sj.y = warp_sum(sj.y); sb.x = warp_sum(sb.x); sb.y = warp_sum(sb.y);
             sn.x = warp_sum(sn.x); sn.y = warp_sum(sn.y); ss.x = warp_sum(ss.x); ss.y = warp_sum(ss.y);

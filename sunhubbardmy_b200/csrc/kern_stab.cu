@@ -367,7 +367,7 @@ void launch_stack_identity(const ChainDev* chains, int nchains, int slot, cudaSt
 void launch_zgemm_test(const ChainDev* chains, int nchains, int m, int n, int k, int opa, int opb,
                        int a_id, int b_id, int c_id, double beta_re, cudaStream_t st) {
     stab_attrs();
-    dim3 grid(4, nchains);
+    dim3 grid(1, nchains);   // one CTA per chain, as in the stabilisation kernels
     k_zgemm_test<<<grid, 256, GemmBig::SMEM_ELEMS * sizeof(double2), st>>>(chains, m, n, k, opa, opb, a_id, b_id, c_id, beta_re);
 }
 
