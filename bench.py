@@ -36,6 +36,12 @@ CONFIG = dict(lattice=1, l1=16, l2=16, beta=10.0, dtau=0.05, rhub=4.0, nflr=2, m
               kinetic=1, update=1, hs=1, nwrap=10, nublock=32)
 WORKLOAD = "square L=16 (N=256) SU(2) Hubbard U=4 beta=10 dtau=0.05 (ltrot=200) FFT kinetic, delay nublock=32, general 4-comp HS, nwrap=10"
 METRIC = "HS site-slice updates/s"
+# batched configuration: SU(4) Hubbard, honeycomb L = 6/9/12 (N = 72/162/288,
+# 48/48/32 chains), U = 6, beta = 8, dtau = 0.1, exact 4-component HS,
+# submatrix update with the flush depth autotuned over {16, 32, 64}
+CONFIG3 = [(dict(lattice=2, l1=L, l2=L, beta=8.0, dtau=0.1, rhub=6.0, nflr=4, kinetic=0, update=2, hs=0,
+                 nwrap=10, nublock=32), n) for L, n in ((6, 48), (9, 48), (12, 32))]
+WORKLOAD3 = "honeycomb L=6/9/12 (N=72/162/288, 48/48/32 chains) SU(4) Hubbard U=6 beta=8 dtau=0.1 (ltrot=80), exact HS, submatrix, autotuned flush depth"
 
 
 def test_seed(irank: int) -> int:
@@ -176,10 +182,21 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    C = args.chains
-    p = sb.DqmcParams.make(**CONFIG)
-    N, lt = p.ndim, p.ltrot
-    g = sb.Dqmc(p, n_chains=C, seeds=[test_seed(rank * C + c) for c in range(C)])
+    tune_report = None
+    if args.workload == "config3":
+        from sunhubbardmy_b200.autotune import batched
+        groups = [(sb.DqmcParams.make(**kw), n) for kw, n in CONFIG3]
+        g, tune_report = batched(groups, tune=True, seed0=rank * sum(n for _, n in CONFIG3))
+        workload = WORKLOAD3
+    else:
+        p0 = sb.DqmcParams.make(**CONFIG)
+        g = sb.Dqmc(p0, n_chains=args.chains, seeds=[test_seed(rank * args.chains + c) for c in range(args.chains)])
+        workload = WORKLOAD
+    C = g.n_chains
+    p = g.params[0]
+    lt = p.ltrot
+    Ns = np.array([g.ndim(c) for c in range(C)], dtype=np.float64)
+    N = int(Ns.max())
     g.sweep_start()
     g.obser_init()
     g.sweeps(max(args.warmup, 1), True)
@@ -198,7 +215,7 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
     if dist is not None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms = float(t.item())
-    per_step = world * C * 2 * lt * N
+    per_step = world * int(2 * lt * Ns.sum())
     value = per_step / (ms * 1e-3)
     kernels_per_sweep = g.sweep_kernels()
     d0 = g.diag(0)
@@ -207,10 +224,10 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
 
     # end to end through the public API with host buffers: h2d of every chain's
     # HS field, sweep_start + one sweep, d2h of every chain's bins and field
-    nconf = C * lt * N
+    nconf = int(lt * Ns.sum())
     conf_host = torch.empty(nconf, dtype=torch.int32, pin_memory=True).numpy()
     g.conf_all(conf_host)
-    nbins = len(g.bins_raw(0))
+    nbins = sum(len(g.bins_raw(c)) for c in range(C)) / C
     e2e_steps = max(1, min(args.steps, 2))
     barrier()
     t0 = time.perf_counter()
@@ -238,23 +255,22 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
         share = {k: ops[k] * per_sweep[k] for k in ops}
         total = sum(share.values())
         dom = max(share, key=share.get)
-        N3 = float(N) ** 3
+        N3 = float((Ns ** 3).sum())        # sum over chains
         flops = {1: 18.0 + 2.0 / 3.0, 2: 41.0 + 1.0 / 3.0}   # real flops / N^3 per chain
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
         fp64 = fp64_peak_tflops()
         if dom in flops:
-            ach = C * flops[dom] * N3 / (ops[dom] * 1e-3) / 1e12
+            ach = flops[dom] * N3 / (ops[dom] * 1e-3) / 1e12
             roof = {"kernel": names[dom], "bound": "tensor", "achieved": ach, "peak": fp64, "unit": "TFLOP/s",
                     "frac": ach / fp64, "traffic": None,
                     "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (FP64 tensor)"}
         elif dom in (3, 5):
-            ach = C * 32.0 * N * N / (ops[dom] * 1e-3) / 1e9
+            ach = 32.0 * float((Ns ** 2).sum()) / (ops[dom] * 1e-3) / 1e9
             pk = peaks.get("hbm_gbs", 6650.0)
             roof = {"kernel": names[dom], "bound": "hbm", "achieved": ach, "peak": pk, "unit": "GB/s",
                     "frac": ach / pk, "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
         else:
-            acc_n = acc * N
-            ach = C * 8.0 * N * N * acc_n / (ops[dom] * 1e-3) / 1e12
+            ach = 8.0 * acc * float((Ns ** 3).sum()) / (ops[dom] * 1e-3) / 1e12
             roof = {"kernel": names[dom], "bound": "tensor", "achieved": ach, "peak": fp64, "unit": "TFLOP/s",
                     "frac": ach / fp64, "traffic": None,
                     "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (FP64 tensor)"}
@@ -271,18 +287,38 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128",
             "data": "synthetic (HS field drawn from the reference's -DTEST seeds, one per chain)",
-            "config": {"workload": WORKLOAD, "chains_per_gpu": C, "parallelism": f"replicas x{world}",
+            "config": {"workload": workload, "chains_per_gpu": C, "parallelism": f"replicas x{world}",
                        "l2": "working set ~52 MiB/chain >> L2 (no flush needed)",
                        "acceptance": acc, "max_wrap_error": wrap},
             "e2e": {"value": per_step / e2e_s, "unit": "updates/s",
                     "h2d_bytes_per_step": nconf * 4,
-                    "d2h_bytes_per_step": C * nbins * 16 + nconf * 4,
+                    "d2h_bytes_per_step": int(C * nbins * 16 + nconf * 4),
                     "note": "per step: set_conf_all (pinned host) + sweep_start + 1 sweep + get_bins + get_conf_all"},
             "gpu_launches": kernels_per_sweep * args.steps,
             "roofline": roof,
             "clocks": clk.summary(),
         }
-        if world == 1 and not args.no_cpu:
+        if tune_report is not None:
+            result["config"]["autotune"] = {str(k): v for k, v in tune_report.items()}
+        if args.ess > 0:
+            from sunhubbardmy_b200.stats import double_occupancy, ess
+            series = []
+            g.sweeps(args.ess_warmup, False)     # equilibrate before the series
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(args.ess):
+                g.obser_init()
+                g.sweeps(1, True)
+                series.append(double_occupancy(g.energy_all(), Ns))
+            wall = time.perf_counter() - t0
+            x = np.array(series).T            # [chain, sweep]
+            n_ess, tau = ess(x)
+            result["ess"] = {"observable": "double occupancy (per-sweep, per chain)", "sweeps": args.ess,
+                             "warmup_sweeps": args.ess_warmup + args.warmup + args.steps,
+                             "chains": C, "tau_int_sweeps": tau, "ess": n_ess, "ess_per_s": n_ess / wall,
+                             "mean": float(x.mean()), "stderr": float(x.std(ddof=1) / np.sqrt(n_ess)),
+                             "wall_s": wall}
+        if world == 1 and not args.no_cpu and args.workload == "config2":
             per, times, _ = cpu_sample(20, os.cpu_count() or 1, steps=1)
             cv = per / times[0]
             result["cpu_baseline"] = {"value": cv, "unit": "updates/s", "cores": os.cpu_count() or 1, "kind": "port",
@@ -303,6 +339,9 @@ def main():
     ap.add_argument("--chains", type=int, default=296)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--workload", default="config2", choices=["config2", "config3"])
+    ap.add_argument("--ess", type=int, default=0, help="extra sweeps for the ESS/s of double occupancy")
+    ap.add_argument("--ess-warmup", type=int, default=20, help="equilibration sweeps before the ESS series")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

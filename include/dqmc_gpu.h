@@ -76,13 +76,22 @@ typedef struct dqmc_diag {
 
 typedef struct dqmc_handle dqmc_handle;
 
+/* Host-only: the lattice and kinetic tables the library builds for p, in the
+ * reference's 1-based conventions (src/lattice.f90, dqmc_set_h0conf.f90):
+ * nnlist[ndim][nn_nf], nnlf_list[nn_lf], list[ndim][2], imj[lq][lq],
+ * plq_cord[lq][z_plq], snlist[ndim][4 or 6], urt[nn_nf*nn_lf][2][2] complex,
+ * exph0k[lq] complex (FFT only).  Any pointer may be NULL.  Needs no GPU. */
+int dqmc_model_tables(const dqmc_params* p, int32_t* nnlist, int32_t* nnlf_list, int32_t* list,
+                      int32_t* imj, int32_t* plq_cord, int32_t* snlist, double* urt, double* exph0k);
+
 /* Derive ndim, lq, ltrot, nst, ne, lcomp and the default nublock exactly as
  * make_tables does (src/model_para.f90:334-453). */
 int dqmc_params_derive(dqmc_params* p);
 
 /* Create n_chains chains on the current CUDA device.  params points to
  * n_params parameter sets; chain c uses params[c % n_params] (all sets must
- * share beta, dtau and nwrap).  seeds[c] seeds chain c's SFMT generator
+ * share beta, dtau and nwrap; lattice sizes may differ, and identical sets
+ * share one copy of the model tables).  seeds[c] seeds chain c's SFMT generator
  * (spring_sfmt_init, lib/m_spring.f90:187); if draw_conf is nonzero the HS
  * field is drawn from it as dqmc_input_conf does for a fresh start
  * (src/dqmc_config_u/dqmc_input_conf.f90:55-63).  Replaces dqmc_start's
@@ -123,6 +132,9 @@ int dqmc_gpu_obser_init(dqmc_handle* h);
 int dqmc_gpu_nbins(dqmc_handle* h, int chain);
 int dqmc_gpu_get_bins(dqmc_handle* h, int chain, double* out);
 int dqmc_gpu_get_diag(dqmc_handle* h, int chain, dqmc_diag* out);
+/* energy_bin(1:10) of every chain (10 complex per chain, chain after chain):
+ * the per-sweep series of sign, density, energies and double occupancy. */
+int dqmc_gpu_get_energy_all(dqmc_handle* h, double* out);
 int dqmc_gpu_reset_diag(dqmc_handle* h);
 
 /* Operator-level entry points of the reference's type-bound procedures

@@ -480,6 +480,28 @@ struct HostSfmt {
     double stream() { return ((double)next() + 0.5) * (1.0 / 4294967296.0); }
 };
 
+// host-only view of the model tables (no device needed)
+extern "C" int dqmc_model_tables(const dqmc_params* pin, int32_t* nnlist, int32_t* nnlf_list, int32_t* list,
+                                 int32_t* imj, int32_t* plq_cord, int32_t* snlist, double* urt, double* exph0k) {
+    if (!pin) return fail(DQMC_EINVAL, "null params");
+    HostModel m;
+    m.p = *pin;
+    int rc = dqmc_params_derive(&m.p);
+    if (rc) return rc;
+    if ((rc = build_model(m))) return rc;
+    int N = m.N, lq = m.lq;
+    if (nnlist) for (int i = 0; i < N * m.nn_nf; ++i) nnlist[i] = m.nnlist[i] + 1;
+    if (nnlf_list) for (int i = 0; i < m.nn_lf; ++i) nnlf_list[i] = m.nnlf[i] + 1;
+    if (list) for (int i = 0; i < N; ++i) { list[2 * i] = i / m.nsub + 1; list[2 * i + 1] = i % m.nsub + 1; }
+    if (imj) for (int i = 0; i < lq * lq; ++i) imj[i] = m.imj[i] + 1;
+    if (plq_cord) for (int i = 0; i < lq * m.z_plq; ++i) plq_cord[i] = m.plq[i] + 1;
+    if (snlist) for (int i = 0; i < N * m.nsn; ++i) snlist[i] = m.snlist[i] + 1;
+    if (urt) memcpy(urt, m.urt.data(), m.urt.size() * sizeof(zc));
+    if (exph0k && !m.exph0k.empty())
+        for (int k = 0; k < lq; ++k) { exph0k[2 * k] = m.exph0k[k].real() * lq; exph0k[2 * k + 1] = m.exph0k[k].imag() * lq; }
+    return DQMC_OK;
+}
+
 // ---------------------------------------------------------------------------
 // handle
 // ---------------------------------------------------------------------------
@@ -534,16 +556,27 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
     dqmc_handle* h = new dqmc_handle();
     *out = nullptr;
     int rc;
+    std::vector<int> model_of(n_params);
     for (int k = 0; k < n_params; ++k) {
+        // identical parameter sets share one model (tables uploaded once)
+        int same = -1;
+        for (int q = 0; q < k && same < 0; ++q)
+            if (memcmp(&params[q], &params[k], sizeof(dqmc_params)) == 0) same = model_of[q];
+        if (same >= 0) { model_of[k] = same; continue; }
+        model_of[k] = (int)h->models.size();
         HostModel* m = new HostModel();
         m->p = params[k];
         if ((rc = dqmc_params_derive(&m->p))) { delete m; dqmc_gpu_destroy(h); return rc; }
         if ((rc = build_model(*m))) { delete m; dqmc_gpu_destroy(h); return rc; }
         h->models.push_back(m);
-        if (k == 0) { h->ltrot = m->p.ltrot; h->nst = m->p.nst; h->nwrap = m->p.nwrap; }
+        if (h->models.size() == 1) { h->ltrot = m->p.ltrot; h->nst = m->p.nst; h->nwrap = m->p.nwrap; }
         else if (m->p.ltrot != h->ltrot || m->p.nst != h->nst || m->p.nwrap != h->nwrap) {
             dqmc_gpu_destroy(h);
             return fail(DQMC_EINVAL, "all parameter sets of a handle must share ltrot and nwrap");
+        } else if (m->p.lattice != h->models[0]->p.lattice || m->p.kinetic != h->models[0]->p.kinetic ||
+                   (m->p.rt == 0.0) != (h->models[0]->p.rt == 0.0) || (m->p.rhub == 0.0) != (h->models[0]->p.rhub == 0.0)) {
+            dqmc_gpu_destroy(h);
+            return fail(DQMC_EINVAL, "all parameter sets of a handle must share lattice kind and kinetic propagator");
         }
         if ((rc = upload_model(*m))) { dqmc_gpu_destroy(h); return rc; }
         h->maxN = std::max(h->maxN, m->N);
@@ -562,9 +595,9 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
     }
     h->chains.resize(n_chains);
     for (int c = 0; c < n_chains; ++c) {
-        HostModel* m = h->models[c % n_params];
+        HostModel* m = h->models[model_of[c % n_params]];
         ChainHost& ch = h->chains[c];
-        ch.model = c % n_params;
+        ch.model = model_of[c % n_params];
         ChainDev& d = ch.dev;
         memset(&d, 0, sizeof(d));
         int N = m->N;
@@ -955,6 +988,14 @@ extern "C" int dqmc_gpu_get_bins(dqmc_handle* h, int chain, double* out) {
     int rc = chk_chain(h, chain); if (rc) return rc;
     int nb = dqmc_gpu_nbins(h, chain);
     CK(cudaMemcpy(out, h->chains[chain].dev.bins, (size_t)nb * sizeof(double2), cudaMemcpyDeviceToHost));
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_get_energy_all(dqmc_handle* h, double* out) {
+    if (!h || !out) return fail(DQMC_EINVAL, "invalid arguments");
+    for (int c = 0; c < h->nch; ++c)
+        CK(cudaMemcpyAsync(out + 20 * (size_t)c, h->chains[c].dev.bins, 10 * sizeof(double2), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
     return DQMC_OK;
 }
 

@@ -223,7 +223,9 @@ __global__ void __launch_bounds__(256) k_measure(const ChainDev* __restrict__ ch
 
 __global__ void k_bins_clear(const ChainDev* __restrict__ chains, int nbins) {
     const ChainDev c = chains[blockIdx.x];
-    for (int e = threadIdx.x; e < nbins; e += blockDim.x) c.bins[e] = cmk(0, 0);
+    (void)nbins;
+    const int nb = 10 + 20 * c.md->lq + 4;     // this chain's own bin count
+    for (int e = threadIdx.x; e < nb; e += blockDim.x) c.bins[e] = cmk(0, 0);
     if (threadIdx.x == 0) c.stats[ST_NOBS] = 0.0;
 }
 

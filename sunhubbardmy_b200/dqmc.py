@@ -59,6 +59,22 @@ class DqmcParams(C.Structure):
             raise DqmcError(f"dqmc_params_derive: {_last_error()}")
         return p
 
+    def tables(self) -> dict:
+        """Lattice / kinetic tables built by the library (1-based, host only)."""
+        N, lq = self.ndim, self.lq
+        hc = self.lattice == HONEYCOMB
+        nnf, z, nsn = (3, 6, 6) if hc else (4, 4, 4)
+        nlf = lq if hc else lq // 2
+        t = dict(nnlist=np.zeros((N, nnf), np.int32), nnlf_list=np.zeros(nlf, np.int32),
+                 list=np.zeros((N, 2), np.int32), imj=np.zeros((lq, lq), np.int32),
+                 plq_cord=np.zeros((lq, z), np.int32), snlist=np.zeros((N, nsn), np.int32),
+                 urt=np.zeros((nnf * nlf, 2, 2), complex), exph0k=np.zeros(lq, complex))
+        rc = load_library().dqmc_model_tables(C.byref(self), *[_ptr(t[k]) for k in
+                                              ("nnlist", "nnlf_list", "list", "imj", "plq_cord", "snlist", "urt", "exph0k")])
+        if rc != 0:
+            raise DqmcError(f"dqmc_model_tables: {_last_error()}")
+        return t
+
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
 
@@ -75,6 +91,7 @@ _lib = None
 _vp, _i, _d = C.c_void_p, C.c_int, C.c_double
 SIGNATURES = {
     "dqmc_params_derive": (_i, [_vp]),
+    "dqmc_model_tables": (_i, [_vp] * 9),
     "dqmc_gpu_create": (_i, [_vp, _i, _i, _vp, _i, C.POINTER(_vp)]),
     "dqmc_gpu_destroy": (_i, [_vp]),
     "dqmc_gpu_last_error": (C.c_char_p, []),
@@ -92,6 +109,7 @@ SIGNATURES = {
     "dqmc_gpu_nbins": (_i, [_vp, _i]),
     "dqmc_gpu_get_bins": (_i, [_vp, _i, _vp]),
     "dqmc_gpu_get_diag": (_i, [_vp, _i, _vp]),
+    "dqmc_gpu_get_energy_all": (_i, [_vp, _vp]),
     "dqmc_gpu_reset_diag": (_i, [_vp]),
     "dqmc_gpu_h0_prop": (_i, [_vp, _i, _i]),
     "dqmc_gpu_u_prop": (_i, [_vp, _i, _i]),
@@ -295,6 +313,12 @@ class Dqmc:
                     avglog10error=d.avglog10error_sum, logcount=d.logcount,
                     avgexpphasediff=d.avgexpphasediff_sum, accepted=d.accepted, proposed=d.proposed,
                     nobs=d.nobs)
+
+    def energy_all(self) -> np.ndarray:
+        """energy_bin(1:10) of every chain, shape (n_chains, 10) complex."""
+        out = np.zeros((self.n_chains, 10), complex)
+        _check(load_library().dqmc_gpu_get_energy_all(self.h, _ptr(out)), "get_energy_all")
+        return out
 
     def reset_diag(self) -> None:
         _check(load_library().dqmc_gpu_reset_diag(self.h), "reset_diag")

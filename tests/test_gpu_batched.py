@@ -1,0 +1,66 @@
+"""Batched chains of uneven lattice sizes in one handle (one CTA per chain),
+each chain checked against its own oracle chain: identical HS fields and
+accept counts, Green's functions within 1e-10, energy bins within 1e-8."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GROUPS = {
+    "honeycomb_su4_L2_L3": [
+        (dict(lattice=2, l1=2, l2=2, beta=1.6, dtau=0.1, rhub=6.0, nflr=4, kinetic=0, update=2, hs=0, nwrap=8, nublock=16), 3),
+        (dict(lattice=2, l1=3, l2=3, beta=1.6, dtau=0.1, rhub=6.0, nflr=4, kinetic=0, update=2, hs=0, nwrap=8, nublock=32), 2),
+    ],
+    "square_fft_L4_L6": [
+        (dict(lattice=1, l1=4, l2=4, beta=1.0, dtau=0.05, rhub=4.0, nflr=2, kinetic=1, update=1, hs=1, nwrap=10, nublock=8), 2),
+        (dict(lattice=1, l1=6, l2=6, beta=1.0, dtau=0.05, rhub=4.0, nflr=2, kinetic=1, update=1, hs=1, nwrap=10, nublock=16), 2),
+    ],
+}
+
+
+@pytest.mark.parametrize("name", list(GROUPS))
+def test_mixed_sizes_match_oracle(oracle, name):
+    import sunhubbardmy_b200 as sb
+    plist, kws = [], []
+    for kw, n in GROUPS[name]:
+        plist += [sb.DqmcParams.make(**kw)] * n
+        kws += [kw] * n
+    nch = len(plist)
+    g = sb.Dqmc(plist, n_chains=nch, seeds=[sb.test_seed(c) for c in range(nch)])
+    models = {}
+    chains = []
+    for c, kw in enumerate(kws):
+        key = tuple(sorted(kw.items()))
+        if key not in models:
+            models[key] = oracle.Model(**kw)
+        chains.append(oracle.Chain(models[key], sb.test_seed(c)))
+    g.sweep_start(); g.obser_init()
+    for ch in chains:
+        ch.sweep_start(); ch.obser_init()
+    g.sweeps(1, True)
+    for ch in chains:
+        ch.sweep_b0(); ch.sweep_0b()
+    for c, ch in enumerate(chains):
+        assert g.ndim(c) == ch.model.ndim
+        assert np.array_equal(g.conf(c), ch.conf()), c
+        assert np.max(np.abs(g.green(c) - ch.green())) < 1e-10
+        dg, dc = g.diag(c), ch.diag()
+        assert dg["accepted"] == dc["accepted"]
+        eg, ec = g.bins(c)["energy"], ch.bins()["energy"]
+        assert np.max(np.abs(eg - ec)) < 1e-8 * max(1.0, np.max(np.abs(ec)))
+
+
+def test_autotuner_keeps_results(oracle):
+    """The tuned flush depth changes only the speed: the tuned handle's chains
+    still reproduce the oracle."""
+    import sunhubbardmy_b200 as sb
+    from sunhubbardmy_b200.autotune import batched
+    kw = dict(lattice=2, l1=3, l2=3, beta=1.6, dtau=0.1, rhub=6.0, nflr=4, kinetic=0, update=2, hs=0, nwrap=8, nublock=32)
+    g, report = batched([(sb.DqmcParams.make(**kw), 2)], candidates=(8, 16), tune_chains=2)
+    assert report[18]["nublock"] in (8, 16)
+    m = oracle.Model(**kw)
+    ch = oracle.Chain(m, sb.test_seed(0))
+    g.sweep_start(); ch.sweep_start()
+    g.sweep_b0(); g.sweep_0b(); ch.sweep_b0(); ch.sweep_0b()
+    assert np.array_equal(g.conf(0), ch.conf())
+    assert np.max(np.abs(g.green(0) - ch.green())) < 1e-10
