@@ -57,6 +57,9 @@ typedef struct dqmc_params {
     int32_t nflr, lproju, lstabilize;
     int32_t nwrap, nsweep, nbin, nublock;
     int32_t update, kinetic, hs;
+    /* projective run (dqmc_proj_ctrl instead of dqmc_ft_ctrl), lprojv of
+     * &model_para and obs_eqt_mid_len of &ctrl_para (0 = default 1) */
+    int32_t proj, lprojv, obs_mid_len;
     /* derived (src/model_para.f90:334-453) */
     int32_t ndim, lq, ltrot, nst, ne, lcomp;
 } dqmc_params;
@@ -70,8 +73,9 @@ typedef struct dqmc_diag {
     double avglog10error_sum;           /* sum of log10(wrap error) */
     double logcount;                    /* number of wrap checks */
     double avgexpphasediff_sum;
-    double accepted, proposed;          /* main_obs(3) */
+    double accepted, proposed;          /* main_obs(3): site (U) field */
     double nobs;                        /* measurements in the current bin */
+    double accepted_v, proposed_v;      /* main_obs(4): bond (t-V) field */
 } dqmc_diag;
 
 typedef struct dqmc_handle dqmc_handle;
@@ -174,6 +178,48 @@ int dqmc_gpu_sweep_kernels(dqmc_handle* h);
  * 3 kinetic + HS column pass, 4 equal-time measurement, 5 row pass.  Modifies
  * chain state; intended for benchmarks after the timed sweeps. */
 int dqmc_gpu_time_op(dqmc_handle* h, int op, int reps, double* ms_out);
+
+/* ---------------------------------------------------------------------------
+ * Projective (ground-state) path, params.proj = 1 (src/dqmc_proj_ctrl.f90,
+ * src/dqmc_proj_core/).  A walker holds UR = B(tau,0) P (ndim x ne),
+ * UL = P^H B(beta,tau) (ne x ndim), (UL UR)^-1 and the stack Ust(0:nst).
+ * dqmc_gpu_create draws, per walker and in the reference's order, the U field
+ * (if rhub != 0), the t-V bond field (if rv != 0;
+ * src/dqmc_config_v/dqmc_input_conf.f90:55-63) and the nn_lf*nn_nf hopping
+ * perturbations of set_trial_h0 (src/dqmc_config_h0/set_trial_h0.f90), and
+ * takes the ne lowest eigenvectors of that trial Hamiltonian as projL = projR
+ * (dqmc_set_proj, src/dqmc_proj_core/dqmc_set_proj.f90:1-78).
+ * dqmc_gpu_sweep_start / _sweep_b0 / _sweep_0b / _sweeps then run
+ * dqmc_proj_sweep_start_0b / dqmc_proj_sweep_b0 / dqmc_proj_sweep_0b, with the
+ * equal-time measurement on the obs_eqt_mid_len middle slices.
+ * --------------------------------------------------------------------------- */
+
+/* t-V bond field vconf%conf(nsites, nn_nf, ltrot) of one walker: int32
+ * [ltrot][nn_nf][ndim], values 1..2; entries with bond index >= nn_lf are kept
+ * but unused, as in the reference. */
+int dqmc_gpu_set_vconf(dqmc_handle* h, int chain, const int32_t* vconf);
+int dqmc_gpu_get_vconf(dqmc_handle* h, int chain, int32_t* vconf);
+/* trial state of one walker: proj (ndim x ndim complex, ascending eigenvectors
+ * of the trial Hamiltonian, first ne columns used), w (ndim eigenvalues; may be
+ * NULL).  set_trial replaces projL = projR (e.g. with a caller's eigenvectors). */
+int dqmc_gpu_get_trial(dqmc_handle* h, int chain, double* proj, double* w);
+int dqmc_gpu_set_trial(dqmc_handle* h, int chain, const double* proj);
+/* UR (ndim x ne), UL (ne x ndim) and ULRINV (ne x ne) of one walker, column-major
+ * complex; any pointer may be NULL. */
+int dqmc_gpu_get_proj(dqmc_handle* h, int chain, double* ur, double* ul, double* ulrinv);
+int dqmc_gpu_set_proj(dqmc_handle* h, int chain, const double* ur, const double* ul, const double* ulrinv);
+/* proj_update(nt, nf, UL, UR, ULRINV) of every walker (nf = 1..nn_nf: bond
+ * family of vconf; nf = 0: the U field of uconf), consuming two draws per bond
+ * or site (src/dqmc_config_v/dqmc_proj_update_submatrix_LR.f90,
+ * src/dqmc_config_u/dqmc_proj_update_submatrix_LR.f90). */
+int dqmc_gpu_proj_update(dqmc_handle* h, int nt, int nf);
+/* green_equaltime of the projective core (src/dqmc_proj_core/green_equaltime.f90)
+ * after a fresh ULRINV = (UL UR)^-1, into each walker's G. */
+int dqmc_gpu_proj_green(dqmc_handle* h);
+/* Host-only: the trial state dqmc_gpu_create computes for a walker seeded
+ * with `seed` (draws the fields first when draw_conf is nonzero, as create
+ * does).  proj: ndim x ndim complex; w: ndim.  Needs no GPU. */
+int dqmc_trial_state(const dqmc_params* p, int32_t seed, int draw_conf, double* proj, double* w);
 
 /* Allocation-free QR factorisation with log det Q.  No counterpart in the
  * reference: it is an extra entry point for host codes that cannot allocate

@@ -52,6 +52,8 @@ typedef struct {
     int32_t nflr, lproju, lstabilize;
     int32_t nwrap, nsweep, nbin, nublock;
     int32_t update, kinetic, hs;
+    /* projective run (dqmc_proj_ctrl), lprojv and obs_eqt_mid_len of &ctrl_para */
+    int32_t proj, lprojv, obs_mid_len;
 } orc_params;
 
 typedef struct orc_model orc_model;
@@ -69,6 +71,9 @@ typedef void (*orc_zungqr_fn)(const int*, const int*, const int*, void*, const i
 typedef void (*orc_zgetrf_fn)(const int*, const int*, void*, const int*, int*, int*);
 typedef void (*orc_ztrtri_fn)(const char*, const char*, const int*, void*, const int*, int*);
 void orc_set_lapack(orc_zgemm_fn, orc_zgeqrf_fn, orc_zgeqp3_fn, orc_zungqr_fn, orc_zgetrf_fn, orc_ztrtri_fn);
+typedef void (*orc_zheev_fn)(const char*, const char*, const int*, void*, const int*, double*, void*,
+                             const int*, double*, int*);
+void orc_set_zheev(orc_zheev_fn);
 
 /* ---------- model / chain ---------- */
 orc_model *orc_model_new(const orc_params *p);
@@ -95,7 +100,8 @@ void orc_chain_set_green(orc_chain *c, const double *g);
 void orc_chain_get_green(const orc_chain *c, double *g);
 void orc_chain_set_phase(orc_chain *c, double re, double im);
 /* diag: [0]=phase.re [1]=phase.im [2]=logw.re [3]=logw.im [4]=max_wrap_error
- * [5]=max_phasediff [6]=avglog10error [7]=logcount [8]=accepted [9]=proposed */
+ * [5]=max_phasediff [6]=avglog10error [7]=logcount [8]=accepted [9]=proposed
+ * [10]=accepted bond-field [11]=proposed bond-field */
 void orc_chain_get_diag(const orc_chain *c, double *out);
 double orc_chain_uniform(orc_chain *c);
 
@@ -131,6 +137,28 @@ int  orc_green_equaltime(int n, const double *ur, const double *dr, const double
 /* bins: energy[20] (10 complex), nobs, then the per-array bins */
 int  orc_bins_size(const orc_model *m);
 void orc_get_bins(const orc_chain *c, double *out);
+
+/* ---------- projective path (src/dqmc_proj_core/ directory) ----------
+ * The chain of a model with proj = 1 holds UR (N x ne), UL (ne x N), (UL UR)^-1
+ * and the stack Ust(0:nst) of N x ne matrices; the t-V bond field (rv != 0)
+ * is int32 [ltrot][nn_nf][nsites], values 1..2. */
+int  orc_proj_sweep_start_0b(orc_chain *c);
+int  orc_proj_sweep_b0(orc_chain *c, int lupdate, int lmeasure);
+int  orc_proj_sweep_0b(orc_chain *c, int lupdate, int lmeasure);
+/* trial state: proj (N x N, ascending eigenvectors of set_trial_h0) and its eigenvalues */
+void orc_proj_get_trial(const orc_chain *c, double *proj, double *w);
+void orc_proj_set_trial(orc_chain *c, const double *proj);
+void orc_proj_get(const orc_chain *c, double *ur, double *ul, double *ulrinv);
+void orc_proj_set(orc_chain *c, const double *ur, const double *ul, const double *ulrinv);
+void orc_proj_green(orc_chain *c);                  /* gf from UR, UL, ULRINV */
+void orc_vconf_get(const orc_chain *c, int32_t *v);
+void orc_vconf_set(orc_chain *c, const int32_t *v);
+/* one projective update of slice nt (family nf for the bond field, nf = 0 for the site field) */
+void orc_proj_update(orc_chain *c, int nt, int nf);
+/* vconf props on an explicit matrix: left ops on N x n2, right ops on n2 x N */
+void orc_vconf_prop(const orc_model *m, const int32_t *vconf, int op, int nt, int nf, int nflag, double *g, int n2);
+double orc_qr_pqmc_d(int rdim, int cdim, const double *a, double *q);
+void orc_eig_he_d(int n, const double *h, double *w, double *v);
 
 /* linear-algebra restatements exposed for pinning against LAPACK */
 void   orc_zgeqr2(int m, int n, double *a, int lda, double *tau);

@@ -249,6 +249,9 @@ orc_model *orc_model_new(const orc_params *pin) {
     }
     set_hs(m);
     set_h0(m);
+    m->proj = p->proj != 0;
+    m->obs_mid_len = p->obs_mid_len > 0 ? p->obs_mid_len : 1;
+    orc_set_vconf(m);
     return m;
 }
 
@@ -310,7 +313,7 @@ orc_chain *orc_chain_new(const orc_model *m, int32_t seed, int draw_conf) {
     int N = m->ndim, lt = m->ltrot, nst = m->nst, lq = m->lq;
     orc_sfmt_init(&c->rng, seed);
     c->conf = calloc((size_t)N * lt, sizeof(int32_t));
-    if (draw_conf) {  /* dqmc_input_conf.f90:55-63: nt outer, site inner */
+    if (draw_conf && m->lwrapu) {  /* dqmc_input_conf.f90:55-63: nt outer, site inner */
         for (int nt = 0; nt < lt; ++nt)
             for (int i = 0; i < N; ++i)
                 c->conf[nt * N + i] = (int32_t)ceil(orc_sfmt_stream(&c->rng) * m->lcomp);
@@ -333,6 +336,7 @@ orc_chain *orc_chain_new(const orc_model *m, int32_t seed, int draw_conf) {
     c->znn_bin = zalloc(lq * 4); c->pair_onsite_bin = zalloc(lq * 4);
     c->zjj_bin = zalloc(lq); c->zbb_bin = zalloc(lq);
     c->pair_nn_bin = zalloc(lq); c->pair_sn_bin = zalloc(lq);
+    orc_proj_chain_init(c, draw_conf);
     return c;
 }
 
@@ -343,6 +347,7 @@ void orc_chain_free(orc_chain *c) {
     free(c->conf); free(c->gf); free(c->gfc);
     free(c->zcpcm_bin); free(c->zspsm_bin); free(c->znn_bin); free(c->pair_onsite_bin);
     free(c->zjj_bin); free(c->zbb_bin); free(c->pair_nn_bin); free(c->pair_sn_bin);
+    orc_proj_chain_free(c);
     free(c);
 }
 
@@ -367,6 +372,7 @@ void orc_chain_get_diag(const orc_chain *c, double *out) {
     out[4] = c->max_wrap_error; out[5] = c->max_phasediff;
     out[6] = c->avglog10error; out[7] = c->logcount;
     out[8] = c->acc_u; out[9] = c->prop_u;
+    out[10] = c->acc_v; out[11] = c->prop_v;
 }
 
 /* ------------------------------------------------------------------ */
@@ -502,7 +508,7 @@ static zc zpow(zc z, int n) { zc r = 1; for (int i = 0; i < n; ++i) r *= z; retu
 
 /* ratio of the flip (is -> isp) given the fermion part ratio1;
  * dqmc_update.f90:52-60 */
-static zc total_ratio(const orc_model *m, zc ratio1, int is, int iflip, int isp) {
+zc orc_total_ratio(const orc_model *m, zc ratio1, int is, int iflip, int isp) {
     int lc = m->lcomp;
     zc r = zpow(ratio1, m->p.nflr);
     zc pr = m->phase_ratio[(is - 1) * (lc - 1) + (iflip - 1)];
@@ -528,7 +534,7 @@ static void update_fast(orc_chain *c, int nt, int32_t *acc) {
         zc dlt = m->delta[(is - 1) * (lc - 1) + (iflip - 1)];
         zc ratio1 = vk[is_] * dlt + 1.0;
         zc sscl = dlt / ratio1;
-        zc rt = total_ratio(m, ratio1, is, iflip, isp);
+        zc rt = orc_total_ratio(m, ratio1, is, iflip, isp);
         double rre = creal(rt * c->phase) / creal(c->phase);
         double rabs = rre < 0 ? -rre : rre;
         double rnd = orc_sfmt_stream(&c->rng);
@@ -565,7 +571,7 @@ static void update_delay(orc_chain *c, int nt, int32_t *acc) {
         zc dlt = m->delta[(is - 1) * (lc - 1) + (iflip - 1)];
         zc ratio1 = (1.0 - diag[s]) * dlt + 1.0;
         zc sscl = dlt / ratio1;
-        zc rt = total_ratio(m, ratio1, is, iflip, isp);
+        zc rt = orc_total_ratio(m, ratio1, is, iflip, isp);
         double rre = creal(rt * c->phase) / creal(c->phase);
         double rabs = rre < 0 ? -rre : rre;
         double rnd = orc_sfmt_stream(&c->rng);
@@ -635,7 +641,7 @@ static void update_submatrix(orc_chain *c, int nt, int32_t *acc) {
         zc v2 = v + g[ZIDX(s, s, N)] - 1.0;
         zc dlt = m->delta[(is - 1) * (lc - 1) + (iflip - 1)];
         zc ratio1 = -v2 * dlt + 1.0;
-        zc rt = total_ratio(m, ratio1, is, iflip, isp);
+        zc rt = orc_total_ratio(m, ratio1, is, iflip, isp);
         double rre = creal(rt * c->phase) / creal(c->phase);
         double rabs = rre < 0 ? -rre : rre;
         double rnd = orc_sfmt_stream(&c->rng);
@@ -885,7 +891,7 @@ static int green_equaltimebb(int N, const zc *ure, const double *dre, const zc *
 }
 
 /* set_phase (src/dqmc_ft_core/set_phase.f90:1-24) */
-static zc set_phase(const orc_chain *c, zc logw) {
+zc orc_set_phase(const orc_chain *c, zc logw) {
     const orc_model *m = c->m;
     zc ph = cexp(I * (m->p.nflr * cimag(logw)));
     if (m->lwrapu && m->p.rhub > 0.0) {
@@ -896,7 +902,7 @@ static zc set_phase(const orc_chain *c, zc logw) {
     return ph;
 }
 
-static double compare_max(int N, const zc *a, const zc *b) {   /* s_compare_max_z */
+double orc_compare_max(int N, const zc *a, const zc *b) {   /* s_compare_max_z */
     double mx = 0;
     for (size_t k = 0; k < (size_t)N * N; ++k) { double t = cabs(a[k] - b[k]); if (t > mx) mx = t; }
     return mx;
@@ -913,7 +919,7 @@ int orc_sweep_start_0b(orc_chain *c) {
         c->logdetQst[0] = 0;
         for (int n = 1; n <= m->nst; ++n) orc_stablize_0b(c, n);
         green_equaltimebb(N, c->Ust[m->nst], c->Dst[m->nst], c->Vst[m->nst], c->gf, c->logdetQst[m->nst], &c->logweightf);
-        c->phase = set_phase(c, c->logweightf);
+        c->phase = orc_set_phase(c, c->logweightf);
     } else {
         memset(c->gf, 0, sizeof(zc) * (size_t)N * N);
         for (int i = 0; i < N; ++i) c->gf[ZIDX(i, i, N)] = 1;
@@ -1128,9 +1134,9 @@ static void h0_half(orc_chain *c, int left_op, int right_op, int reversed) {
 
 static void record_wrap(orc_chain *c, const zc *gtmp, zc logw) {
     int N = c->m->ndim;
-    double err = compare_max(N, gtmp, c->gf);
+    double err = orc_compare_max(N, gtmp, c->gf);
     if (err > c->max_wrap_error) c->max_wrap_error = err;
-    zc ph = set_phase(c, logw);
+    zc ph = orc_set_phase(c, logw);
     double pd = cabs(c->phase - ph);
     if (pd > c->max_phasediff) c->max_phasediff = pd;
     c->logcount += 1.0;

@@ -50,6 +50,11 @@ struct orc_model {
     zc *tw1, *tw2;            /* DFT twiddles exp(-2 pi i k / l) */
     zc *h0mat;                /* [N*N] */
     zc *expar_nn;             /* [nsites][nn_nf] */
+    /* projective path and the t-V bond field (src/dqmc_config_v/dqmc_set_conf.f90) */
+    int proj, lwrapv, obs_mid_len;
+    double v_alpha;
+    zc vbp[2], vbm[2], vbpi[2], vbmi[2];   /* bmat_p, bmat_m, bmat_p_inv, bmat_m_inv */
+    zc vdp[2], vdm[2];                     /* delta_bmat_p(1,is), delta_bmat_m(1,is) */
 };
 
 struct orc_chain {
@@ -69,6 +74,14 @@ struct orc_chain {
     zc *zcpcm_bin, *zspsm_bin, *znn_bin, *pair_onsite_bin;  /* [lq][2][2] */
     zc *zjj_bin, *zbb_bin, *pair_nn_bin, *pair_sn_bin;       /* [lq] */
     zc zn_bin[2], zj_bin, zb_bin;
+    /* projective path (src/dqmc_proj_core.f90:11-19) */
+    int32_t *vconf;           /* [ltrot][nn_nf][nsites]: vconf%conf(nsites, nn_nf, ltrot) */
+    zc *projR, *projL;        /* N x N trial eigenvectors, first ne columns used */
+    double *trial_w;          /* trial eigenvalues */
+    zc *UR, *UL, *ULRINV;     /* N x ne, ne x N, ne x ne */
+    zc **Pst;                 /* Ust(0:nst) of the projective stack, N x ne */
+    double *logwDV;           /* logwDV(0:nst) */
+    double acc_v, prop_v;     /* main_obs(4) */
 };
 
 /* linear algebra helpers (orc_linalg.c) */
@@ -79,5 +92,18 @@ void orc_qrpt_logdet(int n, zc *a, zc *q, zc *r, int32_t *jpvt, zc *logdet); /* 
 void orc_zinv_logdet(int n, zc *a, zc *logdet);                              /* s_inv_logdet_lu_z */
 void orc_zinv(int n, zc *a);                                                 /* s_invlu_z */
 double orc_dznrm2(int n, const zc *x, int incx);
+double orc_qr_pqmc(int rdim, int cdim, const zc *amat, zc *qmat);             /* s_zgeQR_pqmc */
+void orc_eig_he(int n, const zc *h, double *w, zc *v);                       /* s_eig_he */
+
+/* shared with the projective path (orc_dqmc.c) */
+zc orc_total_ratio(const orc_model *m, zc ratio1, int is, int iflip, int isp);
+zc orc_set_phase(const orc_chain *c, zc logw);
+double orc_compare_max(int N, const zc *a, const zc *b);
+
+/* projective path (orc_proj.c) */
+void orc_set_vconf(orc_model *m);
+void orc_proj_chain_init(orc_chain *c, int draw_conf);
+void orc_proj_chain_free(orc_chain *c);
+void orc_v_prop(const orc_model *m, const int32_t *vconf, int op, int nt, int nf, int nflag, zc *g, int n2);
 
 #endif

@@ -407,3 +407,129 @@ void orc_inv_logdet_lu(int n, double *a, double *logdet) {
     orc_zinv_logdet(n, (zc *)a, &z);
     logdet[0] = creal(z); logdet[1] = cimag(z);
 }
+
+/* ------------------------------------------------------------------ */
+/* projective-path helpers                                             */
+/* ------------------------------------------------------------------ */
+static orc_zheev_fn p_zheev;
+void orc_set_zheev(orc_zheev_fn f) { p_zheev = f; }
+
+/* s_zgeQR_pqmc (lib/s_matrix.f90:1822-1996): Q of amat (rdim x cdim) with
+ * det R > 0, returns log |det R|.  A wide amat is factored through its plain
+ * transpose and Q is returned transposed (rdim x cdim). */
+double orc_qr_pqmc(int rdim, int cdim, const zc *amat, zc *qmat) {
+    int tall = rdim >= cdim;
+    int n1 = tall ? rdim : cdim, n2 = tall ? cdim : rdim, mn = n2;
+    zc *a = malloc(sizeof(zc) * (size_t)n1 * n2), *tau = malloc(sizeof(zc) * mn);
+    zc *q = malloc(sizeof(zc) * (size_t)n1 * n2);
+    for (int j = 0; j < n2; ++j)
+        for (int i = 0; i < n1; ++i)
+            a[ZIDX(i, j, n1)] = tall ? amat[ZIDX(i, j, rdim)] : amat[ZIDX(j, i, rdim)];
+    if (p_zgeqrf) {
+        int lwork = 64 * n1, info;
+        zc *work = malloc(sizeof(zc) * lwork);
+        p_zgeqrf(&n1, &n2, a, &n1, tau, work, &lwork, &info);
+        free(work);
+    } else {
+        orc_zgeqr2(n1, n2, (double *)a, n1, (double *)tau);
+    }
+    int isgn = 0;
+    double rlogdet = 0.0;
+    for (int i = 0; i < mn; ++i) {
+        double r = creal(a[ZIDX(i, i, n1)]);
+        if (r < 0.0) { ++isgn; rlogdet += log(-r); } else rlogdet += log(r);
+    }
+    for (int j = 0; j < mn; ++j)
+        for (int i = 0; i < n1; ++i)
+            q[ZIDX(i, j, n1)] = (i > j) ? a[ZIDX(i, j, n1)] : (i == j ? 1.0 : 0.0);
+    if (p_zungqr) {
+        int lwork = 64 * n1, info;
+        zc *work = malloc(sizeof(zc) * lwork);
+        p_zungqr(&n1, &mn, &mn, q, &n1, tau, work, &lwork, &info);
+        free(work);
+    } else {
+        orc_zung2r(n1, mn, mn, (double *)q, n1, (const double *)tau);
+    }
+    if (isgn % 2 == 1)
+        for (int i = 0; i < n1; ++i) q[ZIDX(i, 0, n1)] = -q[ZIDX(i, 0, n1)];
+    for (int j = 0; j < n2; ++j)
+        for (int i = 0; i < n1; ++i) {
+            if (tall) qmat[ZIDX(i, j, rdim)] = q[ZIDX(i, j, n1)];
+            else qmat[ZIDX(j, i, rdim)] = q[ZIDX(i, j, n1)];
+        }
+    free(a); free(tau); free(q);
+    return rlogdet;
+}
+
+/* cyclic complex Jacobi for a Hermitian matrix (used when no LAPACK zheev is
+ * hooked); eigenvalues ascending, eigenvectors in the columns of v */
+static void jacobi_he(int n, const zc *h, double *w, zc *v) {
+    zc *a = malloc(sizeof(zc) * (size_t)n * n);
+    memcpy(a, h, sizeof(zc) * (size_t)n * n);
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) v[ZIDX(i, j, n)] = (i == j) ? 1.0 : 0.0;
+    for (int sweep = 0; sweep < 100; ++sweep) {
+        double off = 0.0, dia = 0.0;
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                double t = cabs(a[ZIDX(i, j, n)]);
+                if (i != j) off += t * t; else dia += t * t;
+            }
+        if (off <= 1e-30 * (dia > 1e-300 ? dia : 1e-300)) break;
+        for (int p = 0; p < n - 1; ++p)
+            for (int q = p + 1; q < n; ++q) {
+                zc apq = a[ZIDX(p, q, n)];
+                double ab = cabs(apq);
+                if (ab < 1e-300) continue;
+                double app = creal(a[ZIDX(p, p, n)]), aqq = creal(a[ZIDX(q, q, n)]);
+                zc ph = apq / ab;                     /* apq = |apq| e^{i phi} */
+                double theta = 0.5 * atan2(2.0 * ab, aqq - app);
+                double cs = cos(theta), sn = sin(theta);
+                /* rotation J: columns p,q -> p' = c p - s conj(ph) q ... written as
+                 * J = [[c, s ph], [-s conj(ph), c]] acting on the (p,q) plane */
+                zc jpp = cs, jpq = sn * ph, jqp = -sn * conj(ph), jqq = cs;
+                for (int k = 0; k < n; ++k) {         /* A <- A J */
+                    zc x = a[ZIDX(k, p, n)], y = a[ZIDX(k, q, n)];
+                    a[ZIDX(k, p, n)] = x * jpp + y * jqp;
+                    a[ZIDX(k, q, n)] = x * jpq + y * jqq;
+                }
+                for (int k = 0; k < n; ++k) {         /* A <- J^H A */
+                    zc x = a[ZIDX(p, k, n)], y = a[ZIDX(q, k, n)];
+                    a[ZIDX(p, k, n)] = conj(jpp) * x + conj(jqp) * y;
+                    a[ZIDX(q, k, n)] = conj(jpq) * x + conj(jqq) * y;
+                }
+                for (int k = 0; k < n; ++k) {         /* V <- V J */
+                    zc x = v[ZIDX(k, p, n)], y = v[ZIDX(k, q, n)];
+                    v[ZIDX(k, p, n)] = x * jpp + y * jqp;
+                    v[ZIDX(k, q, n)] = x * jpq + y * jqq;
+                }
+                a[ZIDX(p, q, n)] = 0; a[ZIDX(q, p, n)] = 0;
+            }
+    }
+    /* ascending selection sort of eigenpairs */
+    for (int i = 0; i < n; ++i) w[i] = creal(a[ZIDX(i, i, n)]);
+    for (int i = 0; i < n; ++i) {
+        int k = i;
+        for (int j = i + 1; j < n; ++j) if (w[j] < w[k]) k = j;
+        if (k != i) {
+            double t = w[i]; w[i] = w[k]; w[k] = t;
+            for (int r = 0; r < n; ++r) { zc x = v[ZIDX(r, i, n)]; v[ZIDX(r, i, n)] = v[ZIDX(r, k, n)]; v[ZIDX(r, k, n)] = x; }
+        }
+    }
+    free(a);
+}
+
+/* s_eig_he (lib/s_matrix.f90:202-253): zheev('V','U') */
+void orc_eig_he(int n, const zc *h, double *w, zc *v) {
+    if (p_zheev) {
+        memcpy(v, h, sizeof(zc) * (size_t)n * n);
+        int lwork = 2 * n - 1 > 64 * n ? 2 * n - 1 : 64 * n, info;
+        zc *work = malloc(sizeof(zc) * lwork);
+        double *rwork = malloc(sizeof(double) * (3 * n > 1 ? 3 * n : 1));
+        char jv = 'V', up = 'U';
+        p_zheev(&jv, &up, &n, v, &n, w, work, &lwork, rwork, &info);
+        free(work); free(rwork);
+    } else {
+        jacobi_he(n, h, w, v);
+    }
+}

@@ -1,0 +1,558 @@
+/* Projective (ground-state) DQMC sweep and the t-V bond field, restated
+ * from the Fortran reference.  Test infrastructure only (see dqmc_oracle.h).
+ *
+ *  - vconf constants, field draw and propagators:
+ *      src/dqmc_config_v/dqmc_set_conf.f90:1-79, dqmc_input_conf.f90:36-63,
+ *      dqmc_{left,right}_{forward,backward}_prop.f90, _hc
+ *  - projective updates, fast flavour (the delayed / submatrix flavours give
+ *    the same accept sequence):
+ *      src/dqmc_config_v/dqmc_proj_update.f90:1-104 (bond, rank 2)
+ *      src/dqmc_config_u/dqmc_proj_update.f90:1-92  (site, rank 1)
+ *  - trial state: src/dqmc_config_h0/set_trial_h0.f90:1-29,
+ *      src/dqmc_proj_core/dqmc_set_proj.f90:1-78
+ *  - core: src/dqmc_proj_core/dqmc_proj_sweep_start_0b.f90:1-48,
+ *      dqmc_proj_sweep_b0.f90:1-220, dqmc_proj_sweep_0b.f90:1-235,
+ *      dqmc_proj_stablize_{0b,b0}_qr.f90, green_equaltime.f90, set_phase.f90
+ *
+ * Layouts follow the reference: UR is ndim x ne, UL is ne x ndim, both
+ * column-major; the stack keeps Ust(n) as ndim x ne.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include "orc_internal.h"
+
+static zc *zalloc(size_t n) { return calloc(n ? n : 1, sizeof(zc)); }
+
+/* ------------------------------------------------------------------ */
+/* vconf constants (src/dqmc_config_v/dqmc_set_conf.f90:1-79)          */
+/* ------------------------------------------------------------------ */
+void orc_set_vconf(orc_model *m) {
+    const orc_params *p = &m->p;
+    m->lwrapv = (p->rv != 0.0);
+    if (!m->lwrapv) return;
+    const double etal[2] = {-1.0, 1.0};
+    double al = acosh(exp(p->dtau * p->rv * 0.5));
+    m->v_alpha = al;
+    for (int is = 1; is <= 2; ++is) {
+        if (p->lprojv) {
+            zc z = cexp(I * (M_PI * 2.0 * is / 2.0));
+            m->vbp[is - 1] = z; m->vbm[is - 1] = z;
+            m->vbpi[is - 1] = conj(z); m->vbmi[is - 1] = conj(z);
+        } else {
+            m->vbp[is - 1] = exp(al * etal[is - 1]);
+            m->vbpi[is - 1] = exp(-al * etal[is - 1]);
+            m->vbm[is - 1] = exp(-al * etal[is - 1]);
+            m->vbmi[is - 1] = exp(al * etal[is - 1]);
+        }
+        int isp = is % 2 + 1;   /* mod(is+iflip-1, lcomp)+1 with iflip = 1 */
+        if (p->lprojv) {
+            m->vdp[is - 1] = cexp(I * (M_PI * (2.0 * isp - 2.0 * is) / 2.0)) - 1.0;
+            m->vdm[is - 1] = exp(al * (etal[isp - 1] - etal[is - 1])) - 1.0;
+        } else {
+            m->vdp[is - 1] = exp(al * (etal[isp - 1] - etal[is - 1])) - 1.0;
+            m->vdm[is - 1] = exp(-al * (etal[isp - 1] - etal[is - 1])) - 1.0;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* vconf props: B_nf = U diag(bmat_p, bmat_m) U^T per bond, U the 2x2   */
+/* Hadamard; nflag 2 and 1 are the two halves around the update.       */
+/* ------------------------------------------------------------------ */
+void orc_v_prop(const orc_model *m, const int32_t *vconf, int op, int nt, int nf, int nflag, zc *g, int n2) {
+    const orc_latt *L = &m->L;
+    int N = m->ndim, lf = L->nn_lf, nnf = L->nn_nf;
+    const double h = 1.0 / sqrt(2.0);
+    const zc u11 = h, u12 = h, u21 = h, u22 = -h;   /* u = ut (dqmc_config_v.f90:20-21) */
+    const int32_t *cf = vconf + ((size_t)(nt - 1) * nnf + (nf - 1)) * N;
+    int left = (op == ORC_LEFT_FORWARD || op == ORC_LEFT_BACKWARD || op == ORC_LEFT_FORWARD_HC);
+    for (int b = 0; b < lf; ++b) {
+        int i1 = L->nnlf_list[b] - 1;
+        int i2 = L->nnlist[i1 * nnf + nf - 1] - 1;
+        int is = cf[b] - 1;
+        if (left) {
+            /* rows i1, i2 of an N x n2 matrix */
+            for (int j = 0; j < n2; ++j) {
+                zc x1 = g[ZIDX(i1, j, N)], x2 = g[ZIDX(i2, j, N)];
+                if (op == ORC_LEFT_FORWARD || op == ORC_LEFT_FORWARD_HC) {
+                    if (nflag == 2) {
+                        zc v1 = u11 * x1 + u12 * x2, v2 = u21 * x1 + u22 * x2;
+                        x1 = m->vbp[is] * v1; x2 = m->vbm[is] * v2;
+                    } else {
+                        zc v1 = u11 * x1 + u12 * x2, v2 = u21 * x1 + u22 * x2;
+                        x1 = v1; x2 = v2;
+                    }
+                } else {   /* LEFT_BACKWARD */
+                    if (nflag == 2) {
+                        zc v1 = u11 * x1 + u12 * x2, v2 = u21 * x1 + u22 * x2;
+                        x1 = v1; x2 = v2;
+                    } else {
+                        x1 = m->vbpi[is] * x1; x2 = m->vbmi[is] * x2;
+                        zc v1 = u11 * x1 + u12 * x2, v2 = u21 * x1 + u22 * x2;
+                        x1 = v1; x2 = v2;
+                    }
+                }
+                g[ZIDX(i1, j, N)] = x1; g[ZIDX(i2, j, N)] = x2;
+            }
+        } else {
+            /* columns i1, i2 of an n2 x N matrix */
+            for (int j = 0; j < n2; ++j) {
+                zc x1 = g[ZIDX(j, i1, n2)], x2 = g[ZIDX(j, i2, n2)];
+                if (op == ORC_RIGHT_FORWARD) {
+                    if (nflag == 2) {
+                        zc v1 = x1 * u11 + x2 * u21, v2 = x1 * u12 + x2 * u22;
+                        x1 = v1; x2 = v2;
+                    } else {
+                        x1 = m->vbp[is] * x1; x2 = m->vbm[is] * x2;
+                        zc v1 = x1 * u11 + x2 * u21, v2 = x1 * u12 + x2 * u22;
+                        x1 = v1; x2 = v2;
+                    }
+                } else {   /* RIGHT_BACKWARD */
+                    if (nflag == 2) {
+                        zc v1 = x1 * u11 + x2 * u21, v2 = x1 * u12 + x2 * u22;
+                        x1 = m->vbpi[is] * v1; x2 = m->vbmi[is] * v2;
+                    } else {
+                        zc v1 = x1 * u11 + x2 * u21, v2 = x1 * u12 + x2 * u22;
+                        x1 = v1; x2 = v2;
+                    }
+                }
+                g[ZIDX(j, i1, n2)] = x1; g[ZIDX(j, i2, n2)] = x2;
+            }
+        }
+    }
+}
+
+void orc_vconf_prop(const orc_model *m, const int32_t *vconf, int op, int nt, int nf, int nflag, double *g, int n2) {
+    orc_v_prop(m, vconf, op, nt, nf, nflag, (zc *)g, n2);
+}
+
+/* ------------------------------------------------------------------ */
+/* chain state                                                         */
+/* ------------------------------------------------------------------ */
+
+/* set_trial_h0 (src/dqmc_config_h0/set_trial_h0.f90:1-29) + dqmc_set_proj */
+static void set_proj(orc_chain *c) {
+    const orc_model *m = c->m;
+    const orc_latt *L = &m->L;
+    const orc_params *p = &m->p;
+    int N = m->ndim, nnf = L->nn_nf;
+    zc *h = zalloc((size_t)N * N);
+    for (int b = 0; b < L->nn_lf; ++b) {
+        int i0 = L->nnlf_list[b] - 1;
+        for (int nf = 1; nf <= nnf; ++nf) {
+            int in = L->nnlist[i0 * nnf + nf - 1] - 1;
+            double r = orc_sfmt_stream(&c->rng);
+            zc z1 = (-p->rt + p->rndness * (r - 1.0)) * orc_expar(L, i0, nf, p->xmag, p->flux_x, p->flux_y, p->dimer);
+            h[ZIDX(i0, in, N)] += z1;
+            h[ZIDX(in, i0, N)] += conj(z1);
+        }
+    }
+    for (int i = 0; i < N; ++i) h[ZIDX(i, i, N)] -= p->mu;
+    orc_eig_he(N, h, c->trial_w, c->projR);
+    memcpy(c->projL, c->projR, sizeof(zc) * (size_t)N * N);
+    free(h);
+}
+
+void orc_proj_chain_init(orc_chain *c, int draw_conf) {
+    const orc_model *m = c->m;
+    int N = m->ndim, lt = m->ltrot, nnf = m->L.nn_nf, ne = m->ne, nst = m->nst;
+    if (m->lwrapv) {
+        c->vconf = calloc((size_t)lt * nnf * N, sizeof(int32_t));
+        for (size_t e = 0; e < (size_t)lt * nnf * N; ++e) c->vconf[e] = 1;
+        if (draw_conf)   /* dqmc_config_v/dqmc_input_conf.f90:55-63: nt, site, family */
+            for (int nt = 0; nt < lt; ++nt)
+                for (int i = 0; i < N; ++i)
+                    for (int nf = 0; nf < nnf; ++nf)
+                        c->vconf[((size_t)nt * nnf + nf) * N + i] = (int32_t)ceil(orc_sfmt_stream(&c->rng) * 2);
+    }
+    if (!m->proj) return;
+    c->projR = zalloc((size_t)N * N);
+    c->projL = zalloc((size_t)N * N);
+    c->trial_w = calloc(N, sizeof(double));
+    c->UR = zalloc((size_t)N * ne);
+    c->UL = zalloc((size_t)N * ne);
+    c->ULRINV = zalloc((size_t)ne * ne);
+    c->Pst = calloc(nst + 1, sizeof(zc *));
+    for (int n = 0; n <= nst; ++n) c->Pst[n] = zalloc((size_t)N * ne);
+    c->logwDV = calloc(nst + 1, sizeof(double));
+    set_proj(c);
+}
+
+void orc_proj_chain_free(orc_chain *c) {
+    free(c->vconf);
+    if (!c->m->proj) return;
+    for (int n = 0; n <= c->m->nst; ++n) free(c->Pst[n]);
+    free(c->Pst); free(c->logwDV);
+    free(c->projR); free(c->projL); free(c->trial_w);
+    free(c->UR); free(c->UL); free(c->ULRINV);
+}
+
+void orc_proj_get_trial(const orc_chain *c, double *proj, double *w) {
+    int N = c->m->ndim;
+    if (proj) memcpy(proj, c->projR, sizeof(zc) * (size_t)N * N);
+    if (w) memcpy(w, c->trial_w, sizeof(double) * N);
+}
+void orc_proj_set_trial(orc_chain *c, const double *proj) {
+    int N = c->m->ndim;
+    memcpy(c->projR, proj, sizeof(zc) * (size_t)N * N);
+    memcpy(c->projL, proj, sizeof(zc) * (size_t)N * N);
+}
+void orc_proj_get(const orc_chain *c, double *ur, double *ul, double *ulrinv) {
+    int N = c->m->ndim, ne = c->m->ne;
+    if (ur) memcpy(ur, c->UR, sizeof(zc) * (size_t)N * ne);
+    if (ul) memcpy(ul, c->UL, sizeof(zc) * (size_t)N * ne);
+    if (ulrinv) memcpy(ulrinv, c->ULRINV, sizeof(zc) * (size_t)ne * ne);
+}
+void orc_proj_set(orc_chain *c, const double *ur, const double *ul, const double *ulrinv) {
+    int N = c->m->ndim, ne = c->m->ne;
+    if (ur) memcpy(c->UR, ur, sizeof(zc) * (size_t)N * ne);
+    if (ul) memcpy(c->UL, ul, sizeof(zc) * (size_t)N * ne);
+    if (ulrinv) memcpy(c->ULRINV, ulrinv, sizeof(zc) * (size_t)ne * ne);
+}
+void orc_vconf_get(const orc_chain *c, int32_t *v) {
+    const orc_model *m = c->m;
+    if (c->vconf) memcpy(v, c->vconf, sizeof(int32_t) * (size_t)m->ltrot * m->L.nn_nf * m->ndim);
+}
+void orc_vconf_set(orc_chain *c, const int32_t *v) {
+    const orc_model *m = c->m;
+    if (c->vconf) memcpy(c->vconf, v, sizeof(int32_t) * (size_t)m->ltrot * m->L.nn_nf * m->ndim);
+}
+
+/* ------------------------------------------------------------------ */
+/* core helpers                                                        */
+/* ------------------------------------------------------------------ */
+
+/* green_equaltime (src/dqmc_proj_core/green_equaltime.f90): gr = I - UR ULRINV UL */
+static void proj_green(int N, int ne, const zc *ul, const zc *ur, const zc *ulrinv, zc *gr) {
+    zc *t = zalloc((size_t)N * ne);
+    orc_zgemm('N', 'N', N, ne, ne, 1.0, ur, N, ulrinv, ne, 0.0, t, N);
+    orc_zgemm('N', 'N', N, N, ne, -1.0, t, N, ul, ne, 0.0, gr, N);
+    for (int i = 0; i < N; ++i) gr[ZIDX(i, i, N)] += 1.0;
+    free(t);
+}
+
+void orc_proj_green(orc_chain *c) {
+    proj_green(c->m->ndim, c->m->ne, c->UL, c->UR, c->ULRINV, c->gf);
+}
+
+/* ULR = UL UR; inverse (s_invlu_z or s_inv_logdet_lu_z) into out */
+static void ulr_inverse(int N, int ne, const zc *ul, const zc *ur, zc *out, zc *logdet) {
+    orc_zgemm('N', 'N', ne, ne, N, 1.0, ul, ne, ur, N, 0.0, out, ne);
+    if (logdet) orc_zinv_logdet(ne, out, logdet);
+    else orc_zinv(ne, out);
+}
+
+/* dqmc_proj_update, bond field (src/dqmc_config_v/dqmc_proj_update.f90:1-104) */
+static void proj_update_v(orc_chain *c, int nt, int nf) {
+    const orc_model *m = c->m;
+    const orc_latt *L = &m->L;
+    int N = m->ndim, ne = m->ne, nnf = L->nn_nf;
+    int32_t *cf = c->vconf + ((size_t)(nt - 1) * nnf + (nf - 1)) * N;
+    zc *vk_tmp = zalloc(2 * (size_t)ne), *vk = zalloc(2 * (size_t)ne), *uk = zalloc(2 * (size_t)ne);
+    zc *lruk = zalloc(2 * (size_t)ne), *vuvk = zalloc(2 * (size_t)ne);
+    double accm = 0.0;
+    for (int b = 0; b < L->nn_lf; ++b) {
+        int i1 = L->nnlf_list[b] - 1;
+        int i2 = L->nnlist[i1 * nnf + nf - 1] - 1;
+        int is = cf[b];
+        int iflip = (int)ceil(orc_sfmt_stream(&c->rng) * 1);
+        int isp = (is + iflip - 1) % 2 + 1;
+        zc dp = m->vdp[is - 1], dm = m->vdm[is - 1];
+        for (int l = 0; l < ne; ++l) {
+            vk_tmp[2 * l] = dp * c->UR[ZIDX(i1, l, N)];        /* D * vuvkmat, 2 x ne */
+            vk_tmp[2 * l + 1] = dm * c->UR[ZIDX(i2, l, N)];
+            uk[l] = c->UL[ZIDX(l, i1, ne)];                    /* ukmat, ne x 2 */
+            uk[ne + l] = c->UL[ZIDX(l, i2, ne)];
+        }
+        orc_zgemm('N', 'N', 2, ne, ne, 1.0, vk_tmp, 2, c->ULRINV, ne, 0.0, vk, 2);
+        zc vuk[4] = {1.0, 0.0, 0.0, 1.0};
+        orc_zgemm('N', 'N', 2, 2, ne, 1.0, vk, 2, uk, ne, 1.0, vuk, 2);
+        zc det = vuk[0] * vuk[3] - vuk[2] * vuk[1];
+        zc inv[4] = {vuk[3] / det, -vuk[1] / det, -vuk[2] / det, vuk[0] / det};
+        zc ratiotot = det;
+        double ratio_re = creal(ratiotot * c->phase) / creal(c->phase);
+        double ratio_abs = ratio_re < 0 ? -ratio_re : ratio_re;
+        double random = orc_sfmt_stream(&c->rng);
+        if (ratio_abs > random) {
+            accm += 1.0;
+            double weight = sqrt(creal(ratiotot * conj(ratiotot)));
+            c->phase = c->phase * ratiotot / weight;
+            for (int l = 0; l < ne; ++l) {
+                c->UR[ZIDX(i1, l, N)] += vk_tmp[2 * l];
+                c->UR[ZIDX(i2, l, N)] += vk_tmp[2 * l + 1];
+            }
+            orc_zgemm('N', 'N', 2, ne, 2, 1.0, inv, 2, vk, 2, 0.0, vuvk, 2);
+            orc_zgemm('N', 'N', ne, 2, ne, 1.0, c->ULRINV, ne, uk, ne, 0.0, lruk, ne);
+            orc_zgemm('N', 'N', ne, ne, 2, -1.0, lruk, ne, vuvk, 2, 1.0, c->ULRINV, ne);
+            cf[b] = isp;
+        }
+    }
+    c->acc_v += accm;
+    c->prop_v += L->nn_lf;
+    free(vk_tmp); free(vk); free(uk); free(lruk); free(vuvk);
+}
+
+/* dqmc_proj_update, site field (src/dqmc_config_u/dqmc_proj_update.f90:1-92) */
+static void proj_update_u(orc_chain *c, int nt) {
+    const orc_model *m = c->m;
+    int N = m->ndim, ne = m->ne, lc = m->lcomp;
+    int32_t *cf = c->conf + (size_t)(nt - 1) * N;
+    zc *vk_tmp = zalloc(ne), *vk = zalloc(ne), *uk = zalloc(ne), *lruk = zalloc(ne);
+    double accm = 0.0;
+    for (int i = 0; i < N; ++i) {
+        int is = cf[i];
+        int iflip = (int)ceil(orc_sfmt_stream(&c->rng) * (lc - 1));
+        int isp = (is + iflip - 1) % lc + 1;
+        zc d = m->delta[(is - 1) * (lc - 1) + iflip - 1];
+        for (int l = 0; l < ne; ++l) { vk_tmp[l] = d * c->UR[ZIDX(i, l, N)]; uk[l] = c->UL[ZIDX(l, i, ne)]; }
+        for (int l = 0; l < ne; ++l) {
+            zc s = 0;
+            for (int k = 0; k < ne; ++k) s += vk_tmp[k] * c->ULRINV[ZIDX(k, l, ne)];
+            vk[l] = s;
+        }
+        zc ratio1 = 1.0;
+        for (int l = 0; l < ne; ++l) ratio1 += vk[l] * uk[l];
+        zc sscl = 1.0 / ratio1;
+        zc ratiotot = orc_total_ratio(m, ratio1, is, iflip, isp);
+        double ratio_re = creal(ratiotot * c->phase) / creal(c->phase);
+        double ratio_abs = ratio_re < 0 ? -ratio_re : ratio_re;
+        double random = orc_sfmt_stream(&c->rng);
+        if (ratio_abs > random) {
+            accm += 1.0;
+            double weight = sqrt(creal(ratiotot * conj(ratiotot)));
+            c->phase = c->phase * ratiotot / weight;
+            for (int l = 0; l < ne; ++l) c->UR[ZIDX(i, l, N)] += vk_tmp[l];
+            for (int l = 0; l < ne; ++l) {
+                zc s = 0;
+                for (int k = 0; k < ne; ++k) s += c->ULRINV[ZIDX(l, k, ne)] * uk[k];
+                lruk[l] = s;
+            }
+            for (int k = 0; k < ne; ++k) {
+                zc w = sscl * vk[k];
+                for (int l = 0; l < ne; ++l) c->ULRINV[ZIDX(l, k, ne)] -= lruk[l] * w;
+            }
+            cf[i] = isp;
+        }
+    }
+    c->acc_u += accm;
+    c->prop_u += N;
+    free(vk_tmp); free(vk); free(uk); free(lruk);
+}
+
+void orc_proj_update(orc_chain *c, int nt, int nf) {
+    if (nf > 0) proj_update_v(c, nt, nf);
+    else proj_update_u(c, nt);
+}
+
+/* h0 half step on UR (left op) and UL (right op), families in order or reversed */
+static void h0_pair(orc_chain *c, int lop, int rop, int reversed) {
+    const orc_model *m = c->m;
+    int ne = m->ne, nnf = m->L.nn_nf;
+    if (!m->lwrapT) return;
+    if (m->p.kinetic == ORC_CHECKERBOARD) {
+        for (int k = 1; k <= nnf; ++k) {
+            int nf = reversed ? nnf + 1 - k : k;
+            /* the reference applies the UL side first in the b0 sweep and the
+             * UR side first in the 0b sweep; the two act on different matrices */
+            orc_h0_prop(m, lop, nf, (double *)c->UR, ne);
+            orc_h0_prop(m, rop, nf, (double *)c->UL, ne);
+        }
+    } else {
+        orc_h0_prop(m, lop, 0, (double *)c->UR, ne);
+        orc_h0_prop(m, rop, 0, (double *)c->UL, ne);
+    }
+}
+
+/* Bmat_left_forward over slices nt2..nt1 (src/dqmc_proj_core.f90:61-104) on an N x ne matrix */
+static void bmat_left_forward_proj(const orc_chain *c, int nt1, int nt2, zc *x) {
+    const orc_model *m = c->m;
+    int ne = m->ne, nnf = m->L.nn_nf;
+    for (int nt = nt2; nt <= nt1; ++nt) {
+        if (m->lwrapT) {
+            if (m->p.kinetic == ORC_CHECKERBOARD)
+                for (int nf = 1; nf <= nnf; ++nf) orc_h0_prop(m, ORC_LEFT_FORWARD, nf, (double *)x, ne);
+            else orc_h0_prop(m, ORC_LEFT_FORWARD, 0, (double *)x, ne);
+        }
+        if (m->lwrapv)
+            for (int nf = 1; nf <= nnf; ++nf) {
+                orc_v_prop(m, c->vconf, ORC_LEFT_FORWARD, nt, nf, 2, x, ne);
+                orc_v_prop(m, c->vconf, ORC_LEFT_FORWARD, nt, nf, 1, x, ne);
+            }
+        if (m->lwrapu) orc_u_prop(m, c->conf, ORC_LEFT_FORWARD, nt, (double *)x, ne);
+        if (m->lwrapT) {
+            if (m->p.kinetic == ORC_CHECKERBOARD)
+                for (int nf = nnf; nf >= 1; --nf) orc_h0_prop(m, ORC_LEFT_FORWARD, nf, (double *)x, ne);
+            else orc_h0_prop(m, ORC_LEFT_FORWARD, 0, (double *)x, ne);
+        }
+    }
+}
+
+static int in_mid(const orc_model *m, int nt) {
+    int lt = m->ltrot, len = m->obs_mid_len;
+    return nt > (lt / 2 - (len + 1) / 2) && nt <= (lt / 2 + len / 2);
+}
+
+static void measure_here(orc_chain *c, int nt) {
+    const orc_model *m = c->m;
+    ulr_inverse(m->ndim, m->ne, c->UL, c->UR, c->ULRINV, NULL);
+    orc_proj_green(c);
+    orc_measure(c, nt);
+}
+
+/* wrap-error bookkeeping of the WRAPERROR blocks, then adopt the new weight */
+static void record_proj_wrap(orc_chain *c, const zc *ultmp, const zc *urtmp, zc lw) {
+    const orc_model *m = c->m;
+    int N = m->ndim, ne = m->ne;
+    zc *inv = zalloc((size_t)ne * ne), *gtmp = zalloc((size_t)N * N);
+    ulr_inverse(N, ne, ultmp, urtmp, inv, NULL);
+    proj_green(N, ne, ultmp, urtmp, inv, gtmp);
+    double err = orc_compare_max(N, gtmp, c->gf);
+    if (err > c->max_wrap_error) c->max_wrap_error = err;
+    zc ph = orc_set_phase(c, lw);
+    double pd = cabs(c->phase - ph);
+    if (pd > c->max_phasediff) c->max_phasediff = pd;
+    c->logcount += 1.0;
+    c->avglog10error += log10(err);
+    c->avgexpphasediff += exp(pd);
+    c->phase = ph;
+    c->logweightf = lw;
+    free(inv); free(gtmp);
+}
+
+/* ------------------------------------------------------------------ */
+/* sweeps                                                              */
+/* ------------------------------------------------------------------ */
+
+/* dqmc_proj_sweep_start_0b (src/dqmc_proj_core/dqmc_proj_sweep_start_0b.f90:1-48) */
+int orc_proj_sweep_start_0b(orc_chain *c) {
+    const orc_model *m = c->m;
+    int N = m->ndim, ne = m->ne, nst = m->nst;
+    for (int l = 0; l < ne; ++l)
+        for (int i = 0; i < N; ++i) {
+            c->UR[ZIDX(i, l, N)] = c->projR[ZIDX(i, l, N)];
+            c->Pst[nst][ZIDX(i, l, N)] = conj(c->projL[ZIDX(i, l, N)]);
+        }
+    c->logweightf = 0;
+    c->logwDV[0] = 0.0;
+    zc *tmp = zalloc((size_t)N * ne);
+    for (int n = 1; n <= nst; ++n) {
+        bmat_left_forward_proj(c, m->wrap_step[(n - 1) * 2 + 1], m->wrap_step[(n - 1) * 2], c->UR);
+        double lw = orc_qr_pqmc(N, ne, c->UR, tmp);
+        memcpy(c->UR, tmp, sizeof(zc) * (size_t)N * ne);
+        memcpy(c->Pst[n], c->UR, sizeof(zc) * (size_t)N * ne);
+        c->logwDV[n] = c->logwDV[n - 1] + lw;
+    }
+    for (int l = 0; l < ne; ++l)
+        for (int i = 0; i < N; ++i) c->UL[ZIDX(l, i, ne)] = conj(c->projL[ZIDX(i, l, N)]);
+    zc zlogw;
+    ulr_inverse(N, ne, c->UL, c->UR, c->ULRINV, &zlogw);
+    c->phase = orc_set_phase(c, zlogw);
+    c->logweightf = c->logwDV[nst] + zlogw;
+    free(tmp);
+    return 0;
+}
+
+/* dqmc_proj_sweep_b0 (src/dqmc_proj_core/dqmc_proj_sweep_b0.f90:1-220) */
+int orc_proj_sweep_b0(orc_chain *c, int lupdate, int lmeasure) {
+    const orc_model *m = c->m;
+    int N = m->ndim, ne = m->ne, nst = m->nst, nnf = m->L.nn_nf;
+    zc *ultmp = zalloc((size_t)N * ne), *urtmp = zalloc((size_t)N * ne), *q = zalloc((size_t)N * ne);
+    for (int l = 0; l < ne; ++l)
+        for (int i = 0; i < N; ++i) {
+            c->UL[ZIDX(l, i, ne)] = conj(c->projL[ZIDX(i, l, N)]);
+            c->Pst[0][ZIDX(i, l, N)] = c->projR[ZIDX(i, l, N)];
+        }
+    for (int nt = m->ltrot; nt >= 1; --nt) {
+        if (lmeasure && in_mid(m, nt)) measure_here(c, nt);
+        h0_pair(c, ORC_LEFT_BACKWARD, ORC_RIGHT_FORWARD, 0);
+        if (m->lwrapu) {
+            if (lupdate) proj_update_u(c, nt);
+            orc_u_prop(m, c->conf, ORC_RIGHT_FORWARD, nt, (double *)c->UL, ne);
+            orc_u_prop(m, c->conf, ORC_LEFT_BACKWARD, nt, (double *)c->UR, ne);
+        }
+        if (m->lwrapv)
+            for (int nf = nnf; nf >= 1; --nf) {
+                orc_v_prop(m, c->vconf, ORC_RIGHT_FORWARD, nt, nf, 2, c->UL, ne);
+                orc_v_prop(m, c->vconf, ORC_LEFT_BACKWARD, nt, nf, 2, c->UR, ne);
+                if (lupdate) proj_update_v(c, nt, nf);
+                orc_v_prop(m, c->vconf, ORC_RIGHT_FORWARD, nt, nf, 1, c->UL, ne);
+                orc_v_prop(m, c->vconf, ORC_LEFT_BACKWARD, nt, nf, 1, c->UR, ne);
+            }
+        h0_pair(c, ORC_LEFT_BACKWARD, ORC_RIGHT_FORWARD, 1);
+        if ((m->iwrap_nt[nt - 1] > 0 || m->p.nwrap == 1) || nt == 1) {
+            int n = m->iwrap_nt[nt - 1];
+            memcpy(urtmp, c->UR, sizeof(zc) * (size_t)N * ne);
+            memcpy(ultmp, c->UL, sizeof(zc) * (size_t)N * ne);
+            memcpy(c->UR, c->Pst[n], sizeof(zc) * (size_t)N * ne);
+            double lwt = orc_qr_pqmc(ne, N, c->UL, q);       /* stablize_b0_qr */
+            memcpy(c->UL, q, sizeof(zc) * (size_t)N * ne);
+            c->logwDV[n + 1] = (n + 1 == nst) ? lwt : c->logwDV[n + 2] + lwt;
+            zc zlogw;
+            ulr_inverse(N, ne, c->UL, c->UR, c->ULRINV, &zlogw);
+            zc lw = (n == 0) ? c->logwDV[n + 1] + zlogw : c->logwDV[n + 1] + c->logwDV[n] + zlogw;
+            orc_proj_green(c);
+            record_proj_wrap(c, ultmp, urtmp, lw);
+            for (int l = 0; l < ne; ++l)
+                for (int i = 0; i < N; ++i) c->Pst[n][ZIDX(i, l, N)] = c->UL[ZIDX(l, i, ne)];
+        }
+    }
+    free(ultmp); free(urtmp); free(q);
+    return 0;
+}
+
+/* dqmc_proj_sweep_0b (src/dqmc_proj_core/dqmc_proj_sweep_0b.f90:1-235), ltau off */
+int orc_proj_sweep_0b(orc_chain *c, int lupdate, int lmeasure) {
+    const orc_model *m = c->m;
+    int N = m->ndim, ne = m->ne, nst = m->nst, nnf = m->L.nn_nf;
+    zc *ultmp = zalloc((size_t)N * ne), *urtmp = zalloc((size_t)N * ne), *q = zalloc((size_t)N * ne);
+    for (int l = 0; l < ne; ++l)
+        for (int i = 0; i < N; ++i) {
+            c->UR[ZIDX(i, l, N)] = c->projR[ZIDX(i, l, N)];
+            c->Pst[nst][ZIDX(i, l, N)] = conj(c->projL[ZIDX(i, l, N)]);
+        }
+    c->logwDV[0] = 0.0;
+    for (int nt = 1; nt <= m->ltrot; ++nt) {
+        h0_pair(c, ORC_LEFT_FORWARD, ORC_RIGHT_BACKWARD, 0);
+        if (m->lwrapv)
+            for (int nf = 1; nf <= nnf; ++nf) {
+                orc_v_prop(m, c->vconf, ORC_LEFT_FORWARD, nt, nf, 2, c->UR, ne);
+                orc_v_prop(m, c->vconf, ORC_RIGHT_BACKWARD, nt, nf, 2, c->UL, ne);
+                if (lupdate) proj_update_v(c, nt, nf);
+                orc_v_prop(m, c->vconf, ORC_LEFT_FORWARD, nt, nf, 1, c->UR, ne);
+                orc_v_prop(m, c->vconf, ORC_RIGHT_BACKWARD, nt, nf, 1, c->UL, ne);
+            }
+        if (m->lwrapu) {
+            orc_u_prop(m, c->conf, ORC_LEFT_FORWARD, nt, (double *)c->UR, ne);
+            orc_u_prop(m, c->conf, ORC_RIGHT_BACKWARD, nt, (double *)c->UL, ne);
+            if (lupdate) proj_update_u(c, nt);
+        }
+        h0_pair(c, ORC_LEFT_FORWARD, ORC_RIGHT_BACKWARD, 1);
+        if (lmeasure && in_mid(m, nt)) measure_here(c, nt);
+        if (m->iwrap_nt[nt] > 0) {
+            int n = m->iwrap_nt[nt];
+            memcpy(ultmp, c->UL, sizeof(zc) * (size_t)N * ne);
+            memcpy(urtmp, c->UR, sizeof(zc) * (size_t)N * ne);
+            for (int l = 0; l < ne; ++l)
+                for (int i = 0; i < N; ++i) c->UL[ZIDX(l, i, ne)] = c->Pst[n][ZIDX(i, l, N)];
+            double lwt = orc_qr_pqmc(N, ne, c->UR, q);       /* stablize_0b_qr */
+            memcpy(c->UR, q, sizeof(zc) * (size_t)N * ne);
+            c->logwDV[n] = c->logwDV[n - 1] + lwt;
+            zc zlogw;
+            ulr_inverse(N, ne, c->UL, c->UR, c->ULRINV, &zlogw);
+            zc lw = (n == nst) ? c->logwDV[n] + zlogw : c->logwDV[n] + c->logwDV[n + 1] + zlogw;
+            orc_proj_green(c);
+            record_proj_wrap(c, ultmp, urtmp, lw);
+            memcpy(c->Pst[n], c->UR, sizeof(zc) * (size_t)N * ne);
+        }
+    }
+    free(ultmp); free(urtmp); free(q);
+    return 0;
+}
+
+double orc_qr_pqmc_d(int rdim, int cdim, const double *a, double *q) {
+    return orc_qr_pqmc(rdim, cdim, (const zc *)a, (zc *)q);
+}
+void orc_eig_he_d(int n, const double *h, double *w, double *v) {
+    orc_eig_he(n, (const zc *)h, w, (zc *)v);
+}

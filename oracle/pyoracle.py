@@ -39,6 +39,7 @@ class OrcParams(C.Structure):
         ("nflr", C.c_int32), ("lproju", C.c_int32), ("lstabilize", C.c_int32),
         ("nwrap", C.c_int32), ("nsweep", C.c_int32), ("nbin", C.c_int32), ("nublock", C.c_int32),
         ("update", C.c_int32), ("kinetic", C.c_int32), ("hs", C.c_int32),
+        ("proj", C.c_int32), ("lprojv", C.c_int32), ("obs_mid_len", C.c_int32),
     ]
 
 
@@ -95,6 +96,22 @@ def lib() -> C.CDLL:
         L.orc_zgetf2.argtypes = [C.c_int, C.c_int, vp, C.c_int, vp]
         L.orc_zmcpt.argtypes = [C.c_int, C.c_int, vp, vp]
         L.orc_inv_logdet_lu.argtypes = [C.c_int, vp, vp]
+        for name in ("orc_proj_sweep_start_0b",):
+            getattr(L, name).argtypes = [vp]
+        L.orc_proj_sweep_b0.argtypes = [vp, C.c_int, C.c_int]
+        L.orc_proj_sweep_0b.argtypes = [vp, C.c_int, C.c_int]
+        L.orc_proj_get_trial.argtypes = [vp, vp, vp]
+        L.orc_proj_set_trial.argtypes = [vp, vp]
+        L.orc_proj_get.argtypes = [vp, vp, vp, vp]
+        L.orc_proj_set.argtypes = [vp, vp, vp, vp]
+        L.orc_proj_green.argtypes = [vp]
+        L.orc_vconf_get.argtypes = [vp, vp]
+        L.orc_vconf_set.argtypes = [vp, vp]
+        L.orc_proj_update.argtypes = [vp, C.c_int, C.c_int]
+        L.orc_vconf_prop.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, C.c_int]
+        L.orc_qr_pqmc_d.argtypes = [C.c_int, C.c_int, vp, vp]
+        L.orc_qr_pqmc_d.restype = dbl
+        L.orc_eig_he_d.argtypes = [C.c_int, vp, vp, vp]
         for name in ("orc_model_dims", "orc_model_tables", "orc_model_hs", "orc_model_kinetic",
                      "orc_model_h0mat", "orc_chain_set_conf", "orc_chain_get_conf",
                      "orc_chain_set_green", "orc_chain_get_green", "orc_chain_get_diag",
@@ -115,6 +132,8 @@ def use_scipy_lapack(enable: bool = True) -> None:
     L = lib()
     if not enable:
         L.orc_set_lapack(None, None, None, None, None, None)
+        L.orc_set_zheev.argtypes = [C.c_void_p]
+        L.orc_set_zheev(None)
         return
     from scipy.linalg import cython_blas, cython_lapack
 
@@ -129,6 +148,8 @@ def use_scipy_lapack(enable: bool = True) -> None:
     L.orc_set_lapack.argtypes = [C.c_void_p] * 6
     L.orc_set_lapack(fp(cython_blas, "zgemm"), fp(cython_lapack, "zgeqrf"), fp(cython_lapack, "zgeqp3"),
                      fp(cython_lapack, "zungqr"), fp(cython_lapack, "zgetrf"), fp(cython_lapack, "ztrtri"))
+    L.orc_set_zheev.argtypes = [C.c_void_p]
+    L.orc_set_zheev(fp(cython_lapack, "zheev"))
 
 
 def make_params(**kw) -> OrcParams:
@@ -136,7 +157,8 @@ def make_params(**kw) -> OrcParams:
     d = dict(lattice=SQUARE, l1=2, l2=2, beta=20.0, dtau=0.05, rt=1.0, t2=0.0, t3=0.0, nu=0.0,
              mu=0.0, rhub=0.0, rv=0.0, alpha=0.2, theta=0.0, xmag=0.0, flux_x=0.0, flux_y=0.0,
              dimer=0.0, rndness=0.0, nflr=2, lproju=0, lstabilize=1, nwrap=10, nsweep=20, nbin=10,
-             nublock=0, update=DELAY, kinetic=CHECKERBOARD, hs=HS_GENERAL4)
+             nublock=0, update=DELAY, kinetic=CHECKERBOARD, hs=HS_GENERAL4, proj=0, lprojv=0,
+             obs_mid_len=1)
     d.update(kw)
     return OrcParams(**d)
 
@@ -151,6 +173,8 @@ class Model:
         lib().orc_model_dims(C.c_void_p(self.ptr), _ptr(dims))
         (self.ndim, self.lq, self.ltrot, self.nst, self.nublock, self.lcomp,
          self.nn_nf, self.nn_lf, self.nsub, self.z_plq) = (int(x) for x in dims)
+        self.ne = self.ndim // 2 + int(self.params.nu * self.ndim / 8.0)   # model_para.f90:376
+        self.proj = bool(self.params.proj)
 
     def __del__(self):
         if getattr(self, "ptr", None):
@@ -244,10 +268,69 @@ class Chain:
         lib().orc_chain_set_phase(self._p, z.real, z.imag)
 
     def diag(self) -> dict:
-        d = np.zeros(10)
+        d = np.zeros(12)
         lib().orc_chain_get_diag(self._p, _ptr(d))
         return dict(phase=complex(d[0], d[1]), logweight=complex(d[2], d[3]), max_wrap_error=d[4],
-                    max_phasediff=d[5], avglog10error=d[6], logcount=d[7], accepted=d[8], proposed=d[9])
+                    max_phasediff=d[5], avglog10error=d[6], logcount=d[7], accepted=d[8], proposed=d[9],
+                    accepted_v=d[10], proposed_v=d[11])
+
+    # ---- projective path ----
+    def vconf(self) -> np.ndarray:
+        m = self.model
+        v = np.zeros((m.ltrot, m.nn_nf, m.ndim), np.int32)
+        lib().orc_vconf_get(self._p, _ptr(v))
+        return v
+
+    def set_vconf(self, v: np.ndarray) -> None:
+        v = np.ascontiguousarray(v, np.int32)
+        lib().orc_vconf_set(self._p, _ptr(v))
+
+    def trial(self):
+        N = self.model.ndim
+        p = np.zeros((N, N), complex, order="F")
+        w = np.zeros(N)
+        lib().orc_proj_get_trial(self._p, _ptr(p), _ptr(w))
+        return p, w
+
+    def set_trial(self, p: np.ndarray) -> None:
+        p = np.asfortranarray(p, complex)
+        lib().orc_proj_set_trial(self._p, _ptr(p))
+
+    def proj_state(self):
+        N, ne = self.model.ndim, self.model.ne
+        ur = np.zeros((N, ne), complex, order="F")
+        ul = np.zeros((ne, N), complex, order="F")
+        li = np.zeros((ne, ne), complex, order="F")
+        lib().orc_proj_get(self._p, _ptr(ur), _ptr(ul), _ptr(li))
+        return ur, ul, li
+
+    def set_proj_state(self, ur=None, ul=None, ulrinv=None) -> None:
+        args = []
+        keep = []
+        for a in (ur, ul, ulrinv):
+            if a is None:
+                args.append(None)
+            else:
+                a = np.asfortranarray(a, complex)
+                keep.append(a)
+                args.append(_ptr(a))
+        lib().orc_proj_set(self._p, *args)
+
+    def proj_green(self) -> np.ndarray:
+        lib().orc_proj_green(self._p)
+        return self.green()
+
+    def proj_update(self, nt: int, nf: int) -> None:
+        lib().orc_proj_update(self._p, nt, nf)
+
+    def proj_sweep_start(self) -> None:
+        lib().orc_proj_sweep_start_0b(self._p)
+
+    def proj_sweep_b0(self, lupdate=True, lmeasure=True) -> None:
+        lib().orc_proj_sweep_b0(self._p, int(lupdate), int(lmeasure))
+
+    def proj_sweep_0b(self, lupdate=True, lmeasure=True) -> None:
+        lib().orc_proj_sweep_0b(self._p, int(lupdate), int(lmeasure))
 
     def uniform(self) -> float:
         return lib().orc_chain_uniform(self._p)
@@ -295,6 +378,30 @@ class Chain:
 
     def bmat_left_forward_hc(self, nt1: int, nt2: int, g: np.ndarray) -> None:
         lib().orc_bmat_left_forward_hc(self._p, nt1, nt2, _ptr(g))
+
+
+def vconf_prop(model: Model, vconf: np.ndarray, op: int, nt: int, nf: int, nflag: int, g: np.ndarray) -> None:
+    vconf = np.ascontiguousarray(vconf, np.int32)
+    assert g.dtype == complex and g.flags["F_CONTIGUOUS"]
+    n2 = g.shape[1] if op in (LEFT_FORWARD, LEFT_BACKWARD, LEFT_FORWARD_HC) else g.shape[0]
+    lib().orc_vconf_prop(C.c_void_p(model.ptr), _ptr(vconf), op, nt, nf, nflag, _ptr(g), n2)
+
+
+def qr_pqmc(a: np.ndarray):
+    """s_zgeQR_pqmc: (Q, log|det R|) with det R > 0."""
+    a = np.asfortranarray(a, complex)
+    q = np.zeros_like(a, order="F")
+    lw = lib().orc_qr_pqmc_d(a.shape[0], a.shape[1], _ptr(a), _ptr(q))
+    return q, lw
+
+
+def eig_he(h: np.ndarray):
+    h = np.asfortranarray(h, complex)
+    n = h.shape[0]
+    w = np.zeros(n)
+    v = np.zeros((n, n), complex, order="F")
+    lib().orc_eig_he_d(n, _ptr(h), _ptr(w), _ptr(v))
+    return w, v
 
 
 def unpack_bins(flat: np.ndarray, lq: int) -> dict:

@@ -1,7 +1,8 @@
 """B200-native (sm_100a) DQMC sweep for sun-hubbard (YuanyueChen/sunhubbardmy).
 
 The hot path -- local HS updates, time-slice wrap, UDV-stabilised Green's
-function and equal-time measurement of the finite-temperature sweep -- runs in
+function and equal-time measurement of the finite-temperature sweep, and the
+projective (ground-state) sweep with the t-V bond field -- runs in
 ``_lib/libdqmc_gpu.so`` behind the C ABI of ``include/dqmc_gpu.h``.  This
 package is the Python host mirror of the reference's driver and operator
 procedures; there is no CPU fallback: every call goes through the CUDA
@@ -10,6 +11,7 @@ library and fails loudly if it is missing.
 from .dqmc import (  # noqa: F401
     CHECKERBOARD, DELAY, FAST, FFT, GENERAL4, EXACT, HONEYCOMB, SQUARE, SUBMATRIX,
     Dqmc, DqmcError, DqmcParams, lib_path, load_library, qr_logdet_noalloc, read_dqmc_in, test_seed,
+    trial_state,
 )
 from .io import (  # noqa: F401
     equaltime_output, read_conf, unpack_bins, write_conf,

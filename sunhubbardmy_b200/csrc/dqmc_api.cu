@@ -7,7 +7,9 @@
 // dqmc_ft_sweep_start_0b.f90); every chain of a handle is advanced by the same
 // kernel launches (one CTA, or a few, per chain), and a full sweep is captured
 // once into a CUDA graph and replayed.
+#include <algorithm>
 #include <cmath>
+#include <thread>
 #include <complex>
 #include <cstdio>
 #include <cstring>
@@ -54,6 +56,11 @@ extern "C" int dqmc_params_derive(dqmc_params* p) {
     if (p->lproju) p->lcomp = p->nflr / 2 + 1 + (int)(0.5 * std::fabs(p->nu));
     else if (p->hs == DQMC_HS_EXACT && p->nflr == 2) p->lcomp = 2;
     else p->lcomp = 4;
+    if (p->obs_mid_len <= 0) p->obs_mid_len = 1;
+    if (p->proj && p->nst < 1) return fail(DQMC_EINVAL, "the projective sweep needs lstabilize and ltrot >= nwrap");
+    if (!p->proj && p->rv != 0.0) return fail(DQMC_EINVAL, "the t-V bond field (rv != 0) is supported on the projective path only");
+    if (p->rv < 0.0) return fail(DQMC_EINVAL, "rv must be >= 0 (acosh(exp(dtau rv / 2)))");
+    if (p->proj && (p->ne < 1 || p->ne > p->ndim)) return fail(DQMC_EINVAL, "ne out of range 1..ndim");
     return DQMC_OK;
 }
 
@@ -235,7 +242,6 @@ static void exp2x2(double d, zc z, double s, zc* out) {
 static int build_model(HostModel& m) {
     dqmc_params& p = m.p;
     if (p.t3 != 0.0) return fail(DQMC_EINVAL, "t3 != 0 is not supported");
-    if (p.rv != 0.0) return fail(DQMC_EINVAL, "nearest-neighbour V (t-V) is not supported by the finite-T GPU sweep");
     if (p.kinetic == DQMC_KIN_FFT && (p.lattice != DQMC_LATT_SQUARE || p.l1 != p.l2))
         return fail(DQMC_EINVAL, "FFT kinetic term needs a square lattice with l1 == l2");
     if (p.lattice == DQMC_LATT_SQUARE && ((p.l1 * p.l2) % 2 != 0 || p.l1 % 2 || p.l2 % 2) && p.kinetic == DQMC_KIN_CHECKERBOARD)
@@ -403,6 +409,33 @@ static int upload_model(HostModel& m) {
     d.phase_on = (p.rhub > 0.0) ? 1 : 0;
     d.rt = p.rt; d.rv = p.rv; d.t2 = p.t2; d.theta = p.theta * M_PI;
     set_hs(m, d);
+    // projective path and vconf constants (src/dqmc_config_v/dqmc_set_conf.f90:1-79)
+    d.proj = p.proj ? 1 : 0;
+    d.ne = p.ne;
+    d.lwrapv = (p.rv != 0.0);
+    d.rps = d.proj ? ((d.lwrapu ? 2 * m.N : 0) + (d.lwrapv ? 2 * m.nn_lf * m.nn_nf : 0)) : 2 * m.N;
+    if (d.lwrapv) {
+        const double etal[2] = {-1.0, 1.0};
+        double al = std::acosh(std::exp(p.dtau * p.rv * 0.5));
+        auto put = [](double2& o, zc z) { o.x = z.real(); o.y = z.imag(); };
+        for (int is = 1; is <= 2; ++is) {
+            int isp = is % 2 + 1;
+            if (p.lprojv) {
+                zc z = std::exp(zc(0, M_PI * 2.0 * is / 2.0));
+                put(d.vbp[is - 1], z); put(d.vbm[is - 1], z);
+                put(d.vbpi[is - 1], std::conj(z)); put(d.vbmi[is - 1], std::conj(z));
+                put(d.vdp[is - 1], std::exp(zc(0, M_PI * (2.0 * isp - 2.0 * is) / 2.0)) - 1.0);
+                put(d.vdm[is - 1], zc(std::exp(al * (etal[isp - 1] - etal[is - 1])) - 1.0, 0.0));
+            } else {
+                put(d.vbp[is - 1], zc(std::exp(al * etal[is - 1]), 0.0));
+                put(d.vbpi[is - 1], zc(std::exp(-al * etal[is - 1]), 0.0));
+                put(d.vbm[is - 1], zc(std::exp(-al * etal[is - 1]), 0.0));
+                put(d.vbmi[is - 1], zc(std::exp(al * etal[is - 1]), 0.0));
+                put(d.vdp[is - 1], zc(std::exp(al * (etal[isp - 1] - etal[is - 1])) - 1.0, 0.0));
+                put(d.vdm[is - 1], zc(std::exp(-al * (etal[isp - 1] - etal[is - 1])) - 1.0, 0.0));
+            }
+        }
+    }
     int rc;
     if ((rc = upload(m, m.bond_i1, &d.bond_i1))) return rc;
     if ((rc = upload(m, m.bond_i2, &d.bond_i2))) return rc;
@@ -480,6 +513,196 @@ struct HostSfmt {
     double stream() { return ((double)next() + 0.5) * (1.0 / 4294967296.0); }
 };
 
+// ---------------------------------------------------------------------------
+// trial state of the projective path (dqmc_set_proj, src/dqmc_proj_core/
+// dqmc_set_proj.f90:1-78, with set_trial_h0, src/dqmc_config_h0/
+// set_trial_h0.f90:1-29).  The Hermitian eigenproblem (s_eig_he / zheev in
+// the reference) is solved on the host: Householder reduction to a real
+// symmetric tridiagonal matrix (reflectors with a real beta, as in LAPACK's
+// zhetrd), then the implicit QL iteration with Wilkinson-type shifts of the
+// EISPACK tql2 procedure, accumulated into the complex eigenvectors.
+// ---------------------------------------------------------------------------
+static void eig_herm(int n, std::vector<zc>& a, std::vector<double>& w) {
+    // a: n x n Hermitian (column-major) in, eigenvectors (columns) out
+    std::vector<zc> q(n * n, 0.0), v(n), pv(n), row(n);
+    for (int i = 0; i < n; ++i) q[i + i * n] = 1.0;
+    std::vector<double> d(n), e(n, 0.0);
+    auto A = [&](int i, int j) -> zc& { return a[i + (size_t)j * n]; };
+    for (int k = 0; k + 2 < n; ++k) {
+        int m = n - k - 1;                     // reflector acts on rows/cols k+1..n-1
+        zc alpha = A(k + 1, k);
+        double xn2 = 0.0;
+        for (int i = k + 2; i < n; ++i) xn2 += std::norm(A(i, k));
+        double xnorm = std::sqrt(xn2);
+        zc tau = 0.0;
+        if (!(xnorm == 0.0 && alpha.imag() == 0.0)) {
+            double beta = -std::copysign(std::sqrt(std::norm(alpha) + xn2), alpha.real());
+            tau = zc((beta - alpha.real()) / beta, -alpha.imag() / beta);
+            zc scal = 1.0 / (alpha - beta);
+            v[0] = 1.0;
+            for (int i = 1; i < m; ++i) v[i] = A(k + 1 + i, k) * scal;
+            // B <- B H (B = trailing block), H = I - tau v v^H
+            for (int i = 0; i < m; ++i) pv[i] = 0.0;
+            for (int j = 0; j < m; ++j) {
+                zc vj = v[j];
+                const zc* col = &A(k + 1, k + 1 + j);
+                for (int i = 0; i < m; ++i) pv[i] += col[i] * vj;
+            }
+            for (int j = 0; j < m; ++j) {
+                zc f = tau * std::conj(v[j]);
+                for (int i = 0; i < m; ++i) A(k + 1 + i, k + 1 + j) -= pv[i] * f;
+            }
+            // B <- H^H B
+            for (int j = 0; j < m; ++j) {
+                zc s = 0.0;
+                for (int i = 0; i < m; ++i) s += std::conj(v[i]) * A(k + 1 + i, k + 1 + j);
+                row[j] = s;
+            }
+            for (int j = 0; j < m; ++j) {
+                zc f = std::conj(tau) * row[j];
+                for (int i = 0; i < m; ++i) A(k + 1 + i, k + 1 + j) -= v[i] * f;
+            }
+            // Q <- Q H
+            std::vector<zc>& qs = row;
+            for (int i = 0; i < n; ++i) qs[i] = 0.0;
+            for (int j = 0; j < m; ++j) {
+                zc vj = v[j];
+                const zc* col = &q[(size_t)(k + 1 + j) * n];
+                for (int i = 0; i < n; ++i) qs[i] += col[i] * vj;
+            }
+            for (int j = 0; j < m; ++j) {
+                zc f = tau * std::conj(v[j]);
+                zc* col = &q[(size_t)(k + 1 + j) * n];
+                for (int i = 0; i < n; ++i) col[i] -= qs[i] * f;
+            }
+            alpha = beta;
+        }
+        e[k] = alpha.real();                 // real after the reflection (or already real)
+        // a complex subdiagonal left by a zero reflector is made real by a phase
+        if (alpha.imag() != 0.0) e[k] = std::abs(alpha);
+        if (alpha.imag() != 0.0) {
+            zc ph = alpha / std::abs(alpha);  // scale basis vector k+1 by ph
+            for (int j = 0; j < n; ++j) A(k + 1, j) *= std::conj(ph);
+            for (int i = 0; i < n; ++i) A(i, k + 1) *= ph;
+            for (int i = 0; i < n; ++i) q[i + (size_t)(k + 1) * n] *= ph;
+        }
+    }
+    if (n >= 2) {
+        zc last = A(n - 1, n - 2);
+        if (last.imag() != 0.0) {
+            zc ph = last / std::abs(last);
+            for (int j = 0; j < n; ++j) A(n - 1, j) *= std::conj(ph);
+            for (int i = 0; i < n; ++i) A(i, n - 1) *= ph;
+            for (int i = 0; i < n; ++i) q[i + (size_t)(n - 1) * n] *= ph;
+        }
+        e[n - 2] = A(n - 1, n - 2).real();
+    }
+    for (int i = 0; i < n; ++i) d[i] = A(i, i).real();
+    // implicit QL on (d, e), e[i] couples i and i+1
+    const double eps = 2.220446049250313e-16;
+    for (int l = 0; l < n; ++l) {
+        for (int iter = 0; iter < 60; ++iter) {
+            int mm = l;
+            for (; mm < n - 1; ++mm) {
+                double dd = std::fabs(d[mm]) + std::fabs(d[mm + 1]);
+                if (std::fabs(e[mm]) <= eps * dd) break;
+            }
+            if (mm == l) break;
+            double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+            double r = std::hypot(g, 1.0);
+            g = d[mm] - d[l] + e[l] / (g + std::copysign(r, g));
+            double sn = 1.0, cs = 1.0, pp = 0.0;
+            int i = mm - 1;
+            bool underflow = false;
+            for (; i >= l; --i) {
+                double f = sn * e[i], b = cs * e[i];
+                r = std::hypot(f, g);
+                e[i + 1] = r;
+                if (r == 0.0) { d[i + 1] -= pp; e[mm] = 0.0; underflow = true; break; }
+                sn = f / r; cs = g / r;
+                g = d[i + 1] - pp;
+                r = (d[i] - g) * sn + 2.0 * cs * b;
+                pp = sn * r;
+                d[i + 1] = g + pp;
+                g = cs * r - b;
+                for (int k = 0; k < n; ++k) {
+                    zc fz = q[k + (size_t)(i + 1) * n];
+                    q[k + (size_t)(i + 1) * n] = sn * q[k + (size_t)i * n] + cs * fz;
+                    q[k + (size_t)i * n] = cs * q[k + (size_t)i * n] - sn * fz;
+                }
+            }
+            if (underflow) continue;
+            d[l] -= pp; e[l] = g; e[mm] = 0.0;
+        }
+    }
+    // ascending order
+    std::vector<int> idx(n);
+    for (int i = 0; i < n; ++i) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return d[x] < d[y]; });
+    w.resize(n);
+    for (int j = 0; j < n; ++j) {
+        w[j] = d[idx[j]];
+        for (int i = 0; i < n; ++i) a[i + (size_t)j * n] = q[i + (size_t)idx[j] * n];
+    }
+}
+
+// set_trial_h0: nn_lf * nn_nf draws in (bond, family) order, then -mu
+static void trial_hamiltonian(const HostModel& m, HostSfmt& rng, std::vector<zc>& H) {
+    const dqmc_params& p = m.p;
+    int N = m.N;
+    H.assign((size_t)N * N, 0.0);
+    for (int b = 0; b < m.nn_lf; ++b) {
+        int i0 = m.nnlf[b];
+        for (int f = 1; f <= m.nn_nf; ++f) {
+            int in = m.nnlist[i0 * m.nn_nf + f - 1];
+            double r = rng.stream();
+            zc z1 = (-p.rt + p.rndness * (r - 1.0)) * m.expar[i0 * m.nn_nf + f - 1];
+            H[i0 + (size_t)in * N] += z1;
+            H[in + (size_t)i0 * N] += std::conj(z1);
+        }
+    }
+    for (int i = 0; i < N; ++i) H[i + (size_t)i * N] -= p.mu;
+}
+
+// the fresh-start draws of one chain, in the reference's order: U field
+// (uconf%input_conf), bond field (vconf%input_conf), then the trial hopping
+static void draw_fields(const HostModel& m, HostSfmt& rng, int draw_conf, std::vector<int32_t>& conf,
+                        std::vector<int32_t>& vconf) {
+    int N = m.N, lt = m.p.ltrot, nnf = m.nn_nf;
+    conf.assign((size_t)lt * N, 1);
+    if (draw_conf && m.p.rhub != 0.0)
+        for (size_t e = 0; e < conf.size(); ++e) conf[e] = (int32_t)std::ceil(rng.stream() * m.lcomp);
+    vconf.clear();
+    if (m.p.rv != 0.0) {
+        vconf.assign((size_t)lt * nnf * N, 1);
+        if (draw_conf)
+            for (int nt = 0; nt < lt; ++nt)
+                for (int i = 0; i < N; ++i)
+                    for (int f = 0; f < nnf; ++f)
+                        vconf[((size_t)nt * nnf + f) * N + i] = (int32_t)std::ceil(rng.stream() * 2);
+    }
+}
+
+extern "C" int dqmc_trial_state(const dqmc_params* pin, int32_t seed, int draw_conf, double* proj, double* w) {
+    if (!pin || !proj) return fail(DQMC_EINVAL, "null argument");
+    HostModel m;
+    m.p = *pin;
+    int rc = dqmc_params_derive(&m.p);
+    if (rc) return rc;
+    if ((rc = build_model(m))) return rc;
+    HostSfmt rng;
+    sfmt_seed(rng.st, seed);
+    std::vector<int32_t> conf, vconf;
+    draw_fields(m, rng, draw_conf, conf, vconf);
+    std::vector<zc> H;
+    trial_hamiltonian(m, rng, H);
+    std::vector<double> ww;
+    eig_herm(m.N, H, ww);
+    memcpy(proj, H.data(), H.size() * sizeof(zc));
+    if (w) memcpy(w, ww.data(), ww.size() * sizeof(double));
+    return DQMC_OK;
+}
+
 // host-only view of the model tables (no device needed)
 extern "C" int dqmc_model_tables(const dqmc_params* pin, int32_t* nnlist, int32_t* nnlf_list, int32_t* list,
                                  int32_t* imj, int32_t* plq_cord, int32_t* snlist, double* urt, double* exph0k) {
@@ -508,6 +731,8 @@ extern "C" int dqmc_model_tables(const dqmc_params* pin, int32_t* nnlist, int32_
 struct ChainHost {
     int model;
     ChainDev dev;
+    std::vector<zc> trial;           // projective path: trial eigenvectors (N x N)
+    std::vector<double> trial_w;     // and eigenvalues
 };
 
 struct dqmc_handle {
@@ -525,6 +750,7 @@ struct dqmc_handle {
     double last_ms = 0.0;
     int ctas_per_chain = 1;
     size_t graph_nodes = 0;
+    int proj = 0;
 };
 
 static void* dalloc(dqmc_handle* h, size_t bytes) {
@@ -545,6 +771,18 @@ extern "C" int dqmc_gpu_destroy(dqmc_handle* h) {
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->st) cudaStreamDestroy(h->st);
     delete h;
+    return DQMC_OK;
+}
+
+// projR = first ne trial vectors, projLc = their complex conjugate (UL^T of P^H)
+static int upload_trial(dqmc_handle* h, int c) {
+    ChainHost& ch = h->chains[c];
+    const HostModel& m = *h->models[ch.model];
+    int N = m.N, ne = m.p.ne;
+    std::vector<zc> pr((size_t)N * ne), pl((size_t)N * ne);
+    for (size_t e = 0; e < pr.size(); ++e) { pr[e] = ch.trial[e]; pl[e] = std::conj(ch.trial[e]); }
+    CK(cudaMemcpy(ch.dev.projR, pr.data(), pr.size() * sizeof(zc), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ch.dev.projLc, pl.data(), pl.size() * sizeof(zc), cudaMemcpyHostToDevice));
     return DQMC_OK;
 }
 
@@ -574,9 +812,11 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
             dqmc_gpu_destroy(h);
             return fail(DQMC_EINVAL, "all parameter sets of a handle must share ltrot and nwrap");
         } else if (m->p.lattice != h->models[0]->p.lattice || m->p.kinetic != h->models[0]->p.kinetic ||
-                   (m->p.rt == 0.0) != (h->models[0]->p.rt == 0.0) || (m->p.rhub == 0.0) != (h->models[0]->p.rhub == 0.0)) {
+                   (m->p.rt == 0.0) != (h->models[0]->p.rt == 0.0) || (m->p.rhub == 0.0) != (h->models[0]->p.rhub == 0.0) ||
+                   (m->p.rv == 0.0) != (h->models[0]->p.rv == 0.0) || (m->p.proj != 0) != (h->models[0]->p.proj != 0)) {
             dqmc_gpu_destroy(h);
-            return fail(DQMC_EINVAL, "all parameter sets of a handle must share lattice kind and kinetic propagator");
+            return fail(DQMC_EINVAL, "all parameter sets of a handle must share lattice kind, kinetic propagator, "
+                                     "the presence of the U / V / hopping terms and the projective flag");
         }
         if ((rc = upload_model(*m))) { dqmc_gpu_destroy(h); return rc; }
         h->maxN = std::max(h->maxN, m->N);
@@ -594,6 +834,8 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
         cudaMemcpy(h->d_slotmap, sm.data(), sizeof(int) * (nst + 2), cudaMemcpyHostToDevice);
     }
     h->chains.resize(n_chains);
+    h->proj = h->models[0]->p.proj != 0;
+    std::vector<std::vector<zc>> trial_H(n_chains);
     for (int c = 0; c < n_chains; ++c) {
         HostModel* m = h->models[model_of[c % n_params]];
         ChainHost& ch = h->chains[c];
@@ -604,15 +846,34 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
         size_t NN = (size_t)N * N, z = sizeof(double2);
         d.md = m->d_dev;
         d.N = N;
+        const bool proj = m->p.proj != 0;
+        const int ne = m->p.ne, nnf = m->nn_nf;
         d.G = (double2*)dalloc(h, NN * z);
         d.Gnew = (double2*)dalloc(h, NN * z);
         for (int k = 0; k < 6; ++k) d.W[k] = (double2*)dalloc(h, NN * z);
-        d.U = (double2*)dalloc(h, (size_t)(nst + 2) * NN * z);
-        d.V = (double2*)dalloc(h, (size_t)(nst + 2) * NN * z);
-        d.D = (double*)dalloc(h, (size_t)(nst + 2) * N * sizeof(double));
-        d.logdetQ = (double2*)dalloc(h, (size_t)(nst + 2) * z);
-        d.A = (double2*)dalloc(h, (size_t)N * m->nublock_dev * z);
-        d.B = (double2*)dalloc(h, (size_t)N * m->nublock_dev * z);
+        if (!proj) {
+            d.U = (double2*)dalloc(h, (size_t)(nst + 2) * NN * z);
+            d.V = (double2*)dalloc(h, (size_t)(nst + 2) * NN * z);
+            d.D = (double*)dalloc(h, (size_t)(nst + 2) * N * sizeof(double));
+            d.logdetQ = (double2*)dalloc(h, (size_t)(nst + 2) * z);
+            d.A = (double2*)dalloc(h, (size_t)N * m->nublock_dev * z);
+            d.B = (double2*)dalloc(h, (size_t)N * m->nublock_dev * z);
+        } else {
+            size_t Nne = (size_t)N * ne;
+            d.UR = (double2*)dalloc(h, Nne * z);
+            d.ULT = (double2*)dalloc(h, Nne * z);
+            d.ULRINV = (double2*)dalloc(h, (size_t)ne * ne * z);
+            d.Pst = (double2*)dalloc(h, (size_t)(nst + 1) * Nne * z);
+            d.projR = (double2*)dalloc(h, Nne * z);
+            d.projLc = (double2*)dalloc(h, Nne * z);
+            d.logwDV = (double*)dalloc(h, (size_t)(nst + 2) * sizeof(double));
+            d.pw = (double2*)dalloc(h, ((size_t)5 * 32 * ne + 2 * 32 * 32) * z);
+            if (!d.UR || !d.ULT || !d.ULRINV || !d.Pst || !d.projR || !d.projLc || !d.logwDV || !d.pw) {
+                dqmc_gpu_destroy(h);
+                return fail(DQMC_ENOMEM, "device allocation failed");
+            }
+        }
+        if (m->p.rv != 0.0) d.vconf = (int32_t*)dalloc(h, (size_t)lt * nnf * N * sizeof(int32_t));
         d.tau = (double2*)dalloc(h, (size_t)N * z);
         d.T = (double2*)dalloc(h, (size_t)(N / 16 + 1) * 256 * z);
         d.smallw = (double2*)dalloc(h, (size_t)32 * N * z);
@@ -620,25 +881,46 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
         d.perm = (int*)dalloc(h, (size_t)N * sizeof(int));
         d.conf = (int32_t*)dalloc(h, (size_t)lt * N * sizeof(int32_t));
         d.sfmt = (uint32_t*)dalloc(h, 625 * sizeof(uint32_t));
-        d.rnd = (uint32_t*)dalloc(h, (size_t)lt * 2 * N * sizeof(uint32_t));
+        d.rnd = (uint32_t*)dalloc(h, (size_t)lt * std::max(2 * N, m->dev.rps) * sizeof(uint32_t));
         d.bins = (double2*)dalloc(h, (size_t)(10 + 20 * m->lq + 4) * z);
         d.stats = (double*)dalloc(h, ST_COUNT * sizeof(double));
         d.slotmap = h->d_slotmap;
-        if (!d.G || !d.Gnew || !d.W[5] || !d.U || !d.V || !d.D || !d.rnd || !d.stats || !d.bins) {
+        if (!d.G || !d.Gnew || !d.W[5] || (!proj && (!d.U || !d.V || !d.D)) || !d.rnd || !d.stats || !d.bins ||
+            (m->p.rv != 0.0 && !d.vconf)) {
             dqmc_gpu_destroy(h);
             return fail(DQMC_ENOMEM, "device allocation failed");
         }
-        // generator state and fresh-start field
+        // generator state and fresh-start fields, drawn in the reference's order
         HostSfmt rng;
         sfmt_seed(rng.st, seeds ? seeds[c] : 0);
-        std::vector<int32_t> conf((size_t)lt * N, 1);
-        if (draw_conf)
-            for (size_t e = 0; e < conf.size(); ++e) conf[e] = (int32_t)std::ceil(rng.stream() * m->lcomp);
+        std::vector<int32_t> conf, vconf;
+        draw_fields(*m, rng, draw_conf, conf, vconf);
+        if (proj) {
+            trial_hamiltonian(*m, rng, trial_H[c]);
+        }
         cudaMemcpy(d.sfmt, rng.st, 625 * sizeof(uint32_t), cudaMemcpyHostToDevice);
         cudaMemcpy(d.conf, conf.data(), conf.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+        if (!vconf.empty()) cudaMemcpy(d.vconf, vconf.data(), vconf.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
         double stats[ST_COUNT] = {0};
         stats[ST_PHASE_RE] = 1.0;
         cudaMemcpy(d.stats, stats, sizeof(stats), cudaMemcpyHostToDevice);
+    }
+    if (h->proj) {
+        // eigenvectors of every walker's trial Hamiltonian, on the host cores
+        unsigned nth = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+        std::vector<std::vector<double>> ws(n_chains);
+        std::vector<std::thread> pool;
+        for (unsigned t = 0; t < nth; ++t)
+            pool.emplace_back([&, t]() {
+                for (int c = (int)t; c < n_chains; c += (int)nth) eig_herm(h->chains[c].dev.N, trial_H[c], ws[c]);
+            });
+        for (auto& th : pool) th.join();
+        for (int c = 0; c < n_chains; ++c) {
+            h->chains[c].trial = std::move(trial_H[c]);
+            h->chains[c].trial_w = std::move(ws[c]);
+            int rc2 = upload_trial(h, c);
+            if (rc2) { dqmc_gpu_destroy(h); return rc2; }
+        }
     }
     h->d_chains = (ChainDev*)dalloc(h, sizeof(ChainDev) * n_chains);
     {
@@ -647,6 +929,7 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
         cudaMemcpy(h->d_chains, v.data(), sizeof(ChainDev) * n_chains, cudaMemcpyHostToDevice);
     }
     set_stab_maxN(h->maxN);
+    if (h->proj) set_proj_maxN(h->maxN);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
     h->ctas_per_chain = std::max(1, std::min(h->maxN / 16, (2 * sms + n_chains - 1) / n_chains));
@@ -732,8 +1015,193 @@ static void stab_b0(dqmc_handle* h, int n) {
     launch_swap_slots(h->d_slotmap, n, spare, h->st);
 }
 
+// ---------------------------------------------------------------------------
+// projective path (src/dqmc_proj_core/): pending propagation ops of UR (left
+// multiplications) and UL^T (right multiplications) are collected and run as
+// one pass each whenever an update, a measurement or a stabilisation needs
+// the current matrices.
+// ---------------------------------------------------------------------------
+enum { PMAT_W3 = 5, PMAT_UR = 10, PMAT_ULT = 11, PMAT_PROJR = 12, PMAT_PROJLC = 13, PMAT_ULRINV = 14,
+       PMAT_PST0 = 1000, PMAT_G = 0, PMAT_GNEW = 1 };
+
+struct ProjPass {
+    PropProg r, l;   // r: ops on UR (left), l: ops on UL^T (right)
+    ProjPass() { r.n = 0; l.n = 0; }
+};
+
+static void pflush(dqmc_handle* h, ProjPass& pp) {
+    if (pp.r.n) launch_prop_tall(h->d_chains, h->nch, h->maxN, PMAT_UR, pp.r, 0, h->ctas_per_chain, h->st);
+    if (pp.l.n) launch_prop_tall(h->d_chains, h->nch, h->maxN, PMAT_ULT, pp.l, 1, h->ctas_per_chain, h->st);
+    pp.r.n = 0; pp.l.n = 0;
+}
+static void padd(dqmc_handle* h, ProjPass& pp, PropProg& p, int kind, int which, int nf, int nt) {
+    if (p.n >= DQ_MAX_PROG) pflush(h, pp);
+    prog_add(p, kind, which, nf, nt);
+}
+// kinetic half step: families 1..nnf (or reversed) with urt (which = PW_FWD) or urtm1
+static void pk(dqmc_handle* h, ProjPass& pp, PropProg& p, int which, int reversed) {
+    const HostModel& m = *h->models[0];
+    if (m.p.rt == 0.0) return;
+    if (m.p.kinetic == DQMC_KIN_FFT) { padd(h, pp, p, PK_FFT, which, 0, 0); return; }
+    for (int k = 1; k <= m.nn_nf; ++k) padd(h, pp, p, PK_CB, which, reversed ? m.nn_nf + 1 - k : k, 0);
+}
+
+static bool proj_mid(const HostModel& m, int nt) {
+    int lt = m.p.ltrot, len = m.p.obs_mid_len;
+    return nt > (lt / 2 - (len + 1) / 2) && nt <= (lt / 2 + len / 2);
+}
+
+// ULRINV = (UL UR)^-1 fresh, G = I - UR ULRINV UL, equaltime_measure
+static void proj_measure(dqmc_handle* h) {
+    launch_proj_ulr(h->d_chains, h->nch, PMAT_ULRINV, 0, 0, -1, h->st);
+    launch_proj_green(h->d_chains, h->nch, PMAT_ULRINV, PMAT_G, h->ctas_per_chain, h->st);
+    launch_measure(h->d_chains, h->nch, h->ctas_per_chain, h->st);
+}
+
+// G of the current (UL, UR) into G, before a stabilisation replaces them
+static void proj_old_green(dqmc_handle* h) {
+    launch_proj_ulr(h->d_chains, h->nch, PMAT_W3, 0, 0, -1, h->st);
+    launch_proj_green(h->d_chains, h->nch, PMAT_W3, PMAT_G, h->ctas_per_chain, h->st);
+}
+
+// dqmc_proj_sweep_0b.f90:133-190 at wrap point n
+static void stab_proj_0b(dqmc_handle* h, int n) {
+    int nst = h->nst;
+    proj_old_green(h);
+    launch_tall_copy(h->d_chains, h->nch, PMAT_ULT, PMAT_PST0 + n, h->st);
+    launch_proj_qr(h->d_chains, h->nch, PMAT_UR, n, n - 1, h->st);
+    launch_proj_ulr(h->d_chains, h->nch, PMAT_ULRINV, 1, n, n == nst ? -1 : n + 1, h->st);
+    launch_proj_green(h->d_chains, h->nch, PMAT_ULRINV, PMAT_GNEW, h->ctas_per_chain, h->st);
+    launch_wrap_check(h->d_chains, h->nch, 1, h->st);
+    launch_tall_copy(h->d_chains, h->nch, PMAT_PST0 + n, PMAT_UR, h->st);
+}
+
+// dqmc_proj_sweep_b0.f90:128-190 at wrap point n
+static void stab_proj_b0(dqmc_handle* h, int n) {
+    int nst = h->nst;
+    proj_old_green(h);
+    launch_tall_copy(h->d_chains, h->nch, PMAT_UR, PMAT_PST0 + n, h->st);
+    launch_proj_qr(h->d_chains, h->nch, PMAT_ULT, n + 1, (n + 1 == nst) ? -1 : n + 2, h->st);
+    launch_proj_ulr(h->d_chains, h->nch, PMAT_ULRINV, 1, n + 1, n == 0 ? -1 : n, h->st);
+    launch_proj_green(h->d_chains, h->nch, PMAT_ULRINV, PMAT_GNEW, h->ctas_per_chain, h->st);
+    launch_wrap_check(h->d_chains, h->nch, 1, h->st);
+    launch_tall_copy(h->d_chains, h->nch, PMAT_PST0 + n, PMAT_ULT, h->st);
+}
+
+// Bmat_left_forward on UR over slices nt2..nt1 (src/dqmc_proj_core.f90:61-104)
+static void proj_bmat(dqmc_handle* h, ProjPass& pp, int nt1, int nt2) {
+    const HostModel& m = *h->models[0];
+    for (int nt = nt2; nt <= nt1; ++nt) {
+        pk(h, pp, pp.r, PW_FWD, 0);
+        if (m.p.rv != 0.0)
+            for (int nf = 1; nf <= m.nn_nf; ++nf) {
+                padd(h, pp, pp.r, PK_VMIX, 0, nf, nt);
+                padd(h, pp, pp.r, PK_VSCALE, PW_FWD, nf, nt);
+                padd(h, pp, pp.r, PK_VMIX, 0, nf, nt);
+            }
+        if (m.p.rhub != 0.0) padd(h, pp, pp.r, PK_DIAG, PW_FWD, 0, nt);
+        pk(h, pp, pp.r, PW_FWD, 1);
+    }
+}
+
+// dqmc_proj_sweep_start_0b (src/dqmc_proj_core/dqmc_proj_sweep_start_0b.f90:1-48)
+static int proj_sweep_start(dqmc_handle* h) {
+    const HostModel& m = *h->models[0];
+    int nst = h->nst;
+    launch_tall_copy(h->d_chains, h->nch, PMAT_UR, PMAT_PROJR, h->st);
+    launch_tall_copy(h->d_chains, h->nch, PMAT_PST0 + nst, PMAT_PROJLC, h->st);
+    for (int n = 1; n <= nst; ++n) {
+        ProjPass pp;
+        proj_bmat(h, pp, m.wrap_step[(n - 1) * 2 + 1], m.wrap_step[(n - 1) * 2]);
+        pflush(h, pp);
+        launch_proj_qr(h->d_chains, h->nch, PMAT_UR, n, n - 1, h->st);
+        launch_tall_copy(h->d_chains, h->nch, PMAT_PST0 + n, PMAT_UR, h->st);
+    }
+    launch_tall_copy(h->d_chains, h->nch, PMAT_ULT, PMAT_PROJLC, h->st);
+    launch_proj_ulr(h->d_chains, h->nch, PMAT_ULRINV, 1, nst, -1, h->st);
+    launch_proj_green(h->d_chains, h->nch, PMAT_ULRINV, PMAT_GNEW, h->ctas_per_chain, h->st);
+    launch_wrap_check(h->d_chains, h->nch, 0, h->st);
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaGetLastError());
+    h->started = 1;
+    return DQMC_OK;
+}
+
+// dqmc_proj_sweep_b0 (src/dqmc_proj_core/dqmc_proj_sweep_b0.f90:1-220)
+static void enqueue_proj_b0(dqmc_handle* h, int lupdate, int lmeasure) {
+    const HostModel& m = *h->models[0];
+    int lt = h->ltrot, nnf = m.nn_nf;
+    bool lu = m.p.rhub != 0.0, lv = m.p.rv != 0.0;
+    launch_tall_copy(h->d_chains, h->nch, PMAT_ULT, PMAT_PROJLC, h->st);
+    launch_tall_copy(h->d_chains, h->nch, PMAT_PST0 + 0, PMAT_PROJR, h->st);
+    if (lupdate && (lu || lv)) launch_sfmt(h->d_chains, h->nch, lt, h->st);
+    ProjPass pp;
+    for (int nt = lt; nt >= 1; --nt) {
+        int visit = lt - nt;
+        if (lmeasure && proj_mid(m, nt)) { pflush(h, pp); proj_measure(h); }
+        pk(h, pp, pp.r, PW_INV, 0);     // h0 left_backward on UR
+        pk(h, pp, pp.l, PW_FWD, 0);     // h0 right_forward on UL
+        if (lu) {
+            if (lupdate) { pflush(h, pp); launch_proj_update(h->d_chains, h->nch, nt, 0, visit, 1, -1, h->st); }
+            padd(h, pp, pp.l, PK_DIAG, PW_FWD, 0, nt);
+            padd(h, pp, pp.r, PK_DIAG, PW_INV, 0, nt);
+        }
+        if (lv)
+            for (int nf = nnf; nf >= 1; --nf) {
+                padd(h, pp, pp.l, PK_VMIX, 0, nf, nt);           // right_forward, nflag 2
+                padd(h, pp, pp.r, PK_VMIX, 0, nf, nt);           // left_backward, nflag 2
+                if (lupdate) { pflush(h, pp); launch_proj_update(h->d_chains, h->nch, nt, nf, visit, 1, -1, h->st); }
+                padd(h, pp, pp.l, PK_VSCALE, PW_FWD, nf, nt);    // right_forward, nflag 1
+                padd(h, pp, pp.l, PK_VMIX, 0, nf, nt);
+                padd(h, pp, pp.r, PK_VSCALE, PW_INV, nf, nt);    // left_backward, nflag 1
+                padd(h, pp, pp.r, PK_VMIX, 0, nf, nt);
+            }
+        pk(h, pp, pp.r, PW_INV, 1);
+        pk(h, pp, pp.l, PW_FWD, 1);
+        if ((m.iwrap_nt[nt - 1] > 0 || m.p.nwrap == 1) || nt == 1) { pflush(h, pp); stab_proj_b0(h, m.iwrap_nt[nt - 1]); }
+    }
+    pflush(h, pp);
+}
+
+// dqmc_proj_sweep_0b (src/dqmc_proj_core/dqmc_proj_sweep_0b.f90:1-235), lmeasure_dyn off
+static void enqueue_proj_0b(dqmc_handle* h, int lupdate, int lmeasure) {
+    const HostModel& m = *h->models[0];
+    int lt = h->ltrot, nnf = m.nn_nf, nst = h->nst;
+    bool lu = m.p.rhub != 0.0, lv = m.p.rv != 0.0;
+    launch_tall_copy(h->d_chains, h->nch, PMAT_UR, PMAT_PROJR, h->st);
+    launch_tall_copy(h->d_chains, h->nch, PMAT_PST0 + nst, PMAT_PROJLC, h->st);
+    if (lupdate && (lu || lv)) launch_sfmt(h->d_chains, h->nch, lt, h->st);
+    ProjPass pp;
+    for (int nt = 1; nt <= lt; ++nt) {
+        int visit = nt - 1;
+        pk(h, pp, pp.r, PW_FWD, 0);     // h0 left_forward on UR
+        pk(h, pp, pp.l, PW_INV, 0);     // h0 right_backward on UL
+        if (lv)
+            for (int nf = 1; nf <= nnf; ++nf) {
+                padd(h, pp, pp.r, PK_VMIX, 0, nf, nt);           // left_forward, nflag 2
+                padd(h, pp, pp.r, PK_VSCALE, PW_FWD, nf, nt);
+                padd(h, pp, pp.l, PK_VMIX, 0, nf, nt);           // right_backward, nflag 2
+                padd(h, pp, pp.l, PK_VSCALE, PW_INV, nf, nt);
+                if (lupdate) { pflush(h, pp); launch_proj_update(h->d_chains, h->nch, nt, nf, visit, 0, -1, h->st); }
+                padd(h, pp, pp.r, PK_VMIX, 0, nf, nt);           // nflag 1
+                padd(h, pp, pp.l, PK_VMIX, 0, nf, nt);
+            }
+        if (lu) {
+            padd(h, pp, pp.r, PK_DIAG, PW_FWD, 0, nt);
+            padd(h, pp, pp.l, PK_DIAG, PW_INV, 0, nt);
+            if (lupdate) { pflush(h, pp); launch_proj_update(h->d_chains, h->nch, nt, 0, visit, 0, -1, h->st); }
+        }
+        pk(h, pp, pp.r, PW_FWD, 1);
+        pk(h, pp, pp.l, PW_INV, 1);
+        if (lmeasure && proj_mid(m, nt)) { pflush(h, pp); proj_measure(h); }
+        if (m.iwrap_nt[nt] > 0) { pflush(h, pp); stab_proj_0b(h, m.iwrap_nt[nt]); }
+    }
+    pflush(h, pp);
+}
+
 extern "C" int dqmc_gpu_sweep_start(dqmc_handle* h) {
     if (!h) return fail(DQMC_EINVAL, "null handle");
+    if (h->proj) return proj_sweep_start(h);
     const HostModel& m = *h->models[0];
     {
         std::vector<int> sm(h->nst + 2);
@@ -808,7 +1276,8 @@ static void enqueue_0b(dqmc_handle* h, int lupdate, int lmeasure) {
 extern "C" int dqmc_gpu_sweep_b0(dqmc_handle* h, int lupdate, int lmeasure) {
     if (!h) return fail(DQMC_EINVAL, "null handle");
     if (!h->started) return fail(DQMC_ESTATE, "sweep before sweep_start");
-    enqueue_b0(h, lupdate, lmeasure);
+    if (h->proj) enqueue_proj_b0(h, lupdate, lmeasure);
+    else enqueue_b0(h, lupdate, lmeasure);
     CK(cudaStreamSynchronize(h->st));
     CK(cudaGetLastError());
     return DQMC_OK;
@@ -817,7 +1286,8 @@ extern "C" int dqmc_gpu_sweep_b0(dqmc_handle* h, int lupdate, int lmeasure) {
 extern "C" int dqmc_gpu_sweep_0b(dqmc_handle* h, int lupdate, int lmeasure) {
     if (!h) return fail(DQMC_EINVAL, "null handle");
     if (!h->started) return fail(DQMC_ESTATE, "sweep before sweep_start");
-    enqueue_0b(h, lupdate, lmeasure);
+    if (h->proj) enqueue_proj_0b(h, lupdate, lmeasure);
+    else enqueue_0b(h, lupdate, lmeasure);
     CK(cudaStreamSynchronize(h->st));
     CK(cudaGetLastError());
     return DQMC_OK;
@@ -831,8 +1301,13 @@ extern "C" int dqmc_gpu_sweeps(dqmc_handle* h, int n, int lmeasure) {
         if (h->sweep_graph) { cudaGraphExecDestroy(h->sweep_graph); h->sweep_graph = nullptr; }
         cudaGraph_t g;
         CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
-        enqueue_b0(h, 1, lmeasure);
-        enqueue_0b(h, 1, lmeasure);
+        if (h->proj) {
+            enqueue_proj_b0(h, 1, lmeasure);
+            enqueue_proj_0b(h, 1, lmeasure);
+        } else {
+            enqueue_b0(h, 1, lmeasure);
+            enqueue_0b(h, 1, lmeasure);
+        }
         CK(cudaStreamEndCapture(h->st, &g));
         CK(cudaGraphInstantiate(&h->sweep_graph, g, 0));
         size_t nn = 0;
@@ -1009,6 +1484,7 @@ extern "C" int dqmc_gpu_get_diag(dqmc_handle* h, int chain, dqmc_diag* out) {
     out->avglog10error_sum = st[ST_AVGLOG10]; out->logcount = st[ST_LOGCOUNT];
     out->avgexpphasediff_sum = st[ST_AVGEXPPD];
     out->accepted = st[ST_ACC]; out->proposed = st[ST_PROP]; out->nobs = st[ST_NOBS];
+    out->accepted_v = st[ST_ACCV]; out->proposed_v = st[ST_PROPV];
     return DQMC_OK;
 }
 
@@ -1018,7 +1494,7 @@ extern "C" int dqmc_gpu_reset_diag(dqmc_handle* h) {
         double st[ST_COUNT];
         CK(cudaMemcpy(st, h->chains[c].dev.stats, sizeof(st), cudaMemcpyDeviceToHost));
         st[ST_MAX_WRAP] = st[ST_MAX_PHASEDIFF] = st[ST_AVGLOG10] = st[ST_LOGCOUNT] = st[ST_AVGEXPPD] = 0.0;
-        st[ST_ACC] = st[ST_PROP] = 0.0;
+        st[ST_ACC] = st[ST_PROP] = st[ST_ACCV] = st[ST_PROPV] = 0.0;
         CK(cudaMemcpy(h->chains[c].dev.stats, st, sizeof(st), cudaMemcpyHostToDevice));
     }
     return DQMC_OK;
@@ -1127,5 +1603,112 @@ extern "C" int dqmc_gpu_time_op(dqmc_handle* h, int op, int reps, double* ms_out
     float ms = 0;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
     *ms_out = ms / reps;
+    return DQMC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// projective path: data access and operator-level entry points
+// ---------------------------------------------------------------------------
+static int chk_proj(dqmc_handle* h, int c) {
+    int rc = chk_chain(h, c); if (rc) return rc;
+    if (!h->proj) return fail(DQMC_ESTATE, "not a projective handle (params.proj = 0)");
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_set_vconf(dqmc_handle* h, int chain, const int32_t* v) {
+    int rc = chk_chain(h, chain); if (rc) return rc;
+    const ChainDev& d = h->chains[chain].dev;
+    if (!d.vconf) return fail(DQMC_ESTATE, "no bond field (rv == 0)");
+    size_t n = (size_t)h->ltrot * h->models[h->chains[chain].model]->nn_nf * d.N;
+    for (size_t e = 0; e < n; ++e)
+        if (v[e] < 1 || v[e] > 2) return fail(DQMC_EINVAL, "bond field value out of range 1..2");
+    CK(cudaMemcpy(d.vconf, v, n * sizeof(int32_t), cudaMemcpyHostToDevice));
+    h->started = 0;
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_get_vconf(dqmc_handle* h, int chain, int32_t* v) {
+    int rc = chk_chain(h, chain); if (rc) return rc;
+    const ChainDev& d = h->chains[chain].dev;
+    if (!d.vconf) return fail(DQMC_ESTATE, "no bond field (rv == 0)");
+    size_t n = (size_t)h->ltrot * h->models[h->chains[chain].model]->nn_nf * d.N;
+    CK(cudaMemcpy(v, d.vconf, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_get_trial(dqmc_handle* h, int chain, double* proj, double* w) {
+    int rc = chk_proj(h, chain); if (rc) return rc;
+    const ChainHost& ch = h->chains[chain];
+    if (proj) memcpy(proj, ch.trial.data(), ch.trial.size() * sizeof(zc));
+    if (w) memcpy(w, ch.trial_w.data(), ch.trial_w.size() * sizeof(double));
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_set_trial(dqmc_handle* h, int chain, const double* proj) {
+    int rc = chk_proj(h, chain); if (rc) return rc;
+    ChainHost& ch = h->chains[chain];
+    memcpy(ch.trial.data(), proj, ch.trial.size() * sizeof(zc));
+    h->started = 0;
+    return upload_trial(h, chain);
+}
+
+extern "C" int dqmc_gpu_get_proj(dqmc_handle* h, int chain, double* ur, double* ul, double* ulrinv) {
+    int rc = chk_proj(h, chain); if (rc) return rc;
+    const ChainDev& d = h->chains[chain].dev;
+    int N = d.N, ne = h->models[h->chains[chain].model]->p.ne;
+    size_t Nne = (size_t)N * ne;
+    if (ur) CK(cudaMemcpy(ur, d.UR, Nne * sizeof(zc), cudaMemcpyDeviceToHost));
+    if (ul) {
+        std::vector<zc> t(Nne);
+        CK(cudaMemcpy(t.data(), d.ULT, Nne * sizeof(zc), cudaMemcpyDeviceToHost));
+        zc* o = (zc*)ul;
+        for (int l = 0; l < ne; ++l)
+            for (int i = 0; i < N; ++i) o[l + (size_t)i * ne] = t[i + (size_t)l * N];
+    }
+    if (ulrinv) CK(cudaMemcpy(ulrinv, d.ULRINV, (size_t)ne * ne * sizeof(zc), cudaMemcpyDeviceToHost));
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_set_proj(dqmc_handle* h, int chain, const double* ur, const double* ul, const double* ulrinv) {
+    int rc = chk_proj(h, chain); if (rc) return rc;
+    const ChainDev& d = h->chains[chain].dev;
+    int N = d.N, ne = h->models[h->chains[chain].model]->p.ne;
+    size_t Nne = (size_t)N * ne;
+    if (ur) CK(cudaMemcpy(d.UR, ur, Nne * sizeof(zc), cudaMemcpyHostToDevice));
+    if (ul) {
+        std::vector<zc> t(Nne);
+        const zc* in = (const zc*)ul;
+        for (int l = 0; l < ne; ++l)
+            for (int i = 0; i < N; ++i) t[i + (size_t)l * N] = in[l + (size_t)i * ne];
+        CK(cudaMemcpy(d.ULT, t.data(), Nne * sizeof(zc), cudaMemcpyHostToDevice));
+    }
+    if (ulrinv) CK(cudaMemcpy(d.ULRINV, ulrinv, (size_t)ne * ne * sizeof(zc), cudaMemcpyHostToDevice));
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_proj_update(dqmc_handle* h, int nt, int nf) {
+    if (!h) return fail(DQMC_EINVAL, "null handle");
+    if (!h->proj) return fail(DQMC_ESTATE, "not a projective handle (params.proj = 0)");
+    const HostModel& m = *h->models[0];
+    if (nt < 1 || nt > h->ltrot || nf < 0 || nf > m.nn_nf) return fail(DQMC_EINVAL, "nt or nf out of range");
+    if (nf == 0 && m.p.rhub == 0.0) return fail(DQMC_EINVAL, "no U field (rhub == 0)");
+    if (nf > 0 && m.p.rv == 0.0) return fail(DQMC_EINVAL, "no bond field (rv == 0)");
+    for (int c = 0; c < h->nch; ++c) {
+        const HostModel& mc = *h->models[h->chains[c].model];
+        launch_sfmt_raw(h->d_chains, c, 2 * (nf > 0 ? mc.nn_lf : mc.N), h->st);
+    }
+    launch_proj_update(h->d_chains, h->nch, nt, nf, 0, 0, 0, h->st);
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaGetLastError());
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_proj_green(dqmc_handle* h) {
+    if (!h) return fail(DQMC_EINVAL, "null handle");
+    if (!h->proj) return fail(DQMC_ESTATE, "not a projective handle (params.proj = 0)");
+    launch_proj_ulr(h->d_chains, h->nch, PMAT_ULRINV, 0, 0, -1, h->st);
+    launch_proj_green(h->d_chains, h->nch, PMAT_ULRINV, PMAT_G, h->ctas_per_chain, h->st);
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaGetLastError());
     return DQMC_OK;
 }

@@ -4,7 +4,7 @@
 #include <stdint.h>
 
 #define DQ_MAX_LCOMP 4
-#define DQ_MAX_PROG 160   // propagation ops per pass (nwrap slices x (2 nn_nf + 1))
+#define DQ_MAX_PROG 256   // propagation ops per pass (nwrap slices x ops per slice)
 
 // Model tables for one lattice/parameter set (read-only during a sweep).
 struct ModelDev {
@@ -33,6 +33,10 @@ struct ModelDev {
     const int* snlist;         // [N][nsn]
     const int* plq_cord;       // [lq][z_plq]
     const double2* expar_nn;   // [N][nn_nf]
+    // projective path and the t-V bond field (src/dqmc_config_v/dqmc_set_conf.f90)
+    int proj, ne, lwrapv, rps;         // rps: random words drawn per time slice by the updates
+    double2 vbp[2], vbm[2], vbpi[2], vbmi[2];   // bmat_p, bmat_m and inverses, by field value
+    double2 vdp[2], vdm[2];                     // delta_bmat_p(1,is), delta_bmat_m(1,is)
 };
 
 // Per-chain state.  All pointers are device memory.
@@ -59,6 +63,16 @@ struct ChainDev {
     double2* bins;             // measurement bins (layout: see kern_measure.cu)
     const int* slotmap;        // logical stack slot -> physical slot (shared by all chains)
     double* stats;             // per-chain scalars, see ST_* below
+    // projective path (src/dqmc_proj_core.f90:11-19); N x ne matrices have ld N
+    double2* UR;               // N x ne
+    double2* ULT;              // N x ne, the transpose of UL (ne x N)
+    double2* ULRINV;           // ne x ne, (UL UR)^-1
+    double2* Pst;              // (nst+1) x N x ne: Ust(0:nst)
+    double2* projR;            // N x ne: first ne trial vectors
+    double2* projLc;           // N x ne: conj(projL), i.e. UL^T of the left trial state
+    double* logwDV;            // nst+2
+    int32_t* vconf;            // ltrot x nn_nf x N (bond index fastest), values 1..2
+    double2* pw;               // update window scratch
 };
 
 // indices into ChainDev::stats
@@ -66,11 +80,12 @@ enum {
     ST_PHASE_RE = 0, ST_PHASE_IM, ST_LOGW_RE, ST_LOGW_IM,
     ST_MAX_WRAP, ST_MAX_PHASEDIFF, ST_AVGLOG10, ST_LOGCOUNT, ST_AVGEXPPD,
     ST_ACC, ST_PROP, ST_NOBS, ST_INFO, ST_LOGDETM_RE, ST_LOGDETM_IM, ST_LAST_WRAP,
+    ST_ACCV, ST_PROPV,
     ST_COUNT = 24
 };
 
 // propagation op encoding: kind | which << 4 | nf << 8 | nt << 16
-enum { PK_CB = 1, PK_FFT = 2, PK_DIAG = 3 };
+enum { PK_CB = 1, PK_FFT = 2, PK_DIAG = 3, PK_VMIX = 4, PK_VSCALE = 5 };
 enum { PW_FWD = 0, PW_INV = 1, PW_CONJ = 2 };   // urt/bmat/exph0k, urtm1/bmat_inv/exph0kinv, conj(...)
 struct PropProg {
     int n;

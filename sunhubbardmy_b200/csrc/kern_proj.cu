@@ -1,0 +1,437 @@
+// Projective (ground-state) DQMC: updates, stabilisation and Green's function
+// of the projector path, one CTA per walker for the sequential parts.
+//
+// State per walker: UR = B(tau,0) P (N x ne), UL = P^H B(beta,tau) (ne x N,
+// stored transposed as ULT = UL^T, N x ne), ULRINV = (UL UR)^-1 (ne x ne) and
+// the stack Ust(0:nst) of N x ne matrices (src/dqmc_proj_core.f90:11-19).
+//
+// Reference routines:
+//  * k_proj_update: dqmc_proj_update_submatrix_LR (src/dqmc_config_v/
+//    dqmc_proj_update_submatrix_LR.f90:1-298 for the bond field,
+//    src/dqmc_config_u/dqmc_proj_update_submatrix_LR.f90:1-282 for the site
+//    field).  Units (bonds of one family, or sites) are visited in order in
+//    windows of `wrows` rows (nustock): the window's rows of R = UR ULRINV and
+//    of F = R UL are formed by two GEMMs, the accept/reject sequence runs on
+//    the F block in shared memory while Gamma^-1 = (I + Delta F_AA)^-1 Delta
+//    is bordered one accepted unit at a time, and the window is flushed with
+//    ULRINV -= (ULRINV UL_A)(Gamma^-1 R_A) and UR_A <- (I + Delta) UR_A.
+//    Instead of re-evaluating F_rr - F_rA Gamma^-1 F_Ar for each unit, the
+//    kernel keeps the trailing block of F updated (rank-2 Schur complement
+//    per accept), which gives the same numbers in exact arithmetic.
+//  * k_proj_qr: s_zgeQR_pqmc (lib/s_matrix.f90:1822-1996) as used by
+//    dqmc_proj_stablize_0b_qr / _b0_qr: Q of a tall N x ne matrix with an
+//    even number of negative R diagonal entries (else column 1 is negated)
+//    and log |det R|.  The wide UL is factored through its transpose, which
+//    is the stored layout.
+//  * k_proj_ulr: ULR = UL UR and its inverse (s_invlu_z /
+//    s_inv_logdet_lu_z); the inverse is taken through a Householder QR, and
+//    log det ULR = log det Q + sum log R_ii.
+//  * k_proj_t1 + k_proj_gmat: green_equaltime (src/dqmc_proj_core/
+//    green_equaltime.f90): G = I - (UR ULRINV) UL, several CTAs per walker.
+#include "chain_access.cuh"
+#include "kernels.h"
+#include "linalg.cuh"
+
+#define PW_MAXR 32          // largest update window (rows)
+#define PW_LD (PW_MAXR + 1)
+
+struct ProjSmem {
+    LinalgSmem L;
+    double red[64];
+};
+
+DQ_DEV LinalgScratch proj_scratch(const ChainDev& c) {
+    LinalgScratch s;
+    s.Vs = c.W[5];
+    s.Ws = c.smallw;
+    s.Ws2 = c.smallw + (size_t)QR_NB * c.N;
+    s.T = c.T;
+    s.tau = c.tau;
+    return s;
+}
+
+static size_t proj_la_smem(int maxN) {
+    size_t a = (size_t)maxN * QR_NB;
+    size_t b = GemmBig::SMEM_ELEMS;
+    if ((size_t)GemmWide::SMEM_ELEMS > b) b = GemmWide::SMEM_ELEMS;
+    return (a > b ? a : b) * sizeof(double2) + sizeof(ProjSmem) + 64;
+}
+
+// ---------------------------------------------------------------------------
+// s_zgeQR_pqmc on the N x ne matrix mat_id, in place (X <- Q); the log of
+// |det R| goes to logwDV[dst] = logwDV[add] + log|det R| (add < 0: nothing added).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_proj_qr(const ChainDev* __restrict__ chains, int mat_id, int dst, int add) {
+    extern __shared__ double2 ssm[];
+    const ChainDev c = chains[blockIdx.x];
+    const ModelDev& md = *c.md;
+    const int N = c.N, ne = md.ne, tid = threadIdx.x, nth = blockDim.x;
+    double2* buf = ssm;
+    ProjSmem* S = (ProjSmem*)(ssm + (((size_t)N * QR_NB > (size_t)GemmBig::SMEM_ELEMS) ? (size_t)N * QR_NB : (size_t)GemmBig::SMEM_ELEMS));
+    LinalgScratch sc = proj_scratch(c);
+    double2* X = chain_mat(c, mat_id);
+    double2* A = c.W[1];
+    for (size_t e = tid; e < (size_t)N * ne; e += nth) A[e] = X[e];
+    __syncthreads();
+    cta_qr(A, N, sc, buf, buf, &S->L, ne);
+    double lg = 0.0, neg = 0.0;
+    for (int i = tid; i < ne; i += nth) {
+        double r = A[MIDX(i, i, N)].x;
+        lg += log(fabs(r));
+        neg += (r < 0.0) ? 1.0 : 0.0;
+    }
+    lg = block_sum(lg, S->red);
+    neg = block_sum(neg, S->red);
+    cta_form_q(A, N, X, sc, buf, ne);
+    __syncthreads();
+    if (((long long)llround(neg)) & 1)
+        for (int i = tid; i < N; i += nth) X[i] = cmk(-X[i].x, -X[i].y);
+    if (tid == 0) c.logwDV[dst] = (add >= 0 ? c.logwDV[add] : 0.0) + lg;
+}
+
+// ---------------------------------------------------------------------------
+// out = (ULT^T UR)^-1; with logdet, stats[LOGDETM] = logwDV[ia] (+ logwDV[ib]) +
+// log det(UL UR), the logweightf of the sweep routines.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_proj_ulr(const ChainDev* __restrict__ chains, int out_id, int logdet, int ia, int ib) {
+    extern __shared__ double2 ssm[];
+    const ChainDev c = chains[blockIdx.x];
+    const ModelDev& md = *c.md;
+    const int N = c.N, ne = md.ne, tid = threadIdx.x, nth = blockDim.x;
+    double2* buf = ssm;
+    ProjSmem* S = (ProjSmem*)(ssm + (((size_t)N * QR_NB > (size_t)GemmBig::SMEM_ELEMS) ? (size_t)N * QR_NB : (size_t)GemmBig::SMEM_ELEMS));
+    LinalgScratch sc = proj_scratch(c);
+    double2* M = c.W[2];
+    ZGemmArgs g;
+    g.M = ne; g.N = ne; g.K = N; g.alpha = cmk(1, 0); g.beta = cmk(0, 0);
+    g.A = c.ULT; g.lda = N; g.opA = OP_T; g.B = c.UR; g.ldb = N; g.opB = OP_N; g.C = M; g.ldc = ne;
+    zgemm_cta<GemmBig>(g, 0, 1, buf);
+    cta_qr(M, ne, sc, buf, buf, &S->L);
+    double2 ld = cmk(0, 0);
+    if (logdet) {
+        ld = cta_logdet_q(sc.tau, ne, S->red);
+        double2 lr = cmk(0, 0);
+        for (int i = tid; i < ne; i += nth) {
+            double r = M[MIDX(i, i, ne)].x;
+            lr = cadd(lr, cmk(log(fabs(r)), r < 0.0 ? M_PI : 0.0));
+        }
+        lr = block_csum(lr, S->red);
+        ld = cadd(ld, lr);
+    }
+    double2* X = chain_mat(c, out_id);
+    for (int e = tid; e < ne * ne; e += nth) X[e] = cmk((e % ne) == (e / ne) ? 1.0 : 0.0, 0.0);
+    __syncthreads();
+    cta_apply_qh(M, ne, X, sc, buf);
+    cta_trsm_upper(M, ne, X, buf, &S->L);
+    if (logdet && tid == 0) {
+        double w = c.logwDV[ia] + (ib >= 0 ? c.logwDV[ib] : 0.0);
+        c.stats[ST_LOGDETM_RE] = ld.x + w;
+        c.stats[ST_LOGDETM_IM] = ld.y;
+    }
+}
+
+// T1 = UR * INV (N x ne), tiles shared by gridDim.x CTAs per walker
+__global__ void __launch_bounds__(256) k_proj_t1(const ChainDev* __restrict__ chains, int inv_id) {
+    extern __shared__ double2 ssm[];
+    const ChainDev c = chains[blockIdx.y];
+    const int N = c.N, ne = c.md->ne;
+    ZGemmArgs g;
+    g.M = N; g.N = ne; g.K = ne; g.alpha = cmk(1, 0); g.beta = cmk(0, 0);
+    g.A = c.UR; g.lda = N; g.opA = OP_N; g.B = chain_mat(c, inv_id); g.ldb = ne; g.opB = OP_N;
+    g.C = c.W[0]; g.ldc = N;
+    zgemm_cta<GemmBig>(g, blockIdx.x, gridDim.x, ssm);
+}
+
+// dst = I - T1 * ULT^T (N x N)
+__global__ void __launch_bounds__(256) k_proj_gmat(const ChainDev* __restrict__ chains, int dst_id) {
+    extern __shared__ double2 ssm[];
+    const ChainDev c = chains[blockIdx.y];
+    const int N = c.N, ne = c.md->ne;
+    double2* D = chain_mat(c, dst_id);
+    ZGemmArgs g;
+    g.M = N; g.N = N; g.K = ne; g.alpha = cmk(-1, 0); g.beta = cmk(0, 0);
+    g.A = c.W[0]; g.lda = N; g.opA = OP_N; g.B = c.ULT; g.ldb = N; g.opB = OP_T;
+    g.C = D; g.ldc = N;
+    zgemm_cta<GemmBig>(g, blockIdx.x, gridDim.x, ssm);
+    // the diagonal of the tiles this CTA wrote
+    const int tm = (N + GemmBig::BM - 1) / GemmBig::BM, tn = (N + GemmBig::BN - 1) / GemmBig::BN;
+    for (int t = blockIdx.x; t < tm * tn; t += gridDim.x) {
+        int m0 = (t % tm) * GemmBig::BM, n0 = (t / tm) * GemmBig::BN;
+        int lo = max(m0, n0), hi = min(min(m0 + GemmBig::BM, n0 + GemmBig::BN), N);
+        for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) D[MIDX(i, i, N)].x += 1.0;
+    }
+}
+
+// copy of an N x ne matrix (conj = 1: complex conjugate)
+__global__ void k_tall_copy(const ChainDev* __restrict__ chains, int dst_id, int src_id) {
+    const ChainDev c = chains[blockIdx.y];
+    const size_t n = (size_t)c.N * c.md->ne;
+    double2* d = chain_mat(c, dst_id);
+    const double2* s = chain_mat(c, src_id);
+    for (size_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) d[e] = s[e];
+}
+
+// ---------------------------------------------------------------------------
+// projective local update (submatrix-LR), see the file header
+// ---------------------------------------------------------------------------
+struct PUpdSmem {
+    double2 F[PW_MAXR * PW_LD];     // F block of the window (window-start values)
+    double2 Pc[PW_MAXR * PW_LD];    // F block with the window's accepted changes folded in
+    double2 Gm[PW_MAXR * PW_LD];    // Gamma^-1 in window coordinates (zero off the accepted rows)
+    double2 colr[PW_MAXR * 2], rowr[PW_MAXR * 2], ikk[PW_MAXR * 2], kik[PW_MAXR * 2];
+    double2 gkk[4];
+    double2 dl[PW_MAXR];
+    double2 phase;
+    int rows[PW_MAXR];
+    int accr[PW_MAXR];
+    int acc_flag, nacc;
+    double accm;
+};
+
+DQ_DEV double u32_stream(uint32_t u) { return ((double)u + 0.5) * (1.0 / 4294967296.0); }
+
+// visit: slices already updated in this half sweep; dir 0 = 0b (bond families
+// 1..nn_nf, then sites), 1 = b0 (sites, then families nn_nf..1) fixes where
+// this call's draws sit in the half sweep's random words; rnd_off >= 0
+// overrides that offset.  The window is the model's nublock (nustock) rows.
+__global__ void __launch_bounds__(256) k_proj_update(const ChainDev* __restrict__ chains, int nt, int nf, int visit,
+                                                     int dir, int rnd_off) {
+    extern __shared__ double2 ssm[];
+    const ChainDev c = chains[blockIdx.x];
+    const ModelDev& md = *c.md;
+    const int N = c.N, ne = md.ne, tid = threadIdx.x, nth = blockDim.x;
+    double2* buf = ssm;
+    PUpdSmem* S = (PUpdSmem*)(ssm + GemmBig::SMEM_ELEMS);
+    const int bond = nf > 0;
+    const int b = bond ? 2 : 1;
+    const int nunits = bond ? md.nn_lf : N;
+    const int lc = bond ? 2 : md.lcomp;
+    int R = min(md.nublock, PW_MAXR);
+    R -= R % b;
+    if (R < b) R = b;
+    const int upw = R / b;
+    if (rnd_off < 0) {
+        const int vw = md.lwrapv ? 2 * md.nn_lf * md.nn_nf : 0, uw = md.lwrapu ? 2 * N : 0;
+        int within;
+        if (dir == 0) within = bond ? (nf - 1) * 2 * md.nn_lf : vw;
+        else within = bond ? uw + (md.nn_nf - nf) * 2 * md.nn_lf : 0;
+        rnd_off = visit * md.rps + within;
+    }
+    const uint32_t* rnd = c.rnd + rnd_off;
+    int32_t* cf = bond ? c.vconf + ((size_t)(nt - 1) * md.nn_nf + (nf - 1)) * N : c.conf + (size_t)(nt - 1) * N;
+    double2* Xg = c.pw;
+    double2* Yg = Xg + (size_t)R * ne;
+    double2* Rg = Yg + (size_t)R * ne;
+    double2* Fg = Rg + (size_t)R * ne;
+    double2* Gg = Fg + (size_t)R * R;
+    double2* Ut = Gg + (size_t)R * R;
+    double2* Vt = Ut + (size_t)ne * R;
+    if (tid == 0) {
+        S->phase = cmk(c.stats[ST_PHASE_RE], c.stats[ST_PHASE_IM]);
+        S->accm = 0.0;
+    }
+    for (int u0 = 0; u0 < nunits; u0 += upw) {
+        const int nu = min(upw, nunits - u0), nr = nu * b;
+        for (int k = tid; k < nu; k += nth) {
+            if (bond) {
+                int ist = (nf - 1) * md.nn_lf + u0 + k;
+                S->rows[2 * k] = md.bond_i1[ist];
+                S->rows[2 * k + 1] = md.bond_i2[ist];
+            } else {
+                S->rows[k] = u0 + k;
+            }
+        }
+        __syncthreads();
+        for (int e = tid; e < nr * ne; e += nth) {
+            int x = e % nr, l = e / nr;
+            Xg[e] = c.UR[MIDX(S->rows[x], l, N)];
+            Yg[e] = c.ULT[MIDX(S->rows[x], l, N)];
+        }
+        __syncthreads();
+        {
+            ZGemmArgs g;
+            g.M = nr; g.N = ne; g.K = ne; g.alpha = cmk(1, 0); g.beta = cmk(0, 0);
+            g.A = Xg; g.lda = nr; g.opA = OP_N; g.B = c.ULRINV; g.ldb = ne; g.opB = OP_N; g.C = Rg; g.ldc = nr;
+            zgemm_cta<GemmBig>(g, 0, 1, buf);
+            g.M = nr; g.N = nr; g.K = ne;
+            g.A = Rg; g.lda = nr; g.B = Yg; g.ldb = nr; g.opB = OP_T; g.C = Fg; g.ldc = nr;
+            zgemm_cta<GemmBig>(g, 0, 1, buf);
+        }
+        for (int e = tid; e < nr * nr; e += nth) {
+            int x = e % nr, y = e / nr;
+            double2 v = Fg[e];
+            S->F[x + y * PW_LD] = v;
+            S->Pc[x + y * PW_LD] = v;
+            S->Gm[x + y * PW_LD] = cmk(0, 0);
+        }
+        for (int x = tid; x < nr; x += nth) { S->dl[x] = cmk(0, 0); S->accr[x] = 0; }
+        if (tid == 0) S->nacc = 0;
+        __syncthreads();
+        for (int k = 0; k < nu; ++k) {
+            const int r0 = k * b;
+            if (tid == 0) {
+                const int u = u0 + k;
+                const int is = cf[u];
+                const double r1 = u32_stream(rnd[2 * u]), r2 = u32_stream(rnd[2 * u + 1]);
+                const int iflip = (int)ceil(r1 * (lc - 1));
+                const int isp = (is + iflip - 1) % lc + 1;
+                double2 ratiotot, g11, g12 = cmk(0, 0), g21 = cmk(0, 0), g22 = cmk(0, 0), d1, d2 = cmk(0, 0);
+                if (bond) {
+                    d1 = md.vdp[is - 1];
+                    d2 = md.vdm[is - 1];
+                    double2 v11 = cadd(cmk(1, 0), cmul(S->Pc[r0 + r0 * PW_LD], d1));
+                    double2 v21 = cmul(S->Pc[r0 + 1 + r0 * PW_LD], d1);
+                    double2 v12 = cmul(S->Pc[r0 + (r0 + 1) * PW_LD], d2);
+                    double2 v22 = cadd(cmk(1, 0), cmul(S->Pc[r0 + 1 + (r0 + 1) * PW_LD], d2));
+                    double2 det = csub(cmul(v11, v22), cmul(v12, v21));
+                    ratiotot = det;
+                    double2 id = cdiv(cmk(1, 0), det);
+                    g11 = cmul(cmul(v22, d1), id);
+                    g12 = cmul(cmul(cmk(-v12.x, -v12.y), d1), id);
+                    g21 = cmul(cmul(cmk(-v21.x, -v21.y), d2), id);
+                    g22 = cmul(cmul(v11, d2), id);
+                } else {
+                    const int kk = (is - 1) * (lc - 1) + (iflip - 1);
+                    d1 = md.delta[kk];
+                    double2 ratio1 = cadd(cmk(1, 0), cmul(S->Pc[r0 + r0 * PW_LD], d1));
+                    double2 r = ratio1;
+                    for (int f = 1; f < md.nflr; ++f) r = cmul(r, ratio1);
+                    r = cscale(r, md.gam_ratio[kk]);
+                    ratiotot = cmul(r, md.phase_ratio[kk]);
+                    g11 = cdiv(d1, ratio1);
+                }
+                const double2 ph = S->phase;
+                double ratio_re = cmul(ratiotot, ph).x / ph.x;
+                int acc = fabs(ratio_re) > r2;
+                if (acc) {
+                    double wgt = sqrt(cmul(ratiotot, cconj(ratiotot)).x);
+                    S->phase = cscale(cmul(ph, ratiotot), 1.0 / wgt);
+                    cf[u] = isp;
+                    S->accm += 1.0;
+                    S->gkk[0] = g11; S->gkk[1] = g21; S->gkk[2] = g12; S->gkk[3] = g22;   // column-major b x b
+                    S->dl[r0] = d1;
+                    S->accr[r0] = 1;
+                    if (bond) { S->dl[r0 + 1] = d2; S->accr[r0 + 1] = 1; }
+                    S->nacc += b;
+                }
+                S->acc_flag = acc;
+            }
+            __syncthreads();
+            if (!S->acc_flag) continue;
+            // snapshots: columns/rows r of the current block, Gamma F_Ar and F_rA Gamma
+            for (int e = tid; e < nr * b; e += nth) {
+                int x = e % nr, cc = e / nr;
+                S->colr[x + cc * PW_MAXR] = S->Pc[x + (r0 + cc) * PW_LD];
+                S->rowr[x + cc * PW_MAXR] = S->Pc[r0 + cc + x * PW_LD];
+                double2 a = cmk(0, 0), bb = cmk(0, 0);
+                for (int y = 0; y < r0; ++y) {
+                    a = cfma(S->Gm[x + y * PW_LD], S->F[y + (r0 + cc) * PW_LD], a);
+                    bb = cfma(S->F[r0 + cc + y * PW_LD], S->Gm[y + x * PW_LD], bb);
+                }
+                S->ikk[x + cc * PW_MAXR] = a;
+                S->kik[x + cc * PW_MAXR] = bb;
+            }
+            __syncthreads();
+            for (int e = tid; e < nr * nr; e += nth) {
+                int x = e % nr, y = e / nr;
+                const bool xr = (x >= r0 && x < r0 + b), yr = (y >= r0 && y < r0 + b);
+                if (x < r0 && y < r0) {
+                    double2 s = cmk(0, 0);
+                    for (int p = 0; p < b; ++p)
+                        for (int q = 0; q < b; ++q)
+                            s = cfma(cmul(S->ikk[x + p * PW_MAXR], S->gkk[p + q * b]), S->kik[y + q * PW_MAXR], s);
+                    S->Gm[x + y * PW_LD] = cadd(S->Gm[x + y * PW_LD], s);
+                } else if (xr && y < r0) {
+                    double2 s = cmk(0, 0);
+                    for (int q = 0; q < b; ++q) s = cfma(S->gkk[(x - r0) + q * b], S->kik[y + q * PW_MAXR], s);
+                    S->Gm[x + y * PW_LD] = cmk(-s.x, -s.y);
+                } else if (x < r0 && yr) {
+                    double2 s = cmk(0, 0);
+                    for (int p = 0; p < b; ++p) s = cfma(S->ikk[x + p * PW_MAXR], S->gkk[p + (y - r0) * b], s);
+                    S->Gm[x + y * PW_LD] = cmk(-s.x, -s.y);
+                } else if (xr && yr) {
+                    S->Gm[x + y * PW_LD] = S->gkk[(x - r0) + (y - r0) * b];
+                } else if (x >= r0 + b && y >= r0 + b) {
+                    double2 s = cmk(0, 0);
+                    for (int p = 0; p < b; ++p)
+                        for (int q = 0; q < b; ++q)
+                            s = cfma(cmul(S->colr[x + p * PW_MAXR], S->gkk[p + q * b]), S->rowr[y + q * PW_MAXR], s);
+                    S->Pc[x + y * PW_LD] = csub(S->Pc[x + y * PW_LD], s);
+                }
+            }
+            __syncthreads();
+        }
+        if (S->nacc > 0) {
+            for (int e = tid; e < nr * nr; e += nth) {
+                int x = e % nr, y = e / nr;
+                Gg[e] = S->Gm[x + y * PW_LD];
+            }
+            __syncthreads();
+            ZGemmArgs g;
+            g.M = ne; g.N = nr; g.K = ne; g.alpha = cmk(1, 0); g.beta = cmk(0, 0);
+            g.A = c.ULRINV; g.lda = ne; g.opA = OP_N; g.B = Yg; g.ldb = nr; g.opB = OP_T; g.C = Ut; g.ldc = ne;
+            zgemm_cta<GemmBig>(g, 0, 1, buf);
+            g.M = nr; g.N = ne; g.K = nr;
+            g.A = Gg; g.lda = nr; g.B = Rg; g.ldb = nr; g.opB = OP_N; g.C = Vt; g.ldc = nr;
+            zgemm_cta<GemmBig>(g, 0, 1, buf);
+            g.M = ne; g.N = ne; g.K = nr; g.alpha = cmk(-1, 0); g.beta = cmk(1, 0);
+            g.A = Ut; g.lda = ne; g.B = Vt; g.ldb = nr; g.C = c.ULRINV; g.ldc = ne;
+            zgemm_cta<GemmBig>(g, 0, 1, buf);
+            for (int e = tid; e < nr * ne; e += nth) {
+                int x = e % nr, l = e / nr;
+                if (S->accr[x]) {
+                    double2* p = c.UR + MIDX(S->rows[x], l, N);
+                    double2 v = *p;
+                    *p = cadd(v, cmul(S->dl[x], v));
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        c.stats[ST_PHASE_RE] = S->phase.x;
+        c.stats[ST_PHASE_IM] = S->phase.y;
+        c.stats[bond ? ST_ACCV : ST_ACC] += S->accm;
+        c.stats[bond ? ST_PROPV : ST_PROP] += (double)nunits;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static int g_proj_attr = 0;
+static size_t g_proj_la = 0, g_proj_upd = 0;
+
+void set_proj_maxN(int maxN) {
+    g_proj_la = proj_la_smem(maxN);
+    g_proj_upd = (size_t)GemmBig::SMEM_ELEMS * sizeof(double2) + sizeof(PUpdSmem) + 64;
+    cudaFuncSetAttribute(k_proj_qr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g_proj_la);
+    cudaFuncSetAttribute(k_proj_ulr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g_proj_la);
+    cudaFuncSetAttribute(k_proj_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g_proj_upd);
+    cudaFuncSetAttribute(k_proj_t1, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmBig::SMEM_ELEMS * (int)sizeof(double2));
+    cudaFuncSetAttribute(k_proj_gmat, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmBig::SMEM_ELEMS * (int)sizeof(double2));
+    g_proj_attr = 1;
+}
+
+void launch_proj_qr(const ChainDev* chains, int nchains, int mat_id, int dst, int add, cudaStream_t st) {
+    k_proj_qr<<<nchains, 256, g_proj_la, st>>>(chains, mat_id, dst, add);
+}
+
+void launch_proj_ulr(const ChainDev* chains, int nchains, int out_id, int logdet, int ia, int ib, cudaStream_t st) {
+    k_proj_ulr<<<nchains, 256, g_proj_la, st>>>(chains, out_id, logdet, ia, ib);
+}
+
+void launch_proj_green(const ChainDev* chains, int nchains, int inv_id, int dst_id, int ctas, cudaStream_t st) {
+    size_t sm = (size_t)GemmBig::SMEM_ELEMS * sizeof(double2);
+    k_proj_t1<<<dim3(ctas, nchains), 256, sm, st>>>(chains, inv_id);
+    k_proj_gmat<<<dim3(ctas, nchains), 256, sm, st>>>(chains, dst_id);
+}
+
+void launch_tall_copy(const ChainDev* chains, int nchains, int dst_id, int src_id, cudaStream_t st) {
+    k_tall_copy<<<dim3(8, nchains), 256, 0, st>>>(chains, dst_id, src_id);
+}
+
+void launch_proj_update(const ChainDev* chains, int nchains, int nt, int nf, int visit, int dir, int rnd_off,
+                        cudaStream_t st) {
+    k_proj_update<<<nchains, 256, g_proj_upd, st>>>(chains, nt, nf, visit, dir, rnd_off);
+}

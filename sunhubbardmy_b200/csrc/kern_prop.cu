@@ -3,7 +3,11 @@
 // left (column pass) or from the right (row pass) to a per-chain N x N matrix.
 //
 // Reference operators: src/dqmc_config_h0/dqmc_{left,right}_{forward,backward}_prop.f90
-// and _hc (checkerboard 18-44, FFT 95-134), src/dqmc_config_u/dqmc_*_prop.f90 (27-32).
+// and _hc (checkerboard 18-44, FFT 95-134), src/dqmc_config_u/dqmc_*_prop.f90 (27-32),
+// src/dqmc_config_v/dqmc_*_prop.f90 (t-V bond field: per bond U diag(bp, bm) U^T with
+// U the 2x2 Hadamard, split at nflag into a mix op PK_VMIX and a scale op PK_VSCALE).
+// The projective path propagates UR (N x ne) from the left and UL (ne x N) from the
+// right; UL is stored transposed (N x ne), so both are passes over site vectors.
 // A pass streams each column (row) of the matrix through shared memory once and
 // applies a whole program of such operators to it, so a full slice wrap (or
 // an nwrap-slice B product for the stabilisation) costs one read and one write
@@ -14,7 +18,7 @@
 // One operator applied to `nv` vectors held in shared memory (vector v at
 // S + v*vs, element stride 1).  right = 0: vectors are columns and the operator
 // multiplies from the left; right = 1: vectors are rows (x -> x * Op).
-__device__ void apply_op(const ModelDev& md, const int32_t* conf, int code, int right,
+__device__ void apply_op(const ModelDev& md, const int32_t* conf, const int32_t* vconf, int code, int right,
                          double2* S, int nv, int vs) {
     const int kind = code & 15, which = (code >> 4) & 15, nf = (code >> 8) & 255, nt = code >> 16;
     const int N = md.N, tid = threadIdx.x, nth = blockDim.x;
@@ -45,6 +49,27 @@ __device__ void apply_op(const ModelDev& md, const int32_t* conf, int code, int 
             if (which == PW_CONJ) b.y = -b.y;
             double2* x = S + (size_t)v * vs;
             x[i] = cmul(x[i], b);
+        }
+    } else if (kind == PK_VMIX || kind == PK_VSCALE) {
+        // bond (i1, i2) of family nf: x <- H x (H = H^T = [[1,1],[1,-1]]/sqrt2, the same
+        // from either side) or x_i1 *= s1(is), x_i2 *= s2(is)
+        const int lf = md.nn_lf;
+        const double h = 1.0 / sqrt(2.0);
+        const int32_t* vc = vconf + ((size_t)(nt - 1) * md.nn_nf + (nf - 1)) * N;
+        for (int w = tid; w < nv * lf; w += nth) {
+            int v = w / lf, b = w % lf;
+            int ist = (nf - 1) * lf + b;
+            int i1 = md.bond_i1[ist], i2 = md.bond_i2[ist];
+            double2* x = S + (size_t)v * vs;
+            double2 a = x[i1], c = x[i2];
+            if (kind == PK_VMIX) {
+                x[i1] = cadd(cscale(a, h), cscale(c, h));
+                x[i2] = cadd(cscale(a, h), cscale(c, -h));
+            } else {
+                int is = vc[b] - 1;
+                x[i1] = cmul((which == PW_INV) ? md.vbpi[is] : md.vbp[is], a);
+                x[i2] = cmul((which == PW_INV) ? md.vbmi[is] : md.vbm[is], c);
+            }
         }
     } else if (kind == PK_FFT) {
         // left:  x <- F^-1 D F x ; right (row r): r <- F D F^-1 r  (F symmetric)
@@ -85,19 +110,23 @@ __device__ void apply_op(const ModelDev& md, const int32_t* conf, int code, int 
     __syncthreads();
 }
 
-// Column pass: X <- Op_k ... Op_1 X for the program prog.
-__global__ void __launch_bounds__(256, 2) k_prop_cols(const ChainDev* __restrict__ chains, int mat_id, PropProg prog, int cb) {
+// Column pass: X <- Op_k ... Op_1 X for the program prog.  tall = 1: X is one
+// of the N x ne matrices of the projective path; right = 1 applies the
+// operators as right multiplications of the transposed matrix (UL^T).
+__global__ void __launch_bounds__(256, 2) k_prop_cols(const ChainDev* __restrict__ chains, int mat_id, PropProg prog, int cb,
+                                                      int tall, int right) {
     extern __shared__ double2 sm[];
     const ChainDev c = chains[blockIdx.y];
     const ModelDev& md = *c.md;
     const int N = c.N;
+    const int ncol = tall ? md.ne : N;
     double2* X = chain_mat(c, mat_id);
     const int vs = N + 1;   // odd vector stride: conflict-free strided lines
-    for (int c0 = blockIdx.x * cb; c0 < N; c0 += gridDim.x * cb) {
-        int nv = min(cb, N - c0);
+    for (int c0 = blockIdx.x * cb; c0 < ncol; c0 += gridDim.x * cb) {
+        int nv = min(cb, ncol - c0);
         for (int e = threadIdx.x; e < nv * N; e += blockDim.x) sm[(e / N) * vs + e % N] = X[(size_t)c0 * N + e];
         __syncthreads();
-        for (int k = 0; k < prog.n; ++k) apply_op(md, c.conf, prog.op[k], 0, sm, nv, vs);
+        for (int k = 0; k < prog.n; ++k) apply_op(md, c.conf, c.vconf, prog.op[k], right, sm, nv, vs);
         for (int e = threadIdx.x; e < nv * N; e += blockDim.x) X[(size_t)c0 * N + e] = sm[(e / N) * vs + e % N];
         __syncthreads();
     }
@@ -117,7 +146,7 @@ __global__ void __launch_bounds__(256, 2) k_prop_rows(const ChainDev* __restrict
             sm[r * vs + j] = X[MIDX(r0 + r, j, N)];
         }
         __syncthreads();
-        for (int k = 0; k < prog.n; ++k) apply_op(md, c.conf, prog.op[k], 1, sm, nv, vs);
+        for (int k = 0; k < prog.n; ++k) apply_op(md, c.conf, c.vconf, prog.op[k], 1, sm, nv, vs);
         for (int e = threadIdx.x; e < nv * N; e += blockDim.x) {
             int r = e % nv, j = e / nv;
             X[MIDX(r0 + r, j, N)] = sm[r * vs + j];
@@ -139,5 +168,18 @@ void launch_prop(const ChainDev* chains, int nchains, int maxN, int mat_id, cons
     }
     dim3 grid(ctas_per_chain, nchains);
     if (right) k_prop_rows<<<grid, 256, smem, st>>>(chains, mat_id, prog, nb);
-    else k_prop_cols<<<grid, 256, smem, st>>>(chains, mat_id, prog, nb);
+    else k_prop_cols<<<grid, 256, smem, st>>>(chains, mat_id, prog, nb, 0, 0);
+}
+
+void launch_prop_tall(const ChainDev* chains, int nchains, int maxN, int mat_id, const PropProg& prog,
+                      int right, int ctas_per_chain, cudaStream_t st) {
+    const int nb = 16;
+    size_t smem = (size_t)nb * (maxN + 1) * sizeof(double2);
+    if (!g_prop_smem_ok) {
+        cudaFuncSetAttribute(k_prop_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(k_prop_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        g_prop_smem_ok = 1;
+    }
+    dim3 grid(ctas_per_chain, nchains);
+    k_prop_cols<<<grid, 256, smem, st>>>(chains, mat_id, prog, nb, 1, right);
 }

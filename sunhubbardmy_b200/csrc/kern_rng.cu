@@ -46,11 +46,12 @@ __device__ void sfmt_gen_all(uint32_t* st) {
     }
 }
 
-// count = slices * 2 * N draws per chain (slices > 0), or exactly -slices draws
+// count = slices * rps draws per chain (slices > 0; rps = words per time slice
+// of the chain's model), or exactly -slices draws
 __global__ void k_sfmt_fill(const ChainDev* __restrict__ chains, int ch0, int nchains, int slices) {
     int ch = ch0 + blockIdx.x * blockDim.x + threadIdx.x;
     if (ch >= ch0 + nchains) return;
-    const int count = slices > 0 ? slices * 2 * chains[ch].N : -slices;
+    const int count = slices > 0 ? slices * chains[ch].md->rps : -slices;
     uint32_t* st = chains[ch].sfmt;
     uint32_t* out = chains[ch].rnd;
     int idx = (int)st[SFMT_N32];

@@ -29,3 +29,15 @@ void launch_wrap_check(const ChainDev* chains, int nchains, int record, cudaStre
 void launch_zgemm_test(const ChainDev* chains, int nchains, int m, int n, int k, int opa, int opb,
                        int a_id, int b_id, int c_id, double beta_re, cudaStream_t st);
 void launch_qr_test(const ChainDev* chains, int nchains, int a_id, int q_id, cudaStream_t st);
+
+// projective path (kern_proj.cu, kern_prop.cu)
+void set_proj_maxN(int maxN);
+// one pass of prog over the N x ne matrix mat_id (right = 1: right multiplications of UL, stored as UL^T)
+void launch_prop_tall(const ChainDev* chains, int nchains, int maxN, int mat_id, const PropProg& prog,
+                      int right, int ctas_per_chain, cudaStream_t st);
+void launch_proj_qr(const ChainDev* chains, int nchains, int mat_id, int dst, int add, cudaStream_t st);
+void launch_proj_ulr(const ChainDev* chains, int nchains, int out_id, int logdet, int ia, int ib, cudaStream_t st);
+void launch_proj_green(const ChainDev* chains, int nchains, int inv_id, int dst_id, int ctas, cudaStream_t st);
+void launch_tall_copy(const ChainDev* chains, int nchains, int dst_id, int src_id, cudaStream_t st);
+void launch_proj_update(const ChainDev* chains, int nchains, int nt, int nf, int visit, int dir, int rnd_off,
+                        cudaStream_t st);

@@ -183,11 +183,14 @@ static __device__ void apply_block(const double2* Vs, const double2* Tp, int N, 
     zgemm_cta<GemmBig>(g, 0, 1, gsm);
 }
 
-// In-place QR of A (N x N): R in the upper triangle, reflectors below,
-// tau and the per-panel T factors in the scratch.  smem_panel holds >= N*16 double2.
-static __device__ void cta_qr(double2* A, int N, LinalgScratch& sc, double2* smem_panel, cplx* gsm, LinalgSmem* L) {
-    for (int p = 0; p < N; p += QR_NB) {
-        const int jb = min(QR_NB, N - p), m = N - p;
+// In-place QR of the first ncol columns of A (N rows, ld N; ncol <= N, default
+// all N): R in the upper triangle, reflectors below, tau and the per-panel T
+// factors in the scratch.  smem_panel holds >= N*16 double2.
+static __device__ void cta_qr(double2* A, int N, LinalgScratch& sc, double2* smem_panel, cplx* gsm, LinalgSmem* L,
+                              int ncol = -1) {
+    if (ncol < 0) ncol = N;
+    for (int p = 0; p < ncol; p += QR_NB) {
+        const int jb = min(QR_NB, ncol - p), m = N - p;
         double2* P = smem_panel;
         for (int e = threadIdx.x; e < m * jb; e += blockDim.x) {
             int r = e % m, cc = e / m;
@@ -203,7 +206,7 @@ static __device__ void cta_qr(double2* A, int N, LinalgScratch& sc, double2* sme
             sc.Vs[MIDX(r, cc, N)] = (r < cc) ? cmk(0, 0) : (r == cc) ? cmk(1, 0) : P[(size_t)cc * m + r];
         }
         __syncthreads();
-        if (p + jb < N) apply_block(sc.Vs, Tp, N, p, jb, A, p + jb, N - p - jb, 1, sc, gsm);
+        if (p + jb < ncol) apply_block(sc.Vs, Tp, N, p, jb, A, p + jb, ncol - p - jb, 1, sc, gsm);
     }
 }
 
@@ -221,19 +224,21 @@ static __device__ double2 cta_logdet_q(const double2* tau, int N, double* red) {
     return block_csum(acc, red);
 }
 
-// Q (N x N) from the factored A into Qout (zungqr, blocked backward).
-static __device__ void cta_form_q(const double2* A, int N, double2* Qout, LinalgScratch& sc, cplx* gsm) {
-    for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
+// The first ncol columns of Q (N x ncol, ld N) from the factored A into Qout
+// (zungqr, blocked backward; ncol defaults to N).
+static __device__ void cta_form_q(const double2* A, int N, double2* Qout, LinalgScratch& sc, cplx* gsm, int ncol = -1) {
+    if (ncol < 0) ncol = N;
+    for (int e = threadIdx.x; e < N * ncol; e += blockDim.x) {
         int r = e % N, cc = e / N;
         Qout[e] = cmk(r == cc ? 1.0 : 0.0, 0.0);
     }
     __syncthreads();
-    int last = ((N - 1) / QR_NB) * QR_NB;
+    int last = ((ncol - 1) / QR_NB) * QR_NB;
     for (int p = last; p >= 0; p -= QR_NB) {
-        const int jb = min(QR_NB, N - p);
+        const int jb = min(QR_NB, ncol - p);
         build_vblock(A, N, p, jb, sc.Vs);
         const double2* Tp = sc.T + (size_t)(p / QR_NB) * QR_NB * QR_NB;
-        apply_block(sc.Vs, Tp, N, p, jb, Qout, p, N - p, 0, sc, gsm);
+        apply_block(sc.Vs, Tp, N, p, jb, Qout, p, ncol - p, 0, sc, gsm);
     }
 }
 

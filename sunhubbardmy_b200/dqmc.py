@@ -1,9 +1,10 @@
 """ctypes host mirror of the reference's sweep driver over libdqmc_gpu.so.
 
 Names follow the reference: ``dqmc.in`` namelists (src/model_para.f90),
-``sweep_start`` (dqmc_ft_sweep_start_0b), ``sweep_b0`` / ``sweep_0b``
-(dqmc_ft_sweep_b0/0b), ``obser_init``, ``update``, ``h0_prop`` / ``u_prop``
-(the h0conf / uconf type-bound procedures).
+``sweep_start`` (dqmc_ft_sweep_start_0b, or dqmc_proj_sweep_start_0b when
+``proj=1``), ``sweep_b0`` / ``sweep_0b`` (dqmc_ft_sweep_b0/0b or
+dqmc_proj_sweep_b0/0b), ``obser_init``, ``update`` / ``proj_update``,
+``h0_prop`` / ``u_prop`` (the h0conf / uconf type-bound procedures).
 """
 from __future__ import annotations
 
@@ -41,6 +42,7 @@ class DqmcParams(C.Structure):
         ("nflr", C.c_int32), ("lproju", C.c_int32), ("lstabilize", C.c_int32),
         ("nwrap", C.c_int32), ("nsweep", C.c_int32), ("nbin", C.c_int32), ("nublock", C.c_int32),
         ("update", C.c_int32), ("kinetic", C.c_int32), ("hs", C.c_int32),
+        ("proj", C.c_int32), ("lprojv", C.c_int32), ("obs_mid_len", C.c_int32),
         ("ndim", C.c_int32), ("lq", C.c_int32), ("ltrot", C.c_int32), ("nst", C.c_int32),
         ("ne", C.c_int32), ("lcomp", C.c_int32),
     ]
@@ -51,7 +53,8 @@ class DqmcParams(C.Structure):
         d = dict(lattice=SQUARE, l1=2, l2=2, beta=20.0, dtau=0.05, rt=1.0, t2=0.0, t3=0.0, nu=0.0,
                  mu=0.0, rhub=0.0, rv=0.0, alpha=0.2, theta=0.0, xmag=0.0, flux_x=0.0, flux_y=0.0,
                  dimer=0.0, rndness=0.0, nflr=2, lproju=0, lstabilize=1, nwrap=10, nsweep=20,
-                 nbin=10, nublock=0, update=DELAY, kinetic=CHECKERBOARD, hs=GENERAL4)
+                 nbin=10, nublock=0, update=DELAY, kinetic=CHECKERBOARD, hs=GENERAL4, proj=0,
+                 lprojv=0, obs_mid_len=1)
         d.update(kw)
         p = cls(**d)
         rc = load_library().dqmc_params_derive(C.byref(p))
@@ -82,7 +85,8 @@ class DqmcParams(C.Structure):
 class DqmcDiag(C.Structure):
     _fields_ = [(n, C.c_double) for n in (
         "phase_re", "phase_im", "logweight_re", "logweight_im", "max_wrap_error", "max_phasediff",
-        "avglog10error_sum", "logcount", "avgexpphasediff_sum", "accepted", "proposed", "nobs")]
+        "avglog10error_sum", "logcount", "avgexpphasediff_sum", "accepted", "proposed", "nobs",
+        "accepted_v", "proposed_v")]
 
 
 _lib = None
@@ -126,6 +130,15 @@ SIGNATURES = {
     "dqmc_gpu_sweep_kernels": (_i, [_vp]),
     "dqmc_gpu_qr_logdet_noalloc": (_i, [_i, _vp, _vp, _vp, _vp]),
     "dqmc_gpu_noalloc_error": (C.c_char_p, []),
+    "dqmc_gpu_set_vconf": (_i, [_vp, _i, _vp]),
+    "dqmc_gpu_get_vconf": (_i, [_vp, _i, _vp]),
+    "dqmc_gpu_get_trial": (_i, [_vp, _i, _vp, _vp]),
+    "dqmc_gpu_set_trial": (_i, [_vp, _i, _vp]),
+    "dqmc_gpu_get_proj": (_i, [_vp, _i, _vp, _vp, _vp]),
+    "dqmc_gpu_set_proj": (_i, [_vp, _i, _vp, _vp, _vp]),
+    "dqmc_gpu_proj_update": (_i, [_vp, _i, _i]),
+    "dqmc_gpu_proj_green": (_i, [_vp]),
+    "dqmc_trial_state": (_i, [_vp, C.c_int32, _i, _vp, _vp]),
 }
 
 
@@ -177,6 +190,17 @@ def qr_logdet_noalloc(n: int, a_dev: int, q_dev: int, logdetq_dev: int, stream: 
                                       C.c_void_p(logdetq_dev), C.c_void_p(stream))
     if rc != 0:
         raise DqmcError(f"qr_logdet_noalloc failed ({rc}): {L.dqmc_gpu_noalloc_error().decode()}")
+
+
+def trial_state(params: DqmcParams, seed: int, draw_conf: bool = True):
+    """Host-only: the trial state (eigenvectors, eigenvalues) dqmc_gpu_create
+    computes for a walker with this seed (no GPU needed)."""
+    N = params.ndim
+    p = np.zeros((N, N), complex, order="F")
+    w = np.zeros(N)
+    _check(load_library().dqmc_trial_state(C.byref(params), int(seed), int(draw_conf), _ptr(p), _ptr(w)),
+           "dqmc_trial_state")
+    return p, w
 
 
 # ----------------------------------------------------------------------------
@@ -312,7 +336,7 @@ class Dqmc:
                     max_wrap_error=d.max_wrap_error, max_phasediff=d.max_phasediff,
                     avglog10error=d.avglog10error_sum, logcount=d.logcount,
                     avgexpphasediff=d.avgexpphasediff_sum, accepted=d.accepted, proposed=d.proposed,
-                    nobs=d.nobs)
+                    nobs=d.nobs, accepted_v=d.accepted_v, proposed_v=d.proposed_v)
 
     def energy_all(self) -> np.ndarray:
         """energy_bin(1:10) of every chain, shape (n_chains, 10) complex."""
@@ -395,6 +419,50 @@ class Dqmc:
 
     def test_zgemm(self, m, n, k, opa, opb, a, b, c, beta=0.0) -> None:
         _check(load_library().dqmc_gpu_test_zgemm(self.h, m, n, k, opa, opb, a, b, c, float(beta)), "test_zgemm")
+
+    # projective path (params.proj = 1)
+    def vconf(self, c: int = 0) -> np.ndarray:
+        """t-V bond field vconf%conf as [ltrot][nn_nf][ndim] (bond index fastest)."""
+        nnf = 3 if self.chain_params(c).lattice == HONEYCOMB else 4
+        out = np.zeros((self.ltrot, nnf, self.ndim(c)), np.int32)
+        _check(load_library().dqmc_gpu_get_vconf(self.h, c, _ptr(out)), "get_vconf")
+        return out
+
+    def set_vconf(self, v: np.ndarray, c: int = 0) -> None:
+        a = np.ascontiguousarray(v, np.int32)
+        _check(load_library().dqmc_gpu_set_vconf(self.h, c, _ptr(a)), "set_vconf")
+
+    def trial(self, c: int = 0):
+        """(proj, w): trial eigenvectors (ndim x ndim) and eigenvalues of walker c."""
+        N = self.ndim(c)
+        p = np.zeros((N, N), complex, order="F")
+        w = np.zeros(N)
+        _check(load_library().dqmc_gpu_get_trial(self.h, c, _ptr(p), _ptr(w)), "get_trial")
+        return p, w
+
+    def set_trial(self, proj: np.ndarray, c: int = 0) -> None:
+        a = np.asfortranarray(proj, complex)
+        _check(load_library().dqmc_gpu_set_trial(self.h, c, _ptr(a)), "set_trial")
+
+    def proj_state(self, c: int = 0):
+        """(UR, UL, ULRINV) of walker c in the reference's layouts."""
+        N, ne = self.ndim(c), self.chain_params(c).ne
+        ur = np.zeros((N, ne), complex, order="F")
+        ul = np.zeros((ne, N), complex, order="F")
+        li = np.zeros((ne, ne), complex, order="F")
+        _check(load_library().dqmc_gpu_get_proj(self.h, c, _ptr(ur), _ptr(ul), _ptr(li)), "get_proj")
+        return ur, ul, li
+
+    def set_proj_state(self, ur=None, ul=None, ulrinv=None, c: int = 0) -> None:
+        keep = [None if a is None else np.asfortranarray(a, complex) for a in (ur, ul, ulrinv)]
+        ptrs = [None if a is None else _ptr(a) for a in keep]
+        _check(load_library().dqmc_gpu_set_proj(self.h, c, *ptrs), "set_proj")
+
+    def proj_update(self, nt: int, nf: int) -> None:
+        _check(load_library().dqmc_gpu_proj_update(self.h, nt, nf), "proj_update")
+
+    def proj_green(self) -> None:
+        _check(load_library().dqmc_gpu_proj_green(self.h), "proj_green")
 
     def test_qr(self, a: int, q: int) -> np.ndarray:
         ld = np.zeros(2 * self.n_chains)
