@@ -42,6 +42,13 @@ METRIC = "HS site-slice updates/s"
 CONFIG3 = [(dict(lattice=2, l1=L, l2=L, beta=8.0, dtau=0.1, rhub=6.0, nflr=4, kinetic=0, update=2, hs=0,
                  nwrap=10, nublock=32), n) for L, n in ((6, 48), (9, 48), (12, 32))]
 WORKLOAD3 = "honeycomb L=6/9/12 (N=72/162/288, 48/48/32 chains) SU(4) Hubbard U=6 beta=8 dtau=0.1 (ltrot=80), exact HS, submatrix, autotuned flush depth"
+# projective t-V: spinless honeycomb L=12 (N=288, ne=144), V/t=1, projection
+# length 20, dtau=0.1 (ltrot=200, nwrap=10, nst=20), submatrix-LR with
+# nustock=32, trial state = H0 eigenvectors with the reference's rndness=1e-3
+# random hopping perturbation lifting the Dirac-point degeneracy; 64 walkers
+CONFIG4 = dict(lattice=2, l1=12, l2=12, beta=20.0, dtau=0.1, rv=1.0, rhub=0.0, nflr=1, kinetic=0, update=2,
+               nwrap=10, nublock=32, proj=1, rndness=1e-3)
+WORKLOAD4 = "projective spinless t-V, honeycomb L=12 (N=288, ne=144) V=1 theta=20 dtau=0.1 (ltrot=200), submatrix-LR nustock=32, rndness=1e-3 trial, 64 walkers"
 
 
 def test_seed(irank: int) -> int:
@@ -130,21 +137,58 @@ def cpu_sample(nslices: int, threads: int, steps: int = 1, warmup: int = 0):
     return per_step, times, model
 
 
+def cpu_sample_proj(nslices: int, threads: int, steps: int = 1, warmup: int = 0):
+    """The projective workload on the oracle (submatrix-LR bond update, as the
+    reference's -DSUBMATRIX build): one walker per core, nslices slices of a
+    b0 projective sweep per step."""
+    from threadpoolctl import threadpool_limits
+
+    from oracle import pyoracle
+    pyoracle.build()
+    pyoracle.use_scipy_lapack(True)
+    model = pyoracle.Model(**CONFIG4)
+    chains = [pyoracle.Chain(model, test_seed(c)) for c in range(threads)]
+
+    def run(fn):
+        ts = [threading.Thread(target=fn, args=(c,)) for c in chains]
+        t0 = time.perf_counter()
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        return time.perf_counter() - t0
+
+    with threadpool_limits(1):
+        run(lambda c: c.proj_sweep_start())
+        for _ in range(warmup):
+            run(lambda c: c.proj_sweep_b0_slices(nslices))
+        times = [run(lambda c: c.proj_sweep_b0_slices(nslices)) for _ in range(steps)]
+    per_step = threads * nslices * model.nn_nf * model.nn_lf
+    return per_step, times, model
+
+
 def reference_arm(args, rank: int) -> None:
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    nsl = 20
-    per_step, times, model = cpu_sample(nsl, threads, steps=args.steps, warmup=args.warmup)
+    if args.workload == "config4":
+        nsl = 4
+        per_step, times, model = cpu_sample_proj(nsl, threads, steps=args.steps, warmup=min(args.warmup, 1))
+        workload = WORKLOAD4
+        sample = f"{nsl} slices of a b0 projective sweep per walker per step, {threads} walkers on {threads} cores"
+    else:
+        nsl = 20
+        per_step, times, model = cpu_sample(nsl, threads, steps=args.steps, warmup=args.warmup)
+        workload = WORKLOAD
+        sample = f"{nsl} slices of a b0 sweep per chain per step, {threads} chains on {threads} cores (one per core)"
     tot = sum(times)
     value = per_step * len(times) / tot
-    sample = f"{nsl} slices of a b0 sweep per chain per step, {threads} chains on {threads} cores (one per core)"
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
         "data": "synthetic (HS field drawn from the reference's -DTEST seeds)",
-        "config": {"workload": WORKLOAD, "chains": threads, "threads": threads,
+        "config": {"workload": workload, "chains": threads, "threads": threads,
                    "implementation": "C restatement of the Fortran reference (oracle/), OpenBLAS single-threaded per chain"},
         "cpu_baseline": {"value": value, "unit": "updates/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -183,7 +227,12 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     tune_report = None
-    if args.workload == "config3":
+    if args.workload == "config4":
+        p4 = sb.DqmcParams.make(**CONFIG4)
+        nw = args.chains if args.chains_set else 64
+        g = sb.Dqmc(p4, n_chains=nw, seeds=[test_seed(rank * nw + c) for c in range(nw)])
+        workload = WORKLOAD4
+    elif args.workload == "config3":
         from sunhubbardmy_b200.autotune import batched
         groups = [(sb.DqmcParams.make(**kw), n) for kw, n in CONFIG3]
         g, tune_report = batched(groups, tune=True, seed0=rank * sum(n for _, n in CONFIG3))
@@ -215,29 +264,57 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
     if dist is not None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms = float(t.item())
-    per_step = world * int(2 * lt * Ns.sum())
+    proj = bool(p.proj)
+    if proj:
+        nnf = 3 if p.lattice == 2 else 4
+        units = np.array([(nnf * (Nc // 2 if p.lattice == 2 else Nc // 2) if p.rv != 0 else 0) +
+                          (Nc if p.rhub != 0 else 0) for Nc in Ns])
+        per_step = world * int(2 * lt * units.sum())
+    else:
+        per_step = world * int(2 * lt * Ns.sum())
     value = per_step / (ms * 1e-3)
     kernels_per_sweep = g.sweep_kernels()
     d0 = g.diag(0)
     wrap = max(g.diag(c)["max_wrap_error"] for c in range(C))
-    acc = d0["accepted"] / max(1.0, d0["proposed"])
+    if proj and p.rv != 0:
+        acc = d0["accepted_v"] / max(1.0, d0["proposed_v"])
+    else:
+        acc = d0["accepted"] / max(1.0, d0["proposed"])
 
     # end to end through the public API with host buffers: h2d of every chain's
     # HS field, sweep_start + one sweep, d2h of every chain's bins and field
-    nconf = int(lt * Ns.sum())
-    conf_host = torch.empty(nconf, dtype=torch.int32, pin_memory=True).numpy()
-    g.conf_all(conf_host)
     nbins = sum(len(g.bins_raw(c)) for c in range(C)) / C
     e2e_steps = max(1, min(args.steps, 2))
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        g.set_conf_all(conf_host)
-        g.sweep_start()
-        g.sweeps(1, True)
-        bins = [g.bins_raw(c) for c in range(C)]
+    if proj and p.rv != 0:
+        # the bond field of every walker (vconf%conf), walker by walker
+        vhost = [torch.empty(g.vconf(c).shape, dtype=torch.int32, pin_memory=True).numpy() for c in range(C)]
+        for c in range(C):
+            vhost[c][...] = g.vconf(c)
+        nconf = sum(v.size for v in vhost)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            for c in range(C):
+                g.set_vconf(vhost[c], c)
+            g.sweep_start()
+            g.sweeps(1, True)
+            bins = [g.bins_raw(c) for c in range(C)]
+            for c in range(C):
+                vhost[c][...] = g.vconf(c)
+        barrier()
+    else:
+        nconf = int(lt * Ns.sum())
+        conf_host = torch.empty(nconf, dtype=torch.int32, pin_memory=True).numpy()
         g.conf_all(conf_host)
-    barrier()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            g.set_conf_all(conf_host)
+            g.sweep_start()
+            g.sweeps(1, True)
+            bins = [g.bins_raw(c) for c in range(C)]
+            g.conf_all(conf_host)
+        barrier()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
     t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
     if dist is not None:
@@ -246,7 +323,10 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
     del bins
 
     result = None
-    if rank == 0:
+    if rank == 0 and proj:
+        result = proj_roofline_and_line(args, g, p, Ns, ms, value, per_step, world, workload, acc, wrap,
+                                        kernels_per_sweep, clk, e2e_s, nconf, nbins)
+    elif rank == 0:
         # roofline of the dominant kernel: per-kernel device times (CUDA events)
         names = {0: "k_update_delay", 1: "k_stab", 2: "k_green", 3: "k_prop_cols", 4: "k_measure", 5: "k_prop_rows"}
         ops = {k: g.time_op(k, 3) for k in (1, 2, 3, 5, 4, 0)}
@@ -331,18 +411,93 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
         print(json.dumps(result), flush=True)
 
 
+def proj_roofline_and_line(args, g, p, Ns, ms, value, per_step, world, workload, acc, wrap,
+                           kernels_per_sweep, clk, e2e_s, nconf, nbins):
+    """JSON line of the projective workload.  Dominant-kernel roofline from
+    per-kernel CUDA-event times; algorithmic flops of the submatrix-LR update
+    per bond family and walker: 8 [N ne^2 + N R ne + a (2 N ne^2 + N R ne)]
+    (Rrows and Felms GEMMs of every window, the flush GEMMs of accepted rows;
+    R = nustock window rows, a = acceptance)."""
+    import numpy as np
+    C = g.n_chains
+    lt, nst, ne = p.ltrot, p.nst, p.ne
+    R = min(32, p.nublock)
+    names = {0: "k_proj_update", 1: "k_proj_qr", 2: "k_proj_ulr+k_proj_t1+k_proj_gmat", 3: "k_prop_cols (UR)",
+             4: "k_measure", 5: "k_prop_cols (UL^T)"}
+    ops = {k: g.time_op(k, 3) for k in (0, 1, 2, 3, 5, 4)}
+    nnf = 3 if p.lattice == 2 else 4
+    mid = p.obs_mid_len
+    per_sweep = {0: 2 * lt * nnf, 3: 2 * lt * nnf, 5: 2 * lt * nnf, 1: 2 * nst, 2: 4 * nst + 2 * mid, 4: 2 * mid}
+    share = {k: ops[k] * per_sweep[k] for k in ops}
+    total = sum(share.values())
+    dom = max(share, key=share.get)
+    fp64 = fp64_peak_tflops()
+    N = Ns
+    upd = 8.0 * (N * ne ** 2 + N * R * ne + acc * (2 * N * ne ** 2 + N * R * ne))
+    qr = 16.0 * (N * ne ** 2 - ne ** 3 / 3.0)
+    ulrg = 8.0 * (ne ** 2 * N + (2.0 / 3.0 + 1.0 + 0.5) * ne ** 3 + N * ne ** 2 + N * N * ne)
+    flops = {0: float(upd.sum()), 1: float(qr.sum()), 2: float(ulrg.sum())}
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    if dom in flops:
+        ach = flops[dom] / (ops[dom] * 1e-3) / 1e12
+        roof = {"kernel": names[dom], "bound": "tensor", "achieved": ach, "peak": fp64, "unit": "TFLOP/s",
+                "frac": ach / fp64, "traffic": None,
+                "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (FP64 tensor)"}
+    else:
+        byts = 32.0 * float((N * ne).sum()) if dom in (3, 5) else 16.0 * float((N * N).sum())
+        ach = byts / (ops[dom] * 1e-3) / 1e9
+        pk = peaks.get("hbm_gbs", 6650.0)
+        roof = {"kernel": names[dom], "bound": "hbm", "achieved": ach, "peak": pk, "unit": "GB/s",
+                "frac": ach / pk, "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
+    roof["kernel_ms_per_launch"] = {names[k]: ops[k] for k in ops}
+    roof["sweep_share"] = {names[k]: share[k] / total for k in ops}
+    roof["algorithmic_flops_per_launch"] = {names[k]: flops[k] for k in flops}
+    trf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(trf):
+        tr = json.load(open(trf)).get(roof["kernel"])
+        if tr:
+            roof["traffic"] = tr["bytes_per_chain"] * C
+            roof["traffic_note"] = tr.get("note", "")
+    result = {
+        "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic (bond field drawn from the reference's -DTEST seeds, one per walker)",
+        "config": {"workload": workload, "chains_per_gpu": C, "parallelism": f"replicas x{world}",
+                   "l2": "working set ~30 MiB/walker x 64 >> L2 (no flush needed)",
+                   "acceptance": acc, "max_wrap_error": wrap},
+        "e2e": {"value": per_step / e2e_s, "unit": "updates/s",
+                "h2d_bytes_per_step": nconf * 4,
+                "d2h_bytes_per_step": int(C * nbins * 16 + nconf * 4),
+                "note": "per step: set_vconf of every walker (pinned host) + sweep_start + 1 sweep + get_bins + get_vconf"},
+        "gpu_launches": kernels_per_sweep * args.steps,
+        "roofline": roof,
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu:
+        per, times, _ = cpu_sample_proj(4, os.cpu_count() or 1, steps=1)
+        cv = per / times[0]
+        result["cpu_baseline"] = {"value": cv, "unit": "updates/s", "cores": os.cpu_count() or 1, "kind": "port",
+                                  "sample": f"4 slices of a b0 projective sweep per walker, one walker per core "
+                                            f"({os.cpu_count()} cores), submatrix-LR, OpenBLAS"}
+    return result
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--chains", type=int, default=296)
+    ap.add_argument("--chains", type=int, default=None)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--workload", default="config2", choices=["config2", "config3"])
+    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4"])
     ap.add_argument("--ess", type=int, default=0, help="extra sweeps for the ESS/s of double occupancy")
     ap.add_argument("--ess-warmup", type=int, default=20, help="equilibration sweeps before the ESS series")
     args = ap.parse_args()
+    args.chains_set = args.chains is not None
+    if args.chains is None:
+        args.chains = 296
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))

@@ -144,6 +144,7 @@ void orc_get_bins(const orc_chain *c, double *out);
  * is int32 [ltrot][nn_nf][nsites], values 1..2. */
 int  orc_proj_sweep_start_0b(orc_chain *c);
 int  orc_proj_sweep_b0(orc_chain *c, int lupdate, int lmeasure);
+int  orc_proj_sweep_b0_slices(orc_chain *c, int lupdate, int lmeasure, int nslices);
 int  orc_proj_sweep_0b(orc_chain *c, int lupdate, int lmeasure);
 /* trial state: proj (N x N, ascending eigenvectors of set_trial_h0) and its eigenvalues */
 void orc_proj_get_trial(const orc_chain *c, double *proj, double *w);
@@ -155,6 +156,8 @@ void orc_vconf_get(const orc_chain *c, int32_t *v);
 void orc_vconf_set(orc_chain *c, const int32_t *v);
 /* one projective update of slice nt (family nf for the bond field, nf = 0 for the site field) */
 void orc_proj_update(orc_chain *c, int nt, int nf);
+/* explicit flavour: ORC_SUBMATRIX = submatrix-LR bond update, else the fast one */
+void orc_proj_update_flavour(orc_chain *c, int nt, int nf, int flavour);
 /* vconf props on an explicit matrix: left ops on N x n2, right ops on n2 x N */
 void orc_vconf_prop(const orc_model *m, const int32_t *vconf, int op, int nt, int nf, int nflag, double *g, int n2);
 double orc_qr_pqmc_d(int rdim, int cdim, const double *a, double *q);

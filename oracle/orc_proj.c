@@ -4,10 +4,11 @@
  *  - vconf constants, field draw and propagators:
  *      src/dqmc_config_v/dqmc_set_conf.f90:1-79, dqmc_input_conf.f90:36-63,
  *      dqmc_{left,right}_{forward,backward}_prop.f90, _hc
- *  - projective updates, fast flavour (the delayed / submatrix flavours give
- *    the same accept sequence):
- *      src/dqmc_config_v/dqmc_proj_update.f90:1-104 (bond, rank 2)
- *      src/dqmc_config_u/dqmc_proj_update.f90:1-92  (site, rank 1)
+ *  - projective updates (all flavours give the same accept sequence):
+ *      src/dqmc_config_v/dqmc_proj_update.f90:1-104 (bond, rank 2, fast)
+ *      src/dqmc_config_v/dqmc_proj_update_submatrix_LR.f90:1-298 (bond,
+ *        submatrix-LR, selected by update = SUBMATRIX as -DSUBMATRIX does)
+ *      src/dqmc_config_u/dqmc_proj_update.f90:1-92  (site, rank 1, fast)
  *  - trial state: src/dqmc_config_h0/set_trial_h0.f90:1-29,
  *      src/dqmc_proj_core/dqmc_set_proj.f90:1-78
  *  - core: src/dqmc_proj_core/dqmc_proj_sweep_start_0b.f90:1-48,
@@ -293,6 +294,134 @@ static void proj_update_v(orc_chain *c, int nt, int nf) {
     free(vk_tmp); free(vk); free(uk); free(lruk); free(vuvk);
 }
 
+/* dqmc_proj_update, bond field, submatrix-LR flavour
+ * (src/dqmc_config_v/dqmc_proj_update_submatrix_LR.f90:1-298): windows of
+ * nustock = nublock rows; per window Rrows = UR(rows,:) ULRINV and
+ * Felms = Rrows UL(:,rows) by GEMM, the accept test on
+ * F_rr - F_rA Gamma F_Ar with Gamma bordered per accepted bond, and the flush
+ * ULRINV -= (ULRINV UL(:,A)) (Gamma Rrows(A,:)), UR(A,:) *= 1 + Delta. */
+static void proj_update_v_lr(orc_chain *c, int nt, int nf) {
+    const orc_model *m = c->m;
+    const orc_latt *L = &m->L;
+    int N = m->ndim, ne = m->ne, nnf = L->nn_nf, lf = L->nn_lf;
+    int nus = m->nublock > 1 ? m->nublock : 2;
+    nus -= nus % 2;
+    int32_t *cf = c->vconf + ((size_t)(nt - 1) * nnf + (nf - 1)) * N;
+    zc *urP = zalloc((size_t)nus * ne), *ulP = zalloc((size_t)ne * nus), *Rrows = zalloc((size_t)nus * ne);
+    zc *Felms = zalloc((size_t)nus * nus), *Gam = zalloc((size_t)nus * nus);
+    zc *Vmat = zalloc((size_t)nus * ne), *Umat = zalloc((size_t)ne * nus);
+    zc *Vtmp = zalloc((size_t)nus * ne), *Utmp = zalloc((size_t)ne * nus);
+    zc *ikk = zalloc((size_t)nus * 2), *kik = zalloc((size_t)2 * nus), *Gtmp = zalloc((size_t)nus * nus);
+    int *xvec = calloc(nus, sizeof(int)), *svec = calloc(nus, sizeof(int));
+    zc *dvec = zalloc(nus);
+    double accm = 0.0;
+    int ik = 0, istk_s = 0, istk_e = -1, nstk = 0;
+    for (int b = 0; b < lf; ++b) {
+        int i1 = L->nnlf_list[b] - 1;
+        int i2 = L->nnlist[i1 * nnf + nf - 1] - 1;
+        int is = cf[b];
+        int iflip = (int)ceil(orc_sfmt_stream(&c->rng) * 1);
+        int isp = (is + iflip - 1) % 2 + 1;
+        if (nstk == 0) {
+            int nup = nus < (lf - b) * 2 ? nus : (lf - b) * 2;
+            for (int k = 0; k < nup / 2; ++k) {
+                int j1 = L->nnlf_list[b + k] - 1, j2 = L->nnlist[j1 * nnf + nf - 1] - 1;
+                for (int l = 0; l < ne; ++l) {
+                    ulP[ZIDX(l, 2 * k, ne)] = c->UL[ZIDX(l, j1, ne)];
+                    ulP[ZIDX(l, 2 * k + 1, ne)] = c->UL[ZIDX(l, j2, ne)];
+                    urP[ZIDX(2 * k, l, nus)] = c->UR[ZIDX(j1, l, N)];
+                    urP[ZIDX(2 * k + 1, l, nus)] = c->UR[ZIDX(j2, l, N)];
+                }
+            }
+            orc_zgemm('N', 'N', nup, ne, ne, 1.0, urP, nus, c->ULRINV, ne, 0.0, Rrows, nus);
+            orc_zgemm('N', 'N', nup, nup, ne, 1.0, Rrows, nus, ulP, ne, 0.0, Felms, nus);
+            istk_s = b; istk_e = b + nup / 2 - 1; nstk = nup / 2;
+        }
+        int s1 = (b - istk_s) * 2, s2 = s1 + 1;
+        zc v[4];   /* vukmat column-major: v[0]=(1,1) v[1]=(2,1) v[2]=(1,2) v[3]=(2,2) */
+        v[0] = Felms[ZIDX(s1, s1, nus)]; v[1] = Felms[ZIDX(s2, s1, nus)];
+        v[2] = Felms[ZIDX(s1, s2, nus)]; v[3] = Felms[ZIDX(s2, s2, nus)];
+        if (ik > 0) {
+            /* ikktmp = Gamma F(A, r) ; vukmat -= F(r, A) ikktmp */
+            for (int cc = 0; cc < 2; ++cc)
+                for (int x = 0; x < ik; ++x) {
+                    zc sacc = 0;
+                    for (int y = 0; y < ik; ++y) sacc += Gam[ZIDX(x, y, nus)] * Felms[ZIDX(svec[y], s1 + cc, nus)];
+                    ikk[ZIDX(x, cc, nus)] = sacc;
+                }
+            for (int rr = 0; rr < 2; ++rr)
+                for (int cc = 0; cc < 2; ++cc) {
+                    zc sacc = 0;
+                    for (int x = 0; x < ik; ++x) sacc += Felms[ZIDX(s1 + rr, svec[x], nus)] * ikk[ZIDX(x, cc, nus)];
+                    v[rr + 2 * cc] -= sacc;
+                }
+        }
+        zc dp = m->vdp[is - 1], dm = m->vdm[is - 1];
+        v[0] = 1.0 + v[0] * dp; v[1] = v[1] * dp; v[2] = v[2] * dm; v[3] = 1.0 + v[3] * dm;
+        zc ratio1 = v[0] * v[3] - v[2] * v[1];
+        zc ratiotot = ratio1;
+        double ratio_re = creal(ratiotot * c->phase) / creal(c->phase);
+        double ratio_abs = ratio_re < 0 ? -ratio_re : ratio_re;
+        double random = orc_sfmt_stream(&c->rng);
+        if (ratio_abs > random) {
+            accm += 1.0;
+            double weight = sqrt(creal(ratiotot * conj(ratiotot)));
+            c->phase = c->phase * ratiotot / weight;
+            zc gk[4];   /* Gammainv_kk column-major */
+            gk[0] = v[3] * dp / ratio1; gk[2] = -v[2] * dp / ratio1;
+            gk[1] = -v[1] * dm / ratio1; gk[3] = v[0] * dm / ratio1;
+            if (ik > 0) {
+                /* kiktmp = F(r, A) Gamma */
+                for (int rr = 0; rr < 2; ++rr)
+                    for (int y = 0; y < ik; ++y) {
+                        zc sacc = 0;
+                        for (int x = 0; x < ik; ++x) sacc += Felms[ZIDX(s1 + rr, svec[x], nus)] * Gam[ZIDX(x, y, nus)];
+                        kik[ZIDX(rr, y, 2)] = sacc;
+                    }
+                /* new row block -gk kik, new column block -ikk gk, Gamma_AA += ikk gk kik */
+                for (int rr = 0; rr < 2; ++rr)
+                    for (int y = 0; y < ik; ++y)
+                        Gam[ZIDX(ik + rr, y, nus)] = -(gk[rr] * kik[ZIDX(0, y, 2)] + gk[rr + 2] * kik[ZIDX(1, y, 2)]);
+                for (int x = 0; x < ik; ++x)
+                    for (int cc = 0; cc < 2; ++cc)
+                        Gam[ZIDX(x, ik + cc, nus)] = -(ikk[ZIDX(x, 0, nus)] * gk[2 * cc] + ikk[ZIDX(x, 1, nus)] * gk[1 + 2 * cc]);
+                for (int y = 0; y < ik; ++y)
+                    for (int x = 0; x < ik; ++x)
+                        Gam[ZIDX(x, y, nus)] -= ikk[ZIDX(x, 0, nus)] * Gam[ZIDX(ik, y, nus)] + ikk[ZIDX(x, 1, nus)] * Gam[ZIDX(ik + 1, y, nus)];
+            }
+            Gam[ZIDX(ik, ik, nus)] = gk[0]; Gam[ZIDX(ik + 1, ik, nus)] = gk[1];
+            Gam[ZIDX(ik, ik + 1, nus)] = gk[2]; Gam[ZIDX(ik + 1, ik + 1, nus)] = gk[3];
+            xvec[ik] = i1; xvec[ik + 1] = i2;
+            svec[ik] = s1; svec[ik + 1] = s2;
+            dvec[ik] = dp; dvec[ik + 1] = dm;
+            for (int l = 0; l < ne; ++l) {
+                Vmat[ZIDX(ik, l, nus)] = Rrows[ZIDX(s1, l, nus)];
+                Vmat[ZIDX(ik + 1, l, nus)] = Rrows[ZIDX(s2, l, nus)];
+                Umat[ZIDX(l, ik, ne)] = ulP[ZIDX(l, s1, ne)];
+                Umat[ZIDX(l, ik + 1, ne)] = ulP[ZIDX(l, s2, ne)];
+            }
+            ik += 2;
+            cf[b] = isp;
+        }
+        if (b == istk_e || b == lf - 1) {
+            if (ik > 0) {
+                orc_zgemm('N', 'N', ik, ne, ik, 1.0, Gam, nus, Vmat, nus, 0.0, Vtmp, nus);
+                orc_zgemm('N', 'N', ne, ik, ne, 1.0, c->ULRINV, ne, Umat, ne, 0.0, Utmp, ne);
+                orc_zgemm('N', 'N', ne, ne, ik, -1.0, Utmp, ne, Vtmp, nus, 1.0, c->ULRINV, ne);
+                for (int k = 0; k < ik; ++k)
+                    for (int l = 0; l < ne; ++l)
+                        c->UR[ZIDX(xvec[k], l, N)] += dvec[k] * c->UR[ZIDX(xvec[k], l, N)];
+            }
+            ik = 0; nstk = 0;
+            memset(Gam, 0, sizeof(zc) * (size_t)nus * nus);
+        }
+    }
+    c->acc_v += accm;
+    c->prop_v += lf;
+    free(urP); free(ulP); free(Rrows); free(Felms); free(Gam); free(Vmat); free(Umat); free(Vtmp); free(Utmp);
+    free(ikk); free(kik); free(Gtmp); free(xvec); free(svec); free(dvec);
+}
+
 /* dqmc_proj_update, site field (src/dqmc_config_u/dqmc_proj_update.f90:1-92) */
 static void proj_update_u(orc_chain *c, int nt) {
     const orc_model *m = c->m;
@@ -340,8 +469,21 @@ static void proj_update_u(orc_chain *c, int nt) {
     free(vk_tmp); free(vk); free(uk); free(lruk);
 }
 
+/* the build's update flavour: -DSUBMATRIX selects the submatrix-LR bond
+ * update, every other flavour the fast one (same accept sequence) */
+static void proj_update_bond(orc_chain *c, int nt, int nf) {
+    if (c->m->p.update == ORC_SUBMATRIX) proj_update_v_lr(c, nt, nf);
+    else proj_update_v(c, nt, nf);
+}
+
 void orc_proj_update(orc_chain *c, int nt, int nf) {
-    if (nf > 0) proj_update_v(c, nt, nf);
+    if (nf > 0) proj_update_bond(c, nt, nf);
+    else proj_update_u(c, nt);
+}
+
+void orc_proj_update_flavour(orc_chain *c, int nt, int nf, int flavour) {
+    if (nf > 0 && flavour == ORC_SUBMATRIX) proj_update_v_lr(c, nt, nf);
+    else if (nf > 0) proj_update_v(c, nt, nf);
     else proj_update_u(c, nt);
 }
 
@@ -453,8 +595,13 @@ int orc_proj_sweep_start_0b(orc_chain *c) {
     return 0;
 }
 
-/* dqmc_proj_sweep_b0 (src/dqmc_proj_core/dqmc_proj_sweep_b0.f90:1-220) */
+/* dqmc_proj_sweep_b0 (src/dqmc_proj_core/dqmc_proj_sweep_b0.f90:1-220); nslices
+ * limits the sweep to its first nslices time slices (bounded CPU samples). */
+int orc_proj_sweep_b0_slices(orc_chain *c, int lupdate, int lmeasure, int nslices);
 int orc_proj_sweep_b0(orc_chain *c, int lupdate, int lmeasure) {
+    return orc_proj_sweep_b0_slices(c, lupdate, lmeasure, c->m->ltrot);
+}
+int orc_proj_sweep_b0_slices(orc_chain *c, int lupdate, int lmeasure, int nslices) {
     const orc_model *m = c->m;
     int N = m->ndim, ne = m->ne, nst = m->nst, nnf = m->L.nn_nf;
     zc *ultmp = zalloc((size_t)N * ne), *urtmp = zalloc((size_t)N * ne), *q = zalloc((size_t)N * ne);
@@ -463,7 +610,7 @@ int orc_proj_sweep_b0(orc_chain *c, int lupdate, int lmeasure) {
             c->UL[ZIDX(l, i, ne)] = conj(c->projL[ZIDX(i, l, N)]);
             c->Pst[0][ZIDX(i, l, N)] = c->projR[ZIDX(i, l, N)];
         }
-    for (int nt = m->ltrot; nt >= 1; --nt) {
+    for (int nt = m->ltrot; nt >= 1 && nt > m->ltrot - nslices; --nt) {
         if (lmeasure && in_mid(m, nt)) measure_here(c, nt);
         h0_pair(c, ORC_LEFT_BACKWARD, ORC_RIGHT_FORWARD, 0);
         if (m->lwrapu) {
@@ -475,7 +622,7 @@ int orc_proj_sweep_b0(orc_chain *c, int lupdate, int lmeasure) {
             for (int nf = nnf; nf >= 1; --nf) {
                 orc_v_prop(m, c->vconf, ORC_RIGHT_FORWARD, nt, nf, 2, c->UL, ne);
                 orc_v_prop(m, c->vconf, ORC_LEFT_BACKWARD, nt, nf, 2, c->UR, ne);
-                if (lupdate) proj_update_v(c, nt, nf);
+                if (lupdate) proj_update_bond(c, nt, nf);
                 orc_v_prop(m, c->vconf, ORC_RIGHT_FORWARD, nt, nf, 1, c->UL, ne);
                 orc_v_prop(m, c->vconf, ORC_LEFT_BACKWARD, nt, nf, 1, c->UR, ne);
             }
@@ -518,7 +665,7 @@ int orc_proj_sweep_0b(orc_chain *c, int lupdate, int lmeasure) {
             for (int nf = 1; nf <= nnf; ++nf) {
                 orc_v_prop(m, c->vconf, ORC_LEFT_FORWARD, nt, nf, 2, c->UR, ne);
                 orc_v_prop(m, c->vconf, ORC_RIGHT_BACKWARD, nt, nf, 2, c->UL, ne);
-                if (lupdate) proj_update_v(c, nt, nf);
+                if (lupdate) proj_update_bond(c, nt, nf);
                 orc_v_prop(m, c->vconf, ORC_LEFT_FORWARD, nt, nf, 1, c->UR, ne);
                 orc_v_prop(m, c->vconf, ORC_RIGHT_BACKWARD, nt, nf, 1, c->UL, ne);
             }

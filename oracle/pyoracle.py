@@ -108,6 +108,8 @@ def lib() -> C.CDLL:
         L.orc_vconf_get.argtypes = [vp, vp]
         L.orc_vconf_set.argtypes = [vp, vp]
         L.orc_proj_update.argtypes = [vp, C.c_int, C.c_int]
+        L.orc_proj_update_flavour.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+        L.orc_proj_sweep_b0_slices.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         L.orc_vconf_prop.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, C.c_int]
         L.orc_qr_pqmc_d.argtypes = [C.c_int, C.c_int, vp, vp]
         L.orc_qr_pqmc_d.restype = dbl
@@ -320,8 +322,14 @@ class Chain:
         lib().orc_proj_green(self._p)
         return self.green()
 
-    def proj_update(self, nt: int, nf: int) -> None:
-        lib().orc_proj_update(self._p, nt, nf)
+    def proj_update(self, nt: int, nf: int, flavour=None) -> None:
+        if flavour is None:
+            lib().orc_proj_update(self._p, nt, nf)
+        else:
+            lib().orc_proj_update_flavour(self._p, nt, nf, int(flavour))
+
+    def proj_sweep_b0_slices(self, nslices: int, lupdate=True, lmeasure=True) -> None:
+        lib().orc_proj_sweep_b0_slices(self._p, int(lupdate), int(lmeasure), int(nslices))
 
     def proj_sweep_start(self) -> None:
         lib().orc_proj_sweep_start_0b(self._p)

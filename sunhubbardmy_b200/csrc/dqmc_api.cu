@@ -1550,6 +1550,7 @@ extern "C" int dqmc_gpu_u_prop(dqmc_handle* h, int op, int nt) {
 
 extern "C" int dqmc_gpu_update(dqmc_handle* h, int nt) {
     if (!h) return fail(DQMC_EINVAL, "null handle");
+    if (h->proj) return fail(DQMC_ESTATE, "projective handle: use dqmc_gpu_proj_update");
     if (nt < 1 || nt > h->ltrot) return fail(DQMC_EINVAL, "nt out of range");
     launch_sfmt(h->d_chains, h->nch, 1, h->st);
     launch_update(h->d_chains, h->nch, nt, 0, h->st);
@@ -1591,7 +1592,50 @@ extern "C" int dqmc_gpu_time_op(dqmc_handle* h, int op, int reps, double* ms_out
         default: break;
         }
     };
+    // projective handles: 0 bond-family (or site) update, 1 tall QR, 2 (UL UR)^-1
+    // with log det and G, 3 / 5 one slice of propagation over UR / UL^T, 4 measurement
+    int pnf = (m.p.rv != 0.0) ? 1 : 0;
+    auto enqueue_proj = [&]() {
+        switch (op) {
+        case 0: launch_proj_update(h->d_chains, h->nch, 1, pnf, 0, 0, -1, h->st); break;
+        case 1: launch_proj_qr(h->d_chains, h->nch, PMAT_UR, 1, 0, h->st); break;
+        case 2: launch_proj_ulr(h->d_chains, h->nch, PMAT_ULRINV, 1, 1, -1, h->st);
+                launch_proj_green(h->d_chains, h->nch, PMAT_ULRINV, PMAT_GNEW, h->ctas_per_chain, h->st); break;
+        case 3: case 5: {
+            ProjPass pp;
+            PropProg& pr = (op == 3) ? pp.r : pp.l;
+            pk(h, pp, pr, PW_FWD, 0);
+            if (m.p.rv != 0.0)
+                for (int nf = 1; nf <= m.nn_nf; ++nf) {
+                    padd(h, pp, pr, PK_VMIX, 0, nf, 1);
+                    padd(h, pp, pr, PK_VSCALE, PW_FWD, nf, 1);
+                    padd(h, pp, pr, PK_VMIX, 0, nf, 1);
+                }
+            if (m.p.rhub != 0.0) padd(h, pp, pr, PK_DIAG, PW_FWD, 0, 1);
+            pk(h, pp, pr, PW_FWD, 1);
+            pflush(h, pp);
+            break;
+        }
+        case 4: launch_measure(h->d_chains, h->nch, h->ctas_per_chain, h->st); break;
+        default: break;
+        }
+    };
     if (op < 0 || op > 5) return fail(DQMC_EINVAL, "op 0..5");
+    if (h->proj) {
+        if (!h->started) return fail(DQMC_ESTATE, "time_op before sweep_start");
+        if (op == 0) launch_sfmt(h->d_chains, h->nch, 1, h->st);
+        enqueue_proj();
+        CK(cudaStreamSynchronize(h->st));
+        CK(cudaEventRecord(h->ev0, h->st));
+        for (int r = 0; r < reps; ++r) enqueue_proj();
+        CK(cudaEventRecord(h->ev1, h->st));
+        CK(cudaStreamSynchronize(h->st));
+        CK(cudaGetLastError());
+        float ms = 0;
+        cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+        *ms_out = ms / reps;
+        return DQMC_OK;
+    }
     if (op == 0) launch_sfmt(h->d_chains, h->nch, 1, h->st);
     enqueue();   // warm-up
     CK(cudaStreamSynchronize(h->st));
