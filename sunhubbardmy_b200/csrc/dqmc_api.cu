@@ -19,6 +19,7 @@
 #include "../../include/dqmc_gpu.h"
 #include "dqmc_types.h"
 #include "kernels.h"
+#include "zgemm.cuh"
 
 typedef std::complex<double> zc;
 
@@ -456,6 +457,15 @@ static int upload_model(HostModel& m) {
     if ((rc = upload(m, m.snlist, &d.snlist))) return rc;
     if ((rc = upload(m, m.plq, &d.plq_cord))) return rc;
     t = to_d2(m.expar); if ((rc = upload(m, t, &d.expar_nn))) return rc;
+    {
+        std::vector<int> vr(2 * m.nn_lf * m.nn_nf);
+        for (int f = 0; f < m.nn_nf; ++f)
+            for (int b = 0; b < m.nn_lf; ++b) {
+                vr[f * 2 * m.nn_lf + 2 * b] = m.bond_i1[f * m.nn_lf + b];
+                vr[f * 2 * m.nn_lf + 2 * b + 1] = m.bond_i2[f * m.nn_lf + b];
+            }
+        if ((rc = upload(m, vr, &d.vrows))) return rc;
+    }
     void* pd = nullptr;
     if (cudaMalloc(&pd, sizeof(ModelDev)) != cudaSuccess) return fail(DQMC_ENOMEM, "cudaMalloc model");
     m.allocs.push_back(pd);
@@ -868,6 +878,7 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
             d.projLc = (double2*)dalloc(h, Nne * z);
             d.logwDV = (double*)dalloc(h, (size_t)(nst + 2) * sizeof(double));
             d.pw = (double2*)dalloc(h, ((size_t)5 * 32 * ne + 2 * 32 * 32) * z);
+            d.pw_flag = (int*)dalloc(h, 16 * sizeof(int));
             if (!d.UR || !d.ULT || !d.ULRINV || !d.Pst || !d.projR || !d.projLc || !d.logwDV || !d.pw) {
                 dqmc_gpu_destroy(h);
                 return fail(DQMC_ENOMEM, "device allocation failed");
@@ -987,6 +998,28 @@ static PropProg prog_bmat_hc(const HostModel& m, int nt1, int nt2) {
 }
 
 enum { MAT_G = 0, MAT_U = 100, MAT_V = 400 };
+
+// one projective update call (a bond family, or the site field when nf = 0):
+// window count and per-walker CTA counts of the window GEMMs, maximised over
+// the handle's models
+static void proj_update(dqmc_handle* h, int nt, int nf, int visit, int dir, int rnd_off) {
+    int nwin = 0, grg = 1, gfl = 1;
+    for (const HostModel* m : h->models) {
+        int b = nf > 0 ? 2 : 1;
+        int units = nf > 0 ? m->nn_lf : m->N;
+        int R = std::min(m->nublock_dev, 32);
+        R -= R % b;
+        if (R < b) R = b;
+        int upw = R / b, ne = m->p.ne;
+        nwin = std::max(nwin, (units + upw - 1) / upw);
+        int nr = std::min(R, units * b);
+        int t1 = zt_tiles(zt_pick(nr, ne), nr, ne) + zt_tiles(zt_pick(ne, nr), ne, nr);
+        int t3 = zt_tiles(zt_pick(ne, ne), ne, ne);
+        grg = std::max(grg, std::min(t1, 16));
+        gfl = std::max(gfl, std::min(t3, 16));
+    }
+    launch_proj_update(h->d_chains, h->nch, nt, nf, visit, dir, rnd_off, nwin, grg, gfl, h->st);
+}
 
 // one stabilisation of the 0b sweep at stack index n: new factor into the spare
 // slot, Green's function from (new R, old L), wrap check, then swap slots.
@@ -1142,7 +1175,7 @@ static void enqueue_proj_b0(dqmc_handle* h, int lupdate, int lmeasure) {
         pk(h, pp, pp.r, PW_INV, 0);     // h0 left_backward on UR
         pk(h, pp, pp.l, PW_FWD, 0);     // h0 right_forward on UL
         if (lu) {
-            if (lupdate) { pflush(h, pp); launch_proj_update(h->d_chains, h->nch, nt, 0, visit, 1, -1, h->st); }
+            if (lupdate) { pflush(h, pp); proj_update(h, nt, 0, visit, 1, -1); }
             padd(h, pp, pp.l, PK_DIAG, PW_FWD, 0, nt);
             padd(h, pp, pp.r, PK_DIAG, PW_INV, 0, nt);
         }
@@ -1150,7 +1183,7 @@ static void enqueue_proj_b0(dqmc_handle* h, int lupdate, int lmeasure) {
             for (int nf = nnf; nf >= 1; --nf) {
                 padd(h, pp, pp.l, PK_VMIX, 0, nf, nt);           // right_forward, nflag 2
                 padd(h, pp, pp.r, PK_VMIX, 0, nf, nt);           // left_backward, nflag 2
-                if (lupdate) { pflush(h, pp); launch_proj_update(h->d_chains, h->nch, nt, nf, visit, 1, -1, h->st); }
+                if (lupdate) { pflush(h, pp); proj_update(h, nt, nf, visit, 1, -1); }
                 padd(h, pp, pp.l, PK_VSCALE, PW_FWD, nf, nt);    // right_forward, nflag 1
                 padd(h, pp, pp.l, PK_VMIX, 0, nf, nt);
                 padd(h, pp, pp.r, PK_VSCALE, PW_INV, nf, nt);    // left_backward, nflag 1
@@ -1182,14 +1215,14 @@ static void enqueue_proj_0b(dqmc_handle* h, int lupdate, int lmeasure) {
                 padd(h, pp, pp.r, PK_VSCALE, PW_FWD, nf, nt);
                 padd(h, pp, pp.l, PK_VMIX, 0, nf, nt);           // right_backward, nflag 2
                 padd(h, pp, pp.l, PK_VSCALE, PW_INV, nf, nt);
-                if (lupdate) { pflush(h, pp); launch_proj_update(h->d_chains, h->nch, nt, nf, visit, 0, -1, h->st); }
+                if (lupdate) { pflush(h, pp); proj_update(h, nt, nf, visit, 0, -1); }
                 padd(h, pp, pp.r, PK_VMIX, 0, nf, nt);           // nflag 1
                 padd(h, pp, pp.l, PK_VMIX, 0, nf, nt);
             }
         if (lu) {
             padd(h, pp, pp.r, PK_DIAG, PW_FWD, 0, nt);
             padd(h, pp, pp.l, PK_DIAG, PW_INV, 0, nt);
-            if (lupdate) { pflush(h, pp); launch_proj_update(h->d_chains, h->nch, nt, 0, visit, 0, -1, h->st); }
+            if (lupdate) { pflush(h, pp); proj_update(h, nt, 0, visit, 0, -1); }
         }
         pk(h, pp, pp.r, PW_FWD, 1);
         pk(h, pp, pp.l, PW_INV, 1);
@@ -1597,7 +1630,7 @@ extern "C" int dqmc_gpu_time_op(dqmc_handle* h, int op, int reps, double* ms_out
     int pnf = (m.p.rv != 0.0) ? 1 : 0;
     auto enqueue_proj = [&]() {
         switch (op) {
-        case 0: launch_proj_update(h->d_chains, h->nch, 1, pnf, 0, 0, -1, h->st); break;
+        case 0: proj_update(h, 1, pnf, 0, 0, -1); break;
         case 1: launch_proj_qr(h->d_chains, h->nch, PMAT_UR, 1, 0, h->st); break;
         case 2: launch_proj_ulr(h->d_chains, h->nch, PMAT_ULRINV, 1, 1, -1, h->st);
                 launch_proj_green(h->d_chains, h->nch, PMAT_ULRINV, PMAT_GNEW, h->ctas_per_chain, h->st); break;
@@ -1741,7 +1774,7 @@ extern "C" int dqmc_gpu_proj_update(dqmc_handle* h, int nt, int nf) {
         const HostModel& mc = *h->models[h->chains[c].model];
         launch_sfmt_raw(h->d_chains, c, 2 * (nf > 0 ? mc.nn_lf : mc.N), h->st);
     }
-    launch_proj_update(h->d_chains, h->nch, nt, nf, 0, 0, 0, h->st);
+    proj_update(h, nt, nf, 0, 0, 0);
     CK(cudaStreamSynchronize(h->st));
     CK(cudaGetLastError());
     return DQMC_OK;

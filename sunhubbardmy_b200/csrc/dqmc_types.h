@@ -37,6 +37,7 @@ struct ModelDev {
     int proj, ne, lwrapv, rps;         // rps: random words drawn per time slice by the updates
     double2 vbp[2], vbm[2], vbpi[2], vbmi[2];   // bmat_p, bmat_m and inverses, by field value
     double2 vdp[2], vdm[2];                     // delta_bmat_p(1,is), delta_bmat_m(1,is)
+    const int* vrows;          // [nn_nf][2 nn_lf]: rows (i1, i2) of each bond, bonds in order
 };
 
 // Per-chain state.  All pointers are device memory.
@@ -73,6 +74,7 @@ struct ChainDev {
     double* logwDV;            // nst+2
     int32_t* vconf;            // ltrot x nn_nf x N (bond index fastest), values 1..2
     double2* pw;               // update window scratch
+    int* pw_flag;              // per-walker flag: the current window accepted something
 };
 
 // indices into ChainDev::stats

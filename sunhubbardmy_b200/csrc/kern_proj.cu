@@ -172,7 +172,16 @@ __global__ void k_tall_copy(const ChainDev* __restrict__ chains, int dst_id, int
 }
 
 // ---------------------------------------------------------------------------
-// projective local update (submatrix-LR), see the file header
+// projective local update (submatrix-LR), see the file header.  One window of
+// one bond family (or of the sites) is three launches:
+//   k_pwin_rg    (several CTAs per walker)  Rg = UR(rows,:) ULRINV  [nr x ne]
+//                                           Ut = ULRINV UL(:,rows)  [ne x nr]
+//   k_pwin_seq   (one CTA per walker)       F = Rg UL(:,rows), the accept /
+//                reject sequence with Gamma bordering, Vt = Gamma Rg,
+//                UR(A,:) *= 1 + Delta
+//   k_pwin_flush (several CTAs per walker)  ULRINV -= Ut Vt
+// so the window GEMMs use all SMs while the sequential part runs one CTA per
+// walker.  Scratch per walker in pw: Rg (nr x ne), Fg, Gg (nr x nr), Ut, Vt.
 // ---------------------------------------------------------------------------
 struct PUpdSmem {
     double2 F[PW_MAXR * PW_LD];     // F block of the window (window-start values)
@@ -184,32 +193,110 @@ struct PUpdSmem {
     double2 phase;
     int rows[PW_MAXR];
     int accr[PW_MAXR];
-    int acc_flag, nacc;
+    int acc_flag[2], nacc;
     double accm;
+    // per-unit proposal, prepared in parallel before the sequential walk
+    double2 ud1[PW_MAXR], ud2[PW_MAXR];   // Delta of the unit's rows
+    double ur2[PW_MAXR];                  // accept threshold (second draw)
+    int uisp[PW_MAXR], ukk[PW_MAXR];      // proposed value, HS-table index (site field)
 };
 
 DQ_DEV double u32_stream(uint32_t u) { return ((double)u + 0.5) * (1.0 / 4294967296.0); }
 
+// window geometry of one walker: returns false when window w is past the end
+struct PWin {
+    int bond, b, nunits, R, upw, u0, nu, nr;
+    const int* rows;     // global row list of the window (bond field), nullptr for sites
+};
+DQ_DEV bool pwin(const ChainDev& c, int nf, int w, PWin& p) {
+    const ModelDev& md = *c.md;
+    p.bond = nf > 0;
+    p.b = p.bond ? 2 : 1;
+    p.nunits = p.bond ? md.nn_lf : c.N;
+    int R = min(md.nublock, PW_MAXR);
+    R -= R % p.b;
+    if (R < p.b) R = p.b;
+    p.R = R;
+    p.upw = R / p.b;
+    p.u0 = w * p.upw;
+    if (p.u0 >= p.nunits) return false;
+    p.nu = min(p.upw, p.nunits - p.u0);
+    p.nr = p.nu * p.b;
+    p.rows = p.bond ? md.vrows + (size_t)(nf - 1) * 2 * md.nn_lf + 2 * p.u0 : nullptr;
+    return true;
+}
+
+DQ_DEV void pw_ptrs(const ChainDev& c, int R, double2*& Rg, double2*& Fg, double2*& Gg, double2*& Ut, double2*& Vt) {
+    const int ne = c.md->ne;
+    Rg = c.pw;
+    Fg = Rg + (size_t)R * ne;
+    Gg = Fg + (size_t)R * R;
+    Ut = Gg + (size_t)R * R;
+    Vt = Ut + (size_t)ne * R;
+}
+
+// Rg = UR(rows,:) ULRINV and Ut = ULRINV UL(:,rows) = ULRINV ULT(rows,:)^T
+__global__ void __launch_bounds__(256) k_pwin_rg(const ChainDev* __restrict__ chains, int nf, int w) {
+    extern __shared__ double2 ssm[];
+    const ChainDev& c = chains[blockIdx.y];
+    PWin p;
+    if (!pwin(c, nf, w, p)) return;
+    const int N = c.N, ne = c.md->ne;
+    double2 *Rg, *Fg, *Gg, *Ut, *Vt;
+    pw_ptrs(c, p.R, Rg, Fg, Gg, Ut, Vt);
+    ZGemmArgs ga;   // Rg
+    ga.M = p.nr; ga.N = ne; ga.K = ne; ga.alpha = cmk(1, 0); ga.beta = cmk(0, 0);
+    ga.A = p.rows ? c.UR : c.UR + p.u0; ga.lda = N; ga.opA = OP_N; ga.arow = p.rows;
+    ga.B = c.ULRINV; ga.ldb = ne; ga.opB = OP_N; ga.C = Rg; ga.ldc = p.nr;
+    ZGemmArgs gb;   // Ut
+    gb.M = ne; gb.N = p.nr; gb.K = ne; gb.alpha = cmk(1, 0); gb.beta = cmk(0, 0);
+    gb.A = c.ULRINV; gb.lda = ne; gb.opA = OP_N;
+    gb.B = p.rows ? c.ULT : c.ULT + p.u0; gb.ldb = N; gb.opB = OP_T; gb.brow = p.rows;
+    gb.C = Ut; gb.ldc = ne;
+    const int ca = zt_pick(ga.M, ga.N), cb = zt_pick(gb.M, gb.N);
+    const int ta = zt_tiles(ca, ga.M, ga.N), tb = zt_tiles(cb, gb.M, gb.N);
+    for (int t = blockIdx.x; t < ta + tb; t += gridDim.x) {
+        if (t < ta) zgemm_tile(ga, ca, t, ssm);
+        else zgemm_tile(gb, cb, t - ta, ssm);
+    }
+}
+
+// ULRINV -= Ut Vt (skipped when the window accepted nothing)
+__global__ void __launch_bounds__(256) k_pwin_flush(const ChainDev* __restrict__ chains, int nf, int w) {
+    extern __shared__ double2 ssm[];
+    const ChainDev& c = chains[blockIdx.y];
+    PWin p;
+    if (!pwin(c, nf, w, p)) return;
+    if (c.pw_flag[0] == 0) return;
+    const int ne = c.md->ne;
+    double2 *Rg, *Fg, *Gg, *Ut, *Vt;
+    pw_ptrs(c, p.R, Rg, Fg, Gg, Ut, Vt);
+    ZGemmArgs g;
+    g.M = ne; g.N = ne; g.K = p.nr; g.alpha = cmk(-1, 0); g.beta = cmk(1, 0);
+    g.A = Ut; g.lda = ne; g.opA = OP_N; g.B = Vt; g.ldb = p.nr; g.opB = OP_N; g.C = c.ULRINV; g.ldc = ne;
+    const int cl = zt_pick(g.M, g.N), nt = zt_tiles(cl, g.M, g.N);
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) zgemm_tile(g, cl, t, ssm);
+}
+
 // visit: slices already updated in this half sweep; dir 0 = 0b (bond families
 // 1..nn_nf, then sites), 1 = b0 (sites, then families nn_nf..1) fixes where
 // this call's draws sit in the half sweep's random words; rnd_off >= 0
-// overrides that offset.  The window is the model's nublock (nustock) rows.
-__global__ void __launch_bounds__(256) k_proj_update(const ChainDev* __restrict__ chains, int nt, int nf, int visit,
-                                                     int dir, int rnd_off) {
+// overrides that offset.  last = 1 on the family's last window (statistics).
+__global__ void __launch_bounds__(256) k_pwin_seq(const ChainDev* __restrict__ chains, int nt, int nf, int w, int visit,
+                                                  int dir, int rnd_off) {
     extern __shared__ double2 ssm[];
-    const ChainDev c = chains[blockIdx.x];
+    const ChainDev& c = chains[blockIdx.x];
     const ModelDev& md = *c.md;
     const int N = c.N, ne = md.ne, tid = threadIdx.x, nth = blockDim.x;
+    PWin p;
+    if (!pwin(c, nf, w, p)) {
+        if (tid == 0) c.pw_flag[0] = 0;
+        return;
+    }
     double2* buf = ssm;
-    PUpdSmem* S = (PUpdSmem*)(ssm + GemmBig::SMEM_ELEMS);
-    const int bond = nf > 0;
-    const int b = bond ? 2 : 1;
-    const int nunits = bond ? md.nn_lf : N;
+    PUpdSmem* S = (PUpdSmem*)(ssm + ZT_SMEM_ELEMS);
+    const int bond = p.bond, b = p.b, nu = p.nu, nr = p.nr, u0 = p.u0;
     const int lc = bond ? 2 : md.lcomp;
-    int R = min(md.nublock, PW_MAXR);
-    R -= R % b;
-    if (R < b) R = b;
-    const int upw = R / b;
     if (rnd_off < 0) {
         const int vw = md.lwrapv ? 2 * md.nn_lf * md.nn_nf : 0, uw = md.lwrapu ? 2 * N : 0;
         int within;
@@ -219,66 +306,57 @@ __global__ void __launch_bounds__(256) k_proj_update(const ChainDev* __restrict_
     }
     const uint32_t* rnd = c.rnd + rnd_off;
     int32_t* cf = bond ? c.vconf + ((size_t)(nt - 1) * md.nn_nf + (nf - 1)) * N : c.conf + (size_t)(nt - 1) * N;
-    double2* Xg = c.pw;
-    double2* Yg = Xg + (size_t)R * ne;
-    double2* Rg = Yg + (size_t)R * ne;
-    double2* Fg = Rg + (size_t)R * ne;
-    double2* Gg = Fg + (size_t)R * R;
-    double2* Ut = Gg + (size_t)R * R;
-    double2* Vt = Ut + (size_t)ne * R;
+    double2 *Rg, *Fg, *Gg, *Ut, *Vt;
+    pw_ptrs(c, p.R, Rg, Fg, Gg, Ut, Vt);
+    for (int x = tid; x < nr; x += nth) S->rows[x] = p.rows ? p.rows[x] : u0 + x;
     if (tid == 0) {
         S->phase = cmk(c.stats[ST_PHASE_RE], c.stats[ST_PHASE_IM]);
         S->accm = 0.0;
+        S->nacc = 0;
     }
-    for (int u0 = 0; u0 < nunits; u0 += upw) {
-        const int nu = min(upw, nunits - u0), nr = nu * b;
-        for (int k = tid; k < nu; k += nth) {
-            if (bond) {
-                int ist = (nf - 1) * md.nn_lf + u0 + k;
-                S->rows[2 * k] = md.bond_i1[ist];
-                S->rows[2 * k + 1] = md.bond_i2[ist];
-            } else {
-                S->rows[k] = u0 + k;
-            }
+    {   // F = Rg UL(:,rows) = Rg ULT(rows,:)^T
+        ZGemmArgs g;
+        g.M = nr; g.N = nr; g.K = ne; g.alpha = cmk(1, 0); g.beta = cmk(0, 0);
+        g.A = Rg; g.lda = nr; g.opA = OP_N;
+        g.B = p.rows ? c.ULT : c.ULT + u0; g.ldb = N; g.opB = OP_T; g.brow = p.rows;
+        g.C = Fg; g.ldc = nr;
+        zgemm_fit(g, buf);
+    }
+    for (int e = tid; e < nr * nr; e += nth) {
+        int x = e % nr, y = e / nr;
+        double2 v = Fg[e];
+        S->F[x + y * PW_LD] = v;
+        S->Pc[x + y * PW_LD] = v;
+        S->Gm[x + y * PW_LD] = cmk(0, 0);
+    }
+    for (int x = tid; x < nr; x += nth) { S->dl[x] = cmk(0, 0); S->accr[x] = 0; }
+    for (int k = tid; k < nu; k += nth) {
+        const int u = u0 + k;
+        const int is = cf[u];
+        const double r1 = u32_stream(rnd[2 * u]);
+        const int iflip = (int)ceil(r1 * (lc - 1));
+        S->uisp[k] = (is + iflip - 1) % lc + 1;
+        S->ur2[k] = u32_stream(rnd[2 * u + 1]);
+        if (bond) {
+            S->ud1[k] = md.vdp[is - 1];
+            S->ud2[k] = md.vdm[is - 1];
+            S->ukk[k] = 0;
+        } else {
+            const int kk = (is - 1) * (lc - 1) + (iflip - 1);
+            S->ud1[k] = md.delta[kk];
+            S->ud2[k] = cmk(0, 0);
+            S->ukk[k] = kk;
         }
-        __syncthreads();
-        for (int e = tid; e < nr * ne; e += nth) {
-            int x = e % nr, l = e / nr;
-            Xg[e] = c.UR[MIDX(S->rows[x], l, N)];
-            Yg[e] = c.ULT[MIDX(S->rows[x], l, N)];
-        }
-        __syncthreads();
-        {
-            ZGemmArgs g;
-            g.M = nr; g.N = ne; g.K = ne; g.alpha = cmk(1, 0); g.beta = cmk(0, 0);
-            g.A = Xg; g.lda = nr; g.opA = OP_N; g.B = c.ULRINV; g.ldb = ne; g.opB = OP_N; g.C = Rg; g.ldc = nr;
-            zgemm_cta<GemmBig>(g, 0, 1, buf);
-            g.M = nr; g.N = nr; g.K = ne;
-            g.A = Rg; g.lda = nr; g.B = Yg; g.ldb = nr; g.opB = OP_T; g.C = Fg; g.ldc = nr;
-            zgemm_cta<GemmBig>(g, 0, 1, buf);
-        }
-        for (int e = tid; e < nr * nr; e += nth) {
-            int x = e % nr, y = e / nr;
-            double2 v = Fg[e];
-            S->F[x + y * PW_LD] = v;
-            S->Pc[x + y * PW_LD] = v;
-            S->Gm[x + y * PW_LD] = cmk(0, 0);
-        }
-        for (int x = tid; x < nr; x += nth) { S->dl[x] = cmk(0, 0); S->accr[x] = 0; }
-        if (tid == 0) S->nacc = 0;
-        __syncthreads();
-        for (int k = 0; k < nu; ++k) {
-            const int r0 = k * b;
+    }
+    __syncthreads();
+    const int warp = tid >> 5;
+    for (int k = 0; k < nu; ++k) {
+        const int r0 = k * b;
+        if (warp == 0) {
             if (tid == 0) {
-                const int u = u0 + k;
-                const int is = cf[u];
-                const double r1 = u32_stream(rnd[2 * u]), r2 = u32_stream(rnd[2 * u + 1]);
-                const int iflip = (int)ceil(r1 * (lc - 1));
-                const int isp = (is + iflip - 1) % lc + 1;
-                double2 ratiotot, g11, g12 = cmk(0, 0), g21 = cmk(0, 0), g22 = cmk(0, 0), d1, d2 = cmk(0, 0);
+                double2 ratiotot, g11, g12 = cmk(0, 0), g21 = cmk(0, 0), g22 = cmk(0, 0);
+                const double2 d1 = S->ud1[k], d2 = S->ud2[k];
                 if (bond) {
-                    d1 = md.vdp[is - 1];
-                    d2 = md.vdm[is - 1];
                     double2 v11 = cadd(cmk(1, 0), cmul(S->Pc[r0 + r0 * PW_LD], d1));
                     double2 v21 = cmul(S->Pc[r0 + 1 + r0 * PW_LD], d1);
                     double2 v12 = cmul(S->Pc[r0 + (r0 + 1) * PW_LD], d2);
@@ -291,8 +369,7 @@ __global__ void __launch_bounds__(256) k_proj_update(const ChainDev* __restrict_
                     g21 = cmul(cmul(cmk(-v21.x, -v21.y), d2), id);
                     g22 = cmul(cmul(v11, d2), id);
                 } else {
-                    const int kk = (is - 1) * (lc - 1) + (iflip - 1);
-                    d1 = md.delta[kk];
+                    const int kk = S->ukk[k];
                     double2 ratio1 = cadd(cmk(1, 0), cmul(S->Pc[r0 + r0 * PW_LD], d1));
                     double2 r = ratio1;
                     for (int f = 1; f < md.nflr; ++f) r = cmul(r, ratio1);
@@ -302,11 +379,11 @@ __global__ void __launch_bounds__(256) k_proj_update(const ChainDev* __restrict_
                 }
                 const double2 ph = S->phase;
                 double ratio_re = cmul(ratiotot, ph).x / ph.x;
-                int acc = fabs(ratio_re) > r2;
+                int acc = fabs(ratio_re) > S->ur2[k];
                 if (acc) {
                     double wgt = sqrt(cmul(ratiotot, cconj(ratiotot)).x);
                     S->phase = cscale(cmul(ph, ratiotot), 1.0 / wgt);
-                    cf[u] = isp;
+                    cf[u0 + k] = S->uisp[k];
                     S->accm += 1.0;
                     S->gkk[0] = g11; S->gkk[1] = g21; S->gkk[2] = g12; S->gkk[3] = g22;   // column-major b x b
                     S->dl[r0] = d1;
@@ -314,85 +391,89 @@ __global__ void __launch_bounds__(256) k_proj_update(const ChainDev* __restrict_
                     if (bond) { S->dl[r0 + 1] = d2; S->accr[r0 + 1] = 1; }
                     S->nacc += b;
                 }
-                S->acc_flag = acc;
+                S->acc_flag[k & 1] = acc;
             }
-            __syncthreads();
-            if (!S->acc_flag) continue;
-            // snapshots: columns/rows r of the current block, Gamma F_Ar and F_rA Gamma
-            for (int e = tid; e < nr * b; e += nth) {
+        } else {
+            // warps 1..7, while warp 0 decides: columns / rows r of the current
+            // block and Gamma F_Ar, F_rA Gamma (four partial sums per product)
+            for (int e = tid - 32; e < nr * b; e += nth - 32) {
                 int x = e % nr, cc = e / nr;
                 S->colr[x + cc * PW_MAXR] = S->Pc[x + (r0 + cc) * PW_LD];
                 S->rowr[x + cc * PW_MAXR] = S->Pc[r0 + cc + x * PW_LD];
-                double2 a = cmk(0, 0), bb = cmk(0, 0);
-                for (int y = 0; y < r0; ++y) {
-                    a = cfma(S->Gm[x + y * PW_LD], S->F[y + (r0 + cc) * PW_LD], a);
-                    bb = cfma(S->F[r0 + cc + y * PW_LD], S->Gm[y + x * PW_LD], bb);
+                double2 a[4] = {cmk(0, 0), cmk(0, 0), cmk(0, 0), cmk(0, 0)};
+                double2 bb[4] = {cmk(0, 0), cmk(0, 0), cmk(0, 0), cmk(0, 0)};
+                int y = 0;
+                for (; y + 3 < r0; y += 4)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        a[q] = cfma(S->Gm[x + (y + q) * PW_LD], S->F[y + q + (r0 + cc) * PW_LD], a[q]);
+                        bb[q] = cfma(S->F[r0 + cc + (y + q) * PW_LD], S->Gm[y + q + x * PW_LD], bb[q]);
+                    }
+                for (; y < r0; ++y) {
+                    a[0] = cfma(S->Gm[x + y * PW_LD], S->F[y + (r0 + cc) * PW_LD], a[0]);
+                    bb[0] = cfma(S->F[r0 + cc + y * PW_LD], S->Gm[y + x * PW_LD], bb[0]);
                 }
-                S->ikk[x + cc * PW_MAXR] = a;
-                S->kik[x + cc * PW_MAXR] = bb;
+                S->ikk[x + cc * PW_MAXR] = cadd(cadd(a[0], a[1]), cadd(a[2], a[3]));
+                S->kik[x + cc * PW_MAXR] = cadd(cadd(bb[0], bb[1]), cadd(bb[2], bb[3]));
             }
-            __syncthreads();
-            for (int e = tid; e < nr * nr; e += nth) {
-                int x = e % nr, y = e / nr;
-                const bool xr = (x >= r0 && x < r0 + b), yr = (y >= r0 && y < r0 + b);
-                if (x < r0 && y < r0) {
-                    double2 s = cmk(0, 0);
-                    for (int p = 0; p < b; ++p)
-                        for (int q = 0; q < b; ++q)
-                            s = cfma(cmul(S->ikk[x + p * PW_MAXR], S->gkk[p + q * b]), S->kik[y + q * PW_MAXR], s);
-                    S->Gm[x + y * PW_LD] = cadd(S->Gm[x + y * PW_LD], s);
-                } else if (xr && y < r0) {
-                    double2 s = cmk(0, 0);
-                    for (int q = 0; q < b; ++q) s = cfma(S->gkk[(x - r0) + q * b], S->kik[y + q * PW_MAXR], s);
-                    S->Gm[x + y * PW_LD] = cmk(-s.x, -s.y);
-                } else if (x < r0 && yr) {
-                    double2 s = cmk(0, 0);
-                    for (int p = 0; p < b; ++p) s = cfma(S->ikk[x + p * PW_MAXR], S->gkk[p + (y - r0) * b], s);
-                    S->Gm[x + y * PW_LD] = cmk(-s.x, -s.y);
-                } else if (xr && yr) {
-                    S->Gm[x + y * PW_LD] = S->gkk[(x - r0) + (y - r0) * b];
-                } else if (x >= r0 + b && y >= r0 + b) {
-                    double2 s = cmk(0, 0);
-                    for (int p = 0; p < b; ++p)
-                        for (int q = 0; q < b; ++q)
-                            s = cfma(cmul(S->colr[x + p * PW_MAXR], S->gkk[p + q * b]), S->rowr[y + q * PW_MAXR], s);
-                    S->Pc[x + y * PW_LD] = csub(S->Pc[x + y * PW_LD], s);
-                }
-            }
-            __syncthreads();
         }
-        if (S->nacc > 0) {
-            for (int e = tid; e < nr * nr; e += nth) {
-                int x = e % nr, y = e / nr;
-                Gg[e] = S->Gm[x + y * PW_LD];
-            }
-            __syncthreads();
-            ZGemmArgs g;
-            g.M = ne; g.N = nr; g.K = ne; g.alpha = cmk(1, 0); g.beta = cmk(0, 0);
-            g.A = c.ULRINV; g.lda = ne; g.opA = OP_N; g.B = Yg; g.ldb = nr; g.opB = OP_T; g.C = Ut; g.ldc = ne;
-            zgemm_cta<GemmBig>(g, 0, 1, buf);
-            g.M = nr; g.N = ne; g.K = nr;
-            g.A = Gg; g.lda = nr; g.B = Rg; g.ldb = nr; g.opB = OP_N; g.C = Vt; g.ldc = nr;
-            zgemm_cta<GemmBig>(g, 0, 1, buf);
-            g.M = ne; g.N = ne; g.K = nr; g.alpha = cmk(-1, 0); g.beta = cmk(1, 0);
-            g.A = Ut; g.lda = ne; g.B = Vt; g.ldb = nr; g.C = c.ULRINV; g.ldc = ne;
-            zgemm_cta<GemmBig>(g, 0, 1, buf);
-            for (int e = tid; e < nr * ne; e += nth) {
-                int x = e % nr, l = e / nr;
-                if (S->accr[x]) {
-                    double2* p = c.UR + MIDX(S->rows[x], l, N);
-                    double2 v = *p;
-                    *p = cadd(v, cmul(S->dl[x], v));
-                }
+        __syncthreads();
+        if (!S->acc_flag[k & 1]) continue;
+        for (int e = tid; e < nr * nr; e += nth) {
+            int x = e % nr, y = e / nr;
+            const bool xr = (x >= r0 && x < r0 + b), yr = (y >= r0 && y < r0 + b);
+            if (x < r0 && y < r0) {
+                double2 sacc = cmk(0, 0);
+                for (int pp = 0; pp < b; ++pp)
+                    for (int q = 0; q < b; ++q)
+                        sacc = cfma(cmul(S->ikk[x + pp * PW_MAXR], S->gkk[pp + q * b]), S->kik[y + q * PW_MAXR], sacc);
+                S->Gm[x + y * PW_LD] = cadd(S->Gm[x + y * PW_LD], sacc);
+            } else if (xr && y < r0) {
+                double2 sacc = cmk(0, 0);
+                for (int q = 0; q < b; ++q) sacc = cfma(S->gkk[(x - r0) + q * b], S->kik[y + q * PW_MAXR], sacc);
+                S->Gm[x + y * PW_LD] = cmk(-sacc.x, -sacc.y);
+            } else if (x < r0 && yr) {
+                double2 sacc = cmk(0, 0);
+                for (int pp = 0; pp < b; ++pp) sacc = cfma(S->ikk[x + pp * PW_MAXR], S->gkk[pp + (y - r0) * b], sacc);
+                S->Gm[x + y * PW_LD] = cmk(-sacc.x, -sacc.y);
+            } else if (xr && yr) {
+                S->Gm[x + y * PW_LD] = S->gkk[(x - r0) + (y - r0) * b];
+            } else if (x >= r0 + b && y >= r0 + b) {
+                double2 sacc = cmk(0, 0);
+                for (int pp = 0; pp < b; ++pp)
+                    for (int q = 0; q < b; ++q)
+                        sacc = cfma(cmul(S->colr[x + pp * PW_MAXR], S->gkk[pp + q * b]), S->rowr[y + q * PW_MAXR], sacc);
+                S->Pc[x + y * PW_LD] = csub(S->Pc[x + y * PW_LD], sacc);
             }
         }
         __syncthreads();
     }
+    const int any = S->nacc > 0;
+    if (any) {
+        for (int e = tid; e < nr * nr; e += nth) {
+            int x = e % nr, y = e / nr;
+            Gg[e] = S->Gm[x + y * PW_LD];
+        }
+        __syncthreads();
+        ZGemmArgs g;   // Vt = Gamma Rg
+        g.M = nr; g.N = ne; g.K = nr; g.alpha = cmk(1, 0); g.beta = cmk(0, 0);
+        g.A = Gg; g.lda = nr; g.opA = OP_N; g.B = Rg; g.ldb = nr; g.opB = OP_N; g.C = Vt; g.ldc = nr;
+        zgemm_fit(g, buf);
+        for (int e = tid; e < nr * ne; e += nth) {
+            int x = e % nr, l = e / nr;
+            if (S->accr[x]) {
+                double2* q = c.UR + MIDX(S->rows[x], l, N);
+                double2 v = *q;
+                *q = cadd(v, cmul(S->dl[x], v));
+            }
+        }
+    }
     if (tid == 0) {
+        c.pw_flag[0] = any;
         c.stats[ST_PHASE_RE] = S->phase.x;
         c.stats[ST_PHASE_IM] = S->phase.y;
         c.stats[bond ? ST_ACCV : ST_ACC] += S->accm;
-        c.stats[bond ? ST_PROPV : ST_PROP] += (double)nunits;
+        c.stats[bond ? ST_PROPV : ST_PROP] += (double)nu;
     }
 }
 
@@ -404,10 +485,12 @@ static size_t g_proj_la = 0, g_proj_upd = 0;
 
 void set_proj_maxN(int maxN) {
     g_proj_la = proj_la_smem(maxN);
-    g_proj_upd = (size_t)GemmBig::SMEM_ELEMS * sizeof(double2) + sizeof(PUpdSmem) + 64;
+    g_proj_upd = (size_t)ZT_SMEM_ELEMS * sizeof(double2) + sizeof(PUpdSmem) + 64;
     cudaFuncSetAttribute(k_proj_qr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g_proj_la);
     cudaFuncSetAttribute(k_proj_ulr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g_proj_la);
-    cudaFuncSetAttribute(k_proj_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g_proj_upd);
+    cudaFuncSetAttribute(k_pwin_seq, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g_proj_upd);
+    cudaFuncSetAttribute(k_pwin_rg, cudaFuncAttributeMaxDynamicSharedMemorySize, ZT_SMEM_ELEMS * (int)sizeof(double2));
+    cudaFuncSetAttribute(k_pwin_flush, cudaFuncAttributeMaxDynamicSharedMemorySize, ZT_SMEM_ELEMS * (int)sizeof(double2));
     cudaFuncSetAttribute(k_proj_t1, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmBig::SMEM_ELEMS * (int)sizeof(double2));
     cudaFuncSetAttribute(k_proj_gmat, cudaFuncAttributeMaxDynamicSharedMemorySize, GemmBig::SMEM_ELEMS * (int)sizeof(double2));
     g_proj_attr = 1;
@@ -431,7 +514,14 @@ void launch_tall_copy(const ChainDev* chains, int nchains, int dst_id, int src_i
     k_tall_copy<<<dim3(8, nchains), 256, 0, st>>>(chains, dst_id, src_id);
 }
 
+// one family (nf >= 1) or the site field (nf = 0) of slice nt: nwin windows,
+// g_rg / g_fl CTAs per walker for the window GEMMs
 void launch_proj_update(const ChainDev* chains, int nchains, int nt, int nf, int visit, int dir, int rnd_off,
-                        cudaStream_t st) {
-    k_proj_update<<<nchains, 256, g_proj_upd, st>>>(chains, nt, nf, visit, dir, rnd_off);
+                        int nwin, int g_rg, int g_fl, cudaStream_t st) {
+    size_t sm = (size_t)ZT_SMEM_ELEMS * sizeof(double2);
+    for (int w = 0; w < nwin; ++w) {
+        k_pwin_rg<<<dim3(g_rg, nchains), 256, sm, st>>>(chains, nf, w);
+        k_pwin_seq<<<nchains, 256, g_proj_upd, st>>>(chains, nt, nf, w, visit, dir, rnd_off);
+        k_pwin_flush<<<dim3(g_fl, nchains), 256, sm, st>>>(chains, nf, w);
+    }
 }

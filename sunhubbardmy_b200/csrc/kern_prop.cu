@@ -22,53 +22,70 @@ __device__ void apply_op(const ModelDev& md, const int32_t* conf, const int32_t*
                          double2* S, int nv, int vs) {
     const int kind = code & 15, which = (code >> 4) & 15, nf = (code >> 8) & 255, nt = code >> 16;
     const int N = md.N, tid = threadIdx.x, nth = blockDim.x;
-    if (kind == PK_CB) {
+    // CB, DIAG and bond-field ops: a thread owns one bond (or site) and applies
+    // it to a group of the nv vectors, so the bond's indices and coefficients
+    // are loaded once per op instead of once per vector
+    if (kind == PK_CB || kind == PK_VMIX || kind == PK_VSCALE) {
         const int lf = md.nn_lf;
+        const int ngrp = max(1, min(nv, nth / lf));
+        const int per = (nv + ngrp - 1) / ngrp;
+        const double h = 1.0 / sqrt(2.0);
         const double2* U = (which == PW_INV) ? md.urtm1 : md.urt;
-        for (int w = tid; w < nv * lf; w += nth) {
-            int v = w / lf, b = w % lf;
-            int ist = (nf - 1) * lf + b;
-            int i1 = md.bond_i1[ist], i2 = md.bond_i2[ist];
-            const double2* u = U + 4 * ist;   // u[0]=(1,1) u[1]=(1,2) u[2]=(2,1) u[3]=(2,2)
-            double2* x = S + (size_t)v * vs;
-            double2 a = x[i1], c = x[i2];
-            if (!right) {
-                x[i1] = cadd(cmul(u[0], a), cmul(u[1], c));
-                x[i2] = cadd(cmul(u[2], a), cmul(u[3], c));
+        const int32_t* vc = (kind == PK_VSCALE) ? vconf + ((size_t)(nt - 1) * md.nn_nf + (nf - 1)) * N : nullptr;
+        for (int w = tid; w < lf * ngrp; w += nth) {
+            const int b = w % lf, g = w / lf;
+            const int v0 = g * per, v1 = min(nv, v0 + per);
+            const int ist = (nf - 1) * lf + b;
+            const int i1 = __ldg(&md.bond_i1[ist]), i2 = __ldg(&md.bond_i2[ist]);
+            double2 c0, c1, c2, c3;   // x1' = c0 x1 + c1 x2, x2' = c2 x1 + c3 x2
+            if (kind == PK_CB) {
+                const double2* u = U + 4 * ist;   // u[0]=(1,1) u[1]=(1,2) u[2]=(2,1) u[3]=(2,2)
+                if (!right) { c0 = __ldg(&u[0]); c1 = __ldg(&u[1]); c2 = __ldg(&u[2]); c3 = __ldg(&u[3]); }
+                else { c0 = __ldg(&u[0]); c1 = __ldg(&u[2]); c2 = __ldg(&u[1]); c3 = __ldg(&u[3]); }
+                for (int v = v0; v < v1; ++v) {
+                    double2* x = S + (size_t)v * vs;
+                    double2 a = x[i1], c = x[i2];
+                    if (!right) {
+                        x[i1] = cadd(cmul(c0, a), cmul(c1, c));
+                        x[i2] = cadd(cmul(c2, a), cmul(c3, c));
+                    } else {
+                        x[i1] = cadd(cmul(a, c0), cmul(c, c1));
+                        x[i2] = cadd(cmul(a, c2), cmul(c, c3));
+                    }
+                }
+            } else if (kind == PK_VMIX) {
+                // x <- H x, H = H^T = [[1,1],[1,-1]]/sqrt2 (the same from either side)
+                for (int v = v0; v < v1; ++v) {
+                    double2* x = S + (size_t)v * vs;
+                    double2 a = x[i1], c = x[i2];
+                    x[i1] = cadd(cscale(a, h), cscale(c, h));
+                    x[i2] = cadd(cscale(a, h), cscale(c, -h));
+                }
             } else {
-                x[i1] = cadd(cmul(a, u[0]), cmul(c, u[2]));
-                x[i2] = cadd(cmul(a, u[1]), cmul(c, u[3]));
+                // x_i1 *= s1(is), x_i2 *= s2(is)
+                const int is = __ldg(&vc[b]) - 1;
+                const double2 s1 = (which == PW_INV) ? md.vbpi[is] : md.vbp[is];
+                const double2 s2 = (which == PW_INV) ? md.vbmi[is] : md.vbm[is];
+                for (int v = v0; v < v1; ++v) {
+                    double2* x = S + (size_t)v * vs;
+                    x[i1] = cmul(s1, x[i1]);
+                    x[i2] = cmul(s2, x[i2]);
+                }
             }
         }
     } else if (kind == PK_DIAG) {
         const int32_t* cf = conf + (size_t)(nt - 1) * N;
-        for (int w = tid; w < nv * N; w += nth) {
-            int v = w / N, i = w % N;
-            int is = cf[i] - 1;
+        const int ngrp = max(1, min(nv, nth / N));
+        const int per = (nv + ngrp - 1) / ngrp;
+        for (int w = tid; w < N * ngrp; w += nth) {
+            const int i = w % N, g = w / N;
+            const int v0 = g * per, v1 = min(nv, v0 + per);
+            const int is = __ldg(&cf[i]) - 1;
             double2 b = (which == PW_INV) ? md.bmat_inv[is] : md.bmat[is];
             if (which == PW_CONJ) b.y = -b.y;
-            double2* x = S + (size_t)v * vs;
-            x[i] = cmul(x[i], b);
-        }
-    } else if (kind == PK_VMIX || kind == PK_VSCALE) {
-        // bond (i1, i2) of family nf: x <- H x (H = H^T = [[1,1],[1,-1]]/sqrt2, the same
-        // from either side) or x_i1 *= s1(is), x_i2 *= s2(is)
-        const int lf = md.nn_lf;
-        const double h = 1.0 / sqrt(2.0);
-        const int32_t* vc = vconf + ((size_t)(nt - 1) * md.nn_nf + (nf - 1)) * N;
-        for (int w = tid; w < nv * lf; w += nth) {
-            int v = w / lf, b = w % lf;
-            int ist = (nf - 1) * lf + b;
-            int i1 = md.bond_i1[ist], i2 = md.bond_i2[ist];
-            double2* x = S + (size_t)v * vs;
-            double2 a = x[i1], c = x[i2];
-            if (kind == PK_VMIX) {
-                x[i1] = cadd(cscale(a, h), cscale(c, h));
-                x[i2] = cadd(cscale(a, h), cscale(c, -h));
-            } else {
-                int is = vc[b] - 1;
-                x[i1] = cmul((which == PW_INV) ? md.vbpi[is] : md.vbp[is], a);
-                x[i2] = cmul((which == PW_INV) ? md.vbmi[is] : md.vbm[is], c);
+            for (int v = v0; v < v1; ++v) {
+                double2* x = S + (size_t)v * vs;
+                x[i] = cmul(x[i], b);
             }
         }
     } else if (kind == PK_FFT) {

@@ -40,4 +40,4 @@ void launch_proj_ulr(const ChainDev* chains, int nchains, int out_id, int logdet
 void launch_proj_green(const ChainDev* chains, int nchains, int inv_id, int dst_id, int ctas, cudaStream_t st);
 void launch_tall_copy(const ChainDev* chains, int nchains, int dst_id, int src_id, cudaStream_t st);
 void launch_proj_update(const ChainDev* chains, int nchains, int nt, int nf, int visit, int dir, int rnd_off,
-                        cudaStream_t st);
+                        int nwin, int g_rg, int g_fl, cudaStream_t st);

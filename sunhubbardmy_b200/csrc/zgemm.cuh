@@ -19,6 +19,10 @@ struct ZGemmArgs {
     const cplx* A; int lda; int opA;
     const cplx* B; int ldb; int opB;
     cplx* C; int ldc;
+    // optional row gathers: row m of op(A) = A row arow[m] (opA = OP_N), row n of
+    // op(B)^T = B row brow[n] (opB = OP_T / OP_C); nullptr = contiguous rows
+    const int* arow = nullptr;
+    const int* brow = nullptr;
 };
 
 // no `volatile`: the compiler may interleave independent DMMAs
@@ -59,7 +63,7 @@ DQ_DEV void zgemm_load_stage(const ZGemmArgs& g, int m0, int n0, int k0, cplx* A
             int m = e % BM, k = e / BM;
             int gm = m0 + m, gk = k0 + k;
             bool v = gm < g.M && gk < g.K;
-            const cplx* src = v ? g.A + MIDX(gm, gk, g.lda) : g.A;
+            const cplx* src = v ? g.A + MIDX(g.arow ? g.arow[gm] : gm, gk, g.lda) : g.A;
             cp_async16(&As[k * Cfg::LDA + m], src, v);
         }
     } else {
@@ -85,7 +89,7 @@ DQ_DEV void zgemm_load_stage(const ZGemmArgs& g, int m0, int n0, int k0, cplx* A
             int n = e % BN, k = e / BN;
             int gn = n0 + n, gk = k0 + k;
             bool v = gn < g.N && gk < g.K;
-            const cplx* src = v ? g.B + MIDX(gn, gk, g.ldb) : g.B;
+            const cplx* src = v ? g.B + MIDX(g.brow ? g.brow[gn] : gn, gk, g.ldb) : g.B;
             cp_async16(&Bs[k * Cfg::LDB + n], src, v);
         }
     }
@@ -203,3 +207,44 @@ __device__ void zgemm_cta(const ZGemmArgs& g, int tile0, int tstep, cplx* smem) 
 typedef ZGemmCfg<64, 64, 16, 2, 4> GemmBig;     // square-ish products
 typedef ZGemmCfg<32, 64, 16, 2, 4> GemmMid;     // panels with M <= 32
 typedef ZGemmCfg<16, 128, 16, 1, 8> GemmWide;   // M = 16 rows (reflector blocks)
+// small shapes whose sides are multiples of 16 or 48 (the projective update's
+// window GEMMs: window rows 32, ne = 144 at the benchmark size)
+typedef ZGemmCfg<48, 48, 16, 3, 2> Gemm48x48;
+typedef ZGemmCfg<32, 48, 16, 2, 2> Gemm32x48;
+typedef ZGemmCfg<48, 32, 16, 3, 2> Gemm48x32;
+typedef ZGemmCfg<32, 32, 16, 2, 2> Gemm32x32;
+
+// tile shape with the least padded area for an M x N product (ties: larger tiles)
+enum { ZT_64x64 = 0, ZT_48x48, ZT_32x48, ZT_48x32, ZT_32x32, ZT_COUNT };
+__host__ __device__ inline int zt_bm(int c) { const int v[ZT_COUNT] = {64, 48, 32, 48, 32}; return v[c]; }
+__host__ __device__ inline int zt_bn(int c) { const int v[ZT_COUNT] = {64, 48, 48, 32, 32}; return v[c]; }
+__host__ __device__ inline int zt_tiles(int c, int M, int N) {
+    return ((M + zt_bm(c) - 1) / zt_bm(c)) * ((N + zt_bn(c) - 1) / zt_bn(c));
+}
+__host__ __device__ inline int zt_pick(int M, int N) {
+    int best = 0;
+    long long ba = (long long)zt_tiles(0, M, N) * 64 * 64;
+    for (int c = 1; c < ZT_COUNT; ++c) {
+        long long a = (long long)zt_tiles(c, M, N) * zt_bm(c) * zt_bn(c);
+        if (a < ba) { ba = a; best = c; }
+    }
+    return best;
+}
+constexpr int ZT_SMEM_ELEMS = GemmBig::SMEM_ELEMS;   // the largest of the shapes above
+
+// tile t (0 <= t < zt_tiles) of C = alpha op(A) op(B) + beta C in shape class cls
+DQ_DEV void zgemm_tile(const ZGemmArgs& g, int cls, int t, cplx* smem) {
+    const int big = 1 << 30;
+    switch (cls) {
+    case ZT_48x48: zgemm_cta<Gemm48x48>(g, t, big, smem); break;
+    case ZT_32x48: zgemm_cta<Gemm32x48>(g, t, big, smem); break;
+    case ZT_48x32: zgemm_cta<Gemm48x32>(g, t, big, smem); break;
+    case ZT_32x32: zgemm_cta<Gemm32x32>(g, t, big, smem); break;
+    default: zgemm_cta<GemmBig>(g, t, big, smem); break;
+    }
+}
+// every tile, by the whole CTA, in the best-fitting shape
+DQ_DEV void zgemm_fit(const ZGemmArgs& g, cplx* smem) {
+    const int cls = zt_pick(g.M, g.N), nt = zt_tiles(cls, g.M, g.N);
+    for (int t = 0; t < nt; ++t) zgemm_tile(g, cls, t, smem);
+}
