@@ -148,3 +148,40 @@ def test_replica_bin_reduction_two_gloo_ranks():
         assert abs(e0 - 8.0 / (4 * 3)) < 1e-12
     assert res[0][1] == [1909706392, 501232835]
     assert set(res[0][1]).isdisjoint(res[1][1])
+
+
+@pytest.mark.parametrize("kw", [
+    dict(lattice=2, l1=3, l2=3, beta=2.0, dtau=0.1, rv=1.0, nflr=1, nwrap=5, proj=1, rndness=1e-3),
+    dict(lattice=2, l1=3, l2=3, beta=2.0, dtau=0.1, rv=1.0, nflr=1, nwrap=5, proj=1, rndness=0.3, flux_x=0.3, mu=0.1),
+    dict(lattice=1, l1=4, l2=4, beta=2.0, dtau=0.1, rhub=4.0, nflr=2, nwrap=5, proj=1, rndness=0.2, xmag=1.0),
+])
+def test_trial_state_matches_oracle(oracle, kw):
+    """The library's host eigensolver (tridiagonalisation + implicit QL) gives
+    the trial state of dqmc_set_proj after the reference's draw order: same
+    eigenvalues as zheev (scipy) and the same projector onto the ne lowest
+    states (the basis inside a level may differ)."""
+    import sunhubbardmy_b200 as sb
+    oracle.use_scipy_lapack(True)
+    try:
+        p = sb.DqmcParams.make(**kw)
+        for seed in (sb.test_seed(0), sb.test_seed(5)):
+            P, w = sb.trial_state(p, seed)
+            m = oracle.Model(**kw)
+            c = oracle.Chain(m, seed)
+            Po, wo = c.trial()
+            ne = p.ne
+            assert np.max(np.abs(w - wo)) < 1e-12
+            assert np.max(np.abs(P.conj().T @ P - np.eye(p.ndim))) < 1e-13
+            assert np.max(np.abs(P[:, :ne] @ P[:, :ne].conj().T - Po[:, :ne] @ Po[:, :ne].conj().T)) < 1e-10
+    finally:
+        oracle.use_scipy_lapack(False)
+
+
+def test_projective_params():
+    import sunhubbardmy_b200 as sb
+    p = sb.DqmcParams.make(lattice=2, l1=12, l2=12, beta=20.0, dtau=0.1, rv=1.0, nflr=1, proj=1, update=2)
+    assert (p.ndim, p.ne, p.ltrot, p.nst, p.obs_mid_len, p.nublock) == (288, 144, 200, 20, 1, 32)
+    with pytest.raises(sb.DqmcError):
+        sb.DqmcParams.make(rv=1.0, proj=0)       # t-V runs on the projective path only
+    with pytest.raises(sb.DqmcError):
+        sb.DqmcParams.make(rv=1.0, proj=1, lstabilize=0)

@@ -236,3 +236,151 @@ def test_lattice_tables(oracle):
         for i in range(lq):
             assert sorted(t["imj"][i].tolist()) == list(range(1, lq + 1))
         assert t["list"][:, 0].max() == lq and t["list"][:, 1].max() == m.nsub
+
+
+# ---------------------------------------------------------------- projective path
+PROJ_TV = dict(lattice=2, l1=3, l2=3, beta=2.0, dtau=0.1, rv=1.2, rhub=0.0, nflr=1, kinetic=0,
+               nwrap=5, proj=1, rndness=1e-3, update=2, nublock=8)
+
+
+def test_qr_pqmc_tall_and_wide(oracle):
+    """s_zgeQR_pqmc: orthonormal Q spanning the columns (rows) of A with
+    det R > 0 and log|det R| returned."""
+    rng = np.random.default_rng(3)
+    for shape in ((18, 9), (9, 18)):
+        a = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+        q, lw = oracle.qr_pqmc(a)
+        if shape[0] >= shape[1]:
+            assert np.allclose(q.conj().T @ q, np.eye(shape[1]), atol=1e-13)
+            r = q.conj().T @ a
+            assert np.allclose(q @ r, a, atol=1e-12)
+            assert np.allclose(np.tril(r, -1), 0, atol=1e-12)
+        else:
+            # wide: factored through the plain transpose, Q returned transposed
+            qt = q.T
+            assert np.allclose(qt.conj().T @ qt, np.eye(shape[0]), atol=1e-13)
+            r = qt.conj().T @ a.T
+            assert np.allclose(np.tril(r, -1), 0, atol=1e-12)
+        d = np.diag(r)
+        assert np.allclose(d.imag, 0, atol=1e-12)
+        assert np.prod(np.sign(d.real)) > 0
+        assert abs(lw - np.sum(np.log(np.abs(d.real)))) < 1e-10
+
+
+def test_bond_field_hs_identity(oracle):
+    """vconf: per bond B_s = U diag(e^{a s}, e^{-a s}) U^T = exp(a s sigma_x) with
+    cosh a = exp(dtau V / 2), and lambda sum_s det(1 + B_s) equals the Fock-space
+    trace of exp(-dtau V (n1 - 1/2)(n2 - 1/2)) (two sites, one flavour):
+    2 e^{-dtau V/4} + 2 e^{dtau V/4}, with lambda = exp(-dtau V / 4) / 2
+    (src/dqmc_config_v/dqmc_set_conf.f90:20-22)."""
+    m = oracle.Model(**PROJ_TV)
+    dtau, V = PROJ_TV["dtau"], PROJ_TV["rv"]
+    a = np.arccosh(np.exp(dtau * V / 2))
+    t = m.tables()
+    nnf = m.nn_nf
+    b0 = 0
+    i1 = t["nnlf_list"][b0] - 1
+    i2 = t["nnlist"][i1, 0] - 1
+    lam = 0.5 * np.exp(-dtau * V / 4)
+    total = 0.0
+    for s, val in ((-1, 1), (1, 2)):
+        vconf = np.ones((m.ltrot, nnf, m.ndim), np.int32)
+        vconf[0, 0, b0] = val
+        g = np.asfortranarray(np.eye(m.ndim, dtype=complex))
+        oracle.vconf_prop(m, vconf, oracle.LEFT_FORWARD, 1, 1, 2, g)
+        oracle.vconf_prop(m, vconf, oracle.LEFT_FORWARD, 1, 1, 1, g)
+        blk = g[np.ix_([i1, i2], [i1, i2])]
+        assert np.allclose(blk, sl.expm(a * s * np.array([[0, 1], [1, 0]])), atol=1e-14)
+        total += lam * np.linalg.det(np.eye(2) + blk).real
+    assert abs(total - (2 * np.exp(-dtau * V / 4) + 2 * np.exp(dtau * V / 4))) < 1e-13
+    # inverse props undo the forward ones (left and right)
+    g = np.asfortranarray(np.eye(m.ndim, dtype=complex) + 0.1)
+    g0 = g.copy()
+    vconf = np.random.default_rng(1).integers(1, 3, size=(m.ltrot, nnf, m.ndim)).astype(np.int32)
+    for op_f, op_b in ((oracle.LEFT_FORWARD, oracle.LEFT_BACKWARD), (oracle.RIGHT_FORWARD, oracle.RIGHT_BACKWARD)):
+        for nflag in (2, 1):
+            oracle.vconf_prop(m, vconf, op_f, 3, 2, nflag, g)
+        for nflag in (2, 1):
+            oracle.vconf_prop(m, vconf, op_b, 3, 2, nflag, g)
+        assert np.allclose(g, g0, atol=1e-13)
+
+
+def _dense_bmat(oracle, m, nt_from, nt_to):
+    """B(nt_to, nt_from-1) of the free (field-free) projective model from the
+    oracle's kinetic props: prod over slices of e^{-dtau K/2}(nf..1) e^{-dtau K/2}(1..nf)."""
+    B = np.asfortranarray(np.eye(m.ndim, dtype=complex))
+    for _ in range(nt_from, nt_to + 1):
+        for nf in range(1, m.nn_nf + 1):
+            m.h0_prop(oracle.LEFT_FORWARD, nf, B)
+        for nf in range(m.nn_nf, 0, -1):
+            m.h0_prop(oracle.LEFT_FORWARD, nf, B)
+    return B
+
+
+def test_projective_free_fermion_green(oracle):
+    """Without interactions, the stabilised projective stack reproduces the
+    dense G(tau) = I - B(tau,0) P [P^H B(beta,0) P]^-1 P^H B(beta,tau) at
+    tau = beta (sweep_start) and at the measured middle slice of both sweeps."""
+    kw = dict(lattice=2, l1=3, l2=3, beta=3.0, dtau=0.1, rv=0.0, rhub=0.0, nflr=1, kinetic=0,
+              nwrap=7, proj=1, rndness=0.05, mu=0.1)
+    m = oracle.Model(**kw)
+    c = oracle.Chain(m, 12345)
+    P, _ = c.trial()
+    P = P[:, :m.ne]
+    lt = m.ltrot
+
+    def g_at(nt):
+        Bl = _dense_bmat(oracle, m, 1, nt)
+        Br = _dense_bmat(oracle, m, nt + 1, lt)
+        UR = Bl @ P
+        UL = P.conj().T @ Br
+        return np.eye(m.ndim) - UR @ np.linalg.solve(UL @ UR, UL)
+
+    c.proj_sweep_start()
+    assert np.max(np.abs(c.proj_green() - g_at(lt))) < 1e-11
+    c.obser_init()
+    c.proj_sweep_b0(lupdate=False, lmeasure=True)
+    d = c.diag()
+    assert d["max_wrap_error"] < 1e-11
+    # the measurement sits at nt = ltrot/2 (obs_eqt_mid_len = 1); its G is the
+    # chain's last G only until the next stabilisation, so recompute the density
+    gmid = g_at(lt // 2)
+    dens = np.real(np.trace(np.eye(m.ndim) - gmid)) / m.lq
+    e = c.bins()["energy"]
+    # energy_bin(2) accumulates sum_i Gc_ii / lq, weighted by the sign
+    assert abs(e[1].real / e[0].real - dens) < 1e-10
+    c.proj_sweep_0b(lupdate=False, lmeasure=False)
+    assert c.diag()["max_wrap_error"] < 1e-11
+
+
+def test_projective_update_flavours_agree(oracle):
+    """Fast rank-2 bond update (dqmc_proj_update.f90) and submatrix-LR
+    (dqmc_proj_update_submatrix_LR.f90): same fields, same UR and (UL UR)^-1."""
+    for nub in (2, 4, 8, 32):
+        kw = dict(PROJ_TV, nublock=nub)
+        m = oracle.Model(**kw)
+        a = oracle.Chain(m, 7)
+        b = oracle.Chain(m, 7)
+        a.proj_sweep_start(); b.proj_sweep_start()
+        for nt in (m.ltrot, m.ltrot - 1):
+            for nf in (1, 2, 3):
+                a.proj_update(nt, nf, flavour=oracle.FAST)
+                b.proj_update(nt, nf, flavour=oracle.SUBMATRIX)
+        assert np.array_equal(a.vconf(), b.vconf())
+        for x, y in zip(a.proj_state(), b.proj_state()):
+            assert np.max(np.abs(x - y)) < 1e-12 * max(1.0, np.max(np.abs(y)))
+        assert a.diag()["accepted_v"] == b.diag()["accepted_v"] > 0
+
+
+def test_projective_sweeps_wrap_error(oracle):
+    """Two sweeps of the t-V projector with updates keep the wrap error and the
+    phase difference at the rounding level."""
+    m = oracle.Model(**PROJ_TV)
+    c = oracle.Chain(m, 99)
+    c.proj_sweep_start(); c.obser_init()
+    for _ in range(2):
+        c.proj_sweep_b0(); c.proj_sweep_0b()
+    d = c.diag()
+    assert d["max_wrap_error"] < 1e-9 and d["max_phasediff"] < 1e-9
+    assert d["logcount"] == 4 * m.nst
+    assert d["proposed_v"] == 4 * m.ltrot * m.nn_nf * m.nn_lf
