@@ -76,6 +76,8 @@ typedef struct dqmc_diag {
     double accepted, proposed;          /* main_obs(3): site (U) field */
     double nobs;                        /* measurements in the current bin */
     double accepted_v, proposed_v;      /* main_obs(4): bond (t-V) field */
+    double blk_proposed, blk_stage1, blk_accepted;   /* global block moves (dqmc_gpu_sweep_learned) */
+    double blk_sum_logratio;            /* sum of Re log R over the accepted blocks */
 } dqmc_diag;
 
 typedef struct dqmc_handle dqmc_handle;
@@ -220,6 +222,54 @@ int dqmc_gpu_proj_green(dqmc_handle* h);
  * with `seed` (draws the fields first when draw_conf is nonzero, as create
  * does).  proj: ndim x ndim complex; w: ndim.  Needs no GPU. */
 int dqmc_trial_state(const dqmc_params* p, int32_t seed, int draw_conf, double* proj, double* w);
+
+/* ---------------------------------------------------------------------------
+ * Learned effective action and global block moves.  No counterpart in the
+ * reference: an extra Monte Carlo move beside its local updates, which stay
+ * the judge of every proposal (delayed-acceptance Metropolis-Hastings with the
+ * exact determinant ratio as the second stage).
+ *
+ * The effective action is a 3-layer periodic convolutional network over the
+ * (ltrot x L x L) HS field s = +-1 of the square lattice:
+ *   h1 = tanh(W1 * s + b1), h2 = tanh(W2 * h1 + b2)  (3x3x3 convolutions over
+ *   (t, y, x), 32 channels), S = sum over space-time of w3 . h2 + b3 V.
+ * BF16 weights and activations in the tensor-core kernels, FP32 accumulation
+ * and FP32 master weights (Adam).  Parameters, flat FP32: W1[27][32], b1[32],
+ * W2[27][32 in][32 out], b2[32], w3[32], b3 (tap = 9 (dt+1) + 3 (dy+1) + (dx+1)
+ * for the offsets dt, dy, dx in -1..1; a correlation, out(v) = sum W in(v+off)).
+ * Fields are int8 +-1 arrays [ltrot][L][L] (x fastest: the site order of conf).
+ * --------------------------------------------------------------------------- */
+typedef struct dqmc_nn dqmc_nn;
+int dqmc_nn_create(int ltrot, int l, int max_batch, uint64_t seed, dqmc_nn** out);
+int dqmc_nn_destroy(dqmc_nn* nn);
+int dqmc_nn_nparams(void);
+int dqmc_nn_set_params(dqmc_nn* nn, const float* theta);
+int dqmc_nn_get_params(dqmc_nn* nn, float* theta);
+/* S of B host fields */
+int dqmc_nn_forward(dqmc_nn* nn, const int8_t* fields, int B, double* S);
+/* S of B fields and the gradient of sum_b r_b S_b with respect to the parameters */
+int dqmc_nn_gradient(dqmc_nn* nn, const int8_t* fields, int B, const double* r, double* S, float* grad);
+/* one Adam step on the centred squared error mean_b (S_b - y_b - mean(S - y))^2 */
+int dqmc_nn_train_step(dqmc_nn* nn, const int8_t* fields, const double* y, int B, double lr, double* loss);
+/* the same on pairs recorded by the handle (indices idx, targets y) */
+int dqmc_nn_train_recorded(dqmc_nn* nn, dqmc_handle* h, const int32_t* idx, const double* y, int B, double lr,
+                           double* loss);
+
+/* Record (HS field as int8 +-1, nflr Re log W) of every chain at every
+ * stabilisation of the finite-temperature sweeps into a ring of `capacity`
+ * pairs (capacity 0 stops recording).  All chains must have one size. */
+int dqmc_gpu_record(dqmc_handle* h, int capacity);
+int dqmc_gpu_record_count(dqmc_handle* h);
+int dqmc_gpu_record_get(dqmc_handle* h, int i, int8_t* field, double* value);
+int dqmc_gpu_record_values(dqmc_handle* h, double* values /* capacity */);
+
+/* n learned sweeps: b0 as dqmc_gpu_sweep_b0 (local updates if lupdate), then 0b with one proposal of an
+ * 8 x 4 x 4 block flip (slices x y x x) at the first slice of every other
+ * stabilisation interval (which ones alternates at random), each walker at its
+ * own random spatial origin.  Square lattice, two-valued HS field (lcomp = 2).
+ * seed != 0 reseeds the block-move generator.  Block statistics go to
+ * dqmc_diag.blk_*.  Device time per sweep: dqmc_gpu_last_sweeps_ms. */
+int dqmc_gpu_sweep_learned(dqmc_handle* h, dqmc_nn* nn, int n, int lupdate, int lmeasure, uint64_t seed);
 
 /* Allocation-free QR factorisation with log det Q.  No counterpart in the
  * reference: it is an extra entry point for host codes that cannot allocate

@@ -19,6 +19,7 @@
 #include "../../include/dqmc_gpu.h"
 #include "dqmc_types.h"
 #include "kernels.h"
+#include "nn.h"
 #include "zgemm.cuh"
 
 typedef std::complex<double> zc;
@@ -761,6 +762,17 @@ struct dqmc_handle {
     int ctas_per_chain = 1;
     size_t graph_nodes = 0;
     int proj = 0;
+    // recording of (HS field, nflr Re log weight) pairs at every stabilisation
+    int rec_on = 0, rec_cap = 0, rec_V = 0;
+    int8_t* rec_f = nullptr;
+    double* rec_v = nullptr;
+    int* rec_count = nullptr;
+    // global block moves
+    int blocks = 0;
+    int* d_org = nullptr;        // [nch][3]
+    double* d_u = nullptr;       // [nch][2]
+    double* d_S = nullptr;       // [nch][2]
+    uint64_t blk_rng = 0x9e3779b97f4a7c15ULL;
 };
 
 static void* dalloc(dqmc_handle* h, size_t bytes) {
@@ -1023,6 +1035,10 @@ static void proj_update(dqmc_handle* h, int nt, int nf, int visit, int dir, int 
 
 // one stabilisation of the 0b sweep at stack index n: new factor into the spare
 // slot, Green's function from (new R, old L), wrap check, then swap slots.
+static void maybe_record(dqmc_handle* h) {
+    if (h->rec_on) launch_record(h->d_chains, h->nch, h->rec_f, h->rec_v, h->rec_count, h->rec_cap, h->rec_V, h->st);
+}
+
 static void stab_0b(dqmc_handle* h, int n, int record) {
     const HostModel& m = *h->models[0];
     int spare = h->nst + 1;
@@ -1033,6 +1049,7 @@ static void stab_0b(dqmc_handle* h, int n, int record) {
     launch_green(h->d_chains, h->nch, spare, n, 0, 0, 0, 0, 0, h->st);
     launch_wrap_check(h->d_chains, h->nch, record, h->st);
     launch_swap_slots(h->d_slotmap, n, spare, h->st);
+    maybe_record(h);
 }
 
 // one stabilisation of the b0 sweep at stack index n (stablize_b0(n+1))
@@ -1046,6 +1063,7 @@ static void stab_b0(dqmc_handle* h, int n) {
     launch_green(h->d_chains, h->nch, n, spare, 0, 0, 0, 0, 0, h->st);
     launch_wrap_check(h->d_chains, h->nch, 1, h->st);
     launch_swap_slots(h->d_slotmap, n, spare, h->st);
+    maybe_record(h);
 }
 
 // ---------------------------------------------------------------------------
@@ -1330,7 +1348,7 @@ extern "C" int dqmc_gpu_sweeps(dqmc_handle* h, int n, int lmeasure) {
     if (!h) return fail(DQMC_EINVAL, "null handle");
     if (!h->started) return fail(DQMC_ESTATE, "sweep before sweep_start");
     if (n <= 0) return DQMC_OK;
-    if (!h->sweep_graph || h->graph_meas != lmeasure) {
+    if (!h->sweep_graph || h->graph_meas != lmeasure + 2 * h->rec_on) {
         if (h->sweep_graph) { cudaGraphExecDestroy(h->sweep_graph); h->sweep_graph = nullptr; }
         cudaGraph_t g;
         CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
@@ -1347,7 +1365,7 @@ extern "C" int dqmc_gpu_sweeps(dqmc_handle* h, int n, int lmeasure) {
         cudaGraphGetNodes(g, nullptr, &nn);
         h->graph_nodes = nn;
         cudaGraphDestroy(g);
-        h->graph_meas = lmeasure;
+        h->graph_meas = lmeasure + 2 * h->rec_on;
     }
     CK(cudaEventRecord(h->ev0, h->st));
     for (int i = 0; i < n; ++i) CK(cudaGraphLaunch(h->sweep_graph, h->st));
@@ -1518,6 +1536,8 @@ extern "C" int dqmc_gpu_get_diag(dqmc_handle* h, int chain, dqmc_diag* out) {
     out->avgexpphasediff_sum = st[ST_AVGEXPPD];
     out->accepted = st[ST_ACC]; out->proposed = st[ST_PROP]; out->nobs = st[ST_NOBS];
     out->accepted_v = st[ST_ACCV]; out->proposed_v = st[ST_PROPV];
+    out->blk_proposed = st[ST_BLK_PROP]; out->blk_stage1 = st[ST_BLK_S1]; out->blk_accepted = st[ST_BLK_ACC];
+    out->blk_sum_logratio = st[ST_BLK_SUMLR];
     return DQMC_OK;
 }
 
@@ -1528,6 +1548,7 @@ extern "C" int dqmc_gpu_reset_diag(dqmc_handle* h) {
         CK(cudaMemcpy(st, h->chains[c].dev.stats, sizeof(st), cudaMemcpyDeviceToHost));
         st[ST_MAX_WRAP] = st[ST_MAX_PHASEDIFF] = st[ST_AVGLOG10] = st[ST_LOGCOUNT] = st[ST_AVGEXPPD] = 0.0;
         st[ST_ACC] = st[ST_PROP] = st[ST_ACCV] = st[ST_PROPV] = 0.0;
+        st[ST_BLK_PROP] = st[ST_BLK_S1] = st[ST_BLK_ACC] = st[ST_BLK_SUMLR] = 0.0;
         CK(cudaMemcpy(h->chains[c].dev.stats, st, sizeof(st), cudaMemcpyHostToDevice));
     }
     return DQMC_OK;
@@ -1787,5 +1808,385 @@ extern "C" int dqmc_gpu_proj_green(dqmc_handle* h) {
     launch_proj_green(h->d_chains, h->nch, PMAT_ULRINV, PMAT_G, h->ctas_per_chain, h->st);
     CK(cudaStreamSynchronize(h->st));
     CK(cudaGetLastError());
+    return DQMC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// learned effective action (kern_nn.cu) and global block moves (kern_block.cu)
+// ---------------------------------------------------------------------------
+struct dqmc_nn {
+    int Lt = 0, L = 0, V = 0, maxB = 0, step = 0, nsm = 148;
+    float b3 = 0.f;
+    float *theta = nullptr, *grad = nullptr, *m1 = nullptr, *m2 = nullptr;
+    __nv_bfloat16 *W2T = nullptr, *W2R = nullptr, *h1 = nullptr, *h2 = nullptr, *dp2 = nullptr;
+    int8_t* fbuf = nullptr;
+    double *S = nullptr, *r = nullptr;
+    cudaStream_t st = nullptr;
+    std::vector<void*> allocs;
+};
+
+static NNW nn_w(const dqmc_nn* nn) {
+    NNW w;
+    w.W1 = nn->theta; w.b1 = nn->theta + NN_GB1; w.W2T = nn->W2T; w.W2R = nn->W2R;
+    w.b2 = nn->theta + NN_GB2; w.w3 = nn->theta + NN_GW3; w.b3 = nn->b3;
+    return w;
+}
+static NNIn nn_in_fields(const dqmc_nn* nn) {
+    NNIn in;
+    in.mode = 0; in.f8 = nn->fbuf; in.chains = nullptr;
+    in.Lt = nn->Lt; in.L = nn->L; in.V = nn->V; in.t_lo = 0; in.nT = nn->Lt;
+    return in;
+}
+
+extern "C" int dqmc_nn_nparams(void) { return NN_NPARAM; }
+
+extern "C" int dqmc_nn_destroy(dqmc_nn* nn) {
+    if (!nn) return DQMC_OK;
+    if (nn->st) cudaStreamSynchronize(nn->st);
+    for (void* p : nn->allocs) cudaFree(p);
+    if (nn->st) cudaStreamDestroy(nn->st);
+    delete nn;
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_nn_create(int ltrot, int l, int max_batch, uint64_t seed, dqmc_nn** out) {
+    if (!out || ltrot < 1 || l < 2 || max_batch < 1) return fail(DQMC_EINVAL, "invalid arguments");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(DQMC_ECUDA, "no CUDA device");
+    dqmc_nn* nn = new dqmc_nn();
+    nn->Lt = ltrot; nn->L = l; nn->V = ltrot * l * l; nn->maxB = max_batch;
+    cudaDeviceGetAttribute(&nn->nsm, cudaDevAttrMultiProcessorCount, 0);
+    auto al = [&](size_t bytes) -> void* {
+        void* p = nullptr;
+        if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess) return nullptr;
+        cudaMemset(p, 0, bytes ? bytes : 16);
+        nn->allocs.push_back(p);
+        return p;
+    };
+    size_t act = (size_t)max_batch * nn->V * 32 * sizeof(__nv_bfloat16);
+    nn->theta = (float*)al(NN_NPARAM * sizeof(float));
+    nn->grad = (float*)al(NN_NPARAM * sizeof(float));
+    nn->m1 = (float*)al(NN_NPARAM * sizeof(float));
+    nn->m2 = (float*)al(NN_NPARAM * sizeof(float));
+    nn->W2T = (__nv_bfloat16*)al(32 * 872 * sizeof(__nv_bfloat16));
+    nn->W2R = (__nv_bfloat16*)al(32 * 872 * sizeof(__nv_bfloat16));
+    nn->h1 = (__nv_bfloat16*)al(act);
+    nn->h2 = (__nv_bfloat16*)al(act);
+    nn->dp2 = (__nv_bfloat16*)al(act);
+    nn->fbuf = (int8_t*)al((size_t)max_batch * nn->V);
+    nn->S = (double*)al((size_t)max_batch * sizeof(double));
+    nn->r = (double*)al((size_t)max_batch * sizeof(double));
+    if (!nn->theta || !nn->h1 || !nn->h2 || !nn->dp2 || !nn->fbuf || !nn->S || !nn->r) {
+        dqmc_nn_destroy(nn);
+        return fail(DQMC_ENOMEM, "device allocation failed (effective action)");
+    }
+    if (cudaStreamCreateWithFlags(&nn->st, cudaStreamNonBlocking) != cudaSuccess) {
+        dqmc_nn_destroy(nn);
+        return fail(DQMC_ECUDA, "stream");
+    }
+    // initial weights: uniform in +-sqrt(3/fan_in) (unit-variance pre-activations)
+    std::vector<float> th(NN_NPARAM, 0.f);
+    uint64_t z = seed ? seed : 1;
+    auto uni = [&]() {
+        z += 0x9e3779b97f4a7c15ULL;
+        uint64_t x = z;
+        x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ULL;
+        x = (x ^ (x >> 27)) * 0x94d049bb133111ebULL;
+        x ^= x >> 31;
+        return ((double)(x >> 11) + 0.5) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+    };
+    for (int i = 0; i < 27 * 32; ++i) th[i] = (float)(uni() * std::sqrt(3.0 / 27.0));
+    for (int i = 0; i < 27 * 32 * 32; ++i) th[NN_GW2 + i] = (float)(uni() * std::sqrt(3.0 / 864.0));
+    for (int i = 0; i < 32; ++i) th[NN_GW3 + i] = (float)(uni() * std::sqrt(3.0 / 32.0));
+    cudaMemcpy(nn->theta, th.data(), th.size() * sizeof(float), cudaMemcpyHostToDevice);
+    launch_nn_pack(nn->theta, nn->W2T, nn->W2R, nn->st);
+    if (cudaStreamSynchronize(nn->st) != cudaSuccess) { dqmc_nn_destroy(nn); return fail(DQMC_ECUDA, "init"); }
+    *out = nn;
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_nn_set_params(dqmc_nn* nn, const float* theta) {
+    if (!nn || !theta) return fail(DQMC_EINVAL, "invalid arguments");
+    CK(cudaMemcpy(nn->theta, theta, NN_NPARAM * sizeof(float), cudaMemcpyHostToDevice));
+    nn->b3 = theta[NN_GB3];
+    CK(cudaMemset(nn->m1, 0, NN_NPARAM * sizeof(float)));
+    CK(cudaMemset(nn->m2, 0, NN_NPARAM * sizeof(float)));
+    nn->step = 0;
+    launch_nn_pack(nn->theta, nn->W2T, nn->W2R, nn->st);
+    CK(cudaStreamSynchronize(nn->st));
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_nn_get_params(dqmc_nn* nn, float* theta) {
+    if (!nn || !theta) return fail(DQMC_EINVAL, "invalid arguments");
+    CK(cudaMemcpy(theta, nn->theta, NN_NPARAM * sizeof(float), cudaMemcpyDeviceToHost));
+    theta[NN_GB3] = nn->b3;
+    return DQMC_OK;
+}
+
+static int nn_load_fields(dqmc_nn* nn, const int8_t* fields, int B) {
+    if (B < 1 || B > nn->maxB) return fail(DQMC_EINVAL, "batch size out of range 1..max_batch");
+    CK(cudaMemcpyAsync(nn->fbuf, fields, (size_t)B * nn->V, cudaMemcpyHostToDevice, nn->st));
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_nn_forward(dqmc_nn* nn, const int8_t* fields, int B, double* S) {
+    if (!nn || !fields || !S) return fail(DQMC_EINVAL, "invalid arguments");
+    int rc = nn_load_fields(nn, fields, B); if (rc) return rc;
+    CK(cudaMemsetAsync(nn->S, 0, B * sizeof(double), nn->st));
+    launch_nn_forward(nn_w(nn), nn_in_fields(nn), B, nn->S, nullptr, nullptr, nn->st);
+    CK(cudaMemcpyAsync(S, nn->S, B * sizeof(double), cudaMemcpyDeviceToHost, nn->st));
+    CK(cudaStreamSynchronize(nn->st));
+    CK(cudaGetLastError());
+    return DQMC_OK;
+}
+
+// forward with stored activations, then the gradient of sum_b r_b S_b into grad
+static int nn_fwd_bwd(dqmc_nn* nn, int B, const double* r_host, double* S_host) {
+    CK(cudaMemsetAsync(nn->S, 0, B * sizeof(double), nn->st));
+    NNIn in = nn_in_fields(nn);
+    launch_nn_forward(nn_w(nn), in, B, nn->S, nn->h1, nn->h2, nn->st);
+    CK(cudaMemcpyAsync(S_host, nn->S, B * sizeof(double), cudaMemcpyDeviceToHost, nn->st));
+    CK(cudaStreamSynchronize(nn->st));
+    if (!r_host) return DQMC_OK;
+    CK(cudaMemcpyAsync(nn->r, r_host, B * sizeof(double), cudaMemcpyHostToDevice, nn->st));
+    CK(cudaMemsetAsync(nn->grad, 0, NN_NPARAM * sizeof(float), nn->st));
+    launch_nn_backward(nn_w(nn), in, B, nn->r, nn->h1, nn->h2, nn->dp2, nn->grad, 2 * nn->nsm, nn->st);
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_nn_gradient(dqmc_nn* nn, const int8_t* fields, int B, const double* r, double* S, float* grad) {
+    if (!nn || !fields || !r || !S || !grad) return fail(DQMC_EINVAL, "invalid arguments");
+    int rc = nn_load_fields(nn, fields, B); if (rc) return rc;
+    if ((rc = nn_fwd_bwd(nn, B, r, S))) return rc;
+    CK(cudaMemcpyAsync(grad, nn->grad, NN_NPARAM * sizeof(float), cudaMemcpyDeviceToHost, nn->st));
+    CK(cudaStreamSynchronize(nn->st));
+    CK(cudaGetLastError());
+    return DQMC_OK;
+}
+
+// one Adam step on the centred squared error of S against the targets y
+static int nn_train_loaded(dqmc_nn* nn, const double* y, int B, double lr, double* loss) {
+    std::vector<double> S(B), r(B);
+    int rc = nn_fwd_bwd(nn, B, nullptr, S.data()); if (rc) return rc;
+    double mean = 0.0;
+    for (int b = 0; b < B; ++b) mean += (S[b] - y[b]) / B;
+    double l = 0.0;
+    for (int b = 0; b < B; ++b) {
+        double d = S[b] - y[b] - mean;
+        l += d * d / B;
+        r[b] = 2.0 * d / B;
+    }
+    if ((rc = nn_fwd_bwd(nn, B, r.data(), S.data()))) return rc;
+    nn->step += 1;
+    const float b1c = 1.f - (float)std::pow(0.9, nn->step), b2c = 1.f - (float)std::pow(0.999, nn->step);
+    launch_nn_adam(nn->theta, nn->grad, nn->m1, nn->m2, NN_NPARAM, (float)lr, b1c, b2c, nn->W2T, nn->W2R, nn->st);
+    CK(cudaStreamSynchronize(nn->st));
+    CK(cudaGetLastError());
+    if (loss) *loss = l;
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_nn_train_step(dqmc_nn* nn, const int8_t* fields, const double* y, int B, double lr, double* loss) {
+    if (!nn || !fields || !y) return fail(DQMC_EINVAL, "invalid arguments");
+    int rc = nn_load_fields(nn, fields, B); if (rc) return rc;
+    return nn_train_loaded(nn, y, B, lr, loss);
+}
+
+// ---- recording of training pairs during the sweeps ----
+extern "C" int dqmc_gpu_record(dqmc_handle* h, int capacity) {
+    if (!h) return fail(DQMC_EINVAL, "null handle");
+    if (h->proj) return fail(DQMC_ESTATE, "recording is for the finite-temperature sweep");
+    if (capacity <= 0) { h->rec_on = 0; return DQMC_OK; }
+    int V = h->ltrot * h->chains[0].dev.N;
+    for (auto& ch : h->chains)
+        if (ch.dev.N * h->ltrot != V) return fail(DQMC_EINVAL, "recording needs chains of one size");
+    if (capacity != h->rec_cap) {
+        h->rec_f = (int8_t*)dalloc(h, (size_t)capacity * V);
+        h->rec_v = (double*)dalloc(h, (size_t)capacity * sizeof(double));
+        h->rec_count = (int*)dalloc(h, sizeof(int));
+        if (!h->rec_f || !h->rec_v || !h->rec_count) return fail(DQMC_ENOMEM, "record buffers");
+        h->rec_cap = capacity;
+    }
+    h->rec_V = V;
+    CK(cudaMemset(h->rec_count, 0, sizeof(int)));
+    h->rec_on = 1;
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_record_count(dqmc_handle* h) {
+    if (!h || !h->rec_count) return 0;
+    int n = 0;
+    cudaMemcpy(&n, h->rec_count, sizeof(int), cudaMemcpyDeviceToHost);
+    long long tot = (long long)n * h->nch;
+    return (int)std::min<long long>(tot, h->rec_cap);
+}
+
+extern "C" int dqmc_gpu_record_get(dqmc_handle* h, int i, int8_t* field, double* value) {
+    if (!h || !h->rec_f || i < 0 || i >= h->rec_cap) return fail(DQMC_EINVAL, "record index out of range");
+    if (field) CK(cudaMemcpy(field, h->rec_f + (size_t)i * h->rec_V, h->rec_V, cudaMemcpyDeviceToHost));
+    if (value) CK(cudaMemcpy(value, h->rec_v + i, sizeof(double), cudaMemcpyDeviceToHost));
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_record_values(dqmc_handle* h, double* values) {
+    if (!h || !h->rec_v || !values) return fail(DQMC_EINVAL, "no record buffer");
+    CK(cudaMemcpy(values, h->rec_v, (size_t)h->rec_cap * sizeof(double), cudaMemcpyDeviceToHost));
+    return DQMC_OK;
+}
+
+// one Adam step on recorded pairs idx[0..B) of the handle (targets -values, i.e.
+// the effective action is fitted to -log|W| up to a constant)
+extern "C" int dqmc_nn_train_recorded(dqmc_nn* nn, dqmc_handle* h, const int32_t* idx, const double* y, int B,
+                                      double lr, double* loss) {
+    if (!nn || !h || !idx || !y || !h->rec_f) return fail(DQMC_EINVAL, "invalid arguments");
+    if (B < 1 || B > nn->maxB) return fail(DQMC_EINVAL, "batch size out of range 1..max_batch");
+    if (h->rec_V != nn->V) return fail(DQMC_EINVAL, "field size differs from the effective action's");
+    CK(cudaStreamSynchronize(h->st));
+    for (int b = 0; b < B; ++b) {
+        if (idx[b] < 0 || idx[b] >= h->rec_cap) return fail(DQMC_EINVAL, "record index out of range");
+        CK(cudaMemcpyAsync(nn->fbuf + (size_t)b * nn->V, h->rec_f + (size_t)idx[b] * nn->V, nn->V,
+                           cudaMemcpyDeviceToDevice, nn->st));
+    }
+    return nn_train_loaded(nn, y, B, lr, loss);
+}
+
+// ---- global block moves inside the 0b sweep ----
+static int enable_blocks(dqmc_handle* h) {
+    if (h->blocks) return DQMC_OK;
+    for (auto& ch : h->chains) {
+        ChainDev& d = ch.dev;
+        int N = d.N;
+        d.blk = (int*)dalloc(h, (size_t)(N + 8) * sizeof(int));
+        d.Gsave = (double2*)dalloc(h, (size_t)N * N * sizeof(double2));
+        d.confsave = (int32_t*)dalloc(h, (size_t)NN_BLK_T * N * sizeof(int32_t));
+        if (!d.blk || !d.Gsave || !d.confsave) return fail(DQMC_ENOMEM, "block buffers");
+    }
+    h->d_org = (int*)dalloc(h, (size_t)h->nch * 3 * sizeof(int));
+    h->d_u = (double*)dalloc(h, (size_t)h->nch * 2 * sizeof(double));
+    h->d_S = (double*)dalloc(h, (size_t)h->nch * 2 * sizeof(double));
+    std::vector<ChainDev> v(h->nch);
+    for (int c = 0; c < h->nch; ++c) v[c] = h->chains[c].dev;
+    CK(cudaMemcpy(h->d_chains, v.data(), sizeof(ChainDev) * h->nch, cudaMemcpyHostToDevice));
+    h->blocks = 1;
+    if (h->sweep_graph) { cudaGraphExecDestroy(h->sweep_graph); h->sweep_graph = nullptr; }
+    return DQMC_OK;
+}
+
+static uint64_t blk_next(uint64_t& z) {
+    z += 0x9e3779b97f4a7c15ULL;
+    uint64_t x = z;
+    x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    x = (x ^ (x >> 27)) * 0x94d049bb133111ebULL;
+    return x ^ (x >> 31);
+}
+
+// one block proposal with its first slice at nt = t0 (G at the update point of t0)
+static void block_move(dqmc_handle* h, dqmc_nn* nn, int t0) {
+    const HostModel& m = *h->models[0];
+    const int L = m.p.l1, nch = h->nch;
+    std::vector<int> org(3 * nch);
+    std::vector<double> u(2 * nch);
+    for (int c = 0; c < nch; ++c) {
+        org[3 * c] = t0 - 1;
+        org[3 * c + 1] = (int)(blk_next(h->blk_rng) % (uint64_t)L);
+        org[3 * c + 2] = (int)(blk_next(h->blk_rng) % (uint64_t)L);
+        u[2 * c] = ((double)(blk_next(h->blk_rng) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+        u[2 * c + 1] = ((double)(blk_next(h->blk_rng) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+    }
+    cudaMemcpyAsync(h->d_org, org.data(), org.size() * sizeof(int), cudaMemcpyHostToDevice, h->st);
+    cudaMemcpyAsync(h->d_u, u.data(), u.size() * sizeof(double), cudaMemcpyHostToDevice, h->st);
+    launch_blk_setup(h->d_chains, nch, h->d_org, L, h->st);
+    cudaMemsetAsync(h->d_S, 0, 2 * nch * sizeof(double), h->st);
+    NNIn in;
+    in.mode = 1; in.f8 = nullptr; in.chains = h->d_chains;
+    in.Lt = nn->Lt; in.L = nn->L; in.V = nn->V;
+    in.t_lo = t0 - 1 - 2; in.nT = NN_BLK_T + 4;
+    launch_nn_forward(nn_w(nn), in, 2 * nch, h->d_S, nullptr, nullptr, h->st);
+    launch_blk_begin(h->d_chains, nch, h->d_S, h->d_u, t0, NN_BLK_T, h->st);
+    for (int j = 0; j < NN_BLK_T; ++j) {
+        launch_update(h->d_chains, nch, t0 + j, 0, h->st, 1);
+        if (j + 1 < NN_BLK_T) {
+            PropProg pl; pl.n = 0; PropProg pr; pr.n = 0;
+            prog_k(m, pl, PW_FWD, 1); prog_k(m, pl, PW_FWD, 0); prog_v(m, pl, PW_FWD, t0 + j + 1);
+            prog_k(m, pr, PW_INV, 1); prog_k(m, pr, PW_INV, 0); prog_v(m, pr, PW_INV, t0 + j + 1);
+            launch_prog(h, MAT_G, pl, 0);
+            launch_prog(h, MAT_G, pr, 1);
+        }
+    }
+    launch_blk_decide(h->d_chains, nch, h->st);
+    // back to the update point of t0 through the (possibly flipped) slices
+    for (int j = NN_BLK_T - 1; j >= 1; --j) {
+        PropProg pl; pl.n = 0; PropProg pr; pr.n = 0;
+        prog_v(m, pl, PW_INV, t0 + j); prog_k(m, pl, PW_INV, 1); prog_k(m, pl, PW_INV, 0);
+        prog_v(m, pr, PW_FWD, t0 + j); prog_k(m, pr, PW_FWD, 1); prog_k(m, pr, PW_FWD, 0);
+        launch_prog(h, MAT_G, pl, 0);
+        launch_prog(h, MAT_G, pr, 1);
+    }
+    launch_blk_end(h->d_chains, nch, t0, NN_BLK_T, h->st);
+}
+
+// dqmc_ft_sweep_0b with a block proposal at the first slice of the chosen
+// stabilisation intervals (intervals n with n % 2 == parity; the slice offset
+// inside the interval is drawn so the block stays inside it)
+static void enqueue_0b_blocks(dqmc_handle* h, dqmc_nn* nn, int lupdate, int lmeasure, int parity) {
+    const HostModel& m = *h->models[0];
+    int lt = h->ltrot;
+    std::vector<int> start(lt + 2, 0);
+    for (int n = 1; n <= h->nst; ++n) {
+        if (n % 2 != parity) continue;
+        int a = m.wrap_step[(n - 1) * 2], b = m.wrap_step[(n - 1) * 2 + 1];
+        int len = b - a + 1;
+        if (len < NN_BLK_T) continue;
+        int off = (int)(blk_next(h->blk_rng) % (uint64_t)(len - NN_BLK_T + 1));
+        start[a + off] = 1;
+    }
+    launch_stack_identity(h->d_chains, h->nch, 0, h->st);
+    if (lupdate) launch_sfmt(h->d_chains, h->nch, lt, h->st);
+    for (int nt = 1; nt <= lt; ++nt) {
+        int visit = nt - 1;
+        PropProg pl; pl.n = 0; PropProg pr; pr.n = 0;
+        prog_k(m, pl, PW_FWD, 0);
+        prog_v(m, pl, PW_FWD, nt);
+        prog_k(m, pr, PW_INV, 0);
+        prog_v(m, pr, PW_INV, nt);
+        launch_prog(h, MAT_G, pl, 0);
+        launch_prog(h, MAT_G, pr, 1);
+        if (start[nt]) block_move(h, nn, nt);
+        if (lupdate) launch_update(h->d_chains, h->nch, nt, visit, h->st);
+        pl.n = 0; pr.n = 0;
+        prog_k(m, pl, PW_FWD, 1);
+        prog_k(m, pr, PW_INV, 1);
+        launch_prog(h, MAT_G, pl, 0);
+        launch_prog(h, MAT_G, pr, 1);
+        if (lmeasure) launch_measure(h->d_chains, h->nch, h->ctas_per_chain, h->st);
+        if (m.iwrap_nt[nt] > 0) stab_0b(h, m.iwrap_nt[nt], 1);
+    }
+}
+
+extern "C" int dqmc_gpu_sweep_learned(dqmc_handle* h, dqmc_nn* nn, int n, int lupdate, int lmeasure, uint64_t seed) {
+    if (!h || !nn) return fail(DQMC_EINVAL, "null argument");
+    if (!h->started) return fail(DQMC_ESTATE, "sweep before sweep_start");
+    if (h->proj) return fail(DQMC_ESTATE, "block moves are for the finite-temperature sweep");
+    const HostModel& m = *h->models[0];
+    if (h->models.size() != 1 || m.p.lattice != DQMC_LATT_SQUARE || m.p.l1 != nn->L || m.p.l2 != nn->L ||
+        m.p.ltrot != nn->Lt)
+        return fail(DQMC_EINVAL, "the effective action's lattice differs from the handle's (square L x L, ltrot)");
+    if (m.lcomp != 2) return fail(DQMC_EINVAL, "block flips need a two-valued HS field (lcomp = 2)");
+    if (m.p.rhub == 0.0) return fail(DQMC_EINVAL, "no HS field (rhub == 0)");
+    int rc = enable_blocks(h); if (rc) return rc;
+    if (seed) h->blk_rng = seed;
+    cudaEvent_t e0 = h->ev0, e1 = h->ev1;
+    CK(cudaEventRecord(e0, h->st));
+    for (int i = 0; i < n; ++i) {
+        enqueue_b0(h, lupdate, lmeasure);
+        enqueue_0b_blocks(h, nn, lupdate, lmeasure, (int)(blk_next(h->blk_rng) & 1));
+    }
+    CK(cudaEventRecord(e1, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaGetLastError());
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    h->last_ms = n > 0 ? ms / n : 0.0;
     return DQMC_OK;
 }

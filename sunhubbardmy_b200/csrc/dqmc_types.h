@@ -75,6 +75,12 @@ struct ChainDev {
     int32_t* vconf;            // ltrot x nn_nf x N (bond index fastest), values 1..2
     double2* pw;               // update window scratch
     int* pw_flag;              // per-walker flag: the current window accepted something
+    // global block proposals (learned effective action): [0, N) site mask of the
+    // block's spatial patch, [N] stage-1 passed, [N+1] accepted, [N+4..N+6]
+    // block origin (t, y, x), 0-based
+    int* blk;
+    double2* Gsave;            // G at the block's first slice
+    int32_t* confsave;         // HS field of the block's slices
 };
 
 // indices into ChainDev::stats
@@ -83,7 +89,9 @@ enum {
     ST_MAX_WRAP, ST_MAX_PHASEDIFF, ST_AVGLOG10, ST_LOGCOUNT, ST_AVGEXPPD,
     ST_ACC, ST_PROP, ST_NOBS, ST_INFO, ST_LOGDETM_RE, ST_LOGDETM_IM, ST_LAST_WRAP,
     ST_ACCV, ST_PROPV,
-    ST_COUNT = 24
+    ST_BLK_LR_RE, ST_BLK_LR_IM, ST_BLK_PH_RE, ST_BLK_PH_IM, ST_BLK_PROP, ST_BLK_S1, ST_BLK_ACC,
+    ST_BLK_DS, ST_BLK_U2, ST_BLK_SUMLR,
+    ST_COUNT = 32
 };
 
 // propagation op encoding: kind | which << 4 | nf << 8 | nt << 16

@@ -59,11 +59,16 @@ DQ_DEV double2 flip_ratio(const ModelDev& md, double2 diag_s, int is, int iflip,
     return cmul(r, md.phase_ratio[k]);
 }
 
-__global__ void __launch_bounds__(256) k_update_delay(const ChainDev* __restrict__ chains, int nt, int visit) {
+// forced = 1: the global block move's forced flips of slice nt (sites with
+// blk[i] != 0 go to the next field value, no random test, chains whose block
+// did not pass the first stage do nothing); the log of the product of the
+// flips' ratios is accumulated in stats[ST_BLK_LR_*].
+__global__ void __launch_bounds__(256) k_update_delay(const ChainDev* __restrict__ chains, int nt, int visit, int forced) {
     extern __shared__ double2 dsm[];
     const ChainDev c = chains[blockIdx.x];
     const ModelDev& md = *c.md;
     const int N = c.N, nb = md.nublock, lc = md.lcomp;
+    if (forced && c.blk[N] == 0) return;
     const int tid = threadIdx.x, nth = blockDim.x;
     cplx* gsm = dsm;                                   // GEMM staging
     double2* diag = dsm + UpdGemm::SMEM_ELEMS;         // N
@@ -87,10 +92,12 @@ __global__ void __launch_bounds__(256) k_update_delay(const ChainDev* __restrict
         const double2 ph = S->phase;
         int myfirst = N;
         for (int j = s + tid; j < N; j += nth) {
+            if (forced) {
+                if (c.blk[j]) { myfirst = j; break; }
+                continue;
+            }
             int is = cf[j];
             int iflip = (int)ceil(u32_to_stream(rw[2 * j]) * (lc - 1));
-            int isp = (is + iflip - 1) % lc + 1;
-            (void)isp;
             double2 rt = flip_ratio(md, diag[j], is, iflip, nullptr);
             double rre = cmul(rt, ph).x / ph.x;
             double rabs = fabs(rre);
@@ -101,7 +108,7 @@ __global__ void __launch_bounds__(256) k_update_delay(const ChainDev* __restrict
         // accept site `first`
         if (tid == 0) {
             int is = cf[first];
-            int iflip = (int)ceil(u32_to_stream(rw[2 * first]) * (lc - 1));
+            int iflip = forced ? 1 : (int)ceil(u32_to_stream(rw[2 * first]) * (lc - 1));
             int isp = (is + iflip - 1) % lc + 1;
             double2 sscl;
             double2 rt = flip_ratio(md, diag[first], is, iflip, &sscl);
@@ -109,6 +116,11 @@ __global__ void __launch_bounds__(256) k_update_delay(const ChainDev* __restrict
             S->phase = cscale(cmul(S->phase, rt), 1.0 / w);
             S->sscl = sscl;
             S->acc += 1.0;
+            if (forced) {
+                double2 l = clog_(rt);
+                c.stats[ST_BLK_LR_RE] += l.x;
+                c.stats[ST_BLK_LR_IM] += l.y;
+            }
             cf[first] = isp;
         }
         for (int m = tid; m < ik; m += nth) {
@@ -152,18 +164,20 @@ __global__ void __launch_bounds__(256) k_update_delay(const ChainDev* __restrict
     if (tid == 0) {
         c.stats[ST_PHASE_RE] = S->phase.x;
         c.stats[ST_PHASE_IM] = S->phase.y;
-        c.stats[ST_ACC] += S->acc;
-        c.stats[ST_PROP] += N;
+        if (!forced) {
+            c.stats[ST_ACC] += S->acc;
+            c.stats[ST_PROP] += N;
+        }
     }
 }
 
 static int g_upd_attr = 0;
 
-void launch_update(const ChainDev* chains, int nchains, int nt, int visit, cudaStream_t st) {
+void launch_update(const ChainDev* chains, int nchains, int nt, int visit, cudaStream_t st, int forced) {
     size_t smem = UpdGemm::SMEM_ELEMS * sizeof(double2) + (size_t)(512 + 2 * 64) * sizeof(double2) + sizeof(UpdSmem) + 64;
     if (!g_upd_attr) {
         cudaFuncSetAttribute(k_update_delay, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         g_upd_attr = 1;
     }
-    k_update_delay<<<nchains, 256, smem, st>>>(chains, nt, visit);
+    k_update_delay<<<nchains, 256, smem, st>>>(chains, nt, visit, forced);
 }

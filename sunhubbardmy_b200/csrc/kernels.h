@@ -8,7 +8,7 @@ void launch_prop(const ChainDev* chains, int nchains, int maxN, int mat_id, cons
                  int right, int ctas_per_chain, cudaStream_t st);
 void launch_sfmt(const ChainDev* chains, int nchains, int slices, cudaStream_t st);
 void launch_sfmt_raw(const ChainDev* chains, int chain, int count, cudaStream_t st);
-void launch_update(const ChainDev* chains, int nchains, int nt, int visit, cudaStream_t st);
+void launch_update(const ChainDev* chains, int nchains, int nt, int visit, cudaStream_t st, int forced = 0);
 void launch_measure(const ChainDev* chains, int nchains, int ctas_per_chain, cudaStream_t st);
 void launch_bins_clear(const ChainDev* chains, int nchains, int nbins, cudaStream_t st);
 void launch_stab_slots(const ChainDev* chains, int nchains, int src, int dst, cudaStream_t st);
@@ -41,3 +41,11 @@ void launch_proj_green(const ChainDev* chains, int nchains, int inv_id, int dst_
 void launch_tall_copy(const ChainDev* chains, int nchains, int dst_id, int src_id, cudaStream_t st);
 void launch_proj_update(const ChainDev* chains, int nchains, int nt, int nf, int visit, int dir, int rnd_off,
                         int nwin, int g_rg, int g_fl, cudaStream_t st);
+
+// global block moves and training-pair recording (kern_block.cu)
+void launch_blk_setup(const ChainDev* chains, int nchains, const int* org, int L, cudaStream_t st);
+void launch_blk_begin(const ChainDev* chains, int nchains, const double* S, const double* u, int t0, int nsl, cudaStream_t st);
+void launch_blk_decide(const ChainDev* chains, int nchains, cudaStream_t st);
+void launch_blk_end(const ChainDev* chains, int nchains, int t0, int nsl, cudaStream_t st);
+void launch_record(const ChainDev* chains, int nchains, int8_t* fields, double* vals, int* count, int capacity, int V,
+                   cudaStream_t st);

@@ -86,7 +86,7 @@ class DqmcDiag(C.Structure):
     _fields_ = [(n, C.c_double) for n in (
         "phase_re", "phase_im", "logweight_re", "logweight_im", "max_wrap_error", "max_phasediff",
         "avglog10error_sum", "logcount", "avgexpphasediff_sum", "accepted", "proposed", "nobs",
-        "accepted_v", "proposed_v")]
+        "accepted_v", "proposed_v", "blk_proposed", "blk_stage1", "blk_accepted", "blk_sum_logratio")]
 
 
 _lib = None
@@ -139,6 +139,20 @@ SIGNATURES = {
     "dqmc_gpu_proj_update": (_i, [_vp, _i, _i]),
     "dqmc_gpu_proj_green": (_i, [_vp]),
     "dqmc_trial_state": (_i, [_vp, C.c_int32, _i, _vp, _vp]),
+    "dqmc_nn_create": (_i, [_i, _i, _i, C.c_uint64, C.POINTER(_vp)]),
+    "dqmc_nn_destroy": (_i, [_vp]),
+    "dqmc_nn_nparams": (_i, []),
+    "dqmc_nn_set_params": (_i, [_vp, _vp]),
+    "dqmc_nn_get_params": (_i, [_vp, _vp]),
+    "dqmc_nn_forward": (_i, [_vp, _vp, _i, _vp]),
+    "dqmc_nn_gradient": (_i, [_vp, _vp, _i, _vp, _vp, _vp]),
+    "dqmc_nn_train_step": (_i, [_vp, _vp, _vp, _i, _d, _vp]),
+    "dqmc_nn_train_recorded": (_i, [_vp, _vp, _vp, _vp, _i, _d, _vp]),
+    "dqmc_gpu_record": (_i, [_vp, _i]),
+    "dqmc_gpu_record_count": (_i, [_vp]),
+    "dqmc_gpu_record_get": (_i, [_vp, _i, _vp, _vp]),
+    "dqmc_gpu_record_values": (_i, [_vp, _vp]),
+    "dqmc_gpu_sweep_learned": (_i, [_vp, _vp, _i, _i, _i, C.c_uint64]),
 }
 
 
@@ -336,7 +350,9 @@ class Dqmc:
                     max_wrap_error=d.max_wrap_error, max_phasediff=d.max_phasediff,
                     avglog10error=d.avglog10error_sum, logcount=d.logcount,
                     avgexpphasediff=d.avgexpphasediff_sum, accepted=d.accepted, proposed=d.proposed,
-                    nobs=d.nobs, accepted_v=d.accepted_v, proposed_v=d.proposed_v)
+                    nobs=d.nobs, accepted_v=d.accepted_v, proposed_v=d.proposed_v,
+                    blk_proposed=d.blk_proposed, blk_stage1=d.blk_stage1, blk_accepted=d.blk_accepted,
+                    blk_sum_logratio=d.blk_sum_logratio)
 
     def energy_all(self) -> np.ndarray:
         """energy_bin(1:10) of every chain, shape (n_chains, 10) complex."""
@@ -419,6 +435,35 @@ class Dqmc:
 
     def test_zgemm(self, m, n, k, opa, opb, a, b, c, beta=0.0) -> None:
         _check(load_library().dqmc_gpu_test_zgemm(self.h, m, n, k, opa, opb, a, b, c, float(beta)), "test_zgemm")
+
+    # training pairs and learned sweeps (finite temperature, square lattice)
+    def record(self, capacity: int) -> None:
+        """Record (field, nflr Re log W) of every chain at every stabilisation
+        into a ring of `capacity` pairs (0 stops recording)."""
+        _check(load_library().dqmc_gpu_record(self.h, int(capacity)), "record")
+
+    def record_count(self) -> int:
+        return load_library().dqmc_gpu_record_count(self.h)
+
+    def record_get(self, i: int):
+        p = self.chain_params(0)
+        f = np.zeros((p.ltrot, p.l1, p.l2), np.int8)
+        v = C.c_double()
+        _check(load_library().dqmc_gpu_record_get(self.h, int(i), _ptr(f), C.byref(v)), "record_get")
+        return f, v.value
+
+    def record_values(self, capacity: int) -> np.ndarray:
+        out = np.zeros(capacity)
+        _check(load_library().dqmc_gpu_record_values(self.h, _ptr(out)), "record_values")
+        return out
+
+    def sweeps_learned(self, nn, n: int, lmeasure: bool = True, seed: int = 0, lupdate: bool = True) -> float:
+        """n sweeps with global block proposals from the effective action nn;
+        returns device ms per sweep."""
+        L = load_library()
+        _check(L.dqmc_gpu_sweep_learned(self.h, nn.h, int(n), int(lupdate), int(lmeasure), C.c_uint64(seed)),
+               "sweep_learned")
+        return L.dqmc_gpu_last_sweeps_ms(self.h)
 
     # projective path (params.proj = 1)
     def vconf(self, c: int = 0) -> np.ndarray:

@@ -384,3 +384,21 @@ def test_projective_sweeps_wrap_error(oracle):
     assert d["max_wrap_error"] < 1e-9 and d["max_phasediff"] < 1e-9
     assert d["logcount"] == 4 * m.nst
     assert d["proposed_v"] == 4 * m.ltrot * m.nn_nf * m.nn_lf
+
+
+def test_effective_action_gradient_by_finite_differences():
+    """The numpy restatement of the learned effective action (the checker of
+    the tensor-core network kernels): backpropagated gradient against central
+    differences of its own forward value."""
+    from oracle import nn_oracle as no
+    rng = np.random.default_rng(0)
+    th = rng.standard_normal(no.NP) * 0.2
+    fields = [rng.choice([-1, 1], size=(4, 4, 4)) for _ in range(2)]
+    r = np.array([0.7, -0.3])
+    _, g = no.gradient(th, fields, r, emulate_bf16=False)
+    eps = 1e-6
+    for idx in (0, 5, 27 * 32 + 3, 27 * 32 + 32 + 100, no.NP - 40, no.NP - 2, no.NP - 1):
+        tp = th.copy(); tp[idx] += eps
+        tm = th.copy(); tm[idx] -= eps
+        fd = sum(rr * (no.forward(tp, f, False) - no.forward(tm, f, False)) / (2 * eps) for f, rr in zip(fields, r))
+        assert abs(g[idx] - fd) < 1e-7 * max(1.0, abs(fd))
