@@ -48,6 +48,12 @@ WORKLOAD3 = "honeycomb L=6/9/12 (N=72/162/288, 48/48/32 chains) SU(4) Hubbard U=
 # random hopping perturbation lifting the Dirac-point degeneracy; 64 walkers
 CONFIG4 = dict(lattice=2, l1=12, l2=12, beta=20.0, dtau=0.1, rv=1.0, rhub=0.0, nflr=1, kinetic=0, update=2,
                nwrap=10, nublock=32, proj=1, rndness=1e-3)
+# learned proposal: SU(2) Hubbard square L=20 (N=400), U=6, mu=0, beta=12,
+# dtau=0.1 (ltrot=120), delay update (the plain base), exact two-valued HS
+# field (the block flip needs lcomp = 2), checkerboard kinetic term, 64 chains
+CONFIG5 = dict(lattice=1, l1=20, l2=20, beta=12.0, dtau=0.1, rhub=6.0, nflr=2, mu=0.0, kinetic=0, update=1, hs=0,
+               nwrap=10)
+WORKLOAD5 = "square L=20 (N=400) SU(2) Hubbard U=6 beta=12 dtau=0.1 (ltrot=120), delay, exact 2-comp HS, 64 chains; learned 8x4x4 block proposals vs plain"
 WORKLOAD4 = "projective spinless t-V, honeycomb L=12 (N=288, ne=144) V=1 theta=20 dtau=0.1 (ltrot=200), submatrix-LR nustock=32, rndness=1e-3 trial, 64 walkers"
 
 
@@ -483,6 +489,93 @@ def proj_roofline_and_line(args, g, p, Ns, ms, value, per_step, world, workload,
     return result
 
 
+def learned_arm(args, rank: int, local_rank: int) -> None:
+    """ESS/s of the per-sweep double occupancy: plain sweeps (which also record
+    the training pairs at every stabilisation), then the effective action is
+    trained on the recorded pairs, then learned sweeps (plain local updates +
+    global block proposals) continue the same chains."""
+    import numpy as np
+    import torch
+    import sunhubbardmy_b200 as sb
+    from sunhubbardmy_b200.learned import EffectiveAction, train
+    from sunhubbardmy_b200.stats import double_occupancy, ess
+
+    torch.cuda.set_device(local_rank)
+    p = sb.DqmcParams.make(**CONFIG5)
+    nch = args.chains if args.chains_set else 64
+    g = sb.Dqmc(p, n_chains=nch, seeds=[test_seed(rank * nch + c) for c in range(nch)])
+    Ns = np.full(nch, float(p.ndim))
+    g.sweep_start()
+    g.sweeps(max(args.ess_warmup, 1), False)
+
+    def run(step, n):
+        xs, dev = [], 0.0
+        t0 = time.perf_counter()
+        for _ in range(n):
+            g.obser_init()
+            dev += step()
+            xs.append(double_occupancy(g.energy_all(), Ns))
+        return np.array(xs).T, time.perf_counter() - t0, dev * 1e-3
+
+    cap = max(args.pairs, 1)
+    g.record(cap)
+    with ClockSampler(local_rank) as clk_p:
+        xp, wall_p, dev_p = run(lambda: g.sweeps(1, True), args.ess)
+    npairs = g.record_count()
+    targets = -g.record_values(cap)[:npairs]
+    g.record(0)
+    ess_p, tau_p = ess(xp)
+
+    nn = EffectiveAction(p.ltrot, p.l1, max_batch=32, seed=1)
+    rng = np.random.default_rng(0)
+    perm = rng.permutation(npairs)
+    nval = min(256, npairs // 10)
+    val, tr = perm[:nval], perm[nval:]
+    vf = np.stack([g.record_get(int(i))[0] for i in val])
+
+    def val_loss():
+        S = np.concatenate([nn.forward(vf[k:k + 32]) for k in range(0, len(vf), 32)])
+        d = S - targets[val]
+        return float(np.var(d)), float(np.var(targets[val]))
+
+    l0, var_y = val_loss()
+    t0 = time.perf_counter()
+    losses = train(nn, g, targets[tr], args.train_steps, batch=32, lr=args.lr, seed=1)
+    train_s = time.perf_counter() - t0
+    l1, _ = val_loss()
+
+    g.reset_diag()
+    with ClockSampler(local_rank) as clk_l:
+        xl, wall_l, dev_l = run(lambda: g.sweeps_learned(nn, 1, True), args.ess)
+    ess_l, tau_l = ess(xl)
+    ds = [g.diag(c) for c in range(nch)]
+    tot = {k: sum(d[k] for d in ds) for k in ("blk_proposed", "blk_stage1", "blk_accepted", "blk_err_learned", "blk_err_zero")}
+    line = {
+        "metric": "ESS/s of double occupancy (learned + batched vs plain)", "value": ess_l / wall_l, "unit": "1/s",
+        "n_gpus": 1, "steps": args.ess, "warmup": args.ess_warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128 (DQMC), bf16/fp32 (effective action)",
+        "data": "synthetic (HS fields drawn from the reference's -DTEST seeds; training pairs recorded from the plain chains)",
+        "config": {"workload": WORKLOAD5, "chains": nch},
+        "plain": {"ess": ess_p, "tau_int_sweeps": tau_p, "wall_s": wall_p, "device_s": dev_p,
+                  "ess_per_s": ess_p / wall_p, "mean": float(xp.mean()),
+                  "stderr": float(xp.std(ddof=1) / np.sqrt(ess_p)), "clocks": clk_p.summary()},
+        "learned": {"ess": ess_l, "tau_int_sweeps": tau_l, "wall_s": wall_l, "device_s": dev_l,
+                    "ess_per_s": ess_l / wall_l, "mean": float(xl.mean()),
+                    "stderr": float(xl.std(ddof=1) / np.sqrt(ess_l)), "clocks": clk_l.summary(),
+                    "blocks_proposed": tot["blk_proposed"],
+                    "stage1_pass": tot["blk_stage1"] / max(1.0, tot["blk_proposed"]),
+                    "accepted": tot["blk_accepted"] / max(1.0, tot["blk_proposed"]),
+                    "ratio_prediction_mse_learned": tot["blk_err_learned"] / max(1.0, tot["blk_stage1"]),
+                    "ratio_prediction_mse_zero": tot["blk_err_zero"] / max(1.0, tot["blk_stage1"])},
+        "ess_per_s_ratio_learned_vs_plain": (ess_l / wall_l) / (ess_p / wall_p),
+        "training": {"pairs": int(npairs), "steps": args.train_steps, "batch": 32, "lr": args.lr, "wall_s": train_s,
+                     "heldout_var_residual_before": l0, "heldout_var_residual_after": l1,
+                     "heldout_var_target": var_y, "loss_first": float(np.mean(losses[:20])),
+                     "loss_last": float(np.mean(losses[-20:]))},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -491,7 +584,10 @@ def main():
     ap.add_argument("--chains", type=int, default=None)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4"])
+    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "config5"])
+    ap.add_argument("--pairs", type=int, default=200000, help="config5: training-pair ring capacity")
+    ap.add_argument("--train-steps", type=int, default=2000, help="config5: Adam steps of 32 pairs")
+    ap.add_argument("--lr", type=float, default=1e-3, help="config5: Adam learning rate")
     ap.add_argument("--ess", type=int, default=0, help="extra sweeps for the ESS/s of double occupancy")
     ap.add_argument("--ess-warmup", type=int, default=20, help="equilibration sweeps before the ESS series")
     args = ap.parse_args()
@@ -503,6 +599,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         reference_arm(args, rank)
+        return
+    if args.workload == "config5":
+        if rank == 0:
+            learned_arm(args, rank, local_rank)
         return
     gpu_arm(args, rank, world, local_rank)
 

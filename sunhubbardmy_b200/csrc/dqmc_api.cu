@@ -1538,6 +1538,7 @@ extern "C" int dqmc_gpu_get_diag(dqmc_handle* h, int chain, dqmc_diag* out) {
     out->accepted_v = st[ST_ACCV]; out->proposed_v = st[ST_PROPV];
     out->blk_proposed = st[ST_BLK_PROP]; out->blk_stage1 = st[ST_BLK_S1]; out->blk_accepted = st[ST_BLK_ACC];
     out->blk_sum_logratio = st[ST_BLK_SUMLR];
+    out->blk_err_learned = st[ST_BLK_ERR1]; out->blk_err_zero = st[ST_BLK_ERR0];
     return DQMC_OK;
 }
 
@@ -1549,6 +1550,7 @@ extern "C" int dqmc_gpu_reset_diag(dqmc_handle* h) {
         st[ST_MAX_WRAP] = st[ST_MAX_PHASEDIFF] = st[ST_AVGLOG10] = st[ST_LOGCOUNT] = st[ST_AVGEXPPD] = 0.0;
         st[ST_ACC] = st[ST_PROP] = st[ST_ACCV] = st[ST_PROPV] = 0.0;
         st[ST_BLK_PROP] = st[ST_BLK_S1] = st[ST_BLK_ACC] = st[ST_BLK_SUMLR] = 0.0;
+        st[ST_BLK_ERR1] = st[ST_BLK_ERR0] = 0.0;
         CK(cudaMemcpy(h->chains[c].dev.stats, st, sizeof(st), cudaMemcpyHostToDevice));
     }
     return DQMC_OK;

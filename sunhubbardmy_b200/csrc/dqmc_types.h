@@ -90,7 +90,7 @@ enum {
     ST_ACC, ST_PROP, ST_NOBS, ST_INFO, ST_LOGDETM_RE, ST_LOGDETM_IM, ST_LAST_WRAP,
     ST_ACCV, ST_PROPV,
     ST_BLK_LR_RE, ST_BLK_LR_IM, ST_BLK_PH_RE, ST_BLK_PH_IM, ST_BLK_PROP, ST_BLK_S1, ST_BLK_ACC,
-    ST_BLK_DS, ST_BLK_U2, ST_BLK_SUMLR,
+    ST_BLK_DS, ST_BLK_U2, ST_BLK_SUMLR, ST_BLK_ERR1, ST_BLK_ERR0,
     ST_COUNT = 32
 };
 

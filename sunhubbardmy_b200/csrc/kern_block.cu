@@ -71,6 +71,10 @@ __global__ void k_blk_decide(const ChainDev* __restrict__ chains, int nchains) {
         if (rre != 0.0) {
             const double logr = lr.x + log(fabs(rre));
             acc = log(c.stats[ST_BLK_U2]) < logr + c.stats[ST_BLK_DS];
+            // how well -dS predicts the exact log ratio, against predicting 0
+            const double e1 = logr + c.stats[ST_BLK_DS];
+            c.stats[ST_BLK_ERR1] += e1 * e1;
+            c.stats[ST_BLK_ERR0] += logr * logr;
         }
     }
     c.blk[N + 1] = acc;

@@ -86,7 +86,8 @@ class DqmcDiag(C.Structure):
     _fields_ = [(n, C.c_double) for n in (
         "phase_re", "phase_im", "logweight_re", "logweight_im", "max_wrap_error", "max_phasediff",
         "avglog10error_sum", "logcount", "avgexpphasediff_sum", "accepted", "proposed", "nobs",
-        "accepted_v", "proposed_v", "blk_proposed", "blk_stage1", "blk_accepted", "blk_sum_logratio")]
+        "accepted_v", "proposed_v", "blk_proposed", "blk_stage1", "blk_accepted", "blk_sum_logratio",
+        "blk_err_learned", "blk_err_zero")]
 
 
 _lib = None
@@ -352,7 +353,8 @@ class Dqmc:
                     avgexpphasediff=d.avgexpphasediff_sum, accepted=d.accepted, proposed=d.proposed,
                     nobs=d.nobs, accepted_v=d.accepted_v, proposed_v=d.proposed_v,
                     blk_proposed=d.blk_proposed, blk_stage1=d.blk_stage1, blk_accepted=d.blk_accepted,
-                    blk_sum_logratio=d.blk_sum_logratio)
+                    blk_sum_logratio=d.blk_sum_logratio, blk_err_learned=d.blk_err_learned,
+                    blk_err_zero=d.blk_err_zero)
 
     def energy_all(self) -> np.ndarray:
         """energy_bin(1:10) of every chain, shape (n_chains, 10) complex."""
