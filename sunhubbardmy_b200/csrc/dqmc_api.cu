@@ -899,7 +899,8 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
         if (m->p.rv != 0.0) d.vconf = (int32_t*)dalloc(h, (size_t)lt * nnf * N * sizeof(int32_t));
         d.tau = (double2*)dalloc(h, (size_t)N * z);
         d.T = (double2*)dalloc(h, (size_t)(N / 16 + 1) * 256 * z);
-        d.smallw = (double2*)dalloc(h, (size_t)32 * N * z);
+        d.T64 = (double2*)dalloc(h, (size_t)(N / 64 + 1) * 4096 * z);
+        d.smallw = (double2*)dalloc(h, (size_t)128 * N * z);
         d.vecs = (double*)dalloc(h, (size_t)8 * N * sizeof(double));
         d.perm = (int*)dalloc(h, (size_t)N * sizeof(int));
         d.conf = (int32_t*)dalloc(h, (size_t)lt * N * sizeof(int32_t));

@@ -55,7 +55,8 @@ struct ChainDev {
     double2* B;
     double2* tau;              // N (Householder scalars)
     double2* T;                // (N/16+1) x 16 x 16 block-reflector factors
-    double2* smallw;           // 32 x N scratch
+    double2* T64;              // (N/64+1) x 64 x 64 factors of the 64-wide blocks
+    double2* smallw;           // 128 x N scratch
     double* vecs;              // 8 x N real scratch (norms, dmax/dmin)
     int* perm;                 // N
     int32_t* conf;             // ltrot x N (site fastest), values 1..lcomp

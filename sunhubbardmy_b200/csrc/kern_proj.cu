@@ -44,9 +44,10 @@ DQ_DEV LinalgScratch proj_scratch(const ChainDev& c) {
     LinalgScratch s;
     s.Vs = c.W[5];
     s.Ws = c.smallw;
-    s.Ws2 = c.smallw + (size_t)QR_NB * c.N;
+    s.Ws2 = c.smallw + (size_t)QR_NB2 * c.N;
     s.T = c.T;
     s.tau = c.tau;
+    s.T64 = c.T64;
     return s;
 }
 
@@ -73,7 +74,7 @@ __global__ void __launch_bounds__(256) k_proj_qr(const ChainDev* __restrict__ ch
     double2* A = c.W[1];
     for (size_t e = tid; e < (size_t)N * ne; e += nth) A[e] = X[e];
     __syncthreads();
-    cta_qr(A, N, sc, buf, buf, &S->L, ne);
+    cta_qr64(A, N, sc, buf, buf, &S->L, ne);
     double lg = 0.0, neg = 0.0;
     for (int i = tid; i < ne; i += nth) {
         double r = A[MIDX(i, i, N)].x;
@@ -82,7 +83,7 @@ __global__ void __launch_bounds__(256) k_proj_qr(const ChainDev* __restrict__ ch
     }
     lg = block_sum(lg, S->red);
     neg = block_sum(neg, S->red);
-    cta_form_q(A, N, X, sc, buf, ne);
+    cta_form_q64(A, N, X, sc, buf, ne);
     __syncthreads();
     if (((long long)llround(neg)) & 1)
         for (int i = tid; i < N; i += nth) X[i] = cmk(-X[i].x, -X[i].y);
@@ -106,7 +107,7 @@ __global__ void __launch_bounds__(256) k_proj_ulr(const ChainDev* __restrict__ c
     g.M = ne; g.N = ne; g.K = N; g.alpha = cmk(1, 0); g.beta = cmk(0, 0);
     g.A = c.ULT; g.lda = N; g.opA = OP_T; g.B = c.UR; g.ldb = N; g.opB = OP_N; g.C = M; g.ldc = ne;
     zgemm_cta<GemmBig>(g, 0, 1, buf);
-    cta_qr(M, ne, sc, buf, buf, &S->L);
+    cta_qr64(M, ne, sc, buf, buf, &S->L);
     double2 ld = cmk(0, 0);
     if (logdet) {
         ld = cta_logdet_q(sc.tau, ne, S->red);
@@ -121,7 +122,7 @@ __global__ void __launch_bounds__(256) k_proj_ulr(const ChainDev* __restrict__ c
     double2* X = chain_mat(c, out_id);
     for (int e = tid; e < ne * ne; e += nth) X[e] = cmk((e % ne) == (e / ne) ? 1.0 : 0.0, 0.0);
     __syncthreads();
-    cta_apply_qh(M, ne, X, sc, buf);
+    cta_apply_qh64(M, ne, X, sc, buf);
     cta_trsm_upper(M, ne, X, buf, &S->L);
     if (logdet && tid == 0) {
         double w = c.logwDV[ia] + (ib >= 0 ? c.logwDV[ib] : 0.0);

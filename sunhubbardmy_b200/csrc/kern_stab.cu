@@ -25,9 +25,10 @@ DQ_DEV LinalgScratch make_scratch(const ChainDev& c) {
     LinalgScratch s;
     s.Vs = c.W[5];
     s.Ws = c.smallw;
-    s.Ws2 = c.smallw + (size_t)QR_NB * c.N;
+    s.Ws2 = c.smallw + (size_t)QR_NB2 * c.N;
     s.T = c.T;
     s.tau = c.tau;
+    s.T64 = c.T64;
     return s;
 }
 
@@ -84,7 +85,7 @@ __global__ void __launch_bounds__(256) k_stab(const ChainDev* __restrict__ chain
         W2[e] = cscale(W0[MIDX(r, j, N)], Dsrc[j]);
     }
     __syncthreads();
-    cta_qr(W2, N, sc, buf, buf, &S->L);
+    cta_qr64(W2, N, sc, buf, buf, &S->L);
     for (int i = tid; i < N; i += nth) Ddst[i] = W2[MIDX(i, i, N)].x;
     double2 ldq = cta_logdet_q(sc.tau, N, S->red);
     if (tid == 0) c.logdetQ[dst] = ldq;
@@ -101,7 +102,7 @@ __global__ void __launch_bounds__(256) k_stab(const ChainDev* __restrict__ chain
         W4[e] = Vsrc[MIDX(perm[r], k, N)];
     }
     __syncthreads();
-    cta_form_q(W2, N, c.U + (size_t)dst * NN, sc, buf);
+    cta_form_q64(W2, N, c.U + (size_t)dst * NN, sc, buf);
     ZGemmArgs g;
     g.M = N; g.N = N; g.K = N; g.alpha = cmk(1, 0); g.beta = cmk(0, 0);
     g.A = W3; g.lda = N; g.opA = OP_N; g.B = W4; g.ldb = N; g.opB = OP_N;
@@ -117,7 +118,7 @@ DQ_DEV void dminmax(double d, double& dmax, double& dmin) {
 
 // Green's function into Gnew.  mode 0: green_equaltime(R = slot nr, L = slot nl);
 // mode 1: green_equaltimebb (R = slot nr).  New log weight -> stats[ST_LOGDETM_*].
-__global__ void __launch_bounds__(256) k_green(const ChainDev* __restrict__ chains, int nr, int nl, int mode) {
+__global__ void __launch_bounds__(256, 2) k_green(const ChainDev* __restrict__ chains, int nr, int nl, int mode) {
     extern __shared__ double2 ssm[];
     const ChainDev c = chains[blockIdx.x];
     const int N = c.N, tid = threadIdx.x, nth = blockDim.x;
@@ -174,7 +175,7 @@ __global__ void __launch_bounds__(256) k_green(const ChainDev* __restrict__ chai
     }
     slog = block_sum(slog, S->red);
     __syncthreads();
-    cta_qr(M, N, sc, buf, buf, &S->L);
+    cta_qr64(M, N, sc, buf, buf, &S->L);
     double2 ldm = cta_logdet_q(sc.tau, N, S->red);
     double2 lr = cmk(0, 0);
     for (int i = tid; i < N; i += nth) {
@@ -189,7 +190,7 @@ __global__ void __launch_bounds__(256) k_green(const ChainDev* __restrict__ chai
         X[e] = cscale(cconj(UR[MIDX(j, i, N)]), 1.0 / drmax[i]);
     }
     __syncthreads();
-    cta_apply_qh(M, N, X, sc, buf);
+    cta_apply_qh64(M, N, X, sc, buf);
     cta_trsm_upper(M, N, X, buf, &S->L);
     if (mode == 0) {
         const double2* UL = c.U + (size_t)nl * NN;
@@ -300,11 +301,11 @@ __global__ void __launch_bounds__(256) k_qr_test(const ChainDev* __restrict__ ch
     StabSmem* S = (StabSmem*)(ssm + (((size_t)N * QR_NB > (size_t)GemmBig::SMEM_ELEMS) ? (size_t)N * QR_NB : (size_t)GemmBig::SMEM_ELEMS));
     LinalgScratch sc = make_scratch(c);
     double2* A = chain_mat(c, a_id);
-    cta_qr(A, N, sc, ssm, ssm, &S->L);
+    cta_qr64(A, N, sc, ssm, ssm, &S->L);
     double2 ld = cta_logdet_q(sc.tau, N, S->red);
     if (threadIdx.x == 0) { c.stats[ST_LOGDETM_RE] = ld.x; c.stats[ST_LOGDETM_IM] = ld.y; }
     __syncthreads();
-    cta_form_q(A, N, chain_mat(c, q_id), sc, ssm);
+    cta_form_q64(A, N, chain_mat(c, q_id), sc, ssm);
 }
 
 // swap logical slot n with the spare slot (logical id `spare`)

@@ -11,11 +11,12 @@
 #define QR_NB 16
 
 struct LinalgScratch {
-    double2* Vs;      // N x 16 explicit reflector block (ld N)
-    double2* Ws;      // 16 x N (ld 16)
-    double2* Ws2;     // 16 x N (ld 16)
-    double2* T;       // (N/16 + 1) x 16 x 16 block-reflector triangles
+    double2* Vs;      // N x 64 explicit reflector block (ld N)
+    double2* Ws;      // 64 x N (ld 16 for 16-wide blocks, 64 for 64-wide ones)
+    double2* Ws2;     // 64 x N
+    double2* T;       // (N/16 + 1) x 16 x 16 block-reflector triangles of the panels
     double2* tau;     // N
+    double2* T64 = nullptr;   // (N/64 + 1) x 64 x 64 triangles of the 64-wide blocks (two-level QR)
 };
 
 struct LinalgSmem {
@@ -281,5 +282,140 @@ static __device__ void cta_trsm_upper(const double2* A, int N, double2* X, cplx*
             for (int a = 0; a < jb; ++a) X[MIDX(p + a, cc, N)] = x[a];
         }
         __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Two-level blocked QR: 16-wide panels inside 64-wide blocks.  The panels of a
+// block update only the block's own columns; the trailing matrix and the later
+// applications of Q use the block's 64-wide reflector (I - V T V^H), whose
+// GEMMs have an inner dimension of 64 instead of 16.  T of a block is built
+// from its panels' triangles: for H = H_a H_b,
+//   T = [[T_a, -T_a (V_a^H V_b) T_b], [0, T_b]].
+// ---------------------------------------------------------------------------
+#define QR_NB2 64
+
+// X[p:N, c0:c0+nc] <- (I - V T V^H)^op X for a jb-wide block (jb <= 64; T ld 64)
+static __device__ void apply_block64(const double2* Vs, const double2* Tp, int N, int p, int jb,
+                                     double2* X, int c0, int nc, int use_th, LinalgScratch& sc, cplx* gsm) {
+    if (nc <= 0) return;
+    const int m = N - p;
+    ZGemmArgs g;
+    g.M = jb; g.N = nc; g.K = m; g.alpha = cmk(1, 0); g.beta = cmk(0, 0);
+    g.A = Vs; g.lda = N; g.opA = OP_C;
+    g.B = X + MIDX(p, c0, N); g.ldb = N; g.opB = OP_N;
+    g.C = sc.Ws; g.ldc = QR_NB2;
+    zgemm_cta<GemmBig>(g, 0, 1, gsm);
+    g.M = jb; g.N = nc; g.K = jb;
+    g.A = Tp; g.lda = QR_NB2; g.opA = use_th ? OP_C : OP_N;
+    g.B = sc.Ws; g.ldb = QR_NB2; g.opB = OP_N;
+    g.C = sc.Ws2; g.ldc = QR_NB2;
+    zgemm_cta<GemmBig>(g, 0, 1, gsm);
+    g.M = m; g.N = nc; g.K = jb; g.alpha = cmk(-1, 0); g.beta = cmk(1, 0);
+    g.A = Vs; g.lda = N; g.opA = OP_N;
+    g.B = sc.Ws2; g.ldb = QR_NB2; g.opB = OP_N;
+    g.C = X + MIDX(p, c0, N); g.ldc = N;
+    zgemm_cta<GemmBig>(g, 0, 1, gsm);
+}
+
+// T (64 x 64, ld 64, zero outside the upper triangle) of the block whose explicit
+// V (jb2 columns, rows from the block's first row, ld N) is in sc.Vs, from the
+// 16 x 16 triangles of its panels (Tp16, consecutive)
+static __device__ void build_t64(int N, int P, int jb2, const double2* Tp16, double2* T64, LinalgScratch& sc,
+                                 cplx* gsm) {
+    const int tid = threadIdx.x, nth = blockDim.x, m = N - P;
+    for (int e = tid; e < QR_NB2 * QR_NB2; e += nth) {
+        const int a = e % QR_NB2, b = e / QR_NB2;
+        T64[e] = (a < QR_NB && b < QR_NB && b < jb2) ? Tp16[a + b * QR_NB] : cmk(0, 0);
+    }
+    __syncthreads();
+    for (int k = QR_NB; k < jb2; k += QR_NB) {
+        const int jb = min(QR_NB, jb2 - k);
+        const double2* Tb = Tp16 + (size_t)(k / QR_NB) * QR_NB * QR_NB;
+        ZGemmArgs g;   // X = V_a^H V_b  (k x jb)
+        g.M = k; g.N = jb; g.K = m; g.alpha = cmk(1, 0); g.beta = cmk(0, 0);
+        g.A = sc.Vs; g.lda = N; g.opA = OP_C;
+        g.B = sc.Vs + (size_t)k * N; g.ldb = N; g.opB = OP_N;
+        g.C = sc.Ws; g.ldc = QR_NB2;
+        zgemm_cta<GemmBig>(g, 0, 1, gsm);
+        // Y = T_a X (T_a upper triangular)
+        for (int e = tid; e < k * jb; e += nth) {
+            const int a = e % k, b = e / k;
+            double2 acc = cmk(0, 0);
+            for (int c = a; c < k; ++c) acc = cfma(T64[a + c * QR_NB2], sc.Ws[c + b * QR_NB2], acc);
+            sc.Ws2[a + b * QR_NB2] = acc;
+        }
+        __syncthreads();
+        // T(0:k, k:k+jb) = -Y T_b ; T(k:k+jb, k:k+jb) = T_b
+        for (int e = tid; e < k * jb; e += nth) {
+            const int a = e % k, b = e / k;
+            double2 acc = cmk(0, 0);
+            for (int c = 0; c <= b; ++c) acc = cfma(sc.Ws2[a + c * QR_NB2], Tb[c + b * QR_NB], acc);
+            T64[a + (k + b) * QR_NB2] = cmk(-acc.x, -acc.y);
+        }
+        for (int e = tid; e < jb * jb; e += nth) {
+            const int a = e % jb, b = e / jb;
+            T64[(k + a) + (k + b) * QR_NB2] = Tb[a + b * QR_NB];
+        }
+        __syncthreads();
+    }
+}
+
+// In-place QR of the first ncol columns of A (ld N), two-level blocked; R above
+// the diagonal, reflectors below, tau, panel triangles in sc.T and block
+// triangles in sc.T64.  smem_panel holds >= N*16 double2.
+static __device__ void cta_qr64(double2* A, int N, LinalgScratch& sc, double2* smem_panel, cplx* gsm, LinalgSmem* L,
+                                int ncol = -1) {
+    if (ncol < 0) ncol = N;
+    for (int P = 0; P < ncol; P += QR_NB2) {
+        const int jb2 = min(QR_NB2, ncol - P);
+        for (int p = P; p < P + jb2; p += QR_NB) {
+            const int jb = min(QR_NB, P + jb2 - p), m = N - p;
+            double2* Pn = smem_panel;
+            for (int e = threadIdx.x; e < m * jb; e += blockDim.x) {
+                int r = e % m, cc = e / m;
+                Pn[(size_t)cc * m + r] = A[MIDX(p + r, p + cc, N)];
+            }
+            __syncthreads();
+            panel_qr(Pn, m, jb, sc.tau + p, L);
+            double2* Tp = sc.T + (size_t)(p / QR_NB) * QR_NB * QR_NB;
+            panel_larft(Pn, m, jb, sc.tau + p, Tp, L);
+            for (int e = threadIdx.x; e < m * jb; e += blockDim.x) {
+                int r = e % m, cc = e / m;
+                A[MIDX(p + r, p + cc, N)] = Pn[(size_t)cc * m + r];
+                sc.Vs[MIDX(r, cc, N)] = (r < cc) ? cmk(0, 0) : (r == cc) ? cmk(1, 0) : Pn[(size_t)cc * m + r];
+            }
+            __syncthreads();
+            if (p + jb < P + jb2) apply_block(sc.Vs, Tp, N, p, jb, A, p + jb, P + jb2 - p - jb, 1, sc, gsm);
+        }
+        build_vblock(A, N, P, jb2, sc.Vs);
+        double2* T64 = sc.T64 + (size_t)(P / QR_NB2) * QR_NB2 * QR_NB2;
+        build_t64(N, P, jb2, sc.T + (size_t)(P / QR_NB) * QR_NB * QR_NB, T64, sc, gsm);
+        if (P + jb2 < ncol) apply_block64(sc.Vs, T64, N, P, jb2, A, P + jb2, ncol - P - jb2, 1, sc, gsm);
+    }
+}
+
+// The first ncol columns of Q (ld N) from cta_qr64's factors into Qout.
+static __device__ void cta_form_q64(const double2* A, int N, double2* Qout, LinalgScratch& sc, cplx* gsm, int ncol = -1) {
+    if (ncol < 0) ncol = N;
+    for (int e = threadIdx.x; e < N * ncol; e += blockDim.x) {
+        int r = e % N, cc = e / N;
+        Qout[e] = cmk(r == cc ? 1.0 : 0.0, 0.0);
+    }
+    __syncthreads();
+    const int last = ((ncol - 1) / QR_NB2) * QR_NB2;
+    for (int P = last; P >= 0; P -= QR_NB2) {
+        const int jb2 = min(QR_NB2, ncol - P);
+        build_vblock(A, N, P, jb2, sc.Vs);
+        apply_block64(sc.Vs, sc.T64 + (size_t)(P / QR_NB2) * QR_NB2 * QR_NB2, N, P, jb2, Qout, P, ncol - P, 0, sc, gsm);
+    }
+}
+
+// X <- Q^H X for all N columns of X (Q from cta_qr64 of an N x N matrix).
+static __device__ void cta_apply_qh64(const double2* A, int N, double2* X, LinalgScratch& sc, cplx* gsm) {
+    for (int P = 0; P < N; P += QR_NB2) {
+        const int jb2 = min(QR_NB2, N - P);
+        build_vblock(A, N, P, jb2, sc.Vs);
+        apply_block64(sc.Vs, sc.T64 + (size_t)(P / QR_NB2) * QR_NB2 * QR_NB2, N, P, jb2, X, 0, N, 1, sc, gsm);
     }
 }
