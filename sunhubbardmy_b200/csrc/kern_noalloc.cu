@@ -35,14 +35,14 @@ struct NoallocSmem {
 };
 
 static size_t noalloc_smem_bytes(int n) {
-    size_t a = (size_t)n * QR_NB, b = GemmBig::SMEM_ELEMS;
+    size_t a = QR_PANEL_ELEMS(n), b = GemmBig::SMEM_ELEMS;
     if ((size_t)GemmWide::SMEM_ELEMS > b) b = GemmWide::SMEM_ELEMS;
     return (a > b ? a : b) * sizeof(double2) + sizeof(NoallocSmem) + 64;
 }
 
 __global__ void __launch_bounds__(256) k_qr_noalloc(int n, double2* A, double2* Q, double2* logdet, double2* scratch) {
     extern __shared__ double2 nsm[];
-    size_t off = ((size_t)n * QR_NB > (size_t)GemmBig::SMEM_ELEMS) ? (size_t)n * QR_NB : (size_t)GemmBig::SMEM_ELEMS;
+    size_t off = (QR_PANEL_ELEMS(n) > (size_t)GemmBig::SMEM_ELEMS) ? QR_PANEL_ELEMS(n) : (size_t)GemmBig::SMEM_ELEMS;
     NoallocSmem* S = (NoallocSmem*)(nsm + off);
     LinalgScratch sc;
     sc.Vs = scratch;

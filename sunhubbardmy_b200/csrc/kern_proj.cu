@@ -52,7 +52,7 @@ DQ_DEV LinalgScratch proj_scratch(const ChainDev& c) {
 }
 
 static size_t proj_la_smem(int maxN) {
-    size_t a = (size_t)maxN * QR_NB;
+    size_t a = QR_PANEL_ELEMS(maxN);
     size_t b = GemmBig::SMEM_ELEMS;
     if ((size_t)GemmWide::SMEM_ELEMS > b) b = GemmWide::SMEM_ELEMS;
     return (a > b ? a : b) * sizeof(double2) + sizeof(ProjSmem) + 64;
@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(256) k_proj_qr(const ChainDev* __restrict__ ch
     const ModelDev& md = *c.md;
     const int N = c.N, ne = md.ne, tid = threadIdx.x, nth = blockDim.x;
     double2* buf = ssm;
-    ProjSmem* S = (ProjSmem*)(ssm + (((size_t)N * QR_NB > (size_t)GemmBig::SMEM_ELEMS) ? (size_t)N * QR_NB : (size_t)GemmBig::SMEM_ELEMS));
+    ProjSmem* S = (ProjSmem*)(ssm + ((QR_PANEL_ELEMS(N) > (size_t)GemmBig::SMEM_ELEMS) ? QR_PANEL_ELEMS(N) : (size_t)GemmBig::SMEM_ELEMS));
     LinalgScratch sc = proj_scratch(c);
     double2* X = chain_mat(c, mat_id);
     double2* A = c.W[1];
@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(256) k_proj_ulr(const ChainDev* __restrict__ c
     const ModelDev& md = *c.md;
     const int N = c.N, ne = md.ne, tid = threadIdx.x, nth = blockDim.x;
     double2* buf = ssm;
-    ProjSmem* S = (ProjSmem*)(ssm + (((size_t)N * QR_NB > (size_t)GemmBig::SMEM_ELEMS) ? (size_t)N * QR_NB : (size_t)GemmBig::SMEM_ELEMS));
+    ProjSmem* S = (ProjSmem*)(ssm + ((QR_PANEL_ELEMS(N) > (size_t)GemmBig::SMEM_ELEMS) ? QR_PANEL_ELEMS(N) : (size_t)GemmBig::SMEM_ELEMS));
     LinalgScratch sc = proj_scratch(c);
     double2* M = c.W[2];
     ZGemmArgs g;

@@ -33,7 +33,7 @@ DQ_DEV LinalgScratch make_scratch(const ChainDev& c) {
 }
 
 static size_t stab_smem_bytes(int maxN) {
-    size_t a = (size_t)maxN * QR_NB;
+    size_t a = QR_PANEL_ELEMS(maxN);
     size_t b = GemmBig::SMEM_ELEMS;
     if ((size_t)GemmWide::SMEM_ELEMS > b) b = GemmWide::SMEM_ELEMS;
     return (a > b ? a : b) * sizeof(double2) + sizeof(StabSmem) + 64;
@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(256) k_stab(const ChainDev* __restrict__ chain
     const int N = c.N, tid = threadIdx.x, nth = blockDim.x;
     const size_t NN = (size_t)N * N;
     double2* buf = ssm;
-    StabSmem* S = (StabSmem*)(ssm + (((size_t)N * QR_NB > (size_t)GemmBig::SMEM_ELEMS) ? (size_t)N * QR_NB : (size_t)GemmBig::SMEM_ELEMS));
+    StabSmem* S = (StabSmem*)(ssm + ((QR_PANEL_ELEMS(N) > (size_t)GemmBig::SMEM_ELEMS) ? QR_PANEL_ELEMS(N) : (size_t)GemmBig::SMEM_ELEMS));
     LinalgScratch sc = make_scratch(c);
     double2* W0 = c.W[0];
     double2* W2 = c.W[1];
@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(256, 2) k_green(const ChainDev* __restrict__ c
     const int N = c.N, tid = threadIdx.x, nth = blockDim.x;
     const size_t NN = (size_t)N * N;
     double2* buf = ssm;
-    StabSmem* S = (StabSmem*)(ssm + (((size_t)N * QR_NB > (size_t)GemmBig::SMEM_ELEMS) ? (size_t)N * QR_NB : (size_t)GemmBig::SMEM_ELEMS));
+    StabSmem* S = (StabSmem*)(ssm + ((QR_PANEL_ELEMS(N) > (size_t)GemmBig::SMEM_ELEMS) ? QR_PANEL_ELEMS(N) : (size_t)GemmBig::SMEM_ELEMS));
     LinalgScratch sc = make_scratch(c);
     nr = c.slotmap[nr];
     if (mode == 0) nl = c.slotmap[nl];
@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(256) k_qr_test(const ChainDev* __restrict__ ch
     extern __shared__ double2 ssm[];
     const ChainDev c = chains[blockIdx.x];
     const int N = c.N;
-    StabSmem* S = (StabSmem*)(ssm + (((size_t)N * QR_NB > (size_t)GemmBig::SMEM_ELEMS) ? (size_t)N * QR_NB : (size_t)GemmBig::SMEM_ELEMS));
+    StabSmem* S = (StabSmem*)(ssm + ((QR_PANEL_ELEMS(N) > (size_t)GemmBig::SMEM_ELEMS) ? QR_PANEL_ELEMS(N) : (size_t)GemmBig::SMEM_ELEMS));
     LinalgScratch sc = make_scratch(c);
     double2* A = chain_mat(c, a_id);
     cta_qr64(A, N, sc, ssm, ssm, &S->L);

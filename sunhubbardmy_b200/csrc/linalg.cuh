@@ -9,6 +9,9 @@
 #include "zgemm.cuh"
 
 #define QR_NB 16
+// shared memory of a panel: m x 16 with an odd leading dimension (m or m + 1),
+// so that the 16 columns fall in different banks
+#define QR_PANEL_ELEMS(N) ((size_t)((N) + 1) * QR_NB)
 
 struct LinalgScratch {
     double2* Vs;      // N x 64 explicit reflector block (ld N)
@@ -29,10 +32,10 @@ struct LinalgSmem {
 };
 
 // ---- panel factorisation (zgeqr2 on an m x jb panel in shared memory) ----
-static __device__ void panel_qr(double2* P, int m, int jb, double2* taus, LinalgSmem* L) {
+static __device__ void panel_qr(double2* P, int m, int ldp, int jb, double2* taus, LinalgSmem* L) {
     const int tid = threadIdx.x, nth = blockDim.x;
     for (int j = 0; j < jb; ++j) {
-        double2* col = P + (size_t)j * m;
+        double2* col = P + (size_t)j * ldp;
         double ss = 0.0;
         for (int r = j + 1 + tid; r < m; r += nth) ss += cabs2(col[r]);
         ss = block_sum(ss, L->red);
@@ -76,7 +79,7 @@ static __device__ void panel_qr(double2* P, int m, int jb, double2* taus, Linalg
             const bool ok = cc < jb;
             double2 acc = cmk(0, 0);
             if (ok) {
-                const double2* pc = P + (size_t)cc * m;
+                const double2* pc = P + (size_t)cc * ldp;
                 if (gl == 0) acc = pc[j];
                 for (int r = j + 1 + gl; r < m; r += 16) acc = cfma(cconj(col[r]), pc[r], acc);
             }
@@ -95,7 +98,7 @@ static __device__ void panel_qr(double2* P, int m, int jb, double2* taus, Linalg
             int cc = j + 1 + e / nr, r = j + e % nr;
             double2 v = (r == j) ? cmk(1, 0) : col[r];
             double2 f = cmul(ctau, L->w[cc]);
-            P[(size_t)cc * m + r] = csub(P[(size_t)cc * m + r], cmul(v, f));
+            P[(size_t)cc * ldp + r] = csub(P[(size_t)cc * ldp + r], cmul(v, f));
         }
         __syncthreads();
     }
@@ -103,15 +106,15 @@ static __device__ void panel_qr(double2* P, int m, int jb, double2* taus, Linalg
 
 // T (jb x jb upper) of the block reflector H_1..H_jb = I - V T V^H (zlarft 'F','C').
 // V is the unit-lower panel in shared memory (m x jb).
-static __device__ void panel_larft(const double2* P, int m, int jb, const double2* taus, double2* Tout, LinalgSmem* L) {
+static __device__ void panel_larft(const double2* P, int m, int ldp, int jb, const double2* taus, double2* Tout, LinalgSmem* L) {
     const int tid = threadIdx.x;
     // Gram S(a,b) = V(:,a)^H V(:,b) for a < b
     for (int e = tid; e < jb * jb; e += blockDim.x) {
         int a = e % jb, b = e / jb;
         if (a < b) {
-            double2 s = P[(size_t)a * m + b];          // V(b,a)^* * V(b,b)=1, rows r >= b
+            double2 s = P[(size_t)a * ldp + b];          // V(b,a)^* * V(b,b)=1, rows r >= b
             s = cconj(s);
-            for (int r = b + 1; r < m; ++r) s = cfma(cconj(P[(size_t)a * m + r]), P[(size_t)b * m + r], s);
+            for (int r = b + 1; r < m; ++r) s = cfma(cconj(P[(size_t)a * ldp + r]), P[(size_t)b * ldp + r], s);
             L->S[a + b * QR_NB] = s;
         }
     }
@@ -186,25 +189,25 @@ static __device__ void apply_block(const double2* Vs, const double2* Tp, int N, 
 
 // In-place QR of the first ncol columns of A (N rows, ld N; ncol <= N, default
 // all N): R in the upper triangle, reflectors below, tau and the per-panel T
-// factors in the scratch.  smem_panel holds >= N*16 double2.
+// factors in the scratch.  smem_panel holds >= QR_PANEL_ELEMS(N) double2.
 static __device__ void cta_qr(double2* A, int N, LinalgScratch& sc, double2* smem_panel, cplx* gsm, LinalgSmem* L,
                               int ncol = -1) {
     if (ncol < 0) ncol = N;
     for (int p = 0; p < ncol; p += QR_NB) {
-        const int jb = min(QR_NB, ncol - p), m = N - p;
+        const int jb = min(QR_NB, ncol - p), m = N - p, ldp = m + ((m & 1) ^ 1);
         double2* P = smem_panel;
         for (int e = threadIdx.x; e < m * jb; e += blockDim.x) {
             int r = e % m, cc = e / m;
-            P[(size_t)cc * m + r] = A[MIDX(p + r, p + cc, N)];
+            P[(size_t)cc * ldp + r] = A[MIDX(p + r, p + cc, N)];
         }
         __syncthreads();
-        panel_qr(P, m, jb, sc.tau + p, L);
+        panel_qr(P, m, ldp, jb, sc.tau + p, L);
         double2* Tp = sc.T + (size_t)(p / QR_NB) * QR_NB * QR_NB;
-        panel_larft(P, m, jb, sc.tau + p, Tp, L);
+        panel_larft(P, m, ldp, jb, sc.tau + p, Tp, L);
         for (int e = threadIdx.x; e < m * jb; e += blockDim.x) {
             int r = e % m, cc = e / m;
-            A[MIDX(p + r, p + cc, N)] = P[(size_t)cc * m + r];
-            sc.Vs[MIDX(r, cc, N)] = (r < cc) ? cmk(0, 0) : (r == cc) ? cmk(1, 0) : P[(size_t)cc * m + r];
+            A[MIDX(p + r, p + cc, N)] = P[(size_t)cc * ldp + r];
+            sc.Vs[MIDX(r, cc, N)] = (r < cc) ? cmk(0, 0) : (r == cc) ? cmk(1, 0) : P[(size_t)cc * ldp + r];
         }
         __syncthreads();
         if (p + jb < ncol) apply_block(sc.Vs, Tp, N, p, jb, A, p + jb, ncol - p - jb, 1, sc, gsm);
@@ -363,27 +366,27 @@ static __device__ void build_t64(int N, int P, int jb2, const double2* Tp16, dou
 
 // In-place QR of the first ncol columns of A (ld N), two-level blocked; R above
 // the diagonal, reflectors below, tau, panel triangles in sc.T and block
-// triangles in sc.T64.  smem_panel holds >= N*16 double2.
+// triangles in sc.T64.  smem_panel holds >= QR_PANEL_ELEMS(N) double2.
 static __device__ void cta_qr64(double2* A, int N, LinalgScratch& sc, double2* smem_panel, cplx* gsm, LinalgSmem* L,
                                 int ncol = -1) {
     if (ncol < 0) ncol = N;
     for (int P = 0; P < ncol; P += QR_NB2) {
         const int jb2 = min(QR_NB2, ncol - P);
         for (int p = P; p < P + jb2; p += QR_NB) {
-            const int jb = min(QR_NB, P + jb2 - p), m = N - p;
+            const int jb = min(QR_NB, P + jb2 - p), m = N - p, ldp = m + ((m & 1) ^ 1);
             double2* Pn = smem_panel;
             for (int e = threadIdx.x; e < m * jb; e += blockDim.x) {
                 int r = e % m, cc = e / m;
-                Pn[(size_t)cc * m + r] = A[MIDX(p + r, p + cc, N)];
+                Pn[(size_t)cc * ldp + r] = A[MIDX(p + r, p + cc, N)];
             }
             __syncthreads();
-            panel_qr(Pn, m, jb, sc.tau + p, L);
+            panel_qr(Pn, m, ldp, jb, sc.tau + p, L);
             double2* Tp = sc.T + (size_t)(p / QR_NB) * QR_NB * QR_NB;
-            panel_larft(Pn, m, jb, sc.tau + p, Tp, L);
+            panel_larft(Pn, m, ldp, jb, sc.tau + p, Tp, L);
             for (int e = threadIdx.x; e < m * jb; e += blockDim.x) {
                 int r = e % m, cc = e / m;
-                A[MIDX(p + r, p + cc, N)] = Pn[(size_t)cc * m + r];
-                sc.Vs[MIDX(r, cc, N)] = (r < cc) ? cmk(0, 0) : (r == cc) ? cmk(1, 0) : Pn[(size_t)cc * m + r];
+                A[MIDX(p + r, p + cc, N)] = Pn[(size_t)cc * ldp + r];
+                sc.Vs[MIDX(r, cc, N)] = (r < cc) ? cmk(0, 0) : (r == cc) ? cmk(1, 0) : Pn[(size_t)cc * ldp + r];
             }
             __syncthreads();
             if (p + jb < P + jb2) apply_block(sc.Vs, Tp, N, p, jb, A, p + jb, P + jb2 - p - jb, 1, sc, gsm);
