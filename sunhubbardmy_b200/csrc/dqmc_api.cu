@@ -1944,18 +1944,24 @@ extern "C" int dqmc_nn_forward(dqmc_nn* nn, const int8_t* fields, int B, double*
     return DQMC_OK;
 }
 
-// forward with stored activations, then the gradient of sum_b r_b S_b into grad
-static int nn_fwd_bwd(dqmc_nn* nn, int B, const double* r_host, double* S_host) {
+// forward with stored activations (S to the host), then, if r_host is given, the
+// gradient of sum_b r_b S_b into grad
+static int nn_fwd(dqmc_nn* nn, int B, double* S_host) {
     CK(cudaMemsetAsync(nn->S, 0, B * sizeof(double), nn->st));
-    NNIn in = nn_in_fields(nn);
-    launch_nn_forward(nn_w(nn), in, B, nn->S, nn->h1, nn->h2, nn->st);
+    launch_nn_forward(nn_w(nn), nn_in_fields(nn), B, nn->S, nn->h1, nn->h2, nn->st);
     CK(cudaMemcpyAsync(S_host, nn->S, B * sizeof(double), cudaMemcpyDeviceToHost, nn->st));
     CK(cudaStreamSynchronize(nn->st));
-    if (!r_host) return DQMC_OK;
+    return DQMC_OK;
+}
+static int nn_bwd(dqmc_nn* nn, int B, const double* r_host) {
     CK(cudaMemcpyAsync(nn->r, r_host, B * sizeof(double), cudaMemcpyHostToDevice, nn->st));
     CK(cudaMemsetAsync(nn->grad, 0, NN_NPARAM * sizeof(float), nn->st));
-    launch_nn_backward(nn_w(nn), in, B, nn->r, nn->h1, nn->h2, nn->dp2, nn->grad, 2 * nn->nsm, nn->st);
+    launch_nn_backward(nn_w(nn), nn_in_fields(nn), B, nn->r, nn->h1, nn->h2, nn->dp2, nn->grad, 2 * nn->nsm, nn->st);
     return DQMC_OK;
+}
+static int nn_fwd_bwd(dqmc_nn* nn, int B, const double* r_host, double* S_host) {
+    int rc = nn_fwd(nn, B, S_host); if (rc) return rc;
+    return r_host ? nn_bwd(nn, B, r_host) : DQMC_OK;
 }
 
 extern "C" int dqmc_nn_gradient(dqmc_nn* nn, const int8_t* fields, int B, const double* r, double* S, float* grad) {
@@ -1971,7 +1977,7 @@ extern "C" int dqmc_nn_gradient(dqmc_nn* nn, const int8_t* fields, int B, const 
 // one Adam step on the centred squared error of S against the targets y
 static int nn_train_loaded(dqmc_nn* nn, const double* y, int B, double lr, double* loss) {
     std::vector<double> S(B), r(B);
-    int rc = nn_fwd_bwd(nn, B, nullptr, S.data()); if (rc) return rc;
+    int rc = nn_fwd(nn, B, S.data()); if (rc) return rc;
     double mean = 0.0;
     for (int b = 0; b < B; ++b) mean += (S[b] - y[b]) / B;
     double l = 0.0;
@@ -1980,7 +1986,7 @@ static int nn_train_loaded(dqmc_nn* nn, const double* y, int B, double lr, doubl
         l += d * d / B;
         r[b] = 2.0 * d / B;
     }
-    if ((rc = nn_fwd_bwd(nn, B, r.data(), S.data()))) return rc;
+    if ((rc = nn_bwd(nn, B, r.data()))) return rc;   // the activations of the forward above
     nn->step += 1;
     const float b1c = 1.f - (float)std::pow(0.9, nn->step), b2c = 1.f - (float)std::pow(0.999, nn->step);
     launch_nn_adam(nn->theta, nn->grad, nn->m1, nn->m2, NN_NPARAM, (float)lr, b1c, b2c, nn->W2T, nn->W2R, nn->st);
