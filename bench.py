@@ -540,7 +540,7 @@ def learned_arm(args, rank: int, local_rank: int) -> None:
 
     l0, var_y = val_loss()
     t0 = time.perf_counter()
-    losses = train(nn, g, targets[tr], args.train_steps, batch=32, lr=args.lr, seed=1)
+    losses = train(nn, g, targets[tr], args.train_steps, batch=32, lr=args.lr, seed=1, slots=tr)
     train_s = time.perf_counter() - t0
     l1, _ = val_loss()
 

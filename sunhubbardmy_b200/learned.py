@@ -101,12 +101,17 @@ def collect(g, sweeps: int, capacity: int) -> np.ndarray:
 
 
 def train(nn: EffectiveAction, g, targets: np.ndarray, steps: int, batch: int = 32, lr: float = 1e-3,
-          seed: int = 0) -> list:
-    """Adam on minibatches of the recorded pairs; returns the loss history."""
+          seed: int = 0, slots=None) -> list:
+    """Adam on minibatches of the recorded pairs; returns the loss history.
+    targets[k] is the target of record slot slots[k] (slots defaults to
+    0..len(targets)-1, i.e. all recorded pairs in order)."""
     rng = np.random.default_rng(seed)
     n = len(targets)
+    slots = np.arange(n, dtype=np.int32) if slots is None else np.asarray(slots, np.int32)
+    if len(slots) != n:
+        raise ValueError("slots and targets differ in length")
     losses = []
     for _ in range(steps):
-        idx = rng.integers(0, n, size=min(batch, n)).astype(np.int32)
-        losses.append(nn.train_recorded(g, idx, targets[idx], lr))
+        k = rng.integers(0, n, size=min(batch, n))
+        losses.append(nn.train_recorded(g, slots[k], targets[k], lr))
     return losses
