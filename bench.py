@@ -586,8 +586,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "config5"])
     ap.add_argument("--pairs", type=int, default=200000, help="config5: training-pair ring capacity")
-    ap.add_argument("--train-steps", type=int, default=2000, help="config5: Adam steps of 32 pairs")
-    ap.add_argument("--lr", type=float, default=1e-3, help="config5: Adam learning rate")
+    ap.add_argument("--train-steps", type=int, default=3000, help="config5: Adam steps of 32 pairs")
+    ap.add_argument("--lr", type=float, default=3e-4, help="config5: Adam learning rate")
     ap.add_argument("--ess", type=int, default=0, help="extra sweeps for the ESS/s of double occupancy")
     ap.add_argument("--ess-warmup", type=int, default=20, help="equilibration sweeps before the ESS series")
     args = ap.parse_args()

@@ -1887,7 +1887,10 @@ extern "C" int dqmc_nn_create(int ltrot, int l, int max_batch, uint64_t seed, dq
         dqmc_nn_destroy(nn);
         return fail(DQMC_ECUDA, "stream");
     }
-    // initial weights: uniform in +-sqrt(3/fan_in) (unit-variance pre-activations)
+    // initial weights: uniform in +-sqrt(3/fan_in) (unit-variance pre-activations);
+    // the readout w3 is scaled by 0.01 so that S starts close to a constant
+    // (a sum over all sites of an O(1) readout would start with fluctuations far
+    // larger than those of -log|W|)
     std::vector<float> th(NN_NPARAM, 0.f);
     uint64_t z = seed ? seed : 1;
     auto uni = [&]() {
@@ -1900,7 +1903,7 @@ extern "C" int dqmc_nn_create(int ltrot, int l, int max_batch, uint64_t seed, dq
     };
     for (int i = 0; i < 27 * 32; ++i) th[i] = (float)(uni() * std::sqrt(3.0 / 27.0));
     for (int i = 0; i < 27 * 32 * 32; ++i) th[NN_GW2 + i] = (float)(uni() * std::sqrt(3.0 / 864.0));
-    for (int i = 0; i < 32; ++i) th[NN_GW3 + i] = (float)(uni() * std::sqrt(3.0 / 32.0));
+    for (int i = 0; i < 32; ++i) th[NN_GW3 + i] = (float)(0.01 * uni() * std::sqrt(3.0 / 32.0));
     cudaMemcpy(nn->theta, th.data(), th.size() * sizeof(float), cudaMemcpyHostToDevice);
     launch_nn_pack(nn->theta, nn->W2T, nn->W2R, nn->st);
     if (cudaStreamSynchronize(nn->st) != cudaSuccess) { dqmc_nn_destroy(nn); return fail(DQMC_ECUDA, "init"); }
