@@ -221,6 +221,64 @@ def fp64_peak_tflops() -> float:
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
+def make_handle(args, rank: int):
+    """The DQMC handle of the selected workload, chains seeded from the
+    reference's -DTEST seeds offset by rank; returns (handle, workload, tuning)."""
+    import sunhubbardmy_b200 as sb
+    if args.workload == "config4":
+        p4 = sb.DqmcParams.make(**CONFIG4)
+        nw = args.chains if args.chains_set else 64
+        return sb.Dqmc(p4, n_chains=nw, seeds=[test_seed(rank * nw + c) for c in range(nw)]), WORKLOAD4, None
+    if args.workload == "config3":
+        from sunhubbardmy_b200.autotune import batched
+        groups = [(sb.DqmcParams.make(**kw), n) for kw, n in CONFIG3]
+        g, tune_report = batched(groups, tune=True, seed0=rank * sum(n for _, n in CONFIG3))
+        return g, WORKLOAD3, tune_report
+    p0 = sb.DqmcParams.make(**CONFIG)
+    g = sb.Dqmc(p0, n_chains=args.chains, seeds=[test_seed(rank * args.chains + c) for c in range(args.chains)])
+    return g, WORKLOAD, None
+
+
+def profile_arm(args) -> None:
+    """Single-kernel runs for profiling on one GPU, after sweep_start.
+
+    --profile 2,1,0 launches each named operation of dqmc_gpu_time_op once
+    untimed and --reps times timed, in the given order (finite T: 0 delayed
+    update of one slice, 1 stabilisation step, 2 Green's function, 3 / 5 one
+    slice of propagation of G from the left / right, 4 measurement;
+    projective: 0 one bond family of updates, 1 tall QR, 2 (UL UR)^-1 and G,
+    3 / 5 one slice of propagation of UR / UL^T, 4 measurement) and prints the
+    per-launch milliseconds.  --profile sweep runs one full sweep with
+    measurement.  --profile nn (effective action of the learned workload) runs
+    one forward and one training step of 8 random fields."""
+    import numpy as np
+    import torch
+    torch.cuda.set_device(0)
+    if args.profile == "nn":
+        from sunhubbardmy_b200.learned import EffectiveAction
+        import sunhubbardmy_b200 as sb
+        p = sb.DqmcParams.make(**CONFIG5)
+        nn = EffectiveAction(p.ltrot, p.l1, max_batch=8)
+        rng = np.random.default_rng(0)
+        f = rng.choice(np.array([-1, 1], np.int8), size=(8, p.ltrot, p.l1, p.l1))
+        S = nn.forward(f)
+        loss = nn.train_step(f, rng.standard_normal(8), 1e-3)
+        print(json.dumps({"profile": "nn", "S0": float(S[0]), "loss": float(loss)}), flush=True)
+        return
+    g, workload, _ = make_handle(args, 0)
+    g.sweep_start()
+    if args.profile == "sweep":
+        g.obser_init()
+        ms = g.sweeps(1, True)
+        print(json.dumps({"profile": "sweep", "workload": workload, "chains": g.n_chains, "ms": ms}), flush=True)
+    else:
+        ops = [int(x) for x in args.profile.split(",")]
+        out = {str(op): g.time_op(op, args.reps) for op in ops}
+        print(json.dumps({"profile": "ops", "workload": workload, "chains": g.n_chains, "reps": args.reps,
+                          "ms_per_launch": out}), flush=True)
+    g.close()
+
+
 def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
     import numpy as np
     import torch
@@ -232,21 +290,7 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    tune_report = None
-    if args.workload == "config4":
-        p4 = sb.DqmcParams.make(**CONFIG4)
-        nw = args.chains if args.chains_set else 64
-        g = sb.Dqmc(p4, n_chains=nw, seeds=[test_seed(rank * nw + c) for c in range(nw)])
-        workload = WORKLOAD4
-    elif args.workload == "config3":
-        from sunhubbardmy_b200.autotune import batched
-        groups = [(sb.DqmcParams.make(**kw), n) for kw, n in CONFIG3]
-        g, tune_report = batched(groups, tune=True, seed0=rank * sum(n for _, n in CONFIG3))
-        workload = WORKLOAD3
-    else:
-        p0 = sb.DqmcParams.make(**CONFIG)
-        g = sb.Dqmc(p0, n_chains=args.chains, seeds=[test_seed(rank * args.chains + c) for c in range(args.chains)])
-        workload = WORKLOAD
+    g, workload, tune_report = make_handle(args, rank)
     C = g.n_chains
     p = g.params[0]
     lt = p.ltrot
@@ -362,6 +406,15 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
                     "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (FP64 tensor)"}
         roof["kernel_ms_per_launch"] = {names[k]: ops[k] for k in ops}
         roof["sweep_share"] = {names[k]: share[k] / total for k in ops}
+        # the delayed update's rank-k flush GEMMs: 8 N^2 real flop per accepted
+        # site (G += a b^T), per slice a_c N_c accepts in chain c; divided by
+        # the whole update kernel's time (the sequential accept walk included)
+        acc_c = np.array([g.diag(c)["accepted"] / max(1.0, g.diag(c)["proposed"]) for c in range(C)])
+        fl_u = 8.0 * float((acc_c * Ns ** 3).sum())
+        ach_u = fl_u / (ops[0] * 1e-3) / 1e12
+        roof["update_gemm"] = {"kernel": "k_update_delay", "bound": "tensor", "achieved": ach_u, "peak": fp64,
+                               "unit": "TFLOP/s", "frac": ach_u / fp64, "algorithmic_flops_per_launch": fl_u,
+                               "note": "flush GEMM flops (8 N^2 per accepted site) over the whole update kernel time"}
         trf = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(trf):
             tr = json.load(open(trf)).get(roof["kernel"])
@@ -590,6 +643,9 @@ def main():
     ap.add_argument("--lr", type=float, default=3e-4, help="config5: Adam learning rate")
     ap.add_argument("--ess", type=int, default=0, help="extra sweeps for the ESS/s of double occupancy")
     ap.add_argument("--ess-warmup", type=int, default=20, help="equilibration sweeps before the ESS series")
+    ap.add_argument("--profile", default=None,
+                    help="single-kernel runs for profiling: comma-separated time_op ids, 'sweep' or 'nn'")
+    ap.add_argument("--reps", type=int, default=1, help="--profile: timed launches per operation")
     args = ap.parse_args()
     args.chains_set = args.chains is not None
     if args.chains is None:
@@ -599,6 +655,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         reference_arm(args, rank)
+        return
+    if args.profile:
+        profile_arm(args)
         return
     if args.workload == "config5":
         if rank == 0:

@@ -769,6 +769,9 @@ struct dqmc_handle {
     int* rec_count = nullptr;
     // global block moves
     int blocks = 0;
+    // register-resident FFT propagation (square l x l lattice, one site per
+    // cell, l = 4, 8, 16, the same size in every parameter set), else 0
+    int fft_L = 0, maxNe = 0;
     int* d_org = nullptr;        // [nch][3]
     double* d_u = nullptr;       // [nch][2]
     double* d_S = nullptr;       // [nch][2]
@@ -843,6 +846,14 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
         if ((rc = upload_model(*m))) { dqmc_gpu_destroy(h); return rc; }
         h->maxN = std::max(h->maxN, m->N);
         h->nnf_max = std::max(h->nnf_max, m->nn_nf);
+        h->maxNe = std::max(h->maxNe, m->p.ne);
+    }
+    {
+        const dqmc_params& p0 = h->models[0]->p;
+        int L = p0.l1;
+        bool ok = p0.kinetic == DQMC_KIN_FFT && p0.l1 == p0.l2 && (L == 4 || L == 8 || L == 16);
+        for (HostModel* m : h->models) ok = ok && m->N == L * L && m->p.l1 == L && m->p.l2 == L;
+        h->fft_L = ok ? L : 0;
     }
     if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) { dqmc_gpu_destroy(h); return fail(DQMC_ECUDA, "stream"); }
     cudaEventCreate(&h->ev0);
@@ -985,7 +996,10 @@ static void prog_v(const HostModel& m, PropProg& p, int which, int nt) {
 // per handle for a given lattice kind)
 static int launch_prog(dqmc_handle* h, int mat_id, const PropProg& prog, int right) {
     if (prog.n == 0) return DQMC_OK;
-    launch_prop(h->d_chains, h->nch, h->maxN, mat_id, prog, right, h->ctas_per_chain, h->st);
+    if (h->fft_L && prop_fft_eligible(prog))
+        launch_prop_fft(h->d_chains, h->nch, h->fft_L, h->maxN, mat_id, prog, right, right, 0, h->st);
+    else
+        launch_prop(h->d_chains, h->nch, h->maxN, mat_id, prog, right, h->ctas_per_chain, h->st);
     return DQMC_OK;
 }
 
@@ -1082,8 +1096,15 @@ struct ProjPass {
 };
 
 static void pflush(dqmc_handle* h, ProjPass& pp) {
-    if (pp.r.n) launch_prop_tall(h->d_chains, h->nch, h->maxN, PMAT_UR, pp.r, 0, h->ctas_per_chain, h->st);
-    if (pp.l.n) launch_prop_tall(h->d_chains, h->nch, h->maxN, PMAT_ULT, pp.l, 1, h->ctas_per_chain, h->st);
+    for (int side = 0; side < 2; ++side) {
+        const PropProg& pr = side ? pp.l : pp.r;
+        const int mat = side ? PMAT_ULT : PMAT_UR;
+        if (!pr.n) continue;
+        if (h->fft_L && prop_fft_eligible(pr))
+            launch_prop_fft(h->d_chains, h->nch, h->fft_L, h->maxNe, mat, pr, 0, side, 1, h->st);
+        else
+            launch_prop_tall(h->d_chains, h->nch, h->maxN, mat, pr, side, h->ctas_per_chain, h->st);
+    }
     pp.r.n = 0; pp.l.n = 0;
 }
 static void padd(dqmc_handle* h, ProjPass& pp, PropProg& p, int kind, int which, int nf, int nt) {

@@ -14,6 +14,7 @@
 // of the matrix per side: the pass is HBM/L2-bandwidth bound.
 #include "chain_access.cuh"
 #include "kernels.h"
+#include <cmath>
 
 // One operator applied to `nv` vectors held in shared memory (vector v at
 // S + v*vs, element stride 1).  right = 0: vectors are columns and the operator
@@ -169,6 +170,176 @@ __global__ void __launch_bounds__(256, 2) k_prop_rows(const ChainDev* __restrict
             X[MIDX(r0 + r, j, N)] = sm[r * vs + j];
         }
         __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// FFT kinetic term with register-resident vectors.  For a square l x l lattice
+// with one site per cell (l = 4, 8, 16; site i = j1 + l j2), a group of l
+// threads owns one vector: thread g holds the dim-2 line j1 = g (l values) in
+// registers.  A PK_FFT op is   dim-2 DFT -> transpose (shared memory, within
+// the warp) -> dim-1 DFT -> x exph0k(k) -> inverse dim-1 -> transpose back ->
+// inverse dim-2, and a PK_DIAG op scales the registers by the HS factor of its
+// sites, so a whole program (an nwrap-slice B product included) costs one read
+// and one write of the matrix and two shared-memory transposes per FFT op.
+// Columns (rows = 0) are loaded with consecutive threads on consecutive sites;
+// rows (rows = 1) with the two rows of a warp on adjacent addresses.
+// ---------------------------------------------------------------------------
+
+// x * w with w = exp(-SG 2 pi i m / 16) (SG = +1: forward sign, -1: backward),
+// the trivial angles folded at compile time; c1 = cos(pi/8), s1 = sin(pi/8),
+// h = cos(pi/4)
+template <int SG>
+DQ_DEV double2 tw_mul(int m, double2 x, double c1, double s1, double h) {
+    double wr, wi;   // forward twiddle exp(-2 pi i m / 16)
+    switch (m) {
+    case 0: return x;
+    case 4: return SG > 0 ? cmk(x.y, -x.x) : cmk(-x.y, x.x);
+    case 2: return SG > 0 ? cmk(h * (x.x + x.y), h * (x.y - x.x)) : cmk(h * (x.x - x.y), h * (x.y + x.x));
+    case 6: return SG > 0 ? cmk(h * (x.y - x.x), -h * (x.x + x.y)) : cmk(-h * (x.x + x.y), h * (x.x - x.y));
+    case 1: wr = c1; wi = -s1; break;
+    case 3: wr = s1; wi = -c1; break;
+    case 5: wr = -s1; wi = -c1; break;
+    default: wr = -c1; wi = -s1; break;   // 7
+    }
+    if (SG < 0) wi = -wi;
+    return cmk(wr * x.x - wi * x.y, wr * x.y + wi * x.x);
+}
+
+// unnormalised radix-2 DFT of n <= 16 values in registers, natural order in
+// and out; SG = +1: exp(-2 pi i jk/n), SG = -1: exp(+2 pi i jk/n)
+template <int n>
+DQ_DEV constexpr int bit_reverse(int i) {
+    int j = 0;
+    for (int b = 1; b < n; b <<= 1, i >>= 1) j = (j << 1) | (i & 1);
+    return j;
+}
+
+// one radix-2 stage of butterflies of length LEN over n registers
+template <int n, int LEN, int SG>
+DQ_DEV void fft_stage(double2 (&r)[n], double c1, double s1, double h) {
+    constexpr int half = LEN / 2;
+#pragma unroll
+    for (int s0 = 0; s0 < n; s0 += LEN)
+#pragma unroll
+        for (int k = 0; k < half; ++k) {
+            double2 u = r[s0 + k], v = tw_mul<SG>(k * (16 / LEN), r[s0 + k + half], c1, s1, h);
+            r[s0 + k] = cadd(u, v);
+            r[s0 + k + half] = csub(u, v);
+        }
+}
+
+template <int n, int SG>
+DQ_DEV void fft_reg(double2 (&x)[n], double c1, double s1, double h) {
+    double2 r[n];
+#pragma unroll
+    for (int i = 0; i < n; ++i) r[bit_reverse<n>(i)] = x[i];
+    fft_stage<n, 2, SG>(r, c1, s1, h);
+    if constexpr (n >= 4) fft_stage<n, 4, SG>(r, c1, s1, h);
+    if constexpr (n >= 8) fft_stage<n, 8, SG>(r, c1, s1, h);
+    if constexpr (n >= 16) fft_stage<n, 16, SG>(r, c1, s1, h);
+#pragma unroll
+    for (int i = 0; i < n; ++i) x[i] = r[i];
+}
+
+// SG = +1 for the forward sign exp(-2 pi i jk/n)
+template <int L>
+DQ_DEV void fft_dir(double2 (&x)[L], int sg, double c1, double s1, double h) {
+    if (sg > 0) fft_reg<L, 1>(x, c1, s1, h);
+    else fft_reg<L, -1>(x, c1, s1, h);
+}
+
+template <int L>
+__global__ void __launch_bounds__(128, 4) k_prop_fft(const ChainDev* __restrict__ chains, int mat_id, PropProg prog,
+                                                     int rows, int right, int tall, double c1, double s1, double h) {
+    constexpr int VPC = 128 / L;    // vectors per CTA
+    constexpr int LD = L + 1;       // odd row pitch: conflict-free transposes
+    __shared__ double2 tb[VPC * L * LD];
+    const ChainDev& c = chains[blockIdx.y];
+    const ModelDev& md = *c.md;
+    const int N = c.N;
+    const int nvec = (tall && !rows) ? md.ne : N;
+    double2* X = chain_mat(c, mat_id);
+    const int g = threadIdx.x % L, vl = threadIdx.x / L;
+    double2* T = tb + vl * L * LD;
+    // left multiplication: F^-1 D F (forward sign first); right: F D F^-1
+    const int sg = right ? -1 : 1;
+    for (int v0 = blockIdx.x * VPC; v0 < nvec; v0 += gridDim.x * VPC) {
+        const int v = v0 + vl;
+        const bool act = v < nvec;      // uniform over the l threads of a vector
+        double2 x[L];
+#pragma unroll
+        for (int j = 0; j < L; ++j) {
+            const int i = g + L * j;
+            x[j] = !act ? cmk(0, 0) : rows ? X[(size_t)i * N + v] : X[(size_t)v * N + i];
+        }
+        for (int k = 0; k < prog.n; ++k) {
+            const int code = prog.op[k];
+            const int kind = code & 15, which = (code >> 4) & 15, nt = code >> 16;
+            if (kind == PK_DIAG) {
+                const int32_t* cf = c.conf + (size_t)(nt - 1) * N;
+                const double2* bt = (which == PW_INV) ? md.bmat_inv : md.bmat;
+#pragma unroll
+                for (int j = 0; j < L; ++j) {
+                    double2 b = bt[__ldg(&cf[g + L * j]) - 1];
+                    if (which == PW_CONJ) b.y = -b.y;
+                    x[j] = cmul(x[j], b);
+                }
+                continue;
+            }
+            // PK_FFT
+            const double2* d = (which == PW_INV) ? md.exph0kinv : md.exph0k;
+            fft_dir<L>(x, sg, c1, s1, h);                 // dim 2: x[k2] at j1 = g
+#pragma unroll
+            for (int j = 0; j < L; ++j) T[j * LD + g] = x[j];
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < L; ++j) x[j] = T[g * LD + j];   // k2 = g, j1 = j
+            __syncwarp();
+            fft_dir<L>(x, sg, c1, s1, h);                 // dim 1: x[k1] at k2 = g
+#pragma unroll
+            for (int j = 0; j < L; ++j) {
+                double2 dk = __ldg(&d[j + L * g]);
+                if (which == PW_CONJ) dk.y = -dk.y;
+                x[j] = cmul(x[j], dk);
+            }
+            fft_dir<L>(x, -sg, c1, s1, h);                // inverse dim 1
+#pragma unroll
+            for (int j = 0; j < L; ++j) T[g * LD + j] = x[j];
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < L; ++j) x[j] = T[j * LD + g];   // j1 = g, k2 = j
+            __syncwarp();
+            fft_dir<L>(x, -sg, c1, s1, h);                // inverse dim 2
+        }
+        if (act) {
+#pragma unroll
+            for (int j = 0; j < L; ++j) {
+                const int i = g + L * j;
+                if (rows) X[(size_t)i * N + v] = x[j];
+                else X[(size_t)v * N + i] = x[j];
+            }
+        }
+    }
+}
+
+int prop_fft_eligible(const PropProg& prog) {
+    for (int k = 0; k < prog.n; ++k) {
+        const int kind = prog.op[k] & 15;
+        if (kind != PK_FFT && kind != PK_DIAG) return 0;
+    }
+    return prog.n > 0;
+}
+
+void launch_prop_fft(const ChainDev* chains, int nchains, int L, int nvec, int mat_id, const PropProg& prog,
+                     int rows, int right, int tall, cudaStream_t st) {
+    const double c1 = std::cos(M_PI / 8), s1 = std::sin(M_PI / 8), h = std::sqrt(0.5);
+    const int vpc = 128 / L;
+    dim3 grid((nvec + vpc - 1) / vpc, nchains);
+    switch (L) {
+    case 16: k_prop_fft<16><<<grid, 128, 0, st>>>(chains, mat_id, prog, rows, right, tall, c1, s1, h); break;
+    case 8: k_prop_fft<8><<<grid, 128, 0, st>>>(chains, mat_id, prog, rows, right, tall, c1, s1, h); break;
+    default: k_prop_fft<4><<<grid, 128, 0, st>>>(chains, mat_id, prog, rows, right, tall, c1, s1, h); break;
     }
 }
 

@@ -6,6 +6,12 @@
 
 void launch_prop(const ChainDev* chains, int nchains, int maxN, int mat_id, const PropProg& prog,
                  int right, int ctas_per_chain, cudaStream_t st);
+// register-resident FFT pass (square l x l lattice, one site per cell, l = 4, 8, 16) for
+// programs of PK_FFT and PK_DIAG ops only; rows = 1: the vectors are the rows of an
+// N x N matrix, else its columns (nvec of them)
+int prop_fft_eligible(const PropProg& prog);
+void launch_prop_fft(const ChainDev* chains, int nchains, int L, int nvec, int mat_id, const PropProg& prog,
+                     int rows, int right, int tall, cudaStream_t st);
 void launch_sfmt(const ChainDev* chains, int nchains, int slices, cudaStream_t st);
 void launch_sfmt_raw(const ChainDev* chains, int chain, int count, cudaStream_t st);
 void launch_update(const ChainDev* chains, int nchains, int nt, int visit, cudaStream_t st, int forced = 0);

@@ -17,6 +17,13 @@ CASES = {
                            kinetic=0, update=2, hs=0, nwrap=10, nublock=8),
     "sq6_cb_gen4_delay_mu": dict(lattice=1, l1=6, l2=6, beta=1.5, dtau=0.1, rhub=3.0, nflr=2, mu=0.3,
                                  kinetic=0, update=1, hs=1, nwrap=5, nublock=8),
+    # FFT kinetic term on 8 x 8 and 16 x 16 (the register-resident FFT pass)
+    "sq8_fft_exact_delay": dict(lattice=1, l1=8, l2=8, beta=1.0, dtau=0.05, rhub=4.0, nflr=2, mu=0.2,
+                                kinetic=1, update=1, hs=0, nwrap=10, nublock=16),
+    # (U = 2 with mu = 0.3 keeps I + B(beta, 0) of the random start well conditioned
+    # at this size, so G itself is accurate to ~1e-12)
+    "sq16_fft_gen4_delay": dict(lattice=1, l1=16, l2=16, beta=1.0, dtau=0.05, rhub=2.0, nflr=2, mu=0.3,
+                                kinetic=1, update=1, hs=1, nwrap=10, nublock=32),
 }
 
 TEST_SEED0 = 1909706392   # abs((0*1981+2008)*951049)
