@@ -447,6 +447,17 @@ static int upload_model(HostModel& m) {
     if (p.kinetic == DQMC_KIN_FFT) {
         t = to_d2(m.exph0k); if ((rc = upload(m, t, &d.exph0k))) return rc;
         t = to_d2(m.exph0kinv); if ((rc = upload(m, t, &d.exph0kinv))) return rc;
+        if (p.l1 == p.l2) {
+            const int l = p.l1;
+            std::vector<zc> tk(m.exph0k.size()), tki(m.exph0k.size());
+            for (int k1 = 0; k1 < l; ++k1)
+                for (int k2 = 0; k2 < l; ++k2) {
+                    tk[k2 + l * k1] = m.exph0k[k1 + l * k2];
+                    tki[k2 + l * k1] = m.exph0kinv[k1 + l * k2];
+                }
+            t = to_d2(tk); if ((rc = upload(m, t, &d.exph0kT))) return rc;
+            t = to_d2(tki); if ((rc = upload(m, t, &d.exph0kinvT))) return rc;
+        }
         std::vector<zc> w1(p.l1), w2(p.l2);
         for (int k = 0; k < p.l1; ++k) w1[k] = std::exp(zc(0, -2 * M_PI * k / p.l1));
         for (int k = 0; k < p.l2; ++k) w2[k] = std::exp(zc(0, -2 * M_PI * k / p.l2));

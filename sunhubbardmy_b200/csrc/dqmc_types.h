@@ -25,6 +25,8 @@ struct ModelDev {
     const double2* urtm1;
     const double2* exph0k;     // [lq], already divided by lq (FFT normalisation)
     const double2* exph0kinv;
+    const double2* exph0kT;    // the same, index k2 + l1 k1 (l1 == l2): rows on adjacent lanes
+    const double2* exph0kinvT;
     const double2* tw1;        // [l1] exp(-2 pi i k / l1)
     const double2* tw2;        // [l2]
     // measurement tables (0-based)

@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(128, 4) k_prop_fft(const ChainDev* __restrict_
                 continue;
             }
             // PK_FFT
-            const double2* d = (which == PW_INV) ? md.exph0kinv : md.exph0k;
+            const double2* d = (which == PW_INV) ? md.exph0kinvT : md.exph0kT;
             fft_dir<L>(x, sg, c1, s1, h);                 // dim 2: x[k2] at j1 = g
 #pragma unroll
             for (int j = 0; j < L; ++j) T[j * LD + g] = x[j];
@@ -299,7 +299,7 @@ __global__ void __launch_bounds__(128, 4) k_prop_fft(const ChainDev* __restrict_
             fft_dir<L>(x, sg, c1, s1, h);                 // dim 1: x[k1] at k2 = g
 #pragma unroll
             for (int j = 0; j < L; ++j) {
-                double2 dk = __ldg(&d[j + L * g]);
+                double2 dk = __ldg(&d[g + L * j]);       // exph0k(k1 = j, k2 = g)
                 if (which == PW_CONJ) dk.y = -dk.y;
                 x[j] = cmul(x[j], dk);
             }
