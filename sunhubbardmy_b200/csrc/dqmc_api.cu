@@ -894,6 +894,7 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
         const int ne = m->p.ne, nnf = m->nn_nf;
         d.G = (double2*)dalloc(h, NN * z);
         d.Gnew = (double2*)dalloc(h, NN * z);
+        d.GT = (double2*)dalloc(h, NN * z);
         for (int k = 0; k < 6; ++k) d.W[k] = (double2*)dalloc(h, NN * z);
         if (!proj) {
             d.U = (double2*)dalloc(h, (size_t)(nst + 2) * NN * z);
@@ -1139,7 +1140,7 @@ static bool proj_mid(const HostModel& m, int nt) {
 static void proj_measure(dqmc_handle* h) {
     launch_proj_ulr(h->d_chains, h->nch, PMAT_ULRINV, 0, 0, -1, h->st);
     launch_proj_green(h->d_chains, h->nch, PMAT_ULRINV, PMAT_G, h->ctas_per_chain, h->st);
-    launch_measure(h->d_chains, h->nch, h->ctas_per_chain, h->st);
+    launch_measure(h->d_chains, h->nch, h->maxN, h->ctas_per_chain, h->st);
 }
 
 // G of the current (UL, UR) into G, before a stabilisation replaces them
@@ -1314,7 +1315,7 @@ static void enqueue_b0(dqmc_handle* h, int lupdate, int lmeasure) {
     if (lupdate && m.p.rhub != 0.0) launch_sfmt(h->d_chains, h->nch, lt, h->st);
     for (int nt = lt; nt >= 1; --nt) {
         int visit = lt - nt;
-        if (lmeasure) launch_measure(h->d_chains, h->nch, h->ctas_per_chain, h->st);
+        if (lmeasure) launch_measure(h->d_chains, h->nch, h->maxN, h->ctas_per_chain, h->st);
         PropProg pl; pl.n = 0; PropProg pr; pr.n = 0;
         prog_k(m, pl, PW_INV, 0);          // left_backward, nf = 1..nnf
         prog_k(m, pr, PW_FWD, 0);          // right_forward, nf = 1..nnf
@@ -1352,7 +1353,7 @@ static void enqueue_0b(dqmc_handle* h, int lupdate, int lmeasure) {
         prog_k(m, pr, PW_INV, 1);
         launch_prog(h, MAT_G, pl, 0);
         launch_prog(h, MAT_G, pr, 1);
-        if (lmeasure) launch_measure(h->d_chains, h->nch, h->ctas_per_chain, h->st);
+        if (lmeasure) launch_measure(h->d_chains, h->nch, h->maxN, h->ctas_per_chain, h->st);
         if (m.iwrap_nt[nt] > 0) stab_0b(h, m.iwrap_nt[nt], 1);
     }
 }
@@ -1650,7 +1651,7 @@ extern "C" int dqmc_gpu_update(dqmc_handle* h, int nt) {
 
 extern "C" int dqmc_gpu_measure(dqmc_handle* h) {
     if (!h) return fail(DQMC_EINVAL, "null handle");
-    launch_measure(h->d_chains, h->nch, h->ctas_per_chain, h->st);
+    launch_measure(h->d_chains, h->nch, h->maxN, h->ctas_per_chain, h->st);
     CK(cudaStreamSynchronize(h->st));
     CK(cudaGetLastError());
     return DQMC_OK;
@@ -1675,7 +1676,7 @@ extern "C" int dqmc_gpu_time_op(dqmc_handle* h, int op, int reps, double* ms_out
         case 2: launch_green(h->d_chains, h->nch, 1, 0, 0, 0, 0, 0, 0, h->st); break;
         case 3: { PropProg p; p.n = 0; prog_k(m, p, PW_INV, 0); prog_v(m, p, PW_INV, 1); prog_k(m, p, PW_INV, 1);
                   launch_prog(h, MAT_G, p, 0); break; }
-        case 4: launch_measure(h->d_chains, h->nch, h->ctas_per_chain, h->st); break;
+        case 4: launch_measure(h->d_chains, h->nch, h->maxN, h->ctas_per_chain, h->st); break;
         case 5: { PropProg p; p.n = 0; prog_k(m, p, PW_FWD, 0); prog_v(m, p, PW_FWD, 1); prog_k(m, p, PW_FWD, 1);
                   launch_prog(h, MAT_G, p, 1); break; }
         default: break;
@@ -1705,7 +1706,7 @@ extern "C" int dqmc_gpu_time_op(dqmc_handle* h, int op, int reps, double* ms_out
             pflush(h, pp);
             break;
         }
-        case 4: launch_measure(h->d_chains, h->nch, h->ctas_per_chain, h->st); break;
+        case 4: launch_measure(h->d_chains, h->nch, h->maxN, h->ctas_per_chain, h->st); break;
         default: break;
         }
     };
@@ -2203,7 +2204,7 @@ static void enqueue_0b_blocks(dqmc_handle* h, dqmc_nn* nn, int lupdate, int lmea
         prog_k(m, pr, PW_INV, 1);
         launch_prog(h, MAT_G, pl, 0);
         launch_prog(h, MAT_G, pr, 1);
-        if (lmeasure) launch_measure(h->d_chains, h->nch, h->ctas_per_chain, h->st);
+        if (lmeasure) launch_measure(h->d_chains, h->nch, h->maxN, h->ctas_per_chain, h->st);
         if (m.iwrap_nt[nt] > 0) stab_0b(h, m.iwrap_nt[nt], 1);
     }
 }

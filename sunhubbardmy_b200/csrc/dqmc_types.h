@@ -48,6 +48,7 @@ struct ChainDev {
     int N;
     double2* G;                // current equal-time Green's function
     double2* Gnew;             // scratch Green's function
+    double2* GT;               // G transposed (written before each measurement)
     double2* W[6];             // N x N work matrices
     double2* U;                // stack (nst+1) x N x N
     double2* V;

@@ -3,10 +3,12 @@
 // Reference: src/dqmc_measure/equaltime_measure.f90 (equaltime_measure 1-69,
 // zkint, zint_u, zint_v, zqsq, ztsq, ztq, measure_cpcm/spsm/nn/jj/bondcorr/
 // paircorr).  Observables use Gc(i,j) = delta_ij - G(j,i) and are weighted
-// with zphi = sgn/Re(phase) * phase.  The distance-binned correlations are
-// accumulated without atomics: one warp owns one bin (distance d, orbitals
-// a, b), its lanes walk the unit cells j, pairing each with cell i = j + d from
-// a precomputed table (imj(i, j) = d), and a warp reduction closes the bin.
+// with zphi = sgn/Re(phase) * phase.  G^T is written first (a tiled
+// transpose), so that every correlation term reads a column of G or of G^T.
+// The distance-binned correlations are accumulated without atomics: one
+// thread owns one bin (distance d, orbitals a, b) and walks the unit cells j,
+// pairing each with cell i = j + d from a precomputed table (imj(i, j) = d);
+// the threads of consecutive d read consecutive rows of the same columns.
 // The single-number energy terms run on the chain's first CTA.
 //
 // Bin layout per chain (complex): energy[10], cpcm, spsm, nn, pair_onsite
@@ -51,7 +53,10 @@ __global__ void __launch_bounds__(256) k_measure(const ChainDev* __restrict__ ch
         bcell[cc] = cadd(cmul(e, gcf(G, N, i0, inb)), cmul(cconj(e), gcf(G, N, inb, i0)));
     }
     __syncthreads();
-    // ---- distance-binned correlations: one warp per bin, lanes over cells ----
+    // ---- distance-binned correlations: one thread per bin, looping over the
+    // cells j; for fixed j the threads of consecutive distances read G and G^T
+    // down a column, so every access is coalesced and each bin is summed in a
+    // fixed order without atomics ----
     double2* cpcm = bins + 10;
     double2* spsm = cpcm + 4 * lq;
     double2* znn = spsm + 4 * lq;
@@ -60,66 +65,71 @@ __global__ void __launch_bounds__(256) k_measure(const ChainDev* __restrict__ ch
     double2* zbb = zjj + lq;
     double2* pnn = zbb + lq;
     double2* psn = pnn + lq;
+    const double2* GT = c.GT;
     const int nsub = md.nsub;
-    const int lane = tid & 31;
     const int nbin_a = lq * nsub * nsub, nbin = nbin_a + lq;
-    const int gw0 = blockIdx.x * (nth >> 5) + (tid >> 5), gws = gridDim.x * (nth >> 5);
-    for (int bin = gw0; bin < nbin; bin += gws) {
+    for (int bin = blockIdx.x * nth + tid; bin < nbin; bin += gridDim.x * nth) {
         if (bin < nbin_a) {
-            int d = bin % lq, ab = bin / lq, a = ab % nsub, b = ab / nsub;
+            const int d = bin % lq, ab = bin / lq, a = ab % nsub, b = ab / nsub;
+            const int* cp = md.cell_plus + (size_t)d * lq;
             double2 s1 = cmk(0, 0), s2 = cmk(0, 0), s3 = cmk(0, 0), s4 = cmk(0, 0);
-            for (int cj = lane; cj < lq; cj += 32) {
-                int ci = md.cell_plus[d * lq + cj];
-                int i = ci * nsub + a, j = cj * nsub + b;
-                double2 gc = gcf(G, N, i, j), g = gf(G, N, i, j);
+#pragma unroll 4
+            for (int cj = 0; cj < lq; ++cj) {
+                const int i = __ldg(&cp[cj]) * nsub + a, j = cj * nsub + b;
+                const size_t o = (size_t)i + (size_t)N * j;
+                const double2 gt = GT[o], g = G[o];          // G(j,i), G(i,j)
+                const double2 gc = cmk((i == j ? 1.0 : 0.0) - gt.x, -gt.y);
+                const double2 gcg = cmul(gc, g);
                 s1 = cadd(s1, gc);
-                s2 = cfma(gc, g, s2);
-                s3 = cadd(s3, cadd(cmul(gcd[i], gcd[j]), cscale(cmul(gc, g), fn)));
+                s2 = cadd(s2, gcg);
+                s3 = cadd(s3, cadd(cmul(gcd[i], gcd[j]), cscale(gcg, fn)));
                 s4 = cfma(g, g, s4);
             }
-            s1.x = warp_sum(s1.x); s1.y = warp_sum(s1.y); s2.x = warp_sum(s2.x); s2.y = warp_sum(s2.y);
-            s3.x = warp_sum(s3.x); s3.y = warp_sum(s3.y); s4.x = warp_sum(s4.x); s4.y = warp_sum(s4.y);
-            if (lane == 0) {
-                int k = d + lq * (a + 2 * b);
-                cpcm[k] = cfma(s1, zphi, cpcm[k]);
-                spsm[k] = cfma(cscale(s2, fsp), zphi, spsm[k]);
-                znn[k] = cfma(s3, zphi, znn[k]);
-                pons[k] = cfma(s4, zphi, pons[k]);
-            }
+            const int k = d + lq * (a + 2 * b);
+            cpcm[k] = cfma(s1, zphi, cpcm[k]);
+            spsm[k] = cfma(cscale(s2, fsp), zphi, spsm[k]);
+            znn[k] = cfma(s3, zphi, znn[k]);
+            pons[k] = cfma(s4, zphi, pons[k]);
         } else {
-            int d = bin - nbin_a;
+            const int d = bin - nbin_a;
+            const int* cp = md.cell_plus + (size_t)d * lq;
+            // element (r, s) of G is G[r + N s], of G^T (= G(s, r)) GT[r + N s]
+            auto gg = [&](int r, int s_) { return G[(size_t)r + (size_t)N * s_]; };
+            auto gtt = [&](int r, int s_) { return GT[(size_t)r + (size_t)N * s_]; };
+            auto cc = [&](int r, int s_) {            // Gc(r, s) = delta_rs - G(s, r)
+                double2 t = gtt(r, s_);
+                return cmk((r == s_ ? 1.0 : 0.0) - t.x, -t.y);
+            };
             double2 sj = cmk(0, 0), sb = cmk(0, 0), sn = cmk(0, 0), ss = cmk(0, 0);
-            for (int cj = lane; cj < lq; cj += 32) {
-                int ci = md.cell_plus[d * lq + cj];
-                int j0 = hc ? 2 * cj : cj, i0 = hc ? 2 * ci : ci;
-                int jnj = pj[cj], inj = pj[ci], jnb = pb[cj], inb = pb[ci];
-                double2 g00 = gf(G, N, i0, j0), gc00 = gcf(G, N, i0, j0);
+#pragma unroll 2
+            for (int cj = 0; cj < lq; ++cj) {
+                const int ci = __ldg(&cp[cj]);
+                const int j0 = hc ? 2 * cj : cj, i0 = hc ? 2 * ci : ci;
+                const int jnj = pj[cj], inj = pj[ci], jnb = pb[cj], inb = pb[ci];
+                const double2 g00 = gg(i0, j0), gc00 = cc(i0, j0);
                 // current-current, connected part (measure_jj)
-                double2 z3 = cadd(cmul(gcf(G, N, i0, jnj), gf(G, N, inj, j0)), cmul(gcf(G, N, inj, j0), gf(G, N, i0, jnj)));
-                double2 gnn_j = gf(G, N, inj, jnj), gcnn_j = gcf(G, N, inj, jnj);
+                double2 z3 = cadd(cmul(cc(i0, jnj), gg(inj, j0)), cmul(cc(inj, j0), gg(i0, jnj)));
+                const double2 gnn_j = gg(inj, jnj), gcnn_j = cc(inj, jnj);
                 z3 = csub(z3, cadd(cmul(gc00, gnn_j), cmul(gcnn_j, g00)));
                 sj = csub(sj, cadd(cmul(jcell[ci], jcell[cj]), cscale(z3, fn)));
                 // bond-bond (measure_bondcorr)
-                double2 ej = md.expar_nn[j0 * nnf], ei = md.expar_nn[i0 * nnf];
-                double2 gnn_b = (jnb == jnj && inb == inj) ? gnn_j : gf(G, N, inb, jnb);
-                double2 gcnn_b = (jnb == jnj && inb == inj) ? gcnn_j : gcf(G, N, inb, jnb);
-                double2 x = cmul(cmul(ei, ej), cmul(gcf(G, N, i0, jnb), gf(G, N, inb, j0)));
-                x = cadd(x, cmul(cmul(cconj(ei), cconj(ej)), cmul(gcf(G, N, inb, j0), gf(G, N, i0, jnb))));
+                const double2 ej = md.expar_nn[j0 * nnf], ei = md.expar_nn[i0 * nnf];
+                const bool same = (jnb == jnj && inb == inj);
+                const double2 gnn_b = same ? gnn_j : gg(inb, jnb);
+                const double2 gcnn_b = same ? gcnn_j : cc(inb, jnb);
+                double2 x = cmul(cmul(ei, ej), cmul(cc(i0, jnb), gg(inb, j0)));
+                x = cadd(x, cmul(cmul(cconj(ei), cconj(ej)), cmul(cc(inb, j0), gg(i0, jnb))));
                 x = cadd(x, cmul(cmul(ei, cconj(ej)), cmul(gc00, gnn_b)));
                 x = cadd(x, cmul(cmul(cconj(ei), ej), cmul(gcnn_b, g00)));
                 sb = cadd(sb, cadd(cmul(bcell[cj], bcell[ci]), cscale(x, fn)));
                 // pair correlations (measure_paircorr)
                 sn = cfma(g00, gnn_b, sn);
-                ss = cfma(g00, gf(G, N, ps[ci], ps[cj]), ss);
+                ss = cfma(g00, gg(ps[ci], ps[cj]), ss);
             }
-            sj.x = warp_sum(sj.x); sj.y = warp_sum(sj.y); sb.x = warp_sum(sb.x); sb.y = warp_sum(sb.y);
-            sn.x = warp_sum(sn.x); sn.y = warp_sum(sn.y); ss.x = warp_sum(ss.x); ss.y = warp_sum(ss.y);
-            if (lane == 0) {
-                zjj[d] = cfma(sj, zphi, zjj[d]);
-                zbb[d] = cfma(sb, zphi, zbb[d]);
-                pnn[d] = cfma(sn, zphi, pnn[d]);
-                psn[d] = cfma(ss, zphi, psn[d]);
-            }
+            zjj[d] = cfma(sj, zphi, zjj[d]);
+            zbb[d] = cfma(sb, zphi, zbb[d]);
+            pnn[d] = cfma(sn, zphi, pnn[d]);
+            psn[d] = cfma(ss, zphi, psn[d]);
         }
     }
     if (blockIdx.x != 0) return;
@@ -229,7 +239,28 @@ __global__ void k_bins_clear(const ChainDev* __restrict__ chains, int nbins) {
     if (threadIdx.x == 0) c.stats[ST_NOBS] = 0.0;
 }
 
-void launch_measure(const ChainDev* chains, int nchains, int ctas_per_chain, cudaStream_t st) {
+// GT = G^T per chain, 32 x 32 tiles through shared memory (odd pitch)
+__global__ void __launch_bounds__(256) k_transpose_g(const ChainDev* __restrict__ chains) {
+    __shared__ double2 t[32][33];
+    const ChainDev& c = chains[blockIdx.z];
+    const int N = c.N;
+    const int r0 = blockIdx.x * 32, s0 = blockIdx.y * 32;
+    if (r0 >= N || s0 >= N) return;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int k = ty; k < 32; k += 8) {
+        const int r = r0 + tx, s_ = s0 + k;
+        if (r < N && s_ < N) t[k][tx] = c.G[(size_t)r + (size_t)N * s_];
+    }
+    __syncthreads();
+    for (int k = ty; k < 32; k += 8) {
+        const int r = s0 + tx, s_ = r0 + k;       // GT(r, s) = G(s, r)
+        if (r < N && s_ < N) c.GT[(size_t)r + (size_t)N * s_] = t[tx][k];
+    }
+}
+
+void launch_measure(const ChainDev* chains, int nchains, int maxN, int ctas_per_chain, cudaStream_t st) {
+    const int nt = (maxN + 31) / 32;
+    k_transpose_g<<<dim3(nt, nt, nchains), 256, 0, st>>>(chains);
     dim3 grid(ctas_per_chain, nchains);
     k_measure<<<grid, 256, 0, st>>>(chains);
 }
