@@ -221,6 +221,44 @@ def fp64_peak_tflops() -> float:
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
+def sweep_roofline(prof: dict, work: dict, names: dict, fp64: float) -> dict:
+    """Roofline of the kernel with the largest share of an event-timed sweep
+    (dqmc_gpu_sweep_profile: an event after every launch group), with every
+    kind's per-launch time, share and fraction of its peak."""
+    hbm = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0) \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
+    total = sum(v[0] for v in prof.values())
+    kinds = {}
+    for k, (ms, n) in prof.items():
+        if n == 0:
+            continue
+        per = ms / n
+        ent = {"kernel": names.get(k, k), "ms_per_launch": per, "launches": n, "sweep_share": ms / total}
+        fl, by = work.get(k, (None, None))
+        if fl is not None:
+            ach = fl / (per * 1e-3) / 1e12
+            ent.update({"bound": "tensor", "achieved": ach, "peak": fp64, "unit": "TFLOP/s", "frac": ach / fp64,
+                        "algorithmic_flops_per_launch": fl})
+        elif by is not None:
+            ach = by / (per * 1e-3) / 1e9
+            ent.update({"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                        "algorithmic_bytes_per_launch": by})
+        kinds[k] = ent
+    dom = max((k for k in kinds if "frac" in kinds[k]), key=lambda k: kinds[k]["sweep_share"])
+    d = kinds[dom]
+    roof = {"kernel": d["kernel"], "bound": d["bound"], "achieved": d["achieved"], "peak": d["peak"],
+            "unit": d["unit"], "frac": d["frac"], "traffic": None,
+            "peak_source": ("measured in this run: cuBLAS DGEMM 8192^3 (FP64 tensor)" if d["bound"] == "tensor"
+                            else "MEASURED_PEAKS.json hbm_gbs"),
+            "timing": "one extra sweep launched kernel by kernel with a CUDA event after each launch group",
+            "kinds": kinds}
+    if "update" in kinds and "frac" in kinds["update"]:
+        roof["update_gemm"] = {k: kinds["update"][k] for k in ("kernel", "achieved", "peak", "unit", "frac")}
+        roof["update_gemm"]["note"] = ("flush GEMM flops (8 N^2 per accepted site) over the whole update "
+                                       "kernel time, sequential accept walk included")
+    return roof
+
+
 def make_handle(args, rank: int):
     """The DQMC handle of the selected workload, chains seeded from the
     reference's -DTEST seeds offset by rank; returns (handle, workload, tuning)."""
@@ -377,44 +415,22 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
         result = proj_roofline_and_line(args, g, p, Ns, ms, value, per_step, world, workload, acc, wrap,
                                         kernels_per_sweep, clk, e2e_s, nconf, nbins)
     elif rank == 0:
-        # roofline of the dominant kernel: per-kernel device times (CUDA events)
-        names = {0: "k_update_delay", 1: "k_stab", 2: "k_green", 3: "k_prop_cols", 4: "k_measure", 5: "k_prop_rows"}
-        ops = {k: g.time_op(k, 3) for k in (1, 2, 3, 5, 4, 0)}
-        nst = p.nst
-        per_sweep = {1: 2 * nst, 2: 2 * nst, 3: 4 * lt + 2 * nst, 5: 4 * lt, 4: 2 * lt, 0: 2 * lt}
-        share = {k: ops[k] * per_sweep[k] for k in ops}
-        total = sum(share.values())
-        dom = max(share, key=share.get)
-        N3 = float((Ns ** 3).sum())        # sum over chains
-        flops = {1: 18.0 + 2.0 / 3.0, 2: 41.0 + 1.0 / 3.0}   # real flops / N^3 per chain
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
-        fp64 = fp64_peak_tflops()
-        if dom in flops:
-            ach = flops[dom] * N3 / (ops[dom] * 1e-3) / 1e12
-            roof = {"kernel": names[dom], "bound": "tensor", "achieved": ach, "peak": fp64, "unit": "TFLOP/s",
-                    "frac": ach / fp64, "traffic": None,
-                    "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (FP64 tensor)"}
-        elif dom in (3, 5):
-            ach = 32.0 * float((Ns ** 2).sum()) / (ops[dom] * 1e-3) / 1e9
-            pk = peaks.get("hbm_gbs", 6650.0)
-            roof = {"kernel": names[dom], "bound": "hbm", "achieved": ach, "peak": pk, "unit": "GB/s",
-                    "frac": ach / pk, "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
-        else:
-            ach = 8.0 * acc * float((Ns ** 3).sum()) / (ops[dom] * 1e-3) / 1e12
-            roof = {"kernel": names[dom], "bound": "tensor", "achieved": ach, "peak": fp64, "unit": "TFLOP/s",
-                    "frac": ach / fp64, "traffic": None,
-                    "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (FP64 tensor)"}
-        roof["kernel_ms_per_launch"] = {names[k]: ops[k] for k in ops}
-        roof["sweep_share"] = {names[k]: share[k] / total for k in ops}
-        # the delayed update's rank-k flush GEMMs: 8 N^2 real flop per accepted
-        # site (G += a b^T), per slice a_c N_c accepts in chain c; divided by
-        # the whole update kernel's time (the sequential accept walk included)
         acc_c = np.array([g.diag(c)["accepted"] / max(1.0, g.diag(c)["proposed"]) for c in range(C)])
-        fl_u = 8.0 * float((acc_c * Ns ** 3).sum())
-        ach_u = fl_u / (ops[0] * 1e-3) / 1e12
-        roof["update_gemm"] = {"kernel": "k_update_delay", "bound": "tensor", "achieved": ach_u, "peak": fp64,
-                               "unit": "TFLOP/s", "frac": ach_u / fp64, "algorithmic_flops_per_launch": fl_u,
-                               "note": "flush GEMM flops (8 N^2 per accepted site) over the whole update kernel time"}
+        fp64 = fp64_peak_tflops()
+        N2, N3 = float((Ns ** 2).sum()), float((Ns ** 3).sum())     # sums over chains
+        work = {   # algorithmic work of one launch group over all chains: (flops, bytes)
+            "update": (8.0 * float((acc_c * Ns ** 3).sum()), None),   # flush GEMMs: 8 N^2 per accepted site
+            "stab": ((18.0 + 2.0 / 3.0) * N3, None),
+            "green": ((41.0 + 1.0 / 3.0) * N3, None),
+            "prop_left": (None, 32.0 * N2), "prop_right": (None, 32.0 * N2), "bprod": (None, 32.0 * N2),
+            "measure": (None, 16.0 * N2),
+        }
+        names = {"update": "k_update_delay", "stab": "k_stab", "green": "k_green",
+                 "prop_left": "k_prop_fft (columns)" if p.kinetic == 1 else "k_prop_cols",
+                 "prop_right": "k_prop_fft (rows)" if p.kinetic == 1 else "k_prop_rows",
+                 "bprod": "B product of the stabilisation", "measure": "k_transpose_g + k_measure",
+                 "other": "copies, wrap checks, SFMT"}
+        roof = sweep_roofline(g.sweep_profile(1, True), work, names, fp64)
         trf = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(trf):
             tr = json.load(open(trf)).get(roof["kernel"])
@@ -481,36 +497,19 @@ def proj_roofline_and_line(args, g, p, Ns, ms, value, per_step, world, workload,
     C = g.n_chains
     lt, nst, ne = p.ltrot, p.nst, p.ne
     R = min(32, p.nublock)
-    names = {0: "k_proj_update", 1: "k_proj_qr", 2: "k_proj_ulr+k_proj_t1+k_proj_gmat", 3: "k_prop_cols (UR)",
-             4: "k_measure", 5: "k_prop_cols (UL^T)"}
-    ops = {k: g.time_op(k, 3) for k in (0, 1, 2, 3, 5, 4)}
-    nnf = 3 if p.lattice == 2 else 4
-    mid = p.obs_mid_len
-    per_sweep = {0: 2 * lt * nnf, 3: 2 * lt * nnf, 5: 2 * lt * nnf, 1: 2 * nst, 2: 4 * nst + 2 * mid, 4: 2 * mid}
-    share = {k: ops[k] * per_sweep[k] for k in ops}
-    total = sum(share.values())
-    dom = max(share, key=share.get)
     fp64 = fp64_peak_tflops()
     N = Ns
     upd = 8.0 * (N * ne ** 2 + N * R * ne + acc * (2 * N * ne ** 2 + N * R * ne))
     qr = 16.0 * (N * ne ** 2 - ne ** 3 / 3.0)
     ulrg = 8.0 * (ne ** 2 * N + (2.0 / 3.0 + 1.0 + 0.5) * ne ** 3 + N * ne ** 2 + N * N * ne)
-    flops = {0: float(upd.sum()), 1: float(qr.sum()), 2: float(ulrg.sum())}
-    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
-    if dom in flops:
-        ach = flops[dom] / (ops[dom] * 1e-3) / 1e12
-        roof = {"kernel": names[dom], "bound": "tensor", "achieved": ach, "peak": fp64, "unit": "TFLOP/s",
-                "frac": ach / fp64, "traffic": None,
-                "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (FP64 tensor)"}
-    else:
-        byts = 32.0 * float((N * ne).sum()) if dom in (3, 5) else 16.0 * float((N * N).sum())
-        ach = byts / (ops[dom] * 1e-3) / 1e9
-        pk = peaks.get("hbm_gbs", 6650.0)
-        roof = {"kernel": names[dom], "bound": "hbm", "achieved": ach, "peak": pk, "unit": "GB/s",
-                "frac": ach / pk, "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
-    roof["kernel_ms_per_launch"] = {names[k]: ops[k] for k in ops}
-    roof["sweep_share"] = {names[k]: share[k] / total for k in ops}
-    roof["algorithmic_flops_per_launch"] = {names[k]: flops[k] for k in flops}
+    work = {"update": (float(upd.sum()), None), "stab": (float(qr.sum()), None), "green": (float(ulrg.sum()), None),
+            "prop_left": (None, 32.0 * float((N * ne).sum())), "prop_right": (None, 32.0 * float((N * ne).sum())),
+            "measure": (None, 16.0 * float((N * N).sum()))}
+    names = {"update": "k_pwin_rg + k_pwin_seq + k_pwin_flush (one bond family)", "stab": "k_proj_qr",
+             "green": "k_proj_ulr + k_proj_t1 + k_proj_gmat", "prop_left": "k_prop_cols (UR)",
+             "prop_right": "k_prop_cols (UL^T)", "measure": "k_transpose_g + k_measure",
+             "other": "copies, wrap checks, SFMT"}
+    roof = sweep_roofline(g.sweep_profile(1, True), work, names, fp64)
     trf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(trf):
         tr = json.load(open(trf)).get(roof["kernel"])

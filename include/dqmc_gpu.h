@@ -182,6 +182,24 @@ int dqmc_gpu_sweep_kernels(dqmc_handle* h);
  * chain state; intended for benchmarks after the timed sweeps. */
 int dqmc_gpu_time_op(dqmc_handle* h, int op, int reps, double* ms_out);
 
+/* Per-kind device time of whole sweeps, the counterpart of the reference's
+ * -DTIMING breakdown (src/dqmc_util.f90:287-369, dqmc_timing).  Runs `nsweeps`
+ * sweeps (b0 + 0b, updates on, measurement if lmeasure) launch by launch, not
+ * as a graph, with a CUDA event after every launch group; the time between
+ * consecutive events is charged to the group's kind.  ms[k] receives the total
+ * device ms and groups[k] the number of launch groups of kind k, for
+ * k < DQMC_PROF_KINDS.  Advances the chains like dqmc_gpu_sweeps. */
+#define DQMC_PROF_UPDATE 0    /* local updates (k_update_delay; projective: one window sequence) */
+#define DQMC_PROF_STAB 1      /* UDV stabilisation step (k_stab; projective: tall QR) */
+#define DQMC_PROF_GREEN 2     /* Green's function (k_green; projective: (UL UR)^-1 and G) */
+#define DQMC_PROF_PROP_L 3    /* propagation from the left (G columns; projective: UR) */
+#define DQMC_PROF_MEASURE 4   /* equal-time measurement (transpose + k_measure) */
+#define DQMC_PROF_PROP_R 5    /* propagation from the right (G rows; projective: UL^T) */
+#define DQMC_PROF_BPROD 6     /* B(tau2, tau1) product of a stabilisation */
+#define DQMC_PROF_OTHER 7     /* copies, wrap checks, random numbers, recording */
+#define DQMC_PROF_KINDS 8
+int dqmc_gpu_sweep_profile(dqmc_handle* h, int nsweeps, int lmeasure, double* ms, int* groups);
+
 /* ---------------------------------------------------------------------------
  * Projective (ground-state) path, params.proj = 1 (src/dqmc_proj_ctrl.f90,
  * src/dqmc_proj_core/).  A walker holds UR = B(tau,0) P (ndim x ne),

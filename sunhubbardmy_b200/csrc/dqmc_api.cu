@@ -783,6 +783,11 @@ struct dqmc_handle {
     // register-resident FFT propagation (square l x l lattice, one site per
     // cell, l = 4, 8, 16, the same size in every parameter set), else 0
     int fft_L = 0, maxNe = 0;
+    // per-launch timing of a sweep (dqmc_gpu_sweep_profile): an event after
+    // every launch group, tagged with its kind
+    int tm_on = 0, tm_n = 0;
+    std::vector<cudaEvent_t> tm_ev;
+    std::vector<int> tm_kind;
     int* d_org = nullptr;        // [nch][3]
     double* d_u = nullptr;       // [nch][2]
     double* d_S = nullptr;       // [nch][2]
@@ -805,6 +810,7 @@ extern "C" int dqmc_gpu_destroy(dqmc_handle* h) {
     for (HostModel* m : h->models) { for (void* p : m->allocs) cudaFree(p); delete m; }
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    for (cudaEvent_t e : h->tm_ev) cudaEventDestroy(e);
     if (h->st) cudaStreamDestroy(h->st);
     delete h;
     return DQMC_OK;
@@ -987,6 +993,24 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
 }
 
 // ---------------------------------------------------------------------------
+// sweep profiling: an event after each launch group while tm_on is set (never
+// during graph capture); the interval since the previous event is charged to
+// the group's kind (DQMC_PROF_*)
+// ---------------------------------------------------------------------------
+static void tmark(dqmc_handle* h, int kind) {
+    if (!h->tm_on) return;
+    if (h->tm_n >= (int)h->tm_ev.size()) {
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess) { h->tm_on = 0; return; }
+        h->tm_ev.push_back(e);
+        h->tm_kind.push_back(0);
+    }
+    cudaEventRecord(h->tm_ev[h->tm_n], h->st);
+    h->tm_kind[h->tm_n] = kind;
+    ++h->tm_n;
+}
+
+// ---------------------------------------------------------------------------
 // propagation programs
 // ---------------------------------------------------------------------------
 static void prog_add(PropProg& p, int kind, int which, int nf, int nt) {
@@ -1070,13 +1094,18 @@ static void stab_0b(dqmc_handle* h, int n, int record) {
     const HostModel& m = *h->models[0];
     int spare = h->nst + 1;
     launch_copy_mat(h->d_chains, h->nch, 2 /*W0*/, MAT_U + (n - 1), 0, h->st);
+    tmark(h, DQMC_PROF_OTHER);
     PropProg p = prog_bmat(m, m.wrap_step[(n - 1) * 2 + 1], m.wrap_step[(n - 1) * 2]);
     launch_prog(h, 2, p, 0);
+    tmark(h, DQMC_PROF_BPROD);
     launch_stab_slots(h->d_chains, h->nch, n - 1, spare, h->st);
+    tmark(h, DQMC_PROF_STAB);
     launch_green(h->d_chains, h->nch, spare, n, 0, 0, 0, 0, 0, h->st);
+    tmark(h, DQMC_PROF_GREEN);
     launch_wrap_check(h->d_chains, h->nch, record, h->st);
     launch_swap_slots(h->d_slotmap, n, spare, h->st);
     maybe_record(h);
+    tmark(h, DQMC_PROF_OTHER);
 }
 
 // one stabilisation of the b0 sweep at stack index n (stablize_b0(n+1))
@@ -1084,13 +1113,18 @@ static void stab_b0(dqmc_handle* h, int n) {
     const HostModel& m = *h->models[0];
     int spare = h->nst + 1;
     launch_copy_mat(h->d_chains, h->nch, 2, MAT_U + (n + 1), 0, h->st);
+    tmark(h, DQMC_PROF_OTHER);
     PropProg p = prog_bmat_hc(m, m.wrap_step[n * 2 + 1], m.wrap_step[n * 2]);
     launch_prog(h, 2, p, 0);
+    tmark(h, DQMC_PROF_BPROD);
     launch_stab_slots(h->d_chains, h->nch, n + 1, spare, h->st);
+    tmark(h, DQMC_PROF_STAB);
     launch_green(h->d_chains, h->nch, n, spare, 0, 0, 0, 0, 0, h->st);
+    tmark(h, DQMC_PROF_GREEN);
     launch_wrap_check(h->d_chains, h->nch, 1, h->st);
     launch_swap_slots(h->d_slotmap, n, spare, h->st);
     maybe_record(h);
+    tmark(h, DQMC_PROF_OTHER);
 }
 
 // ---------------------------------------------------------------------------
@@ -1116,6 +1150,7 @@ static void pflush(dqmc_handle* h, ProjPass& pp) {
             launch_prop_fft(h->d_chains, h->nch, h->fft_L, h->maxNe, mat, pr, 0, side, 1, h->st);
         else
             launch_prop_tall(h->d_chains, h->nch, h->maxN, mat, pr, side, h->ctas_per_chain, h->st);
+        tmark(h, side ? DQMC_PROF_PROP_R : DQMC_PROF_PROP_L);
     }
     pp.r.n = 0; pp.l.n = 0;
 }
@@ -1140,13 +1175,16 @@ static bool proj_mid(const HostModel& m, int nt) {
 static void proj_measure(dqmc_handle* h) {
     launch_proj_ulr(h->d_chains, h->nch, PMAT_ULRINV, 0, 0, -1, h->st);
     launch_proj_green(h->d_chains, h->nch, PMAT_ULRINV, PMAT_G, h->ctas_per_chain, h->st);
+    tmark(h, DQMC_PROF_GREEN);
     launch_measure(h->d_chains, h->nch, h->maxN, h->ctas_per_chain, h->st);
+    tmark(h, DQMC_PROF_MEASURE);
 }
 
 // G of the current (UL, UR) into G, before a stabilisation replaces them
 static void proj_old_green(dqmc_handle* h) {
     launch_proj_ulr(h->d_chains, h->nch, PMAT_W3, 0, 0, -1, h->st);
     launch_proj_green(h->d_chains, h->nch, PMAT_W3, PMAT_G, h->ctas_per_chain, h->st);
+    tmark(h, DQMC_PROF_GREEN);
 }
 
 // dqmc_proj_sweep_0b.f90:133-190 at wrap point n
@@ -1154,11 +1192,15 @@ static void stab_proj_0b(dqmc_handle* h, int n) {
     int nst = h->nst;
     proj_old_green(h);
     launch_tall_copy(h->d_chains, h->nch, PMAT_ULT, PMAT_PST0 + n, h->st);
+    tmark(h, DQMC_PROF_OTHER);
     launch_proj_qr(h->d_chains, h->nch, PMAT_UR, n, n - 1, h->st);
+    tmark(h, DQMC_PROF_STAB);
     launch_proj_ulr(h->d_chains, h->nch, PMAT_ULRINV, 1, n, n == nst ? -1 : n + 1, h->st);
     launch_proj_green(h->d_chains, h->nch, PMAT_ULRINV, PMAT_GNEW, h->ctas_per_chain, h->st);
+    tmark(h, DQMC_PROF_GREEN);
     launch_wrap_check(h->d_chains, h->nch, 1, h->st);
     launch_tall_copy(h->d_chains, h->nch, PMAT_PST0 + n, PMAT_UR, h->st);
+    tmark(h, DQMC_PROF_OTHER);
 }
 
 // dqmc_proj_sweep_b0.f90:128-190 at wrap point n
@@ -1166,11 +1208,15 @@ static void stab_proj_b0(dqmc_handle* h, int n) {
     int nst = h->nst;
     proj_old_green(h);
     launch_tall_copy(h->d_chains, h->nch, PMAT_UR, PMAT_PST0 + n, h->st);
+    tmark(h, DQMC_PROF_OTHER);
     launch_proj_qr(h->d_chains, h->nch, PMAT_ULT, n + 1, (n + 1 == nst) ? -1 : n + 2, h->st);
+    tmark(h, DQMC_PROF_STAB);
     launch_proj_ulr(h->d_chains, h->nch, PMAT_ULRINV, 1, n + 1, n == 0 ? -1 : n, h->st);
     launch_proj_green(h->d_chains, h->nch, PMAT_ULRINV, PMAT_GNEW, h->ctas_per_chain, h->st);
+    tmark(h, DQMC_PROF_GREEN);
     launch_wrap_check(h->d_chains, h->nch, 1, h->st);
     launch_tall_copy(h->d_chains, h->nch, PMAT_PST0 + n, PMAT_ULT, h->st);
+    tmark(h, DQMC_PROF_OTHER);
 }
 
 // Bmat_left_forward on UR over slices nt2..nt1 (src/dqmc_proj_core.f90:61-104)
@@ -1220,6 +1266,7 @@ static void enqueue_proj_b0(dqmc_handle* h, int lupdate, int lmeasure) {
     launch_tall_copy(h->d_chains, h->nch, PMAT_ULT, PMAT_PROJLC, h->st);
     launch_tall_copy(h->d_chains, h->nch, PMAT_PST0 + 0, PMAT_PROJR, h->st);
     if (lupdate && (lu || lv)) launch_sfmt(h->d_chains, h->nch, lt, h->st);
+    tmark(h, DQMC_PROF_OTHER);
     ProjPass pp;
     for (int nt = lt; nt >= 1; --nt) {
         int visit = lt - nt;
@@ -1227,7 +1274,7 @@ static void enqueue_proj_b0(dqmc_handle* h, int lupdate, int lmeasure) {
         pk(h, pp, pp.r, PW_INV, 0);     // h0 left_backward on UR
         pk(h, pp, pp.l, PW_FWD, 0);     // h0 right_forward on UL
         if (lu) {
-            if (lupdate) { pflush(h, pp); proj_update(h, nt, 0, visit, 1, -1); }
+            if (lupdate) { pflush(h, pp); proj_update(h, nt, 0, visit, 1, -1); tmark(h, DQMC_PROF_UPDATE); }
             padd(h, pp, pp.l, PK_DIAG, PW_FWD, 0, nt);
             padd(h, pp, pp.r, PK_DIAG, PW_INV, 0, nt);
         }
@@ -1235,7 +1282,7 @@ static void enqueue_proj_b0(dqmc_handle* h, int lupdate, int lmeasure) {
             for (int nf = nnf; nf >= 1; --nf) {
                 padd(h, pp, pp.l, PK_VMIX, 0, nf, nt);           // right_forward, nflag 2
                 padd(h, pp, pp.r, PK_VMIX, 0, nf, nt);           // left_backward, nflag 2
-                if (lupdate) { pflush(h, pp); proj_update(h, nt, nf, visit, 1, -1); }
+                if (lupdate) { pflush(h, pp); proj_update(h, nt, nf, visit, 1, -1); tmark(h, DQMC_PROF_UPDATE); }
                 padd(h, pp, pp.l, PK_VSCALE, PW_FWD, nf, nt);    // right_forward, nflag 1
                 padd(h, pp, pp.l, PK_VMIX, 0, nf, nt);
                 padd(h, pp, pp.r, PK_VSCALE, PW_INV, nf, nt);    // left_backward, nflag 1
@@ -1256,6 +1303,7 @@ static void enqueue_proj_0b(dqmc_handle* h, int lupdate, int lmeasure) {
     launch_tall_copy(h->d_chains, h->nch, PMAT_UR, PMAT_PROJR, h->st);
     launch_tall_copy(h->d_chains, h->nch, PMAT_PST0 + nst, PMAT_PROJLC, h->st);
     if (lupdate && (lu || lv)) launch_sfmt(h->d_chains, h->nch, lt, h->st);
+    tmark(h, DQMC_PROF_OTHER);
     ProjPass pp;
     for (int nt = 1; nt <= lt; ++nt) {
         int visit = nt - 1;
@@ -1267,14 +1315,14 @@ static void enqueue_proj_0b(dqmc_handle* h, int lupdate, int lmeasure) {
                 padd(h, pp, pp.r, PK_VSCALE, PW_FWD, nf, nt);
                 padd(h, pp, pp.l, PK_VMIX, 0, nf, nt);           // right_backward, nflag 2
                 padd(h, pp, pp.l, PK_VSCALE, PW_INV, nf, nt);
-                if (lupdate) { pflush(h, pp); proj_update(h, nt, nf, visit, 0, -1); }
+                if (lupdate) { pflush(h, pp); proj_update(h, nt, nf, visit, 0, -1); tmark(h, DQMC_PROF_UPDATE); }
                 padd(h, pp, pp.r, PK_VMIX, 0, nf, nt);           // nflag 1
                 padd(h, pp, pp.l, PK_VMIX, 0, nf, nt);
             }
         if (lu) {
             padd(h, pp, pp.r, PK_DIAG, PW_FWD, 0, nt);
             padd(h, pp, pp.l, PK_DIAG, PW_INV, 0, nt);
-            if (lupdate) { pflush(h, pp); proj_update(h, nt, 0, visit, 0, -1); }
+            if (lupdate) { pflush(h, pp); proj_update(h, nt, 0, visit, 0, -1); tmark(h, DQMC_PROF_UPDATE); }
         }
         pk(h, pp, pp.r, PW_FWD, 1);
         pk(h, pp, pp.l, PW_INV, 1);
@@ -1313,22 +1361,27 @@ static void enqueue_b0(dqmc_handle* h, int lupdate, int lmeasure) {
     int lt = h->ltrot;
     launch_stack_identity(h->d_chains, h->nch, h->nst, h->st);
     if (lupdate && m.p.rhub != 0.0) launch_sfmt(h->d_chains, h->nch, lt, h->st);
+    tmark(h, DQMC_PROF_OTHER);
     for (int nt = lt; nt >= 1; --nt) {
         int visit = lt - nt;
-        if (lmeasure) launch_measure(h->d_chains, h->nch, h->maxN, h->ctas_per_chain, h->st);
+        if (lmeasure) { launch_measure(h->d_chains, h->nch, h->maxN, h->ctas_per_chain, h->st); tmark(h, DQMC_PROF_MEASURE); }
         PropProg pl; pl.n = 0; PropProg pr; pr.n = 0;
         prog_k(m, pl, PW_INV, 0);          // left_backward, nf = 1..nnf
         prog_k(m, pr, PW_FWD, 0);          // right_forward, nf = 1..nnf
         launch_prog(h, MAT_G, pl, 0);
+        tmark(h, DQMC_PROF_PROP_L);
         launch_prog(h, MAT_G, pr, 1);
-        if (lupdate && m.p.rhub != 0.0) launch_update(h->d_chains, h->nch, nt, visit, h->st);
+        tmark(h, DQMC_PROF_PROP_R);
+        if (lupdate && m.p.rhub != 0.0) { launch_update(h->d_chains, h->nch, nt, visit, h->st); tmark(h, DQMC_PROF_UPDATE); }
         pl.n = 0; pr.n = 0;
         prog_v(m, pl, PW_INV, nt);         // u left_backward
         prog_k(m, pl, PW_INV, 1);          // h0 left_backward, nf = nnf..1
         prog_v(m, pr, PW_FWD, nt);         // u right_forward
         prog_k(m, pr, PW_FWD, 1);
         launch_prog(h, MAT_G, pl, 0);
+        tmark(h, DQMC_PROF_PROP_L);
         launch_prog(h, MAT_G, pr, 1);
+        tmark(h, DQMC_PROF_PROP_R);
         if ((m.iwrap_nt[nt - 1] > 0 || m.p.nwrap == 1) || nt == 1) stab_b0(h, m.iwrap_nt[nt - 1]);
     }
 }
@@ -1338,6 +1391,7 @@ static void enqueue_0b(dqmc_handle* h, int lupdate, int lmeasure) {
     int lt = h->ltrot;
     launch_stack_identity(h->d_chains, h->nch, 0, h->st);
     if (lupdate && m.p.rhub != 0.0) launch_sfmt(h->d_chains, h->nch, lt, h->st);
+    tmark(h, DQMC_PROF_OTHER);
     for (int nt = 1; nt <= lt; ++nt) {
         int visit = nt - 1;
         PropProg pl; pl.n = 0; PropProg pr; pr.n = 0;
@@ -1346,14 +1400,18 @@ static void enqueue_0b(dqmc_handle* h, int lupdate, int lmeasure) {
         prog_k(m, pr, PW_INV, 0);          // right_backward
         prog_v(m, pr, PW_INV, nt);         // u right_backward
         launch_prog(h, MAT_G, pl, 0);
+        tmark(h, DQMC_PROF_PROP_L);
         launch_prog(h, MAT_G, pr, 1);
-        if (lupdate && m.p.rhub != 0.0) launch_update(h->d_chains, h->nch, nt, visit, h->st);
+        tmark(h, DQMC_PROF_PROP_R);
+        if (lupdate && m.p.rhub != 0.0) { launch_update(h->d_chains, h->nch, nt, visit, h->st); tmark(h, DQMC_PROF_UPDATE); }
         pl.n = 0; pr.n = 0;
         prog_k(m, pl, PW_FWD, 1);
         prog_k(m, pr, PW_INV, 1);
         launch_prog(h, MAT_G, pl, 0);
+        tmark(h, DQMC_PROF_PROP_L);
         launch_prog(h, MAT_G, pr, 1);
-        if (lmeasure) launch_measure(h->d_chains, h->nch, h->maxN, h->ctas_per_chain, h->st);
+        tmark(h, DQMC_PROF_PROP_R);
+        if (lmeasure) { launch_measure(h->d_chains, h->nch, h->maxN, h->ctas_per_chain, h->st); tmark(h, DQMC_PROF_MEASURE); }
         if (m.iwrap_nt[nt] > 0) stab_0b(h, m.iwrap_nt[nt], 1);
     }
 }
@@ -1737,6 +1795,32 @@ extern "C" int dqmc_gpu_time_op(dqmc_handle* h, int op, int reps, double* ms_out
     float ms = 0;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
     *ms_out = ms / reps;
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_sweep_profile(dqmc_handle* h, int nsweeps, int lmeasure, double* ms, int* groups) {
+    if (!h || nsweeps < 1 || !ms || !groups) return fail(DQMC_EINVAL, "invalid arguments");
+    if (!h->started) return fail(DQMC_ESTATE, "sweep_profile before sweep_start");
+    CK(cudaStreamSynchronize(h->st));
+    h->tm_on = 1;
+    h->tm_n = 0;
+    tmark(h, -1);
+    for (int s = 0; s < nsweeps; ++s) {
+        if (h->proj) { enqueue_proj_b0(h, 1, lmeasure); enqueue_proj_0b(h, 1, lmeasure); }
+        else { enqueue_b0(h, 1, lmeasure); enqueue_0b(h, 1, lmeasure); }
+    }
+    const int ok = h->tm_on;
+    h->tm_on = 0;
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaGetLastError());
+    if (!ok) return fail(DQMC_ECUDA, "could not create the profiling events");
+    for (int k = 0; k < DQMC_PROF_KINDS; ++k) { ms[k] = 0.0; groups[k] = 0; }
+    for (int i = 1; i < h->tm_n; ++i) {
+        float dt = 0.f;
+        CK(cudaEventElapsedTime(&dt, h->tm_ev[i - 1], h->tm_ev[i]));
+        const int k = h->tm_kind[i];
+        if (k >= 0 && k < DQMC_PROF_KINDS) { ms[k] += dt; groups[k] += 1; }
+    }
     return DQMC_OK;
 }
 

@@ -129,6 +129,7 @@ SIGNATURES = {
     "dqmc_gpu_last_sweeps_ms": (_d, [_vp]),
     "dqmc_gpu_time_op": (_i, [_vp, _i, _i, _vp]),
     "dqmc_gpu_sweep_kernels": (_i, [_vp]),
+    "dqmc_gpu_sweep_profile": (_i, [_vp, _i, _i, _vp, _vp]),
     "dqmc_gpu_qr_logdet_noalloc": (_i, [_i, _vp, _vp, _vp, _vp]),
     "dqmc_gpu_noalloc_error": (C.c_char_p, []),
     "dqmc_gpu_set_vconf": (_i, [_vp, _i, _vp]),
@@ -423,6 +424,16 @@ class Dqmc:
         ms = C.c_double()
         _check(load_library().dqmc_gpu_time_op(self.h, op, reps, C.byref(ms)), "time_op")
         return ms.value
+
+    PROFILE_KINDS = ("update", "stab", "green", "prop_left", "measure", "prop_right", "bprod", "other")
+
+    def sweep_profile(self, n: int = 1, lmeasure: bool = True) -> dict:
+        """Device time per kind over n sweeps run launch by launch (events
+        after every launch group): {kind: (total ms, launch groups)}."""
+        ms = (C.c_double * 8)()
+        gr = (C.c_int * 8)()
+        _check(load_library().dqmc_gpu_sweep_profile(self.h, n, int(lmeasure), ms, gr), "sweep_profile")
+        return {k: (ms[i], gr[i]) for i, k in enumerate(self.PROFILE_KINDS)}
 
     # diagnostics on the tensor-core kernels
     def set_work(self, which: int, m: np.ndarray, c: int = 0) -> None:
