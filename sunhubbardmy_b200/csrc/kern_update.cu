@@ -5,167 +5,356 @@
 // update).  All three visit the sites in order with two SFMT draws per site
 // and accept with |Re(R phase)/Re(phase)| > r; they differ only in how the
 // accepted rank-1 changes are folded into G.  This kernel runs all of them as
-// a delayed update:
-//   * every round, all threads evaluate the acceptance test of every
-//     remaining site with the current diagonal and phase; the first accepted
-//     site is found with a block reduction, so rejected sites cost one
-//     parallel pass instead of a sequential step each;
-//   * an accepted site s appends a_k = s_k (G(:,s) + A B(s,:)^T) and
-//     b_k = G(s,:)^T + B A(s,:)^T - e_s to the N x k factors (A, B) and
-//     updates the running diagonal;
-//   * after nublock accepted sites (and at the end of the slice) the factors
-//     are flushed, G += A B^T, as one DMMA tensor-core GEMM.
-// The accept/reject sequence equals the reference's in exact arithmetic.
+// one scheme: the accept walk of a window of consecutive sites needs only the
+// window's block of G plus the window's own new columns (the submatrix
+// update's observation), all in shared memory and walked by one warp; the
+// rank-1 changes are carried as delayed columns (A, B), G' = G + A B^T, and
+// flushed after nublock accepted sites as one DMMA tensor-core GEMM (the
+// delayed update's blocking).  The accept/reject sequence equals the
+// reference's in exact arithmetic.
 #include "chain_access.cuh"
 #include "kernels.h"
 #include "zgemm.cuh"
 
 typedef GemmBig UpdGemm;
 
-struct UpdSmem {
-    double red[64];
-    int redi[32];
-    int first;
-    double2 phase;
-    double2 sscl;
-    double acc;
-};
-
-DQ_DEV int block_min_int(int v, int* red) {
-    int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
-    __syncthreads();
-    if (lane == 0) red[w] = v;
-    __syncthreads();
-    int t = (lane < nw) ? red[lane] : 0x7fffffff;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) t = min(t, __shfl_xor_sync(0xffffffffu, t, o));
-    return t;
-}
+#define UPD_NT 256                 // threads per CTA
 
 DQ_DEV double u32_to_stream(uint32_t u) { return ((double)u + 0.5) * (1.0 / 4294967296.0); }
 
-// total ratio of flipping site s (dqmc_update_delay.f90:52-60)
-DQ_DEV double2 flip_ratio(const ModelDev& md, double2 diag_s, int is, int iflip, double2* sscl_out) {
-    int lc = md.lcomp;
-    int k = (is - 1) * (lc - 1) + (iflip - 1);
-    double2 dlt = md.delta[k];
-    double2 ratio1 = cadd(cmul(csub(cmk(1, 0), diag_s), dlt), cmk(1, 0));
-    if (sscl_out) *sscl_out = cdiv(dlt, ratio1);
-    double2 r = ratio1;
-    for (int f = 1; f < md.nflr; ++f) r = cmul(r, ratio1);
-    r = cscale(r, md.gam_ratio[k]);
-    return cmul(r, md.phase_ratio[k]);
+// G += A B^T over the first K columns of the N x nb factors (alpha = beta = 1),
+// every output tile by this CTA: the accumulators start from the G tile (read
+// while the first A and B stages are in flight) and are stored straight back,
+// so the epilogue needs no shared-memory pass and no second read of G.
+DQ_DEV void flush_addto(double2* G, const double2* A, const double2* B, int N, int K, cplx* smem) {
+    typedef UpdGemm Cfg;
+    constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, FM = Cfg::FM, FN = Cfg::FN;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const bool mathw = warp < Cfg::WM * Cfg::WN;
+    const int wm0 = (warp % Cfg::WM) * Cfg::WTM, wn0 = (warp / Cfg::WM) * Cfg::WTN;
+    const int tm = (N + BM - 1) / BM, ntiles = tm * tm;
+    ZGemmArgs g;
+    g.M = N; g.N = N; g.K = K; g.alpha = cmk(1, 0); g.beta = cmk(1, 0);
+    g.A = A; g.lda = N; g.opA = OP_N; g.B = B; g.ldb = N; g.opB = OP_T; g.C = G; g.ldc = N;
+    cplx* As0 = smem;
+    cplx* Bs0 = smem + Cfg::SA;
+    cplx* As1 = smem + Cfg::SA + Cfg::SB;
+    cplx* Bs1 = smem + 2 * Cfg::SA + Cfg::SB;
+    const int nk = (K + BK - 1) / BK;
+    for (int t = 0; t < ntiles; ++t) {
+        const int m0 = (t % tm) * BM, n0 = (t / tm) * BN;
+        zgemm_load_stage<Cfg>(g, m0, n0, 0, As0, Bs0, tid, nthr);
+        cp_async_commit();
+        double accr[FM][FN][2], acci[FM][FN][2];
+#pragma unroll
+        for (int a = 0; a < FM; ++a)
+#pragma unroll
+            for (int b = 0; b < FN; ++b) {
+                const int m = m0 + wm0 + a * 8 + (lane >> 2), n = n0 + wn0 + b * 8 + (lane & 3) * 2;
+                double2 c0 = cmk(0, 0), c1 = cmk(0, 0);
+                if (mathw && m < N && n < N) c0 = G[MIDX(m, n, N)];
+                if (mathw && m < N && n + 1 < N) c1 = G[MIDX(m, n + 1, N)];
+                accr[a][b][0] = c0.x; acci[a][b][0] = c0.y;
+                accr[a][b][1] = c1.x; acci[a][b][1] = c1.y;
+            }
+        for (int kt = 0; kt < nk; ++kt) {
+            cplx* As = (kt & 1) ? As1 : As0;
+            cplx* Bs = (kt & 1) ? Bs1 : Bs0;
+            if (kt + 1 < nk) {
+                zgemm_load_stage<Cfg>(g, m0, n0, (kt + 1) * BK, (kt & 1) ? As0 : As1, (kt & 1) ? Bs0 : Bs1, tid, nthr);
+                cp_async_commit();
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncthreads();
+            if (mathw) {
+#pragma unroll
+                for (int kk = 0; kk < BK; kk += 4) {
+                    const int kr = kk + (lane & 3);
+                    double ar[FM], ai[FM], ain[FM], br[FN], bi[FN];
+#pragma unroll
+                    for (int a = 0; a < FM; ++a) {
+                        cplx v = As[kr * Cfg::LDA + wm0 + a * 8 + (lane >> 2)];
+                        ar[a] = v.x; ai[a] = v.y; ain[a] = -v.y;
+                    }
+#pragma unroll
+                    for (int b = 0; b < FN; ++b) {
+                        cplx v = Bs[kr * Cfg::LDB + wn0 + b * 8 + (lane >> 2)];
+                        br[b] = v.x; bi[b] = v.y;
+                    }
+#pragma unroll
+                    for (int a = 0; a < FM; ++a)
+#pragma unroll
+                        for (int b = 0; b < FN; ++b) dmma(accr[a][b][0], accr[a][b][1], ar[a], br[b]);
+#pragma unroll
+                    for (int a = 0; a < FM; ++a)
+#pragma unroll
+                        for (int b = 0; b < FN; ++b) dmma(acci[a][b][0], acci[a][b][1], ar[a], bi[b]);
+#pragma unroll
+                    for (int a = 0; a < FM; ++a)
+#pragma unroll
+                        for (int b = 0; b < FN; ++b) dmma(accr[a][b][0], accr[a][b][1], ain[a], bi[b]);
+#pragma unroll
+                    for (int a = 0; a < FM; ++a)
+#pragma unroll
+                        for (int b = 0; b < FN; ++b) dmma(acci[a][b][0], acci[a][b][1], ai[a], br[b]);
+                }
+            }
+            __syncthreads();
+        }
+        if (mathw) {
+#pragma unroll
+            for (int a = 0; a < FM; ++a)
+#pragma unroll
+                for (int b = 0; b < FN; ++b) {
+                    const int m = m0 + wm0 + a * 8 + (lane >> 2), n = n0 + wn0 + b * 8 + (lane & 3) * 2;
+                    if (m < N && n < N) G[MIDX(m, n, N)] = cmk(accr[a][b][0], acci[a][b][0]);
+                    if (m < N && n + 1 < N) G[MIDX(m, n + 1, N)] = cmk(accr[a][b][1], acci[a][b][1]);
+                }
+        }
+    }
+    __syncthreads();
 }
 
+// Window of UPD_L consecutive sites, walked by warp 0 (lane p owns site
+// w0 + p).  Its state overlays the GEMM staging buffer, which is only used by
+// the flush after the window has been closed.
+#define UPD_L 32
+#define UPD_LP (UPD_L + 1)       // odd pitch: rows and columns of gW are both conflict-free
+#define UPD_CH 8                 // window columns extended to all rows per pass
+struct UpdWin {
+    double2 gW[UPD_L * UPD_LP];  // G'(w0 + p, w0 + q) at gW[q * UPD_LP + p], G' = G + A B^T
+    double2 aW[UPD_L][UPD_L];    // [m][p]: window row p of the window's m-th new column of A
+    double2 bW[UPD_L][UPD_L];    // the same for B
+    double2 sg[UPD_L];           // scale of the m-th accepted flip (delta / ratio)
+    int pm[UPD_L];               // window position of the m-th accepted site
+    int r, wend;                 // accepted sites; sites the walk consumed
+};
+static_assert(sizeof(UpdWin) % 16 == 0, "window state alignment");
+// the window state plus the staged rows (2 UPD_CH nb <= 2 UPD_CH 64 values) fit the staging buffer
+static_assert(sizeof(UpdWin) + 2 * UPD_CH * 64 * sizeof(double2) <= UpdGemm::SMEM_ELEMS * sizeof(double2),
+              "window state must fit the staging buffer");
+
+// One CTA per chain; the slice's sites are visited in windows of UPD_L:
+//   1. the window block of the current G' = G + A B^T (A, B: the k delayed
+//      columns since the last flush) is formed in shared memory;
+//   2. warp 0 walks the window: lane p tests site w0 + p against its running
+//      diagonal, the first passing lane (a ballot) is accepted, every lane
+//      updates the phase identically and appends its row of the new window
+//      columns (a = s (G'(:,f) + Aw Bw(f,:)^T), b = G'(f,:)^T + Bw Aw(f,:)^T - e_f
+//      restricted to the window) -- no block barrier per accepted site;
+//   3. the whole CTA extends A and B by the window's columns on all N rows;
+//   4. after nublock delayed columns (and at the end of the slice) the
+//      factors are flushed, G += A B^T, on the FP64 tensor pipe.
+// A window also ends at the accepted site that fills the nublock columns.
+//
 // forced = 1: the global block move's forced flips of slice nt (sites with
 // blk[i] != 0 go to the next field value, no random test, chains whose block
 // did not pass the first stage do nothing); the log of the product of the
 // flips' ratios is accumulated in stats[ST_BLK_LR_*].
-__global__ void __launch_bounds__(256) k_update_delay(const ChainDev* __restrict__ chains, int nt, int visit, int forced) {
+__global__ void __launch_bounds__(UPD_NT, 2) k_update_delay(const ChainDev* __restrict__ chains, int nt, int visit, int forced) {
     extern __shared__ double2 dsm[];
-    const ChainDev c = chains[blockIdx.x];
+    const ChainDev& c = chains[blockIdx.x];
     const ModelDev& md = *c.md;
-    const int N = c.N, nb = md.nublock, lc = md.lcomp;
+    const int N = c.N, nb = md.nublock, lc = md.lcomp, nflr = md.nflr;
     if (forced && c.blk[N] == 0) return;
-    const int tid = threadIdx.x, nth = blockDim.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nth = blockDim.x;
     cplx* gsm = dsm;                                   // GEMM staging
-    double2* diag = dsm + UpdGemm::SMEM_ELEMS;         // N
-    double2* arow = diag + N;                          // nb
-    double2* brow = arow + nb;                         // nb
-    UpdSmem* S = (UpdSmem*)(brow + nb);
+    UpdWin* W = (UpdWin*)dsm;                          // window state (same memory)
     int32_t* cf = c.conf + (size_t)(nt - 1) * N;
     const uint32_t* rw = c.rnd + (size_t)visit * 2 * N;
     double2* G = c.G;
+    double2* A = c.A;
+    double2* B = c.B;
 
-    for (int i = tid; i < N; i += nth) diag[i] = G[MIDX(i, i, N)];
-    if (tid == 0) {
-        S->phase = cmk(c.stats[ST_PHASE_RE], c.stats[ST_PHASE_IM]);
-        S->acc = 0.0;
-    }
-    __syncthreads();
+    // walk state, kept by warp 0
+    double2 ph = cmk(c.stats[ST_PHASE_RE], c.stats[ST_PHASE_IM]);
+    double acc = 0.0, lr_re = 0.0, lr_im = 0.0;
+    if (forced && tid == 0) { lr_re = c.stats[ST_BLK_LR_RE]; lr_im = c.stats[ST_BLK_LR_IM]; }
 
-    int ik = 0, s = 0;
+    int k = 0, s = 0;
     while (s < N) {
-        // parallel acceptance test of all remaining sites
-        const double2 ph = S->phase;
-        int myfirst = N;
-        for (int j = s + tid; j < N; j += nth) {
-            if (forced) {
-                if (c.blk[j]) { myfirst = j; break; }
-                continue;
+        const int w0 = s, L = min(UPD_L, N - w0);
+        // 1. window block of G': thread (p, g) forms rows p of the columns
+        //    q = g + 8 u, so each A(w0 + p, m) is loaded once for four products
+        {
+            const int p = tid % UPD_L, g = tid / UPD_L;     // 8 column groups
+            double2 v[UPD_L / 8];
+#pragma unroll
+            for (int u = 0; u < UPD_L / 8; ++u) {
+                const int q = g + 8 * u;
+                v[u] = (p < L && q < L) ? G[MIDX(w0 + p, w0 + q, N)] : cmk(0, 0);
             }
-            int is = cf[j];
-            int iflip = (int)ceil(u32_to_stream(rw[2 * j]) * (lc - 1));
-            double2 rt = flip_ratio(md, diag[j], is, iflip, nullptr);
-            double rre = cmul(rt, ph).x / ph.x;
-            double rabs = fabs(rre);
-            if (rabs > u32_to_stream(rw[2 * j + 1])) { myfirst = j; break; }
-        }
-        int first = block_min_int(myfirst, S->redi);
-        if (first >= N) break;
-        // accept site `first`
-        if (tid == 0) {
-            int is = cf[first];
-            int iflip = forced ? 1 : (int)ceil(u32_to_stream(rw[2 * first]) * (lc - 1));
-            int isp = (is + iflip - 1) % lc + 1;
-            double2 sscl;
-            double2 rt = flip_ratio(md, diag[first], is, iflip, &sscl);
-            double w = sqrt(cmulc(rt, rt).x);
-            S->phase = cscale(cmul(S->phase, rt), 1.0 / w);
-            S->sscl = sscl;
-            S->acc += 1.0;
-            if (forced) {
-                double2 l = clog_(rt);
-                c.stats[ST_BLK_LR_RE] += l.x;
-                c.stats[ST_BLK_LR_IM] += l.y;
+            if (p < L) {
+#pragma unroll 4
+                for (int m = 0; m < k; ++m) {
+                    const double2 a = A[MIDX(w0 + p, m, N)];
+#pragma unroll
+                    for (int u = 0; u < UPD_L / 8; ++u) {
+                        const int q = g + 8 * u;
+                        if (q < L) v[u] = cfma(a, B[MIDX(w0 + q, m, N)], v[u]);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < UPD_L / 8; ++u) {
+                    const int q = g + 8 * u;
+                    if (q < L) W->gW[q * UPD_LP + p] = v[u];
+                }
             }
-            cf[first] = isp;
-        }
-        for (int m = tid; m < ik; m += nth) {
-            arow[m] = c.A[MIDX(first, m, N)];
-            brow[m] = c.B[MIDX(first, m, N)];
         }
         __syncthreads();
-        const double2 sscl = S->sscl;
-        for (int i = tid; i < N; i += nth) {
-            double2 a = G[MIDX(i, first, N)];
-            double2 b = G[MIDX(first, i, N)];
-            for (int m = 0; m < ik; ++m) {
-                a = cfma(brow[m], c.A[MIDX(i, m, N)], a);
-                b = cfma(arow[m], c.B[MIDX(i, m, N)], b);
+        // 2. walk (dqmc_update_delay.f90:52-60 per site)
+        if (warp == 0) {
+            const int p = lane, j = w0 + p;
+            bool cand = false;
+            double2 dl = cmk(0, 0), phr = cmk(0, 0), dW = cmk(0, 0);
+            double gam = 0.0, thr = 0.0;
+            int nvv = 0;
+            if (p < L) {
+                const int is = cf[j];
+                const int iflip = forced ? 1 : (int)ceil(u32_to_stream(rw[2 * j]) * (lc - 1));
+                const int kk = (is - 1) * (lc - 1) + (iflip - 1);
+                dl = md.delta[kk];
+                gam = md.gam_ratio[kk];
+                phr = md.phase_ratio[kk];
+                thr = forced ? 0.0 : u32_to_stream(rw[2 * j + 1]);
+                nvv = (is + iflip - 1) % lc + 1;
+                cand = !forced || c.blk[j] != 0;
+                dW = W->gW[p * UPD_LP + p];
             }
-            a = cmul(a, sscl);
-            if (i == first) b.x -= 1.0;
-            c.A[MIDX(i, ik, N)] = a;
-            c.B[MIDX(i, ik, N)] = b;
-            diag[i] = cfma(a, b, diag[i]);
+            int r = 0, pc = 0, wend = L;
+            while (pc < L) {
+                bool pass = false;
+                double2 rt = cmk(0, 0), sscl = cmk(0, 0);
+                if (cand && p >= pc) {
+                    const double2 ratio1 = cadd(cmul(csub(cmk(1, 0), dW), dl), cmk(1, 0));
+                    double2 rr = ratio1;
+                    for (int f = 1; f < nflr; ++f) rr = cmul(rr, ratio1);
+                    rr = cscale(rr, gam);
+                    rt = cmul(rr, phr);
+                    pass = forced ? true : fabs(cmul(rt, ph).x / ph.x) > thr;
+                    if (pass) sscl = cdiv(dl, ratio1);
+                }
+                const unsigned bal = __ballot_sync(0xffffffffu, pass);
+                if (bal == 0) break;
+                const int pf = __ffs(bal) - 1;
+                rt.x = __shfl_sync(0xffffffffu, rt.x, pf);
+                rt.y = __shfl_sync(0xffffffffu, rt.y, pf);
+                sscl.x = __shfl_sync(0xffffffffu, sscl.x, pf);
+                sscl.y = __shfl_sync(0xffffffffu, sscl.y, pf);
+                const double w = sqrt(cmulc(rt, rt).x);
+                ph = cscale(cmul(ph, rt), 1.0 / w);
+                if (lane == 0) {
+                    acc += 1.0;
+                    if (forced) {
+                        const double2 l = clog_(rt);
+                        lr_re += l.x;
+                        lr_im += l.y;
+                    }
+                    W->sg[r] = sscl;
+                    W->pm[r] = pf;
+                }
+                if (p == pf) { cand = false; cf[j] = nvv; }
+                if (p < L) {
+                    double2 a = W->gW[pf * UPD_LP + p];          // G'(p, f)
+                    double2 b = W->gW[p * UPD_LP + pf];          // G'(f, p)
+                    for (int m = 0; m < r; ++m) {
+                        a = cfma(W->bW[m][pf], W->aW[m][p], a);
+                        b = cfma(W->aW[m][pf], W->bW[m][p], b);
+                    }
+                    a = cmul(a, sscl);
+                    if (p == pf) b.x -= 1.0;
+                    W->aW[r][p] = a;
+                    W->bW[r][p] = b;
+                    dW = cfma(a, b, dW);
+                }
+                ++r;
+                pc = pf + 1;
+                __syncwarp();
+                if (k + r == nb) { wend = pc; break; }
+            }
+            if (lane == 0) { W->r = r; W->wend = wend; }
         }
-        ++ik;
-        s = first + 1;
         __syncthreads();
-        if (ik == nb && s < N) {
-            ZGemmArgs g;
-            g.M = N; g.N = N; g.K = ik; g.alpha = cmk(1, 0); g.beta = cmk(1, 0);
-            g.A = c.A; g.lda = N; g.opA = OP_N; g.B = c.B; g.ldb = N; g.opB = OP_T; g.C = G; g.ldc = N;
-            zgemm_cta<UpdGemm>(g, 0, 1, gsm);
-            for (int i = tid; i < N; i += nth) diag[i] = G[MIDX(i, i, N)];
-            ik = 0;
+        // 3. the window's columns on all rows: column m of this window is
+        //    a = s_m (c1_m + sum_{m' < m} a_m' b_m'(f_m)), b = c2_m + sum_{m' < m} b_m' a_m'(f_m)
+        //    with c1_m = G'(:,f_m), c2_m = G'(f_m,:)^T - e_f; rows of the delayed
+        //    factors at the accepted sites are staged per chunk of UPD_CH columns
+        const int r = W->r, wend = W->wend;
+        double2* As = (double2*)(W + 1);                // [UPD_CH][nb]: A(f_m, :)
+        double2* Bs = As + UPD_CH * nb;                 // [UPD_CH][nb]: B(f_m, :)
+        for (int m0 = 0; m0 < r; m0 += UPD_CH) {
+            const int mc = min(UPD_CH, r - m0);
+            for (int e = tid; e < mc * k; e += nth) {
+                const int mm = e % mc, m2 = e / mc, sm = w0 + W->pm[m0 + mm];
+                As[mm * nb + m2] = A[MIDX(sm, m2, N)];
+                Bs[mm * nb + m2] = B[MIDX(sm, m2, N)];
+            }
+            __syncthreads();
+            for (int i = tid; i < N; i += nth) {
+                double2 c1[UPD_CH], c2[UPD_CH];
+                int pmm[UPD_CH];
+#pragma unroll
+                for (int mm = 0; mm < UPD_CH; ++mm) {
+                    pmm[mm] = W->pm[m0 + min(mm, mc - 1)];
+                    c1[mm] = G[MIDX(i, w0 + pmm[mm], N)];
+                    c2[mm] = G[MIDX(w0 + pmm[mm], i, N)];
+                }
+                // delayed columns since the last flush: G' = G + A B^T
+#pragma unroll 4
+                for (int m2 = 0; m2 < k; ++m2) {
+                    const double2 ai = A[MIDX(i, m2, N)], bi = B[MIDX(i, m2, N)];
+#pragma unroll
+                    for (int mm = 0; mm < UPD_CH; ++mm) {
+                        c1[mm] = cfma(ai, Bs[mm * nb + m2], c1[mm]);
+                        c2[mm] = cfma(As[mm * nb + m2], bi, c2[mm]);
+                    }
+                }
+                // this window's earlier chunks
+#pragma unroll 2
+                for (int m1 = 0; m1 < m0; ++m1) {
+                    const double2 a1 = A[MIDX(i, k + m1, N)], b1 = B[MIDX(i, k + m1, N)];
+#pragma unroll
+                    for (int mm = 0; mm < UPD_CH; ++mm) {
+                        c1[mm] = cfma(W->bW[m1][pmm[mm]], a1, c1[mm]);
+                        c2[mm] = cfma(W->aW[m1][pmm[mm]], b1, c2[mm]);
+                    }
+                }
+                // this chunk, in order
+#pragma unroll
+                for (int mm = 0; mm < UPD_CH; ++mm) {
+                    if (mm >= mc) break;
+#pragma unroll
+                    for (int m1 = 0; m1 < mm; ++m1) {
+                        c1[mm] = cfma(W->bW[m0 + m1][pmm[mm]], c1[m1], c1[mm]);
+                        c2[mm] = cfma(W->aW[m0 + m1][pmm[mm]], c2[m1], c2[mm]);
+                    }
+                    c1[mm] = cmul(c1[mm], W->sg[m0 + mm]);
+                    if (i == w0 + pmm[mm]) c2[mm].x -= 1.0;
+                    A[MIDX(i, k + m0 + mm, N)] = c1[mm];
+                    B[MIDX(i, k + m0 + mm, N)] = c2[mm];
+                }
+            }
             __syncthreads();
         }
-    }
-    if (ik > 0) {
-        ZGemmArgs g;
-        g.M = N; g.N = N; g.K = ik; g.alpha = cmk(1, 0); g.beta = cmk(1, 0);
-        g.A = c.A; g.lda = N; g.opA = OP_N; g.B = c.B; g.ldb = N; g.opB = OP_T; g.C = G; g.ldc = N;
-        zgemm_cta<UpdGemm>(g, 0, 1, gsm);
+        k += r;
+        s = w0 + wend;
+        __syncthreads();
+        if (k == nb || (s >= N && k > 0)) {
+            flush_addto(G, A, B, N, k, gsm);
+            k = 0;
+        }
     }
     if (tid == 0) {
-        c.stats[ST_PHASE_RE] = S->phase.x;
-        c.stats[ST_PHASE_IM] = S->phase.y;
-        if (!forced) {
-            c.stats[ST_ACC] += S->acc;
+        c.stats[ST_PHASE_RE] = ph.x;
+        c.stats[ST_PHASE_IM] = ph.y;
+        if (forced) {
+            c.stats[ST_BLK_LR_RE] = lr_re;
+            c.stats[ST_BLK_LR_IM] = lr_im;
+        } else {
+            c.stats[ST_ACC] += acc;
             c.stats[ST_PROP] += N;
         }
     }
@@ -174,10 +363,10 @@ __global__ void __launch_bounds__(256) k_update_delay(const ChainDev* __restrict
 static int g_upd_attr = 0;
 
 void launch_update(const ChainDev* chains, int nchains, int nt, int visit, cudaStream_t st, int forced) {
-    size_t smem = UpdGemm::SMEM_ELEMS * sizeof(double2) + (size_t)(512 + 2 * 64) * sizeof(double2) + sizeof(UpdSmem) + 64;
+    size_t smem = UpdGemm::SMEM_ELEMS * sizeof(double2);
     if (!g_upd_attr) {
         cudaFuncSetAttribute(k_update_delay, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         g_upd_attr = 1;
     }
-    k_update_delay<<<nchains, 256, smem, st>>>(chains, nt, visit, forced);
+    k_update_delay<<<nchains, UPD_NT, smem, st>>>(chains, nt, visit, forced);
 }
