@@ -794,10 +794,25 @@ struct dqmc_handle {
     uint64_t blk_rng = 0x9e3779b97f4a7c15ULL;
 };
 
+// Host <-> device copies of the entry points, ordered on the library's stream:
+// the stream is non-blocking, so a plain cudaMemcpy on the legacy stream is not
+// ordered with its kernels (a pageable host-to-device copy may still be in
+// flight when the next kernel on the stream starts).
+static cudaError_t copy_sync(cudaStream_t st, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, st);
+    cudaError_t e2 = cudaStreamSynchronize(st);
+    return e != cudaSuccess ? e : e2;
+}
+
 static void* dalloc(dqmc_handle* h, size_t bytes) {
     void* p = nullptr;
     if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess) return nullptr;
-    cudaMemset(p, 0, bytes ? bytes : 16);
+    if (h->st) {           // ordered with the library's (non-blocking) stream
+        cudaMemsetAsync(p, 0, bytes ? bytes : 16, h->st);
+        cudaStreamSynchronize(h->st);
+    } else {
+        cudaMemset(p, 0, bytes ? bytes : 16);   // creation ends with a device synchronisation
+    }
     h->allocs.push_back(p);
     return p;
 }
@@ -1490,7 +1505,7 @@ extern "C" int dqmc_gpu_set_conf(dqmc_handle* h, int chain, const int32_t* conf)
     size_t n = (size_t)h->ltrot * d.N;
     for (size_t e = 0; e < n; ++e)
         if (conf[e] < 1 || conf[e] > lcomp) return fail(DQMC_EINVAL, "HS field value out of range 1..lcomp");
-    CK(cudaMemcpy(d.conf, conf, n * sizeof(int32_t), cudaMemcpyHostToDevice));
+    CK(copy_sync(h->st, d.conf, conf, n * sizeof(int32_t), cudaMemcpyHostToDevice));
     h->started = 0;
     return DQMC_OK;
 }
@@ -1498,7 +1513,7 @@ extern "C" int dqmc_gpu_set_conf(dqmc_handle* h, int chain, const int32_t* conf)
 extern "C" int dqmc_gpu_get_conf(dqmc_handle* h, int chain, int32_t* conf) {
     int rc = chk_chain(h, chain); if (rc) return rc;
     const ChainDev& d = h->chains[chain].dev;
-    CK(cudaMemcpy(conf, d.conf, (size_t)h->ltrot * d.N * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    CK(copy_sync(h->st, conf, d.conf, (size_t)h->ltrot * d.N * sizeof(int32_t), cudaMemcpyDeviceToHost));
     return DQMC_OK;
 }
 
@@ -1535,14 +1550,14 @@ extern "C" int dqmc_gpu_get_conf_all(dqmc_handle* h, int32_t* conf) {
 extern "C" int dqmc_gpu_get_green(dqmc_handle* h, int chain, double* g) {
     int rc = chk_chain(h, chain); if (rc) return rc;
     const ChainDev& d = h->chains[chain].dev;
-    CK(cudaMemcpy(g, d.G, (size_t)d.N * d.N * sizeof(double2), cudaMemcpyDeviceToHost));
+    CK(copy_sync(h->st, g, d.G, (size_t)d.N * d.N * sizeof(double2), cudaMemcpyDeviceToHost));
     return DQMC_OK;
 }
 
 extern "C" int dqmc_gpu_set_green(dqmc_handle* h, int chain, const double* g) {
     int rc = chk_chain(h, chain); if (rc) return rc;
     const ChainDev& d = h->chains[chain].dev;
-    CK(cudaMemcpy(d.G, g, (size_t)d.N * d.N * sizeof(double2), cudaMemcpyHostToDevice));
+    CK(copy_sync(h->st, d.G, g, (size_t)d.N * d.N * sizeof(double2), cudaMemcpyHostToDevice));
     h->started = 1;
     return DQMC_OK;
 }
@@ -1551,7 +1566,7 @@ extern "C" int dqmc_gpu_set_work(dqmc_handle* h, int chain, int which, const dou
     int rc = chk_chain(h, chain); if (rc) return rc;
     if (which < 0 || which > 5) return fail(DQMC_EINVAL, "work index 0..5");
     const ChainDev& d = h->chains[chain].dev;
-    CK(cudaMemcpy(d.W[which], mtx, (size_t)d.N * d.N * sizeof(double2), cudaMemcpyHostToDevice));
+    CK(copy_sync(h->st, d.W[which], mtx, (size_t)d.N * d.N * sizeof(double2), cudaMemcpyHostToDevice));
     return DQMC_OK;
 }
 
@@ -1559,7 +1574,7 @@ extern "C" int dqmc_gpu_get_work(dqmc_handle* h, int chain, int which, double* m
     int rc = chk_chain(h, chain); if (rc) return rc;
     if (which < 0 || which > 5) return fail(DQMC_EINVAL, "work index 0..5");
     const ChainDev& d = h->chains[chain].dev;
-    CK(cudaMemcpy(mtx, d.W[which], (size_t)d.N * d.N * sizeof(double2), cudaMemcpyDeviceToHost));
+    CK(copy_sync(h->st, mtx, d.W[which], (size_t)d.N * d.N * sizeof(double2), cudaMemcpyDeviceToHost));
     return DQMC_OK;
 }
 
@@ -1581,7 +1596,7 @@ extern "C" int dqmc_gpu_test_qr(dqmc_handle* h, int a, int q, double* logdetq) {
     CK(cudaGetLastError());
     for (int c = 0; c < h->nch; ++c) {
         double st[ST_COUNT];
-        CK(cudaMemcpy(st, h->chains[c].dev.stats, sizeof(st), cudaMemcpyDeviceToHost));
+        CK(copy_sync(h->st, st, h->chains[c].dev.stats, sizeof(st), cudaMemcpyDeviceToHost));
         logdetq[2 * c] = st[ST_LOGDETM_RE];
         logdetq[2 * c + 1] = st[ST_LOGDETM_IM];
     }
@@ -1605,7 +1620,7 @@ extern "C" int dqmc_gpu_nbins(dqmc_handle* h, int chain) {
 extern "C" int dqmc_gpu_get_bins(dqmc_handle* h, int chain, double* out) {
     int rc = chk_chain(h, chain); if (rc) return rc;
     int nb = dqmc_gpu_nbins(h, chain);
-    CK(cudaMemcpy(out, h->chains[chain].dev.bins, (size_t)nb * sizeof(double2), cudaMemcpyDeviceToHost));
+    CK(copy_sync(h->st, out, h->chains[chain].dev.bins, (size_t)nb * sizeof(double2), cudaMemcpyDeviceToHost));
     return DQMC_OK;
 }
 
@@ -1620,7 +1635,7 @@ extern "C" int dqmc_gpu_get_energy_all(dqmc_handle* h, double* out) {
 extern "C" int dqmc_gpu_get_diag(dqmc_handle* h, int chain, dqmc_diag* out) {
     int rc = chk_chain(h, chain); if (rc) return rc;
     double st[ST_COUNT];
-    CK(cudaMemcpy(st, h->chains[chain].dev.stats, sizeof(st), cudaMemcpyDeviceToHost));
+    CK(copy_sync(h->st, st, h->chains[chain].dev.stats, sizeof(st), cudaMemcpyDeviceToHost));
     out->phase_re = st[ST_PHASE_RE]; out->phase_im = st[ST_PHASE_IM];
     out->logweight_re = st[ST_LOGW_RE]; out->logweight_im = st[ST_LOGW_IM];
     out->max_wrap_error = st[ST_MAX_WRAP]; out->max_phasediff = st[ST_MAX_PHASEDIFF];
@@ -1638,12 +1653,12 @@ extern "C" int dqmc_gpu_reset_diag(dqmc_handle* h) {
     if (!h) return fail(DQMC_EINVAL, "null handle");
     for (int c = 0; c < h->nch; ++c) {
         double st[ST_COUNT];
-        CK(cudaMemcpy(st, h->chains[c].dev.stats, sizeof(st), cudaMemcpyDeviceToHost));
+        CK(copy_sync(h->st, st, h->chains[c].dev.stats, sizeof(st), cudaMemcpyDeviceToHost));
         st[ST_MAX_WRAP] = st[ST_MAX_PHASEDIFF] = st[ST_AVGLOG10] = st[ST_LOGCOUNT] = st[ST_AVGEXPPD] = 0.0;
         st[ST_ACC] = st[ST_PROP] = st[ST_ACCV] = st[ST_PROPV] = 0.0;
         st[ST_BLK_PROP] = st[ST_BLK_S1] = st[ST_BLK_ACC] = st[ST_BLK_SUMLR] = 0.0;
         st[ST_BLK_ERR1] = st[ST_BLK_ERR0] = 0.0;
-        CK(cudaMemcpy(h->chains[c].dev.stats, st, sizeof(st), cudaMemcpyHostToDevice));
+        CK(copy_sync(h->st, h->chains[c].dev.stats, st, sizeof(st), cudaMemcpyHostToDevice));
     }
     return DQMC_OK;
 }
@@ -1651,7 +1666,7 @@ extern "C" int dqmc_gpu_reset_diag(dqmc_handle* h) {
 extern "C" int dqmc_gpu_set_phase(dqmc_handle* h, int chain, double re, double im) {
     int rc = chk_chain(h, chain); if (rc) return rc;
     double v[2] = {re, im};
-    CK(cudaMemcpy(h->chains[chain].dev.stats + ST_PHASE_RE, v, sizeof(v), cudaMemcpyHostToDevice));
+    CK(copy_sync(h->st, h->chains[chain].dev.stats + ST_PHASE_RE, v, sizeof(v), cudaMemcpyHostToDevice));
     return DQMC_OK;
 }
 
@@ -1661,7 +1676,7 @@ extern "C" int dqmc_gpu_draw_u32(dqmc_handle* h, int chain, int count, uint32_t*
     if (count < 0 || count > h->ltrot * 2 * d.N) return fail(DQMC_EINVAL, "count out of range");
     launch_sfmt_raw(h->d_chains, chain, count, h->st);
     CK(cudaStreamSynchronize(h->st));
-    CK(cudaMemcpy(out, d.rnd, (size_t)count * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    CK(copy_sync(h->st, out, d.rnd, (size_t)count * sizeof(uint32_t), cudaMemcpyDeviceToHost));
     return DQMC_OK;
 }
 
@@ -1840,7 +1855,7 @@ extern "C" int dqmc_gpu_set_vconf(dqmc_handle* h, int chain, const int32_t* v) {
     size_t n = (size_t)h->ltrot * h->models[h->chains[chain].model]->nn_nf * d.N;
     for (size_t e = 0; e < n; ++e)
         if (v[e] < 1 || v[e] > 2) return fail(DQMC_EINVAL, "bond field value out of range 1..2");
-    CK(cudaMemcpy(d.vconf, v, n * sizeof(int32_t), cudaMemcpyHostToDevice));
+    CK(copy_sync(h->st, d.vconf, v, n * sizeof(int32_t), cudaMemcpyHostToDevice));
     h->started = 0;
     return DQMC_OK;
 }
@@ -1850,7 +1865,7 @@ extern "C" int dqmc_gpu_get_vconf(dqmc_handle* h, int chain, int32_t* v) {
     const ChainDev& d = h->chains[chain].dev;
     if (!d.vconf) return fail(DQMC_ESTATE, "no bond field (rv == 0)");
     size_t n = (size_t)h->ltrot * h->models[h->chains[chain].model]->nn_nf * d.N;
-    CK(cudaMemcpy(v, d.vconf, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    CK(copy_sync(h->st, v, d.vconf, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
     return DQMC_OK;
 }
 
@@ -1875,15 +1890,15 @@ extern "C" int dqmc_gpu_get_proj(dqmc_handle* h, int chain, double* ur, double* 
     const ChainDev& d = h->chains[chain].dev;
     int N = d.N, ne = h->models[h->chains[chain].model]->p.ne;
     size_t Nne = (size_t)N * ne;
-    if (ur) CK(cudaMemcpy(ur, d.UR, Nne * sizeof(zc), cudaMemcpyDeviceToHost));
+    if (ur) CK(copy_sync(h->st, ur, d.UR, Nne * sizeof(zc), cudaMemcpyDeviceToHost));
     if (ul) {
         std::vector<zc> t(Nne);
-        CK(cudaMemcpy(t.data(), d.ULT, Nne * sizeof(zc), cudaMemcpyDeviceToHost));
+        CK(copy_sync(h->st, t.data(), d.ULT, Nne * sizeof(zc), cudaMemcpyDeviceToHost));
         zc* o = (zc*)ul;
         for (int l = 0; l < ne; ++l)
             for (int i = 0; i < N; ++i) o[l + (size_t)i * ne] = t[i + (size_t)l * N];
     }
-    if (ulrinv) CK(cudaMemcpy(ulrinv, d.ULRINV, (size_t)ne * ne * sizeof(zc), cudaMemcpyDeviceToHost));
+    if (ulrinv) CK(copy_sync(h->st, ulrinv, d.ULRINV, (size_t)ne * ne * sizeof(zc), cudaMemcpyDeviceToHost));
     return DQMC_OK;
 }
 
@@ -1892,15 +1907,15 @@ extern "C" int dqmc_gpu_set_proj(dqmc_handle* h, int chain, const double* ur, co
     const ChainDev& d = h->chains[chain].dev;
     int N = d.N, ne = h->models[h->chains[chain].model]->p.ne;
     size_t Nne = (size_t)N * ne;
-    if (ur) CK(cudaMemcpy(d.UR, ur, Nne * sizeof(zc), cudaMemcpyHostToDevice));
+    if (ur) CK(copy_sync(h->st, d.UR, ur, Nne * sizeof(zc), cudaMemcpyHostToDevice));
     if (ul) {
         std::vector<zc> t(Nne);
         const zc* in = (const zc*)ul;
         for (int l = 0; l < ne; ++l)
             for (int i = 0; i < N; ++i) t[i + (size_t)l * N] = in[l + (size_t)i * ne];
-        CK(cudaMemcpy(d.ULT, t.data(), Nne * sizeof(zc), cudaMemcpyHostToDevice));
+        CK(copy_sync(h->st, d.ULT, t.data(), Nne * sizeof(zc), cudaMemcpyHostToDevice));
     }
-    if (ulrinv) CK(cudaMemcpy(d.ULRINV, ulrinv, (size_t)ne * ne * sizeof(zc), cudaMemcpyHostToDevice));
+    if (ulrinv) CK(copy_sync(h->st, d.ULRINV, ulrinv, (size_t)ne * ne * sizeof(zc), cudaMemcpyHostToDevice));
     return DQMC_OK;
 }
 
@@ -2004,6 +2019,7 @@ extern "C" int dqmc_nn_create(int ltrot, int l, int max_batch, uint64_t seed, dq
         dqmc_nn_destroy(nn);
         return fail(DQMC_ECUDA, "stream");
     }
+    cudaDeviceSynchronize();   // the allocations were cleared on the legacy stream
     // initial weights: uniform in +-sqrt(3/fan_in) (unit-variance pre-activations);
     // the readout w3 is scaled by 0.01 so that S starts close to a constant
     // (a sum over all sites of an O(1) readout would start with fluctuations far
@@ -2021,7 +2037,7 @@ extern "C" int dqmc_nn_create(int ltrot, int l, int max_batch, uint64_t seed, dq
     for (int i = 0; i < 27 * 32; ++i) th[i] = (float)(uni() * std::sqrt(3.0 / 27.0));
     for (int i = 0; i < 27 * 32 * 32; ++i) th[NN_GW2 + i] = (float)(uni() * std::sqrt(3.0 / 864.0));
     for (int i = 0; i < 32; ++i) th[NN_GW3 + i] = (float)(0.01 * uni() * std::sqrt(3.0 / 32.0));
-    cudaMemcpy(nn->theta, th.data(), th.size() * sizeof(float), cudaMemcpyHostToDevice);
+    copy_sync(nn->st, nn->theta, th.data(), th.size() * sizeof(float), cudaMemcpyHostToDevice);
     launch_nn_pack(nn->theta, nn->W2T, nn->W2R, nn->st);
     if (cudaStreamSynchronize(nn->st) != cudaSuccess) { dqmc_nn_destroy(nn); return fail(DQMC_ECUDA, "init"); }
     *out = nn;
@@ -2030,10 +2046,10 @@ extern "C" int dqmc_nn_create(int ltrot, int l, int max_batch, uint64_t seed, dq
 
 extern "C" int dqmc_nn_set_params(dqmc_nn* nn, const float* theta) {
     if (!nn || !theta) return fail(DQMC_EINVAL, "invalid arguments");
-    CK(cudaMemcpy(nn->theta, theta, NN_NPARAM * sizeof(float), cudaMemcpyHostToDevice));
+    CK(copy_sync(nn->st, nn->theta, theta, NN_NPARAM * sizeof(float), cudaMemcpyHostToDevice));
     nn->b3 = theta[NN_GB3];
-    CK(cudaMemset(nn->m1, 0, NN_NPARAM * sizeof(float)));
-    CK(cudaMemset(nn->m2, 0, NN_NPARAM * sizeof(float)));
+    CK(cudaMemsetAsync(nn->m1, 0, NN_NPARAM * sizeof(float), nn->st));
+    CK(cudaMemsetAsync(nn->m2, 0, NN_NPARAM * sizeof(float), nn->st));
     nn->step = 0;
     launch_nn_pack(nn->theta, nn->W2T, nn->W2R, nn->st);
     CK(cudaStreamSynchronize(nn->st));
@@ -2042,7 +2058,7 @@ extern "C" int dqmc_nn_set_params(dqmc_nn* nn, const float* theta) {
 
 extern "C" int dqmc_nn_get_params(dqmc_nn* nn, float* theta) {
     if (!nn || !theta) return fail(DQMC_EINVAL, "invalid arguments");
-    CK(cudaMemcpy(theta, nn->theta, NN_NPARAM * sizeof(float), cudaMemcpyDeviceToHost));
+    CK(copy_sync(nn->st, theta, nn->theta, NN_NPARAM * sizeof(float), cudaMemcpyDeviceToHost));
     theta[NN_GB3] = nn->b3;
     return DQMC_OK;
 }
@@ -2138,7 +2154,8 @@ extern "C" int dqmc_gpu_record(dqmc_handle* h, int capacity) {
         h->rec_cap = capacity;
     }
     h->rec_V = V;
-    CK(cudaMemset(h->rec_count, 0, sizeof(int)));
+    CK(cudaMemsetAsync(h->rec_count, 0, sizeof(int), h->st));
+    CK(cudaStreamSynchronize(h->st));
     h->rec_on = 1;
     return DQMC_OK;
 }
@@ -2146,21 +2163,21 @@ extern "C" int dqmc_gpu_record(dqmc_handle* h, int capacity) {
 extern "C" int dqmc_gpu_record_count(dqmc_handle* h) {
     if (!h || !h->rec_count) return 0;
     int n = 0;
-    cudaMemcpy(&n, h->rec_count, sizeof(int), cudaMemcpyDeviceToHost);
+    copy_sync(h->st, &n, h->rec_count, sizeof(int), cudaMemcpyDeviceToHost);
     long long tot = (long long)n * h->nch;
     return (int)std::min<long long>(tot, h->rec_cap);
 }
 
 extern "C" int dqmc_gpu_record_get(dqmc_handle* h, int i, int8_t* field, double* value) {
     if (!h || !h->rec_f || i < 0 || i >= h->rec_cap) return fail(DQMC_EINVAL, "record index out of range");
-    if (field) CK(cudaMemcpy(field, h->rec_f + (size_t)i * h->rec_V, h->rec_V, cudaMemcpyDeviceToHost));
-    if (value) CK(cudaMemcpy(value, h->rec_v + i, sizeof(double), cudaMemcpyDeviceToHost));
+    if (field) CK(copy_sync(h->st, field, h->rec_f + (size_t)i * h->rec_V, h->rec_V, cudaMemcpyDeviceToHost));
+    if (value) CK(copy_sync(h->st, value, h->rec_v + i, sizeof(double), cudaMemcpyDeviceToHost));
     return DQMC_OK;
 }
 
 extern "C" int dqmc_gpu_record_values(dqmc_handle* h, double* values) {
     if (!h || !h->rec_v || !values) return fail(DQMC_EINVAL, "no record buffer");
-    CK(cudaMemcpy(values, h->rec_v, (size_t)h->rec_cap * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(copy_sync(h->st, values, h->rec_v, (size_t)h->rec_cap * sizeof(double), cudaMemcpyDeviceToHost));
     return DQMC_OK;
 }
 
@@ -2196,7 +2213,7 @@ static int enable_blocks(dqmc_handle* h) {
     h->d_S = (double*)dalloc(h, (size_t)h->nch * 2 * sizeof(double));
     std::vector<ChainDev> v(h->nch);
     for (int c = 0; c < h->nch; ++c) v[c] = h->chains[c].dev;
-    CK(cudaMemcpy(h->d_chains, v.data(), sizeof(ChainDev) * h->nch, cudaMemcpyHostToDevice));
+    CK(copy_sync(h->st, h->d_chains, v.data(), sizeof(ChainDev) * h->nch, cudaMemcpyHostToDevice));
     h->blocks = 1;
     if (h->sweep_graph) { cudaGraphExecDestroy(h->sweep_graph); h->sweep_graph = nullptr; }
     return DQMC_OK;

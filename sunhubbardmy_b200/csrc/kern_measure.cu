@@ -7,7 +7,7 @@
 // transpose), so that every correlation term reads a column of G or of G^T.
 // The distance-binned correlations are accumulated without atomics: one
 // thread owns one bin (distance d, orbitals a, b) and walks the unit cells j,
-// pairing each with cell i = j + d from a precomputed table (imj(i, j) = d);
+// pairing each with cell i = j + d (imj(i, j) = d, in closed form);
 // the threads of consecutive d read consecutive rows of the same columns.
 // The single-number energy terms run on the chain's first CTA.
 //
@@ -23,9 +23,19 @@ DQ_DEV double2 gcf(const double2* G, int N, int i, int j) {   // Gc(i,j)
 }
 DQ_DEV double2 gf(const double2* G, int N, int i, int j) { return G[MIDX(i, j, N)]; }
 
+// cell i = j + d of the distance table imj(i, j) = d (setup_latt2d_sub): with
+// cells c = c1 l2 + c2 and d = dy + l2 dx, i1 = (j1 + dx + 1) mod l1 and
+// i2 = (j2 + dy + 1) mod l2; dxp = dx + 1, dyp = dy + 1
+DQ_DEV int cell_shift(int cj, int dxp, int dyp, int l1, int l2) {
+    int i1 = cj / l2 + dxp, i2 = cj % l2 + dyp;
+    if (i1 >= l1) i1 -= l1;
+    if (i2 >= l2) i2 -= l2;
+    return i1 * l2 + i2;
+}
+
 __global__ void __launch_bounds__(256) k_measure(const ChainDev* __restrict__ chains) {
     __shared__ double red[64];
-    const ChainDev c = chains[blockIdx.y];
+    const ChainDev& c = chains[blockIdx.y];
     const ModelDev& md = *c.md;
     const int N = c.N, lq = md.lq, tid = threadIdx.x, nth = blockDim.x;
     const int nnf = md.nn_nf, zp = md.z_plq, nflr = md.nflr;
@@ -66,16 +76,16 @@ __global__ void __launch_bounds__(256) k_measure(const ChainDev* __restrict__ ch
     double2* pnn = zbb + lq;
     double2* psn = pnn + lq;
     const double2* GT = c.GT;
-    const int nsub = md.nsub;
+    const int nsub = md.nsub, l1 = md.l1, l2 = md.l2;
     const int nbin_a = lq * nsub * nsub, nbin = nbin_a + lq;
     for (int bin = blockIdx.x * nth + tid; bin < nbin; bin += gridDim.x * nth) {
         if (bin < nbin_a) {
             const int d = bin % lq, ab = bin / lq, a = ab % nsub, b = ab / nsub;
-            const int* cp = md.cell_plus + (size_t)d * lq;
+            const int dxp = d / l2 + 1, dyp = d % l2 + 1;
             double2 s1 = cmk(0, 0), s2 = cmk(0, 0), s3 = cmk(0, 0), s4 = cmk(0, 0);
 #pragma unroll 4
             for (int cj = 0; cj < lq; ++cj) {
-                const int i = __ldg(&cp[cj]) * nsub + a, j = cj * nsub + b;
+                const int i = cell_shift(cj, dxp, dyp, l1, l2) * nsub + a, j = cj * nsub + b;
                 const size_t o = (size_t)i + (size_t)N * j;
                 const double2 gt = GT[o], g = G[o];          // G(j,i), G(i,j)
                 const double2 gc = cmk((i == j ? 1.0 : 0.0) - gt.x, -gt.y);
@@ -92,7 +102,7 @@ __global__ void __launch_bounds__(256) k_measure(const ChainDev* __restrict__ ch
             pons[k] = cfma(s4, zphi, pons[k]);
         } else {
             const int d = bin - nbin_a;
-            const int* cp = md.cell_plus + (size_t)d * lq;
+            const int dxp = d / l2 + 1, dyp = d % l2 + 1;
             // element (r, s) of G is G[r + N s], of G^T (= G(s, r)) GT[r + N s]
             auto gg = [&](int r, int s_) { return G[(size_t)r + (size_t)N * s_]; };
             auto gtt = [&](int r, int s_) { return GT[(size_t)r + (size_t)N * s_]; };
@@ -101,9 +111,9 @@ __global__ void __launch_bounds__(256) k_measure(const ChainDev* __restrict__ ch
                 return cmk((r == s_ ? 1.0 : 0.0) - t.x, -t.y);
             };
             double2 sj = cmk(0, 0), sb = cmk(0, 0), sn = cmk(0, 0), ss = cmk(0, 0);
-#pragma unroll 2
+#pragma unroll 4
             for (int cj = 0; cj < lq; ++cj) {
-                const int ci = __ldg(&cp[cj]);
+                const int ci = cell_shift(cj, dxp, dyp, l1, l2);
                 const int j0 = hc ? 2 * cj : cj, i0 = hc ? 2 * ci : ci;
                 const int jnj = pj[cj], inj = pj[ci], jnb = pb[cj], inb = pb[ci];
                 const double2 g00 = gg(i0, j0), gc00 = cc(i0, j0);

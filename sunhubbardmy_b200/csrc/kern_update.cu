@@ -123,7 +123,7 @@ DQ_DEV void flush_addto(double2* G, const double2* A, const double2* B, int N, i
 // the flush after the window has been closed.
 #define UPD_L 32
 #define UPD_LP (UPD_L + 1)       // odd pitch: rows and columns of gW are both conflict-free
-#define UPD_CH 8                 // window columns extended to all rows per pass
+#define UPD_CH 4                 // window columns extended to all rows per pass
 struct UpdWin {
     double2 gW[UPD_L * UPD_LP];  // G'(w0 + p, w0 + q) at gW[q * UPD_LP + p], G' = G + A B^T
     double2 aW[UPD_L][UPD_L];    // [m][p]: window row p of the window's m-th new column of A
@@ -260,6 +260,7 @@ __global__ void __launch_bounds__(UPD_NT, 2) k_update_delay(const ChainDev* __re
                 if (p < L) {
                     double2 a = W->gW[pf * UPD_LP + p];          // G'(p, f)
                     double2 b = W->gW[p * UPD_LP + pf];          // G'(f, p)
+#pragma unroll 4
                     for (int m = 0; m < r; ++m) {
                         a = cfma(W->bW[m][pf], W->aW[m][p], a);
                         b = cfma(W->aW[m][pf], W->bW[m][p], b);
