@@ -62,6 +62,10 @@ typedef struct dqmc_params {
     int32_t proj, lprojv, obs_mid_len;
     /* derived (src/model_para.f90:334-453) */
     int32_t ndim, lq, ltrot, nst, ne, lcomp;
+    /* unequal-time measurement: ltau and dyntau of &ctrl_para; ntdm =
+     * nint(dyntau / dtau) is derived (src/model_para.f90:455-459) */
+    int32_t ltau, ntdm;
+    double dyntau;
 } dqmc_params;
 
 /* per-chain diagnostics (src/dqmc_util.f90:15-57, 287-299) */
@@ -181,6 +185,24 @@ int dqmc_gpu_sweep_kernels(dqmc_handle* h);
  * 3 kinetic + HS column pass, 4 equal-time measurement, 5 row pass.  Modifies
  * chain state; intended for benchmarks after the timed sweeps. */
 int dqmc_gpu_time_op(dqmc_handle* h, int op, int reps, double* ms_out);
+
+/* Unequal-time measurement (params.ltau = 1, finite temperature): the pass
+ * dqmc_sweep runs between the b0 and the 0b sweep (src/dqmc_ft_ctrl.f90:97-101):
+ * push_stage, dqmc_ft_sweep_0b(lupdate = F, lmeasure_equaltime = F,
+ * lmeasure_dyn = T) -- G(tau,0) and G(0,tau) propagated slice by slice
+ * (src/dqmc_ft_core/dyn.f90) and recomputed by green_tau at every
+ * stabilisation (src/dqmc_ft_core/green_tau.f90), dyn_measure at every time
+ * index (src/dqmc_measure/dyn_measure.f90) -- then pop_stage
+ * (src/dqmc_ft_core.f90:290-312).  It must follow a b0 sweep, whose left
+ * factors it needs (DQMC_ESTATE otherwise); dqmc_gpu_sweeps runs it between the
+ * b0 and the 0b sweep of every measured sweep when ltau = 1. */
+int dqmc_gpu_sweep_dyn(dqmc_handle* h);
+/* znn_tau_bin(lq, 2, 2, ntdm+1) of one chain, Fortran order, complex as
+ * (re, im) pairs: 8 lq (ntdm+1) doubles; obser_init clears it. */
+int dqmc_gpu_get_dyn_bins(dqmc_handle* h, int chain, double* out);
+/* G(0,0), G(tau,0), G(0,tau) (N x N complex, column-major) after the last
+ * unequal-time pass, tau = beta; any pointer may be NULL. */
+int dqmc_gpu_get_dyn_mats(dqmc_handle* h, int chain, double* g00, double* gt0, double* g0t);
 
 /* Per-kind device time of whole sweeps, the counterpart of the reference's
  * -DTIMING breakdown (src/dqmc_util.f90:287-369, dqmc_timing).  Runs `nsweeps`

@@ -54,6 +54,9 @@ typedef struct {
     int32_t update, kinetic, hs;
     /* projective run (dqmc_proj_ctrl), lprojv and obs_eqt_mid_len of &ctrl_para */
     int32_t proj, lprojv, obs_mid_len;
+    /* unequal-time measurement: ltau and dyntau of &ctrl_para */
+    int32_t ltau;
+    double dyntau;
 } orc_params;
 
 typedef struct orc_model orc_model;
@@ -110,6 +113,13 @@ int  orc_sweep_start_0b(orc_chain *c);
 int  orc_sweep_b0(orc_chain *c, int lupdate, int lmeasure);
 int  orc_sweep_b0_slices(orc_chain *c, int lupdate, int lmeasure, int nslices);
 int  orc_sweep_0b(orc_chain *c, int lupdate, int lmeasure);
+/* unequal-time pass of dqmc_sweep (push_stage, 0b sweep with dyn_measure, pop_stage) */
+int  orc_sweep_dyn(orc_chain *c);
+int  orc_dyn_bins(const orc_chain *c, double *out);
+int  orc_dyn_mats(const orc_chain *c, double *g00, double *gt0, double *g0t);
+int  orc_green_tau(int n, const double *ur, const double *dr, const double *vr, const double *vl, const double *dl,
+                   const double *ul, double *g00, double *gt0, double *g0t, double *gtt, const double *logdetqr,
+                   const double *logdetql, double *logw);
 void orc_obser_init(orc_chain *c);
 
 /* operator-level entry points acting on an explicit N x N matrix */

@@ -208,6 +208,8 @@ orc_model *orc_model_new(const orc_params *pin) {
     m->ndim = m->L.nsites;
     m->ne = m->ndim / 2 + (int)(p->nu * m->ndim / 8.0);
     m->ltrot = (int)lround(p->beta / p->dtau);
+    m->ntdm = p->ltau ? (int)lround(p->dyntau / p->dtau) : 0;
+    if (m->ntdm < 0) m->ntdm = 0;
     m->lwrapT = (p->rt != 0.0);
     m->lwrapu = (p->rhub != 0.0);
     int N = m->ndim;
@@ -332,6 +334,17 @@ orc_chain *orc_chain_new(const orc_model *m, int32_t seed, int draw_conf) {
         c->Dst[n] = calloc(N, sizeof(double));
     }
     c->phase = 1.0;
+    if (m->p.ltau) {
+        c->g00 = zalloc((size_t)N * N); c->gt0 = zalloc((size_t)N * N); c->g0t = zalloc((size_t)N * N);
+        c->znn_tau_bin = zalloc((size_t)lq * 4 * (m->ntdm + 1));
+        c->gf_b = zalloc((size_t)N * N);
+        c->Ust_b = calloc(nst + 1, sizeof(zc *)); c->Vst_b = calloc(nst + 1, sizeof(zc *));
+        c->Dst_b = calloc(nst + 1, sizeof(double *)); c->logdetQst_b = zalloc(nst + 1);
+        for (int n = 0; n <= nst; ++n) {
+            c->Ust_b[n] = zalloc((size_t)N * N); c->Vst_b[n] = zalloc((size_t)N * N);
+            c->Dst_b[n] = calloc(N, sizeof(double));
+        }
+    }
     c->zcpcm_bin = zalloc(lq * 4); c->zspsm_bin = zalloc(lq * 4);
     c->znn_bin = zalloc(lq * 4); c->pair_onsite_bin = zalloc(lq * 4);
     c->zjj_bin = zalloc(lq); c->zbb_bin = zalloc(lq);
@@ -345,6 +358,11 @@ void orc_chain_free(orc_chain *c) {
     for (int n = 0; n <= c->m->nst; ++n) { free(c->Ust[n]); free(c->Vst[n]); free(c->Dst[n]); }
     free(c->Ust); free(c->Vst); free(c->Dst); free(c->logdetQst);
     free(c->conf); free(c->gf); free(c->gfc);
+    if (c->m->p.ltau) {
+        for (int n = 0; n <= c->m->nst; ++n) { free(c->Ust_b[n]); free(c->Vst_b[n]); free(c->Dst_b[n]); }
+        free(c->Ust_b); free(c->Vst_b); free(c->Dst_b); free(c->logdetQst_b); free(c->gf_b);
+        free(c->g00); free(c->gt0); free(c->g0t); free(c->znn_tau_bin);
+    }
     free(c->zcpcm_bin); free(c->zspsm_bin); free(c->znn_bin); free(c->pair_onsite_bin);
     free(c->zjj_bin); free(c->zbb_bin); free(c->pair_nn_bin); free(c->pair_sn_bin);
     orc_proj_chain_free(c);
@@ -942,6 +960,7 @@ void orc_obser_init(orc_chain *c) {   /* dqmc_measure_2d.f90:105-130 */
     memset(c->zjj_bin, 0, sizeof(zc) * lq); memset(c->zbb_bin, 0, sizeof(zc) * lq);
     memset(c->pair_nn_bin, 0, sizeof(zc) * lq); memset(c->pair_sn_bin, 0, sizeof(zc) * lq);
     c->zn_bin[0] = c->zn_bin[1] = 0; c->zj_bin = 0; c->zb_bin = 0;
+    if (c->m->p.ltau) memset(c->znn_tau_bin, 0, sizeof(zc) * (size_t)lq * 4 * (c->m->ntdm + 1));
 }
 
 static int npbc_cyc(int nr, int l) { if (nr > l) return nr - l; if (nr < 1) return nr + l; return nr; }
@@ -1185,6 +1204,196 @@ int orc_sweep_b0_slices(orc_chain *c, int lupdate, int lmeasure, int nslices) {
     }
     free(gtmp); free(ur); free(vr); free(dr);
     return 0;
+}
+
+/* Bmat_right_backward (src/dqmc_ft_core.f90:234-288): g * B(nt1,nt2)^-1 */
+static void bmat_right_backward(const orc_chain *c, int nt1, int nt2, zc *g) {
+    const orc_model *m = c->m;
+    int N = m->ndim, nnf = m->L.nn_nf;
+    int cb = (m->p.kinetic == ORC_CHECKERBOARD);
+    for (int nt = nt2; nt <= nt1; ++nt) {
+        if (m->lwrapT) {
+            if (cb) for (int nf = 1; nf <= nnf; ++nf) h0_cb(m, ORC_RIGHT_BACKWARD, nf, g, N);
+            else h0_fft(m, ORC_RIGHT_BACKWARD, g, N);
+        }
+        if (m->lwrapu) u_prop(m, c->conf, ORC_RIGHT_BACKWARD, nt, g, N);
+        if (m->lwrapT) {
+            if (cb) for (int nf = nnf; nf >= 1; --nf) h0_cb(m, ORC_RIGHT_BACKWARD, nf, g, N);
+            else h0_fft(m, ORC_RIGHT_BACKWARD, g, N);
+        }
+    }
+}
+
+/* z = v diag(d or 1/d) u  (or u^H): s_v_d_u, s_v_invd_u, s_v_d_uH, s_v_invd_uH
+ * (lib/s_matrix.f90:597-719) */
+static void v_d_u(int N, const zc *v, const double *d, int inv, const zc *u, char tu, zc *z) {
+    zc *vd = zalloc((size_t)N * N);
+    for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i) vd[ZIDX(i, j, N)] = inv ? v[ZIDX(i, j, N)] / d[j] : v[ZIDX(i, j, N)] * d[j];
+    orc_zgemm('N', tu, N, N, N, 1.0, vd, N, u, N, 0.0, z, N);
+    free(vd);
+}
+
+/* green_tau (src/dqmc_ft_core/green_tau.f90:1-136): G(tau,tau), G(tau,0),
+ * G(0,tau), G(0,0) from the right (ure, dre, vre) and left (ule, dle, vle)
+ * factors */
+static int green_tau(int N, const zc *ure, const double *dre, const zc *vre, const zc *vle, const double *dle,
+                     const zc *ule, zc *g00, zc *gt0, zc *g0t, zc *gtt, zc logdetqr, zc logdetql, zc *logw) {
+    double *drmax = malloc(sizeof(double) * N), *drmin = malloc(sizeof(double) * N);
+    double *dlmax = malloc(sizeof(double) * N), *dlmin = malloc(sizeof(double) * N);
+    size_t NN = (size_t)N * N;
+    zc *vlh = zalloc(NN), *uu = zalloc(NN), *vv = zalloc(NN), *dvvd = zalloc(NN), *bt = zalloc(NN), *vri = zalloc(NN);
+    dvec_min_max(N, dre, drmax, drmin);
+    dvec_min_max(N, dle, dlmax, dlmin);
+    for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i) vlh[ZIDX(i, j, N)] = conj(vle[ZIDX(j, i, N)]);
+    orc_zgemm('C', 'N', N, N, N, 1.0, ure, N, ule, N, 0.0, uu, N);     /* uutmp = ure^H ule */
+    orc_zgemm('N', 'C', N, N, N, 1.0, vre, N, vle, N, 0.0, vv, N);     /* vvtmp = vre vle^H */
+    for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i)
+            dvvd[ZIDX(i, j, N)] = uu[ZIDX(i, j, N)] / (drmax[i] * dlmax[j]) + vv[ZIDX(i, j, N)] * drmin[i] * dlmin[j];
+    zc zl;
+    orc_zinv_logdet(N, dvvd, &zl);
+    v_d_u(N, ule, dlmax, 1, dvvd, 'N', bt);
+    v_d_u(N, bt, drmax, 1, ure, 'C', gtt);
+    double r1 = 0, r2 = 0;
+    for (int i = 0; i < N; ++i) r1 += log(dlmax[i]);
+    for (int i = 0; i < N; ++i) r2 += log(drmax[i]);
+    *logw = -logdetql + logdetqr + zl + (r1 + r2);
+    v_d_u(N, bt, drmin, 0, vre, 'N', gt0);                             /* g(t,0) */
+    memcpy(vri, vre, sizeof(zc) * NN);
+    orc_zinv(N, vri);                                                  /* vre^-1 */
+    orc_zinv(N, vlh);                                                  /* (vle^H)^-1 */
+    orc_zgemm('N', 'N', N, N, N, 1.0, vlh, N, vri, N, 0.0, vv, N);     /* (vre vle^H)^-1 */
+    for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i)
+            dvvd[ZIDX(i, j, N)] = vv[ZIDX(i, j, N)] / (dlmax[i] * drmax[j]) + conj(uu[ZIDX(j, i, N)]) * dlmin[i] * drmin[j];
+    orc_zinv(N, dvvd);
+    v_d_u(N, vri, drmax, 1, dvvd, 'N', bt);
+    v_d_u(N, bt, dlmax, 1, vlh, 'N', g00);                             /* g(0,0) */
+    for (int i = 0; i < N; ++i) dlmin[i] = -dlmin[i];
+    v_d_u(N, bt, dlmin, 0, ule, 'C', g0t);                             /* g(0,t) */
+    free(drmax); free(drmin); free(dlmax); free(dlmin);
+    free(vlh); free(uu); free(vv); free(dvvd); free(bt); free(vri);
+    return 0;
+}
+
+/* dyn_measure (src/dqmc_measure/dyn_measure.f90:1-101): the density-density
+ * correlation znn_tau(imj, no_i, no_j, nt), the only active observable */
+static void dyn_measure(orc_chain *c, int nt, const zc *gt0, const zc *g0t, const zc *gtt, const zc *g00) {
+    const orc_model *m = c->m;
+    const orc_latt *L = &m->L;
+    int N = m->ndim, lq = m->lq;
+    if (nt > m->ntdm + 1) return;     /* outside znn_tau's nt range (dyntau < beta) */
+    double sgn = creal(c->phase) < 0.0 ? -1.0 : 1.0;
+    zc zphi = (sgn / creal(c->phase)) * c->phase;
+    zc *z = zalloc((size_t)lq * 4);
+    for (int j = 0; j < N; ++j) {
+        int nu_j = L->list[j * 2 + 0], no_j = L->list[j * 2 + 1];
+        for (int i = 0; i < N; ++i) {
+            int nu_i = L->list[i * 2 + 0], no_i = L->list[i * 2 + 1];
+            int imj = L->imj[(nu_i - 1) * L->ncell + (nu_j - 1)];
+            z[(imj - 1) + lq * (no_i - 1) + 2 * lq * (no_j - 1)] +=
+                (0.5 - creal(gtt[ZIDX(i, i, N)])) * (0.5 - creal(g00[ZIDX(j, j, N)]))
+                - (1.0 / m->p.nflr) * g0t[ZIDX(j, i, N)] * gt0[ZIDX(i, j, N)];
+        }
+    }
+    zc *bin = c->znn_tau_bin + (size_t)4 * lq * (nt - 1);
+    for (int k = 0; k < 4 * lq; ++k) bin[k] += z[k] * zphi;
+    free(z);
+}
+
+/* The unequal-time pass of dqmc_sweep (src/dqmc_ft_ctrl.f90:97-101):
+ * push_stage, dqmc_ft_sweep_0b(lupdate = F, lmeasure_equaltime = F,
+ * lmeasure_dyn = T) with dyn.f90 and green_tau at the stabilisation points,
+ * pop_stage (src/dqmc_ft_core.f90:290-312). */
+int orc_sweep_dyn(orc_chain *c) {
+    const orc_model *m = c->m;
+    int N = m->ndim, nst = m->nst;
+    size_t NN = (size_t)N * N;
+    if (!m->p.ltau) return -1;
+    for (int n = 0; n <= nst; ++n) {   /* push_stage */
+        memcpy(c->Ust_b[n], c->Ust[n], sizeof(zc) * NN);
+        memcpy(c->Vst_b[n], c->Vst[n], sizeof(zc) * NN);
+        memcpy(c->Dst_b[n], c->Dst[n], sizeof(double) * N);
+        c->logdetQst_b[n] = c->logdetQst[n];
+    }
+    memcpy(c->gf_b, c->gf, sizeof(zc) * NN);
+    zc *gtmp = zalloc(NN), *ul = zalloc(NN), *vl = zalloc(NN);
+    double *dl = calloc(N, sizeof(double));
+    if (nst > 0) {
+        memset(c->Ust[0], 0, sizeof(zc) * NN);
+        memset(c->Vst[0], 0, sizeof(zc) * NN);
+        for (int i = 0; i < N; ++i) { c->Ust[0][ZIDX(i, i, N)] = 1; c->Vst[0][ZIDX(i, i, N)] = 1; c->Dst[0][i] = 1; }
+        c->logdetQst[0] = 0;
+    }
+    memcpy(c->g00, c->gf, sizeof(zc) * NN);
+    memcpy(c->gt0, c->gf, sizeof(zc) * NN);
+    memcpy(c->g0t, c->gf, sizeof(zc) * NN);
+    for (int i = 0; i < N; ++i) c->g0t[ZIDX(i, i, N)] -= 1.0;
+    dyn_measure(c, 1, c->gt0, c->g0t, c->gf, c->g00);
+    for (int nt = 1; nt <= m->ltrot; ++nt) {
+        h0_half(c, ORC_LEFT_FORWARD, ORC_RIGHT_BACKWARD, 0);
+        if (m->lwrapu) {
+            u_prop(m, c->conf, ORC_LEFT_FORWARD, nt, c->gf, N);
+            u_prop(m, c->conf, ORC_RIGHT_BACKWARD, nt, c->gf, N);
+        }
+        h0_half(c, ORC_LEFT_FORWARD, ORC_RIGHT_BACKWARD, 1);
+        if (m->iwrap_nt[nt] > 0) {
+            int n = m->iwrap_nt[nt];
+            memcpy(vl, c->Vst[n], sizeof(zc) * NN);
+            memcpy(dl, c->Dst[n], sizeof(double) * N);
+            memcpy(ul, c->Ust[n], sizeof(zc) * NN);
+            zc ldl = c->logdetQst[n];
+            orc_stablize_0b(c, n);
+            zc lw;
+            green_tau(N, c->Ust[n], c->Dst[n], c->Vst[n], vl, dl, ul, c->g00, c->gt0, c->g0t, gtmp,
+                      c->logdetQst[n], ldl, &lw);
+            record_wrap(c, gtmp, lw);
+        } else {
+            bmat_left_forward(c, nt, nt, c->gt0);
+            bmat_right_backward(c, nt, nt, c->g0t);
+        }
+        dyn_measure(c, nt + 1, c->gt0, c->g0t, c->gf, c->g00);
+    }
+    for (int n = 0; n <= nst; ++n) {   /* pop_stage */
+        memcpy(c->Ust[n], c->Ust_b[n], sizeof(zc) * NN);
+        memcpy(c->Vst[n], c->Vst_b[n], sizeof(zc) * NN);
+        memcpy(c->Dst[n], c->Dst_b[n], sizeof(double) * N);
+        c->logdetQst[n] = c->logdetQst_b[n];
+    }
+    memcpy(c->gf, c->gf_b, sizeof(zc) * NN);
+    free(gtmp); free(ul); free(vl); free(dl);
+    return 0;
+}
+
+/* znn_tau_bin (lq, 2, 2, ntdm+1), Fortran order, complex as re/im pairs */
+int orc_dyn_bins(const orc_chain *c, double *out) {
+    if (!c->m->p.ltau) return -1;
+    memcpy(out, c->znn_tau_bin, sizeof(zc) * (size_t)c->m->lq * 4 * (c->m->ntdm + 1));
+    return 0;
+}
+
+/* G(0,0), G(tau,0), G(0,tau) of the last unequal-time pass (any may be NULL) */
+int orc_dyn_mats(const orc_chain *c, double *g00, double *gt0, double *g0t) {
+    if (!c->m->p.ltau) return -1;
+    size_t b = sizeof(zc) * (size_t)c->m->ndim * c->m->ndim;
+    if (g00) memcpy(g00, c->g00, b);
+    if (gt0) memcpy(gt0, c->gt0, b);
+    if (g0t) memcpy(g0t, c->g0t, b);
+    return 0;
+}
+
+/* green_tau on given factors (for tests) */
+int orc_green_tau(int n, const double *ur, const double *dr, const double *vr, const double *vl, const double *dl,
+                  const double *ul, double *g00, double *gt0, double *g0t, double *gtt, const double *logdetqr,
+                  const double *logdetql, double *logw) {
+    zc lw;
+    int info = green_tau(n, (const zc *)ur, dr, (const zc *)vr, (const zc *)vl, dl, (const zc *)ul, (zc *)g00,
+                         (zc *)gt0, (zc *)g0t, (zc *)gtt, logdetqr[0] + I * logdetqr[1],
+                         logdetql[0] + I * logdetql[1], &lw);
+    logw[0] = creal(lw); logw[1] = cimag(lw);
+    return info;
 }
 
 /* dqmc_ft_sweep_0b (src/dqmc_ft_core/dqmc_ft_sweep_0b.f90:1-288), ltau off */

@@ -35,6 +35,7 @@ struct orc_model {
     orc_params p;
     orc_latt L;
     int ndim, lq, ltrot, nst, nublock, ne;
+    int ntdm;        /* nint(dyntau / dtau) when ltau (src/model_para.f90:455-459) */
     int lwrapT, lwrapu;
     int *iwrap_nt;   /* [ltrot+1] */
     int *wrap_step;  /* [nst][2] 1-based slice range */
@@ -82,6 +83,12 @@ struct orc_chain {
     zc **Pst;                 /* Ust(0:nst) of the projective stack, N x ne */
     double *logwDV;           /* logwDV(0:nst) */
     double acc_v, prop_v;     /* main_obs(4) */
+    /* unequal-time measurement (ltau): G(0,0), G(tau,0), G(0,tau), the
+     * znn_tau_bin(lq,2,2,ntdm+1) bins and the push_stage copies */
+    zc *g00, *gt0, *g0t;
+    zc *znn_tau_bin;
+    zc **Ust_b, **Vst_b, *gf_b, *logdetQst_b;
+    double **Dst_b;
 };
 
 /* linear algebra helpers (orc_linalg.c) */

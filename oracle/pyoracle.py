@@ -40,6 +40,7 @@ class OrcParams(C.Structure):
         ("nwrap", C.c_int32), ("nsweep", C.c_int32), ("nbin", C.c_int32), ("nublock", C.c_int32),
         ("update", C.c_int32), ("kinetic", C.c_int32), ("hs", C.c_int32),
         ("proj", C.c_int32), ("lprojv", C.c_int32), ("obs_mid_len", C.c_int32),
+        ("ltau", C.c_int32), ("dyntau", C.c_double),
     ]
 
 
@@ -75,6 +76,10 @@ def lib() -> C.CDLL:
             getattr(L, name).argtypes = [vp]
         L.orc_sweep_b0.argtypes = [vp, C.c_int, C.c_int]
         L.orc_sweep_0b.argtypes = [vp, C.c_int, C.c_int]
+        L.orc_sweep_dyn.argtypes = [vp]
+        L.orc_dyn_bins.argtypes = [vp, vp]
+        L.orc_dyn_mats.argtypes = [vp, vp, vp, vp]
+        L.orc_green_tau.argtypes = [C.c_int] + [vp] * 13
         L.orc_sweep_b0_slices.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         L.orc_bins_size.argtypes = [vp]
         L.orc_bins_size.restype = C.c_int
@@ -160,7 +165,7 @@ def make_params(**kw) -> OrcParams:
              mu=0.0, rhub=0.0, rv=0.0, alpha=0.2, theta=0.0, xmag=0.0, flux_x=0.0, flux_y=0.0,
              dimer=0.0, rndness=0.0, nflr=2, lproju=0, lstabilize=1, nwrap=10, nsweep=20, nbin=10,
              nublock=0, update=DELAY, kinetic=CHECKERBOARD, hs=HS_GENERAL4, proj=0, lprojv=0,
-             obs_mid_len=1)
+             obs_mid_len=1, ltau=0, dyntau=0.0)
     d.update(kw)
     return OrcParams(**d)
 
@@ -177,6 +182,8 @@ class Model:
          self.nn_nf, self.nn_lf, self.nsub, self.z_plq) = (int(x) for x in dims)
         self.ne = self.ndim // 2 + int(self.params.nu * self.ndim / 8.0)   # model_para.f90:376
         self.proj = bool(self.params.proj)
+        # src/model_para.f90:455-459
+        self.ntdm = max(0, int(round(self.params.dyntau / self.params.dtau))) if self.params.ltau else 0
 
     def __del__(self):
         if getattr(self, "ptr", None):
@@ -357,6 +364,27 @@ class Chain:
 
     def obser_init(self) -> None:
         lib().orc_obser_init(self._p)
+
+    # ---- unequal-time measurement (ltau) ----
+    def sweep_dyn(self) -> None:
+        """push_stage, 0b sweep without updates measuring znn_tau, pop_stage."""
+        if lib().orc_sweep_dyn(self._p) != 0:
+            raise RuntimeError("sweep_dyn needs ltau = 1")
+
+    def dyn_bins(self) -> np.ndarray:
+        """znn_tau_bin as [ntdm+1, 2 (no_j), 2 (no_i), lq] complex."""
+        m = self.model
+        out = np.zeros(m.lq * 4 * (m.ntdm + 1), complex)
+        if lib().orc_dyn_bins(self._p, _ptr(out)) != 0:
+            raise RuntimeError("dyn_bins needs ltau = 1")
+        return out.reshape(m.ntdm + 1, 2, 2, m.lq)
+
+    def dyn_mats(self):
+        """(G(0,0), G(tau,0), G(0,tau)) after the last unequal-time pass."""
+        N = self.model.ndim
+        g00, gt0, g0t = (np.zeros((N, N), complex, order="F") for _ in range(3))
+        lib().orc_dyn_mats(self._p, _ptr(g00), _ptr(gt0), _ptr(g0t))
+        return g00, gt0, g0t
 
     def update(self, nt: int) -> np.ndarray:
         acc = np.zeros(self.model.ndim, np.int32)

@@ -59,6 +59,10 @@ extern "C" int dqmc_params_derive(dqmc_params* p) {
     else if (p->hs == DQMC_HS_EXACT && p->nflr == 2) p->lcomp = 2;
     else p->lcomp = 4;
     if (p->obs_mid_len <= 0) p->obs_mid_len = 1;
+    p->ntdm = p->ltau ? (int)std::lround(p->dyntau / p->dtau) : 0;
+    if (p->ntdm < 0) p->ntdm = 0;
+    if (p->ltau && p->proj) return fail(DQMC_EINVAL, "unequal-time measurement (ltau) is supported on the finite-temperature path only");
+    if (p->ltau && p->nst < 1) return fail(DQMC_EINVAL, "unequal-time measurement (ltau) needs lstabilize and ltrot >= nwrap");
     if (p->proj && p->nst < 1) return fail(DQMC_EINVAL, "the projective sweep needs lstabilize and ltrot >= nwrap");
     if (!p->proj && p->rv != 0.0) return fail(DQMC_EINVAL, "the t-V bond field (rv != 0) is supported on the projective path only");
     if (p->rv < 0.0) return fail(DQMC_EINVAL, "rv must be >= 0 (acosh(exp(dtau rv / 2)))");
@@ -407,6 +411,7 @@ static int upload_model(HostModel& m) {
     d.N = m.N; d.lq = m.lq; d.nsub = m.nsub; d.l1 = p.l1; d.l2 = p.l2; d.nn_nf = m.nn_nf; d.nn_lf = m.nn_lf;
     d.z_plq = m.z_plq; d.nsn = m.nsn; d.lcomp = m.lcomp; d.nflr = p.nflr; d.lproju = p.lproju;
     d.kinetic = p.kinetic; d.update = p.update; d.nublock = m.nublock_dev; d.ltrot = p.ltrot; d.nst = p.nst;
+    d.ntdm = p.ltau ? p.ntdm : -1;
     d.nwrap = p.nwrap; d.lwrapT = (p.rt != 0.0); d.lwrapu = (p.rhub != 0.0);
     d.phase_on = (p.rhub > 0.0) ? 1 : 0;
     d.rt = p.rt; d.rv = p.rv; d.t2 = p.t2; d.theta = p.theta * M_PI;
@@ -762,6 +767,8 @@ struct dqmc_handle {
     std::vector<ChainHost> chains;
     ChainDev* d_chains = nullptr;
     int* d_slotmap = nullptr;
+    int* d_slotmap_b = nullptr;      // push_stage copy of the slot map (ltau)
+    int after_b0 = 0;                // the stack holds the left factors of a b0 sweep
     std::vector<void*> allocs;
     cudaStream_t st = nullptr;
     int nch = 0, maxN = 0, ltrot = 0, nst = 0, nwrap = 0, nnf_max = 0;
@@ -870,10 +877,11 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
             return fail(DQMC_EINVAL, "all parameter sets of a handle must share ltrot and nwrap");
         } else if (m->p.lattice != h->models[0]->p.lattice || m->p.kinetic != h->models[0]->p.kinetic ||
                    (m->p.rt == 0.0) != (h->models[0]->p.rt == 0.0) || (m->p.rhub == 0.0) != (h->models[0]->p.rhub == 0.0) ||
-                   (m->p.rv == 0.0) != (h->models[0]->p.rv == 0.0) || (m->p.proj != 0) != (h->models[0]->p.proj != 0)) {
+                   (m->p.rv == 0.0) != (h->models[0]->p.rv == 0.0) || (m->p.proj != 0) != (h->models[0]->p.proj != 0) ||
+                   (m->p.ltau != 0) != (h->models[0]->p.ltau != 0)) {
             dqmc_gpu_destroy(h);
             return fail(DQMC_EINVAL, "all parameter sets of a handle must share lattice kind, kinetic propagator, "
-                                     "the presence of the U / V / hopping terms and the projective flag");
+                                     "the presence of the U / V / hopping terms, the projective flag and ltau");
         }
         if ((rc = upload_model(*m))) { dqmc_gpu_destroy(h); return rc; }
         h->maxN = std::max(h->maxN, m->N);
@@ -893,6 +901,7 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
     h->nch = n_chains;
     int nst = h->nst, lt = h->ltrot;
     h->d_slotmap = (int*)dalloc(h, sizeof(int) * (nst + 2));
+    if (h->models[0]->p.ltau) h->d_slotmap_b = (int*)dalloc(h, sizeof(int) * (nst + 2));
     {
         std::vector<int> sm(nst + 2);
         for (int i = 0; i < nst + 2; ++i) sm[i] = i;
@@ -924,6 +933,17 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
             d.logdetQ = (double2*)dalloc(h, (size_t)(nst + 2) * z);
             d.A = (double2*)dalloc(h, (size_t)N * m->nublock_dev * z);
             d.B = (double2*)dalloc(h, (size_t)N * m->nublock_dev * z);
+            if (m->p.ltau) {
+                d.gt0 = (double2*)dalloc(h, NN * z);
+                d.g0t = (double2*)dalloc(h, NN * z);
+                d.g00 = (double2*)dalloc(h, NN * z);
+                d.dynbins = (double2*)dalloc(h, (size_t)m->lq * 4 * (m->p.ntdm + 1) * z);
+                d.Ub = (double2*)dalloc(h, (size_t)(nst + 2) * NN * z);
+                d.Vb = (double2*)dalloc(h, (size_t)(nst + 2) * NN * z);
+                d.Db = (double*)dalloc(h, (size_t)(nst + 2) * N * sizeof(double));
+                d.ldqb = (double2*)dalloc(h, (size_t)(nst + 2) * z);
+                d.Gb = (double2*)dalloc(h, NN * z);
+            }
         } else {
             size_t Nne = (size_t)N * ne;
             d.UR = (double2*)dalloc(h, Nne * z);
@@ -1075,7 +1095,7 @@ static PropProg prog_bmat_hc(const HostModel& m, int nt1, int nt2) {
     return p;
 }
 
-enum { MAT_G = 0, MAT_U = 100, MAT_V = 400 };
+enum { MAT_G = 0, MAT_GT0 = 15, MAT_G0T = 16, MAT_U = 100, MAT_V = 400 };   // ids of chain_access.cuh
 
 // one projective update call (a bond family, or the site field when nf = 0):
 // window count and per-walker CTA counts of the window GEMMs, maximised over
@@ -1349,6 +1369,7 @@ static void enqueue_proj_0b(dqmc_handle* h, int lupdate, int lmeasure) {
 
 extern "C" int dqmc_gpu_sweep_start(dqmc_handle* h) {
     if (!h) return fail(DQMC_EINVAL, "null handle");
+    h->after_b0 = 0;
     if (h->proj) return proj_sweep_start(h);
     const HostModel& m = *h->models[0];
     {
@@ -1431,11 +1452,96 @@ static void enqueue_0b(dqmc_handle* h, int lupdate, int lmeasure) {
     }
 }
 
+static int chk_chain(dqmc_handle* h, int c);
+
+// one stabilisation of the unequal-time pass (dqmc_ft_sweep_0b.f90:145-230 with
+// lmeasure_dyn): new right factor into the spare slot, green_tau from (new R,
+// old L), wrap check, swap
+static void stab_dyn(dqmc_handle* h, int n) {
+    const HostModel& m = *h->models[0];
+    int spare = h->nst + 1;
+    launch_copy_mat(h->d_chains, h->nch, 2 /*W0*/, MAT_U + (n - 1), 0, h->st);
+    PropProg p = prog_bmat(m, m.wrap_step[(n - 1) * 2 + 1], m.wrap_step[(n - 1) * 2]);
+    launch_prog(h, 2, p, 0);
+    launch_stab_slots(h->d_chains, h->nch, n - 1, spare, h->st);
+    launch_green_tau(h->d_chains, h->nch, spare, n, h->st);
+    launch_wrap_check(h->d_chains, h->nch, 1, h->st);
+    launch_swap_slots(h->d_slotmap, n, spare, h->st);
+}
+
+// The unequal-time pass of dqmc_sweep (src/dqmc_ft_ctrl.f90:97-101): push_stage,
+// dqmc_ft_sweep_0b(lupdate = F, lmeasure_equaltime = F, lmeasure_dyn = T) with
+// dyn.f90 (G(t',0) = B(t',t) G(t,0), G(0,t') = G(0,t) B(t',t)^-1 between
+// stabilisations, green_tau at them) and dyn_measure at every time index, then
+// pop_stage (src/dqmc_ft_core.f90:290-312).
+static void enqueue_dyn(dqmc_handle* h) {
+    const HostModel& m = *h->models[0];
+    const int lt = h->ltrot, nslots = h->nst + 2;
+    launch_stage(h->d_chains, h->nch, nslots, 0, h->st);
+    cudaMemcpyAsync(h->d_slotmap_b, h->d_slotmap, sizeof(int) * nslots, cudaMemcpyDeviceToDevice, h->st);
+    launch_stack_identity(h->d_chains, h->nch, 0, h->st);
+    launch_dyn_init(h->d_chains, h->nch, h->st);
+    launch_dyn_measure(h->d_chains, h->nch, h->maxN, 1, h->st);
+    for (int nt = 1; nt <= lt; ++nt) {
+        PropProg pl; pl.n = 0; PropProg pr; pr.n = 0;
+        prog_k(m, pl, PW_FWD, 0);
+        prog_v(m, pl, PW_FWD, nt);
+        prog_k(m, pl, PW_FWD, 1);
+        prog_k(m, pr, PW_INV, 0);
+        prog_v(m, pr, PW_INV, nt);
+        prog_k(m, pr, PW_INV, 1);
+        launch_prog(h, MAT_G, pl, 0);
+        launch_prog(h, MAT_G, pr, 1);
+        if (m.iwrap_nt[nt] > 0) {
+            stab_dyn(h, m.iwrap_nt[nt]);
+        } else {
+            launch_prog(h, MAT_GT0, pl, 0);     // Bmat_left_forward(nt, nt, gt0)
+            launch_prog(h, MAT_G0T, pr, 1);     // Bmat_right_backward(nt, nt, g0t)
+        }
+        launch_dyn_measure(h->d_chains, h->nch, h->maxN, nt + 1, h->st);
+    }
+    launch_stage(h->d_chains, h->nch, nslots, 1, h->st);
+    cudaMemcpyAsync(h->d_slotmap, h->d_slotmap_b, sizeof(int) * nslots, cudaMemcpyDeviceToDevice, h->st);
+}
+
+extern "C" int dqmc_gpu_sweep_dyn(dqmc_handle* h) {
+    if (!h) return fail(DQMC_EINVAL, "null handle");
+    if (!h->started) return fail(DQMC_ESTATE, "sweep before sweep_start");
+    if (h->proj || !h->models[0]->p.ltau) return fail(DQMC_ESTATE, "the unequal-time pass needs a finite-temperature handle with ltau = 1");
+    if (!h->after_b0) return fail(DQMC_ESTATE, "the unequal-time pass follows a b0 sweep (it needs the b0 sweep's left factors)");
+    enqueue_dyn(h);
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaGetLastError());
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_get_dyn_bins(dqmc_handle* h, int chain, double* out) {
+    int rc = chk_chain(h, chain); if (rc) return rc;
+    if (!out) return fail(DQMC_EINVAL, "null output");
+    const HostModel& m = *h->models[h->chains[chain].model];
+    if (!m.p.ltau) return fail(DQMC_ESTATE, "ltau = 0: no unequal-time bins");
+    CK(copy_sync(h->st, out, h->chains[chain].dev.dynbins, (size_t)m.lq * 4 * (m.p.ntdm + 1) * sizeof(double2),
+                 cudaMemcpyDeviceToHost));
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_get_dyn_mats(dqmc_handle* h, int chain, double* g00, double* gt0, double* g0t) {
+    int rc = chk_chain(h, chain); if (rc) return rc;
+    const ChainDev& d = h->chains[chain].dev;
+    if (!d.gt0) return fail(DQMC_ESTATE, "ltau = 0: no unequal-time Green's functions");
+    const size_t b = (size_t)d.N * d.N * sizeof(double2);
+    if (g00) CK(copy_sync(h->st, g00, d.g00, b, cudaMemcpyDeviceToHost));
+    if (gt0) CK(copy_sync(h->st, gt0, d.gt0, b, cudaMemcpyDeviceToHost));
+    if (g0t) CK(copy_sync(h->st, g0t, d.g0t, b, cudaMemcpyDeviceToHost));
+    return DQMC_OK;
+}
+
 extern "C" int dqmc_gpu_sweep_b0(dqmc_handle* h, int lupdate, int lmeasure) {
     if (!h) return fail(DQMC_EINVAL, "null handle");
     if (!h->started) return fail(DQMC_ESTATE, "sweep before sweep_start");
     if (h->proj) enqueue_proj_b0(h, lupdate, lmeasure);
     else enqueue_b0(h, lupdate, lmeasure);
+    h->after_b0 = 1;
     CK(cudaStreamSynchronize(h->st));
     CK(cudaGetLastError());
     return DQMC_OK;
@@ -1446,6 +1552,7 @@ extern "C" int dqmc_gpu_sweep_0b(dqmc_handle* h, int lupdate, int lmeasure) {
     if (!h->started) return fail(DQMC_ESTATE, "sweep before sweep_start");
     if (h->proj) enqueue_proj_0b(h, lupdate, lmeasure);
     else enqueue_0b(h, lupdate, lmeasure);
+    h->after_b0 = 0;
     CK(cudaStreamSynchronize(h->st));
     CK(cudaGetLastError());
     return DQMC_OK;
@@ -1464,6 +1571,7 @@ extern "C" int dqmc_gpu_sweeps(dqmc_handle* h, int n, int lmeasure) {
             enqueue_proj_0b(h, 1, lmeasure);
         } else {
             enqueue_b0(h, 1, lmeasure);
+            if (lmeasure && h->models[0]->p.ltau) enqueue_dyn(h);   // dqmc_sweep (src/dqmc_ft_ctrl.f90:97-101)
             enqueue_0b(h, 1, lmeasure);
         }
         CK(cudaStreamEndCapture(h->st, &g));
@@ -1474,6 +1582,7 @@ extern "C" int dqmc_gpu_sweeps(dqmc_handle* h, int n, int lmeasure) {
         cudaGraphDestroy(g);
         h->graph_meas = lmeasure + 2 * h->rec_on;
     }
+    h->after_b0 = 0;
     CK(cudaEventRecord(h->ev0, h->st));
     for (int i = 0; i < n; ++i) CK(cudaGraphLaunch(h->sweep_graph, h->st));
     CK(cudaEventRecord(h->ev1, h->st));
@@ -1823,6 +1932,7 @@ extern "C" int dqmc_gpu_sweep_profile(dqmc_handle* h, int nsweeps, int lmeasure,
     for (int s = 0; s < nsweeps; ++s) {
         if (h->proj) { enqueue_proj_b0(h, 1, lmeasure); enqueue_proj_0b(h, 1, lmeasure); }
         else { enqueue_b0(h, 1, lmeasure); enqueue_0b(h, 1, lmeasure); }
+        h->after_b0 = 0;
     }
     const int ok = h->tm_on;
     h->tm_on = 0;
@@ -2327,6 +2437,7 @@ extern "C" int dqmc_gpu_sweep_learned(dqmc_handle* h, dqmc_nn* nn, int n, int lu
     for (int i = 0; i < n; ++i) {
         enqueue_b0(h, lupdate, lmeasure);
         enqueue_0b_blocks(h, nn, lupdate, lmeasure, (int)(blk_next(h->blk_rng) & 1));
+        h->after_b0 = 0;
     }
     CK(cudaEventRecord(e1, h->st));
     CK(cudaStreamSynchronize(h->st));

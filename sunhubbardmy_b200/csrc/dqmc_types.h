@@ -10,6 +10,7 @@
 struct ModelDev {
     int N, lq, nsub, l1, l2, nn_nf, nn_lf, z_plq, nsn;
     int lcomp, nflr, lproju, kinetic, update, nublock, ltrot, nst, nwrap;
+    int ntdm;                            // unequal-time bins cover nt = 1 .. ntdm+1 (-1: ltau off)
     int lwrapT, lwrapu, phase_on;        // phase_on: rhub > 0 (set_phase multiplies conf phases)
     double rt, rv, t2, theta;
     // HS constants (src/dqmc_config_u/dqmc_set_conf.f90)
@@ -85,6 +86,17 @@ struct ChainDev {
     int* blk;
     double2* Gsave;            // G at the block's first slice
     int32_t* confsave;         // HS field of the block's slices
+    // unequal-time measurement (params.ltau): G(tau,0), G(0,tau), G(0,0), the
+    // znn_tau bins (lq, 2, 2, ntdm+1) and push_stage copies of the stack and G
+    double2* gt0;
+    double2* g0t;
+    double2* g00;
+    double2* dynbins;
+    double2* Ub;
+    double2* Vb;
+    double* Db;
+    double2* ldqb;
+    double2* Gb;
 };
 
 // indices into ChainDev::stats

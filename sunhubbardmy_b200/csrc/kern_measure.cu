@@ -246,20 +246,25 @@ __global__ void k_bins_clear(const ChainDev* __restrict__ chains, int nbins) {
     (void)nbins;
     const int nb = 10 + 20 * c.md->lq + 4;     // this chain's own bin count
     for (int e = threadIdx.x; e < nb; e += blockDim.x) c.bins[e] = cmk(0, 0);
+    if (c.dynbins) {
+        const int nd = 4 * c.md->lq * (c.md->ntdm + 1);
+        for (int e = threadIdx.x; e < nd; e += blockDim.x) c.dynbins[e] = cmk(0, 0);
+    }
     if (threadIdx.x == 0) c.stats[ST_NOBS] = 0.0;
 }
 
-// GT = G^T per chain, 32 x 32 tiles through shared memory (odd pitch)
-__global__ void __launch_bounds__(256) k_transpose_g(const ChainDev* __restrict__ chains) {
+// GT = (matrix src_id)^T per chain, 32 x 32 tiles through shared memory (odd pitch)
+__global__ void __launch_bounds__(256) k_transpose_g(const ChainDev* __restrict__ chains, int src_id) {
     __shared__ double2 t[32][33];
     const ChainDev& c = chains[blockIdx.z];
+    const double2* Src = chain_mat(c, src_id);
     const int N = c.N;
     const int r0 = blockIdx.x * 32, s0 = blockIdx.y * 32;
     if (r0 >= N || s0 >= N) return;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     for (int k = ty; k < 32; k += 8) {
         const int r = r0 + tx, s_ = s0 + k;
-        if (r < N && s_ < N) t[k][tx] = c.G[(size_t)r + (size_t)N * s_];
+        if (r < N && s_ < N) t[k][tx] = Src[(size_t)r + (size_t)N * s_];
     }
     __syncthreads();
     for (int k = ty; k < 32; k += 8) {
@@ -270,9 +275,48 @@ __global__ void __launch_bounds__(256) k_transpose_g(const ChainDev* __restrict_
 
 void launch_measure(const ChainDev* chains, int nchains, int maxN, int ctas_per_chain, cudaStream_t st) {
     const int nt = (maxN + 31) / 32;
-    k_transpose_g<<<dim3(nt, nt, nchains), 256, 0, st>>>(chains);
+    k_transpose_g<<<dim3(nt, nt, nchains), 256, 0, st>>>(chains, MAT_G);
     dim3 grid(ctas_per_chain, nchains);
     k_measure<<<grid, 256, 0, st>>>(chains);
+}
+
+// dyn_measure (src/dqmc_measure/dyn_measure.f90:1-101) at time index nt: the
+// density correlation znn_tau(imj, no_i, no_j, nt) +=
+//   (1/2 - Re G(t,t)_ii)(1/2 - Re G(0,0)_jj) - G(0,t)_ji G(t,0)_ij / nflr,
+// weighted with zphi; G(0,t)^T is in GT.  One thread per bin, cells j in
+// order (the reference's summation order for a bin).
+__global__ void __launch_bounds__(256) k_dyn_measure(const ChainDev* __restrict__ chains, int nt) {
+    const ChainDev& c = chains[blockIdx.y];
+    const ModelDev& md = *c.md;
+    if (nt > md.ntdm + 1) return;
+    const int N = c.N, lq = md.lq, nsub = md.nsub, l1 = md.l1, l2 = md.l2;
+    const double2 phase = cmk(c.stats[ST_PHASE_RE], c.stats[ST_PHASE_IM]);
+    const double sgn = phase.x < 0.0 ? -1.0 : 1.0;
+    const double2 zphi = cscale(phase, sgn / phase.x);
+    const double fn = 1.0 / (double)md.nflr;
+    const double2 *G = c.G, *GT = c.GT, *gt0 = c.gt0, *g00 = c.g00;
+    double2* bin = c.dynbins + (size_t)4 * lq * (nt - 1);
+    const int nbin = lq * nsub * nsub;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nbin; b += gridDim.x * blockDim.x) {
+        const int d = b % lq, ab = b / lq, a = ab % nsub, bb = ab / nsub;
+        const int dxp = d / l2 + 1, dyp = d % l2 + 1;
+        double2 z = cmk(0, 0);
+#pragma unroll 4
+        for (int cj = 0; cj < lq; ++cj) {
+            const int i = cell_shift(cj, dxp, dyp, l1, l2) * nsub + a, j = cj * nsub + bb;
+            const size_t o = (size_t)i + (size_t)N * j;
+            const double v = (0.5 - G[(size_t)i * (N + 1)].x) * (0.5 - g00[(size_t)j * (N + 1)].x);
+            z = csub(cadd(z, cmk(v, 0.0)), cmul(cscale(GT[o], fn), gt0[o]));
+        }
+        const size_t k = (size_t)d + (size_t)lq * a + (size_t)2 * lq * bb;
+        bin[k] = cfma(z, zphi, bin[k]);
+    }
+}
+
+void launch_dyn_measure(const ChainDev* chains, int nchains, int maxN, int nt, cudaStream_t st) {
+    const int ntl = (maxN + 31) / 32;
+    k_transpose_g<<<dim3(ntl, ntl, nchains), 256, 0, st>>>(chains, MAT_G0T);
+    k_dyn_measure<<<dim3(2, nchains), 256, 0, st>>>(chains, nt);
 }
 
 void launch_bins_clear(const ChainDev* chains, int nchains, int nbins, cudaStream_t st) {

@@ -214,6 +214,171 @@ __global__ void __launch_bounds__(256, 2) k_green(const ChainDev* __restrict__ c
     }
 }
 
+// green_tau (src/dqmc_ft_core/green_tau.f90:1-136) at a stabilisation point of
+// the unequal-time pass: from the right factors (slot nr: UR DR VR = B(tau,0))
+// and the left ones (slot nl: UL DL VL), with d = dmax dmin split as in
+// green_equaltime,
+//   G(tau,tau) = UL dlmax^-1 M^-1 drmax^-1 UR^H          -> Gnew
+//   G(tau,0)   = UL dlmax^-1 M^-1 drmin VR                -> gt0
+//   G(0,0)     = VR^-1 drmax^-1 M2^-1 dlmax^-1 (VL^H)^-1  -> g00
+//   G(0,tau)   = -VR^-1 drmax^-1 M2^-1 dlmin UL^H         -> g0t
+// with M = drmax^-1 UR^H UL dlmax^-1 + drmin VR VL^H dlmin and
+// M2 = dlmax^-1 (VR VL^H)^-1 drmax^-1 + dlmin UL^H UR drmin.  Inverses are
+// taken through QR factors (solves with Q^H and R), as in k_green, instead of
+// LU; log det M (the new log weight) as in k_green.  Scratch W0..W4 (W5 holds
+// the reflector blocks of the QR).
+__global__ void __launch_bounds__(256, 2) k_green_tau(const ChainDev* __restrict__ chains, int nr, int nl) {
+    extern __shared__ double2 ssm[];
+    const ChainDev& c = chains[blockIdx.x];
+    const int N = c.N, tid = threadIdx.x, nth = blockDim.x;
+    const size_t NN = (size_t)N * N;
+    double2* buf = ssm;
+    StabSmem* S = (StabSmem*)(ssm + ((QR_PANEL_ELEMS(N) > (size_t)GemmBig::SMEM_ELEMS) ? QR_PANEL_ELEMS(N) : (size_t)GemmBig::SMEM_ELEMS));
+    LinalgScratch sc = make_scratch(c);
+    nr = c.slotmap[nr];
+    nl = c.slotmap[nl];
+    const double2* UR = c.U + (size_t)nr * NN;
+    const double2* VR = c.V + (size_t)nr * NN;
+    const double* DR = c.D + (size_t)nr * N;
+    const double2* UL = c.U + (size_t)nl * NN;
+    const double2* VL = c.V + (size_t)nl * NN;
+    const double* DL = c.D + (size_t)nl * N;
+    double* drmax = c.vecs + 0 * N;
+    double* drmin = c.vecs + 1 * N;
+    double* dlmax = c.vecs + 2 * N;
+    double* dlmin = c.vecs + 3 * N;
+    double2 *W0 = c.W[0], *W1 = c.W[1], *W2 = c.W[2], *W3 = c.W[3], *W4 = c.W[4];
+    double slog = 0.0;
+    for (int i = tid; i < N; i += nth) {
+        double a, b;
+        dminmax(DR[i], a, b);
+        drmax[i] = a; drmin[i] = b;
+        slog += log(a);
+        dminmax(DL[i], a, b);
+        dlmax[i] = a; dlmin[i] = b;
+        slog += log(a);
+    }
+    __syncthreads();
+    ZGemmArgs g;
+    g.M = N; g.N = N; g.K = N; g.alpha = cmk(1, 0); g.beta = cmk(0, 0); g.lda = N; g.ldb = N; g.ldc = N;
+    auto gemm = [&](const double2* A, int opA, const double2* B, int opB, double2* C, double alpha) {
+        g.A = A; g.opA = opA; g.B = B; g.opB = opB; g.C = C; g.alpha = cmk(alpha, 0);
+        zgemm_cta<GemmBig>(g, 0, 1, buf);
+    };
+    // uu = UR^H UL (W1, kept for M2), vv = VR VL^H (W2)
+    gemm(UR, OP_C, UL, OP_N, W1, 1.0);
+    gemm(VR, OP_N, VL, OP_C, W2, 1.0);
+    for (size_t e = tid; e < NN; e += nth) {
+        const int i = (int)(e % N), j = (int)(e / N);
+        W0[e] = cadd(cscale(W1[e], 1.0 / (drmax[i] * dlmax[j])), cscale(W2[e], drmin[i] * dlmin[j]));
+    }
+    slog = block_sum(slog, S->red);
+    __syncthreads();
+    cta_qr64(W0, N, sc, buf, buf, &S->L);
+    double2 ldm = cta_logdet_q(sc.tau, N, S->red);
+    double2 lr = cmk(0, 0);
+    for (int i = tid; i < N; i += nth) {
+        const double r = W0[MIDX(i, i, N)].x;
+        lr = cadd(lr, cmk(log(fabs(r)), r < 0.0 ? M_PI : 0.0));
+    }
+    lr = block_csum(lr, S->red);
+    ldm = cadd(ldm, lr);
+    // X = M^-1 drmax^-1 UR^H (W2), Y = M^-1 drmin VR (W3)
+    for (size_t e = tid; e < NN; e += nth) {
+        const int i = (int)(e % N), j = (int)(e / N);
+        W2[e] = cscale(cconj(UR[MIDX(j, i, N)]), 1.0 / drmax[i]);
+        W3[e] = cscale(VR[e], drmin[i]);
+    }
+    __syncthreads();
+    cta_apply_qh64(W0, N, W2, sc, buf);
+    cta_trsm_upper(W0, N, W2, buf, &S->L);
+    cta_apply_qh64(W0, N, W3, sc, buf);
+    cta_trsm_upper(W0, N, W3, buf, &S->L);
+    // UL dlmax^-1 (W4); G(tau,tau) and G(tau,0)
+    for (size_t e = tid; e < NN; e += nth) W4[e] = cscale(UL[e], 1.0 / dlmax[(int)(e / N)]);
+    __syncthreads();
+    gemm(W4, OP_N, W2, OP_N, c.Gnew, 1.0);
+    gemm(W4, OP_N, W3, OP_N, c.gt0, 1.0);
+    // VR^-1 (W2) and (VL^H)^-1 (W3) through QR: W0 <- A, W <- I, solve
+    for (int pass = 0; pass < 2; ++pass) {
+        double2* Xi = pass == 0 ? W2 : W3;
+        for (size_t e = tid; e < NN; e += nth) {
+            const int i = (int)(e % N), j = (int)(e / N);
+            W0[e] = pass == 0 ? VR[e] : cconj(VL[MIDX(j, i, N)]);
+            Xi[e] = cmk(i == j ? 1.0 : 0.0, 0.0);
+        }
+        __syncthreads();
+        cta_qr64(W0, N, sc, buf, buf, &S->L);
+        cta_apply_qh64(W0, N, Xi, sc, buf);
+        cta_trsm_upper(W0, N, Xi, buf, &S->L);
+    }
+    // (VR VL^H)^-1 = (VL^H)^-1 VR^-1 (W4); M2 (W0)
+    gemm(W3, OP_N, W2, OP_N, W4, 1.0);
+    for (size_t e = tid; e < NN; e += nth) {
+        const int i = (int)(e % N), j = (int)(e / N);
+        W0[e] = cadd(cscale(W4[e], 1.0 / (dlmax[i] * drmax[j])), cscale(cconj(W1[MIDX(j, i, N)]), dlmin[i] * drmin[j]));
+    }
+    __syncthreads();
+    cta_qr64(W0, N, sc, buf, buf, &S->L);
+    // Z = M2^-1 dlmax^-1 (VL^H)^-1 (W3), Wm = M2^-1 (-dlmin UL^H) (W4)
+    for (size_t e = tid; e < NN; e += nth) {
+        const int i = (int)(e % N), j = (int)(e / N);
+        W3[e] = cscale(W3[e], 1.0 / dlmax[i]);
+        W4[e] = cscale(cconj(UL[MIDX(j, i, N)]), -dlmin[i]);
+    }
+    __syncthreads();
+    cta_apply_qh64(W0, N, W3, sc, buf);
+    cta_trsm_upper(W0, N, W3, buf, &S->L);
+    cta_apply_qh64(W0, N, W4, sc, buf);
+    cta_trsm_upper(W0, N, W4, buf, &S->L);
+    // VR^-1 drmax^-1 (W2); G(0,0), G(0,tau)
+    for (size_t e = tid; e < NN; e += nth) W2[e] = cscale(W2[e], 1.0 / drmax[(int)(e / N)]);
+    __syncthreads();
+    gemm(W2, OP_N, W3, OP_N, c.g00, 1.0);
+    gemm(W2, OP_N, W4, OP_N, c.g0t, 1.0);
+    if (tid == 0) {
+        double2 lw = cadd(ldm, cmk(slog, 0.0));
+        lw = cadd(lw, c.logdetQ[nr]);
+        lw = csub(lw, c.logdetQ[nl]);
+        c.stats[ST_LOGDETM_RE] = lw.x;
+        c.stats[ST_LOGDETM_IM] = lw.y;
+    }
+}
+
+// push_stage / pop_stage (src/dqmc_ft_core.f90:290-312): the whole UDV stack
+// and G to (dir 0) or from (dir 1) the chain's backup
+__global__ void k_stage(const ChainDev* __restrict__ chains, int nslots, int dir) {
+    const ChainDev& c = chains[blockIdx.y];
+    const size_t NN = (size_t)c.N * c.N, nmat = (size_t)nslots * NN;
+    const size_t stride = (size_t)gridDim.x * blockDim.x, t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double2 *u = c.U, *v = c.V, *ub = c.Ub, *vb = c.Vb, *gg = c.G, *gb = c.Gb, *lq = c.logdetQ, *lb = c.ldqb;
+    double *d = c.D, *db = c.Db;
+    if (dir == 0) {
+        for (size_t e = t0; e < nmat; e += stride) { ub[e] = u[e]; vb[e] = v[e]; }
+        for (size_t e = t0; e < NN; e += stride) gb[e] = gg[e];
+        for (size_t e = t0; e < (size_t)nslots * c.N; e += stride) db[e] = d[e];
+        for (size_t e = t0; e < (size_t)nslots; e += stride) lb[e] = lq[e];
+    } else {
+        for (size_t e = t0; e < nmat; e += stride) { u[e] = ub[e]; v[e] = vb[e]; }
+        for (size_t e = t0; e < NN; e += stride) gg[e] = gb[e];
+        for (size_t e = t0; e < (size_t)nslots * c.N; e += stride) d[e] = db[e];
+        for (size_t e = t0; e < (size_t)nslots; e += stride) lq[e] = lb[e];
+    }
+}
+
+// start of the unequal-time pass (dqmc_ft_sweep_0b.f90:39-43): g00 = gt0 = G, g0t = G - I
+__global__ void k_dyn_init(const ChainDev* __restrict__ chains) {
+    const ChainDev& c = chains[blockIdx.y];
+    const int N = c.N;
+    const size_t NN = (size_t)N * N;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < NN; e += (size_t)gridDim.x * blockDim.x) {
+        const double2 g = c.G[e];
+        c.g00[e] = g;
+        c.gt0[e] = g;
+        c.g0t[e] = ((int)(e % N) == (int)(e / N)) ? cmk(g.x - 1.0, g.y) : g;
+    }
+}
+
 // s_compare_max_z + set_phase + replacement of G (dqmc_ft_sweep_b0.f90:145-194)
 __global__ void __launch_bounds__(256) k_wrap_check(const ChainDev* __restrict__ chains, int record) {
     __shared__ double red[64];
@@ -320,6 +485,7 @@ static void stab_attrs() {
     if (g_stab_attr) return;
     cudaFuncSetAttribute(k_stab, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(k_green, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_green_tau, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(k_qr_test, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(k_zgemm_test, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     g_stab_attr = 1;
@@ -345,6 +511,19 @@ void launch_green(const ChainDev* chains, int nchains, int nr, int nl, int rmat_
     (void)rmat_u; (void)rmat_v; (void)lmat_u; (void)lmat_v;
     stab_attrs();
     k_green<<<nchains, 256, stab_smem_bytes(g_maxN), st>>>(chains, nr, nl, mode);
+}
+
+void launch_green_tau(const ChainDev* chains, int nchains, int nr, int nl, cudaStream_t st) {
+    stab_attrs();
+    k_green_tau<<<nchains, 256, stab_smem_bytes(g_maxN), st>>>(chains, nr, nl);
+}
+
+void launch_stage(const ChainDev* chains, int nchains, int nslots, int dir, cudaStream_t st) {
+    k_stage<<<dim3(64, nchains), 256, 0, st>>>(chains, nslots, dir);
+}
+
+void launch_dyn_init(const ChainDev* chains, int nchains, cudaStream_t st) {
+    k_dyn_init<<<dim3(32, nchains), 256, 0, st>>>(chains);
 }
 
 void launch_wrap_check(const ChainDev* chains, int nchains, int record, cudaStream_t st) {

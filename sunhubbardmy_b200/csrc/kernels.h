@@ -30,6 +30,14 @@ void launch_stab(const ChainDev* chains, int nchains, int n, int dir, int pivote
 // green_equaltime, 1 = green_equaltimebb (l side = identity)
 void launch_green(const ChainDev* chains, int nchains, int nr, int nl, int rmat_u, int rmat_v,
                   int lmat_u, int lmat_v, int mode, cudaStream_t st);
+// green_tau: G(tau,tau) into Gnew, G(tau,0), G(0,tau), G(0,0) into gt0, g0t, g00
+// (R = slot nr, L = slot nl); new log weight -> stats[ST_LOGDETM_*]
+void launch_green_tau(const ChainDev* chains, int nchains, int nr, int nl, cudaStream_t st);
+// push_stage (dir 0) / pop_stage (dir 1) of nslots stack slots and G
+void launch_stage(const ChainDev* chains, int nchains, int nslots, int dir, cudaStream_t st);
+void launch_dyn_init(const ChainDev* chains, int nchains, cudaStream_t st);
+// unequal-time measurement of time index nt (1-based): znn_tau
+void launch_dyn_measure(const ChainDev* chains, int nchains, int maxN, int nt, cudaStream_t st);
 // wrap check: compare Gnew with G, recompute the phase, replace G (record = 0: just replace)
 void launch_wrap_check(const ChainDev* chains, int nchains, int record, cudaStream_t st);
 // generic batched complex GEMM on per-chain matrices (diagnostics)

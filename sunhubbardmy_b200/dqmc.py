@@ -45,6 +45,7 @@ class DqmcParams(C.Structure):
         ("proj", C.c_int32), ("lprojv", C.c_int32), ("obs_mid_len", C.c_int32),
         ("ndim", C.c_int32), ("lq", C.c_int32), ("ltrot", C.c_int32), ("nst", C.c_int32),
         ("ne", C.c_int32), ("lcomp", C.c_int32),
+        ("ltau", C.c_int32), ("ntdm", C.c_int32), ("dyntau", C.c_double),
     ]
 
     @classmethod
@@ -54,7 +55,7 @@ class DqmcParams(C.Structure):
                  mu=0.0, rhub=0.0, rv=0.0, alpha=0.2, theta=0.0, xmag=0.0, flux_x=0.0, flux_y=0.0,
                  dimer=0.0, rndness=0.0, nflr=2, lproju=0, lstabilize=1, nwrap=10, nsweep=20,
                  nbin=10, nublock=0, update=DELAY, kinetic=CHECKERBOARD, hs=GENERAL4, proj=0,
-                 lprojv=0, obs_mid_len=1)
+                 lprojv=0, obs_mid_len=1, ltau=0, dyntau=0.0)
         d.update(kw)
         p = cls(**d)
         rc = load_library().dqmc_params_derive(C.byref(p))
@@ -130,6 +131,9 @@ SIGNATURES = {
     "dqmc_gpu_time_op": (_i, [_vp, _i, _i, _vp]),
     "dqmc_gpu_sweep_kernels": (_i, [_vp]),
     "dqmc_gpu_sweep_profile": (_i, [_vp, _i, _i, _vp, _vp]),
+    "dqmc_gpu_sweep_dyn": (_i, [_vp]),
+    "dqmc_gpu_get_dyn_bins": (_i, [_vp, _i, _vp]),
+    "dqmc_gpu_get_dyn_mats": (_i, [_vp, _i, _vp, _vp, _vp]),
     "dqmc_gpu_qr_logdet_noalloc": (_i, [_i, _vp, _vp, _vp, _vp]),
     "dqmc_gpu_noalloc_error": (C.c_char_p, []),
     "dqmc_gpu_set_vconf": (_i, [_vp, _i, _vp]),
@@ -424,6 +428,26 @@ class Dqmc:
         ms = C.c_double()
         _check(load_library().dqmc_gpu_time_op(self.h, op, reps, C.byref(ms)), "time_op")
         return ms.value
+
+    # unequal-time measurement (params.ltau = 1)
+    def sweep_dyn(self) -> None:
+        """push_stage, 0b sweep without updates measuring znn_tau, pop_stage
+        (the ltau pass of dqmc_sweep)."""
+        _check(load_library().dqmc_gpu_sweep_dyn(self.h), "sweep_dyn")
+
+    def dyn_bins(self, c: int = 0) -> np.ndarray:
+        """znn_tau_bin of chain c as [ntdm+1, 2 (no_j), 2 (no_i), lq] complex."""
+        p = self.chain_params(c)
+        out = np.zeros(p.lq * 4 * (p.ntdm + 1), complex)
+        _check(load_library().dqmc_gpu_get_dyn_bins(self.h, c, _ptr(out)), "get_dyn_bins")
+        return out.reshape(p.ntdm + 1, 2, 2, p.lq)
+
+    def dyn_mats(self, c: int = 0):
+        """(G(0,0), G(beta,0), G(0,beta)) after the last unequal-time pass."""
+        N = self.ndim(c)
+        mats = [np.zeros((N, N), complex, order="F") for _ in range(3)]
+        _check(load_library().dqmc_gpu_get_dyn_mats(self.h, c, *[_ptr(x) for x in mats]), "get_dyn_mats")
+        return tuple(mats)
 
     PROFILE_KINDS = ("update", "stab", "green", "prop_left", "measure", "prop_right", "bprod", "other")
 

@@ -7,6 +7,9 @@
 * ``energy.bin`` and the ``*.bin`` files of equaltime_output
   (src/dqmc_measure/equaltime_output.f90:67-180): per bin, the bin sums
   reduced over chains and divided by ``n_chains * nobs``.
+* ``nn_rtau.bin`` / ``nn_ktau.bin`` of dyn_output
+  (src/dqmc_measure/dyn_output.f90): the unequal-time density correlation
+  reduced over chains and divided by ``nsweep * n_chains``.
 """
 from __future__ import annotations
 
@@ -98,3 +101,35 @@ def equaltime_output(bins_per_chain, outdir: str = ".", zexpiqr: np.ndarray | No
                 kk = _fourier(arr.reshape(-1, arr.shape[-1]).T, zexpiqr).T.reshape(-1)
                 f.write("".join(f"{v:16.8e}" for z in kk for v in (z.real, z.imag)) + "\n")
     return red
+
+
+def dyn_output(dyn_bins_per_chain, nsweep: int, nsub: int, outdir: str = ".",
+               zexpiqr: np.ndarray | None = None, listk: np.ndarray | None = None,
+               l1: int = 1, l2: int = 1) -> np.ndarray:
+    """dyn_output (src/dqmc_measure/dyn_output.f90:1-68, fourier_trans_tau_22):
+    reduce the znn_tau bins of the chains (as Dqmc.dyn_bins returns them,
+    [ntdm+1, 2 (no_j), 2 (no_i), lq]), normalise by nsweep * n_chains and
+    append nn_rtau.bin (per distance imj, per time index: the nsub x nsub
+    block, column-major) and, given zexpiqr[nk, imj] and listk[nk, 2],
+    nn_ktau.bin (per momentum: its coordinates, then the block at every time
+    index, gk = sum_imj gr / zexpiqr(nk, imj) / lq)."""
+    gr = sum(np.asarray(b) for b in dyn_bins_per_chain) / float(nsweep * len(dyn_bins_per_chain))
+    ntp, _, _, lq = gr.shape
+    os.makedirs(outdir, exist_ok=True)
+
+    def block(a, nt):        # a[nt, no_j, no_i] -> (no_i, no_j) column-major over 1..nsub
+        return [a[nt, j, i] for j in range(nsub) for i in range(nsub)]
+
+    with open(os.path.join(outdir, "nn_rtau.bin"), "a") as f:
+        for imj in range(lq):
+            for nt in range(ntp):
+                f.write("".join(f"{v:16.8e}" for z in block(gr[..., imj], nt) for v in (z.real, z.imag)) + "\n")
+    if zexpiqr is not None:
+        gk = np.einsum("tjim,km->tjik", gr, 1.0 / np.asarray(zexpiqr)) / lq
+        with open(os.path.join(outdir, "nn_ktau.bin"), "a") as f:
+            for nk in range(lq):
+                if listk is not None:
+                    f.write(f"{listk[nk][0] / l1:16.8f}{listk[nk][1] / l2:16.8f}\n")
+                for nt in range(ntp):
+                    f.write("".join(f"{v:16.8e}" for z in block(gk[..., nk], nt) for v in (z.real, z.imag)) + "\n")
+    return gr

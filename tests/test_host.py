@@ -185,3 +185,26 @@ def test_projective_params():
         sb.DqmcParams.make(rv=1.0, proj=0)       # t-V runs on the projective path only
     with pytest.raises(sb.DqmcError):
         sb.DqmcParams.make(rv=1.0, proj=1, lstabilize=0)
+
+
+def test_dyn_output_files(tmp_path):
+    """dyn_output: chains reduced and normalised by nsweep * n_chains; nn_rtau.bin
+    holds, per distance and time index, the nsub x nsub block; nn_ktau.bin the
+    transform with zexpiqr."""
+    from sunhubbardmy_b200.io import dyn_output
+    rng = np.random.default_rng(0)
+    lq, ntp, nsub = 4, 3, 2
+    bins = [rng.standard_normal((ntp, 2, 2, lq)) + 1j * rng.standard_normal((ntp, 2, 2, lq)) for _ in range(2)]
+    zq = np.exp(1j * rng.uniform(0, 2 * np.pi, (lq, lq)))
+    gr = dyn_output(bins, 5, nsub, str(tmp_path), zexpiqr=zq, listk=np.ones((lq, 2)), l1=2, l2=2)
+    assert np.allclose(gr, (bins[0] + bins[1]) / 10.0)
+    rows = [np.array(l.split(), float) for l in open(tmp_path / "nn_rtau.bin")]
+    assert len(rows) == lq * ntp and all(len(r) == 8 for r in rows)
+    r = rows[1 * ntp + 2]                                   # imj = 2, nt = 3
+    z = r[0::2] + 1j * r[1::2]
+    assert np.allclose(z, [gr[2, 0, 0, 1], gr[2, 0, 1, 1], gr[2, 1, 0, 1], gr[2, 1, 1, 1]], atol=1e-7)
+    krows = open(tmp_path / "nn_ktau.bin").read().splitlines()
+    assert len(krows) == lq * (ntp + 1)
+    k1 = np.array(krows[1].split(), float)                  # nk = 1, nt = 1
+    gk = (gr[0, 0, 0, :] / zq[0, :]).sum() / lq
+    assert np.allclose(k1[0] + 1j * k1[1], gk, atol=1e-7)

@@ -402,3 +402,41 @@ def test_effective_action_gradient_by_finite_differences():
         tm = th.copy(); tm[idx] -= eps
         fd = sum(rr * (no.forward(tp, f, False) - no.forward(tm, f, False)) / (2 * eps) for f, rr in zip(fields, r))
         assert abs(g[idx] - fd) < 1e-7 * max(1.0, abs(fd))
+
+
+@pytest.mark.parametrize("lattice,kinetic", [(1, 1), (2, 0)])
+def test_dyn_pass_free_fermions(oracle, lattice, kinetic):
+    """U = 0: the unequal-time pass gives G(tau,0) = B(tau) G0, G(0,tau) =
+    -(1 - G0) B(tau)^-1, G(tau,tau) = B(tau) G0 B(tau)^-1 with G0 = (1 + B(beta))^-1,
+    so znn_tau follows in closed form; phase 1.  Also: the pass restores the
+    stack and G (pop_stage)."""
+    kw = dict(lattice=lattice, l1=3 if lattice == 2 else 4, l2=3 if lattice == 2 else 4, beta=1.2, dtau=0.1,
+              rhub=0.0, nflr=2, kinetic=kinetic, nwrap=4, ltau=1, dyntau=1.2)
+    m = oracle.Model(**kw)
+    c = oracle.Chain(m, 11)
+    c.sweep_start()
+    c.sweep_b0(lupdate=False, lmeasure=False)
+    g_before = c.green()
+    c.obser_init()
+    c.sweep_dyn()
+    assert np.max(np.abs(c.green() - g_before)) == 0.0
+    N, lq, lt = m.ndim, m.lq, m.ltrot
+    Bb = np.asfortranarray(np.eye(N, dtype=complex))
+    c.bmat_left_forward(lt, 1, Bb)
+    G0 = np.linalg.inv(np.eye(N) + Bb)
+    t = m.tables()                                      # 1-based list, imj
+    cell, orb, imj = t["list"][:, 0] - 1, t["list"][:, 1] - 1, t["imj"] - 1
+    expect = np.zeros((m.ntdm + 1, 2, 2, lq), complex)
+    for nt in range(1, lt + 2):
+        B = np.asfortranarray(np.eye(N, dtype=complex))
+        if nt > 1:
+            c.bmat_left_forward(nt - 1, 1, B)
+        Bi = np.linalg.inv(B)
+        gt0, g0t, gtt = B @ G0, -(np.eye(N) - G0) @ Bi, B @ G0 @ Bi
+        for j in range(N):
+            for i in range(N):
+                d = imj[cell[i], cell[j]]
+                expect[nt - 1, orb[j], orb[i], d] += ((0.5 - gtt[i, i].real) * (0.5 - G0[j, j].real)
+                                                      - 0.5 * g0t[j, i] * gt0[i, j])
+    got = c.dyn_bins()
+    assert np.max(np.abs(got - expect)) < 1e-9 * max(1.0, np.max(np.abs(expect)))
