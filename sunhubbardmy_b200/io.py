@@ -7,6 +7,9 @@
 * ``energy.bin`` and the ``*.bin`` files of equaltime_output
   (src/dqmc_measure/equaltime_output.f90:67-180): per bin, the bin sums
   reduced over chains and divided by ``n_chains * nobs``.
+* ``dqmc.out``: the parameter banner (dqmc_initial_print), the wrap-error
+  lines (wrap_error_print) and the end of run with the -DTIMING breakdown
+  (dqmc_end), src/dqmc_util.f90.
 * ``nn_rtau.bin`` / ``nn_ktau.bin`` of dyn_output
   (src/dqmc_measure/dyn_output.f90): the unequal-time density correlation
   reduced over chains and divided by ``nsweep * n_chains``.
@@ -133,3 +136,115 @@ def dyn_output(dyn_bins_per_chain, nsweep: int, nsub: int, outdir: str = ".",
                 for nt in range(ntp):
                     f.write("".join(f"{v:16.8e}" for z in block(gk[..., nk], nt) for v in (z.real, z.imag)) + "\n")
     return gr
+
+
+# ----------------------------------------------------------------------------
+# dqmc.out (src/dqmc_util.f90): parameter banner, wrap-error lines, end of run
+# ----------------------------------------------------------------------------
+def fortran_e(v: float, w: int = 16, d: int = 8) -> str:
+    """Fortran Ew.d: 0.ddddddddE+xx, right-justified in w columns."""
+    v = float(v)
+    if v == 0.0 or not np.isfinite(v):
+        s = f"{0.0:.{d}f}E+00" if v == 0.0 else str(v)
+    else:
+        e = int(np.floor(np.log10(abs(v)))) + 1
+        m = abs(v) / 10.0 ** e
+        if round(m, d) >= 1.0:
+            m /= 10.0
+            e += 1
+        s = f"{'-' if v < 0 else ''}0.{int(round(m * 10 ** d)):0{d}d}E{'+' if e >= 0 else '-'}{abs(e):02d}"
+    return s.rjust(w)
+
+
+def _lg(b) -> str:
+    return "T" if b else "F"
+
+
+def dqmc_initial_print(f, p, wrap_step=None, nustock: int = 0) -> None:
+    """dqmc_initial_print (src/dqmc_util.f90:208-285) for the parameter set p
+    (DqmcParams or a dict of the same fields); wrap_step: (start, end) slice
+    pairs of the stabilisation intervals, 1-based."""
+    g = p if isinstance(p, dict) else p.as_dict()
+    w = f.write
+    w("\n --------------------- \n The input parameters  \n --------------------- \n\n")
+    w(f" t      = {g['rt']:6.2f}\n")
+    w(f" mu     = {g['mu']:7.3f}\n")
+    w(f" rhub_plq  = {0.0:7.3f}\n")
+    w(f" lprojplqu =  {_lg(0)}\n")
+    w(f" rhub      = {g['rhub']:7.3f}\n")
+    w(f" lproju    =  {_lg(g['lproju'])}\n")
+    w(f" rv      = {g['rv']:7.3f}\n")
+    w(f" lprojv   =  {_lg(g['lprojv'])}\n")
+    w(f" la     = {g['l1']:4d}\n")
+    w(f" lb     = {g['l2']:4d}\n")
+    w(f" beta   = {g['beta']:6.2f}\n")
+    w(f" dtau   = {g['dtau']:7.3f}\n")
+    for k, name in (("ndim", "ndim"), ("ne", "ne  "), ("nwrap", "nwrap "), ("nsweep", "nsweep"),
+                    ("nbin", "nbin"), ("nublock", "nublock")):
+        w(f" {name} = {g[k]:6d}\n")
+    w(f" nustock = {nustock:6d}\n")
+    w(f" B      = {g['xmag']:6.2f}\n")
+    w(f" flux_x = {g['flux_x']:8.5f}\n")
+    w(f" flux_y = {g['flux_y']:8.5f}\n")
+    w(f" dimer  = {g['dimer']:8.5f}\n")
+    w(f" alpha  = {g['alpha']:8.5f}\n")
+    w(f" theta  = {g['theta']:8.5f}\n")
+    w(f" nflr   = {g['nflr']:4d}\n")
+    w(f"  ltau =  {_lg(g.get('ltau', 0))}\n")
+    if g.get("ltau", 0):
+        ntdm = g.get("ntdm", 0)
+        w(f" ntauin = {(g['ltrot'] - ntdm) // 2:6d}\n")
+        w(f" ntdm = {ntdm:6d}\n")
+    w("\n --------------------- \n wrapping coordinates  \n --------------------- \n")
+    w("       wrap_step(1,i)   wrap_step(2,i)   iwrap_nt(nt) \n")
+    for i, (a, b) in enumerate(wrap_step or [], start=1):
+        w(f"{a:16d}{b:16d}{i:16d}\n")
+    w(" \n")
+    w(("honeycomb_lattice" if g["lattice"] == 2 else "square_lattice") + "\n")
+
+
+def wrap_step_of(p) -> list:
+    """The stabilisation intervals (wrap_step(1:2, n), src/model_para.f90:420-452)."""
+    g = p if isinstance(p, dict) else p.as_dict()
+    lt, nw, nst = g["ltrot"], g["nwrap"], g["nst"]
+    return [((n - 1) * nw + 1, min(n * nw, lt)) for n in range(1, nst + 1)]
+
+
+def wrap_error_print(f, diags) -> None:
+    """wrap_error_print (src/dqmc_util.f90:15-57) of the chains' diagnostics
+    (Dqmc.diag dicts): max over chains, averages over all wrap checks."""
+    mw = max(d["max_wrap_error"] for d in diags)
+    mp = max(d["max_phasediff"] for d in diags)
+    cnt = sum(d["logcount"] for d in diags)
+    a10 = sum(d["avglog10error"] for d in diags) / cnt if cnt else 0.0
+    aph = sum(d["avgexpphasediff"] for d in diags) / cnt if cnt else 0.0
+    f.write(f"--------------max_wrap_error  = {fortran_e(mw)}\n")
+    f.write(f"--------------max_phasediff   = {fortran_e(mp)}\n")
+    f.write(f"--------------avglog10error     = {a10:16.8f}\n")
+    f.write(f"--------------avgexpphasediff = {aph:16.8f}\n")
+
+
+def dqmc_end_print(f, diags, total_s: float, profile: dict | None = None, date: str = "") -> None:
+    """dqmc_end (src/dqmc_util.f90:287-369): acceptance of the U (and t-V bond)
+    field over all chains, total time and, given a sweep profile
+    (Dqmc.sweep_profile: {kind: (ms, groups)}), the -DTIMING breakdown."""
+    def acc(a, p):
+        return sum(d[a] for d in diags) / max(1.0, sum(d[p] for d in diags))
+    if sum(d.get("proposed_v", 0.0) for d in diags) > 0:
+        f.write(f" >>> accep_v     = {fortran_e(acc('accepted_v', 'proposed_v'))}\n")
+    if sum(d["proposed"] for d in diags) > 0:
+        f.write(f" >>> accep_u     = {fortran_e(acc('accepted', 'proposed'))}\n")
+    f.write("\n")
+    f.write(f" >>> Total time spent:{total_s:10.2f}s\n")
+    f.write(f" >>> Happy ending at {date}\n\n")
+    if profile:
+        s = {k: v[0] * 1e-3 for k, v in profile.items()}
+        tot = sum(s.values())
+        rows = [("The_time_of_propagating:        ", s["prop_left"] + s["prop_right"] + s["bprod"]),
+                ("The_time_of_ft_delay_update:    ", s["update"]),
+                ("The_time_of_stabilization:      ", s["stab"] + s["green"] + s["other"]),
+                ("The_time_of_measuring_equaltime:", s["measure"])]
+        f.write(f"The_time_of_sweep_in_total:     {tot:10.3f}s\n")
+        for name, t in rows:
+            f.write(f"{name}{t:10.3f}s = {100.0 * t / tot if tot else 0.0:6.2f}%\n")
+    f.write(" The simulation done !!! \n")

@@ -208,3 +208,40 @@ def test_dyn_output_files(tmp_path):
     k1 = np.array(krows[1].split(), float)                  # nk = 1, nt = 1
     gk = (gr[0, 0, 0, :] / zq[0, :]).sum() / lq
     assert np.allclose(k1[0] + 1j * k1[1], gk, atol=1e-7)
+
+
+def test_dqmc_out_writers():
+    """dqmc.out pieces: Fortran E16.8 numbers, the parameter banner with the
+    wrapping coordinates, wrap-error lines and the end-of-run acceptances."""
+    import io as pyio
+    import sunhubbardmy_b200 as sb
+    from sunhubbardmy_b200.io import (dqmc_end_print, dqmc_initial_print, fortran_e, wrap_error_print,
+                                      wrap_step_of)
+    assert fortran_e(1.5) == "  0.15000000E+01"
+    assert fortran_e(-1.23456789e-4) == " -0.12345679E-03"
+    assert fortran_e(0.0) == "  0.00000000E+00"
+    assert fortran_e(9.999999999) == "  0.10000000E+02"
+    p = sb.DqmcParams.make(lattice=1, l1=4, l2=4, beta=4.0, dtau=0.1, rhub=4.0, nwrap=10, ltau=1, dyntau=4.0)
+    ws = wrap_step_of(p)
+    assert ws == [(1, 10), (11, 20), (21, 30), (31, 40)]
+    f = pyio.StringIO()
+    dqmc_initial_print(f, p, ws)
+    txt = f.getvalue()
+    assert " beta   =   4.00\n" in txt and " rhub      =   4.000\n" in txt and " ntdm =     40\n" in txt
+    assert "              21              30               3\n" in txt and txt.endswith("square_lattice\n")
+    diags = [dict(max_wrap_error=1e-11, max_phasediff=0.0, avglog10error=-22.0, logcount=2.0, avgexpphasediff=2.0,
+                  accepted=30.0, proposed=100.0, accepted_v=0.0, proposed_v=0.0),
+             dict(max_wrap_error=3e-11, max_phasediff=1e-14, avglog10error=-21.0, logcount=2.0, avgexpphasediff=2.0,
+                  accepted=20.0, proposed=100.0, accepted_v=0.0, proposed_v=0.0)]
+    f = pyio.StringIO()
+    wrap_error_print(f, diags)
+    lines = f.getvalue().splitlines()
+    assert lines[0] == "--------------max_wrap_error  =   0.30000000E-10"
+    assert lines[2] == f"--------------avglog10error     = {-10.75:16.8f}"
+    f = pyio.StringIO()
+    dqmc_end_print(f, diags, 12.5, {"update": (100.0, 1), "stab": (50.0, 1), "green": (30.0, 1),
+                                    "prop_left": (10.0, 1), "measure": (5.0, 1), "prop_right": (5.0, 1),
+                                    "bprod": (0.0, 1), "other": (0.0, 1)})
+    out = f.getvalue()
+    assert " >>> accep_u     =   0.25000000E+00\n" in out and " >>> Total time spent:     12.50s\n" in out
+    assert "The_time_of_ft_delay_update:         0.100s =  50.00%\n" in out
