@@ -177,6 +177,13 @@ int dqmc_gpu_test_qr(dqmc_handle* h, int a, int q, double* logdetq /* 2 per chai
 /* Stream-ordered timing helper: average device time (ms) of the last
  * dqmc_gpu_sweeps call, measured with CUDA events on the library's stream. */
 double dqmc_gpu_last_sweeps_ms(dqmc_handle* h);
+/* n whole sweeps of several handles at once (every handle as in
+ * dqmc_gpu_sweeps): each handle's captured sweep runs on its own stream,
+ * forked from and joined to the first handle's stream, so that kernels of
+ * different handles -- different phases of independent chains -- share the SMs.
+ * *ms_out (may be NULL): device ms per sweep between fork and join.  The
+ * reference's counterpart is several MPI ranks sharing a node. */
+int dqmc_gpu_sweeps_multi(dqmc_handle* const* hs, int nh, int n, int lmeasure, double* ms_out);
 /* Number of kernel launches in one captured sweep (b0 + 0b) of dqmc_gpu_sweeps. */
 int dqmc_gpu_sweep_kernels(dqmc_handle* h);
 /* Average device time (ms) of `reps` back-to-back launches of one sweep kernel

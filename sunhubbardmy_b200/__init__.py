@@ -10,9 +10,9 @@ library and fails loudly if it is missing.
 """
 from .dqmc import (  # noqa: F401
     CHECKERBOARD, DELAY, FAST, FFT, GENERAL4, EXACT, HONEYCOMB, SQUARE, SUBMATRIX,
-    Dqmc, DqmcError, DqmcParams, lib_path, load_library, qr_logdet_noalloc, read_dqmc_in, test_seed,
-    trial_state,
+    Dqmc, DqmcError, DqmcParams, lib_path, load_library, qr_logdet_noalloc, read_dqmc_in, sweeps_concurrent,
+    test_seed, trial_state,
 )
 from .io import (  # noqa: F401
-    equaltime_output, read_conf, unpack_bins, write_conf,
+    dyn_output, equaltime_output, read_conf, unpack_bins, write_conf,
 )

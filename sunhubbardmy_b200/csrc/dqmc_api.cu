@@ -1558,10 +1558,9 @@ extern "C" int dqmc_gpu_sweep_0b(dqmc_handle* h, int lupdate, int lmeasure) {
     return DQMC_OK;
 }
 
-extern "C" int dqmc_gpu_sweeps(dqmc_handle* h, int n, int lmeasure) {
-    if (!h) return fail(DQMC_EINVAL, "null handle");
-    if (!h->started) return fail(DQMC_ESTATE, "sweep before sweep_start");
-    if (n <= 0) return DQMC_OK;
+// the captured sweep (b0 + 0b) of dqmc_gpu_sweeps, rebuilt when lmeasure or
+// recording changed
+static int ensure_sweep_graph(dqmc_handle* h, int lmeasure) {
     if (!h->sweep_graph || h->graph_meas != lmeasure + 2 * h->rec_on) {
         if (h->sweep_graph) { cudaGraphExecDestroy(h->sweep_graph); h->sweep_graph = nullptr; }
         cudaGraph_t g;
@@ -1582,6 +1581,14 @@ extern "C" int dqmc_gpu_sweeps(dqmc_handle* h, int n, int lmeasure) {
         cudaGraphDestroy(g);
         h->graph_meas = lmeasure + 2 * h->rec_on;
     }
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_sweeps(dqmc_handle* h, int n, int lmeasure) {
+    if (!h) return fail(DQMC_EINVAL, "null handle");
+    if (!h->started) return fail(DQMC_ESTATE, "sweep before sweep_start");
+    if (n <= 0) return DQMC_OK;
+    int rc = ensure_sweep_graph(h, lmeasure); if (rc) return rc;
     h->after_b0 = 0;
     CK(cudaEventRecord(h->ev0, h->st));
     for (int i = 0; i < n; ++i) CK(cudaGraphLaunch(h->sweep_graph, h->st));
@@ -1591,6 +1598,49 @@ extern "C" int dqmc_gpu_sweeps(dqmc_handle* h, int n, int lmeasure) {
     float ms = 0;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
     h->last_ms = ms / n;
+    return DQMC_OK;
+}
+
+// n sweeps of several handles at once: each handle's sweep graph on its own
+// stream, forked from and joined to the first handle's stream, so that the
+// kernels of different handles (different phases of their sweeps) share the
+// SMs.  The device time between fork and join goes to every handle's last_ms
+// and to *ms_out.
+extern "C" int dqmc_gpu_sweeps_multi(dqmc_handle* const* hs, int nh, int n, int lmeasure, double* ms_out) {
+    if (!hs || nh < 1 || nh > 16) return fail(DQMC_EINVAL, "1..16 handles");
+    for (int k = 0; k < nh; ++k) {
+        if (!hs[k]) return fail(DQMC_EINVAL, "null handle");
+        if (!hs[k]->started) return fail(DQMC_ESTATE, "sweep before sweep_start");
+        for (int q = 0; q < k; ++q)
+            if (hs[q] == hs[k]) return fail(DQMC_EINVAL, "a handle appears twice");
+    }
+    if (n <= 0) return DQMC_OK;
+    for (int k = 0; k < nh; ++k) {
+        int rc = ensure_sweep_graph(hs[k], lmeasure); if (rc) return rc;
+        hs[k]->after_b0 = 0;
+    }
+    dqmc_handle* h0 = hs[0];
+    cudaEvent_t fork = nullptr, join[16] = {};
+    CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    for (int k = 1; k < nh; ++k) CK(cudaEventCreateWithFlags(&join[k], cudaEventDisableTiming));
+    CK(cudaEventRecord(h0->ev0, h0->st));
+    CK(cudaEventRecord(fork, h0->st));
+    for (int k = 1; k < nh; ++k) CK(cudaStreamWaitEvent(hs[k]->st, fork, 0));
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < nh; ++k) CK(cudaGraphLaunch(hs[k]->sweep_graph, hs[k]->st));
+    for (int k = 1; k < nh; ++k) {
+        CK(cudaEventRecord(join[k], hs[k]->st));
+        CK(cudaStreamWaitEvent(h0->st, join[k], 0));
+    }
+    CK(cudaEventRecord(h0->ev1, h0->st));
+    CK(cudaStreamSynchronize(h0->st));
+    CK(cudaGetLastError());
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h0->ev0, h0->ev1);
+    cudaEventDestroy(fork);
+    for (int k = 1; k < nh; ++k) cudaEventDestroy(join[k]);
+    for (int k = 0; k < nh; ++k) hs[k]->last_ms = ms / n;
+    if (ms_out) *ms_out = ms / n;
     return DQMC_OK;
 }
 

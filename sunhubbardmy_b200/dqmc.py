@@ -132,6 +132,7 @@ SIGNATURES = {
     "dqmc_gpu_sweep_kernels": (_i, [_vp]),
     "dqmc_gpu_sweep_profile": (_i, [_vp, _i, _i, _vp, _vp]),
     "dqmc_gpu_sweep_dyn": (_i, [_vp]),
+    "dqmc_gpu_sweeps_multi": (_i, [_vp, _i, _i, _i, _vp]),
     "dqmc_gpu_get_dyn_bins": (_i, [_vp, _i, _vp]),
     "dqmc_gpu_get_dyn_mats": (_i, [_vp, _i, _vp, _vp, _vp]),
     "dqmc_gpu_qr_logdet_noalloc": (_i, [_i, _vp, _vp, _vp, _vp]),
@@ -210,6 +211,15 @@ def qr_logdet_noalloc(n: int, a_dev: int, q_dev: int, logdetq_dev: int, stream: 
                                       C.c_void_p(logdetq_dev), C.c_void_p(stream))
     if rc != 0:
         raise DqmcError(f"qr_logdet_noalloc failed ({rc}): {L.dqmc_gpu_noalloc_error().decode()}")
+
+
+def sweeps_concurrent(handles, n: int, lmeasure: bool = True) -> float:
+    """n whole sweeps of several Dqmc handles at once, each on its own stream
+    (dqmc_gpu_sweeps_multi); returns the device ms per sweep of all of them."""
+    arr = (C.c_void_p * len(handles))(*[g.h for g in handles])
+    ms = C.c_double()
+    _check(load_library().dqmc_gpu_sweeps_multi(arr, len(handles), n, int(lmeasure), C.byref(ms)), "sweeps_multi")
+    return ms.value
 
 
 def trial_state(params: DqmcParams, seed: int, draw_conf: bool = True):

@@ -18,3 +18,10 @@ def oracle():
     from oracle import pyoracle
     pyoracle.build()
     return pyoracle
+
+
+@pytest.fixture(scope="session")
+def sb():
+    """The package (its CUDA library loads on first use)."""
+    import sunhubbardmy_b200
+    return sunhubbardmy_b200
