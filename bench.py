@@ -659,7 +659,8 @@ def learned_arm(args, rank: int, local_rank: int) -> None:
 
     l0, var_y = val_loss()
     t0 = time.perf_counter()
-    losses = train(nn, g, targets[tr], args.train_steps, batch=32, lr=args.lr, seed=1, slots=tr)
+    losses = train(nn, g, targets[tr], args.train_steps, batch=32, lr=args.lr, seed=1, slots=tr,
+                   pair_lag=nch, diff_every=args.diff_every)
     train_s = time.perf_counter() - t0
     l1, _ = val_loss()
 
@@ -688,6 +689,7 @@ def learned_arm(args, rank: int, local_rank: int) -> None:
                     "ratio_prediction_mse_zero": tot["blk_err_zero"] / max(1.0, tot["blk_stage1"])},
         "ess_per_s_ratio_learned_vs_plain": (ess_l / wall_l) / (ess_p / wall_p),
         "training": {"pairs": int(npairs), "steps": args.train_steps, "batch": 32, "lr": args.lr, "wall_s": train_s,
+                     "diff_every": args.diff_every,
                      "heldout_var_residual_before": l0, "heldout_var_residual_after": l1,
                      "heldout_var_target": var_y, "loss_first": float(np.mean(losses[:20])),
                      "loss_last": float(np.mean(losses[-20:]))},
@@ -707,6 +709,8 @@ def main():
     ap.add_argument("--pairs", type=int, default=200000, help="config5: training-pair ring capacity")
     ap.add_argument("--train-steps", type=int, default=3000, help="config5: Adam steps of 32 pairs")
     ap.add_argument("--lr", type=float, default=3e-4, help="config5: Adam learning rate")
+    ap.add_argument("--diff-every", type=int, default=1,
+                    help="config5: every n-th Adam step fits the change of -log|W| between a chain's consecutive records (0: off)")
     ap.add_argument("--ess", type=int, default=0, help="extra sweeps for the ESS/s of double occupancy")
     ap.add_argument("--ess-warmup", type=int, default=20, help="equilibration sweeps before the ESS series")
     ap.add_argument("--streams", type=int, default=0,

@@ -302,6 +302,14 @@ int dqmc_nn_train_step(dqmc_nn* nn, const int8_t* fields, const double* y, int B
 /* the same on pairs recorded by the handle (indices idx, targets y) */
 int dqmc_nn_train_recorded(dqmc_nn* nn, dqmc_handle* h, const int32_t* idx, const double* y, int B, double lr,
                            double* loss);
+/* One Adam step on differences of recorded pairs: minimises the mean of
+ * ((S(record idx_b[b]) - S(record idx_a[b])) - dy[b])^2 over the B pairs
+ * (2 B <= max_batch).  With idx_b = idx_a + n_chains (the same chain one
+ * stabilisation later) and dy the difference of the recorded values, the
+ * network learns how the weight changes under one interval of local updates,
+ * the scale of a block proposal; no counterpart in the reference. */
+int dqmc_nn_train_recorded_pairs(dqmc_nn* nn, dqmc_handle* h, const int32_t* idx_a, const int32_t* idx_b,
+                                 const double* dy, int B, double lr, double* loss);
 
 /* Record (HS field as int8 +-1, nflr Re log W) of every chain at every
  * stabilisation of the finite-temperature sweeps into a ring of `capacity`

@@ -2357,6 +2357,41 @@ extern "C" int dqmc_nn_train_recorded(dqmc_nn* nn, dqmc_handle* h, const int32_t
     return nn_train_loaded(nn, y, B, lr, loss);
 }
 
+// One Adam step on differences of recorded pairs: loss = mean over b of
+// ((S(field idx_b[b]) - S(field idx_a[b])) - dy[b])^2, so that the network
+// learns how log|W| changes between nearby fields (the pairs of one chain one
+// stabilisation apart differ by one interval of local updates).
+extern "C" int dqmc_nn_train_recorded_pairs(dqmc_nn* nn, dqmc_handle* h, const int32_t* idx_a, const int32_t* idx_b,
+                                            const double* dy, int B, double lr, double* loss) {
+    if (!nn || !h || !idx_a || !idx_b || !dy || !h->rec_f) return fail(DQMC_EINVAL, "invalid arguments");
+    if (B < 1 || 2 * B > nn->maxB) return fail(DQMC_EINVAL, "2 B must be within 1..max_batch");
+    if (h->rec_V != nn->V) return fail(DQMC_EINVAL, "field size differs from the effective action's");
+    CK(cudaStreamSynchronize(h->st));
+    for (int b = 0; b < 2 * B; ++b) {
+        const int i = b < B ? idx_a[b] : idx_b[b - B];
+        if (i < 0 || i >= h->rec_cap) return fail(DQMC_EINVAL, "record index out of range");
+        CK(cudaMemcpyAsync(nn->fbuf + (size_t)b * nn->V, h->rec_f + (size_t)i * nn->V, nn->V,
+                           cudaMemcpyDeviceToDevice, nn->st));
+    }
+    std::vector<double> S(2 * B), r(2 * B);
+    int rc = nn_fwd(nn, 2 * B, S.data()); if (rc) return rc;
+    double l = 0.0;
+    for (int b = 0; b < B; ++b) {
+        const double d = (S[B + b] - S[b]) - dy[b];
+        l += d * d / B;
+        r[b] = -2.0 * d / B;
+        r[B + b] = 2.0 * d / B;
+    }
+    if ((rc = nn_bwd(nn, 2 * B, r.data()))) return rc;
+    nn->step += 1;
+    const float b1c = 1.f - (float)std::pow(0.9, nn->step), b2c = 1.f - (float)std::pow(0.999, nn->step);
+    launch_nn_adam(nn->theta, nn->grad, nn->m1, nn->m2, NN_NPARAM, (float)lr, b1c, b2c, nn->W2T, nn->W2R, nn->st);
+    CK(cudaStreamSynchronize(nn->st));
+    CK(cudaGetLastError());
+    if (loss) *loss = l;
+    return DQMC_OK;
+}
+
 // ---- global block moves inside the 0b sweep ----
 static int enable_blocks(dqmc_handle* h) {
     if (h->blocks) return DQMC_OK;

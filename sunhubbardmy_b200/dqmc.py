@@ -155,6 +155,7 @@ SIGNATURES = {
     "dqmc_nn_gradient": (_i, [_vp, _vp, _i, _vp, _vp, _vp]),
     "dqmc_nn_train_step": (_i, [_vp, _vp, _vp, _i, _d, _vp]),
     "dqmc_nn_train_recorded": (_i, [_vp, _vp, _vp, _vp, _i, _d, _vp]),
+    "dqmc_nn_train_recorded_pairs": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _d, _vp]),
     "dqmc_gpu_record": (_i, [_vp, _i]),
     "dqmc_gpu_record_count": (_i, [_vp]),
     "dqmc_gpu_record_get": (_i, [_vp, _i, _vp, _vp]),

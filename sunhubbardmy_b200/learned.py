@@ -88,6 +88,16 @@ class EffectiveAction:
                                                      C.byref(loss)), "nn_train_recorded")
         return loss.value
 
+    def train_recorded_pairs(self, g, idx_a, idx_b, dy, lr: float = 1e-3) -> float:
+        """One Adam step on (S(b) - S(a) - dy)^2 over recorded pairs."""
+        ia = np.ascontiguousarray(idx_a, np.int32)
+        ib = np.ascontiguousarray(idx_b, np.int32)
+        yy = np.ascontiguousarray(dy, np.float64)
+        loss = C.c_double()
+        _check(load_library().dqmc_nn_train_recorded_pairs(self.h, g.h, _ptr(ia), _ptr(ib), _ptr(yy), len(ia),
+                                                           float(lr), C.byref(loss)), "nn_train_recorded_pairs")
+        return loss.value
+
 
 def collect(g, sweeps: int, capacity: int) -> np.ndarray:
     """Run `sweeps` plain sweeps recording (field, nflr Re log W) at every
@@ -101,17 +111,28 @@ def collect(g, sweeps: int, capacity: int) -> np.ndarray:
 
 
 def train(nn: EffectiveAction, g, targets: np.ndarray, steps: int, batch: int = 32, lr: float = 1e-3,
-          seed: int = 0, slots=None) -> list:
+          seed: int = 0, slots=None, pair_lag: int = 0, diff_every: int = 0) -> list:
     """Adam on minibatches of the recorded pairs; returns the loss history.
     targets[k] is the target of record slot slots[k] (slots defaults to
-    0..len(targets)-1, i.e. all recorded pairs in order)."""
+    0..len(targets)-1, i.e. all recorded pairs in order).  With pair_lag > 0
+    and diff_every = d > 0, every d-th step instead fits the difference of the
+    targets of slots s and s + pair_lag (the same chain one stabilisation later
+    when pair_lag = n_chains), among the slots given."""
     rng = np.random.default_rng(seed)
     n = len(targets)
     slots = np.arange(n, dtype=np.int32) if slots is None else np.asarray(slots, np.int32)
     if len(slots) != n:
         raise ValueError("slots and targets differ in length")
+    by_slot = {int(sl): t for sl, t in zip(slots, targets)}
+    pairs = np.array([sl for sl in slots if int(sl) + pair_lag in by_slot], np.int32) if pair_lag > 0 else None
     losses = []
-    for _ in range(steps):
-        k = rng.integers(0, n, size=min(batch, n))
-        losses.append(nn.train_recorded(g, slots[k], targets[k], lr))
+    for step in range(steps):
+        if diff_every > 0 and pairs is not None and len(pairs) and step % diff_every == diff_every - 1:
+            a = pairs[rng.integers(0, len(pairs), size=min(batch // 2, len(pairs)))]
+            b = a + pair_lag
+            dy = np.array([by_slot[int(y)] - by_slot[int(x)] for x, y in zip(a, b)])
+            losses.append(nn.train_recorded_pairs(g, a, b, dy, lr))
+        else:
+            k = rng.integers(0, n, size=min(batch, n))
+            losses.append(nn.train_recorded(g, slots[k], targets[k], lr))
     return losses
