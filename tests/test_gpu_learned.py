@@ -167,3 +167,19 @@ def test_training_on_recorded_pairs_learns_the_weight(sb):
     S = np.concatenate([nn.forward(vf[i:i + 32]) for i in range(0, len(vf), 32)])
     r2 = 1 - np.var(S - y[val]) / np.var(y[val])
     assert r2 > 0.2, r2
+
+
+def test_training_on_record_differences_lowers_its_loss(sb):
+    """dqmc_nn_train_recorded_pairs: fitting the change of -log|W| between a
+    chain's consecutive records lowers the pair loss."""
+    from sunhubbardmy_b200.learned import EffectiveAction, collect, train
+    kw = dict(HUB, beta=2.0, rhub=6.0)
+    p = sb.DqmcParams.make(**kw)
+    nch = 16
+    g = sb.Dqmc(p, n_chains=nch)
+    g.sweep_start()
+    g.sweeps(2, False)
+    y = collect(g, 8, 4096)
+    nn = EffectiveAction(p.ltrot, p.l1, max_batch=32, seed=3)
+    losses = train(nn, g, y, 400, batch=32, lr=1e-3, seed=2, pair_lag=nch, diff_every=1)
+    assert np.mean(losses[-40:]) < 0.7 * np.mean(losses[:40])
