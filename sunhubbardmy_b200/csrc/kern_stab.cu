@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(256, 2) k_green(const ChainDev* __restrict__ c
     }
     __syncthreads();
     cta_apply_qh64(M, N, X, sc, buf);
-    cta_trsm_upper(M, N, X, buf, &S->L);
+    cta_trsm_upper64(M, N, X, buf, &S->L);
     if (mode == 0) {
         const double2* UL = c.U + (size_t)nl * NN;
         double2* UL2 = c.W[2];
@@ -291,9 +291,9 @@ __global__ void __launch_bounds__(256, 2) k_green_tau(const ChainDev* __restrict
     }
     __syncthreads();
     cta_apply_qh64(W0, N, W2, sc, buf);
-    cta_trsm_upper(W0, N, W2, buf, &S->L);
+    cta_trsm_upper64(W0, N, W2, buf, &S->L);
     cta_apply_qh64(W0, N, W3, sc, buf);
-    cta_trsm_upper(W0, N, W3, buf, &S->L);
+    cta_trsm_upper64(W0, N, W3, buf, &S->L);
     // UL dlmax^-1 (W4); G(tau,tau) and G(tau,0)
     for (size_t e = tid; e < NN; e += nth) W4[e] = cscale(UL[e], 1.0 / dlmax[(int)(e / N)]);
     __syncthreads();
@@ -310,7 +310,7 @@ __global__ void __launch_bounds__(256, 2) k_green_tau(const ChainDev* __restrict
         __syncthreads();
         cta_qr64(W0, N, sc, buf, buf, &S->L);
         cta_apply_qh64(W0, N, Xi, sc, buf);
-        cta_trsm_upper(W0, N, Xi, buf, &S->L);
+        cta_trsm_upper64(W0, N, Xi, buf, &S->L);
     }
     // (VR VL^H)^-1 = (VL^H)^-1 VR^-1 (W4); M2 (W0)
     gemm(W3, OP_N, W2, OP_N, W4, 1.0);
@@ -328,9 +328,9 @@ __global__ void __launch_bounds__(256, 2) k_green_tau(const ChainDev* __restrict
     }
     __syncthreads();
     cta_apply_qh64(W0, N, W3, sc, buf);
-    cta_trsm_upper(W0, N, W3, buf, &S->L);
+    cta_trsm_upper64(W0, N, W3, buf, &S->L);
     cta_apply_qh64(W0, N, W4, sc, buf);
-    cta_trsm_upper(W0, N, W4, buf, &S->L);
+    cta_trsm_upper64(W0, N, W4, buf, &S->L);
     // VR^-1 drmax^-1 (W2); G(0,0), G(0,tau)
     for (size_t e = tid; e < NN; e += nth) W2[e] = cscale(W2[e], 1.0 / drmax[(int)(e / N)]);
     __syncthreads();

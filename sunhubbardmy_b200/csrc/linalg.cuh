@@ -257,35 +257,49 @@ static __device__ void cta_apply_qh(const double2* A, int N, double2* X, LinalgS
 }
 
 // X <- R^{-1} X with R the upper triangle of A (blocked back substitution).
-static __device__ void cta_trsm_upper(const double2* A, int N, double2* X, cplx* gsm, LinalgSmem* L) {
-    int last = ((N - 1) / QR_NB) * QR_NB;
-    for (int p = last; p >= 0; p -= QR_NB) {
-        const int jb = min(QR_NB, N - p);
-        if (p + jb < N) {
+static __device__ void trsm_rows16(const double2* A, int N, double2* X, int p0, int p1, cplx* gsm, LinalgSmem* L) {
+    const int last = p0 + ((p1 - p0 - 1) / QR_NB) * QR_NB;
+    for (int p = last; p >= p0; p -= QR_NB) {
+        const int jb = min(QR_NB, p1 - p);
+        if (p + jb < p1) {
             ZGemmArgs g;
-            g.M = jb; g.N = N; g.K = N - p - jb; g.alpha = cmk(-1, 0); g.beta = cmk(1, 0);
+            g.M = jb; g.N = N; g.K = p1 - p - jb; g.alpha = cmk(-1, 0); g.beta = cmk(1, 0);
             g.A = A + MIDX(p, p + jb, N); g.lda = N; g.opA = OP_N;
             g.B = X + (p + jb); g.ldb = N; g.opB = OP_N;
             g.C = X + p; g.ldc = N;
             zgemm_cta<GemmWide>(g, 0, 1, gsm);
         }
+        // The diagonal is stored as its reciprocal so the solve multiplies.
         for (int e = threadIdx.x; e < jb * jb; e += blockDim.x) {
             int a = e % jb, b = e / jb;
-            L->S[a + b * QR_NB] = A[MIDX(p + a, p + b, N)];
+            double2 v = A[MIDX(p + a, p + b, N)];
+            L->S[a + b * QR_NB] = (a == b) ? cdiv(cmk(1, 0), v) : v;
         }
         __syncthreads();
         for (int cc = threadIdx.x; cc < N; cc += blockDim.x) {
             double2 x[QR_NB];
-            for (int a = 0; a < jb; ++a) x[a] = X[MIDX(p + a, cc, N)];
-            for (int a = jb - 1; a >= 0; --a) {
-                double2 s = x[a];
-                for (int b = a + 1; b < jb; ++b) s = csub(s, cmul(L->S[a + b * QR_NB], x[b]));
-                x[a] = cdiv(s, L->S[a + a * QR_NB]);
+#pragma unroll
+            for (int a = 0; a < QR_NB; ++a) x[a] = (a < jb) ? X[MIDX(p + a, cc, N)] : cmk(0, 0);
+#pragma unroll
+            for (int a = QR_NB - 1; a >= 0; --a) {
+                if (a < jb) {
+                    double2 sm = x[a];
+#pragma unroll
+                    for (int b = a + 1; b < QR_NB; ++b)
+                        if (b < jb) sm = csub(sm, cmul(L->S[a + b * QR_NB], x[b]));
+                    x[a] = cmul(sm, L->S[a + a * QR_NB]);
+                }
             }
-            for (int a = 0; a < jb; ++a) X[MIDX(p + a, cc, N)] = x[a];
+#pragma unroll
+            for (int a = 0; a < QR_NB; ++a)
+                if (a < jb) X[MIDX(p + a, cc, N)] = x[a];
         }
         __syncthreads();
     }
+}
+
+static __device__ void cta_trsm_upper(const double2* A, int N, double2* X, cplx* gsm, LinalgSmem* L) {
+    trsm_rows16(A, N, X, 0, N, gsm, L);
 }
 
 // ---------------------------------------------------------------------------
@@ -297,6 +311,26 @@ static __device__ void cta_trsm_upper(const double2* A, int N, double2* X, cplx*
 //   T = [[T_a, -T_a (V_a^H V_b) T_b], [0, T_b]].
 // ---------------------------------------------------------------------------
 #define QR_NB2 64
+
+// X <- R^{-1} X, two-level: block rows of 64 are first updated with the solved
+// rows below them by one 64-row GEMM (GemmBig), then solved with the 16-row
+// scheme of trsm_rows16 restricted to the block, so most of the work runs
+// in 64-row DMMA tiles instead of 16-row ones.
+static __device__ void cta_trsm_upper64(const double2* A, int N, double2* X, cplx* gsm, LinalgSmem* L) {
+    const int last64 = ((N - 1) / QR_NB2) * QR_NB2;
+    for (int P = last64; P >= 0; P -= QR_NB2) {
+        const int jb2 = min(QR_NB2, N - P);
+        if (P + jb2 < N) {
+            ZGemmArgs g;
+            g.M = jb2; g.N = N; g.K = N - P - jb2; g.alpha = cmk(-1, 0); g.beta = cmk(1, 0);
+            g.A = A + MIDX(P, P + jb2, N); g.lda = N; g.opA = OP_N;
+            g.B = X + (P + jb2); g.ldb = N; g.opB = OP_N;
+            g.C = X + P; g.ldc = N;
+            zgemm_cta<GemmBig>(g, 0, 1, gsm);
+        }
+        trsm_rows16(A, N, X, P, P + jb2, gsm, L);
+    }
+}
 
 // X[p:N, c0:c0+nc] <- (I - V T V^H)^op X for a jb-wide block (jb <= 64; T ld 64)
 static __device__ void apply_block64(const double2* Vs, const double2* Tp, int N, int p, int jb,
