@@ -254,24 +254,41 @@ __global__ void __launch_bounds__(128, 4) k_prop_fft(const ChainDev* __restrict_
                                                      int rows, int right, int tall, double c1, double s1, double h) {
     constexpr int VPC = 128 / L;    // vectors per CTA
     constexpr int LD = L + 1;       // odd row pitch: conflict-free transposes
-    __shared__ double2 tb[VPC * L * LD];
+    constexpr int TS = L * LD + 1;  // per-vector region; the +1 spreads the row-tile stores over the banks
+    __shared__ double2 tb[VPC * TS];
     const ChainDev& c = chains[blockIdx.y];
     const ModelDev& md = *c.md;
     const int N = c.N;
     const int nvec = (tall && !rows) ? md.ne : N;
     double2* X = chain_mat(c, mat_id);
     const int g = threadIdx.x % L, vl = threadIdx.x / L;
-    double2* T = tb + vl * L * LD;
+    double2* T = tb + vl * TS;
     // left multiplication: F^-1 D F (forward sign first); right: F D F^-1
     const int sg = right ? -1 : 1;
     for (int v0 = blockIdx.x * VPC; v0 < nvec; v0 += gridDim.x * VPC) {
         const int v = v0 + vl;
         const bool act = v < nvec;      // uniform over the l threads of a vector
         double2 x[L];
+        if (rows) {
+            // Rows are strided by N: stage the (L*L) x VPC tile through shared
+            // memory with consecutive threads on consecutive vectors.
+            // L * L * VPC = 128 * L: L elements per thread, all loads in flight
 #pragma unroll
-        for (int j = 0; j < L; ++j) {
-            const int i = g + L * j;
-            x[j] = !act ? cmk(0, 0) : rows ? X[(size_t)i * N + v] : X[(size_t)v * N + i];
+            for (int k = 0; k < L; ++k) {
+                const int e = threadIdx.x + 128 * k, vv = e % VPC, i = e / VPC;
+                x[k] = (v0 + vv < nvec) ? X[(size_t)i * N + v0 + vv] : cmk(0, 0);
+            }
+#pragma unroll
+            for (int k = 0; k < L; ++k) {
+                const int e = threadIdx.x + 128 * k, vv = e % VPC, i = e / VPC;
+                tb[vv * TS + (i / L) * LD + (i % L)] = x[k];
+            }
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < L; ++j) x[j] = act ? T[j * LD + g] : cmk(0, 0);
+        } else {
+#pragma unroll
+            for (int j = 0; j < L; ++j) x[j] = act ? X[(size_t)v * N + g + L * j] : cmk(0, 0);
         }
         for (int k = 0; k < prog.n; ++k) {
             const int code = prog.op[k];
@@ -312,13 +329,20 @@ __global__ void __launch_bounds__(128, 4) k_prop_fft(const ChainDev* __restrict_
             __syncwarp();
             fft_dir<L>(x, -sg, c1, s1, h);                // inverse dim 2
         }
-        if (act) {
+        if (rows) {
+            __syncthreads();            // all warps are done with their transposes
 #pragma unroll
-            for (int j = 0; j < L; ++j) {
-                const int i = g + L * j;
-                if (rows) X[(size_t)i * N + v] = x[j];
-                else X[(size_t)v * N + i] = x[j];
+            for (int j = 0; j < L; ++j) T[j * LD + g] = x[j];
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < L; ++k) {
+                const int e = threadIdx.x + 128 * k, vv = e % VPC, i = e / VPC;
+                if (v0 + vv < nvec) X[(size_t)i * N + v0 + vv] = tb[vv * TS + (i / L) * LD + (i % L)];
             }
+            __syncthreads();            // the tile is free for the next vectors
+        } else if (act) {
+#pragma unroll
+            for (int j = 0; j < L; ++j) X[(size_t)v * N + g + L * j] = x[j];
         }
     }
 }
