@@ -778,6 +778,7 @@ struct dqmc_handle {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0.0;
     int ctas_per_chain = 1;
+    int max_lq = 0;           // largest number of unit cells over the models
     size_t graph_nodes = 0;
     int proj = 0;
     // recording of (HS field, nflr Re log weight) pairs at every stabilisation
@@ -887,6 +888,7 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
         h->maxN = std::max(h->maxN, m->N);
         h->nnf_max = std::max(h->nnf_max, m->nn_nf);
         h->maxNe = std::max(h->maxNe, m->p.ne);
+        h->max_lq = std::max(h->max_lq, m->lq);
     }
     {
         const dqmc_params& p0 = h->models[0]->p;
@@ -1211,7 +1213,7 @@ static void proj_measure(dqmc_handle* h) {
     launch_proj_ulr(h->d_chains, h->nch, PMAT_ULRINV, 0, 0, -1, h->st);
     launch_proj_green(h->d_chains, h->nch, PMAT_ULRINV, PMAT_G, h->ctas_per_chain, h->st);
     tmark(h, DQMC_PROF_GREEN);
-    launch_measure(h->d_chains, h->nch, h->maxN, h->ctas_per_chain, h->st);
+    launch_measure(h->d_chains, h->nch, h->maxN, h->models[0]->nsub == 2, h->max_lq, h->st);
     tmark(h, DQMC_PROF_MEASURE);
 }
 
@@ -1400,7 +1402,7 @@ static void enqueue_b0(dqmc_handle* h, int lupdate, int lmeasure) {
     tmark(h, DQMC_PROF_OTHER);
     for (int nt = lt; nt >= 1; --nt) {
         int visit = lt - nt;
-        if (lmeasure) { launch_measure(h->d_chains, h->nch, h->maxN, h->ctas_per_chain, h->st); tmark(h, DQMC_PROF_MEASURE); }
+        if (lmeasure) { launch_measure(h->d_chains, h->nch, h->maxN, h->models[0]->nsub == 2, h->max_lq, h->st); tmark(h, DQMC_PROF_MEASURE); }
         PropProg pl; pl.n = 0; PropProg pr; pr.n = 0;
         prog_k(m, pl, PW_INV, 0);          // left_backward, nf = 1..nnf
         prog_k(m, pr, PW_FWD, 0);          // right_forward, nf = 1..nnf
@@ -1447,7 +1449,7 @@ static void enqueue_0b(dqmc_handle* h, int lupdate, int lmeasure) {
         tmark(h, DQMC_PROF_PROP_L);
         launch_prog(h, MAT_G, pr, 1);
         tmark(h, DQMC_PROF_PROP_R);
-        if (lmeasure) { launch_measure(h->d_chains, h->nch, h->maxN, h->ctas_per_chain, h->st); tmark(h, DQMC_PROF_MEASURE); }
+        if (lmeasure) { launch_measure(h->d_chains, h->nch, h->maxN, h->models[0]->nsub == 2, h->max_lq, h->st); tmark(h, DQMC_PROF_MEASURE); }
         if (m.iwrap_nt[nt] > 0) stab_0b(h, m.iwrap_nt[nt], 1);
     }
 }
@@ -1883,7 +1885,7 @@ extern "C" int dqmc_gpu_update(dqmc_handle* h, int nt) {
 
 extern "C" int dqmc_gpu_measure(dqmc_handle* h) {
     if (!h) return fail(DQMC_EINVAL, "null handle");
-    launch_measure(h->d_chains, h->nch, h->maxN, h->ctas_per_chain, h->st);
+    launch_measure(h->d_chains, h->nch, h->maxN, h->models[0]->nsub == 2, h->max_lq, h->st);
     CK(cudaStreamSynchronize(h->st));
     CK(cudaGetLastError());
     return DQMC_OK;
@@ -1908,7 +1910,7 @@ extern "C" int dqmc_gpu_time_op(dqmc_handle* h, int op, int reps, double* ms_out
         case 2: launch_green(h->d_chains, h->nch, 1, 0, 0, 0, 0, 0, 0, h->st); break;
         case 3: { PropProg p; p.n = 0; prog_k(m, p, PW_INV, 0); prog_v(m, p, PW_INV, 1); prog_k(m, p, PW_INV, 1);
                   launch_prog(h, MAT_G, p, 0); break; }
-        case 4: launch_measure(h->d_chains, h->nch, h->maxN, h->ctas_per_chain, h->st); break;
+        case 4: launch_measure(h->d_chains, h->nch, h->maxN, h->models[0]->nsub == 2, h->max_lq, h->st); break;
         case 5: { PropProg p; p.n = 0; prog_k(m, p, PW_FWD, 0); prog_v(m, p, PW_FWD, 1); prog_k(m, p, PW_FWD, 1);
                   launch_prog(h, MAT_G, p, 1); break; }
         default: break;
@@ -1938,7 +1940,7 @@ extern "C" int dqmc_gpu_time_op(dqmc_handle* h, int op, int reps, double* ms_out
             pflush(h, pp);
             break;
         }
-        case 4: launch_measure(h->d_chains, h->nch, h->maxN, h->ctas_per_chain, h->st); break;
+        case 4: launch_measure(h->d_chains, h->nch, h->maxN, h->models[0]->nsub == 2, h->max_lq, h->st); break;
         default: break;
         }
     };
@@ -2500,7 +2502,7 @@ static void enqueue_0b_blocks(dqmc_handle* h, dqmc_nn* nn, int lupdate, int lmea
         prog_k(m, pr, PW_INV, 1);
         launch_prog(h, MAT_G, pl, 0);
         launch_prog(h, MAT_G, pr, 1);
-        if (lmeasure) launch_measure(h->d_chains, h->nch, h->maxN, h->ctas_per_chain, h->st);
+        if (lmeasure) launch_measure(h->d_chains, h->nch, h->maxN, h->models[0]->nsub == 2, h->max_lq, h->st);
         if (m.iwrap_nt[nt] > 0) stab_0b(h, m.iwrap_nt[nt], 1);
     }
 }

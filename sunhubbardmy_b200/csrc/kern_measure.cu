@@ -1,15 +1,17 @@
-// Equal-time measurement of one time slice; a few CTAs per chain.
+// Equal-time measurement of one time slice; two CTAs per chain.
 //
 // Reference: src/dqmc_measure/equaltime_measure.f90 (equaltime_measure 1-69,
 // zkint, zint_u, zint_v, zqsq, ztsq, ztq, measure_cpcm/spsm/nn/jj/bondcorr/
 // paircorr).  Observables use Gc(i,j) = delta_ij - G(j,i) and are weighted
 // with zphi = sgn/Re(phase) * phase.  G^T is written first (a tiled
 // transpose), so that every correlation term reads a column of G or of G^T.
-// The distance-binned correlations are accumulated without atomics: one
-// thread owns one bin (distance d, orbitals a, b) and walks the unit cells j,
-// pairing each with cell i = j + d (imj(i, j) = d, in closed form);
-// the threads of consecutive d read consecutive rows of the same columns.
-// The single-number energy terms run on the chain's first CTA.
+// The distance-binned correlations are accumulated without atomics: the
+// chain's first CTA walks the unit cells j in order, stages the few columns
+// of G and G^T that cell j pairs with into shared memory (double-buffered
+// cp.async), and every thread adds cell j's term to the two bins (distance
+// d, orbitals a, b) it owns, pairing j with cell i = j + d (imj(i, j) = d, in
+// closed form).  Each column crosses L2 once per cell instead of once per
+// 32 bins.  The single-number energy terms run on the chain's second CTA.
 //
 // Bin layout per chain (complex): energy[10], cpcm, spsm, nn, pair_onsite
 // [lq*4 each, index (d) + lq*(no_i + 2 no_j)], jj, bb, pair_nn, pair_sn [lq
@@ -17,11 +19,14 @@
 #include "chain_access.cuh"
 #include "kernels.h"
 
+#define MEAS_NT 256
+
 DQ_DEV double2 gcf(const double2* G, int N, int i, int j) {   // Gc(i,j)
     double2 g = G[MIDX(j, i, N)];
     return cmk((i == j ? 1.0 : 0.0) - g.x, -g.y);
 }
 DQ_DEV double2 gf(const double2* G, int N, int i, int j) { return G[MIDX(i, j, N)]; }
+DQ_DEV double2 rfma(double a, double2 b, double2 c) { return cmk(fma(a, b.x, c.x), fma(a, b.y, c.y)); }   // a b + c, a real
 
 // cell i = j + d of the distance table imj(i, j) = d (setup_latt2d_sub): with
 // cells c = c1 l2 + c2 and d = dy + l2 dx, i1 = (j1 + dx + 1) mod l1 and
@@ -33,116 +38,16 @@ DQ_DEV int cell_shift(int cj, int dxp, int dyp, int l1, int l2) {
     return i1 * l2 + i2;
 }
 
-__global__ void __launch_bounds__(256) k_measure(const ChainDev* __restrict__ chains) {
+// Energy terms and the background sums zn, zj, zb (single numbers per chain),
+// computed by the chain's second CTA while the first one sums the bins.
+DQ_DEV void meas_energy(const ChainDev& c, double2 zphi, double sgn) {
     __shared__ double red[64];
-    const ChainDev& c = chains[blockIdx.y];
     const ModelDev& md = *c.md;
     const int N = c.N, lq = md.lq, tid = threadIdx.x, nth = blockDim.x;
     const int nnf = md.nn_nf, zp = md.z_plq, nflr = md.nflr;
     const double2* G = c.G;
     double2* bins = c.bins;
-    const double2 phase = cmk(c.stats[ST_PHASE_RE], c.stats[ST_PHASE_IM]);
-    const double sgn = phase.x < 0.0 ? -1.0 : 1.0;
-    const double2 zphi = cscale(phase, sgn / phase.x);
-    const double fsp = 1.0 - 1.0 / (double)(nflr * nflr), fn = 1.0 / (double)nflr;
     const bool hc = (md.nsub == 2);
-
-    // ---- per-site and per-cell quantities shared by all bins (shared memory) ----
-    __shared__ double2 gcd[512];     // Gc(i,i)
-    __shared__ double2 jcell[512];   // Gc(i0,in) - Gc(in,i0), current partner
-    __shared__ double2 bcell[512];   // e Gc(i0,ib) + conj(e) Gc(ib,i0), bond partner
-    __shared__ int pj[512], pb[512], ps[512];
-    for (int i = tid; i < N; i += nth) gcd[i] = gcf(G, N, i, i);
-    for (int cc = tid; cc < lq; cc += nth) {
-        int i0 = hc ? 2 * cc : cc;
-        int inj = hc ? md.snlist[i0 * md.nsn] : md.nnlist[i0 * nnf];
-        int inb = md.nnlist[i0 * nnf];
-        double2 e = md.expar_nn[i0 * nnf];
-        pj[cc] = inj; pb[cc] = inb; ps[cc] = md.snlist[i0 * md.nsn];
-        jcell[cc] = csub(gcf(G, N, i0, inj), gcf(G, N, inj, i0));
-        bcell[cc] = cadd(cmul(e, gcf(G, N, i0, inb)), cmul(cconj(e), gcf(G, N, inb, i0)));
-    }
-    __syncthreads();
-    // ---- distance-binned correlations: one thread per bin, looping over the
-    // cells j; for fixed j the threads of consecutive distances read G and G^T
-    // down a column, so every access is coalesced and each bin is summed in a
-    // fixed order without atomics ----
-    double2* cpcm = bins + 10;
-    double2* spsm = cpcm + 4 * lq;
-    double2* znn = spsm + 4 * lq;
-    double2* pons = znn + 4 * lq;
-    double2* zjj = pons + 4 * lq;
-    double2* zbb = zjj + lq;
-    double2* pnn = zbb + lq;
-    double2* psn = pnn + lq;
-    const double2* GT = c.GT;
-    const int nsub = md.nsub, l1 = md.l1, l2 = md.l2;
-    const int nbin_a = lq * nsub * nsub, nbin = nbin_a + lq;
-    for (int bin = blockIdx.x * nth + tid; bin < nbin; bin += gridDim.x * nth) {
-        if (bin < nbin_a) {
-            const int d = bin % lq, ab = bin / lq, a = ab % nsub, b = ab / nsub;
-            const int dxp = d / l2 + 1, dyp = d % l2 + 1;
-            double2 s1 = cmk(0, 0), s2 = cmk(0, 0), s3 = cmk(0, 0), s4 = cmk(0, 0);
-#pragma unroll 4
-            for (int cj = 0; cj < lq; ++cj) {
-                const int i = cell_shift(cj, dxp, dyp, l1, l2) * nsub + a, j = cj * nsub + b;
-                const size_t o = (size_t)i + (size_t)N * j;
-                const double2 gt = GT[o], g = G[o];          // G(j,i), G(i,j)
-                const double2 gc = cmk((i == j ? 1.0 : 0.0) - gt.x, -gt.y);
-                const double2 gcg = cmul(gc, g);
-                s1 = cadd(s1, gc);
-                s2 = cadd(s2, gcg);
-                s3 = cadd(s3, cadd(cmul(gcd[i], gcd[j]), cscale(gcg, fn)));
-                s4 = cfma(g, g, s4);
-            }
-            const int k = d + lq * (a + 2 * b);
-            cpcm[k] = cfma(s1, zphi, cpcm[k]);
-            spsm[k] = cfma(cscale(s2, fsp), zphi, spsm[k]);
-            znn[k] = cfma(s3, zphi, znn[k]);
-            pons[k] = cfma(s4, zphi, pons[k]);
-        } else {
-            const int d = bin - nbin_a;
-            const int dxp = d / l2 + 1, dyp = d % l2 + 1;
-            // element (r, s) of G is G[r + N s], of G^T (= G(s, r)) GT[r + N s]
-            auto gg = [&](int r, int s_) { return G[(size_t)r + (size_t)N * s_]; };
-            auto gtt = [&](int r, int s_) { return GT[(size_t)r + (size_t)N * s_]; };
-            auto cc = [&](int r, int s_) {            // Gc(r, s) = delta_rs - G(s, r)
-                double2 t = gtt(r, s_);
-                return cmk((r == s_ ? 1.0 : 0.0) - t.x, -t.y);
-            };
-            double2 sj = cmk(0, 0), sb = cmk(0, 0), sn = cmk(0, 0), ss = cmk(0, 0);
-#pragma unroll 4
-            for (int cj = 0; cj < lq; ++cj) {
-                const int ci = cell_shift(cj, dxp, dyp, l1, l2);
-                const int j0 = hc ? 2 * cj : cj, i0 = hc ? 2 * ci : ci;
-                const int jnj = pj[cj], inj = pj[ci], jnb = pb[cj], inb = pb[ci];
-                const double2 g00 = gg(i0, j0), gc00 = cc(i0, j0);
-                // current-current, connected part (measure_jj)
-                double2 z3 = cadd(cmul(cc(i0, jnj), gg(inj, j0)), cmul(cc(inj, j0), gg(i0, jnj)));
-                const double2 gnn_j = gg(inj, jnj), gcnn_j = cc(inj, jnj);
-                z3 = csub(z3, cadd(cmul(gc00, gnn_j), cmul(gcnn_j, g00)));
-                sj = csub(sj, cadd(cmul(jcell[ci], jcell[cj]), cscale(z3, fn)));
-                // bond-bond (measure_bondcorr)
-                const double2 ej = md.expar_nn[j0 * nnf], ei = md.expar_nn[i0 * nnf];
-                const bool same = (jnb == jnj && inb == inj);
-                const double2 gnn_b = same ? gnn_j : gg(inb, jnb);
-                const double2 gcnn_b = same ? gcnn_j : cc(inb, jnb);
-                double2 x = cmul(cmul(ei, ej), cmul(cc(i0, jnb), gg(inb, j0)));
-                x = cadd(x, cmul(cmul(cconj(ei), cconj(ej)), cmul(cc(inb, j0), gg(i0, jnb))));
-                x = cadd(x, cmul(cmul(ei, cconj(ej)), cmul(gc00, gnn_b)));
-                x = cadd(x, cmul(cmul(cconj(ei), ej), cmul(gcnn_b, g00)));
-                sb = cadd(sb, cadd(cmul(bcell[cj], bcell[ci]), cscale(x, fn)));
-                // pair correlations (measure_paircorr)
-                sn = cfma(g00, gnn_b, sn);
-                ss = cfma(g00, gg(ps[ci], ps[cj]), ss);
-            }
-            zjj[d] = cfma(sj, zphi, zjj[d]);
-            zbb[d] = cfma(sb, zphi, zbb[d]);
-            pnn[d] = cfma(sn, zphi, pnn[d]);
-            psn[d] = cfma(ss, zphi, psn[d]);
-        }
-    }
-    if (blockIdx.x != 0) return;
     // ---- energy terms ----
     double2 zne = cmk(0, 0), zu = cmk(0, 0), zk = cmk(0, 0), zv = cmk(0, 0);
     for (int i = tid; i < N; i += nth) {
@@ -241,6 +146,165 @@ __global__ void __launch_bounds__(256) k_measure(const ChainDev* __restrict__ ch
     }
 }
 
+// Site-correlation bins (cpcm, spsm, nn, pair_onsite): one thread per bin
+// (distance d, orbitals a, b) walks the cells j in order.  Accumulates
+// S1 = sum GTc, B = sum GTc G, A = sum gcd_i gcd_j, S4 = sum G G with
+// GTc(i, j) = GT(i, j) - delta_ij = -Gc(i, j); whether site i of cell j + d
+// is site j is the same for every cell j (a translation), so it is taken
+// from cell 0.
+template <bool HC>
+DQ_DEV void meas_site(const ChainDev& c, int bin, double2 zphi) {
+    constexpr int NS = HC ? 2 : 1;
+    __shared__ double2 gcd[512];     // Gc(i,i)
+    const ModelDev& md = *c.md;
+    const int N = c.N, lq = md.lq, l1 = md.l1, l2 = md.l2, nflr = md.nflr;
+    const double2 *G = c.G, *GT = c.GT;
+    for (int i = threadIdx.x; i < N; i += MEAS_NT) gcd[i] = gcf(G, N, i, i);
+    __syncthreads();
+    if (bin >= lq * NS * NS) return;
+    const double fsp = 1.0 - 1.0 / (double)(nflr * nflr), fn = 1.0 / (double)nflr;
+    const int d = bin % lq, ab = bin / lq, a = ab % NS, b = ab / NS;
+    const int dxp = d / l2 + 1, dyp = d % l2 + 1;
+    const double fd = (cell_shift(0, dxp, dyp, l1, l2) == 0 && a == b) ? 1.0 : 0.0;
+    double2 s1 = cmk(0, 0), sB = cmk(0, 0), sA = cmk(0, 0), s4 = cmk(0, 0);
+#pragma unroll 4
+    for (int cj = 0; cj < lq; ++cj) {
+        const int i = cell_shift(cj, dxp, dyp, l1, l2) * NS + a, j = cj * NS + b;
+        const size_t o = (size_t)i + (size_t)N * j;
+        double2 gtc = GT[o];
+        const double2 g = G[o];
+        gtc.x -= fd;
+        s1 = cadd(s1, gtc);
+        sB = cfma(gtc, g, sB);
+        sA = cfma(gcd[i], gcd[j], sA);
+        s4 = cfma(g, g, s4);
+    }
+    double2* bins = c.bins;
+    double2* cpcm = bins + 10;
+    double2* spsm = cpcm + 4 * lq;
+    double2* znn = spsm + 4 * lq;
+    double2* pons = znn + 4 * lq;
+    const int k = d + lq * (a + 2 * b);
+    cpcm[k] = cfma(cmk(-s1.x, -s1.y), zphi, cpcm[k]);
+    spsm[k] = cfma(cscale(cmk(-sB.x, -sB.y), fsp), zphi, spsm[k]);
+    znn[k] = cfma(rfma(-fn, sB, sA), zphi, znn[k]);
+    pons[k] = cfma(s4, zphi, pons[k]);
+}
+
+// Bond-correlation bins (jj, bb, pair_nn, pair_sn): one thread per distance d
+// walks the cells j in order, pairing site i0 of cell i = j + d and its
+// partners with site j0 and its partners.  The partners are translations
+// (current partner pj: nearest neighbour on the square lattice, second
+// neighbour on the honeycomb; bond partner pb: nearest neighbour; pair
+// partner ps: second neighbour), so on the square lattice the Kronecker
+// deltas of Gc = delta - GT depend on d only and are taken from cell 0.
+template <bool HC>
+DQ_DEV void meas_bond(const ChainDev& c, int d, double2 zphi) {
+    constexpr int NS = HC ? 2 : 1;
+    __shared__ double2 jcell[512];   // Gc(i0,in) - Gc(in,i0), current partner
+    __shared__ double2 bcell[512];   // e Gc(i0,ib) + conj(e) Gc(ib,i0), bond partner
+    __shared__ double2 pe[512];      // e = expar_nn(i0, first direction)
+    __shared__ int pj[512], pb[512], ps[512];
+    const ModelDev& md = *c.md;
+    const int N = c.N, lq = md.lq, l1 = md.l1, l2 = md.l2, nnf = md.nn_nf;
+    const double2 *G = c.G, *GT = c.GT;
+    for (int cc = threadIdx.x; cc < lq; cc += MEAS_NT) {
+        const int i0 = cc * NS;
+        const int inj = HC ? md.snlist[i0 * md.nsn] : md.nnlist[i0 * nnf];
+        const int inb = md.nnlist[i0 * nnf];
+        const double2 e = md.expar_nn[i0 * nnf];
+        pj[cc] = inj; pb[cc] = inb; ps[cc] = md.snlist[i0 * md.nsn]; pe[cc] = e;
+        jcell[cc] = csub(gcf(G, N, i0, inj), gcf(G, N, inj, i0));
+        bcell[cc] = cadd(cmul(e, gcf(G, N, i0, inb)), cmul(cconj(e), gcf(G, N, inb, i0)));
+    }
+    __syncthreads();
+    if (d >= lq) return;
+    const double fn = 1.0 / (double)md.nflr;
+    const int dxp = d / l2 + 1, dyp = d % l2 + 1;
+    auto gg = [&](int r, int s_) { return G[(size_t)r + (size_t)N * s_]; };
+    auto gt = [&](int r, int s_) { return GT[(size_t)r + (size_t)N * s_]; };
+    // deltas of the square lattice, from cell 0: [i0 == j0], [in == j0], [i0 == jn], [in == jn]
+    double f00 = 0, fn0 = 0, f0n = 0, fnn = 0;
+    if (!HC) {
+        const int ci = cell_shift(0, dxp, dyp, l1, l2), in = pj[ci], jn = pj[0];
+        f00 = ci == 0; fn0 = in == 0; f0n = ci == jn; fnn = in == jn;
+    }
+    double2 sj = cmk(0, 0), sb = cmk(0, 0), sn = cmk(0, 0), ss = cmk(0, 0);
+#pragma unroll 4
+    for (int cj = 0; cj < lq; ++cj) {
+        const int ci = cell_shift(cj, dxp, dyp, l1, l2);
+        const int j0 = cj * NS, i0 = ci * NS, jnj = pj[cj], inj = pj[ci];
+        const double2 ei = pe[ci], ej = pe[cj];
+        // G and GTc = GT - delta (= -Gc) at rows i0, in of columns j0, jn
+        const double2 g00 = gg(i0, j0), an = gg(inj, j0), b0v = gg(i0, jnj), gnn_j = gg(inj, jnj);
+        double2 t0 = gt(i0, j0), tn = gt(inj, j0), u0 = gt(i0, jnj), un = gt(inj, jnj);
+        if (HC) {
+            t0.x -= i0 == j0; tn.x -= inj == j0; u0.x -= i0 == jnj; un.x -= inj == jnj;
+        } else {
+            t0.x -= f00; tn.x -= fn0; u0.x -= f0n; un.x -= fnn;
+        }
+        // connected current-current part (measure_jj), Gc = -GTc:
+        // z3 = Gc(i0,jn) G(in,j0) + Gc(in,j0) G(i0,jn) - Gc(i0,j0) G(in,jn) - Gc(in,jn) G(i0,j0)
+        const double2 q1 = cmul(u0, an), q2 = cmul(tn, b0v);
+        const double2 q3 = cmul(t0, gnn_j), q4 = cmul(un, g00);
+        const double2 z3 = csub(cadd(q3, q4), cadd(q1, q2));
+        sj = csub(sj, rfma(fn, z3, cmul(jcell[ci], jcell[cj])));
+        // bond-bond (measure_bondcorr): x = ei ej Gc(i0,jb) G(ib,j0)
+        //   + conj(ei ej) Gc(ib,j0) G(i0,jb) + ei conj(ej) Gc(i0,j0) G(ib,jb)
+        //   + conj(ei) ej Gc(ib,jb) G(i0,j0), accumulated here negated
+        const double2 ee = cmul(ei, ej), ef = cmul(ei, cconj(ej));
+        double2 x, gnn_b;
+        if (!HC) {
+            // square lattice: the bond partner is the current partner (pb == pj)
+            gnn_b = gnn_j;
+            x = cmul(ee, q1);
+            x = cfma(cconj(ee), q2, x);
+            x = cfma(ef, q3, x);
+            x = cfma(cconj(ef), q4, x);
+        } else {
+            const int jnb = pb[cj], inb = pb[ci];
+            const bool same = (jnb == jnj && inb == inj);
+            gnn_b = same ? gnn_j : gg(inb, jnb);
+            double2 tnb = un;                                    // GTc(ib, jb)
+            if (!same) { tnb = gt(inb, jnb); tnb.x -= inb == jnb; }
+            double2 v1 = gt(i0, jnb), v2 = gt(inb, j0);
+            v1.x -= i0 == jnb; v2.x -= inb == j0;
+            const double2 r1 = cmul(v1, gg(inb, j0)), r2 = cmul(v2, gg(i0, jnb));
+            const double2 r3 = cmul(t0, gnn_b), r4 = cmul(tnb, g00);
+            x = cmul(ee, r1);
+            x = cfma(cconj(ee), r2, x);
+            x = cfma(ef, r3, x);
+            x = cfma(cconj(ef), r4, x);
+        }
+        sb = cadd(sb, rfma(-fn, x, cmul(bcell[cj], bcell[ci])));
+        // pair correlations (measure_paircorr)
+        sn = cfma(g00, gnn_b, sn);
+        ss = cfma(g00, gg(ps[ci], ps[cj]), ss);
+    }
+    double2* zjj = c.bins + 10 + 16 * (size_t)lq;
+    double2* zbb = zjj + lq;
+    double2* pnn = zbb + lq;
+    double2* psn = pnn + lq;
+    zjj[d] = cfma(sj, zphi, zjj[d]);
+    zbb[d] = cfma(sb, zphi, zbb[d]);
+    pnn[d] = cfma(sn, zphi, pnn[d]);
+    psn[d] = cfma(ss, zphi, psn[d]);
+}
+
+// grid (1 + na + nb, chains): x = 0 the energy terms, then na CTAs of site
+// bins and nb CTAs of bond bins (sized for the largest lattice of the handle)
+template <bool HC>
+__global__ void __launch_bounds__(MEAS_NT, 2) k_measure(const ChainDev* __restrict__ chains, int na) {
+    const ChainDev& c = chains[blockIdx.y];
+    const double2 phase = cmk(c.stats[ST_PHASE_RE], c.stats[ST_PHASE_IM]);
+    const double sgn = phase.x < 0.0 ? -1.0 : 1.0;
+    const double2 zphi = cscale(phase, sgn / phase.x);
+    const int x = blockIdx.x;
+    if (x == 0) meas_energy(c, zphi, sgn);
+    else if (x <= na) meas_site<HC>(c, (x - 1) * MEAS_NT + threadIdx.x, zphi);
+    else meas_bond<HC>(c, (x - 1 - na) * MEAS_NT + threadIdx.x, zphi);
+}
+
 __global__ void k_bins_clear(const ChainDev* __restrict__ chains, int nbins) {
     const ChainDev c = chains[blockIdx.x];
     (void)nbins;
@@ -273,11 +337,14 @@ __global__ void __launch_bounds__(256) k_transpose_g(const ChainDev* __restrict_
     }
 }
 
-void launch_measure(const ChainDev* chains, int nchains, int maxN, int ctas_per_chain, cudaStream_t st) {
+void launch_measure(const ChainDev* chains, int nchains, int maxN, int hc, int maxlq, cudaStream_t st) {
     const int nt = (maxN + 31) / 32;
     k_transpose_g<<<dim3(nt, nt, nchains), 256, 0, st>>>(chains, MAT_G);
-    dim3 grid(ctas_per_chain, nchains);
-    k_measure<<<grid, 256, 0, st>>>(chains);
+    const int ns = hc ? 2 : 1;
+    const int na = (maxlq * ns * ns + MEAS_NT - 1) / MEAS_NT, nb = (maxlq + MEAS_NT - 1) / MEAS_NT;
+    const dim3 grid(1 + na + nb, nchains);
+    if (hc) k_measure<true><<<grid, MEAS_NT, 0, st>>>(chains, na);
+    else k_measure<false><<<grid, MEAS_NT, 0, st>>>(chains, na);
 }
 
 // dyn_measure (src/dqmc_measure/dyn_measure.f90:1-101) at time index nt: the

@@ -249,9 +249,10 @@ DQ_DEV void fft_dir(double2 (&x)[L], int sg, double c1, double s1, double h) {
     else fft_reg<L, -1>(x, c1, s1, h);
 }
 
-template <int L>
+template <int L, bool ROWS>
 __global__ void __launch_bounds__(128, 4) k_prop_fft(const ChainDev* __restrict__ chains, int mat_id, PropProg prog,
-                                                     int rows, int right, int tall, double c1, double s1, double h) {
+                                                     int right, int tall, double c1, double s1, double h) {
+    constexpr bool rows = ROWS;
     constexpr int VPC = 128 / L;    // vectors per CTA
     constexpr int LD = L + 1;       // odd row pitch: conflict-free transposes
     constexpr int TS = L * LD + 1;  // per-vector region; the +1 spreads the row-tile stores over the banks
@@ -360,11 +361,15 @@ void launch_prop_fft(const ChainDev* chains, int nchains, int L, int nvec, int m
     const double c1 = std::cos(M_PI / 8), s1 = std::sin(M_PI / 8), h = std::sqrt(0.5);
     const int vpc = 128 / L;
     dim3 grid((nvec + vpc - 1) / vpc, nchains);
+#define PROP_FFT_CASE(LL)                                                                        \
+    if (rows) k_prop_fft<LL, true><<<grid, 128, 0, st>>>(chains, mat_id, prog, right, tall, c1, s1, h); \
+    else k_prop_fft<LL, false><<<grid, 128, 0, st>>>(chains, mat_id, prog, right, tall, c1, s1, h);
     switch (L) {
-    case 16: k_prop_fft<16><<<grid, 128, 0, st>>>(chains, mat_id, prog, rows, right, tall, c1, s1, h); break;
-    case 8: k_prop_fft<8><<<grid, 128, 0, st>>>(chains, mat_id, prog, rows, right, tall, c1, s1, h); break;
-    default: k_prop_fft<4><<<grid, 128, 0, st>>>(chains, mat_id, prog, rows, right, tall, c1, s1, h); break;
+    case 16: PROP_FFT_CASE(16) break;
+    case 8: PROP_FFT_CASE(8) break;
+    default: PROP_FFT_CASE(4) break;
     }
+#undef PROP_FFT_CASE
 }
 
 static int g_prop_smem_ok = 0;

@@ -16,7 +16,7 @@ void launch_sfmt(const ChainDev* chains, int nchains, int slices, cudaStream_t s
 void launch_sfmt_raw(const ChainDev* chains, int chain, int count, cudaStream_t st);
 void launch_update(const ChainDev* chains, int nchains, int nt, int visit, cudaStream_t st, int forced = 0);
 // equal-time measurement: G^T into GT (tiled transpose), then the observables
-void launch_measure(const ChainDev* chains, int nchains, int maxN, int ctas_per_chain, cudaStream_t st);
+void launch_measure(const ChainDev* chains, int nchains, int maxN, int hc, int maxlq, cudaStream_t st);
 void launch_bins_clear(const ChainDev* chains, int nchains, int nbins, cudaStream_t st);
 void launch_stab_slots(const ChainDev* chains, int nchains, int src, int dst, cudaStream_t st);
 void launch_swap_slots(int* slotmap, int n, int spare, cudaStream_t st);
