@@ -20,6 +20,8 @@
 #include "kernels.h"
 
 #define MEAS_NT 256
+#define MEAS_SPLIT 2                       // threads per bin
+#define MEAS_BH (MEAS_NT / MEAS_SPLIT)    // bins per CTA
 
 DQ_DEV double2 gcf(const double2* G, int N, int i, int j) {   // Gc(i,j)
     double2 g = G[MIDX(j, i, N)];
@@ -146,14 +148,29 @@ DQ_DEV void meas_energy(const ChainDev& c, double2 zphi, double sgn) {
     }
 }
 
-// Site-correlation bins (cpcm, spsm, nn, pair_onsite): one thread per bin
-// (distance d, orbitals a, b) walks the cells j in order.  Accumulates
+// The cells of a bin are split by residue mod MEAS_SPLIT between threads
+// t + k MEAS_BH of the CTA; the partial sums are added to thread t's in the
+// order k = 1, 2, ..., so the result does not depend on scheduling.
+DQ_DEV void meas_combine(double2& a0, double2& a1, double2& a2, double2& a3, int h) {
+    __shared__ double2 part[4][MEAS_BH];
+    const int t = threadIdx.x % MEAS_BH;
+#pragma unroll
+    for (int k = 1; k < MEAS_SPLIT; ++k) {
+        if (h == k) { part[0][t] = a0; part[1][t] = a1; part[2][t] = a2; part[3][t] = a3; }
+        __syncthreads();
+        if (h == 0) { a0 = cadd(a0, part[0][t]); a1 = cadd(a1, part[1][t]); a2 = cadd(a2, part[2][t]); a3 = cadd(a3, part[3][t]); }
+        __syncthreads();
+    }
+}
+
+// Site-correlation bins (cpcm, spsm, nn, pair_onsite): MEAS_SPLIT threads per
+// bin (distance d, orbitals a, b) walk interleaved cells j in order.  Accumulates
 // S1 = sum GTc, B = sum GTc G, A = sum gcd_i gcd_j, S4 = sum G G with
 // GTc(i, j) = GT(i, j) - delta_ij = -Gc(i, j); whether site i of cell j + d
 // is site j is the same for every cell j (a translation), so it is taken
 // from cell 0.
 template <bool HC>
-DQ_DEV void meas_site(const ChainDev& c, int bin, double2 zphi) {
+DQ_DEV void meas_site(const ChainDev& c, int bin, double2 zphi) {   // bin of thread t % MEAS_BH
     constexpr int NS = HC ? 2 : 1;
     __shared__ double2 gcd[512];     // Gc(i,i)
     const ModelDev& md = *c.md;
@@ -161,14 +178,16 @@ DQ_DEV void meas_site(const ChainDev& c, int bin, double2 zphi) {
     const double2 *G = c.G, *GT = c.GT;
     for (int i = threadIdx.x; i < N; i += MEAS_NT) gcd[i] = gcf(G, N, i, i);
     __syncthreads();
-    if (bin >= lq * NS * NS) return;
+    const bool valid = bin < lq * NS * NS;
+    const int h = threadIdx.x / MEAS_BH;      // cells j = h (mod MEAS_SPLIT)
+    if (!valid) bin = 0;
     const double fsp = 1.0 - 1.0 / (double)(nflr * nflr), fn = 1.0 / (double)nflr;
     const int d = bin % lq, ab = bin / lq, a = ab % NS, b = ab / NS;
     const int dxp = d / l2 + 1, dyp = d % l2 + 1;
     const double fd = (cell_shift(0, dxp, dyp, l1, l2) == 0 && a == b) ? 1.0 : 0.0;
     double2 s1 = cmk(0, 0), sB = cmk(0, 0), sA = cmk(0, 0), s4 = cmk(0, 0);
 #pragma unroll 4
-    for (int cj = 0; cj < lq; ++cj) {
+    for (int cj = valid ? h : lq; cj < lq; cj += MEAS_SPLIT) {
         const int i = cell_shift(cj, dxp, dyp, l1, l2) * NS + a, j = cj * NS + b;
         const size_t o = (size_t)i + (size_t)N * j;
         double2 gtc = GT[o];
@@ -179,6 +198,8 @@ DQ_DEV void meas_site(const ChainDev& c, int bin, double2 zphi) {
         sA = cfma(gcd[i], gcd[j], sA);
         s4 = cfma(g, g, s4);
     }
+    meas_combine(s1, sB, sA, s4, h);
+    if (!valid || h) return;
     double2* bins = c.bins;
     double2* cpcm = bins + 10;
     double2* spsm = cpcm + 4 * lq;
@@ -191,15 +212,15 @@ DQ_DEV void meas_site(const ChainDev& c, int bin, double2 zphi) {
     pons[k] = cfma(s4, zphi, pons[k]);
 }
 
-// Bond-correlation bins (jj, bb, pair_nn, pair_sn): one thread per distance d
-// walks the cells j in order, pairing site i0 of cell i = j + d and its
+// Bond-correlation bins (jj, bb, pair_nn, pair_sn): MEAS_SPLIT threads per
+// distance d walk interleaved cells j in order, pairing site i0 of cell i = j + d and its
 // partners with site j0 and its partners.  The partners are translations
 // (current partner pj: nearest neighbour on the square lattice, second
 // neighbour on the honeycomb; bond partner pb: nearest neighbour; pair
 // partner ps: second neighbour), so on the square lattice the Kronecker
 // deltas of Gc = delta - GT depend on d only and are taken from cell 0.
 template <bool HC>
-DQ_DEV void meas_bond(const ChainDev& c, int d, double2 zphi) {
+DQ_DEV void meas_bond(const ChainDev& c, int d, double2 zphi) {   // distance of thread t % MEAS_BH
     constexpr int NS = HC ? 2 : 1;
     __shared__ double2 jcell[512];   // Gc(i0,in) - Gc(in,i0), current partner
     __shared__ double2 bcell[512];   // e Gc(i0,ib) + conj(e) Gc(ib,i0), bond partner
@@ -218,7 +239,9 @@ DQ_DEV void meas_bond(const ChainDev& c, int d, double2 zphi) {
         bcell[cc] = cadd(cmul(e, gcf(G, N, i0, inb)), cmul(cconj(e), gcf(G, N, inb, i0)));
     }
     __syncthreads();
-    if (d >= lq) return;
+    const bool valid = d < lq;
+    const int h = threadIdx.x / MEAS_BH;      // cells j = h (mod MEAS_SPLIT)
+    if (!valid) d = 0;
     const double fn = 1.0 / (double)md.nflr;
     const int dxp = d / l2 + 1, dyp = d % l2 + 1;
     auto gg = [&](int r, int s_) { return G[(size_t)r + (size_t)N * s_]; };
@@ -231,7 +254,7 @@ DQ_DEV void meas_bond(const ChainDev& c, int d, double2 zphi) {
     }
     double2 sj = cmk(0, 0), sb = cmk(0, 0), sn = cmk(0, 0), ss = cmk(0, 0);
 #pragma unroll 4
-    for (int cj = 0; cj < lq; ++cj) {
+    for (int cj = valid ? h : lq; cj < lq; cj += MEAS_SPLIT) {
         const int ci = cell_shift(cj, dxp, dyp, l1, l2);
         const int j0 = cj * NS, i0 = ci * NS, jnj = pj[cj], inj = pj[ci];
         const double2 ei = pe[ci], ej = pe[cj];
@@ -281,6 +304,8 @@ DQ_DEV void meas_bond(const ChainDev& c, int d, double2 zphi) {
         sn = cfma(g00, gnn_b, sn);
         ss = cfma(g00, gg(ps[ci], ps[cj]), ss);
     }
+    meas_combine(sj, sb, sn, ss, h);
+    if (!valid || h) return;
     double2* zjj = c.bins + 10 + 16 * (size_t)lq;
     double2* zbb = zjj + lq;
     double2* pnn = zbb + lq;
@@ -301,8 +326,8 @@ __global__ void __launch_bounds__(MEAS_NT, 2) k_measure(const ChainDev* __restri
     const double2 zphi = cscale(phase, sgn / phase.x);
     const int x = blockIdx.x;
     if (x == 0) meas_energy(c, zphi, sgn);
-    else if (x <= na) meas_site<HC>(c, (x - 1) * MEAS_NT + threadIdx.x, zphi);
-    else meas_bond<HC>(c, (x - 1 - na) * MEAS_NT + threadIdx.x, zphi);
+    else if (x <= na) meas_site<HC>(c, (x - 1) * MEAS_BH + threadIdx.x % MEAS_BH, zphi);
+    else meas_bond<HC>(c, (x - 1 - na) * MEAS_BH + threadIdx.x % MEAS_BH, zphi);
 }
 
 __global__ void k_bins_clear(const ChainDev* __restrict__ chains, int nbins) {
@@ -341,7 +366,7 @@ void launch_measure(const ChainDev* chains, int nchains, int maxN, int hc, int m
     const int nt = (maxN + 31) / 32;
     k_transpose_g<<<dim3(nt, nt, nchains), 256, 0, st>>>(chains, MAT_G);
     const int ns = hc ? 2 : 1;
-    const int na = (maxlq * ns * ns + MEAS_NT - 1) / MEAS_NT, nb = (maxlq + MEAS_NT - 1) / MEAS_NT;
+    const int na = (maxlq * ns * ns + MEAS_BH - 1) / MEAS_BH, nb = (maxlq + MEAS_BH - 1) / MEAS_BH;
     const dim3 grid(1 + na + nb, nchains);
     if (hc) k_measure<true><<<grid, MEAS_NT, 0, st>>>(chains, na);
     else k_measure<false><<<grid, MEAS_NT, 0, st>>>(chains, na);
