@@ -32,73 +32,129 @@ struct LinalgSmem {
 };
 
 // ---- panel factorisation (zgeqr2 on an m x jb panel in shared memory) ----
+// Reflector of column j from alpha = P(j, j) and xnorm = ||P(j+1:m, j)|| (zlarfg),
+// computed by thread 0: tau, the scale 1 / (alpha - beta) of the vector, and
+// P(j, j) = beta.
+static __device__ void panel_reflector(double2* col, int j, double xnorm, double2* taus, LinalgSmem* L) {
+    double2 alpha = col[j];
+    if (xnorm == 0.0 && alpha.y == 0.0) {
+        L->tau_j = cmk(0, 0);
+        L->scal = cmk(1, 0);
+    } else {
+        double ax = fabs(alpha.x), ay = fabs(alpha.y);
+        double w = fmax(ax, fmax(ay, xnorm));
+        double nrm = w * sqrt((ax / w) * (ax / w) + (ay / w) * (ay / w) + (xnorm / w) * (xnorm / w));
+        double beta = -copysign(nrm, alpha.x);
+        L->tau_j = cmk((beta - alpha.x) / beta, -alpha.y / beta);
+        L->scal = cdiv(cmk(1, 0), csub(alpha, cmk(beta, 0)));
+        col[j] = cmk(beta, 0.0);
+    }
+    taus[j] = L->tau_j;
+}
+
+// Column j of the panel when the plain sum of squares under/overflows: the
+// norm is taken with rescaling and the vector is scaled before the products.
+static __device__ void panel_column_careful(double2* P, int m, int ldp, int jb, int j, double2* taus, LinalgSmem* L) {
+    const int tid = threadIdx.x, nth = blockDim.x;
+    double2* col = P + (size_t)j * ldp;
+    double mx = 0.0;
+    for (int r = j + 1 + tid; r < m; r += nth) mx = fmax(mx, fmax(fabs(col[r].x), fabs(col[r].y)));
+    mx = block_max(mx, L->red);
+    double s2 = 0.0;
+    if (mx > 0.0)
+        for (int r = j + 1 + tid; r < m; r += nth) s2 += cabs2(cscale(col[r], 1.0 / mx));
+    s2 = block_sum(s2, L->red);
+    if (tid == 0) panel_reflector(col, j, mx * sqrt(s2), taus, L);
+    __syncthreads();
+    const double2 tau = L->tau_j, scal = L->scal;
+    if (tau.x == 0.0 && tau.y == 0.0) { __syncthreads(); return; }
+    for (int r = j + 1 + tid; r < m; r += nth) col[r] = cmul(col[r], scal);
+    __syncthreads();
+    // w_c = v^H P[:, c], c > j ; groups of 16 threads
+    const int grp = tid >> 4, gl = tid & 15;
+    for (int base = j + 1; base < jb; base += nth / 16) {     // uniform trip count
+        const int cc = base + grp;
+        const bool ok = cc < jb;
+        double2 acc = cmk(0, 0);
+        if (ok) {
+            const double2* pc = P + (size_t)cc * ldp;
+            if (gl == 0) acc = pc[j];
+            for (int r = j + 1 + gl; r < m; r += 16) acc = cfma(cconj(col[r]), pc[r], acc);
+        }
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) {
+            acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o, 16);
+            acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o, 16);
+        }
+        if (ok && gl == 0) L->w[cc] = acc;
+    }
+    __syncthreads();
+    // P[r, c] -= conj(tau) v_r w_c
+    const double2 ctau = cconj(tau);
+    const int nc = jb - j - 1, nr = m - j;
+    for (int e = tid; e < nc * nr; e += nth) {
+        int cc = j + 1 + e / nr, r = j + e % nr;
+        double2 v = (r == j) ? cmk(1, 0) : col[r];
+        double2 f = cmul(ctau, L->w[cc]);
+        P[(size_t)cc * ldp + r] = csub(P[(size_t)cc * ldp + r], cmul(v, f));
+    }
+    __syncthreads();
+}
+
+// Householder QR of the m x jb panel, three barriers per column: one pass
+// forms ||P(j+1:m, j)||^2 and the raw products d_c = P(j+1:m, j)^H P(j+1:m, c)
+// together (16-thread groups, one per column), thread 0 forms the reflector
+// and w_c = v^H P(:, c) = P(j, c) + conj(scal) d_c, and one row-owned pass
+// scales the vector and applies P(r, c) -= conj(tau) v_r w_c.
 static __device__ void panel_qr(double2* P, int m, int ldp, int jb, double2* taus, LinalgSmem* L) {
     const int tid = threadIdx.x, nth = blockDim.x;
+    const int grp = tid >> 4, gl = tid & 15;
     for (int j = 0; j < jb; ++j) {
         double2* col = P + (size_t)j * ldp;
-        double ss = 0.0;
-        for (int r = j + 1 + tid; r < m; r += nth) ss += cabs2(col[r]);
-        ss = block_sum(ss, L->red);
-        double xnorm = sqrt(ss);
-        // rescale when the plain sum of squares under/overflows (block-uniform branch)
-        if (!(ss < 1e300) || (ss > 0.0 && ss < 1e-280)) {
-            double mx = 0.0;
-            for (int r = j + 1 + tid; r < m; r += nth) mx = fmax(mx, fmax(fabs(col[r].x), fabs(col[r].y)));
-            mx = block_max(mx, L->red);
-            double s2 = 0.0;
-            if (mx > 0.0)
-                for (int r = j + 1 + tid; r < m; r += nth) s2 += cabs2(cscale(col[r], 1.0 / mx));
-            s2 = block_sum(s2, L->red);
-            xnorm = mx * sqrt(s2);
-        }
-        if (tid == 0) {
-            double2 alpha = col[j];
-            if (xnorm == 0.0 && alpha.y == 0.0) {
-                L->tau_j = cmk(0, 0);
-                L->scal = cmk(1, 0);
-            } else {
-                double ax = fabs(alpha.x), ay = fabs(alpha.y);
-                double w = fmax(ax, fmax(ay, xnorm));
-                double nrm = w * sqrt((ax / w) * (ax / w) + (ay / w) * (ay / w) + (xnorm / w) * (xnorm / w));
-                double beta = -copysign(nrm, alpha.x);
-                L->tau_j = cmk((beta - alpha.x) / beta, -alpha.y / beta);
-                L->scal = cdiv(cmk(1, 0), csub(alpha, cmk(beta, 0)));
-                col[j] = cmk(beta, 0.0);
-            }
-            taus[j] = L->tau_j;
-        }
-        __syncthreads();
-        const double2 tau = L->tau_j, scal = L->scal;
-        if (tau.x == 0.0 && tau.y == 0.0) { __syncthreads(); continue; }
-        for (int r = j + 1 + tid; r < m; r += nth) col[r] = cmul(col[r], scal);
-        __syncthreads();
-        // w_c = v^H P[:, c], c > j ; 16 groups of 16 threads
-        const int grp = tid >> 4, gl = tid & 15;
-        for (int base = j + 1; base < jb; base += nth / 16) {     // uniform trip count
-            const int cc = base + grp;
-            const bool ok = cc < jb;
+        for (int base = 0; base < jb - j; base += nth / 16) {    // uniform trip count
+            const int g = base + grp;
+            const bool ok = g < jb - j;
             double2 acc = cmk(0, 0);
             if (ok) {
-                const double2* pc = P + (size_t)cc * ldp;
-                if (gl == 0) acc = pc[j];
-                for (int r = j + 1 + gl; r < m; r += 16) acc = cfma(cconj(col[r]), pc[r], acc);
+                if (g == 0) {
+                    for (int r = j + 1 + gl; r < m; r += 16) acc.x += cabs2(col[r]);
+                } else {
+                    const double2* pc = P + (size_t)(j + g) * ldp;
+                    for (int r = j + 1 + gl; r < m; r += 16) acc = cfma(cconj(col[r]), pc[r], acc);
+                }
             }
 #pragma unroll
             for (int o = 8; o > 0; o >>= 1) {
                 acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o, 16);
                 acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o, 16);
             }
-            if (ok && gl == 0) L->w[cc] = acc;
+            if (ok && gl == 0) L->w[j + g] = acc;
         }
         __syncthreads();
-        // P[r, c] -= conj(tau) v_r w_c
+        if (tid == 0) {
+            const double ss = L->w[j].x;
+            const int careful = !(ss < 1e300) || (ss > 0.0 && ss < 1e-280);
+            L->flag = careful;
+            if (!careful) {
+                panel_reflector(col, j, sqrt(ss), taus, L);
+                const double2 cs = cconj(L->scal);
+                for (int cc = j + 1; cc < jb; ++cc) L->w[cc] = cfma(cs, L->w[cc], P[(size_t)cc * ldp + j]);
+            }
+        }
+        __syncthreads();
+        if (L->flag) {
+            panel_column_careful(P, m, ldp, jb, j, taus, L);
+            continue;
+        }
+        const double2 tau = L->tau_j, scal = L->scal;
+        if (tau.x == 0.0 && tau.y == 0.0) continue;
         const double2 ctau = cconj(tau);
-        const int nc = jb - j - 1, nr = m - j;
-        for (int e = tid; e < nc * nr; e += nth) {
-            int cc = j + 1 + e / nr, r = j + e % nr;
-            double2 v = (r == j) ? cmk(1, 0) : col[r];
-            double2 f = cmul(ctau, L->w[cc]);
-            P[(size_t)cc * ldp + r] = csub(P[(size_t)cc * ldp + r], cmul(v, f));
+        for (int r = j + tid; r < m; r += nth) {
+            const double2 v = (r == j) ? cmk(1, 0) : cmul(col[r], scal);
+            const double2 cv = cmul(ctau, v);
+            for (int cc = j + 1; cc < jb; ++cc)
+                P[(size_t)cc * ldp + r] = csub(P[(size_t)cc * ldp + r], cmul(cv, L->w[cc]));
+            if (r > j) col[r] = v;
         }
         __syncthreads();
     }
