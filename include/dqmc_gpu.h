@@ -45,6 +45,7 @@ extern "C" {
 #define DQMC_UPD_SUBMATRIX 2   /* -DSUBMATRIX */
 #define DQMC_KIN_CHECKERBOARD 0 /* -DBREAKUP_T */
 #define DQMC_KIN_FFT 1          /* -DFFT (square lattice, l1 == l2) */
+#define DQMC_KIN_DENSE 2        /* neither: zgemm with the dense exp(-+dtau H0 / 2) */
 #define DQMC_HS_EXACT 0        /* -DEXACTHS */
 #define DQMC_HS_GENERAL4 1     /* no -DEXACTHS */
 

@@ -171,6 +171,26 @@ static void set_h0(orc_model *m) {
                 exp2x2(d, z, 0.5 * p->dtau, &m->urt[ist * 4]);
                 exp2x2(d, z, -0.5 * p->dtau, &m->urtm1[ist * 4]);
             }
+    } else if (p->kinetic == ORC_DENSE) {
+        /* urt = U exp(-dtau e / 2) U^H, urtm1 = U exp(+dtau e / 2) U^H from the
+         * eigen-decomposition of h0mat (dqmc_set_h0conf.f90:484-509) */
+        m->urtd = zalloc((size_t)N * N);
+        m->urtm1d = zalloc((size_t)N * N);
+        double *w = (double *)malloc(sizeof(double) * N);
+        zc *u = zalloc((size_t)N * N);
+        orc_eig_he(N, m->h0mat, w, u);
+        for (int i = 0; i < N; ++i)
+            for (int j = 0; j < N; ++j) {
+                zc z0 = 0, z1 = 0;
+                for (int k = 0; k < N; ++k) {
+                    zc t = u[ZIDX(i, k, N)] * conj(u[ZIDX(j, k, N)]);
+                    z0 += t * exp(-0.5 * p->dtau * w[k]);
+                    z1 += t * exp(0.5 * p->dtau * w[k]);
+                }
+                m->urtd[ZIDX(i, j, N)] = z0;
+                m->urtm1d[ZIDX(i, j, N)] = z1;
+            }
+        free(w); free(u);
     } else {
         /* h0k = diag(F H F^-1) with F the scaled forward DFT over (l1, l2) */
         int lq = m->lq;
@@ -261,7 +281,7 @@ void orc_model_free(orc_model *m) {
     if (!m) return;
     orc_latt_free(&m->L);
     free(m->iwrap_nt); free(m->wrap_step); free(m->urt); free(m->urtm1);
-    free(m->exph0k); free(m->exph0kinv); free(m->tw1); free(m->tw2); free(m->h0mat); free(m->expar_nn);
+    free(m->exph0k); free(m->exph0kinv); free(m->urtd); free(m->urtm1d); free(m->tw1); free(m->tw2); free(m->h0mat); free(m->expar_nn);
     free(m);
 }
 
@@ -426,7 +446,39 @@ static void h0_cb(const orc_model *m, int op, int nf, zc *g, int n2) {
 }
 
 /* FFT h0conf props (-DFFT, square): B_K = F^-1 diag(exph0k) F */
+/* dense kinetic step, the zgemm branch of the h0conf props
+ * (src/dqmc_config_h0/dqmc_left_forward_prop.f90:235-246, _hc.f90:240,
+ * dqmc_left_backward_prop.f90:236, dqmc_right_forward_prop.f90:276,
+ * dqmc_right_backward_prop.f90:268): left ops g (N x n2) <- K g, right ops
+ * g (n2 x N) <- g K, K = urtm1 for the backward ops and urt otherwise (urt is
+ * Hermitian, so the _hc op uses it as well) */
+static void h0_dense(const orc_model *m, int op, zc *g, int n2) {
+    int N = m->ndim;
+    zc *t = zalloc((size_t)N * n2);
+    if (op == ORC_LEFT_FORWARD || op == ORC_LEFT_BACKWARD || op == ORC_LEFT_FORWARD_HC) {
+        const zc *K = (op == ORC_LEFT_BACKWARD) ? m->urtm1d : m->urtd;
+        for (int j = 0; j < n2; ++j)
+            for (int i = 0; i < N; ++i) {
+                zc acc = 0;
+                for (int k = 0; k < N; ++k) acc += K[ZIDX(i, k, N)] * g[ZIDX(k, j, N)];
+                t[ZIDX(i, j, N)] = acc;
+            }
+    } else {
+        const zc *K = (op == ORC_RIGHT_BACKWARD) ? m->urtm1d : m->urtd;
+        for (int j = 0; j < N; ++j)
+            for (int i = 0; i < n2; ++i) {
+                zc acc = 0;
+                for (int k = 0; k < N; ++k) acc += g[ZIDX(i, k, n2)] * K[ZIDX(k, j, N)];
+                t[ZIDX(i, j, n2)] = acc;
+            }
+    }
+    memcpy(g, t, sizeof(zc) * (size_t)N * n2);
+    free(t);
+}
+
+/* the whole kinetic half step as one operator: FFT, or the dense matrix */
 static void h0_fft(const orc_model *m, int op, zc *g, int n2) {
+    if (m->p.kinetic == ORC_DENSE) { h0_dense(m, op, g, n2); return; }
     int lq = m->lq;
     zc *v = zalloc(lq);
     if (op == ORC_LEFT_FORWARD || op == ORC_LEFT_BACKWARD || op == ORC_LEFT_FORWARD_HC) {

@@ -48,6 +48,7 @@ struct orc_model {
     /* kinetic */
     zc *urt, *urtm1;          /* [ist][2][2] with urt[ist*4 + (i-1)*2 + (j-1)] */
     zc *exph0k, *exph0kinv;   /* [lq] */
+    zc *urtd, *urtm1d;        /* [N*N] dense exp(-+dtau h0mat / 2) */
     zc *tw1, *tw2;            /* DFT twiddles exp(-2 pi i k / l) */
     zc *h0mat;                /* [N*N] */
     zc *expar_nn;             /* [nsites][nn_nf] */

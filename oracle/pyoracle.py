@@ -23,7 +23,7 @@ _LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
 
 SQUARE, HONEYCOMB = 1, 2
 FAST, DELAY, SUBMATRIX = 0, 1, 2
-CHECKERBOARD, FFT = 0, 1
+CHECKERBOARD, FFT, DENSE = 0, 1, 2
 HS_EXACT, HS_GENERAL4 = 0, 1
 LEFT_FORWARD, LEFT_BACKWARD, RIGHT_FORWARD, RIGHT_BACKWARD, LEFT_FORWARD_HC = range(5)
 

@@ -90,6 +90,7 @@ struct HostModel {
     std::vector<zc> expar;                // [site][nf]
     std::vector<zc> urt, urtm1;           // [bond][4]
     std::vector<zc> exph0k, exph0kinv;    // divided by lq
+    std::vector<zc> urtd, urtm1d;         // dense kinetic exp(-+dtau H0 / 2), N x N
     std::vector<int> bond_i1, bond_i2;
     std::vector<int> cell_plus;           // [d][j]
     ModelDev dev;                         // host copy with device pointers
@@ -245,9 +246,12 @@ static void exp2x2(double d, zc z, double s, zc* out) {
     out[0] = e * ch; out[1] = -e * sh * z; out[2] = -e * sh * std::conj(z); out[3] = e * ch;
 }
 
+static void eig_herm(int n, std::vector<zc>& a, std::vector<double>& w);
+
 static int build_model(HostModel& m) {
     dqmc_params& p = m.p;
     if (p.t3 != 0.0) return fail(DQMC_EINVAL, "t3 != 0 is not supported");
+    if (p.kinetic < DQMC_KIN_CHECKERBOARD || p.kinetic > DQMC_KIN_DENSE) return fail(DQMC_EINVAL, "kinetic must be 0, 1 or 2");
     if (p.kinetic == DQMC_KIN_FFT && (p.lattice != DQMC_LATT_SQUARE || p.l1 != p.l2))
         return fail(DQMC_EINVAL, "FFT kinetic term needs a square lattice with l1 == l2");
     if (p.lattice == DQMC_LATT_SQUARE && ((p.l1 * p.l2) % 2 != 0 || p.l1 % 2 || p.l2 % 2) && p.kinetic == DQMC_KIN_CHECKERBOARD)
@@ -276,6 +280,39 @@ static int build_model(HostModel& m) {
             exp2x2(d, z, 0.5 * p.dtau, &m.urt[ist * 4]);
             exp2x2(d, z, -0.5 * p.dtau, &m.urtm1[ist * 4]);
         }
+    if (p.kinetic == DQMC_KIN_DENSE) {
+        // urt = U exp(-dtau e / 2) U^H and urtm1 = U exp(+dtau e / 2) U^H from the
+        // eigen-decomposition of the seth0 matrix (dqmc_set_h0conf.f90:484-509,
+        // seth0.f90): nearest-neighbour bonds -rt expar, diagonal -mu
+        std::vector<zc> H((size_t)N * N, 0.0);
+        for (int b = 0; b < m.nn_lf; ++b) {
+            int i0 = m.nnlf[b];
+            for (int f = 1; f <= m.nn_nf; ++f) {
+                int in = m.nnlist[i0 * m.nn_nf + f - 1];
+                zc z1 = -p.rt * m.expar[i0 * m.nn_nf + f - 1];
+                H[i0 + (size_t)in * N] += z1;
+                H[in + (size_t)i0 * N] += std::conj(z1);
+            }
+        }
+        for (int i = 0; i < N; ++i) H[i + (size_t)i * N] -= p.mu;
+        std::vector<double> w;
+        eig_herm(N, H, w);
+        m.urtd.assign((size_t)N * N, 0.0);
+        m.urtm1d.assign((size_t)N * N, 0.0);
+        std::vector<double> em(N), ep(N);
+        for (int k = 0; k < N; ++k) { em[k] = std::exp(-0.5 * p.dtau * w[k]); ep[k] = std::exp(0.5 * p.dtau * w[k]); }
+        for (int j = 0; j < N; ++j)
+            for (int i = 0; i < N; ++i) {
+                zc z0 = 0, z1 = 0;
+                for (int k = 0; k < N; ++k) {
+                    zc t = H[i + (size_t)k * N] * std::conj(H[j + (size_t)k * N]);
+                    z0 += t * em[k];
+                    z1 += t * ep[k];
+                }
+                m.urtd[i + (size_t)j * N] = z0;
+                m.urtm1d[i + (size_t)j * N] = z1;
+            }
+    }
     if (p.kinetic == DQMC_KIN_FFT) {
         // eigenvalues h0k = diag(F H F^-1), F the unitary forward DFT over (l1, l2)
         // with column index j1 + l1 j2 (dqmc_set_h0conf.f90:225-291); H from seth0.f90
@@ -449,6 +486,10 @@ static int upload_model(HostModel& m) {
     std::vector<double2> t;
     t = to_d2(m.urt); if ((rc = upload(m, t, &d.urt))) return rc;
     t = to_d2(m.urtm1); if ((rc = upload(m, t, &d.urtm1))) return rc;
+    if (p.kinetic == DQMC_KIN_DENSE) {
+        t = to_d2(m.urtd); if ((rc = upload(m, t, &d.urtd))) return rc;
+        t = to_d2(m.urtm1d); if ((rc = upload(m, t, &d.urtm1d))) return rc;
+    }
     if (p.kinetic == DQMC_KIN_FFT) {
         t = to_d2(m.exph0k); if ((rc = upload(m, t, &d.exph0k))) return rc;
         t = to_d2(m.exph0kinv); if ((rc = upload(m, t, &d.exph0kinv))) return rc;
@@ -1058,6 +1099,7 @@ static void prog_add(PropProg& p, int kind, int which, int nf, int nt) {
 static void prog_k(const HostModel& m, PropProg& p, int which, int reversed) {
     if (m.p.rt == 0.0) return;
     if (m.p.kinetic == DQMC_KIN_FFT) { prog_add(p, PK_FFT, which, 0, 0); return; }
+    if (m.p.kinetic == DQMC_KIN_DENSE) { prog_add(p, PK_DENSE, which, 0, 0); return; }
     for (int k = 1; k <= m.nn_nf; ++k) prog_add(p, PK_CB, which == PW_CONJ ? PW_FWD : which, reversed ? m.nn_nf + 1 - k : k, 0);
 }
 static void prog_v(const HostModel& m, PropProg& p, int which, int nt) {
@@ -1069,10 +1111,23 @@ static void prog_v(const HostModel& m, PropProg& p, int which, int nt) {
 // per handle for a given lattice kind)
 static int launch_prog(dqmc_handle* h, int mat_id, const PropProg& prog, int right) {
     if (prog.n == 0) return DQMC_OK;
-    if (h->fft_L && prop_fft_eligible(prog))
+    if (h->fft_L && prop_fft_eligible(prog)) {
         launch_prop_fft(h->d_chains, h->nch, h->fft_L, h->maxN, mat_id, prog, right, right, 0, h->st);
-    else
-        launch_prop(h->d_chains, h->nch, h->maxN, mat_id, prog, right, h->ctas_per_chain, h->st);
+        return DQMC_OK;
+    }
+    // dense kinetic steps are GEMMs of their own; the element-wise ops between
+    // them run as one propagation kernel per stretch
+    PropProg seg; seg.n = 0;
+    for (int k = 0; k <= prog.n; ++k) {
+        const bool dense = k < prog.n && (prog.op[k] & 15) == PK_DENSE;
+        if (k == prog.n || dense) {
+            if (seg.n) launch_prop(h->d_chains, h->nch, h->maxN, mat_id, seg, right, h->ctas_per_chain, h->st);
+            seg.n = 0;
+            if (dense) launch_kin_dense(h->d_chains, h->nch, h->maxN, mat_id, (prog.op[k] >> 4) & 15, right, 0, h->st);
+        } else {
+            seg.op[seg.n++] = prog.op[k];
+        }
+    }
     return DQMC_OK;
 }
 
@@ -1183,10 +1238,21 @@ static void pflush(dqmc_handle* h, ProjPass& pp) {
         const PropProg& pr = side ? pp.l : pp.r;
         const int mat = side ? PMAT_ULT : PMAT_UR;
         if (!pr.n) continue;
-        if (h->fft_L && prop_fft_eligible(pr))
+        if (h->fft_L && prop_fft_eligible(pr)) {
             launch_prop_fft(h->d_chains, h->nch, h->fft_L, h->maxNe, mat, pr, 0, side, 1, h->st);
-        else
-            launch_prop_tall(h->d_chains, h->nch, h->maxN, mat, pr, side, h->ctas_per_chain, h->st);
+        } else {
+            PropProg seg; seg.n = 0;
+            for (int k = 0; k <= pr.n; ++k) {
+                const bool dense = k < pr.n && (pr.op[k] & 15) == PK_DENSE;
+                if (k == pr.n || dense) {
+                    if (seg.n) launch_prop_tall(h->d_chains, h->nch, h->maxN, mat, seg, side, h->ctas_per_chain, h->st);
+                    seg.n = 0;
+                    if (dense) launch_kin_dense(h->d_chains, h->nch, h->maxN, mat, (pr.op[k] >> 4) & 15, side, 1, h->st);
+                } else {
+                    seg.op[seg.n++] = pr.op[k];
+                }
+            }
+        }
         tmark(h, side ? DQMC_PROF_PROP_R : DQMC_PROF_PROP_L);
     }
     pp.r.n = 0; pp.l.n = 0;
@@ -1200,6 +1266,7 @@ static void pk(dqmc_handle* h, ProjPass& pp, PropProg& p, int which, int reverse
     const HostModel& m = *h->models[0];
     if (m.p.rt == 0.0) return;
     if (m.p.kinetic == DQMC_KIN_FFT) { padd(h, pp, p, PK_FFT, which, 0, 0); return; }
+    if (m.p.kinetic == DQMC_KIN_DENSE) { padd(h, pp, p, PK_DENSE, which, 0, 0); return; }
     for (int k = 1; k <= m.nn_nf; ++k) padd(h, pp, p, PK_CB, which, reversed ? m.nn_nf + 1 - k : k, 0);
 }
 
@@ -1852,6 +1919,7 @@ extern "C" int dqmc_gpu_h0_prop(dqmc_handle* h, int op, int nf) {
     PropProg p; p.n = 0;
     int which = (op == 1 || op == 3) ? PW_INV : (op == 4 ? PW_CONJ : PW_FWD);
     if (m.p.kinetic == DQMC_KIN_FFT) prog_add(p, PK_FFT, which, 0, 0);
+    else if (m.p.kinetic == DQMC_KIN_DENSE) prog_add(p, PK_DENSE, which, 0, 0);
     else prog_add(p, PK_CB, which == PW_CONJ ? PW_FWD : which, nf, 0);
     launch_prog(h, MAT_G, p, (op == 2 || op == 3) ? 1 : 0);
     CK(cudaStreamSynchronize(h->st));

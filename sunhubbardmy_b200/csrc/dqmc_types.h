@@ -28,6 +28,8 @@ struct ModelDev {
     const double2* exph0kinv;
     const double2* exph0kT;    // the same, index k2 + l1 k1 (l1 == l2): rows on adjacent lanes
     const double2* exph0kinvT;
+    const double2* urtd;       // dense kinetic: exp(-dtau H0 / 2), N x N (column-major)
+    const double2* urtm1d;     // exp(+dtau H0 / 2)
     const double2* tw1;        // [l1] exp(-2 pi i k / l1)
     const double2* tw2;        // [l2]
     // measurement tables (0-based)
@@ -111,7 +113,7 @@ enum {
 };
 
 // propagation op encoding: kind | which << 4 | nf << 8 | nt << 16
-enum { PK_CB = 1, PK_FFT = 2, PK_DIAG = 3, PK_VMIX = 4, PK_VSCALE = 5 };
+enum { PK_CB = 1, PK_FFT = 2, PK_DIAG = 3, PK_VMIX = 4, PK_VSCALE = 5, PK_DENSE = 6 };
 enum { PW_FWD = 0, PW_INV = 1, PW_CONJ = 2 };   // urt/bmat/exph0k, urtm1/bmat_inv/exph0kinv, conj(...)
 struct PropProg {
     int n;

@@ -544,6 +544,58 @@ void launch_stack_identity(const ChainDev* chains, int nchains, int slot, cudaSt
     k_stack_identity<<<grid, 256, 0, st>>>(chains, slot);
 }
 
+// Dense kinetic step, the zgemm branch of the h0conf props
+// (src/dqmc_config_h0/dqmc_left_forward_prop.f90:235-246 and its siblings):
+// W4 = K X (left), X K (right) or K^T X (right side on the transposed tall
+// UL^T, where (UL K)^T = K^T UL^T), K = urtm1 for the backward ops and urt
+// otherwise (urt is Hermitian, so the _hc op uses it too).  The CTAs of a
+// chain share its output tiles; k_kin_copy writes the result back.
+__global__ void __launch_bounds__(256) k_kin_dense(const ChainDev* __restrict__ chains, int mat_id, int which,
+                                                   int right, int tall) {
+    extern __shared__ double2 dsm[];
+    const ChainDev& c = chains[blockIdx.y];
+    const ModelDev& md = *c.md;
+    const int N = c.N, nv = tall ? md.ne : N;
+    const double2* K = (which == PW_INV) ? md.urtm1d : md.urtd;
+    const double2* X = chain_mat(c, mat_id);
+    ZGemmArgs g;
+    g.alpha = cmk(1, 0); g.beta = cmk(0, 0);
+    g.C = c.W[4]; g.ldc = N;
+    if (right && !tall) {
+        g.M = N; g.N = N; g.K = N;
+        g.A = X; g.lda = N; g.opA = OP_N;
+        g.B = K; g.ldb = N; g.opB = OP_N;
+    } else {
+        g.M = N; g.N = nv; g.K = N;
+        g.A = K; g.lda = N; g.opA = right ? OP_T : OP_N;
+        g.B = X; g.ldb = N; g.opB = OP_N;
+    }
+    zgemm_cta<GemmBig>(g, blockIdx.x, gridDim.x, dsm);
+}
+
+__global__ void k_kin_copy(const ChainDev* __restrict__ chains, int mat_id, int tall) {
+    const ChainDev& c = chains[blockIdx.y];
+    const int N = c.N, nv = tall ? c.md->ne : N;
+    double2* X = chain_mat(c, mat_id);
+    const size_t n = (size_t)N * nv;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+        X[e] = c.W[4][e];
+}
+
+static int g_kin_attr = 0;
+
+void launch_kin_dense(const ChainDev* chains, int nchains, int maxN, int mat_id, int which, int right, int tall,
+                      cudaStream_t st) {
+    if (!g_kin_attr) {
+        cudaFuncSetAttribute(k_kin_dense, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(GemmBig::SMEM_ELEMS * sizeof(double2)));
+        g_kin_attr = 1;
+    }
+    const int tiles = ((maxN + GemmBig::BM - 1) / GemmBig::BM) * ((maxN + GemmBig::BN - 1) / GemmBig::BN);
+    k_kin_dense<<<dim3(tiles, nchains), 256, GemmBig::SMEM_ELEMS * sizeof(double2), st>>>(chains, mat_id, which, right, tall);
+    k_kin_copy<<<dim3((maxN * maxN + 255) / 256, nchains), 256, 0, st>>>(chains, mat_id, tall);
+}
+
 void launch_zgemm_test(const ChainDev* chains, int nchains, int m, int n, int k, int opa, int opb,
                        int a_id, int b_id, int c_id, double beta_re, cudaStream_t st) {
     stab_attrs();

@@ -41,6 +41,10 @@ void launch_dyn_measure(const ChainDev* chains, int nchains, int maxN, int nt, c
 // wrap check: compare Gnew with G, recompute the phase, replace G (record = 0: just replace)
 void launch_wrap_check(const ChainDev* chains, int nchains, int record, cudaStream_t st);
 // generic batched complex GEMM on per-chain matrices (diagnostics)
+// dense kinetic step on matrix mat_id: X <- K X (left), X K (right) or K^T X
+// (right side of the transposed tall UL^T), K = urt (which != PW_INV) or urtm1
+void launch_kin_dense(const ChainDev* chains, int nchains, int maxN, int mat_id, int which, int right, int tall,
+                      cudaStream_t st);
 void launch_zgemm_test(const ChainDev* chains, int nchains, int m, int n, int k, int opa, int opb,
                        int a_id, int b_id, int c_id, double beta_re, cudaStream_t st);
 void launch_qr_test(const ChainDev* chains, int nchains, int a_id, int q_id, cudaStream_t st);

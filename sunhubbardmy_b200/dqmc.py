@@ -16,7 +16,7 @@ import numpy as np
 
 SQUARE, HONEYCOMB = 1, 2
 FAST, DELAY, SUBMATRIX = 0, 1, 2
-CHECKERBOARD, FFT = 0, 1
+CHECKERBOARD, FFT, DENSE = 0, 1, 2
 EXACT, GENERAL4 = 0, 1
 
 _HERE = os.path.dirname(os.path.abspath(__file__))

@@ -1,8 +1,8 @@
 """Shared parameter sets and helpers for the parity tests.
 
 The cases are small versions of the benchmark configurations (square Hubbard
-with checkerboard or FFT kinetic term, exact or general HS field; honeycomb
-SU(4)) sized so the oracle finishes each in well under a second.
+with checkerboard, FFT or dense kinetic term, exact or general HS field;
+honeycomb SU(4)) sized so the oracle finishes each in well under a second.
 """
 import numpy as np
 
@@ -24,6 +24,11 @@ CASES = {
     # at this size, so G itself is accurate to ~1e-12)
     "sq16_fft_gen4_delay": dict(lattice=1, l1=16, l2=16, beta=1.0, dtau=0.05, rhub=2.0, nflr=2, mu=0.3,
                                 kinetic=1, update=1, hs=1, nwrap=10, nublock=32),
+    # dense kinetic term (the zgemm branch of the h0conf props)
+    "sq4_dense_gen4_delay": dict(lattice=1, l1=4, l2=4, beta=2.0, dtau=0.1, rhub=4.0, nflr=2, mu=0.2,
+                                 kinetic=2, update=1, hs=1, nwrap=10, nublock=8),
+    "hc3_dense_su4_sub": dict(lattice=2, l1=3, l2=3, beta=1.6, dtau=0.1, rhub=6.0, nflr=4,
+                              kinetic=2, update=2, hs=0, nwrap=8, nublock=8),
 }
 
 TEST_SEED0 = 1909706392   # abs((0*1981+2008)*951049)

@@ -22,6 +22,8 @@ DCASES = {
                          nwrap=10, nublock=4, ltau=1, dyntau=1.0),
     "hc3_su4": dict(lattice=2, l1=3, l2=3, beta=1.0, dtau=0.1, rhub=6.0, nflr=4, kinetic=0, update=2, hs=0,
                     nwrap=5, nublock=8, ltau=1, dyntau=1.0),
+    "sq4_dense_gen4": dict(lattice=1, l1=4, l2=4, beta=1.0, dtau=0.1, rhub=4.0, nflr=2, kinetic=2, update=1, hs=1,
+                           nwrap=5, nublock=4, ltau=1, dyntau=1.0),
 }
 
 

@@ -27,6 +27,8 @@ PCASES = {
                     nwrap=4, proj=1, rndness=0.05, update=2, hs=0, nublock=4),
     "sq4_tv_fft": dict(lattice=1, l1=4, l2=4, beta=1.5, dtau=0.05, rv=1.0, rhub=0.0, nflr=1, kinetic=1,
                        nwrap=10, proj=1, rndness=0.02, update=2),
+    "hc3_tv_dense": dict(lattice=2, l1=3, l2=3, beta=2.0, dtau=0.1, rv=1.0, rhub=0.0, nflr=1, kinetic=2,
+                         nwrap=5, proj=1, rndness=1e-3, update=2),
 }
 
 

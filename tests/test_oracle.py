@@ -177,6 +177,29 @@ def test_free_fermion_green_checkerboard(oracle):
     assert np.max(np.abs(kin["urt"][0] - sl.expm(-0.5 * kw["dtau"] * h))) < 1e-14
 
 
+@pytest.mark.parametrize("lattice", [1, 2])
+def test_free_fermion_green_dense(oracle, lattice):
+    """Dense kinetic term: every h0 op is exp(-+dtau/2 H0) from the left or the
+    right, and the U = 0 Green's function is (1 + exp(-beta H0))^-1."""
+    kw = dict(lattice=lattice, l1=4 if lattice == 1 else 3, l2=4 if lattice == 1 else 3, beta=2.0, dtau=0.1,
+              rhub=0.0, kinetic=2, nwrap=5, mu=0.3, xmag=0.2)
+    m = oracle.Model(**kw)
+    H = m.h0mat()
+    N = m.ndim
+    km, kp = sl.expm(-0.5 * kw["dtau"] * H), sl.expm(0.5 * kw["dtau"] * H)
+    X = np.asfortranarray(np.random.default_rng(5).standard_normal((N, N)) + 0j)
+    for op, ref in ((oracle.LEFT_FORWARD, km @ X), (oracle.LEFT_BACKWARD, kp @ X), (oracle.RIGHT_FORWARD, X @ km),
+                    (oracle.RIGHT_BACKWARD, X @ kp), (oracle.LEFT_FORWARD_HC, km.conj().T @ X)):
+        g = X.copy(order="F")
+        m.h0_prop(op, 1, g)
+        assert np.max(np.abs(g - ref)) < 1e-12, op
+    c = oracle.Chain(m, 1)
+    c.sweep_start()
+    w, v = np.linalg.eigh(H)
+    g_ex = (v * (1.0 / (1.0 + np.exp(-kw["beta"] * w)))[None, :]) @ v.conj().T
+    assert np.max(np.abs(c.green() - g_ex)) < 1e-11
+
+
 def test_hubbard_atom_double_occupancy(oracle):
     """rt = 0: independent sites, H = U/2 (n - 1)^2 per site at half filling;
     D = e^{-beta U / 2} / (2 (1 + e^{-beta U/2})).  EXACTHS is exact here, so the
