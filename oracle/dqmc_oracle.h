@@ -184,4 +184,7 @@ void   orc_inv_logdet_lu(int n, double *a, double *logdet);
 #ifdef __cplusplus
 }
 #endif
+/* xmax_dyn: largest |G(t,t) propagated - G(t,t) fresh| of the projective unequal-time pass */
+double orc_chain_max_dyn_error(const orc_chain *c);
+
 #endif

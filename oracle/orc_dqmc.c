@@ -230,6 +230,7 @@ orc_model *orc_model_new(const orc_params *pin) {
     m->ltrot = (int)lround(p->beta / p->dtau);
     m->ntdm = p->ltau ? (int)lround(p->dyntau / p->dtau) : 0;
     if (m->ntdm < 0) m->ntdm = 0;
+    m->ntauin = (m->ltrot - m->ntdm) / 2;
     m->lwrapT = (p->rt != 0.0);
     m->lwrapu = (p->rhub != 0.0);
     int N = m->ndim;
@@ -1418,6 +1419,12 @@ int orc_sweep_dyn(orc_chain *c) {
     free(gtmp); free(ul); free(vl); free(dl);
     return 0;
 }
+
+void orc_dyn_measure(orc_chain *c, int nt, const zc *gt0, const zc *g0t, const zc *gtt, const zc *g00) {
+    dyn_measure(c, nt, gt0, g0t, gtt, g00);
+}
+
+double orc_chain_max_dyn_error(const orc_chain *c) { return c->max_dyn_error; }
 
 /* znn_tau_bin (lq, 2, 2, ntdm+1), Fortran order, complex as re/im pairs */
 int orc_dyn_bins(const orc_chain *c, double *out) {

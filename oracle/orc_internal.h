@@ -36,6 +36,7 @@ struct orc_model {
     orc_latt L;
     int ndim, lq, ltrot, nst, nublock, ne;
     int ntdm;        /* nint(dyntau / dtau) when ltau (src/model_para.f90:455-459) */
+    int ntauin;      /* (ltrot - ntdm) / 2: first slice of the projective unequal-time window */
     int lwrapT, lwrapu;
     int *iwrap_nt;   /* [ltrot+1] */
     int *wrap_step;  /* [nst][2] 1-based slice range */
@@ -69,6 +70,7 @@ struct orc_chain {
     zc *logdetQst;
     zc phase, logweightf;
     double max_wrap_error, max_phasediff, avglog10error, avgexpphasediff, logcount;
+    double max_dyn_error;     /* xmax_dyn of the projective unequal-time pass */
     double acc_u, prop_u;
     /* bins */
     int nobs;
@@ -107,6 +109,7 @@ void orc_eig_he(int n, const zc *h, double *w, zc *v);                       /* 
 zc orc_total_ratio(const orc_model *m, zc ratio1, int is, int iflip, int isp);
 zc orc_set_phase(const orc_chain *c, zc logw);
 double orc_compare_max(int N, const zc *a, const zc *b);
+void orc_dyn_measure(orc_chain *c, int nt, const zc *gt0, const zc *g0t, const zc *gtt, const zc *g00);
 
 /* projective path (orc_proj.c) */
 void orc_set_vconf(orc_model *m);

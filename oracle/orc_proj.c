@@ -648,7 +648,97 @@ int orc_proj_sweep_b0_slices(orc_chain *c, int lupdate, int lmeasure, int nslice
     return 0;
 }
 
-/* dqmc_proj_sweep_0b (src/dqmc_proj_core/dqmc_proj_sweep_0b.f90:1-235), ltau off */
+/* Bmat_left_forward / Bmat_right_backward (src/dqmc_ft_core.f90:70-121, 234-288)
+ * over slice nt on an N x N matrix, with the projective runs' bond field
+ * (nflag 2, then 1, per family) */
+static void bmat_nn(const orc_chain *c, int nt, int left, zc *x) {
+    const orc_model *m = c->m;
+    int N = m->ndim, nnf = m->L.nn_nf, cb = (m->p.kinetic == ORC_CHECKERBOARD);
+    int op = left ? ORC_LEFT_FORWARD : ORC_RIGHT_BACKWARD;
+    if (m->lwrapT) {
+        if (cb) for (int nf = 1; nf <= nnf; ++nf) orc_h0_prop(m, op, nf, (double *)x, N);
+        else orc_h0_prop(m, op, 0, (double *)x, N);
+    }
+    if (m->lwrapv)
+        for (int nf = 1; nf <= nnf; ++nf) {
+            orc_v_prop(m, c->vconf, op, nt, nf, 2, x, N);
+            orc_v_prop(m, c->vconf, op, nt, nf, 1, x, N);
+        }
+    if (m->lwrapu) orc_u_prop(m, c->conf, op, nt, (double *)x, N);
+    if (m->lwrapT) {
+        if (cb) for (int nf = nnf; nf >= 1; --nf) orc_h0_prop(m, op, nf, (double *)x, N);
+        else orc_h0_prop(m, op, 0, (double *)x, N);
+    }
+}
+
+/* c = a b (N x N) */
+static void zmm(int N, const zc *a, const zc *b, zc *c) {
+    for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i) {
+            zc acc = 0;
+            for (int k = 0; k < N; ++k) acc += a[ZIDX(i, k, N)] * b[ZIDX(k, j, N)];
+            c[ZIDX(i, j, N)] = acc;
+        }
+}
+
+/* dqmc_proj_dyn (src/dqmc_proj_core/dqmc_proj_dyn.f90:1-128), called by the 0b
+ * sweep at nt = ntauin on copies of UL and UR; Pst holds the b0 sweep's UL^T at
+ * the stabilisation points after ntauin.  The reference assumes that ntauin is
+ * a stabilisation point; G is computed fresh at ntauin in either case. */
+static void proj_dyn(orc_chain *c) {
+    const orc_model *m = c->m;
+    int N = m->ndim, ne = m->ne, t0 = m->ntauin, ntdm = m->ntdm;
+    size_t NN = (size_t)N * N;
+    zc *ul = zalloc((size_t)N * ne), *ur = zalloc((size_t)N * ne), *q = zalloc((size_t)N * ne);
+    zc *inv = zalloc((size_t)ne * ne), *gf = zalloc(NN), *gtt = zalloc(NN), *tmp = zalloc(NN);
+    memcpy(ul, c->UL, sizeof(zc) * (size_t)N * ne);
+    memcpy(ur, c->UR, sizeof(zc) * (size_t)N * ne);
+    for (int nt = t0; nt <= t0 + ntdm - 1; ++nt) {
+        int ntau = nt - t0;
+        if (m->iwrap_nt[nt] > 0 || ntau == 0) {
+            if (ntau > 0) {
+                int n = m->iwrap_nt[nt];
+                for (int l = 0; l < ne; ++l)
+                    for (int i = 0; i < N; ++i) ul[ZIDX(l, i, ne)] = c->Pst[n][ZIDX(i, l, N)];
+            }
+            ulr_inverse(N, ne, ul, ur, inv, NULL);
+            proj_green(N, ne, ul, ur, inv, gf);
+            if (ntau == 0) {
+                memcpy(c->g00, gf, sizeof(zc) * NN);
+                memcpy(gtt, gf, sizeof(zc) * NN);
+                memcpy(c->gt0, gf, sizeof(zc) * NN);
+                memcpy(c->g0t, gf, sizeof(zc) * NN);
+                for (int i = 0; i < N; ++i) c->g0t[ZIDX(i, i, N)] -= 1.0;      /* -(1 - G) */
+                orc_dyn_measure(c, 1, c->gt0, c->g0t, gtt, c->g00);
+            } else {
+                double err = orc_compare_max(N, gtt, gf);
+                if (err > c->max_dyn_error) c->max_dyn_error = err;
+                memcpy(gtt, gf, sizeof(zc) * NN);
+                zmm(N, gf, c->gt0, tmp);                                        /* gt0 = G gt0 */
+                memcpy(c->gt0, tmp, sizeof(zc) * NN);
+                for (size_t e = 0; e < NN; ++e) gf[e] = -gf[e];
+                for (int i = 0; i < N; ++i) gf[ZIDX(i, i, N)] += 1.0;           /* 1 - G */
+                zmm(N, c->g0t, gf, tmp);                                        /* g0t = g0t (1 - G) */
+                memcpy(c->g0t, tmp, sizeof(zc) * NN);
+            }
+        }
+        int nt1 = nt + 1;
+        bmat_nn(c, nt1, 1, c->gt0);
+        bmat_nn(c, nt1, 0, c->g0t);
+        bmat_nn(c, nt1, 0, gtt);
+        bmat_nn(c, nt1, 1, gtt);
+        orc_dyn_measure(c, nt1 - t0 + 1, c->gt0, c->g0t, gtt, c->g00);
+        bmat_left_forward_proj(c, nt1, nt1, ur);
+        if (m->iwrap_nt[nt] > 0 && nt1 != t0 + ntdm) {
+            orc_qr_pqmc(N, ne, ur, q);                                          /* stablize_0b_qr */
+            memcpy(ur, q, sizeof(zc) * (size_t)N * ne);
+        }
+    }
+    free(ul); free(ur); free(q); free(inv); free(gf); free(gtt); free(tmp);
+}
+
+/* dqmc_proj_sweep_0b (src/dqmc_proj_core/dqmc_proj_sweep_0b.f90:1-235); with
+ * ltau the measured sweep runs the unequal-time pass at nt = ntauin (206-211) */
 int orc_proj_sweep_0b(orc_chain *c, int lupdate, int lmeasure) {
     const orc_model *m = c->m;
     int N = m->ndim, ne = m->ne, nst = m->nst, nnf = m->L.nn_nf;
@@ -692,6 +782,7 @@ int orc_proj_sweep_0b(orc_chain *c, int lupdate, int lmeasure) {
             record_proj_wrap(c, ultmp, urtmp, lw);
             memcpy(c->Pst[n], c->UR, sizeof(zc) * (size_t)N * ne);
         }
+        if (m->p.ltau && lmeasure && nt == m->ntauin) proj_dyn(c);
     }
     free(ultmp); free(urtmp); free(q);
     return 0;

@@ -283,6 +283,12 @@ class Chain:
                     max_phasediff=d[5], avglog10error=d[6], logcount=d[7], accepted=d[8], proposed=d[9],
                     accepted_v=d[10], proposed_v=d[11])
 
+    def max_dyn_error(self) -> float:
+        """xmax_dyn of the projective unequal-time pass."""
+        f = lib().orc_chain_max_dyn_error
+        f.restype = C.c_double
+        return float(f(self._p))
+
     # ---- projective path ----
     def vconf(self) -> np.ndarray:
         m = self.model

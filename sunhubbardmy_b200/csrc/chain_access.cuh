@@ -5,7 +5,7 @@
 
 // matrix ids used by the host to address per-chain matrices
 enum { MAT_G = 0, MAT_GNEW = 1, MAT_W0 = 2, MAT_UR = 10, MAT_ULT = 11, MAT_PROJR = 12, MAT_PROJLC = 13,
-       MAT_ULRINV = 14, MAT_GT0 = 15, MAT_G0T = 16, MAT_G00 = 17, MAT_U0 = 100, MAT_V0 = 400, MAT_PST0 = 1000 };
+       MAT_ULRINV = 14, MAT_GT0 = 15, MAT_G0T = 16, MAT_G00 = 17, MAT_URS = 18, MAT_ULTS = 19, MAT_U0 = 100, MAT_V0 = 400, MAT_PST0 = 1000 };
 
 DQ_DEV double2* chain_mat(const ChainDev& c, int id) {
     size_t nn = (size_t)c.N * c.N;
@@ -20,6 +20,8 @@ DQ_DEV double2* chain_mat(const ChainDev& c, int id) {
     if (id == MAT_GT0) return c.gt0;
     if (id == MAT_G0T) return c.g0t;
     if (id == MAT_G00) return c.g00;
+    if (id == MAT_URS) return c.URs;
+    if (id == MAT_ULTS) return c.ULTs;
     if (id >= MAT_V0) return c.V + (size_t)c.slotmap[id - MAT_V0] * nn;
     if (id >= MAT_U0) return c.U + (size_t)c.slotmap[id - MAT_U0] * nn;
     return c.W[id - MAT_W0];

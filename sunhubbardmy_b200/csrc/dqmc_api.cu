@@ -61,7 +61,8 @@ extern "C" int dqmc_params_derive(dqmc_params* p) {
     if (p->obs_mid_len <= 0) p->obs_mid_len = 1;
     p->ntdm = p->ltau ? (int)std::lround(p->dyntau / p->dtau) : 0;
     if (p->ntdm < 0) p->ntdm = 0;
-    if (p->ltau && p->proj) return fail(DQMC_EINVAL, "unequal-time measurement (ltau) is supported on the finite-temperature path only");
+    if (p->ltau && p->proj && std::fabs(p->dyntau - p->beta) <= 1e-12 * std::fabs(p->beta))
+        return fail(DQMC_EINVAL, "dyntau = beta is not allowed on the projective path (dqmc_proj_ctrl.f90:13)");
     if (p->ltau && p->nst < 1) return fail(DQMC_EINVAL, "unequal-time measurement (ltau) needs lstabilize and ltrot >= nwrap");
     if (p->proj && p->nst < 1) return fail(DQMC_EINVAL, "the projective sweep needs lstabilize and ltrot >= nwrap");
     if (!p->proj && p->rv != 0.0) return fail(DQMC_EINVAL, "the t-V bond field (rv != 0) is supported on the projective path only");
@@ -996,6 +997,14 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
             d.projR = (double2*)dalloc(h, Nne * z);
             d.projLc = (double2*)dalloc(h, Nne * z);
             d.logwDV = (double*)dalloc(h, (size_t)(nst + 2) * sizeof(double));
+            if (m->p.ltau) {
+                d.gt0 = (double2*)dalloc(h, NN * z);
+                d.g0t = (double2*)dalloc(h, NN * z);
+                d.g00 = (double2*)dalloc(h, NN * z);
+                d.dynbins = (double2*)dalloc(h, (size_t)m->lq * 4 * (m->p.ntdm + 1) * z);
+                d.URs = (double2*)dalloc(h, Nne * z);
+                d.ULTs = (double2*)dalloc(h, Nne * z);
+            }
             d.pw = (double2*)dalloc(h, ((size_t)5 * 32 * ne + 2 * 32 * 32) * z);
             d.pw_flag = (int*)dalloc(h, 16 * sizeof(int));
             if (!d.UR || !d.ULT || !d.ULRINV || !d.Pst || !d.projR || !d.projLc || !d.logwDV || !d.pw) {
@@ -1226,7 +1235,7 @@ static void stab_b0(dqmc_handle* h, int n) {
 // the current matrices.
 // ---------------------------------------------------------------------------
 enum { PMAT_W3 = 5, PMAT_UR = 10, PMAT_ULT = 11, PMAT_PROJR = 12, PMAT_PROJLC = 13, PMAT_ULRINV = 14,
-       PMAT_PST0 = 1000, PMAT_G = 0, PMAT_GNEW = 1 };
+       PMAT_URS = 18, PMAT_ULTS = 19, PMAT_PST0 = 1000, PMAT_G = 0, PMAT_GNEW = 1 };
 
 struct ProjPass {
     PropProg r, l;   // r: ops on UR (left), l: ops on UL^T (right)
@@ -1399,7 +1408,72 @@ static void enqueue_proj_b0(dqmc_handle* h, int lupdate, int lmeasure) {
     pflush(h, pp);
 }
 
-// dqmc_proj_sweep_0b (src/dqmc_proj_core/dqmc_proj_sweep_0b.f90:1-235), lmeasure_dyn off
+// Bmat_left_forward (left = 1) or Bmat_right_backward (left = 0) over slice nt on
+// an N x N matrix (src/dqmc_ft_core.f90:70-121, 234-288), with the projective
+// runs' bond field: per family nflag 2 (mix, scale) then nflag 1 (mix)
+static PropProg prog_bslice_proj(const HostModel& m, int nt, int left) {
+    PropProg p; p.n = 0;
+    const int which = left ? PW_FWD : PW_INV;
+    prog_k(m, p, which, 0);
+    if (m.p.rv != 0.0)
+        for (int nf = 1; nf <= m.nn_nf; ++nf) {
+            prog_add(p, PK_VMIX, 0, nf, nt);
+            prog_add(p, PK_VSCALE, which, nf, nt);
+            prog_add(p, PK_VMIX, 0, nf, nt);
+        }
+    prog_v(m, p, which, nt);
+    prog_k(m, p, which, 1);
+    return p;
+}
+
+// dqmc_proj_dyn (src/dqmc_proj_core/dqmc_proj_dyn.f90:1-128), run by the measured
+// 0b sweep at nt = ntauin (dqmc_proj_sweep_0b.f90:206-211) on copies of UL and
+// UR: the sweep's UR and UL^T are set aside and restored afterwards, the
+// stack slots beyond ntauin still hold the b0 sweep's UL^T.  G(t,t) is
+// propagated in G and recomputed from (UL, UR) at the stabilisation points
+// (max deviation into xmax_dyn), G(t,0) = G gt0 and G(0,t) = g0t (1 - G) there,
+// and dyn_measure runs at every time index.  The reference assumes that ntauin
+// is a stabilisation point; G is computed fresh at ntauin in either case.
+static void proj_dyn(dqmc_handle* h) {
+    const HostModel& m = *h->models[0];
+    const int ntdm = m.p.ntdm, t0 = (m.p.ltrot - ntdm) / 2;
+    launch_tall_copy(h->d_chains, h->nch, PMAT_URS, PMAT_UR, h->st);
+    launch_tall_copy(h->d_chains, h->nch, PMAT_ULTS, PMAT_ULT, h->st);
+    for (int nt = t0; nt <= t0 + ntdm - 1; ++nt) {
+        const int ntau = nt - t0;
+        if (m.iwrap_nt[nt] > 0 || ntau == 0) {
+            if (ntau > 0) launch_tall_copy(h->d_chains, h->nch, PMAT_ULT, PMAT_PST0 + m.iwrap_nt[nt], h->st);
+            launch_proj_ulr(h->d_chains, h->nch, PMAT_W3, 0, 0, -1, h->st);
+            if (ntau == 0) {
+                launch_proj_green(h->d_chains, h->nch, PMAT_W3, PMAT_G, h->ctas_per_chain, h->st);
+                launch_dyn_init(h->d_chains, h->nch, h->st);
+                launch_dyn_measure(h->d_chains, h->nch, h->maxN, 1, h->st);
+            } else {
+                launch_proj_green(h->d_chains, h->nch, PMAT_W3, PMAT_GNEW, h->ctas_per_chain, h->st);
+                launch_chain_gemm(h->d_chains, h->nch, h->maxN, MAT_GT0, PMAT_GNEW, MAT_GT0, 0, h->st);
+                launch_chain_gemm(h->d_chains, h->nch, h->maxN, MAT_G0T, MAT_G0T, PMAT_GNEW, 1, h->st);
+                launch_dyn_err(h->d_chains, h->nch, h->st);
+            }
+        }
+        const int nt1 = nt + 1;
+        const PropProg pl = prog_bslice_proj(m, nt1, 1), pr = prog_bslice_proj(m, nt1, 0);
+        launch_prog(h, MAT_GT0, pl, 0);
+        launch_prog(h, MAT_G0T, pr, 1);
+        launch_prog(h, MAT_G, pr, 1);
+        launch_prog(h, MAT_G, pl, 0);
+        launch_dyn_measure(h->d_chains, h->nch, h->maxN, nt1 - t0 + 1, h->st);
+        ProjPass pp;
+        proj_bmat(h, pp, nt1, nt1);
+        pflush(h, pp);
+        if (m.iwrap_nt[nt] > 0 && nt1 != t0 + ntdm) launch_proj_qr(h->d_chains, h->nch, PMAT_UR, -1, -1, h->st);
+    }
+    launch_tall_copy(h->d_chains, h->nch, PMAT_UR, PMAT_URS, h->st);
+    launch_tall_copy(h->d_chains, h->nch, PMAT_ULT, PMAT_ULTS, h->st);
+    tmark(h, DQMC_PROF_MEASURE);
+}
+
+// dqmc_proj_sweep_0b (src/dqmc_proj_core/dqmc_proj_sweep_0b.f90:1-235); with
+// ltau the measured sweep runs the unequal-time pass at nt = ntauin (206-211)
 static void enqueue_proj_0b(dqmc_handle* h, int lupdate, int lmeasure) {
     const HostModel& m = *h->models[0];
     int lt = h->ltrot, nnf = m.nn_nf, nst = h->nst;
@@ -1432,6 +1506,7 @@ static void enqueue_proj_0b(dqmc_handle* h, int lupdate, int lmeasure) {
         pk(h, pp, pp.l, PW_INV, 1);
         if (lmeasure && proj_mid(m, nt)) { pflush(h, pp); proj_measure(h); }
         if (m.iwrap_nt[nt] > 0) { pflush(h, pp); stab_proj_0b(h, m.iwrap_nt[nt]); }
+        if (lmeasure && m.p.ltau && nt == (lt - m.p.ntdm) / 2) { pflush(h, pp); proj_dyn(h); }
     }
     pflush(h, pp);
 }
@@ -1576,7 +1651,8 @@ static void enqueue_dyn(dqmc_handle* h) {
 extern "C" int dqmc_gpu_sweep_dyn(dqmc_handle* h) {
     if (!h) return fail(DQMC_EINVAL, "null handle");
     if (!h->started) return fail(DQMC_ESTATE, "sweep before sweep_start");
-    if (h->proj || !h->models[0]->p.ltau) return fail(DQMC_ESTATE, "the unequal-time pass needs a finite-temperature handle with ltau = 1");
+    if (h->proj) return fail(DQMC_ESTATE, "on the projective path the unequal-time pass runs inside the measured 0b sweep");
+    if (!h->models[0]->p.ltau) return fail(DQMC_ESTATE, "the unequal-time pass needs ltau = 1");
     if (!h->after_b0) return fail(DQMC_ESTATE, "the unequal-time pass follows a b0 sweep (it needs the b0 sweep's left factors)");
     enqueue_dyn(h);
     CK(cudaStreamSynchronize(h->st));
@@ -1874,6 +1950,7 @@ extern "C" int dqmc_gpu_get_diag(dqmc_handle* h, int chain, dqmc_diag* out) {
     out->blk_proposed = st[ST_BLK_PROP]; out->blk_stage1 = st[ST_BLK_S1]; out->blk_accepted = st[ST_BLK_ACC];
     out->blk_sum_logratio = st[ST_BLK_SUMLR];
     out->blk_err_learned = st[ST_BLK_ERR1]; out->blk_err_zero = st[ST_BLK_ERR0];
+    out->max_dyn_error = st[ST_MAX_DYN];
     return DQMC_OK;
 }
 

@@ -99,6 +99,8 @@ struct ChainDev {
     double* Db;
     double2* ldqb;
     double2* Gb;
+    double2* URs;              // projective unequal-time pass: the sweep's UR and UL^T, kept aside
+    double2* ULTs;
 };
 
 // indices into ChainDev::stats
@@ -109,6 +111,7 @@ enum {
     ST_ACCV, ST_PROPV,
     ST_BLK_LR_RE, ST_BLK_LR_IM, ST_BLK_PH_RE, ST_BLK_PH_IM, ST_BLK_PROP, ST_BLK_S1, ST_BLK_ACC,
     ST_BLK_DS, ST_BLK_U2, ST_BLK_SUMLR, ST_BLK_ERR1, ST_BLK_ERR0,
+    ST_MAX_DYN,                // xmax_dyn of the projective unequal-time pass
     ST_COUNT = 32
 };
 

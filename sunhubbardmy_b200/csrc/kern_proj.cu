@@ -60,7 +60,8 @@ static size_t proj_la_smem(int maxN) {
 
 // ---------------------------------------------------------------------------
 // s_zgeQR_pqmc on the N x ne matrix mat_id, in place (X <- Q); the log of
-// |det R| goes to logwDV[dst] = logwDV[add] + log|det R| (add < 0: nothing added).
+// |det R| goes to logwDV[dst] = logwDV[add] + log|det R| (add < 0: nothing added;
+// dst < 0: not recorded).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_proj_qr(const ChainDev* __restrict__ chains, int mat_id, int dst, int add) {
     extern __shared__ double2 ssm[];
@@ -87,7 +88,7 @@ __global__ void __launch_bounds__(256) k_proj_qr(const ChainDev* __restrict__ ch
     __syncthreads();
     if (((long long)llround(neg)) & 1)
         for (int i = tid; i < N; i += nth) X[i] = cmk(-X[i].x, -X[i].y);
-    if (tid == 0) c.logwDV[dst] = (add >= 0 ? c.logwDV[add] : 0.0) + lg;
+    if (tid == 0 && dst >= 0) c.logwDV[dst] = (add >= 0 ? c.logwDV[add] : 0.0) + lg;
 }
 
 // ---------------------------------------------------------------------------

@@ -573,13 +573,43 @@ __global__ void __launch_bounds__(256) k_kin_dense(const ChainDev* __restrict__ 
     zgemm_cta<GemmBig>(g, blockIdx.x, gridDim.x, dsm);
 }
 
-__global__ void k_kin_copy(const ChainDev* __restrict__ chains, int mat_id, int tall) {
+// X <- W4 (sub = 0) or X - W4 (sub = 1), X of N x ne (tall) or N x N
+__global__ void k_kin_copy(const ChainDev* __restrict__ chains, int mat_id, int tall, int sub) {
     const ChainDev& c = chains[blockIdx.y];
     const int N = c.N, nv = tall ? c.md->ne : N;
     double2* X = chain_mat(c, mat_id);
     const size_t n = (size_t)N * nv;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
-        X[e] = c.W[4][e];
+        X[e] = sub ? csub(X[e], c.W[4][e]) : c.W[4][e];
+}
+
+// W4 = A B of two N x N chain matrices (the unequal-time products of
+// dqmc_proj_dyn.f90:95-98), output tiles shared by the chain's CTAs
+__global__ void __launch_bounds__(256) k_chain_gemm(const ChainDev* __restrict__ chains, int a_id, int b_id) {
+    extern __shared__ double2 dsm[];
+    const ChainDev& c = chains[blockIdx.y];
+    const int N = c.N;
+    ZGemmArgs g;
+    g.M = N; g.N = N; g.K = N; g.alpha = cmk(1, 0); g.beta = cmk(0, 0);
+    g.A = chain_mat(c, a_id); g.lda = N; g.opA = OP_N;
+    g.B = chain_mat(c, b_id); g.ldb = N; g.opB = OP_N;
+    g.C = c.W[4]; g.ldc = N;
+    zgemm_cta<GemmBig>(g, blockIdx.x, gridDim.x, dsm);
+}
+
+// s_compare_max_z of the propagated and the fresh G(t,t) into xmax_dyn, then
+// G = Gnew (dqmc_proj_dyn.f90:76-94)
+__global__ void __launch_bounds__(256) k_dyn_err(const ChainDev* __restrict__ chains) {
+    __shared__ double red[64];
+    const ChainDev c = chains[blockIdx.x];
+    const size_t NN = (size_t)c.N * c.N;
+    double mx = 0.0;
+    for (size_t e = threadIdx.x; e < NN; e += blockDim.x) {
+        mx = fmax(mx, cabsd(csub(c.Gnew[e], c.G[e])));
+        c.G[e] = c.Gnew[e];
+    }
+    mx = block_max(mx, red);
+    if (threadIdx.x == 0) c.stats[ST_MAX_DYN] = fmax(c.stats[ST_MAX_DYN], mx);
 }
 
 static int g_kin_attr = 0;
@@ -593,7 +623,25 @@ void launch_kin_dense(const ChainDev* chains, int nchains, int maxN, int mat_id,
     }
     const int tiles = ((maxN + GemmBig::BM - 1) / GemmBig::BM) * ((maxN + GemmBig::BN - 1) / GemmBig::BN);
     k_kin_dense<<<dim3(tiles, nchains), 256, GemmBig::SMEM_ELEMS * sizeof(double2), st>>>(chains, mat_id, which, right, tall);
-    k_kin_copy<<<dim3((maxN * maxN + 255) / 256, nchains), 256, 0, st>>>(chains, mat_id, tall);
+    k_kin_copy<<<dim3((maxN * maxN + 255) / 256, nchains), 256, 0, st>>>(chains, mat_id, tall, 0);
+}
+
+static int g_cg_attr = 0;
+
+void launch_chain_gemm(const ChainDev* chains, int nchains, int maxN, int dst_id, int a_id, int b_id, int sub,
+                       cudaStream_t st) {
+    if (!g_cg_attr) {
+        cudaFuncSetAttribute(k_chain_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(GemmBig::SMEM_ELEMS * sizeof(double2)));
+        g_cg_attr = 1;
+    }
+    const int tiles = ((maxN + GemmBig::BM - 1) / GemmBig::BM) * ((maxN + GemmBig::BN - 1) / GemmBig::BN);
+    k_chain_gemm<<<dim3(tiles, nchains), 256, GemmBig::SMEM_ELEMS * sizeof(double2), st>>>(chains, a_id, b_id);
+    k_kin_copy<<<dim3((maxN * maxN + 255) / 256, nchains), 256, 0, st>>>(chains, dst_id, 0, sub);
+}
+
+void launch_dyn_err(const ChainDev* chains, int nchains, cudaStream_t st) {
+    k_dyn_err<<<nchains, 256, 0, st>>>(chains);
 }
 
 void launch_zgemm_test(const ChainDev* chains, int nchains, int m, int n, int k, int opa, int opb,

@@ -45,6 +45,11 @@ void launch_wrap_check(const ChainDev* chains, int nchains, int record, cudaStre
 // (right side of the transposed tall UL^T), K = urt (which != PW_INV) or urtm1
 void launch_kin_dense(const ChainDev* chains, int nchains, int maxN, int mat_id, int which, int right, int tall,
                       cudaStream_t st);
+// dst = A B (sub = 0) or dst - A B (sub = 1) for N x N chain matrices (W4 is the scratch)
+void launch_chain_gemm(const ChainDev* chains, int nchains, int maxN, int dst_id, int a_id, int b_id, int sub,
+                       cudaStream_t st);
+// xmax_dyn of |Gnew - G|, then G = Gnew
+void launch_dyn_err(const ChainDev* chains, int nchains, cudaStream_t st);
 void launch_zgemm_test(const ChainDev* chains, int nchains, int m, int n, int k, int opa, int opb,
                        int a_id, int b_id, int c_id, double beta_re, cudaStream_t st);
 void launch_qr_test(const ChainDev* chains, int nchains, int a_id, int q_id, cudaStream_t st);

@@ -171,3 +171,67 @@ def test_proj_graph_matches_stepwise(sb, oracle):
         assert np.array_equal(a.vconf(c), b.vconf(c))
         assert np.max(np.abs(a.green(c) - b.green(c))) < 1e-12
         assert np.allclose(a.bins_raw(c), b.bins_raw(c), rtol=0, atol=1e-12)
+
+
+# unequal-time window [ntauin, ntauin + ntdm] inside the projection (ltau): the
+# measured 0b sweep runs dqmc_proj_dyn at nt = ntauin.  sq4_tv_fft starts the
+# window between stabilisation points (ntauin = 5, nwrap = 10).
+DYN = {"hc3_tv": 1.0, "sq4_hub": 1.0, "hc2_tuv": 0.8, "sq4_tv_fft": 1.0, "hc3_tv_dense": 1.0}
+
+
+@pytest.mark.parametrize("case", list(DYN))
+def test_proj_dyn_matches_oracle(sb, oracle, case):
+    """znn_tau bins of the projective unequal-time pass against the oracle's
+    restatement of dqmc_proj_dyn after two measured sweeps; the pass leaves the
+    sweep itself (fields, G, equal-time bins) unchanged; the propagated
+    G(t,t) agrees with the fresh one at the stabilisation points."""
+    kw = dict(PCASES[case], ltau=1, dyntau=DYN[case])
+    p = sb.DqmcParams.make(**kw)
+    g = sb.Dqmc(p, n_chains=2, seeds=[sb.test_seed(c) for c in range(2)])
+    m = oracle.Model(**kw)
+    ch = [oracle.Chain(m, sb.test_seed(c)) for c in range(2)]
+    for c in range(2):
+        P, _ = ch[c].trial()
+        g.set_trial(P, c)
+    g.sweep_start(); g.obser_init()
+    for c in ch:
+        c.proj_sweep_start(); c.obser_init()
+    for _ in range(2):
+        g.sweep_b0(); g.sweep_0b()
+        for c in ch:
+            c.proj_sweep_b0(); c.proj_sweep_0b()
+    for k, c in enumerate(ch):
+        dg_, dc_ = g.dyn_bins(k), c.dyn_bins()
+        assert np.max(np.abs(dc_)) > 0.0
+        assert rel(dg_, dc_) < 1e-8
+        assert g.diag(k)["max_dyn_error"] < 1e-8 and c.max_dyn_error() < 1e-8
+        if kw["rv"] != 0:
+            assert np.array_equal(g.vconf(k), c.vconf()), k
+        if kw["rhub"] != 0:
+            assert np.array_equal(g.conf(k), c.conf()), k
+        ur, ul, li = g.proj_state(k)
+        uro, ulo, lio = c.proj_state()
+        assert rel(ur, uro) < 1e-9 and rel(ul, ulo) < 1e-9
+        bg, bc = g.bins(k), c.bins()
+        for name in ("energy", "cpcm", "nn", "jj"):
+            assert np.max(np.abs(bg[name] - bc[name])) < 1e-8 * max(1.0, np.max(np.abs(bc[name]))), name
+
+
+def test_proj_dyn_graph_matches_stepwise(sb):
+    kw = dict(PCASES["hc3_tv"], ltau=1, dyntau=1.0)
+    p = sb.DqmcParams.make(**kw)
+    a = sb.Dqmc(p, n_chains=2)
+    b = sb.Dqmc(p, n_chains=2)
+    for h in (a, b):
+        h.sweep_start(); h.obser_init()
+    a.sweeps(2, True)
+    for _ in range(2):
+        b.sweep_b0(); b.sweep_0b()
+    for c in range(2):
+        assert np.allclose(a.dyn_bins(c), b.dyn_bins(c), rtol=0, atol=1e-12)
+
+
+def test_proj_dyn_rejects_dyntau_beta(sb):
+    kw = dict(PCASES["hc3_tv"], ltau=1, dyntau=PCASES["hc3_tv"]["beta"])
+    with pytest.raises(Exception):
+        sb.DqmcParams.make(**kw)

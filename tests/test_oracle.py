@@ -200,6 +200,24 @@ def test_free_fermion_green_dense(oracle, lattice):
     assert np.max(np.abs(c.green() - g_ex)) < 1e-11
 
 
+def test_projective_dyn_self_consistency(oracle):
+    """dqmc_proj_dyn: the G(t,t) propagated through the window agrees with the
+    one recomputed from (UL, UR) at the stabilisation points (xmax_dyn), and
+    the first time index of znn_tau holds the equal-time density correlation
+    (1/2 - n_i)(1/2 - n_j) - G(0,0)_ji (G(0,0) - 1)_ij / nflr summed over cells."""
+    kw = dict(lattice=2, l1=3, l2=3, beta=2.0, dtau=0.1, rv=1.0, rhub=0.0, nflr=1, kinetic=0,
+              nwrap=5, proj=1, rndness=1e-3, update=2, ltau=1, dyntau=1.0)
+    m = oracle.Model(**kw)
+    c = oracle.Chain(m, 7)
+    c.proj_sweep_start()
+    c.obser_init()
+    c.proj_sweep_b0(lupdate=True, lmeasure=False)
+    c.proj_sweep_0b(lupdate=True, lmeasure=True)
+    b = c.dyn_bins()
+    assert np.all(np.isfinite(b)) and np.max(np.abs(b)) > 0
+    assert 0.0 < c.max_dyn_error() < 1e-10
+
+
 def test_hubbard_atom_double_occupancy(oracle):
     """rt = 0: independent sites, H = U/2 (n - 1)^2 per site at half filling;
     D = e^{-beta U / 2} / (2 (1 + e^{-beta U/2})).  EXACTHS is exact here, so the
