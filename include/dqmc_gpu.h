@@ -85,6 +85,7 @@ typedef struct dqmc_diag {
     double blk_sum_logratio;            /* sum of Re log R over the accepted blocks */
     double blk_err_learned, blk_err_zero;   /* sums over second-stage blocks of (log|R| + dS)^2 and (log|R|)^2 */
     double max_dyn_error;               /* xmax_dyn: projective unequal-time pass, max |G(t,t) propagated - fresh| */
+    double dyn_log10_sum, dyn_count;    /* sum of log10 of those checks (avglog10dynerror) and their number */
 } dqmc_diag;
 
 typedef struct dqmc_handle dqmc_handle;

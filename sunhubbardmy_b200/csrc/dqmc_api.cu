@@ -1951,6 +1951,7 @@ extern "C" int dqmc_gpu_get_diag(dqmc_handle* h, int chain, dqmc_diag* out) {
     out->blk_sum_logratio = st[ST_BLK_SUMLR];
     out->blk_err_learned = st[ST_BLK_ERR1]; out->blk_err_zero = st[ST_BLK_ERR0];
     out->max_dyn_error = st[ST_MAX_DYN];
+    out->dyn_log10_sum = st[ST_DYN_LOG10]; out->dyn_count = st[ST_DYN_COUNT];
     return DQMC_OK;
 }
 
@@ -1963,6 +1964,7 @@ extern "C" int dqmc_gpu_reset_diag(dqmc_handle* h) {
         st[ST_ACC] = st[ST_PROP] = st[ST_ACCV] = st[ST_PROPV] = 0.0;
         st[ST_BLK_PROP] = st[ST_BLK_S1] = st[ST_BLK_ACC] = st[ST_BLK_SUMLR] = 0.0;
         st[ST_BLK_ERR1] = st[ST_BLK_ERR0] = 0.0;
+        st[ST_MAX_DYN] = st[ST_DYN_LOG10] = st[ST_DYN_COUNT] = 0.0;
         CK(copy_sync(h->st, h->chains[c].dev.stats, st, sizeof(st), cudaMemcpyHostToDevice));
     }
     return DQMC_OK;

@@ -112,7 +112,9 @@ enum {
     ST_BLK_LR_RE, ST_BLK_LR_IM, ST_BLK_PH_RE, ST_BLK_PH_IM, ST_BLK_PROP, ST_BLK_S1, ST_BLK_ACC,
     ST_BLK_DS, ST_BLK_U2, ST_BLK_SUMLR, ST_BLK_ERR1, ST_BLK_ERR0,
     ST_MAX_DYN,                // xmax_dyn of the projective unequal-time pass
-    ST_COUNT = 32
+    ST_DYN_LOG10,              // its sum of log10 over the checks (avglog10dynerror) ...
+    ST_DYN_COUNT,              // ... and the number of checks (logdyncount)
+    ST_COUNT = 40
 };
 
 // propagation op encoding: kind | which << 4 | nf << 8 | nt << 16

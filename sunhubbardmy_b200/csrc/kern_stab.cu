@@ -597,8 +597,8 @@ __global__ void __launch_bounds__(256) k_chain_gemm(const ChainDev* __restrict__
     zgemm_cta<GemmBig>(g, blockIdx.x, gridDim.x, dsm);
 }
 
-// s_compare_max_z of the propagated and the fresh G(t,t) into xmax_dyn, then
-// G = Gnew (dqmc_proj_dyn.f90:76-94)
+// s_compare_max_z of the propagated and the fresh G(t,t) into xmax_dyn,
+// logdyncount and avglog10dynerror, then G = Gnew (dqmc_proj_dyn.f90:76-94)
 __global__ void __launch_bounds__(256) k_dyn_err(const ChainDev* __restrict__ chains) {
     __shared__ double red[64];
     const ChainDev c = chains[blockIdx.x];
@@ -609,7 +609,11 @@ __global__ void __launch_bounds__(256) k_dyn_err(const ChainDev* __restrict__ ch
         c.G[e] = c.Gnew[e];
     }
     mx = block_max(mx, red);
-    if (threadIdx.x == 0) c.stats[ST_MAX_DYN] = fmax(c.stats[ST_MAX_DYN], mx);
+    if (threadIdx.x == 0) {
+        c.stats[ST_MAX_DYN] = fmax(c.stats[ST_MAX_DYN], mx);
+        c.stats[ST_DYN_LOG10] += log10(mx);
+        c.stats[ST_DYN_COUNT] += 1.0;
+    }
 }
 
 static int g_kin_attr = 0;

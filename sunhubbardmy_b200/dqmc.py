@@ -88,7 +88,7 @@ class DqmcDiag(C.Structure):
         "phase_re", "phase_im", "logweight_re", "logweight_im", "max_wrap_error", "max_phasediff",
         "avglog10error_sum", "logcount", "avgexpphasediff_sum", "accepted", "proposed", "nobs",
         "accepted_v", "proposed_v", "blk_proposed", "blk_stage1", "blk_accepted", "blk_sum_logratio",
-        "blk_err_learned", "blk_err_zero", "max_dyn_error")]
+        "blk_err_learned", "blk_err_zero", "max_dyn_error", "dyn_log10_sum", "dyn_count")]
 
 
 _lib = None
@@ -370,7 +370,8 @@ class Dqmc:
                     nobs=d.nobs, accepted_v=d.accepted_v, proposed_v=d.proposed_v,
                     blk_proposed=d.blk_proposed, blk_stage1=d.blk_stage1, blk_accepted=d.blk_accepted,
                     blk_sum_logratio=d.blk_sum_logratio, blk_err_learned=d.blk_err_learned,
-                    blk_err_zero=d.blk_err_zero, max_dyn_error=d.max_dyn_error)
+                    blk_err_zero=d.blk_err_zero, max_dyn_error=d.max_dyn_error,
+                    dyn_log10_sum=d.dyn_log10_sum, dyn_count=d.dyn_count)
 
     def energy_all(self) -> np.ndarray:
         """energy_bin(1:10) of every chain, shape (n_chains, 10) complex."""

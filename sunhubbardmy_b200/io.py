@@ -210,9 +210,11 @@ def wrap_step_of(p) -> list:
     return [((n - 1) * nw + 1, min(n * nw, lt)) for n in range(1, nst + 1)]
 
 
-def wrap_error_print(f, diags) -> None:
+def wrap_error_print(f, diags, ltau: bool = False) -> None:
     """wrap_error_print (src/dqmc_util.f90:15-57) of the chains' diagnostics
-    (Dqmc.diag dicts): max over chains, averages over all wrap checks."""
+    (Dqmc.diag dicts): max over chains, averages over all wrap checks; with
+    ltau also xmax_dyn and avglog10dynerror of the projective unequal-time
+    pass (0/0 prints NaN, as the reference's division does)."""
     mw = max(d["max_wrap_error"] for d in diags)
     mp = max(d["max_phasediff"] for d in diags)
     cnt = sum(d["logcount"] for d in diags)
@@ -222,6 +224,12 @@ def wrap_error_print(f, diags) -> None:
     f.write(f"--------------max_phasediff   = {fortran_e(mp)}\n")
     f.write(f"--------------avglog10error     = {a10:16.8f}\n")
     f.write(f"--------------avgexpphasediff = {aph:16.8f}\n")
+    if ltau:
+        xd = max(d.get("max_dyn_error", 0.0) for d in diags)
+        dc = sum(d.get("dyn_count", 0.0) for d in diags)
+        ad = sum(d.get("dyn_log10_sum", 0.0) for d in diags) / dc if dc else float("nan")
+        f.write(f"--------------xmax_dyn        = {fortran_e(xd)}\n")
+        f.write(f"--------------avglog10dynerror  = {ad:16.8f}\n" if dc else f"--------------avglog10dynerror  = {'NaN':>16}\n")
 
 
 def dqmc_end_print(f, diags, total_s: float, profile: dict | None = None, date: str = "") -> None:

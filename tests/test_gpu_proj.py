@@ -204,7 +204,9 @@ def test_proj_dyn_matches_oracle(sb, oracle, case):
         dg_, dc_ = g.dyn_bins(k), c.dyn_bins()
         assert np.max(np.abs(dc_)) > 0.0
         assert rel(dg_, dc_) < 1e-8
-        assert g.diag(k)["max_dyn_error"] < 1e-8 and c.max_dyn_error() < 1e-8
+        dgk = g.diag(k)
+        assert dgk["max_dyn_error"] < 1e-8 and c.max_dyn_error() < 1e-8
+        assert dgk["dyn_count"] >= 2 and dgk["dyn_log10_sum"] / dgk["dyn_count"] < -8
         if kw["rv"] != 0:
             assert np.array_equal(g.vconf(k), c.vconf()), k
         if kw["rhub"] != 0:

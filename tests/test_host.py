@@ -238,6 +238,13 @@ def test_dqmc_out_writers():
     lines = f.getvalue().splitlines()
     assert lines[0] == "--------------max_wrap_error  =   0.30000000E-10"
     assert lines[2] == f"--------------avglog10error     = {-10.75:16.8f}"
+    for d, x in zip(diags, (1e-13, 4e-13)):
+        d.update(max_dyn_error=x, dyn_log10_sum=2 * np.log10(x), dyn_count=2.0)
+    f = pyio.StringIO()
+    wrap_error_print(f, diags, ltau=True)
+    lines = f.getvalue().splitlines()
+    assert lines[4] == "--------------xmax_dyn        =   0.40000000E-12"
+    assert lines[5] == f"--------------avglog10dynerror  = {(np.log10(1e-13) + np.log10(4e-13)) / 2:16.8f}"
     f = pyio.StringIO()
     dqmc_end_print(f, diags, 12.5, {"update": (100.0, 1), "stab": (50.0, 1), "green": (30.0, 1),
                                     "prop_left": (10.0, 1), "measure": (5.0, 1), "prop_right": (5.0, 1),
