@@ -1,4 +1,4 @@
-// SFMT-19937 on the device, one thread per chain.
+// SFMT-19937 on the device, one warp per chain.
 //
 // Reference: lib/m_spring.f90:187-379 (spring_sfmt_init/_source/_kernel/_core);
 // spring_sfmt_stream maps the 32-bit output u to (u + 0.5) / 2^32.  The
@@ -47,26 +47,44 @@ __device__ void sfmt_gen_all(uint32_t* st) {
 }
 
 // count = slices * rps draws per chain (slices > 0; rps = words per time slice
-// of the chain's model), or exactly -slices draws
-__global__ void k_sfmt_fill(const ChainDev* __restrict__ chains, int ch0, int nchains, int slices) {
-    int ch = ch0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (ch >= ch0 + nchains) return;
+// of the chain's model), or exactly -slices draws.  One warp per chain: the
+// state is held in shared memory while lane 0 runs the recursion (the serial
+// part), and the warp copies each block of 624 outputs to the chain's draw
+// buffer with coalesced stores.
+#define SFMT_WARPS 4
+__global__ void __launch_bounds__(32 * SFMT_WARPS) k_sfmt_fill(const ChainDev* __restrict__ chains, int ch0,
+                                                               int nchains, int slices) {
+    __shared__ uint32_t sst[SFMT_WARPS][SFMT_N32];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ch = ch0 + blockIdx.x * SFMT_WARPS + w;
+    if (ch >= ch0 + nchains) return;      // whole warps; no block barrier below
     const int count = slices > 0 ? slices * chains[ch].md->rps : -slices;
-    uint32_t* st = chains[ch].sfmt;
+    uint32_t* gst = chains[ch].sfmt;
     uint32_t* out = chains[ch].rnd;
-    int idx = (int)st[SFMT_N32];
-    for (int k = 0; k < count; ++k) {
-        if (idx >= SFMT_N32) { sfmt_gen_all(st); idx = 0; }
-        out[k] = st[idx++];
+    uint32_t* s = sst[w];
+    for (int e = lane; e < SFMT_N32; e += 32) s[e] = gst[e];
+    int idx = (int)gst[SFMT_N32];
+    __syncwarp();
+    for (int k = 0; k < count;) {
+        if (idx >= SFMT_N32) {
+            if (lane == 0) sfmt_gen_all(s);
+            __syncwarp();
+            idx = 0;
+        }
+        const int n = min(SFMT_N32 - idx, count - k);
+        for (int e = lane; e < n; e += 32) out[k + e] = s[idx + e];
+        k += n;
+        idx += n;
+        __syncwarp();                     // the block is read before it is regenerated
     }
-    st[SFMT_N32] = (uint32_t)idx;
+    for (int e = lane; e < SFMT_N32; e += 32) gst[e] = s[e];
+    if (lane == 0) gst[SFMT_N32] = (uint32_t)idx;
 }
 
 void launch_sfmt(const ChainDev* chains, int nchains, int slices, cudaStream_t st) {
-    int tpb = 32;
-    k_sfmt_fill<<<(nchains + tpb - 1) / tpb, tpb, 0, st>>>(chains, 0, nchains, slices);
+    k_sfmt_fill<<<(nchains + SFMT_WARPS - 1) / SFMT_WARPS, 32 * SFMT_WARPS, 0, st>>>(chains, 0, nchains, slices);
 }
 
 void launch_sfmt_raw(const ChainDev* chains, int chain, int count, cudaStream_t st) {
-    k_sfmt_fill<<<1, 32, 0, st>>>(chains, chain, 1, -count);
+    k_sfmt_fill<<<1, 32 * SFMT_WARPS, 0, st>>>(chains, chain, 1, -count);
 }
