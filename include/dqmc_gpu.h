@@ -40,6 +40,7 @@ extern "C" {
 /* enums (compile-time RUNMODE flags of src/make.sys.* turned into values) */
 #define DQMC_LATT_SQUARE 1     /* -DSQUARE */
 #define DQMC_LATT_HONEYCOMB 2  /* -DHONEYCOMB */
+#define DQMC_LATT_CHAIN 3      /* -DCHAIN: l2 = 1, even l1; checkerboard or dense kinetic term */
 #define DQMC_UPD_FAST 0        /* default (no flag) */
 #define DQMC_UPD_DELAY 1       /* -DDELAY */
 #define DQMC_UPD_SUBMATRIX 2   /* -DSUBMATRIX */

@@ -40,7 +40,7 @@ double   orc_sfmt_stream(orc_sfmt *s);
 int32_t  orc_test_seed(int32_t irank);   /* src/dqmc_util.f90:72 under -DTEST */
 
 /* ---------- parameters (src/model_para.f90 &model_para/&ctrl_para) ---------- */
-enum { ORC_SQUARE = 1, ORC_HONEYCOMB = 2 };
+enum { ORC_SQUARE = 1, ORC_HONEYCOMB = 2, ORC_CHAIN = 3 };
 enum { ORC_FAST = 0, ORC_DELAY = 1, ORC_SUBMATRIX = 2 };
 enum { ORC_CHECKERBOARD = 0, ORC_FFT = 1, ORC_DENSE = 2 };
 enum { ORC_HS_EXACT = 0, ORC_HS_GENERAL4 = 1 };

@@ -1037,29 +1037,32 @@ void orc_measure(orc_chain *c, int nt) {
     zc zne = 0;
     for (int i = 0; i < N; ++i) zne += GC(i, i);
     c->energy_bin[1] += zne * zphi / (double)lq;
-    /* zkint */
+    /* zkint; the chain's (equaltime_measure1d.f90) carries the factor nflr rt on
+     * the bonds and 2 t2 on the two second neighbours */
+    const int chain = (L->kind == ORC_CHAIN);
     zc zk = 0;
     for (int b = 0; b < L->nn_lf; ++b) {
         int i0 = L->nnlf_list[b] - 1;
         for (int nf = 1; nf <= nnf; ++nf) {
             int in = L->nnlist[i0 * nnf + nf - 1] - 1;
-            zk += -2.0 * creal(GC(i0, in) * m->expar_nn[i0 * nnf + nf - 1]);
+            zk += (chain ? -2.0 * nflr * p->rt : -2.0) * creal(GC(i0, in) * m->expar_nn[i0 * nnf + nf - 1]);
         }
     }
     if (p->t2 != 0.0) {
-        int ns = (L->kind == ORC_SQUARE) ? 4 : 6;
+        int ns = chain ? 2 : (L->kind == ORC_SQUARE) ? 4 : 6;
         for (int i0 = 0; i0 < L->nsites; ++i0)
-            for (int nf = 0; nf < ns; ++nf) zk += -p->t2 * creal(GC(i0, L->snlist[i0 * L->nsn + nf] - 1));
+            for (int nf = 0; nf < ns; ++nf)
+                zk += (chain ? -2.0 * p->t2 : -p->t2) * creal(GC(i0, L->snlist[i0 * L->nsn + nf] - 1));
     }
     c->energy_bin[2] += zk * zphi;
     /* zint_u */
     zc zu = 0;
     for (int i = 0; i < L->nsites; ++i) zu += GC(i, i) * GC(i, i);
     c->energy_bin[3] += zu * zphi;
-    /* zqsq, ztsq, ztq */
+    /* zqsq, ztsq, ztq (2D only) */
     zc zq = 0, zt = 0, ztq = 0;
     zc e_m = cexp(-I * p->theta), e_p = cexp(I * p->theta);
-    for (int q = 0; q < lq; ++q) {
+    for (int q = 0; q < (chain ? 0 : lq); ++q) {
         const int *pc = &L->plq_cord[q * zp];
         zc tmp = 0;
         for (int a = 0; a < zp; ++a) tmp += GC(pc[a] - 1, pc[a] - 1);
@@ -1102,16 +1105,20 @@ void orc_measure(orc_chain *c, int nt) {
             }
         }
     }
-    c->energy_bin[4] += zq * (1.0 / 9.0) * zphi;
-    c->energy_bin[5] += zt * zphi;
-    c->energy_bin[6] += ztq * zphi;
     /* zint_v */
     zc zv = 0;
     for (int b = 0; b < L->nn_lf; ++b) {
         int i0 = L->nnlf_list[b] - 1;
         for (int nf = 1; nf <= nnf; ++nf) zv += creal(GC(i0, L->nnlist[i0 * nnf + nf - 1] - 1));
     }
-    c->energy_bin[7] += zv * p->rv * zphi;
+    if (chain) {
+        c->energy_bin[4] += zv * zphi;                /* energy_bin(5), without rv */
+    } else {
+        c->energy_bin[4] += zq * (1.0 / 9.0) * zphi;
+        c->energy_bin[5] += zt * zphi;
+        c->energy_bin[6] += ztq * zphi;
+        c->energy_bin[7] += zv * p->rv * zphi;
+    }
     /* cpcm, spsm, nn, pair_onsite: [imj][no_i][no_j], index (imj-1) + lq*((no_i-1) + 2*(no_j-1)) */
     double fsp = 1.0 - 1.0 / (double)(nflr * nflr), fn = 1.0 / (double)nflr;
     zc zn[2] = {0, 0};

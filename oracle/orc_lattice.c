@@ -1,7 +1,8 @@
-/* Square and honeycomb lattice tables, restated from src/lattice.f90
+/* Square, honeycomb and chain lattice tables, restated from src/lattice.f90
  * (setup_latt2d_sub 386-491, setup_honeycomb_sub 611-776,
- * setup_square_sub 792-961) and the hopping phase expar
- * (src/dqmc_config_h0/expar.f90).  Test infrastructure only.
+ * setup_square_sub 792-961, setup_latt1d_sub 67-135, setup_chain_sub 240-316)
+ * and the hopping phase expar (src/dqmc_config_h0/expar.f90, expar1d.f90).
+ * Test infrastructure only.
  * Stored values are 1-based as in the reference. */
 #include <math.h>
 #include <stdlib.h>
@@ -221,10 +222,51 @@ static void setup_honeycomb(orc_latt *L, int l1, int l2) {
         }
 }
 
+/* setup_chain_sub: l1 sites, one orbital, bond families +a1 and -a1 from the
+ * A sites (even, 1-based), second neighbours at +-2 a1.  The distance table
+ * imj(i, j) = npbc(i - j, l1) and zexpiqr are the 2D ones with l2 = 1. */
+static void setup_chain(orc_latt *L, int l1) {
+    const double a1[2] = {1.0, 0.0}, a2[2] = {0.0, 1.0};
+    setup_2d(L, l1, 1, a1, a2);
+    L->kind = ORC_CHAIN; L->nsub = 1; L->nsites = l1; L->z_plq = 1;
+    L->nn_nf = 2; L->nn_lf = l1 / 2; L->nsn = 2;
+    int ns = L->nsites;
+    L->cord = malloc(sizeof(int) * 2 * ns);
+    L->rcord = malloc(sizeof(double) * 2 * ns);
+    L->nnlf_list = malloc(sizeof(int) * (L->nn_lf > 0 ? L->nn_lf : 1));
+    L->list = malloc(sizeof(int) * 2 * ns);
+    int ind = 0;
+    for (int i1 = 1; i1 <= l1; ++i1) {
+        L->list[(i1 - 1) * 2] = i1; L->list[(i1 - 1) * 2 + 1] = 1;
+        L->rcord[(i1 - 1) * 2] = i1; L->rcord[(i1 - 1) * 2 + 1] = 1;
+        if (i1 % 2 == 0 && ind < L->nn_lf) L->nnlf_list[ind++] = i1;
+    }
+    memcpy(L->cord, L->ulist, sizeof(int) * 2 * ns);
+    L->nnvecr = malloc(sizeof(double) * ns * 2 * 2);
+    L->nnveci = malloc(sizeof(int) * ns * 2 * 2);
+    for (int i = 0; i < ns; ++i)
+        for (int nf = 0; nf < 2; ++nf) {
+            L->nnvecr[(i * 2 + nf) * 2] = nf == 0 ? 1.0 : -1.0; L->nnvecr[(i * 2 + nf) * 2 + 1] = 0.0;
+            L->nnveci[(i * 2 + nf) * 2] = nf == 0 ? 1 : -1; L->nnveci[(i * 2 + nf) * 2 + 1] = 0;
+        }
+    L->nnlist = malloc(sizeof(int) * ns * 2);
+    L->snlist = malloc(sizeof(int) * ns * 2);
+    for (int i = 0; i < ns; ++i) {
+        int u1 = L->ulist[i * 2];
+        L->nnlist[i * 2 + 0] = npbc(u1 + 1, l1);
+        L->nnlist[i * 2 + 1] = npbc(u1 - 1, l1);
+        L->snlist[i * 2 + 0] = npbc(u1 + 2, l1);
+        L->snlist[i * 2 + 1] = npbc(u1 - 2, l1);
+    }
+    L->plq_cord = malloc(sizeof(int) * ns);
+    for (int i = 0; i < ns; ++i) L->plq_cord[i] = i + 1;
+}
+
 int orc_latt_build(orc_latt *L, int kind, int l1, int l2) {
     memset(L, 0, sizeof(*L));
     if (kind == ORC_SQUARE) setup_square(L, l1, l2);
     else if (kind == ORC_HONEYCOMB) setup_honeycomb(L, l1, l2);
+    else if (kind == ORC_CHAIN) setup_chain(L, l1);
     else return -1;
     return 0;
 }
@@ -237,7 +279,8 @@ zc orc_expar(const orc_latt *L, int i, int nf, double xmag, double fx, double fy
     double vr1 = L->nnvecr[k], vr2 = L->nnvecr[k + 1];
     double rc1 = L->rcord[i * 2], rc2 = L->rcord[i * 2 + 1];
     int c1 = L->cord[i * 2], c2 = L->cord[i * 2 + 1];
-    double xmag1 = xmag / L->ncell * (L->a1[0] * L->a2[1] - L->a1[1] * L->a2[0]);
+    /* the chain has no Peierls phase (expar1d.f90: x = x1 = 0) */
+    double xmag1 = (L->kind == ORC_CHAIN) ? 0.0 : xmag / L->ncell * (L->a1[0] * L->a2[1] - L->a1[1] * L->a2[0]);
     double x = -xmag1 * vr1 * (2.0 * rc2 + vr2) * M_PI;
     double x1 = 0.0;
     int edge2 = ((c2 == L->l2 && nay > 0) || (c2 == 1 && nay < 0));

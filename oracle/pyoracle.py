@@ -21,7 +21,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
 
-SQUARE, HONEYCOMB = 1, 2
+SQUARE, HONEYCOMB, CHAIN = 1, 2, 3
 FAST, DELAY, SUBMATRIX = 0, 1, 2
 CHECKERBOARD, FFT, DENSE = 0, 1, 2
 HS_EXACT, HS_GENERAL4 = 0, 1
@@ -192,7 +192,7 @@ class Model:
 
     def tables(self):
         N, lq = self.ndim, self.lq
-        nsn = 4 if self.params.lattice == SQUARE else 6
+        nsn = {SQUARE: 4, HONEYCOMB: 6, CHAIN: 2}[self.params.lattice]
         nnlist = np.zeros((N, self.nn_nf), np.int32)
         nnlf = np.zeros(self.nn_lf, np.int32)
         lst = np.zeros((N, 2), np.int32)

@@ -35,12 +35,16 @@ extern "C" const char* dqmc_gpu_last_error(void) { return g_err.c_str(); }
 // ---------------------------------------------------------------------------
 extern "C" int dqmc_params_derive(dqmc_params* p) {
     if (!p) return fail(DQMC_EINVAL, "null params");
-    if (p->lattice != DQMC_LATT_SQUARE && p->lattice != DQMC_LATT_HONEYCOMB)
-        return fail(DQMC_EINVAL, "lattice must be square or honeycomb");
-    if (p->l1 < 2 || p->l2 < 2) return fail(DQMC_EINVAL, "l1, l2 must be >= 2");
+    if (p->lattice != DQMC_LATT_SQUARE && p->lattice != DQMC_LATT_HONEYCOMB && p->lattice != DQMC_LATT_CHAIN)
+        return fail(DQMC_EINVAL, "lattice must be square, honeycomb or chain");
+    if (p->lattice == DQMC_LATT_CHAIN) {
+        if (p->l2 != 1 || p->l1 < 4 || p->l1 % 2) return fail(DQMC_EINVAL, "the chain needs l2 = 1 and an even l1 >= 4");
+    } else if (p->l1 < 2 || p->l2 < 2) {
+        return fail(DQMC_EINVAL, "l1, l2 must be >= 2");
+    }
     if (p->dtau <= 0 || p->beta <= 0) return fail(DQMC_EINVAL, "beta, dtau must be > 0");
     p->lq = p->l1 * p->l2;
-    p->ndim = (p->lattice == DQMC_LATT_SQUARE) ? p->lq : 2 * p->lq;
+    p->ndim = (p->lattice == DQMC_LATT_HONEYCOMB) ? 2 * p->lq : p->lq;
     p->ne = p->ndim / 2 + (int)(p->nu * p->ndim / 8.0);
     p->ltrot = (int)std::lround(p->beta / p->dtau);
     if (p->nublock == 0) {
@@ -106,6 +110,39 @@ static void build_lattice(HostModel& m) {
     const dqmc_params& p = m.p;
     int l1 = p.l1, l2 = p.l2;
     m.lq = l1 * l2;
+    if (p.lattice == DQMC_LATT_CHAIN) {
+        // setup_latt1d_sub / setup_chain_sub (src/lattice.f90:67-135, 240-316): bond
+        // families +a1 and -a1 from the A sites (even, 1-based), second neighbours
+        // at +-2 a1; imj(i, j) = npbc(i - j, l1) is the 2D table with l2 = 1
+        m.a1[0] = 1; m.a1[1] = 0; m.a2[0] = 0; m.a2[1] = 1;
+        m.nsub = 1; m.N = l1; m.nn_nf = 2; m.nn_lf = l1 / 2; m.z_plq = 1; m.nsn = 2;
+        const int N = m.N;
+        m.cell1.resize(N); m.cell2.assign(N, 1); m.rc1.resize(N); m.rc2.assign(N, 1.0);
+        m.nnlist.assign(N * 2, 0); m.snlist.assign(N * 2, 0);
+        m.nnveci.assign(N * 2 * 2, 0); m.nnvecr.assign(N * 2 * 2, 0.0);
+        for (int i = 0; i < N; ++i) {
+            const int i1 = i + 1;
+            m.cell1[i] = i1; m.rc1[i] = i1;
+            m.nnlist[i * 2 + 0] = npbc(i1 + 1, l1) - 1;
+            m.nnlist[i * 2 + 1] = npbc(i1 - 1, l1) - 1;
+            m.snlist[i * 2 + 0] = npbc(i1 + 2, l1) - 1;
+            m.snlist[i * 2 + 1] = npbc(i1 - 2, l1) - 1;
+            m.nnveci[(i * 2 + 0) * 2] = 1; m.nnvecr[(i * 2 + 0) * 2] = 1.0;
+            m.nnveci[(i * 2 + 1) * 2] = -1; m.nnvecr[(i * 2 + 1) * 2] = -1.0;
+            if (i1 % 2 == 0) m.nnlf.push_back(i);
+        }
+        m.imj.assign(m.lq * m.lq, 0);
+        m.cell_plus.assign(m.lq * m.lq, 0);
+        for (int j = 0; j < m.lq; ++j)
+            for (int i = 0; i < m.lq; ++i) {
+                const int d = npbc(i - j, l1) - 1;
+                m.imj[i * m.lq + j] = d;
+                m.cell_plus[d * m.lq + j] = i;
+            }
+        m.plq.resize(m.lq);
+        for (int c = 0; c < m.lq; ++c) m.plq[c] = c;
+        return;
+    }
     bool sq = (p.lattice == DQMC_LATT_SQUARE);
     if (sq) { m.a1[0] = 1; m.a1[1] = 0; m.a2[0] = 0; m.a2[1] = 1; }
     else { m.a1[0] = 0.5; m.a1[1] = -0.5 * std::sqrt(3.0); m.a2[0] = 0.5; m.a2[1] = 0.5 * std::sqrt(3.0); }
@@ -222,7 +259,8 @@ static zc expar(const HostModel& m, int i, int nf) {
     double vr1 = m.nnvecr[k], vr2 = m.nnvecr[k + 1];
     double rc1 = m.rc1[i], rc2 = m.rc2[i];
     int c1 = m.cell1[i], c2 = m.cell2[i];
-    double xmag1 = p.xmag / m.lq * (m.a1[0] * m.a2[1] - m.a1[1] * m.a2[0]);
+    // the chain has no Peierls phase (expar1d.f90: x = x1 = 0)
+    double xmag1 = (p.lattice == DQMC_LATT_CHAIN) ? 0.0 : p.xmag / m.lq * (m.a1[0] * m.a2[1] - m.a1[1] * m.a2[0]);
     double x = -xmag1 * vr1 * (2.0 * rc2 + vr2) * M_PI, x1 = 0.0;
     bool e2 = (c2 == p.l2 && nay > 0) || (c2 == 1 && nay < 0);
     bool e1 = (c1 == p.l1 && nax > 0) || (c1 == 1 && nax < 0);
@@ -253,6 +291,9 @@ static int build_model(HostModel& m) {
     dqmc_params& p = m.p;
     if (p.t3 != 0.0) return fail(DQMC_EINVAL, "t3 != 0 is not supported");
     if (p.kinetic < DQMC_KIN_CHECKERBOARD || p.kinetic > DQMC_KIN_DENSE) return fail(DQMC_EINVAL, "kinetic must be 0, 1 or 2");
+    if (p.lattice < DQMC_LATT_SQUARE || p.lattice > DQMC_LATT_CHAIN) return fail(DQMC_EINVAL, "lattice must be 1, 2 or 3");
+    if (p.lattice == DQMC_LATT_CHAIN && (p.l2 != 1 || p.l1 < 4 || p.l1 % 2))
+        return fail(DQMC_EINVAL, "the chain needs l2 = 1 and an even l1 >= 4");
     if (p.kinetic == DQMC_KIN_FFT && (p.lattice != DQMC_LATT_SQUARE || p.l1 != p.l2))
         return fail(DQMC_EINVAL, "FFT kinetic term needs a square lattice with l1 == l2");
     if (p.lattice == DQMC_LATT_SQUARE && ((p.l1 * p.l2) % 2 != 0 || p.l1 % 2 || p.l2 % 2) && p.kinetic == DQMC_KIN_CHECKERBOARD)
@@ -453,6 +494,7 @@ static int upload_model(HostModel& m) {
     d.nwrap = p.nwrap; d.lwrapT = (p.rt != 0.0); d.lwrapu = (p.rhub != 0.0);
     d.phase_on = (p.rhub > 0.0) ? 1 : 0;
     d.rt = p.rt; d.rv = p.rv; d.t2 = p.t2; d.theta = p.theta * M_PI;
+    d.chain = p.lattice == DQMC_LATT_CHAIN;
     set_hs(m, d);
     // projective path and vconf constants (src/dqmc_config_v/dqmc_set_conf.f90:1-79)
     d.proj = p.proj ? 1 : 0;

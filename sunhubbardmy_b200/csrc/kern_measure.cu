@@ -2,7 +2,8 @@
 //
 // Reference: src/dqmc_measure/equaltime_measure.f90 (equaltime_measure 1-69,
 // zkint, zint_u, zint_v, zqsq, ztsq, ztq, measure_cpcm/spsm/nn/jj/bondcorr/
-// paircorr).  Observables use Gc(i,j) = delta_ij - G(j,i) and are weighted
+// paircorr) and, for the chain, equaltime_measure1d.f90 (the same bins with
+// one cell row; energy_bin 3 scaled by nflr rt, energy_bin 5 = zint_v).  Observables use Gc(i,j) = delta_ij - G(j,i) and are weighted
 // with zphi = sgn/Re(phase) * phase.  G^T is written first (a tiled
 // transpose), so that every correlation term reads a column of G or of G^T.
 // The distance-binned correlations are accumulated without atomics: the
@@ -52,25 +53,29 @@ DQ_DEV void meas_energy(const ChainDev& c, double2 zphi, double sgn) {
     const bool hc = (md.nsub == 2);
     // ---- energy terms ----
     double2 zne = cmk(0, 0), zu = cmk(0, 0), zk = cmk(0, 0), zv = cmk(0, 0);
+    // the chain's kinetic energy (equaltime_measure1d.f90) carries nflr rt on the
+    // bonds and 2 t2 on its two second neighbours
+    const bool chain = md.chain != 0;
+    const double kb = chain ? -2.0 * nflr * md.rt : -2.0, k2 = chain ? -2.0 * md.t2 : -md.t2;
     for (int i = tid; i < N; i += nth) {
         double2 d = gcf(G, N, i, i);
         zne = cadd(zne, d);
         zu = cadd(zu, cmul(d, d));
         if (md.t2 != 0.0) {
-            int ns = hc ? 6 : 4;
-            for (int f = 0; f < ns; ++f) zk.x += -md.t2 * gcf(G, N, i, md.snlist[i * md.nsn + f]).x;
+            int ns = chain ? 2 : hc ? 6 : 4;
+            for (int f = 0; f < ns; ++f) zk.x += k2 * gcf(G, N, i, md.snlist[i * md.nsn + f]).x;
         }
     }
     for (int b = tid; b < md.nn_lf * nnf; b += nth) {
         int i1 = md.bond_i1[b], i2 = md.bond_i2[b], nf = b / md.nn_lf;
         double2 g = gcf(G, N, i1, i2);
-        zk.x += -2.0 * cmul(g, md.expar_nn[i1 * nnf + nf]).x;
+        zk.x += kb * cmul(g, md.expar_nn[i1 * nnf + nf]).x;
         zv.x += g.x;
     }
     // plaquette terms
     double2 zq = cmk(0, 0), zt = cmk(0, 0), ztq = cmk(0, 0);
     const double2 em = cexpi(-md.theta), ep = cexpi(md.theta);
-    for (int q = tid; q < lq; q += nth) {
+    for (int q = tid; q < (chain ? 0 : lq); q += nth) {      // plaquette terms: 2D only
         const int* pc = md.plq_cord + q * zp;
         double2 tmp = cmk(0, 0);
         for (int a = 0; a < zp; ++a) tmp = cadd(tmp, gcf(G, N, pc[a], pc[a]));
@@ -135,10 +140,14 @@ DQ_DEV void meas_energy(const ChainDev& c, double2 zphi, double sgn) {
         bins[1] = cadd(bins[1], cscale(cmul(zne, zphi), 1.0 / lq));
         bins[2] = cadd(bins[2], cmul(zk, zphi));
         bins[3] = cadd(bins[3], cmul(zu, zphi));
-        bins[4] = cadd(bins[4], cscale(cmul(zq, zphi), 1.0 / 9.0));
-        bins[5] = cadd(bins[5], cmul(zt, zphi));
-        bins[6] = cadd(bins[6], cmul(ztq, zphi));
-        bins[7] = cadd(bins[7], cscale(cmul(zv, zphi), md.rv));
+        if (chain) {
+            bins[4] = cadd(bins[4], cmul(zv, zphi));     // energy_bin(5) of the chain, without rv
+        } else {
+            bins[4] = cadd(bins[4], cscale(cmul(zq, zphi), 1.0 / 9.0));
+            bins[5] = cadd(bins[5], cmul(zt, zphi));
+            bins[6] = cadd(bins[6], cmul(ztq, zphi));
+            bins[7] = cadd(bins[7], cscale(cmul(zv, zphi), md.rv));
+        }
         size_t tail = 10 + 20 * (size_t)lq;
         bins[tail + 0] = cadd(bins[tail + 0], cmul(zn0, zphi));
         bins[tail + 1] = cadd(bins[tail + 1], cmul(zn1, zphi));

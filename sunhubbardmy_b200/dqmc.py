@@ -14,7 +14,7 @@ import re
 
 import numpy as np
 
-SQUARE, HONEYCOMB = 1, 2
+SQUARE, HONEYCOMB, CHAIN = 1, 2, 3
 FAST, DELAY, SUBMATRIX = 0, 1, 2
 CHECKERBOARD, FFT, DENSE = 0, 1, 2
 EXACT, GENERAL4 = 0, 1
@@ -67,7 +67,7 @@ class DqmcParams(C.Structure):
         """Lattice / kinetic tables built by the library (1-based, host only)."""
         N, lq = self.ndim, self.lq
         hc = self.lattice == HONEYCOMB
-        nnf, z, nsn = (3, 6, 6) if hc else (4, 4, 4)
+        nnf, z, nsn = {HONEYCOMB: (3, 6, 6), CHAIN: (2, 1, 2)}.get(self.lattice, (4, 4, 4))
         nlf = lq if hc else lq // 2
         t = dict(nnlist=np.zeros((N, nnf), np.int32), nnlf_list=np.zeros(nlf, np.int32),
                  list=np.zeros((N, 2), np.int32), imj=np.zeros((lq, lq), np.int32),
@@ -517,7 +517,7 @@ class Dqmc:
     # projective path (params.proj = 1)
     def vconf(self, c: int = 0) -> np.ndarray:
         """t-V bond field vconf%conf as [ltrot][nn_nf][ndim] (bond index fastest)."""
-        nnf = 3 if self.chain_params(c).lattice == HONEYCOMB else 4
+        nnf = {HONEYCOMB: 3, CHAIN: 2}.get(self.chain_params(c).lattice, 4)
         out = np.zeros((self.ltrot, nnf, self.ndim(c)), np.int32)
         _check(load_library().dqmc_gpu_get_vconf(self.h, c, _ptr(out)), "get_vconf")
         return out

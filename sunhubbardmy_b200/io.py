@@ -73,9 +73,12 @@ def _fourier(gr: np.ndarray, zexpiqr: np.ndarray) -> np.ndarray:
     return zexpiqr @ gr
 
 
-def equaltime_output(bins_per_chain, outdir: str = ".", zexpiqr: np.ndarray | None = None) -> dict:
+def equaltime_output(bins_per_chain, outdir: str = ".", zexpiqr: np.ndarray | None = None,
+                     chain: bool = False) -> dict:
     """Reduce chain bins, normalise by n_chains*nobs and append to the
-    reference's files (energy.bin '(16e16.8)', n.bin, j.bin, b.bin, *_r.bin)."""
+    reference's files (energy.bin '(16e16.8)', n.bin, j.bin, b.bin, *_r.bin);
+    for the 1D chain energy.bin holds all ten energies ('(20e16.8)',
+    equaltime_output1d.f90)."""
     n = len(bins_per_chain)
     nobs = bins_per_chain[0]["nobs"]
     rnorm = float(n * nobs)
@@ -86,7 +89,7 @@ def equaltime_output(bins_per_chain, outdir: str = ".", zexpiqr: np.ndarray | No
         red[key] = sum(b[key] for b in bins_per_chain) / rnorm
     os.makedirs(outdir, exist_ok=True)
     with open(os.path.join(outdir, "energy.bin"), "a") as f:
-        e = red["energy"][:8]
+        e = red["energy"][:10] if chain else red["energy"][:8]
         f.write("".join(f"{v:16.8e}" for z in e for v in (z.real, z.imag)) + "\n")
     with open(os.path.join(outdir, "n.bin"), "a") as f:
         f.write("".join(f"{v:16.8e}" for z in red["zn"] for v in (z.real, z.imag)) + "\n")
@@ -131,8 +134,9 @@ def dyn_output(dyn_bins_per_chain, nsweep: int, nsub: int, outdir: str = ".",
         gk = np.einsum("tjim,km->tjik", gr, 1.0 / np.asarray(zexpiqr)) / lq
         with open(os.path.join(outdir, "nn_ktau.bin"), "a") as f:
             for nk in range(lq):
-                if listk is not None:
-                    f.write(f"{listk[nk][0] / l1:16.8f}{listk[nk][1] / l2:16.8f}\n")
+                if listk is not None:     # the chain writes k1 / l1 only (dyn_output1d.f90)
+                    f.write(f"{listk[nk][0] / l1:16.8f}{listk[nk][1] / l2:16.8f}\n" if l2 > 1
+                            else f"{listk[nk][0] / l1:16.8f}\n")
                 for nt in range(ntp):
                     f.write("".join(f"{v:16.8e}" for z in block(gk[..., nk], nt) for v in (z.real, z.imag)) + "\n")
     return gr

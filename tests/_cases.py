@@ -2,7 +2,7 @@
 
 The cases are small versions of the benchmark configurations (square Hubbard
 with checkerboard, FFT or dense kinetic term, exact or general HS field;
-honeycomb SU(4)) sized so the oracle finishes each in well under a second.
+honeycomb SU(4); the 1D chain) sized so the oracle finishes each in well under a second.
 """
 import numpy as np
 
@@ -29,6 +29,11 @@ CASES = {
                                  kinetic=2, update=1, hs=1, nwrap=10, nublock=8),
     "hc3_dense_su4_sub": dict(lattice=2, l1=3, l2=3, beta=1.6, dtau=0.1, rhub=6.0, nflr=4,
                               kinetic=2, update=2, hs=0, nwrap=8, nublock=8),
+    # the 1D chain (its own build of the reference, equaltime_measure1d.f90)
+    "ch8_cb_gen4_delay": dict(lattice=3, l1=8, l2=1, beta=2.0, dtau=0.1, rhub=4.0, nflr=2, mu=0.2, t2=0.3,
+                              flux_x=0.1, kinetic=0, update=1, hs=1, nwrap=5, nublock=4),
+    "ch10_dense_exact_sub": dict(lattice=3, l1=10, l2=1, beta=2.0, dtau=0.1, rhub=3.0, nflr=2,
+                                 kinetic=2, update=2, hs=0, nwrap=10, nublock=8),
 }
 
 TEST_SEED0 = 1909706392   # abs((0*1981+2008)*951049)

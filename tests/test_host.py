@@ -42,6 +42,25 @@ def test_params_derive_matches_oracle(oracle, case):
         assert p.nublock == m.nublock
 
 
+@pytest.mark.parametrize("kinetic", [0, 2])
+def test_chain_tables_match_oracle(oracle, kinetic):
+    """The library's chain (lattice 3) tables and bond exponentials equal the
+    oracle's restatement of setup_chain_sub and expar1d."""
+    import sunhubbardmy_b200 as sb
+    kw = dict(lattice=3, l1=10, l2=1, beta=1.0, dtau=0.1, rhub=2.0, mu=0.1, flux_x=0.2, dimer=0.1, kinetic=kinetic)
+    p = sb.DqmcParams.make(**kw)
+    m = oracle.Model(**kw)
+    t, to = p.tables(), m.tables()
+    for k in ("nnlist", "nnlf_list", "list", "imj", "plq_cord", "snlist"):
+        assert np.array_equal(t[k], to[k]), k
+    if kinetic == 0:
+        assert np.max(np.abs(t["urt"] - m.kinetic()["urt"])) < 1e-15
+    with pytest.raises(sb.DqmcError):
+        sb.DqmcParams.make(**dict(kw, l1=9))
+    with pytest.raises(sb.DqmcError):
+        sb.DqmcParams.make(**dict(kw, kinetic=1)).tables()     # the FFT pass is square-only
+
+
 def test_params_defaults_like_make_tables():
     import sunhubbardmy_b200 as sb
     # nublock defaults (src/model_para.f90:384-415)
@@ -112,6 +131,8 @@ def test_equaltime_output_normalisation(tmp_path):
     assert np.allclose(red["energy"], (flat[0][:10] + flat[1][:10]) / 10.0)
     line = (tmp_path / "energy.bin").read_text().strip()
     assert len(line.split()) == 16
+    sb.equaltime_output(bins, str(tmp_path / "chain"), chain=True)      # equaltime_output1d: all ten
+    assert len((tmp_path / "chain" / "energy.bin").read_text().split()) == 20
 
 
 def _gloo_worker(rank, world, port, q):

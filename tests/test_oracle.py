@@ -218,6 +218,42 @@ def test_projective_dyn_self_consistency(oracle):
     assert 0.0 < c.max_dyn_error() < 1e-10
 
 
+def test_chain_energy_terms(oracle):
+    """The chain's energy_bin of one measurement against the formulas of
+    equaltime_measure1d.f90 evaluated from G directly: density, kinetic energy
+    -2 nflr rt Re(Gc expar) over the bonds plus -2 t2 Re Gc over the two second
+    neighbours, double occupancy and the bond term; plaquette bins stay zero."""
+    kw = dict(lattice=3, l1=8, l2=1, beta=1.0, dtau=0.1, rhub=3.0, nflr=2, mu=0.2, t2=0.3, flux_x=0.1,
+              kinetic=2, update=1, hs=1, nwrap=5, nublock=4)
+    m = oracle.Model(**kw)
+    c = oracle.Chain(m, 3)
+    c.sweep_start()
+    c.obser_init()
+    c.measure()
+    g = c.green()
+    N = m.ndim
+    gc = np.eye(N) - g.T
+    ph = c.diag()["phase"]
+    zphi = (np.sign(ph.real) / ph.real) * ph
+    t = m.tables()
+    kin = 0.0
+    for i0 in t["nnlf_list"] - 1:
+        for nf, d in ((0, 1), (1, -1)):
+            i_n = t["nnlist"][i0, nf] - 1
+            e = np.exp(2j * np.pi * kw["flux_x"] * d / kw["l1"])
+            kin += -2 * kw["nflr"] * 1.0 * (gc[i0, i_n] * e).real
+    for i in range(N):
+        for nf in range(2):
+            kin += -2 * kw["t2"] * gc[i, t["snlist"][i, nf] - 1].real
+    zv = sum(gc[i0, t["nnlist"][i0, nf] - 1].real for i0 in t["nnlf_list"] - 1 for nf in range(2))
+    e = c.bins()["energy"]
+    assert abs(e[1] - np.trace(gc) / N * zphi) < 1e-12
+    assert abs(e[2] - kin * zphi) < 1e-12
+    assert abs(e[3] - np.sum(np.diag(gc) ** 2) * zphi) < 1e-12
+    assert abs(e[4] - zv * zphi) < 1e-12
+    assert np.all(e[5:8] == 0)
+
+
 def test_hubbard_atom_double_occupancy(oracle):
     """rt = 0: independent sites, H = U/2 (n - 1)^2 per site at half filling;
     D = e^{-beta U / 2} / (2 (1 + e^{-beta U/2})).  EXACTHS is exact here, so the
@@ -263,7 +299,7 @@ def test_update_flavours_agree(oracle, case):
 
 
 def test_lattice_tables(oracle):
-    for kw in (dict(lattice=1, l1=4, l2=6), dict(lattice=2, l1=3, l2=4)):
+    for kw in (dict(lattice=1, l1=4, l2=6), dict(lattice=2, l1=3, l2=4), dict(lattice=3, l1=8, l2=1)):
         m = oracle.Model(beta=1.0, dtau=0.1, **kw)
         t = m.tables()
         N, lq = m.ndim, m.lq
