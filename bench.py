@@ -538,6 +538,17 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
                              "chains": C, "tau_int_sweeps": tau, "ess": n_ess, "ess_per_s": n_ess / wall,
                              "mean": float(x.mean()), "stderr": float(x.std(ddof=1) / np.sqrt(n_ess)),
                              "wall_s": wall}
+        if args.workload == "config2" and hasattr(g, "time_op"):
+            # the delayed-update GEMM alone (dqmc_gpu_time_op 6: G += A B^T over
+            # nublock columns, one CTA per chain); it modifies G, so it runs last
+            fms = g.time_op(6, 5)
+            fl = 8.0 * float((Ns ** 2).sum()) * p.nublock
+            ach = fl / (fms * 1e-3) / 1e12
+            roof["update_gemm_isolated"] = {
+                "kernel": "k_update_flush (the flush_addto of k_update_delay)", "ms_per_launch": fms,
+                "achieved": ach, "peak": fp64, "unit": "TFLOP/s", "frac": ach / fp64,
+                "note": f"G += A B^T with N = {int(Ns.max())}, K = nublock = {p.nublock}, one CTA per chain "
+                        f"({C} chains) as inside the update kernel"}
         if world == 1 and not args.no_cpu and args.workload == "config2":
             per, times, _ = cpu_sample(20, os.cpu_count() or 1, steps=1)
             cv = per / times[0]

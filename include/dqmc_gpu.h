@@ -278,7 +278,7 @@ int dqmc_trial_state(const dqmc_params* p, int32_t seed, int draw_conf, double* 
 /* ---------------------------------------------------------------------------
  * Learned effective action and global block moves.  No counterpart in the
  * reference: an extra Monte Carlo move beside its local updates, which stay
- * the judge of every proposal (delayed-acceptance Metropolis-Hastings with the
+ * the arbiter of every proposal (delayed-acceptance Metropolis-Hastings with the
  * exact determinant ratio as the second stage).
  *
  * The effective action is a 3-layer periodic convolutional network over the

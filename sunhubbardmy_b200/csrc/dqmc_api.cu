@@ -2085,8 +2085,9 @@ extern "C" int dqmc_gpu_measure(dqmc_handle* h) {
 // the roofline of the dominant kernel.  op: 0 update (slice 1), 1 UDV step
 // (stabilisation kernel, into the spare stack slot), 2 Green's function
 // (equal-time, stack slots 1 and 0, into Gnew), 3 kinetic+HS column pass on
-// G, 4 measurement, 5 kinetic+HS row pass on G.  The chains' state is
-// modified (update, measurement): call it after the timed region.
+// G, 4 measurement, 5 kinetic+HS row pass on G, 6 the delayed update's flush
+// GEMM alone (G += A B^T over nublock columns).  The chains' state is modified
+// (update, measurement, flush): call it after the timed region.
 // ---------------------------------------------------------------------------
 extern "C" int dqmc_gpu_time_op(dqmc_handle* h, int op, int reps, double* ms_out) {
     if (!h || reps < 1 || !ms_out) return fail(DQMC_EINVAL, "invalid arguments");
@@ -2102,6 +2103,7 @@ extern "C" int dqmc_gpu_time_op(dqmc_handle* h, int op, int reps, double* ms_out
         case 4: launch_measure(h->d_chains, h->nch, h->maxN, h->models[0]->nsub == 2, h->max_lq, h->st); break;
         case 5: { PropProg p; p.n = 0; prog_k(m, p, PW_FWD, 0); prog_v(m, p, PW_FWD, 1); prog_k(m, p, PW_FWD, 1);
                   launch_prog(h, MAT_G, p, 1); break; }
+        case 6: launch_update_flush(h->d_chains, h->nch, h->st); break;
         default: break;
         }
     };
@@ -2133,7 +2135,7 @@ extern "C" int dqmc_gpu_time_op(dqmc_handle* h, int op, int reps, double* ms_out
         default: break;
         }
     };
-    if (op < 0 || op > 5) return fail(DQMC_EINVAL, "op 0..5");
+    if (op < 0 || op > 6 || (op == 6 && h->proj)) return fail(DQMC_EINVAL, "op 0..5 (0..6 at finite temperature)");
     if (h->proj) {
         if (!h->started) return fail(DQMC_ESTATE, "time_op before sweep_start");
         if (op == 0) launch_sfmt(h->d_chains, h->nch, 1, h->st);

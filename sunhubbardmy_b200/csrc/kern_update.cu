@@ -361,6 +361,15 @@ __global__ void __launch_bounds__(UPD_NT, 2) k_update_delay(const ChainDev* __re
     }
 }
 
+// The flush alone, G += A B^T over the model's nublock delayed columns, one
+// CTA per chain with the staging of k_update_delay: the delayed-update GEMM's
+// own rate (dqmc_gpu_time_op 6).  Modifies G.
+__global__ void __launch_bounds__(UPD_NT, 2) k_update_flush(const ChainDev* __restrict__ chains) {
+    extern __shared__ double2 dsm[];
+    const ChainDev& c = chains[blockIdx.x];
+    flush_addto(c.G, c.A, c.B, c.N, c.md->nublock, dsm);
+}
+
 static int g_upd_attr = 0;
 
 void launch_update(const ChainDev* chains, int nchains, int nt, int visit, cudaStream_t st, int forced) {
@@ -370,4 +379,15 @@ void launch_update(const ChainDev* chains, int nchains, int nt, int visit, cudaS
         g_upd_attr = 1;
     }
     k_update_delay<<<nchains, UPD_NT, smem, st>>>(chains, nt, visit, forced);
+}
+
+static int g_flush_attr = 0;
+
+void launch_update_flush(const ChainDev* chains, int nchains, cudaStream_t st) {
+    size_t smem = UpdGemm::SMEM_ELEMS * sizeof(double2);
+    if (!g_flush_attr) {
+        cudaFuncSetAttribute(k_update_flush, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        g_flush_attr = 1;
+    }
+    k_update_flush<<<nchains, UPD_NT, smem, st>>>(chains);
 }

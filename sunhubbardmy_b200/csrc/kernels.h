@@ -15,6 +15,7 @@ void launch_prop_fft(const ChainDev* chains, int nchains, int L, int nvec, int m
 void launch_sfmt(const ChainDev* chains, int nchains, int slices, cudaStream_t st);
 void launch_sfmt_raw(const ChainDev* chains, int chain, int count, cudaStream_t st);
 void launch_update(const ChainDev* chains, int nchains, int nt, int visit, cudaStream_t st, int forced = 0);
+void launch_update_flush(const ChainDev* chains, int nchains, cudaStream_t st);   // G += A B^T alone
 // equal-time measurement: G^T into GT (tiled transpose), then the observables
 void launch_measure(const ChainDev* chains, int nchains, int maxN, int hc, int maxlq, cudaStream_t st);
 void launch_bins_clear(const ChainDev* chains, int nchains, int nbins, cudaStream_t st);
