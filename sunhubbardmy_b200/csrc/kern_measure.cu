@@ -1,18 +1,19 @@
-// Equal-time measurement of one time slice; two CTAs per chain.
+// Equal-time measurement of one time slice.
 //
 // Reference: src/dqmc_measure/equaltime_measure.f90 (equaltime_measure 1-69,
 // zkint, zint_u, zint_v, zqsq, ztsq, ztq, measure_cpcm/spsm/nn/jj/bondcorr/
 // paircorr) and, for the chain, equaltime_measure1d.f90 (the same bins with
-// one cell row; energy_bin 3 scaled by nflr rt, energy_bin 5 = zint_v).  Observables use Gc(i,j) = delta_ij - G(j,i) and are weighted
-// with zphi = sgn/Re(phase) * phase.  G^T is written first (a tiled
-// transpose), so that every correlation term reads a column of G or of G^T.
-// The distance-binned correlations are accumulated without atomics: the
-// chain's first CTA walks the unit cells j in order, stages the few columns
-// of G and G^T that cell j pairs with into shared memory (double-buffered
-// cp.async), and every thread adds cell j's term to the two bins (distance
-// d, orbitals a, b) it owns, pairing j with cell i = j + d (imj(i, j) = d, in
-// closed form).  Each column crosses L2 once per cell instead of once per
-// 32 bins.  The single-number energy terms run on the chain's second CTA.
+// one cell row; energy_bin 3 scaled by nflr rt, energy_bin 5 = zint_v).
+// Observables use Gc(i,j) = delta_ij - G(j,i) and are weighted with
+// zphi = sgn/Re(phase) * phase.  G^T is written first (a tiled transpose), so
+// that every correlation term reads a column of G or of G^T.  Per chain, one
+// CTA sums the single-number energy terms, and CTAs of site bins (cpcm, spsm,
+// nn, pair_onsite) and of bond bins (jj, bb, pair_nn, pair_sn) follow.  Two
+// threads own a bin (distance d, orbitals a, b); they walk the even and the
+// odd unit cells j in order, pairing j with cell i = j + d (imj(i, j) = d, in
+// closed form), and their sums are added in a fixed order, so no atomics are
+// needed and the result does not depend on scheduling.  Threads of
+// consecutive d read consecutive rows of the same columns (coalesced).
 //
 // Bin layout per chain (complex): energy[10], cpcm, spsm, nn, pair_onsite
 // [lq*4 each, index (d) + lq*(no_i + 2 no_j)], jj, bb, pair_nn, pair_sn [lq
