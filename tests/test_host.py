@@ -229,6 +229,9 @@ def test_dyn_output_files(tmp_path):
     k1 = np.array(krows[1].split(), float)                  # nk = 1, nt = 1
     gk = (gr[0, 0, 0, :] / zq[0, :]).sum() / lq
     assert np.allclose(k1[0] + 1j * k1[1], gk, atol=1e-7)
+    # the chain (dyn_output1d.f90) lists k1 / l1 only
+    dyn_output(bins, 5, 1, str(tmp_path / "chain"), zexpiqr=zq, listk=np.ones((lq, 2)), l1=4, l2=1)
+    assert open(tmp_path / "chain" / "nn_ktau.bin").read().splitlines()[0].split() == [f"{0.25:.8f}"]
 
 
 def test_dqmc_out_writers():
