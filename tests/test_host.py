@@ -276,3 +276,32 @@ def test_dqmc_out_writers():
     out = f.getvalue()
     assert " >>> accep_u     =   0.25000000E+00\n" in out and " >>> Total time spent:     12.50s\n" in out
     assert "The_time_of_ft_delay_update:         0.100s =  50.00%\n" in out
+
+
+def _c_fields(header: str, name: str):
+    import re
+    i = header.index(f"typedef struct {name} {{")
+    j = header.index(f"}} {name};")
+    body = re.sub(r"/\*.*?\*/", "", header[i:j], flags=re.S)
+    return [("i" if t == "int32_t" else "d", x.strip())
+            for t, names in re.findall(r"(int32_t|double)\s+([^;]+);", body) for x in names.split(",")]
+
+
+def _f_fields(doc: str, name: str):
+    import re
+    a = doc.index(f"type, bind(C) :: {name}")
+    b = doc.index("end type", a)
+    return [("i" if t.startswith("integer") else "d", x.strip())
+            for t, names in re.findall(r"(integer\(c_int32_t\)|real\(c_double\))\s*::\s*(.+)", doc[a:b])
+            for x in names.split(",")]
+
+
+def test_fortran_binding_types_mirror_the_header():
+    """The iso_c_binding types of the integration guide list the C structs'
+    fields in the same order and kind, so dqmc_gpu_get_diag and
+    dqmc_params_derive never write past a Fortran caller's variable."""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    header = open(os.path.join(root, "include", "dqmc_gpu.h")).read()
+    doc = open(os.path.join(root, "INTEGRATION.md")).read()
+    assert _c_fields(header, "dqmc_params") == _f_fields(doc, "dqmc_params_c")
+    assert _c_fields(header, "dqmc_diag") == _f_fields(doc, "dqmc_diag_c")
