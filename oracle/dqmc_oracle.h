@@ -6,20 +6,24 @@
  * check and the cpu_baseline / reference arm of bench.py may load it.  The
  * product library (sunhubbardmy_b200) never links, loads or calls it.
  *
- * It restates, in plain C99, the Fortran reference's finite-temperature hot
- * path: SFMT RNG (lib/m_spring.f90), square/honeycomb lattice tables
- * (src/lattice.f90), HS constants (src/dqmc_config_u/dqmc_set_conf.f90),
- * kinetic propagators (src/dqmc_config_h0/ directory), local updates
+ * It restates, in plain C99, the Fortran reference's hot path: SFMT RNG
+ * (lib/m_spring.f90), square/honeycomb/chain lattice tables (src/lattice.f90),
+ * HS constants (src/dqmc_config_u/dqmc_set_conf.f90), kinetic propagators
+ * (checkerboard, FFT and dense; src/dqmc_config_h0/ directory), local updates
  * (src/dqmc_config_u/dqmc_update*.f90), the UDV stack
  * (src/dqmc_ft_core/dqmc_ft_stablize_*.f90, lib/s_matrix.f90), the Green's
- * functions (src/dqmc_ft_core/green_equaltime*.f90) and the equal-time
- * measurement (src/dqmc_measure/equaltime_measure.f90).
+ * functions (src/dqmc_ft_core/green_equaltime*.f90, green_tau.f90), the
+ * equal-time and unequal-time measurements (src/dqmc_measure/
+ * equaltime_measure.f90, equaltime_measure1d.f90, dyn_measure.f90) and the
+ * projective core with its unequal-time pass (src/dqmc_proj_core/, in
+ * orc_proj.c).
  *
  * Parity status: UNPINNED against reference output.  The reference is Fortran
  * + MPI + MKL; none of the three exist on either machine, and the reference
  * ships no golden vectors or stored outputs.  The oracle is pinned instead by
  * known answers (free-fermion Green's function, atomic limit, an independent
- * SFMT restatement, scipy LAPACK for the linear-algebra kernels).
+ * SFMT restatement, scipy LAPACK for the linear-algebra kernels, expm for the
+ * dense kinetic operators).
  *
  * Matrices are column-major complex128 (Fortran layout), indices 0-based
  * internally; HS-field values are 1..lcomp exactly as in the reference.
