@@ -909,6 +909,21 @@ static void* dalloc(dqmc_handle* h, size_t bytes) {
     return p;
 }
 
+// frees one allocation made by dalloc (and forgets it)
+static void dfree(dqmc_handle* h, void* p) {
+    if (!p) return;
+    for (size_t k = 0; k < h->allocs.size(); ++k)
+        if (h->allocs[k] == p) { h->allocs.erase(h->allocs.begin() + k); break; }
+    cudaFree(p);
+}
+
+// the captured sweep holds device pointers and sizes as kernel arguments: any
+// change of them (record buffers) must drop it
+static void drop_sweep_graph(dqmc_handle* h) {
+    if (h->sweep_graph) { cudaGraphExecDestroy(h->sweep_graph); h->sweep_graph = nullptr; }
+    h->graph_meas = -1;
+}
+
 extern "C" int dqmc_gpu_destroy(dqmc_handle* h) {
     if (!h) return DQMC_OK;
     if (h->st) cudaStreamSynchronize(h->st);
@@ -1182,25 +1197,29 @@ static int launch_prog(dqmc_handle* h, int mat_id, const PropProg& prog, int rig
     return DQMC_OK;
 }
 
-// B(nt1, nt2) from the left (Bmat_left_forward, src/dqmc_ft_core.f90:70-121)
-static PropProg prog_bmat(const HostModel& m, int nt1, int nt2) {
+// B(nt1, nt2) from the left (Bmat_left_forward, src/dqmc_ft_core.f90:70-121) or
+// B(nt1, nt2)^H (Bmat_left_forward_hc, 123-175) applied to matrix mat_id.  The
+// slices are collected into programs of at most DQ_MAX_PROG ops, each launched
+// when the next slice would not fit, so any nwrap is applied in full (a
+// checkerboard slice is 2 nn_nf + 1 ops).  Splitting a program only stores and
+// reloads the vectors between two ops, so the result does not depend on it.
+static int launch_bmat(dqmc_handle* h, int mat_id, int nt1, int nt2, int hc) {
+    const HostModel& m = *h->models[0];
     PropProg p; p.n = 0;
-    for (int nt = nt2; nt <= nt1; ++nt) {
-        prog_k(m, p, PW_FWD, 0);
-        prog_v(m, p, PW_FWD, nt);
-        prog_k(m, p, PW_FWD, 1);
+    for (int s = 0; s <= nt1 - nt2; ++s) {
+        const int nt = hc ? nt1 - s : nt2 + s;
+        const int which = hc ? PW_CONJ : PW_FWD;
+        PropProg sl; sl.n = 0;
+        prog_k(m, sl, which, 0);
+        prog_v(m, sl, which, nt);
+        prog_k(m, sl, which, 1);
+        if (p.n + sl.n > DQ_MAX_PROG) {
+            int rc = launch_prog(h, mat_id, p, 0); if (rc) return rc;
+            p.n = 0;
+        }
+        for (int k = 0; k < sl.n; ++k) p.op[p.n++] = sl.op[k];
     }
-    return p;
-}
-// B(nt1, nt2)^H from the left (Bmat_left_forward_hc, src/dqmc_ft_core.f90:123-175)
-static PropProg prog_bmat_hc(const HostModel& m, int nt1, int nt2) {
-    PropProg p; p.n = 0;
-    for (int nt = nt1; nt >= nt2; --nt) {
-        prog_k(m, p, PW_CONJ, 0);
-        prog_v(m, p, PW_CONJ, nt);
-        prog_k(m, p, PW_CONJ, 1);
-    }
-    return p;
+    return launch_prog(h, mat_id, p, 0);
 }
 
 enum { MAT_G = 0, MAT_GT0 = 15, MAT_G0T = 16, MAT_U = 100, MAT_V = 400 };   // ids of chain_access.cuh
@@ -1238,8 +1257,7 @@ static void stab_0b(dqmc_handle* h, int n, int record) {
     int spare = h->nst + 1;
     launch_copy_mat(h->d_chains, h->nch, 2 /*W0*/, MAT_U + (n - 1), 0, h->st);
     tmark(h, DQMC_PROF_OTHER);
-    PropProg p = prog_bmat(m, m.wrap_step[(n - 1) * 2 + 1], m.wrap_step[(n - 1) * 2]);
-    launch_prog(h, 2, p, 0);
+    launch_bmat(h, 2, m.wrap_step[(n - 1) * 2 + 1], m.wrap_step[(n - 1) * 2], 0);
     tmark(h, DQMC_PROF_BPROD);
     launch_stab_slots(h->d_chains, h->nch, n - 1, spare, h->st);
     tmark(h, DQMC_PROF_STAB);
@@ -1257,8 +1275,7 @@ static void stab_b0(dqmc_handle* h, int n) {
     int spare = h->nst + 1;
     launch_copy_mat(h->d_chains, h->nch, 2, MAT_U + (n + 1), 0, h->st);
     tmark(h, DQMC_PROF_OTHER);
-    PropProg p = prog_bmat_hc(m, m.wrap_step[n * 2 + 1], m.wrap_step[n * 2]);
-    launch_prog(h, 2, p, 0);
+    launch_bmat(h, 2, m.wrap_step[n * 2 + 1], m.wrap_step[n * 2], 1);
     tmark(h, DQMC_PROF_BPROD);
     launch_stab_slots(h->d_chains, h->nch, n + 1, spare, h->st);
     tmark(h, DQMC_PROF_STAB);
@@ -1566,8 +1583,7 @@ extern "C" int dqmc_gpu_sweep_start(dqmc_handle* h) {
     launch_stack_identity(h->d_chains, h->nch, 0, h->st);
     for (int n = 1; n <= h->nst; ++n) {
         launch_copy_mat(h->d_chains, h->nch, 2, MAT_U + (n - 1), 0, h->st);
-        PropProg p = prog_bmat(m, m.wrap_step[(n - 1) * 2 + 1], m.wrap_step[(n - 1) * 2]);
-        launch_prog(h, 2, p, 0);
+        launch_bmat(h, 2, m.wrap_step[(n - 1) * 2 + 1], m.wrap_step[(n - 1) * 2], 0);
         launch_stab_slots(h->d_chains, h->nch, n - 1, n, h->st);
     }
     launch_green(h->d_chains, h->nch, h->nst, 0, 0, 0, 0, 0, 1, h->st);
@@ -1647,8 +1663,7 @@ static void stab_dyn(dqmc_handle* h, int n) {
     const HostModel& m = *h->models[0];
     int spare = h->nst + 1;
     launch_copy_mat(h->d_chains, h->nch, 2 /*W0*/, MAT_U + (n - 1), 0, h->st);
-    PropProg p = prog_bmat(m, m.wrap_step[(n - 1) * 2 + 1], m.wrap_step[(n - 1) * 2]);
-    launch_prog(h, 2, p, 0);
+    launch_bmat(h, 2, m.wrap_step[(n - 1) * 2 + 1], m.wrap_step[(n - 1) * 2], 0);
     launch_stab_slots(h->d_chains, h->nch, n - 1, spare, h->st);
     launch_green_tau(h->d_chains, h->nch, spare, n, h->st);
     launch_wrap_check(h->d_chains, h->nch, 1, h->st);
@@ -1749,8 +1764,8 @@ extern "C" int dqmc_gpu_sweep_0b(dqmc_handle* h, int lupdate, int lmeasure) {
 // recording changed
 static int ensure_sweep_graph(dqmc_handle* h, int lmeasure) {
     if (!h->sweep_graph || h->graph_meas != lmeasure + 2 * h->rec_on) {
-        if (h->sweep_graph) { cudaGraphExecDestroy(h->sweep_graph); h->sweep_graph = nullptr; }
-        cudaGraph_t g;
+        drop_sweep_graph(h);
+        cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
         if (h->proj) {
             enqueue_proj_b0(h, 1, lmeasure);
@@ -1760,12 +1775,23 @@ static int ensure_sweep_graph(dqmc_handle* h, int lmeasure) {
             if (lmeasure && h->models[0]->p.ltau) enqueue_dyn(h);   // dqmc_sweep (src/dqmc_ft_ctrl.f90:97-101)
             enqueue_0b(h, 1, lmeasure);
         }
-        CK(cudaStreamEndCapture(h->st, &g));
-        CK(cudaGraphInstantiate(&h->sweep_graph, g, 0));
+        // the capture always ends here, so the stream leaves capture mode on
+        // every path; a failed capture's partial graph is discarded
+        cudaError_t e = cudaStreamEndCapture(h->st, &g);
+        if (e != cudaSuccess || !g) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return fail(DQMC_ECUDA, std::string("sweep capture: ") + cudaGetErrorString(e));
+        }
+        e = cudaGraphInstantiate(&h->sweep_graph, g, 0);
         size_t nn = 0;
-        cudaGraphGetNodes(g, nullptr, &nn);
-        h->graph_nodes = nn;
+        if (e == cudaSuccess) cudaGraphGetNodes(g, nullptr, &nn);
         cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            h->sweep_graph = nullptr;
+            return fail(DQMC_ECUDA, std::string("sweep graph instantiation: ") + cudaGetErrorString(e));
+        }
+        h->graph_nodes = nn;
         h->graph_meas = lmeasure + 2 * h->rec_on;
     }
     return DQMC_OK;
@@ -1808,24 +1834,31 @@ extern "C" int dqmc_gpu_sweeps_multi(dqmc_handle* const* hs, int nh, int n, int 
     }
     dqmc_handle* h0 = hs[0];
     cudaEvent_t fork = nullptr, join[16] = {};
-    CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
-    for (int k = 1; k < nh; ++k) CK(cudaEventCreateWithFlags(&join[k], cudaEventDisableTiming));
-    CK(cudaEventRecord(h0->ev0, h0->st));
-    CK(cudaEventRecord(fork, h0->st));
-    for (int k = 1; k < nh; ++k) CK(cudaStreamWaitEvent(hs[k]->st, fork, 0));
-    for (int i = 0; i < n; ++i)
-        for (int k = 0; k < nh; ++k) CK(cudaGraphLaunch(hs[k]->sweep_graph, hs[k]->st));
-    for (int k = 1; k < nh; ++k) {
-        CK(cudaEventRecord(join[k], hs[k]->st));
-        CK(cudaStreamWaitEvent(h0->st, join[k], 0));
+    // the first error is kept; every stream is still joined and every event
+    // destroyed before returning
+    cudaError_t err = cudaSuccess;
+    auto keep = [&](cudaError_t e) { if (err == cudaSuccess && e != cudaSuccess) err = e; };
+    keep(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    for (int k = 1; k < nh; ++k) keep(cudaEventCreateWithFlags(&join[k], cudaEventDisableTiming));
+    if (err == cudaSuccess) {
+        keep(cudaEventRecord(h0->ev0, h0->st));
+        keep(cudaEventRecord(fork, h0->st));
+        for (int k = 1; k < nh; ++k) keep(cudaStreamWaitEvent(hs[k]->st, fork, 0));
+        for (int i = 0; i < n && err == cudaSuccess; ++i)
+            for (int k = 0; k < nh; ++k) keep(cudaGraphLaunch(hs[k]->sweep_graph, hs[k]->st));
+        for (int k = 1; k < nh; ++k) {
+            keep(cudaEventRecord(join[k], hs[k]->st));
+            keep(cudaStreamWaitEvent(h0->st, join[k], 0));
+        }
+        keep(cudaEventRecord(h0->ev1, h0->st));
     }
-    CK(cudaEventRecord(h0->ev1, h0->st));
-    CK(cudaStreamSynchronize(h0->st));
-    CK(cudaGetLastError());
+    for (int k = 0; k < nh; ++k) keep(cudaStreamSynchronize(hs[k]->st));
+    keep(cudaGetLastError());
     float ms = 0;
-    cudaEventElapsedTime(&ms, h0->ev0, h0->ev1);
-    cudaEventDestroy(fork);
-    for (int k = 1; k < nh; ++k) cudaEventDestroy(join[k]);
+    if (err == cudaSuccess) keep(cudaEventElapsedTime(&ms, h0->ev0, h0->ev1));
+    if (fork) cudaEventDestroy(fork);
+    for (int k = 1; k < nh; ++k) if (join[k]) cudaEventDestroy(join[k]);
+    if (err != cudaSuccess) return fail(DQMC_ECUDA, std::string("sweeps_multi: ") + cudaGetErrorString(err));
     for (int k = 0; k < nh; ++k) hs[k]->last_ms = ms / n;
     if (ms_out) *ms_out = ms / n;
     return DQMC_OK;
@@ -2500,6 +2533,13 @@ extern "C" int dqmc_gpu_record(dqmc_handle* h, int capacity) {
     for (auto& ch : h->chains)
         if (ch.dev.N * h->ltrot != V) return fail(DQMC_EINVAL, "recording needs chains of one size");
     if (capacity != h->rec_cap) {
+        // a captured sweep that records still points at the old buffers
+        CK(cudaStreamSynchronize(h->st));
+        drop_sweep_graph(h);
+        dfree(h, h->rec_f);
+        dfree(h, h->rec_v);
+        dfree(h, h->rec_count);
+        h->rec_f = nullptr; h->rec_v = nullptr; h->rec_count = nullptr; h->rec_cap = 0;
         h->rec_f = (int8_t*)dalloc(h, (size_t)capacity * V);
         h->rec_v = (double*)dalloc(h, (size_t)capacity * sizeof(double));
         h->rec_count = (int*)dalloc(h, sizeof(int));

@@ -16,7 +16,9 @@
 // kernel.  All calls share the array: no part of it is read before the same
 // call has written it, so nothing has to be cleared between calls, but two
 // calls whose kernels overlap on the GPU race on it.
+#include <atomic>
 #include <cstdio>
+#include <mutex>
 
 #include "../../include/dqmc_gpu.h"
 #include "linalg.cuh"
@@ -58,8 +60,14 @@ __global__ void __launch_bounds__(256) k_qr_noalloc(int n, double2* A, double2* 
 }
 
 #define NOALLOC_MAX_DEVICES 64
-static void* g_noalloc_ptr[NOALLOC_MAX_DEVICES];
-static int g_noalloc_attr[NOALLOC_MAX_DEVICES];
+// per-device set-up (scratch address, shared-memory attribute), done once per
+// device under a lock so that host threads making their first call on a
+// device at the same time do not race on it; later calls only read the
+// published address.  The address belongs to the device's current context: a
+// cudaDeviceReset invalidates it, and calls after such a reset are not
+// supported.
+static std::atomic<void*> g_noalloc_ptr[NOALLOC_MAX_DEVICES];
+static std::mutex g_noalloc_lock;
 
 static thread_local char g_noalloc_err[256] = "";
 
@@ -81,26 +89,30 @@ extern "C" int dqmc_gpu_qr_logdet_noalloc(int n, double* a, double* q, double* l
         snprintf(g_noalloc_err, sizeof(g_noalloc_err), "dqmc_gpu_qr_logdet_noalloc: no usable current device");
         return DQMC_ECUDA;
     }
-    if (!g_noalloc_ptr[dev]) {
-        // first call on this device: device address of the static scratch
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            snprintf(g_noalloc_err, sizeof(g_noalloc_err), "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
-            return DQMC_ECUDA;
+    void* scratch = g_noalloc_ptr[dev].load(std::memory_order_acquire);
+    if (!scratch) {
+        // first call on this device: device address of the static scratch and
+        // the kernel's shared-memory limit, published only once both are set
+        std::lock_guard<std::mutex> lock(g_noalloc_lock);
+        scratch = g_noalloc_ptr[dev].load(std::memory_order_acquire);
+        if (!scratch) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess || !p) {
+                snprintf(g_noalloc_err, sizeof(g_noalloc_err), "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+                return DQMC_ECUDA;
+            }
+            e = cudaFuncSetAttribute(k_qr_noalloc, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            if (e != cudaSuccess) {
+                snprintf(g_noalloc_err, sizeof(g_noalloc_err), "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+                return DQMC_ECUDA;
+            }
+            g_noalloc_ptr[dev].store(p, std::memory_order_release);
+            scratch = p;
         }
-        g_noalloc_ptr[dev] = p;
-    }
-    if (!g_noalloc_attr[dev]) {
-        e = cudaFuncSetAttribute(k_qr_noalloc, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        if (e != cudaSuccess) {
-            snprintf(g_noalloc_err, sizeof(g_noalloc_err), "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
-            return DQMC_ECUDA;
-        }
-        g_noalloc_attr[dev] = 1;
     }
     k_qr_noalloc<<<1, 256, noalloc_smem_bytes(n), (cudaStream_t)stream>>>(
-        n, (double2*)a, (double2*)q, (double2*)logdetq, (double2*)g_noalloc_ptr[dev]);
+        n, (double2*)a, (double2*)q, (double2*)logdetq, (double2*)scratch);
     e = cudaGetLastError();
     if (e != cudaSuccess) {
         snprintf(g_noalloc_err, sizeof(g_noalloc_err), "k_qr_noalloc launch: %s", cudaGetErrorString(e));

@@ -95,6 +95,27 @@ def test_recorded_pairs_are_fields_and_weights(sb):
     g.record(0)
 
 
+def test_record_with_new_capacity_after_stop(sb):
+    """record(a), sweeps, record(0), record(b != a), sweeps: the captured sweep
+    must write into the new buffers, which then hold the new pairs."""
+    p = sb.DqmcParams.make(**HUB)
+    g = sb.Dqmc(p, n_chains=2)
+    g.sweep_start()
+    g.record(100)
+    g.sweeps(1, False)
+    assert g.record_count() == 2 * 2 * p.nst
+    g.record(0)
+    g.record(300)
+    assert g.record_count() == 0
+    g.sweeps(1, False)
+    n = g.record_count()
+    assert n == 2 * 2 * p.nst
+    f, v = g.record_get(n - 1)
+    assert np.array_equal(f.reshape(p.ltrot, -1), 2 * g.conf(1) - 3)
+    assert abs(v - p.nflr * g.diag(1)["logweight"].real) < 1e-9 * max(1.0, abs(v))
+    g.record(0)
+
+
 def test_block_moves_are_exact(sb):
     """Local updates off: every change of the field comes from accepted
     blocks, so nflr * (Re log W_end - Re log W_start) must equal the sum of

@@ -1,7 +1,10 @@
 """Edge sizes on the GPU against the oracle: the largest supported lattice
 (honeycomb 16 x 16, N = 512, the shared-memory limit of the per-chain
 kernels), a stabilisation interval that does not divide ltrot (ragged last
-interval), and a single time slice per interval (nwrap = 1)."""
+interval), a single time slice per interval (nwrap = 1), and long
+intervals whose B(tau2, tau1) products hold more propagation ops than one
+launch takes (nwrap = 40: 9 ops per checkerboard slice on the square lattice,
+7 on the honeycomb one), so the product runs as several launches."""
 import numpy as np
 import pytest
 
@@ -14,6 +17,10 @@ SIZES = {
                             nwrap=5, nublock=8),
     "sq4_nwrap1": dict(lattice=1, l1=4, l2=4, beta=0.5, dtau=0.1, rhub=4.0, nflr=2, kinetic=1, update=1, hs=0,
                        nwrap=1, nublock=4),
+    "sq4_cb_nwrap40": dict(lattice=1, l1=4, l2=4, beta=2.0, dtau=0.05, rhub=2.0, nflr=2, kinetic=0, update=1,
+                           hs=1, nwrap=40, nublock=8),
+    "hc3_cb_nwrap40": dict(lattice=2, l1=3, l2=3, beta=2.0, dtau=0.05, rhub=2.0, nflr=2, kinetic=0, update=2,
+                           hs=0, nwrap=40, nublock=8),
 }
 
 

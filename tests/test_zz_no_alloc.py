@@ -26,11 +26,16 @@ def _graded(n, seed):
 
 
 def _reference_qr(sb, a):
-    """QR through the existing handle-based entry point."""
+    """QR through the existing handle-based entry point (a handle whose chain
+    has N = n sites: a square lattice when n is a square, else a honeycomb one)."""
     n = a.shape[0]
     side = int(round(np.sqrt(n)))
-    assert side * side == n
-    p = sb.DqmcParams.make(lattice=1, l1=side, l2=side, beta=1.0, dtau=0.1, rhub=4.0, nwrap=10)
+    if side * side == n:
+        p = sb.DqmcParams.make(lattice=1, l1=side, l2=side, beta=1.0, dtau=0.1, rhub=4.0, nwrap=10)
+    else:
+        side = int(round(np.sqrt(n // 2)))
+        assert 2 * side * side == n
+        p = sb.DqmcParams.make(lattice=2, l1=side, l2=side, beta=1.0, dtau=0.1, rhub=4.0, nwrap=10)
     with sb.Dqmc(p, 1) as g:
         g.set_work(0, a)
         ld = g.test_qr(0, 1)[0]
@@ -41,7 +46,9 @@ def _rel(x, y):
     return float(np.max(np.abs(x - y)) / max(1e-300, np.max(np.abs(y))))
 
 
-@pytest.mark.parametrize("n", [64, 256])
+# 64 and 256 fill whole 16-column panels and 64-column blocks; 36, 100 and
+# 484 end on a ragged panel (n mod 16 = 4); 512 is the scratch limit
+@pytest.mark.parametrize("n", [36, 64, 100, 256, 484, 512])
 def test_noalloc_qr_matches_handle_qr_twice(n):
     import torch
     import sunhubbardmy_b200 as sb
