@@ -6,7 +6,7 @@
  * (YuanyueChen/sunhubbardmy).  In the reference the path is reached through
  * Fortran module procedures (no FFI exists); each entry point below names the
  * reference routine whose effect it reproduces, so a Fortran iso_c_binding
- * shim can replace them one by one.
+ * shim (include/dqmc_gpu_f.f90) can replace them one by one.
  *
  * Conventions
  *  - Matrices are complex128, column-major (Fortran layout), passed as
@@ -36,6 +36,20 @@ extern "C" {
 #define DQMC_ECUDA (-2)      /* CUDA runtime error */
 #define DQMC_ENOMEM (-3)     /* device allocation failed */
 #define DQMC_ESTATE (-4)     /* call out of order (e.g. sweep before sweep_start) */
+/* numerical failure: a zero or non-finite pivot in the QR of a UDV step, of the
+ * middle matrix of green_equaltime / green_tau or of UL UR, or a freshly
+ * computed Green's function that is not finite.  The reference stops the run
+ * there (the LAPACK info /= 0 stops of lib/s_matrix.f90:1260-1267 and
+ * src/dqmc_ft_core/dqmc_ft_sweep_b0.f90:188-194); the chain keeps its
+ * propagated G, and dqmc_diag.info holds the DQMC_FAIL_* bits per chain. */
+#define DQMC_ENUMERIC (-5)
+/* a wrap check exceeded the tolerance set by dqmc_gpu_set_checks */
+#define DQMC_EWRAP (-6)
+
+/* dqmc_diag.info bits */
+#define DQMC_FAIL_SINGULAR 1
+#define DQMC_FAIL_NONFINITE 2
+#define DQMC_FAIL_WRAP 4
 
 /* enums (compile-time RUNMODE flags of src/make.sys.* turned into values) */
 #define DQMC_LATT_SQUARE 1     /* -DSQUARE */
@@ -87,6 +101,8 @@ typedef struct dqmc_diag {
     double blk_err_learned, blk_err_zero;   /* sums over second-stage blocks of (log|R| + dS)^2 and (log|R|)^2 */
     double max_dyn_error;               /* xmax_dyn: projective unequal-time pass, max |G(t,t) propagated - fresh| */
     double dyn_log10_sum, dyn_count;    /* sum of log10 of those checks (avglog10dynerror) and their number */
+    double info;                        /* OR of the DQMC_FAIL_* codes this chain raised since reset_diag */
+    double restabilized;                /* re-stabilisations of the handle (dqmc_gpu_set_checks) since reset_diag */
 } dqmc_diag;
 
 typedef struct dqmc_handle dqmc_handle;
@@ -126,6 +142,26 @@ int dqmc_gpu_get_conf_all(dqmc_handle* h, int32_t* conf);
 /* Equal-time Green's function G = <c c^+> of one chain (gf%blk1). */
 int dqmc_gpu_get_green(dqmc_handle* h, int chain, double* g);
 int dqmc_gpu_set_green(dqmc_handle* h, int chain, const double* g);
+
+/* Entry n = 0..nst of the finite-temperature UDV stack of one chain: Ust(n)
+ * and Vst(n) (N x N complex), Dst(n) (N doubles) and logdetQst(n) (one
+ * complex), the module arrays of src/dqmc_ft_core.f90:11-19.  Any pointer may
+ * be NULL.  DQMC_ESTATE on a projective handle. */
+int dqmc_gpu_get_stack(dqmc_handle* h, int chain, int n, double* u, double* d, double* v, double* logdetq);
+int dqmc_gpu_set_stack(dqmc_handle* h, int chain, int n, const double* u, const double* d, const double* v,
+                       const double* logdetq);
+
+/* Numerical checks of the sweep entry points (sweep_start, sweep_b0/_0b,
+ * sweeps, sweeps_multi, sweep_dyn, sweep_learned).  Singular and non-finite
+ * Green's functions are always reported (DQMC_ENUMERIC).  wrap_tol > 0 also
+ * reports a wrap check (s_compare_max_z at a stabilisation) above wrap_tol, or
+ * not finite, as DQMC_EWRAP (0 = no tolerance, the default).  restabilize != 0:
+ * instead of returning either code, a call that ends at tau = beta (sweep_0b,
+ * sweeps, sweeps_multi, sweep_learned) rebuilds every chain's stack and G
+ * from its HS field (dqmc_ft_sweep_start_0b / dqmc_proj_sweep_start_0b) and
+ * returns 0 if the rebuilt G is sound; dqmc_diag.restabilized counts these.
+ * A call always runs all its sweeps; the status is read at its end. */
+int dqmc_gpu_set_checks(dqmc_handle* h, double wrap_tol, int restabilize);
 
 /* dqmc_ft_sweep_start_0b (src/dqmc_ft_core/dqmc_ft_sweep_start_0b.f90): UDV
  * stack 0 -> beta and G(beta, beta). */
@@ -168,6 +204,12 @@ int dqmc_gpu_measure(dqmc_handle* h);
 int dqmc_gpu_set_phase(dqmc_handle* h, int chain, double re, double im);
 /* raw SFMT draws (spring_sfmt_source) of a chain, advancing its generator */
 int dqmc_gpu_draw_u32(dqmc_handle* h, int chain, int count, uint32_t* out);
+/* SFMT-19937 state of one chain as the reference holds it (lib/m_spring.f90:66-71):
+ * 625 int32 words, pt32(0:623) then the read index idx (0..624; 624 = the next
+ * draw regenerates the block).  set_rng continues a caller's stream (e.g. a
+ * Fortran rank's generator after spring_sfmt_init and its own draws). */
+int dqmc_gpu_get_rng(dqmc_handle* h, int chain, int32_t* state);
+int dqmc_gpu_set_rng(dqmc_handle* h, int chain, const int32_t* state);
 
 /* Diagnostics: batched complex GEMM C = op(A) op(B) + beta C on per-chain
  * N x N work matrices, and a QR factorisation (R, Q, log det Q) of one; used

@@ -27,6 +27,15 @@ DQ_DEV double2* chain_mat(const ChainDev& c, int id) {
     return c.W[id - MAT_W0];
 }
 
+// Record a numerical failure of chain c (one thread calls it): the chain's
+// sticky stats[ST_INFO] and the handle's fail word.  The reference stops the
+// run at these points (lib/s_matrix.f90:1264-1267, dqmc_ft_sweep_b0.f90:188-194);
+// the library reports them to the host instead.
+DQ_DEV void chain_raise(const ChainDev& c, int code) {
+    c.stats[ST_INFO] = (double)((int)c.stats[ST_INFO] | code);
+    if (c.fail) atomicOr(c.fail, code);
+}
+
 // Radix-2 DFT of a length-n line held in registers (n a power of two, fully
 // unrolled).  tw[k] = exp(-2 pi i k / n); sign -1 forward, +1 backward.
 template <int n>

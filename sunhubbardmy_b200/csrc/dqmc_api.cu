@@ -884,6 +884,13 @@ struct dqmc_handle {
     double* d_u = nullptr;       // [nch][2]
     double* d_S = nullptr;       // [nch][2]
     uint64_t blk_rng = 0x9e3779b97f4a7c15ULL;
+    // numerical-failure reporting: the device word the kernels raise DQ_FAIL_*
+    // codes into, the control words they read (wrap-error tolerance), and the
+    // host-side re-stabilisation policy and count
+    int* d_fail = nullptr;
+    double* d_ctl = nullptr;
+    int restab = 0;
+    double n_restab = 0.0;
 };
 
 // Host <-> device copies of the entry points, ordered on the library's stream:
@@ -1000,6 +1007,9 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
     cudaEventCreate(&h->ev0);
     cudaEventCreate(&h->ev1);
     h->nch = n_chains;
+    h->d_fail = (int*)dalloc(h, 16);
+    h->d_ctl = (double*)dalloc(h, 4 * sizeof(double));
+    if (!h->d_fail || !h->d_ctl) { dqmc_gpu_destroy(h); return fail(DQMC_ENOMEM, "device allocation failed"); }
     int nst = h->nst, lt = h->ltrot;
     h->d_slotmap = (int*)dalloc(h, sizeof(int) * (nst + 2));
     if (h->models[0]->p.ltau) h->d_slotmap_b = (int*)dalloc(h, sizeof(int) * (nst + 2));
@@ -1082,6 +1092,8 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
         d.bins = (double2*)dalloc(h, (size_t)(10 + 20 * m->lq + 4) * z);
         d.stats = (double*)dalloc(h, ST_COUNT * sizeof(double));
         d.slotmap = h->d_slotmap;
+        d.fail = h->d_fail;
+        d.ctl = h->d_ctl;
         if (!d.G || !d.Gnew || !d.W[5] || (!proj && (!d.U || !d.V || !d.D)) || !d.rnd || !d.stats || !d.bins ||
             (m->p.rv != 0.0 && !d.vconf)) {
             dqmc_gpu_destroy(h);
@@ -1570,8 +1582,7 @@ static void enqueue_proj_0b(dqmc_handle* h, int lupdate, int lmeasure) {
     pflush(h, pp);
 }
 
-extern "C" int dqmc_gpu_sweep_start(dqmc_handle* h) {
-    if (!h) return fail(DQMC_EINVAL, "null handle");
+static int sweep_start_impl(dqmc_handle* h) {
     h->after_b0 = 0;
     if (h->proj) return proj_sweep_start(h);
     const HostModel& m = *h->models[0];
@@ -1591,6 +1602,69 @@ extern "C" int dqmc_gpu_sweep_start(dqmc_handle* h) {
     CK(cudaStreamSynchronize(h->st));
     CK(cudaGetLastError());
     h->started = 1;
+    return DQMC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// numerical-failure status.  The kernels raise DQ_FAIL_* codes into the
+// handle's fail word (and each chain's stats[ST_INFO]); every sweep entry point
+// clears the word before its launches and reads it after them.  The reference
+// stops the run at these points (lib/s_matrix.f90:1264-1267,
+// src/dqmc_ft_core/dqmc_ft_sweep_b0.f90:188-194); the library returns
+// DQMC_ENUMERIC (singular or non-finite Green's function) or DQMC_EWRAP (wrap
+// error above the caller's tolerance) instead, or, with re-stabilisation on,
+// rebuilds the UDV stack and G of every chain from its HS field
+// (dqmc_ft_sweep_start_0b / dqmc_proj_sweep_start_0b) and goes on.
+// ---------------------------------------------------------------------------
+static void clear_fail(dqmc_handle* h) { cudaMemsetAsync(h->d_fail, 0, sizeof(int), h->st); }
+
+static int report_fail(dqmc_handle* h, int f) {
+    std::string msg = (f & (DQ_FAIL_SINGULAR | DQ_FAIL_NONFINITE))
+                          ? "numerical failure (singular or non-finite Green's function)"
+                          : "wrap error above the tolerance";
+    msg += ", code " + std::to_string(f) + "; chains:";
+    int listed = 0;
+    for (int c = 0; c < h->nch && listed < 16; ++c) {
+        double info = 0.0;
+        if (copy_sync(h->st, &info, h->chains[c].dev.stats + ST_INFO, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+            break;
+        if (info != 0.0) { msg += " " + std::to_string(c) + " (" + std::to_string((int)info) + ")"; ++listed; }
+    }
+    return fail((f & (DQ_FAIL_SINGULAR | DQ_FAIL_NONFINITE)) ? DQMC_ENUMERIC : DQMC_EWRAP, msg);
+}
+
+// end of a sweep entry point: wait, then read the fail word.  at_beta: the
+// call left the chains at tau = beta with the stack of a 0b sweep, the state
+// sweep_start rebuilds, so re-stabilisation applies.
+static int finish_checked(dqmc_handle* h, int at_beta) {
+    CK(cudaStreamSynchronize(h->st));
+    CK(cudaGetLastError());
+    int f = 0;
+    CK(copy_sync(h->st, &f, h->d_fail, sizeof(int), cudaMemcpyDeviceToHost));
+    if (!f) return DQMC_OK;
+    if (h->restab && at_beta) {
+        clear_fail(h);
+        int rc = sweep_start_impl(h); if (rc) return rc;
+        h->n_restab += 1.0;
+        CK(copy_sync(h->st, &f, h->d_fail, sizeof(int), cudaMemcpyDeviceToHost));
+        if (!f) return DQMC_OK;
+    }
+    return report_fail(h, f);
+}
+
+extern "C" int dqmc_gpu_sweep_start(dqmc_handle* h) {
+    if (!h) return fail(DQMC_EINVAL, "null handle");
+    clear_fail(h);
+    int rc = sweep_start_impl(h); if (rc) return rc;
+    return finish_checked(h, 0);
+}
+
+extern "C" int dqmc_gpu_set_checks(dqmc_handle* h, double wrap_tol, int restabilize) {
+    if (!h) return fail(DQMC_EINVAL, "null handle");
+    if (!(wrap_tol >= 0.0)) return fail(DQMC_EINVAL, "wrap_tol must be >= 0");
+    double ctl[4] = {wrap_tol, 0.0, 0.0, 0.0};
+    CK(copy_sync(h->st, h->d_ctl, ctl, sizeof(ctl), cudaMemcpyHostToDevice));
+    h->restab = restabilize != 0;
     return DQMC_OK;
 }
 
@@ -1711,10 +1785,9 @@ extern "C" int dqmc_gpu_sweep_dyn(dqmc_handle* h) {
     if (h->proj) return fail(DQMC_ESTATE, "on the projective path the unequal-time pass runs inside the measured 0b sweep");
     if (!h->models[0]->p.ltau) return fail(DQMC_ESTATE, "the unequal-time pass needs ltau = 1");
     if (!h->after_b0) return fail(DQMC_ESTATE, "the unequal-time pass follows a b0 sweep (it needs the b0 sweep's left factors)");
+    clear_fail(h);
     enqueue_dyn(h);
-    CK(cudaStreamSynchronize(h->st));
-    CK(cudaGetLastError());
-    return DQMC_OK;
+    return finish_checked(h, 0);
 }
 
 extern "C" int dqmc_gpu_get_dyn_bins(dqmc_handle* h, int chain, double* out) {
@@ -1741,23 +1814,21 @@ extern "C" int dqmc_gpu_get_dyn_mats(dqmc_handle* h, int chain, double* g00, dou
 extern "C" int dqmc_gpu_sweep_b0(dqmc_handle* h, int lupdate, int lmeasure) {
     if (!h) return fail(DQMC_EINVAL, "null handle");
     if (!h->started) return fail(DQMC_ESTATE, "sweep before sweep_start");
+    clear_fail(h);
     if (h->proj) enqueue_proj_b0(h, lupdate, lmeasure);
     else enqueue_b0(h, lupdate, lmeasure);
     h->after_b0 = 1;
-    CK(cudaStreamSynchronize(h->st));
-    CK(cudaGetLastError());
-    return DQMC_OK;
+    return finish_checked(h, 0);
 }
 
 extern "C" int dqmc_gpu_sweep_0b(dqmc_handle* h, int lupdate, int lmeasure) {
     if (!h) return fail(DQMC_EINVAL, "null handle");
     if (!h->started) return fail(DQMC_ESTATE, "sweep before sweep_start");
+    clear_fail(h);
     if (h->proj) enqueue_proj_0b(h, lupdate, lmeasure);
     else enqueue_0b(h, lupdate, lmeasure);
     h->after_b0 = 0;
-    CK(cudaStreamSynchronize(h->st));
-    CK(cudaGetLastError());
-    return DQMC_OK;
+    return finish_checked(h, 1);
 }
 
 // the captured sweep (b0 + 0b) of dqmc_gpu_sweeps, rebuilt when lmeasure or
@@ -1803,6 +1874,7 @@ extern "C" int dqmc_gpu_sweeps(dqmc_handle* h, int n, int lmeasure) {
     if (n <= 0) return DQMC_OK;
     int rc = ensure_sweep_graph(h, lmeasure); if (rc) return rc;
     h->after_b0 = 0;
+    clear_fail(h);
     CK(cudaEventRecord(h->ev0, h->st));
     for (int i = 0; i < n; ++i) CK(cudaGraphLaunch(h->sweep_graph, h->st));
     CK(cudaEventRecord(h->ev1, h->st));
@@ -1811,7 +1883,7 @@ extern "C" int dqmc_gpu_sweeps(dqmc_handle* h, int n, int lmeasure) {
     float ms = 0;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
     h->last_ms = ms / n;
-    return DQMC_OK;
+    return finish_checked(h, 1);
 }
 
 // n sweeps of several handles at once: each handle's sweep graph on its own
@@ -1831,6 +1903,7 @@ extern "C" int dqmc_gpu_sweeps_multi(dqmc_handle* const* hs, int nh, int n, int 
     for (int k = 0; k < nh; ++k) {
         int rc = ensure_sweep_graph(hs[k], lmeasure); if (rc) return rc;
         hs[k]->after_b0 = 0;
+        clear_fail(hs[k]);
     }
     dqmc_handle* h0 = hs[0];
     cudaEvent_t fork = nullptr, join[16] = {};
@@ -1861,6 +1934,9 @@ extern "C" int dqmc_gpu_sweeps_multi(dqmc_handle* const* hs, int nh, int n, int 
     if (err != cudaSuccess) return fail(DQMC_ECUDA, std::string("sweeps_multi: ") + cudaGetErrorString(err));
     for (int k = 0; k < nh; ++k) hs[k]->last_ms = ms / n;
     if (ms_out) *ms_out = ms / n;
+    for (int k = 0; k < nh; ++k) {
+        int rc = finish_checked(hs[k], 1); if (rc) return rc;
+    }
     return DQMC_OK;
 }
 
@@ -1938,6 +2014,41 @@ extern "C" int dqmc_gpu_set_green(dqmc_handle* h, int chain, const double* g) {
     const ChainDev& d = h->chains[chain].dev;
     CK(copy_sync(h->st, d.G, g, (size_t)d.N * d.N * sizeof(double2), cudaMemcpyHostToDevice));
     h->started = 1;
+    return DQMC_OK;
+}
+
+// Ust(n), Dst(n), Vst(n), logdetQst(n) of the finite-temperature UDV stack
+// (src/dqmc_ft_core.f90:11-19), logical index n = 0..nst, through the slot map
+static int stack_slot(dqmc_handle* h, int chain, int n, int* slot) {
+    int rc = chk_chain(h, chain); if (rc) return rc;
+    if (h->proj) return fail(DQMC_ESTATE, "the projective path has no UDV stack");
+    if (n < 0 || n > h->nst) return fail(DQMC_EINVAL, "stack index 0..nst");
+    CK(copy_sync(h->st, slot, h->d_slotmap + n, sizeof(int), cudaMemcpyDeviceToHost));
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_get_stack(dqmc_handle* h, int chain, int n, double* u, double* d, double* v, double* logdetq) {
+    int slot = 0;
+    int rc = stack_slot(h, chain, n, &slot); if (rc) return rc;
+    const ChainDev& c = h->chains[chain].dev;
+    const size_t NN = (size_t)c.N * c.N;
+    if (u) CK(copy_sync(h->st, u, c.U + slot * NN, NN * sizeof(double2), cudaMemcpyDeviceToHost));
+    if (v) CK(copy_sync(h->st, v, c.V + slot * NN, NN * sizeof(double2), cudaMemcpyDeviceToHost));
+    if (d) CK(copy_sync(h->st, d, c.D + (size_t)slot * c.N, c.N * sizeof(double), cudaMemcpyDeviceToHost));
+    if (logdetq) CK(copy_sync(h->st, logdetq, c.logdetQ + slot, sizeof(double2), cudaMemcpyDeviceToHost));
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_set_stack(dqmc_handle* h, int chain, int n, const double* u, const double* d, const double* v,
+                                  const double* logdetq) {
+    int slot = 0;
+    int rc = stack_slot(h, chain, n, &slot); if (rc) return rc;
+    const ChainDev& c = h->chains[chain].dev;
+    const size_t NN = (size_t)c.N * c.N;
+    if (u) CK(copy_sync(h->st, c.U + slot * NN, u, NN * sizeof(double2), cudaMemcpyHostToDevice));
+    if (v) CK(copy_sync(h->st, c.V + slot * NN, v, NN * sizeof(double2), cudaMemcpyHostToDevice));
+    if (d) CK(copy_sync(h->st, c.D + (size_t)slot * c.N, d, c.N * sizeof(double), cudaMemcpyHostToDevice));
+    if (logdetq) CK(copy_sync(h->st, c.logdetQ + slot, logdetq, sizeof(double2), cudaMemcpyHostToDevice));
     return DQMC_OK;
 }
 
@@ -2027,6 +2138,8 @@ extern "C" int dqmc_gpu_get_diag(dqmc_handle* h, int chain, dqmc_diag* out) {
     out->blk_err_learned = st[ST_BLK_ERR1]; out->blk_err_zero = st[ST_BLK_ERR0];
     out->max_dyn_error = st[ST_MAX_DYN];
     out->dyn_log10_sum = st[ST_DYN_LOG10]; out->dyn_count = st[ST_DYN_COUNT];
+    out->info = st[ST_INFO];
+    out->restabilized = h->n_restab;
     return DQMC_OK;
 }
 
@@ -2040,8 +2153,10 @@ extern "C" int dqmc_gpu_reset_diag(dqmc_handle* h) {
         st[ST_BLK_PROP] = st[ST_BLK_S1] = st[ST_BLK_ACC] = st[ST_BLK_SUMLR] = 0.0;
         st[ST_BLK_ERR1] = st[ST_BLK_ERR0] = 0.0;
         st[ST_MAX_DYN] = st[ST_DYN_LOG10] = st[ST_DYN_COUNT] = 0.0;
+        st[ST_INFO] = 0.0;
         CK(copy_sync(h->st, h->chains[c].dev.stats, st, sizeof(st), cudaMemcpyHostToDevice));
     }
+    h->n_restab = 0.0;
     return DQMC_OK;
 }
 
@@ -2049,6 +2164,26 @@ extern "C" int dqmc_gpu_set_phase(dqmc_handle* h, int chain, double re, double i
     int rc = chk_chain(h, chain); if (rc) return rc;
     double v[2] = {re, im};
     CK(copy_sync(h->st, h->chains[chain].dev.stats + ST_PHASE_RE, v, sizeof(v), cudaMemcpyHostToDevice));
+    return DQMC_OK;
+}
+
+// SFMT-19937 state of one chain in the reference's representation
+// (lib/m_spring.f90:66-71): pt32(0:623), the 32-bit view of the 128-bit state
+// array, then the read index idx (624 = the next draw regenerates the block).
+// The device generator keeps exactly these 625 words, so a mid-run state
+// handed over by a Fortran caller continues its stream.
+extern "C" int dqmc_gpu_get_rng(dqmc_handle* h, int chain, int32_t* state) {
+    int rc = chk_chain(h, chain); if (rc) return rc;
+    if (!state) return fail(DQMC_EINVAL, "null state");
+    CK(copy_sync(h->st, state, h->chains[chain].dev.sfmt, 625 * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_set_rng(dqmc_handle* h, int chain, const int32_t* state) {
+    int rc = chk_chain(h, chain); if (rc) return rc;
+    if (!state) return fail(DQMC_EINVAL, "null state");
+    if (state[624] < 0 || state[624] > 624) return fail(DQMC_EINVAL, "SFMT read index outside 0..624");
+    CK(copy_sync(h->st, h->chains[chain].dev.sfmt, state, 625 * sizeof(uint32_t), cudaMemcpyHostToDevice));
     return DQMC_OK;
 }
 
@@ -2325,11 +2460,10 @@ extern "C" int dqmc_gpu_proj_update(dqmc_handle* h, int nt, int nf) {
 extern "C" int dqmc_gpu_proj_green(dqmc_handle* h) {
     if (!h) return fail(DQMC_EINVAL, "null handle");
     if (!h->proj) return fail(DQMC_ESTATE, "not a projective handle (params.proj = 0)");
+    clear_fail(h);
     launch_proj_ulr(h->d_chains, h->nch, PMAT_ULRINV, 0, 0, -1, h->st);
     launch_proj_green(h->d_chains, h->nch, PMAT_ULRINV, PMAT_G, h->ctas_per_chain, h->st);
-    CK(cudaStreamSynchronize(h->st));
-    CK(cudaGetLastError());
-    return DQMC_OK;
+    return finish_checked(h, 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -2750,6 +2884,7 @@ extern "C" int dqmc_gpu_sweep_learned(dqmc_handle* h, dqmc_nn* nn, int n, int lu
     if (m.p.rhub == 0.0) return fail(DQMC_EINVAL, "no HS field (rhub == 0)");
     int rc = enable_blocks(h); if (rc) return rc;
     if (seed) h->blk_rng = seed;
+    clear_fail(h);
     cudaEvent_t e0 = h->ev0, e1 = h->ev1;
     CK(cudaEventRecord(e0, h->st));
     for (int i = 0; i < n; ++i) {
@@ -2763,5 +2898,5 @@ extern "C" int dqmc_gpu_sweep_learned(dqmc_handle* h, dqmc_nn* nn, int n, int lu
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     h->last_ms = n > 0 ? ms / n : 0.0;
-    return DQMC_OK;
+    return finish_checked(h, 1);
 }

@@ -102,6 +102,18 @@ struct ChainDev {
     double2* Gb;
     double2* URs;              // projective unequal-time pass: the sweep's UR and UL^T, kept aside
     double2* ULTs;
+    // numerical-failure reporting (shared by the handle's chains): fail[0] is
+    // the OR of the DQ_FAIL_* codes raised since the host last cleared it;
+    // ctl[0] is the wrap-error tolerance (0 = none)
+    int* fail;
+    const double* ctl;
+};
+
+// numerical-failure codes (stats[ST_INFO] per chain, fail[0] per handle)
+enum {
+    DQ_FAIL_SINGULAR = 1,      // zero or non-finite pivot: QR of the UDV step, of M in green_equaltime, of UL UR
+    DQ_FAIL_NONFINITE = 2,     // the freshly computed Green's function is not finite
+    DQ_FAIL_WRAP = 4           // wrap error above the tolerance ctl[0] (or not finite while a tolerance is set)
 };
 
 // indices into ChainDev::stats
@@ -115,6 +127,7 @@ enum {
     ST_MAX_DYN,                // xmax_dyn of the projective unequal-time pass
     ST_DYN_LOG10,              // its sum of log10 over the checks (avglog10dynerror) ...
     ST_DYN_COUNT,              // ... and the number of checks (logdyncount)
+    ST_GINFO,                  // DQ_FAIL_SINGULAR of the latest Green's-function computation (overwritten by each)
     ST_COUNT = 40
 };
 

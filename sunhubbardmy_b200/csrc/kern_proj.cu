@@ -110,6 +110,14 @@ __global__ void __launch_bounds__(256) k_proj_ulr(const ChainDev* __restrict__ c
     zgemm_cta<GemmBig>(g, 0, 1, buf);
     cta_qr64(M, ne, sc, buf, buf, &S->L);
     double2 ld = cmk(0, 0);
+    int bad = 0;
+    for (int i = tid; i < ne; i += nth) {
+        const double r = M[MIDX(i, i, ne)].x;
+        bad |= (r == 0.0 || !isfinite(r));
+    }
+    // a zero or non-finite pivot of UL UR: zgetrf's info > 0 in s_inv_logdet_lu_z
+    bad = __syncthreads_or(bad);
+    if (bad && tid == 0) chain_raise(c, DQ_FAIL_SINGULAR);
     if (logdet) {
         ld = cta_logdet_q(sc.tau, ne, S->red);
         double2 lr = cmk(0, 0);
@@ -129,6 +137,7 @@ __global__ void __launch_bounds__(256) k_proj_ulr(const ChainDev* __restrict__ c
         double w = c.logwDV[ia] + (ib >= 0 ? c.logwDV[ib] : 0.0);
         c.stats[ST_LOGDETM_RE] = ld.x + w;
         c.stats[ST_LOGDETM_IM] = ld.y;
+        c.stats[ST_GINFO] = (bad || !isfinite(ld.x + w) || !isfinite(ld.y)) ? (double)DQ_FAIL_SINGULAR : 0.0;
     }
 }
 

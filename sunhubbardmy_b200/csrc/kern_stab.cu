@@ -86,7 +86,14 @@ __global__ void __launch_bounds__(256) k_stab(const ChainDev* __restrict__ chain
     }
     __syncthreads();
     cta_qr64(W2, N, sc, buf, buf, &S->L);
-    for (int i = tid; i < N; i += nth) Ddst[i] = W2[MIDX(i, i, N)].x;
+    int bad = 0;
+    for (int i = tid; i < N; i += nth) {
+        const double d = W2[MIDX(i, i, N)].x;
+        Ddst[i] = d;
+        bad |= (d == 0.0 || !isfinite(d));
+    }
+    // a zero or non-finite R_ii (the zgeqp3 / zgeqrf step of the reference)
+    if (__syncthreads_or(bad) && tid == 0) chain_raise(c, DQ_FAIL_SINGULAR);
     double2 ldq = cta_logdet_q(sc.tau, N, S->red);
     if (tid == 0) c.logdetQ[dst] = ldq;
     __syncthreads();
@@ -178,10 +185,14 @@ __global__ void __launch_bounds__(256, 2) k_green(const ChainDev* __restrict__ c
     cta_qr64(M, N, sc, buf, buf, &S->L);
     double2 ldm = cta_logdet_q(sc.tau, N, S->red);
     double2 lr = cmk(0, 0);
+    int bad = 0;
     for (int i = tid; i < N; i += nth) {
         double r = M[MIDX(i, i, N)].x;
+        bad |= (r == 0.0 || !isfinite(r));
         lr = cadd(lr, cmk(log(fabs(r)), r < 0.0 ? M_PI : 0.0));
     }
+    // a zero or non-finite pivot of M: zgetrf's info > 0 in s_inv_logdet_lu_z
+    bad = __syncthreads_or(bad);
     lr = block_csum(lr, S->red);
     ldm = cadd(ldm, lr);
     double2* X = (mode == 0) ? Z : c.Gnew;
@@ -211,6 +222,7 @@ __global__ void __launch_bounds__(256, 2) k_green(const ChainDev* __restrict__ c
         if (mode == 0) lw = csub(lw, c.logdetQ[nl]);
         c.stats[ST_LOGDETM_RE] = lw.x;
         c.stats[ST_LOGDETM_IM] = lw.y;
+        c.stats[ST_GINFO] = (bad || !isfinite(lw.x) || !isfinite(lw.y)) ? (double)DQ_FAIL_SINGULAR : 0.0;
     }
 }
 
@@ -277,10 +289,13 @@ __global__ void __launch_bounds__(256, 2) k_green_tau(const ChainDev* __restrict
     cta_qr64(W0, N, sc, buf, buf, &S->L);
     double2 ldm = cta_logdet_q(sc.tau, N, S->red);
     double2 lr = cmk(0, 0);
+    int bad = 0;
     for (int i = tid; i < N; i += nth) {
         const double r = W0[MIDX(i, i, N)].x;
+        bad |= (r == 0.0 || !isfinite(r));
         lr = cadd(lr, cmk(log(fabs(r)), r < 0.0 ? M_PI : 0.0));
     }
+    bad = __syncthreads_or(bad);
     lr = block_csum(lr, S->red);
     ldm = cadd(ldm, lr);
     // X = M^-1 drmax^-1 UR^H (W2), Y = M^-1 drmin VR (W3)
@@ -342,6 +357,7 @@ __global__ void __launch_bounds__(256, 2) k_green_tau(const ChainDev* __restrict
         lw = csub(lw, c.logdetQ[nl]);
         c.stats[ST_LOGDETM_RE] = lw.x;
         c.stats[ST_LOGDETM_IM] = lw.y;
+        c.stats[ST_GINFO] = (bad || !isfinite(lw.x) || !isfinite(lw.y)) ? (double)DQ_FAIL_SINGULAR : 0.0;
     }
 }
 
@@ -379,7 +395,13 @@ __global__ void k_dyn_init(const ChainDev* __restrict__ chains) {
     }
 }
 
-// s_compare_max_z + set_phase + replacement of G (dqmc_ft_sweep_b0.f90:145-194)
+// s_compare_max_z + set_phase + replacement of G (dqmc_ft_sweep_b0.f90:145-194).
+// Where the reference stops on info /= 0 (188-194), the fresh G is not taken:
+// a chain whose Green's function computation hit a singular pivot, or whose
+// fresh G is not finite, keeps its propagated G, phase and log weight, and the
+// failure is raised (chain_raise) for the host to report.  With a wrap-error
+// tolerance ctl[0] > 0, a recorded check above it (or not finite) raises
+// DQ_FAIL_WRAP; the fresh G is still taken then.
 __global__ void __launch_bounds__(256) k_wrap_check(const ChainDev* __restrict__ chains, int record) {
     __shared__ double red[64];
     const ChainDev c = chains[blockIdx.x];
@@ -387,11 +409,20 @@ __global__ void __launch_bounds__(256) k_wrap_check(const ChainDev* __restrict__
     const int N = c.N, tid = threadIdx.x, nth = blockDim.x;
     const size_t NN = (size_t)N * N;
     double mx = 0.0;
+    int nonfin = 0, wnan = 0;
     for (size_t e = tid; e < NN; e += nth) {
-        double2 d = csub(c.Gnew[e], c.G[e]);
-        mx = fmax(mx, cabsd(d));
-        c.G[e] = c.Gnew[e];
+        const double2 gn = c.Gnew[e];
+        nonfin |= !(isfinite(gn.x) && isfinite(gn.y));
+        const double a = cabsd(csub(gn, c.G[e]));
+        wnan |= !isfinite(a);
+        mx = fmax(mx, a);
     }
+    nonfin = __syncthreads_or(nonfin);
+    wnan = __syncthreads_or(wnan);
+    const int ginfo = (int)c.stats[ST_GINFO];
+    const bool keep = nonfin || (ginfo & DQ_FAIL_SINGULAR);
+    if (!keep)
+        for (size_t e = tid; e < NN; e += nth) c.G[e] = c.Gnew[e];
     mx = block_max(mx, red);
     double ang = 0.0;
     if (md.phase_on) {
@@ -402,6 +433,10 @@ __global__ void __launch_bounds__(256) k_wrap_check(const ChainDev* __restrict__
     if (tid == 0) {
         double2 lw = cmk(c.stats[ST_LOGDETM_RE], c.stats[ST_LOGDETM_IM]);
         double2 ph = cexpi(md.nflr * lw.y + ang);
+        int code = (ginfo & DQ_FAIL_SINGULAR) | (nonfin ? DQ_FAIL_NONFINITE : 0);
+        const double tol = c.ctl ? c.ctl[0] : 0.0;
+        if (record && tol > 0.0 && (wnan || mx > tol)) code |= DQ_FAIL_WRAP;
+        if (code) chain_raise(c, code);
         if (record) {
             double2 old = cmk(c.stats[ST_PHASE_RE], c.stats[ST_PHASE_IM]);
             double pd = cabsd(csub(old, ph));
@@ -412,10 +447,12 @@ __global__ void __launch_bounds__(256) k_wrap_check(const ChainDev* __restrict__
             c.stats[ST_AVGEXPPD] += exp(pd);
             c.stats[ST_LAST_WRAP] = mx;
         }
-        c.stats[ST_PHASE_RE] = ph.x;
-        c.stats[ST_PHASE_IM] = ph.y;
-        c.stats[ST_LOGW_RE] = lw.x;
-        c.stats[ST_LOGW_IM] = lw.y;
+        if (!keep) {
+            c.stats[ST_PHASE_RE] = ph.x;
+            c.stats[ST_PHASE_IM] = ph.y;
+            c.stats[ST_LOGW_RE] = lw.x;
+            c.stats[ST_LOGW_IM] = lw.y;
+        }
     }
 }
 

@@ -26,8 +26,17 @@ def lib_path() -> str:
     return os.path.join(_HERE, "_lib", "libdqmc_gpu.so")
 
 
+# return codes of include/dqmc_gpu.h
+EINVAL, ECUDA, ENOMEM, ESTATE, ENUMERIC, EWRAP = -1, -2, -3, -4, -5, -6
+FAIL_SINGULAR, FAIL_NONFINITE, FAIL_WRAP = 1, 2, 4
+
+
 class DqmcError(RuntimeError):
-    pass
+    """A failed library call; ``code`` is its DQMC_E* return value."""
+
+    def __init__(self, msg: str, code: int = 0):
+        super().__init__(msg)
+        self.code = code
 
 
 class DqmcParams(C.Structure):
@@ -88,7 +97,8 @@ class DqmcDiag(C.Structure):
         "phase_re", "phase_im", "logweight_re", "logweight_im", "max_wrap_error", "max_phasediff",
         "avglog10error_sum", "logcount", "avgexpphasediff_sum", "accepted", "proposed", "nobs",
         "accepted_v", "proposed_v", "blk_proposed", "blk_stage1", "blk_accepted", "blk_sum_logratio",
-        "blk_err_learned", "blk_err_zero", "max_dyn_error", "dyn_log10_sum", "dyn_count")]
+        "blk_err_learned", "blk_err_zero", "max_dyn_error", "dyn_log10_sum", "dyn_count", "info",
+        "restabilized")]
 
 
 _lib = None
@@ -107,6 +117,9 @@ SIGNATURES = {
     "dqmc_gpu_get_conf_all": (_i, [_vp, _vp]),
     "dqmc_gpu_get_green": (_i, [_vp, _i, _vp]),
     "dqmc_gpu_set_green": (_i, [_vp, _i, _vp]),
+    "dqmc_gpu_get_stack": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp]),
+    "dqmc_gpu_set_stack": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp]),
+    "dqmc_gpu_set_checks": (_i, [_vp, _d, _i]),
     "dqmc_gpu_sweep_start": (_i, [_vp]),
     "dqmc_gpu_sweep_b0": (_i, [_vp, _i, _i]),
     "dqmc_gpu_sweep_0b": (_i, [_vp, _i, _i]),
@@ -123,6 +136,8 @@ SIGNATURES = {
     "dqmc_gpu_measure": (_i, [_vp]),
     "dqmc_gpu_set_phase": (_i, [_vp, _i, _d, _d]),
     "dqmc_gpu_draw_u32": (_i, [_vp, _i, _i, _vp]),
+    "dqmc_gpu_get_rng": (_i, [_vp, _i, _vp]),
+    "dqmc_gpu_set_rng": (_i, [_vp, _i, _vp]),
     "dqmc_gpu_set_work": (_i, [_vp, _i, _i, _vp]),
     "dqmc_gpu_get_work": (_i, [_vp, _i, _i, _vp]),
     "dqmc_gpu_test_zgemm": (_i, [_vp, _i, _i, _i, _i, _i, _i, _i, _i, _d]),
@@ -188,7 +203,7 @@ def _last_error() -> str:
 
 def _check(rc: int, what: str) -> None:
     if rc != 0:
-        raise DqmcError(f"{what} failed ({rc}): {_last_error()}")
+        raise DqmcError(f"{what} failed ({rc}): {_last_error()}", rc)
 
 
 def _ptr(a: np.ndarray) -> C.c_void_p:
@@ -357,6 +372,48 @@ class Dqmc:
         a = np.asfortranarray(g, complex)
         _check(load_library().dqmc_gpu_set_green(self.h, c, _ptr(a)), "set_green")
 
+    def stack(self, n: int, c: int = 0):
+        """(Ust(n), Dst(n), Vst(n), logdetQst(n)) of one chain's UDV stack."""
+        N = self.ndim(c)
+        u = np.zeros((N, N), complex, order="F")
+        v = np.zeros((N, N), complex, order="F")
+        d = np.zeros(N)
+        ld = np.zeros(1, complex)
+        _check(load_library().dqmc_gpu_get_stack(self.h, c, int(n), _ptr(u), _ptr(d), _ptr(v), _ptr(ld)),
+               "get_stack")
+        return u, d, v, complex(ld[0])
+
+    def set_stack(self, n: int, u=None, d=None, v=None, logdetq=None, c: int = 0) -> None:
+        """Overwrite parts of stack entry n (None keeps a part)."""
+        keep = []
+
+        def arg(x, dtype, fortran=False):
+            if x is None:
+                return None
+            a = np.asfortranarray(x, dtype) if fortran else np.ascontiguousarray(x, dtype)
+            keep.append(a)
+            return _ptr(a)
+        ld = None if logdetq is None else np.array([logdetq], complex)
+        _check(load_library().dqmc_gpu_set_stack(self.h, c, int(n), arg(u, complex, True), arg(d, float),
+                                                 arg(v, complex, True), arg(ld, complex)), "set_stack")
+
+    def rng_state(self, c: int = 0) -> np.ndarray:
+        """SFMT state of chain c: 625 int32 words, pt32(0:623) then idx."""
+        out = np.zeros(625, np.int32)
+        _check(load_library().dqmc_gpu_get_rng(self.h, c, _ptr(out)), "get_rng")
+        return out
+
+    def set_rng_state(self, state: np.ndarray, c: int = 0) -> None:
+        a = np.ascontiguousarray(state, np.int32)
+        assert a.size == 625
+        _check(load_library().dqmc_gpu_set_rng(self.h, c, _ptr(a)), "set_rng")
+
+    def set_checks(self, wrap_tol: float = 0.0, restabilize: bool = False) -> None:
+        """Numerical checks of the sweep calls (dqmc_gpu_set_checks): a wrap
+        error above wrap_tol (> 0) raises DqmcError with code EWRAP; with
+        restabilize the stack and G are rebuilt from the HS field instead."""
+        _check(load_library().dqmc_gpu_set_checks(self.h, float(wrap_tol), int(restabilize)), "set_checks")
+
     def set_phase(self, z: complex, c: int = 0) -> None:
         _check(load_library().dqmc_gpu_set_phase(self.h, c, z.real, z.imag), "set_phase")
 
@@ -371,7 +428,8 @@ class Dqmc:
                     blk_proposed=d.blk_proposed, blk_stage1=d.blk_stage1, blk_accepted=d.blk_accepted,
                     blk_sum_logratio=d.blk_sum_logratio, blk_err_learned=d.blk_err_learned,
                     blk_err_zero=d.blk_err_zero, max_dyn_error=d.max_dyn_error,
-                    dyn_log10_sum=d.dyn_log10_sum, dyn_count=d.dyn_count)
+                    dyn_log10_sum=d.dyn_log10_sum, dyn_count=d.dyn_count, info=int(d.info),
+                    restabilized=int(d.restabilized))
 
     def energy_all(self) -> np.ndarray:
         """energy_bin(1:10) of every chain, shape (n_chains, 10) complex."""

@@ -76,7 +76,8 @@ def _fourier(gr: np.ndarray, zexpiqr: np.ndarray) -> np.ndarray:
 def equaltime_output(bins_per_chain, outdir: str = ".", zexpiqr: np.ndarray | None = None,
                      chain: bool = False) -> dict:
     """Reduce chain bins, normalise by n_chains*nobs and append to the
-    reference's files (energy.bin '(16e16.8)', n.bin, j.bin, b.bin, *_r.bin);
+    reference's files (energy.bin '(16e16.8)', n.bin, j.bin, b.bin, nnnn.bin,
+    Crmax.bin, *_r.bin);
     for the 1D chain energy.bin holds all ten energies ('(20e16.8)',
     equaltime_output1d.f90)."""
     n = len(bins_per_chain)
@@ -97,6 +98,11 @@ def equaltime_output(bins_per_chain, outdir: str = ".", zexpiqr: np.ndarray | No
         with open(os.path.join(outdir, name), "a") as f:
             z = red[key]
             f.write(f"{z.real:16.8e}{z.imag:16.8e}\n")
+    # znnnn and zCrmax: the reference appends them every bin, but their
+    # accumulation is commented out (equaltime_measure.f90:54-57), so they are 0
+    for name in ("nnnn.bin", "Crmax.bin"):
+        with open(os.path.join(outdir, name), "a") as f:
+            f.write(f"{0.0:16.8e}{0.0:16.8e}\n")
     for key in ("cpcm", "spsm", "nn", "pair_onsite", "jj", "bb", "pair_nn", "pair_sn"):
         with open(os.path.join(outdir, f"{key}_r.bin"), "a") as f:
             arr = np.asarray(red[key]).reshape(-1)
@@ -236,10 +242,26 @@ def wrap_error_print(f, diags, ltau: bool = False) -> None:
         f.write(f"--------------avglog10dynerror  = {ad:16.8f}\n" if dc else f"--------------avglog10dynerror  = {'NaN':>16}\n")
 
 
-def dqmc_end_print(f, diags, total_s: float, profile: dict | None = None, date: str = "") -> None:
+def update_flavour(p) -> str:
+    """The -DTIMING name of the update of a parameter set: ft_ / proj_ and
+    fast / delay / submatrix, as dqmc_end prints it (src/dqmc_util.f90:316-355)."""
+    g = p if isinstance(p, dict) else p.as_dict()
+    kind = {0: "fast", 1: "delay", 2: "submatrix"}[int(g.get("update", 1))]
+    return f"{'proj' if g.get('proj', 0) else 'ft'}_{kind}_update"
+
+
+def dqmc_end_print(f, diags, total_s: float, profile: dict | None = None, date: str = "", params=None,
+                   gfunc_s: float = 0.0, dyn_s: float = 0.0, output_s: float = 0.0) -> None:
     """dqmc_end (src/dqmc_util.f90:287-369): acceptance of the U (and t-V bond)
     field over all chains, total time and, given a sweep profile
-    (Dqmc.sweep_profile: {kind: (ms, groups)}), the -DTIMING breakdown."""
+    (Dqmc.sweep_profile: {kind: (ms, groups)}), the -DTIMING breakdown with the
+    reference's line names, the update named by its flavour (params: the
+    handle's parameter set; default ft_delay_update).  gfunc_s is the part of
+    the update spent updating G (the reference's timecalculation(18..21)); the
+    ratio line is the rest, so the two lines add up to the update time as in
+    the reference.  The propagation kernels apply the kinetic and the HS
+    factors of a slice in one pass, so that pass is charged to H0 and the HI
+    lines read zero."""
     def acc(a, p):
         return sum(d[a] for d in diags) / max(1.0, sum(d[p] for d in diags))
     if sum(d.get("proposed_v", 0.0) for d in diags) > 0:
@@ -251,12 +273,27 @@ def dqmc_end_print(f, diags, total_s: float, profile: dict | None = None, date: 
     f.write(f" >>> Happy ending at {date}\n\n")
     if profile:
         s = {k: v[0] * 1e-3 for k, v in profile.items()}
-        tot = sum(s.values())
-        rows = [("The_time_of_propagating:        ", s["prop_left"] + s["prop_right"] + s["bprod"]),
-                ("The_time_of_ft_delay_update:    ", s["update"]),
-                ("The_time_of_stabilization:      ", s["stab"] + s["green"] + s["other"]),
-                ("The_time_of_measuring_equaltime:", s["measure"])]
-        f.write(f"The_time_of_sweep_in_total:     {tot:10.3f}s\n")
-        for name, t in rows:
-            f.write(f"{name}{t:10.3f}s = {100.0 * t / tot if tot else 0.0:6.2f}%\n")
+        inside = sum(s.values())
+        tot = inside + output_s
+        pct = (lambda t: 100.0 * t / tot if tot else 0.0)
+        fl = update_flavour(params) if params is not None else "ft_delay_update"
+        upd = s["update"]
+        prop = s["prop_left"] + s["prop_right"] + s["bprod"]
+        w = f.write
+        w(f"The_time_of_sweep_in_total:     {tot:10.3f}s\n")
+        w(f"The_time_of_sweep_inside:       {inside:10.3f}s = {pct(inside):6.2f}%\n")
+        w(f"The_time_of_propagating:        {prop:10.3f}s = {pct(prop):6.2f}%\n")
+        w(f"The_time_of_{fl}:".ljust(32) + f"{upd:10.3f}s = {pct(upd):6.2f}%\n")
+        if not fl.endswith("fast_update"):
+            w(f"The_time_of_update_gfunc_{fl}:  {gfunc_s:10.3f}s\n")
+            w(f"The_time_of_update_ratio_{fl}:  {upd - gfunc_s:10.3f}s\n")
+        stab = s["stab"] + s["green"] + s["other"]
+        w(f"The_time_of_stabilization:      {stab:10.3f}s = {pct(stab):6.2f}%\n")
+        w(f"The_time_of_measuring_equaltime:{s['measure']:10.3f}s = {pct(s['measure']):6.2f}%\n")
+        w(f"The_time_of_measuring_dynamic:  {dyn_s:10.3f}s = {pct(dyn_s):6.2f}%\n")
+        w(f"The_time_of_outputing_bins      {output_s:10.3f}s = {pct(output_s):6.2f}%\n")
+        w(f"The_time_of_H0_left:            {s['prop_left']:10.3f}s\n")
+        w(f"The_time_of_H0_right:           {s['prop_right']:10.3f}s\n")
+        w(f"The_time_of_HI_left:            {0.0:10.3f}s\n")
+        w(f"The_time_of_HI_right:           {0.0:10.3f}s\n")
     f.write(" The simulation done !!! \n")

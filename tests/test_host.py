@@ -133,6 +133,10 @@ def test_equaltime_output_normalisation(tmp_path):
     assert len(line.split()) == 16
     sb.equaltime_output(bins, str(tmp_path / "chain"), chain=True)      # equaltime_output1d: all ten
     assert len((tmp_path / "chain" / "energy.bin").read_text().split()) == 20
+    # every file equaltime_output appends, nnnn.bin and Crmax.bin (zeros) included
+    for name in ("n.bin", "j.bin", "b.bin", "nnnn.bin", "Crmax.bin", "cpcm_r.bin", "pair_sn_r.bin"):
+        assert (tmp_path / name).exists(), name
+    assert (tmp_path / "nnnn.bin").read_text() == f"{0.0:16.8e}{0.0:16.8e}\n"
 
 
 def _gloo_worker(rank, world, port, q):
@@ -278,6 +282,51 @@ def test_dqmc_out_writers():
     assert "The_time_of_ft_delay_update:         0.100s =  50.00%\n" in out
 
 
+# the three greps of the reference's timing analysis
+# (examples/run_square_time/ana_time.sh:24-26), run by bash on a dqmc.out
+ANA_TIME = r"""
+time=$(grep -E "The_time_of_update_ratio.*_update"  dqmc.out|awk -F: '{printf "%.2f\n", $2}')
+time1=$(grep -E "The_time_of_update_gfunc.*_update"  dqmc.out|awk -F: '{printf "%.2f\n", $2}')
+time3=$(grep 'The_time_of_sweep_in_total'  dqmc.out|awk -F: '{printf "%.2f\n", $2}')
+echo ${time} ${time1} ${time3}
+"""
+
+
+@pytest.mark.parametrize("update,proj,name", [(1, 0, "ft_delay_update"), (2, 0, "ft_submatrix_update"),
+                                              (2, 1, "proj_submatrix_update"), (1, 1, "proj_delay_update")])
+def test_timing_lines_feed_the_reference_analysis(tmp_path, update, proj, name):
+    """dqmc_end's -DTIMING lines carry the update flavour in their names, so
+    the reference's ana_time.sh reads the ratio, gfunc and total times."""
+    import subprocess
+    import sunhubbardmy_b200 as sb
+    from sunhubbardmy_b200.io import dqmc_end_print, update_flavour
+    kw = dict(lattice=1, l1=4, l2=4, beta=2.0, dtau=0.1, rhub=4.0, update=update, nwrap=5)
+    if proj:
+        kw.update(lattice=2, l1=3, l2=3, rhub=0.0, rv=1.0, nflr=1, proj=1)
+    p = sb.DqmcParams.make(**kw)
+    assert update_flavour(p) == name
+    prof = {"update": (1234.0, 1), "stab": (500.0, 1), "green": (300.0, 1), "prop_left": (100.0, 1),
+            "measure": (50.0, 1), "prop_right": (50.0, 1), "bprod": (10.0, 1), "other": (6.0, 1)}
+    with open(tmp_path / "dqmc.out", "w") as f:
+        dqmc_end_print(f, [dict(accepted=1.0, proposed=2.0)], 3.0, prof, params=p, gfunc_s=0.634)
+    out = subprocess.run(["bash", "-c", ANA_TIME], cwd=tmp_path, capture_output=True, text=True, check=True)
+    assert out.stdout.split() == ["0.60", "0.63", "2.25"]
+    txt = (tmp_path / "dqmc.out").read_text()
+    assert f"The_time_of_{name}:" in txt
+
+
+def test_fast_update_timing_line(tmp_path):
+    import sunhubbardmy_b200 as sb
+    from sunhubbardmy_b200.io import dqmc_end_print
+    import io as pyio
+    p = sb.DqmcParams.make(lattice=1, l1=4, l2=4, beta=2.0, dtau=0.1, rhub=4.0, update=0, nwrap=5)
+    prof = {k: (10.0, 1) for k in ("update", "stab", "green", "prop_left", "measure", "prop_right", "bprod", "other")}
+    f = pyio.StringIO()
+    dqmc_end_print(f, [dict(accepted=1.0, proposed=2.0)], 1.0, prof, params=p)
+    txt = f.getvalue()
+    assert "The_time_of_ft_fast_update:          0.010s" in txt and "update_gfunc" not in txt
+
+
 def _c_fields(header: str, name: str):
     import re
     i = header.index(f"typedef struct {name} {{")
@@ -297,11 +346,91 @@ def _f_fields(doc: str, name: str):
 
 
 def test_fortran_binding_types_mirror_the_header():
-    """The iso_c_binding types of the integration guide list the C structs'
+    """The iso_c_binding types of include/dqmc_gpu_f.f90 list the C structs'
     fields in the same order and kind, so dqmc_gpu_get_diag and
     dqmc_params_derive never write past a Fortran caller's variable."""
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     header = open(os.path.join(root, "include", "dqmc_gpu.h")).read()
-    doc = open(os.path.join(root, "INTEGRATION.md")).read()
-    assert _c_fields(header, "dqmc_params") == _f_fields(doc, "dqmc_params_c")
-    assert _c_fields(header, "dqmc_diag") == _f_fields(doc, "dqmc_diag_c")
+    mod = open(os.path.join(root, "include", "dqmc_gpu_f.f90")).read()
+    assert _c_fields(header, "dqmc_params") == _f_fields(mod, "dqmc_params_c")
+    assert _c_fields(header, "dqmc_diag") == _f_fields(mod, "dqmc_diag_c")
+
+
+def test_fortran_interfaces_match_the_header():
+    """Every bind(C) interface of the Fortran module names a function of the C
+    header with the same number of arguments, and its integer constants
+    repeat the header's values."""
+    import re
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    header = re.sub(r"/\*.*?\*/", "", open(os.path.join(root, "include", "dqmc_gpu.h")).read(), flags=re.S)
+    mod = open(os.path.join(root, "include", "dqmc_gpu_f.f90")).read()
+    c_funcs = {}
+    for name, args in re.findall(r"\b(dqmc_\w+)\s*\(([^;{]*?)\)\s*;", header):
+        a = args.strip()
+        c_funcs[name] = 0 if a in ("", "void") else a.count(",") + 1
+    f_funcs = re.findall(r"function\s+(dqmc_\w+)\s*\(([^)]*)\)\s*bind\(C\)", mod)
+    assert len(f_funcs) >= 35
+    for name, args in f_funcs:
+        assert name in c_funcs, name
+        n = 0 if not args.strip() else args.count(",") + 1
+        assert n == c_funcs[name], (name, n, c_funcs[name])
+    for name, val in re.findall(r"(DQMC_\w+) = (-?\d+)", mod):
+        m = re.search(rf"#define {name} \(?(-?\d+)\)?", header)
+        assert m and int(m.group(1)) == int(val), name
+
+
+REPLAY_STUB = r"""
+#include <stdio.h>
+#include <string.h>
+#include "dqmc_gpu.h"
+/* handle-less stand-in for libdqmc_gpu.so: logs every call */
+static int lg(const char* n) { printf("%s\n", n); return 0; }
+int dqmc_params_derive(dqmc_params* p) {
+    lg("dqmc_params_derive");
+    p->ndim = p->l1 * p->l2 * (p->lattice == 2 ? 2 : 1);
+    p->ltrot = (int)(p->beta / p->dtau + 0.5);
+    return 0;
+}
+const char* dqmc_gpu_last_error(void) { return ""; }
+int dqmc_gpu_create(const dqmc_params* p, int np, int nch, const int32_t* s, int d, dqmc_handle** h) {
+    *h = (dqmc_handle*)1; printf("dqmc_gpu_create %d %d %d %d\n", np, nch, (int)s[0], d); return 0; }
+int dqmc_gpu_destroy(dqmc_handle* h) { return lg("dqmc_gpu_destroy"); }
+int dqmc_gpu_set_conf(dqmc_handle* h, int c, const int32_t* x) { return lg("dqmc_gpu_set_conf"); }
+int dqmc_gpu_get_conf(dqmc_handle* h, int c, int32_t* x) { return lg("dqmc_gpu_get_conf"); }
+int dqmc_gpu_sweep_start(dqmc_handle* h) { return lg("dqmc_gpu_sweep_start"); }
+int dqmc_gpu_sweep_b0(dqmc_handle* h, int u, int m) { printf("dqmc_gpu_sweep_b0 %d %d\n", u, m); return 0; }
+int dqmc_gpu_sweep_0b(dqmc_handle* h, int u, int m) { printf("dqmc_gpu_sweep_0b %d %d\n", u, m); return 0; }
+int dqmc_gpu_sweep_dyn(dqmc_handle* h) { return lg("dqmc_gpu_sweep_dyn"); }
+int dqmc_gpu_obser_init(dqmc_handle* h) { return lg("dqmc_gpu_obser_init"); }
+int dqmc_gpu_nbins(dqmc_handle* h, int c) { lg("dqmc_gpu_nbins"); return 14; }
+int dqmc_gpu_get_bins(dqmc_handle* h, int c, double* o) { memset(o, 0, 28 * sizeof(double)); return lg("dqmc_gpu_get_bins"); }
+int dqmc_gpu_get_diag(dqmc_handle* h, int c, dqmc_diag* d) { memset(d, 0, sizeof(*d)); return lg("dqmc_gpu_get_diag"); }
+"""
+
+
+def test_replay_driver_makes_the_reference_call_order(tmp_path):
+    """replay_ft (the reference's dqmc_main / dqmc_ft_ctrl call order through
+    the C ABI) built against a logging stub: dqmc_start, dqmc_warmup, then
+    nbin x (obser_init, nsweep x (b0, [dyn,] 0b), equaltime_output,
+    dqmc_timing), dqmc_end."""
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    (tmp_path / "stub.c").write_text(REPLAY_STUB)
+    exe = tmp_path / "replay_stub"
+    subprocess.run(["gcc", "-std=c99", "-o", str(exe), os.path.join(root, "sunhubbardmy_b200", "csrc", "replay_ft.c"),
+                    str(tmp_path / "stub.c"), "-I", os.path.join(root, "include")], check=True)
+    (tmp_path / "dqmc.in").write_text("&model_para\nla = 4, lb = 4,\nbeta = 1.d0\ndtau = 0.1d0,\nrhub = 4.0\n/\n"
+                                      "&ctrl_para\nnwrap = 5, nsweep = 2, nbin = 2, ltau = .true.\n/\n")
+    out = subprocess.run([str(exe), "dqmc.in", "nwarmup=1"], cwd=tmp_path, capture_output=True, text=True, check=True)
+    calls = out.stdout.split("\n")[:-1]
+    sweep = ["dqmc_gpu_sweep_b0 1 1", "dqmc_gpu_sweep_dyn", "dqmc_gpu_sweep_0b 1 1"]
+    binl = ["dqmc_gpu_obser_init"] + sweep * 2 + ["dqmc_gpu_nbins", "dqmc_gpu_get_bins", "dqmc_gpu_get_diag",
+                                                   "dqmc_gpu_get_conf"]
+    expect = (["dqmc_params_derive", "dqmc_gpu_create 1 1 1909706392 1", "dqmc_gpu_sweep_start",
+               "dqmc_gpu_sweep_b0 1 0", "dqmc_gpu_sweep_0b 1 0"] + binl * 2
+              + ["dqmc_gpu_get_diag", "dqmc_gpu_destroy"])
+    assert calls == expect
+    lines = (tmp_path / "replay.out").read_text().split("\n")
+    assert lines[0].startswith("bin 1 ") and lines[1].startswith("bin 2 ")
+    conf = (tmp_path / "conf_u.out").read_text().split()
+    assert conf[0] == "1" and len(conf) == 1 + 16 * 10
