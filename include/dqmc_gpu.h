@@ -103,6 +103,8 @@ typedef struct dqmc_diag {
     double dyn_log10_sum, dyn_count;    /* sum of log10 of those checks (avglog10dynerror) and their number */
     double info;                        /* OR of the DQMC_FAIL_* codes this chain raised since reset_diag */
     double restabilized;                /* re-stabilisations of the handle (dqmc_gpu_set_checks) since reset_diag */
+    double near_ties;                   /* accept tests with | |Re(R phase)/Re(phase)| - r | < 1e-12: their
+                                           outcome may depend on rounding (logged, not altered) */
 } dqmc_diag;
 
 typedef struct dqmc_handle dqmc_handle;
@@ -142,6 +144,15 @@ int dqmc_gpu_get_conf_all(dqmc_handle* h, int32_t* conf);
 /* Equal-time Green's function G = <c c^+> of one chain (gf%blk1). */
 int dqmc_gpu_get_green(dqmc_handle* h, int chain, double* g);
 int dqmc_gpu_set_green(dqmc_handle* h, int chain, const double* g);
+
+/* Wrap trace of one chain, the counterpart of the reference's -DTEST_LEVEL3
+ * print of the scratch Green's function at every stabilisation
+ * (src/dqmc_ft_core/dqmc_ft_sweep_b0.f90:160-179): the next `capacity`
+ * recorded wrap checks store the freshly computed G (N x N complex) and the
+ * wrap error max|G_fresh - G_propagated|.  capacity 0 stops and frees it. */
+int dqmc_gpu_trace_wraps(dqmc_handle* h, int chain, int capacity);
+int dqmc_gpu_trace_count(dqmc_handle* h, int chain);
+int dqmc_gpu_trace_get(dqmc_handle* h, int chain, int i, double* g, double* err);
 
 /* Entry n = 0..nst of the finite-temperature UDV stack of one chain: Ust(n)
  * and Vst(n) (N x N complex), Dst(n) (N doubles) and logdetQst(n) (one

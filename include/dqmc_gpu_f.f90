@@ -46,6 +46,7 @@ module dqmc_gpu_f
      real(c_double) :: blk_err_learned, blk_err_zero
      real(c_double) :: max_dyn_error, dyn_log10_sum, dyn_count
      real(c_double) :: info, restabilized
+     real(c_double) :: near_ties
   end type
 
   interface

@@ -109,7 +109,10 @@ void orc_chain_set_phase(orc_chain *c, double re, double im);
 /* diag: [0]=phase.re [1]=phase.im [2]=logw.re [3]=logw.im [4]=max_wrap_error
  * [5]=max_phasediff [6]=avglog10error [7]=logcount [8]=accepted [9]=proposed
  * [10]=accepted bond-field [11]=proposed bond-field */
-void orc_chain_get_diag(const orc_chain *c, double *out);
+void orc_chain_get_diag(const orc_chain *c, double *out);   /* 13 doubles; out[12] = near ties */
+void orc_chain_trace(orc_chain *c, int cap);
+int orc_chain_trace_count(const orc_chain *c);
+void orc_chain_trace_get(const orc_chain *c, int i, double *g, double *err);
 double orc_chain_uniform(orc_chain *c);
 
 /* drivers (src/dqmc_ft_core/ directory) */

@@ -387,6 +387,7 @@ void orc_chain_free(orc_chain *c) {
     free(c->zcpcm_bin); free(c->zspsm_bin); free(c->znn_bin); free(c->pair_onsite_bin);
     free(c->zjj_bin); free(c->zbb_bin); free(c->pair_nn_bin); free(c->pair_sn_bin);
     orc_proj_chain_free(c);
+    free(c->trace_g); free(c->trace_err);
     free(c);
 }
 
@@ -412,6 +413,26 @@ void orc_chain_get_diag(const orc_chain *c, double *out) {
     out[6] = c->avglog10error; out[7] = c->logcount;
     out[8] = c->acc_u; out[9] = c->prop_u;
     out[10] = c->acc_v; out[11] = c->prop_v;
+    out[12] = c->near_ties;
+}
+
+/* trace of (fresh G, wrap error) at the next `cap` recorded wrap checks
+ * (cap = 0 stops and frees it) */
+void orc_chain_trace(orc_chain *c, int cap) {
+    free(c->trace_g); free(c->trace_err);
+    c->trace_g = NULL; c->trace_err = NULL; c->trace_cap = 0; c->trace_n = 0;
+    if (cap <= 0) return;
+    size_t NN = (size_t)c->m->ndim * c->m->ndim;
+    c->trace_g = calloc(NN * (size_t)cap, sizeof(zc));
+    c->trace_err = calloc((size_t)cap, sizeof(double));
+    c->trace_cap = (c->trace_g && c->trace_err) ? cap : 0;
+}
+int orc_chain_trace_count(const orc_chain *c) { return c->trace_n; }
+void orc_chain_trace_get(const orc_chain *c, int i, double *g, double *err) {
+    size_t NN = (size_t)c->m->ndim * c->m->ndim;
+    if (i < 0 || i >= c->trace_n) return;
+    if (g) memcpy(g, c->trace_g + (size_t)i * NN, sizeof(zc) * NN);
+    if (err) *err = c->trace_err[i];
 }
 
 /* ------------------------------------------------------------------ */
@@ -609,6 +630,7 @@ static void update_fast(orc_chain *c, int nt, int32_t *acc) {
         double rre = creal(rt * c->phase) / creal(c->phase);
         double rabs = rre < 0 ? -rre : rre;
         double rnd = orc_sfmt_stream(&c->rng);
+        ORC_COUNT_TIE(c, rabs, rnd);
         int a = rabs > rnd;
         if (acc) acc[is_] = a;
         if (a) {
@@ -646,6 +668,7 @@ static void update_delay(orc_chain *c, int nt, int32_t *acc) {
         double rre = creal(rt * c->phase) / creal(c->phase);
         double rabs = rre < 0 ? -rre : rre;
         double rnd = orc_sfmt_stream(&c->rng);
+        ORC_COUNT_TIE(c, rabs, rnd);
         int a = rabs > rnd;
         if (acc) acc[s] = a;
         if (a) {
@@ -716,6 +739,7 @@ static void update_submatrix(orc_chain *c, int nt, int32_t *acc) {
         double rre = creal(rt * c->phase) / creal(c->phase);
         double rabs = rre < 0 ? -rre : rre;
         double rnd = orc_sfmt_stream(&c->rng);
+        ORC_COUNT_TIE(c, rabs, rnd);
         int a = rabs > rnd;
         if (acc) acc[s] = a;
         if (a) {
@@ -1214,6 +1238,10 @@ static void h0_half(orc_chain *c, int left_op, int right_op, int reversed) {
 static void record_wrap(orc_chain *c, const zc *gtmp, zc logw) {
     int N = c->m->ndim;
     double err = orc_compare_max(N, gtmp, c->gf);
+    if (c->trace_g && c->trace_n < c->trace_cap) {
+        memcpy(c->trace_g + (size_t)c->trace_n * N * N, gtmp, sizeof(zc) * (size_t)N * N);
+        c->trace_err[c->trace_n++] = err;
+    }
     if (err > c->max_wrap_error) c->max_wrap_error = err;
     zc ph = orc_set_phase(c, logw);
     double pd = cabs(c->phase - ph);

@@ -92,7 +92,18 @@ struct orc_chain {
     zc *znn_tau_bin;
     zc **Ust_b, **Vst_b, *gf_b, *logdetQst_b;
     double **Dst_b;
+    /* test instrumentation: accept tests decided within ORC_NEAR_TIE of the
+     * random number, and a trace of (fresh G, wrap error) at every recorded
+     * wrap check (the reference's -DTEST_LEVEL3 print of gf_tmp) */
+    double near_ties;
+    zc *trace_g;
+    double *trace_err;
+    int trace_cap, trace_n;
 };
+
+#define ORC_NEAR_TIE 1e-12
+#define ORC_COUNT_TIE(c, ratio_abs, random) \
+    do { if (fabs((ratio_abs) - (random)) < ORC_NEAR_TIE) (c)->near_ties += 1.0; } while (0)
 
 /* linear algebra helpers (orc_linalg.c) */
 void orc_zgemm(char ta, char tb, int m, int n, int k, zc alpha, const zc *a, int lda,

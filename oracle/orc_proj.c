@@ -275,6 +275,7 @@ static void proj_update_v(orc_chain *c, int nt, int nf) {
         double ratio_re = creal(ratiotot * c->phase) / creal(c->phase);
         double ratio_abs = ratio_re < 0 ? -ratio_re : ratio_re;
         double random = orc_sfmt_stream(&c->rng);
+        ORC_COUNT_TIE(c, ratio_abs, random);
         if (ratio_abs > random) {
             accm += 1.0;
             double weight = sqrt(creal(ratiotot * conj(ratiotot)));
@@ -363,6 +364,7 @@ static void proj_update_v_lr(orc_chain *c, int nt, int nf) {
         double ratio_re = creal(ratiotot * c->phase) / creal(c->phase);
         double ratio_abs = ratio_re < 0 ? -ratio_re : ratio_re;
         double random = orc_sfmt_stream(&c->rng);
+        ORC_COUNT_TIE(c, ratio_abs, random);
         if (ratio_abs > random) {
             accm += 1.0;
             double weight = sqrt(creal(ratiotot * conj(ratiotot)));
@@ -447,6 +449,7 @@ static void proj_update_u(orc_chain *c, int nt) {
         double ratio_re = creal(ratiotot * c->phase) / creal(c->phase);
         double ratio_abs = ratio_re < 0 ? -ratio_re : ratio_re;
         double random = orc_sfmt_stream(&c->rng);
+        ORC_COUNT_TIE(c, ratio_abs, random);
         if (ratio_abs > random) {
             accm += 1.0;
             double weight = sqrt(creal(ratiotot * conj(ratiotot)));
@@ -551,6 +554,10 @@ static void record_proj_wrap(orc_chain *c, const zc *ultmp, const zc *urtmp, zc 
     proj_green(N, ne, ultmp, urtmp, inv, gtmp);
     double err = orc_compare_max(N, gtmp, c->gf);
     if (err > c->max_wrap_error) c->max_wrap_error = err;
+    if (c->trace_g && c->trace_n < c->trace_cap) {
+        memcpy(c->trace_g + (size_t)c->trace_n * N * N, gtmp, sizeof(zc) * (size_t)N * N);
+        c->trace_err[c->trace_n++] = err;
+    }
     zc ph = orc_set_phase(c, lw);
     double pd = cabs(c->phase - ph);
     if (pd > c->max_phasediff) c->max_phasediff = pd;

@@ -116,6 +116,10 @@ def lib() -> C.CDLL:
         L.orc_proj_update_flavour.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         L.orc_proj_sweep_b0_slices.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         L.orc_vconf_prop.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, C.c_int]
+        L.orc_chain_trace.argtypes = [vp, C.c_int]
+        L.orc_chain_trace_count.argtypes = [vp]
+        L.orc_chain_trace_count.restype = C.c_int
+        L.orc_chain_trace_get.argtypes = [vp, C.c_int, vp, vp]
         L.orc_qr_pqmc_d.argtypes = [C.c_int, C.c_int, vp, vp]
         L.orc_qr_pqmc_d.restype = dbl
         L.orc_eig_he_d.argtypes = [C.c_int, vp, vp, vp]
@@ -277,11 +281,28 @@ class Chain:
         lib().orc_chain_set_phase(self._p, z.real, z.imag)
 
     def diag(self) -> dict:
-        d = np.zeros(12)
+        d = np.zeros(13)
         lib().orc_chain_get_diag(self._p, _ptr(d))
         return dict(phase=complex(d[0], d[1]), logweight=complex(d[2], d[3]), max_wrap_error=d[4],
                     max_phasediff=d[5], avglog10error=d[6], logcount=d[7], accepted=d[8], proposed=d[9],
-                    accepted_v=d[10], proposed_v=d[11])
+                    accepted_v=d[10], proposed_v=d[11], near_ties=int(d[12]))
+
+    def trace(self, capacity: int) -> None:
+        """Record (fresh G, wrap error) at the next `capacity` wrap checks."""
+        lib().orc_chain_trace(self._p, int(capacity))
+
+    def trace_get(self):
+        """[(G, wrap error)] recorded since trace()."""
+        L = lib()
+        n = L.orc_chain_trace_count(self._p)
+        N = self.model.ndim
+        out = []
+        for i in range(n):
+            g = np.zeros((N, N), complex, order="F")
+            e = C.c_double()
+            L.orc_chain_trace_get(self._p, i, _ptr(g), C.byref(e))
+            out.append((g, e.value))
+        return out
 
     def max_dyn_error(self) -> float:
         """xmax_dyn of the projective unequal-time pass."""

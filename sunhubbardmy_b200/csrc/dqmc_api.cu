@@ -2017,6 +2017,52 @@ extern "C" int dqmc_gpu_set_green(dqmc_handle* h, int chain, const double* g) {
     return DQMC_OK;
 }
 
+// wrap trace of one chain: the fresh G and the wrap error at each of the next
+// `capacity` recorded wrap checks (capacity 0 stops it and frees the buffers);
+// the counterpart of the reference's -DTEST_LEVEL3 print of gf_tmp at every
+// stabilisation (src/dqmc_ft_core/dqmc_ft_sweep_b0.f90:160-179)
+extern "C" int dqmc_gpu_trace_wraps(dqmc_handle* h, int chain, int capacity) {
+    int rc = chk_chain(h, chain); if (rc) return rc;
+    if (capacity < 0) return fail(DQMC_EINVAL, "capacity >= 0");
+    ChainDev& d = h->chains[chain].dev;
+    CK(cudaStreamSynchronize(h->st));
+    dfree(h, d.trace_g); dfree(h, d.trace_err); dfree(h, d.trace_n);
+    d.trace_g = nullptr; d.trace_err = nullptr; d.trace_n = nullptr; d.trace_cap = 0;
+    if (capacity > 0) {
+        d.trace_g = (double2*)dalloc(h, (size_t)capacity * d.N * d.N * sizeof(double2));
+        d.trace_err = (double*)dalloc(h, (size_t)capacity * sizeof(double));
+        d.trace_n = (int*)dalloc(h, sizeof(int));
+        if (!d.trace_g || !d.trace_err || !d.trace_n) {
+            dfree(h, d.trace_g); dfree(h, d.trace_err); dfree(h, d.trace_n);
+            d.trace_g = nullptr; d.trace_err = nullptr; d.trace_n = nullptr;
+            CK(copy_sync(h->st, h->d_chains + chain, &d, sizeof(ChainDev), cudaMemcpyHostToDevice));
+            return fail(DQMC_ENOMEM, "trace buffers");
+        }
+        d.trace_cap = capacity;
+    }
+    CK(copy_sync(h->st, h->d_chains + chain, &d, sizeof(ChainDev), cudaMemcpyHostToDevice));
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_trace_count(dqmc_handle* h, int chain) {
+    int rc = chk_chain(h, chain); if (rc) return rc;
+    const ChainDev& d = h->chains[chain].dev;
+    if (!d.trace_n) return 0;
+    int n = 0;
+    CK(copy_sync(h->st, &n, d.trace_n, sizeof(int), cudaMemcpyDeviceToHost));
+    return n;
+}
+
+extern "C" int dqmc_gpu_trace_get(dqmc_handle* h, int chain, int i, double* g, double* err) {
+    int n = dqmc_gpu_trace_count(h, chain); if (n < 0) return n;
+    if (i < 0 || i >= n) return fail(DQMC_EINVAL, "trace index out of range");
+    const ChainDev& d = h->chains[chain].dev;
+    const size_t NN = (size_t)d.N * d.N;
+    if (g) CK(copy_sync(h->st, g, d.trace_g + (size_t)i * NN, NN * sizeof(double2), cudaMemcpyDeviceToHost));
+    if (err) CK(copy_sync(h->st, err, d.trace_err + i, sizeof(double), cudaMemcpyDeviceToHost));
+    return DQMC_OK;
+}
+
 // Ust(n), Dst(n), Vst(n), logdetQst(n) of the finite-temperature UDV stack
 // (src/dqmc_ft_core.f90:11-19), logical index n = 0..nst, through the slot map
 static int stack_slot(dqmc_handle* h, int chain, int n, int* slot) {
@@ -2140,6 +2186,7 @@ extern "C" int dqmc_gpu_get_diag(dqmc_handle* h, int chain, dqmc_diag* out) {
     out->dyn_log10_sum = st[ST_DYN_LOG10]; out->dyn_count = st[ST_DYN_COUNT];
     out->info = st[ST_INFO];
     out->restabilized = h->n_restab;
+    out->near_ties = st[ST_NEAR_TIE];
     return DQMC_OK;
 }
 
@@ -2154,6 +2201,7 @@ extern "C" int dqmc_gpu_reset_diag(dqmc_handle* h) {
         st[ST_BLK_ERR1] = st[ST_BLK_ERR0] = 0.0;
         st[ST_MAX_DYN] = st[ST_DYN_LOG10] = st[ST_DYN_COUNT] = 0.0;
         st[ST_INFO] = 0.0;
+        st[ST_NEAR_TIE] = 0.0;
         CK(copy_sync(h->st, h->chains[c].dev.stats, st, sizeof(st), cudaMemcpyHostToDevice));
     }
     h->n_restab = 0.0;

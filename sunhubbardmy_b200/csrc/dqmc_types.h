@@ -107,7 +107,17 @@ struct ChainDev {
     // ctl[0] is the wrap-error tolerance (0 = none)
     int* fail;
     const double* ctl;
+    // wrap trace (dqmc_gpu_trace_wraps): the fresh G and the wrap error of
+    // each recorded wrap check, up to trace_cap of them (null: off)
+    double2* trace_g;
+    double* trace_err;
+    int* trace_n;
+    int trace_cap;
 };
+
+// an accept test |Re(R phase)/Re(phase)| > r whose two sides differ by less than
+// this is counted in stats[ST_NEAR_TIE]: its outcome may depend on rounding
+#define DQ_NEAR_TIE 1e-12
 
 // numerical-failure codes (stats[ST_INFO] per chain, fail[0] per handle)
 enum {
@@ -128,6 +138,7 @@ enum {
     ST_DYN_LOG10,              // its sum of log10 over the checks (avglog10dynerror) ...
     ST_DYN_COUNT,              // ... and the number of checks (logdyncount)
     ST_GINFO,                  // DQ_FAIL_SINGULAR of the latest Green's-function computation (overwritten by each)
+    ST_NEAR_TIE,               // accept tests decided with | |ratio| - r | < DQ_NEAR_TIE
     ST_COUNT = 40
 };
 

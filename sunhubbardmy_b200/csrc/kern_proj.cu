@@ -205,7 +205,7 @@ struct PUpdSmem {
     int rows[PW_MAXR];
     int accr[PW_MAXR];
     int acc_flag[2], nacc;
-    double accm;
+    double accm, nties;
     // per-unit proposal, prepared in parallel before the sequential walk
     double2 ud1[PW_MAXR], ud2[PW_MAXR];   // Delta of the unit's rows
     double ur2[PW_MAXR];                  // accept threshold (second draw)
@@ -323,6 +323,7 @@ __global__ void __launch_bounds__(256) k_pwin_seq(const ChainDev* __restrict__ c
     if (tid == 0) {
         S->phase = cmk(c.stats[ST_PHASE_RE], c.stats[ST_PHASE_IM]);
         S->accm = 0.0;
+        S->nties = 0.0;
         S->nacc = 0;
     }
     {   // F = Rg UL(:,rows) = Rg ULT(rows,:)^T
@@ -391,6 +392,7 @@ __global__ void __launch_bounds__(256) k_pwin_seq(const ChainDev* __restrict__ c
                 const double2 ph = S->phase;
                 double ratio_re = cmul(ratiotot, ph).x / ph.x;
                 int acc = fabs(ratio_re) > S->ur2[k];
+                if (fabs(fabs(ratio_re) - S->ur2[k]) < DQ_NEAR_TIE) S->nties += 1.0;
                 if (acc) {
                     double wgt = sqrt(cmul(ratiotot, cconj(ratiotot)).x);
                     S->phase = cscale(cmul(ph, ratiotot), 1.0 / wgt);
@@ -484,6 +486,7 @@ __global__ void __launch_bounds__(256) k_pwin_seq(const ChainDev* __restrict__ c
         c.stats[ST_PHASE_RE] = S->phase.x;
         c.stats[ST_PHASE_IM] = S->phase.y;
         c.stats[bond ? ST_ACCV : ST_ACC] += S->accm;
+        c.stats[ST_NEAR_TIE] += S->nties;
         c.stats[bond ? ST_PROPV : ST_PROP] += (double)nu;
     }
 }

@@ -421,6 +421,11 @@ __global__ void __launch_bounds__(256) k_wrap_check(const ChainDev* __restrict__
     wnan = __syncthreads_or(wnan);
     const int ginfo = (int)c.stats[ST_GINFO];
     const bool keep = nonfin || (ginfo & DQ_FAIL_SINGULAR);
+    // wrap trace: the fresh G of this check (the reference's -DTEST_LEVEL3
+    // print of gf_tmp, dqmc_ft_sweep_b0.f90:160-179)
+    const int tslot = (record && c.trace_g) ? *c.trace_n : c.trace_cap;
+    if (tslot < c.trace_cap)
+        for (size_t e = tid; e < NN; e += nth) c.trace_g[(size_t)tslot * NN + e] = c.Gnew[e];
     if (!keep)
         for (size_t e = tid; e < NN; e += nth) c.G[e] = c.Gnew[e];
     mx = block_max(mx, red);
@@ -437,6 +442,7 @@ __global__ void __launch_bounds__(256) k_wrap_check(const ChainDev* __restrict__
         const double tol = c.ctl ? c.ctl[0] : 0.0;
         if (record && tol > 0.0 && (wnan || mx > tol)) code |= DQ_FAIL_WRAP;
         if (code) chain_raise(c, code);
+        if (tslot < c.trace_cap) { c.trace_err[tslot] = mx; *c.trace_n = tslot + 1; }
         if (record) {
             double2 old = cmk(c.stats[ST_PHASE_RE], c.stats[ST_PHASE_IM]);
             double pd = cabsd(csub(old, ph));

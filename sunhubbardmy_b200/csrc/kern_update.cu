@@ -224,9 +224,9 @@ __global__ void __launch_bounds__(UPD_NT, 2) k_update_delay(const ChainDev* __re
                 cand = !forced || c.blk[j] != 0;
                 dW = W->gW[p * UPD_LP + p];
             }
-            int r = 0, pc = 0, wend = L;
+            int r = 0, pc = 0, wend = L, nties = 0;
             while (pc < L) {
-                bool pass = false;
+                bool pass = false, tie = false;
                 double2 rt = cmk(0, 0), sscl = cmk(0, 0);
                 if (cand && p >= pc) {
                     const double2 ratio1 = cadd(cmul(csub(cmk(1, 0), dW), dl), cmk(1, 0));
@@ -234,10 +234,16 @@ __global__ void __launch_bounds__(UPD_NT, 2) k_update_delay(const ChainDev* __re
                     for (int f = 1; f < nflr; ++f) rr = cmul(rr, ratio1);
                     rr = cscale(rr, gam);
                     rt = cmul(rr, phr);
-                    pass = forced ? true : fabs(cmul(rt, ph).x / ph.x) > thr;
+                    const double ra = fabs(cmul(rt, ph).x / ph.x);
+                    pass = forced ? true : ra > thr;
+                    tie = !forced && fabs(ra - thr) < DQ_NEAR_TIE;
                     if (pass) sscl = cdiv(dl, ratio1);
                 }
                 const unsigned bal = __ballot_sync(0xffffffffu, pass);
+                // this iteration decides the lanes up to the first passing one
+                // (all remaining lanes when none passes); later lanes are
+                // tested again with the updated diagonal
+                nties += tie && (bal == 0 || p <= __ffs(bal) - 1);
                 if (bal == 0) break;
                 const int pf = __ffs(bal) - 1;
                 rt.x = __shfl_sync(0xffffffffu, rt.x, pf);
@@ -277,6 +283,8 @@ __global__ void __launch_bounds__(UPD_NT, 2) k_update_delay(const ChainDev* __re
                 if (k + r == nb) { wend = pc; break; }
             }
             if (lane == 0) { W->r = r; W->wend = wend; }
+            nties = warp_sum(nties);
+            if (lane == 0 && nties) c.stats[ST_NEAR_TIE] += (double)nties;
         }
         __syncthreads();
         // 3. the window's columns on all rows: column m of this window is

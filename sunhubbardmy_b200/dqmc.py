@@ -98,7 +98,7 @@ class DqmcDiag(C.Structure):
         "avglog10error_sum", "logcount", "avgexpphasediff_sum", "accepted", "proposed", "nobs",
         "accepted_v", "proposed_v", "blk_proposed", "blk_stage1", "blk_accepted", "blk_sum_logratio",
         "blk_err_learned", "blk_err_zero", "max_dyn_error", "dyn_log10_sum", "dyn_count", "info",
-        "restabilized")]
+        "restabilized", "near_ties")]
 
 
 _lib = None
@@ -120,6 +120,9 @@ SIGNATURES = {
     "dqmc_gpu_get_stack": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp]),
     "dqmc_gpu_set_stack": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp]),
     "dqmc_gpu_set_checks": (_i, [_vp, _d, _i]),
+    "dqmc_gpu_trace_wraps": (_i, [_vp, _i, _i]),
+    "dqmc_gpu_trace_count": (_i, [_vp, _i]),
+    "dqmc_gpu_trace_get": (_i, [_vp, _i, _i, _vp, _vp]),
     "dqmc_gpu_sweep_start": (_i, [_vp]),
     "dqmc_gpu_sweep_b0": (_i, [_vp, _i, _i]),
     "dqmc_gpu_sweep_0b": (_i, [_vp, _i, _i]),
@@ -408,6 +411,24 @@ class Dqmc:
         assert a.size == 625
         _check(load_library().dqmc_gpu_set_rng(self.h, c, _ptr(a)), "set_rng")
 
+    def trace_wraps(self, capacity: int, c: int = 0) -> None:
+        """Record (fresh G, wrap error) at the next `capacity` wrap checks of chain c."""
+        _check(load_library().dqmc_gpu_trace_wraps(self.h, c, int(capacity)), "trace_wraps")
+
+    def trace_get(self, c: int = 0):
+        """[(G, wrap error)] recorded since trace_wraps."""
+        L = load_library()
+        n = L.dqmc_gpu_trace_count(self.h, c)
+        _check(min(n, 0), "trace_count")
+        N = self.ndim(c)
+        out = []
+        for i in range(n):
+            g = np.zeros((N, N), complex, order="F")
+            e = C.c_double()
+            _check(L.dqmc_gpu_trace_get(self.h, c, i, _ptr(g), C.byref(e)), "trace_get")
+            out.append((g, e.value))
+        return out
+
     def set_checks(self, wrap_tol: float = 0.0, restabilize: bool = False) -> None:
         """Numerical checks of the sweep calls (dqmc_gpu_set_checks): a wrap
         error above wrap_tol (> 0) raises DqmcError with code EWRAP; with
@@ -429,7 +450,7 @@ class Dqmc:
                     blk_sum_logratio=d.blk_sum_logratio, blk_err_learned=d.blk_err_learned,
                     blk_err_zero=d.blk_err_zero, max_dyn_error=d.max_dyn_error,
                     dyn_log10_sum=d.dyn_log10_sum, dyn_count=d.dyn_count, info=int(d.info),
-                    restabilized=int(d.restabilized))
+                    restabilized=int(d.restabilized), near_ties=int(d.near_ties))
 
     def energy_all(self) -> np.ndarray:
         """energy_bin(1:10) of every chain, shape (n_chains, 10) complex."""
