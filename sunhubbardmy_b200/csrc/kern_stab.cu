@@ -40,7 +40,7 @@ static size_t stab_smem_bytes(int maxN) {
 }
 
 // one UDV step: W0 holds B(slices) * U[src]; writes U/D/V/logdetQ of slot dst.
-__global__ void __launch_bounds__(256) k_stab(const ChainDev* __restrict__ chains, int src, int dst) {
+__global__ void __launch_bounds__(256, 2) k_stab(const ChainDev* __restrict__ chains, int src, int dst) {
     extern __shared__ double2 ssm[];
     const ChainDev c = chains[blockIdx.x];
     const int N = c.N, tid = threadIdx.x, nth = blockDim.x;
