@@ -210,7 +210,102 @@ def dqmc_initial_print(f, p, wrap_step=None, nustock: int = 0) -> None:
     for i, (a, b) in enumerate(wrap_step or [], start=1):
         w(f"{a:16d}{b:16d}{i:16d}\n")
     w(" \n")
-    w(("honeycomb_lattice" if g["lattice"] == 2 else "square_lattice") + "\n")
+    w({2: "honeycomb_lattice", 3: "chain_lattice"}.get(g["lattice"], "square_lattice") + "\n")
+    if not isinstance(p, dict):
+        print_latt(f, p)
+
+
+def _f16_12(v: float) -> str:
+    """Fortran f16.12."""
+    return f"{v:16.12f}"
+
+
+def lattice_lists(p) -> dict:
+    """The lattice tables that print_latt writes (1-based), for a DqmcParams p:
+    list/cord (setup_honeycomb_sub, setup_square_sub, setup_chain_sub in
+    src/lattice.f90), nnlist/snlist/plq_cord from the library's own tables,
+    tnlist (third neighbours, src/lattice.f90:312-313, 716-731, 892-895), listk
+    (the k list of setup_latt2d_sub / setup_latt1d_sub) and the primitive and
+    reciprocal vectors (src/model_para.f90:342-357)."""
+    t = p.tables()
+    l1, l2, lat = int(p.l1), int(p.l2), int(p.lattice)
+    N = int(p.ndim)
+
+    def npbc(nr, l):
+        return nr - l if nr > l else (nr + l if nr < 1 else nr)
+
+    if lat == 3:      # chain
+        a1, a2 = np.array([1.0]), None
+        cord = np.array([[i] for i in range(1, l1 + 1)], dtype=np.int64)
+        tn = np.array([[npbc(i + 3, l1), npbc(i - 3, l1)] for i in range(1, l1 + 1)], dtype=np.int64)
+        listk = np.array([[m] for m in range(-((l1 + 1) // 2) + 1, l1 // 2 + 1)], dtype=np.int64)
+    else:
+        hc = lat == 2
+        if hc:
+            a1 = np.array([0.5, -0.5 * np.sqrt(3.0)]); a2 = np.array([0.5, 0.5 * np.sqrt(3.0)])
+        else:
+            a1 = np.array([1.0, 0.0]); a2 = np.array([0.0, 1.0])
+        nsub = 2 if hc else 1
+        cord = np.zeros((N, 2), dtype=np.int64)
+        tn = np.zeros((N, 3 if hc else 4), dtype=np.int64)
+        for i1 in range(1, l1 + 1):
+            for i2 in range(1, l2 + 1):
+                for o in range(nsub):
+                    cord[((i1 - 1) * l2 + i2 - 1) * nsub + o] = (i1, i2)
+
+        def cs(c1, c2):
+            return (npbc(c1, l1) - 1) * l2 + npbc(c2, l2)
+        for i in range(N):
+            c1, c2 = cord[i]
+            if hc and i % 2 == 0:      # A site (1-based odd)
+                tn[i] = (cs(c1 + 1, c2 - 1) * 2, cs(c1 - 1, c2 - 1) * 2, cs(c1 + 1, c2 + 1) * 2)
+            elif hc:                    # B site
+                tn[i] = (cs(c1 - 1, c2 + 1) * 2 - 1, cs(c1 + 1, c2 + 1) * 2 - 1, cs(c1 - 1, c2 - 1) * 2 - 1)
+            else:
+                tn[i] = (cs(c1 + 2, c2), cs(c1, c2 + 2), cs(c1 - 2, c2), cs(c1, c2 - 2))
+        listk = np.array([[m, n] for m in range(-((l1 + 1) // 2) + 1, l1 // 2 + 1)
+                          for n in range(-((l2 + 1) // 2) + 1, l2 // 2 + 1)], dtype=np.int64)
+    if a2 is None:
+        bz1, bz2 = np.array([2.0 * np.pi / a1[0]]), None
+    else:
+        x = a1[0] * a2[1] - a2[0] * a1[1]
+        bz1 = 2.0 * np.pi * np.array([a2[1] / x, -a2[0] / x])
+        bz2 = 2.0 * np.pi * np.array([-a1[1] / x, a1[0] / x])
+    return dict(list=t["list"], cord=cord, nnlist=t["nnlist"], snlist=t["snlist"], tnlist=tn,
+                plq_cord=None if lat == 3 else t["plq_cord"], listk=listk, a1=a1, a2=a2, bz1=bz1, bz2=bz2)
+
+
+def print_latt(f, p) -> None:
+    """print_latt2d_sub / print_latt1d_sub (src/lattice.f90:146-226, 502-597):
+    the lattice block of dqmc.out, without the PLEVEL2 imj table."""
+    L = lattice_lists(p)
+    w = f.write
+
+    def vec(a):
+        return "".join(_f16_12(float(v)) for v in a)
+
+    def section(title, head, rows, fmt):
+        w(" \n --------------------- \n")
+        w(f" {title} \n --------------------- \n")
+        w(f"{head} \n")
+        for i, r in enumerate(rows, start=1):
+            w(f"{i:6d}" + "".join(fmt.format(int(v)) for v in r) + "\n")
+
+    w("lattice information: \n")
+    w(" primitive lattice  vector a1_p(:) =  " + vec(L["a1"]) + "\n")
+    if L["a2"] is not None:
+        w(" primitive lattice  vector a2_p(:) =  " + vec(L["a2"]) + "\n")
+    w(" primitive reciprocal vector bz1_p / 2pi = " + vec(L["bz1"] / (2.0 * np.pi)) + "\n")
+    if L["bz2"] is not None:
+        w(" primitive reciprocal vector bz2_p / 2pi = " + vec(L["bz2"] / (2.0 * np.pi)) + "\n")
+    section("The lattice sites list", "   i     list(i,:)", L["list"], "{:4d}")
+    section("The lattice sites cord", "   i     cord(i,:)", L["cord"], "{:4d}")
+    section("The lattice nnlist", "   i     nnlist(i,:)", L["nnlist"], "{:4d}")
+    section("The lattice snlist", "   i     snlist(i,:)", L["snlist"], "{:4d}")
+    section("The lattice tnlist", "   i     tnlist(i,:)", L["tnlist"], "{:4d}")
+    if L["plq_cord"] is not None:
+        section("The lattice plq_cord", "   i     plq_cord(:,i)", L["plq_cord"], "{:4d}")
+    section("The momentum listk", "   i     listk(i,:)", L["listk"], "{:4d}")
 
 
 def wrap_step_of(p) -> list:

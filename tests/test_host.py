@@ -256,7 +256,7 @@ def test_dqmc_out_writers():
     dqmc_initial_print(f, p, ws)
     txt = f.getvalue()
     assert " beta   =   4.00\n" in txt and " rhub      =   4.000\n" in txt and " ntdm =     40\n" in txt
-    assert "              21              30               3\n" in txt and txt.endswith("square_lattice\n")
+    assert "              21              30               3\n" in txt and "\nsquare_lattice\nlattice information: \n" in txt
     diags = [dict(max_wrap_error=1e-11, max_phasediff=0.0, avglog10error=-22.0, logcount=2.0, avgexpphasediff=2.0,
                   accepted=30.0, proposed=100.0, accepted_v=0.0, proposed_v=0.0),
              dict(max_wrap_error=3e-11, max_phasediff=1e-14, avglog10error=-21.0, logcount=2.0, avgexpphasediff=2.0,
@@ -280,6 +280,38 @@ def test_dqmc_out_writers():
     out = f.getvalue()
     assert " >>> accep_u     =   0.25000000E+00\n" in out and " >>> Total time spent:     12.50s\n" in out
     assert "The_time_of_ft_delay_update:         0.100s =  50.00%\n" in out
+
+
+@pytest.mark.parametrize("lattice,l1,l2", [(1, 4, 4), (2, 3, 3), (3, 8, 1)])
+def test_print_latt_block(lattice, l1, l2):
+    """The lattice block of dqmc.out (print_latt2d_sub / print_latt1d_sub,
+    src/lattice.f90:146-226, 502-597): every section with one row per site
+    (per cell for listk and plq_cord), the neighbour lists of the library's
+    tables, and the third-neighbour and k lists of the reference's formulas."""
+    import io as pyio
+    import sunhubbardmy_b200 as sb
+    from sunhubbardmy_b200.io import lattice_lists, print_latt
+    p = sb.DqmcParams.make(lattice=lattice, l1=l1, l2=l2, beta=1.0, dtau=0.1, rhub=4.0)
+    f = pyio.StringIO()
+    print_latt(f, p)
+    txt = f.getvalue()
+    N, lq = int(p.ndim), int(p.lq)
+    L = lattice_lists(p)
+    secs = ["list", "cord", "nnlist", "snlist", "tnlist"] + ([] if lattice == 3 else ["plq_cord"]) + ["listk"]
+    for name in secs:
+        assert f" --------------------- \n" in txt and (f"     {name}(" in txt)
+    rows = [ln for ln in txt.splitlines() if ln[:6].strip().isdigit() and len(ln) >= 10]
+    assert len(rows) == 5 * N + (0 if lattice == 3 else lq) + lq
+    # site 1's neighbour rows are the library's tables
+    t = p.tables()
+    nn_row = "     1" + "".join(f"{int(v):4d}" for v in t["nnlist"][0])
+    assert nn_row in txt.splitlines()
+    assert sorted(tuple(k) for k in L["listk"]) == sorted(set(tuple(k) for k in L["listk"])) and len(L["listk"]) == lq
+    if lattice == 1:   # square: third neighbours at +-2 along each axis
+        assert list(L["tnlist"][0]) == [1 + 2 * l2, 3, 1 + (l1 - 2) * l2, l2 - 1]
+        assert " primitive lattice  vector a1_p(:) =    1.000000000000  0.000000000000\n" in txt
+    if lattice == 2:   # honeycomb: reciprocal vectors of a1 = (1/2, -sqrt3/2), a2 = (1/2, sqrt3/2)
+        assert np.allclose(L["bz1"] / (2 * np.pi), [1.0, -1.0 / np.sqrt(3.0)])
 
 
 # the three greps of the reference's timing analysis
