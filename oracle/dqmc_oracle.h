@@ -45,7 +45,7 @@ int32_t  orc_test_seed(int32_t irank);   /* src/dqmc_util.f90:72 under -DTEST */
 
 /* ---------- parameters (src/model_para.f90 &model_para/&ctrl_para) ---------- */
 enum { ORC_SQUARE = 1, ORC_HONEYCOMB = 2, ORC_CHAIN = 3 };
-enum { ORC_FAST = 0, ORC_DELAY = 1, ORC_SUBMATRIX = 2 };
+enum { ORC_FAST = 0, ORC_DELAY = 1, ORC_SUBMATRIX = 2, ORC_SUBMATRIX_G = 3, ORC_SUBMATRIX_G_EXACT = 4 };
 enum { ORC_CHECKERBOARD = 0, ORC_FFT = 1, ORC_DENSE = 2 };
 enum { ORC_HS_EXACT = 0, ORC_HS_GENERAL4 = 1 };
 
@@ -173,7 +173,11 @@ void orc_vconf_get(const orc_chain *c, int32_t *v);
 void orc_vconf_set(orc_chain *c, const int32_t *v);
 /* one projective update of slice nt (family nf for the bond field, nf = 0 for the site field) */
 void orc_proj_update(orc_chain *c, int nt, int nf);
-/* explicit flavour: ORC_SUBMATRIX = submatrix-LR bond update, else the fast one */
+/* explicit flavour of one projective update: ORC_FAST (dqmc_proj_update.f90),
+ * ORC_DELAY (dqmc_proj_update_delay.f90), ORC_SUBMATRIX (submatrix-LR, bond
+ * field; the site field runs fast), ORC_SUBMATRIX_G (-DDELAYG,
+ * dqmc_proj_update_submatrix_G.f90) or ORC_SUBMATRIX_G_EXACT (the same with
+ * the exact inverse of the bond's 2 x 2 block) */
 void orc_proj_update_flavour(orc_chain *c, int nt, int nf, int flavour);
 /* vconf props on an explicit matrix: left ops on N x n2, right ops on n2 x N */
 void orc_vconf_prop(const orc_model *m, const int32_t *vconf, int op, int nt, int nf, int nflag, double *g, int n2);

@@ -472,6 +472,374 @@ static void proj_update_u(orc_chain *c, int nt) {
     free(vk_tmp); free(vk); free(uk); free(lruk);
 }
 
+/* G = I - UR (ULRINV UL) of the current walker (gmmat of the delayed updates) */
+static void proj_gmat(const orc_chain *c, zc *gm) {
+    const orc_model *m = c->m;
+    int N = m->ndim, ne = m->ne;
+    zc *lu = zalloc((size_t)ne * N);
+    orc_zgemm('N', 'N', ne, N, ne, 1.0, c->ULRINV, ne, c->UL, ne, 0.0, lu, ne);
+    for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i) gm[ZIDX(i, j, N)] = (i == j) ? 1.0 : 0.0;
+    orc_zgemm('N', 'N', N, N, ne, -1.0, c->UR, N, lu, ne, 1.0, gm, N);
+    free(lu);
+}
+
+/* end of a delayed or submatrix-G sweep over one family: UR = urrecord and
+ * ULRINV = (UL UR)^-1 by LU (s_invlu_z) */
+static void proj_close(orc_chain *c, const zc *urrecord) {
+    const orc_model *m = c->m;
+    memcpy(c->UR, urrecord, sizeof(zc) * (size_t)m->ndim * m->ne);
+    ulr_inverse(m->ndim, m->ne, c->UL, c->UR, c->ULRINV, NULL);
+}
+
+/* dqmc_proj_update, site field, delayed flavour
+ * (src/dqmc_config_u/dqmc_proj_update_delay.f90): rank-1 changes of G are
+ * carried in avec/bvec and flushed every nublock accepts, the diagonal of G
+ * is tracked, UR rows are scaled per accept, and ULRINV is rebuilt at the end */
+static void proj_update_u_delay(orc_chain *c, int nt) {
+    const orc_model *m = c->m;
+    int N = m->ndim, ne = m->ne, lc = m->lcomp, nb = m->nublock > 0 ? m->nublock : 1;
+    int32_t *cf = c->conf + (size_t)(nt - 1) * N;
+    zc *gm = zalloc((size_t)N * N), *av = zalloc((size_t)N * nb), *bv = zalloc((size_t)N * nb);
+    zc *dg = zalloc(N), *urr = zalloc((size_t)N * ne);
+    memcpy(urr, c->UR, sizeof(zc) * (size_t)N * ne);
+    proj_gmat(c, gm);
+    for (int i = 0; i < N; ++i) dg[i] = gm[ZIDX(i, i, N)];
+    double accm = 0.0;
+    int ik = 0;
+    for (int i = 0; i < N; ++i) {
+        int is = cf[i];
+        int iflip = (int)ceil(orc_sfmt_stream(&c->rng) * (lc - 1));
+        int isp = (is + iflip - 1) % lc + 1;
+        zc d = m->delta[(is - 1) * (lc - 1) + iflip - 1];
+        zc ratio1 = (1.0 - dg[i]) * d + 1.0;
+        zc sscl = d / ratio1;
+        zc ratiotot = orc_total_ratio(m, ratio1, is, iflip, isp);
+        double ratio_re = creal(ratiotot * c->phase) / creal(c->phase);
+        double ratio_abs = ratio_re < 0 ? -ratio_re : ratio_re;
+        double random = orc_sfmt_stream(&c->rng);
+        ORC_COUNT_TIE(c, ratio_abs, random);
+        if (ratio_abs > random) {
+            accm += 1.0;
+            double weight = sqrt(creal(ratiotot * conj(ratiotot)));
+            c->phase = c->phase * ratiotot / weight;
+            zc *a = av + (size_t)ik * N, *b = bv + (size_t)ik * N;
+            for (int r = 0; r < N; ++r) { a[r] = gm[ZIDX(r, i, N)]; b[r] = gm[ZIDX(i, r, N)]; }
+            for (int q = 0; q < ik; ++q) {
+                zc bq = bv[(size_t)q * N + i], aq = av[(size_t)q * N + i];
+                for (int r = 0; r < N; ++r) {
+                    a[r] += bq * av[(size_t)q * N + r];
+                    b[r] += aq * bv[(size_t)q * N + r];
+                }
+            }
+            for (int r = 0; r < N; ++r) a[r] *= sscl;
+            b[i] -= 1.0;
+            for (int r = 0; r < N; ++r) dg[r] += a[r] * b[r];
+            for (int l = 0; l < ne; ++l) urr[ZIDX(i, l, N)] += d * urr[ZIDX(i, l, N)];
+            cf[i] = isp;
+            ++ik;
+        }
+        if (ik == nb && i < N - 1) {
+            orc_zgemm('N', 'T', N, N, nb, 1.0, av, N, bv, N, 1.0, gm, N);
+            for (int r = 0; r < N; ++r) dg[r] = gm[ZIDX(r, r, N)];
+            memset(av, 0, sizeof(zc) * (size_t)N * nb);
+            memset(bv, 0, sizeof(zc) * (size_t)N * nb);
+            ik = 0;
+        }
+    }
+    proj_close(c, urr);
+    c->acc_u += accm;
+    c->prop_u += N;
+    free(gm); free(av); free(bv); free(dg); free(urr);
+}
+
+/* dqmc_proj_update, bond field, delayed flavour
+ * (src/dqmc_config_v/dqmc_proj_update_delay.f90): per accepted bond two
+ * delayed columns avec = [G(:,i1) G(:,i2)] S and bvec = [G(i1,:) G(i2,:)]^T - e,
+ * S = diag(dp, dm) (I + vukmat)^-1, flushed every nublock columns */
+static void proj_update_v_delay(orc_chain *c, int nt, int nf) {
+    const orc_model *m = c->m;
+    const orc_latt *L = &m->L;
+    int N = m->ndim, ne = m->ne, nnf = L->nn_nf, lf = L->nn_lf;
+    int nb = m->nublock > 1 ? m->nublock : 2;
+    nb -= nb % 2;
+    int32_t *cf = c->vconf + ((size_t)(nt - 1) * nnf + (nf - 1)) * N;
+    zc *gm = zalloc((size_t)N * N), *av = zalloc((size_t)N * nb), *bv = zalloc((size_t)N * nb);
+    zc *g1 = zalloc(N), *g2 = zalloc(N), *urr = zalloc((size_t)N * ne);
+    memcpy(urr, c->UR, sizeof(zc) * (size_t)N * ne);
+    proj_gmat(c, gm);
+    double accm = 0.0;
+    int ik = 0;
+    for (int b = 0; b < lf; ++b) {
+        int i1 = L->nnlf_list[b] - 1;
+        int i2 = L->nnlist[i1 * nnf + nf - 1] - 1;
+        int is = cf[b];
+        int iflip = (int)ceil(orc_sfmt_stream(&c->rng) * 1);
+        int isp = (is + iflip - 1) % 2 + 1;
+        zc gp[4];   /* gpart column-major: (1,1) (2,1) (1,2) (2,2) */
+        gp[0] = gm[ZIDX(i1, i1, N)]; gp[1] = gm[ZIDX(i2, i1, N)];
+        gp[2] = gm[ZIDX(i1, i2, N)]; gp[3] = gm[ZIDX(i2, i2, N)];
+        for (int q = 0; q < ik; ++q) {
+            const zc *a = av + (size_t)q * N, *bb = bv + (size_t)q * N;
+            gp[0] += a[i1] * bb[i1]; gp[2] += a[i1] * bb[i2];
+            gp[1] += a[i2] * bb[i1]; gp[3] += a[i2] * bb[i2];
+        }
+        zc dp = m->vdp[is - 1], dm = m->vdm[is - 1];
+        zc v[4];
+        v[0] = (1.0 - gp[0]) * dp + 1.0; v[2] = -gp[2] * dm;
+        v[1] = -gp[1] * dp;              v[3] = (1.0 - gp[3]) * dm + 1.0;
+        zc ratio1 = v[0] * v[3] - v[2] * v[1];
+        zc inv[4] = {v[3] / ratio1, -v[1] / ratio1, -v[2] / ratio1, v[0] / ratio1};
+        zc sm[4];   /* smat = diag(dp, dm) inv */
+        sm[0] = dp * inv[0]; sm[2] = dp * inv[2];
+        sm[1] = dm * inv[1]; sm[3] = dm * inv[3];
+        zc ratiotot = ratio1;
+        double ratio_re = creal(ratiotot * c->phase) / creal(c->phase);
+        double ratio_abs = ratio_re < 0 ? -ratio_re : ratio_re;
+        double random = orc_sfmt_stream(&c->rng);
+        ORC_COUNT_TIE(c, ratio_abs, random);
+        if (ratio_abs > random) {
+            accm += 1.0;
+            double weight = sqrt(creal(ratiotot * conj(ratiotot)));
+            c->phase = c->phase * ratiotot / weight;
+            zc *b1 = bv + (size_t)ik * N, *b2 = bv + (size_t)(ik + 1) * N;
+            for (int r = 0; r < N; ++r) {
+                g1[r] = gm[ZIDX(r, i1, N)]; g2[r] = gm[ZIDX(r, i2, N)];
+                b1[r] = gm[ZIDX(i1, r, N)]; b2[r] = gm[ZIDX(i2, r, N)];
+            }
+            b1[i1] = gm[ZIDX(i1, i1, N)] - 1.0;
+            b2[i2] = gm[ZIDX(i2, i2, N)] - 1.0;
+            for (int q = 0; q < ik; ++q) {
+                const zc *a = av + (size_t)q * N, *bb = bv + (size_t)q * N;
+                zc bq1 = bb[i1], bq2 = bb[i2], aq1 = a[i1], aq2 = a[i2];
+                for (int r = 0; r < N; ++r) {
+                    g1[r] += a[r] * bq1;
+                    g2[r] += a[r] * bq2;
+                    b1[r] += aq1 * bb[r];
+                    b2[r] += aq2 * bb[r];
+                }
+            }
+            zc *a1 = av + (size_t)ik * N, *a2 = av + (size_t)(ik + 1) * N;
+            for (int r = 0; r < N; ++r) {
+                a1[r] = g1[r] * sm[0] + g2[r] * sm[1];
+                a2[r] = g1[r] * sm[2] + g2[r] * sm[3];
+            }
+            for (int l = 0; l < ne; ++l) {
+                urr[ZIDX(i1, l, N)] += dp * urr[ZIDX(i1, l, N)];
+                urr[ZIDX(i2, l, N)] += dm * urr[ZIDX(i2, l, N)];
+            }
+            cf[b] = isp;
+            ik += 2;
+        }
+        if (ik == nb && b < lf - 1) {
+            orc_zgemm('N', 'T', N, N, nb, 1.0, av, N, bv, N, 1.0, gm, N);
+            memset(av, 0, sizeof(zc) * (size_t)N * nb);
+            memset(bv, 0, sizeof(zc) * (size_t)N * nb);
+            ik = 0;
+        }
+    }
+    proj_close(c, urr);
+    c->acc_v += accm;
+    c->prop_v += lf;
+    free(gm); free(av); free(bv); free(g1); free(g2); free(urr);
+}
+
+/* dqmc_proj_update, site field, submatrix-G flavour
+ * (src/dqmc_config_u/dqmc_proj_update_submatrix_G.f90): F = UR ULRINV UL,
+ * the ratio from F(i,i) - F(i,A) Gammainv F(A,i), Gammainv bordered per accept,
+ * F -= F(:,A) Gammainv F(A,:) every nublock accepts */
+static void proj_update_u_subg(orc_chain *c, int nt) {
+    const orc_model *m = c->m;
+    int N = m->ndim, ne = m->ne, lc = m->lcomp, nb = m->nublock > 0 ? m->nublock : 1;
+    int32_t *cf = c->conf + (size_t)(nt - 1) * N;
+    zc *F = zalloc((size_t)N * N), *gi = zalloc((size_t)nb * nb), *cv = zalloc(nb), *bvv = zalloc(nb);
+    zc *v1 = zalloc(nb), *v4 = zalloc(nb), *t1 = zalloc((size_t)N * nb), *t2 = zalloc((size_t)nb * N);
+    zc *G1 = zalloc((size_t)N * nb), *urr = zalloc((size_t)N * ne);
+    int *pv = calloc(nb, sizeof(int));
+    memcpy(urr, c->UR, sizeof(zc) * (size_t)N * ne);
+    proj_gmat(c, F);
+    for (int j = 0; j < N; ++j)          /* F = I - G */
+        for (int i = 0; i < N; ++i) F[ZIDX(i, j, N)] = (i == j ? 1.0 : 0.0) - F[ZIDX(i, j, N)];
+    double accm = 0.0;
+    int ik = 0;
+    for (int i = 0; i < N; ++i) {
+        int is = cf[i];
+        int iflip = (int)ceil(orc_sfmt_stream(&c->rng) * (lc - 1));
+        int isp = (is + iflip - 1) % lc + 1;
+        zc d = m->delta[(is - 1) * (lc - 1) + iflip - 1];
+        for (int q = 0; q < ik; ++q) { cv[q] = F[ZIDX(i, pv[q], N)]; bvv[q] = F[ZIDX(pv[q], i, N)]; }
+        zc v = 0.0;
+        for (int q = 0; q < ik; ++q) {
+            zc s2 = 0.0;
+            for (int r = 0; r < ik; ++r) s2 += cv[r] * gi[ZIDX(r, q, nb)];
+            v1[q] = s2;
+        }
+        for (int q = 0; q < ik; ++q) v += v1[q] * bvv[q];
+        zc v2 = F[ZIDX(i, i, N)] - v;
+        zc ratio1 = v2 * d + 1.0;
+        zc ratiotot = orc_total_ratio(m, ratio1, is, iflip, isp);
+        double ratio_re = creal(ratiotot * c->phase) / creal(c->phase);
+        double ratio_abs = ratio_re < 0 ? -ratio_re : ratio_re;
+        double random = orc_sfmt_stream(&c->rng);
+        ORC_COUNT_TIE(c, ratio_abs, random);
+        if (ratio_abs > random) {
+            accm += 1.0;
+            double weight = sqrt(creal(ratiotot * conj(ratiotot)));
+            c->phase = c->phase * ratiotot / weight;
+            zc v3 = 1.0 / (-v + 1.0 / d + F[ZIDX(i, i, N)]);
+            for (int q = 0; q < ik; ++q) {
+                zc s2 = 0.0;
+                for (int r = 0; r < ik; ++r) s2 += gi[ZIDX(q, r, nb)] * bvv[r];
+                v4[q] = s2;
+            }
+            for (int q = 0; q < ik; ++q) {
+                gi[ZIDX(ik, q, nb)] = -v3 * v1[q];
+                gi[ZIDX(q, ik, nb)] = -v4[q] * v3;
+            }
+            for (int r = 0; r < ik; ++r)
+                for (int q = 0; q < ik; ++q) gi[ZIDX(q, r, nb)] += v4[q] * v3 * v1[r];
+            gi[ZIDX(ik, ik, nb)] = v3;
+            pv[ik] = i;
+            for (int l = 0; l < ne; ++l) urr[ZIDX(i, l, N)] += d * urr[ZIDX(i, l, N)];
+            for (int r = 0; r < N; ++r) { t1[ZIDX(r, ik, N)] = F[ZIDX(r, i, N)]; t2[ZIDX(ik, r, nb)] = F[ZIDX(i, r, N)]; }
+            cf[i] = isp;
+            ++ik;
+        }
+        if (ik == nb && i < N - 1) {
+            orc_zgemm('N', 'N', N, nb, ik, 1.0, t1, N, gi, nb, 0.0, G1, N);
+            orc_zgemm('N', 'N', N, N, ik, -1.0, G1, N, t2, nb, 1.0, F, N);
+            memset(gi, 0, sizeof(zc) * (size_t)nb * nb);
+            ik = 0;
+        }
+    }
+    proj_close(c, urr);
+    c->acc_u += accm;
+    c->prop_u += N;
+    free(F); free(gi); free(cv); free(bvv); free(v1); free(v4); free(t1); free(t2); free(G1); free(urr); free(pv);
+}
+
+/* dqmc_proj_update, bond field, submatrix-G flavour
+ * (src/dqmc_config_v/dqmc_proj_update_submatrix_G.f90): the site-field scheme
+ * with 2 x 2 blocks per bond (rows/columns i1, i2).  exact = 0 inverts the
+ * accepted bond's 2 x 2 block v5 = [[a, b], [c, d]] with the reference's
+ * expressions (submatrix_G.f90 v3(:,:)), whose (2,1) entry
+ * -(1/a) c / (a - c b / d) equals the true -c / (ad - bc) only when a = d;
+ * exact = 1 uses the true inverse, which is what the fast, delayed and
+ * submatrix-LR flavours (and the GPU) amount to. */
+static void proj_update_v_subg(orc_chain *c, int nt, int nf, int exact) {
+    const orc_model *m = c->m;
+    const orc_latt *L = &m->L;
+    int N = m->ndim, ne = m->ne, nnf = L->nn_nf, lf = L->nn_lf;
+    int nb = m->nublock > 1 ? m->nublock : 2;
+    nb -= nb % 2;
+    int32_t *cf = c->vconf + ((size_t)(nt - 1) * nnf + (nf - 1)) * N;
+    zc *F = zalloc((size_t)N * N), *gi = zalloc((size_t)nb * nb), *cv = zalloc(2 * (size_t)nb), *bvv = zalloc(2 * (size_t)nb);
+    zc *v1 = zalloc(2 * (size_t)nb), *v4 = zalloc(2 * (size_t)nb), *t1 = zalloc((size_t)N * nb), *t2 = zalloc((size_t)nb * N);
+    zc *G1 = zalloc((size_t)N * nb), *urr = zalloc((size_t)N * ne);
+    int *pv = calloc(nb, sizeof(int));
+    memcpy(urr, c->UR, sizeof(zc) * (size_t)N * ne);
+    proj_gmat(c, F);
+    for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i) F[ZIDX(i, j, N)] = (i == j ? 1.0 : 0.0) - F[ZIDX(i, j, N)];
+    double accm = 0.0;
+    int ik = 0;
+    for (int b = 0; b < lf; ++b) {
+        int i1 = L->nnlf_list[b] - 1;
+        int i2 = L->nnlist[i1 * nnf + nf - 1] - 1;
+        int is = cf[b];
+        int iflip = (int)ceil(orc_sfmt_stream(&c->rng) * 1);
+        int isp = (is + iflip - 1) % 2 + 1;
+        const int ii[2] = {i1, i2};
+        /* cvec (2 x ik) = F(ii, A), bvec (ik x 2) = F(A, ii) */
+        for (int q = 0; q < ik; ++q)
+            for (int x = 0; x < 2; ++x) { cv[ZIDX(x, q, 2)] = F[ZIDX(ii[x], pv[q], N)]; bvv[ZIDX(q, x, nb)] = F[ZIDX(pv[q], ii[x], N)]; }
+        /* v1 = cvec Gammainv (2 x ik), v = v1 bvec (2 x 2) */
+        for (int q = 0; q < ik; ++q)
+            for (int x = 0; x < 2; ++x) {
+                zc s2 = 0.0;
+                for (int r = 0; r < ik; ++r) s2 += cv[ZIDX(x, r, 2)] * gi[ZIDX(r, q, nb)];
+                v1[ZIDX(x, q, 2)] = s2;
+            }
+        zc v[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int y = 0; y < 2; ++y)
+            for (int x = 0; x < 2; ++x)
+                for (int q = 0; q < ik; ++q) v[x + 2 * y] += v1[ZIDX(x, q, 2)] * bvv[ZIDX(q, y, nb)];
+        zc dp = m->vdp[is - 1], dm = m->vdm[is - 1];
+        zc w2[4];
+        w2[0] = dp * (-v[0] + F[ZIDX(i1, i1, N)]) + 1.0; w2[2] = dm * (-v[2] + F[ZIDX(i1, i2, N)]);
+        w2[1] = dp * (-v[1] + F[ZIDX(i2, i1, N)]);       w2[3] = dm * (-v[3] + F[ZIDX(i2, i2, N)]) + 1.0;
+        zc ratio1 = w2[0] * w2[3] - w2[2] * w2[1];
+        zc ratiotot = ratio1;
+        double ratio_re = creal(ratiotot * c->phase) / creal(c->phase);
+        double ratio_abs = ratio_re < 0 ? -ratio_re : ratio_re;
+        double random = orc_sfmt_stream(&c->rng);
+        ORC_COUNT_TIE(c, ratio_abs, random);
+        if (ratio_abs > random) {
+            accm += 1.0;
+            double weight = sqrt(creal(ratiotot * conj(ratiotot)));
+            c->phase = c->phase * ratiotot / weight;
+            /* v5 = diag(1/dp, 1/dm) + F(ii,ii) - v; v3 = v5^-1 by the reference's
+             * block formulas */
+            zc v5[4];
+            v5[0] = 1.0 / dp + F[ZIDX(i1, i1, N)] - v[0]; v5[2] = F[ZIDX(i1, i2, N)] - v[2];
+            v5[1] = F[ZIDX(i2, i1, N)] - v[1];           v5[3] = 1.0 / dm + F[ZIDX(i2, i2, N)] - v[3];
+            zc v3[4];
+            zc s11 = 1.0 / v5[0], s22 = 1.0 / v5[3];
+            zc sc1 = 1.0 / (v5[3] - s11 * v5[2] * v5[1]);
+            zc sc2 = 1.0 / (v5[0] - s22 * v5[1] * v5[2]);
+            v3[0] = s11 + s11 * v5[2] * sc1 * s11 * v5[1];
+            v3[2] = -s11 * v5[2] * sc1;
+            v3[1] = -s11 * v5[1] * sc2;
+            v3[3] = sc1;
+            if (exact) {
+                zc det5 = v5[0] * v5[3] - v5[2] * v5[1];
+                v3[0] = v5[3] / det5; v3[2] = -v5[2] / det5;
+                v3[1] = -v5[1] / det5; v3[3] = v5[0] / det5;
+            }
+            /* v4 = Gammainv bvec (ik x 2) with the old Gammainv */
+            for (int y = 0; y < 2; ++y)
+                for (int q = 0; q < ik; ++q) {
+                    zc s2 = 0.0;
+                    for (int r = 0; r < ik; ++r) s2 += gi[ZIDX(q, r, nb)] * bvv[ZIDX(r, y, nb)];
+                    v4[ZIDX(q, y, nb)] = s2;
+                }
+            const int n0 = ik;
+            for (int y = 0; y < 2; ++y)
+                for (int x = 0; x < 2; ++x) gi[ZIDX(n0 + x, n0 + y, nb)] = v3[x + 2 * y];
+            for (int q = 0; q < n0; ++q)
+                for (int x = 0; x < 2; ++x) {
+                    gi[ZIDX(n0 + x, q, nb)] = -(v3[x] * v1[ZIDX(0, q, 2)] + v3[x + 2] * v1[ZIDX(1, q, 2)]);
+                    gi[ZIDX(q, n0 + x, nb)] = -(v4[ZIDX(q, 0, nb)] * v3[2 * x] + v4[ZIDX(q, 1, nb)] * v3[1 + 2 * x]);
+                }
+            for (int r = 0; r < n0; ++r)
+                for (int q = 0; q < n0; ++q)
+                    gi[ZIDX(q, r, nb)] -= v4[ZIDX(q, 0, nb)] * gi[ZIDX(n0, r, nb)] + v4[ZIDX(q, 1, nb)] * gi[ZIDX(n0 + 1, r, nb)];
+            pv[n0] = i1; pv[n0 + 1] = i2;
+            for (int l = 0; l < ne; ++l) {
+                urr[ZIDX(i1, l, N)] += dp * urr[ZIDX(i1, l, N)];
+                urr[ZIDX(i2, l, N)] += dm * urr[ZIDX(i2, l, N)];
+            }
+            for (int r = 0; r < N; ++r)
+                for (int x = 0; x < 2; ++x) {
+                    t1[ZIDX(r, n0 + x, N)] = F[ZIDX(r, ii[x], N)];
+                    t2[ZIDX(n0 + x, r, nb)] = F[ZIDX(ii[x], r, N)];
+                }
+            cf[b] = isp;
+            ik += 2;
+        }
+        if (ik == nb && b < lf - 1) {
+            orc_zgemm('N', 'N', N, nb, ik, 1.0, t1, N, gi, nb, 0.0, G1, N);
+            orc_zgemm('N', 'N', N, N, ik, -1.0, G1, N, t2, nb, 1.0, F, N);
+            memset(gi, 0, sizeof(zc) * (size_t)nb * nb);
+            ik = 0;
+        }
+    }
+    proj_close(c, urr);
+    c->acc_v += accm;
+    c->prop_v += lf;
+    free(F); free(gi); free(cv); free(bvv); free(v1); free(v4); free(t1); free(t2); free(G1); free(urr); free(pv);
+}
+
 /* the build's update flavour: -DSUBMATRIX selects the submatrix-LR bond
  * update, every other flavour the fast one (same accept sequence) */
 static void proj_update_bond(orc_chain *c, int nt, int nf) {
@@ -485,9 +853,17 @@ void orc_proj_update(orc_chain *c, int nt, int nf) {
 }
 
 void orc_proj_update_flavour(orc_chain *c, int nt, int nf, int flavour) {
-    if (nf > 0 && flavour == ORC_SUBMATRIX) proj_update_v_lr(c, nt, nf);
-    else if (nf > 0) proj_update_v(c, nt, nf);
-    else proj_update_u(c, nt);
+    if (nf > 0) {
+        if (flavour == ORC_SUBMATRIX) proj_update_v_lr(c, nt, nf);
+        else if (flavour == ORC_DELAY) proj_update_v_delay(c, nt, nf);
+        else if (flavour == ORC_SUBMATRIX_G) proj_update_v_subg(c, nt, nf, 0);
+        else if (flavour == ORC_SUBMATRIX_G_EXACT) proj_update_v_subg(c, nt, nf, 1);
+        else proj_update_v(c, nt, nf);
+    } else {
+        if (flavour == ORC_DELAY) proj_update_u_delay(c, nt);
+        else if (flavour == ORC_SUBMATRIX_G || flavour == ORC_SUBMATRIX_G_EXACT) proj_update_u_subg(c, nt);
+        else proj_update_u(c, nt);
+    }
 }
 
 /* h0 half step on UR (left op) and UL (right op), families in order or reversed */

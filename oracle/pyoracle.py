@@ -22,7 +22,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
 
 SQUARE, HONEYCOMB, CHAIN = 1, 2, 3
-FAST, DELAY, SUBMATRIX = 0, 1, 2
+FAST, DELAY, SUBMATRIX, SUBMATRIX_G, SUBMATRIX_G_EXACT = 0, 1, 2, 3, 4
 CHECKERBOARD, FFT, DENSE = 0, 1, 2
 HS_EXACT, HS_GENERAL4 = 0, 1
 LEFT_FORWARD, LEFT_BACKWARD, RIGHT_FORWARD, RIGHT_BACKWARD, LEFT_FORWARD_HC = range(5)

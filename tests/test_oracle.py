@@ -449,6 +449,60 @@ def test_projective_update_flavours_agree(oracle):
         assert a.diag()["accepted_v"] == b.diag()["accepted_v"] > 0
 
 
+PROJ_U = dict(lattice=1, l1=4, l2=4, beta=2.0, dtau=0.1, rv=0.0, rhub=4.0, nflr=2, kinetic=0, nwrap=5, proj=1,
+              rndness=0.05, hs=0, mu=0.0)
+
+
+@pytest.mark.parametrize("field,flavour", [("bond", "DELAY"), ("bond", "SUBMATRIX_G_EXACT"), ("site", "DELAY"),
+                                           ("site", "SUBMATRIX_G")])
+def test_projective_delay_flavours(oracle, field, flavour):
+    """The delayed (dqmc_proj_update_delay.f90) and submatrix-G
+    (dqmc_proj_update_submatrix_G.f90, -DDELAYG) projective updates of both
+    fields against the fast flavour over three slices: same fields and accept
+    counts, UR and (UL UR)^-1 to rounding.  For the bond field the
+    submatrix-G flavour is taken with the exact inverse of the bond's 2 x 2
+    block; the reference's own expressions for that inverse give different
+    ratios (test_reference_delayg_block_inverse)."""
+    f = getattr(oracle, flavour)
+    kw0 = PROJ_TV if field == "bond" else PROJ_U
+    nfs = (1, 2, 3) if field == "bond" else (0,)
+    for nub in (2, 4, 8, 16):
+        m = oracle.Model(**dict(kw0, nublock=nub))
+        a = oracle.Chain(m, 11)
+        b = oracle.Chain(m, 11)
+        a.proj_sweep_start(); b.proj_sweep_start()
+        for nt in (m.ltrot, m.ltrot - 1, m.ltrot - 2):
+            for nf in nfs:
+                a.proj_update(nt, nf, flavour=oracle.FAST)
+                b.proj_update(nt, nf, flavour=f)
+        key = "accepted_v" if field == "bond" else "accepted"
+        assert np.array_equal(a.vconf(), b.vconf()) and np.array_equal(a.conf(), b.conf())
+        for x, y in zip(a.proj_state(), b.proj_state()):
+            assert np.max(np.abs(x - y)) < 1e-11 * max(1.0, np.max(np.abs(y)))
+        assert a.diag()[key] == b.diag()[key] > 0
+
+
+def test_reference_delayg_block_inverse():
+    """The bond-field submatrix-G update inverts the accepted bond's 2 x 2 block
+    v5 = [[a, b], [c, d]] with v3(1,1) = 1/a + (1/a) b (1/(d - b c / a)) (1/a) c,
+    v3(1,2) = -(1/a) b / (d - b c / a), v3(2,1) = -(1/a) c / (a - c b / d),
+    v3(2,2) = 1 / (d - b c / a) (src/dqmc_config_v/dqmc_proj_update_submatrix_G.f90).
+    Three entries are those of the inverse; the (2,1) entry is the inverse's
+    -c / (ad - bc) times d / a, so the flavour's later ratios in a block
+    differ from the other flavours' unless a = d (they are 1/dp + ... and
+    1/dm + ..., which differ for the t-V field)."""
+    rng = np.random.default_rng(0)
+    a, b, c, d = rng.normal(size=4) + 1j * rng.normal(size=4)
+    v3 = np.array([[1 / a + (1 / a) * b * (1 / (d - (1 / a) * b * c)) * (1 / a) * c, -(1 / a) * b / (d - (1 / a) * b * c)],
+                   [-(1 / a) * c / (a - (1 / d) * c * b), 1 / (d - (1 / a) * b * c)]])
+    inv = np.linalg.inv(np.array([[a, b], [c, d]]))
+    assert abs(v3[0, 0] - inv[0, 0]) < 1e-12 and abs(v3[0, 1] - inv[0, 1]) < 1e-12 and abs(v3[1, 1] - inv[1, 1]) < 1e-12
+    assert abs(v3[1, 0] - inv[1, 0] * d / a) < 1e-12 and abs(v3[1, 0] - inv[1, 0]) > 1e-3
+    # a = d: the expressions agree with the inverse
+    v3s = np.array([[0, 0], [-(1 / a) * c / (a - (1 / a) * c * b), 0]])
+    assert abs(v3s[1, 0] - np.linalg.inv(np.array([[a, b], [c, a]]))[1, 0]) < 1e-12
+
+
 def test_projective_sweeps_wrap_error(oracle):
     """Two sweeps of the t-V projector with updates keep the wrap error and the
     phase difference at the rounding level."""
