@@ -96,6 +96,8 @@ struct HostModel {
     std::vector<zc> urt, urtm1;           // [bond][4]
     std::vector<zc> exph0k, exph0kinv;    // divided by lq
     std::vector<zc> urtd, urtm1d;         // dense kinetic exp(-+dtau H0 / 2), N x N
+    bool dense_on_device = false;         // dense kinetic: keep seth0 and build urtd on the device
+    std::vector<zc> seth0;                // the hopping matrix of the dense kinetic term (device build)
     std::vector<int> bond_i1, bond_i2;
     std::vector<int> cell_plus;           // [d][j]
     ModelDev dev;                         // host copy with device pointers
@@ -337,23 +339,27 @@ static int build_model(HostModel& m) {
             }
         }
         for (int i = 0; i < N; ++i) H[i + (size_t)i * N] -= p.mu;
-        std::vector<double> w;
-        eig_herm(N, H, w);
-        m.urtd.assign((size_t)N * N, 0.0);
-        m.urtm1d.assign((size_t)N * N, 0.0);
-        std::vector<double> em(N), ep(N);
-        for (int k = 0; k < N; ++k) { em[k] = std::exp(-0.5 * p.dtau * w[k]); ep[k] = std::exp(0.5 * p.dtau * w[k]); }
-        for (int j = 0; j < N; ++j)
-            for (int i = 0; i < N; ++i) {
-                zc z0 = 0, z1 = 0;
-                for (int k = 0; k < N; ++k) {
-                    zc t = H[i + (size_t)k * N] * std::conj(H[j + (size_t)k * N]);
-                    z0 += t * em[k];
-                    z1 += t * ep[k];
+        if (m.dense_on_device) {
+            m.seth0 = std::move(H);       // upload_model diagonalises it on the device
+        } else {
+            std::vector<double> w;
+            eig_herm(N, H, w);
+            m.urtd.assign((size_t)N * N, 0.0);
+            m.urtm1d.assign((size_t)N * N, 0.0);
+            std::vector<double> em(N), ep(N);
+            for (int k = 0; k < N; ++k) { em[k] = std::exp(-0.5 * p.dtau * w[k]); ep[k] = std::exp(0.5 * p.dtau * w[k]); }
+            for (int j = 0; j < N; ++j)
+                for (int i = 0; i < N; ++i) {
+                    zc z0 = 0, z1 = 0;
+                    for (int k = 0; k < N; ++k) {
+                        zc t = H[i + (size_t)k * N] * std::conj(H[j + (size_t)k * N]);
+                        z0 += t * em[k];
+                        z1 += t * ep[k];
+                    }
+                    m.urtd[i + (size_t)j * N] = z0;
+                    m.urtm1d[i + (size_t)j * N] = z1;
                 }
-                m.urtd[i + (size_t)j * N] = z0;
-                m.urtm1d[i + (size_t)j * N] = z1;
-            }
+        }
     }
     if (p.kinetic == DQMC_KIN_FFT) {
         // eigenvalues h0k = diag(F H F^-1), F the unitary forward DFT over (l1, l2)
@@ -529,7 +535,16 @@ static int upload_model(HostModel& m) {
     std::vector<double2> t;
     t = to_d2(m.urt); if ((rc = upload(m, t, &d.urt))) return rc;
     t = to_d2(m.urtm1); if ((rc = upload(m, t, &d.urtm1))) return rc;
-    if (p.kinetic == DQMC_KIN_DENSE) {
+    if (p.kinetic == DQMC_KIN_DENSE && m.dense_on_device) {
+        // urt / urtm1 from the device eigen-decomposition of seth0
+        std::vector<double2> z((size_t)m.N * m.N, make_double2(0.0, 0.0));
+        if ((rc = upload(m, z, &d.urtd))) return rc;
+        if ((rc = upload(m, z, &d.urtm1d))) return rc;
+        std::vector<double2> H = to_d2(m.seth0);
+        const int sw = dense_kinetic_device(H.data(), m.N, p.dtau, (double2*)d.urtd, (double2*)d.urtm1d, nullptr);
+        if (sw == -2) return fail(DQMC_ENUMERIC, "the seth0 eigensolver did not converge");
+        if (sw < 0) return fail(DQMC_ECUDA, "device eigensolver of seth0 failed");
+    } else if (p.kinetic == DQMC_KIN_DENSE) {
         t = to_d2(m.urtd); if ((rc = upload(m, t, &d.urtd))) return rc;
         t = to_d2(m.urtm1d); if ((rc = upload(m, t, &d.urtm1d))) return rc;
     }
@@ -975,6 +990,7 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
         model_of[k] = (int)h->models.size();
         HostModel* m = new HostModel();
         m->p = params[k];
+        m->dense_on_device = true;
         if ((rc = dqmc_params_derive(&m->p))) { delete m; dqmc_gpu_destroy(h); return rc; }
         if ((rc = build_model(*m))) { delete m; dqmc_gpu_destroy(h); return rc; }
         h->models.push_back(m);
@@ -1115,15 +1131,31 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
         cudaMemcpy(d.stats, stats, sizeof(stats), cudaMemcpyHostToDevice);
     }
     if (h->proj) {
-        // eigenvectors of every walker's trial Hamiltonian, on the host cores
-        unsigned nth = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+        // eigenvectors of every walker's trial Hamiltonian (set_trial_h0): one
+        // batched device eigensolve per lattice size
         std::vector<std::vector<double>> ws(n_chains);
-        std::vector<std::thread> pool;
-        for (unsigned t = 0; t < nth; ++t)
-            pool.emplace_back([&, t]() {
-                for (int c = (int)t; c < n_chains; c += (int)nth) eig_herm(h->chains[c].dev.N, trial_H[c], ws[c]);
-            });
-        for (auto& th : pool) th.join();
+        std::vector<int> sizes;
+        for (int c = 0; c < n_chains; ++c)
+            if (std::find(sizes.begin(), sizes.end(), h->chains[c].dev.N) == sizes.end()) sizes.push_back(h->chains[c].dev.N);
+        for (int Nb : sizes) {
+            std::vector<int> cs;
+            for (int c = 0; c < n_chains; ++c) if (h->chains[c].dev.N == Nb) cs.push_back(c);
+            const size_t nn = (size_t)Nb * Nb;
+            std::vector<double2> Hb(nn * cs.size()), Vb(nn * cs.size());
+            std::vector<double> wb((size_t)Nb * cs.size());
+            for (size_t q = 0; q < cs.size(); ++q)
+                memcpy(&Hb[q * nn], trial_H[cs[q]].data(), nn * sizeof(double2));
+            const int sw = eig_herm_device(Hb.data(), Nb, (int)cs.size(), Vb.data(), wb.data(), h->st);
+            if (sw < 0) {
+                dqmc_gpu_destroy(h);
+                return sw == -2 ? fail(DQMC_ENUMERIC, "the trial-state eigensolver did not converge")
+                                : fail(DQMC_ECUDA, "device eigensolver of the trial states failed");
+            }
+            for (size_t q = 0; q < cs.size(); ++q) {
+                memcpy(trial_H[cs[q]].data(), &Vb[q * nn], nn * sizeof(double2));
+                ws[cs[q]].assign(wb.begin() + q * Nb, wb.begin() + (q + 1) * Nb);
+            }
+        }
         for (int c = 0; c < n_chains; ++c) {
             h->chains[c].trial = std::move(trial_H[c]);
             h->chains[c].trial_w = std::move(ws[c]);
@@ -1355,12 +1387,17 @@ static bool proj_mid(const HostModel& m, int nt) {
     return nt > (lt / 2 - (len + 1) / 2) && nt <= (lt / 2 + len / 2);
 }
 
+// equal-time measurement of the current G (equaltime_measure)
+static void launch_measure_h(dqmc_handle* h) {
+    launch_measure(h->d_chains, h->nch, h->maxN, h->models[0]->nsub == 2, h->max_lq, h->st);
+}
+
 // ULRINV = (UL UR)^-1 fresh, G = I - UR ULRINV UL, equaltime_measure
 static void proj_measure(dqmc_handle* h) {
     launch_proj_ulr(h->d_chains, h->nch, PMAT_ULRINV, 0, 0, -1, h->st);
     launch_proj_green(h->d_chains, h->nch, PMAT_ULRINV, PMAT_G, h->ctas_per_chain, h->st);
     tmark(h, DQMC_PROF_GREEN);
-    launch_measure(h->d_chains, h->nch, h->maxN, h->models[0]->nsub == 2, h->max_lq, h->st);
+    launch_measure_h(h);
     tmark(h, DQMC_PROF_MEASURE);
 }
 
@@ -1676,7 +1713,7 @@ static void enqueue_b0(dqmc_handle* h, int lupdate, int lmeasure) {
     tmark(h, DQMC_PROF_OTHER);
     for (int nt = lt; nt >= 1; --nt) {
         int visit = lt - nt;
-        if (lmeasure) { launch_measure(h->d_chains, h->nch, h->maxN, h->models[0]->nsub == 2, h->max_lq, h->st); tmark(h, DQMC_PROF_MEASURE); }
+        if (lmeasure) { launch_measure_h(h); tmark(h, DQMC_PROF_MEASURE); }
         PropProg pl; pl.n = 0; PropProg pr; pr.n = 0;
         prog_k(m, pl, PW_INV, 0);          // left_backward, nf = 1..nnf
         prog_k(m, pr, PW_FWD, 0);          // right_forward, nf = 1..nnf
@@ -1723,7 +1760,7 @@ static void enqueue_0b(dqmc_handle* h, int lupdate, int lmeasure) {
         tmark(h, DQMC_PROF_PROP_L);
         launch_prog(h, MAT_G, pr, 1);
         tmark(h, DQMC_PROF_PROP_R);
-        if (lmeasure) { launch_measure(h->d_chains, h->nch, h->maxN, h->models[0]->nsub == 2, h->max_lq, h->st); tmark(h, DQMC_PROF_MEASURE); }
+        if (lmeasure) { launch_measure_h(h); tmark(h, DQMC_PROF_MEASURE); }
         if (m.iwrap_nt[nt] > 0) stab_0b(h, m.iwrap_nt[nt], 1);
     }
 }
@@ -2290,7 +2327,7 @@ extern "C" int dqmc_gpu_update(dqmc_handle* h, int nt) {
 
 extern "C" int dqmc_gpu_measure(dqmc_handle* h) {
     if (!h) return fail(DQMC_EINVAL, "null handle");
-    launch_measure(h->d_chains, h->nch, h->maxN, h->models[0]->nsub == 2, h->max_lq, h->st);
+    launch_measure_h(h);
     CK(cudaStreamSynchronize(h->st));
     CK(cudaGetLastError());
     return DQMC_OK;
@@ -2316,7 +2353,7 @@ extern "C" int dqmc_gpu_time_op(dqmc_handle* h, int op, int reps, double* ms_out
         case 2: launch_green(h->d_chains, h->nch, 1, 0, 0, 0, 0, 0, 0, h->st); break;
         case 3: { PropProg p; p.n = 0; prog_k(m, p, PW_INV, 0); prog_v(m, p, PW_INV, 1); prog_k(m, p, PW_INV, 1);
                   launch_prog(h, MAT_G, p, 0); break; }
-        case 4: launch_measure(h->d_chains, h->nch, h->maxN, h->models[0]->nsub == 2, h->max_lq, h->st); break;
+        case 4: launch_measure_h(h); break;
         case 5: { PropProg p; p.n = 0; prog_k(m, p, PW_FWD, 0); prog_v(m, p, PW_FWD, 1); prog_k(m, p, PW_FWD, 1);
                   launch_prog(h, MAT_G, p, 1); break; }
         case 6: launch_update_flush(h->d_chains, h->nch, h->st); break;
@@ -2347,7 +2384,7 @@ extern "C" int dqmc_gpu_time_op(dqmc_handle* h, int op, int reps, double* ms_out
             pflush(h, pp);
             break;
         }
-        case 4: launch_measure(h->d_chains, h->nch, h->maxN, h->models[0]->nsub == 2, h->max_lq, h->st); break;
+        case 4: launch_measure_h(h); break;
         default: break;
         }
     };
@@ -2915,7 +2952,7 @@ static void enqueue_0b_blocks(dqmc_handle* h, dqmc_nn* nn, int lupdate, int lmea
         prog_k(m, pr, PW_INV, 1);
         launch_prog(h, MAT_G, pl, 0);
         launch_prog(h, MAT_G, pr, 1);
-        if (lmeasure) launch_measure(h->d_chains, h->nch, h->maxN, h->models[0]->nsub == 2, h->max_lq, h->st);
+        if (lmeasure) launch_measure_h(h);
         if (m.iwrap_nt[nt] > 0) stab_0b(h, m.iwrap_nt[nt], 1);
     }
 }

@@ -74,3 +74,9 @@ void launch_blk_decide(const ChainDev* chains, int nchains, cudaStream_t st);
 void launch_blk_end(const ChainDev* chains, int nchains, int t0, int nsl, cudaStream_t st);
 void launch_record(const ChainDev* chains, int nchains, int8_t* fields, double* vals, int* count, int capacity, int V,
                    cudaStream_t st);
+
+// set-up eigenproblems on the device (kern_eig.cu): batched cyclic Jacobi of
+// Hermitian matrices; return the sweep count, -1 on a CUDA error, -2 without
+// convergence
+int eig_herm_device(const double2* Hh, int N, int nmat, double2* Vh, double* wh, cudaStream_t st);
+int dense_kinetic_device(const double2* Hh, int N, double dtau, double2* d_urt, double2* d_urtm1, cudaStream_t st);
