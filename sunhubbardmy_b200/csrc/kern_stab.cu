@@ -114,6 +114,7 @@ __global__ void __launch_bounds__(256, 2) k_stab(const ChainDev* __restrict__ ch
     g.M = N; g.N = N; g.K = N; g.alpha = cmk(1, 0); g.beta = cmk(0, 0);
     g.A = W3; g.lda = N; g.opA = OP_N; g.B = W4; g.ldb = N; g.opB = OP_N;
     g.C = c.V + (size_t)dst * NN; g.ldc = N;
+    g.triA = 1;                          // D^-1 R is upper triangular
     zgemm_cta<GemmBig>(g, 0, 1, buf);
 }
 

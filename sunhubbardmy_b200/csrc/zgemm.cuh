@@ -23,6 +23,9 @@ struct ZGemmArgs {
     // op(B)^T = B row brow[n] (opB = OP_T / OP_C); nullptr = contiguous rows
     const int* arow = nullptr;
     const int* brow = nullptr;
+    // op(A) upper triangular (opA = OP_N): A(m, k) = 0 for k < m, so a tile of
+    // rows m0.. starts its k loop at m0
+    int triA = 0;
 };
 
 // no `volatile`: the compiler may interleave independent DMMAs
@@ -49,8 +52,6 @@ struct ZGemmCfg {
     static constexpr int LDA = BM + 2, LDB = BN + 2;       // = 2 (mod 8): conflict-free fragments
     static constexpr int SA = BK * LDA, SB = BK * LDB;
     static constexpr int SMEM_ELEMS = 2 * (SA + SB);       // double2 elements
-    static constexpr int LDC = BM + 1;
-    static_assert(BN * LDC <= SMEM_ELEMS, "epilogue tile must fit in the staging buffers");
     static_assert(BK % 4 == 0 && WTM % 8 == 0 && WTN % 8 == 0, "tile shape");
 };
 
@@ -122,16 +123,17 @@ __device__ void zgemm_cta(const ZGemmArgs& g, int tile0, int tstep, cplx* smem) 
 #pragma unroll
             for (int b = 0; b < FN; ++b) { accr[a][b][0] = accr[a][b][1] = acci[a][b][0] = acci[a][b][1] = 0.0; }
 
-        const int nk = (g.K + BK - 1) / BK;
+        const int kbeg = g.triA ? (m0 / BK) * BK : 0;
+        const int nk = (g.K - kbeg + BK - 1) / BK;
         if (nk > 0) {
-            zgemm_load_stage<Cfg>(g, m0, n0, 0, As0, Bs0, tid, nthr);
+            zgemm_load_stage<Cfg>(g, m0, n0, kbeg, As0, Bs0, tid, nthr);
             cp_async_commit();
         }
         for (int kt = 0; kt < nk; ++kt) {
             cplx* As = (kt & 1) ? As1 : As0;
             cplx* Bs = (kt & 1) ? Bs1 : Bs0;
             if (kt + 1 < nk) {
-                zgemm_load_stage<Cfg>(g, m0, n0, (kt + 1) * BK, (kt & 1) ? As0 : As1, (kt & 1) ? Bs0 : Bs1, tid, nthr);
+                zgemm_load_stage<Cfg>(g, m0, n0, kbeg + (kt + 1) * BK, (kt & 1) ? As0 : As1, (kt & 1) ? Bs0 : Bs1, tid, nthr);
                 cp_async_commit();
                 cp_async_wait<1>();
             } else {
@@ -175,32 +177,26 @@ __device__ void zgemm_cta(const ZGemmArgs& g, int tile0, int tstep, cplx* smem) 
             }
             __syncthreads();
         }
-        // epilogue through shared memory: Cs[n][m], ld = BM + 1
-        cplx* Cs = smem;
+        // epilogue straight from the accumulators: C(m, n) = alpha acc + beta C;
+        // the 8 lanes of a (lane & 3) group store 8 consecutive rows of a column
         if (mathw) {
 #pragma unroll
             for (int a = 0; a < FM; ++a)
 #pragma unroll
-                for (int b = 0; b < FN; ++b) {
-                    int m = wm0 + a * 8 + (lane >> 2);
-                    int n = wn0 + b * 8 + (lane & 3) * 2;
-                    Cs[n * Cfg::LDC + m] = cmk(accr[a][b][0], acci[a][b][0]);
-                    Cs[(n + 1) * Cfg::LDC + m] = cmk(accr[a][b][1], acci[a][b][1]);
-                }
+                for (int b = 0; b < FN; ++b)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int gm = m0 + wm0 + a * 8 + (lane >> 2), gn = n0 + wn0 + b * 8 + (lane & 3) * 2 + h;
+                        if (gm < g.M && gn < g.N) {
+                            cplx* cp = g.C + MIDX(gm, gn, g.ldc);
+                            cplx r = cmul(g.alpha, cmk(accr[a][b][h], acci[a][b][h]));
+                            if (!beta0) r = cfma(g.beta, *cp, r);
+                            *cp = r;
+                        }
+                    }
         }
-        __syncthreads();
-        for (int e = tid; e < BM * BN; e += nthr) {
-            int m = e % BM, n = e / BM;
-            int gm = m0 + m, gn = n0 + n;
-            if (gm < g.M && gn < g.N) {
-                cplx r = cmul(g.alpha, Cs[n * Cfg::LDC + m]);
-                cplx* cp = g.C + MIDX(gm, gn, g.ldc);
-                if (!beta0) r = cfma(g.beta, *cp, r);
-                *cp = r;
-            }
-        }
-        __syncthreads();
     }
+    __syncthreads();     // C is complete for every thread of the CTA
 }
 
 // Default tile configurations (256 threads).
