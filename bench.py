@@ -382,6 +382,52 @@ def profile_arm(args) -> None:
     g.close()
 
 
+def single_chain_block(args, result: dict, Ns, lt: int) -> dict:
+    """The single-chain drop-in (one Markov chain on the GPU, the reference's
+    one-chain-per-rank case): device sweep time and updates/s, the same through
+    the C ABI with host buffers, and the batched/plain ESS/s ratio of double
+    occupancy (the batched run's tau_int stands for both: same model and
+    update)."""
+    import numpy as np
+    import torch
+    import sunhubbardmy_b200 as sb
+    p0 = sb.DqmcParams.make(**CONFIG)
+    g1 = sb.Dqmc(p0, n_chains=1, seeds=[test_seed(0)])
+    g1.sweep_start()
+    g1.obser_init()
+    g1.sweeps(2, True)
+    torch.cuda.synchronize()
+    n = 3
+    ms = g1.sweeps(n, True) / n
+    per = 2 * lt * int(Ns[0])
+    conf = torch.empty(lt * int(Ns[0]), dtype=torch.int32, pin_memory=True).numpy()
+    g1.conf_all(conf)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(n):
+        g1.set_conf_all(conf)
+        g1.sweep_start()
+        g1.sweeps(1, True)
+        g1.bins_raw(0)
+        g1.conf_all(conf)
+    e2e_s = (time.perf_counter() - t0) / n
+    g1.close()
+    out = {"chains": 1, "ms_per_sweep": ms, "value": per / (ms * 1e-3), "unit": "updates/s",
+           "e2e": {"value": per / e2e_s, "unit": "updates/s", "note": "set_conf_all + sweep_start + 1 sweep + "
+                   "get_bins + get_conf_all, pinned host buffers"}}
+    cb = result.get("cpu_baseline")
+    if cb:
+        out["cpu_one_core"] = cb["value"] / cb["cores"]
+        out["vs_one_core"] = out["value"] / out["cpu_one_core"]
+    es = result.get("ess")
+    if es:
+        tau = max(es["tau_int_sweeps"], 0.5)
+        single = (1.0 / (2.0 * tau)) / (ms * 1e-3)
+        out["ess_per_s"] = single
+        out["batched_vs_single_ess_per_s"] = es["ess_per_s"] / single
+    return out
+
+
 def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
     import numpy as np
     import torch
@@ -485,7 +531,7 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
         N2, N3 = float((Ns ** 2).sum()), float((Ns ** 3).sum())     # sums over chains
         work = {   # algorithmic work of one launch group over all chains: (flops, bytes)
             "update": (8.0 * float((acc_c * Ns ** 3).sum()), None),   # flush GEMMs: 8 N^2 per accepted site
-            "stab": ((18.0 + 2.0 / 3.0) * N3, None),
+            "stab": ((14.0 + 2.0 / 3.0) * N3, None),   # QR 16/3, Q 16/3, triangular (D^-1 R) V 4
             "green": ((41.0 + 1.0 / 3.0) * N3, None),
             "prop_left": (None, 32.0 * N2), "prop_right": (None, 32.0 * N2), "bprod": (None, 32.0 * N2),
             "measure": (None, 16.0 * N2),
@@ -520,21 +566,22 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
         }
         if tune_report is not None:
             result["config"]["autotune"] = {str(k): v for k, v in tune_report.items()}
-        if args.ess > 0:
+        ess_sweeps = args.ess if args.ess > 0 else (10 if args.workload == "config2" else 0)
+        if ess_sweeps > 0:
             from sunhubbardmy_b200.stats import double_occupancy, ess
             series = []
-            g.sweeps(args.ess_warmup, False)     # equilibrate before the series
+            g.sweeps(args.ess_warmup if args.ess > 0 else 0, False)     # equilibrate before the series
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            for _ in range(args.ess):
+            for _ in range(ess_sweeps):
                 g.obser_init()
                 g.sweeps(1, True)
                 series.append(double_occupancy(g.energy_all(), Ns))
             wall = time.perf_counter() - t0
             x = np.array(series).T            # [chain, sweep]
             n_ess, tau = ess(x)
-            result["ess"] = {"observable": "double occupancy (per-sweep, per chain)", "sweeps": args.ess,
-                             "warmup_sweeps": args.ess_warmup + args.warmup + args.steps,
+            result["ess"] = {"observable": "double occupancy (per-sweep, per chain)", "sweeps": ess_sweeps,
+                             "warmup_sweeps": (args.ess_warmup if args.ess > 0 else 0) + args.warmup + args.steps,
                              "chains": C, "tau_int_sweeps": tau, "ess": n_ess, "ess_per_s": n_ess / wall,
                              "mean": float(x.mean()), "stderr": float(x.std(ddof=1) / np.sqrt(n_ess)),
                              "wall_s": wall}
@@ -554,6 +601,8 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
             cv = per / times[0]
             result["cpu_baseline"] = {"value": cv, "unit": "updates/s", "cores": os.cpu_count() or 1, "kind": "port",
                                       "sample": f"20 slices of a b0 sweep per chain, one chain per core ({os.cpu_count()} cores), OpenBLAS"}
+        if args.workload == "config2" and C > 1 and world == 1:
+            result["single_chain"] = single_chain_block(args, result, Ns, lt)
     g.close()
     if dist is not None:
         dist.barrier()

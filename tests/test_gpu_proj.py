@@ -123,6 +123,40 @@ def test_proj_update_operator(sb, oracle, case):
     assert abs(dg["phase"] - dc["phase"]) < 1e-10
 
 
+@pytest.mark.parametrize("update,flavour", [(0, "FAST"), (1, "DELAY"), (2, "SUBMATRIX_G_EXACT"), (2, "SUBMATRIX")])
+@pytest.mark.parametrize("case", ["hc3_tv_win8", "sq4_hub", "hc2_tuv"])
+def test_proj_update_flavours(sb, oracle, case, update, flavour):
+    """A GPU handle built with update = fast (0), delay (1) or submatrix (2)
+    against the oracle's restatement of the matching projective update
+    (dqmc_proj_update.f90, dqmc_proj_update_delay.f90, the submatrix-G and
+    submatrix-LR flavours) over every family of two slices: identical fields
+    and accept counts, UR and (UL UR)^-1 to 1e-9.  (The submatrix-G bond
+    update is taken with the exact inverse of the bond's 2 x 2 block; the
+    reference's expressions differ in one entry, see test_oracle.)"""
+    kw = dict(PCASES[case], update=update)
+    p = sb.DqmcParams.make(**kw)
+    g = sb.Dqmc(p, n_chains=1, seeds=[sb.test_seed(0)])
+    m = oracle.Model(**kw)
+    ch = oracle.Chain(m, sb.test_seed(0))
+    g.set_trial(ch.trial()[0], 0)
+    g.sweep_start(); ch.proj_sweep_start()
+    nf_list = (list(range(1, m.nn_nf + 1)) if kw["rv"] != 0 else []) + ([0] if kw["rhub"] != 0 else [])
+    f = getattr(oracle, flavour)
+    for nt in (m.ltrot, m.ltrot - 1):
+        for nf in nf_list:
+            g.proj_update(nt, nf)
+            ch.proj_update(nt, nf, flavour=f)
+    if kw["rv"] != 0:
+        assert np.array_equal(g.vconf(0), ch.vconf())
+    if kw["rhub"] != 0:
+        assert np.array_equal(g.conf(0), ch.conf())
+    for x, y in zip(g.proj_state(0), ch.proj_state()):
+        assert rel(x, y) < 1e-9
+    dg, dc = g.diag(0), ch.diag()
+    assert dg["accepted_v"] == dc["accepted_v"] and dg["accepted"] == dc["accepted"]
+    g.close()
+
+
 @pytest.mark.parametrize("case", list(PCASES))
 def test_proj_sweeps_match_oracle(sb, oracle, case):
     """Two full sweeps (b0 + 0b) with updates and the mid-slice measurement."""
