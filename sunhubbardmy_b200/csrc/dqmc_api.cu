@@ -2682,6 +2682,7 @@ extern "C" int dqmc_nn_forward(dqmc_nn* nn, const int8_t* fields, int B, double*
     CK(cudaMemcpyAsync(S, nn->S, B * sizeof(double), cudaMemcpyDeviceToHost, nn->st));
     CK(cudaStreamSynchronize(nn->st));
     CK(cudaGetLastError());
+    if (nn_timed_out()) return fail(DQMC_ECUDA, "a tensor-core wait of the network kernels ran out");
     return DQMC_OK;
 }
 
@@ -2692,6 +2693,7 @@ static int nn_fwd(dqmc_nn* nn, int B, double* S_host) {
     launch_nn_forward(nn_w(nn), nn_in_fields(nn), B, nn->S, nn->h1, nn->h2, nn->st);
     CK(cudaMemcpyAsync(S_host, nn->S, B * sizeof(double), cudaMemcpyDeviceToHost, nn->st));
     CK(cudaStreamSynchronize(nn->st));
+    if (nn_timed_out()) return fail(DQMC_ECUDA, "a tensor-core wait of the network kernels ran out");
     return DQMC_OK;
 }
 static int nn_bwd(dqmc_nn* nn, int B, const double* r_host) {
@@ -2712,6 +2714,7 @@ extern "C" int dqmc_nn_gradient(dqmc_nn* nn, const int8_t* fields, int B, const 
     CK(cudaMemcpyAsync(grad, nn->grad, NN_NPARAM * sizeof(float), cudaMemcpyDeviceToHost, nn->st));
     CK(cudaStreamSynchronize(nn->st));
     CK(cudaGetLastError());
+    if (nn_timed_out()) return fail(DQMC_ECUDA, "a tensor-core wait of the network kernels ran out");
     return DQMC_OK;
 }
 

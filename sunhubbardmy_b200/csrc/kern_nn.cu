@@ -5,11 +5,14 @@
 //   S  = sum_v w3 . h2(v) + b3 V  1x1x1 conv to one channel, summed over space-time
 //
 // s = +-1 is the HS field (value 1 -> -1, 2 -> +1).  The 32 -> 32 layer runs on
-// the tensor cores as an implicit GEMM (M = sites, N = 32, K = 27 taps x 32
-// channels) with mma.sync m16n8k16 BF16 x BF16 -> FP32: BF16 weights and
-// activations, FP32 accumulation.  Its data gradient is the same GEMM with
-// mirrored taps and transposed weights; its weight gradient is a per-tap GEMM
-// over sites.  Layer 1 and the reductions run on the FP32 pipes.
+// the fifth-generation tensor cores as an implicit GEMM per brick of 128 sites
+// (M = 128 sites, N = 32 channels, K = 27 taps x 32 channels): one thread issues
+// tcgen05.mma kind::f16 (BF16 x BF16 -> FP32) with the accumulator in tensor
+// memory, the tap's im2col tile and the weights staged in shared memory in the
+// canonical K-major layout, and the result read back with tcgen05.ld.  Its data
+// gradient is the same GEMM with mirrored taps and transposed weights.  The
+// weight gradient (a per-tap 32 x 32 product over sites) stays on mma.sync
+// m16n8k16, and layer 1 and the reductions run on the FP32 pipes.
 //
 // Sites are processed in bricks of 4 x 4 x 8 (t, y, x) with a one-site halo
 // for layer 2 (two for layer 1), gathered with periodic wrap-around.
@@ -97,32 +100,127 @@ DQ_DEV float field_at(const NNIn& in, int b, int t, int y, int x) {
 }
 
 // ---------------------------------------------------------------------------
-// layer-2 implicit GEMM of one warp: acc[4][4] (n-tiles of 8 channels) for the
-// warp's 16 core sites; A rows from the halo H (stride HLD), B from Wt
-// ([32 n][NN_WLD], k = tap*32 + channel)
+// tcgen05 (UMMA) implicit GEMM of the 32 -> 32 layer
 // ---------------------------------------------------------------------------
-DQ_DEV void conv_mma(const bf16* H, const bf16* Wt, int warp, int lane, float acc[4][4]) {
-    const int r = (lane & 7) + ((lane >> 3) & 1) * 8;
-    const int koffA = (lane >> 4) * 8;
-    const int q = warp * 16 + r;
-    const int m = lane >> 3;
-    const int nB = (m >> 1) * 8 + (lane & 7), koffB = (m & 1) * 8;
-#pragma unroll 1
+DQ_DEV uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// canonical K-major, no-swizzle operand layout: element (row, k) of a tile with
+// G groups of 8 rows sits in the 8 x 8 core matrix (k / 8, row / 8), 128 bytes
+// each, core matrices k-group major: ((k / 8) G + row / 8) 64 + (row % 8) 8 + k % 8
+__host__ __device__ inline int umma_canon(int row, int k, int G) {
+    return ((k >> 3) * G + (row >> 3)) * 64 + (row & 7) * 8 + (k & 7);
+}
+// shared-memory matrix descriptor: start address, leading (k-group) and stride
+// (row-group) byte offsets, version 1, no swizzle
+DQ_DEV uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | ((uint64_t)1 << 46);
+}
+// instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
+// K-major, N = 32, M = 128
+constexpr uint32_t NN_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+#define NN_TAP_B 1024            // canonical weights of one tap: 32 x 32 bf16
+#define NN_TILE_A 4096           // canonical im2col tile of one tap: 128 x 32 bf16
+#define NN_SPIN (1 << 24)        // bound of every mbarrier wait
+
+__device__ int g_nn_timeout;     // set when a tensor-core wait ran out (checked by the host)
+
+DQ_DEV bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    for (int it = 0; it < NN_SPIN; ++it) {
+        uint32_t ok;
+        asm volatile("{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                     "selp.b32 %0, 1, 0, P1;\n\t}\n" : "=r"(ok) : "r"(smem_addr(bar)), "r"(parity) : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+// Weights of the layer in canonical per-tap tiles: Bc[tap][umma_canon(n, k, 4)]
+// = Wt[n][tap 32 + k] (Wt: [32 n][NN_WLD] with k = tap*32 + channel), 16-byte copies.
+DQ_DEV void load_wt_canon(bf16* Bc, const bf16* Wt) {
+    for (int e = threadIdx.x; e < 27 * NN_C * 4; e += blockDim.x) {
+        const int kg = e & 3, n = (e >> 2) % NN_C, tap = e / (NN_C * 4);
+        *(uint4*)(Bc + tap * NN_TAP_B + umma_canon(n, kg * 8, 4)) = *(const uint4*)(Wt + (size_t)n * NN_WLD + tap * NN_C + kg * 8);
+    }
+}
+
+// D[q][n] = sum_tap sum_c X(halo_row(q, tap))[c] B[n][tap 32 + c] for the 128 core
+// sites q of the brick, accumulated in tensor memory (128 lanes x 32 columns).
+// X: the halo (stride HLD bf16), Bc: canonical weights, At: two canonical
+// im2col tiles, bars: three mbarriers, tslot: the tensor-memory address.
+// Tap t's tile is gathered while the MMAs of tap t - 1 run; a tile is
+// overwritten only after the MMAs that read it completed.  On return warps
+// 0..3 hold the accumulator row 32 w + lane in acc[32] (other warps: zeros);
+// the caller frees the tensor memory with umma_free after its last use.
+// Returns false (and sets g_nn_timeout) when a wait ran out.
+DQ_DEV bool conv_umma(const bf16* X, const bf16* Bc, bf16* At, uint64_t* bars, uint32_t* tslot, float acc[32]) {
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" :: "r"(smem_addr(tslot)), "r"(32));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 0) {
+        for (int k = 0; k < 3; ++k) asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_addr(&bars[k])), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::);
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::);
+    const uint32_t tmem = *tslot;
+    bool ok = true;
     for (int tap = 0; tap < 27; ++tap) {
-        const bf16* arow = H + halo_row(q, tap) * HLD + koffA;
+        const int buf = tap & 1;
+        bf16* A = At + buf * NN_TILE_A;
+        if (tap >= 2) ok = mbar_wait(&bars[buf], ((tap - 2) >> 1) & 1) && ok;   // MMAs of tap - 2 done
+        for (int e = tid; e < 128 * 4; e += blockDim.x) {
+            const int m = e >> 2, kg = e & 3;
+            *(uint4*)(A + umma_canon(m, kg * 8, 16)) = *(const uint4*)(X + halo_row(m, tap) * HLD + kg * 8);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::);
 #pragma unroll
-        for (int ch = 0; ch < 2; ++ch) {
-            uint32_t a0, a1, a2, a3, b0, b1, b2, b3, b4, b5, b6, b7;
-            ldsm_x4(a0, a1, a2, a3, arow + ch * 16);
-            const int kb = tap * 32 + ch * 16 + koffB;
-            ldsm_x4(b0, b1, b2, b3, Wt + nB * NN_WLD + kb);
-            ldsm_x4(b4, b5, b6, b7, Wt + (nB + 16) * NN_WLD + kb);
-            mma_bf16(acc[0], a0, a1, a2, a3, b0, b1);
-            mma_bf16(acc[1], a0, a1, a2, a3, b2, b3);
-            mma_bf16(acc[2], a0, a1, a2, a3, b4, b5);
-            mma_bf16(acc[3], a0, a1, a2, a3, b6, b7);
+            for (int c = 0; c < 2; ++c) {
+                const uint64_t da = umma_desc(smem_addr(A + c * 2 * 16 * 64), 16 * 128, 128);
+                const uint64_t db = umma_desc(smem_addr(Bc + tap * NN_TAP_B + c * 2 * 4 * 64), 4 * 128, 128);
+                const uint32_t en = (tap | c) ? 1u : 0u, z = 0u;
+                asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                             :: "r"(tmem), "l"(da), "l"(db), "r"(NN_IDESC), "r"(en), "r"(z), "r"(z), "r"(z), "r"(z));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         :: "r"(smem_addr(&bars[buf])));
         }
     }
+    if (tid == 0)
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" :: "r"(smem_addr(&bars[2])));
+    ok = mbar_wait(&bars[2], 0) && ok;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::);
+#pragma unroll
+    for (int c = 0; c < 32; ++c) acc[c] = 0.f;
+    if (warp < 4 && ok) {
+        uint32_t r[32];
+        const uint32_t ta = tmem + ((uint32_t)(32 * warp) << 16);
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                     "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                       "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+                       "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+                       "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                     : "r"(ta));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::);
+#pragma unroll
+        for (int c = 0; c < 32; ++c) acc[c] = __uint_as_float(r[c]);
+    }
+    if (!ok && lane == 0) atomicExch(&g_nn_timeout, 1);
+    return ok;
+}
+
+// Releases the tensor memory of conv_umma (every thread of the CTA calls it).
+DQ_DEV void umma_free(const uint32_t* tslot) {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::);
+    __syncthreads();
+    if ((threadIdx.x >> 5) == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(*tslot), "r"(32));
 }
 
 struct NNSmem {
@@ -131,28 +229,28 @@ struct NNSmem {
     float red[32];
 };
 
+// canonical weights, halo, two im2col tiles, NNSmem, three mbarriers and the
+// tensor-memory address
 static size_t nn_fwd_smem() {
-    return (size_t)NN_C * NN_WLD * sizeof(bf16) + (size_t)HQ * HLD * sizeof(bf16) + sizeof(NNSmem) + 64;
+    return (size_t)(27 * NN_TAP_B + HQ * HLD + 2 * NN_TILE_A) * sizeof(bf16) + sizeof(NNSmem) + 64;
 }
 
-DQ_DEV void load_wt(bf16* dst, const bf16* src) {
-    const uint4* s4 = (const uint4*)src;
-    uint4* d4 = (uint4*)dst;
-    for (int e = threadIdx.x; e < NN_C * NN_WLD / 8; e += blockDim.x) d4[e] = s4[e];
-}
 
 // Forward: S[b] += sum over the output range of field b.  train: store h1 and
 // h2 (bf16, [b][v][32]) of the core sites for the backward kernels.
 template <bool TRAIN>
 __global__ void __launch_bounds__(256) k_nn_fwd(NNW w, NNIn in, double* S, bf16* h1g, bf16* h2g) {
     extern __shared__ __align__(16) unsigned char smraw[];
-    bf16* Wt = (bf16*)smraw;
-    bf16* H = Wt + NN_C * NN_WLD;
-    NNSmem* sm = (NNSmem*)(H + HQ * HLD);
+    bf16* Bc = (bf16*)smraw;
+    bf16* H = Bc + 27 * NN_TAP_B;
+    bf16* At = H + HQ * HLD;
+    NNSmem* sm = (NNSmem*)(At + 2 * NN_TILE_A);
+    uint64_t* bars = (uint64_t*)(sm + 1);
+    uint32_t* tslot = (uint32_t*)(bars + 3);
     const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5;
     const int b = blockIdx.y;
     const Brick br = brick_of(in, blockIdx.x);
-    load_wt(Wt, w.W2T);
+    load_wt_canon(Bc, w.W2T);
     for (int e = tid; e < 27 * NN_C; e += nth) sm->W1[e] = w.W1[e];
     if (tid < NN_C) { sm->b1[tid] = w.b1[tid]; sm->b2[tid] = w.b2[tid]; sm->w3[tid] = w.w3[tid]; }
     for (int e = tid; e < SIQ; e += nth) {
@@ -173,28 +271,28 @@ __global__ void __launch_bounds__(256) k_nn_fwd(NNW w, NNIn in, double* S, bf16*
         H[hs * HLD + ch] = __float2bfloat16(tanhf(pre));
     }
     __syncthreads();
-    float acc[4][4] = {};
-    conv_mma(H, Wt, warp, lane, acc);
-    // epilogue: rows g and g + 8 of the warp's 16 sites, channels 8j + 2t, +1
-    const int g = lane >> 2, t4 = lane & 3;
-    float e0 = 0.f, e1 = 0.f;
-    const int q0 = warp * 16 + g, q1 = q0 + 8;
-    const bool v0 = core_valid(in, br, q0), v1 = core_valid(in, br, q1);
-    const int s0 = v0 ? core_site(in, br, q0) : 0, s1 = v1 ? core_site(in, br, q1) : 0;
+    float acc[32];
+    conv_umma(H, Bc, At, bars, tslot, acc);
+    // epilogue: warps 0..3 hold the row of core site q = 32 warp + lane
+    float e0 = 0.f;
+    const int q0 = 32 * warp + lane;
+    const bool v0 = warp < 4 && core_valid(in, br, q0);
+    if (v0) {
+        const int s0 = core_site(in, br, q0);
+        bf16 hv[NN_C];
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-        for (int cc = 0; cc < 2; ++cc) {
-            const int co = 8 * j + 2 * t4 + cc;
-            const float h20 = tanhf(acc[j][cc] + sm->b2[co]);
-            const float h21 = tanhf(acc[j][2 + cc] + sm->b2[co]);
-            e0 = fmaf(sm->w3[co], h20, e0);
-            e1 = fmaf(sm->w3[co], h21, e1);
-            if (TRAIN) {
-                if (v0) h2g[((size_t)b * in.V + s0) * NN_C + co] = __float2bfloat16(h20);
-                if (v1) h2g[((size_t)b * in.V + s1) * NN_C + co] = __float2bfloat16(h21);
-            }
+        for (int co = 0; co < NN_C; ++co) {
+            const float h2 = tanhf(acc[co] + sm->b2[co]);
+            e0 = fmaf(sm->w3[co], h2, e0);
+            hv[co] = __float2bfloat16(h2);
         }
+        if (TRAIN) {
+            uint4* dst = (uint4*)(h2g + ((size_t)b * in.V + s0) * NN_C);
+#pragma unroll
+            for (int k = 0; k < NN_C / 8; ++k) dst[k] = *(const uint4*)(hv + 8 * k);
+        }
+    }
+    umma_free(tslot);
     if (TRAIN) {
         // h1 of the core sites (the halo row of tap 13 = no shift)
         for (int e = tid; e < BQ * NN_C; e += nth) {
@@ -203,7 +301,7 @@ __global__ void __launch_bounds__(256) k_nn_fwd(NNW w, NNIn in, double* S, bf16*
                 h1g[((size_t)b * in.V + core_site(in, br, q)) * NN_C + ch] = H[halo_row(q, 13) * HLD + ch];
         }
     }
-    float tot = (v0 ? e0 : 0.f) + (v1 ? e1 : 0.f);
+    float tot = v0 ? e0 : 0.f;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
     if (lane == 0) sm->red[warp] = tot;
@@ -229,21 +327,27 @@ struct NNBSmem {
     float dp1[BQ * NN_C];
 };
 
+// canonical weights, the dpre2 halo, NNBSmem (whose dp1 holds the two im2col
+// tiles during the convolution), three mbarriers and the tensor-memory address
 static size_t nn_bwd_smem() {
-    return (size_t)NN_C * NN_WLD * sizeof(bf16) + (size_t)HQ * HLD * sizeof(bf16) + sizeof(NNBSmem) + 64;
+    return (size_t)(27 * NN_TAP_B + HQ * HLD) * sizeof(bf16) + sizeof(NNBSmem) + 64;
 }
+static_assert(sizeof(float) * BQ * NN_C >= sizeof(bf16) * 2 * NN_TILE_A, "im2col tiles overlay dp1");
 
 __global__ void __launch_bounds__(256) k_nn_bwd_data(NNW w, NNIn in, const double* r, const bf16* h1g, const bf16* h2g,
                                                      bf16* dp2g, float* grad) {
     extern __shared__ __align__(16) unsigned char smraw[];
-    bf16* Wt = (bf16*)smraw;
-    bf16* D = Wt + NN_C * NN_WLD;          // dpre2 on the halo
+    bf16* Bc = (bf16*)smraw;
+    bf16* D = Bc + 27 * NN_TAP_B;          // dpre2 on the halo
     NNBSmem* sm = (NNBSmem*)(D + HQ * HLD);
+    bf16* At = (bf16*)sm->dp1;             // im2col tiles, before dp1 is written
+    uint64_t* bars = (uint64_t*)(sm + 1);
+    uint32_t* tslot = (uint32_t*)(bars + 3);
     const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5;
     const int b = blockIdx.y;
     const Brick br = brick_of(in, blockIdx.x);
     const float rb = (float)r[b];
-    load_wt(Wt, w.W2R);
+    load_wt_canon(Bc, w.W2R);
     for (int e = tid; e < 27 * NN_C; e += nth) sm->W1g[e] = 0.f;
     if (tid < NN_C) { sm->b1g[tid] = 0.f; sm->b2g[tid] = 0.f; sm->w3g[tid] = 0.f; sm->w3[tid] = w.w3[tid]; }
     for (int e = tid; e < SIQ; e += nth) {
@@ -270,23 +374,22 @@ __global__ void __launch_bounds__(256) k_nn_bwd_data(NNW w, NNIn in, const doubl
         atomicAdd(&sm->b2g[ch], __bfloat162float(d));
         atomicAdd(&sm->w3g[ch], rb * __bfloat162float(h2g[gi]));
     }
-    float acc[4][4] = {};
-    conv_mma(D, Wt, warp, lane, acc);   // W2R holds mirrored taps: the transposed convolution
-    const int g = lane >> 2, t4 = lane & 3;
-    const int q0 = warp * 16 + g, q1 = q0 + 8;
-    const bool v0 = core_valid(in, br, q0), v1 = core_valid(in, br, q1);
-    const int s0 = v0 ? core_site(in, br, q0) : 0, s1 = v1 ? core_site(in, br, q1) : 0;
+    float acc[32];
+    conv_umma(D, Bc, At, bars, tslot, acc);   // W2R holds mirrored taps: the transposed convolution
+    // warps 0..3 hold the row of core site q = 32 warp + lane (the MMAs that
+    // read the im2col tiles have completed, so dp1 may be written)
+    if (warp < 4) {
+        const int q0 = 32 * warp + lane;
+        const bool v0 = core_valid(in, br, q0);
+        const int s0 = v0 ? core_site(in, br, q0) : 0;
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-        for (int cc = 0; cc < 2; ++cc) {
-            const int ch = 8 * j + 2 * t4 + cc;
-            float d0 = 0.f, d1 = 0.f;
-            if (v0) { float h1 = __bfloat162float(h1g[((size_t)b * in.V + s0) * NN_C + ch]); d0 = acc[j][cc] * (1.f - h1 * h1); }
-            if (v1) { float h1 = __bfloat162float(h1g[((size_t)b * in.V + s1) * NN_C + ch]); d1 = acc[j][2 + cc] * (1.f - h1 * h1); }
+        for (int ch = 0; ch < NN_C; ++ch) {
+            float d0 = 0.f;
+            if (v0) { const float h1 = __bfloat162float(h1g[((size_t)b * in.V + s0) * NN_C + ch]); d0 = acc[ch] * (1.f - h1 * h1); }
             sm->dp1[q0 * NN_C + ch] = d0;
-            sm->dp1[q1 * NN_C + ch] = d1;
         }
+    }
+    umma_free(tslot);
     __syncthreads();
     // dW1[tap][c] = sum_q s(q + tap) dpre1(q)[c]; db1 = sum dpre1
     for (int e = tid; e < 28 * NN_C; e += nth) {
@@ -462,4 +565,12 @@ void launch_nn_adam(float* theta, const float* grad, float* m1, float* m2, int n
 
 void launch_nn_pack(const float* theta, bf16* W2T, bf16* W2R, cudaStream_t st) {
     k_nn_pack<<<(NN_C * NN_WLD + 255) / 256, 256, 0, st>>>(theta, W2T, W2R);
+}
+
+// 1 when a tensor-core wait of the network kernels ran out since the last call (then cleared)
+int nn_timed_out() {
+    int v = 0, z = 0;
+    cudaMemcpyFromSymbol(&v, g_nn_timeout, sizeof(int));
+    if (v) cudaMemcpyToSymbol(g_nn_timeout, &z, sizeof(int));
+    return v;
 }

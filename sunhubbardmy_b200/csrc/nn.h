@@ -45,3 +45,5 @@ void launch_nn_backward(const NNW& w, const NNIn& in, int B, const double* r, co
 void launch_nn_adam(float* theta, const float* grad, float* m1, float* m2, int n, float lr, float b1c, float b2c,
                     __nv_bfloat16* W2T, __nv_bfloat16* W2R, cudaStream_t st);
 void launch_nn_pack(const float* theta, __nv_bfloat16* W2T, __nv_bfloat16* W2R, cudaStream_t st);
+// 1 when a tensor-core wait of the network kernels ran out since the last call (then cleared)
+int nn_timed_out();
