@@ -223,14 +223,19 @@ static __device__ void apply_block(const double2* Vs, const double2* Tp, int N, 
     g.B = X + MIDX(p, c0, N); g.ldb = N; g.opB = OP_N;
     g.C = sc.Ws; g.ldc = QR_NB;
     zgemm_cta<GemmWide>(g, 0, 1, gsm);
-    // W2 = T^H W  or  T W
+    // W2 = T^H W  or  T W, with T (16 x 16) in shared memory (the staging
+    // buffer is free between the GEMMs)
+    double2* Ts = gsm;
+    for (int e = threadIdx.x; e < QR_NB * QR_NB; e += blockDim.x) Ts[e] = Tp[e];
+    __syncthreads();
     for (int e = threadIdx.x; e < jb * nc; e += blockDim.x) {
         int a = e % jb, cc = e / jb;
+        const double2* w = sc.Ws + (size_t)cc * QR_NB;
         double2 acc = cmk(0, 0);
         if (use_th) {
-            for (int b = 0; b <= a; ++b) acc = cfma(cconj(Tp[b + a * QR_NB]), sc.Ws[b + cc * QR_NB], acc);
+            for (int b = 0; b <= a; ++b) acc = cfma(cconj(Ts[b + a * QR_NB]), w[b], acc);
         } else {
-            for (int b = a; b < jb; ++b) acc = cfma(Tp[a + b * QR_NB], sc.Ws[b + cc * QR_NB], acc);
+            for (int b = a; b < jb; ++b) acc = cfma(Ts[a + b * QR_NB], w[b], acc);
         }
         sc.Ws2[a + cc * QR_NB] = acc;
     }
@@ -431,19 +436,29 @@ static __device__ void build_t64(int N, int P, int jb2, const double2* Tp16, dou
         g.B = sc.Vs + (size_t)k * N; g.ldb = N; g.opB = OP_N;
         g.C = sc.Ws; g.ldc = QR_NB2;
         zgemm_cta<GemmBig>(g, 0, 1, gsm);
-        // Y = T_a X (T_a upper triangular)
+        // Y = T_a X (T_a upper triangular), then T(0:k, k:k+jb) = -Y T_b, with
+        // T_a (k x k, ld k), X and Y (k x jb, ld k) and T_b staged in shared
+        // memory (the GEMM staging buffer: k^2 + 2 k QR_NB + QR_NB^2 <= 4096
+        // elements for k <= 48)
+        double2* Tas = gsm;
+        double2* Xs = Tas + k * k;
+        double2* Ys = Xs + k * QR_NB;
+        double2* Tbs = Ys + k * QR_NB;
+        for (int e = tid; e < k * k; e += nth) Tas[e] = T64[(e % k) + (e / k) * QR_NB2];
+        for (int e = tid; e < k * jb; e += nth) Xs[e] = sc.Ws[(e % k) + (e / k) * QR_NB2];
+        for (int e = tid; e < QR_NB * QR_NB; e += nth) Tbs[e] = Tb[e];
+        __syncthreads();
         for (int e = tid; e < k * jb; e += nth) {
             const int a = e % k, b = e / k;
             double2 acc = cmk(0, 0);
-            for (int c = a; c < k; ++c) acc = cfma(T64[a + c * QR_NB2], sc.Ws[c + b * QR_NB2], acc);
-            sc.Ws2[a + b * QR_NB2] = acc;
+            for (int c = a; c < k; ++c) acc = cfma(Tas[a + c * k], Xs[c + b * k], acc);
+            Ys[a + b * k] = acc;
         }
         __syncthreads();
-        // T(0:k, k:k+jb) = -Y T_b ; T(k:k+jb, k:k+jb) = T_b
         for (int e = tid; e < k * jb; e += nth) {
             const int a = e % k, b = e / k;
             double2 acc = cmk(0, 0);
-            for (int c = 0; c <= b; ++c) acc = cfma(sc.Ws2[a + c * QR_NB2], Tb[c + b * QR_NB], acc);
+            for (int c = 0; c <= b; ++c) acc = cfma(Ys[a + c * k], Tbs[c + b * QR_NB], acc);
             T64[a + (k + b) * QR_NB2] = cmk(-acc.x, -acc.y);
         }
         for (int e = tid; e < jb * jb; e += nth) {
