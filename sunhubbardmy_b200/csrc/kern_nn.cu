@@ -139,7 +139,7 @@ DQ_DEV bool mbar_wait(uint64_t* bar, uint32_t parity) {
 // = Wt[n][tap 32 + k] (Wt: [32 n][NN_WLD] with k = tap*32 + channel), 16-byte copies.
 DQ_DEV void load_wt_canon(bf16* Bc, const bf16* Wt) {
     for (int e = threadIdx.x; e < 27 * NN_C * 4; e += blockDim.x) {
-        const int kg = e & 3, n = (e >> 2) % NN_C, tap = e / (NN_C * 4);
+        const int n = e % NN_C, kg = (e / NN_C) & 3, tap = e / (NN_C * 4);
         *(uint4*)(Bc + tap * NN_TAP_B + umma_canon(n, kg * 8, 4)) = *(const uint4*)(Wt + (size_t)n * NN_WLD + tap * NN_C + kg * 8);
     }
 }
@@ -172,7 +172,9 @@ DQ_DEV bool conv_umma(const bf16* X, const bf16* Bc, bf16* At, uint64_t* bars, u
         bf16* A = At + buf * NN_TILE_A;
         if (tap >= 2) ok = mbar_wait(&bars[buf], ((tap - 2) >> 1) & 1) && ok;   // MMAs of tap - 2 done
         for (int e = tid; e < 128 * 4; e += blockDim.x) {
-            const int m = e >> 2, kg = e & 3;
+            // consecutive threads take consecutive rows of one k group: 16-byte
+            // steps inside the core matrices, conflict-free stores
+            const int m = e & 127, kg = e >> 7;
             *(uint4*)(A + umma_canon(m, kg * 8, 16)) = *(const uint4*)(X + halo_row(m, tap) * HLD + kg * 8);
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -225,9 +227,12 @@ DQ_DEV void umma_free(const uint32_t* tslot) {
 
 struct NNSmem {
     float W1[27 * NN_C], b1[NN_C], b2[NN_C], w3[NN_C];
-    float Sin[SIQ];
+    __align__(16) float Sin[SIQ];     // rows of SIX = 12 floats, read as float4
     float red[32];
 };
+
+static_assert((27 * NN_TAP_B + HQ * HLD + 2 * NN_TILE_A) * sizeof(bf16) % 16 == 0 && SIX % 4 == 0,
+              "NNSmem and its Sin rows start on 16-byte boundaries");
 
 // canonical weights, halo, two im2col tiles, NNSmem, three mbarriers and the
 // tensor-memory address
@@ -258,17 +263,33 @@ __global__ void __launch_bounds__(256) k_nn_fwd(NNW w, NNIn in, double* S, bf16*
         sm->Sin[e] = field_at(in, b, in.t_lo + br.t0 - 2 + it, br.y0 - 2 + iy, br.x0 - 2 + ix);
     }
     __syncthreads();
-    // layer 1 on the halo
-    for (int e = tid; e < HQ * NN_C; e += nth) {
-        const int hs = e / NN_C, ch = e % NN_C;
-        const int ht = hs / (HY * HX), hy = (hs / HX) % HY, hx = hs % HX;
-        float pre = sm->b1[ch];
+    // layer 1 on the halo: lane = channel (its 27 weights in registers), one
+    // warp per halo row of HX sites, the input rows read as float4 broadcasts
+    // and reused across the three x taps (taps accumulated in order 0..26)
+    {
+        float w1r[27];
 #pragma unroll
-        for (int tap = 0; tap < 27; ++tap) {
-            const int dt = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
-            pre = fmaf(sm->W1[tap * NN_C + ch], sm->Sin[((ht + dt) * SIY + (hy + dy)) * SIX + (hx + dx)], pre);
+        for (int tap = 0; tap < 27; ++tap) w1r[tap] = sm->W1[tap * NN_C + lane];
+        const float bias = sm->b1[lane];
+        for (int row = warp; row < HT * HY; row += nth >> 5) {
+            const int ht = row / HY, hy = row % HY;
+            float pre[HX];
+#pragma unroll
+            for (int hx = 0; hx < HX; ++hx) pre[hx] = bias;
+#pragma unroll
+            for (int tdy = 0; tdy < 9; ++tdy) {
+                const float4* src = (const float4*)(sm->Sin + ((ht + tdy / 3) * SIY + (hy + tdy % 3)) * SIX);
+                float sv[SIX];
+#pragma unroll
+                for (int k = 0; k < SIX / 4; ++k) *(float4*)&sv[4 * k] = src[k];
+#pragma unroll
+                for (int dx = 0; dx < 3; ++dx)
+#pragma unroll
+                    for (int hx = 0; hx < HX; ++hx) pre[hx] = fmaf(w1r[tdy * 3 + dx], sv[hx + dx], pre[hx]);
+            }
+#pragma unroll
+            for (int hx = 0; hx < HX; ++hx) H[(row * HX + hx) * HLD + lane] = __float2bfloat16(tanhf(pre[hx]));
         }
-        H[hs * HLD + ch] = __float2bfloat16(tanhf(pre));
     }
     __syncthreads();
     float acc[32];
@@ -321,10 +342,11 @@ __global__ void __launch_bounds__(256) k_nn_fwd(NNW w, NNIn in, double* S, bf16*
 // dpre1 = dh1 (1 - h1^2); accumulates dW1, db1, db2, dw3, db3 and writes dpre2
 // (bf16, [b][v][32]) for the weight-gradient kernel.
 // ---------------------------------------------------------------------------
+#define NN_DP1 (NN_C + 1)     // padded dp1 row: a warp's per-site column writes hit 32 banks
 struct NNBSmem {
     float W1g[27 * NN_C], b1g[NN_C], b2g[NN_C], w3g[NN_C], w3[NN_C];
-    float Sin[SIQ];
-    float dp1[BQ * NN_C];
+    __align__(16) float Sin[SIQ];     // rows of SIX = 12 floats, read as float4
+    float dp1[BQ * NN_DP1];           // dpre1 of the core sites, row q at q NN_DP1
 };
 
 // canonical weights, the dpre2 halo, NNBSmem (whose dp1 holds the two im2col
@@ -332,7 +354,8 @@ struct NNBSmem {
 static size_t nn_bwd_smem() {
     return (size_t)(27 * NN_TAP_B + HQ * HLD) * sizeof(bf16) + sizeof(NNBSmem) + 64;
 }
-static_assert(sizeof(float) * BQ * NN_C >= sizeof(bf16) * 2 * NN_TILE_A, "im2col tiles overlay dp1");
+static_assert(sizeof(float) * BQ * NN_DP1 >= sizeof(bf16) * 2 * NN_TILE_A, "im2col tiles overlay dp1");
+static_assert((27 * NN_TAP_B + HQ * HLD) * sizeof(bf16) % 16 == 0, "NNBSmem starts on a 16-byte boundary");
 
 __global__ void __launch_bounds__(256) k_nn_bwd_data(NNW w, NNIn in, const double* r, const bf16* h1g, const bf16* h2g,
                                                      bf16* dp2g, float* grad) {
@@ -355,24 +378,53 @@ __global__ void __launch_bounds__(256) k_nn_bwd_data(NNW w, NNIn in, const doubl
         sm->Sin[e] = field_at(in, b, in.t_lo + br.t0 - 2 + it, br.y0 - 2 + iy, br.x0 - 2 + ix);
     }
     __syncthreads();
-    // dpre2 on the halo (periodic gather of h2)
-    for (int e = tid; e < HQ * NN_C; e += nth) {
-        const int hs = e / NN_C, ch = e % NN_C;
+    // dpre2 on the halo (periodic gather of h2, 16 bytes = 8 channels a thread)
+    for (int e = tid; e < HQ * 4; e += nth) {
+        const int hs = e >> 2, piece = e & 3;
         const int ht = hs / (HY * HX), hy = (hs / HX) % HY, hx = hs % HX;
         const int t = pmod(in.t_lo + br.t0 - 1 + ht, in.Lt), y = pmod(br.y0 - 1 + hy, in.L), x = pmod(br.x0 - 1 + hx, in.L);
-        const float h2 = __bfloat162float(h2g[((size_t)b * in.V + (t * in.L + y) * in.L + x) * NN_C + ch]);
-        D[hs * HLD + ch] = __float2bfloat16(rb * sm->w3[ch] * (1.f - h2 * h2));
+        const uint4 u = ((const uint4*)(h2g + ((size_t)b * in.V + (t * in.L + y) * in.L + x) * NN_C))[piece];
+        const bf16* hv = (const bf16*)&u;
+        uint4 o;
+        bf16* ov = (bf16*)&o;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const float h2 = __bfloat162float(hv[j]);
+            ov[j] = __float2bfloat16(rb * sm->w3[piece * 8 + j] * (1.f - h2 * h2));
+        }
+        *(uint4*)(D + hs * HLD + piece * 8) = o;
     }
     __syncthreads();
-    // core-site sums: db2 = sum dpre2, dw3 = r_b sum h2
-    for (int e = tid; e < BQ * NN_C; e += nth) {
-        const int q = e / NN_C, ch = e % NN_C;
-        if (!core_valid(in, br, q)) continue;
-        const size_t gi = ((size_t)b * in.V + core_site(in, br, q)) * NN_C + ch;
-        const bf16 d = D[halo_row(q, 13) * HLD + ch];
-        dp2g[gi] = d;
-        atomicAdd(&sm->b2g[ch], __bfloat162float(d));
-        atomicAdd(&sm->w3g[ch], rb * __bfloat162float(h2g[gi]));
+    // core-site sums: db2 = sum dpre2, dw3 = r_b sum h2 (a thread keeps one
+    // 8-channel piece; the eight lanes of a piece are summed by shuffles)
+    {
+        float b2p[8], w3p[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) b2p[j] = w3p[j] = 0.f;
+        const int piece = tid & 3;
+        for (int e = tid; e < BQ * 4; e += nth) {
+            const int q = e >> 2;
+            if (!core_valid(in, br, q)) continue;
+            const size_t gi = ((size_t)b * in.V + core_site(in, br, q)) * NN_C + piece * 8;
+            const uint4 d = *(const uint4*)(D + halo_row(q, 13) * HLD + piece * 8);
+            *(uint4*)(dp2g + gi) = d;
+            const uint4 u = *(const uint4*)(h2g + gi);
+            const bf16* dv = (const bf16*)&d;
+            const bf16* hv = (const bf16*)&u;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) { b2p[j] += __bfloat162float(dv[j]); w3p[j] += rb * __bfloat162float(hv[j]); }
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+#pragma unroll
+            for (int o = 4; o < 32; o <<= 1) {
+                b2p[j] += __shfl_xor_sync(0xffffffffu, b2p[j], o);
+                w3p[j] += __shfl_xor_sync(0xffffffffu, w3p[j], o);
+            }
+        if (lane < 4) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) { atomicAdd(&sm->b2g[lane * 8 + j], b2p[j]); atomicAdd(&sm->w3g[lane * 8 + j], w3p[j]); }
+        }
     }
     float acc[32];
     conv_umma(D, Bc, At, bars, tslot, acc);   // W2R holds mirrored taps: the transposed convolution
@@ -381,29 +433,50 @@ __global__ void __launch_bounds__(256) k_nn_bwd_data(NNW w, NNIn in, const doubl
     if (warp < 4) {
         const int q0 = 32 * warp + lane;
         const bool v0 = core_valid(in, br, q0);
-        const int s0 = v0 ? core_site(in, br, q0) : 0;
+        uint4 h1r[NN_C / 8];      // the site's h1 row, 64 bytes
+#pragma unroll
+        for (int k = 0; k < NN_C / 8; ++k) h1r[k] = make_uint4(0u, 0u, 0u, 0u);
+        if (v0) {
+            const uint4* src = (const uint4*)(h1g + ((size_t)b * in.V + core_site(in, br, q0)) * NN_C);
+#pragma unroll
+            for (int k = 0; k < NN_C / 8; ++k) h1r[k] = src[k];
+        }
+        const bf16* h1 = (const bf16*)h1r;
 #pragma unroll
         for (int ch = 0; ch < NN_C; ++ch) {
-            float d0 = 0.f;
-            if (v0) { const float h1 = __bfloat162float(h1g[((size_t)b * in.V + s0) * NN_C + ch]); d0 = acc[ch] * (1.f - h1 * h1); }
-            sm->dp1[q0 * NN_C + ch] = d0;
+            const float hv = __bfloat162float(h1[ch]);
+            sm->dp1[q0 * NN_DP1 + ch] = v0 ? acc[ch] * (1.f - hv * hv) : 0.f;
         }
     }
     umma_free(tslot);
     __syncthreads();
-    // dW1[tap][c] = sum_q s(q + tap) dpre1(q)[c]; db1 = sum dpre1
-    for (int e = tid; e < 28 * NN_C; e += nth) {
-        const int tap = e / NN_C, ch = e % NN_C;
-        float a = 0.f;
-        for (int q = 0; q < BQ; ++q) {
-            const float d = sm->dp1[q * NN_C + ch];
-            if (tap == 27) { a += d; continue; }
-            const int qt = q / (BY * BX), qy = (q / BX) % BY, qx = q % BX;
-            const int dt = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
-            a = fmaf(sm->Sin[((qt + 1 + dt) * SIY + (qy + 1 + dy)) * SIX + (qx + 1 + dx)], d, a);
+    // dW1[tap][c] = sum_q s(q + tap) dpre1(q)[c]; db1 = sum dpre1.  Lane =
+    // channel, one warp per row of BX core sites; the field rows are read as
+    // float4 broadcasts and the warps' partial sums added in shared memory.
+    {
+        float a[28];
+#pragma unroll
+        for (int k = 0; k < 28; ++k) a[k] = 0.f;
+        for (int row = warp; row < BT * BY; row += nth >> 5) {
+            const int qt = row / BY, qy = row % BY;
+            float d[BX];
+#pragma unroll
+            for (int qx = 0; qx < BX; ++qx) { d[qx] = sm->dp1[(row * BX + qx) * NN_DP1 + lane]; a[27] += d[qx]; }
+#pragma unroll
+            for (int tdy = 0; tdy < 9; ++tdy) {
+                const float4* src = (const float4*)(sm->Sin + ((qt + 1 + tdy / 3) * SIY + (qy + 1 + tdy % 3)) * SIX);
+                float sv[SIX];
+#pragma unroll
+                for (int k = 0; k < SIX / 4; ++k) *(float4*)&sv[4 * k] = src[k];
+#pragma unroll
+                for (int dx = 0; dx < 3; ++dx)
+#pragma unroll
+                    for (int qx = 0; qx < BX; ++qx) a[tdy * 3 + dx] = fmaf(sv[qx + 1 + dx], d[qx], a[tdy * 3 + dx]);
+            }
         }
-        if (tap < 27) sm->W1g[tap * NN_C + ch] = a;
-        else sm->b1g[ch] = a;
+#pragma unroll
+        for (int tap = 0; tap < 27; ++tap) atomicAdd(&sm->W1g[tap * NN_C + lane], a[tap]);
+        atomicAdd(&sm->b1g[lane], a[27]);
     }
     __syncthreads();
     // gradient layout: W1 [27][32], b1 [32], W2 [27][32][32], b2 [32], w3 [32], b3
@@ -421,79 +494,102 @@ __global__ void __launch_bounds__(256) k_nn_bwd_data(NNW w, NNIn in, const doubl
 }
 
 // ---------------------------------------------------------------------------
-// backward, weight part: dW2[tap][ci][co] = sum_v h1(v + tap)[ci] dpre2(v)[co],
-// per brick as 27 GEMMs (M = ci, N = co, K = 128 sites); a persistent CTA
-// accumulates its bricks in shared memory and adds them to grad once.
+// backward, weight part: dW2[tap][ci][co] = sum over fields b and core sites q
+// of h1(q + tap)[ci] dpre2(q)[co], per brick a 32 x 32 GEMM with K = 128 sites
+// for each tap.  Grid (CTAs, 3): blockIdx.y = dt, the nine warps take the nine
+// taps (dt, dy, dx).  A CTA walks bricks x fields holding its warps' 32 x 32
+// tiles in registers and adds them to grad once; each job's gather (the h1
+// halo slices dt .. dt + BT - 1 and the dpre2 core) is loaded into registers
+// while the previous job's MMAs run.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_nn_wgrad(NNIn in, int nbricks, int B, const bf16* h1g, const bf16* dp2g,
-                                                  float* grad) {
+#define WG_THREADS 288
+#define WG_H (BT * HY * HX)                                  // halo sites of one dt range: 144
+#define WG_PIECES ((WG_H + BQ) * NN_C / 8)                    // 16-byte pieces per job: 1088
+#define WG_PER ((WG_PIECES + WG_THREADS - 1) / WG_THREADS)   // 4
+
+__global__ void __launch_bounds__(WG_THREADS, 2) k_nn_wgrad(NNIn in, int nbricks, int B, const bf16* h1g,
+                                                        const bf16* dp2g, float* grad) {
     extern __shared__ __align__(16) unsigned char smraw[];
-    float* acc_s = (float*)smraw;                       // 27 x 32 x 32
-    bf16* H = (bf16*)(acc_s + 27 * NN_C * NN_C);        // h1 halo, HQ x HLD
+    bf16* H = (bf16*)smraw;                             // h1 halo, HQ x HLD (slices dt .. dt + BT - 1 filled)
     bf16* D = H + HQ * HLD;                             // dpre2 core, BQ x HLD
-    const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5;
-    for (int e = tid; e < 27 * NN_C * NN_C; e += nth) acc_s[e] = 0.f;
-    for (int job = blockIdx.x; job < nbricks * B; job += gridDim.x) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int dt = blockIdx.y, tap = 9 * dt + warp;
+    const int njobs = nbricks * B;
+    uint4 pre[WG_PER];
+    auto fetch = [&](int job) {
         const int b = job / nbricks;
         const Brick br = brick_of(in, job % nbricks);
-        __syncthreads();
-        for (int e = tid; e < HQ * NN_C; e += nth) {
-            const int hs = e / NN_C, ch = e % NN_C;
-            const int ht = hs / (HY * HX), hy = (hs / HX) % HY, hx = hs % HX;
-            const int t = pmod(in.t_lo + br.t0 - 1 + ht, in.Lt), y = pmod(br.y0 - 1 + hy, in.L), x = pmod(br.x0 - 1 + hx, in.L);
-            H[hs * HLD + ch] = h1g[((size_t)b * in.V + (t * in.L + y) * in.L + x) * NN_C + ch];
-        }
-        for (int e = tid; e < BQ * NN_C; e += nth) {
-            const int q = e / NN_C, ch = e % NN_C;
-            D[q * HLD + ch] = core_valid(in, br, q) ? dp2g[((size_t)b * in.V + core_site(in, br, q)) * NN_C + ch]
-                                                    : __float2bfloat16(0.f);
-        }
-        __syncthreads();
-        const int mm = lane >> 3;
-        for (int tap = warp; tap < 27; tap += nth / 32) {
-            float c[2][4][4] = {};
-#pragma unroll 1
-            for (int kb = 0; kb < BQ; kb += 16) {
-                uint32_t a[2][4], bq[2][4];
-                // A[m = ci][k = site]: stored rows = sites (k), columns = ci -> transposed loads
 #pragma unroll
-                for (int mt = 0; mt < 2; ++mt) {
-                    const int site = kb + (mm >> 1) * 8 + (lane & 7);
-                    const bf16* p = H + halo_row(site, tap) * HLD + mt * 16 + (mm & 1) * 8;
-                    ldsm_x4_t(a[mt][0], a[mt][1], a[mt][2], a[mt][3], p);
-                }
-                // B[k = site][n = co]: stored rows = sites, columns = co -> transposed loads
-#pragma unroll
-                for (int np = 0; np < 2; ++np) {
-                    const int site = kb + (mm & 1) * 8 + (lane & 7);
-                    const bf16* p = D + site * HLD + np * 16 + (mm >> 1) * 8;
-                    ldsm_x4_t(bq[np][0], bq[np][1], bq[np][2], bq[np][3], p);
-                }
-#pragma unroll
-                for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-                    for (int np = 0; np < 2; ++np) {
-                        mma_bf16(c[mt][2 * np], a[mt][0], a[mt][1], a[mt][2], a[mt][3], bq[np][0], bq[np][1]);
-                        mma_bf16(c[mt][2 * np + 1], a[mt][0], a[mt][1], a[mt][2], a[mt][3], bq[np][2], bq[np][3]);
-                    }
+        for (int k = 0; k < WG_PER; ++k) {
+            const int e = tid + k * WG_THREADS, r = e >> 2, piece = e & 3;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (r < WG_H) {
+                const int hs = dt * HY * HX + r;
+                const int ht = hs / (HY * HX), hy = (hs / HX) % HY, hx = hs % HX;
+                const int t = pmod(in.t_lo + br.t0 - 1 + ht, in.Lt), y = pmod(br.y0 - 1 + hy, in.L),
+                          x = pmod(br.x0 - 1 + hx, in.L);
+                v = ((const uint4*)(h1g + ((size_t)b * in.V + (t * in.L + y) * in.L + x) * NN_C))[piece];
+            } else if (r < WG_H + BQ && core_valid(in, br, r - WG_H)) {
+                v = ((const uint4*)(dp2g + ((size_t)b * in.V + core_site(in, br, r - WG_H)) * NN_C))[piece];
             }
-            const int g = lane >> 2, t4 = lane & 3;
+            pre[k] = v;
+        }
+    };
+    float c[2][4][4] = {};
+    int job = blockIdx.x;
+    if (job < njobs) fetch(job);
+    for (; job < njobs; job += gridDim.x) {
+        __syncthreads();                                // the previous job's MMAs are done with H and D
+#pragma unroll
+        for (int k = 0; k < WG_PER; ++k) {
+            const int e = tid + k * WG_THREADS, r = e >> 2, piece = e & 3;
+            if (r < WG_H + BQ) {
+                bf16* dst = r < WG_H ? H + (dt * HY * HX + r) * HLD : D + (r - WG_H) * HLD;
+                *(uint4*)(dst + piece * 8) = pre[k];
+            }
+        }
+        __syncthreads();
+        if (job + (int)gridDim.x < njobs) fetch(job + gridDim.x);
+        const int mm = lane >> 3;
+#pragma unroll 1
+        for (int kb = 0; kb < BQ; kb += 16) {
+            uint32_t a[2][4], bq[2][4];
+            // A[m = ci][k = site]: stored rows = sites (k), columns = ci -> transposed loads
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt) {
+                const int site = kb + (mm >> 1) * 8 + (lane & 7);
+                const bf16* p = H + halo_row(site, tap) * HLD + mt * 16 + (mm & 1) * 8;
+                ldsm_x4_t(a[mt][0], a[mt][1], a[mt][2], a[mt][3], p);
+            }
+            // B[k = site][n = co]: stored rows = sites, columns = co -> transposed loads
+#pragma unroll
+            for (int np = 0; np < 2; ++np) {
+                const int site = kb + (mm & 1) * 8 + (lane & 7);
+                const bf16* p = D + site * HLD + np * 16 + (mm >> 1) * 8;
+                ldsm_x4_t(bq[np][0], bq[np][1], bq[np][2], bq[np][3], p);
+            }
 #pragma unroll
             for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int ci0 = mt * 16 + g, co = 8 * j + 2 * t4;
-                    float* dst = acc_s + (tap * NN_C) * NN_C;
-                    dst[ci0 * NN_C + co] += c[mt][j][0];
-                    dst[ci0 * NN_C + co + 1] += c[mt][j][1];
-                    dst[(ci0 + 8) * NN_C + co] += c[mt][j][2];
-                    dst[(ci0 + 8) * NN_C + co + 1] += c[mt][j][3];
+                for (int np = 0; np < 2; ++np) {
+                    mma_bf16(c[mt][2 * np], a[mt][0], a[mt][1], a[mt][2], a[mt][3], bq[np][0], bq[np][1]);
+                    mma_bf16(c[mt][2 * np + 1], a[mt][0], a[mt][1], a[mt][2], a[mt][3], bq[np][2], bq[np][3]);
                 }
         }
     }
-    __syncthreads();
-    for (int e = tid; e < 27 * NN_C * NN_C; e += nth) atomicAdd(&grad[NN_GW2 + e], acc_s[e]);
+    const int g = lane >> 2, t4 = lane & 3;
+    float* dst = grad + NN_GW2 + tap * NN_C * NN_C;
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int ci0 = mt * 16 + g, co = 8 * j + 2 * t4;
+            atomicAdd((float2*)(dst + ci0 * NN_C + co), make_float2(c[mt][j][0], c[mt][j][1]));
+            atomicAdd((float2*)(dst + (ci0 + 8) * NN_C + co), make_float2(c[mt][j][2], c[mt][j][3]));
+        }
 }
+static size_t nn_wgrad_smem() { return (size_t)(HQ + BQ) * HLD * sizeof(bf16); }
+static_assert(NN_GW2 % 2 == 0, "float2 atomics on the W2 gradient");
 
 // Adam on the FP32 master weights, then the BF16 tiles of W2 for both GEMMs.
 __global__ void k_nn_adam(float* theta, const float* grad, float* m1, float* m2, int n, float lr, float b1c, float b2c) {
@@ -530,8 +626,7 @@ static void nn_attrs() {
     cudaFuncSetAttribute(k_nn_fwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nn_fwd_smem());
     cudaFuncSetAttribute(k_nn_fwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nn_fwd_smem());
     cudaFuncSetAttribute(k_nn_bwd_data, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nn_bwd_smem());
-    size_t wg = (size_t)27 * NN_C * NN_C * sizeof(float) + (size_t)(HQ + BQ) * HLD * sizeof(bf16) + 64;
-    cudaFuncSetAttribute(k_nn_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wg);
+    cudaFuncSetAttribute(k_nn_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nn_wgrad_smem());
     g_nn_attr = 1;
 }
 
@@ -551,10 +646,11 @@ void launch_nn_backward(const NNW& w, const NNIn& in, int B, const double* r, co
     nn_attrs();
     dim3 grid(nn_nbricks(in), B);
     k_nn_bwd_data<<<grid, 256, nn_bwd_smem(), st>>>(w, in, r, h1g, h2g, dp2g, grad);
-    size_t wg = (size_t)27 * NN_C * NN_C * sizeof(float) + (size_t)(HQ + BQ) * HLD * sizeof(bf16) + 64;
+    // about two CTAs per SM over the three tap groups; each CTA adds its
+    // 9 x 32 x 32 tile to grad once
     int nb = nn_nbricks(in);
-    int g = std::min(nb * B, nsm);
-    k_nn_wgrad<<<g, 256, wg, st>>>(in, nb, B, h1g, dp2g, grad);
+    int gx = std::max(1, std::min(nb * B, (2 * nsm + 2) / 3));
+    k_nn_wgrad<<<dim3(gx, 3), WG_THREADS, nn_wgrad_smem(), st>>>(in, nb, B, h1g, dp2g, grad);
 }
 
 void launch_nn_adam(float* theta, const float* grad, float* m1, float* m2, int n, float lr, float b1c, float b2c,
