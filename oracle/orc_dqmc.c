@@ -222,9 +222,10 @@ orc_model *orc_model_new(const orc_params *pin) {
     orc_model *m = calloc(1, sizeof(orc_model));
     m->p = *pin;
     orc_params *p = &m->p;
-    if (orc_latt_build(&m->L, p->lattice, p->l1, p->l2) != 0) { free(m); return NULL; }
+    if (p->lattice != ORC_CUBIC) p->l3 = 1;
+    if (orc_latt_build(&m->L, p->lattice, p->l1, p->l2, p->l3) != 0) { free(m); return NULL; }
     p->theta = p->theta * M_PI;
-    m->lq = p->l1 * p->l2;
+    m->lq = m->L.ncell;
     m->ndim = m->L.nsites;
     m->ne = m->ndim / 2 + (int)(p->nu * m->ndim / 8.0);
     m->ltrot = (int)lround(p->beta / p->dtau);
@@ -1042,6 +1043,71 @@ void orc_obser_init(orc_chain *c) {   /* dqmc_measure_2d.f90:105-130 */
 
 static int npbc_cyc(int nr, int l) { if (nr > l) return nr - l; if (nr < 1) return nr + l; return nr; }
 
+/* equaltime_measure of the cubic lattice after energy_bin(1:2)
+ * (src/dqmc_measure/equaltime_measure3d.f90:43-179): zkint over the six bond
+ * families of the A sites (no rt, no t2 term), zint_u, and cpcm, spsm, nn (+ zn),
+ * bondcorr (+ zb) with the bond partner nnlist(j, 1).  The bins are the
+ * (no_i, no_j) = (1, 1) block of the 2D layout; pair_onsite, jj, pair_nn,
+ * pair_sn, zj and energy_bin(5:10) do not exist here and stay 0.  c->gfc
+ * already holds Gc. */
+static void measure_3d(orc_chain *c, zc zphi) {
+    const orc_model *m = c->m;
+    const orc_latt *L = &m->L;
+    const int N = m->ndim, lq = m->lq, nnf = L->nn_nf, nflr = m->p.nflr;
+    const zc *g = c->gf, *gc = c->gfc;
+#define GC3(i, j) gc[ZIDX((i), (j), N)]
+#define GF3(i, j) g[ZIDX((i), (j), N)]
+    zc zk = 0;
+    for (int b = 0; b < L->nn_lf; ++b) {
+        const int i0 = L->nnlf_list[b] - 1;
+        for (int nf = 1; nf <= nnf; ++nf) {
+            const int in = L->nnlist[i0 * nnf + nf - 1] - 1;
+            zk += -2.0 * creal(GC3(i0, in) * m->expar_nn[i0 * nnf + nf - 1]);
+        }
+    }
+    c->energy_bin[2] += zk * zphi;
+    zc zu = 0;
+    for (int i = 0; i < L->nsites; ++i) zu += GC3(i, i) * GC3(i, i);
+    c->energy_bin[3] += zu * zphi;
+    const double fsp = 1.0 - 1.0 / (double)(nflr * nflr), fn = 1.0 / (double)nflr;
+    zc *cp = zalloc(lq), *sp = zalloc(lq), *nn = zalloc(lq), *bb = zalloc(lq);
+    zc zn = 0, zb = 0;
+    for (int j = 0; j < N; ++j) {
+        const int nuj = L->list[j * 2] - 1;
+        zn += GC3(j, j);
+        for (int i = 0; i < N; ++i) {
+            const int k = L->imj[(L->list[i * 2] - 1) * lq + nuj] - 1;
+            cp[k] += GC3(i, j);
+            sp[k] += GC3(i, j) * GF3(i, j) * fsp;
+            nn[k] += GC3(i, i) * GC3(j, j) + fn * GC3(i, j) * GF3(i, j);
+        }
+    }
+    for (int nuj = 0; nuj < lq; ++nuj) {
+        const int j0 = nuj, jn = L->nnlist[j0 * nnf] - 1;
+        const zc zj = m->expar_nn[j0 * nnf];
+        zb += zj * GC3(j0, jn) + conj(zj) * GC3(jn, j0);
+        for (int nui = 0; nui < lq; ++nui) {
+            const int i0 = nui, in = L->nnlist[i0 * nnf] - 1;
+            const zc zi = m->expar_nn[i0 * nnf];
+            const int k = L->imj[nui * lq + nuj] - 1;
+            bb[k] += (zj * GC3(j0, jn) + conj(zj) * GC3(jn, j0)) * (zi * GC3(i0, in) + conj(zi) * GC3(in, i0)) +
+                     (zi * zj * GC3(i0, jn) * GF3(in, j0) + conj(zi) * conj(zj) * GC3(in, j0) * GF3(i0, jn) +
+                      zi * conj(zj) * GC3(i0, j0) * GF3(in, jn) + conj(zi) * zj * GC3(in, jn) * GF3(i0, j0)) * fn;
+        }
+    }
+    for (int k = 0; k < lq; ++k) {
+        c->zcpcm_bin[k] += cp[k] * zphi;
+        c->zspsm_bin[k] += sp[k] * zphi;
+        c->znn_bin[k] += nn[k] * zphi;
+        c->zbb_bin[k] += bb[k] * zphi;
+    }
+    c->zn_bin[0] += zn * zphi;
+    c->zb_bin += zb * zphi;
+    free(cp); free(sp); free(nn); free(bb);
+#undef GC3
+#undef GF3
+}
+
 void orc_measure(orc_chain *c, int nt) {
     (void)nt;
     const orc_model *m = c->m;
@@ -1061,6 +1127,7 @@ void orc_measure(orc_chain *c, int nt) {
     zc zne = 0;
     for (int i = 0; i < N; ++i) zne += GC(i, i);
     c->energy_bin[1] += zne * zphi / (double)lq;
+    if (L->kind == ORC_CUBIC) { measure_3d(c, zphi); return; }
     /* zkint; the chain's (equaltime_measure1d.f90) carries the factor nflr rt on
      * the bonds and 2 t2 on the two second neighbours */
     const int chain = (L->kind == ORC_CHAIN);
@@ -1367,7 +1434,10 @@ static int green_tau(int N, const zc *ure, const double *dre, const zc *vre, con
 }
 
 /* dyn_measure (src/dqmc_measure/dyn_measure.f90:1-101): the density-density
- * correlation znn_tau(imj, no_i, no_j, nt), the only active observable */
+ * correlation znn_tau(imj, no_i, no_j, nt), the only active observable.  On
+ * the cubic lattice (dyn_measure3d.f90:44-66) also zspsm_tau(imj, nt) +=
+ * -G(0,t)_ji G(t,0)_ij (1 - 1/nflr^2) and gtau0(imj, nt) += G(t,0)_ij, kept in
+ * the (no_i, no_j) = (2, 1) and (1, 2) slots of the 2D layout. */
 static void dyn_measure(orc_chain *c, int nt, const zc *gt0, const zc *g0t, const zc *gtt, const zc *g00) {
     const orc_model *m = c->m;
     const orc_latt *L = &m->L;
@@ -1384,6 +1454,11 @@ static void dyn_measure(orc_chain *c, int nt, const zc *gt0, const zc *g0t, cons
             z[(imj - 1) + lq * (no_i - 1) + 2 * lq * (no_j - 1)] +=
                 (0.5 - creal(gtt[ZIDX(i, i, N)])) * (0.5 - creal(g00[ZIDX(j, j, N)]))
                 - (1.0 / m->p.nflr) * g0t[ZIDX(j, i, N)] * gt0[ZIDX(i, j, N)];
+            if (L->kind == ORC_CUBIC) {
+                const double fsp = 1.0 - 1.0 / (double)(m->p.nflr * m->p.nflr);
+                z[(imj - 1) + lq] += -g0t[ZIDX(j, i, N)] * gt0[ZIDX(i, j, N)] * fsp;
+                z[(imj - 1) + 2 * lq] += gt0[ZIDX(i, j, N)];
+            }
         }
     }
     zc *bin = c->znn_tau_bin + (size_t)4 * lq * (nt - 1);

@@ -10,9 +10,10 @@ typedef double _Complex zc;
 #define ZIDX(i, j, ld) ((size_t)(i) + (size_t)(j) * (size_t)(ld))
 
 typedef struct {
-    int kind, l1, l2, ncell, nsub, nsites, z_plq, nn_nf, nn_lf, nsn;
+    int kind, l1, l2, l3, ncell, nsub, nsites, z_plq, nn_nf, nn_lf, nsn;
     double a1[2], a2[2], b1[2], b2[2];
     int *ulist;      /* [ncell][2] 1-based cell coordinates, ulist[c*2+d]        */
+    int *ulist3;     /* cubic: [ncell][3] (i1, i2, i3), ulist3[c*3+d]             */
     int *list;       /* [nsites][2] (cell, orb), 1-based values                  */
     int *cord;       /* [nsites][2] cell coordinates                              */
     double *rcord;   /* [nsites][2]                                               */
@@ -27,7 +28,7 @@ typedef struct {
     zc *zexpiqr;     /* [ncell(site)][ncell(k)] zexpiqr(nk,i) at [i*ncell+nk]    */
 } orc_latt;
 
-int  orc_latt_build(orc_latt *L, int kind, int l1, int l2);
+int  orc_latt_build(orc_latt *L, int kind, int l1, int l2, int l3);
 void orc_latt_free(orc_latt *L);
 zc   orc_expar(const orc_latt *L, int i, int nf, double xmag, double fx, double fy, double dimer);
 

@@ -1,7 +1,8 @@
-/* Square, honeycomb and chain lattice tables, restated from src/lattice.f90
- * (setup_latt2d_sub 386-491, setup_honeycomb_sub 611-776,
- * setup_square_sub 792-961, setup_latt1d_sub 67-135, setup_chain_sub 240-316)
- * and the hopping phase expar (src/dqmc_config_h0/expar.f90, expar1d.f90).
+/* Square, honeycomb, chain and cubic lattice tables, restated from
+ * src/lattice.f90 (setup_latt2d_sub 386-491, setup_honeycomb_sub 611-776,
+ * setup_square_sub 792-961, setup_latt1d_sub 67-135, setup_chain_sub 240-316,
+ * setup_latt3d_sub 1033-1157, setup_cubic_sub 1280-1472) and the hopping
+ * phase expar (src/dqmc_config_h0/expar.f90, expar1d.f90, expar3d.f90).
  * Test infrastructure only.
  * Stored values are 1-based as in the reference. */
 #include <math.h>
@@ -18,7 +19,7 @@ static int npbc(int nr, int l) {   /* lattice.f90:493-500 */
 void orc_latt_free(orc_latt *L) {
     free(L->ulist); free(L->list); free(L->cord); free(L->rcord); free(L->nnlist);
     free(L->snlist); free(L->nnlf_list); free(L->nnveci); free(L->nnvecr); free(L->imj);
-    free(L->plq_cord); free(L->listk); free(L->zexpiqr);
+    free(L->plq_cord); free(L->listk); free(L->zexpiqr); free(L->ulist3);
     memset(L, 0, sizeof(*L));
 }
 
@@ -262,11 +263,100 @@ static void setup_chain(orc_latt *L, int l1) {
     for (int i = 0; i < ns; ++i) L->plq_cord[i] = i + 1;
 }
 
-int orc_latt_build(orc_latt *L, int kind, int l1, int l2) {
+/* setup_latt3d_sub + setup_cubic_sub.  Cell (= site) index
+ * (i3-1) l1 l2 + (i1-1) l2 + i2; listk with l (a3) outermost, then m (a1),
+ * then n (a2); zexpiqr(nk, i) = exp(i k.R_i) with k = 2 pi (m/l1, n/l2, l/l3);
+ * nnlist directions +a3, +a1, +a2, -a3, -a1, -a2; nnlf_list the sites with
+ * i1 + i2 + i3 even in loop order (i1 outer, i3 inner); twelve second
+ * neighbours; plq_cord the eight corners of the cube at each cell, the cells
+ * grouped by the parities of (i1, i2, i3). */
+static void setup_cubic(orc_latt *L, int l1, int l2, int l3) {
+    L->kind = ORC_CUBIC; L->l1 = l1; L->l2 = l2; L->l3 = l3;
+    const int nc = l1 * l2 * l3;
+    L->ncell = nc; L->nsub = 1; L->nsites = nc; L->z_plq = 8; L->nn_nf = 6; L->nn_lf = nc / 2; L->nsn = 12;
+#define CELL(a, b, c) ((npbc((c), l3) - 1) * l1 * l2 + (npbc((a), l1) - 1) * l2 + npbc((b), l2))
+    L->ulist3 = malloc(sizeof(int) * 3 * nc);
+    L->list = malloc(sizeof(int) * 2 * nc);
+    L->nnlf_list = malloc(sizeof(int) * (L->nn_lf > 0 ? L->nn_lf : 1));
+    int ind = 0;
+    for (int i1 = 1; i1 <= l1; ++i1)
+        for (int i2 = 1; i2 <= l2; ++i2)
+            for (int i3 = 1; i3 <= l3; ++i3) {
+                const int c = CELL(i1, i2, i3) - 1;
+                L->ulist3[c * 3] = i1; L->ulist3[c * 3 + 1] = i2; L->ulist3[c * 3 + 2] = i3;
+                L->list[c * 2] = c + 1; L->list[c * 2 + 1] = 1;
+                if ((i1 + i2 + i3) % 2 == 0 && ind < L->nn_lf) L->nnlf_list[ind++] = c + 1;
+            }
+    L->listk = malloc(sizeof(int) * 3 * nc);
+    int k = 0;
+    for (int l = -(l3 + 1) / 2 + 1; l <= l3 / 2; ++l)
+        for (int mm = -(l1 + 1) / 2 + 1; mm <= l1 / 2; ++mm)
+            for (int n = -(l2 + 1) / 2 + 1; n <= l2 / 2; ++n) {
+                L->listk[k * 3] = mm; L->listk[k * 3 + 1] = n; L->listk[k * 3 + 2] = l; ++k;
+            }
+    L->imj = malloc(sizeof(int) * nc * nc);
+    for (int j = 0; j < nc; ++j)
+        for (int i = 0; i < nc; ++i) {
+            int nx = npbc(L->ulist3[i * 3] - L->ulist3[j * 3], l1);
+            int ny = npbc(L->ulist3[i * 3 + 1] - L->ulist3[j * 3 + 1], l2);
+            int nz = npbc(L->ulist3[i * 3 + 2] - L->ulist3[j * 3 + 2], l3);
+            L->imj[i * nc + j] = (nz - 1) * l1 * l2 + ny + (nx - 1) * l2;
+        }
+    L->zexpiqr = malloc(sizeof(zc) * nc * nc);
+    for (int i = 0; i < nc; ++i)
+        for (int nk = 0; nk < nc; ++nk) {
+            double ph = 2.0 * M_PI * ((double)L->listk[nk * 3] * L->ulist3[i * 3] / l1 +
+                                      (double)L->listk[nk * 3 + 1] * L->ulist3[i * 3 + 1] / l2 +
+                                      (double)L->listk[nk * 3 + 2] * L->ulist3[i * 3 + 2] / l3);
+            L->zexpiqr[i * nc + nk] = cexp(I * ph);
+        }
+    static const int dnn[6][3] = {{0, 0, 1}, {1, 0, 0}, {0, 1, 0}, {0, 0, -1}, {-1, 0, 0}, {0, -1, 0}};
+    static const int dsn[12][3] = {{1, 1, 0}, {-1, 1, 0}, {-1, -1, 0}, {1, -1, 0}, {0, 1, 1}, {0, 1, -1},
+                                   {0, -1, -1}, {0, -1, 1}, {1, 0, 1}, {1, 0, -1}, {-1, 0, -1}, {-1, 0, 1}};
+    L->nnlist = malloc(sizeof(int) * nc * 6);
+    L->snlist = malloc(sizeof(int) * nc * 12);
+    for (int i = 0; i < nc; ++i) {
+        const int u1 = L->ulist3[i * 3], u2 = L->ulist3[i * 3 + 1], u3 = L->ulist3[i * 3 + 2];
+        for (int f = 0; f < 6; ++f) L->nnlist[i * 6 + f] = CELL(u1 + dnn[f][0], u2 + dnn[f][1], u3 + dnn[f][2]);
+        for (int f = 0; f < 12; ++f) L->snlist[i * 12 + f] = CELL(u1 + dsn[f][0], u2 + dsn[f][1], u3 + dsn[f][2]);
+    }
+    /* the bonds of expar3d carry no phase: zero vectors */
+    L->nnveci = calloc((size_t)nc * 6 * 2, sizeof(int));
+    L->nnvecr = calloc((size_t)nc * 6 * 2, sizeof(double));
+    L->cord = malloc(sizeof(int) * 2 * nc);
+    L->rcord = malloc(sizeof(double) * 2 * nc);
+    for (int i = 0; i < nc; ++i) {
+        L->cord[i * 2] = L->ulist3[i * 3]; L->cord[i * 2 + 1] = L->ulist3[i * 3 + 1];
+        L->rcord[i * 2] = L->ulist3[i * 3]; L->rcord[i * 2 + 1] = L->ulist3[i * 3 + 1];
+    }
+    int nd[8] = {0}, id[8] = {0};
+#define PTYPE(a, b, c) (((a) % 2 == 0) * 4 + ((b) % 2 == 0) * 2 + ((c) % 2 == 0))
+    for (int i1 = 1; i1 <= l1; ++i1)
+        for (int i2 = 1; i2 <= l2; ++i2)
+            for (int i3 = 1; i3 <= l3; ++i3) nd[PTYPE(i1, i2, i3)]++;
+    L->plq_cord = malloc(sizeof(int) * 8 * nc);
+    for (int i1 = 1; i1 <= l1; ++i1)
+        for (int i2 = 1; i2 <= l2; ++i2)
+            for (int i3 = 1; i3 <= l3; ++i3) {
+                const int t = PTYPE(i1, i2, i3);
+                int q = id[t]++;
+                for (int u = 0; u < t; ++u) q += nd[u];
+                int *pc = &L->plq_cord[q * 8];
+                pc[0] = CELL(i1, i2, i3);         pc[1] = CELL(i1 + 1, i2, i3);
+                pc[2] = CELL(i1 + 1, i2 + 1, i3); pc[3] = CELL(i1, i2 + 1, i3);
+                pc[4] = CELL(i1, i2, i3 + 1);     pc[5] = CELL(i1 + 1, i2, i3 + 1);
+                pc[6] = CELL(i1 + 1, i2 + 1, i3 + 1); pc[7] = CELL(i1, i2 + 1, i3 + 1);
+            }
+#undef PTYPE
+#undef CELL
+}
+
+int orc_latt_build(orc_latt *L, int kind, int l1, int l2, int l3) {
     memset(L, 0, sizeof(*L));
     if (kind == ORC_SQUARE) setup_square(L, l1, l2);
     else if (kind == ORC_HONEYCOMB) setup_honeycomb(L, l1, l2);
     else if (kind == ORC_CHAIN) setup_chain(L, l1);
+    else if (kind == ORC_CUBIC) setup_cubic(L, l1, l2, l3);
     else return -1;
     return 0;
 }
@@ -274,6 +364,7 @@ int orc_latt_build(orc_latt *L, int kind, int l1, int l2) {
 /* expar.f90: Landau-gauge Peierls phase for bond (i, nf), twist flux and
  * dimerisation.  i is 0-based, nf is 1-based as in the reference. */
 zc orc_expar(const orc_latt *L, int i, int nf, double xmag, double fx, double fy, double dimer) {
+    if (L->kind == ORC_CUBIC) return 1.0;      /* expar3d.f90 */
     int k = (i * L->nn_nf + (nf - 1)) * 2;
     int nax = L->nnveci[k], nay = L->nnveci[k + 1];
     double vr1 = L->nnvecr[k], vr2 = L->nnvecr[k + 1];

@@ -35,15 +35,21 @@ extern "C" const char* dqmc_gpu_last_error(void) { return g_err.c_str(); }
 // ---------------------------------------------------------------------------
 extern "C" int dqmc_params_derive(dqmc_params* p) {
     if (!p) return fail(DQMC_EINVAL, "null params");
-    if (p->lattice != DQMC_LATT_SQUARE && p->lattice != DQMC_LATT_HONEYCOMB && p->lattice != DQMC_LATT_CHAIN)
-        return fail(DQMC_EINVAL, "lattice must be square, honeycomb or chain");
+    if (p->lattice < DQMC_LATT_SQUARE || p->lattice > DQMC_LATT_CUBIC)
+        return fail(DQMC_EINVAL, "lattice must be square, honeycomb, chain or cubic");
+    if (p->lattice != DQMC_LATT_CUBIC) p->l3 = 1;
     if (p->lattice == DQMC_LATT_CHAIN) {
         if (p->l2 != 1 || p->l1 < 4 || p->l1 % 2) return fail(DQMC_EINVAL, "the chain needs l2 = 1 and an even l1 >= 4");
+    } else if (p->lattice == DQMC_LATT_CUBIC) {
+        // the A sublattice (i1 + i2 + i3 even) and its six bond families cover
+        // every bond once only for even lengths (setup_cubic_sub, lattice.f90:1300-1312)
+        if (p->l1 < 2 || p->l2 < 2 || p->l3 < 2 || p->l1 % 2 || p->l2 % 2 || p->l3 % 2)
+            return fail(DQMC_EINVAL, "the cubic lattice needs even l1, l2, l3 >= 2");
     } else if (p->l1 < 2 || p->l2 < 2) {
         return fail(DQMC_EINVAL, "l1, l2 must be >= 2");
     }
     if (p->dtau <= 0 || p->beta <= 0) return fail(DQMC_EINVAL, "beta, dtau must be > 0");
-    p->lq = p->l1 * p->l2;
+    p->lq = p->l1 * p->l2 * p->l3;
     p->ndim = (p->lattice == DQMC_LATT_HONEYCOMB) ? 2 * p->lq : p->lq;
     p->ne = p->ndim / 2 + (int)(p->nu * p->ndim / 8.0);
     p->ltrot = (int)std::lround(p->beta / p->dtau);
@@ -84,7 +90,7 @@ struct HostModel {
     dqmc_params p;
     int N, lq, nsub, nn_nf, nn_lf, z_plq, nsn, lcomp, nublock_dev;
     double a1[2], a2[2];
-    std::vector<int> cell1, cell2;        // unit-cell coordinates of site (1-based)
+    std::vector<int> cell1, cell2, cell3; // unit-cell coordinates of site (1-based; cell3 cubic only)
     std::vector<double> rc1, rc2;         // real-space coordinates of site
     std::vector<int> nnlist, snlist;      // [site][nf] 0-based
     std::vector<int> nnveci;              // [site][nf][2]
@@ -108,9 +114,72 @@ struct HostModel {
     std::vector<int> wrap_step;           // [n][2] 1-based
 };
 
+// setup_latt3d_sub / setup_cubic_sub (src/lattice.f90:1033-1157, 1280-1472).
+// Site s = (i3-1) l1 l2 + (i1-1) l2 + i2 (1-based, i2 fastest) is also the
+// cell.  Bond families from the A sites (i1 + i2 + i3 even, in the order of the
+// loops i1, i2, i3): +a3, +a1, +a2, -a3, -a1, -a2; twelve second neighbours;
+// eight-site cubes in eight parity classes; imj(i, j) = (nz-1) l1 l2 + ny +
+// (nx-1) l2 with n = npbc(u_i - u_j).
+static void build_cubic(HostModel& m) {
+    const dqmc_params& p = m.p;
+    const int l1 = p.l1, l2 = p.l2, l3 = p.l3;
+    m.a1[0] = 1; m.a1[1] = 0; m.a2[0] = 0; m.a2[1] = 1;
+    m.lq = l1 * l2 * l3;
+    m.nsub = 1; m.N = m.lq; m.nn_nf = 6; m.nn_lf = m.lq / 2; m.z_plq = 8; m.nsn = 12;
+    const int N = m.N;
+    auto site = [&](int i1, int i2, int i3) { return (npbc(i3, l3) - 1) * l1 * l2 + (npbc(i1, l1) - 1) * l2 + npbc(i2, l2) - 1; };
+    m.cell1.resize(N); m.cell2.resize(N); m.cell3.resize(N); m.rc1.resize(N); m.rc2.resize(N);
+    for (int i1 = 1; i1 <= l1; ++i1)
+        for (int i2 = 1; i2 <= l2; ++i2)
+            for (int i3 = 1; i3 <= l3; ++i3) {
+                const int s = site(i1, i2, i3);
+                m.cell1[s] = i1; m.cell2[s] = i2; m.cell3[s] = i3; m.rc1[s] = i1; m.rc2[s] = i2;
+                if ((i1 + i2 + i3) % 2 == 0) m.nnlf.push_back(s);
+            }
+    const int nn[6][3] = {{0, 0, 1}, {1, 0, 0}, {0, 1, 0}, {0, 0, -1}, {-1, 0, 0}, {0, -1, 0}};
+    const int sn[12][3] = {{1, 1, 0}, {-1, 1, 0}, {-1, -1, 0}, {1, -1, 0}, {0, 1, 1}, {0, 1, -1},
+                           {0, -1, -1}, {0, -1, 1}, {1, 0, 1}, {1, 0, -1}, {-1, 0, -1}, {-1, 0, 1}};
+    m.nnlist.assign(N * 6, 0); m.snlist.assign(N * 12, 0);
+    m.nnveci.assign(N * 6 * 2, 0); m.nnvecr.assign(N * 6 * 2, 0.0);    // unused: the 3D bonds carry no phase
+    for (int s = 0; s < N; ++s) {
+        const int c1 = m.cell1[s], c2 = m.cell2[s], c3 = m.cell3[s];
+        for (int f = 0; f < 6; ++f) m.nnlist[s * 6 + f] = site(c1 + nn[f][0], c2 + nn[f][1], c3 + nn[f][2]);
+        for (int f = 0; f < 12; ++f) m.snlist[s * 12 + f] = site(c1 + sn[f][0], c2 + sn[f][1], c3 + sn[f][2]);
+    }
+    m.imj.assign(m.lq * m.lq, 0);
+    m.cell_plus.assign(m.lq * m.lq, 0);
+    for (int j = 0; j < m.lq; ++j)
+        for (int i = 0; i < m.lq; ++i) {
+            const int nx = npbc(m.cell1[i] - m.cell1[j], l1), ny = npbc(m.cell2[i] - m.cell2[j], l2);
+            const int nz = npbc(m.cell3[i] - m.cell3[j], l3);
+            const int d = (nz - 1) * l1 * l2 + ny + (nx - 1) * l2 - 1;
+            m.imj[i * m.lq + j] = d;
+            m.cell_plus[d * m.lq + j] = i;
+        }
+    int nd[8] = {0}, id[8] = {0};
+    auto typ = [](int i1, int i2, int i3) { return (i1 % 2 == 0) * 4 + (i2 % 2 == 0) * 2 + (i3 % 2 == 0); };
+    for (int i1 = 1; i1 <= l1; ++i1)
+        for (int i2 = 1; i2 <= l2; ++i2)
+            for (int i3 = 1; i3 <= l3; ++i3) nd[typ(i1, i2, i3)]++;
+    m.plq.assign(m.lq * 8, 0);
+    for (int i1 = 1; i1 <= l1; ++i1)
+        for (int i2 = 1; i2 <= l2; ++i2)
+            for (int i3 = 1; i3 <= l3; ++i3) {
+                const int t = typ(i1, i2, i3);
+                int off = 0;
+                for (int q = 0; q < t; ++q) off += nd[q];
+                int* pc = &m.plq[(id[t]++ + off) * 8];
+                pc[0] = site(i1, i2, i3);         pc[1] = site(i1 + 1, i2, i3);
+                pc[2] = site(i1 + 1, i2 + 1, i3); pc[3] = site(i1, i2 + 1, i3);
+                pc[4] = site(i1, i2, i3 + 1);     pc[5] = site(i1 + 1, i2, i3 + 1);
+                pc[6] = site(i1 + 1, i2 + 1, i3 + 1); pc[7] = site(i1, i2 + 1, i3 + 1);
+            }
+}
+
 static void build_lattice(HostModel& m) {
     const dqmc_params& p = m.p;
     int l1 = p.l1, l2 = p.l2;
+    if (p.lattice == DQMC_LATT_CUBIC) { build_cubic(m); return; }
     m.lq = l1 * l2;
     if (p.lattice == DQMC_LATT_CHAIN) {
         // setup_latt1d_sub / setup_chain_sub (src/lattice.f90:67-135, 240-316): bond
@@ -256,6 +325,7 @@ static void build_lattice(HostModel& m) {
 // Peierls / twist / dimerisation phase of bond (site i, family nf 1-based): expar.f90
 static zc expar(const HostModel& m, int i, int nf) {
     const dqmc_params& p = m.p;
+    if (p.lattice == DQMC_LATT_CUBIC) return zc(1.0, 0.0);    // expar3d.f90: no phase
     int k = (i * m.nn_nf + nf - 1) * 2;
     int nax = m.nnveci[k], nay = m.nnveci[k + 1];
     double vr1 = m.nnvecr[k], vr2 = m.nnvecr[k + 1];
@@ -293,7 +363,9 @@ static int build_model(HostModel& m) {
     dqmc_params& p = m.p;
     if (p.t3 != 0.0) return fail(DQMC_EINVAL, "t3 != 0 is not supported");
     if (p.kinetic < DQMC_KIN_CHECKERBOARD || p.kinetic > DQMC_KIN_DENSE) return fail(DQMC_EINVAL, "kinetic must be 0, 1 or 2");
-    if (p.lattice < DQMC_LATT_SQUARE || p.lattice > DQMC_LATT_CHAIN) return fail(DQMC_EINVAL, "lattice must be 1, 2 or 3");
+    if (p.lattice < DQMC_LATT_SQUARE || p.lattice > DQMC_LATT_CUBIC) return fail(DQMC_EINVAL, "lattice must be 1, 2, 3 or 4");
+    if (p.lattice == DQMC_LATT_CUBIC && (p.l1 < 2 || p.l2 < 2 || p.l3 < 2 || p.l1 % 2 || p.l2 % 2 || p.l3 % 2))
+        return fail(DQMC_EINVAL, "the cubic lattice needs even l1, l2, l3 >= 2");
     if (p.lattice == DQMC_LATT_CHAIN && (p.l2 != 1 || p.l1 < 4 || p.l1 % 2))
         return fail(DQMC_EINVAL, "the chain needs l2 = 1 and an even l1 >= 4");
     if (p.kinetic == DQMC_KIN_FFT && (p.lattice != DQMC_LATT_SQUARE || p.l1 != p.l2))
@@ -501,6 +573,8 @@ static int upload_model(HostModel& m) {
     d.phase_on = (p.rhub > 0.0) ? 1 : 0;
     d.rt = p.rt; d.rv = p.rv; d.t2 = p.t2; d.theta = p.theta * M_PI;
     d.chain = p.lattice == DQMC_LATT_CHAIN;
+    d.cubic = p.lattice == DQMC_LATT_CUBIC;
+    d.l3 = p.l3;
     set_hs(m, d);
     // projective path and vconf constants (src/dqmc_config_v/dqmc_set_conf.f90:1-79)
     d.proj = p.proj ? 1 : 0;
@@ -1389,7 +1463,9 @@ static bool proj_mid(const HostModel& m, int nt) {
 
 // equal-time measurement of the current G (equaltime_measure)
 static void launch_measure_h(dqmc_handle* h) {
-    launch_measure(h->d_chains, h->nch, h->maxN, h->models[0]->nsub == 2, h->max_lq, h->st);
+    const int kind = h->models[0]->p.lattice == DQMC_LATT_CUBIC ? MEAS_CUBIC
+                   : h->models[0]->nsub == 2 ? MEAS_HONEYCOMB : MEAS_ONE_ORBITAL;
+    launch_measure(h->d_chains, h->nch, h->maxN, kind, h->max_lq, h->st);
 }
 
 // ULRINV = (UL UR)^-1 fresh, G = I - UR ULRINV UL, equaltime_measure

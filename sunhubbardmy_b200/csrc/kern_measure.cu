@@ -41,6 +41,30 @@ DQ_DEV int cell_shift(int cj, int dxp, int dyp, int l1, int l2) {
     if (i2 >= l2) i2 -= l2;
     return i1 * l2 + i2;
 }
+// The same for the cubic lattice (setup_latt3d_sub): cells c = (c3 l1 + c1) l2
+// + c2 and d = dz l1 l2 + dx l2 + dy; dzp = dz + 1.  With l3 = 1 (dzp = 1) it
+// is the 2D shift.
+DQ_DEV int cell_shift3(int cj, int dxp, int dyp, int dzp, int l1, int l2, int l3) {
+    const int l12 = l1 * l2;
+    int i3 = cj / l12 + dzp, i1 = (cj / l2) % l1 + dxp, i2 = cj % l2 + dyp;
+    if (i3 >= l3) i3 -= l3;
+    if (i1 >= l1) i1 -= l1;
+    if (i2 >= l2) i2 -= l2;
+    return (i3 * l1 + i1) * l2 + i2;
+}
+// cell i = j + d on either lattice kind (D3: cubic)
+template <bool D3>
+struct CellShift {
+    int dxp, dyp, dzp, l1, l2, l3;
+    DQ_DEV CellShift(int d, const ModelDev& md) : l1(md.l1), l2(md.l2), l3(md.l3) {
+        dxp = (D3 ? (d / l2) % l1 : d / l2) + 1;
+        dyp = d % l2 + 1;
+        dzp = D3 ? d / (l1 * l2) + 1 : 1;
+    }
+    DQ_DEV int operator()(int cj) const {
+        return D3 ? cell_shift3(cj, dxp, dyp, dzp, l1, l2, l3) : cell_shift(cj, dxp, dyp, l1, l2);
+    }
+};
 
 // Energy terms and the background sums zn, zj, zb (single numbers per chain),
 // computed by the chain's second CTA while the first one sums the bins.
@@ -56,13 +80,13 @@ DQ_DEV void meas_energy(const ChainDev& c, double2 zphi, double sgn) {
     double2 zne = cmk(0, 0), zu = cmk(0, 0), zk = cmk(0, 0), zv = cmk(0, 0);
     // the chain's kinetic energy (equaltime_measure1d.f90) carries nflr rt on the
     // bonds and 2 t2 on its two second neighbours
-    const bool chain = md.chain != 0;
+    const bool chain = md.chain != 0, cubic = md.cubic != 0;
     const double kb = chain ? -2.0 * nflr * md.rt : -2.0, k2 = chain ? -2.0 * md.t2 : -md.t2;
     for (int i = tid; i < N; i += nth) {
         double2 d = gcf(G, N, i, i);
         zne = cadd(zne, d);
         zu = cadd(zu, cmul(d, d));
-        if (md.t2 != 0.0) {
+        if (md.t2 != 0.0 && !cubic) {      // zkint of equaltime_measure3d.f90 has no t2 term
             int ns = chain ? 2 : hc ? 6 : 4;
             for (int f = 0; f < ns; ++f) zk.x += k2 * gcf(G, N, i, md.snlist[i * md.nsn + f]).x;
         }
@@ -76,7 +100,7 @@ DQ_DEV void meas_energy(const ChainDev& c, double2 zphi, double sgn) {
     // plaquette terms
     double2 zq = cmk(0, 0), zt = cmk(0, 0), ztq = cmk(0, 0);
     const double2 em = cexpi(-md.theta), ep = cexpi(md.theta);
-    for (int q = tid; q < (chain ? 0 : lq); q += nth) {      // plaquette terms: 2D only
+    for (int q = tid; q < (chain || cubic ? 0 : lq); q += nth) {      // plaquette terms: 2D only
         const int* pc = md.plq_cord + q * zp;
         double2 tmp = cmk(0, 0);
         for (int a = 0; a < zp; ++a) tmp = cadd(tmp, gcf(G, N, pc[a], pc[a]));
@@ -129,7 +153,7 @@ DQ_DEV void meas_energy(const ChainDev& c, double2 zphi, double sgn) {
         int jnb = md.nnlist[j0 * nnf];
         double2 e = md.expar_nn[j0 * nnf];
         double2 dj = csub(gcf(G, N, j0, jnj), gcf(G, N, jnj, j0));
-        zj = cadd(zj, cmk(-dj.y, dj.x));
+        if (!cubic) zj = cadd(zj, cmk(-dj.y, dj.x));
         zb = cadd(zb, cadd(cmul(e, gcf(G, N, j0, jnb)), cmul(cconj(e), gcf(G, N, jnb, j0))));
     }
     zn0 = block_csum(zn0, red);
@@ -143,7 +167,7 @@ DQ_DEV void meas_energy(const ChainDev& c, double2 zphi, double sgn) {
         bins[3] = cadd(bins[3], cmul(zu, zphi));
         if (chain) {
             bins[4] = cadd(bins[4], cmul(zv, zphi));     // energy_bin(5) of the chain, without rv
-        } else {
+        } else if (!cubic) {                             // the cubic lattice fills energy_bin(1:4) only
             bins[4] = cadd(bins[4], cscale(cmul(zq, zphi), 1.0 / 9.0));
             bins[5] = cadd(bins[5], cmul(zt, zphi));
             bins[6] = cadd(bins[6], cmul(ztq, zphi));
@@ -179,12 +203,12 @@ DQ_DEV void meas_combine(double2& a0, double2& a1, double2& a2, double2& a3, int
 // GTc(i, j) = GT(i, j) - delta_ij = -Gc(i, j); whether site i of cell j + d
 // is site j is the same for every cell j (a translation), so it is taken
 // from cell 0.
-template <bool HC>
+template <bool HC, bool D3>
 DQ_DEV void meas_site(const ChainDev& c, int bin, double2 zphi) {   // bin of thread t % MEAS_BH
     constexpr int NS = HC ? 2 : 1;
     __shared__ double2 gcd[512];     // Gc(i,i)
     const ModelDev& md = *c.md;
-    const int N = c.N, lq = md.lq, l1 = md.l1, l2 = md.l2, nflr = md.nflr;
+    const int N = c.N, lq = md.lq, nflr = md.nflr;
     const double2 *G = c.G, *GT = c.GT;
     for (int i = threadIdx.x; i < N; i += MEAS_NT) gcd[i] = gcf(G, N, i, i);
     __syncthreads();
@@ -193,12 +217,12 @@ DQ_DEV void meas_site(const ChainDev& c, int bin, double2 zphi) {   // bin of th
     if (!valid) bin = 0;
     const double fsp = 1.0 - 1.0 / (double)(nflr * nflr), fn = 1.0 / (double)nflr;
     const int d = bin % lq, ab = bin / lq, a = ab % NS, b = ab / NS;
-    const int dxp = d / l2 + 1, dyp = d % l2 + 1;
-    const double fd = (cell_shift(0, dxp, dyp, l1, l2) == 0 && a == b) ? 1.0 : 0.0;
+    const CellShift<D3> shift(d, md);
+    const double fd = (shift(0) == 0 && a == b) ? 1.0 : 0.0;
     double2 s1 = cmk(0, 0), sB = cmk(0, 0), sA = cmk(0, 0), s4 = cmk(0, 0);
 #pragma unroll 4
     for (int cj = valid ? h : lq; cj < lq; cj += MEAS_SPLIT) {
-        const int i = cell_shift(cj, dxp, dyp, l1, l2) * NS + a, j = cj * NS + b;
+        const int i = shift(cj) * NS + a, j = cj * NS + b;
         const size_t o = (size_t)i + (size_t)N * j;
         double2 gtc = GT[o];
         const double2 g = G[o];
@@ -219,7 +243,7 @@ DQ_DEV void meas_site(const ChainDev& c, int bin, double2 zphi) {   // bin of th
     cpcm[k] = cfma(cmk(-s1.x, -s1.y), zphi, cpcm[k]);
     spsm[k] = cfma(cscale(cmk(-sB.x, -sB.y), fsp), zphi, spsm[k]);
     znn[k] = cfma(rfma(-fn, sB, sA), zphi, znn[k]);
-    pons[k] = cfma(s4, zphi, pons[k]);
+    if (!D3) pons[k] = cfma(s4, zphi, pons[k]);     // no pair_onsite on the cubic lattice
 }
 
 // Bond-correlation bins (jj, bb, pair_nn, pair_sn): MEAS_SPLIT threads per
@@ -229,7 +253,7 @@ DQ_DEV void meas_site(const ChainDev& c, int bin, double2 zphi) {   // bin of th
 // neighbour on the honeycomb; bond partner pb: nearest neighbour; pair
 // partner ps: second neighbour), so on the square lattice the Kronecker
 // deltas of Gc = delta - GT depend on d only and are taken from cell 0.
-template <bool HC>
+template <bool HC, bool D3>
 DQ_DEV void meas_bond(const ChainDev& c, int d, double2 zphi) {   // distance of thread t % MEAS_BH
     constexpr int NS = HC ? 2 : 1;
     __shared__ double2 jcell[512];   // Gc(i0,in) - Gc(in,i0), current partner
@@ -237,7 +261,7 @@ DQ_DEV void meas_bond(const ChainDev& c, int d, double2 zphi) {   // distance of
     __shared__ double2 pe[512];      // e = expar_nn(i0, first direction)
     __shared__ int pj[512], pb[512], ps[512];
     const ModelDev& md = *c.md;
-    const int N = c.N, lq = md.lq, l1 = md.l1, l2 = md.l2, nnf = md.nn_nf;
+    const int N = c.N, lq = md.lq, nnf = md.nn_nf;
     const double2 *G = c.G, *GT = c.GT;
     for (int cc = threadIdx.x; cc < lq; cc += MEAS_NT) {
         const int i0 = cc * NS;
@@ -253,19 +277,19 @@ DQ_DEV void meas_bond(const ChainDev& c, int d, double2 zphi) {   // distance of
     const int h = threadIdx.x / MEAS_BH;      // cells j = h (mod MEAS_SPLIT)
     if (!valid) d = 0;
     const double fn = 1.0 / (double)md.nflr;
-    const int dxp = d / l2 + 1, dyp = d % l2 + 1;
+    const CellShift<D3> shift(d, md);
     auto gg = [&](int r, int s_) { return G[(size_t)r + (size_t)N * s_]; };
     auto gt = [&](int r, int s_) { return GT[(size_t)r + (size_t)N * s_]; };
     // deltas of the square lattice, from cell 0: [i0 == j0], [in == j0], [i0 == jn], [in == jn]
     double f00 = 0, fn0 = 0, f0n = 0, fnn = 0;
     if (!HC) {
-        const int ci = cell_shift(0, dxp, dyp, l1, l2), in = pj[ci], jn = pj[0];
+        const int ci = shift(0), in = pj[ci], jn = pj[0];
         f00 = ci == 0; fn0 = in == 0; f0n = ci == jn; fnn = in == jn;
     }
     double2 sj = cmk(0, 0), sb = cmk(0, 0), sn = cmk(0, 0), ss = cmk(0, 0);
 #pragma unroll 4
     for (int cj = valid ? h : lq; cj < lq; cj += MEAS_SPLIT) {
-        const int ci = cell_shift(cj, dxp, dyp, l1, l2);
+        const int ci = shift(cj);
         const int j0 = cj * NS, i0 = ci * NS, jnj = pj[cj], inj = pj[ci];
         const double2 ei = pe[ci], ej = pe[cj];
         // G and GTc = GT - delta (= -Gc) at rows i0, in of columns j0, jn
@@ -320,15 +344,16 @@ DQ_DEV void meas_bond(const ChainDev& c, int d, double2 zphi) {   // distance of
     double2* zbb = zjj + lq;
     double2* pnn = zbb + lq;
     double2* psn = pnn + lq;
-    zjj[d] = cfma(sj, zphi, zjj[d]);
     zbb[d] = cfma(sb, zphi, zbb[d]);
+    if (D3) return;                  // the cubic lattice has bb only (measure_bondcorr of equaltime_measure3d.f90)
+    zjj[d] = cfma(sj, zphi, zjj[d]);
     pnn[d] = cfma(sn, zphi, pnn[d]);
     psn[d] = cfma(ss, zphi, psn[d]);
 }
 
 // grid (1 + na + nb, chains): x = 0 the energy terms, then na CTAs of site
 // bins and nb CTAs of bond bins (sized for the largest lattice of the handle)
-template <bool HC>
+template <bool HC, bool D3>
 __global__ void __launch_bounds__(MEAS_NT, 2) k_measure(const ChainDev* __restrict__ chains, int na) {
     const ChainDev& c = chains[blockIdx.y];
     const double2 phase = cmk(c.stats[ST_PHASE_RE], c.stats[ST_PHASE_IM]);
@@ -336,8 +361,8 @@ __global__ void __launch_bounds__(MEAS_NT, 2) k_measure(const ChainDev* __restri
     const double2 zphi = cscale(phase, sgn / phase.x);
     const int x = blockIdx.x;
     if (x == 0) meas_energy(c, zphi, sgn);
-    else if (x <= na) meas_site<HC>(c, (x - 1) * MEAS_BH + threadIdx.x % MEAS_BH, zphi);
-    else meas_bond<HC>(c, (x - 1 - na) * MEAS_BH + threadIdx.x % MEAS_BH, zphi);
+    else if (x <= na) meas_site<HC, D3>(c, (x - 1) * MEAS_BH + threadIdx.x % MEAS_BH, zphi);
+    else meas_bond<HC, D3>(c, (x - 1 - na) * MEAS_BH + threadIdx.x % MEAS_BH, zphi);
 }
 
 __global__ void k_bins_clear(const ChainDev* __restrict__ chains, int nbins) {
@@ -372,46 +397,56 @@ __global__ void __launch_bounds__(256) k_transpose_g(const ChainDev* __restrict_
     }
 }
 
-void launch_measure(const ChainDev* chains, int nchains, int maxN, int hc, int maxlq, cudaStream_t st) {
+// kind: MEAS_ONE_ORBITAL (square, chain), MEAS_HONEYCOMB or MEAS_CUBIC
+void launch_measure(const ChainDev* chains, int nchains, int maxN, int kind, int maxlq, cudaStream_t st) {
     const int nt = (maxN + 31) / 32;
     k_transpose_g<<<dim3(nt, nt, nchains), 256, 0, st>>>(chains, MAT_G);
-    const int ns = hc ? 2 : 1;
+    const int ns = kind == MEAS_HONEYCOMB ? 2 : 1;
     const int na = (maxlq * ns * ns + MEAS_BH - 1) / MEAS_BH, nb = (maxlq + MEAS_BH - 1) / MEAS_BH;
     const dim3 grid(1 + na + nb, nchains);
-    if (hc) k_measure<true><<<grid, MEAS_NT, 0, st>>>(chains, na);
-    else k_measure<false><<<grid, MEAS_NT, 0, st>>>(chains, na);
+    if (kind == MEAS_HONEYCOMB) k_measure<true, false><<<grid, MEAS_NT, 0, st>>>(chains, na);
+    else if (kind == MEAS_CUBIC) k_measure<false, true><<<grid, MEAS_NT, 0, st>>>(chains, na);
+    else k_measure<false, false><<<grid, MEAS_NT, 0, st>>>(chains, na);
 }
 
 // dyn_measure (src/dqmc_measure/dyn_measure.f90:1-101) at time index nt: the
 // density correlation znn_tau(imj, no_i, no_j, nt) +=
 //   (1/2 - Re G(t,t)_ii)(1/2 - Re G(0,0)_jj) - G(0,t)_ji G(t,0)_ij / nflr,
 // weighted with zphi; G(0,t)^T is in GT.  One thread per bin, cells j in
-// order (the reference's summation order for a bin).
+// order (the reference's summation order for a bin).  On the cubic lattice
+// (dyn_measure3d.f90:44-66) the same znn_tau goes to slot 0 of the time
+// index's 4 lq bins, zspsm_tau(imj) += -G(0,t)_ji G(t,0)_ij (1 - 1/nflr^2) to
+// slot lq and gtau0(imj) += G(t,0)_ij to slot 2 lq.
 __global__ void __launch_bounds__(256) k_dyn_measure(const ChainDev* __restrict__ chains, int nt) {
     const ChainDev& c = chains[blockIdx.y];
     const ModelDev& md = *c.md;
     if (nt > md.ntdm + 1) return;
-    const int N = c.N, lq = md.lq, nsub = md.nsub, l1 = md.l1, l2 = md.l2;
+    const int N = c.N, lq = md.lq, nsub = md.nsub;
     const double2 phase = cmk(c.stats[ST_PHASE_RE], c.stats[ST_PHASE_IM]);
     const double sgn = phase.x < 0.0 ? -1.0 : 1.0;
     const double2 zphi = cscale(phase, sgn / phase.x);
-    const double fn = 1.0 / (double)md.nflr;
+    const double fn = 1.0 / (double)md.nflr, fsp = 1.0 - fn * fn;
     const double2 *G = c.G, *GT = c.GT, *gt0 = c.gt0, *g00 = c.g00;
     double2* bin = c.dynbins + (size_t)4 * lq * (nt - 1);
     const int nbin = lq * nsub * nsub;
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nbin; b += gridDim.x * blockDim.x) {
         const int d = b % lq, ab = b / lq, a = ab % nsub, bb = ab / nsub;
-        const int dxp = d / l2 + 1, dyp = d % l2 + 1;
-        double2 z = cmk(0, 0);
+        const CellShift<true> shift(d, md);     // l3 = 1 off the cubic lattice
+        double2 z = cmk(0, 0), zs = cmk(0, 0), zg = cmk(0, 0);
 #pragma unroll 4
         for (int cj = 0; cj < lq; ++cj) {
-            const int i = cell_shift(cj, dxp, dyp, l1, l2) * nsub + a, j = cj * nsub + bb;
+            const int i = shift(cj) * nsub + a, j = cj * nsub + bb;
             const size_t o = (size_t)i + (size_t)N * j;
             const double v = (0.5 - G[(size_t)i * (N + 1)].x) * (0.5 - g00[(size_t)j * (N + 1)].x);
             z = csub(cadd(z, cmk(v, 0.0)), cmul(cscale(GT[o], fn), gt0[o]));
+            if (md.cubic) { zs = csub(zs, cmul(cscale(GT[o], fsp), gt0[o])); zg = cadd(zg, gt0[o]); }
         }
         const size_t k = (size_t)d + (size_t)lq * a + (size_t)2 * lq * bb;
         bin[k] = cfma(z, zphi, bin[k]);
+        if (md.cubic) {
+            bin[lq + d] = cfma(zs, zphi, bin[lq + d]);
+            bin[2 * lq + d] = cfma(zg, zphi, bin[2 * lq + d]);
+        }
     }
 }
 

@@ -16,12 +16,12 @@
  *
  * Usage: replay_ft [dqmc.in] [key=value ...]
  *   dqmc.in      the &model_para and &ctrl_para namelists (src/model_para.f90:155-218);
- *                keys la, lb, beta, dtau, rt, t2, t3, nu, mu, rhub, rv, alpha, theta,
+ *                keys la, lb, lc, beta, dtau, rt, t2, t3, nu, mu, rhub, rv, alpha, theta,
  *                nflr, lproju, lprojv, xmag, flux_x, flux_y, dimer, rndness,
  *                lstabilize, nwrap, nsweep, nbin, nublock, ltau, dyntau,
  *                obs_eqt_mid_len
  *   key=value    the same keys, plus the RUNMODE build flags of src/make.sys.*:
- *                lattice=1|2|3 (SQUARE|HONEYCOMB|CHAIN), update=0|1|2
+ *                lattice=1|2|3|4 (SQUARE|HONEYCOMB|CHAIN|CUBIC), update=0|1|2
  *                (fast|DELAY|SUBMATRIX), kinetic=0|1|2 (BREAKUP_T|FFT|zgemm),
  *                hs=0|1 (EXACTHS|general), and seed= (default: the -DTEST
  *                seed of rank 0, abs(2008*951049)), nwarmup= (default: nsweep
@@ -75,6 +75,7 @@ static int set_key(dqmc_params* p, const char* key, const char* val, int32_t* se
 #define I(name) if (!strcmp(k, #name)) { p->name = (int32_t)v; return 0; }
     if (!strcmp(k, "la")) { p->l1 = (int32_t)v; return 0; }
     if (!strcmp(k, "lb")) { p->l2 = (int32_t)v; return 0; }
+    if (!strcmp(k, "lc")) { p->l3 = (int32_t)v; return 0; }
     if (!strcmp(k, "obs_eqt_mid_len")) { p->obs_mid_len = (int32_t)v; return 0; }
     if (!strcmp(k, "seed")) { *seed = (int32_t)v; return 0; }
     if (!strcmp(k, "nwarmup")) { *nwarm = (int)v; return 0; }
@@ -85,8 +86,8 @@ static int set_key(dqmc_params* p, const char* key, const char* val, int32_t* se
     I(lattice) I(update) I(kinetic) I(hs) I(proj)
 #undef D
 #undef I
-    /* namelist members with no effect on this path (rhub_plq, lprojplqu, lc, rtd) */
-    if (!strcmp(k, "rhub_plq") || !strcmp(k, "lprojplqu") || !strcmp(k, "lc") || !strcmp(k, "rtd")) return 0;
+    /* namelist members with no effect on this path (rhub_plq, lprojplqu, rtd) */
+    if (!strcmp(k, "rhub_plq") || !strcmp(k, "lprojplqu") || !strcmp(k, "rtd")) return 0;
     fprintf(stderr, "replay_ft: unknown key %s\n", key);
     return -1;
 }
@@ -128,7 +129,7 @@ int main(int argc, char** argv) {
     dqmc_params p;
     memset(&p, 0, sizeof(p));
     /* defaults of src/model_para.f90:166-206 and the square Hubbard build */
-    p.lattice = DQMC_LATT_SQUARE; p.l1 = 2; p.l2 = 2; p.beta = 20.0; p.dtau = 0.05; p.rt = 1.0;
+    p.lattice = DQMC_LATT_SQUARE; p.l1 = 2; p.l2 = 2; p.l3 = 2; p.beta = 20.0; p.dtau = 0.05; p.rt = 1.0;
     p.alpha = 0.2; p.nflr = 2; p.lstabilize = 1; p.nwrap = 10; p.nsweep = 20; p.nbin = 10;
     p.update = DQMC_UPD_DELAY; p.kinetic = DQMC_KIN_CHECKERBOARD; p.hs = DQMC_HS_GENERAL4; p.obs_mid_len = 1;
     int32_t seed = 1909706392;   /* abs((0*1981+2008)*951049), src/dqmc_util.f90:72 under -DTEST */

@@ -14,7 +14,7 @@ import re
 
 import numpy as np
 
-SQUARE, HONEYCOMB, CHAIN = 1, 2, 3
+SQUARE, HONEYCOMB, CHAIN, CUBIC = 1, 2, 3, 4
 FAST, DELAY, SUBMATRIX = 0, 1, 2
 CHECKERBOARD, FFT, DENSE = 0, 1, 2
 EXACT, GENERAL4 = 0, 1
@@ -55,6 +55,7 @@ class DqmcParams(C.Structure):
         ("ndim", C.c_int32), ("lq", C.c_int32), ("ltrot", C.c_int32), ("nst", C.c_int32),
         ("ne", C.c_int32), ("lcomp", C.c_int32),
         ("ltau", C.c_int32), ("ntdm", C.c_int32), ("dyntau", C.c_double),
+        ("l3", C.c_int32),
     ]
 
     @classmethod
@@ -64,7 +65,7 @@ class DqmcParams(C.Structure):
                  mu=0.0, rhub=0.0, rv=0.0, alpha=0.2, theta=0.0, xmag=0.0, flux_x=0.0, flux_y=0.0,
                  dimer=0.0, rndness=0.0, nflr=2, lproju=0, lstabilize=1, nwrap=10, nsweep=20,
                  nbin=10, nublock=0, update=DELAY, kinetic=CHECKERBOARD, hs=GENERAL4, proj=0,
-                 lprojv=0, obs_mid_len=1, ltau=0, dyntau=0.0)
+                 lprojv=0, obs_mid_len=1, ltau=0, dyntau=0.0, l3=1)
         d.update(kw)
         p = cls(**d)
         rc = load_library().dqmc_params_derive(C.byref(p))
@@ -76,7 +77,7 @@ class DqmcParams(C.Structure):
         """Lattice / kinetic tables built by the library (1-based, host only)."""
         N, lq = self.ndim, self.lq
         hc = self.lattice == HONEYCOMB
-        nnf, z, nsn = {HONEYCOMB: (3, 6, 6), CHAIN: (2, 1, 2)}.get(self.lattice, (4, 4, 4))
+        nnf, z, nsn = {HONEYCOMB: (3, 6, 6), CHAIN: (2, 1, 2), CUBIC: (6, 8, 12)}.get(self.lattice, (4, 4, 4))
         nlf = lq if hc else lq // 2
         t = dict(nnlist=np.zeros((N, nnf), np.int32), nnlf_list=np.zeros(nlf, np.int32),
                  list=np.zeros((N, 2), np.int32), imj=np.zeros((lq, lq), np.int32),
@@ -289,6 +290,8 @@ def read_dqmc_in(path_or_text: str) -> dict:
         out["l1"] = out.pop("la")
     if "lb" in out:
         out["l2"] = out.pop("lb")
+    if "lc" in out:            # the cubic lattice's third length (-DCUBIC namelist)
+        out["l3"] = out.pop("lc")
     for k in ("lprojv", "lproju", "lprojplqu", "lstabilize", "ltau"):
         if k in out:
             out[k] = int(bool(out[k]))
@@ -596,7 +599,7 @@ class Dqmc:
     # projective path (params.proj = 1)
     def vconf(self, c: int = 0) -> np.ndarray:
         """t-V bond field vconf%conf as [ltrot][nn_nf][ndim] (bond index fastest)."""
-        nnf = {HONEYCOMB: 3, CHAIN: 2}.get(self.chain_params(c).lattice, 4)
+        nnf = {HONEYCOMB: 3, CHAIN: 2, CUBIC: 6}.get(self.chain_params(c).lattice, 4)
         out = np.zeros((self.ltrot, nnf, self.ndim(c)), np.int32)
         _check(load_library().dqmc_gpu_get_vconf(self.h, c, _ptr(out)), "get_vconf")
         return out

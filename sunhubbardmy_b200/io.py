@@ -148,6 +148,74 @@ def dyn_output(dyn_bins_per_chain, nsweep: int, nsub: int, outdir: str = ".",
     return gr
 
 
+def equaltime_output3d(bins_per_chain, l1: int, l2: int, l3: int, outdir: str = ".") -> dict:
+    """equaltime_output of the cubic lattice (src/dqmc_measure/equaltime_output3d.f90):
+    the chain bins reduced and divided by n_chains * nobs; energy.bin gets
+    energy_bin(1:4) ('(8e16.8)'), n.bin zn and b.bin zb ('(2e16.8)'); cpcm, spsm,
+    nn and bb get *_r.bin (one '(2e16.8)' line per distance imj) and *_k.bin
+    (per momentum '(3f16.8,2e16.8)': k1/l1, k2/l2, k3/l3 and gk = sum_imj
+    gr(imj) / zexpiqr(nk, imj) / lq).  The cubic bins use the (no_i, no_j) =
+    (1, 1) block of the library's site and bond bins."""
+    n = len(bins_per_chain)
+    nobs = bins_per_chain[0]["nobs"]
+    rnorm = float(n * nobs)
+    red = {}
+    for key in ("energy", "cpcm", "spsm", "nn", "bb", "zn", "zb"):
+        red[key] = sum(np.asarray(b[key]) for b in bins_per_chain) / rnorm
+    for key in ("cpcm", "spsm", "nn"):
+        red[key] = red[key][0, 0]
+    red["zn"] = red["zn"][0]
+    os.makedirs(outdir, exist_ok=True)
+    lq = l1 * l2 * l3
+    listk = momentum_list3d(l1, l2, l3)
+    zq = zexpiqr3d(l1, l2, l3)
+    for key in ("cpcm", "spsm", "nn", "bb"):
+        gr = red[key]
+        with open(os.path.join(outdir, f"{key}_r.bin"), "a") as f:
+            for z in gr:
+                f.write(f"{z.real:16.8e}{z.imag:16.8e}\n")
+        gk = (gr[None, :] / zq).sum(axis=1) / lq
+        with open(os.path.join(outdir, f"{key}_k.bin"), "a") as f:
+            for nk in range(lq):
+                f.write(f"{listk[nk][0] / l1:16.8f}{listk[nk][1] / l2:16.8f}{listk[nk][2] / l3:16.8f}"
+                        f"{gk[nk].real:16.8e}{gk[nk].imag:16.8e}\n")
+    with open(os.path.join(outdir, "energy.bin"), "a") as f:
+        f.write("".join(f"{v:16.8e}" for z in red["energy"][:4] for v in (z.real, z.imag)) + "\n")
+    for name, key in (("n.bin", "zn"), ("b.bin", "zb")):
+        with open(os.path.join(outdir, name), "a") as f:
+            z = red[key]
+            f.write(f"{z.real:16.8e}{z.imag:16.8e}\n")
+    return red
+
+
+def dyn_output3d(dyn_bins_per_chain, nsweep: int, l1: int, l2: int, l3: int, outdir: str = ".") -> dict:
+    """dyn_output of the cubic lattice (src/dqmc_measure/dyn_output3d.f90): the
+    chains' znn_tau, zspsm_tau and gtau0 (slots (0, 0), (0, 1) and (1, 0) of
+    Dqmc.dyn_bins' [ntdm+1, 2, 2, lq]) reduced and divided by nsweep *
+    n_chains, written without tau = 0 as nn_, spsm_ and gf_rtau.bin (per
+    distance, per time index a '(2e16.8)' line) and _ktau.bin (per momentum
+    '(3f16.8)' coordinates, then the time indices)."""
+    gr = sum(np.asarray(b) for b in dyn_bins_per_chain) / float(nsweep * len(dyn_bins_per_chain))
+    lq = l1 * l2 * l3
+    listk = momentum_list3d(l1, l2, l3)
+    zq = zexpiqr3d(l1, l2, l3)
+    out = {"nn": gr[:, 0, 0, :], "spsm": gr[:, 0, 1, :], "gf": gr[:, 1, 0, :]}
+    os.makedirs(outdir, exist_ok=True)
+    for tag in ("spsm", "nn", "gf"):
+        a = out[tag]                       # [nt, imj]
+        with open(os.path.join(outdir, f"{tag}_rtau.bin"), "a") as f:
+            for imj in range(lq):
+                for nt in range(1, a.shape[0]):
+                    f.write(f"{a[nt, imj].real:16.8e}{a[nt, imj].imag:16.8e}\n")
+        gk = (a[:, None, :] / zq[None, :, :]).sum(axis=2) / lq      # [nt, nk]
+        with open(os.path.join(outdir, f"{tag}_ktau.bin"), "a") as f:
+            for nk in range(lq):
+                f.write(f"{listk[nk][0] / l1:16.8f}{listk[nk][1] / l2:16.8f}{listk[nk][2] / l3:16.8f}\n")
+                for nt in range(1, a.shape[0]):
+                    f.write(f"{gk[nt, nk].real:16.8e}{gk[nt, nk].imag:16.8e}\n")
+    return out
+
+
 # ----------------------------------------------------------------------------
 # dqmc.out (src/dqmc_util.f90): parameter banner, wrap-error lines, end of run
 # ----------------------------------------------------------------------------
@@ -186,7 +254,10 @@ def dqmc_initial_print(f, p, wrap_step=None, nustock: int = 0) -> None:
     w(f" rv      = {g['rv']:7.3f}\n")
     w(f" lprojv   =  {_lg(g['lprojv'])}\n")
     w(f" la     = {g['l1']:4d}\n")
-    w(f" lb     = {g['l2']:4d}\n")
+    if g["lattice"] != 3:           # -DCHAIN prints la only
+        w(f" lb     = {g['l2']:4d}\n")
+    if g["lattice"] == 4:           # -DCUBIC: lc as well
+        w(f" lc     = {g.get('l3', 1):4d}\n")
     w(f" beta   = {g['beta']:6.2f}\n")
     w(f" dtau   = {g['dtau']:7.3f}\n")
     for k, name in (("ndim", "ndim"), ("ne", "ne  "), ("nwrap", "nwrap "), ("nsweep", "nsweep"),
@@ -210,7 +281,7 @@ def dqmc_initial_print(f, p, wrap_step=None, nustock: int = 0) -> None:
     for i, (a, b) in enumerate(wrap_step or [], start=1):
         w(f"{a:16d}{b:16d}{i:16d}\n")
     w(" \n")
-    w({2: "honeycomb_lattice", 3: "chain_lattice"}.get(g["lattice"], "square_lattice") + "\n")
+    w({2: "honeycomb_lattice", 3: "chain_lattice", 4: "cubic_lattice"}.get(g["lattice"], "square_lattice") + "\n")
     if not isinstance(p, dict):
         print_latt(f, p)
 
@@ -234,6 +305,26 @@ def lattice_lists(p) -> dict:
     def npbc(nr, l):
         return nr - l if nr > l else (nr + l if nr < 1 else nr)
 
+    if lat == 4:      # cubic (setup_latt3d_sub, setup_cubic_sub: src/lattice.f90:1033-1157, 1280-1472)
+        l3 = int(p.l3)
+        cord = np.zeros((N, 3), dtype=np.int64)
+        for i1 in range(1, l1 + 1):
+            for i2 in range(1, l2 + 1):
+                for i3 in range(1, l3 + 1):
+                    cord[(i3 - 1) * l1 * l2 + (i1 - 1) * l2 + i2 - 1] = (i1, i2, i3)
+
+        def cs(c1, c2, c3):
+            return (npbc(c3, l3) - 1) * l1 * l2 + (npbc(c1, l1) - 1) * l2 + npbc(c2, l2)
+        tn = np.zeros((N, 8), dtype=np.int64)
+        steps = ((1, 1, 1), (-1, 1, 1), (-1, -1, 1), (1, -1, 1), (1, 1, -1), (-1, 1, -1), (-1, -1, -1), (1, -1, -1))
+        for i in range(N):
+            c1, c2, c3 = cord[i]
+            tn[i] = [cs(c1 + a, c2 + b, c3 + c) for (a, b, c) in steps]
+        listk = momentum_list3d(l1, l2, l3)
+        eye = np.eye(3)
+        return dict(list=t["list"], cord=cord, nnlist=t["nnlist"], snlist=t["snlist"], tnlist=tn,
+                    plq_cord=t["plq_cord"], listk=listk, a1=eye[0], a2=eye[1], a3=eye[2],
+                    bz1=2.0 * np.pi * eye[0], bz2=2.0 * np.pi * eye[1], bz3=2.0 * np.pi * eye[2])
     if lat == 3:      # chain
         a1, a2 = np.array([1.0]), None
         cord = np.array([[i] for i in range(1, l1 + 1)], dtype=np.int64)
@@ -275,9 +366,29 @@ def lattice_lists(p) -> dict:
                 plq_cord=None if lat == 3 else t["plq_cord"], listk=listk, a1=a1, a2=a2, bz1=bz1, bz2=bz2)
 
 
+def momentum_list3d(l1: int, l2: int, l3: int) -> np.ndarray:
+    """listk of setup_latt3d_sub (src/lattice.f90:1115-1127): (m, n, l) with l
+    outermost, then m (along a1), then n (along a2)."""
+    return np.array([[m, n, l] for l in range(-((l3 + 1) // 2) + 1, l3 // 2 + 1)
+                     for m in range(-((l1 + 1) // 2) + 1, l1 // 2 + 1)
+                     for n in range(-((l2 + 1) // 2) + 1, l2 // 2 + 1)], dtype=np.int64)
+
+
+def zexpiqr3d(l1: int, l2: int, l3: int) -> np.ndarray:
+    """zexpiqr(nk, i) = exp(i k_nk . R_i) of the cubic lattice (setup_latt3d_sub,
+    src/lattice.f90:1143-1150): R_i the unit-cell coordinates (i1, i2, i3) of
+    cell i = (i3-1) l1 l2 + (i1-1) l2 + i2, k = (m/l1, n/l2, l/l3) 2 pi."""
+    lk = momentum_list3d(l1, l2, l3)
+    c = np.array([(i1, i2, i3) for i3 in range(1, l3 + 1) for i1 in range(1, l1 + 1)
+                  for i2 in range(1, l2 + 1)], dtype=float)
+    k = 2.0 * np.pi * lk / np.array([l1, l2, l3], dtype=float)
+    return np.exp(1j * (k @ c.T))
+
+
 def print_latt(f, p) -> None:
-    """print_latt2d_sub / print_latt1d_sub (src/lattice.f90:146-226, 502-597):
-    the lattice block of dqmc.out, without the PLEVEL2 imj table."""
+    """print_latt2d_sub / print_latt1d_sub / print_latt3d_sub (src/lattice.f90:
+    146-226, 502-597, 1169-1263): the lattice block of dqmc.out, without the
+    PLEVEL2 imj table."""
     L = lattice_lists(p)
     w = f.write
 
@@ -290,6 +401,21 @@ def print_latt(f, p) -> None:
         w(f"{head} \n")
         for i, r in enumerate(rows, start=1):
             w(f"{i:6d}" + "".join(fmt.format(int(v)) for v in r) + "\n")
+
+    if "a3" in L:
+        w("lattice information: \n")
+        for k in ("a1", "a2", "a3"):
+            w(f" primitive lattice vector {k}_p(:) = " + vec(L[k]) + "\n")
+        for k in ("bz1", "bz2", "bz3"):
+            w(f" primitive reciprocal vector {k}_p(:) / 2pi = " + vec(L[k] / (2.0 * np.pi)) + "\n")
+        section("The lattice sites list", "   i     list(i,:)", L["list"], "{:4d}")
+        section("The lattice sites cord", "   i     cord(i,:)", L["cord"], "{:4d}")
+        section("The lattice nnlist", "   i     nnlist(i,:)", L["nnlist"], "{:4d}")
+        section("The lattice snlist", "   i     snlist(i,:)", L["snlist"], "{:4d}")
+        section("The lattice tnlist", "   i     tnlist(i,:)", L["tnlist"], "{:4d}")
+        section("The lattice plq_cord", "   i     plq_cord(:,i)", L["plq_cord"], "{:4d}")
+        section("The momentum listk", "   i     listk(i,:)", L["listk"], "{:4d}")
+        return
 
     w("lattice information: \n")
     w(" primitive lattice  vector a1_p(:) =  " + vec(L["a1"]) + "\n")

@@ -2,7 +2,8 @@
 
 The cases are small versions of the benchmark configurations (square Hubbard
 with checkerboard, FFT or dense kinetic term, exact or general HS field;
-honeycomb SU(4); the 1D chain) sized so the oracle finishes each in well under a second.
+honeycomb SU(4); the 1D chain; the cubic lattice) sized so the oracle finishes each in well under
+a second.
 """
 import numpy as np
 
@@ -34,6 +35,13 @@ CASES = {
                               flux_x=0.1, kinetic=0, update=1, hs=1, nwrap=5, nublock=4),
     "ch10_dense_exact_sub": dict(lattice=3, l1=10, l2=1, beta=2.0, dtau=0.1, rhub=3.0, nflr=2,
                                  kinetic=2, update=2, hs=0, nwrap=10, nublock=8),
+    # the cubic lattice (-DCUBIC build, equaltime_measure3d.f90): six bond families
+    "cu4_cb_gen4_delay": dict(lattice=4, l1=4, l2=4, l3=4, beta=1.0, dtau=0.1, rhub=4.0, nflr=2, mu=0.2,
+                              kinetic=0, update=1, hs=1, nwrap=5, nublock=8),
+    "cu422_cb_exact_fast": dict(lattice=4, l1=4, l2=2, l3=2, beta=1.0, dtau=0.1, rhub=4.0, nflr=2,
+                                kinetic=0, update=0, hs=0, nwrap=10),
+    "cu224_dense_exact_sub": dict(lattice=4, l1=2, l2=2, l3=4, beta=1.5, dtau=0.1, rhub=4.0, nflr=2, mu=0.1,
+                                  kinetic=2, update=2, hs=0, nwrap=5, nublock=8),
 }
 
 TEST_SEED0 = 1909706392   # abs((0*1981+2008)*951049)
