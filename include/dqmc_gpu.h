@@ -56,6 +56,7 @@ extern "C" {
 #define DQMC_LATT_HONEYCOMB 2  /* -DHONEYCOMB */
 #define DQMC_LATT_CHAIN 3      /* -DCHAIN: l2 = 1, even l1; checkerboard or dense kinetic term */
 #define DQMC_LATT_CUBIC 4      /* -DCUBIC: l1 x l2 x l3 (la, lb, lc); checkerboard (even lengths) or dense kinetic term */
+#define DQMC_LATT_R_CUBIC 5    /* -DR_CUBIC: rhombohedral stack, six orbitals per cell, interlayer hopping rtd */
 #define DQMC_UPD_FAST 0        /* default (no flag) */
 #define DQMC_UPD_DELAY 1       /* -DDELAY */
 #define DQMC_UPD_SUBMATRIX 2   /* -DSUBMATRIX */
@@ -83,9 +84,12 @@ typedef struct dqmc_params {
      * nint(dyntau / dtau) is derived (src/model_para.f90:455-459) */
     int32_t ltau, ntdm;
     double dyntau;
-    /* lc of &model_para: the length along a3 of the cubic lattice (set to 1
-     * on the other lattices by dqmc_params_derive) */
+    /* lc of &model_para: the length along a3 of the cubic and r_cubic
+     * lattices (set to 1 on the other lattices by dqmc_params_derive) */
     int32_t l3;
+    /* rtd of &model_para (-DR_CUBIC): the hopping of bond family 4 between
+     * the layers of the r_cubic lattice (the reference's default is 1) */
+    double rtd;
 } dqmc_params;
 
 /* per-chain diagnostics (src/dqmc_util.f90:15-57, 287-299) */
@@ -117,7 +121,9 @@ typedef struct dqmc_handle dqmc_handle;
  * reference's 1-based conventions (src/lattice.f90, dqmc_set_h0conf.f90):
  * nnlist[ndim][nn_nf], nnlf_list[nn_lf], list[ndim][2], imj[lq][lq],
  * plq_cord[lq][z_plq], snlist[ndim][nsn] (nsn = 2 chain, 4 square, 6
- * honeycomb, 12 cubic), urt[nn_nf*nn_lf][2][2] complex,
+ * honeycomb, 12 cubic and r_cubic; z_plq = 8 on both 3D lattices, the
+ * r_cubic tables of snlist and plq_cord being zeros as the reference leaves
+ * them), urt[nn_nf*nn_lf][2][2] complex,
  * exph0k[lq] complex (FFT only).  Any pointer may be NULL.  Needs no GPU. */
 int dqmc_model_tables(const dqmc_params* p, int32_t* nnlist, int32_t* nnlf_list, int32_t* list,
                       int32_t* imj, int32_t* plq_cord, int32_t* snlist, double* urt, double* exph0k);

@@ -18,7 +18,7 @@ module dqmc_gpu_f
   integer(c_int), parameter :: DQMC_OK = 0, DQMC_EINVAL = -1, DQMC_ECUDA = -2, DQMC_ENOMEM = -3
   integer(c_int), parameter :: DQMC_ESTATE = -4, DQMC_ENUMERIC = -5, DQMC_EWRAP = -6
   integer(c_int), parameter :: DQMC_LATT_SQUARE = 1, DQMC_LATT_HONEYCOMB = 2, DQMC_LATT_CHAIN = 3, &
-                                DQMC_LATT_CUBIC = 4
+                                DQMC_LATT_CUBIC = 4, DQMC_LATT_R_CUBIC = 5
   integer(c_int), parameter :: DQMC_UPD_FAST = 0, DQMC_UPD_DELAY = 1, DQMC_UPD_SUBMATRIX = 2
   integer(c_int), parameter :: DQMC_KIN_CHECKERBOARD = 0, DQMC_KIN_FFT = 1, DQMC_KIN_DENSE = 2
   integer(c_int), parameter :: DQMC_HS_EXACT = 0, DQMC_HS_GENERAL4 = 1
@@ -36,6 +36,7 @@ module dqmc_gpu_f
      integer(c_int32_t) :: ltau, ntdm
      real(c_double)     :: dyntau
      integer(c_int32_t) :: l3
+     real(c_double)     :: rtd
   end type
 
   ! mirror of dqmc_diag (same field order)

@@ -44,7 +44,7 @@ double   orc_sfmt_stream(orc_sfmt *s);
 int32_t  orc_test_seed(int32_t irank);   /* src/dqmc_util.f90:72 under -DTEST */
 
 /* ---------- parameters (src/model_para.f90 &model_para/&ctrl_para) ---------- */
-enum { ORC_SQUARE = 1, ORC_HONEYCOMB = 2, ORC_CHAIN = 3, ORC_CUBIC = 4 };
+enum { ORC_SQUARE = 1, ORC_HONEYCOMB = 2, ORC_CHAIN = 3, ORC_CUBIC = 4, ORC_R_CUBIC = 5 };
 enum { ORC_FAST = 0, ORC_DELAY = 1, ORC_SUBMATRIX = 2, ORC_SUBMATRIX_G = 3, ORC_SUBMATRIX_G_EXACT = 4 };
 enum { ORC_CHECKERBOARD = 0, ORC_FFT = 1, ORC_DENSE = 2 };
 enum { ORC_HS_EXACT = 0, ORC_HS_GENERAL4 = 1 };
@@ -61,8 +61,10 @@ typedef struct {
     /* unequal-time measurement: ltau and dyntau of &ctrl_para */
     int32_t ltau;
     double dyntau;
-    /* lc of &model_para: the cubic lattice's length along a3 */
+    /* lc of &model_para: the 3D lattices' length along a3; rtd: the r_cubic
+     * interlayer hopping */
     int32_t l3;
+    double rtd;
 } orc_params;
 
 typedef struct orc_model orc_model;

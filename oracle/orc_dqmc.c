@@ -166,7 +166,9 @@ static void set_h0(orc_model *m) {
             for (int iu = 0; iu < lf; ++iu) {
                 int ist = iu + (nf - 1) * lf;
                 int i0 = L->nnlf_list[iu] - 1;
-                zc z = -p->rt * m->expar_nn[i0 * nf_n + nf - 1];
+                /* r_cubic: family 4 hops rtd between the layers (dqmc_set_h0conf.f90:22-73) */
+                const double t = (L->kind == ORC_R_CUBIC && nf == 4) ? p->rtd : p->rt;
+                zc z = -t * m->expar_nn[i0 * nf_n + nf - 1];
                 double d = -p->mu / nf_n;
                 exp2x2(d, z, 0.5 * p->dtau, &m->urt[ist * 4]);
                 exp2x2(d, z, -0.5 * p->dtau, &m->urtm1[ist * 4]);
@@ -222,7 +224,7 @@ orc_model *orc_model_new(const orc_params *pin) {
     orc_model *m = calloc(1, sizeof(orc_model));
     m->p = *pin;
     orc_params *p = &m->p;
-    if (p->lattice != ORC_CUBIC) p->l3 = 1;
+    if (p->lattice != ORC_CUBIC && p->lattice != ORC_R_CUBIC) p->l3 = 1;
     if (orc_latt_build(&m->L, p->lattice, p->l1, p->l2, p->l3) != 0) { free(m); return NULL; }
     p->theta = p->theta * M_PI;
     m->lq = m->L.ncell;
@@ -1043,10 +1045,12 @@ void orc_obser_init(orc_chain *c) {   /* dqmc_measure_2d.f90:105-130 */
 
 static int npbc_cyc(int nr, int l) { if (nr > l) return nr - l; if (nr < 1) return nr + l; return nr; }
 
-/* equaltime_measure of the cubic lattice after energy_bin(1:2)
- * (src/dqmc_measure/equaltime_measure3d.f90:43-179): zkint over the six bond
- * families of the A sites (no rt, no t2 term), zint_u, and cpcm, spsm, nn (+ zn),
- * bondcorr (+ zb) with the bond partner nnlist(j, 1).  The bins are the
+/* equaltime_measure of the cubic and r_cubic lattices after energy_bin(1:2)
+ * (src/dqmc_measure/equaltime_measure3d.f90:43-179): zkint over the bond
+ * families of the A sites (no rt, no t2 term), zint_u, and cpcm, spsm, nn (+ zn)
+ * binned by the cell distance imj(list(i,1), list(j,1)) over all orbital
+ * pairs, bondcorr (+ zb) over the pairs (nu, nnlist(nu, 1)) for nu = 1..lq,
+ * a cell index used as a site index as the reference does.  The bins are the
  * (no_i, no_j) = (1, 1) block of the 2D layout; pair_onsite, jj, pair_nn,
  * pair_sn, zj and energy_bin(5:10) do not exist here and stay 0.  c->gfc
  * already holds Gc. */
@@ -1127,7 +1131,7 @@ void orc_measure(orc_chain *c, int nt) {
     zc zne = 0;
     for (int i = 0; i < N; ++i) zne += GC(i, i);
     c->energy_bin[1] += zne * zphi / (double)lq;
-    if (L->kind == ORC_CUBIC) { measure_3d(c, zphi); return; }
+    if (L->kind == ORC_CUBIC || L->kind == ORC_R_CUBIC) { measure_3d(c, zphi); return; }
     /* zkint; the chain's (equaltime_measure1d.f90) carries the factor nflr rt on
      * the bonds and 2 t2 on the two second neighbours */
     const int chain = (L->kind == ORC_CHAIN);
@@ -1451,10 +1455,11 @@ static void dyn_measure(orc_chain *c, int nt, const zc *gt0, const zc *g0t, cons
         for (int i = 0; i < N; ++i) {
             int nu_i = L->list[i * 2 + 0], no_i = L->list[i * 2 + 1];
             int imj = L->imj[(nu_i - 1) * L->ncell + (nu_j - 1)];
-            z[(imj - 1) + lq * (no_i - 1) + 2 * lq * (no_j - 1)] +=
+            const int d3 = L->kind == ORC_CUBIC || L->kind == ORC_R_CUBIC;   /* orbital pairs summed */
+            z[(imj - 1) + (d3 ? 0 : lq * (no_i - 1) + 2 * lq * (no_j - 1))] +=
                 (0.5 - creal(gtt[ZIDX(i, i, N)])) * (0.5 - creal(g00[ZIDX(j, j, N)]))
                 - (1.0 / m->p.nflr) * g0t[ZIDX(j, i, N)] * gt0[ZIDX(i, j, N)];
-            if (L->kind == ORC_CUBIC) {
+            if (d3) {
                 const double fsp = 1.0 - 1.0 / (double)(m->p.nflr * m->p.nflr);
                 z[(imj - 1) + lq] += -g0t[ZIDX(j, i, N)] * gt0[ZIDX(i, j, N)] * fsp;
                 z[(imj - 1) + 2 * lq] += gt0[ZIDX(i, j, N)];

@@ -351,12 +351,102 @@ static void setup_cubic(orc_latt *L, int l1, int l2, int l3) {
 #undef CELL
 }
 
+/* setup_latt3d_sub + setup_r_cubic_sub (src/lattice.f90:1486-1605): six
+ * sites per cell, (cell-1)*6 + isub with the cells in the order i3, i1, i2;
+ * nnlf_list(i) = 2i - 1 for i = 1..3 lq; nnlist as the reference writes it per
+ * residue of the site index mod 6; snlist and plq_cord zero. */
+static void setup_r_cubic(orc_latt *L, int l1, int l2, int l3) {
+    L->kind = ORC_R_CUBIC; L->l1 = l1; L->l2 = l2; L->l3 = l3;
+    const int nc = l1 * l2 * l3, ns = 6 * nc;
+    L->ncell = nc; L->nsub = 6; L->nsites = ns; L->z_plq = 8; L->nn_nf = 4; L->nn_lf = 3 * nc; L->nsn = 12;
+#define CELL(a, b, c) ((npbc((c), l3) - 1) * l1 * l2 + (npbc((a), l1) - 1) * l2 + npbc((b), l2))
+    L->ulist3 = malloc(sizeof(int) * 3 * nc);
+    L->list = malloc(sizeof(int) * 2 * ns);
+    int *cd = malloc(sizeof(int) * 3 * ns);
+    int ind = 0;
+    for (int i3 = 1; i3 <= l3; ++i3)
+        for (int i1 = 1; i1 <= l1; ++i1)
+            for (int i2 = 1; i2 <= l2; ++i2) {
+                const int c = CELL(i1, i2, i3);
+                L->ulist3[(c - 1) * 3] = i1; L->ulist3[(c - 1) * 3 + 1] = i2; L->ulist3[(c - 1) * 3 + 2] = i3;
+                for (int isub = 1; isub <= 6; ++isub) {
+                    L->list[ind * 2] = c; L->list[ind * 2 + 1] = isub;
+                    cd[ind * 3] = i1; cd[ind * 3 + 1] = i2; cd[ind * 3 + 2] = i3;
+                    ++ind;
+                }
+            }
+    L->nnlf_list = malloc(sizeof(int) * L->nn_lf);
+    for (int i = 1; i <= L->nn_lf; ++i) L->nnlf_list[i - 1] = 2 * i - 1;
+    L->listk = malloc(sizeof(int) * 3 * nc);
+    int k = 0;
+    for (int l = -(l3 + 1) / 2 + 1; l <= l3 / 2; ++l)
+        for (int mm = -(l1 + 1) / 2 + 1; mm <= l1 / 2; ++mm)
+            for (int n = -(l2 + 1) / 2 + 1; n <= l2 / 2; ++n) {
+                L->listk[k * 3] = mm; L->listk[k * 3 + 1] = n; L->listk[k * 3 + 2] = l; ++k;
+            }
+    L->imj = malloc(sizeof(int) * nc * nc);
+    for (int j = 0; j < nc; ++j)
+        for (int i = 0; i < nc; ++i) {
+            int nx = npbc(L->ulist3[i * 3] - L->ulist3[j * 3], l1);
+            int ny = npbc(L->ulist3[i * 3 + 1] - L->ulist3[j * 3 + 1], l2);
+            int nz = npbc(L->ulist3[i * 3 + 2] - L->ulist3[j * 3 + 2], l3);
+            L->imj[i * nc + j] = (nz - 1) * l1 * l2 + ny + (nx - 1) * l2;
+        }
+    L->zexpiqr = malloc(sizeof(zc) * nc * nc);
+    for (int i = 0; i < nc; ++i)
+        for (int nk = 0; nk < nc; ++nk) {
+            double ph = 2.0 * M_PI * ((double)L->listk[nk * 3] * L->ulist3[i * 3] / l1 +
+                                      (double)L->listk[nk * 3 + 1] * L->ulist3[i * 3 + 1] / l2 +
+                                      (double)L->listk[nk * 3 + 2] * L->ulist3[i * 3 + 2] / l3);
+            L->zexpiqr[i * nc + nk] = cexp(I * ph);
+        }
+    L->nnlist = malloc(sizeof(int) * ns * 4);
+    for (int i = 1; i <= ns; ++i) {
+        const int c1 = cd[(i - 1) * 3], c2 = cd[(i - 1) * 3 + 1], c3 = cd[(i - 1) * 3 + 2], r = i % 6;
+        int *nl = &L->nnlist[(i - 1) * 4];
+        if (r == 3 || r == 5) {           /* A2, A3 */
+            nl[0] = i + 1;
+            nl[1] = (CELL(c1 - 1, c2, c3) - 1) * 6 + r + 1;
+            nl[2] = (CELL(c1, c2 - 1, c3) - 1) * 6 + r + 1;
+            nl[3] = i - 1;
+        } else if (r == 1) {              /* A1 */
+            nl[0] = i + 1;
+            nl[1] = (CELL(c1 - 1, c2, c3) - 1) * 6 + r + 1;
+            nl[2] = (CELL(c1, c2 - 1, c3) - 1) * 6 + r + 1;
+            nl[3] = (CELL(c1 - 1, c2 - 1, c3 - 1) - 1) * 6 + r + 1;
+        } else if (r == 2 || r == 4) {    /* B1, B2 */
+            nl[0] = i - 1;
+            nl[1] = (CELL(c1 + 1, c2, c3) - 1) * 6 + r - 1;
+            nl[2] = (CELL(c1, c2 + 1, c3) - 1) * 6 + r - 1;
+            nl[3] = i + 1;
+        } else {                           /* B3 */
+            nl[0] = i - 1;
+            nl[1] = (CELL(c1 + 1, c2, c3) - 1) * 6 + 5;
+            nl[2] = (CELL(c1, c2 + 1, c3) - 1) * 6 + 5;
+            nl[3] = (CELL(c1 + 1, c2 + 1, c3 + 1) - 1) * 6 + 1;
+        }
+    }
+    L->snlist = calloc((size_t)ns * 12, sizeof(int));
+    L->plq_cord = calloc((size_t)nc * 8, sizeof(int));
+    L->nnveci = calloc((size_t)ns * 4 * 2, sizeof(int));
+    L->nnvecr = calloc((size_t)ns * 4 * 2, sizeof(double));
+    L->cord = malloc(sizeof(int) * 2 * ns);
+    L->rcord = malloc(sizeof(double) * 2 * ns);
+    for (int i = 0; i < ns; ++i) {
+        L->cord[i * 2] = cd[i * 3]; L->cord[i * 2 + 1] = cd[i * 3 + 1];
+        L->rcord[i * 2] = cd[i * 3]; L->rcord[i * 2 + 1] = cd[i * 3 + 1];
+    }
+    free(cd);
+#undef CELL
+}
+
 int orc_latt_build(orc_latt *L, int kind, int l1, int l2, int l3) {
     memset(L, 0, sizeof(*L));
     if (kind == ORC_SQUARE) setup_square(L, l1, l2);
     else if (kind == ORC_HONEYCOMB) setup_honeycomb(L, l1, l2);
     else if (kind == ORC_CHAIN) setup_chain(L, l1);
     else if (kind == ORC_CUBIC) setup_cubic(L, l1, l2, l3);
+    else if (kind == ORC_R_CUBIC) setup_r_cubic(L, l1, l2, l3);
     else return -1;
     return 0;
 }
@@ -364,7 +454,7 @@ int orc_latt_build(orc_latt *L, int kind, int l1, int l2, int l3) {
 /* expar.f90: Landau-gauge Peierls phase for bond (i, nf), twist flux and
  * dimerisation.  i is 0-based, nf is 1-based as in the reference. */
 zc orc_expar(const orc_latt *L, int i, int nf, double xmag, double fx, double fy, double dimer) {
-    if (L->kind == ORC_CUBIC) return 1.0;      /* expar3d.f90 */
+    if (L->kind == ORC_CUBIC || L->kind == ORC_R_CUBIC) return 1.0;      /* expar3d.f90 */
     int k = (i * L->nn_nf + (nf - 1)) * 2;
     int nax = L->nnveci[k], nay = L->nnveci[k + 1];
     double vr1 = L->nnvecr[k], vr2 = L->nnvecr[k + 1];

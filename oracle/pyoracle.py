@@ -21,7 +21,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
 
-SQUARE, HONEYCOMB, CHAIN, CUBIC = 1, 2, 3, 4
+SQUARE, HONEYCOMB, CHAIN, CUBIC, R_CUBIC = 1, 2, 3, 4, 5
 FAST, DELAY, SUBMATRIX, SUBMATRIX_G, SUBMATRIX_G_EXACT = 0, 1, 2, 3, 4
 CHECKERBOARD, FFT, DENSE = 0, 1, 2
 HS_EXACT, HS_GENERAL4 = 0, 1
@@ -41,7 +41,7 @@ class OrcParams(C.Structure):
         ("update", C.c_int32), ("kinetic", C.c_int32), ("hs", C.c_int32),
         ("proj", C.c_int32), ("lprojv", C.c_int32), ("obs_mid_len", C.c_int32),
         ("ltau", C.c_int32), ("dyntau", C.c_double),
-        ("l3", C.c_int32),
+        ("l3", C.c_int32), ("rtd", C.c_double),
     ]
 
 
@@ -170,7 +170,7 @@ def make_params(**kw) -> OrcParams:
              mu=0.0, rhub=0.0, rv=0.0, alpha=0.2, theta=0.0, xmag=0.0, flux_x=0.0, flux_y=0.0,
              dimer=0.0, rndness=0.0, nflr=2, lproju=0, lstabilize=1, nwrap=10, nsweep=20, nbin=10,
              nublock=0, update=DELAY, kinetic=CHECKERBOARD, hs=HS_GENERAL4, proj=0, lprojv=0,
-             obs_mid_len=1, ltau=0, dyntau=0.0, l3=1)
+             obs_mid_len=1, ltau=0, dyntau=0.0, l3=1, rtd=1.0)
     d.update(kw)
     return OrcParams(**d)
 
@@ -197,7 +197,7 @@ class Model:
 
     def tables(self):
         N, lq = self.ndim, self.lq
-        nsn = {SQUARE: 4, HONEYCOMB: 6, CHAIN: 2, CUBIC: 12}[self.params.lattice]
+        nsn = {SQUARE: 4, HONEYCOMB: 6, CHAIN: 2, CUBIC: 12, R_CUBIC: 12}[self.params.lattice]
         nnlist = np.zeros((N, self.nn_nf), np.int32)
         nnlf = np.zeros(self.nn_lf, np.int32)
         lst = np.zeros((N, 2), np.int32)

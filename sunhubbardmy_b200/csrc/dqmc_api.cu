@@ -35,9 +35,10 @@ extern "C" const char* dqmc_gpu_last_error(void) { return g_err.c_str(); }
 // ---------------------------------------------------------------------------
 extern "C" int dqmc_params_derive(dqmc_params* p) {
     if (!p) return fail(DQMC_EINVAL, "null params");
-    if (p->lattice < DQMC_LATT_SQUARE || p->lattice > DQMC_LATT_CUBIC)
-        return fail(DQMC_EINVAL, "lattice must be square, honeycomb, chain or cubic");
-    if (p->lattice != DQMC_LATT_CUBIC) p->l3 = 1;
+    if (p->lattice < DQMC_LATT_SQUARE || p->lattice > DQMC_LATT_R_CUBIC)
+        return fail(DQMC_EINVAL, "lattice must be square, honeycomb, chain, cubic or r_cubic");
+    const bool d3 = p->lattice == DQMC_LATT_CUBIC || p->lattice == DQMC_LATT_R_CUBIC;
+    if (!d3) p->l3 = 1;
     if (p->lattice == DQMC_LATT_CHAIN) {
         if (p->l2 != 1 || p->l1 < 4 || p->l1 % 2) return fail(DQMC_EINVAL, "the chain needs l2 = 1 and an even l1 >= 4");
     } else if (p->lattice == DQMC_LATT_CUBIC) {
@@ -45,12 +46,15 @@ extern "C" int dqmc_params_derive(dqmc_params* p) {
         // every bond once only for even lengths (setup_cubic_sub, lattice.f90:1300-1312)
         if (p->l1 < 2 || p->l2 < 2 || p->l3 < 2 || p->l1 % 2 || p->l2 % 2 || p->l3 % 2)
             return fail(DQMC_EINVAL, "the cubic lattice needs even l1, l2, l3 >= 2");
+    } else if (p->lattice == DQMC_LATT_R_CUBIC) {
+        if (p->l1 < 2 || p->l2 < 2 || p->l3 < 2) return fail(DQMC_EINVAL, "the r_cubic lattice needs l1, l2, l3 >= 2");
+        if (p->rv != 0.0) return fail(DQMC_EINVAL, "the t-V bond field is not supported on the r_cubic lattice");
     } else if (p->l1 < 2 || p->l2 < 2) {
         return fail(DQMC_EINVAL, "l1, l2 must be >= 2");
     }
     if (p->dtau <= 0 || p->beta <= 0) return fail(DQMC_EINVAL, "beta, dtau must be > 0");
     p->lq = p->l1 * p->l2 * p->l3;
-    p->ndim = (p->lattice == DQMC_LATT_HONEYCOMB) ? 2 * p->lq : p->lq;
+    p->ndim = (p->lattice == DQMC_LATT_HONEYCOMB) ? 2 * p->lq : (p->lattice == DQMC_LATT_R_CUBIC) ? 6 * p->lq : p->lq;
     p->ne = p->ndim / 2 + (int)(p->nu * p->ndim / 8.0);
     p->ltrot = (int)std::lround(p->beta / p->dtau);
     if (p->nublock == 0) {
@@ -176,10 +180,71 @@ static void build_cubic(HostModel& m) {
             }
 }
 
+// setup_latt3d_sub / setup_r_cubic_sub (src/lattice.f90:1033-1157, 1486-1605):
+// three honeycomb layers per cell, sites (cell - 1) 6 + isub with isub = A1,
+// B1, A2, B2, A3, B3 and cells numbered as on the cubic lattice; the A sites
+// (odd, 1-based) own the nn_lf = 3 lq bonds of the four families.  nnlist is
+// the reference's table as written (family 4 of A1 reaches sub-site 2 of the
+// cell at (-1, -1, -1), so two family-4 bonds share that B1 site); snlist,
+// tnlist and plq_cord are left empty (0 in the reference, -1 here).
+static void build_rcubic(HostModel& m) {
+    const dqmc_params& p = m.p;
+    const int l1 = p.l1, l2 = p.l2, l3 = p.l3;
+    m.a1[0] = 1; m.a1[1] = 0; m.a2[0] = 0; m.a2[1] = 1;
+    m.lq = l1 * l2 * l3;
+    m.nsub = 6; m.N = 6 * m.lq; m.nn_nf = 4; m.nn_lf = 3 * m.lq; m.z_plq = 8; m.nsn = 12;
+    const int N = m.N;
+    auto cell = [&](int i1, int i2, int i3) { return (npbc(i3, l3) - 1) * l1 * l2 + (npbc(i1, l1) - 1) * l2 + npbc(i2, l2) - 1; };
+    m.cell1.resize(N); m.cell2.resize(N); m.cell3.resize(N); m.rc1.resize(N); m.rc2.resize(N);
+    for (int i3 = 1; i3 <= l3; ++i3)
+        for (int i1 = 1; i1 <= l1; ++i1)
+            for (int i2 = 1; i2 <= l2; ++i2)
+                for (int o = 0; o < 6; ++o) {
+                    const int s = cell(i1, i2, i3) * 6 + o;
+                    m.cell1[s] = i1; m.cell2[s] = i2; m.cell3[s] = i3; m.rc1[s] = i1; m.rc2[s] = i2;
+                }
+    for (int b = 0; b < m.nn_lf; ++b) m.nnlf.push_back(2 * b);
+    m.nnlist.assign(N * 4, 0); m.snlist.assign(N * 12, -1);
+    m.nnveci.assign(N * 4 * 2, 0); m.nnvecr.assign(N * 4 * 2, 0.0);
+    for (int s = 0; s < N; ++s) {
+        const int i = s + 1, r = i % 6, c1 = m.cell1[s], c2 = m.cell2[s], c3 = m.cell3[s];
+        int* nl = &m.nnlist[s * 4];
+        if (r == 3 || r == 5 || r == 1) {          // A2, A3, A1
+            nl[0] = s + 1;
+            nl[1] = cell(c1 - 1, c2, c3) * 6 + r;     // 0-based sub-site r = 1-based r + 1
+            nl[2] = cell(c1, c2 - 1, c3) * 6 + r;
+            nl[3] = (r == 1) ? cell(c1 - 1, c2 - 1, c3 - 1) * 6 + r : s - 1;
+        } else if (r == 2 || r == 4) {              // B1, B2
+            nl[0] = s - 1;
+            nl[1] = cell(c1 + 1, c2, c3) * 6 + r - 2;
+            nl[2] = cell(c1, c2 + 1, c3) * 6 + r - 2;
+            nl[3] = s + 1;
+        } else {                                     // B3
+            nl[0] = s - 1;
+            nl[1] = cell(c1 + 1, c2, c3) * 6 + 4;
+            nl[2] = cell(c1, c2 + 1, c3) * 6 + 4;
+            nl[3] = cell(c1 + 1, c2 + 1, c3 + 1) * 6;
+        }
+    }
+    m.imj.assign(m.lq * m.lq, 0);
+    m.cell_plus.assign(m.lq * m.lq, 0);
+    for (int j = 0; j < m.lq; ++j)
+        for (int i = 0; i < m.lq; ++i) {
+            const int si = i * 6, sj = j * 6;
+            const int nx = npbc(m.cell1[si] - m.cell1[sj], l1), ny = npbc(m.cell2[si] - m.cell2[sj], l2);
+            const int nz = npbc(m.cell3[si] - m.cell3[sj], l3);
+            const int d = (nz - 1) * l1 * l2 + ny + (nx - 1) * l2 - 1;
+            m.imj[i * m.lq + j] = d;
+            m.cell_plus[d * m.lq + j] = i;
+        }
+    m.plq.assign(m.lq * 8, -1);
+}
+
 static void build_lattice(HostModel& m) {
     const dqmc_params& p = m.p;
     int l1 = p.l1, l2 = p.l2;
     if (p.lattice == DQMC_LATT_CUBIC) { build_cubic(m); return; }
+    if (p.lattice == DQMC_LATT_R_CUBIC) { build_rcubic(m); return; }
     m.lq = l1 * l2;
     if (p.lattice == DQMC_LATT_CHAIN) {
         // setup_latt1d_sub / setup_chain_sub (src/lattice.f90:67-135, 240-316): bond
@@ -325,7 +390,7 @@ static void build_lattice(HostModel& m) {
 // Peierls / twist / dimerisation phase of bond (site i, family nf 1-based): expar.f90
 static zc expar(const HostModel& m, int i, int nf) {
     const dqmc_params& p = m.p;
-    if (p.lattice == DQMC_LATT_CUBIC) return zc(1.0, 0.0);    // expar3d.f90: no phase
+    if (p.lattice == DQMC_LATT_CUBIC || p.lattice == DQMC_LATT_R_CUBIC) return zc(1.0, 0.0);    // expar3d.f90: no phase
     int k = (i * m.nn_nf + nf - 1) * 2;
     int nax = m.nnveci[k], nay = m.nnveci[k + 1];
     double vr1 = m.nnvecr[k], vr2 = m.nnvecr[k + 1];
@@ -363,7 +428,7 @@ static int build_model(HostModel& m) {
     dqmc_params& p = m.p;
     if (p.t3 != 0.0) return fail(DQMC_EINVAL, "t3 != 0 is not supported");
     if (p.kinetic < DQMC_KIN_CHECKERBOARD || p.kinetic > DQMC_KIN_DENSE) return fail(DQMC_EINVAL, "kinetic must be 0, 1 or 2");
-    if (p.lattice < DQMC_LATT_SQUARE || p.lattice > DQMC_LATT_CUBIC) return fail(DQMC_EINVAL, "lattice must be 1, 2, 3 or 4");
+    if (p.lattice < DQMC_LATT_SQUARE || p.lattice > DQMC_LATT_R_CUBIC) return fail(DQMC_EINVAL, "lattice must be 1 to 5");
     if (p.lattice == DQMC_LATT_CUBIC && (p.l1 < 2 || p.l2 < 2 || p.l3 < 2 || p.l1 % 2 || p.l2 % 2 || p.l3 % 2))
         return fail(DQMC_EINVAL, "the cubic lattice needs even l1, l2, l3 >= 2");
     if (p.lattice == DQMC_LATT_CHAIN && (p.l2 != 1 || p.l1 < 4 || p.l1 % 2))
@@ -391,7 +456,9 @@ static int build_model(HostModel& m) {
             int ist = b + (f - 1) * m.nn_lf;
             int i0 = m.nnlf[b], i1 = m.nnlist[i0 * m.nn_nf + f - 1];
             m.bond_i1[ist] = i0; m.bond_i2[ist] = i1;
-            zc z = -p.rt * m.expar[i0 * m.nn_nf + f - 1];
+            // the r_cubic build hops rtd on family 4 (dqmc_set_h0conf.f90:22-73)
+            const double t = (p.lattice == DQMC_LATT_R_CUBIC && f == 4) ? p.rtd : p.rt;
+            zc z = -t * m.expar[i0 * m.nn_nf + f - 1];
             double d = -p.mu / m.nn_nf;
             exp2x2(d, z, 0.5 * p.dtau, &m.urt[ist * 4]);
             exp2x2(d, z, -0.5 * p.dtau, &m.urtm1[ist * 4]);
@@ -573,7 +640,7 @@ static int upload_model(HostModel& m) {
     d.phase_on = (p.rhub > 0.0) ? 1 : 0;
     d.rt = p.rt; d.rv = p.rv; d.t2 = p.t2; d.theta = p.theta * M_PI;
     d.chain = p.lattice == DQMC_LATT_CHAIN;
-    d.cubic = p.lattice == DQMC_LATT_CUBIC;
+    d.cubic = p.lattice == DQMC_LATT_CUBIC || p.lattice == DQMC_LATT_R_CUBIC;
     d.l3 = p.l3;
     set_hs(m, d);
     // projective path and vconf constants (src/dqmc_config_v/dqmc_set_conf.f90:1-79)
@@ -604,11 +671,43 @@ static int upload_model(HostModel& m) {
         }
     }
     int rc;
-    if ((rc = upload(m, m.bond_i1, &d.bond_i1))) return rc;
-    if ((rc = upload(m, m.bond_i2, &d.bond_i2))) return rc;
+    {
+        // The reference applies the bonds of a family one after the other
+        // (dqmc_left_forward_prop.f90:27-38); the device applies a family's
+        // bonds in parallel, which is the same product only for bonds without
+        // a common site.  Each family is stored as two such phases: the bonds
+        // none of whose sites occurred earlier in the family, then the rest
+        // (the r_cubic family 4 shares its B1 sites); phase 2 runs after phase 1.
+        const int lf = m.nn_lf, nnf = m.nn_nf;
+        if (nnf > DQ_MAX_NNF) return fail(DQMC_EINVAL, "too many bond families");
+        std::vector<int> b1(m.bond_i1.size()), b2(m.bond_i2.size());
+        std::vector<zc> u(m.urt.size()), um(m.urtm1.size());
+        for (int f = 0; f < nnf; ++f) {
+            std::vector<int> seen(m.N, 0), order, late;
+            for (int b = 0; b < lf; ++b) {
+                const int ist = f * lf + b, x = m.bond_i1[ist], y = m.bond_i2[ist];
+                (seen[x] || seen[y] ? late : order).push_back(ist);
+                seen[x]++; seen[y]++;
+            }
+            std::vector<int> seen2(m.N, 0);
+            for (int ist : late)
+                if (seen2[m.bond_i1[ist]]++ || seen2[m.bond_i2[ist]]++)
+                    return fail(DQMC_EINVAL, "a bond family needs more than two disjoint phases");
+            d.cb_split[f] = (int)order.size();
+            order.insert(order.end(), late.begin(), late.end());
+            for (int b = 0; b < lf; ++b) {
+                const int src = order[b], dst = f * lf + b;
+                b1[dst] = m.bond_i1[src]; b2[dst] = m.bond_i2[src];
+                for (int e = 0; e < 4; ++e) { u[dst * 4 + e] = m.urt[src * 4 + e]; um[dst * 4 + e] = m.urtm1[src * 4 + e]; }
+            }
+        }
+        if ((rc = upload(m, b1, &d.bond_i1))) return rc;
+        if ((rc = upload(m, b2, &d.bond_i2))) return rc;
+        std::vector<double2> tb;
+        tb = to_d2(u); if ((rc = upload(m, tb, &d.urt))) return rc;
+        tb = to_d2(um); if ((rc = upload(m, tb, &d.urtm1))) return rc;
+    }
     std::vector<double2> t;
-    t = to_d2(m.urt); if ((rc = upload(m, t, &d.urt))) return rc;
-    t = to_d2(m.urtm1); if ((rc = upload(m, t, &d.urtm1))) return rc;
     if (p.kinetic == DQMC_KIN_DENSE && m.dense_on_device) {
         // urt / urtm1 from the device eigen-decomposition of seth0
         std::vector<double2> z((size_t)m.N * m.N, make_double2(0.0, 0.0));
@@ -1463,7 +1562,8 @@ static bool proj_mid(const HostModel& m, int nt) {
 
 // equal-time measurement of the current G (equaltime_measure)
 static void launch_measure_h(dqmc_handle* h) {
-    const int kind = h->models[0]->p.lattice == DQMC_LATT_CUBIC ? MEAS_CUBIC
+    const int lat = h->models[0]->p.lattice;
+    const int kind = lat == DQMC_LATT_CUBIC ? MEAS_CUBIC : lat == DQMC_LATT_R_CUBIC ? MEAS_R_CUBIC
                    : h->models[0]->nsub == 2 ? MEAS_HONEYCOMB : MEAS_ONE_ORBITAL;
     launch_measure(h->d_chains, h->nch, h->maxN, kind, h->max_lq, h->st);
 }

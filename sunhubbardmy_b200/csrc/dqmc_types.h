@@ -4,6 +4,7 @@
 #include <stdint.h>
 
 #define DQ_MAX_LCOMP 4
+#define DQ_MAX_NNF 8      // bond families
 #define DQ_MAX_PROG 256   // propagation ops per pass (nwrap slices x ops per slice)
 
 // Model tables for one lattice/parameter set (read-only during a sweep).
@@ -14,7 +15,8 @@ struct ModelDev {
     int lwrapT, lwrapu, phase_on;        // phase_on: rhub > 0 (set_phase multiplies conf phases)
     double rt, rv, t2, theta;
     int chain;                 // 1D chain: the energy terms of equaltime_measure1d.f90
-    int cubic, l3;             // cubic lattice (l3 = 1 otherwise): the observables of equaltime_measure3d.f90
+    int cubic, l3;             // cubic or r_cubic lattice (l3 = 1 otherwise): the observables of equaltime_measure3d.f90
+    int cb_split[DQ_MAX_NNF];  // bonds of each family's first disjoint phase (the device bond order)
     // HS constants (src/dqmc_config_u/dqmc_set_conf.f90)
     double2 bmat[DQ_MAX_LCOMP], bmat_inv[DQ_MAX_LCOMP], phase[DQ_MAX_LCOMP];
     double2 delta[DQ_MAX_LCOMP * (DQ_MAX_LCOMP - 1)];        // [(is-1)*(lc-1) + iflip-1]

@@ -203,9 +203,10 @@ DQ_DEV void meas_combine(double2& a0, double2& a1, double2& a2, double2& a3, int
 // GTc(i, j) = GT(i, j) - delta_ij = -Gc(i, j); whether site i of cell j + d
 // is site j is the same for every cell j (a translation), so it is taken
 // from cell 0.
-template <bool HC, bool D3>
+template <bool HC, bool D3, bool RC>
 DQ_DEV void meas_site(const ChainDev& c, int bin, double2 zphi) {   // bin of thread t % MEAS_BH
-    constexpr int NS = HC ? 2 : 1;
+    constexpr int NS = HC ? 2 : 1;        // orbital pairs binned separately
+    constexpr int NO = RC ? 6 : 1;        // orbitals summed into one bin (r_cubic)
     __shared__ double2 gcd[512];     // Gc(i,i)
     const ModelDev& md = *c.md;
     const int N = c.N, lq = md.lq, nflr = md.nflr;
@@ -220,17 +221,40 @@ DQ_DEV void meas_site(const ChainDev& c, int bin, double2 zphi) {   // bin of th
     const CellShift<D3> shift(d, md);
     const double fd = (shift(0) == 0 && a == b) ? 1.0 : 0.0;
     double2 s1 = cmk(0, 0), sB = cmk(0, 0), sA = cmk(0, 0), s4 = cmk(0, 0);
+    if (NO == 1) {
 #pragma unroll 4
-    for (int cj = valid ? h : lq; cj < lq; cj += MEAS_SPLIT) {
-        const int i = shift(cj) * NS + a, j = cj * NS + b;
-        const size_t o = (size_t)i + (size_t)N * j;
-        double2 gtc = GT[o];
-        const double2 g = G[o];
-        gtc.x -= fd;
-        s1 = cadd(s1, gtc);
-        sB = cfma(gtc, g, sB);
-        sA = cfma(gcd[i], gcd[j], sA);
-        s4 = cfma(g, g, s4);
+        for (int cj = valid ? h : lq; cj < lq; cj += MEAS_SPLIT) {
+            const int i = shift(cj) * NS + a, j = cj * NS + b;
+            const size_t o = (size_t)i + (size_t)N * j;
+            double2 gtc = GT[o];
+            const double2 g = G[o];
+            gtc.x -= fd;
+            s1 = cadd(s1, gtc);
+            sB = cfma(gtc, g, sB);
+            sA = cfma(gcd[i], gcd[j], sA);
+            s4 = cfma(g, g, s4);
+        }
+    } else {
+        // every orbital pair (oa, ob) of the cell pair (j + d, j); i == j only
+        // for d = 0 and oa == ob
+        const bool d0 = shift(0) == 0;
+        for (int cj = valid ? h : lq; cj < lq; cj += MEAS_SPLIT) {
+            const int ci = shift(cj);
+            for (int ob = 0; ob < NO; ++ob) {
+                const int j = cj * NO + ob;
+#pragma unroll
+                for (int oa = 0; oa < NO; ++oa) {
+                    const int i = ci * NO + oa;
+                    const size_t o = (size_t)i + (size_t)N * j;
+                    double2 gtc = GT[o];
+                    const double2 g = G[o];
+                    if (d0 && oa == ob) gtc.x -= 1.0;
+                    s1 = cadd(s1, gtc);
+                    sB = cfma(gtc, g, sB);
+                    sA = cfma(gcd[i], gcd[j], sA);
+                }
+            }
+        }
     }
     meas_combine(s1, sB, sA, s4, h);
     if (!valid || h) return;
@@ -253,7 +277,7 @@ DQ_DEV void meas_site(const ChainDev& c, int bin, double2 zphi) {   // bin of th
 // neighbour on the honeycomb; bond partner pb: nearest neighbour; pair
 // partner ps: second neighbour), so on the square lattice the Kronecker
 // deltas of Gc = delta - GT depend on d only and are taken from cell 0.
-template <bool HC, bool D3>
+template <bool HC, bool D3, bool RC>
 DQ_DEV void meas_bond(const ChainDev& c, int d, double2 zphi) {   // distance of thread t % MEAS_BH
     constexpr int NS = HC ? 2 : 1;
     __shared__ double2 jcell[512];   // Gc(i0,in) - Gc(in,i0), current partner
@@ -268,7 +292,7 @@ DQ_DEV void meas_bond(const ChainDev& c, int d, double2 zphi) {   // distance of
         const int inj = HC ? md.snlist[i0 * md.nsn] : md.nnlist[i0 * nnf];
         const int inb = md.nnlist[i0 * nnf];
         const double2 e = md.expar_nn[i0 * nnf];
-        pj[cc] = inj; pb[cc] = inb; ps[cc] = md.snlist[i0 * md.nsn]; pe[cc] = e;
+        pj[cc] = inj; pb[cc] = inb; ps[cc] = D3 ? 0 : md.snlist[i0 * md.nsn]; pe[cc] = e;
         jcell[cc] = csub(gcf(G, N, i0, inj), gcf(G, N, inj, i0));
         bcell[cc] = cadd(cmul(e, gcf(G, N, i0, inb)), cmul(cconj(e), gcf(G, N, inb, i0)));
     }
@@ -282,7 +306,7 @@ DQ_DEV void meas_bond(const ChainDev& c, int d, double2 zphi) {   // distance of
     auto gt = [&](int r, int s_) { return GT[(size_t)r + (size_t)N * s_]; };
     // deltas of the square lattice, from cell 0: [i0 == j0], [in == j0], [i0 == jn], [in == jn]
     double f00 = 0, fn0 = 0, f0n = 0, fnn = 0;
-    if (!HC) {
+    if (!HC && !RC) {
         const int ci = shift(0), in = pj[ci], jn = pj[0];
         f00 = ci == 0; fn0 = in == 0; f0n = ci == jn; fnn = in == jn;
     }
@@ -295,7 +319,10 @@ DQ_DEV void meas_bond(const ChainDev& c, int d, double2 zphi) {   // distance of
         // G and GTc = GT - delta (= -Gc) at rows i0, in of columns j0, jn
         const double2 g00 = gg(i0, j0), an = gg(inj, j0), b0v = gg(i0, jnj), gnn_j = gg(inj, jnj);
         double2 t0 = gt(i0, j0), tn = gt(inj, j0), u0 = gt(i0, jnj), un = gt(inj, jnj);
-        if (HC) {
+        if (HC || RC) {
+            // the r_cubic bond pairs (site nu, nnlist(nu, 1)) with nu a cell
+            // index used as a site index (measure_bondcorr of
+            // equaltime_measure3d.f90) are not translates of each other
             t0.x -= i0 == j0; tn.x -= inj == j0; u0.x -= i0 == jnj; un.x -= inj == jnj;
         } else {
             t0.x -= f00; tn.x -= fn0; u0.x -= f0n; un.x -= fnn;
@@ -334,9 +361,11 @@ DQ_DEV void meas_bond(const ChainDev& c, int d, double2 zphi) {   // distance of
             x = cfma(cconj(ef), r4, x);
         }
         sb = cadd(sb, rfma(-fn, x, cmul(bcell[cj], bcell[ci])));
-        // pair correlations (measure_paircorr)
-        sn = cfma(g00, gnn_b, sn);
-        ss = cfma(g00, gg(ps[ci], ps[cj]), ss);
+        // pair correlations (measure_paircorr; 2D and chain only)
+        if (!D3) {
+            sn = cfma(g00, gnn_b, sn);
+            ss = cfma(g00, gg(ps[ci], ps[cj]), ss);
+        }
     }
     meas_combine(sj, sb, sn, ss, h);
     if (!valid || h) return;
@@ -353,7 +382,7 @@ DQ_DEV void meas_bond(const ChainDev& c, int d, double2 zphi) {   // distance of
 
 // grid (1 + na + nb, chains): x = 0 the energy terms, then na CTAs of site
 // bins and nb CTAs of bond bins (sized for the largest lattice of the handle)
-template <bool HC, bool D3>
+template <bool HC, bool D3, bool RC>
 __global__ void __launch_bounds__(MEAS_NT, 2) k_measure(const ChainDev* __restrict__ chains, int na) {
     const ChainDev& c = chains[blockIdx.y];
     const double2 phase = cmk(c.stats[ST_PHASE_RE], c.stats[ST_PHASE_IM]);
@@ -361,8 +390,8 @@ __global__ void __launch_bounds__(MEAS_NT, 2) k_measure(const ChainDev* __restri
     const double2 zphi = cscale(phase, sgn / phase.x);
     const int x = blockIdx.x;
     if (x == 0) meas_energy(c, zphi, sgn);
-    else if (x <= na) meas_site<HC, D3>(c, (x - 1) * MEAS_BH + threadIdx.x % MEAS_BH, zphi);
-    else meas_bond<HC, D3>(c, (x - 1 - na) * MEAS_BH + threadIdx.x % MEAS_BH, zphi);
+    else if (x <= na) meas_site<HC, D3, RC>(c, (x - 1) * MEAS_BH + threadIdx.x % MEAS_BH, zphi);
+    else meas_bond<HC, D3, RC>(c, (x - 1 - na) * MEAS_BH + threadIdx.x % MEAS_BH, zphi);
 }
 
 __global__ void k_bins_clear(const ChainDev* __restrict__ chains, int nbins) {
@@ -397,16 +426,17 @@ __global__ void __launch_bounds__(256) k_transpose_g(const ChainDev* __restrict_
     }
 }
 
-// kind: MEAS_ONE_ORBITAL (square, chain), MEAS_HONEYCOMB or MEAS_CUBIC
+// kind: MEAS_ONE_ORBITAL (square, chain), MEAS_HONEYCOMB, MEAS_CUBIC or MEAS_R_CUBIC
 void launch_measure(const ChainDev* chains, int nchains, int maxN, int kind, int maxlq, cudaStream_t st) {
     const int nt = (maxN + 31) / 32;
     k_transpose_g<<<dim3(nt, nt, nchains), 256, 0, st>>>(chains, MAT_G);
     const int ns = kind == MEAS_HONEYCOMB ? 2 : 1;
     const int na = (maxlq * ns * ns + MEAS_BH - 1) / MEAS_BH, nb = (maxlq + MEAS_BH - 1) / MEAS_BH;
     const dim3 grid(1 + na + nb, nchains);
-    if (kind == MEAS_HONEYCOMB) k_measure<true, false><<<grid, MEAS_NT, 0, st>>>(chains, na);
-    else if (kind == MEAS_CUBIC) k_measure<false, true><<<grid, MEAS_NT, 0, st>>>(chains, na);
-    else k_measure<false, false><<<grid, MEAS_NT, 0, st>>>(chains, na);
+    if (kind == MEAS_HONEYCOMB) k_measure<true, false, false><<<grid, MEAS_NT, 0, st>>>(chains, na);
+    else if (kind == MEAS_CUBIC) k_measure<false, true, false><<<grid, MEAS_NT, 0, st>>>(chains, na);
+    else if (kind == MEAS_R_CUBIC) k_measure<false, true, true><<<grid, MEAS_NT, 0, st>>>(chains, na);
+    else k_measure<false, false, false><<<grid, MEAS_NT, 0, st>>>(chains, na);
 }
 
 // dyn_measure (src/dqmc_measure/dyn_measure.f90:1-101) at time index nt: the
@@ -428,18 +458,22 @@ __global__ void __launch_bounds__(256) k_dyn_measure(const ChainDev* __restrict_
     const double fn = 1.0 / (double)md.nflr, fsp = 1.0 - fn * fn;
     const double2 *G = c.G, *GT = c.GT, *gt0 = c.gt0, *g00 = c.g00;
     double2* bin = c.dynbins + (size_t)4 * lq * (nt - 1);
-    const int nbin = lq * nsub * nsub;
+    // the 3D lattices sum every orbital pair of a cell pair into one bin
+    const int nbin = md.cubic ? lq : lq * nsub * nsub, no = md.cubic ? nsub : 1;
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nbin; b += gridDim.x * blockDim.x) {
         const int d = b % lq, ab = b / lq, a = ab % nsub, bb = ab / nsub;
-        const CellShift<true> shift(d, md);     // l3 = 1 off the cubic lattice
+        const CellShift<true> shift(d, md);     // l3 = 1 off the 3D lattices
         double2 z = cmk(0, 0), zs = cmk(0, 0), zg = cmk(0, 0);
-#pragma unroll 4
         for (int cj = 0; cj < lq; ++cj) {
-            const int i = shift(cj) * nsub + a, j = cj * nsub + bb;
-            const size_t o = (size_t)i + (size_t)N * j;
-            const double v = (0.5 - G[(size_t)i * (N + 1)].x) * (0.5 - g00[(size_t)j * (N + 1)].x);
-            z = csub(cadd(z, cmk(v, 0.0)), cmul(cscale(GT[o], fn), gt0[o]));
-            if (md.cubic) { zs = csub(zs, cmul(cscale(GT[o], fsp), gt0[o])); zg = cadd(zg, gt0[o]); }
+            const int ci = shift(cj);
+            for (int ob = 0; ob < no; ++ob)
+                for (int oa = 0; oa < no; ++oa) {
+                    const int i = md.cubic ? ci * nsub + oa : ci * nsub + a, j = md.cubic ? cj * nsub + ob : cj * nsub + bb;
+                    const size_t o = (size_t)i + (size_t)N * j;
+                    const double v = (0.5 - G[(size_t)i * (N + 1)].x) * (0.5 - g00[(size_t)j * (N + 1)].x);
+                    z = csub(cadd(z, cmk(v, 0.0)), cmul(cscale(GT[o], fn), gt0[o]));
+                    if (md.cubic) { zs = csub(zs, cmul(cscale(GT[o], fsp), gt0[o])); zg = cadd(zg, gt0[o]); }
+                }
         }
         const size_t k = (size_t)d + (size_t)lq * a + (size_t)2 * lq * bb;
         bin[k] = cfma(z, zphi, bin[k]);

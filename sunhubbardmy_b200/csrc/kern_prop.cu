@@ -33,8 +33,18 @@ __device__ void apply_op(const ModelDev& md, const int32_t* conf, const int32_t*
         const double h = 1.0 / sqrt(2.0);
         const double2* U = (which == PW_INV) ? md.urtm1 : md.urt;
         const int32_t* vc = (kind == PK_VSCALE) ? vconf + ((size_t)(nt - 1) * md.nn_nf + (nf - 1)) * N : nullptr;
-        for (int w = tid; w < lf * ngrp; w += nth) {
-            const int b = w % lf, g = w / lf;
+        // a family's bonds come in two phases of disjoint bonds, the second
+        // applied after the first (the second is empty unless bonds of the
+        // family share a site, as on the r_cubic lattice)
+        const int sp = md.cb_split[nf - 1];
+        for (int ph = 0; ph < 2; ++ph) {
+        const int b0 = ph ? sp : 0, nbp = ph ? lf - sp : sp;
+        if (ph) {
+            if (nbp == 0) break;
+            __syncthreads();
+        }
+        for (int w = tid; w < nbp * ngrp; w += nth) {
+            const int b = b0 + w % nbp, g = w / nbp;
             const int v0 = g * per, v1 = min(nv, v0 + per);
             const int ist = (nf - 1) * lf + b;
             const int i1 = __ldg(&md.bond_i1[ist]), i2 = __ldg(&md.bond_i2[ist]);
@@ -73,6 +83,7 @@ __device__ void apply_op(const ModelDev& md, const int32_t* conf, const int32_t*
                     x[i2] = cmul(s2, x[i2]);
                 }
             }
+        }
         }
     } else if (kind == PK_DIAG) {
         const int32_t* cf = conf + (size_t)(nt - 1) * N;

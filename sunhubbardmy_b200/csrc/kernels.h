@@ -17,7 +17,7 @@ void launch_sfmt_raw(const ChainDev* chains, int chain, int count, cudaStream_t 
 void launch_update(const ChainDev* chains, int nchains, int nt, int visit, cudaStream_t st, int forced = 0);
 void launch_update_flush(const ChainDev* chains, int nchains, cudaStream_t st);   // G += A B^T alone
 // equal-time measurement: G^T into GT (tiled transpose), then the observables
-enum { MEAS_ONE_ORBITAL = 0, MEAS_HONEYCOMB = 1, MEAS_CUBIC = 2 };
+enum { MEAS_ONE_ORBITAL = 0, MEAS_HONEYCOMB = 1, MEAS_CUBIC = 2, MEAS_R_CUBIC = 3 };
 void launch_measure(const ChainDev* chains, int nchains, int maxN, int kind, int maxlq, cudaStream_t st);
 void launch_bins_clear(const ChainDev* chains, int nchains, int nbins, cudaStream_t st);
 void launch_stab_slots(const ChainDev* chains, int nchains, int src, int dst, cudaStream_t st);

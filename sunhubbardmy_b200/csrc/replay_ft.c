@@ -16,12 +16,12 @@
  *
  * Usage: replay_ft [dqmc.in] [key=value ...]
  *   dqmc.in      the &model_para and &ctrl_para namelists (src/model_para.f90:155-218);
- *                keys la, lb, lc, beta, dtau, rt, t2, t3, nu, mu, rhub, rv, alpha, theta,
+ *                keys la, lb, lc, beta, dtau, rt, rtd, t2, t3, nu, mu, rhub, rv, alpha, theta,
  *                nflr, lproju, lprojv, xmag, flux_x, flux_y, dimer, rndness,
  *                lstabilize, nwrap, nsweep, nbin, nublock, ltau, dyntau,
  *                obs_eqt_mid_len
  *   key=value    the same keys, plus the RUNMODE build flags of src/make.sys.*:
- *                lattice=1|2|3|4 (SQUARE|HONEYCOMB|CHAIN|CUBIC), update=0|1|2
+ *                lattice=1..5 (SQUARE|HONEYCOMB|CHAIN|CUBIC|R_CUBIC), update=0|1|2
  *                (fast|DELAY|SUBMATRIX), kinetic=0|1|2 (BREAKUP_T|FFT|zgemm),
  *                hs=0|1 (EXACTHS|general), and seed= (default: the -DTEST
  *                seed of rank 0, abs(2008*951049)), nwarmup= (default: nsweep
@@ -81,13 +81,13 @@ static int set_key(dqmc_params* p, const char* key, const char* val, int32_t* se
     if (!strcmp(k, "nwarmup")) { *nwarm = (int)v; return 0; }
     if (!strcmp(k, "out")) { snprintf(out, 256, "%s", val); return 0; }
     D(beta) D(dtau) D(rt) D(t2) D(t3) D(nu) D(mu) D(rhub) D(rv) D(alpha) D(theta)
-    D(xmag) D(flux_x) D(flux_y) D(dimer) D(rndness) D(dyntau)
+    D(xmag) D(flux_x) D(flux_y) D(dimer) D(rndness) D(dyntau) D(rtd)
     I(l1) I(l2) I(nflr) I(lproju) I(lprojv) I(lstabilize) I(nwrap) I(nsweep) I(nbin) I(nublock) I(ltau)
     I(lattice) I(update) I(kinetic) I(hs) I(proj)
 #undef D
 #undef I
-    /* namelist members with no effect on this path (rhub_plq, lprojplqu, rtd) */
-    if (!strcmp(k, "rhub_plq") || !strcmp(k, "lprojplqu") || !strcmp(k, "rtd")) return 0;
+    /* namelist members with no effect on this path (rhub_plq, lprojplqu) */
+    if (!strcmp(k, "rhub_plq") || !strcmp(k, "lprojplqu")) return 0;
     fprintf(stderr, "replay_ft: unknown key %s\n", key);
     return -1;
 }
@@ -129,7 +129,7 @@ int main(int argc, char** argv) {
     dqmc_params p;
     memset(&p, 0, sizeof(p));
     /* defaults of src/model_para.f90:166-206 and the square Hubbard build */
-    p.lattice = DQMC_LATT_SQUARE; p.l1 = 2; p.l2 = 2; p.l3 = 2; p.beta = 20.0; p.dtau = 0.05; p.rt = 1.0;
+    p.lattice = DQMC_LATT_SQUARE; p.l1 = 2; p.l2 = 2; p.l3 = 2; p.rtd = 1.0; p.beta = 20.0; p.dtau = 0.05; p.rt = 1.0;
     p.alpha = 0.2; p.nflr = 2; p.lstabilize = 1; p.nwrap = 10; p.nsweep = 20; p.nbin = 10;
     p.update = DQMC_UPD_DELAY; p.kinetic = DQMC_KIN_CHECKERBOARD; p.hs = DQMC_HS_GENERAL4; p.obs_mid_len = 1;
     int32_t seed = 1909706392;   /* abs((0*1981+2008)*951049), src/dqmc_util.f90:72 under -DTEST */

@@ -14,7 +14,7 @@ import re
 
 import numpy as np
 
-SQUARE, HONEYCOMB, CHAIN, CUBIC = 1, 2, 3, 4
+SQUARE, HONEYCOMB, CHAIN, CUBIC, R_CUBIC = 1, 2, 3, 4, 5
 FAST, DELAY, SUBMATRIX = 0, 1, 2
 CHECKERBOARD, FFT, DENSE = 0, 1, 2
 EXACT, GENERAL4 = 0, 1
@@ -55,7 +55,7 @@ class DqmcParams(C.Structure):
         ("ndim", C.c_int32), ("lq", C.c_int32), ("ltrot", C.c_int32), ("nst", C.c_int32),
         ("ne", C.c_int32), ("lcomp", C.c_int32),
         ("ltau", C.c_int32), ("ntdm", C.c_int32), ("dyntau", C.c_double),
-        ("l3", C.c_int32),
+        ("l3", C.c_int32), ("rtd", C.c_double),
     ]
 
     @classmethod
@@ -65,7 +65,7 @@ class DqmcParams(C.Structure):
                  mu=0.0, rhub=0.0, rv=0.0, alpha=0.2, theta=0.0, xmag=0.0, flux_x=0.0, flux_y=0.0,
                  dimer=0.0, rndness=0.0, nflr=2, lproju=0, lstabilize=1, nwrap=10, nsweep=20,
                  nbin=10, nublock=0, update=DELAY, kinetic=CHECKERBOARD, hs=GENERAL4, proj=0,
-                 lprojv=0, obs_mid_len=1, ltau=0, dyntau=0.0, l3=1)
+                 lprojv=0, obs_mid_len=1, ltau=0, dyntau=0.0, l3=1, rtd=1.0)
         d.update(kw)
         p = cls(**d)
         rc = load_library().dqmc_params_derive(C.byref(p))
@@ -77,8 +77,9 @@ class DqmcParams(C.Structure):
         """Lattice / kinetic tables built by the library (1-based, host only)."""
         N, lq = self.ndim, self.lq
         hc = self.lattice == HONEYCOMB
-        nnf, z, nsn = {HONEYCOMB: (3, 6, 6), CHAIN: (2, 1, 2), CUBIC: (6, 8, 12)}.get(self.lattice, (4, 4, 4))
-        nlf = lq if hc else lq // 2
+        nnf, z, nsn = {HONEYCOMB: (3, 6, 6), CHAIN: (2, 1, 2), CUBIC: (6, 8, 12),
+                       R_CUBIC: (4, 8, 12)}.get(self.lattice, (4, 4, 4))
+        nlf = {HONEYCOMB: lq, R_CUBIC: 3 * lq}.get(self.lattice, lq // 2)
         t = dict(nnlist=np.zeros((N, nnf), np.int32), nnlf_list=np.zeros(nlf, np.int32),
                  list=np.zeros((N, 2), np.int32), imj=np.zeros((lq, lq), np.int32),
                  plq_cord=np.zeros((lq, z), np.int32), snlist=np.zeros((N, nsn), np.int32),
@@ -599,7 +600,7 @@ class Dqmc:
     # projective path (params.proj = 1)
     def vconf(self, c: int = 0) -> np.ndarray:
         """t-V bond field vconf%conf as [ltrot][nn_nf][ndim] (bond index fastest)."""
-        nnf = {HONEYCOMB: 3, CHAIN: 2, CUBIC: 6}.get(self.chain_params(c).lattice, 4)
+        nnf = {HONEYCOMB: 3, CHAIN: 2, CUBIC: 6, R_CUBIC: 4}.get(self.chain_params(c).lattice, 4)
         out = np.zeros((self.ltrot, nnf, self.ndim(c)), np.int32)
         _check(load_library().dqmc_gpu_get_vconf(self.h, c, _ptr(out)), "get_vconf")
         return out

@@ -254,9 +254,9 @@ def dqmc_initial_print(f, p, wrap_step=None, nustock: int = 0) -> None:
     w(f" rv      = {g['rv']:7.3f}\n")
     w(f" lprojv   =  {_lg(g['lprojv'])}\n")
     w(f" la     = {g['l1']:4d}\n")
-    if g["lattice"] != 3:           # -DCHAIN prints la only
+    if g["lattice"] in (1, 2, 4):   # lb under -DHONEYCOMB, -DSQUARE, -DCUBIC
         w(f" lb     = {g['l2']:4d}\n")
-    if g["lattice"] == 4:           # -DCUBIC: lc as well
+    if g["lattice"] in (4, 5):      # lc under -DCUBIC, -DR_CUBIC
         w(f" lc     = {g.get('l3', 1):4d}\n")
     w(f" beta   = {g['beta']:6.2f}\n")
     w(f" dtau   = {g['dtau']:7.3f}\n")
@@ -281,7 +281,8 @@ def dqmc_initial_print(f, p, wrap_step=None, nustock: int = 0) -> None:
     for i, (a, b) in enumerate(wrap_step or [], start=1):
         w(f"{a:16d}{b:16d}{i:16d}\n")
     w(" \n")
-    w({2: "honeycomb_lattice", 3: "chain_lattice", 4: "cubic_lattice"}.get(g["lattice"], "square_lattice") + "\n")
+    w({2: "honeycomb_lattice", 3: "chain_lattice", 4: "cubic_lattice",
+       5: "rhombohedral_cubic_lattice"}.get(g["lattice"], "square_lattice") + "\n")
     if not isinstance(p, dict):
         print_latt(f, p)
 
@@ -325,6 +326,20 @@ def lattice_lists(p) -> dict:
         return dict(list=t["list"], cord=cord, nnlist=t["nnlist"], snlist=t["snlist"], tnlist=tn,
                     plq_cord=t["plq_cord"], listk=listk, a1=eye[0], a2=eye[1], a3=eye[2],
                     bz1=2.0 * np.pi * eye[0], bz2=2.0 * np.pi * eye[1], bz3=2.0 * np.pi * eye[2])
+    if lat == 5:      # r_cubic (setup_r_cubic_sub, src/lattice.f90:1486-1605; a_p of model_para.f90:366-371)
+        l3 = int(p.l3)
+        cord = np.zeros((N, 3), dtype=np.int64)
+        for i3 in range(1, l3 + 1):
+            for i1 in range(1, l1 + 1):
+                for i2 in range(1, l2 + 1):
+                    c = (i3 - 1) * l1 * l2 + (i1 - 1) * l2 + i2 - 1
+                    cord[6 * c:6 * c + 6] = (i1, i2, i3)
+        a = np.array([[0.5 * np.sqrt(3.0), -0.5, 0.0], [0.5 * np.sqrt(3.0), 0.5, 0.0], [0.0, 0.0, 1.0]])
+        inv = np.linalg.inv(a)          # bz_j(:) = 2 pi inv(:, j)
+        return dict(list=t["list"], cord=cord, nnlist=t["nnlist"], snlist=t["snlist"],
+                    tnlist=np.zeros((N, 8), dtype=np.int64), plq_cord=t["plq_cord"],
+                    listk=momentum_list3d(l1, l2, l3), a1=a[0], a2=a[1], a3=a[2],
+                    bz1=2.0 * np.pi * inv[:, 0], bz2=2.0 * np.pi * inv[:, 1], bz3=2.0 * np.pi * inv[:, 2])
     if lat == 3:      # chain
         a1, a2 = np.array([1.0]), None
         cord = np.array([[i] for i in range(1, l1 + 1)], dtype=np.int64)

@@ -2,8 +2,8 @@
 
 The cases are small versions of the benchmark configurations (square Hubbard
 with checkerboard, FFT or dense kinetic term, exact or general HS field;
-honeycomb SU(4); the 1D chain; the cubic lattice) sized so the oracle finishes each in well under
-a second.
+honeycomb SU(4); the 1D chain; the cubic and r_cubic lattices) sized so the oracle finishes each
+in well under a second.
 """
 import numpy as np
 
@@ -41,6 +41,12 @@ CASES = {
     "cu422_cb_exact_fast": dict(lattice=4, l1=4, l2=2, l3=2, beta=1.0, dtau=0.1, rhub=4.0, nflr=2,
                                 kinetic=0, update=0, hs=0, nwrap=10),
     "cu224_dense_exact_sub": dict(lattice=4, l1=2, l2=2, l3=4, beta=1.5, dtau=0.1, rhub=4.0, nflr=2, mu=0.1,
+                                  kinetic=2, update=2, hs=0, nwrap=5, nublock=8),
+    # the r_cubic lattice (-DR_CUBIC): six orbitals per cell, family 4 with
+    # shared sites and the interlayer hopping rtd
+    "rc222_cb_gen4_delay": dict(lattice=5, l1=2, l2=2, l3=2, beta=1.0, dtau=0.1, rhub=4.0, nflr=2, mu=0.1, rtd=0.7,
+                                kinetic=0, update=1, hs=1, nwrap=5, nublock=8),
+    "rc322_dense_exact_sub": dict(lattice=5, l1=3, l2=2, l3=2, beta=1.0, dtau=0.1, rhub=3.0, nflr=2,
                                   kinetic=2, update=2, hs=0, nwrap=5, nublock=8),
 }
 

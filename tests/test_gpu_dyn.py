@@ -27,6 +27,9 @@ DCASES = {
     # cubic lattice: znn_tau, zspsm_tau and gtau0 (dyn_measure3d.f90)
     "cu422_cb_gen4": dict(lattice=4, l1=4, l2=2, l3=2, beta=1.0, dtau=0.1, rhub=4.0, nflr=2, kinetic=0, update=1,
                           hs=1, nwrap=5, nublock=4, ltau=1, dyntau=0.6),
+    # r_cubic: the same three observables summed over the orbital pairs
+    "rc222_cb_gen4": dict(lattice=5, l1=2, l2=2, l3=2, beta=1.0, dtau=0.1, rhub=4.0, nflr=2, kinetic=0, update=1,
+                          hs=1, nwrap=5, nublock=4, rtd=0.7, ltau=1, dyntau=0.6),
 }
 
 

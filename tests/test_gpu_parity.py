@@ -175,7 +175,15 @@ def test_full_sweeps(sb, oracle, case):
         assert np.max(np.abs(g.green(k) - ch[k].green())) < 1e-10
         dg, dc = g.diag(k), ch[k].diag()
         assert dg["accepted"] == dc["accepted"] and dg["proposed"] == dc["proposed"]
-        assert dg["max_wrap_error"] < 1e-10
+        if CASES[case]["lattice"] == 5 and CASES[case]["kinetic"] == 0:
+            # r_cubic checkerboard: two bonds of family 4 share a site, so the
+            # family's operator is not symmetric and the sweep's wrap, G K^-1 ..
+            # K^T, is not the B product of the stack (dqmc_ft_sweep_b0.f90:58-61
+            # against dqmc_ft_core.f90:80-117); the reference's wrap error is
+            # O(dtau^2) there, and the GPU's must equal the oracle's
+            assert abs(dg["max_wrap_error"] - dc["max_wrap_error"]) < 1e-9 * dc["max_wrap_error"]
+        else:
+            assert dg["max_wrap_error"] < 1e-10
         assert abs(dg["phase"] - dc["phase"]) < 1e-9
         bg, bc = g.bins(k), ch[k].bins()
         assert bg["nobs"] == bc["nobs"]
