@@ -90,6 +90,12 @@ typedef struct dqmc_params {
     /* rtd of &model_para (-DR_CUBIC): the hopping of bond family 4 between
      * the layers of the r_cubic lattice (the reference's default is 1) */
     double rtd;
+    /* rhub_plq and lprojplqu of &model_para: the plaquette interaction, one
+     * HS field per plaquette and slice (hconf, src/dqmc_config_plqu.f90);
+     * finite temperature on the square and honeycomb lattices, without the
+     * unequal-time pass */
+    double rhub_plq;
+    int32_t lprojplqu;
 } dqmc_params;
 
 /* per-chain diagnostics (src/dqmc_util.f90:15-57, 287-299) */
@@ -113,6 +119,7 @@ typedef struct dqmc_diag {
     double restabilized;                /* re-stabilisations of the handle (dqmc_gpu_set_checks) since reset_diag */
     double near_ties;                   /* accept tests with | |Re(R phase)/Re(phase)| - r | < 1e-12: their
                                            outcome may depend on rounding (logged, not altered) */
+    double accepted_plq, proposed_plq;  /* main_obs(2): plaquette field */
 } dqmc_diag;
 
 typedef struct dqmc_handle dqmc_handle;
@@ -317,6 +324,12 @@ int dqmc_gpu_sweep_profile(dqmc_handle* h, int nsweeps, int lmeasure, double* ms
  * but unused, as in the reference. */
 int dqmc_gpu_set_vconf(dqmc_handle* h, int chain, const int32_t* vconf);
 int dqmc_gpu_get_vconf(dqmc_handle* h, int chain, int32_t* vconf);
+
+/* plaquette field hconf%conf_plqu(lq, ltrot) of one chain: int32 [ltrot][lq],
+ * plaquette fastest, values 1..lcomp (dqmc_input_plqconf / dqmc_output_plqconf).
+ * DQMC_ESTATE when the chain's model has rhub_plq = 0. */
+int dqmc_gpu_set_conf_plq(dqmc_handle* h, int chain, const int32_t* conf);
+int dqmc_gpu_get_conf_plq(dqmc_handle* h, int chain, int32_t* conf);
 /* trial state of one walker: proj (ndim x ndim complex, ascending eigenvectors
  * of the trial Hamiltonian, first ne columns used), w (ndim eigenvalues; may be
  * NULL).  set_trial replaces projL = projR (e.g. with a caller's eigenvectors). */

@@ -37,6 +37,8 @@ module dqmc_gpu_f
      real(c_double)     :: dyntau
      integer(c_int32_t) :: l3
      real(c_double)     :: rtd
+     real(c_double)     :: rhub_plq
+     integer(c_int32_t) :: lprojplqu
   end type
 
   ! mirror of dqmc_diag (same field order)
@@ -50,6 +52,7 @@ module dqmc_gpu_f
      real(c_double) :: max_dyn_error, dyn_log10_sum, dyn_count
      real(c_double) :: info, restabilized
      real(c_double) :: near_ties
+     real(c_double) :: accepted_plq, proposed_plq
   end type
 
   interface
@@ -166,6 +169,12 @@ module dqmc_gpu_f
        import; type(c_ptr), value :: h; integer(c_int), value :: c; integer(c_int32_t) :: v(*)
      end function
      integer(c_int) function dqmc_gpu_get_vconf(h, c, v) bind(C)
+       import; type(c_ptr), value :: h; integer(c_int), value :: c; integer(c_int32_t) :: v(*)
+     end function
+     integer(c_int) function dqmc_gpu_set_conf_plq(h, c, v) bind(C)
+       import; type(c_ptr), value :: h; integer(c_int), value :: c; integer(c_int32_t) :: v(*)
+     end function
+     integer(c_int) function dqmc_gpu_get_conf_plq(h, c, v) bind(C)
        import; type(c_ptr), value :: h; integer(c_int), value :: c; integer(c_int32_t) :: v(*)
      end function
      integer(c_int) function dqmc_gpu_get_trial(h, c, proj, w) bind(C)

@@ -65,6 +65,9 @@ typedef struct {
      * interlayer hopping */
     int32_t l3;
     double rtd;
+    /* rhub_plq and lprojplqu of &model_para: the plaquette field */
+    double rhub_plq;
+    int32_t lprojplqu;
 } orc_params;
 
 typedef struct orc_model orc_model;
@@ -107,13 +110,16 @@ orc_chain *orc_chain_new(const orc_model *m, int32_t seed, int draw_conf);
 void       orc_chain_free(orc_chain *c);
 void orc_chain_set_conf(orc_chain *c, const int32_t *conf);
 void orc_chain_get_conf(const orc_chain *c, int32_t *conf);
+/* plaquette field conf_plqu(lq, ltrot), plaquette fastest (rhub_plq != 0) */
+void orc_chain_set_conf_plq(orc_chain *c, const int32_t *conf);
+void orc_chain_get_conf_plq(const orc_chain *c, int32_t *conf);
 void orc_chain_set_green(orc_chain *c, const double *g);
 void orc_chain_get_green(const orc_chain *c, double *g);
 void orc_chain_set_phase(orc_chain *c, double re, double im);
 /* diag: [0]=phase.re [1]=phase.im [2]=logw.re [3]=logw.im [4]=max_wrap_error
  * [5]=max_phasediff [6]=avglog10error [7]=logcount [8]=accepted [9]=proposed
  * [10]=accepted bond-field [11]=proposed bond-field */
-void orc_chain_get_diag(const orc_chain *c, double *out);   /* 13 doubles; out[12] = near ties */
+void orc_chain_get_diag(const orc_chain *c, double *out);   /* 15 doubles; out[12] = near ties, out[13:15] plaquette accepts/proposals */
 void orc_chain_trace(orc_chain *c, int cap);
 int orc_chain_trace_count(const orc_chain *c);
 void orc_chain_trace_get(const orc_chain *c, int i, double *g, double *err);

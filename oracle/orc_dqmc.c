@@ -275,6 +275,10 @@ orc_model *orc_model_new(const orc_params *pin) {
     }
     set_hs(m);
     set_h0(m);
+    /* the plaquette field (dqmc_ft_ctrl.f90:19-23, dqmc_proj_ctrl.f90:21-24);
+     * the unequal-time pass with it is not restated */
+    m->lwrapplqu = p->rhub_plq != 0.0;
+    if (m->lwrapplqu && (p->ltau || orc_plq_setup(m) != 0)) { orc_model_free(m); return NULL; }
     m->proj = p->proj != 0;
     m->obs_mid_len = p->obs_mid_len > 0 ? p->obs_mid_len : 1;
     orc_set_vconf(m);
@@ -286,6 +290,7 @@ void orc_model_free(orc_model *m) {
     orc_latt_free(&m->L);
     free(m->iwrap_nt); free(m->wrap_step); free(m->urt); free(m->urtm1);
     free(m->exph0k); free(m->exph0kinv); free(m->urtd); free(m->urtm1d); free(m->tw1); free(m->tw2); free(m->h0mat); free(m->expar_nn);
+    orc_plq_free(m);
     free(m);
 }
 
@@ -338,6 +343,11 @@ orc_chain *orc_chain_new(const orc_model *m, int32_t seed, int draw_conf) {
     c->m = m;
     int N = m->ndim, lt = m->ltrot, nst = m->nst, lq = m->lq;
     orc_sfmt_init(&c->rng, seed);
+    if (m->lwrapplqu) {       /* dqmc_input_plqconf.f90:53-60, before the U field: nt outer, plaquette inner */
+        c->conf_plq = calloc((size_t)lq * lt, sizeof(int32_t));
+        for (size_t e = 0; e < (size_t)lq * lt; ++e)
+            c->conf_plq[e] = draw_conf ? (int32_t)ceil(orc_sfmt_stream(&c->rng) * m->plq_lcomp) : 1;
+    }
     c->conf = calloc((size_t)N * lt, sizeof(int32_t));
     if (draw_conf && m->lwrapu) {  /* dqmc_input_conf.f90:55-63: nt outer, site inner */
         for (int nt = 0; nt < lt; ++nt)
@@ -381,7 +391,7 @@ void orc_chain_free(orc_chain *c) {
     if (!c) return;
     for (int n = 0; n <= c->m->nst; ++n) { free(c->Ust[n]); free(c->Vst[n]); free(c->Dst[n]); }
     free(c->Ust); free(c->Vst); free(c->Dst); free(c->logdetQst);
-    free(c->conf); free(c->gf); free(c->gfc);
+    free(c->conf); free(c->conf_plq); free(c->gf); free(c->gfc);
     if (c->m->p.ltau) {
         for (int n = 0; n <= c->m->nst; ++n) { free(c->Ust_b[n]); free(c->Vst_b[n]); free(c->Dst_b[n]); }
         free(c->Ust_b); free(c->Vst_b); free(c->Dst_b); free(c->logdetQst_b); free(c->gf_b);
@@ -417,6 +427,14 @@ void orc_chain_get_diag(const orc_chain *c, double *out) {
     out[8] = c->acc_u; out[9] = c->prop_u;
     out[10] = c->acc_v; out[11] = c->prop_v;
     out[12] = c->near_ties;
+    out[13] = c->plq_accepted; out[14] = c->plq_proposed;
+}
+
+void orc_chain_set_conf_plq(orc_chain *c, const int32_t *conf) {
+    if (c->conf_plq) memcpy(c->conf_plq, conf, sizeof(int32_t) * (size_t)c->m->lq * c->m->ltrot);
+}
+void orc_chain_get_conf_plq(const orc_chain *c, int32_t *conf) {
+    if (c->conf_plq) memcpy(conf, c->conf_plq, sizeof(int32_t) * (size_t)c->m->lq * c->m->ltrot);
 }
 
 /* trace of (fresh G, wrap error) at the next `cap` recorded wrap checks
@@ -566,6 +584,8 @@ static void bmat_left_forward(const orc_chain *c, int nt1, int nt2, zc *g) {
             if (cb) for (int nf = 1; nf <= nnf; ++nf) h0_cb(m, ORC_LEFT_FORWARD, nf, g, N);
             else h0_fft(m, ORC_LEFT_FORWARD, g, N);
         }
+        if (m->lwrapplqu)
+            for (int i = 0; i < m->lq; ++i) orc_plq_prop(m, c->conf_plq, ORC_LEFT_FORWARD, i, nt, g, N);
         if (m->lwrapu) u_prop(m, c->conf, ORC_LEFT_FORWARD, nt, g, N);
         if (m->lwrapT) {
             if (cb) for (int nf = nnf; nf >= 1; --nf) h0_cb(m, ORC_LEFT_FORWARD, nf, g, N);
@@ -585,6 +605,8 @@ static void bmat_left_forward_hc(const orc_chain *c, int nt1, int nt2, zc *g) {
             else h0_fft(m, ORC_LEFT_FORWARD_HC, g, N);
         }
         if (m->lwrapu) u_prop(m, c->conf, ORC_LEFT_FORWARD_HC, nt, g, N);
+        if (m->lwrapplqu)
+            for (int i = m->lq - 1; i >= 0; --i) orc_plq_prop(m, c->conf_plq, ORC_LEFT_FORWARD_HC, i, nt, g, N);
         if (m->lwrapT) {
             if (cb) for (int nf = nnf; nf >= 1; --nf) h0_cb(m, ORC_LEFT_FORWARD_HC, nf, g, N);
             else h0_fft(m, ORC_LEFT_FORWARD_HC, g, N);
@@ -992,6 +1014,9 @@ static int green_equaltimebb(int N, const zc *ure, const double *dre, const zc *
 zc orc_set_phase(const orc_chain *c, zc logw) {
     const orc_model *m = c->m;
     zc ph = cexp(I * (m->p.nflr * cimag(logw)));
+    if (m->lwrapplqu)
+        for (int nt = 0; nt < m->ltrot; ++nt)
+            for (int i = 0; i < m->lq; ++i) ph *= m->plq_phase[c->conf_plq[(size_t)nt * m->lq + i] - 1];
     if (m->lwrapu && m->p.rhub > 0.0) {
         int N = m->ndim;
         for (int nt = 0; nt < m->ltrot; ++nt)
@@ -1348,6 +1373,12 @@ int orc_sweep_b0_slices(orc_chain *c, int lupdate, int lmeasure, int nslices) {
             u_prop(m, c->conf, ORC_RIGHT_FORWARD, nt, c->gf, N);
             u_prop(m, c->conf, ORC_LEFT_BACKWARD, nt, c->gf, N);
         }
+        if (m->lwrapplqu)       /* dqmc_ft_sweep_b0.f90:91-101 */
+            for (int i = m->lq - 1; i >= 0; --i) {
+                if (lupdate) orc_plq_update(c, i, nt);
+                orc_plq_prop(m, c->conf_plq, ORC_RIGHT_FORWARD, i, nt, c->gf, N);
+                orc_plq_prop(m, c->conf_plq, ORC_LEFT_BACKWARD, i, nt, c->gf, N);
+            }
         h0_half(c, ORC_LEFT_BACKWARD, ORC_RIGHT_FORWARD, 1);
         if ((m->iwrap_nt[nt - 1] > 0 || m->p.nwrap == 1) || nt == 1) {
             int n = m->iwrap_nt[nt - 1];
@@ -1375,6 +1406,8 @@ static void bmat_right_backward(const orc_chain *c, int nt1, int nt2, zc *g) {
             if (cb) for (int nf = 1; nf <= nnf; ++nf) h0_cb(m, ORC_RIGHT_BACKWARD, nf, g, N);
             else h0_fft(m, ORC_RIGHT_BACKWARD, g, N);
         }
+        if (m->lwrapplqu)
+            for (int i = 0; i < m->lq; ++i) orc_plq_prop(m, c->conf_plq, ORC_RIGHT_BACKWARD, i, nt, g, N);
         if (m->lwrapu) u_prop(m, c->conf, ORC_RIGHT_BACKWARD, nt, g, N);
         if (m->lwrapT) {
             if (cb) for (int nf = nnf; nf >= 1; --nf) h0_cb(m, ORC_RIGHT_BACKWARD, nf, g, N);
@@ -1584,6 +1617,12 @@ int orc_sweep_0b(orc_chain *c, int lupdate, int lmeasure) {
     }
     for (int nt = 1; nt <= m->ltrot; ++nt) {
         h0_half(c, ORC_LEFT_FORWARD, ORC_RIGHT_BACKWARD, 0);
+        if (m->lwrapplqu)       /* dqmc_ft_sweep_0b.f90:82-93 */
+            for (int i = 0; i < m->lq; ++i) {
+                orc_plq_prop(m, c->conf_plq, ORC_LEFT_FORWARD, i, nt, c->gf, N);
+                orc_plq_prop(m, c->conf_plq, ORC_RIGHT_BACKWARD, i, nt, c->gf, N);
+                if (lupdate) orc_plq_update(c, i, nt);
+            }
         if (m->lwrapu) {
             u_prop(m, c->conf, ORC_LEFT_FORWARD, nt, c->gf, N);
             u_prop(m, c->conf, ORC_RIGHT_BACKWARD, nt, c->gf, N);

@@ -54,6 +54,14 @@ struct orc_model {
     zc *tw1, *tw2;            /* DFT twiddles exp(-2 pi i k / l) */
     zc *h0mat;                /* [N*N] */
     zc *expar_nn;             /* [nsites][nn_nf] */
+    /* plaquette field (src/dqmc_config_plqu/dqmc_set_plqconf.f90), when rhub_plq != 0 */
+    int lwrapplqu, plq_proj, plq_lcomp;
+    double plq_alpha;
+    zc *plq_bmat, *plq_bmat_inv;   /* [lcomp][z][z] column-major blocks */
+    zc *plq_delta;                  /* [lcomp][lcomp-1][z][z]: bmat(isp) bmat(is)^-1 - I */
+    zc *plq_phase;                  /* [lcomp] */
+    zc *plq_phase_ratio;            /* [(is-1)(lcomp-1) + iflip-1] */
+    double *plq_gam_ratio;          /* gaml(isp)/gaml(is), or 1 under lprojplqu */
     /* projective path and the t-V bond field (src/dqmc_config_v/dqmc_set_conf.f90) */
     int proj, lwrapv, obs_mid_len;
     double v_alpha;
@@ -65,6 +73,8 @@ struct orc_chain {
     const orc_model *m;
     orc_sfmt rng;
     int32_t *conf;            /* [ltrot][nsites], site fastest */
+    int32_t *conf_plq;        /* [ltrot][lq] plaquette field, plaquette fastest (hconf%conf_plqu) */
+    double plq_accepted, plq_proposed;   /* main_obs(2) */
     zc *gf, *gfc;             /* N*N */
     zc **Ust, **Vst;          /* (nst+1) of N*N */
     double **Dst;
@@ -116,6 +126,12 @@ void orc_zinv(int n, zc *a);                                                 /* 
 double orc_dznrm2(int n, const zc *x, int incx);
 double orc_qr_pqmc(int rdim, int cdim, const zc *amat, zc *qmat);             /* s_zgeQR_pqmc */
 void orc_eig_he(int n, const zc *h, double *w, zc *v);                       /* s_eig_he */
+/* plaquette field (orc_plqu.c) */
+int  orc_plq_setup(orc_model *m);
+void orc_plq_free(orc_model *m);
+void orc_plq_prop(const orc_model *m, const int32_t *conf_plq, int op, int isite, int nt, zc *g, int n2);
+void orc_plq_update(orc_chain *c, int isite, int nt);
+void orc_plq_proj_update(orc_chain *c, int isite, int nt);
 
 /* shared with the projective path (orc_dqmc.c) */
 zc orc_total_ratio(const orc_model *m, zc ratio1, int is, int iflip, int isp);

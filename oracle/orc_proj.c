@@ -895,6 +895,8 @@ static void bmat_left_forward_proj(const orc_chain *c, int nt1, int nt2, zc *x) 
                 for (int nf = 1; nf <= nnf; ++nf) orc_h0_prop(m, ORC_LEFT_FORWARD, nf, (double *)x, ne);
             else orc_h0_prop(m, ORC_LEFT_FORWARD, 0, (double *)x, ne);
         }
+        if (m->lwrapplqu)      /* dqmc_proj_core.f90:89-94 */
+            for (int i = 0; i < m->lq; ++i) orc_plq_prop(m, c->conf_plq, ORC_LEFT_FORWARD, i, nt, x, ne);
         if (m->lwrapv)
             for (int nf = 1; nf <= nnf; ++nf) {
                 orc_v_prop(m, c->vconf, ORC_LEFT_FORWARD, nt, nf, 2, x, ne);
@@ -1008,6 +1010,12 @@ int orc_proj_sweep_b0_slices(orc_chain *c, int lupdate, int lmeasure, int nslice
                 if (lupdate) proj_update_bond(c, nt, nf);
                 orc_v_prop(m, c->vconf, ORC_RIGHT_FORWARD, nt, nf, 1, c->UL, ne);
                 orc_v_prop(m, c->vconf, ORC_LEFT_BACKWARD, nt, nf, 1, c->UR, ne);
+            }
+        if (m->lwrapplqu)      /* dqmc_proj_sweep_b0.f90:91-99 */
+            for (int i = m->lq - 1; i >= 0; --i) {
+                if (lupdate) orc_plq_proj_update(c, i, nt);
+                orc_plq_prop(m, c->conf_plq, ORC_RIGHT_FORWARD, i, nt, c->UL, ne);
+                orc_plq_prop(m, c->conf_plq, ORC_LEFT_BACKWARD, i, nt, c->UR, ne);
             }
         h0_pair(c, ORC_LEFT_BACKWARD, ORC_RIGHT_FORWARD, 1);
         if ((m->iwrap_nt[nt - 1] > 0 || m->p.nwrap == 1) || nt == 1) {
@@ -1134,6 +1142,12 @@ int orc_proj_sweep_0b(orc_chain *c, int lupdate, int lmeasure) {
     c->logwDV[0] = 0.0;
     for (int nt = 1; nt <= m->ltrot; ++nt) {
         h0_pair(c, ORC_LEFT_FORWARD, ORC_RIGHT_BACKWARD, 0);
+        if (m->lwrapplqu)      /* dqmc_proj_sweep_0b.f90:61-68 */
+            for (int i = 0; i < m->lq; ++i) {
+                orc_plq_prop(m, c->conf_plq, ORC_LEFT_FORWARD, i, nt, c->UR, ne);
+                orc_plq_prop(m, c->conf_plq, ORC_RIGHT_BACKWARD, i, nt, c->UL, ne);
+                if (lupdate) orc_plq_proj_update(c, i, nt);
+            }
         if (m->lwrapv)
             for (int nf = 1; nf <= nnf; ++nf) {
                 orc_v_prop(m, c->vconf, ORC_LEFT_FORWARD, nt, nf, 2, c->UR, ne);

@@ -42,6 +42,7 @@ class OrcParams(C.Structure):
         ("proj", C.c_int32), ("lprojv", C.c_int32), ("obs_mid_len", C.c_int32),
         ("ltau", C.c_int32), ("dyntau", C.c_double),
         ("l3", C.c_int32), ("rtd", C.c_double),
+        ("rhub_plq", C.c_double), ("lprojplqu", C.c_int32),
     ]
 
 
@@ -170,7 +171,7 @@ def make_params(**kw) -> OrcParams:
              mu=0.0, rhub=0.0, rv=0.0, alpha=0.2, theta=0.0, xmag=0.0, flux_x=0.0, flux_y=0.0,
              dimer=0.0, rndness=0.0, nflr=2, lproju=0, lstabilize=1, nwrap=10, nsweep=20, nbin=10,
              nublock=0, update=DELAY, kinetic=CHECKERBOARD, hs=HS_GENERAL4, proj=0, lprojv=0,
-             obs_mid_len=1, ltau=0, dyntau=0.0, l3=1, rtd=1.0)
+             obs_mid_len=1, ltau=0, dyntau=0.0, l3=1, rtd=1.0, rhub_plq=0.0, lprojplqu=0)
     d.update(kw)
     return OrcParams(**d)
 
@@ -282,11 +283,22 @@ class Chain:
         lib().orc_chain_set_phase(self._p, z.real, z.imag)
 
     def diag(self) -> dict:
-        d = np.zeros(13)
+        d = np.zeros(15)
         lib().orc_chain_get_diag(self._p, _ptr(d))
         return dict(phase=complex(d[0], d[1]), logweight=complex(d[2], d[3]), max_wrap_error=d[4],
                     max_phasediff=d[5], avglog10error=d[6], logcount=d[7], accepted=d[8], proposed=d[9],
-                    accepted_v=d[10], proposed_v=d[11], near_ties=int(d[12]))
+                    accepted_v=d[10], proposed_v=d[11], near_ties=int(d[12]), accepted_plq=d[13],
+                    proposed_plq=d[14])
+
+    def conf_plq(self) -> np.ndarray:
+        """The plaquette field conf_plqu as [ltrot][lq]."""
+        out = np.zeros((self.model.ltrot, self.model.lq), np.int32)
+        lib().orc_chain_get_conf_plq(self._p, _ptr(out))
+        return out
+
+    def set_conf_plq(self, conf: np.ndarray) -> None:
+        a = np.ascontiguousarray(conf, np.int32)
+        lib().orc_chain_set_conf_plq(self._p, _ptr(a))
 
     def trace(self, capacity: int) -> None:
         """Record (fresh G, wrap error) at the next `capacity` wrap checks."""

@@ -82,6 +82,12 @@ extern "C" int dqmc_params_derive(dqmc_params* p) {
     if (!p->proj && p->rv != 0.0) return fail(DQMC_EINVAL, "the t-V bond field (rv != 0) is supported on the projective path only");
     if (p->rv < 0.0) return fail(DQMC_EINVAL, "rv must be >= 0 (acosh(exp(dtau rv / 2)))");
     if (p->proj && (p->ne < 1 || p->ne > p->ndim)) return fail(DQMC_EINVAL, "ne out of range 1..ndim");
+    if (p->rhub_plq != 0.0) {
+        if (p->lattice != DQMC_LATT_SQUARE && p->lattice != DQMC_LATT_HONEYCOMB)
+            return fail(DQMC_EINVAL, "the plaquette field needs the square or honeycomb lattice");
+        if (p->ltau) return fail(DQMC_EINVAL, "the plaquette field is not supported with the unequal-time pass (ltau)");
+        if (p->rhub_plq < 0.0) return fail(DQMC_EINVAL, "rhub_plq must be >= 0 (sqrt(dtau rhub_plq))");
+    }
     return DQMC_OK;
 }
 
@@ -110,6 +116,11 @@ struct HostModel {
     std::vector<zc> seth0;                // the hopping matrix of the dense kinetic term (device build)
     std::vector<int> bond_i1, bond_i2;
     std::vector<int> cell_plus;           // [d][j]
+    // plaquette field (dqmc_set_plqconf.f90): z x z blocks per field value
+    bool plq_on = false;
+    int plq_lcomp = 0;
+    std::vector<zc> plq_bmat, plq_bmat_inv, plq_delta, plq_phase, plq_phase_ratio;
+    std::vector<double> plq_gam_ratio;
     ModelDev dev;                         // host copy with device pointers
     ModelDev* d_dev = nullptr;
     std::vector<void*> allocs;
@@ -423,6 +434,7 @@ static void exp2x2(double d, zc z, double s, zc* out) {
 }
 
 static void eig_herm(int n, std::vector<zc>& a, std::vector<double>& w);
+static void set_plq(HostModel& m);
 
 static int build_model(HostModel& m) {
     dqmc_params& p = m.p;
@@ -527,6 +539,7 @@ static int build_model(HostModel& m) {
             m.exph0kinv[k] = std::exp(0.5 * p.dtau * h) / (double)lq;
         }
     }
+    set_plq(m);
     // stabilisation schedule
     m.iwrap_nt.assign(p.ltrot + 1, 0);
     m.wrap_step.assign(2 * p.nst, 0);
@@ -537,6 +550,64 @@ static int build_model(HostModel& m) {
         m.wrap_step[(i - 1) * 2 + 1] = hi;
     }
     return DQMC_OK;
+}
+
+// Plaquette-field constants (src/dqmc_config_plqu/dqmc_set_plqconf.f90:1-200):
+// vstmat has 1/nn_nf on the diagonal and alpha e^{-+i theta} around the
+// plaquette (the reference's column-major listing); bmat(is) =
+// U exp(i a_is e) U^H with a_is = sqrt(dtau rhub_plq) eta(is), or
+// pi 2 nn_nf is / lcomp under lprojplqu (nu integer); the field values follow
+// the 4-component eta/gamma of dqmc_config_plqu.f90:44-52.
+static void set_plq(HostModel& m) {
+    const dqmc_params& p = m.p;
+    m.plq_on = p.rhub_plq != 0.0;
+    if (!m.plq_on) return;
+    const int z = m.z_plq, nnf = m.nn_nf;
+    const bool hc = p.lattice == DQMC_LATT_HONEYCOMB;
+    const bool lproj = p.lprojplqu && (double)(int)p.nu == p.nu;
+    m.plq_lcomp = lproj ? (hc ? nnf * (int)(p.nflr + std::fabs(p.nu)) + 1 : (int)(nnf * (0.5 * p.nflr + std::fabs(p.nu))) + 1) : 4;
+    const int lc = m.plq_lcomp;
+    const double ap = std::sqrt(p.dtau * p.rhub_plq), th = p.theta * M_PI;
+    const zc z0 = 1.0 / nnf, z1 = p.alpha * std::exp(zc(0, -th)), z1h = p.alpha * std::exp(zc(0, th)), o = 0.0;
+    std::vector<zc> v;
+    if (z == 6) v = {z0, z1, o, o, o, -z1,  z1h, z0, -z1h, o, o, o,  o, -z1, z0, z1, o, o,
+                     o, o, z1h, z0, -z1h, o,  o, o, o, -z1, z0, z1,  -z1h, o, o, o, z1h, z0};
+    else v = {z0, z1, o, -z1,  z1h, z0, -z1h, o,  o, -z1, z0, z1,  -z1h, o, z1h, z0};
+    std::vector<double> e;
+    eig_herm(z, v, e);                                  // v <- eigenvectors (columns)
+    auto eta = [](int is) {
+        const double a = std::sqrt(2.0 * (3.0 + std::sqrt(6.0))), b = std::sqrt(2.0 * (3.0 - std::sqrt(6.0)));
+        return is == 1 ? -a : is == 2 ? -b : is == 3 ? b : a;
+    };
+    auto gam = [](int is) { return (is == 1 || is == 4) ? 1.0 - std::sqrt(6.0) / 3.0 : 1.0 + std::sqrt(6.0) / 3.0; };
+    auto block = [&](double a, zc* out, double shift) {
+        for (int j = 0; j < z; ++j)
+            for (int i = 0; i < z; ++i) {
+                zc s0 = 0;
+                for (int k = 0; k < z; ++k) s0 += v[i + z * k] * std::exp(zc(0, e[k] * a)) * std::conj(v[j + z * k]);
+                out[i + z * j] = (i == j) ? s0 - shift : s0;
+            }
+    };
+    const double fac = hc ? 1.0 : 0.5;
+    m.plq_bmat.assign((size_t)lc * z * z, 0.0); m.plq_bmat_inv.assign((size_t)lc * z * z, 0.0);
+    m.plq_delta.assign((size_t)lc * (lc - 1) * z * z, 0.0); m.plq_phase.assign(lc, 0.0);
+    m.plq_phase_ratio.assign((size_t)lc * (lc - 1), 0.0); m.plq_gam_ratio.assign((size_t)lc * (lc - 1), 1.0);
+    for (int is = 1; is <= lc; ++is) {
+        const double a = lproj ? M_PI * 2.0 * nnf * is / lc : ap * eta(is);
+        block(a, &m.plq_bmat[(size_t)(is - 1) * z * z], 0.0);
+        block(-a, &m.plq_bmat_inv[(size_t)(is - 1) * z * z], 0.0);
+        m.plq_phase[is - 1] = lproj ? std::exp(zc(0, M_PI * (-2.0 * nnf * is) * fac * (p.nflr + p.nu) / lc))
+                                    : std::exp(zc(0, ap * (-eta(is)) * fac * (p.nflr + p.nu)));
+        for (int iflip = 1; iflip <= lc - 1; ++iflip) {
+            const int isp = (is + iflip - 1) % lc + 1;
+            const size_t k2 = (size_t)(is - 1) * (lc - 1) + (iflip - 1);
+            const double ad = lproj ? M_PI * (2.0 * nnf * isp - 2.0 * nnf * is) / lc : ap * (eta(isp) - eta(is));
+            block(ad, &m.plq_delta[k2 * z * z], 1.0);
+            m.plq_phase_ratio[k2] = lproj ? std::exp(zc(0, M_PI * (2.0 * nnf * is - 2.0 * nnf * isp) * fac * (p.nflr + p.nu) / lc))
+                                          : std::exp(zc(0, ap * (eta(is) - eta(isp)) * fac * (p.nflr + p.nu)));
+            m.plq_gam_ratio[k2] = lproj ? 1.0 : gam(isp) / gam(is);
+        }
+    }
 }
 
 // HS constants (src/dqmc_config_u/dqmc_set_conf.f90:1-176)
@@ -648,6 +719,21 @@ static int upload_model(HostModel& m) {
     d.ne = p.ne;
     d.lwrapv = (p.rv != 0.0);
     d.rps = d.proj ? ((d.lwrapu ? 2 * m.N : 0) + (d.lwrapv ? 2 * m.nn_lf * m.nn_nf : 0)) : 2 * m.N;
+    if (m.plq_on) {
+        // a slice's draws in the reference's order: 0b visits the plaquettes
+        // before the U (and bond) fields (dqmc_ft_sweep_0b.f90:82-119,
+        // dqmc_proj_sweep_0b.f90:61-90), b0 after them (dqmc_ft_sweep_b0.f90:70-101,
+        // dqmc_proj_sweep_b0.f90:70-99)
+        const int wu = d.lwrapu ? 2 * m.N : 0, wp = 2 * m.lq;
+        const int wv = (d.proj && d.lwrapv) ? 2 * m.nn_lf * m.nn_nf : 0;
+        d.rps = wu + wv + wp;
+        d.rw_plq[0] = 0; d.rw_u[0] = wp;
+        d.rw_u[1] = 0; d.rw_plq[1] = wu + wv;
+        d.rw_pre0 = wp;
+        d.plq = 1; d.plq_z = m.z_plq; d.plq_lcomp = m.plq_lcomp;
+        if (m.plq_lcomp > DQ_MAX_PLQ_LCOMP) return fail(DQMC_EINVAL, "too many plaquette field values");
+        for (int is = 0; is < m.plq_lcomp; ++is) d.plq_phase_angle[is] = std::arg(m.plq_phase[is]);
+    }
     if (d.lwrapv) {
         const double etal[2] = {-1.0, 1.0};
         double al = std::acosh(std::exp(p.dtau * p.rv * 0.5));
@@ -740,6 +826,13 @@ static int upload_model(HostModel& m) {
         for (int k = 0; k < p.l2; ++k) w2[k] = std::exp(zc(0, -2 * M_PI * k / p.l2));
         t = to_d2(w1); if ((rc = upload(m, t, &d.tw1))) return rc;
         t = to_d2(w2); if ((rc = upload(m, t, &d.tw2))) return rc;
+    }
+    if (m.plq_on) {
+        t = to_d2(m.plq_bmat); if ((rc = upload(m, t, &d.plq_bmat))) return rc;
+        t = to_d2(m.plq_bmat_inv); if ((rc = upload(m, t, &d.plq_bmat_inv))) return rc;
+        t = to_d2(m.plq_delta); if ((rc = upload(m, t, &d.plq_delta))) return rc;
+        t = to_d2(m.plq_phase_ratio); if ((rc = upload(m, t, &d.plq_phase_ratio))) return rc;
+        if ((rc = upload(m, m.plq_gam_ratio, &d.plq_gam_ratio))) return rc;
     }
     if ((rc = upload(m, m.cell_plus, &d.cell_plus))) return rc;
     if ((rc = upload(m, m.nnlist, &d.nnlist))) return rc;
@@ -963,11 +1056,18 @@ static void trial_hamiltonian(const HostModel& m, HostSfmt& rng, std::vector<zc>
     for (int i = 0; i < N; ++i) H[i + (size_t)i * N] -= p.mu;
 }
 
-// the fresh-start draws of one chain, in the reference's order: U field
+// the fresh-start draws of one chain, in the reference's order (dqmc_start,
+// src/dqmc_ft_ctrl.f90:9-45): plaquette field (hconf%input_plqconf), U field
 // (uconf%input_conf), bond field (vconf%input_conf), then the trial hopping
 static void draw_fields(const HostModel& m, HostSfmt& rng, int draw_conf, std::vector<int32_t>& conf,
-                        std::vector<int32_t>& vconf) {
+                        std::vector<int32_t>& vconf, std::vector<int32_t>* conf_plq = nullptr) {
     int N = m.N, lt = m.p.ltrot, nnf = m.nn_nf;
+    if (m.plq_on) {          // dqmc_input_plqconf.f90:53-60: nt outer, plaquette inner
+        std::vector<int32_t> cp((size_t)lt * m.lq, 1);
+        if (draw_conf)
+            for (size_t e = 0; e < cp.size(); ++e) cp[e] = (int32_t)std::ceil(rng.stream() * m.plq_lcomp);
+        if (conf_plq) *conf_plq = std::move(cp);
+    }
     conf.assign((size_t)lt * N, 1);
     if (draw_conf && m.p.rhub != 0.0)
         for (size_t e = 0; e < conf.size(); ++e) conf[e] = (int32_t)std::ceil(rng.stream() * m.lcomp);
@@ -1276,6 +1376,7 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
         d.vecs = (double*)dalloc(h, (size_t)8 * N * sizeof(double));
         d.perm = (int*)dalloc(h, (size_t)N * sizeof(int));
         d.conf = (int32_t*)dalloc(h, (size_t)lt * N * sizeof(int32_t));
+        if (m->plq_on) d.conf_plq = (int32_t*)dalloc(h, (size_t)lt * m->lq * sizeof(int32_t));
         d.sfmt = (uint32_t*)dalloc(h, 625 * sizeof(uint32_t));
         d.rnd = (uint32_t*)dalloc(h, (size_t)lt * std::max(2 * N, m->dev.rps) * sizeof(uint32_t));
         d.bins = (double2*)dalloc(h, (size_t)(10 + 20 * m->lq + 4) * z);
@@ -1291,14 +1392,18 @@ extern "C" int dqmc_gpu_create(const dqmc_params* params, int n_params, int n_ch
         // generator state and fresh-start fields, drawn in the reference's order
         HostSfmt rng;
         sfmt_seed(rng.st, seeds ? seeds[c] : 0);
-        std::vector<int32_t> conf, vconf;
-        draw_fields(*m, rng, draw_conf, conf, vconf);
+        std::vector<int32_t> conf, vconf, conf_plq;
+        draw_fields(*m, rng, draw_conf, conf, vconf, &conf_plq);
         if (proj) {
             trial_hamiltonian(*m, rng, trial_H[c]);
         }
         cudaMemcpy(d.sfmt, rng.st, 625 * sizeof(uint32_t), cudaMemcpyHostToDevice);
         cudaMemcpy(d.conf, conf.data(), conf.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
         if (!vconf.empty()) cudaMemcpy(d.vconf, vconf.data(), vconf.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+        if (m->plq_on) {
+            if (!d.conf_plq) { dqmc_gpu_destroy(h); return fail(DQMC_ENOMEM, "device allocation failed"); }
+            cudaMemcpy(d.conf_plq, conf_plq.data(), conf_plq.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+        }
         double stats[ST_COUNT] = {0};
         stats[ST_PHASE_RE] = 1.0;
         cudaMemcpy(d.stats, stats, sizeof(stats), cudaMemcpyHostToDevice);
@@ -1428,7 +1533,11 @@ static int launch_bmat(dqmc_handle* h, int mat_id, int nt1, int nt2, int hc) {
         const int which = hc ? PW_CONJ : PW_FWD;
         PropProg sl; sl.n = 0;
         prog_k(m, sl, which, 0);
+        // plaquettes ascending before the U field (Bmat_left_forward), descending
+        // after it with bmat^H = bmat_inv (Bmat_left_forward_hc)
+        if (m.plq_on && !hc) prog_add(sl, PK_PLQ, PW_FWD, 0, nt);
         prog_v(m, sl, which, nt);
+        if (m.plq_on && hc) prog_add(sl, PK_PLQ, PW_INV, 1, nt);
         prog_k(m, sl, which, 1);
         if (p.n + sl.n > DQ_MAX_PROG) {
             int rc = launch_prog(h, mat_id, p, 0); if (rc) return rc;
@@ -1621,6 +1730,7 @@ static void proj_bmat(dqmc_handle* h, ProjPass& pp, int nt1, int nt2) {
     const HostModel& m = *h->models[0];
     for (int nt = nt2; nt <= nt1; ++nt) {
         pk(h, pp, pp.r, PW_FWD, 0);
+        if (m.plq_on) padd(h, pp, pp.r, PK_PLQ, PW_FWD, 0, nt);     // dqmc_proj_core.f90:89-94
         if (m.p.rv != 0.0)
             for (int nf = 1; nf <= m.nn_nf; ++nf) {
                 padd(h, pp, pp.r, PK_VMIX, 0, nf, nt);
@@ -1662,7 +1772,7 @@ static void enqueue_proj_b0(dqmc_handle* h, int lupdate, int lmeasure) {
     bool lu = m.p.rhub != 0.0, lv = m.p.rv != 0.0;
     launch_tall_copy(h->d_chains, h->nch, PMAT_ULT, PMAT_PROJLC, h->st);
     launch_tall_copy(h->d_chains, h->nch, PMAT_PST0 + 0, PMAT_PROJR, h->st);
-    if (lupdate && (lu || lv)) launch_sfmt(h->d_chains, h->nch, lt, h->st);
+    if (lupdate && (lu || lv || m.plq_on)) launch_sfmt(h->d_chains, h->nch, lt, h->st);
     tmark(h, DQMC_PROF_OTHER);
     ProjPass pp;
     for (int nt = lt; nt >= 1; --nt) {
@@ -1685,6 +1795,11 @@ static void enqueue_proj_b0(dqmc_handle* h, int lupdate, int lmeasure) {
                 padd(h, pp, pp.r, PK_VSCALE, PW_INV, nf, nt);    // left_backward, nflag 1
                 padd(h, pp, pp.r, PK_VMIX, 0, nf, nt);
             }
+        if (m.plq_on) {                 // plaquettes: update, then props, descending
+            pflush(h, pp);
+            launch_plq_proj_slice(h->d_chains, h->nch, h->maxNe, nt, visit, 1, lupdate, h->st);
+            tmark(h, DQMC_PROF_UPDATE);
+        }
         pk(h, pp, pp.r, PW_INV, 1);
         pk(h, pp, pp.l, PW_FWD, 1);
         if ((m.iwrap_nt[nt - 1] > 0 || m.p.nwrap == 1) || nt == 1) { pflush(h, pp); stab_proj_b0(h, m.iwrap_nt[nt - 1]); }
@@ -1764,13 +1879,18 @@ static void enqueue_proj_0b(dqmc_handle* h, int lupdate, int lmeasure) {
     bool lu = m.p.rhub != 0.0, lv = m.p.rv != 0.0;
     launch_tall_copy(h->d_chains, h->nch, PMAT_UR, PMAT_PROJR, h->st);
     launch_tall_copy(h->d_chains, h->nch, PMAT_PST0 + nst, PMAT_PROJLC, h->st);
-    if (lupdate && (lu || lv)) launch_sfmt(h->d_chains, h->nch, lt, h->st);
+    if (lupdate && (lu || lv || m.plq_on)) launch_sfmt(h->d_chains, h->nch, lt, h->st);
     tmark(h, DQMC_PROF_OTHER);
     ProjPass pp;
     for (int nt = 1; nt <= lt; ++nt) {
         int visit = nt - 1;
         pk(h, pp, pp.r, PW_FWD, 0);     // h0 left_forward on UR
         pk(h, pp, pp.l, PW_INV, 0);     // h0 right_backward on UL
+        if (m.plq_on) {                 // plaquettes: props, then update, ascending
+            pflush(h, pp);
+            launch_plq_proj_slice(h->d_chains, h->nch, h->maxNe, nt, visit, 0, lupdate, h->st);
+            tmark(h, DQMC_PROF_UPDATE);
+        }
         if (lv)
             for (int nf = 1; nf <= nnf; ++nf) {
                 padd(h, pp, pp.r, PK_VMIX, 0, nf, nt);           // left_forward, nflag 2
@@ -1885,7 +2005,8 @@ static void enqueue_b0(dqmc_handle* h, int lupdate, int lmeasure) {
     const HostModel& m = *h->models[0];
     int lt = h->ltrot;
     launch_stack_identity(h->d_chains, h->nch, h->nst, h->st);
-    if (lupdate && m.p.rhub != 0.0) launch_sfmt(h->d_chains, h->nch, lt, h->st);
+    const bool plq = m.plq_on;
+    if (lupdate && (m.p.rhub != 0.0 || plq)) launch_sfmt(h->d_chains, h->nch, lt, h->st);
     tmark(h, DQMC_PROF_OTHER);
     for (int nt = lt; nt >= 1; --nt) {
         int visit = lt - nt;
@@ -1897,11 +2018,21 @@ static void enqueue_b0(dqmc_handle* h, int lupdate, int lmeasure) {
         tmark(h, DQMC_PROF_PROP_L);
         launch_prog(h, MAT_G, pr, 1);
         tmark(h, DQMC_PROF_PROP_R);
-        if (lupdate && m.p.rhub != 0.0) { launch_update(h->d_chains, h->nch, nt, visit, h->st); tmark(h, DQMC_PROF_UPDATE); }
+        if (lupdate && m.p.rhub != 0.0) { launch_update(h->d_chains, h->nch, nt, visit, h->st, 0, 1); tmark(h, DQMC_PROF_UPDATE); }
         pl.n = 0; pr.n = 0;
         prog_v(m, pl, PW_INV, nt);         // u left_backward
-        prog_k(m, pl, PW_INV, 1);          // h0 left_backward, nf = nnf..1
         prog_v(m, pr, PW_FWD, nt);         // u right_forward
+        if (plq) {
+            // the plaquettes (update, then props, descending) between the U field
+            // and the kinetic half step (dqmc_ft_sweep_b0.f90:91-101)
+            launch_prog(h, MAT_G, pl, 0);
+            launch_prog(h, MAT_G, pr, 1);
+            tmark(h, DQMC_PROF_PROP_L);
+            launch_plq_slice(h->d_chains, h->nch, h->maxN, nt, visit, 1, lupdate, h->st);
+            tmark(h, DQMC_PROF_UPDATE);
+            pl.n = 0; pr.n = 0;
+        }
+        prog_k(m, pl, PW_INV, 1);          // h0 left_backward, nf = nnf..1
         prog_k(m, pr, PW_FWD, 1);
         launch_prog(h, MAT_G, pl, 0);
         tmark(h, DQMC_PROF_PROP_L);
@@ -1915,14 +2046,25 @@ static void enqueue_0b(dqmc_handle* h, int lupdate, int lmeasure) {
     const HostModel& m = *h->models[0];
     int lt = h->ltrot;
     launch_stack_identity(h->d_chains, h->nch, 0, h->st);
-    if (lupdate && m.p.rhub != 0.0) launch_sfmt(h->d_chains, h->nch, lt, h->st);
+    const bool plq = m.plq_on;
+    if (lupdate && (m.p.rhub != 0.0 || plq)) launch_sfmt(h->d_chains, h->nch, lt, h->st);
     tmark(h, DQMC_PROF_OTHER);
     for (int nt = 1; nt <= lt; ++nt) {
         int visit = nt - 1;
         PropProg pl; pl.n = 0; PropProg pr; pr.n = 0;
         prog_k(m, pl, PW_FWD, 0);          // left_forward, nf = 1..nnf
-        prog_v(m, pl, PW_FWD, nt);         // u left_forward
         prog_k(m, pr, PW_INV, 0);          // right_backward
+        if (plq) {
+            // the plaquettes (props, then update, ascending) between the kinetic
+            // half step and the U field (dqmc_ft_sweep_0b.f90:82-93)
+            launch_prog(h, MAT_G, pl, 0);
+            launch_prog(h, MAT_G, pr, 1);
+            tmark(h, DQMC_PROF_PROP_L);
+            launch_plq_slice(h->d_chains, h->nch, h->maxN, nt, visit, 0, lupdate, h->st);
+            tmark(h, DQMC_PROF_UPDATE);
+            pl.n = 0; pr.n = 0;
+        }
+        prog_v(m, pl, PW_FWD, nt);         // u left_forward
         prog_v(m, pr, PW_INV, nt);         // u right_backward
         launch_prog(h, MAT_G, pl, 0);
         tmark(h, DQMC_PROF_PROP_L);
@@ -2400,6 +2542,7 @@ extern "C" int dqmc_gpu_get_diag(dqmc_handle* h, int chain, dqmc_diag* out) {
     out->info = st[ST_INFO];
     out->restabilized = h->n_restab;
     out->near_ties = st[ST_NEAR_TIE];
+    out->accepted_plq = st[ST_ACCP]; out->proposed_plq = st[ST_PROPP];
     return DQMC_OK;
 }
 
@@ -2409,7 +2552,7 @@ extern "C" int dqmc_gpu_reset_diag(dqmc_handle* h) {
         double st[ST_COUNT];
         CK(copy_sync(h->st, st, h->chains[c].dev.stats, sizeof(st), cudaMemcpyDeviceToHost));
         st[ST_MAX_WRAP] = st[ST_MAX_PHASEDIFF] = st[ST_AVGLOG10] = st[ST_LOGCOUNT] = st[ST_AVGEXPPD] = 0.0;
-        st[ST_ACC] = st[ST_PROP] = st[ST_ACCV] = st[ST_PROPV] = 0.0;
+        st[ST_ACC] = st[ST_PROP] = st[ST_ACCV] = st[ST_PROPV] = st[ST_ACCP] = st[ST_PROPP] = 0.0;
         st[ST_BLK_PROP] = st[ST_BLK_S1] = st[ST_BLK_ACC] = st[ST_BLK_SUMLR] = 0.0;
         st[ST_BLK_ERR1] = st[ST_BLK_ERR0] = 0.0;
         st[ST_MAX_DYN] = st[ST_DYN_LOG10] = st[ST_DYN_COUNT] = 0.0;
@@ -2494,8 +2637,16 @@ extern "C" int dqmc_gpu_update(dqmc_handle* h, int nt) {
     if (!h) return fail(DQMC_EINVAL, "null handle");
     if (h->proj) return fail(DQMC_ESTATE, "projective handle: use dqmc_gpu_proj_update");
     if (nt < 1 || nt > h->ltrot) return fail(DQMC_EINVAL, "nt out of range");
-    launch_sfmt(h->d_chains, h->nch, 1, h->st);
-    launch_update(h->d_chains, h->nch, nt, 0, h->st);
+    const HostModel& m0 = *h->models[0];
+    if (m0.plq_on) {
+        // exactly the 2 N draws of uconf%update (the slice layout of a sweep also
+        // holds the plaquette words); the U words start the b0 layout
+        launch_sfmt(h->d_chains, h->nch, -2 * m0.N, h->st);
+        launch_update(h->d_chains, h->nch, nt, 0, h->st, 0, 1);
+    } else {
+        launch_sfmt(h->d_chains, h->nch, 1, h->st);
+        launch_update(h->d_chains, h->nch, nt, 0, h->st);
+    }
     CK(cudaStreamSynchronize(h->st));
     CK(cudaGetLastError());
     return DQMC_OK;
@@ -2648,6 +2799,31 @@ extern "C" int dqmc_gpu_get_vconf(dqmc_handle* h, int chain, int32_t* v) {
     if (!d.vconf) return fail(DQMC_ESTATE, "no bond field (rv == 0)");
     size_t n = (size_t)h->ltrot * h->models[h->chains[chain].model]->nn_nf * d.N;
     CK(copy_sync(h->st, v, d.vconf, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    return DQMC_OK;
+}
+
+// plaquette field conf_plqu of one chain (dqmc_input_plqconf / dqmc_output_plqconf)
+extern "C" int dqmc_gpu_set_conf_plq(dqmc_handle* h, int chain, const int32_t* v) {
+    int rc = chk_chain(h, chain); if (rc) return rc;
+    if (!v) return fail(DQMC_EINVAL, "null field");
+    const ChainDev& d = h->chains[chain].dev;
+    const HostModel& m = *h->models[h->chains[chain].model];
+    if (!d.conf_plq) return fail(DQMC_ESTATE, "no plaquette field (rhub_plq == 0)");
+    const size_t n = (size_t)h->ltrot * m.lq;
+    for (size_t e = 0; e < n; ++e)
+        if (v[e] < 1 || v[e] > m.plq_lcomp) return fail(DQMC_EINVAL, "plaquette field value out of range 1..lcomp");
+    CK(copy_sync(h->st, d.conf_plq, v, n * sizeof(int32_t), cudaMemcpyHostToDevice));
+    h->started = 0;
+    return DQMC_OK;
+}
+
+extern "C" int dqmc_gpu_get_conf_plq(dqmc_handle* h, int chain, int32_t* v) {
+    int rc = chk_chain(h, chain); if (rc) return rc;
+    if (!v) return fail(DQMC_EINVAL, "null field");
+    const ChainDev& d = h->chains[chain].dev;
+    if (!d.conf_plq) return fail(DQMC_ESTATE, "no plaquette field (rhub_plq == 0)");
+    const size_t n = (size_t)h->ltrot * h->models[h->chains[chain].model]->lq;
+    CK(copy_sync(h->st, v, d.conf_plq, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
     return DQMC_OK;
 }
 

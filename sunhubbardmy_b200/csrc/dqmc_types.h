@@ -5,6 +5,7 @@
 
 #define DQ_MAX_LCOMP 4
 #define DQ_MAX_NNF 8      // bond families
+#define DQ_MAX_PLQ_LCOMP 8  // field values of the plaquette field
 #define DQ_MAX_PROG 256   // propagation ops per pass (nwrap slices x ops per slice)
 
 // Model tables for one lattice/parameter set (read-only during a sweep).
@@ -17,6 +18,16 @@ struct ModelDev {
     int chain;                 // 1D chain: the energy terms of equaltime_measure1d.f90
     int cubic, l3;             // cubic or r_cubic lattice (l3 = 1 otherwise): the observables of equaltime_measure3d.f90
     int cb_split[DQ_MAX_NNF];  // bonds of each family's first disjoint phase (the device bond order)
+    // plaquette field (src/dqmc_config_plqu/dqmc_set_plqconf.f90): z x z blocks per field value
+    int plq, plq_z, plq_lcomp;
+    int rw_u[2], rw_plq[2];    // offsets of the U-field and plaquette words in a slice's draws (0: 0b, 1: b0)
+    int rw_pre0;               // words ahead of the U and bond fields' in the 0b layout (the plaquettes')
+    const double2* plq_bmat;   // [lcomp][z*z] column-major
+    const double2* plq_bmat_inv;
+    const double2* plq_delta;  // [(is-1)(lcomp-1) + iflip-1][z*z]: bmat(isp) bmat(is)^-1 - I
+    const double2* plq_phase_ratio;   // [(is-1)(lcomp-1) + iflip-1]
+    const double* plq_gam_ratio;
+    double plq_phase_angle[DQ_MAX_PLQ_LCOMP];   // arg(phase(is)) for set_phase
     // HS constants (src/dqmc_config_u/dqmc_set_conf.f90)
     double2 bmat[DQ_MAX_LCOMP], bmat_inv[DQ_MAX_LCOMP], phase[DQ_MAX_LCOMP];
     double2 delta[DQ_MAX_LCOMP * (DQ_MAX_LCOMP - 1)];        // [(is-1)*(lc-1) + iflip-1]
@@ -70,6 +81,7 @@ struct ChainDev {
     double* vecs;              // 8 x N real scratch (norms, dmax/dmin)
     int* perm;                 // N
     int32_t* conf;             // ltrot x N (site fastest), values 1..lcomp
+    int32_t* conf_plq;         // ltrot x lq (plaquette fastest): the plaquette field, or null
     uint32_t* sfmt;            // 624 words + index
     uint32_t* rnd;             // random words for the current half sweep
     double2* bins;             // measurement bins (layout: see kern_measure.cu)
@@ -142,11 +154,13 @@ enum {
     ST_DYN_COUNT,              // ... and the number of checks (logdyncount)
     ST_GINFO,                  // DQ_FAIL_SINGULAR of the latest Green's-function computation (overwritten by each)
     ST_NEAR_TIE,               // accept tests decided with | |ratio| - r | < DQ_NEAR_TIE
+    ST_ACCP, ST_PROPP,         // plaquette field: accepted flips, proposals
     ST_COUNT = 40
 };
 
 // propagation op encoding: kind | which << 4 | nf << 8 | nt << 16
-enum { PK_CB = 1, PK_FFT = 2, PK_DIAG = 3, PK_VMIX = 4, PK_VSCALE = 5, PK_DENSE = 6 };
+enum { PK_CB = 1, PK_FFT = 2, PK_DIAG = 3, PK_VMIX = 4, PK_VSCALE = 5, PK_DENSE = 6,
+       PK_PLQ = 7 };    // PK_PLQ: every plaquette's block in turn, nf = 0 ascending, 1 descending
 enum { PW_FWD = 0, PW_INV = 1, PW_CONJ = 2 };   // urt/bmat/exph0k, urtm1/bmat_inv/exph0kinv, conj(...)
 struct PropProg {
     int n;

@@ -1,0 +1,380 @@
+// The plaquette Hubbard-Stratonovich field (hconf): one field per plaquette and
+// time slice whose factor is a dense z x z block on the plaquette's z sites
+// (z = 4 square, 6 honeycomb).
+//
+// Reference: src/dqmc_config_plqu/ -- dqmc_left_forward_prop.f90 and its four
+// siblings (the block on a plaquette's rows or columns) and
+// dqmc_update_plqu.f90 (the flip of one plaquette: ratio det(I + V U) from a
+// z x z matrix, G <- G - G(:,P) S V on acceptance), called plaquette by
+// plaquette in dqmc_ft_sweep_0b.f90:82-93 (ascending: props, then update) and
+// dqmc_ft_sweep_b0.f90:91-101 (descending: update, then props).
+//
+// Plaquettes share sites, so the blocks of one slice are applied one after the
+// other.  In a B product (the PK_PLQ op of kern_prop.cu) every vector of the
+// pass walks the plaquettes sequentially in its own thread; in the sweep,
+// k_plq_slice runs the interleaved props and updates of one slice for one
+// chain per CTA.
+#include "chain_access.cuh"
+#include "kernels.h"
+
+#define PLQ_NT 256
+#define PLQ_ZMAX 6
+
+DQ_DEV double plq_stream(uint32_t u) { return ((double)u + 0.5) * (1.0 / 4294967296.0); }
+
+// rows P of X (ld rows, ncol columns) <- M rows P, or M^T rows P when trans
+// (M z x z, column-major)
+DQ_DEV void plq_rows(double2* X, int ld, int ncol, const int* pc, int z, const double2* M, bool trans = false) {
+    for (int col = threadIdx.x; col < ncol; col += blockDim.x) {
+        double2 a[PLQ_ZMAX];
+#pragma unroll
+        for (int i = 0; i < PLQ_ZMAX; ++i) if (i < z) a[i] = X[(size_t)pc[i] + (size_t)ld * col];
+#pragma unroll
+        for (int i = 0; i < PLQ_ZMAX; ++i) {
+            if (i >= z) break;
+            double2 s = cmk(0, 0);
+#pragma unroll
+            for (int j = 0; j < PLQ_ZMAX; ++j) if (j < z) s = cfma(trans ? M[j + z * i] : M[i + z * j], a[j], s);
+            X[(size_t)pc[i] + (size_t)ld * col] = s;
+        }
+    }
+    __syncthreads();
+}
+
+// columns P of G <- columns P M
+DQ_DEV void plq_cols(double2* G, int N, const int* pc, int z, const double2* M) {
+    for (int r = threadIdx.x; r < N; r += blockDim.x) {
+        double2 a[PLQ_ZMAX];
+#pragma unroll
+        for (int i = 0; i < PLQ_ZMAX; ++i) if (i < z) a[i] = G[MIDX(r, pc[i], N)];
+#pragma unroll
+        for (int i = 0; i < PLQ_ZMAX; ++i) {
+            if (i >= z) break;
+            double2 s = cmk(0, 0);
+#pragma unroll
+            for (int j = 0; j < PLQ_ZMAX; ++j) if (j < z) s = cfma(a[j], M[j + z * i], s);
+            G[MIDX(r, pc[i], N)] = s;
+        }
+    }
+    __syncthreads();
+}
+
+// In-place inverse of the n x n (column-major) matrix a by Gauss-Jordan
+// elimination with partial pivoting; returns det(a).
+DQ_DEV double2 small_inv_det(double2* a, int n) {
+    int piv[PLQ_ZMAX];
+    double2 det = cmk(1, 0);
+    for (int k = 0; k < n; ++k) {
+        int pr = k;
+        double best = cabsd(a[k + n * k]);
+        for (int i = k + 1; i < n; ++i) {
+            const double v = cabsd(a[i + n * k]);
+            if (v > best) { best = v; pr = i; }
+        }
+        piv[k] = pr;
+        if (pr != k) {
+            for (int j = 0; j < n; ++j) { const double2 t = a[k + n * j]; a[k + n * j] = a[pr + n * j]; a[pr + n * j] = t; }
+            det = cmk(-det.x, -det.y);
+        }
+        const double2 d = a[k + n * k];
+        det = cmul(det, d);
+        const double2 di = cdiv(cmk(1, 0), d);
+        a[k + n * k] = cmk(1, 0);
+        for (int j = 0; j < n; ++j) a[k + n * j] = cmul(a[k + n * j], di);
+        for (int i = 0; i < n; ++i) {
+            if (i == k) continue;
+            const double2 f = a[i + n * k];
+            a[i + n * k] = cmk(0, 0);
+            for (int j = 0; j < n; ++j) a[i + n * j] = csub(a[i + n * j], cmul(f, a[k + n * j]));
+        }
+    }
+    for (int k = n - 1; k >= 0; --k)          // undo the row swaps as column swaps
+        if (piv[k] != k)
+            for (int i = 0; i < n; ++i) { const double2 t = a[i + n * k]; a[i + n * k] = a[i + n * piv[k]]; a[i + n * piv[k]] = t; }
+    return det;
+}
+
+// One slice of plaquette props and updates for one chain (one CTA per chain).
+// dir = 0: the 0b order, plaquettes ascending, bmat on the rows and bmat_inv
+// on the columns, then the update; dir = 1: the b0 order, plaquettes
+// descending, the update, then bmat on the columns and bmat_inv on the rows.
+// The k-th visited plaquette uses the random words 2k, 2k + 1 of the slice's
+// plaquette draws (iflip, then the accept test).
+__global__ void __launch_bounds__(PLQ_NT) k_plq_slice(const ChainDev* __restrict__ chains, int nt, int visit, int dir,
+                                                     int lupdate) {
+    extern __shared__ double2 wsm[];           // S V, z x N (row a at wsm + a N)
+    __shared__ double2 s_mat[PLQ_ZMAX * PLQ_ZMAX];
+    __shared__ int s_acc;
+    const ChainDev& c = chains[blockIdx.x];
+    const ModelDev& md = *c.md;
+    if (!md.plq) return;
+    const int N = c.N, z = md.plq_z, lq = md.lq, lc = md.plq_lcomp, tid = threadIdx.x;
+    double2* G = c.G;
+    int32_t* cf = c.conf_plq + (size_t)(nt - 1) * lq;
+    const uint32_t* rw = c.rnd + (size_t)visit * md.rps + md.rw_plq[dir];
+    double2 ph = cmk(c.stats[ST_PHASE_RE], c.stats[ST_PHASE_IM]);
+    double acc = 0.0, nties = 0.0;
+    for (int k = 0; k < lq; ++k) {
+        const int p = dir ? lq - 1 - k : k;
+        const int* pc = md.plq_cord + p * z;
+        if (!dir) {
+            plq_rows(G, N, N, pc, z, md.plq_bmat + (size_t)(cf[p] - 1) * z * z);
+            plq_cols(G, N, pc, z, md.plq_bmat_inv + (size_t)(cf[p] - 1) * z * z);
+        }
+        if (lupdate) {
+            if (tid == 0) {
+                const int is = cf[p];
+                const int iflip = (int)ceil(plq_stream(rw[2 * k]) * (lc - 1));
+                const int isp = (is + iflip - 1) % lc + 1;
+                const int k2 = (is - 1) * (lc - 1) + (iflip - 1);
+                const double2* dl = md.plq_delta + (size_t)k2 * z * z;
+                double2 vpp[PLQ_ZMAX * PLQ_ZMAX], vu[PLQ_ZMAX * PLQ_ZMAX];
+                for (int a = 0; a < z; ++a)
+                    for (int b = 0; b < z; ++b) {
+                        const double2 g = G[MIDX(pc[a], pc[b], N)];
+                        vpp[a + z * b] = cmk((a == b ? 1.0 : 0.0) - g.x, -g.y);
+                    }
+                for (int a = 0; a < z; ++a)            // vukmat = I + V(:, P) delta
+                    for (int b = 0; b < z; ++b) {
+                        double2 s = cmk(a == b ? 1.0 : 0.0, 0.0);
+                        for (int q = 0; q < z; ++q) s = cfma(vpp[a + z * q], dl[q + z * b], s);
+                        vu[a + z * b] = s;
+                    }
+                const double2 ratio1 = small_inv_det(vu, z);
+                for (int a = 0; a < z; ++a)            // smat = delta (I + V U)^-1
+                    for (int b = 0; b < z; ++b) {
+                        double2 s = cmk(0, 0);
+                        for (int q = 0; q < z; ++q) s = cfma(dl[a + z * q], vu[q + z * b], s);
+                        s_mat[a + z * b] = s;
+                    }
+                double2 rt = ratio1;
+                for (int f = 1; f < md.nflr; ++f) rt = cmul(rt, ratio1);
+                rt = cmul(cscale(rt, md.plq_gam_ratio[k2]), md.plq_phase_ratio[k2]);
+                const double ra = fabs(cmul(rt, ph).x / ph.x), r = plq_stream(rw[2 * k + 1]);
+                if (fabs(ra - r) < DQ_NEAR_TIE) nties += 1.0;
+                s_acc = ra > r;
+                if (s_acc) {
+                    acc += 1.0;
+                    ph = cscale(cmul(ph, rt), 1.0 / sqrt(cmulc(rt, rt).x));
+                    cf[p] = isp;
+                }
+            }
+            __syncthreads();
+            if (s_acc) {
+                // W = smat V, V(q, col) = delta(P_q, col) - G(P_q, col)
+                for (int col = tid; col < N; col += blockDim.x) {
+                    double2 v[PLQ_ZMAX];
+#pragma unroll
+                    for (int q = 0; q < PLQ_ZMAX; ++q)
+                        if (q < z) {
+                            const double2 g = G[MIDX(pc[q], col, N)];
+                            v[q] = cmk((pc[q] == col ? 1.0 : 0.0) - g.x, -g.y);
+                        }
+                    for (int a = 0; a < z; ++a) {
+                        double2 s = cmk(0, 0);
+#pragma unroll
+                        for (int q = 0; q < PLQ_ZMAX; ++q) if (q < z) s = cfma(s_mat[a + z * q], v[q], s);
+                        wsm[(size_t)a * N + col] = s;
+                    }
+                }
+                __syncthreads();
+                // G <- G - G(:, P) W, a thread owning whole rows
+                for (int r = tid; r < N; r += blockDim.x) {
+                    double2 gp[PLQ_ZMAX];
+#pragma unroll
+                    for (int a = 0; a < PLQ_ZMAX; ++a) if (a < z) gp[a] = G[MIDX(r, pc[a], N)];
+                    for (int col = 0; col < N; ++col) {
+                        double2 s = cmk(0, 0);
+#pragma unroll
+                        for (int a = 0; a < PLQ_ZMAX; ++a) if (a < z) s = cfma(gp[a], wsm[(size_t)a * N + col], s);
+                        G[MIDX(r, col, N)] = csub(G[MIDX(r, col, N)], s);
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        if (dir) {
+            plq_cols(G, N, pc, z, md.plq_bmat + (size_t)(cf[p] - 1) * z * z);
+            plq_rows(G, N, N, pc, z, md.plq_bmat_inv + (size_t)(cf[p] - 1) * z * z);
+        }
+    }
+    if (tid == 0) {
+        c.stats[ST_PHASE_RE] = ph.x;
+        c.stats[ST_PHASE_IM] = ph.y;
+        if (lupdate) {
+            c.stats[ST_ACCP] += acc;
+            c.stats[ST_PROPP] += lq;
+            c.stats[ST_NEAR_TIE] += nties;
+        }
+    }
+}
+
+// One slice of plaquette props and updates on the projective path (one CTA
+// per walker): UR (N x ne), UL stored as UL^T (N x ne) and ULRINV (ne x ne).
+// dir = 0 (dqmc_proj_sweep_0b.f90:61-68): ascending, UR(P,:) <- bmat UR(P,:),
+// UL(:,P) <- UL(:,P) bmat_inv, then the update; dir = 1
+// (dqmc_proj_sweep_b0.f90:91-99): descending, the update, then
+// UL(:,P) <- UL(:,P) bmat and UR(P,:) <- bmat_inv UR(P,:).  The update
+// (dqmc_proj_update_plqu.f90): vkt = delta UR(P,:), vk = vkt ULRINV, ratio
+// det(I + vk UL(:,P)); on acceptance UR(P,:) += vkt and
+// ULRINV -= ULRINV UL(:,P) (I + vk UL(:,P))^-1 vk.
+__global__ void __launch_bounds__(PLQ_NT) k_plq_proj_slice(const ChainDev* __restrict__ chains, int nt, int visit,
+                                                          int dir, int lupdate) {
+    extern __shared__ double2 psm[];          // vkt [z][ne], vk [z][ne], lru [z][ne]
+    __shared__ double2 s_mat[PLQ_ZMAX * PLQ_ZMAX];
+    __shared__ int s_acc;
+    const ChainDev& c = chains[blockIdx.x];
+    const ModelDev& md = *c.md;
+    if (!md.plq) return;
+    const int N = c.N, ne = md.ne, z = md.plq_z, lq = md.lq, lc = md.plq_lcomp, tid = threadIdx.x;
+    double2 *UR = c.UR, *ULT = c.ULT, *R = c.ULRINV;
+    double2 *vkt = psm, *vk = psm + (size_t)z * ne, *lru = psm + (size_t)2 * z * ne;
+    int32_t* cf = c.conf_plq + (size_t)(nt - 1) * lq;
+    const uint32_t* rw = c.rnd + (size_t)visit * md.rps + md.rw_plq[dir];
+    double2 ph = cmk(c.stats[ST_PHASE_RE], c.stats[ST_PHASE_IM]);
+    double acc = 0.0, nties = 0.0;
+    for (int k = 0; k < lq; ++k) {
+        const int p = dir ? lq - 1 - k : k;
+        const int* pc = md.plq_cord + p * z;
+        if (!dir) {
+            plq_rows(UR, N, ne, pc, z, md.plq_bmat + (size_t)(cf[p] - 1) * z * z);
+            plq_rows(ULT, N, ne, pc, z, md.plq_bmat_inv + (size_t)(cf[p] - 1) * z * z, true);
+        }
+        if (lupdate) {
+            const int is = cf[p];
+            const int iflip = (int)ceil(plq_stream(rw[2 * k]) * (lc - 1));
+            const int k2 = (is - 1) * (lc - 1) + (iflip - 1);
+            const double2* dl = md.plq_delta + (size_t)k2 * z * z;
+            for (int l = tid; l < ne; l += blockDim.x) {          // vkt = delta UR(P,:)
+                double2 u[PLQ_ZMAX];
+#pragma unroll
+                for (int q = 0; q < PLQ_ZMAX; ++q) if (q < z) u[q] = UR[(size_t)pc[q] + (size_t)N * l];
+                for (int a = 0; a < z; ++a) {
+                    double2 s = cmk(0, 0);
+#pragma unroll
+                    for (int q = 0; q < PLQ_ZMAX; ++q) if (q < z) s = cfma(dl[a + z * q], u[q], s);
+                    vkt[(size_t)a * ne + l] = s;
+                }
+            }
+            __syncthreads();
+            for (int l = tid; l < ne; l += blockDim.x) {          // vk = vkt ULRINV
+                double2 s[PLQ_ZMAX];
+#pragma unroll
+                for (int a = 0; a < PLQ_ZMAX; ++a) s[a] = cmk(0, 0);
+                for (int q = 0; q < ne; ++q) {
+                    const double2 r = R[(size_t)q + (size_t)ne * l];
+#pragma unroll
+                    for (int a = 0; a < PLQ_ZMAX; ++a) if (a < z) s[a] = cfma(vkt[(size_t)a * ne + q], r, s[a]);
+                }
+#pragma unroll
+                for (int a = 0; a < PLQ_ZMAX; ++a) if (a < z) vk[(size_t)a * ne + l] = s[a];
+            }
+            __syncthreads();
+            if (tid == 0) {
+                const int isp = (is + iflip - 1) % lc + 1;
+                double2 vu[PLQ_ZMAX * PLQ_ZMAX];
+                for (int a = 0; a < z; ++a)                       // I + vk UL(:,P), UL(l, P_b) = ULT(P_b, l)
+                    for (int b = 0; b < z; ++b) {
+                        double2 s = cmk(a == b ? 1.0 : 0.0, 0.0);
+                        for (int l = 0; l < ne; ++l) s = cfma(vk[(size_t)a * ne + l], ULT[(size_t)pc[b] + (size_t)N * l], s);
+                        vu[a + z * b] = s;
+                    }
+                const double2 ratio1 = small_inv_det(vu, z);
+                for (int e = 0; e < z * z; ++e) s_mat[e] = vu[e];
+                double2 rt = ratio1;
+                for (int f = 1; f < md.nflr; ++f) rt = cmul(rt, ratio1);
+                rt = cmul(cscale(rt, md.plq_gam_ratio[k2]), md.plq_phase_ratio[k2]);
+                const double ra = fabs(cmul(rt, ph).x / ph.x), r = plq_stream(rw[2 * k + 1]);
+                if (fabs(ra - r) < DQ_NEAR_TIE) nties += 1.0;
+                s_acc = ra > r;
+                if (s_acc) {
+                    acc += 1.0;
+                    ph = cscale(cmul(ph, rt), 1.0 / sqrt(cmulc(rt, rt).x));
+                    cf[p] = isp;
+                }
+            }
+            __syncthreads();
+            if (s_acc) {
+                for (int l = tid; l < ne; l += blockDim.x) {
+                    // UR(P,:) += vkt; vk(:,l) <- (I + vk UL(:,P))^-1 vk(:,l)
+                    double2 w[PLQ_ZMAX], v[PLQ_ZMAX];
+#pragma unroll
+                    for (int a = 0; a < PLQ_ZMAX; ++a) if (a < z) v[a] = vk[(size_t)a * ne + l];
+#pragma unroll
+                    for (int a = 0; a < PLQ_ZMAX; ++a) {
+                        if (a >= z) break;
+                        UR[(size_t)pc[a] + (size_t)N * l] = cadd(UR[(size_t)pc[a] + (size_t)N * l], vkt[(size_t)a * ne + l]);
+                        double2 s = cmk(0, 0);
+#pragma unroll
+                        for (int b = 0; b < PLQ_ZMAX; ++b) if (b < z) s = cfma(s_mat[a + z * b], v[b], s);
+                        w[a] = s;
+                    }
+#pragma unroll
+                    for (int a = 0; a < PLQ_ZMAX; ++a) if (a < z) vk[(size_t)a * ne + l] = w[a];
+                }
+                for (int q = tid; q < ne; q += blockDim.x) {      // lru(q, b) = sum_l ULRINV(q,l) UL(l,P_b)
+                    double2 s[PLQ_ZMAX];
+#pragma unroll
+                    for (int b = 0; b < PLQ_ZMAX; ++b) s[b] = cmk(0, 0);
+                    for (int l = 0; l < ne; ++l) {
+                        const double2 r = R[(size_t)q + (size_t)ne * l];
+#pragma unroll
+                        for (int b = 0; b < PLQ_ZMAX; ++b) if (b < z) s[b] = cfma(r, ULT[(size_t)pc[b] + (size_t)N * l], s[b]);
+                    }
+#pragma unroll
+                    for (int b = 0; b < PLQ_ZMAX; ++b) if (b < z) lru[(size_t)b * ne + q] = s[b];
+                }
+                __syncthreads();
+                for (int q = tid; q < ne; q += blockDim.x) {      // ULRINV -= lru W
+                    double2 lr[PLQ_ZMAX];
+#pragma unroll
+                    for (int b = 0; b < PLQ_ZMAX; ++b) if (b < z) lr[b] = lru[(size_t)b * ne + q];
+                    for (int l = 0; l < ne; ++l) {
+                        double2 s = cmk(0, 0);
+#pragma unroll
+                        for (int b = 0; b < PLQ_ZMAX; ++b) if (b < z) s = cfma(lr[b], vk[(size_t)b * ne + l], s);
+                        R[(size_t)q + (size_t)ne * l] = csub(R[(size_t)q + (size_t)ne * l], s);
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        if (dir) {
+            plq_rows(ULT, N, ne, pc, z, md.plq_bmat + (size_t)(cf[p] - 1) * z * z, true);
+            plq_rows(UR, N, ne, pc, z, md.plq_bmat_inv + (size_t)(cf[p] - 1) * z * z);
+        }
+    }
+    if (tid == 0) {
+        c.stats[ST_PHASE_RE] = ph.x;
+        c.stats[ST_PHASE_IM] = ph.y;
+        if (lupdate) {
+            c.stats[ST_ACCP] += acc;
+            c.stats[ST_PROPP] += lq;
+            c.stats[ST_NEAR_TIE] += nties;
+        }
+    }
+}
+
+static int g_plqp_attr = 0;
+
+void launch_plq_proj_slice(const ChainDev* chains, int nchains, int maxNe, int nt, int visit, int dir, int lupdate,
+                           cudaStream_t st) {
+    const size_t smem = (size_t)3 * PLQ_ZMAX * maxNe * sizeof(double2);
+    if (!g_plqp_attr) {
+        cudaFuncSetAttribute(k_plq_proj_slice, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * PLQ_ZMAX * 512 * (int)sizeof(double2));
+        g_plqp_attr = 1;
+    }
+    k_plq_proj_slice<<<nchains, PLQ_NT, smem, st>>>(chains, nt, visit, dir, lupdate);
+}
+
+static int g_plq_attr = 0;
+
+void launch_plq_slice(const ChainDev* chains, int nchains, int maxN, int nt, int visit, int dir, int lupdate,
+                      cudaStream_t st) {
+    const size_t smem = (size_t)PLQ_ZMAX * maxN * sizeof(double2);
+    if (!g_plq_attr) {
+        cudaFuncSetAttribute(k_plq_slice, cudaFuncAttributeMaxDynamicSharedMemorySize, PLQ_ZMAX * 512 * (int)sizeof(double2));
+        g_plq_attr = 1;
+    }
+    k_plq_slice<<<nchains, PLQ_NT, smem, st>>>(chains, nt, visit, dir, lupdate);
+}

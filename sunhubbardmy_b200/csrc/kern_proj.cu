@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(256) k_pwin_seq(const ChainDev* __restrict__ c
     if (rnd_off < 0) {
         const int vw = md.lwrapv ? 2 * md.nn_lf * md.nn_nf : 0, uw = md.lwrapu ? 2 * N : 0;
         int within;
-        if (dir == 0) within = bond ? (nf - 1) * 2 * md.nn_lf : vw;
+        if (dir == 0) within = md.rw_pre0 + (bond ? (nf - 1) * 2 * md.nn_lf : vw);
         else within = bond ? uw + (md.nn_nf - nf) * 2 * md.nn_lf : 0;
         rnd_off = visit * md.rps + within;
     }

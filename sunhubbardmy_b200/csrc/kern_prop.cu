@@ -16,11 +16,49 @@
 #include "kernels.h"
 #include <cmath>
 
+#define PLQ_ZMAX 6   // sites of a plaquette (honeycomb)
+
+// The PK_PLQ op (the plaquette field, src/dqmc_config_plqu/dqmc_*_prop.f90):
+// x <- P_p x (left, vectors are columns) or x <- x P_p (right, vectors are
+// rows) for p over the plaquettes in the op's order, P_p the block bmat
+// (which = PW_FWD) or bmat_inv of the plaquette's field at slice nt.  The
+// plaquettes share sites, so each vector's thread applies them in turn.
+DQ_DEV void plq_apply(const ModelDev& md, const int32_t* conf_plq, int which, int desc, int nt, int right,
+                      double2* S, int nv, int vs) {
+    const int z = md.plq_z, lq = md.lq;
+    const double2* Mb = which == PW_INV ? md.plq_bmat_inv : md.plq_bmat;
+    const int32_t* cf = conf_plq + (size_t)(nt - 1) * lq;
+    for (int v = threadIdx.x; v < nv; v += blockDim.x) {
+        double2* x = S + (size_t)v * vs;
+        for (int k = 0; k < lq; ++k) {
+            const int p = desc ? lq - 1 - k : k;
+            const int* pc = md.plq_cord + p * z;
+            const double2* M = Mb + (size_t)(cf[p] - 1) * z * z;
+            double2 a[PLQ_ZMAX], y[PLQ_ZMAX];
+#pragma unroll
+            for (int i = 0; i < PLQ_ZMAX; ++i) if (i < z) a[i] = x[pc[i]];
+#pragma unroll
+            for (int i = 0; i < PLQ_ZMAX; ++i) {
+                if (i >= z) break;
+                double2 s = cmk(0, 0);
+#pragma unroll
+                for (int j = 0; j < PLQ_ZMAX; ++j) {
+                    if (j >= z) break;
+                    s = right ? cfma(a[j], __ldg(&M[j + z * i]), s) : cfma(__ldg(&M[i + z * j]), a[j], s);
+                }
+                y[i] = s;
+            }
+#pragma unroll
+            for (int i = 0; i < PLQ_ZMAX; ++i) if (i < z) x[pc[i]] = y[i];
+        }
+    }
+}
+
 // One operator applied to `nv` vectors held in shared memory (vector v at
 // S + v*vs, element stride 1).  right = 0: vectors are columns and the operator
 // multiplies from the left; right = 1: vectors are rows (x -> x * Op).
-__device__ void apply_op(const ModelDev& md, const int32_t* conf, const int32_t* vconf, int code, int right,
-                         double2* S, int nv, int vs) {
+__device__ void apply_op(const ModelDev& md, const int32_t* conf, const int32_t* vconf, const int32_t* conf_plq,
+                         int code, int right, double2* S, int nv, int vs) {
     const int kind = code & 15, which = (code >> 4) & 15, nf = (code >> 8) & 255, nt = code >> 16;
     const int N = md.N, tid = threadIdx.x, nth = blockDim.x;
     // CB, DIAG and bond-field ops: a thread owns one bond (or site) and applies
@@ -85,6 +123,8 @@ __device__ void apply_op(const ModelDev& md, const int32_t* conf, const int32_t*
             }
         }
         }
+    } else if (kind == PK_PLQ) {
+        plq_apply(md, conf_plq, which, nf, nt, right, S, nv, vs);
     } else if (kind == PK_DIAG) {
         const int32_t* cf = conf + (size_t)(nt - 1) * N;
         const int ngrp = max(1, min(nv, nth / N));
@@ -155,7 +195,7 @@ __global__ void __launch_bounds__(256, 2) k_prop_cols(const ChainDev* __restrict
         int nv = min(cb, ncol - c0);
         for (int e = threadIdx.x; e < nv * N; e += blockDim.x) sm[(e / N) * vs + e % N] = X[(size_t)c0 * N + e];
         __syncthreads();
-        for (int k = 0; k < prog.n; ++k) apply_op(md, c.conf, c.vconf, prog.op[k], right, sm, nv, vs);
+        for (int k = 0; k < prog.n; ++k) apply_op(md, c.conf, c.vconf, c.conf_plq, prog.op[k], right, sm, nv, vs);
         for (int e = threadIdx.x; e < nv * N; e += blockDim.x) X[(size_t)c0 * N + e] = sm[(e / N) * vs + e % N];
         __syncthreads();
     }
@@ -175,7 +215,7 @@ __global__ void __launch_bounds__(256, 2) k_prop_rows(const ChainDev* __restrict
             sm[r * vs + j] = X[MIDX(r0 + r, j, N)];
         }
         __syncthreads();
-        for (int k = 0; k < prog.n; ++k) apply_op(md, c.conf, c.vconf, prog.op[k], 1, sm, nv, vs);
+        for (int k = 0; k < prog.n; ++k) apply_op(md, c.conf, c.vconf, c.conf_plq, prog.op[k], 1, sm, nv, vs);
         for (int e = threadIdx.x; e < nv * N; e += blockDim.x) {
             int r = e % nv, j = e / nv;
             X[MIDX(r0 + r, j, N)] = sm[r * vs + j];

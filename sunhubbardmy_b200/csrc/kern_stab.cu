@@ -431,6 +431,10 @@ __global__ void __launch_bounds__(256) k_wrap_check(const ChainDev* __restrict__
         for (size_t e = tid; e < NN; e += nth) c.G[e] = c.Gnew[e];
     mx = block_max(mx, red);
     double ang = 0.0;
+    if (md.plq) {            // set_phase.f90:9-15: the plaquette field's phases
+        const size_t nconf = (size_t)md.ltrot * md.lq;
+        for (size_t e = tid; e < nconf; e += nth) ang += md.plq_phase_angle[c.conf_plq[e] - 1];
+    }
     if (md.phase_on) {
         const size_t nconf = (size_t)md.ltrot * N;
         for (size_t e = tid; e < nconf; e += nth) ang += md.phase_angle[c.conf[e] - 1];

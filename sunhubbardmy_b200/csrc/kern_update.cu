@@ -154,7 +154,8 @@ static_assert(sizeof(UpdWin) + 2 * UPD_CH * 64 * sizeof(double2) <= UpdGemm::SME
 // blk[i] != 0 go to the next field value, no random test, chains whose block
 // did not pass the first stage do nothing); the log of the product of the
 // flips' ratios is accumulated in stats[ST_BLK_LR_*].
-__global__ void __launch_bounds__(UPD_NT, 2) k_update_delay(const ChainDev* __restrict__ chains, int nt, int visit, int forced) {
+__global__ void __launch_bounds__(UPD_NT, 2) k_update_delay(const ChainDev* __restrict__ chains, int nt, int visit, int forced,
+                                                            int dir) {
     extern __shared__ double2 dsm[];
     const ChainDev& c = chains[blockIdx.x];
     const ModelDev& md = *c.md;
@@ -164,7 +165,7 @@ __global__ void __launch_bounds__(UPD_NT, 2) k_update_delay(const ChainDev* __re
     cplx* gsm = dsm;                                   // GEMM staging
     UpdWin* W = (UpdWin*)dsm;                          // window state (same memory)
     int32_t* cf = c.conf + (size_t)(nt - 1) * N;
-    const uint32_t* rw = c.rnd + (size_t)visit * 2 * N;
+    const uint32_t* rw = c.rnd + (size_t)visit * md.rps + md.rw_u[dir];
     double2* G = c.G;
     double2* A = c.A;
     double2* B = c.B;
@@ -380,13 +381,13 @@ __global__ void __launch_bounds__(UPD_NT, 2) k_update_flush(const ChainDev* __re
 
 static int g_upd_attr = 0;
 
-void launch_update(const ChainDev* chains, int nchains, int nt, int visit, cudaStream_t st, int forced) {
+void launch_update(const ChainDev* chains, int nchains, int nt, int visit, cudaStream_t st, int forced, int dir) {
     size_t smem = UpdGemm::SMEM_ELEMS * sizeof(double2);
     if (!g_upd_attr) {
         cudaFuncSetAttribute(k_update_delay, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         g_upd_attr = 1;
     }
-    k_update_delay<<<nchains, UPD_NT, smem, st>>>(chains, nt, visit, forced);
+    k_update_delay<<<nchains, UPD_NT, smem, st>>>(chains, nt, visit, forced, dir);
 }
 
 static int g_flush_attr = 0;

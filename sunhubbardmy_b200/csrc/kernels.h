@@ -14,7 +14,14 @@ void launch_prop_fft(const ChainDev* chains, int nchains, int L, int nvec, int m
                      int rows, int right, int tall, cudaStream_t st);
 void launch_sfmt(const ChainDev* chains, int nchains, int slices, cudaStream_t st);
 void launch_sfmt_raw(const ChainDev* chains, int chain, int count, cudaStream_t st);
-void launch_update(const ChainDev* chains, int nchains, int nt, int visit, cudaStream_t st, int forced = 0);
+// dir: the sweep direction of the slice's draws (0: 0b, 1: b0; ModelDev::rw_u)
+void launch_update(const ChainDev* chains, int nchains, int nt, int visit, cudaStream_t st, int forced = 0, int dir = 0);
+// one slice of plaquette-field props and updates (dir 0: the 0b order, 1: the b0 order)
+void launch_plq_slice(const ChainDev* chains, int nchains, int maxN, int nt, int visit, int dir, int lupdate,
+                      cudaStream_t st);
+// the same on the projective path (UR, UL^T, ULRINV)
+void launch_plq_proj_slice(const ChainDev* chains, int nchains, int maxNe, int nt, int visit, int dir, int lupdate,
+                           cudaStream_t st);
 void launch_update_flush(const ChainDev* chains, int nchains, cudaStream_t st);   // G += A B^T alone
 // equal-time measurement: G^T into GT (tiled transpose), then the observables
 enum { MEAS_ONE_ORBITAL = 0, MEAS_HONEYCOMB = 1, MEAS_CUBIC = 2, MEAS_R_CUBIC = 3 };

@@ -16,8 +16,8 @@
  *
  * Usage: replay_ft [dqmc.in] [key=value ...]
  *   dqmc.in      the &model_para and &ctrl_para namelists (src/model_para.f90:155-218);
- *                keys la, lb, lc, beta, dtau, rt, rtd, t2, t3, nu, mu, rhub, rv, alpha, theta,
- *                nflr, lproju, lprojv, xmag, flux_x, flux_y, dimer, rndness,
+ *                keys la, lb, lc, beta, dtau, rt, rtd, t2, t3, nu, mu, rhub, rv, rhub_plq, alpha, theta,
+ *                nflr, lproju, lprojv, lprojplqu, xmag, flux_x, flux_y, dimer, rndness,
  *                lstabilize, nwrap, nsweep, nbin, nublock, ltau, dyntau,
  *                obs_eqt_mid_len
  *   key=value    the same keys, plus the RUNMODE build flags of src/make.sys.*:
@@ -81,13 +81,12 @@ static int set_key(dqmc_params* p, const char* key, const char* val, int32_t* se
     if (!strcmp(k, "nwarmup")) { *nwarm = (int)v; return 0; }
     if (!strcmp(k, "out")) { snprintf(out, 256, "%s", val); return 0; }
     D(beta) D(dtau) D(rt) D(t2) D(t3) D(nu) D(mu) D(rhub) D(rv) D(alpha) D(theta)
-    D(xmag) D(flux_x) D(flux_y) D(dimer) D(rndness) D(dyntau) D(rtd)
-    I(l1) I(l2) I(nflr) I(lproju) I(lprojv) I(lstabilize) I(nwrap) I(nsweep) I(nbin) I(nublock) I(ltau)
+    D(xmag) D(flux_x) D(flux_y) D(dimer) D(rndness) D(dyntau) D(rtd) D(rhub_plq)
+    I(l1) I(l2) I(nflr) I(lproju) I(lprojv) I(lprojplqu) I(lstabilize) I(nwrap) I(nsweep) I(nbin) I(nublock) I(ltau)
     I(lattice) I(update) I(kinetic) I(hs) I(proj)
 #undef D
 #undef I
-    /* namelist members with no effect on this path (rhub_plq, lprojplqu) */
-    if (!strcmp(k, "rhub_plq") || !strcmp(k, "lprojplqu")) return 0;
+
     fprintf(stderr, "replay_ft: unknown key %s\n", key);
     return -1;
 }

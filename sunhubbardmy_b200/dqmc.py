@@ -56,6 +56,7 @@ class DqmcParams(C.Structure):
         ("ne", C.c_int32), ("lcomp", C.c_int32),
         ("ltau", C.c_int32), ("ntdm", C.c_int32), ("dyntau", C.c_double),
         ("l3", C.c_int32), ("rtd", C.c_double),
+        ("rhub_plq", C.c_double), ("lprojplqu", C.c_int32),
     ]
 
     @classmethod
@@ -65,7 +66,7 @@ class DqmcParams(C.Structure):
                  mu=0.0, rhub=0.0, rv=0.0, alpha=0.2, theta=0.0, xmag=0.0, flux_x=0.0, flux_y=0.0,
                  dimer=0.0, rndness=0.0, nflr=2, lproju=0, lstabilize=1, nwrap=10, nsweep=20,
                  nbin=10, nublock=0, update=DELAY, kinetic=CHECKERBOARD, hs=GENERAL4, proj=0,
-                 lprojv=0, obs_mid_len=1, ltau=0, dyntau=0.0, l3=1, rtd=1.0)
+                 lprojv=0, obs_mid_len=1, ltau=0, dyntau=0.0, l3=1, rtd=1.0, rhub_plq=0.0, lprojplqu=0)
         d.update(kw)
         p = cls(**d)
         rc = load_library().dqmc_params_derive(C.byref(p))
@@ -100,7 +101,7 @@ class DqmcDiag(C.Structure):
         "avglog10error_sum", "logcount", "avgexpphasediff_sum", "accepted", "proposed", "nobs",
         "accepted_v", "proposed_v", "blk_proposed", "blk_stage1", "blk_accepted", "blk_sum_logratio",
         "blk_err_learned", "blk_err_zero", "max_dyn_error", "dyn_log10_sum", "dyn_count", "info",
-        "restabilized", "near_ties")]
+        "restabilized", "near_ties", "accepted_plq", "proposed_plq")]
 
 
 _lib = None
@@ -159,6 +160,8 @@ SIGNATURES = {
     "dqmc_gpu_noalloc_error": (C.c_char_p, []),
     "dqmc_gpu_set_vconf": (_i, [_vp, _i, _vp]),
     "dqmc_gpu_get_vconf": (_i, [_vp, _i, _vp]),
+    "dqmc_gpu_set_conf_plq": (_i, [_vp, _i, _vp]),
+    "dqmc_gpu_get_conf_plq": (_i, [_vp, _i, _vp]),
     "dqmc_gpu_get_trial": (_i, [_vp, _i, _vp, _vp]),
     "dqmc_gpu_set_trial": (_i, [_vp, _i, _vp]),
     "dqmc_gpu_get_proj": (_i, [_vp, _i, _vp, _vp, _vp]),
@@ -454,7 +457,8 @@ class Dqmc:
                     blk_sum_logratio=d.blk_sum_logratio, blk_err_learned=d.blk_err_learned,
                     blk_err_zero=d.blk_err_zero, max_dyn_error=d.max_dyn_error,
                     dyn_log10_sum=d.dyn_log10_sum, dyn_count=d.dyn_count, info=int(d.info),
-                    restabilized=int(d.restabilized), near_ties=int(d.near_ties))
+                    restabilized=int(d.restabilized), near_ties=int(d.near_ties),
+                    accepted_plq=d.accepted_plq, proposed_plq=d.proposed_plq)
 
     def energy_all(self) -> np.ndarray:
         """energy_bin(1:10) of every chain, shape (n_chains, 10) complex."""
@@ -608,6 +612,16 @@ class Dqmc:
     def set_vconf(self, v: np.ndarray, c: int = 0) -> None:
         a = np.ascontiguousarray(v, np.int32)
         _check(load_library().dqmc_gpu_set_vconf(self.h, c, _ptr(a)), "set_vconf")
+
+    def conf_plq(self, c: int = 0) -> np.ndarray:
+        """Plaquette field hconf%conf_plqu as [ltrot][lq] (plaquette fastest)."""
+        out = np.zeros((self.ltrot, self.chain_params(c).lq), np.int32)
+        _check(load_library().dqmc_gpu_get_conf_plq(self.h, c, _ptr(out)), "get_conf_plq")
+        return out
+
+    def set_conf_plq(self, v: np.ndarray, c: int = 0) -> None:
+        a = np.ascontiguousarray(v, np.int32)
+        _check(load_library().dqmc_gpu_set_conf_plq(self.h, c, _ptr(a)), "set_conf_plq")
 
     def trial(self, c: int = 0):
         """(proj, w): trial eigenvectors (ndim x ndim) and eigenvalues of walker c."""

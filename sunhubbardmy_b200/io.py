@@ -3,7 +3,10 @@
 * ``conf_u.in`` / ``conf_u.out`` (src/dqmc_config_u/dqmc_input_conf.f90:36-102,
   dqmc_output_conf.f90:27-42): a first line with a nonzero integer, then
   ``ltrot*nsites`` integers, one per line, site fastest, chain (rank) after
-  chain.
+  chain.  ``conf_plqu.in`` / ``conf_plqu.out`` of the plaquette field
+  (src/dqmc_config_plqu/dqmc_input_plqconf.f90, dqmc_output_plqconf.f90) have
+  the same layout with ``lq`` plaquettes per slice: ``write_conf`` and
+  ``read_conf`` serve both (``Dqmc.conf_plq`` / ``set_conf_plq``).
 * ``energy.bin`` and the ``*.bin`` files of equaltime_output
   (src/dqmc_measure/equaltime_output.f90:67-180): per bin, the bin sums
   reduced over chains and divided by ``n_chains * nobs``.
@@ -247,8 +250,8 @@ def dqmc_initial_print(f, p, wrap_step=None, nustock: int = 0) -> None:
     w("\n --------------------- \n The input parameters  \n --------------------- \n\n")
     w(f" t      = {g['rt']:6.2f}\n")
     w(f" mu     = {g['mu']:7.3f}\n")
-    w(f" rhub_plq  = {0.0:7.3f}\n")
-    w(f" lprojplqu =  {_lg(0)}\n")
+    w(f" rhub_plq  = {g.get('rhub_plq', 0.0):7.3f}\n")
+    w(f" lprojplqu =  {_lg(g.get('lprojplqu', 0))}\n")
     w(f" rhub      = {g['rhub']:7.3f}\n")
     w(f" lproju    =  {_lg(g['lproju'])}\n")
     w(f" rv      = {g['rv']:7.3f}\n")

@@ -2,8 +2,8 @@
 
 The cases are small versions of the benchmark configurations (square Hubbard
 with checkerboard, FFT or dense kinetic term, exact or general HS field;
-honeycomb SU(4); the 1D chain; the cubic and r_cubic lattices) sized so the oracle finishes each
-in well under a second.
+honeycomb SU(4); the 1D chain; the cubic and r_cubic lattices; the plaquette field) sized so the
+oracle finishes each in well under a second.
 """
 import numpy as np
 
@@ -48,6 +48,11 @@ CASES = {
                                 kinetic=0, update=1, hs=1, nwrap=5, nublock=8),
     "rc322_dense_exact_sub": dict(lattice=5, l1=3, l2=2, l3=2, beta=1.0, dtau=0.1, rhub=3.0, nflr=2,
                                   kinetic=2, update=2, hs=0, nwrap=5, nublock=8),
+    # the plaquette field (hconf) beside the U field
+    "sq4_plq_gen4_delay": dict(lattice=1, l1=4, l2=4, beta=1.0, dtau=0.1, rhub=3.0, rhub_plq=1.0, alpha=0.3,
+                               theta=0.2, nflr=2, mu=0.1, kinetic=0, update=1, hs=1, nwrap=5, nublock=4),
+    "hc3_plq_dense_exact_fast": dict(lattice=2, l1=3, l2=3, beta=1.0, dtau=0.1, rhub=3.0, rhub_plq=0.8, alpha=0.25,
+                                     theta=0.1, nflr=2, kinetic=2, update=0, hs=0, nwrap=5),
 }
 
 TEST_SEED0 = 1909706392   # abs((0*1981+2008)*951049)

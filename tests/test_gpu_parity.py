@@ -185,6 +185,9 @@ def test_full_sweeps(sb, oracle, case):
         else:
             assert dg["max_wrap_error"] < 1e-10
         assert abs(dg["phase"] - dc["phase"]) < 1e-9
+        if CASES[case].get("rhub_plq", 0.0):
+            assert np.array_equal(g.conf_plq(k), ch[k].conf_plq()), k
+            assert dg["accepted_plq"] == dc["accepted_plq"] and dg["proposed_plq"] == dc["proposed_plq"]
         bg, bc = g.bins(k), ch[k].bins()
         assert bg["nobs"] == bc["nobs"]
         for key in ("energy", "cpcm", "nn", "jj", "bb"):

@@ -29,6 +29,11 @@ PCASES = {
                        nwrap=10, proj=1, rndness=0.02, update=2),
     "hc3_tv_dense": dict(lattice=2, l1=3, l2=3, beta=2.0, dtau=0.1, rv=1.0, rhub=0.0, nflr=1, kinetic=2,
                          nwrap=5, proj=1, rndness=1e-3, update=2),
+    # the plaquette field (dqmc_proj_update_plqu.f90) beside the U field, and beside both U and bond fields
+    "sq4_hub_plq": dict(lattice=1, l1=4, l2=4, beta=2.0, dtau=0.1, rv=0.0, rhub=3.0, nflr=2, kinetic=0,
+                        nwrap=5, proj=1, rndness=0.05, update=2, hs=0, nublock=8, rhub_plq=0.8, alpha=0.3, theta=0.2),
+    "hc2_tuv_plq": dict(lattice=2, l1=2, l2=2, beta=1.6, dtau=0.1, rv=0.8, rhub=2.0, nflr=2, kinetic=0,
+                        nwrap=4, proj=1, rndness=0.05, update=2, hs=0, nublock=4, rhub_plq=0.6, alpha=0.25),
 }
 
 
@@ -69,6 +74,8 @@ def test_fields_and_trial_draws(sb, oracle, case):
             assert np.array_equal(g.vconf(c), ch.vconf())
         if kw["rhub"] != 0:
             assert np.array_equal(g.conf(c), ch.conf())
+        if kw.get("rhub_plq", 0.0):
+            assert np.array_equal(g.conf_plq(c), ch.conf_plq())
         Pg, wg = g.trial(c)
         Po, wo = ch.trial()
         ne = p.ne
@@ -176,6 +183,9 @@ def test_proj_sweeps_match_oracle(sb, oracle, case):
             assert np.array_equal(g.conf(k), c.conf()), k
         dg, dc = g.diag(k), c.diag()
         assert dg["accepted_v"] == dc["accepted_v"] and dg["accepted"] == dc["accepted"]
+        if kw.get("rhub_plq", 0.0):
+            assert np.array_equal(g.conf_plq(k), c.conf_plq()), k
+            assert dg["accepted_plq"] == dc["accepted_plq"] and dg["proposed_plq"] == dc["proposed_plq"]
         assert dg["logcount"] == dc["logcount"]
         assert dg["max_wrap_error"] < 1e-8
         assert abs(dg["phase"] - dc["phase"]) < 1e-9
