@@ -485,7 +485,7 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
     # end to end through the public API with host buffers: h2d of every chain's
     # HS field, sweep_start + one sweep, d2h of every chain's bins and field
     nbins = sum(len(g.bins_raw(c)) for c in range(C)) / C
-    e2e_steps = max(1, min(args.steps, 2))
+    e2e_steps = max(1, min(args.steps, 5))
     if proj and p.rv != 0:
         # the bond field of every walker (vconf%conf), walker by walker
         vhost = [torch.empty(g.vconf(c).shape, dtype=torch.int32, pin_memory=True).numpy() for c in range(C)]
