@@ -275,10 +275,9 @@ orc_model *orc_model_new(const orc_params *pin) {
     }
     set_hs(m);
     set_h0(m);
-    /* the plaquette field (dqmc_ft_ctrl.f90:19-23, dqmc_proj_ctrl.f90:21-24);
-     * the unequal-time pass with it is not restated */
+    /* the plaquette field (dqmc_ft_ctrl.f90:19-23, dqmc_proj_ctrl.f90:21-24) */
     m->lwrapplqu = p->rhub_plq != 0.0;
-    if (m->lwrapplqu && (p->ltau || orc_plq_setup(m) != 0)) { orc_model_free(m); return NULL; }
+    if (m->lwrapplqu && orc_plq_setup(m) != 0) { orc_model_free(m); return NULL; }
     m->proj = p->proj != 0;
     m->obs_mid_len = p->obs_mid_len > 0 ? p->obs_mid_len : 1;
     orc_set_vconf(m);
@@ -1535,6 +1534,11 @@ int orc_sweep_dyn(orc_chain *c) {
     dyn_measure(c, 1, c->gt0, c->g0t, c->gf, c->g00);
     for (int nt = 1; nt <= m->ltrot; ++nt) {
         h0_half(c, ORC_LEFT_FORWARD, ORC_RIGHT_BACKWARD, 0);
+        if (m->lwrapplqu)       /* dqmc_ft_sweep_0b.f90:82-93 without updates */
+            for (int i = 0; i < m->lq; ++i) {
+                orc_plq_prop(m, c->conf_plq, ORC_LEFT_FORWARD, i, nt, c->gf, N);
+                orc_plq_prop(m, c->conf_plq, ORC_RIGHT_BACKWARD, i, nt, c->gf, N);
+            }
         if (m->lwrapu) {
             u_prop(m, c->conf, ORC_LEFT_FORWARD, nt, c->gf, N);
             u_prop(m, c->conf, ORC_RIGHT_BACKWARD, nt, c->gf, N);

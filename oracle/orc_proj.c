@@ -1050,6 +1050,8 @@ static void bmat_nn(const orc_chain *c, int nt, int left, zc *x) {
         if (cb) for (int nf = 1; nf <= nnf; ++nf) orc_h0_prop(m, op, nf, (double *)x, N);
         else orc_h0_prop(m, op, 0, (double *)x, N);
     }
+    if (m->lwrapplqu)          /* Bmat_left_forward / Bmat_right_backward: plaquettes ascending */
+        for (int i = 0; i < m->lq; ++i) orc_plq_prop(m, c->conf_plq, op, i, nt, x, N);
     if (m->lwrapv)
         for (int nf = 1; nf <= nnf; ++nf) {
             orc_v_prop(m, c->vconf, op, nt, nf, 2, x, N);

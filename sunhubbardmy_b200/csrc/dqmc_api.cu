@@ -85,7 +85,6 @@ extern "C" int dqmc_params_derive(dqmc_params* p) {
     if (p->rhub_plq != 0.0) {
         if (p->lattice != DQMC_LATT_SQUARE && p->lattice != DQMC_LATT_HONEYCOMB)
             return fail(DQMC_EINVAL, "the plaquette field needs the square or honeycomb lattice");
-        if (p->ltau) return fail(DQMC_EINVAL, "the plaquette field is not supported with the unequal-time pass (ltau)");
         if (p->rhub_plq < 0.0) return fail(DQMC_EINVAL, "rhub_plq must be >= 0 (sqrt(dtau rhub_plq))");
     }
     return DQMC_OK;
@@ -1814,6 +1813,7 @@ static PropProg prog_bslice_proj(const HostModel& m, int nt, int left) {
     PropProg p; p.n = 0;
     const int which = left ? PW_FWD : PW_INV;
     prog_k(m, p, which, 0);
+    if (m.plq_on) prog_add(p, PK_PLQ, which, 0, nt);      // plaquettes ascending (dqmc_proj_core.f90:89-94, 255-260)
     if (m.p.rv != 0.0)
         for (int nf = 1; nf <= m.nn_nf; ++nf) {
             prog_add(p, PK_VMIX, 0, nf, nt);
@@ -2114,10 +2114,14 @@ static void enqueue_dyn(dqmc_handle* h) {
     launch_dyn_measure(h->d_chains, h->nch, h->maxN, 1, h->st);
     for (int nt = 1; nt <= lt; ++nt) {
         PropProg pl; pl.n = 0; PropProg pr; pr.n = 0;
+        // Bmat_left_forward / Bmat_right_backward of one slice: kinetic, the
+        // plaquettes ascending, the U field, kinetic (src/dqmc_ft_core.f90:80-117, 234-288)
         prog_k(m, pl, PW_FWD, 0);
+        if (m.plq_on) prog_add(pl, PK_PLQ, PW_FWD, 0, nt);
         prog_v(m, pl, PW_FWD, nt);
         prog_k(m, pl, PW_FWD, 1);
         prog_k(m, pr, PW_INV, 0);
+        if (m.plq_on) prog_add(pr, PK_PLQ, PW_INV, 0, nt);
         prog_v(m, pr, PW_INV, nt);
         prog_k(m, pr, PW_INV, 1);
         launch_prog(h, MAT_G, pl, 0);

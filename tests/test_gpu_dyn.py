@@ -30,6 +30,9 @@ DCASES = {
     # r_cubic: the same three observables summed over the orbital pairs
     "rc222_cb_gen4": dict(lattice=5, l1=2, l2=2, l3=2, beta=1.0, dtau=0.1, rhub=4.0, nflr=2, kinetic=0, update=1,
                           hs=1, nwrap=5, nublock=4, rtd=0.7, ltau=1, dyntau=0.6),
+    # the plaquette field's blocks in the propagation of G(tau, 0) and G(0, tau)
+    "sq4_plq_gen4": dict(lattice=1, l1=4, l2=4, beta=1.0, dtau=0.1, rhub=4.0, nflr=2, kinetic=0, update=1, hs=1,
+                         nwrap=5, nublock=4, rhub_plq=0.8, alpha=0.3, theta=0.2, ltau=1, dyntau=0.8),
 }
 
 

@@ -220,7 +220,7 @@ def test_proj_graph_matches_stepwise(sb, oracle):
 # unequal-time window [ntauin, ntauin + ntdm] inside the projection (ltau): the
 # measured 0b sweep runs dqmc_proj_dyn at nt = ntauin.  sq4_tv_fft starts the
 # window between stabilisation points (ntauin = 5, nwrap = 10).
-DYN = {"hc3_tv": 1.0, "sq4_hub": 1.0, "hc2_tuv": 0.8, "sq4_tv_fft": 1.0, "hc3_tv_dense": 1.0}
+DYN = {"hc3_tv": 1.0, "sq4_hub": 1.0, "hc2_tuv": 0.8, "sq4_tv_fft": 1.0, "hc3_tv_dense": 1.0, "sq4_hub_plq": 1.0}
 
 
 @pytest.mark.parametrize("case", list(DYN))

@@ -90,7 +90,8 @@ def test_plaquette_parameter_checks():
     base = dict(lattice=1, l1=4, l2=4, beta=1.0, dtau=0.1, rhub=4.0, rhub_plq=1.0, nwrap=5)
     assert sb.DqmcParams.make(**base).rhub_plq == 1.0
     assert sb.DqmcParams.make(**dict(base, proj=1)).proj == 1       # the projective path takes it too
-    for bad in (dict(lattice=3, l2=1), dict(lattice=4, l3=2), dict(ltau=1, dyntau=0.5), dict(rhub_plq=-1.0)):
+    assert sb.DqmcParams.make(**dict(base, ltau=1, dyntau=0.5)).ltau == 1   # and the unequal-time pass
+    for bad in (dict(lattice=3, l2=1), dict(lattice=4, l3=2), dict(rhub_plq=-1.0)):
         with pytest.raises(sb.DqmcError):
             sb.DqmcParams.make(**dict(base, **bad))
     g = sb.read_dqmc_in("&model_para\nla = 4,\nlb = 4,\nrhub_plq = 0.5,\nlprojplqu = .true.,\n/\n&ctrl_para\n/\n")
