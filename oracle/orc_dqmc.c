@@ -574,6 +574,20 @@ void orc_u_prop(const orc_model *m, const int32_t *conf, int op, int nt, double 
 }
 
 /* Bmat_left_forward (src/dqmc_ft_core.f90:70-121): B(nt1,nt2) * g */
+/* the bond field of slice nt in a B product: per family (1..nnf, or nnf..1
+ * when desc) the nflag = 2 step, then nflag = 1 (src/dqmc_ft_core.f90:98-104,
+ * 150-156, 264-270) */
+static void v_slice(const orc_chain *c, int op, int nt, int desc, zc *g) {
+    const orc_model *m = c->m;
+    if (!m->lwrapv) return;
+    int nnf = m->L.nn_nf;
+    for (int k = 1; k <= nnf; ++k) {
+        int nf = desc ? nnf + 1 - k : k;
+        orc_v_prop(m, c->vconf, op, nt, nf, 2, g, m->ndim);
+        orc_v_prop(m, c->vconf, op, nt, nf, 1, g, m->ndim);
+    }
+}
+
 static void bmat_left_forward(const orc_chain *c, int nt1, int nt2, zc *g) {
     const orc_model *m = c->m;
     int N = m->ndim, nnf = m->L.nn_nf;
@@ -585,6 +599,7 @@ static void bmat_left_forward(const orc_chain *c, int nt1, int nt2, zc *g) {
         }
         if (m->lwrapplqu)
             for (int i = 0; i < m->lq; ++i) orc_plq_prop(m, c->conf_plq, ORC_LEFT_FORWARD, i, nt, g, N);
+        v_slice(c, ORC_LEFT_FORWARD, nt, 0, g);
         if (m->lwrapu) u_prop(m, c->conf, ORC_LEFT_FORWARD, nt, g, N);
         if (m->lwrapT) {
             if (cb) for (int nf = nnf; nf >= 1; --nf) h0_cb(m, ORC_LEFT_FORWARD, nf, g, N);
@@ -604,6 +619,7 @@ static void bmat_left_forward_hc(const orc_chain *c, int nt1, int nt2, zc *g) {
             else h0_fft(m, ORC_LEFT_FORWARD_HC, g, N);
         }
         if (m->lwrapu) u_prop(m, c->conf, ORC_LEFT_FORWARD_HC, nt, g, N);
+        v_slice(c, ORC_LEFT_FORWARD_HC, nt, 1, g);
         if (m->lwrapplqu)
             for (int i = m->lq - 1; i >= 0; --i) orc_plq_prop(m, c->conf_plq, ORC_LEFT_FORWARD_HC, i, nt, g, N);
         if (m->lwrapT) {
@@ -1372,6 +1388,14 @@ int orc_sweep_b0_slices(orc_chain *c, int lupdate, int lmeasure, int nslices) {
             u_prop(m, c->conf, ORC_RIGHT_FORWARD, nt, c->gf, N);
             u_prop(m, c->conf, ORC_LEFT_BACKWARD, nt, c->gf, N);
         }
+        if (m->lwrapv)          /* dqmc_ft_sweep_b0.f90:79-90 */
+            for (int nf = m->L.nn_nf; nf >= 1; --nf) {
+                orc_v_prop(m, c->vconf, ORC_RIGHT_FORWARD, nt, nf, 2, c->gf, N);
+                orc_v_prop(m, c->vconf, ORC_LEFT_BACKWARD, nt, nf, 2, c->gf, N);
+                if (lupdate) orc_ft_update_v(c, nt, nf);
+                orc_v_prop(m, c->vconf, ORC_RIGHT_FORWARD, nt, nf, 1, c->gf, N);
+                orc_v_prop(m, c->vconf, ORC_LEFT_BACKWARD, nt, nf, 1, c->gf, N);
+            }
         if (m->lwrapplqu)       /* dqmc_ft_sweep_b0.f90:91-101 */
             for (int i = m->lq - 1; i >= 0; --i) {
                 if (lupdate) orc_plq_update(c, i, nt);
@@ -1407,6 +1431,7 @@ static void bmat_right_backward(const orc_chain *c, int nt1, int nt2, zc *g) {
         }
         if (m->lwrapplqu)
             for (int i = 0; i < m->lq; ++i) orc_plq_prop(m, c->conf_plq, ORC_RIGHT_BACKWARD, i, nt, g, N);
+        v_slice(c, ORC_RIGHT_BACKWARD, nt, 0, g);
         if (m->lwrapu) u_prop(m, c->conf, ORC_RIGHT_BACKWARD, nt, g, N);
         if (m->lwrapT) {
             if (cb) for (int nf = nnf; nf >= 1; --nf) h0_cb(m, ORC_RIGHT_BACKWARD, nf, g, N);
@@ -1539,6 +1564,12 @@ int orc_sweep_dyn(orc_chain *c) {
                 orc_plq_prop(m, c->conf_plq, ORC_LEFT_FORWARD, i, nt, c->gf, N);
                 orc_plq_prop(m, c->conf_plq, ORC_RIGHT_BACKWARD, i, nt, c->gf, N);
             }
+        if (m->lwrapv)          /* dqmc_ft_sweep_0b.f90:96-106 without updates */
+            for (int nf = 1; nf <= m->L.nn_nf; ++nf)
+                for (int nflag = 2; nflag >= 1; --nflag) {
+                    orc_v_prop(m, c->vconf, ORC_LEFT_FORWARD, nt, nf, nflag, c->gf, N);
+                    orc_v_prop(m, c->vconf, ORC_RIGHT_BACKWARD, nt, nf, nflag, c->gf, N);
+                }
         if (m->lwrapu) {
             u_prop(m, c->conf, ORC_LEFT_FORWARD, nt, c->gf, N);
             u_prop(m, c->conf, ORC_RIGHT_BACKWARD, nt, c->gf, N);
@@ -1626,6 +1657,14 @@ int orc_sweep_0b(orc_chain *c, int lupdate, int lmeasure) {
                 orc_plq_prop(m, c->conf_plq, ORC_LEFT_FORWARD, i, nt, c->gf, N);
                 orc_plq_prop(m, c->conf_plq, ORC_RIGHT_BACKWARD, i, nt, c->gf, N);
                 if (lupdate) orc_plq_update(c, i, nt);
+            }
+        if (m->lwrapv)          /* dqmc_ft_sweep_0b.f90:96-106 */
+            for (int nf = 1; nf <= m->L.nn_nf; ++nf) {
+                orc_v_prop(m, c->vconf, ORC_LEFT_FORWARD, nt, nf, 2, c->gf, N);
+                orc_v_prop(m, c->vconf, ORC_RIGHT_BACKWARD, nt, nf, 2, c->gf, N);
+                if (lupdate) orc_ft_update_v(c, nt, nf);
+                orc_v_prop(m, c->vconf, ORC_LEFT_FORWARD, nt, nf, 1, c->gf, N);
+                orc_v_prop(m, c->vconf, ORC_RIGHT_BACKWARD, nt, nf, 1, c->gf, N);
             }
         if (m->lwrapu) {
             u_prop(m, c->conf, ORC_LEFT_FORWARD, nt, c->gf, N);

@@ -144,5 +144,6 @@ void orc_set_vconf(orc_model *m);
 void orc_proj_chain_init(orc_chain *c, int draw_conf);
 void orc_proj_chain_free(orc_chain *c);
 void orc_v_prop(const orc_model *m, const int32_t *vconf, int op, int nt, int nf, int nflag, zc *g, int n2);
+void orc_ft_update_v(orc_chain *c, int nt, int nf);
 
 #endif

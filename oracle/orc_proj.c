@@ -295,6 +295,65 @@ static void proj_update_v(orc_chain *c, int nt, int nf) {
     free(vk_tmp); free(vk); free(uk); free(lruk); free(vuvk);
 }
 
+/* The finite-temperature bond-field update on the equal-time G
+ * (src/dqmc_config_v/dqmc_update.f90:1-119; the delayed variant
+ * dqmc_update_delay.f90 makes the same draws and decisions): per bond of family
+ * nf, in nnlf_list order, iflip and then the accept word; Delta = diag(dp, dm),
+ * vukmat = I + (1 - G)(P,P) Delta, ratiotot = det vukmat (no flavour power);
+ * on acceptance G <- G - G(:,P) Delta vukmat^-1 (delta(P,:) - G(P,:)). */
+void orc_ft_update_v(orc_chain *c, int nt, int nf) {
+    const orc_model *m = c->m;
+    const orc_latt *L = &m->L;
+    int N = m->ndim, nnf = L->nn_nf;
+    int32_t *cf = c->vconf + ((size_t)(nt - 1) * nnf + (nf - 1)) * N;
+    zc *gc = zalloc(2 * (size_t)N), *vr = zalloc(2 * (size_t)N);
+    zc *g = c->gf;
+    double accm = 0.0;
+    for (int b = 0; b < L->nn_lf; ++b) {
+        int i1 = L->nnlf_list[b] - 1;
+        int i2 = L->nnlist[i1 * nnf + nf - 1] - 1;
+        int is = cf[b];
+        int iflip = (int)ceil(orc_sfmt_stream(&c->rng) * 1);
+        int isp = (is + iflip - 1) % 2 + 1;
+        zc d[2] = {m->vdp[is - 1], m->vdm[is - 1]};
+        int pc[2] = {i1, i2};
+        zc vu[4];                                   /* column-major 2 x 2 */
+        for (int a = 0; a < 2; ++a)
+            for (int q = 0; q < 2; ++q)
+                vu[a + 2 * q] = (a == q ? 1.0 : 0.0) + ((pc[a] == pc[q] ? 1.0 : 0.0) - g[ZIDX(pc[a], pc[q], N)]) * d[q];
+        zc det = vu[0] * vu[3] - vu[2] * vu[1];
+        zc inv[4] = {vu[3] / det, -vu[1] / det, -vu[2] / det, vu[0] / det};
+        zc ratiotot = det;
+        double ratio_re = creal(ratiotot * c->phase) / creal(c->phase);
+        double ratio_abs = ratio_re < 0 ? -ratio_re : ratio_re;
+        double random = orc_sfmt_stream(&c->rng);
+        ORC_COUNT_TIE(c, ratio_abs, random);
+        if (ratio_abs > random) {
+            accm += 1.0;
+            double weight = sqrt(creal(ratiotot * conj(ratiotot)));
+            c->phase = c->phase * ratiotot / weight;
+            zc s[4];                                /* smat = Delta vukmat^-1 */
+            for (int a = 0; a < 2; ++a)
+                for (int q = 0; q < 2; ++q) s[a + 2 * q] = d[a] * inv[a + 2 * q];
+            for (int j = 0; j < N; ++j) {           /* vr = smat (delta(P,:) - G(P,:)), gc = G(:,P) */
+                zc v0 = (j == i1 ? 1.0 : 0.0) - g[ZIDX(i1, j, N)];
+                zc v1 = (j == i2 ? 1.0 : 0.0) - g[ZIDX(i2, j, N)];
+                vr[2 * j] = s[0] * v0 + s[2] * v1;
+                vr[2 * j + 1] = s[1] * v0 + s[3] * v1;
+                gc[j] = g[ZIDX(j, i1, N)];
+                gc[N + j] = g[ZIDX(j, i2, N)];
+            }
+            for (int j = 0; j < N; ++j)
+                for (int i = 0; i < N; ++i)
+                    g[ZIDX(i, j, N)] -= gc[i] * vr[2 * j] + gc[N + i] * vr[2 * j + 1];
+            cf[b] = isp;
+        }
+    }
+    c->acc_v += accm;
+    c->prop_v += L->nn_lf;
+    free(gc); free(vr);
+}
+
 /* dqmc_proj_update, bond field, submatrix-LR flavour
  * (src/dqmc_config_v/dqmc_proj_update_submatrix_LR.f90:1-298): windows of
  * nustock = nublock rows; per window Rrows = UR(rows,:) ULRINV and

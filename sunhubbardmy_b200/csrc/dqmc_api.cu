@@ -48,6 +48,8 @@ extern "C" int dqmc_params_derive(dqmc_params* p) {
             return fail(DQMC_EINVAL, "the cubic lattice needs even l1, l2, l3 >= 2");
     } else if (p->lattice == DQMC_LATT_R_CUBIC) {
         if (p->l1 < 2 || p->l2 < 2 || p->l3 < 2) return fail(DQMC_EINVAL, "the r_cubic lattice needs l1, l2, l3 >= 2");
+        // the bond field's props and updates index the bonds in the reference order,
+        // which the two-phase device order of the r_cubic family 4 differs from
         if (p->rv != 0.0) return fail(DQMC_EINVAL, "the t-V bond field is not supported on the r_cubic lattice");
     } else if (p->l1 < 2 || p->l2 < 2) {
         return fail(DQMC_EINVAL, "l1, l2 must be >= 2");
@@ -79,7 +81,6 @@ extern "C" int dqmc_params_derive(dqmc_params* p) {
         return fail(DQMC_EINVAL, "dyntau = beta is not allowed on the projective path (dqmc_proj_ctrl.f90:13)");
     if (p->ltau && p->nst < 1) return fail(DQMC_EINVAL, "unequal-time measurement (ltau) needs lstabilize and ltrot >= nwrap");
     if (p->proj && p->nst < 1) return fail(DQMC_EINVAL, "the projective sweep needs lstabilize and ltrot >= nwrap");
-    if (!p->proj && p->rv != 0.0) return fail(DQMC_EINVAL, "the t-V bond field (rv != 0) is supported on the projective path only");
     if (p->rv < 0.0) return fail(DQMC_EINVAL, "rv must be >= 0 (acosh(exp(dtau rv / 2)))");
     if (p->proj && (p->ne < 1 || p->ne > p->ndim)) return fail(DQMC_EINVAL, "ne out of range 1..ndim");
     if (p->rhub_plq != 0.0) {
@@ -718,17 +719,20 @@ static int upload_model(HostModel& m) {
     d.ne = p.ne;
     d.lwrapv = (p.rv != 0.0);
     d.rps = d.proj ? ((d.lwrapu ? 2 * m.N : 0) + (d.lwrapv ? 2 * m.nn_lf * m.nn_nf : 0)) : 2 * m.N;
-    if (m.plq_on) {
-        // a slice's draws in the reference's order: 0b visits the plaquettes
-        // before the U (and bond) fields (dqmc_ft_sweep_0b.f90:82-119,
-        // dqmc_proj_sweep_0b.f90:61-90), b0 after them (dqmc_ft_sweep_b0.f90:70-101,
-        // dqmc_proj_sweep_b0.f90:70-99)
-        const int wu = d.lwrapu ? 2 * m.N : 0, wp = 2 * m.lq;
-        const int wv = (d.proj && d.lwrapv) ? 2 * m.nn_lf * m.nn_nf : 0;
+    if (m.plq_on || d.lwrapv) {
+        // a slice's draws in the reference's order: 0b visits the plaquettes,
+        // then the bond families 1..nn_nf, then the U field
+        // (dqmc_ft_sweep_0b.f90:82-119, dqmc_proj_sweep_0b.f90:61-90); b0 the U
+        // field, the families nn_nf..1, then the plaquettes
+        // (dqmc_ft_sweep_b0.f90:70-101, dqmc_proj_sweep_b0.f90:70-99)
+        const int wu = d.lwrapu ? 2 * m.N : 0, wp = m.plq_on ? 2 * m.lq : 0;
+        const int wv = d.lwrapv ? 2 * m.nn_lf * m.nn_nf : 0;
         d.rps = wu + wv + wp;
-        d.rw_plq[0] = 0; d.rw_u[0] = wp;
-        d.rw_u[1] = 0; d.rw_plq[1] = wu + wv;
+        d.rw_plq[0] = 0; d.rw_v[0] = wp; d.rw_u[0] = wp + wv;
+        d.rw_u[1] = 0; d.rw_v[1] = wu; d.rw_plq[1] = wu + wv;
         d.rw_pre0 = wp;
+    }
+    if (m.plq_on) {
         d.plq = 1; d.plq_z = m.z_plq; d.plq_lcomp = m.plq_lcomp;
         if (m.plq_lcomp > DQ_MAX_PLQ_LCOMP) return fail(DQMC_EINVAL, "too many plaquette field values");
         for (int is = 0; is < m.plq_lcomp; ++is) d.plq_phase_angle[is] = std::arg(m.plq_phase[is]);
@@ -1493,6 +1497,19 @@ static void prog_v(const HostModel& m, PropProg& p, int which, int nt) {
     if (m.p.rhub == 0.0) return;
     prog_add(p, PK_DIAG, which, 0, nt);
 }
+// the bond field of slice nt in a B product (left_forward, which = PW_FWD) or
+// B^-1 from the right (right_backward, PW_INV): per family the nflag = 2 step
+// (mix, scale) then nflag = 1 (mix); families 1..nn_nf, or nn_nf..1 when desc
+// (src/dqmc_ft_core.f90:98-104, 150-156, 264-270)
+static void prog_bond(const HostModel& m, PropProg& p, int which, int nt, int desc) {
+    if (m.p.rv == 0.0) return;
+    for (int k = 1; k <= m.nn_nf; ++k) {
+        const int nf = desc ? m.nn_nf + 1 - k : k;
+        prog_add(p, PK_VMIX, 0, nf, nt);
+        prog_add(p, PK_VSCALE, which, nf, nt);
+        prog_add(p, PK_VMIX, 0, nf, nt);
+    }
+}
 
 // all chains share structure; programs are built from model 0 (same nn_nf
 // per handle for a given lattice kind)
@@ -1535,7 +1552,12 @@ static int launch_bmat(dqmc_handle* h, int mat_id, int nt1, int nt2, int hc) {
         // plaquettes ascending before the U field (Bmat_left_forward), descending
         // after it with bmat^H = bmat_inv (Bmat_left_forward_hc)
         if (m.plq_on && !hc) prog_add(sl, PK_PLQ, PW_FWD, 0, nt);
+        if (!hc) prog_bond(m, sl, PW_FWD, nt, 0);
         prog_v(m, sl, which, nt);
+        // the bond field in B^H: families nn_nf..1 with the same steps and
+        // values as in B (dqmc_left_forward_prop_hc.f90 equals
+        // dqmc_left_forward_prop.f90)
+        if (hc) prog_bond(m, sl, PW_FWD, nt, 1);
         if (m.plq_on && hc) prog_add(sl, PK_PLQ, PW_INV, 1, nt);
         prog_k(m, sl, which, 1);
         if (p.n + sl.n > DQ_MAX_PROG) {
@@ -2005,8 +2027,8 @@ static void enqueue_b0(dqmc_handle* h, int lupdate, int lmeasure) {
     const HostModel& m = *h->models[0];
     int lt = h->ltrot;
     launch_stack_identity(h->d_chains, h->nch, h->nst, h->st);
-    const bool plq = m.plq_on;
-    if (lupdate && (m.p.rhub != 0.0 || plq)) launch_sfmt(h->d_chains, h->nch, lt, h->st);
+    const bool plq = m.plq_on, lv = m.p.rv != 0.0;
+    if (lupdate && (m.p.rhub != 0.0 || plq || lv)) launch_sfmt(h->d_chains, h->nch, lt, h->st);
     tmark(h, DQMC_PROF_OTHER);
     for (int nt = lt; nt >= 1; --nt) {
         int visit = lt - nt;
@@ -2022,6 +2044,25 @@ static void enqueue_b0(dqmc_handle* h, int lupdate, int lmeasure) {
         pl.n = 0; pr.n = 0;
         prog_v(m, pl, PW_INV, nt);         // u left_backward
         prog_v(m, pr, PW_FWD, nt);         // u right_forward
+        if (lv)
+            // the bond field, families nn_nf..1: nflag 2 (mix), the update,
+            // nflag 1 (scale, mix) (dqmc_ft_sweep_b0.f90:79-90)
+            for (int nf = m.nn_nf; nf >= 1; --nf) {
+                prog_add(pr, PK_VMIX, 0, nf, nt);            // right_forward
+                prog_add(pl, PK_VMIX, 0, nf, nt);            // left_backward
+                if (lupdate) {
+                    launch_prog(h, MAT_G, pl, 0);
+                    launch_prog(h, MAT_G, pr, 1);
+                    tmark(h, DQMC_PROF_PROP_L);
+                    launch_vbond_slice(h->d_chains, h->nch, h->maxN, nt, nf, visit, 1, h->st);
+                    tmark(h, DQMC_PROF_UPDATE);
+                    pl.n = 0; pr.n = 0;
+                }
+                prog_add(pr, PK_VSCALE, PW_FWD, nf, nt);
+                prog_add(pr, PK_VMIX, 0, nf, nt);
+                prog_add(pl, PK_VSCALE, PW_INV, nf, nt);
+                prog_add(pl, PK_VMIX, 0, nf, nt);
+            }
         if (plq) {
             // the plaquettes (update, then props, descending) between the U field
             // and the kinetic half step (dqmc_ft_sweep_b0.f90:91-101)
@@ -2046,8 +2087,8 @@ static void enqueue_0b(dqmc_handle* h, int lupdate, int lmeasure) {
     const HostModel& m = *h->models[0];
     int lt = h->ltrot;
     launch_stack_identity(h->d_chains, h->nch, 0, h->st);
-    const bool plq = m.plq_on;
-    if (lupdate && (m.p.rhub != 0.0 || plq)) launch_sfmt(h->d_chains, h->nch, lt, h->st);
+    const bool plq = m.plq_on, lv = m.p.rv != 0.0;
+    if (lupdate && (m.p.rhub != 0.0 || plq || lv)) launch_sfmt(h->d_chains, h->nch, lt, h->st);
     tmark(h, DQMC_PROF_OTHER);
     for (int nt = 1; nt <= lt; ++nt) {
         int visit = nt - 1;
@@ -2064,6 +2105,25 @@ static void enqueue_0b(dqmc_handle* h, int lupdate, int lmeasure) {
             tmark(h, DQMC_PROF_UPDATE);
             pl.n = 0; pr.n = 0;
         }
+        if (lv)
+            // the bond field, families 1..nn_nf: nflag 2 (mix, scale), the
+            // update, nflag 1 (mix) (dqmc_ft_sweep_0b.f90:96-106)
+            for (int nf = 1; nf <= m.nn_nf; ++nf) {
+                prog_add(pl, PK_VMIX, 0, nf, nt);            // left_forward
+                prog_add(pl, PK_VSCALE, PW_FWD, nf, nt);
+                prog_add(pr, PK_VMIX, 0, nf, nt);            // right_backward
+                prog_add(pr, PK_VSCALE, PW_INV, nf, nt);
+                if (lupdate) {
+                    launch_prog(h, MAT_G, pl, 0);
+                    launch_prog(h, MAT_G, pr, 1);
+                    tmark(h, DQMC_PROF_PROP_L);
+                    launch_vbond_slice(h->d_chains, h->nch, h->maxN, nt, nf, visit, 0, h->st);
+                    tmark(h, DQMC_PROF_UPDATE);
+                    pl.n = 0; pr.n = 0;
+                }
+                prog_add(pl, PK_VMIX, 0, nf, nt);
+                prog_add(pr, PK_VMIX, 0, nf, nt);
+            }
         prog_v(m, pl, PW_FWD, nt);         // u left_forward
         prog_v(m, pr, PW_INV, nt);         // u right_backward
         launch_prog(h, MAT_G, pl, 0);
@@ -2115,13 +2175,16 @@ static void enqueue_dyn(dqmc_handle* h) {
     for (int nt = 1; nt <= lt; ++nt) {
         PropProg pl; pl.n = 0; PropProg pr; pr.n = 0;
         // Bmat_left_forward / Bmat_right_backward of one slice: kinetic, the
-        // plaquettes ascending, the U field, kinetic (src/dqmc_ft_core.f90:80-117, 234-288)
+        // plaquettes ascending, the bond field, the U field, kinetic
+        // (src/dqmc_ft_core.f90:80-117, 234-288)
         prog_k(m, pl, PW_FWD, 0);
         if (m.plq_on) prog_add(pl, PK_PLQ, PW_FWD, 0, nt);
+        prog_bond(m, pl, PW_FWD, nt, 0);
         prog_v(m, pl, PW_FWD, nt);
         prog_k(m, pl, PW_FWD, 1);
         prog_k(m, pr, PW_INV, 0);
         if (m.plq_on) prog_add(pr, PK_PLQ, PW_INV, 0, nt);
+        prog_bond(m, pr, PW_INV, nt, 0);
         prog_v(m, pr, PW_INV, nt);
         prog_k(m, pr, PW_INV, 1);
         launch_prog(h, MAT_G, pl, 0);
@@ -2642,9 +2705,9 @@ extern "C" int dqmc_gpu_update(dqmc_handle* h, int nt) {
     if (h->proj) return fail(DQMC_ESTATE, "projective handle: use dqmc_gpu_proj_update");
     if (nt < 1 || nt > h->ltrot) return fail(DQMC_EINVAL, "nt out of range");
     const HostModel& m0 = *h->models[0];
-    if (m0.plq_on) {
+    if (m0.plq_on || m0.p.rv != 0.0) {
         // exactly the 2 N draws of uconf%update (the slice layout of a sweep also
-        // holds the plaquette words); the U words start the b0 layout
+        // holds the plaquette and bond words); the U words start the b0 layout
         launch_sfmt(h->d_chains, h->nch, -2 * m0.N, h->st);
         launch_update(h->d_chains, h->nch, nt, 0, h->st, 0, 1);
     } else {
@@ -3326,6 +3389,7 @@ extern "C" int dqmc_gpu_sweep_learned(dqmc_handle* h, dqmc_nn* nn, int n, int lu
         return fail(DQMC_EINVAL, "the effective action's lattice differs from the handle's (square L x L, ltrot)");
     if (m.lcomp != 2) return fail(DQMC_EINVAL, "block flips need a two-valued HS field (lcomp = 2)");
     if (m.p.rhub == 0.0) return fail(DQMC_EINVAL, "no HS field (rhub == 0)");
+    if (m.plq_on || m.p.rv != 0.0) return fail(DQMC_EINVAL, "block moves need the U field alone (rhub_plq = rv = 0)");
     int rc = enable_blocks(h); if (rc) return rc;
     if (seed) h->blk_rng = seed;
     clear_fail(h);

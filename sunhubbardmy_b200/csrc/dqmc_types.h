@@ -22,6 +22,7 @@ struct ModelDev {
     int plq, plq_z, plq_lcomp;
     int rw_u[2], rw_plq[2];    // offsets of the U-field and plaquette words in a slice's draws (0: 0b, 1: b0)
     int rw_pre0;               // words ahead of the U and bond fields' in the 0b layout (the plaquettes')
+    int rw_v[2];               // first bond-field word of a slice (0b: family 1 first; b0: family nn_nf first)
     const double2* plq_bmat;   // [lcomp][z*z] column-major
     const double2* plq_bmat_inv;
     const double2* plq_delta;  // [(is-1)(lcomp-1) + iflip-1][z*z]: bmat(isp) bmat(is)^-1 - I

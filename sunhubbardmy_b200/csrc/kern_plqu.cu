@@ -94,6 +94,41 @@ DQ_DEV double2 small_inv_det(double2* a, int n) {
     return det;
 }
 
+// G <- G - G(:, P) S V with V(q, col) = delta(P_q, col) - G(P_q, col), S the
+// z x z matrix s_mat (column-major); wsm holds W = S V (z x N)
+DQ_DEV void rankz_green(double2* G, int N, const int* pc, int z, const double2* s_mat, double2* wsm) {
+    const int tid = threadIdx.x;
+    for (int col = tid; col < N; col += blockDim.x) {
+        double2 v[PLQ_ZMAX];
+#pragma unroll
+        for (int q = 0; q < PLQ_ZMAX; ++q)
+            if (q < z) {
+                const double2 g = G[MIDX(pc[q], col, N)];
+                v[q] = cmk((pc[q] == col ? 1.0 : 0.0) - g.x, -g.y);
+            }
+        for (int a = 0; a < z; ++a) {
+            double2 s = cmk(0, 0);
+#pragma unroll
+            for (int q = 0; q < PLQ_ZMAX; ++q) if (q < z) s = cfma(s_mat[a + z * q], v[q], s);
+            wsm[(size_t)a * N + col] = s;
+        }
+    }
+    __syncthreads();
+    // a thread owns whole rows
+    for (int r = tid; r < N; r += blockDim.x) {
+        double2 gp[PLQ_ZMAX];
+#pragma unroll
+        for (int a = 0; a < PLQ_ZMAX; ++a) if (a < z) gp[a] = G[MIDX(r, pc[a], N)];
+        for (int col = 0; col < N; ++col) {
+            double2 s = cmk(0, 0);
+#pragma unroll
+            for (int a = 0; a < PLQ_ZMAX; ++a) if (a < z) s = cfma(gp[a], wsm[(size_t)a * N + col], s);
+            G[MIDX(r, col, N)] = csub(G[MIDX(r, col, N)], s);
+        }
+    }
+    __syncthreads();
+}
+
 // One slice of plaquette props and updates for one chain (one CTA per chain).
 // dir = 0: the 0b order, plaquettes ascending, bmat on the rows and bmat_inv
 // on the columns, then the update; dir = 1: the b0 order, plaquettes
@@ -160,38 +195,7 @@ __global__ void __launch_bounds__(PLQ_NT) k_plq_slice(const ChainDev* __restrict
                 }
             }
             __syncthreads();
-            if (s_acc) {
-                // W = smat V, V(q, col) = delta(P_q, col) - G(P_q, col)
-                for (int col = tid; col < N; col += blockDim.x) {
-                    double2 v[PLQ_ZMAX];
-#pragma unroll
-                    for (int q = 0; q < PLQ_ZMAX; ++q)
-                        if (q < z) {
-                            const double2 g = G[MIDX(pc[q], col, N)];
-                            v[q] = cmk((pc[q] == col ? 1.0 : 0.0) - g.x, -g.y);
-                        }
-                    for (int a = 0; a < z; ++a) {
-                        double2 s = cmk(0, 0);
-#pragma unroll
-                        for (int q = 0; q < PLQ_ZMAX; ++q) if (q < z) s = cfma(s_mat[a + z * q], v[q], s);
-                        wsm[(size_t)a * N + col] = s;
-                    }
-                }
-                __syncthreads();
-                // G <- G - G(:, P) W, a thread owning whole rows
-                for (int r = tid; r < N; r += blockDim.x) {
-                    double2 gp[PLQ_ZMAX];
-#pragma unroll
-                    for (int a = 0; a < PLQ_ZMAX; ++a) if (a < z) gp[a] = G[MIDX(r, pc[a], N)];
-                    for (int col = 0; col < N; ++col) {
-                        double2 s = cmk(0, 0);
-#pragma unroll
-                        for (int a = 0; a < PLQ_ZMAX; ++a) if (a < z) s = cfma(gp[a], wsm[(size_t)a * N + col], s);
-                        G[MIDX(r, col, N)] = csub(G[MIDX(r, col, N)], s);
-                    }
-                }
-                __syncthreads();
-            }
+            if (s_acc) rankz_green(G, N, pc, z, s_mat, wsm);
         }
         if (dir) {
             plq_cols(G, N, pc, z, md.plq_bmat + (size_t)(cf[p] - 1) * z * z);
@@ -206,6 +210,72 @@ __global__ void __launch_bounds__(PLQ_NT) k_plq_slice(const ChainDev* __restrict
             c.stats[ST_PROPP] += lq;
             c.stats[ST_NEAR_TIE] += nties;
         }
+    }
+}
+
+// One bond family's updates of one slice on the equal-time G, one CTA per
+// chain (the t-V bond field, src/dqmc_config_v/dqmc_update.f90:34-105): the
+// bonds in nnlf_list order, each a rank-2 change on its sites P = (i1, i2) with
+// Delta = diag(delta_bmat_p, delta_bmat_m) of its field value, vukmat =
+// I + (1 - G)(P,P) Delta, ratiotot = det vukmat and, on acceptance,
+// G <- G - G(:,P) Delta vukmat^-1 (delta(P,:) - G(P,:)).  The field has two
+// values, so iflip = ceil(r (lcomp - 1)) is 1 for every draw r in (0, 1).  The
+// k-th bond uses the words 2k (iflip) and 2k + 1 (the accept test) of the
+// family's 2 nn_lf words: families ascend in the 0b slice layout (dir = 0) and
+// descend in the b0 one (dir = 1).
+__global__ void __launch_bounds__(PLQ_NT) k_vbond_slice(const ChainDev* __restrict__ chains, int nt, int nf, int visit,
+                                                      int dir) {
+    extern __shared__ double2 wsm[];           // S V, 2 x N
+    __shared__ double2 s_mat[4];
+    __shared__ int s_pc[2];
+    __shared__ int s_acc;
+    const ChainDev& c = chains[blockIdx.x];
+    const ModelDev& md = *c.md;
+    if (!md.lwrapv || !c.vconf) return;
+    const int N = c.N, lf = md.nn_lf, nnf = md.nn_nf, tid = threadIdx.x;
+    double2* G = c.G;
+    int32_t* cf = c.vconf + ((size_t)(nt - 1) * nnf + (nf - 1)) * N;
+    const int* rows = md.vrows + (size_t)(nf - 1) * 2 * lf;
+    const uint32_t* rw = c.rnd + (size_t)visit * md.rps + md.rw_v[dir] + (size_t)(dir ? nnf - nf : nf - 1) * 2 * lf;
+    double2 ph = cmk(c.stats[ST_PHASE_RE], c.stats[ST_PHASE_IM]);
+    double acc = 0.0, nties = 0.0;
+    for (int b = 0; b < lf; ++b) {
+        if (tid == 0) {
+            const int i1 = rows[2 * b], i2 = rows[2 * b + 1];
+            s_pc[0] = i1; s_pc[1] = i2;
+            const int is = cf[b];
+            const double2 d0 = md.vdp[is - 1], d1 = md.vdm[is - 1];
+            const double2 g11 = G[MIDX(i1, i1, N)], g12 = G[MIDX(i1, i2, N)];
+            const double2 g21 = G[MIDX(i2, i1, N)], g22 = G[MIDX(i2, i2, N)];
+            // vukmat, column-major
+            const double2 v00 = cadd(cmk(1, 0), cmul(cmk(1.0 - g11.x, -g11.y), d0));
+            const double2 v10 = cmul(cmk(-g21.x, -g21.y), d0);
+            const double2 v01 = cmul(cmk(-g12.x, -g12.y), d1);
+            const double2 v11 = cadd(cmk(1, 0), cmul(cmk(1.0 - g22.x, -g22.y), d1));
+            const double2 det = csub(cmul(v00, v11), cmul(v01, v10));
+            const double2 id = cdiv(cmk(1, 0), det);
+            s_mat[0] = cmul(d0, cmul(v11, id));                      // smat = Delta vukmat^-1
+            s_mat[1] = cmul(d1, cmul(cmk(-v10.x, -v10.y), id));
+            s_mat[2] = cmul(d0, cmul(cmk(-v01.x, -v01.y), id));
+            s_mat[3] = cmul(d1, cmul(v00, id));
+            const double ra = fabs(cmul(det, ph).x / ph.x), r = plq_stream(rw[2 * b + 1]);
+            if (fabs(ra - r) < DQ_NEAR_TIE) nties += 1.0;
+            s_acc = ra > r;
+            if (s_acc) {
+                acc += 1.0;
+                ph = cscale(cmul(ph, det), 1.0 / sqrt(cmulc(det, det).x));
+                cf[b] = is % 2 + 1;
+            }
+        }
+        __syncthreads();
+        if (s_acc) rankz_green(G, N, s_pc, 2, s_mat, wsm);
+    }
+    if (tid == 0) {
+        c.stats[ST_PHASE_RE] = ph.x;
+        c.stats[ST_PHASE_IM] = ph.y;
+        c.stats[ST_ACCV] += acc;
+        c.stats[ST_PROPV] += lf;
+        c.stats[ST_NEAR_TIE] += nties;
     }
 }
 
@@ -377,4 +447,16 @@ void launch_plq_slice(const ChainDev* chains, int nchains, int maxN, int nt, int
         g_plq_attr = 1;
     }
     k_plq_slice<<<nchains, PLQ_NT, smem, st>>>(chains, nt, visit, dir, lupdate);
+}
+
+static int g_vb_attr = 0;
+
+void launch_vbond_slice(const ChainDev* chains, int nchains, int maxN, int nt, int nf, int visit, int dir,
+                        cudaStream_t st) {
+    const size_t smem = (size_t)2 * maxN * sizeof(double2);
+    if (!g_vb_attr) {
+        cudaFuncSetAttribute(k_vbond_slice, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 512 * (int)sizeof(double2));
+        g_vb_attr = 1;
+    }
+    k_vbond_slice<<<nchains, PLQ_NT, smem, st>>>(chains, nt, nf, visit, dir);
 }

@@ -19,6 +19,9 @@ void launch_update(const ChainDev* chains, int nchains, int nt, int visit, cudaS
 // one slice of plaquette-field props and updates (dir 0: the 0b order, 1: the b0 order)
 void launch_plq_slice(const ChainDev* chains, int nchains, int maxN, int nt, int visit, int dir, int lupdate,
                       cudaStream_t st);
+// the finite-temperature bond-field updates of one family nf at slice nt (dir 0: 0b draws, 1: b0)
+void launch_vbond_slice(const ChainDev* chains, int nchains, int maxN, int nt, int nf, int visit, int dir,
+                        cudaStream_t st);
 // the same on the projective path (UR, UL^T, ULRINV)
 void launch_plq_proj_slice(const ChainDev* chains, int nchains, int maxNe, int nt, int visit, int dir, int lupdate,
                            cudaStream_t st);

@@ -2,7 +2,8 @@
 
 The cases are small versions of the benchmark configurations (square Hubbard
 with checkerboard, FFT or dense kinetic term, exact or general HS field;
-honeycomb SU(4); the 1D chain; the cubic and r_cubic lattices; the plaquette field) sized so the
+honeycomb SU(4); the 1D chain; the cubic and r_cubic lattices; the plaquette field; the t-V bond
+field) sized so the
 oracle finishes each in well under a second.
 """
 import numpy as np
@@ -53,6 +54,19 @@ CASES = {
                                theta=0.2, nflr=2, mu=0.1, kinetic=0, update=1, hs=1, nwrap=5, nublock=4),
     "hc3_plq_dense_exact_fast": dict(lattice=2, l1=3, l2=3, beta=1.0, dtau=0.1, rhub=3.0, rhub_plq=0.8, alpha=0.25,
                                      theta=0.1, nflr=2, kinetic=2, update=0, hs=0, nwrap=5),
+    # the t-V bond field (vconf) beside the U field on the finite-temperature path
+    "hc3_tuv_cb_gen4_delay": dict(lattice=2, l1=3, l2=3, beta=1.0, dtau=0.1, rhub=2.0, rv=0.8, nflr=2,
+                                  kinetic=0, update=1, hs=1, nwrap=5, nublock=4),
+    "sq4_tuv_fft_exact_fast": dict(lattice=1, l1=4, l2=4, beta=1.0, dtau=0.05, rhub=2.0, rv=1.0, mu=0.1, nflr=2,
+                                   kinetic=1, update=0, hs=0, nwrap=10),
+    "ch8_tuv_dense_exact_sub": dict(lattice=3, l1=8, l2=1, beta=1.0, dtau=0.1, rhub=2.0, rv=1.2, nflr=2,
+                                    kinetic=2, update=2, hs=0, nwrap=5, nublock=8),
+    "cu422_tuv_cb_gen4_delay": dict(lattice=4, l1=4, l2=2, l3=2, beta=1.0, dtau=0.1, rhub=3.0, rv=0.7, nflr=2,
+                                    kinetic=0, update=1, hs=1, nwrap=5, nublock=8),
+    # all three fields: plaquettes, bonds and sites in one slice
+    "sq4_plq_tuv_cb_gen4_delay": dict(lattice=1, l1=4, l2=4, beta=1.0, dtau=0.1, rhub=2.0, rv=0.6, rhub_plq=0.8,
+                                      alpha=0.3, theta=0.2, nflr=2, mu=0.1, kinetic=0, update=1, hs=1, nwrap=5,
+                                      nublock=4),
 }
 
 TEST_SEED0 = 1909706392   # abs((0*1981+2008)*951049)

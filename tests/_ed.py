@@ -77,6 +77,35 @@ def trotter_ring(L, t, U, beta, dtau, dense=False):
     return dsum / z, ksum / z / L
 
 
+def trotter_tv_ring(L, t, V, beta, dtau):
+    """(density per site, kinetic energy per site) of the Trotterised spinless
+    t-V ring of L sites at mu = 0, as sampled by the bond field.
+
+    The field of bond b = (i, j) enters the slice as exp(a eta K_b), K_b =
+    c_i^+ c_j + c_j^+ c_i and cosh a = exp(dtau V / 2) (the Hadamard mix, the
+    scale by exp(+-a eta), the mix again).  Summed over eta = +-1 it gives
+    2 cosh(a K_b) = 2 exp(dtau V / 2 K_b^2) with K_b^2 = n_i + n_j - 2 n_i n_j
+    diagonal in the occupation basis, so the slice operator is
+    B = K1 K2 W K2 K1 with W = prod_b exp(dtau V / 2 (n_i + n_j - 2 n_i n_j))."""
+    fam = chain_bonds(L)
+    allb = fam[0] + fam[1]
+    Lt = int(round(beta / dtau))
+    z = nsum = ksum = 0.0
+    for n in range(L + 1):
+        sts = list(combinations(range(L), n))
+        idx = {s: k for k, s in enumerate(sts)}
+        k1, k2 = (expm(-0.5 * dtau * _hop(sts, idx, f, t)) for f in fam)
+        occ = np.array([[1.0 if i in s else 0.0 for i in range(L)] for s in sts]).reshape(len(sts), L)
+        ksq = sum(occ[:, i] + occ[:, j] - 2.0 * occ[:, i] * occ[:, j] for (i, j) in allb)
+        W = np.exp(0.5 * dtau * V * ksq)
+        B = (k1 @ k2) @ (W[:, None] * (k2 @ k1))
+        P = np.linalg.matrix_power(B, Lt)
+        z += np.trace(P)
+        nsum += np.trace(P) * n / L
+        ksum += np.trace(P @ _hop(sts, idx, allb, t))
+    return nsum / z, ksum / z / L
+
+
 def binned_mean(x, nbins=20):
     """Mean and standard error from nbins consecutive bins of the series x."""
     x = np.asarray(x, float)

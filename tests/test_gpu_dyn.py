@@ -33,6 +33,11 @@ DCASES = {
     # the plaquette field's blocks in the propagation of G(tau, 0) and G(0, tau)
     "sq4_plq_gen4": dict(lattice=1, l1=4, l2=4, beta=1.0, dtau=0.1, rhub=4.0, nflr=2, kinetic=0, update=1, hs=1,
                          nwrap=5, nublock=4, rhub_plq=0.8, alpha=0.3, theta=0.2, ltau=1, dyntau=0.8),
+    # the bond field's mix and scale steps in the same propagation
+    "hc3_tuv_cb": dict(lattice=2, l1=3, l2=3, beta=1.0, dtau=0.1, rhub=2.0, rv=0.8, nflr=2, kinetic=0, update=1,
+                       hs=1, nwrap=5, nublock=4, ltau=1, dyntau=1.0),
+    "sq4_tv_fft": dict(lattice=1, l1=4, l2=4, beta=1.0, dtau=0.05, rhub=0.0, rv=1.0, nflr=1, kinetic=1, update=1,
+                       hs=1, nwrap=10, nublock=4, ltau=1, dyntau=0.5),
 }
 
 
@@ -66,6 +71,8 @@ def test_dyn_pass_matches_oracle(sb, oracle, case):
     g.sweep_0b(); [c.sweep_0b() for c in ch]
     for k in range(2):
         assert np.array_equal(g.conf(k), ch[k].conf())
+        if kw.get("rv", 0.0):
+            assert np.array_equal(g.vconf(k), ch[k].vconf())
         assert np.max(np.abs(g.green(k) - ch[k].green())) < 1e-10
 
 

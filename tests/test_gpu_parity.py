@@ -188,6 +188,10 @@ def test_full_sweeps(sb, oracle, case):
         if CASES[case].get("rhub_plq", 0.0):
             assert np.array_equal(g.conf_plq(k), ch[k].conf_plq()), k
             assert dg["accepted_plq"] == dc["accepted_plq"] and dg["proposed_plq"] == dc["proposed_plq"]
+        if CASES[case].get("rv", 0.0):
+            assert np.array_equal(g.vconf(k), ch[k].vconf()), k
+            assert dg["accepted_v"] == dc["accepted_v"] and dg["proposed_v"] == dc["proposed_v"]
+            assert 0 < dg["accepted_v"] < dg["proposed_v"]
         bg, bc = g.bins(k), ch[k].bins()
         assert bg["nobs"] == bc["nobs"]
         for key in ("energy", "cpcm", "nn", "jj", "bb"):

@@ -206,8 +206,10 @@ def test_projective_params():
     import sunhubbardmy_b200 as sb
     p = sb.DqmcParams.make(lattice=2, l1=12, l2=12, beta=20.0, dtau=0.1, rv=1.0, nflr=1, proj=1, update=2)
     assert (p.ndim, p.ne, p.ltrot, p.nst, p.obs_mid_len, p.nublock) == (288, 144, 200, 20, 1, 32)
+    ft = sb.DqmcParams.make(rv=1.0, proj=0)      # the bond field on the finite-temperature path
+    assert (ft.proj, ft.rv) == (0, 1.0)
     with pytest.raises(sb.DqmcError):
-        sb.DqmcParams.make(rv=1.0, proj=0)       # t-V runs on the projective path only
+        sb.DqmcParams.make(lattice=sb.R_CUBIC, l1=2, l2=2, l3=2, rv=1.0)
     with pytest.raises(sb.DqmcError):
         sb.DqmcParams.make(rv=1.0, proj=1, lstabilize=0)
 
