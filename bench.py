@@ -261,69 +261,13 @@ def sweep_roofline(prof: dict, work: dict, names: dict, fp64: float) -> dict:
     return roof
 
 
-class HandleGroup:
-    """Several Dqmc handles whose sweeps run concurrently, each on its own
-    stream (dqmc_gpu_sweeps_multi), behind the per-chain interface of one
-    handle (chain c of the group = chain c - offset of its handle)."""
-
-    def __init__(self, handles, params=None, seeds=None):
-        self.handles = handles
-        self._p, self._seeds = params, seeds
-        self.offsets = []
-        k = 0
-        for h in handles:
-            self.offsets.append(k)
-            k += h.n_chains
-        self.n_chains = k
-        self.params = handles[0].params
-
-    def _h(self, c):
-        for h, o in zip(reversed(self.handles), reversed(self.offsets)):
-            if c >= o:
-                return h, c - o
-        raise IndexError(c)
-
-    def sweeps(self, n, lmeasure=True):
-        import sunhubbardmy_b200 as sb
-        return sb.sweeps_concurrent(self.handles, n, lmeasure)
-
-    def sweep_profile(self, n=1, lmeasure=True):
-        """The per-kind profile of one handle holding all the group's chains
-        (built for it, one sweep after sweep_start)."""
-        import sunhubbardmy_b200 as sb
-        g = sb.Dqmc(self._p, n_chains=self.n_chains, seeds=self._seeds)
-        g.sweep_start()
-        g.obser_init()
-        g.sweeps(1, True)
-        prof = g.sweep_profile(n, lmeasure)
-        g.close()
-        return prof
-
-    def sweep_kernels(self):
-        return sum(h.sweep_kernels() for h in self.handles)
-
-    def __getattr__(self, name):
-        if name in ("sweep_start", "obser_init", "reset_diag", "close"):
-            return lambda *a: [getattr(h, name)(*a) for h in self.handles]
-        if name in ("ndim", "diag", "bins_raw", "vconf"):
-            def f(c=0, *a):
-                h, cc = self._h(c)
-                return getattr(h, name)(cc, *a)
-            return f
-        if name == "set_vconf":
-            def f(v, c):
-                h, cc = self._h(c)
-                return h.set_vconf(v, cc)
-            return f
-        raise AttributeError(name)
-
-
 def make_handle(args, rank: int):
     """The DQMC handle of the selected workload, chains seeded from the
     reference's -DTEST seeds offset by rank; returns (handle, workload, tuning).
     With --streams S > 1 the chains are split over S handles whose sweeps run
     concurrently on their own streams."""
     import sunhubbardmy_b200 as sb
+    from sunhubbardmy_b200.autotune import ChainGroup
     if args.workload == "config4":
         p4 = sb.DqmcParams.make(**CONFIG4)
         nw = args.chains if args.chains_set else 64
@@ -332,13 +276,17 @@ def make_handle(args, rank: int):
             k = nw // S
             seeds = [test_seed(rank * nw + c) for c in range(nw)]
             hs = [sb.Dqmc(p4, n_chains=k, seeds=seeds[j * k:(j + 1) * k]) for j in range(S)]
-            return HandleGroup(hs, p4, seeds), WORKLOAD4 + f", {S} concurrent handles of {k} walkers", None
+            return ChainGroup(hs, [p4] * nw, seeds), WORKLOAD4 + f", {S} concurrent handles of {k} walkers", None
         return sb.Dqmc(p4, n_chains=nw, seeds=[test_seed(rank * nw + c) for c in range(nw)]), WORKLOAD4, None
     if args.workload == "config3":
-        from sunhubbardmy_b200.autotune import batched
+        from sunhubbardmy_b200.autotune import batched, size_classes
         groups = [(sb.DqmcParams.make(**kw), n) for kw, n in CONFIG3]
-        g, tune_report = batched(groups, tune=True, seed0=rank * sum(n for _, n in CONFIG3))
-        return g, WORKLOAD3, tune_report
+        seed0 = rank * sum(n for _, n in CONFIG3)
+        if args.streams == 1:
+            g, tune_report = batched(groups, tune=True, seed0=seed0)
+            return g, WORKLOAD3 + ", one handle", tune_report
+        g, tune_report = size_classes(groups, tune=True, seed0=seed0, split=args.streams)
+        return g, WORKLOAD3 + f", size classes on {len(g.handles)} concurrent streams", tune_report
     p0 = sb.DqmcParams.make(**CONFIG)
     g = sb.Dqmc(p0, n_chains=args.chains, seeds=[test_seed(rank * args.chains + c) for c in range(args.chains)])
     return g, WORKLOAD, None
@@ -647,7 +595,8 @@ def proj_roofline_and_line(args, g, p, Ns, ms, value, per_step, world, workload,
              "prop_right": "k_prop_cols (UL^T)", "measure": "k_transpose_g + k_measure",
              "other": "copies, wrap checks, SFMT"}
     roof = sweep_roofline(g.sweep_profile(1, True), work, names, fp64)
-    if isinstance(g, HandleGroup):
+    from sunhubbardmy_b200.autotune import ChainGroup
+    if isinstance(g, ChainGroup):
         roof["timing"] += f" (one handle of all {len(Ns)} walkers, after one warm-up sweep)"
     trf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(trf):
@@ -786,7 +735,8 @@ def main():
     ap.add_argument("--ess", type=int, default=0, help="extra sweeps for the ESS/s of double occupancy")
     ap.add_argument("--ess-warmup", type=int, default=20, help="equilibration sweeps before the ESS series")
     ap.add_argument("--streams", type=int, default=0,
-                    help="split the chains over this many handles swept concurrently (default: 4 for config4, else 1)")
+                    help="config4: handles of walkers swept concurrently (default 4); config3: handles per size "
+                         "class (default: up to 4 per class, 16 in all; 1: one handle of all chains)")
     ap.add_argument("--profile", default=None,
                     help="single-kernel runs for profiling: comma-separated time_op ids, 'sweep' or 'nn'")
     ap.add_argument("--reps", type=int, default=1, help="--profile: timed launches per operation")

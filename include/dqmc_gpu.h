@@ -259,6 +259,12 @@ double dqmc_gpu_last_sweeps_ms(dqmc_handle* h);
  * *ms_out (may be NULL): device ms per sweep between fork and join.  The
  * reference's counterpart is several MPI ranks sharing a node. */
 int dqmc_gpu_sweeps_multi(dqmc_handle* const* hs, int nh, int n, int lmeasure, double* ms_out);
+/* dqmc_gpu_sweep_start of n handles (1..16) at once
+ * (src/dqmc_ft_core/dqmc_ft_sweep_start_0b.f90, dqmc_proj_sweep_start_0b.f90 per
+ * handle): every handle's start-up is enqueued on its own stream before any is
+ * waited for, so they run concurrently; then each handle's failure status is
+ * read as dqmc_gpu_sweep_start reads it. */
+int dqmc_gpu_sweep_start_multi(dqmc_handle* const* hs, int n);
 /* Number of kernel launches in one captured sweep (b0 + 0b) of dqmc_gpu_sweeps. */
 int dqmc_gpu_sweep_kernels(dqmc_handle* h);
 /* Average device time (ms) of `reps` back-to-back launches of one sweep kernel

@@ -11,7 +11,7 @@ library and fails loudly if it is missing.
 from .dqmc import (  # noqa: F401
     CHAIN, CHECKERBOARD, CUBIC, R_CUBIC, DELAY, DENSE, FAST, FFT, GENERAL4, EXACT, HONEYCOMB, SQUARE, SUBMATRIX,
     EINVAL, ECUDA, ENOMEM, ESTATE, ENUMERIC, EWRAP, FAIL_NONFINITE, FAIL_SINGULAR, FAIL_WRAP,
-    Dqmc, DqmcError, DqmcParams, lib_path, load_library, qr_logdet_noalloc, read_dqmc_in, sweeps_concurrent,
+    Dqmc, DqmcError, DqmcParams, lib_path, load_library, qr_logdet_noalloc, read_dqmc_in, sweep_start_concurrent, sweeps_concurrent,
     test_seed, trial_state,
 )
 from .io import (  # noqa: F401

@@ -1764,7 +1764,7 @@ static void proj_bmat(dqmc_handle* h, ProjPass& pp, int nt1, int nt2) {
 }
 
 // dqmc_proj_sweep_start_0b (src/dqmc_proj_core/dqmc_proj_sweep_start_0b.f90:1-48)
-static int proj_sweep_start(dqmc_handle* h) {
+static int proj_sweep_start(dqmc_handle* h, int sync) {
     const HostModel& m = *h->models[0];
     int nst = h->nst;
     launch_tall_copy(h->d_chains, h->nch, PMAT_UR, PMAT_PROJR, h->st);
@@ -1780,8 +1780,10 @@ static int proj_sweep_start(dqmc_handle* h) {
     launch_proj_ulr(h->d_chains, h->nch, PMAT_ULRINV, 1, nst, -1, h->st);
     launch_proj_green(h->d_chains, h->nch, PMAT_ULRINV, PMAT_GNEW, h->ctas_per_chain, h->st);
     launch_wrap_check(h->d_chains, h->nch, 0, h->st);
-    CK(cudaStreamSynchronize(h->st));
-    CK(cudaGetLastError());
+    if (sync) {
+        CK(cudaStreamSynchronize(h->st));
+        CK(cudaGetLastError());
+    }
     h->started = 1;
     return DQMC_OK;
 }
@@ -1937,9 +1939,10 @@ static void enqueue_proj_0b(dqmc_handle* h, int lupdate, int lmeasure) {
     pflush(h, pp);
 }
 
-static int sweep_start_impl(dqmc_handle* h) {
+// sync = 0: enqueue only (the caller synchronises the handle's stream)
+static int sweep_start_impl(dqmc_handle* h, int sync = 1) {
     h->after_b0 = 0;
-    if (h->proj) return proj_sweep_start(h);
+    if (h->proj) return proj_sweep_start(h, sync);
     const HostModel& m = *h->models[0];
     {
         std::vector<int> sm(h->nst + 2);
@@ -1954,8 +1957,10 @@ static int sweep_start_impl(dqmc_handle* h) {
     }
     launch_green(h->d_chains, h->nch, h->nst, 0, 0, 0, 0, 0, 1, h->st);
     launch_wrap_check(h->d_chains, h->nch, 0, h->st);
-    CK(cudaStreamSynchronize(h->st));
-    CK(cudaGetLastError());
+    if (sync) {
+        CK(cudaStreamSynchronize(h->st));
+        CK(cudaGetLastError());
+    }
     h->started = 1;
     return DQMC_OK;
 }
@@ -2012,6 +2017,32 @@ extern "C" int dqmc_gpu_sweep_start(dqmc_handle* h) {
     clear_fail(h);
     int rc = sweep_start_impl(h); if (rc) return rc;
     return finish_checked(h, 0);
+}
+
+// dqmc_gpu_sweep_start of several handles at once: every handle's work is
+// enqueued on its own stream before any of them is waited for, so the
+// handles' start-ups run concurrently.
+extern "C" int dqmc_gpu_sweep_start_multi(dqmc_handle* const* hs, int n) {
+    if (!hs || n < 1 || n > 16) return fail(DQMC_EINVAL, "1..16 handles");
+    for (int k = 0; k < n; ++k)
+        if (!hs[k]) return fail(DQMC_EINVAL, "null handle");
+    int rc0 = DQMC_OK;
+    for (int k = 0; k < n && !rc0; ++k) {
+        clear_fail(hs[k]);
+        rc0 = sweep_start_impl(hs[k], 0);
+    }
+    // every stream is waited for, also after an enqueue error
+    for (int k = 0; k < n; ++k) {
+        const cudaError_t e = cudaStreamSynchronize(hs[k]->st);
+        if (e != cudaSuccess && !rc0) rc0 = fail(DQMC_ECUDA, cudaGetErrorString(e));
+    }
+    if (rc0) return rc0;
+    CK(cudaGetLastError());
+    for (int k = 0; k < n; ++k) {
+        const int rc = finish_checked(hs[k], 0);
+        if (rc) return rc;
+    }
+    return DQMC_OK;
 }
 
 extern "C" int dqmc_gpu_set_checks(dqmc_handle* h, double wrap_tol, int restabilize) {

@@ -154,6 +154,7 @@ SIGNATURES = {
     "dqmc_gpu_sweep_profile": (_i, [_vp, _i, _i, _vp, _vp]),
     "dqmc_gpu_sweep_dyn": (_i, [_vp]),
     "dqmc_gpu_sweeps_multi": (_i, [_vp, _i, _i, _i, _vp]),
+    "dqmc_gpu_sweep_start_multi": (_i, [_vp, _i]),
     "dqmc_gpu_get_dyn_bins": (_i, [_vp, _i, _vp]),
     "dqmc_gpu_get_dyn_mats": (_i, [_vp, _i, _vp, _vp, _vp]),
     "dqmc_gpu_qr_logdet_noalloc": (_i, [_i, _vp, _vp, _vp, _vp]),
@@ -244,6 +245,13 @@ def sweeps_concurrent(handles, n: int, lmeasure: bool = True) -> float:
     ms = C.c_double()
     _check(load_library().dqmc_gpu_sweeps_multi(arr, len(handles), n, int(lmeasure), C.byref(ms)), "sweeps_multi")
     return ms.value
+
+
+def sweep_start_concurrent(handles) -> None:
+    """dqmc_ft_sweep_start_0b of several Dqmc handles at once, each on its own
+    stream (dqmc_gpu_sweep_start_multi)."""
+    arr = (C.c_void_p * len(handles))(*[g.h for g in handles])
+    _check(load_library().dqmc_gpu_sweep_start_multi(arr, len(handles)), "sweep_start_multi")
 
 
 def trial_state(params: DqmcParams, seed: int, draw_conf: bool = True):

@@ -86,3 +86,41 @@ def test_concurrent_handles_equal_separate_sweeps(sb):
             assert np.array_equal(ga.conf(c), gb.conf(c))
             assert np.max(np.abs(ga.green(c) - gb.green(c))) == 0.0
             assert np.array_equal(ga.bins_raw(c), gb.bins_raw(c))
+
+
+@pytest.mark.parametrize("name", list(GROUPS))
+@pytest.mark.parametrize("split", [1, 2])
+def test_size_classes_on_streams_equal_one_handle(name, split):
+    """The size classes as concurrent handles (autotune.size_classes) give the
+    chains of one handle of all of them (autotune.batched), same seeds: the same
+    HS fields and accept counts, Green's functions and bins equal to rounding
+    (one handle of mixed square sizes propagates with the generic pass, a
+    handle of one size with its size's register FFT pass); the whole-field
+    accessors keep the chain order."""
+    import sunhubbardmy_b200 as sb
+    from sunhubbardmy_b200.autotune import batched, size_classes
+    groups = [(sb.DqmcParams.make(**kw), n) for kw, n in GROUPS[name]]
+    one, _ = batched(groups, tune=False, seed0=5)
+    grp, _ = size_classes(groups, tune=False, seed0=5, split=split)
+    assert grp.n_chains == one.n_chains
+    assert len(grp.handles) == sum(min(split, n) for _, n in groups)
+    for g in (one, grp):
+        g.sweep_start(); g.obser_init()
+        g.sweeps(2, True)
+    for c in range(one.n_chains):
+        assert grp.ndim(c) == one.ndim(c)
+        assert np.array_equal(grp.conf(c), one.conf(c)), c
+        assert np.max(np.abs(grp.green(c) - one.green(c))) < 1e-12, c
+        bg, bo = grp.bins_raw(c), one.bins_raw(c)
+        assert np.max(np.abs(bg - bo)) <= 1e-10 * max(1.0, np.max(np.abs(bo))), c
+        dg, do = grp.diag(c), one.diag(c)
+        assert dg["accepted"] == do["accepted"] and abs(dg["phase"] - do["phase"]) < 1e-12, c
+    ca = grp.conf_all()
+    assert np.array_equal(ca, one.conf_all())
+    ca2 = ca.copy()
+    ca2[::7] = 1
+    grp.set_conf_all(ca2)
+    assert np.array_equal(grp.conf_all(), ca2)
+    assert grp.sweep_kernels() > 0
+    grp.close()
+    one.close()
