@@ -271,7 +271,7 @@ def make_handle(args, rank: int):
     if args.workload == "config4":
         p4 = sb.DqmcParams.make(**CONFIG4)
         nw = args.chains if args.chains_set else 64
-        S = args.streams if args.streams else 4
+        S = args.streams if args.streams else 8
         if S > 1 and nw % S == 0:
             k = nw // S
             seeds = [test_seed(rank * nw + c) for c in range(nw)]
@@ -735,7 +735,7 @@ def main():
     ap.add_argument("--ess", type=int, default=0, help="extra sweeps for the ESS/s of double occupancy")
     ap.add_argument("--ess-warmup", type=int, default=20, help="equilibration sweeps before the ESS series")
     ap.add_argument("--streams", type=int, default=0,
-                    help="config4: handles of walkers swept concurrently (default 4); config3: handles per size "
+                    help="config4: handles of walkers swept concurrently (default 8); config3: handles per size "
                          "class (default: up to 4 per class, 16 in all; 1: one handle of all chains)")
     ap.add_argument("--profile", default=None,
                     help="single-kernel runs for profiling: comma-separated time_op ids, 'sweep' or 'nn'")
