@@ -223,17 +223,21 @@ static __device__ void apply_block(const double2* Vs, const double2* Tp, int N, 
     g.B = X + MIDX(p, c0, N); g.ldb = N; g.opB = OP_N;
     g.C = sc.Ws; g.ldc = QR_NB;
     zgemm_cta<GemmWide>(g, 0, 1, gsm);
-    // W2 = T^H W  or  T W, with T (16 x 16) in shared memory (the staging
-    // buffer is free between the GEMMs)
+    // W2 = T^H W  or  T W, with T^H or T (16 x 16) in shared memory (the
+    // staging buffer is free between the GEMMs); stored as the operator
+    // itself, so that threads of consecutive rows a read consecutive elements
     double2* Ts = gsm;
-    for (int e = threadIdx.x; e < QR_NB * QR_NB; e += blockDim.x) Ts[e] = Tp[e];
+    for (int e = threadIdx.x; e < QR_NB * QR_NB; e += blockDim.x) {
+        const int r = e % QR_NB, q = e / QR_NB;
+        Ts[e] = use_th ? cconj(Tp[q + r * QR_NB]) : Tp[e];
+    }
     __syncthreads();
     for (int e = threadIdx.x; e < jb * nc; e += blockDim.x) {
         int a = e % jb, cc = e / jb;
         const double2* w = sc.Ws + (size_t)cc * QR_NB;
         double2 acc = cmk(0, 0);
         if (use_th) {
-            for (int b = 0; b <= a; ++b) acc = cfma(cconj(Ts[b + a * QR_NB]), w[b], acc);
+            for (int b = 0; b <= a; ++b) acc = cfma(Ts[a + b * QR_NB], w[b], acc);
         } else {
             for (int b = a; b < jb; ++b) acc = cfma(Ts[a + b * QR_NB], w[b], acc);
         }
