@@ -526,6 +526,14 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
         }
         if tune_report is not None:
             result["config"]["autotune"] = {str(k): v for k, v in tune_report.items()}
+        ku = roof.get("kinds", {}).get("update")
+        if ku and ku.get("ms_per_launch") and ku.get("launches"):
+            # the same proposals over the update kernel's own device time in one
+            # sweep (in-sweep CUDA events), without propagation, stabilisation,
+            # Green's functions and measurement
+            upd_s = ku["ms_per_launch"] * ku["launches"] * 1e-3
+            result["update_only"] = {"value": per_step / world / upd_s, "unit": "updates/s",
+                                     "kernel": ku.get("kernel"), "s_per_step": upd_s}
         ess_sweeps = args.ess if args.ess > 0 else (10 if args.workload == "config2" else 0)
         if ess_sweeps > 0:
             from sunhubbardmy_b200.stats import double_occupancy, ess
