@@ -49,9 +49,12 @@ struct ZGemmCfg {
     static constexpr int NT = WM * WN * 32;
     static constexpr int WTM = BM / WM, WTN = BN / WN;
     static constexpr int FM = WTM / 8, FN = WTN / 8;
-    // odd pitch (in 16-byte elements): conflict-free fragment loads and also
-    // conflict-free staging stores of the k-fastest (transposed A, plain B) tiles
-    static constexpr int LDA = BM + 1, LDB = BN + 1;
+    // pitch = 2 (mod 8) in 16-byte elements: a quarter warp's fragment load
+    // (k rows lane & 3, columns lane >> 2) touches 8 distinct 16-byte bank
+    // groups.  (An odd pitch makes the staging stores of transposed operands
+    // conflict-free instead, but doubles the wavefronts of every fragment load,
+    // which run 2-4 times per stored element.)
+    static constexpr int LDA = BM + 2, LDB = BN + 2;
     static constexpr int SA = BK * LDA, SB = BK * LDB;
     static constexpr int SMEM_ELEMS = 2 * (SA + SB);       // double2 elements
     static_assert(BK % 4 == 0 && WTM % 8 == 0 && WTN % 8 == 0, "tile shape");
