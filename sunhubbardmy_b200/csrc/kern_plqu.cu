@@ -240,6 +240,9 @@ __global__ void __launch_bounds__(PLQ_NT) k_vbond_slice(const ChainDev* __restri
     double2 ph = cmk(c.stats[ST_PHASE_RE], c.stats[ST_PHASE_IM]);
     double acc = 0.0, nties = 0.0;
     for (int b = 0; b < lf; ++b) {
+        // every thread has read the previous bond's s_acc (a rejected bond has
+        // no barrier of its own) before thread 0 overwrites it
+        __syncthreads();
         if (tid == 0) {
             const int i1 = rows[2 * b], i2 = rows[2 * b + 1];
             s_pc[0] = i1; s_pc[1] = i2;
