@@ -3,7 +3,8 @@
 //   C[M x N] = alpha * op(A)[M x K] * op(B)[K x N] + beta * C
 //
 // Operand tiles are staged global -> shared with 16-byte cp.async (one complex
-// element per copy, zero-filled outside the matrix) in a two-stage pipeline.
+// element per copy, zero-filled outside the matrix) in a ring of Cfg::NS
+// stages with one CTA barrier per stage.
 // A complex product is four real DMMAs on split real/imaginary fragments:
 //   Cr += Ar Br - Ai Bi,  Ci += Ar Bi + Ai Br.
 // The CTA walks output tiles tile0, tile0+tstep, ..., so a single CTA can do a
@@ -43,9 +44,10 @@ DQ_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 DQ_DEV void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" :: "n"(N)); }
 
-template <int BM_, int BN_, int BK_, int WM_, int WN_>
+template <int BM_, int BN_, int BK_, int WM_, int WN_, int NS_ = 2>
 struct ZGemmCfg {
     static constexpr int BM = BM_, BN = BN_, BK = BK_, WM = WM_, WN = WN_;
+    static constexpr int NS = NS_;                         // staging buffers (pipeline depth)
     static constexpr int NT = WM * WN * 32;
     static constexpr int WTM = BM / WM, WTN = BN / WN;
     static constexpr int FM = WTM / 8, FN = WTN / 8;
@@ -56,8 +58,9 @@ struct ZGemmCfg {
     // which run 2-4 times per stored element.)
     static constexpr int LDA = BM + 2, LDB = BN + 2;
     static constexpr int SA = BK * LDA, SB = BK * LDB;
-    static constexpr int SMEM_ELEMS = 2 * (SA + SB);       // double2 elements
+    static constexpr int SMEM_ELEMS = NS * (SA + SB);      // double2 elements
     static_assert(BK % 4 == 0 && WTM % 8 == 0 && WTN % 8 == 0, "tile shape");
+    static_assert(NS >= 2, "at least two staging buffers");
 };
 
 template <class Cfg>
@@ -115,10 +118,7 @@ __device__ void zgemm_cta(const ZGemmArgs& g, int tile0, int tstep, cplx* smem) 
     const int ntiles = tm * tn;
     const bool conjA = (g.opA == OP_C), conjB = (g.opB == OP_C);
     const bool beta0 = (g.beta.x == 0.0 && g.beta.y == 0.0);
-    cplx* As0 = smem;
-    cplx* Bs0 = smem + Cfg::SA;
-    cplx* As1 = smem + Cfg::SA + Cfg::SB;
-    cplx* Bs1 = smem + 2 * Cfg::SA + Cfg::SB;
+    constexpr int NS = Cfg::NS, SST = Cfg::SA + Cfg::SB;
 
     for (int t = tile0; t < ntiles; t += tstep) {
         const int m0 = (t % tm) * BM, n0 = (t / tm) * BN;
@@ -130,21 +130,29 @@ __device__ void zgemm_cta(const ZGemmArgs& g, int tile0, int tstep, cplx* smem) 
 
         const int kbeg = g.triA ? (m0 / BK) * BK : 0;
         const int nk = (g.K - kbeg + BK - 1) / BK;
-        if (nk > 0) {
-            zgemm_load_stage<Cfg>(g, m0, n0, kbeg, As0, Bs0, tid, nthr);
+        // NS-stage ring: stages 0 .. NS-2 in flight before the first product;
+        // one commit group per stage (empty past the end), so that waiting
+        // until NS-2 groups remain means stage kt has landed
+#pragma unroll
+        for (int st = 0; st < NS - 1; ++st) {
+            if (st < nk) zgemm_load_stage<Cfg>(g, m0, n0, kbeg + st * BK, smem + st * SST, smem + st * SST + Cfg::SA, tid, nthr);
             cp_async_commit();
         }
         for (int kt = 0; kt < nk; ++kt) {
-            cplx* As = (kt & 1) ? As1 : As0;
-            cplx* Bs = (kt & 1) ? Bs1 : Bs0;
-            if (kt + 1 < nk) {
-                zgemm_load_stage<Cfg>(g, m0, n0, kbeg + (kt + 1) * BK, (kt & 1) ? As0 : As1, (kt & 1) ? Bs0 : Bs1, tid, nthr);
-                cp_async_commit();
-                cp_async_wait<1>();
-            } else {
-                cp_async_wait<0>();
-            }
+            cp_async_wait<NS - 2>();
+            // stage kt is visible to every thread, and every warp is done with
+            // stage kt - 1, whose buffer the next load reuses
             __syncthreads();
+            {
+                const int st = kt + NS - 1;
+                if (st < nk) {
+                    cplx* b = smem + (st % NS) * SST;
+                    zgemm_load_stage<Cfg>(g, m0, n0, kbeg + st * BK, b, b + Cfg::SA, tid, nthr);
+                }
+                cp_async_commit();
+            }
+            const cplx* As = smem + (kt % NS) * SST;
+            const cplx* Bs = As + Cfg::SA;
             if (mathw) {
 #pragma unroll
                 for (int kk = 0; kk < BK; kk += 4) {
@@ -180,8 +188,9 @@ __device__ void zgemm_cta(const ZGemmArgs& g, int tile0, int tstep, cplx* smem) 
                         for (int b = 0; b < FN; ++b) dmma(acci[a][b][0], acci[a][b][1], ai[a], br[b]);
                 }
             }
-            __syncthreads();
         }
+        // the next tile's first stages overwrite the buffers of the last ones
+        __syncthreads();
         // epilogue straight from the accumulators: C(m, n) = alpha acc + beta C;
         // the 8 lanes of a (lane & 3) group store 8 consecutive rows of a column
         if (mathw) {
