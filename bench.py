@@ -348,7 +348,7 @@ def single_chain_block(args, result: dict, Ns, lt: int) -> dict:
     g1.sweeps(2, True)
     torch.cuda.synchronize()
     n = 3
-    ms = g1.sweeps(n, True) / n
+    ms = g1.sweeps(n, True)          # device ms per sweep
     per = 2 * lt * int(Ns[0])
     conf = torch.empty(lt * int(Ns[0]), dtype=torch.int32, pin_memory=True).numpy()
     g1.conf_all(conf)
