@@ -468,3 +468,18 @@ def test_replay_driver_makes_the_reference_call_order(tmp_path):
     assert lines[0].startswith("bin 1 ") and lines[1].startswith("bin 2 ")
     conf = (tmp_path / "conf_u.out").read_text().split()
     assert conf[0] == "1" and len(conf) == 1 + 16 * 10
+
+
+def test_multi_handle_entry_points_check_their_arguments():
+    """dqmc_gpu_sweep_start_multi and dqmc_gpu_sweeps_multi refuse an empty or
+    oversized handle list (1..16) and null handles before any device work."""
+    import ctypes as C
+    import sunhubbardmy_b200 as sb
+    L = sb.load_library()
+    nulls = (C.c_void_p * 17)()
+    for n in (0, 17):
+        assert L.dqmc_gpu_sweep_start_multi(nulls, n) == sb.EINVAL
+        assert L.dqmc_gpu_sweeps_multi(nulls, n, 1, 1, None) == sb.EINVAL
+    assert L.dqmc_gpu_sweep_start_multi(None, 1) == sb.EINVAL
+    assert L.dqmc_gpu_sweep_start_multi(nulls, 2) == sb.EINVAL      # null handles
+    assert L.dqmc_gpu_sweeps_multi(nulls, 2, 1, 1, None) == sb.EINVAL
