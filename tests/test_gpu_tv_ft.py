@@ -31,6 +31,12 @@ TCASES = {
                              nwrap=5, nublock=8),
     "cu422_tv_cb_delay": dict(lattice=4, l1=4, l2=2, l3=2, beta=0.8, dtau=0.1, rv=1.0, nflr=1, kinetic=0,
                               update=1, nwrap=4, nublock=4),
+    # a ragged last stabilisation interval (ltrot = 13, nwrap = 5) on a larger honeycomb, with the U field
+    "hc6_tuv_ragged": dict(lattice=2, l1=6, l2=6, beta=1.3, dtau=0.1, rhub=2.0, rv=0.8, nflr=2, kinetic=0,
+                           update=1, hs=1, nwrap=5, nublock=16),
+    # a stabilisation after every slice
+    "sq4_tv_nwrap1": dict(lattice=1, l1=4, l2=4, beta=0.4, dtau=0.1, rv=1.0, nflr=1, kinetic=1, update=2,
+                          nwrap=1, nublock=8),
 }
 
 
