@@ -66,6 +66,38 @@ struct CellShift {
     }
 };
 
+// The cells cj = c0, c0 + st, c0 + 2 st, ... with their shifts ci = shift(cj),
+// walked with carries instead of a division per cell: the coordinates of cj
+// advance with carry (j2, then j1, then j3), and each coordinate of ci is the
+// matching one of cj plus the shift, less the length once (the shift is at
+// most the length).
+template <bool D3>
+struct CellWalk {
+    int j1, j2, j3, l1, l2, l3, dxp, dyp, dzp;
+    DQ_DEV CellWalk(const CellShift<D3>& s, int c0)
+        : l1(s.l1), l2(s.l2), l3(s.l3), dxp(s.dxp), dyp(s.dyp), dzp(s.dzp) {
+        j2 = c0 % l2;
+        j1 = D3 ? (c0 / l2) % l1 : c0 / l2;
+        j3 = D3 ? c0 / (l1 * l2) : 0;
+    }
+    DQ_DEV int ci() const {
+        int i1 = j1 + dxp, i2 = j2 + dyp;
+        if (i1 >= l1) i1 -= l1;
+        if (i2 >= l2) i2 -= l2;
+        if (!D3) return i1 * l2 + i2;
+        int i3 = j3 + dzp;
+        if (i3 >= l3) i3 -= l3;
+        return (i3 * l1 + i1) * l2 + i2;
+    }
+    DQ_DEV void step(int st) {
+        j2 += st;
+        while (j2 >= l2) {
+            j2 -= l2;
+            if (++j1 == l1) { j1 = 0; if (D3) ++j3; }
+        }
+    }
+};
+
 // Energy terms and the background sums zn, zj, zb (single numbers per chain),
 // computed by the chain's second CTA while the first one sums the bins.
 DQ_DEV void meas_energy(const ChainDev& c, double2 zphi, double sgn) {
@@ -222,9 +254,10 @@ DQ_DEV void meas_site(const ChainDev& c, int bin, double2 zphi) {   // bin of th
     const double fd = (shift(0) == 0 && a == b) ? 1.0 : 0.0;
     double2 s1 = cmk(0, 0), sB = cmk(0, 0), sA = cmk(0, 0), s4 = cmk(0, 0);
     if (NO == 1) {
+        CellWalk<D3> w(shift, h);
 #pragma unroll 4
-        for (int cj = valid ? h : lq; cj < lq; cj += MEAS_SPLIT) {
-            const int i = shift(cj) * NS + a, j = cj * NS + b;
+        for (int cj = valid ? h : lq; cj < lq; cj += MEAS_SPLIT, w.step(MEAS_SPLIT)) {
+            const int i = w.ci() * NS + a, j = cj * NS + b;
             const size_t o = (size_t)i + (size_t)N * j;
             double2 gtc = GT[o];
             const double2 g = G[o];
@@ -238,8 +271,9 @@ DQ_DEV void meas_site(const ChainDev& c, int bin, double2 zphi) {   // bin of th
         // every orbital pair (oa, ob) of the cell pair (j + d, j); i == j only
         // for d = 0 and oa == ob
         const bool d0 = shift(0) == 0;
-        for (int cj = valid ? h : lq; cj < lq; cj += MEAS_SPLIT) {
-            const int ci = shift(cj);
+        CellWalk<D3> w(shift, h);
+        for (int cj = valid ? h : lq; cj < lq; cj += MEAS_SPLIT, w.step(MEAS_SPLIT)) {
+            const int ci = w.ci();
             for (int ob = 0; ob < NO; ++ob) {
                 const int j = cj * NO + ob;
 #pragma unroll
@@ -311,9 +345,10 @@ DQ_DEV void meas_bond(const ChainDev& c, int d, double2 zphi) {   // distance of
         f00 = ci == 0; fn0 = in == 0; f0n = ci == jn; fnn = in == jn;
     }
     double2 sj = cmk(0, 0), sb = cmk(0, 0), sn = cmk(0, 0), ss = cmk(0, 0);
+    CellWalk<D3> w(shift, h);
 #pragma unroll 4
-    for (int cj = valid ? h : lq; cj < lq; cj += MEAS_SPLIT) {
-        const int ci = shift(cj);
+    for (int cj = valid ? h : lq; cj < lq; cj += MEAS_SPLIT, w.step(MEAS_SPLIT)) {
+        const int ci = w.ci();
         const int j0 = cj * NS, i0 = ci * NS, jnj = pj[cj], inj = pj[ci];
         const double2 ei = pe[ci], ej = pe[cj];
         // G and GTc = GT - delta (= -Gc) at rows i0, in of columns j0, jn
