@@ -2054,6 +2054,16 @@ extern "C" int dqmc_gpu_set_checks(dqmc_handle* h, double wrap_tol, int restabil
     return DQMC_OK;
 }
 
+// one bond family's finite-temperature updates: delayed when every model's
+// flush depth holds two columns (dqmc_update_delay.f90), else rank-2 changes
+// straight on G (dqmc_update.f90)
+static void launch_vbond(dqmc_handle* h, int nt, int nf, int visit, int dir) {
+    int nbmin = 64;
+    for (const HostModel* m : h->models) nbmin = std::min(nbmin, m->nublock_dev);
+    if (!launch_vbond_delay(h->d_chains, h->nch, nbmin, nt, nf, visit, dir, h->st))
+        launch_vbond_slice(h->d_chains, h->nch, h->maxN, nt, nf, visit, dir, h->st);
+}
+
 static void enqueue_b0(dqmc_handle* h, int lupdate, int lmeasure) {
     const HostModel& m = *h->models[0];
     int lt = h->ltrot;
@@ -2085,7 +2095,7 @@ static void enqueue_b0(dqmc_handle* h, int lupdate, int lmeasure) {
                     launch_prog(h, MAT_G, pl, 0);
                     launch_prog(h, MAT_G, pr, 1);
                     tmark(h, DQMC_PROF_PROP_L);
-                    launch_vbond_slice(h->d_chains, h->nch, h->maxN, nt, nf, visit, 1, h->st);
+                    launch_vbond(h, nt, nf, visit, 1);
                     tmark(h, DQMC_PROF_UPDATE);
                     pl.n = 0; pr.n = 0;
                 }
@@ -2148,7 +2158,7 @@ static void enqueue_0b(dqmc_handle* h, int lupdate, int lmeasure) {
                     launch_prog(h, MAT_G, pl, 0);
                     launch_prog(h, MAT_G, pr, 1);
                     tmark(h, DQMC_PROF_PROP_L);
-                    launch_vbond_slice(h->d_chains, h->nch, h->maxN, nt, nf, visit, 0, h->st);
+                    launch_vbond(h, nt, nf, visit, 0);
                     tmark(h, DQMC_PROF_UPDATE);
                     pl.n = 0; pr.n = 0;
                 }

@@ -379,6 +379,134 @@ __global__ void __launch_bounds__(UPD_NT, 2) k_update_flush(const ChainDev* __re
     flush_addto(c.G, c.A, c.B, c.N, c.md->nublock, dsm);
 }
 
+// The t-V bond field's updates of one family nf at slice nt, delayed
+// (src/dqmc_config_v/dqmc_update_delay.f90:30-112): one CTA per chain, the
+// bonds in nnlf_list order.  The accepted rank-2 changes are carried as
+// columns of (A, B), G' = G + A B^T: bond b's 2 x 2 block of G' is
+// G(P,P) + A(P,:) B(P,:)^T (warp 0, lanes over the delayed columns), the ratio
+// det(I + (1 - G')(P,P) Delta) and S = Delta (I + ...)^-1 are thread 0's, and an
+// accepted bond appends the columns a_q = sum_p G'(:,P_p) S(p,q) and
+// b_q = G'(P_q,:)^T - e_(P_q) (whole CTA).  After nublock columns (rounded down
+// to even) and at the family's end the factors are flushed, G += A B^T, on the
+// FP64 tensor pipe.  Iflip is 1 for the two-valued field; bond k uses the
+// words 2k (iflip) and 2k + 1 (accept test) of the family's draws (0b layout:
+// families ascending after the plaquette words; b0: descending after the U
+// field's).
+__global__ void __launch_bounds__(UPD_NT, 2) k_vbond_delay(const ChainDev* __restrict__ chains, int nt, int nf, int visit,
+                                                           int dir) {
+    extern __shared__ double2 dsm[];                  // flush staging
+    __shared__ double2 s_ap[2][64], s_bp[2][64];      // A(P_q, m), B(P_q, m) of the current bond
+    __shared__ double2 s_mat[4];
+    __shared__ int s_pc[2], s_acc;
+    const ChainDev& c = chains[blockIdx.x];
+    const ModelDev& md = *c.md;
+    if (!md.lwrapv || !c.vconf) return;
+    const int N = c.N, lf = md.nn_lf, nnf = md.nn_nf, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nbv = min(md.nublock, 64) & ~1;         // delayed columns per flush (even)
+    double2 *G = c.G, *A = c.A, *B = c.B;
+    int32_t* cf = c.vconf + ((size_t)(nt - 1) * nnf + (nf - 1)) * N;
+    const int* rows = md.vrows + (size_t)(nf - 1) * 2 * lf;
+    const uint32_t* rw = c.rnd + (size_t)visit * md.rps + md.rw_v[dir] + (size_t)(dir ? nnf - nf : nf - 1) * 2 * lf;
+    double2 ph = cmk(c.stats[ST_PHASE_RE], c.stats[ST_PHASE_IM]);
+    double acc = 0.0, nties = 0.0;
+    int k = 0;
+    for (int b = 0; b < lf; ++b) {
+        // every thread is done with the previous bond's shared values
+        __syncthreads();
+        const int i1 = rows[2 * b], i2 = rows[2 * b + 1];
+        if (warp == 0) {
+            // the bond's rows of the delayed factors, and G'(P,P)
+            double2 g[4] = {cmk(0, 0), cmk(0, 0), cmk(0, 0), cmk(0, 0)};   // (0,0) (1,0) (0,1) (1,1)
+            for (int m = lane; m < k; m += 32) {
+                const double2 a0 = A[MIDX(i1, m, N)], a1 = A[MIDX(i2, m, N)];
+                const double2 b0 = B[MIDX(i1, m, N)], b1 = B[MIDX(i2, m, N)];
+                s_ap[0][m] = a0; s_ap[1][m] = a1; s_bp[0][m] = b0; s_bp[1][m] = b1;
+                g[0] = cfma(a0, b0, g[0]); g[1] = cfma(a1, b0, g[1]);
+                g[2] = cfma(a0, b1, g[2]); g[3] = cfma(a1, b1, g[3]);
+            }
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                g[e].x = warp_sum(g[e].x);
+                g[e].y = warp_sum(g[e].y);
+            }
+            if (lane == 0) {
+                s_pc[0] = i1; s_pc[1] = i2;
+                const double2 g11 = cadd(G[MIDX(i1, i1, N)], g[0]), g21 = cadd(G[MIDX(i2, i1, N)], g[1]);
+                const double2 g12 = cadd(G[MIDX(i1, i2, N)], g[2]), g22 = cadd(G[MIDX(i2, i2, N)], g[3]);
+                const int is = cf[b];
+                const double2 d0 = md.vdp[is - 1], d1 = md.vdm[is - 1];
+                const double2 v00 = cadd(cmk(1, 0), cmul(cmk(1.0 - g11.x, -g11.y), d0));
+                const double2 v10 = cmul(cmk(-g21.x, -g21.y), d0);
+                const double2 v01 = cmul(cmk(-g12.x, -g12.y), d1);
+                const double2 v11 = cadd(cmk(1, 0), cmul(cmk(1.0 - g22.x, -g22.y), d1));
+                const double2 det = csub(cmul(v00, v11), cmul(v01, v10));
+                const double2 id = cdiv(cmk(1, 0), det);
+                s_mat[0] = cmul(d0, cmul(v11, id));              // S = Delta vukmat^-1, column-major
+                s_mat[1] = cmul(d1, cmul(cmk(-v10.x, -v10.y), id));
+                s_mat[2] = cmul(d0, cmul(cmk(-v01.x, -v01.y), id));
+                s_mat[3] = cmul(d1, cmul(v00, id));
+                const double ra = fabs(cmul(det, ph).x / ph.x), r = u32_to_stream(rw[2 * b + 1]);
+                if (fabs(ra - r) < DQ_NEAR_TIE) nties += 1.0;
+                s_acc = ra > r;
+                if (s_acc) {
+                    acc += 1.0;
+                    ph = cscale(cmul(ph, det), 1.0 / sqrt(cmulc(det, det).x));
+                    cf[b] = is % 2 + 1;
+                }
+            }
+        }
+        __syncthreads();
+        if (s_acc) {
+            const int p0 = s_pc[0], p1 = s_pc[1];
+            const double2 S00 = s_mat[0], S10 = s_mat[1], S01 = s_mat[2], S11 = s_mat[3];
+            for (int i = tid; i < N; i += blockDim.x) {
+                double2 c0 = G[MIDX(i, p0, N)], c1 = G[MIDX(i, p1, N)];      // G'(i, P)
+                double2 r0 = G[MIDX(p0, i, N)], r1 = G[MIDX(p1, i, N)];      // G'(P, i)
+                for (int m = 0; m < k; ++m) {
+                    const double2 ai = A[MIDX(i, m, N)], bi = B[MIDX(i, m, N)];
+                    c0 = cfma(ai, s_bp[0][m], c0); c1 = cfma(ai, s_bp[1][m], c1);
+                    r0 = cfma(s_ap[0][m], bi, r0); r1 = cfma(s_ap[1][m], bi, r1);
+                }
+                if (i == p0) r0.x -= 1.0;
+                if (i == p1) r1.x -= 1.0;
+                A[MIDX(i, k, N)] = cadd(cmul(c0, S00), cmul(c1, S10));
+                A[MIDX(i, k + 1, N)] = cadd(cmul(c0, S01), cmul(c1, S11));
+                B[MIDX(i, k, N)] = r0;
+                B[MIDX(i, k + 1, N)] = r1;
+            }
+            k += 2;
+            __syncthreads();
+        }
+        if (k > 0 && (k + 2 > nbv || b == lf - 1)) {
+            flush_addto(G, A, B, N, k, dsm);
+            k = 0;
+        }
+    }
+    if (tid == 0) {
+        c.stats[ST_PHASE_RE] = ph.x;
+        c.stats[ST_PHASE_IM] = ph.y;
+        c.stats[ST_ACCV] += acc;
+        c.stats[ST_PROPV] += lf;
+        c.stats[ST_NEAR_TIE] += nties;
+    }
+}
+
+static int g_vbd_attr = 0;
+
+// the delayed bond updates when the flush depth allows two columns, else the
+// rank-2 updates straight on G (kern_plqu.cu)
+int launch_vbond_delay(const ChainDev* chains, int nchains, int nublock, int nt, int nf, int visit, int dir,
+                       cudaStream_t st) {
+    if ((min(nublock, 64) & ~1) < 2) return 0;
+    const size_t smem = UpdGemm::SMEM_ELEMS * sizeof(double2);
+    if (!g_vbd_attr) {
+        cudaFuncSetAttribute(k_vbond_delay, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        g_vbd_attr = 1;
+    }
+    k_vbond_delay<<<nchains, UPD_NT, smem, st>>>(chains, nt, nf, visit, dir);
+    return 1;
+}
+
 static int g_upd_attr = 0;
 
 void launch_update(const ChainDev* chains, int nchains, int nt, int visit, cudaStream_t st, int forced, int dir) {

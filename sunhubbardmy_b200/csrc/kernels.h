@@ -22,6 +22,10 @@ void launch_plq_slice(const ChainDev* chains, int nchains, int maxN, int nt, int
 // the finite-temperature bond-field updates of one family nf at slice nt (dir 0: 0b draws, 1: b0)
 void launch_vbond_slice(const ChainDev* chains, int nchains, int maxN, int nt, int nf, int visit, int dir,
                         cudaStream_t st);
+// the same, delayed (rank-2 columns flushed by a DMMA GEMM); returns 0 without
+// launching when nublock leaves fewer than two delayed columns
+int launch_vbond_delay(const ChainDev* chains, int nchains, int nublock, int nt, int nf, int visit, int dir,
+                       cudaStream_t st);
 // the same on the projective path (UR, UL^T, ULRINV)
 void launch_plq_proj_slice(const ChainDev* chains, int nchains, int maxNe, int nt, int visit, int dir, int lupdate,
                            cudaStream_t st);
