@@ -36,6 +36,12 @@ CONFIG = dict(lattice=1, l1=16, l2=16, beta=10.0, dtau=0.05, rhub=4.0, nflr=2, m
               kinetic=1, update=1, hs=1, nwrap=10, nublock=32)
 WORKLOAD = "square L=16 (N=256) SU(2) Hubbard U=4 beta=10 dtau=0.05 (ltrot=200) FFT kinetic, delay nublock=32, general 4-comp HS, nwrap=10"
 METRIC = "HS site-slice updates/s"
+# finite-temperature spinless t-V on the honeycomb lattice (the bond field's
+# delayed updates; not one of the reference's benchmark configurations):
+# L = 12 (N = 288), V = 1, beta = 4, dtau = 0.1, checkerboard, nublock = 32, 64 chains
+CONFIG_TV = dict(lattice=2, l1=12, l2=12, beta=4.0, dtau=0.1, rv=1.0, nflr=1, kinetic=0, update=1, nwrap=10,
+                 nublock=32)
+WORKLOAD_TV = "honeycomb L=12 (N=288) spinless t-V V=1 beta=4 dtau=0.1 (ltrot=40), finite temperature, delayed bond updates nublock=32"
 # batched configuration: SU(4) Hubbard, honeycomb L = 6/9/12 (N = 72/162/288,
 # 48/48/32 chains), U = 6, beta = 8, dtau = 0.1, exact 4-component HS,
 # submatrix update with the flush depth autotuned over {16, 32, 64}
@@ -278,6 +284,10 @@ def make_handle(args, rank: int):
             hs = [sb.Dqmc(p4, n_chains=k, seeds=seeds[j * k:(j + 1) * k]) for j in range(S)]
             return ChainGroup(hs, [p4] * nw, seeds), WORKLOAD4 + f", {S} concurrent handles of {k} walkers", None
         return sb.Dqmc(p4, n_chains=nw, seeds=[test_seed(rank * nw + c) for c in range(nw)]), WORKLOAD4, None
+    if args.workload == "tvft":
+        ptv = sb.DqmcParams.make(**CONFIG_TV)
+        nw = args.chains if args.chains_set else 64
+        return sb.Dqmc(ptv, n_chains=nw, seeds=[test_seed(rank * nw + c) for c in range(nw)]), WORKLOAD_TV, None
     if args.workload == "config3":
         from sunhubbardmy_b200.autotune import batched, size_classes
         groups = [(sb.DqmcParams.make(**kw), n) for kw, n in CONFIG3]
@@ -414,7 +424,8 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms = float(t.item())
     proj = bool(p.proj)
-    if proj:
+    bond = p.rv != 0 and (proj or p.rhub == 0)     # the bond field's proposals are the unit
+    if proj or p.rv != 0:
         nnf = 3 if p.lattice == 2 else 4
         units = np.array([(nnf * (Nc // 2 if p.lattice == 2 else Nc // 2) if p.rv != 0 else 0) +
                           (Nc if p.rhub != 0 else 0) for Nc in Ns])
@@ -425,7 +436,7 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
     kernels_per_sweep = g.sweep_kernels()
     d0 = g.diag(0)
     wrap = max(g.diag(c)["max_wrap_error"] for c in range(C))
-    if proj and p.rv != 0:
+    if bond:
         acc = d0["accepted_v"] / max(1.0, d0["proposed_v"])
     else:
         acc = d0["accepted"] / max(1.0, d0["proposed"])
@@ -434,7 +445,7 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
     # HS field, sweep_start + one sweep, d2h of every chain's bins and field
     nbins = sum(len(g.bins_raw(c)) for c in range(C)) / C
     e2e_steps = max(1, min(args.steps, 5))
-    if proj and p.rv != 0:
+    if bond:
         # the bond field of every walker (vconf%conf), walker by walker
         vhost = [torch.empty(g.vconf(c).shape, dtype=torch.int32, pin_memory=True).numpy() for c in range(C)]
         for c in range(C):
@@ -476,11 +487,14 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
         result = proj_roofline_and_line(args, g, p, Ns, ms, value, per_step, world, workload, acc, wrap,
                                         kernels_per_sweep, clk, e2e_s, nconf, nbins)
     elif rank == 0:
-        acc_c = np.array([g.diag(c)["accepted"] / max(1.0, g.diag(c)["proposed"]) for c in range(C)])
+        ka, kp = ("accepted_v", "proposed_v") if bond else ("accepted", "proposed")
+        acc_c = np.array([g.diag(c)[ka] / max(1.0, g.diag(c)[kp]) for c in range(C)])
         fp64 = fp64_peak_tflops()
         N2, N3 = float((Ns ** 2).sum()), float((Ns ** 3).sum())     # sums over chains
         work = {   # algorithmic work of one launch group over all chains: (flops, bytes)
-            "update": (8.0 * float((acc_c * Ns ** 3).sum()), None),   # flush GEMMs: 8 N^2 per accepted site
+            # flush GEMMs: 8 N^2 per accepted site, or 16 N^2 per accepted bond of a
+            # family of N / 2 bonds (the honeycomb t-V launch covers one family)
+            "update": (8.0 * float((acc_c * Ns ** 3).sum()), None),
             "stab": ((14.0 + 2.0 / 3.0) * N3, None),   # QR 16/3, Q 16/3, triangular (D^-1 R) V 4
             "green": ((41.0 + 1.0 / 3.0) * N3, None),
             "prop_left": (None, 32.0 * N2), "prop_right": (None, 32.0 * N2), "bprod": (None, 32.0 * N2),
@@ -496,7 +510,7 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
             fft_op = 20.0 * l * l * np.log2(l) + 6.0 * l * l
             per_vec = p.nwrap * (2.0 * fft_op + 6.0 * l * l)
             work["bprod"] = (per_vec * float(Ns.sum()), None)
-        names = {"update": "k_update_delay", "stab": "k_stab", "green": "k_green",
+        names = {"update": "k_vbond_delay (one bond family)" if bond else "k_update_delay", "stab": "k_stab", "green": "k_green",
                  "prop_left": "k_prop_fft (columns)" if p.kinetic == 1 else "k_prop_cols",
                  "prop_right": "k_prop_fft (rows)" if p.kinetic == 1 else "k_prop_rows",
                  "bprod": "B product of the stabilisation (k_prop_fft over nwrap slices)", "measure": "k_transpose_g + k_measure",
@@ -519,7 +533,9 @@ def gpu_arm(args, rank: int, world: int, local_rank: int) -> None:
             "e2e": {"value": per_step / e2e_s, "unit": "updates/s",
                     "h2d_bytes_per_step": nconf * 4,
                     "d2h_bytes_per_step": int(C * nbins * 16 + nconf * 4),
-                    "note": "per step: set_conf_all (pinned host) + sweep_start + 1 sweep + get_bins + get_conf_all"},
+                    "note": ("per step: set_vconf of every chain (pinned host) + sweep_start + 1 sweep + get_bins + get_vconf"
+                             if bond else
+                             "per step: set_conf_all (pinned host) + sweep_start + 1 sweep + get_bins + get_conf_all")},
             "gpu_launches": kernels_per_sweep * args.steps,
             "roofline": roof,
             "clocks": clk.summary(),
@@ -734,7 +750,7 @@ def main():
     ap.add_argument("--chains", type=int, default=None)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "config5"])
+    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "config5", "tvft"])
     ap.add_argument("--pairs", type=int, default=200000, help="config5: training-pair ring capacity")
     ap.add_argument("--train-steps", type=int, default=3000, help="config5: Adam steps of 32 pairs")
     ap.add_argument("--lr", type=float, default=3e-4, help="config5: Adam learning rate")
