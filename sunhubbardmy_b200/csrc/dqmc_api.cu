@@ -2054,6 +2054,16 @@ extern "C" int dqmc_gpu_set_checks(dqmc_handle* h, double wrap_tol, int restabil
     return DQMC_OK;
 }
 
+// one slice of the plaquette field in the finite-temperature sweep: delayed
+// updates when every model's flush depth holds a plaquette's z columns, else
+// rank-z changes straight on G (and the props alone without updates)
+static void launch_plq(dqmc_handle* h, int nt, int visit, int dir, int lupdate) {
+    int nbmin = 64;
+    for (const HostModel* m : h->models) nbmin = std::min(nbmin, m->nublock_dev);
+    if (!lupdate || !launch_plq_delay(h->d_chains, h->nch, nbmin, h->models[0]->z_plq, nt, visit, dir, h->st))
+        launch_plq_slice(h->d_chains, h->nch, h->maxN, nt, visit, dir, lupdate, h->st);
+}
+
 // one bond family's finite-temperature updates: delayed when every model's
 // flush depth holds two columns (dqmc_update_delay.f90), else rank-2 changes
 // straight on G (dqmc_update.f90)
@@ -2110,7 +2120,7 @@ static void enqueue_b0(dqmc_handle* h, int lupdate, int lmeasure) {
             launch_prog(h, MAT_G, pl, 0);
             launch_prog(h, MAT_G, pr, 1);
             tmark(h, DQMC_PROF_PROP_L);
-            launch_plq_slice(h->d_chains, h->nch, h->maxN, nt, visit, 1, lupdate, h->st);
+            launch_plq(h, nt, visit, 1, lupdate);
             tmark(h, DQMC_PROF_UPDATE);
             pl.n = 0; pr.n = 0;
         }
@@ -2142,7 +2152,7 @@ static void enqueue_0b(dqmc_handle* h, int lupdate, int lmeasure) {
             launch_prog(h, MAT_G, pl, 0);
             launch_prog(h, MAT_G, pr, 1);
             tmark(h, DQMC_PROF_PROP_L);
-            launch_plq_slice(h->d_chains, h->nch, h->maxN, nt, visit, 0, lupdate, h->st);
+            launch_plq(h, nt, visit, 0, lupdate);
             tmark(h, DQMC_PROF_UPDATE);
             pl.n = 0; pr.n = 0;
         }

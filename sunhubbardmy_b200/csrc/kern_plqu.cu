@@ -15,6 +15,7 @@
 // k_plq_slice runs the interleaved props and updates of one slice for one
 // chain per CTA.
 #include "chain_access.cuh"
+#include "flush.cuh"
 #include "kernels.h"
 
 #define PLQ_NT 256
@@ -210,6 +211,146 @@ __global__ void __launch_bounds__(PLQ_NT) k_plq_slice(const ChainDev* __restrict
             c.stats[ST_PROPP] += lq;
             c.stats[ST_NEAR_TIE] += nties;
         }
+    }
+}
+
+// One slice of plaquette props and updates for one chain (one CTA per chain),
+// delayed: G' = G + A B^T with the accepted rank-z changes as columns of
+// (A, B), flushed by the DMMA GEMM after nublock columns and at the slice's
+// end (the plaquette counterpart of dqmc_update_delay.f90).  A block on the
+// rows P of G' acts on the rows P of G and of A; a block on its columns P acts
+// on the columns P of G and, transposed, on the rows P of B.  Plaquette p's
+// z x z block of G' is G(P,P) + A(P,:) B(P,:)^T; an accepted plaquette appends
+// a_q = sum_p G'(:,P_p) S(p,q) and b_q = G'(P_q,:)^T - e_(P_q).  Order, draws
+// and decisions as k_plq_slice (lupdate = 1).
+__global__ void __launch_bounds__(PLQ_NT, 2) k_plq_delay(const ChainDev* __restrict__ chains, int nt, int visit, int dir) {
+    extern __shared__ double2 dsm[];                   // flush staging
+    __shared__ double2 s_ap[PLQ_ZMAX][64], s_bp[PLQ_ZMAX][64];   // A(P_a, m), B(P_a, m)
+    __shared__ double2 s_g[PLQ_ZMAX * PLQ_ZMAX];       // G'(P,P), column-major
+    __shared__ double2 s_mat[PLQ_ZMAX * PLQ_ZMAX];
+    __shared__ int s_acc;
+    const ChainDev& c = chains[blockIdx.x];
+    const ModelDev& md = *c.md;
+    if (!md.plq) return;
+    const int N = c.N, z = md.plq_z, lq = md.lq, lc = md.plq_lcomp, tid = threadIdx.x;
+    const int nbv = min(md.nublock, 64);
+    double2 *G = c.G, *A = c.A, *B = c.B;
+    int32_t* cf = c.conf_plq + (size_t)(nt - 1) * lq;
+    const uint32_t* rw = c.rnd + (size_t)visit * md.rps + md.rw_plq[dir];
+    double2 ph = cmk(c.stats[ST_PHASE_RE], c.stats[ST_PHASE_IM]);
+    double acc = 0.0, nties = 0.0;
+    int k = 0;
+    for (int kp = 0; kp < lq; ++kp) {
+        const int p = dir ? lq - 1 - kp : kp;
+        const int* pc = md.plq_cord + p * z;
+        __syncthreads();
+        if (!dir) {
+            const double2* M = md.plq_bmat + (size_t)(cf[p] - 1) * z * z;
+            const double2* Mi = md.plq_bmat_inv + (size_t)(cf[p] - 1) * z * z;
+            plq_rows(G, N, N, pc, z, M);
+            if (k) plq_rows(A, N, k, pc, z, M);
+            plq_cols(G, N, pc, z, Mi);
+            if (k) plq_rows(B, N, k, pc, z, Mi, true);
+        }
+        // the plaquette's rows of the delayed factors and its block of G'
+        for (int e = tid; e < z * k; e += blockDim.x) {
+            const int a = e % z, m = e / z;
+            s_ap[a][m] = A[MIDX(pc[a], m, N)];
+            s_bp[a][m] = B[MIDX(pc[a], m, N)];
+        }
+        __syncthreads();
+        if (tid < z * z) {
+            const int a = tid % z, b = tid / z;
+            double2 g = G[MIDX(pc[a], pc[b], N)];
+            for (int m = 0; m < k; ++m) g = cfma(s_ap[a][m], s_bp[b][m], g);
+            s_g[tid] = g;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            const int is = cf[p];
+            const int iflip = (int)ceil(plq_stream(rw[2 * kp]) * (lc - 1));
+            const int isp = (is + iflip - 1) % lc + 1;
+            const int k2 = (is - 1) * (lc - 1) + (iflip - 1);
+            const double2* dl = md.plq_delta + (size_t)k2 * z * z;
+            double2 vu[PLQ_ZMAX * PLQ_ZMAX];
+            for (int a = 0; a < z; ++a)                  // I + (1 - G')(P,P) delta
+                for (int b = 0; b < z; ++b) {
+                    double2 sv = cmk(a == b ? 1.0 : 0.0, 0.0);
+                    for (int q = 0; q < z; ++q) {
+                        const double2 g = s_g[a + z * q];
+                        sv = cfma(cmk((a == q ? 1.0 : 0.0) - g.x, -g.y), dl[q + z * b], sv);
+                    }
+                    vu[a + z * b] = sv;
+                }
+            const double2 ratio1 = small_inv_det(vu, z);
+            for (int a = 0; a < z; ++a)                  // S = delta (I + ...)^-1
+                for (int b = 0; b < z; ++b) {
+                    double2 sv = cmk(0, 0);
+                    for (int q = 0; q < z; ++q) sv = cfma(dl[a + z * q], vu[q + z * b], sv);
+                    s_mat[a + z * b] = sv;
+                }
+            double2 rt = ratio1;
+            for (int f = 1; f < md.nflr; ++f) rt = cmul(rt, ratio1);
+            rt = cmul(cscale(rt, md.plq_gam_ratio[k2]), md.plq_phase_ratio[k2]);
+            const double ra = fabs(cmul(rt, ph).x / ph.x), r = plq_stream(rw[2 * kp + 1]);
+            if (fabs(ra - r) < DQ_NEAR_TIE) nties += 1.0;
+            s_acc = ra > r;
+            if (s_acc) {
+                acc += 1.0;
+                ph = cscale(cmul(ph, rt), 1.0 / sqrt(cmulc(rt, rt).x));
+                cf[p] = isp;
+            }
+        }
+        __syncthreads();
+        if (s_acc) {
+            int pcs[PLQ_ZMAX];
+#pragma unroll
+            for (int a = 0; a < PLQ_ZMAX; ++a) pcs[a] = a < z ? pc[a] : 0;
+            for (int i = tid; i < N; i += blockDim.x) {
+                double2 cc[PLQ_ZMAX], rr[PLQ_ZMAX];
+#pragma unroll
+                for (int a = 0; a < PLQ_ZMAX; ++a)
+                    if (a < z) { cc[a] = G[MIDX(i, pcs[a], N)]; rr[a] = G[MIDX(pcs[a], i, N)]; }
+                for (int m = 0; m < k; ++m) {
+                    const double2 ai = A[MIDX(i, m, N)], bi = B[MIDX(i, m, N)];
+#pragma unroll
+                    for (int a = 0; a < PLQ_ZMAX; ++a)
+                        if (a < z) { cc[a] = cfma(ai, s_bp[a][m], cc[a]); rr[a] = cfma(s_ap[a][m], bi, rr[a]); }
+                }
+#pragma unroll
+                for (int q = 0; q < PLQ_ZMAX; ++q) {
+                    if (q >= z) break;
+                    double2 sv = cmk(0, 0);
+#pragma unroll
+                    for (int a = 0; a < PLQ_ZMAX; ++a) if (a < z) sv = cfma(cc[a], s_mat[a + z * q], sv);
+                    double2 r = rr[q];
+                    if (i == pcs[q]) r.x -= 1.0;
+                    A[MIDX(i, k + q, N)] = sv;
+                    B[MIDX(i, k + q, N)] = r;
+                }
+            }
+            k += z;
+            __syncthreads();
+        }
+        if (dir) {
+            const double2* M = md.plq_bmat + (size_t)(cf[p] - 1) * z * z;
+            const double2* Mi = md.plq_bmat_inv + (size_t)(cf[p] - 1) * z * z;
+            plq_cols(G, N, pc, z, M);
+            if (k) plq_rows(B, N, k, pc, z, M, true);
+            plq_rows(G, N, N, pc, z, Mi);
+            if (k) plq_rows(A, N, k, pc, z, Mi);
+        }
+        if (k > 0 && (k + z > nbv || kp == lq - 1)) {
+            flush_addto(G, A, B, N, k, dsm);
+            k = 0;
+        }
+    }
+    if (tid == 0) {
+        c.stats[ST_PHASE_RE] = ph.x;
+        c.stats[ST_PHASE_IM] = ph.y;
+        c.stats[ST_ACCP] += acc;
+        c.stats[ST_PROPP] += lq;
+        c.stats[ST_NEAR_TIE] += nties;
     }
 }
 
@@ -441,6 +582,22 @@ void launch_plq_proj_slice(const ChainDev* chains, int nchains, int maxNe, int n
 }
 
 static int g_plq_attr = 0;
+
+static int g_plqd_attr = 0;
+
+// the delayed plaquette updates when every model's flush depth holds one
+// plaquette's z columns; returns 0 without launching otherwise
+int launch_plq_delay(const ChainDev* chains, int nchains, int nublock, int z, int nt, int visit, int dir,
+                     cudaStream_t st) {
+    if (min(nublock, 64) < z) return 0;
+    const size_t smem = UpdGemm::SMEM_ELEMS * sizeof(double2);
+    if (!g_plqd_attr) {
+        cudaFuncSetAttribute(k_plq_delay, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        g_plqd_attr = 1;
+    }
+    k_plq_delay<<<nchains, PLQ_NT, smem, st>>>(chains, nt, visit, dir);
+    return 1;
+}
 
 void launch_plq_slice(const ChainDev* chains, int nchains, int maxN, int nt, int visit, int dir, int lupdate,
                       cudaStream_t st) {

@@ -26,6 +26,10 @@ void launch_vbond_slice(const ChainDev* chains, int nchains, int maxN, int nt, i
 // launching when nublock leaves fewer than two delayed columns
 int launch_vbond_delay(const ChainDev* chains, int nchains, int nublock, int nt, int nf, int visit, int dir,
                        cudaStream_t st);
+// the same delayed (lupdate = 1; the accepted changes flushed by a DMMA GEMM);
+// returns 0 without launching when nublock < z
+int launch_plq_delay(const ChainDev* chains, int nchains, int nublock, int z, int nt, int visit, int dir,
+                     cudaStream_t st);
 // the same on the projective path (UR, UL^T, ULRINV)
 void launch_plq_proj_slice(const ChainDev* chains, int nchains, int maxNe, int nt, int visit, int dir, int lupdate,
                            cudaStream_t st);
