@@ -228,6 +228,7 @@ __global__ void __launch_bounds__(PLQ_NT, 2) k_plq_delay(const ChainDev* __restr
     __shared__ double2 s_ap[PLQ_ZMAX][64], s_bp[PLQ_ZMAX][64];   // A(P_a, m), B(P_a, m)
     __shared__ double2 s_g[PLQ_ZMAX * PLQ_ZMAX];       // G'(P,P), column-major
     __shared__ double2 s_mat[PLQ_ZMAX * PLQ_ZMAX];
+    __shared__ double2 s_vu[PLQ_ZMAX * PLQ_ZMAX];     // thread 0's z x z work matrix
     __shared__ int s_acc;
     const ChainDev& c = chains[blockIdx.x];
     const ModelDev& md = *c.md;
@@ -272,7 +273,7 @@ __global__ void __launch_bounds__(PLQ_NT, 2) k_plq_delay(const ChainDev* __restr
             const int isp = (is + iflip - 1) % lc + 1;
             const int k2 = (is - 1) * (lc - 1) + (iflip - 1);
             const double2* dl = md.plq_delta + (size_t)k2 * z * z;
-            double2 vu[PLQ_ZMAX * PLQ_ZMAX];
+            double2* vu = s_vu;
             for (int a = 0; a < z; ++a)                  // I + (1 - G')(P,P) delta
                 for (int b = 0; b < z; ++b) {
                     double2 sv = cmk(a == b ? 1.0 : 0.0, 0.0);
