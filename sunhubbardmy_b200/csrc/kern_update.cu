@@ -35,9 +35,11 @@ struct UpdWin {
     int r, wend;                 // accepted sites; sites the walk consumed
 };
 static_assert(sizeof(UpdWin) % 16 == 0, "window state alignment");
-// the window state plus the staged rows (2 UPD_CH nb <= 2 UPD_CH 64 values) fit the staging buffer
-static_assert(sizeof(UpdWin) + 2 * UPD_CH * 64 * sizeof(double2) <= UpdGemm::SMEM_ELEMS * sizeof(double2),
-              "window state must fit the staging buffer");
+// dynamic shared memory of the update kernel: the window state plus the staged
+// rows (2 UPD_CH nb <= 2 UPD_CH 64 values), or the flush staging, whichever is larger
+constexpr size_t UPD_WIN_BYTES = sizeof(UpdWin) + 2 * UPD_CH * 64 * sizeof(double2);
+constexpr size_t UPD_SMEM_BYTES = UPD_WIN_BYTES > UpdGemm::SMEM_ELEMS * sizeof(double2)
+                                      ? UPD_WIN_BYTES : UpdGemm::SMEM_ELEMS * sizeof(double2);
 
 // One CTA per chain; the slice's sites are visited in windows of UPD_L:
 //   1. the window block of the current G' = G + A B^T (A, B: the k delayed
@@ -412,7 +414,7 @@ int launch_vbond_delay(const ChainDev* chains, int nchains, int nublock, int nt,
 static int g_upd_attr = 0;
 
 void launch_update(const ChainDev* chains, int nchains, int nt, int visit, cudaStream_t st, int forced, int dir) {
-    size_t smem = UpdGemm::SMEM_ELEMS * sizeof(double2);
+    size_t smem = UPD_SMEM_BYTES;
     if (!g_upd_attr) {
         cudaFuncSetAttribute(k_update_delay, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         g_upd_attr = 1;
